@@ -1,0 +1,269 @@
+/*
+ * photon_cuda.h — C ABI of the B200 (sm_100a) path-tracing device.
+ *
+ * This is the boundary a host renderer binds to: plain pointers, sizes and
+ * status codes, no C++ or torch types.  It fills the empty CUDA slot of the
+ * reference engine's render-device interface:
+ *
+ *   reference interface                                      replaced by
+ *   ---------------------------------------------------------------------------
+ *   RenderDevice::info / features (src/engine/render_device.h:69-70)
+ *                                                            pe_device_info
+ *   RenderDevice::setScene / updateScene (render_device.h:74-79)
+ *                                                            pe_device_set_scene
+ *   RenderDevice::render (render_device.h:84-85)             pe_device_render
+ *   createDevice("cuda:N", &error) (src/engine/render_device.cpp:110-157)
+ *                                                            pe_device_create
+ *   probeCudaDevices() usable=false (src/engine/gpu_probe.cpp:85-127)
+ *                                                            pe_device_count
+ *   Scene::addShape / addLight / setEnvironment / buildAccelerator
+ *     (src/engine/scene.cpp:18-185)                          pe_scene_*
+ *   Film::addBatch (src/core/image/film.cpp:119-137)         accumulation done by
+ *                                                            pe_device_render into
+ *                                                            caller-owned arrays
+ *
+ * Errors: every call returns a pe_status (0 = PE_OK) or a NULL handle; the
+ * message of the last failure on the calling thread is pe_last_error().
+ * No exception crosses this boundary.  Device handles are independent, so
+ * two threads may drive two devices concurrently (as the reference's hybrid
+ * device does); one handle must not be driven by two threads at once.
+ */
+#ifndef PHOTON_CUDA_H
+#define PHOTON_CUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PE_ABI_VERSION 1
+
+typedef enum pe_status {
+    PE_OK = 0,
+    PE_ERR_INVALID = 1,   /* bad argument or handle */
+    PE_ERR_CUDA = 2,      /* CUDA runtime error */
+    PE_ERR_NO_SCENE = 3,  /* render before set_scene */
+    PE_ERR_CANCELLED = 4, /* cancel flag seen; film holds whole samples only */
+    PE_ERR_OOM = 5,       /* device memory exhausted */
+    PE_ERR_DEVICE = 6,    /* kernel reported an error status (bounded wait, bounds) */
+    PE_ERR_LIMIT = 7      /* request larger than a documented maximum */
+} pe_status;
+
+/* ---- materials (src/materials) ------------------------------------------- */
+enum {
+    PE_MAT_LAMBERT = 0,    /* Lambertian (src/materials/lambertian.h:17)          */
+    PE_MAT_DISNEY = 1,     /* DisneyMaterial (src/materials/disney.h:24)          */
+    PE_MAT_DIELECTRIC = 2, /* Dielectric (src/materials/dielectric.h)             */
+    PE_MAT_MIRROR = 3      /* Mirror (src/materials/mirror.h)                     */
+};
+
+/* Resolved, texture-free material parameters.  Field meaning and clamping
+ * follow the reference setters (disney.h:50-160, dielectric.h).  Fill with
+ * pe_material_defaults() and override. */
+typedef struct pe_material {
+    int32_t type;
+    float base_color[3]; /* lambert albedo | disney base | dielectric tint | mirror reflectance */
+    float emission[3];
+    /* Disney / OpenPBR */
+    float metallic, roughness, specular;
+    float clearcoat, clearcoat_roughness;
+    float ior, spec_transmission, coat_ior;
+    float coat_tint[3];
+    float sheen_color[3];
+    int32_t has_sheen_color;
+    float anisotropy, sheen, sheen_roughness;
+    float diffuse_roughness, diffuse_transmission;
+    float subsurface;
+    float subsurface_radius[3];
+    float subsurface_scale, subsurface_anisotropy;
+    float edge_tint[3];
+    float thin_film_thickness, thin_film_ior;
+    float flake_density, flake_size, flake_roughness;
+    float flake_color[3];
+    float opacity;
+    /* Dielectric */
+    float glass_roughness;
+    float abbe;
+    float absorb_color[3];
+    float absorb_distance;
+    float scatter_density;
+    float scatter_color[3];
+    float scatter_anisotropy;
+    int32_t thin_walled;
+    float film_thickness;
+    int32_t has_absorption; /* setAbsorption called (builds the interior medium) */
+    int32_t has_scattering; /* setScattering called */
+} pe_material;
+
+/* Camera as the reference's Camera::describeGpu() (src/camera/camera.h:17-29). */
+typedef struct pe_camera {
+    float position[3];
+    float lower_left[3];
+    float horizontal[3];
+    float vertical[3];
+    float u[3];
+    float v[3];
+    float forward[3];
+    float lens_radius;
+    int32_t orthographic;
+} pe_camera;
+
+enum { PE_FILTER_BOX = 0, PE_FILTER_TRIANGLE = 1, PE_FILTER_GAUSSIAN = 2, PE_FILTER_BLACKMAN_HARRIS = 3 };
+enum { PE_BG_ENVIRONMENT = 0, PE_BG_COLOR = 1, PE_BG_TRANSPARENT = 2 };
+
+/* RenderSettings subset that changes the estimator (src/engine/render_settings.h:19-47). */
+typedef struct pe_settings {
+    int32_t width, height;
+    int32_t max_bounces;    /* PathTracer maxDepth */
+    int32_t rr_depth;       /* Russian roulette after this depth (reference: 3) */
+    int32_t shadow_quality; /* NEE samples per vertex */
+    int32_t filter_type;    /* PE_FILTER_* */
+    float filter_width;
+    float clamp_indirect;   /* 0 = off */
+    uint64_t seed;          /* Owen-Sobol seed (reference renderSamples: 12345) */
+} pe_settings;
+
+/* ---- scene builder --------------------------------------------------------- */
+typedef struct pe_scene pe_scene;
+
+typedef struct pe_scene_info {
+    uint64_t triangles;
+    uint64_t bvh_nodes;   /* interior nodes of the flattened BVH */
+    uint64_t bvh_leaves;
+    uint64_t lights;      /* explicit lights incl. one per emissive triangle */
+    uint64_t light_bvh_nodes;
+    uint64_t device_bytes;
+    int32_t has_environment;
+    int32_t light_sampler_mode; /* 0 uniform, 1 exhaustive, 2 light BVH */
+} pe_scene_info;
+
+void pe_material_defaults(int32_t type, pe_material* out);
+pe_scene* pe_scene_create(void);
+void pe_scene_destroy(pe_scene* s);
+/* Returns the material index (>= 0) or -1. */
+int32_t pe_scene_add_material(pe_scene* s, const pe_material* m);
+/* Scene::addShape(TriangleMesh) — normals/uvs may be NULL (normals are then
+ * computed as in TriangleMesh::calculateNormals, src/geometry/mesh.cpp:30-55).
+ * An emissive material registers one triangle light per triangle. */
+int32_t pe_scene_add_mesh(pe_scene* s, const float* positions, uint32_t n_vertices, const float* normals,
+                          const float* uvs, const uint32_t* indices, uint32_t n_triangles, int32_t material);
+/* Scene::addLight(AreaLight) — rectangle p + s*u + t*v, two-sided, plus its
+ * two emissive triangles in the BVH (src/engine/scene.cpp:65-99). */
+int32_t pe_scene_add_area_light(pe_scene* s, const float p[3], const float u[3], const float v[3],
+                                const float radiance[3], int32_t visible_to_camera);
+/* EnvironmentLight(image, rotation, intensity) (src/lights/environment_light.cpp:64).
+ * rgb == NULL gives the constant grey environment of the reference. */
+int32_t pe_scene_set_environment(pe_scene* s, const float* rgb, int32_t width, int32_t height, float rotation,
+                                 float intensity);
+/* EnvironmentLight::setSun (environment_light.cpp:211-227). */
+int32_t pe_scene_set_sun(pe_scene* s, const float direction[3], float cos_max, const float radiance[3]);
+/* Scene::setBackground (src/engine/scene.h:41). */
+int32_t pe_scene_set_background(pe_scene* s, int32_t mode, const float color[3]);
+/* Scene::buildAccelerator: SAH BVH, light sampler, environment CDFs. */
+int32_t pe_scene_build(pe_scene* s);
+int32_t pe_scene_get_info(const pe_scene* s, pe_scene_info* out);
+
+/* PerspectiveCamera(position, target, up, vfov, aspect) → pe_camera
+ * (src/camera/perspective_camera.cpp:12-32). */
+void pe_camera_perspective(const float position[3], const float target[3], const float up[3], float vfov_deg,
+                           float aspect, pe_camera* out);
+
+/* ---- device ---------------------------------------------------------------- */
+typedef struct pe_device pe_device;
+
+typedef struct pe_device_info {
+    char name[128];
+    uint64_t memory_bytes;
+    int32_t compute_major, compute_minor;
+    int32_t sm_count;
+    int32_t usable;
+    int32_t feature_aovs, feature_light_passes, feature_adaptive;
+} pe_device_info;
+
+typedef struct pe_render_stats {
+    uint64_t paths;            /* camera samples traced */
+    uint64_t closest_rays;     /* closest-hit segments */
+    uint64_t shadow_rays;      /* any-hit segments */
+    uint64_t rejected;         /* non-finite / negative samples counted black */
+    uint64_t waves;
+    float ms_total;            /* device time of the last render call */
+    float ms_intersect;        /* device time in closest-hit traversal */
+    float ms_shadow;           /* device time in any-hit traversal */
+    float ms_shade;
+    uint64_t intersect_launches;
+    uint64_t node_visits;      /* only when counting is enabled */
+    uint64_t tri_tests;
+    uint32_t error_flags;      /* kernel error word (0 = none) */
+} pe_render_stats;
+
+const char* pe_last_error(void);
+int32_t pe_abi_version(void);
+int32_t pe_device_count(void);
+pe_device* pe_device_create(int32_t ordinal, char* err, size_t err_len);
+void pe_device_destroy(pe_device* d);
+int32_t pe_device_info_get(pe_device* d, pe_device_info* out);
+int32_t pe_device_set_scene(pe_device* d, const pe_scene* s);
+int32_t pe_device_has_scene(pe_device* d);
+
+/* RenderDevice::render: adds samples [first_sample, first_sample+count) to every
+ * pixel and accumulates into the caller's host arrays exactly as
+ * Film::addBatch would (sum_rgb: w*h*3 floats, sample_count: w*h, sum_lum_sq:
+ * w*h, may be NULL).  cancel (may be NULL) is polled between waves; a
+ * cancelled call returns PE_ERR_CANCELLED after adding only whole waves. */
+int32_t pe_device_render(pe_device* d, const pe_camera* cam, const pe_settings* st, int32_t first_sample,
+                         int32_t count, const volatile int32_t* cancel, float* sum_rgb, uint32_t* sample_count,
+                         float* sum_lum_sq, uint64_t* samples_traced);
+
+/* Same, accumulating into the device-resident film (kept across calls until
+ * pe_device_film_clear; resized/cleared when width/height change). */
+int32_t pe_device_render_resident(pe_device* d, const pe_camera* cam, const pe_settings* st, int32_t first_sample,
+                                  int32_t count, const volatile int32_t* cancel);
+int32_t pe_device_film_clear(pe_device* d);
+int32_t pe_device_film_read(pe_device* d, float* sum_rgb, uint32_t* sample_count, float* sum_lum_sq);
+int32_t pe_device_synchronize(pe_device* d);
+int32_t pe_device_last_stats(pe_device* d, pe_render_stats* out);
+/* 1 = count BVH node visits and triangle tests in traversal kernels (slower). */
+int32_t pe_device_set_counting(pe_device* d, int32_t enabled);
+
+/* ---- diagnostics used by parity tests --------------------------------------- */
+/* Camera ray of (x, y, sample_index) for every pixel, then closest hit:
+ * shape index (mesh/area-light triangle order of insertion; -1 = miss),
+ * triangle index within the shape, t.  Follows Renderer tracePixel +
+ * BVH::intersect (src/engine/renderer.cpp:139-160, src/geometry/bvh.cpp:322-401). */
+int32_t pe_device_trace_primary(pe_device* d, const pe_camera* cam, const pe_settings* st, int32_t sample_index,
+                                int32_t* out_shape, int32_t* out_prim, float* out_t);
+
+/* Owen-scrambled Sobol values: for each i, (px[i], py[i], index[i]) and
+ * n_dims consecutive 2-D dimensions → out[i*n_dims*2 + 2*k + {0,1}]. */
+int32_t pe_device_sobol(pe_device* d, uint64_t seed, const int32_t* px, const int32_t* py, const int32_t* index,
+                        size_t n, int32_t n_dims, float* out);
+
+/* BSDF probe: evaluates or samples material m of the current scene at a
+ * synthetic shading point. */
+typedef struct pe_bsdf_query {
+    float wo[3], wi[3];
+    float normal[3], ng[3], tangent[3], point[3];
+    int32_t front_face;
+    float wavelength;
+    float uc, u[2];
+} pe_bsdf_query;
+
+typedef struct pe_bsdf_result {
+    float f[3];
+    float pdf;
+    int32_t sampled;  /* sample: success */
+    float wi[3];      /* sample: direction */
+    float sf[3];      /* sample: f */
+    float spdf;       /* sample: pdf */
+    int32_t delta, pass_through, subsurface;
+    float weight[3];  /* sample: subsurface weight */
+} pe_bsdf_result;
+
+int32_t pe_device_bsdf_probe(pe_device* d, int32_t material, const pe_bsdf_query* q, size_t n, pe_bsdf_result* out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PHOTON_CUDA_H */

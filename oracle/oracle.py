@@ -1,0 +1,197 @@
+"""TEST INFRASTRUCTURE (oracle) — not part of the product.
+
+ctypes driver of the reference engine's own CPU path (``_ref/libphoton_ref.so``, built from the
+reference sources by ``oracle/Makefile``) and of the C restatement (``_ref/libpe_oracle.so``).
+Only tests/, ``__graft_entry__.smoke()`` and bench.py's CPU-baseline leg use this module, and
+only as the checker / the timed CPU baseline.
+
+``RefScene(scene)`` replays a product ``Scene`` (its recorded ``ops``, environment and
+background) through the reference's Scene API in the same order, so both sides hold the same
+shapes, lights, light indices and BVH input order.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import pathlib
+
+import numpy as np
+
+HERE = pathlib.Path(__file__).resolve().parent
+REF_DIR = HERE / "_ref"
+PARITY_LIB = REF_DIR / "libphoton_ref.so"
+FAST_LIB = REF_DIR / "libphoton_ref_fast.so"
+RESTATEMENT_LIB = REF_DIR / "libpe_oracle.so"
+
+FP = C.POINTER(C.c_float)
+IP = C.POINTER(C.c_int32)
+UP = C.POINTER(C.c_uint32)
+
+_libs: dict = {}
+
+
+def available(fast: bool = False) -> bool:
+    return (FAST_LIB if fast else PARITY_LIB).exists()
+
+
+def _load(fast: bool = False):
+    key = "fast" if fast else "parity"
+    if key in _libs:
+        return _libs[key]
+    path = FAST_LIB if fast else PARITY_LIB
+    if not path.exists():
+        raise RuntimeError(f"{path} missing: build it with `make -C oracle` where the reference sources exist")
+    lib = C.CDLL(str(path))
+    P = C.c_void_p
+    sig = {
+        "ref_scene_create": (P, []),
+        "ref_scene_destroy": (None, [P]),
+        "ref_scene_add_material": (C.c_int32, [P, C.c_void_p]),
+        "ref_scene_add_mesh": (C.c_int32, [P, FP, C.c_uint32, FP, FP, UP, C.c_uint32, C.c_int32]),
+        "ref_scene_add_area_light": (C.c_int32, [P, FP, FP, FP, FP, C.c_int32]),
+        "ref_scene_set_environment": (C.c_int32, [P, FP, C.c_int32, C.c_int32, C.c_float, C.c_float, FP, C.c_float, FP]),
+        "ref_scene_set_background": (C.c_int32, [P, C.c_int32, FP]),
+        "ref_scene_build": (C.c_int32, [P]),
+        "ref_scene_light_count": (C.c_int32, [P]),
+        "ref_scene_light_mode": (C.c_int32, [P]),
+        "ref_camera_perspective": (None, [FP, FP, FP, C.c_float, C.c_float, C.c_void_p]),
+        "ref_render": (C.c_int32, [P, C.c_void_p, C.c_void_p, C.c_int32, C.c_int32, C.c_int32, FP, UP]),
+        "ref_render_seeded": (C.c_int32, [P, C.c_void_p, C.c_void_p, C.c_int32, C.c_int32, C.c_int32, FP, UP]),
+        "ref_trace_primary": (C.c_int32, [P, C.c_void_p, C.c_void_p, C.c_int32, IP, IP, FP]),
+        "ref_sobol": (C.c_int32, [C.c_uint64, IP, IP, IP, C.c_size_t, C.c_int32, FP]),
+        "ref_sobol_1d": (C.c_int32, [C.c_uint64, C.c_int32, C.c_int32, C.c_int32, C.c_int32, FP]),
+        "ref_bsdf_probe": (C.c_int32, [P, C.c_int32, C.c_void_p, C.c_size_t, C.c_void_p]),
+        "ref_light_pick": (C.c_int32, [P, FP, FP, FP, C.c_size_t, IP, FP, FP]),
+        "ref_light_sample": (C.c_int32, [P, C.c_int32, FP, FP, FP, C.c_size_t, FP, FP, FP, FP]),
+        "ref_env_eval": (C.c_int32, [P, FP, C.c_size_t, FP, FP]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _libs[key] = lib
+    return lib
+
+
+def _f(a):
+    return None if a is None else a.ctypes.data_as(FP)
+
+
+def _f3(v):
+    return (C.c_float * 3)(*[float(x) for x in v])
+
+
+class RefScene:
+    """The reference engine's Scene holding the same content as a product Scene."""
+
+    def __init__(self, scene, fast: bool = False):
+        self.lib = _load(fast)
+        self.h = self.lib.ref_scene_create()
+        mat_index = {}
+        for kind, obj in scene.ops:
+            if kind == "mesh" and id(obj.material) not in mat_index:
+                idx = self.lib.ref_scene_add_material(self.h, C.byref(obj.material.struct))
+                if idx < 0:
+                    raise RuntimeError("reference rejected a material")
+                mat_index[id(obj.material)] = idx
+        self.mat_index = mat_index
+        for kind, obj in scene.ops:
+            if kind == "mesh":
+                rc = self.lib.ref_scene_add_mesh(self.h, _f(obj.positions), obj.positions.shape[0], _f(obj.normals),
+                                                 _f(obj.uvs), obj.indices.ctypes.data_as(UP), obj.indices.shape[0],
+                                                 mat_index[id(obj.material)])
+            else:
+                rc = self.lib.ref_scene_add_area_light(self.h, _f3(obj.position), _f3(obj.u), _f3(obj.v),
+                                                       _f3(obj.radiance), 1 if obj.visible_to_camera else 0)
+            if rc != 0:
+                raise RuntimeError("reference rejected a shape")
+        env = scene.environment
+        if env is not None:
+            img = env.image
+            sun = env.sun
+            self.lib.ref_scene_set_environment(self.h, _f(img), 0 if img is None else img.shape[1],
+                                               0 if img is None else img.shape[0], env.rotation, env.intensity,
+                                               _f3(sun[0]) if sun else None, sun[1] if sun else 1.0,
+                                               _f3(sun[2]) if sun else None)
+        self.lib.ref_scene_set_background(self.h, int(scene.background.mode), _f3(scene.background.color))
+        self.lib.ref_scene_build(self.h)
+
+    def __del__(self):
+        try:
+            self.lib.ref_scene_destroy(self.h)
+        except Exception:
+            pass
+
+    def light_count(self) -> int:
+        return self.lib.ref_scene_light_count(self.h)
+
+    def light_mode(self) -> int:
+        return self.lib.ref_scene_light_mode(self.h)
+
+    def render(self, camera, settings, first: int, count: int, threads: int = 0, seeded: bool = True):
+        """Mean image (h, w, 3) and counts of samples [first, first+count).  ``seeded`` runs the
+        tracePixel loop with settings.seed; otherwise Renderer::renderSamples (seed 12345)."""
+        h, w = settings.height, settings.width
+        mean = np.zeros((h, w, 3), np.float32)
+        cnt = np.zeros((h, w), np.uint32)
+        fn = self.lib.ref_render_seeded if seeded else self.lib.ref_render
+        fn(self.h, C.byref(camera.describe_gpu()), C.byref(settings.to_c()), first, count, threads, _f(mean),
+           cnt.ctypes.data_as(UP))
+        return mean, cnt
+
+    def trace_primary(self, camera, settings, sample_index: int = 0):
+        n = settings.width * settings.height
+        shape = np.empty(n, np.int32)
+        prim = np.empty(n, np.int32)
+        t = np.empty(n, np.float32)
+        self.lib.ref_trace_primary(self.h, C.byref(camera.describe_gpu()), C.byref(settings.to_c()), sample_index,
+                                   shape.ctypes.data_as(IP), prim.ctypes.data_as(IP), _f(t))
+        return shape, prim, t
+
+    def bsdf_probe(self, material, queries, result_type):
+        n = len(queries)
+        q = (type(queries[0]) * n)(*queries)
+        r = (result_type * n)()
+        rc = self.lib.ref_bsdf_probe(self.h, self.mat_index[id(material)], q, n, r)
+        if rc != 0:
+            raise RuntimeError("ref_bsdf_probe failed")
+        return list(r)
+
+    def light_pick(self, p, n, u):
+        p = np.ascontiguousarray(p, np.float32)
+        n = np.ascontiguousarray(n, np.float32)
+        u = np.ascontiguousarray(u, np.float32)
+        k = len(u)
+        idx = np.empty(k, np.int32)
+        pmf = np.empty(k, np.float32)
+        chk = np.empty(k, np.float32)
+        self.lib.ref_light_pick(self.h, _f(p), _f(n), _f(u), k, idx.ctypes.data_as(IP), _f(pmf), _f(chk))
+        return idx, pmf, chk
+
+    def env_eval(self, dirs):
+        dirs = np.ascontiguousarray(dirs, np.float32)
+        k = dirs.shape[0]
+        rgb = np.empty((k, 3), np.float32)
+        pdf = np.empty(k, np.float32)
+        self.lib.ref_env_eval(self.h, _f(dirs), k, _f(rgb), _f(pdf))
+        return rgb, pdf
+
+
+def camera_perspective(position, target, up, vfov, aspect, camera_struct):
+    """The reference PerspectiveCamera's describeGpu() written into ``camera_struct``."""
+    _load().ref_camera_perspective(_f3(position), _f3(target), _f3(up), vfov, aspect, C.byref(camera_struct))
+    return camera_struct
+
+
+def sobol(seed: int, px, py, index, n_dims: int) -> np.ndarray:
+    px = np.ascontiguousarray(px, np.int32)
+    py = np.ascontiguousarray(py, np.int32)
+    index = np.ascontiguousarray(index, np.int32)
+    out = np.empty((len(px), n_dims, 2), np.float32)
+    _load().ref_sobol(seed, px.ctypes.data_as(IP), py.ctypes.data_as(IP), index.ctypes.data_as(IP), len(px), n_dims,
+                      _f(out))
+    return out
+
+
+def cpu_threads() -> int:
+    return len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else (os.cpu_count() or 1)

@@ -1,0 +1,505 @@
+// ref_shim.cpp — TEST INFRASTRUCTURE (oracle): a C ABI over the reference engine's own CPU
+// path, compiled from the reference sources in place.  Only tests/, __graft_entry__.smoke()
+// and bench.py's CPU-baseline leg load the library built from this file; the product never
+// does.  Each entry point drives the reference's public classes exactly as its own code does:
+//
+//   ref_scene_*      Scene::addShape / addLight / setEnvironment / buildAccelerator
+//                    (src/engine/scene.cpp:18-185), own BVH forced (Scene::setPreferOwnBvh)
+//   ref_render       Renderer::renderSamples (src/engine/renderer.cpp:392-531); seed 12345
+//   ref_render_seeded  the same tile loop as renderSamples with a caller seed: tracePixel
+//                    (renderer.cpp:139-160) → PathTracer::Li → Film::addSample
+//   ref_trace_primary  tracePixel's camera ray + Scene::intersect (bvh.cpp:322-401)
+//   ref_sobol        SobolSampler (src/samplers/sobol_sampler.cpp:111-146)
+//   ref_bsdf_probe   Material::evalPdf / sampleFull (src/materials/*.cpp)
+//   ref_light_*      LightSampler::prepare/sample/pmf (src/lights/light_sampler.cpp:150-284)
+#include "photon_cuda.h"
+
+#include "camera/camera.h"
+#include "camera/perspective_camera.h"
+#include "core/image/film.h"
+#include "core/image/image.h"
+#include "core/image/pixel_filter.h"
+#include "engine/renderer.h"
+#include "engine/scene.h"
+#include "geometry/mesh.h"
+#include "integrators/path_tracer.h"
+#include "lights/area_light.h"
+#include "lights/environment_light.h"
+#include "materials/dielectric.h"
+#include "materials/disney.h"
+#include "materials/lambertian.h"
+#include "materials/mirror.h"
+#include "samplers/sobol_sampler.h"
+
+#include <atomic>
+#include <cstring>
+#include <memory>
+#include <thread>
+#include <unordered_map>
+#include <vector>
+
+using namespace photon;
+
+namespace {
+
+Vec3f v3(const float* p) { return Vec3f(p[0], p[1], p[2]); }
+Color3f c3(const float* p) { return Color3f(p[0], p[1], p[2]); }
+
+// Camera whose rays are exactly PerspectiveCamera::generateRay for the given GPU description
+// (perspective_camera.cpp:36-40); cone helpers come from Camera (camera.h:95-110).
+class DescCamera : public Camera {
+public:
+    explicit DescCamera(const pe_camera& c) {
+        m_d.position = v3(c.position);
+        m_d.lowerLeft = v3(c.lower_left);
+        m_d.horizontal = v3(c.horizontal);
+        m_d.vertical = v3(c.vertical);
+        m_d.u = v3(c.u);
+        m_d.v = v3(c.v);
+        m_d.forward = v3(c.forward);
+        m_d.lensRadius = 0.0f;
+        m_d.orthographic = false;
+    }
+    Ray generateRay(float u, float v, const Vec2f&) const override {
+        Vec3f targetPoint = m_d.lowerLeft + u * m_d.horizontal + v * m_d.vertical;
+        Vec3f direction = (targetPoint - m_d.position).normalized();
+        return Ray(m_d.position, direction);
+    }
+    CameraGpuDesc describeGpu() const override { return m_d; }
+
+private:
+    CameraGpuDesc m_d;
+};
+
+struct RefScene {
+    Scene scene;
+    std::vector<std::shared_ptr<Material>> materials;
+    std::unordered_map<const void*, int> shapeIndex; // hitObject → insertion index
+    int nextShape = 0;
+    void indexNewShapes() {
+        const auto& shapes = scene.shapes();
+        for (size_t i = static_cast<size_t>(nextShape); i < shapes.size(); ++i)
+            shapeIndex[shapes[i].get()] = static_cast<int>(i);
+        nextShape = static_cast<int>(shapes.size());
+    }
+};
+
+std::shared_ptr<Material> makeMaterial(const pe_material& m) {
+    switch (m.type) {
+        case PE_MAT_LAMBERT:
+            return std::make_shared<Lambertian>(c3(m.base_color), c3(m.emission));
+        case PE_MAT_DISNEY: {
+            auto d = std::make_shared<DisneyMaterial>(c3(m.base_color), m.metallic, m.roughness, m.specular);
+            d->setClearCoat(m.clearcoat);
+            d->setClearCoatRoughness(m.clearcoat_roughness);
+            d->setIor(m.ior);
+            d->setSpecularTransmission(m.spec_transmission);
+            d->setCoatIor(m.coat_ior);
+            d->setCoatTint(c3(m.coat_tint));
+            if (m.has_sheen_color) d->setSheenColor(c3(m.sheen_color));
+            d->setAnisotropy(m.anisotropy);
+            d->setSheen(m.sheen);
+            d->setSheenRoughness(m.sheen_roughness);
+            d->setDiffuseRoughness(m.diffuse_roughness);
+            d->setDiffuseTransmission(m.diffuse_transmission);
+            d->setSubsurface(m.subsurface);
+            d->setSubsurfaceRadius(c3(m.subsurface_radius));
+            d->setSubsurfaceScale(m.subsurface_scale);
+            d->setSubsurfaceAnisotropy(m.subsurface_anisotropy);
+            d->setEdgeTint(c3(m.edge_tint));
+            d->setThinFilm(m.thin_film_thickness, m.thin_film_ior);
+            if (m.flake_density > 0.0f) d->setFlakes(m.flake_density, m.flake_size, m.flake_roughness, c3(m.flake_color));
+            d->setEmission(c3(m.emission));
+            d->setOpacity(m.opacity);
+            return d;
+        }
+        case PE_MAT_DIELECTRIC: {
+            auto g = std::make_shared<Dielectric>(m.ior, c3(m.base_color), m.glass_roughness);
+            g->setAbbe(m.abbe);
+            if (m.has_absorption) g->setAbsorption(c3(m.absorb_color), m.absorb_distance);
+            if (m.has_scattering) g->setScattering(m.scatter_density, c3(m.scatter_color), m.scatter_anisotropy);
+            g->setThinWalled(m.thin_walled != 0);
+            g->setThinFilm(m.film_thickness);
+            return g;
+        }
+        case PE_MAT_MIRROR:
+            return std::make_shared<Mirror>(c3(m.base_color));
+        default:
+            return nullptr;
+    }
+}
+
+RenderSettings toSettings(const pe_settings& st, int threads) {
+    RenderSettings s;
+    s.width = st.width;
+    s.height = st.height;
+    s.samplesPerPixel = 1;
+    s.maxBounces = st.max_bounces;
+    s.shadowQuality = st.shadow_quality;
+    s.filter.type = static_cast<PixelFilterType>(st.filter_type);
+    s.filter.width = st.filter_width;
+    s.clampIndirect = st.clamp_indirect;
+    s.numThreads = threads;
+    return s;
+}
+
+int hardwareThreads() {
+    const unsigned n = std::thread::hardware_concurrency();
+    return n > 0 ? static_cast<int>(n) : 1;
+}
+
+void exportFilm(const Film& film, int w, int h, float* sum, uint32_t* count) {
+    // Film keeps sum/count private; resolvedPixel × count recovers the sum exactly when the
+    // caller only needs the mean, so the mean image and the counts are exported instead.
+    for (int y = 0; y < h; ++y)
+        for (int x = 0; x < w; ++x) {
+            const size_t i = static_cast<size_t>(y) * static_cast<size_t>(w) + static_cast<size_t>(x);
+            const Color3f c = film.resolvedPixel(x, y);
+            if (sum) {
+                sum[3 * i + 0] = c.r;
+                sum[3 * i + 1] = c.g;
+                sum[3 * i + 2] = c.b;
+            }
+            if (count) count[i] = static_cast<uint32_t>(film.sampleCount(x, y));
+        }
+}
+
+} // namespace
+
+extern "C" {
+
+void* ref_scene_create() {
+    Scene::setPreferOwnBvh(true);
+    return new RefScene();
+}
+
+void ref_scene_destroy(void* s) { delete static_cast<RefScene*>(s); }
+
+int32_t ref_scene_add_material(void* s, const pe_material* m) {
+    auto* rs = static_cast<RefScene*>(s);
+    auto mat = makeMaterial(*m);
+    if (!mat) return -1;
+    rs->materials.push_back(mat);
+    rs->scene.retainMaterial(mat);
+    return static_cast<int32_t>(rs->materials.size() - 1);
+}
+
+int32_t ref_scene_add_mesh(void* s, const float* pos, uint32_t nv, const float* nrm, const float* uv,
+                           const uint32_t* idx, uint32_t ntri, int32_t material) {
+    auto* rs = static_cast<RefScene*>(s);
+    if (material < 0 || material >= static_cast<int32_t>(rs->materials.size())) return -1;
+    std::vector<Vec3f> p(nv), n;
+    std::vector<Vec2f> t;
+    for (uint32_t i = 0; i < nv; ++i) p[i] = v3(pos + 3 * i);
+    if (nrm) {
+        n.resize(nv);
+        for (uint32_t i = 0; i < nv; ++i) n[i] = v3(nrm + 3 * i);
+    }
+    if (uv) {
+        t.resize(nv);
+        for (uint32_t i = 0; i < nv; ++i) t[i] = Vec2f(uv[2 * i], uv[2 * i + 1]);
+    }
+    std::vector<uint32_t> ind(idx, idx + 3 * static_cast<size_t>(ntri));
+    auto mesh = std::make_shared<TriangleMesh>(p, n, t, ind, rs->materials[static_cast<size_t>(material)].get());
+    rs->scene.addShape(mesh);
+    rs->indexNewShapes();
+    return 0;
+}
+
+int32_t ref_scene_add_area_light(void* s, const float* p, const float* u, const float* v, const float* radiance,
+                                 int32_t visible) {
+    auto* rs = static_cast<RefScene*>(s);
+    auto a = std::make_shared<AreaLight>(v3(p), v3(u), v3(v), c3(radiance));
+    a->setVisibleToCamera(visible != 0);
+    rs->scene.addLight(a);
+    rs->indexNewShapes();
+    return 0;
+}
+
+int32_t ref_scene_set_environment(void* s, const float* rgb, int32_t w, int32_t h, float rotation, float intensity,
+                                  const float* sun_dir, float sun_cos_max, const float* sun_radiance) {
+    auto* rs = static_cast<RefScene*>(s);
+    std::shared_ptr<Image> img;
+    if (rgb && w > 0 && h > 0) {
+        img = std::make_shared<Image>(w, h);
+        for (int y = 0; y < h; ++y)
+            for (int x = 0; x < w; ++x) {
+                const float* px = rgb + 3 * (static_cast<size_t>(y) * static_cast<size_t>(w) + static_cast<size_t>(x));
+                img->setPixel(x, y, Color3f(px[0], px[1], px[2]));
+            }
+    }
+    auto env = std::make_shared<EnvironmentLight>(img, rotation, intensity);
+    if (sun_dir) env->setSun(v3(sun_dir), sun_cos_max, c3(sun_radiance));
+    rs->scene.setEnvironment(env);
+    return 0;
+}
+
+int32_t ref_scene_set_background(void* s, int32_t mode, const float* color) {
+    auto* rs = static_cast<RefScene*>(s);
+    Background bg;
+    bg.mode = static_cast<Background::Mode>(mode);
+    bg.color = c3(color);
+    rs->scene.setBackground(bg);
+    return 0;
+}
+
+int32_t ref_scene_build(void* s) {
+    auto* rs = static_cast<RefScene*>(s);
+    rs->scene.buildAccelerator();
+    return 0;
+}
+
+int32_t ref_scene_light_count(void* s) {
+    return static_cast<int32_t>(static_cast<RefScene*>(s)->scene.lights().size());
+}
+
+int32_t ref_scene_light_mode(void* s) {
+    const LightSampler& ls = static_cast<RefScene*>(s)->scene.lightSampler();
+    return ls.usesBvh() ? 2 : 1;
+}
+
+void ref_camera_perspective(const float* pos, const float* target, const float* up, float vfov, float aspect,
+                            pe_camera* out) {
+    PerspectiveCamera cam(v3(pos), v3(target), v3(up), vfov, aspect);
+    const CameraGpuDesc d = cam.describeGpu();
+    auto put = [](float* o, const Vec3f& v) { o[0] = v.x; o[1] = v.y; o[2] = v.z; };
+    put(out->position, d.position);
+    put(out->lower_left, d.lowerLeft);
+    put(out->horizontal, d.horizontal);
+    put(out->vertical, d.vertical);
+    put(out->u, d.u);
+    put(out->v, d.v);
+    put(out->forward, d.forward);
+    out->lens_radius = d.lensRadius;
+    out->orthographic = d.orthographic ? 1 : 0;
+}
+
+// Renderer::renderSamples — the reference's own CPU render path (seed fixed at 12345 there).
+// Returns the mean image and counts.
+int32_t ref_render(void* s, const pe_camera* cam, const pe_settings* st, int32_t first, int32_t count,
+                   int32_t threads, float* mean_rgb, uint32_t* counts) {
+    auto* rs = static_cast<RefScene*>(s);
+    DescCamera camera(*cam);
+    RenderSettings settings = toSettings(*st, threads > 0 ? threads : hardwareThreads());
+    Film film(st->width, st->height);
+    Renderer renderer;
+    renderer.renderSamples(rs->scene, camera, settings, film, first, count, nullptr);
+    exportFilm(film, st->width, st->height, mean_rgb, counts);
+    return 0;
+}
+
+// tracePixel (renderer.cpp:139-160) with a caller-chosen Sobol seed; rows are split over
+// `threads` workers, each pixel accumulating its samples in index order (so the result equals
+// renderSamples' when seed == 12345 and the background mode is Environment).
+int32_t ref_render_seeded(void* s, const pe_camera* cam, const pe_settings* st, int32_t first, int32_t count,
+                          int32_t threads, float* mean_rgb, uint32_t* counts) {
+    auto* rs = static_cast<RefScene*>(s);
+    DescCamera camera(*cam);
+    const int w = st->width, h = st->height;
+    Film film(w, h);
+    PathTracer integrator(st->max_bounces, st->rr_depth, 0.0f, st->shadow_quality);
+    integrator.setClampIndirect(st->clamp_indirect);
+    PixelFilter pf;
+    pf.type = static_cast<PixelFilterType>(st->filter_type);
+    pf.width = st->filter_width;
+    const PixelFilterSampler filter(pf);
+    const int nt = threads > 0 ? threads : hardwareThreads();
+    std::atomic<int> nextRow{0};
+    auto work = [&]() {
+        SobolSampler sampler(st->seed);
+        for (;;) {
+            const int y = nextRow.fetch_add(1);
+            if (y >= h) break;
+            for (int x = 0; x < w; ++x)
+                for (int si = first; si < first + count; ++si) {
+                    sampler.startPixel(x, y);
+                    sampler.startSample(si);
+                    const Vec2f offset = filter.sample(sampler.get2D());
+                    const float sx = (static_cast<float>(x) + 0.5f + offset.x) / static_cast<float>(w);
+                    const float sy = 1.0f - (static_cast<float>(y) + 0.5f + offset.y) / static_cast<float>(h);
+                    const Vec2f lens = sampler.get2D();
+                    Ray ray = camera.generateRay(sx, sy, lens);
+                    ray.coneWidth = camera.pixelConeWidth(h);
+                    ray.coneSpread = camera.pixelConeSpread(h);
+                    film.addSample(x, y, integrator.Li(ray, rs->scene, sampler));
+                }
+        }
+    };
+    std::vector<std::thread> pool;
+    for (int i = 0; i < nt; ++i) pool.emplace_back(work);
+    for (auto& t : pool) t.join();
+    exportFilm(film, w, h, mean_rgb, counts);
+    return 0;
+}
+
+// Primary hit per pixel for one sample index: tracePixel's camera ray, then the first
+// Scene::intersect of PathTracer::Li with the camera visibility mask (path_tracer.cpp:326,420).
+int32_t ref_trace_primary(void* s, const pe_camera* cam, const pe_settings* st, int32_t sample_index,
+                          int32_t* out_shape, int32_t* out_prim, float* out_t) {
+    auto* rs = static_cast<RefScene*>(s);
+    DescCamera camera(*cam);
+    const int w = st->width, h = st->height;
+    PixelFilter pf;
+    pf.type = static_cast<PixelFilterType>(st->filter_type);
+    pf.width = st->filter_width;
+    const PixelFilterSampler filter(pf);
+    const int nt = hardwareThreads();
+    std::atomic<int> nextRow{0};
+    auto work = [&]() {
+        SobolSampler sampler(st->seed);
+        for (;;) {
+            const int y = nextRow.fetch_add(1);
+            if (y >= h) break;
+            for (int x = 0; x < w; ++x) {
+                sampler.startPixel(x, y);
+                sampler.startSample(sample_index);
+                const Vec2f offset = filter.sample(sampler.get2D());
+                const float sx = (static_cast<float>(x) + 0.5f + offset.x) / static_cast<float>(w);
+                const float sy = 1.0f - (static_cast<float>(y) + 0.5f + offset.y) / static_cast<float>(h);
+                const Vec2f lens = sampler.get2D();
+                Ray ray = camera.generateRay(sx, sy, lens);
+                ray.visibilityMask = VisCamera;
+                SurfaceInteraction isect;
+                const size_t i = static_cast<size_t>(y) * static_cast<size_t>(w) + static_cast<size_t>(x);
+                if (rs->scene.intersect(ray, isect)) {
+                    auto it = rs->shapeIndex.find(isect.hitObject);
+                    out_shape[i] = it == rs->shapeIndex.end() ? -2 : it->second;
+                    out_prim[i] = isect.primIndex < 0 ? 0 : isect.primIndex;
+                    out_t[i] = isect.t;
+                } else {
+                    out_shape[i] = -1;
+                    out_prim[i] = -1;
+                    out_t[i] = 0.0f;
+                }
+            }
+        }
+    };
+    std::vector<std::thread> pool;
+    for (int i = 0; i < nt; ++i) pool.emplace_back(work);
+    for (auto& t : pool) t.join();
+    return 0;
+}
+
+int32_t ref_sobol(uint64_t seed, const int32_t* px, const int32_t* py, const int32_t* index, size_t n, int32_t ndims,
+                  float* out) {
+    SobolSampler s(seed);
+    for (size_t i = 0; i < n; ++i) {
+        s.startPixel(px[i], py[i]);
+        s.startSample(index[i]);
+        for (int k = 0; k < ndims; ++k) {
+            const Vec2f v = s.get2D();
+            out[(i * static_cast<size_t>(ndims) + static_cast<size_t>(k)) * 2 + 0] = v.x;
+            out[(i * static_cast<size_t>(ndims) + static_cast<size_t>(k)) * 2 + 1] = v.y;
+        }
+    }
+    return 0;
+}
+
+int32_t ref_sobol_1d(uint64_t seed, int32_t px, int32_t py, int32_t index, int32_t ndims, float* out) {
+    SobolSampler s(seed);
+    s.startPixel(px, py);
+    s.startSample(index);
+    for (int k = 0; k < ndims; ++k) out[k] = s.get1D();
+    return 0;
+}
+
+int32_t ref_bsdf_probe(void* s, int32_t material, const pe_bsdf_query* q, size_t n, pe_bsdf_result* out) {
+    auto* rs = static_cast<RefScene*>(s);
+    if (material < 0 || material >= static_cast<int32_t>(rs->materials.size())) return -1;
+    const Material* m = rs->materials[static_cast<size_t>(material)].get();
+    for (size_t i = 0; i < n; ++i) {
+        SurfaceInteraction si;
+        si.normal = v3(q[i].normal);
+        si.ng = v3(q[i].ng);
+        si.tangent = v3(q[i].tangent);
+        si.point = v3(q[i].point);
+        si.frontFace = q[i].front_face != 0;
+        si.wavelength = q[i].wavelength;
+        si.material = m;
+        pe_bsdf_result r{};
+        float pdf = 0.0f;
+        const Color3f f = m->evalPdf(v3(q[i].wo), v3(q[i].wi), si, pdf);
+        r.f[0] = f.r;
+        r.f[1] = f.g;
+        r.f[2] = f.b;
+        r.pdf = pdf;
+        BSDFSample bs;
+        r.sampled = m->sampleFull(v3(q[i].wo), si, q[i].uc, Vec2f(q[i].u[0], q[i].u[1]), bs) ? 1 : 0;
+        r.wi[0] = bs.wi.x;
+        r.wi[1] = bs.wi.y;
+        r.wi[2] = bs.wi.z;
+        r.sf[0] = bs.f.r;
+        r.sf[1] = bs.f.g;
+        r.sf[2] = bs.f.b;
+        r.spdf = bs.pdf;
+        r.delta = bs.delta;
+        r.pass_through = bs.passThrough;
+        r.subsurface = bs.subsurface;
+        r.weight[0] = bs.weight.r;
+        r.weight[1] = bs.weight.g;
+        r.weight[2] = bs.weight.b;
+        out[i] = r;
+    }
+    return 0;
+}
+
+// LightSampler: for each shading point, prepare() then sample(u) and pmf(index).
+int32_t ref_light_pick(void* s, const float* p, const float* nrm, const float* u, size_t n, int32_t* out_index,
+                       float* out_pmf, float* out_pmf_check) {
+    auto* rs = static_cast<RefScene*>(s);
+    const LightSampler& ls = rs->scene.lightSampler();
+    for (size_t i = 0; i < n; ++i) {
+        const LightSampler::Context c = ls.prepare(v3(p + 3 * i), v3(nrm + 3 * i));
+        float pmf = 0.0f;
+        const int idx = c.sample(u[i], pmf);
+        out_index[i] = idx;
+        out_pmf[i] = pmf;
+        out_pmf_check[i] = idx >= 0 ? c.pmf(idx) : 0.0f;
+    }
+    return 0;
+}
+
+// Light::sampleLi for light `light` (or the environment when light == count) at point p with
+// shading normal n: direction, Li, pdf, distance.
+int32_t ref_light_sample(void* s, int32_t light, const float* p, const float* nrm, const float* u, size_t n,
+                         float* out_wi, float* out_li, float* out_pdf, float* out_dist) {
+    auto* rs = static_cast<RefScene*>(s);
+    const auto& lights = rs->scene.lights();
+    const EnvironmentLight* env = rs->scene.environment();
+    for (size_t i = 0; i < n; ++i) {
+        SurfaceInteraction si;
+        si.point = v3(p + 3 * i);
+        si.normal = v3(nrm + 3 * i);
+        LightSample lsmp;
+        const Vec2f uu(u[2 * i], u[2 * i + 1]);
+        if (light >= 0 && light < static_cast<int32_t>(lights.size())) lsmp = lights[static_cast<size_t>(light)]->sampleLi(si, uu);
+        else if (env) lsmp = env->sampleLi(si, uu);
+        out_wi[3 * i + 0] = lsmp.wi.x;
+        out_wi[3 * i + 1] = lsmp.wi.y;
+        out_wi[3 * i + 2] = lsmp.wi.z;
+        out_li[3 * i + 0] = lsmp.Li.r;
+        out_li[3 * i + 1] = lsmp.Li.g;
+        out_li[3 * i + 2] = lsmp.Li.b;
+        out_pdf[i] = lsmp.pdf;
+        out_dist[i] = lsmp.distance;
+    }
+    return 0;
+}
+
+// EnvironmentLight::eval and pdfLi for directions.
+int32_t ref_env_eval(void* s, const float* dirs, size_t n, float* out_rgb, float* out_pdf) {
+    auto* rs = static_cast<RefScene*>(s);
+    const EnvironmentLight* env = rs->scene.environment();
+    if (!env) return -1;
+    for (size_t i = 0; i < n; ++i) {
+        const Vec3f d = v3(dirs + 3 * i);
+        const Color3f c = env->eval(d);
+        out_rgb[3 * i + 0] = c.r;
+        out_rgb[3 * i + 1] = c.g;
+        out_rgb[3 * i + 2] = c.b;
+        out_pdf[i] = env->pdfLi(d);
+    }
+    return 0;
+}
+
+} // extern "C"

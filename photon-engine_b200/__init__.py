@@ -1,0 +1,12 @@
+"""photon-engine_b200 — B200-native (sm_100a) path-tracing device for the photon engine's render API.
+
+The product is ``libphoton_cuda.so`` (C ABI in ``include/photon_cuda.h``); this package is the
+host-side mirror of the reference's RenderDevice / RenderSession / Scene API over it.
+"""
+from . import _capi
+from .engine import (AreaLight, Background, BackgroundMode, CudaDevice, Dielectric, DeviceFeatures, DeviceInfo,
+                     DisneyMaterial, EnvironmentLight, Film, Lambertian, Material, Mirror, PerspectiveCamera,
+                     PixelFilterType, RenderMode, RenderSession, RenderSettings, RenderTargets, SampleBatchResult,
+                     Scene, SceneUpdateKind, SessionConfig, TriangleMesh, create_device, enumerate_devices, rel_mse)
+
+__all__ = [n for n in dir() if not n.startswith("_")] + ["_capi"]

@@ -1,0 +1,171 @@
+"""ctypes binding of include/photon_cuda.h (the C ABI of libphoton_cuda.so).
+
+The library is built in-tree (``build.py``) and loaded from this folder.  There is no CPU
+fallback: if the library or a CUDA device is missing, the product API raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import pathlib
+
+HERE = pathlib.Path(__file__).resolve().parent
+LIB_PATH = HERE / "libphoton_cuda.so"
+
+PE_OK, PE_ERR_INVALID, PE_ERR_CUDA, PE_ERR_NO_SCENE, PE_ERR_CANCELLED, PE_ERR_OOM, PE_ERR_DEVICE, PE_ERR_LIMIT = range(8)
+STATUS_NAMES = {0: "PE_OK", 1: "PE_ERR_INVALID", 2: "PE_ERR_CUDA", 3: "PE_ERR_NO_SCENE", 4: "PE_ERR_CANCELLED",
+                5: "PE_ERR_OOM", 6: "PE_ERR_DEVICE", 7: "PE_ERR_LIMIT"}
+PE_MAT_LAMBERT, PE_MAT_DISNEY, PE_MAT_DIELECTRIC, PE_MAT_MIRROR = range(4)
+PE_FILTER_BOX, PE_FILTER_TRIANGLE, PE_FILTER_GAUSSIAN, PE_FILTER_BLACKMAN_HARRIS = range(4)
+PE_BG_ENVIRONMENT, PE_BG_COLOR, PE_BG_TRANSPARENT = range(3)
+
+F3 = C.c_float * 3
+
+
+class pe_material(C.Structure):
+    _fields_ = [
+        ("type", C.c_int32), ("base_color", F3), ("emission", F3),
+        ("metallic", C.c_float), ("roughness", C.c_float), ("specular", C.c_float),
+        ("clearcoat", C.c_float), ("clearcoat_roughness", C.c_float),
+        ("ior", C.c_float), ("spec_transmission", C.c_float), ("coat_ior", C.c_float),
+        ("coat_tint", F3), ("sheen_color", F3), ("has_sheen_color", C.c_int32),
+        ("anisotropy", C.c_float), ("sheen", C.c_float), ("sheen_roughness", C.c_float),
+        ("diffuse_roughness", C.c_float), ("diffuse_transmission", C.c_float),
+        ("subsurface", C.c_float), ("subsurface_radius", F3),
+        ("subsurface_scale", C.c_float), ("subsurface_anisotropy", C.c_float),
+        ("edge_tint", F3), ("thin_film_thickness", C.c_float), ("thin_film_ior", C.c_float),
+        ("flake_density", C.c_float), ("flake_size", C.c_float), ("flake_roughness", C.c_float),
+        ("flake_color", F3), ("opacity", C.c_float),
+        ("glass_roughness", C.c_float), ("abbe", C.c_float), ("absorb_color", F3), ("absorb_distance", C.c_float),
+        ("scatter_density", C.c_float), ("scatter_color", F3), ("scatter_anisotropy", C.c_float),
+        ("thin_walled", C.c_int32), ("film_thickness", C.c_float),
+        ("has_absorption", C.c_int32), ("has_scattering", C.c_int32),
+    ]
+
+
+class pe_camera(C.Structure):
+    _fields_ = [("position", F3), ("lower_left", F3), ("horizontal", F3), ("vertical", F3),
+                ("u", F3), ("v", F3), ("forward", F3), ("lens_radius", C.c_float), ("orthographic", C.c_int32)]
+
+
+class pe_settings(C.Structure):
+    _fields_ = [("width", C.c_int32), ("height", C.c_int32), ("max_bounces", C.c_int32), ("rr_depth", C.c_int32),
+                ("shadow_quality", C.c_int32), ("filter_type", C.c_int32), ("filter_width", C.c_float),
+                ("clamp_indirect", C.c_float), ("seed", C.c_uint64)]
+
+
+class pe_scene_info(C.Structure):
+    _fields_ = [("triangles", C.c_uint64), ("bvh_nodes", C.c_uint64), ("bvh_leaves", C.c_uint64),
+                ("lights", C.c_uint64), ("light_bvh_nodes", C.c_uint64), ("device_bytes", C.c_uint64),
+                ("has_environment", C.c_int32), ("light_sampler_mode", C.c_int32)]
+
+
+class pe_device_info(C.Structure):
+    _fields_ = [("name", C.c_char * 128), ("memory_bytes", C.c_uint64), ("compute_major", C.c_int32),
+                ("compute_minor", C.c_int32), ("sm_count", C.c_int32), ("usable", C.c_int32),
+                ("feature_aovs", C.c_int32), ("feature_light_passes", C.c_int32), ("feature_adaptive", C.c_int32)]
+
+
+class pe_render_stats(C.Structure):
+    _fields_ = [("paths", C.c_uint64), ("closest_rays", C.c_uint64), ("shadow_rays", C.c_uint64),
+                ("rejected", C.c_uint64), ("waves", C.c_uint64), ("ms_total", C.c_float),
+                ("ms_intersect", C.c_float), ("ms_shadow", C.c_float), ("ms_shade", C.c_float),
+                ("intersect_launches", C.c_uint64), ("node_visits", C.c_uint64), ("tri_tests", C.c_uint64),
+                ("error_flags", C.c_uint32)]
+
+
+class pe_bsdf_query(C.Structure):
+    _fields_ = [("wo", F3), ("wi", F3), ("normal", F3), ("ng", F3), ("tangent", F3), ("point", F3),
+                ("front_face", C.c_int32), ("wavelength", C.c_float), ("uc", C.c_float), ("u", C.c_float * 2)]
+
+
+class pe_bsdf_result(C.Structure):
+    _fields_ = [("f", F3), ("pdf", C.c_float), ("sampled", C.c_int32), ("wi", F3), ("sf", F3), ("spdf", C.c_float),
+                ("delta", C.c_int32), ("pass_through", C.c_int32), ("subsurface", C.c_int32), ("weight", F3)]
+
+
+# Every symbol include/photon_cuda.h declares, with its ctypes signature.
+P = C.c_void_p
+FP = C.POINTER(C.c_float)
+IP = C.POINTER(C.c_int32)
+UP = C.POINTER(C.c_uint32)
+SIGNATURES = {
+    "pe_last_error": (C.c_char_p, []),
+    "pe_abi_version": (C.c_int32, []),
+    "pe_material_defaults": (None, [C.c_int32, C.POINTER(pe_material)]),
+    "pe_scene_create": (P, []),
+    "pe_scene_destroy": (None, [P]),
+    "pe_scene_add_material": (C.c_int32, [P, C.POINTER(pe_material)]),
+    "pe_scene_add_mesh": (C.c_int32, [P, FP, C.c_uint32, FP, FP, UP, C.c_uint32, C.c_int32]),
+    "pe_scene_add_area_light": (C.c_int32, [P, FP, FP, FP, FP, C.c_int32]),
+    "pe_scene_set_environment": (C.c_int32, [P, FP, C.c_int32, C.c_int32, C.c_float, C.c_float]),
+    "pe_scene_set_sun": (C.c_int32, [P, FP, C.c_float, FP]),
+    "pe_scene_set_background": (C.c_int32, [P, C.c_int32, FP]),
+    "pe_scene_build": (C.c_int32, [P]),
+    "pe_scene_get_info": (C.c_int32, [P, C.POINTER(pe_scene_info)]),
+    "pe_camera_perspective": (None, [FP, FP, FP, C.c_float, C.c_float, C.POINTER(pe_camera)]),
+    "pe_device_count": (C.c_int32, []),
+    "pe_device_create": (P, [C.c_int32, C.c_char_p, C.c_size_t]),
+    "pe_device_destroy": (None, [P]),
+    "pe_device_info_get": (C.c_int32, [P, C.POINTER(pe_device_info)]),
+    "pe_device_set_scene": (C.c_int32, [P, P]),
+    "pe_device_has_scene": (C.c_int32, [P]),
+    "pe_device_render": (C.c_int32, [P, C.POINTER(pe_camera), C.POINTER(pe_settings), C.c_int32, C.c_int32,
+                                     IP, FP, UP, FP, C.POINTER(C.c_uint64)]),
+    "pe_device_render_resident": (C.c_int32, [P, C.POINTER(pe_camera), C.POINTER(pe_settings), C.c_int32, C.c_int32, IP]),
+    "pe_device_film_clear": (C.c_int32, [P]),
+    "pe_device_film_read": (C.c_int32, [P, FP, UP, FP]),
+    "pe_device_synchronize": (C.c_int32, [P]),
+    "pe_device_last_stats": (C.c_int32, [P, C.POINTER(pe_render_stats)]),
+    "pe_device_set_counting": (C.c_int32, [P, C.c_int32]),
+    "pe_device_trace_primary": (C.c_int32, [P, C.POINTER(pe_camera), C.POINTER(pe_settings), C.c_int32, IP, IP, FP]),
+    "pe_device_sobol": (C.c_int32, [P, C.c_uint64, IP, IP, IP, C.c_size_t, C.c_int32, FP]),
+    "pe_device_bsdf_probe": (C.c_int32, [P, C.c_int32, C.POINTER(pe_bsdf_query), C.c_size_t, C.POINTER(pe_bsdf_result)]),
+}
+
+_lib = None
+
+
+def load(path: pathlib.Path | str | None = None) -> C.CDLL:
+    """Loads libphoton_cuda.so (building nothing); raises if it is absent."""
+    global _lib
+    if _lib is not None and path is None:
+        return _lib
+    p = pathlib.Path(path) if path else LIB_PATH
+    if not p.exists():
+        raise RuntimeError(f"{p} is missing: build it with photon-engine_b200/build.py (no CPU fallback exists)")
+    lib = C.CDLL(str(p))
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    if path is None:
+        _lib = lib
+    return lib
+
+
+class PhotonError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__(f"{STATUS_NAMES.get(status, status)}: {message}")
+        self.status = status
+
+
+def check(status: int) -> None:
+    if status != PE_OK:
+        msg = load().pe_last_error()
+        raise PhotonError(status, msg.decode() if msg else "")
+
+
+def fptr(a):
+    return a.ctypes.data_as(FP) if a is not None else None
+
+
+def uptr(a):
+    return a.ctypes.data_as(UP) if a is not None else None
+
+
+def iptr(a):
+    return a.ctypes.data_as(IP) if a is not None else None
+
+
+def f3(v) -> C.Array:
+    return F3(*[float(x) for x in v])

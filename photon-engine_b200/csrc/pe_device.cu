@@ -1,0 +1,777 @@
+// pe_device.cu — the CUDA device behind the pe_device_* C ABI: resident scene upload, the
+// wavefront render loop (RenderDevice::render, src/engine/render_device.h:84-85) and the
+// diagnostics the parity tests call.  Built for sm_100a only.
+#include "photon_cuda.h"
+#include "pe_host.h"
+#include "pe_integrator.cuh"
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <string>
+#include <vector>
+
+using namespace pe;
+
+namespace {
+
+const char* cudaMsg(cudaError_t e) { return cudaGetErrorString(e); }
+
+#define PE_CUDA(call)                                                                              \
+    do {                                                                                           \
+        const cudaError_t err__ = (call);                                                          \
+        if (err__ != cudaSuccess) {                                                                \
+            setError(std::string(#call) + ": " + cudaMsg(err__));                                  \
+            return err__ == cudaErrorMemoryAllocation ? PE_ERR_OOM : PE_ERR_CUDA;                  \
+        }                                                                                          \
+    } while (0)
+
+struct DevBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+};
+
+} // namespace
+
+struct pe_device {
+    int ordinal = 0;
+    cudaStream_t stream = nullptr;
+    cudaDeviceProp prop{};
+    // scene
+    std::vector<DevBuf> sceneBufs;
+    SceneGPU scene{};
+    bool hasScene = false;
+    TablesGPU* dTables = nullptr;
+    TablesGPU hTables{};
+    int filterType = -1;
+    float filterWidth = -1.0f;
+    // wavefront state
+    size_t capacity = 0;
+    std::vector<DevBuf> pathBufs;
+    Paths paths{};
+    unsigned long long* dStats = nullptr; // [0] nodes, [1] tris (closest), [2] nodes, [3] tris (any), [4] rejected
+    uint32_t* hCounters = nullptr;        // pinned
+    // resident film
+    int filmW = 0, filmH = 0;
+    float* fSum = nullptr;
+    uint32_t* fCnt = nullptr;
+    float* fSq = nullptr;
+    // timing
+    cudaEvent_t evStart = nullptr, evStop = nullptr;
+    std::vector<cudaEvent_t> evPool;
+    bool counting = false;
+    pe_render_stats stats{};
+    int blocksIntersect = 0, blocksShade = 0, blocksShadow = 0, blocksGen = 0;
+};
+
+namespace {
+
+template <typename T>
+int32_t devAlloc(std::vector<DevBuf>& list, T*& out, size_t count) {
+    void* p = nullptr;
+    const size_t bytes = std::max<size_t>(count * sizeof(T), 16);
+    const cudaError_t e = cudaMalloc(&p, bytes);
+    if (e != cudaSuccess) {
+        setError(std::string("cudaMalloc(") + std::to_string(bytes) + "): " + cudaMsg(e));
+        return e == cudaErrorMemoryAllocation ? PE_ERR_OOM : PE_ERR_CUDA;
+    }
+    list.push_back({p, bytes});
+    out = static_cast<T*>(p);
+    return PE_OK;
+}
+
+template <typename T>
+int32_t upload(pe_device* d, std::vector<DevBuf>& list, const T*& dst, const std::vector<T>& src) {
+    T* p = nullptr;
+    const int32_t st = devAlloc(list, p, src.size());
+    if (st) return st;
+    if (!src.empty()) PE_CUDA(cudaMemcpyAsync(p, src.data(), src.size() * sizeof(T), cudaMemcpyHostToDevice, d->stream));
+    dst = p;
+    return PE_OK;
+}
+
+void freeList(std::vector<DevBuf>& list) {
+    for (DevBuf& b : list) cudaFree(b.p);
+    list.clear();
+}
+
+int32_t ensureCapacity(pe_device* d, size_t slots) {
+    if (slots <= d->capacity) return PE_OK;
+    freeList(d->pathBufs);
+    d->capacity = 0;
+    Paths& P = d->paths;
+    int32_t st = 0;
+    float4** cols[] = {&P.rayO, &P.rayD, &P.thr, &P.L, &P.lastN, &P.lastP, &P.pickP, &P.pickN, &P.hit};
+    for (float4** c : cols)
+        if ((st = devAlloc(d->pathBufs, *c, slots))) return st;
+    if ((st = devAlloc(d->pathBufs, P.queueA, slots))) return st;
+    if ((st = devAlloc(d->pathBufs, P.queueB, slots))) return st;
+    // shadow records: one per slot and NEE sample (shadow quality <= 4)
+    const size_t sh = slots * 4;
+    if ((st = devAlloc(d->pathBufs, P.shadowQ, sh))) return st;
+    float4** scols[] = {&P.shO, &P.shD, &P.shC, &P.shT};
+    for (float4** c : scols)
+        if ((st = devAlloc(d->pathBufs, *c, sh))) return st;
+    if ((st = devAlloc(d->pathBufs, P.counters, 16))) return st;
+    d->capacity = slots;
+    return PE_OK;
+}
+
+int32_t ensureFilter(pe_device* d, int type, float width) {
+    if (type == d->filterType && width == d->filterWidth) return PE_OK;
+    fillFilterCdf(type, width, d->hTables.filterCdf);
+    PE_CUDA(cudaMemcpyAsync(d->dTables, &d->hTables, sizeof(TablesGPU), cudaMemcpyHostToDevice, d->stream));
+    d->filterType = type;
+    d->filterWidth = width;
+    return PE_OK;
+}
+
+int32_t ensureFilm(pe_device* d, int w, int h) {
+    if (w == d->filmW && h == d->filmH && d->fSum) return PE_OK;
+    cudaFree(d->fSum);
+    cudaFree(d->fCnt);
+    cudaFree(d->fSq);
+    d->fSum = nullptr;
+    d->fCnt = nullptr;
+    d->fSq = nullptr;
+    const size_t n = static_cast<size_t>(w) * static_cast<size_t>(h);
+    PE_CUDA(cudaMalloc(&d->fSum, n * 3 * sizeof(float)));
+    PE_CUDA(cudaMalloc(&d->fCnt, n * sizeof(uint32_t)));
+    PE_CUDA(cudaMalloc(&d->fSq, n * sizeof(float)));
+    PE_CUDA(cudaMemsetAsync(d->fSum, 0, n * 3 * sizeof(float), d->stream));
+    PE_CUDA(cudaMemsetAsync(d->fCnt, 0, n * sizeof(uint32_t), d->stream));
+    PE_CUDA(cudaMemsetAsync(d->fSq, 0, n * sizeof(float), d->stream));
+    d->filmW = w;
+    d->filmH = h;
+    return PE_OK;
+}
+
+int32_t checkSettings(const pe_camera* cam, const pe_settings* st) {
+    if (!cam || !st) {
+        setError("null camera or settings");
+        return PE_ERR_INVALID;
+    }
+    if (st->width <= 0 || st->height <= 0 || st->width > 16384 || st->height > 16384) {
+        setError("film size out of range (1..16384)");
+        return PE_ERR_INVALID;
+    }
+    if (st->shadow_quality < 1 || st->shadow_quality > 1) {
+        setError("shadow_quality other than 1 is not supported by this device");
+        return PE_ERR_LIMIT;
+    }
+    if (cam->orthographic || cam->lens_radius > 0.0f) {
+        setError("only the pinhole perspective camera is supported");
+        return PE_ERR_LIMIT;
+    }
+    return PE_OK;
+}
+
+WaveArgs makeWave(const pe_camera* cam, const pe_settings* st) {
+    WaveArgs A{};
+    A.cam.position = m3f(cam->position);
+    A.cam.lowerLeft = m3f(cam->lower_left);
+    A.cam.horizontal = m3f(cam->horizontal);
+    A.cam.vertical = m3f(cam->vertical);
+    A.width = st->width;
+    A.height = st->height;
+    A.seed = st->seed;
+    A.filterWidth = sclamp(st->filter_width, 0.25f, 8.0f);
+    A.maxDepth = st->max_bounces;
+    A.rrDepth = st->rr_depth;
+    A.shadowSamples = st->shadow_quality < 1 ? 1 : st->shadow_quality;
+    A.clampIndirect = st->clamp_indirect > 0.0f ? st->clamp_indirect : 0.0f;
+    return A;
+}
+
+constexpr size_t kWaveSlots = size_t(1) << 21; // paths in flight per wave
+
+// The wavefront render of samples [first, first+count) into film (sum, cnt, sq) on the device.
+int32_t renderWaves(pe_device* d, const pe_camera* cam, const pe_settings* st, int first, int count,
+                    const volatile int32_t* cancel, float* sum, uint32_t* cnt, float* sq) {
+    const size_t npix = static_cast<size_t>(st->width) * static_cast<size_t>(st->height);
+    const int pixChunk = static_cast<int>(std::min(npix, kWaveSlots));
+    const int samplesPerWave = static_cast<int>(std::max<size_t>(1, std::min<size_t>(static_cast<size_t>(count), kWaveSlots / pixChunk)));
+    int32_t rc = ensureCapacity(d, static_cast<size_t>(samplesPerWave) * static_cast<size_t>(pixChunk));
+    if (rc) return rc;
+    rc = ensureFilter(d, st->filter_type, st->filter_width);
+    if (rc) return rc;
+    WaveArgs A = makeWave(cam, st);
+    const SceneGPU& S = d->scene;
+    Paths& P = d->paths;
+    const int sm = d->prop.multiProcessorCount;
+    pe_render_stats& stats = d->stats;
+    std::memset(&stats, 0, sizeof(stats));
+    PE_CUDA(cudaMemsetAsync(d->dStats, 0, 8 * sizeof(unsigned long long), d->stream));
+    PE_CUDA(cudaEventRecord(d->evStart, d->stream));
+    size_t evUsed = 0;
+    auto event = [&](cudaEvent_t& e) -> int32_t {
+        if (evUsed >= d->evPool.size()) {
+            cudaEvent_t ne;
+            PE_CUDA(cudaEventCreate(&ne));
+            d->evPool.push_back(ne);
+        }
+        e = d->evPool[evUsed++];
+        return PE_OK;
+    };
+    std::vector<std::pair<size_t, size_t>> isectEv, shadowEv, shadeEv;
+    bool cancelled = false;
+    for (int s0 = first; s0 < first + count && !cancelled; s0 += samplesPerWave) {
+        const int ns = std::min(samplesPerWave, first + count - s0);
+        for (size_t p0 = 0; p0 < npix; p0 += static_cast<size_t>(pixChunk)) {
+            if (cancel && *cancel) {
+                cancelled = true;
+                break;
+            }
+            A.pixelFirst = static_cast<int>(p0);
+            A.nPix = static_cast<int>(std::min<size_t>(static_cast<size_t>(pixChunk), npix - p0));
+            A.sampleFirst = s0;
+            A.nSamples = ns;
+            const int nSlots = A.nPix * ns;
+            kGenerate<<<sm * 8, 256, 0, d->stream>>>(S, P, A, nSlots);
+            uint32_t live = static_cast<uint32_t>(nSlots);
+            PE_CUDA(cudaMemcpyAsync(&P.counters[0], &live, sizeof(uint32_t), cudaMemcpyHostToDevice, d->stream));
+            PE_CUDA(cudaMemsetAsync(&P.counters[1], 0, 2 * sizeof(uint32_t), d->stream));
+            int32_t* qIn = P.queueA;
+            int32_t* qOut = P.queueB;
+            uint32_t* cIn = &P.counters[0];
+            uint32_t* cOut = &P.counters[1];
+            stats.paths += static_cast<uint64_t>(nSlots);
+            for (int iter = 0; live > 0; ++iter) {
+                stats.closest_rays += live;
+                cudaEvent_t e0, e1, e2, e3;
+                if ((rc = event(e0)) || (rc = event(e1)) || (rc = event(e2)) || (rc = event(e3))) return rc;
+                PE_CUDA(cudaEventRecord(e0, d->stream));
+                if (d->counting)
+                    kIntersect<true><<<d->blocksIntersect, 128, 0, d->stream>>>(S, P, qIn, cIn, d->dStats);
+                else
+                    kIntersect<false><<<d->blocksIntersect, 128, 0, d->stream>>>(S, P, qIn, cIn, d->dStats);
+                PE_CUDA(cudaEventRecord(e1, d->stream));
+                kShade<<<d->blocksShade, 128, 0, d->stream>>>(S, P, A, qIn, cIn, qOut, cOut);
+                PE_CUDA(cudaEventRecord(e2, d->stream));
+                if (d->counting)
+                    kShadow<true><<<d->blocksShadow, 128, 0, d->stream>>>(S, P, &P.counters[2], A.clampIndirect, d->dStats);
+                else
+                    kShadow<false><<<d->blocksShadow, 128, 0, d->stream>>>(S, P, &P.counters[2], A.clampIndirect, d->dStats);
+                PE_CUDA(cudaEventRecord(e3, d->stream));
+                isectEv.push_back({evUsed - 4, evUsed - 3});
+                shadeEv.push_back({evUsed - 3, evUsed - 2});
+                shadowEv.push_back({evUsed - 2, evUsed - 1});
+                PE_CUDA(cudaMemcpyAsync(d->hCounters, P.counters, 4 * sizeof(uint32_t), cudaMemcpyDeviceToHost, d->stream));
+                PE_CUDA(cudaStreamSynchronize(d->stream));
+                stats.shadow_rays += d->hCounters[2];
+                live = cOut == &P.counters[1] ? d->hCounters[1] : d->hCounters[0];
+                if (iter > 4096) {
+                    setError("wavefront did not drain after 4096 iterations");
+                    return PE_ERR_DEVICE;
+                }
+                // swap queues; reset the consumed counter and the shadow counter
+                PE_CUDA(cudaMemsetAsync(cIn, 0, sizeof(uint32_t), d->stream));
+                PE_CUDA(cudaMemsetAsync(&P.counters[2], 0, sizeof(uint32_t), d->stream));
+                std::swap(qIn, qOut);
+                std::swap(cIn, cOut);
+            }
+            kFilm<<<sm * 4, 256, 0, d->stream>>>(P, A, sum, cnt, sq, &d->dStats[4]);
+            PE_CUDA(cudaGetLastError());
+        }
+    }
+    PE_CUDA(cudaEventRecord(d->evStop, d->stream));
+    unsigned long long hs[8] = {};
+    PE_CUDA(cudaMemcpyAsync(hs, d->dStats, sizeof(hs), cudaMemcpyDeviceToHost, d->stream));
+    PE_CUDA(cudaStreamSynchronize(d->stream));
+    PE_CUDA(cudaGetLastError());
+    float ms = 0.0f;
+    PE_CUDA(cudaEventElapsedTime(&ms, d->evStart, d->evStop));
+    stats.ms_total = ms;
+    for (auto& pr : isectEv) {
+        float t = 0.0f;
+        cudaEventElapsedTime(&t, d->evPool[pr.first], d->evPool[pr.second]);
+        stats.ms_intersect += t;
+    }
+    for (auto& pr : shadeEv) {
+        float t = 0.0f;
+        cudaEventElapsedTime(&t, d->evPool[pr.first], d->evPool[pr.second]);
+        stats.ms_shade += t;
+    }
+    for (auto& pr : shadowEv) {
+        float t = 0.0f;
+        cudaEventElapsedTime(&t, d->evPool[pr.first], d->evPool[pr.second]);
+        stats.ms_shadow += t;
+    }
+    stats.intersect_launches = isectEv.size();
+    stats.node_visits = hs[0] + hs[2];
+    stats.tri_tests = hs[1] + hs[3];
+    stats.rejected = hs[4];
+    stats.waves = isectEv.empty() ? 0 : 1;
+    if (cancelled) {
+        setError("render cancelled");
+        return PE_ERR_CANCELLED;
+    }
+    return PE_OK;
+}
+
+__global__ void kTracePrimary(SceneGPU S, WaveArgs A, int nPix, int32_t* outShape, int32_t* outPrim, float* outT) {
+    for (int pix = blockIdx.x * blockDim.x + threadIdx.x; pix < nPix; pix += gridDim.x * blockDim.x) {
+        const int x = pix % A.width, y = pix / A.width;
+        Sobol sb;
+        sb.pixelHash = pixelHashOf(A.seed, x, y);
+        sb.revIndex = rev32(static_cast<uint32_t>(A.sampleFirst));
+        sb.dim = 0;
+        V3 o, d;
+        cameraRay(S.tables, A.cam, A.filterWidth, x, y, A.width, A.height, sb, o, d);
+        uint32_t a = 0, b = 0;
+        const Hit h = traceClosest<false>(S, o, d, VIS_CAMERA, 0.0f, 1e30f, a, b);
+        if (h.prim < 0) {
+            outShape[pix] = -1;
+            outPrim[pix] = -1;
+            outT[pix] = 0.0f;
+        } else {
+            const float4 e2w = __ldg(&S.tris[3 * h.prim + 2]);
+            const int g = static_cast<int>(__float_as_uint(e2w.w));
+            const int shape = __ldg(&S.triVerts[g]).w;
+            outShape[pix] = shape;
+            outPrim[pix] = g - static_cast<int>(S.shapes[shape].firstTri);
+            outT[pix] = h.t;
+        }
+    }
+}
+
+__global__ void kSobol(const TablesGPU* T, uint64_t seed, const int32_t* px, const int32_t* py, const int32_t* idx, int n,
+                       int nd, float* out) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        Sobol sb;
+        sb.pixelHash = pixelHashOf(seed, px[i], py[i]);
+        sb.revIndex = rev32(static_cast<uint32_t>(idx[i]));
+        sb.dim = 0;
+        for (int k = 0; k < nd; ++k) {
+            const V2 v = get2D(T, sb);
+            out[(static_cast<size_t>(i) * nd + k) * 2 + 0] = v.x;
+            out[(static_cast<size_t>(i) * nd + k) * 2 + 1] = v.y;
+        }
+    }
+}
+
+__global__ void kBsdfProbe(SceneGPU S, int material, const pe_bsdf_query* q, int n, pe_bsdf_result* out) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const MatGPU& m = S.materials[material];
+        ShadePoint sp;
+        sp.p = m3f(q[i].point);
+        sp.n = m3f(q[i].normal);
+        sp.ng = m3f(q[i].ng);
+        sp.tangent = m3f(q[i].tangent);
+        sp.frontFace = q[i].front_face != 0;
+        sp.wavelength = q[i].wavelength;
+        pe_bsdf_result r;
+        memset(&r, 0, sizeof(r));
+        float pdf = 0.0f;
+        const V3 f = bsdfEvalPdf(S.tables, m, m3f(q[i].wo), m3f(q[i].wi), sp, pdf, nullptr);
+        r.f[0] = f.x;
+        r.f[1] = f.y;
+        r.f[2] = f.z;
+        r.pdf = pdf;
+        BsdfSample bs;
+        bs.wi = mk(0.0f);
+        bs.f = mk(0.0f);
+        bs.pdf = 0.0f;
+        bs.delta = bs.passThrough = bs.subsurface = false;
+        bs.weight = mk(0.0f);
+        r.sampled = bsdfSample(S.tables, m, m3f(q[i].wo), sp, q[i].uc, mk2(q[i].u[0], q[i].u[1]), bs) ? 1 : 0;
+        r.wi[0] = bs.wi.x;
+        r.wi[1] = bs.wi.y;
+        r.wi[2] = bs.wi.z;
+        r.sf[0] = bs.f.x;
+        r.sf[1] = bs.f.y;
+        r.sf[2] = bs.f.z;
+        r.spdf = bs.pdf;
+        r.delta = bs.delta;
+        r.pass_through = bs.passThrough;
+        r.subsurface = bs.subsurface;
+        r.weight[0] = bs.weight.x;
+        r.weight[1] = bs.weight.y;
+        r.weight[2] = bs.weight.z;
+        out[i] = r;
+    }
+}
+
+} // namespace
+
+extern "C" {
+
+int32_t pe_device_count(void) {
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess) return 0;
+    return n;
+}
+
+pe_device* pe_device_create(int32_t ordinal, char* err, size_t errLen) {
+    auto fail = [&](const std::string& m) -> pe_device* {
+        setError(m);
+        if (err && errLen > 0) {
+            std::strncpy(err, m.c_str(), errLen - 1);
+            err[errLen - 1] = '\0';
+        }
+        return nullptr;
+    };
+    int n = 0;
+    cudaError_t e = cudaGetDeviceCount(&n);
+    if (e != cudaSuccess || n == 0) return fail(std::string("no CUDA device: ") + (e != cudaSuccess ? cudaMsg(e) : "count 0"));
+    if (ordinal < 0 || ordinal >= n) return fail("CUDA ordinal out of range");
+    pe_device* d = new (std::nothrow) pe_device();
+    if (!d) return fail("host out of memory");
+    d->ordinal = ordinal;
+    if ((e = cudaSetDevice(ordinal)) != cudaSuccess) {
+        delete d;
+        return fail(std::string("cudaSetDevice: ") + cudaMsg(e));
+    }
+    cudaGetDeviceProperties(&d->prop, ordinal);
+    if (d->prop.major < 10) {
+        delete d;
+        return fail("device " + std::string(d->prop.name) + " is not sm_100 class; this build targets sm_100a only");
+    }
+    if (cudaStreamCreateWithFlags(&d->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreate(&d->evStart) != cudaSuccess || cudaEventCreate(&d->evStop) != cudaSuccess ||
+        cudaMalloc(&d->dTables, sizeof(TablesGPU)) != cudaSuccess ||
+        cudaMalloc(&d->dStats, 8 * sizeof(unsigned long long)) != cudaSuccess ||
+        cudaMallocHost(&d->hCounters, 16 * sizeof(uint32_t)) != cudaSuccess) {
+        pe_device_destroy(d);
+        return fail("device initialisation failed");
+    }
+    d->hTables = staticTables();
+    fillFilterCdf(PE_FILTER_BOX, 1.0f, d->hTables.filterCdf);
+    d->filterType = PE_FILTER_BOX;
+    d->filterWidth = 1.0f;
+    cudaMemcpy(d->dTables, &d->hTables, sizeof(TablesGPU), cudaMemcpyHostToDevice);
+    int b = 0;
+    const int sm = d->prop.multiProcessorCount;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kIntersect<false>, 128, 0);
+    d->blocksIntersect = sm * std::max(1, b);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kShade, 128, 0);
+    d->blocksShade = sm * std::max(1, b);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kShadow<false>, 128, 0);
+    d->blocksShadow = sm * std::max(1, b);
+    const cudaError_t le = cudaGetLastError();
+    if (le != cudaSuccess) {
+        pe_device_destroy(d);
+        return fail(std::string("kernel image not loadable on this device: ") + cudaMsg(le));
+    }
+    return d;
+}
+
+void pe_device_destroy(pe_device* d) {
+    if (!d) return;
+    cudaSetDevice(d->ordinal);
+    if (d->stream) cudaStreamSynchronize(d->stream);
+    freeList(d->sceneBufs);
+    freeList(d->pathBufs);
+    cudaFree(d->fSum);
+    cudaFree(d->fCnt);
+    cudaFree(d->fSq);
+    cudaFree(d->dTables);
+    cudaFree(d->dStats);
+    if (d->hCounters) cudaFreeHost(d->hCounters);
+    for (cudaEvent_t e : d->evPool) cudaEventDestroy(e);
+    if (d->evStart) cudaEventDestroy(d->evStart);
+    if (d->evStop) cudaEventDestroy(d->evStop);
+    if (d->stream) cudaStreamDestroy(d->stream);
+    delete d;
+}
+
+int32_t pe_device_info_get(pe_device* d, pe_device_info* out) {
+    if (!d || !out) {
+        setError("pe_device_info_get: null argument");
+        return PE_ERR_INVALID;
+    }
+    std::memset(out, 0, sizeof(*out));
+    std::strncpy(out->name, d->prop.name, sizeof(out->name) - 1);
+    out->memory_bytes = d->prop.totalGlobalMem;
+    out->compute_major = d->prop.major;
+    out->compute_minor = d->prop.minor;
+    out->sm_count = d->prop.multiProcessorCount;
+    out->usable = 1;
+    return PE_OK;
+}
+
+int32_t pe_device_set_scene(pe_device* d, const pe_scene* s) {
+    if (!d || !s) {
+        setError("pe_device_set_scene: null argument");
+        return PE_ERR_INVALID;
+    }
+    if (!s->built) {
+        setError("pe_device_set_scene: scene not built (call pe_scene_build)");
+        return PE_ERR_INVALID;
+    }
+    PE_CUDA(cudaSetDevice(d->ordinal));
+    PE_CUDA(cudaStreamSynchronize(d->stream));
+    freeList(d->sceneBufs);
+    d->hasScene = false;
+    const HostBuild& B = s->build;
+    SceneGPU G{};
+    int32_t rc = 0;
+    if ((rc = upload(d, d->sceneBufs, G.nodes, B.nodes)) || (rc = upload(d, d->sceneBufs, G.tris, B.tris)) ||
+        (rc = upload(d, d->sceneBufs, G.triVerts, B.triVerts)) || (rc = upload(d, d->sceneBufs, G.pos, B.pos)) ||
+        (rc = upload(d, d->sceneBufs, G.nrm, B.nrm)) || (rc = upload(d, d->sceneBufs, G.uv, B.uv)) ||
+        (rc = upload(d, d->sceneBufs, G.shapes, B.shapes)) || (rc = upload(d, d->sceneBufs, G.materials, B.materials)) ||
+        (rc = upload(d, d->sceneBufs, G.lights, B.lights)) || (rc = upload(d, d->sceneBufs, G.lightNodes, B.lightNodes)) ||
+        (rc = upload(d, d->sceneBufs, G.topSlot, B.topSlot)) || (rc = upload(d, d->sceneBufs, G.trail, B.trail)) ||
+        (rc = upload(d, d->sceneBufs, G.trailDepth, B.trailDepth)))
+        return rc;
+    G.rootIsLeaf = B.rootIsLeaf;
+    G.rootFirst = B.rootFirst;
+    G.rootCount = B.rootCount;
+    G.nNodes = static_cast<int32_t>(B.nodes.size() / 4);
+    for (int i = 0; i < 3; ++i) {
+        G.rootMin[i] = B.rootMin[i];
+        G.rootMax[i] = B.rootMax[i];
+    }
+    G.nTris = static_cast<uint32_t>(B.triVerts.size());
+    G.nShapes = static_cast<int32_t>(B.shapes.size());
+    G.nLights = static_cast<int32_t>(B.lights.size());
+    G.lightMode = B.lightMode;
+    G.lightCount = B.lightCount;
+    G.nInfinite = static_cast<int32_t>(B.infinite.size());
+    for (size_t i = 0; i < B.infinite.size() && i < static_cast<size_t>(kMaxInfinite); ++i) G.infinite[i] = B.infinite[i];
+    G.nLightNodes = static_cast<int32_t>(B.lightNodes.size());
+    // environment (the MIS-compensated distribution drives sampling and pdfLi)
+    const HostEnv& e = s->env;
+    EnvGPU& E = G.env;
+    E.present = e.present ? 1 : 0;
+    E.width = e.width;
+    E.height = e.height;
+    E.hasImage = e.hasImage ? 1 : 0;
+    E.rotation = e.rotation;
+    E.intensity = e.intensity;
+    E.meanLuminance = e.meanLuminance;
+    E.sunPdfWeight = e.sunPdfWeight;
+    E.sunDir[0] = e.sunDir.x;
+    E.sunDir[1] = e.sunDir.y;
+    E.sunDir[2] = e.sunDir.z;
+    E.sunCosMax = e.sunCosMax;
+    E.sunRadiance[0] = e.sunRadiance.x;
+    E.sunRadiance[1] = e.sunRadiance.y;
+    E.sunRadiance[2] = e.sunRadiance.z;
+    E.funcInt = e.misInt;
+    E.valid = e.misValid ? 1 : 0;
+    if ((rc = upload(d, d->sceneBufs, E.image, e.image)) || (rc = upload(d, d->sceneBufs, E.func, e.misFunc)) ||
+        (rc = upload(d, d->sceneBufs, E.marginalCdf, e.misMarg)) || (rc = upload(d, d->sceneBufs, E.condCdf, e.misCond)))
+        return rc;
+    G.tables = d->dTables;
+    G.bgMode = s->bgMode;
+    for (int i = 0; i < 3; ++i) G.bgColor[i] = s->bgColor[i];
+    G.hasShadowTransmitters = B.hasShadowTransmitters ? 1 : 0;
+    G.hasVolumes = B.hasVolumes ? 1 : 0;
+    PE_CUDA(cudaStreamSynchronize(d->stream));
+    d->scene = G;
+    d->hasScene = true;
+    return PE_OK;
+}
+
+int32_t pe_device_has_scene(pe_device* d) { return d && d->hasScene ? 1 : 0; }
+
+int32_t pe_device_render_resident(pe_device* d, const pe_camera* cam, const pe_settings* st, int32_t first, int32_t count,
+                                  const volatile int32_t* cancel) {
+    if (!d) {
+        setError("null device");
+        return PE_ERR_INVALID;
+    }
+    if (!d->hasScene) {
+        setError("render before set_scene");
+        return PE_ERR_NO_SCENE;
+    }
+    int32_t rc = checkSettings(cam, st);
+    if (rc) return rc;
+    if (count <= 0) return PE_OK;
+    PE_CUDA(cudaSetDevice(d->ordinal));
+    if ((rc = ensureFilm(d, st->width, st->height))) return rc;
+    return renderWaves(d, cam, st, first, count, cancel, d->fSum, d->fCnt, d->fSq);
+}
+
+int32_t pe_device_film_clear(pe_device* d) {
+    if (!d) {
+        setError("null device");
+        return PE_ERR_INVALID;
+    }
+    if (!d->fSum) return PE_OK;
+    const size_t n = static_cast<size_t>(d->filmW) * static_cast<size_t>(d->filmH);
+    PE_CUDA(cudaMemsetAsync(d->fSum, 0, n * 3 * sizeof(float), d->stream));
+    PE_CUDA(cudaMemsetAsync(d->fCnt, 0, n * sizeof(uint32_t), d->stream));
+    PE_CUDA(cudaMemsetAsync(d->fSq, 0, n * sizeof(float), d->stream));
+    return PE_OK;
+}
+
+int32_t pe_device_film_read(pe_device* d, float* sum, uint32_t* cnt, float* sq) {
+    if (!d) {
+        setError("null device");
+        return PE_ERR_INVALID;
+    }
+    if (!d->fSum) {
+        setError("no resident film");
+        return PE_ERR_INVALID;
+    }
+    const size_t n = static_cast<size_t>(d->filmW) * static_cast<size_t>(d->filmH);
+    if (sum) PE_CUDA(cudaMemcpyAsync(sum, d->fSum, n * 3 * sizeof(float), cudaMemcpyDeviceToHost, d->stream));
+    if (cnt) PE_CUDA(cudaMemcpyAsync(cnt, d->fCnt, n * sizeof(uint32_t), cudaMemcpyDeviceToHost, d->stream));
+    if (sq) PE_CUDA(cudaMemcpyAsync(sq, d->fSq, n * sizeof(float), cudaMemcpyDeviceToHost, d->stream));
+    PE_CUDA(cudaStreamSynchronize(d->stream));
+    return PE_OK;
+}
+
+// RenderDevice::render with host films: the batch is rendered into a zeroed device film, read
+// back, and merged into the caller's arrays as Film::addBatch does (film.cpp:119-137).
+int32_t pe_device_render(pe_device* d, const pe_camera* cam, const pe_settings* st, int32_t first, int32_t count,
+                         const volatile int32_t* cancel, float* sumRgb, uint32_t* sampleCount, float* sumLumSq,
+                         uint64_t* traced) {
+    if (!d) {
+        setError("null device");
+        return PE_ERR_INVALID;
+    }
+    if (!d->hasScene) {
+        setError("render before set_scene");
+        return PE_ERR_NO_SCENE;
+    }
+    int32_t rc = checkSettings(cam, st);
+    if (rc) return rc;
+    if (count <= 0) return PE_OK;
+    PE_CUDA(cudaSetDevice(d->ordinal));
+    if ((rc = ensureFilm(d, st->width, st->height))) return rc;
+    if ((rc = pe_device_film_clear(d))) return rc;
+    const int32_t rr = renderWaves(d, cam, st, first, count, cancel, d->fSum, d->fCnt, d->fSq);
+    if (rr != PE_OK && rr != PE_ERR_CANCELLED) return rr;
+    const size_t n = static_cast<size_t>(st->width) * static_cast<size_t>(st->height);
+    std::vector<float> s(n * 3), q(n);
+    std::vector<uint32_t> c(n);
+    if ((rc = pe_device_film_read(d, s.data(), c.data(), q.data()))) return rc;
+    uint64_t tr = 0;
+    for (size_t i = 0; i < n; ++i) {
+        tr += c[i];
+        if (sampleCount) sampleCount[i] += c[i];
+        if (sumRgb) {
+            sumRgb[3 * i + 0] += s[3 * i + 0];
+            sumRgb[3 * i + 1] += s[3 * i + 1];
+            sumRgb[3 * i + 2] += s[3 * i + 2];
+        }
+        if (sumLumSq) sumLumSq[i] += q[i];
+    }
+    if (traced) *traced = tr;
+    return rr;
+}
+
+int32_t pe_device_synchronize(pe_device* d) {
+    if (!d) return PE_ERR_INVALID;
+    PE_CUDA(cudaStreamSynchronize(d->stream));
+    return PE_OK;
+}
+
+int32_t pe_device_last_stats(pe_device* d, pe_render_stats* out) {
+    if (!d || !out) {
+        setError("null argument");
+        return PE_ERR_INVALID;
+    }
+    *out = d->stats;
+    return PE_OK;
+}
+
+int32_t pe_device_set_counting(pe_device* d, int32_t enabled) {
+    if (!d) return PE_ERR_INVALID;
+    d->counting = enabled != 0;
+    return PE_OK;
+}
+
+int32_t pe_device_trace_primary(pe_device* d, const pe_camera* cam, const pe_settings* st, int32_t sampleIndex,
+                                int32_t* outShape, int32_t* outPrim, float* outT) {
+    if (!d || !outShape || !outPrim || !outT) {
+        setError("null argument");
+        return PE_ERR_INVALID;
+    }
+    if (!d->hasScene) {
+        setError("trace before set_scene");
+        return PE_ERR_NO_SCENE;
+    }
+    int32_t rc = checkSettings(cam, st);
+    if (rc) return rc;
+    PE_CUDA(cudaSetDevice(d->ordinal));
+    if ((rc = ensureFilter(d, st->filter_type, st->filter_width))) return rc;
+    WaveArgs A = makeWave(cam, st);
+    A.sampleFirst = sampleIndex;
+    const int n = st->width * st->height;
+    std::vector<DevBuf> tmp;
+    int32_t* dS = nullptr;
+    int32_t* dP = nullptr;
+    float* dT = nullptr;
+    if ((rc = devAlloc(tmp, dS, n)) || (rc = devAlloc(tmp, dP, n)) || (rc = devAlloc(tmp, dT, n))) {
+        freeList(tmp);
+        return rc;
+    }
+    kTracePrimary<<<d->prop.multiProcessorCount * 8, 128, 0, d->stream>>>(d->scene, A, n, dS, dP, dT);
+    cudaMemcpyAsync(outShape, dS, n * sizeof(int32_t), cudaMemcpyDeviceToHost, d->stream);
+    cudaMemcpyAsync(outPrim, dP, n * sizeof(int32_t), cudaMemcpyDeviceToHost, d->stream);
+    cudaMemcpyAsync(outT, dT, n * sizeof(float), cudaMemcpyDeviceToHost, d->stream);
+    const cudaError_t e = cudaStreamSynchronize(d->stream);
+    freeList(tmp);
+    if (e != cudaSuccess) {
+        setError(std::string("trace_primary: ") + cudaMsg(e));
+        return PE_ERR_CUDA;
+    }
+    return PE_OK;
+}
+
+int32_t pe_device_sobol(pe_device* d, uint64_t seed, const int32_t* px, const int32_t* py, const int32_t* index, size_t n,
+                        int32_t nd, float* out) {
+    if (!d || !px || !py || !index || !out || nd <= 0) {
+        setError("pe_device_sobol: bad argument");
+        return PE_ERR_INVALID;
+    }
+    PE_CUDA(cudaSetDevice(d->ordinal));
+    std::vector<DevBuf> tmp;
+    int32_t *dx = nullptr, *dy = nullptr, *di = nullptr;
+    float* dout = nullptr;
+    int32_t rc;
+    if ((rc = devAlloc(tmp, dx, n)) || (rc = devAlloc(tmp, dy, n)) || (rc = devAlloc(tmp, di, n)) ||
+        (rc = devAlloc(tmp, dout, n * static_cast<size_t>(nd) * 2))) {
+        freeList(tmp);
+        return rc;
+    }
+    cudaMemcpyAsync(dx, px, n * 4, cudaMemcpyHostToDevice, d->stream);
+    cudaMemcpyAsync(dy, py, n * 4, cudaMemcpyHostToDevice, d->stream);
+    cudaMemcpyAsync(di, index, n * 4, cudaMemcpyHostToDevice, d->stream);
+    kSobol<<<d->prop.multiProcessorCount * 4, 128, 0, d->stream>>>(d->dTables, seed, dx, dy, di, static_cast<int>(n), nd, dout);
+    cudaMemcpyAsync(out, dout, n * static_cast<size_t>(nd) * 2 * sizeof(float), cudaMemcpyDeviceToHost, d->stream);
+    const cudaError_t e = cudaStreamSynchronize(d->stream);
+    freeList(tmp);
+    if (e != cudaSuccess) {
+        setError(std::string("sobol: ") + cudaMsg(e));
+        return PE_ERR_CUDA;
+    }
+    return PE_OK;
+}
+
+int32_t pe_device_bsdf_probe(pe_device* d, int32_t material, const pe_bsdf_query* q, size_t n, pe_bsdf_result* out) {
+    if (!d || !q || !out) {
+        setError("pe_device_bsdf_probe: null argument");
+        return PE_ERR_INVALID;
+    }
+    if (!d->hasScene) {
+        setError("probe before set_scene");
+        return PE_ERR_NO_SCENE;
+    }
+    PE_CUDA(cudaSetDevice(d->ordinal));
+    std::vector<DevBuf> tmp;
+    pe_bsdf_query* dq = nullptr;
+    pe_bsdf_result* dr = nullptr;
+    int32_t rc;
+    if ((rc = devAlloc(tmp, dq, n)) || (rc = devAlloc(tmp, dr, n))) {
+        freeList(tmp);
+        return rc;
+    }
+    cudaMemcpyAsync(dq, q, n * sizeof(pe_bsdf_query), cudaMemcpyHostToDevice, d->stream);
+    kBsdfProbe<<<d->prop.multiProcessorCount * 2, 128, 0, d->stream>>>(d->scene, material, dq, static_cast<int>(n), dr);
+    cudaMemcpyAsync(out, dr, n * sizeof(pe_bsdf_result), cudaMemcpyDeviceToHost, d->stream);
+    const cudaError_t e = cudaStreamSynchronize(d->stream);
+    freeList(tmp);
+    if (e != cudaSuccess) {
+        setError(std::string("bsdf_probe: ") + cudaMsg(e));
+        return PE_ERR_CUDA;
+    }
+    return PE_OK;
+}
+
+} // extern "C"

@@ -1,0 +1,1271 @@
+// pe_host.cpp — host side of the scene boundary: accepts the reference engine's scene content
+// (meshes, materials, lights, environment) through the pe_scene_* C ABI and flattens it into
+// the resident GPU layout of pe_scene.h.  The acceleration structures are built with the same
+// algorithms, float operations and tie rules as the reference so the device traverses the same
+// tree:
+//   SAH BVH          src/geometry/bvh.cpp:11-255 (12 buckets, leaf when cost >= N and N <= 255)
+//   vertex normals   src/geometry/mesh.cpp:30-55
+//   emitter lights   src/engine/scene.cpp:18-99 (one TriangleLight per emissive triangle,
+//                    two BVH triangles per area light)
+//   light sampler    src/lights/light_sampler.cpp:42-148 (exhaustive <= 33 candidates, else
+//                    light BVH with PBRT-v4 cost and bit trails)
+//   environment      src/lights/environment_light.cpp:64-227 (full and MIS-compensated CDFs)
+//   energy tables    src/materials/microfacet.cpp:36-163 (deterministic stratified integration)
+// Compiled with -ffp-contract=off so every float result matches the reference's parity build.
+#include "pe_host.h"
+#include "pe_bsdf.h"
+#include "pe_light.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <limits>
+#include <memory>
+
+namespace pe {
+
+namespace {
+thread_local std::string tlsError;
+}
+void setError(const std::string& msg) { tlsError = msg; }
+
+namespace {
+
+// ---------------------------------------------------------------------------------------------
+// AABB with the reference's empty box (+max, -max) and std::min/max merges (aabb.h).
+struct Box {
+    V3 lo, hi;
+    Box() : lo(mk(std::numeric_limits<float>::max())), hi(mk(-std::numeric_limits<float>::max())) {}
+    Box(V3 a, V3 b) : lo(vmin(a, b)), hi(vmax(a, b)) {}
+    Box merged(const Box& o) const {
+        Box r;
+        r.lo = vmin(lo, o.lo);
+        r.hi = vmax(hi, o.hi);
+        return r;
+    }
+    void merge(V3 p) {
+        lo = vmin(lo, p);
+        hi = vmax(hi, p);
+    }
+    void merge(const Box& o) {
+        lo = vmin(lo, o.lo);
+        hi = vmax(hi, o.hi);
+    }
+    V3 centroid() const { return (lo + hi) * 0.5f; }
+    V3 diagonal() const { return hi - lo; }
+    float surfaceArea() const {
+        const V3 d = diagonal();
+        return 2.0f * (d.x * d.y + d.x * d.z + d.y * d.z);
+    }
+    int maxExtent() const {
+        const V3 d = diagonal();
+        if (d.x > d.y && d.x > d.z) return 0;
+        if (d.y > d.z) return 1;
+        return 2;
+    }
+    V3 offset(V3 p) const {
+        V3 o = p - lo;
+        const V3 d = diagonal();
+        if (d.x > 0.0f) o.x /= d.x;
+        if (d.y > 0.0f) o.y /= d.y;
+        if (d.z > 0.0f) o.z /= d.z;
+        return o;
+    }
+};
+
+struct BuildPrim {
+    size_t primIndex;
+    Box bounds;
+    V3 centroid;
+    BuildPrim(size_t i, const Box& b) : primIndex(i), bounds(b), centroid(b.centroid()) {}
+};
+
+struct BuildNode {
+    Box bounds;
+    BuildNode* child[2] = {nullptr, nullptr};
+    int axis = 0;
+    int first = 0;
+    int count = 0;
+};
+
+struct RefNode { // BVHNode (bvh.h:27-36): 32-byte depth-first node
+    Box bounds;
+    int offset;  // leaf: first prim; interior: second child
+    int count;   // leaf prim count, 0 for interior
+};
+
+class SahBuilder {
+public:
+    std::vector<BuildPrim> prims;
+    std::vector<size_t> ordered; // leaf order → ref index
+    int total = 0;
+    std::vector<std::unique_ptr<BuildNode>> pool;
+
+    BuildNode* newNode() {
+        pool.emplace_back(new BuildNode());
+        return pool.back().get();
+    }
+    void makeLeaf(BuildNode* n, int start, int end, const Box& b) {
+        n->first = static_cast<int>(ordered.size());
+        for (int i = start; i < end; ++i) ordered.push_back(prims[static_cast<size_t>(i)].primIndex);
+        n->count = end - start;
+        n->bounds = b;
+    }
+    void makeInterior(BuildNode* n, int axis, BuildNode* c0, BuildNode* c1) {
+        n->child[0] = c0;
+        n->child[1] = c1;
+        n->bounds = c0->bounds.merged(c1->bounds);
+        n->axis = axis;
+        n->count = 0;
+    }
+    // BVH::recursiveBuild (bvh.cpp:100-238).
+    BuildNode* build(int start, int end) {
+        ++total;
+        BuildNode* node = newNode();
+        Box bounds;
+        for (int i = start; i < end; ++i) bounds = bounds.merged(prims[static_cast<size_t>(i)].bounds);
+        const int n = end - start;
+        if (n == 1) {
+            makeLeaf(node, start, end, bounds);
+            return node;
+        }
+        Box cb;
+        for (int i = start; i < end; ++i) cb.merge(prims[static_cast<size_t>(i)].centroid);
+        const int dim = cb.maxExtent();
+        if (get(cb.hi, dim) == get(cb.lo, dim)) {
+            if (n > 4) {
+                const int mid = (start + end) / 2;
+                BuildNode* a = build(start, mid);
+                BuildNode* b = build(mid, end);
+                makeInterior(node, dim, a, b);
+                return node;
+            }
+            makeLeaf(node, start, end, bounds);
+            return node;
+        }
+        int mid = (start + end) / 2;
+        if (n <= 2) {
+            std::nth_element(prims.begin() + start, prims.begin() + mid, prims.begin() + end,
+                             [dim](const BuildPrim& a, const BuildPrim& b) { return get(a.centroid, dim) < get(b.centroid, dim); });
+        } else {
+            constexpr int nB = 12;
+            int cnt[nB] = {};
+            Box bb[nB];
+            for (int i = start; i < end; ++i) {
+                int b = static_cast<int>(nB * get(cb.offset(prims[static_cast<size_t>(i)].centroid), dim));
+                if (b == nB) b = nB - 1;
+                cnt[b]++;
+                bb[b] = bb[b].merged(prims[static_cast<size_t>(i)].bounds);
+            }
+            float cost[nB - 1];
+            for (int i = 0; i < nB - 1; ++i) {
+                Box b0, b1;
+                int c0 = 0, c1 = 0;
+                for (int j = 0; j <= i; ++j) {
+                    b0 = b0.merged(bb[j]);
+                    c0 += cnt[j];
+                }
+                for (int j = i + 1; j < nB; ++j) {
+                    b1 = b1.merged(bb[j]);
+                    c1 += cnt[j];
+                }
+                cost[i] = 1.0f + (c0 * b0.surfaceArea() + c1 * b1.surfaceArea()) / bounds.surfaceArea();
+            }
+            float minCost = cost[0];
+            int split = 0;
+            for (int i = 1; i < nB - 1; ++i)
+                if (cost[i] < minCost) {
+                    minCost = cost[i];
+                    split = i;
+                }
+            const float leafCost = static_cast<float>(n);
+            if (n > 255 || minCost < leafCost) {
+                auto pm = std::partition(prims.begin() + start, prims.begin() + end, [=](const BuildPrim& bp) {
+                    int b = static_cast<int>(nB * get(cb.offset(bp.centroid), dim));
+                    if (b == nB) b = nB - 1;
+                    return b <= split;
+                });
+                mid = static_cast<int>(pm - prims.begin());
+                if (mid != start && mid != end) {
+                    BuildNode* a = build(start, mid);
+                    BuildNode* b = build(mid, end);
+                    makeInterior(node, dim, a, b);
+                    return node;
+                }
+            }
+            makeLeaf(node, start, end, bounds);
+            return node;
+        }
+        BuildNode* a = build(start, mid);
+        BuildNode* b = build(mid, end);
+        makeInterior(node, dim, a, b);
+        return node;
+    }
+    // BVH::flattenBVHTree (bvh.cpp:240-255): depth-first, first child follows its parent.
+    int flatten(BuildNode* node, std::vector<RefNode>& out, int* offset, int depth, int& maxDepth) {
+        if (depth > maxDepth) maxDepth = depth;
+        const int my = (*offset)++;
+        out[static_cast<size_t>(my)].bounds = node->bounds;
+        if (node->count > 0) {
+            out[static_cast<size_t>(my)].offset = node->first;
+            out[static_cast<size_t>(my)].count = node->count;
+        } else {
+            out[static_cast<size_t>(my)].count = 0;
+            flatten(node->child[0], out, offset, depth + 1, maxDepth);
+            out[static_cast<size_t>(my)].offset = flatten(node->child[1], out, offset, depth + 1, maxDepth);
+        }
+        return my;
+    }
+};
+
+inline float4 f4(float x, float y, float z, float w) {
+    float4 r;
+    r.x = x;
+    r.y = y;
+    r.z = z;
+    r.w = w;
+    return r;
+}
+
+// ---------------------------------------------------------------------------------------------
+// light BVH (light_sampler.cpp:24-148, light_bounds.cpp:73-109)
+struct LBounds {
+    Box bounds;
+    V3 w{0.0f, 0.0f, 1.0f};
+    float phi = 0.0f;
+    float cosThetaO = 1.0f;
+    float cosThetaE = 0.0f;
+    bool twoSided = false;
+};
+float safeAcos(float x) { return std::acos(sclamp(x, -1.0f, 1.0f)); }
+V3 rotateAround(V3 v, V3 axis, float theta) {
+    const float c = std::cos(theta), s = std::sin(theta);
+    return v * c + cross(axis, v) * s + axis * (dot(axis, v) * (1.0f - c));
+}
+LBounds unionBounds(const LBounds& a, const LBounds& b) {
+    if (!(a.phi > 0.0f)) return b;
+    if (!(b.phi > 0.0f)) return a;
+    LBounds u;
+    u.bounds = a.bounds.merged(b.bounds);
+    u.phi = a.phi + b.phi;
+    u.cosThetaE = smin(a.cosThetaE, b.cosThetaE);
+    u.twoSided = a.twoSided || b.twoSided;
+    const float thetaA = safeAcos(a.cosThetaO), thetaB = safeAcos(b.cosThetaO);
+    const float thetaD = safeAcos(dot(a.w, b.w));
+    if (smin(thetaD + thetaB, kPi) <= thetaA) {
+        u.w = a.w;
+        u.cosThetaO = a.cosThetaO;
+        return u;
+    }
+    if (smin(thetaD + thetaA, kPi) <= thetaB) {
+        u.w = b.w;
+        u.cosThetaO = b.cosThetaO;
+        return u;
+    }
+    const float thetaO = 0.5f * (thetaA + thetaD + thetaB);
+    const V3 axis = cross(a.w, b.w);
+    if (thetaO >= kPi || len2(axis) < 1e-12f) {
+        u.w = a.w;
+        u.cosThetaO = -1.0f;
+        return u;
+    }
+    u.w = normalize(rotateAround(a.w, normalize(axis), thetaO - thetaA));
+    u.cosThetaO = std::cos(thetaO);
+    return u;
+}
+float groupCost(const LBounds& b, const Box& parent, int dim) {
+    const float thetaO = std::acos(sclamp(b.cosThetaO, -1.0f, 1.0f));
+    const float thetaE = std::acos(sclamp(b.cosThetaE, -1.0f, 1.0f));
+    const float thetaW = smin(thetaO + thetaE, kPi);
+    const float sinO = std::sqrt(smax(0.0f, 1.0f - b.cosThetaO * b.cosThetaO));
+    const float mOmega = kTwoPi * (1.0f - b.cosThetaO) +
+                         0.5f * kPi * (2.0f * thetaW * sinO - std::cos(thetaO - 2.0f * thetaW) - 2.0f * thetaO * sinO + b.cosThetaO);
+    const V3 d = parent.diagonal();
+    const float maxD = smax3(d.x, d.y, d.z);
+    const float kr = get(d, dim) > 0.0f ? maxD / get(d, dim) : 1.0f;
+    return b.phi * mOmega * kr * b.bounds.surfaceArea();
+}
+struct LItem {
+    int index;
+    LBounds lb;
+};
+struct LightBvhBuilder {
+    std::vector<LightNodeGPU> nodes;
+    std::vector<LBounds> nodeBounds;
+    std::vector<unsigned long long>* trail;
+    std::vector<uint8_t>* depthOut;
+    int build(std::vector<LItem>& items, int begin, int end, unsigned long long tr, int depth) {
+        const int idx = static_cast<int>(nodes.size());
+        nodes.emplace_back();
+        nodeBounds.emplace_back();
+        std::memset(&nodes.back(), 0, sizeof(LightNodeGPU));
+        nodes.back().child1 = -1;
+        nodes.back().light = -1;
+        if (end - begin == 1) {
+            const LItem& it = items[static_cast<size_t>(begin)];
+            nodeBounds[static_cast<size_t>(idx)] = it.lb;
+            nodes[static_cast<size_t>(idx)].light = it.index;
+            (*trail)[static_cast<size_t>(it.index)] = tr;
+            (*depthOut)[static_cast<size_t>(it.index)] = static_cast<uint8_t>(depth);
+            return idx;
+        }
+        Box bounds, centroids;
+        for (int i = begin; i < end; ++i) {
+            bounds.merge(items[static_cast<size_t>(i)].lb.bounds);
+            centroids.merge(items[static_cast<size_t>(i)].lb.bounds.centroid());
+        }
+        constexpr int kB = 12;
+        float bestCost = std::numeric_limits<float>::infinity();
+        int bestDim = -1, bestBucket = -1;
+        if (depth < 63 - 8) {
+            for (int dim = 0; dim < 3; ++dim) {
+                const float lo = get(centroids.lo, dim), hi = get(centroids.hi, dim);
+                if (!(hi > lo)) continue;
+                LBounds bucket[kB];
+                for (int i = begin; i < end; ++i) {
+                    const LBounds& lb = items[static_cast<size_t>(i)].lb;
+                    int b = static_cast<int>(kB * (get(lb.bounds.centroid(), dim) - lo) / (hi - lo));
+                    b = iclamp(b, 0, kB - 1);
+                    bucket[b] = unionBounds(bucket[b], lb);
+                }
+                for (int split = 0; split < kB - 1; ++split) {
+                    LBounds below, above;
+                    for (int b = 0; b <= split; ++b) below = unionBounds(below, bucket[b]);
+                    for (int b = split + 1; b < kB; ++b) above = unionBounds(above, bucket[b]);
+                    if (!(below.phi > 0.0f) || !(above.phi > 0.0f)) continue;
+                    const float cost = groupCost(below, bounds, dim) + groupCost(above, bounds, dim);
+                    if (cost > 0.0f && cost < bestCost) {
+                        bestCost = cost;
+                        bestDim = dim;
+                        bestBucket = split;
+                    }
+                }
+            }
+        }
+        int mid = -1;
+        if (bestDim >= 0) {
+            const float lo = get(centroids.lo, bestDim), hi = get(centroids.hi, bestDim);
+            auto it = std::partition(items.begin() + begin, items.begin() + end, [&](const LItem& item) {
+                int b = static_cast<int>(kB * (get(item.lb.bounds.centroid(), bestDim) - lo) / (hi - lo));
+                return iclamp(b, 0, kB - 1) <= bestBucket;
+            });
+            mid = static_cast<int>(it - items.begin());
+        }
+        if (mid <= begin || mid >= end) {
+            mid = (begin + end) / 2;
+            const int dim = centroids.maxExtent();
+            std::nth_element(items.begin() + begin, items.begin() + mid, items.begin() + end,
+                             [dim](const LItem& a, const LItem& b) {
+                                 return get(a.lb.bounds.centroid(), dim) < get(b.lb.bounds.centroid(), dim);
+                             });
+        }
+        const int c0 = build(items, begin, mid, tr, depth + 1);
+        const int c1 = build(items, mid, end, tr | (1ull << depth), depth + 1);
+        nodeBounds[static_cast<size_t>(idx)] = unionBounds(nodeBounds[static_cast<size_t>(c0)], nodeBounds[static_cast<size_t>(c1)]);
+        nodes[static_cast<size_t>(idx)].child1 = c1;
+        return idx;
+    }
+};
+
+bool lightBounds(const LightGPU& l, LBounds& out) {
+    const V3 rad = lightRadiance(l);
+    if (!(l.area > 0.0f) || isBlack(rad)) return false;
+    if (l.type == LT_TRIANGLE) {
+        const V3 p0 = m3f(l.p0), p1 = m3f(l.p1), p2 = m3f(l.p2);
+        out.bounds = Box(vmin(vmin(p0, p1), p2), vmax(vmax(p0, p1), p2));
+    } else {
+        const V3 p = m3f(l.p0), u = m3f(l.p1), v = m3f(l.p2);
+        Box b;
+        b.lo = p;
+        b.hi = p;
+        b.merge(p + u);
+        b.merge(p + v);
+        b.merge(p + u + v);
+        out.bounds = b;
+    }
+    out.w = m3f(l.normal);
+    out.phi = smax(0.0f, luminance(rad)) * l.area * kPi;
+    out.cosThetaO = 1.0f;
+    out.cosThetaE = 0.0f;
+    out.twoSided = true;
+    return true;
+}
+
+// ---------------------------------------------------------------------------------------------
+// environment distributions (environment_light.cpp:82-163)
+void buildCdf(const HostEnv& e, const std::vector<float>& func, std::vector<float>& marg, std::vector<float>& cond,
+              float& funcInt, bool& valid) {
+    const int w = e.width, h = e.height;
+    marg.assign(static_cast<size_t>(h) + 1, 0.0f);
+    cond.assign(static_cast<size_t>(h) * static_cast<size_t>(w + 1), 0.0f);
+    for (int y = 0; y < h; ++y) {
+        float* row = cond.data() + static_cast<size_t>(y) * static_cast<size_t>(w + 1);
+        row[0] = 0.0f;
+        for (int x = 0; x < w; ++x) row[x + 1] = row[x] + func[static_cast<size_t>(y) * static_cast<size_t>(w) + static_cast<size_t>(x)];
+        marg[static_cast<size_t>(y) + 1] = marg[static_cast<size_t>(y)] + row[w];
+    }
+    funcInt = marg[static_cast<size_t>(h)];
+    if (!(funcInt > 0.0f)) {
+        funcInt = 0.0f;
+        marg.clear();
+        valid = false;
+        return;
+    }
+    const float inv = 1.0f / funcInt;
+    for (float& c : marg) c *= inv;
+    for (int y = 0; y < h; ++y) {
+        float* row = cond.data() + static_cast<size_t>(y) * static_cast<size_t>(w + 1);
+        const float rowSum = row[w];
+        if (rowSum <= 0.0f) continue;
+        const float invRow = 1.0f / rowSum;
+        for (int x = 0; x <= w; ++x) row[x] *= invRow;
+    }
+    valid = true;
+}
+
+V3 envPixelHost(const HostEnv& e, int x, int y) {
+    const float* p = e.image.data() + 3 * (static_cast<size_t>(y) * static_cast<size_t>(e.width) + static_cast<size_t>(x));
+    return mk(p[0], p[1], p[2]);
+}
+
+void buildEnvironment(HostEnv& e) {
+    e.fullValid = e.misValid = false;
+    e.fullFunc.clear();
+    e.misFunc.clear();
+    e.fullMarg.clear();
+    e.misMarg.clear();
+    e.fullCond.clear();
+    e.misCond.clear();
+    e.fullInt = e.misInt = 0.0f;
+    if (e.hasImage && e.width > 0 && e.height > 0) {
+        const int w = e.width, h = e.height;
+        e.fullFunc.assign(static_cast<size_t>(w) * static_cast<size_t>(h), 0.0f);
+        std::vector<float> sinRow(static_cast<size_t>(h));
+        double weighted = 0.0, weights = 0.0;
+        for (int y = 0; y < h; ++y) {
+            const float sinTheta = std::sin(kPi * (static_cast<float>(y) + 0.5f) / static_cast<float>(h));
+            sinRow[static_cast<size_t>(y)] = sinTheta;
+            for (int x = 0; x < w; ++x) {
+                float L = luminance(envPixelHost(e, x, y));
+                if (!(L > 0.0f)) L = 0.0f;
+                e.fullFunc[static_cast<size_t>(y) * static_cast<size_t>(w) + static_cast<size_t>(x)] = L * sinTheta;
+                weighted += static_cast<double>(L) * sinTheta;
+                weights += sinTheta;
+            }
+        }
+        buildCdf(e, e.fullFunc, e.fullMarg, e.fullCond, e.fullInt, e.fullValid);
+        if (e.fullValid) {
+            const float meanL = weights > 0.0 ? static_cast<float>(weighted / weights) : 0.0f;
+            e.misFunc.resize(e.fullFunc.size());
+            double misTotal = 0.0, fullTotal = 0.0;
+            for (int y = 0; y < h; ++y) {
+                const float s = sinRow[static_cast<size_t>(y)];
+                for (int x = 0; x < w; ++x) {
+                    const size_t i = static_cast<size_t>(y) * static_cast<size_t>(w) + static_cast<size_t>(x);
+                    float L = luminance(envPixelHost(e, x, y));
+                    if (!(L > 0.0f)) L = 0.0f;
+                    const float excess = L - meanL;
+                    e.misFunc[i] = excess > 1e-4f * meanL ? excess * s : 0.0f;
+                    misTotal += e.misFunc[i];
+                    fullTotal += e.fullFunc[i];
+                }
+            }
+            bool comp = misTotal > 1e-3 * fullTotal;
+            if (comp) buildCdf(e, e.misFunc, e.misMarg, e.misCond, e.misInt, e.misValid);
+            comp = comp && e.misValid;
+            if (!comp) {
+                e.misFunc = e.fullFunc;
+                e.misMarg = e.fullMarg;
+                e.misCond = e.fullCond;
+                e.misInt = e.fullInt;
+                e.misValid = e.fullValid;
+            }
+        }
+    }
+    // power() (environment_light.cpp:305-322) and the mean luminance of the constructor.
+    V3 pw;
+    if (!e.hasImage || e.width <= 0) {
+        pw = mk(0.5f) * e.intensity * 4.0f * kPi;
+    } else {
+        V3 sum = mk(0.0f);
+        float wsum = 0.0f;
+        for (int y = 0; y < e.height; y += 4) {
+            const float s = std::sin(kPi * (static_cast<float>(y) + 0.5f) / static_cast<float>(e.height));
+            for (int x = 0; x < e.width; x += 4) {
+                sum += envPixelHost(e, x, y) * s;
+                wsum += s;
+            }
+        }
+        pw = (wsum > 0.0f ? sum / wsum : sum) * e.intensity * 4.0f * kPi;
+    }
+    e.meanLuminance = smax(0.0f, luminance(pw) / (4.0f * kPi));
+    // setSun (environment_light.cpp:211-227)
+    e.sunPdfWeight = 0.0f;
+    if (e.hasSun) {
+        e.sunDir = normalize(e.sunDirIn);
+        e.sunCosMax = sclamp(e.sunCosIn, -0.999f, 0.9999999f);
+        e.sunRadiance = e.sunRadIn * e.intensity;
+        const float omega = kTwoPi * (1.0f - e.sunCosMax);
+        const float sunPower = smax(0.0f, luminance(e.sunRadiance)) * omega;
+        const float skyPower = 4.0f * kPi * e.meanLuminance;
+        if (sunPower > 0.0f) {
+            e.sunPdfWeight = sclamp(sunPower / (sunPower + skyPower), 0.15f, 0.85f);
+            if (!e.fullValid) e.sunPdfWeight = 1.0f;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
+// Material parameters with the reference setters' clamps.
+MatGPU resolveMaterial(const pe_material& m) {
+    MatGPU g;
+    std::memset(&g, 0, sizeof(g));
+    g.type = m.type;
+    auto c3 = [](float* dst, const float* src) { dst[0] = src[0]; dst[1] = src[1]; dst[2] = src[2]; };
+    auto cc3 = [](float* dst, const float* src, float lo, float hi) {
+        for (int i = 0; i < 3; ++i) dst[i] = smax(lo, smin(src[i], hi));
+    };
+    c3(g.base, m.base_color);
+    c3(g.emission, m.emission);
+    if (m.type == PE_MAT_DISNEY) {
+        g.metallic = m.metallic;
+        g.roughness = smax(0.001f, m.roughness);
+        g.specular = m.specular;
+        g.clearcoat = sclamp(m.clearcoat, 0.0f, 1.0f);
+        g.clearcoatRoughness = smax(0.001f, m.clearcoat_roughness);
+        g.ior = sclamp(m.ior, 1.0001f, 3.0f);
+        g.specTrans = sclamp(m.spec_transmission, 0.0f, 1.0f);
+        g.coatIor = sclamp(m.coat_ior, 1.0001f, 3.0f);
+        cc3(g.coatTint, m.coat_tint, 0.0f, 1.0f);
+        if (m.has_sheen_color) {
+            cc3(g.sheenColor, m.sheen_color, 0.0f, 1.0f);
+            g.hasSheenColor = 1;
+        } else {
+            g.sheenColor[0] = g.sheenColor[1] = g.sheenColor[2] = 1.0f;
+        }
+        g.anisotropy = sclamp(m.anisotropy, 0.0f, 1.0f);
+        g.sheen = sclamp(m.sheen, 0.0f, 1.0f);
+        g.sheenRoughness = sclamp(m.sheen_roughness, 0.02f, 1.0f);
+        g.diffuseRoughness = sclamp(m.diffuse_roughness, 0.0f, 1.0f);
+        g.diffuseTransmission = sclamp(m.diffuse_transmission, 0.0f, 1.0f);
+        g.subsurface = sclamp(m.subsurface, 0.0f, 1.0f);
+        cc3(g.ssRadius, m.subsurface_radius, 1e-4f, 1e4f);
+        g.ssScale = smax(m.subsurface_scale, 1e-6f);
+        g.ssAniso = sclamp(m.subsurface_anisotropy, -0.9f, 0.9f);
+        cc3(g.edgeTint, m.edge_tint, 0.0f, 1.0f);
+        g.thinFilmThickness = sclamp(m.thin_film_thickness, 0.0f, 2000.0f);
+        g.thinFilmIor = sclamp(m.thin_film_ior, 1.0f, 3.0f);
+        if (m.flake_density > 0.0f) {
+            g.flakeDensity = sclamp(m.flake_density, 0.0f, 1.0f);
+            g.flakeSize = smax(m.flake_size, 1e-6f);
+            g.flakeRoughness = sclamp(m.flake_roughness, 0.0f, 1.0f);
+            cc3(g.flakeColor, m.flake_color, 0.0f, 1.0f);
+        } else {
+            g.flakeDensity = 0.0f;
+            g.flakeSize = 0.004f;
+            g.flakeRoughness = 0.3f;
+            g.flakeColor[0] = g.flakeColor[1] = g.flakeColor[2] = 0.9f;
+        }
+        g.opacity = sclamp(m.opacity, 0.0f, 1.0f);
+        if (g.specTrans > 0.0f) g.flags |= MF_VOLUME_BOUNDARY;
+        if (g.opacity < 1.0f) g.flags |= MF_TRANSMITS_SHADOWS;
+    } else if (m.type == PE_MAT_DIELECTRIC) {
+        g.ior = m.ior;
+        g.glassRoughness = m.glass_roughness;
+        g.abbe = m.abbe > 0.0f ? smax(m.abbe, 10.0f) : 0.0f;
+        g.thinWalled = m.thin_walled ? 1 : 0;
+        g.filmThickness = m.film_thickness > 0.0f ? m.film_thickness : 0.0f;
+        // rebuildMedium (dielectric.cpp:140-148), evaluated only when a setter called it.
+        if (m.has_absorption || m.has_scattering) {
+            float absorb[3] = {1.0f, 1.0f, 1.0f};
+            float absorbDist = 1.0f;
+            float density = 0.0f;
+            float scol[3] = {1.0f, 1.0f, 1.0f};
+            float aniso = 0.0f;
+            if (m.has_absorption) {
+                cc3(absorb, m.absorb_color, 0.0f, 1.0f);
+                absorbDist = smax(m.absorb_distance, 1e-5f);
+            }
+            if (m.has_scattering) {
+                density = smax(m.scatter_density, 0.0f);
+                cc3(scol, m.scatter_color, 0.0f, 1.0f);
+                aniso = sclamp(m.scatter_anisotropy, -0.95f, 0.95f);
+            }
+            for (int c = 0; c < 3; ++c) {
+                g.sigmaA[c] = -std::log(smax(absorb[c], 1e-4f)) / absorbDist;
+                g.sigmaS[c] = scol[c] * density;
+                g.sigmaA[c] += (1.0f - scol[c]) * density;
+            }
+            g.mediumG = aniso;
+        }
+        if (g.thinWalled || g.glassRoughness <= 1e-3f) g.flags |= MF_DELTA;
+        if (!g.thinWalled) g.flags |= MF_VOLUME_BOUNDARY;
+        if (g.thinWalled) g.flags |= MF_TRANSMITS_SHADOWS;
+        if (g.abbe > 0.0f) g.flags |= MF_DISPERSIVE;
+        const bool emptyMedium = isBlack(m3f(g.sigmaA)) && isBlack(m3f(g.sigmaS));
+        if (!g.thinWalled && !emptyMedium) g.flags |= MF_HAS_MEDIUM;
+        if (!isBlack(m3f(g.sigmaS))) g.flags |= MF_MEDIUM_SCATTERS;
+    } else if (m.type == PE_MAT_MIRROR) {
+        g.flags |= MF_DELTA;
+    }
+    if ((m.type == PE_MAT_LAMBERT || m.type == PE_MAT_DISNEY) && !isBlack(m3f(g.emission))) g.flags |= MF_EMISSIVE;
+    if (!(m.type == PE_MAT_LAMBERT || m.type == PE_MAT_DISNEY)) g.emission[0] = g.emission[1] = g.emission[2] = 0.0f;
+    return g;
+}
+
+// ---------------------------------------------------------------------------------------------
+// GGX / sheen energy tables (microfacet.cpp:36-133), Sobol byte tables, spectral tables.
+float nodeMu(int im) { return smax(static_cast<float>(im) / (kTableN - 1), 1e-3f); }
+
+void buildGgxTables(TablesGPU& T) {
+    constexpr int kS = 24;
+    for (int ia = 0; ia < kTableN; ++ia) {
+        const float alpha = static_cast<float>(ia) / (kTableN - 1);
+        for (int im = 0; im < kTableN; ++im) {
+            const float mu = nodeMu(im);
+            const V3 wo = mk(std::sqrt(smax(0.0f, 1.0f - mu * mu)), 0.0f, mu);
+            const float g1 = ggxG1(wo, alpha, alpha);
+            double sum = 0.0, sumA = 0.0, sumB = 0.0;
+            for (int sy = 0; sy < kS; ++sy)
+                for (int sx = 0; sx < kS; ++sx) {
+                    const float u1 = (static_cast<float>(sx) + 0.5f) / kS;
+                    const float u2 = (static_cast<float>(sy) + 0.5f) / kS;
+                    const V3 h = ggxSampleVisibleNormal(wo, alpha, alpha, u1, u2);
+                    const float c = dot(wo, h);
+                    const V3 wi = h * (2.0f * c) - wo;
+                    if (wi.z <= 0.0f) continue;
+                    const double w = ggxG(wo, wi, alpha, alpha) / g1;
+                    const double s5 = pow5(1.0f - sclamp(c, 0.0f, 1.0f));
+                    sum += w;
+                    sumA += w * (1.0 - s5);
+                    sumB += w * s5;
+                }
+            const int k = ia * kTableN + im;
+            T.ggxE[k] = static_cast<float>(sum / (kS * kS));
+            T.ggxEa[k] = static_cast<float>(sumA / (kS * kS));
+            T.ggxEb[k] = static_cast<float>(sumB / (kS * kS));
+        }
+    }
+    constexpr int kM = 256;
+    for (int ia = 0; ia < kTableN; ++ia) {
+        const float alpha = static_cast<float>(ia) / (kTableN - 1);
+        double a0 = 0.0, a1 = 0.0, a2 = 0.0;
+        for (int i = 0; i < kM; ++i) {
+            const float mu = (static_cast<float>(i) + 0.5f) / kM;
+            const float E = sclamp(tableLookup2D(T.ggxE, mu, alpha), 1e-3f, 1.0f);
+            const float m = 1.0f / E - 1.0f;
+            const float A = tableLookup2D(T.ggxEa, mu, alpha), B = tableLookup2D(T.ggxEb, mu, alpha);
+            const double w = 2.0 * mu / kM;
+            a0 += w * B;
+            a1 += w * (A + B * m);
+            a2 += w * (A * m);
+        }
+        T.avg0[ia] = static_cast<float>(a0);
+        T.avg1[ia] = static_cast<float>(a1);
+        T.avg2[ia] = static_cast<float>(a2);
+    }
+    constexpr int kC = 96, kP = 48;
+    for (int ir = 0; ir < kTableN; ++ir) {
+        const float r = smax(static_cast<float>(ir) / (kTableN - 1), 0.02f);
+        for (int im = 0; im < kTableN; ++im) {
+            const float mu = nodeMu(im);
+            const V3 wo = mk(std::sqrt(smax(0.0f, 1.0f - mu * mu)), 0.0f, mu);
+            double sum = 0.0;
+            for (int i = 0; i < kC; ++i) {
+                const float cz = (static_cast<float>(i) + 0.5f) / kC;
+                const float s = std::sqrt(smax(0.0f, 1.0f - cz * cz));
+                for (int j = 0; j < kP; ++j) {
+                    const float phi = kPi * (static_cast<float>(j) + 0.5f) / kP;
+                    const V3 wi = mk(s * std::cos(phi), s * std::sin(phi), cz);
+                    const V3 h = normalize(wo + wi);
+                    sum += charlieD(h.z, r) * charlieV(cz, mu) * cz;
+                }
+            }
+            T.sheenE[ir * kTableN + im] = static_cast<float>(sum * (1.0 / kC) * (kTwoPi / kP));
+        }
+    }
+}
+
+// Wyman–Sloan–Shirley 2013 CIE fit → linear sRGB (spectral.cpp:15-31).
+float gpiece(float x, float mu, float s1, float s2) {
+    const float t = (x - mu) / (x < mu ? s1 : s2);
+    return std::exp(-0.5f * t * t);
+}
+V3 rawRGB(float l) {
+    const float X = 1.056f * gpiece(l, 599.8f, 37.9f, 31.0f) + 0.362f * gpiece(l, 442.0f, 16.0f, 26.7f) -
+                    0.065f * gpiece(l, 501.1f, 20.4f, 26.2f);
+    const float Y = 0.821f * gpiece(l, 568.8f, 46.9f, 40.5f) + 0.286f * gpiece(l, 530.9f, 16.3f, 31.1f);
+    const float Z = 1.217f * gpiece(l, 437.0f, 11.8f, 36.0f) + 0.681f * gpiece(l, 459.0f, 26.0f, 13.8f);
+    const float r = 3.2404542f * X - 1.5371385f * Y - 0.4985314f * Z;
+    const float gg = -0.9692660f * X + 1.8760108f * Y + 0.0415560f * Z;
+    const float b = 0.0556434f * X - 0.2040259f * Y + 1.0572252f * Z;
+    return mk(smax(0.0f, r), smax(0.0f, gg), smax(0.0f, b));
+}
+void buildSpectral(TablesGPU& T) {
+    const float lmin = 380.0f, lmax = 730.0f;
+    constexpr int kBins = 350;
+    V3 sum = mk(0.0f);
+    constexpr int kSteps = 3500;
+    const float dl = (lmax - lmin) / static_cast<float>(kSteps);
+    for (int i = 0; i < kSteps; ++i) sum += rawRGB(lmin + (static_cast<float>(i) + 0.5f) * dl);
+    const V3 mean = sum / static_cast<float>(kSteps);
+    const V3 norm = mk(1.0f / mean.x, 1.0f / mean.y, 1.0f / mean.z);
+    const float bw = (lmax - lmin) / static_cast<float>(kBins);
+    float acc = 0.0f;
+    T.spectralCdf[0] = 0.0f;
+    float s[kBins];
+    for (int i = 0; i < kBins; ++i) {
+        const V3 c = rawRGB(lmin + (static_cast<float>(i) + 0.5f) * bw) * norm;
+        s[i] = c.x + c.y + c.z + 0.02f;
+        acc += s[i];
+        T.spectralCdf[i + 1] = acc;
+    }
+    for (int i = 0; i <= kBins; ++i) T.spectralCdf[i] /= acc;
+    for (int i = 0; i < kBins; ++i) T.spectralPdf[i] = s[i] / (acc * bw);
+    T.spectralNorm[0] = norm.x;
+    T.spectralNorm[1] = norm.y;
+    T.spectralNorm[2] = norm.z;
+}
+
+} // namespace
+
+const TablesGPU& staticTables() {
+    static const TablesGPU* t = [] {
+        auto* T = new TablesGPU();
+        std::memset(T, 0, sizeof(TablesGPU));
+        buildGgxTables(*T);
+        for (int k = 0; k < 4; ++k)
+            for (uint32_t b = 0; b < 256; ++b) T->sobolTab[k][b] = sobolTableEntry(k, b);
+        buildSpectral(*T);
+        return T;
+    }();
+    return *t;
+}
+
+// PixelFilterSampler (pixel_filter.cpp:39-91): inverse CDF of the separable filter.
+void fillFilterCdf(int type, float width, float* cdf) {
+    width = sclamp(width, 0.25f, 8.0f);
+    const float radius = 0.5f * width;
+    for (int i = 0; i <= kFilterBins; ++i) cdf[i] = 0.0f;
+    if (type == PE_FILTER_BOX) {
+        cdf[0] = -1.0f; // marker: box
+        return;
+    }
+    auto evaluate = [&](float x) -> float {
+        if (std::fabs(x) > radius) return 0.0f;
+        switch (type) {
+            case PE_FILTER_TRIANGLE: return smax(0.0f, 1.0f - std::fabs(x) / radius);
+            case PE_FILTER_GAUSSIAN: {
+                const float s = width / 6.0f;
+                const float k = 1.0f / (2.0f * s * s);
+                return smax(0.0f, std::exp(-k * x * x) - std::exp(-k * radius * radius));
+            }
+            default: {
+                const float a = kTwoPi * (x / width + 0.5f);
+                return 0.35875f - 0.48829f * std::cos(a) + 0.14128f * std::cos(2.0f * a) - 0.01168f * std::cos(3.0f * a);
+            }
+        }
+    };
+    const float dx = width / kFilterBins;
+    double acc = 0.0;
+    for (int i = 0; i < kFilterBins; ++i) {
+        acc += smax(0.0f, evaluate(-radius + (static_cast<float>(i) + 0.5f) * dx));
+        cdf[i + 1] = static_cast<float>(acc);
+    }
+    if (!(acc > 0.0)) {
+        cdf[0] = -1.0f;
+        return;
+    }
+    for (int i = 0; i <= kFilterBins; ++i) cdf[i] = static_cast<float>(cdf[i] / acc);
+    cdf[kFilterBins] = 1.0f;
+}
+
+// ---------------------------------------------------------------------------------------------
+static int32_t buildScene(pe_scene* s) {
+    HostBuild& B = s->build;
+    B = HostBuild{};
+    B.materials = s->materials;
+    // shapes and global triangle / vertex numbering
+    uint32_t nTris = 0, nVerts = 0;
+    for (const HostShape& sh : s->shapes) {
+        nTris += static_cast<uint32_t>(sh.idx.size() / 3);
+        nVerts += static_cast<uint32_t>(sh.pos.size());
+    }
+    if (nTris >= (1u << 23)) {
+        setError("scene has " + std::to_string(nTris) + " triangles; the flattened BVH encodes at most 8388607");
+        return PE_ERR_LIMIT;
+    }
+    B.triVerts.resize(nTris);
+    B.pos.resize(nVerts);
+    B.nrm.resize(nVerts);
+    B.uv.resize(nVerts);
+    B.shapes.resize(s->shapes.size());
+    std::vector<Box> triBounds(nTris);
+    std::vector<uint8_t> triMask(nTris);
+    uint32_t t0 = 0, v0 = 0;
+    for (size_t si = 0; si < s->shapes.size(); ++si) {
+        const HostShape& sh = s->shapes[si];
+        ShapeInfo& info = B.shapes[si];
+        info.material = sh.material;
+        info.emitter = sh.emitter;
+        info.flags = sh.flags;
+        info.firstTri = t0;
+        for (size_t v = 0; v < sh.pos.size(); ++v) {
+            B.pos[v0 + v] = f4(sh.pos[v].x, sh.pos[v].y, sh.pos[v].z, 0.0f);
+            const V3 n = v < sh.nrm.size() ? sh.nrm[v] : mk(0.0f);
+            B.nrm[v0 + v] = f4(n.x, n.y, n.z, 0.0f);
+            float2 uv;
+            uv.x = v < sh.uv.size() ? sh.uv[v].x : 0.0f;
+            uv.y = v < sh.uv.size() ? sh.uv[v].y : 0.0f;
+            B.uv[v0 + v] = uv;
+        }
+        const size_t nt = sh.idx.size() / 3;
+        for (size_t t = 0; t < nt; ++t) {
+            int4 tv;
+            tv.x = static_cast<int>(v0 + sh.idx[3 * t + 0]);
+            tv.y = static_cast<int>(v0 + sh.idx[3 * t + 1]);
+            tv.z = static_cast<int>(v0 + sh.idx[3 * t + 2]);
+            tv.w = static_cast<int>(si);
+            B.triVerts[t0 + t] = tv;
+            const V3 p0 = sh.pos[sh.idx[3 * t]], p1 = sh.pos[sh.idx[3 * t + 1]], p2 = sh.pos[sh.idx[3 * t + 2]];
+            Box b;
+            b.lo = vmin(vmin(p0, p1), p2);
+            b.hi = vmax(vmax(p0, p1), p2);
+            triBounds[t0 + t] = b;
+            triMask[t0 + t] = sh.mask;
+        }
+        t0 += static_cast<uint32_t>(nt);
+        v0 += static_cast<uint32_t>(sh.pos.size());
+        const MatGPU& mg = s->materials[static_cast<size_t>(sh.material)];
+        if (mg.flags & MF_TRANSMITS_SHADOWS) B.hasShadowTransmitters = true;
+    }
+    for (const MatGPU& m : s->materials)
+        if (m.flags & MF_TRANSMITS_SHADOWS) B.hasShadowTransmitters = true; // Scene::retainMaterial
+    for (const MatGPU& m : s->materials)
+        if (m.flags & (MF_VOLUME_BOUNDARY)) B.hasVolumes = true;
+
+    // SAH BVH
+    if (nTris > 0) {
+        SahBuilder sb;
+        sb.prims.reserve(nTris);
+        for (uint32_t i = 0; i < nTris; ++i) sb.prims.emplace_back(i, triBounds[i]);
+        sb.ordered.reserve(nTris);
+        BuildNode* root = sb.build(0, static_cast<int>(nTris));
+        std::vector<RefNode> ref(static_cast<size_t>(sb.total));
+        int offset = 0;
+        sb.flatten(root, ref, &offset, 0, B.maxDepth);
+        if (B.maxDepth + 2 > kMaxStack) {
+            setError("BVH depth " + std::to_string(B.maxDepth) + " exceeds the traversal stack of " +
+                     std::to_string(kMaxStack));
+            return PE_ERR_LIMIT;
+        }
+        // lean triangles in leaf order
+        B.tris.resize(static_cast<size_t>(nTris) * 3);
+        for (size_t i = 0; i < sb.ordered.size(); ++i) {
+            const uint32_t g = static_cast<uint32_t>(sb.ordered[i]);
+            const int4 tv = B.triVerts[g];
+            const V3 p0 = mk(B.pos[tv.x].x, B.pos[tv.x].y, B.pos[tv.x].z);
+            const V3 p1 = mk(B.pos[tv.y].x, B.pos[tv.y].y, B.pos[tv.y].z);
+            const V3 p2 = mk(B.pos[tv.z].x, B.pos[tv.z].y, B.pos[tv.z].z);
+            const V3 e1 = p1 - p0, e2 = p2 - p0;
+            const float eps = 1e-14f * len2(e1) * len2(e2);
+            B.tris[3 * i + 0] = f4(p0.x, p0.y, p0.z, eps);
+            B.tris[3 * i + 1] = f4(e1.x, e1.y, e1.z, bitsf(triMask[g]));
+            B.tris[3 * i + 2] = f4(e2.x, e2.y, e2.z, bitsf(g));
+        }
+        // interior nodes → 64-byte child-box nodes
+        std::vector<int> gpuIndex(ref.size(), -1);
+        int nInterior = 0;
+        for (size_t i = 0; i < ref.size(); ++i) {
+            if (ref[i].count == 0) gpuIndex[i] = nInterior++;
+            else ++B.leaves;
+            if (ref[i].count > 256) {
+                setError("BVH leaf with more than 256 triangles");
+                return PE_ERR_LIMIT;
+            }
+        }
+        auto childRef = [&](int c) -> int {
+            const RefNode& n = ref[static_cast<size_t>(c)];
+            if (n.count > 0) return ~((n.offset << 8) | (n.count - 1));
+            return gpuIndex[static_cast<size_t>(c)];
+        };
+        B.nodes.resize(static_cast<size_t>(nInterior) * 4);
+        for (size_t i = 0; i < ref.size(); ++i) {
+            if (ref[i].count != 0) continue;
+            const int c0 = static_cast<int>(i) + 1, c1 = ref[i].offset;
+            const Box& b0 = ref[static_cast<size_t>(c0)].bounds;
+            const Box& b1 = ref[static_cast<size_t>(c1)].bounds;
+            const size_t k = static_cast<size_t>(gpuIndex[i]) * 4;
+            B.nodes[k + 0] = f4(b0.lo.x, b0.hi.x, b0.lo.y, b0.hi.y);
+            B.nodes[k + 1] = f4(b1.lo.x, b1.hi.x, b1.lo.y, b1.hi.y);
+            B.nodes[k + 2] = f4(b0.lo.z, b0.hi.z, b1.lo.z, b1.hi.z);
+            B.nodes[k + 3] = f4(bitsf(static_cast<uint32_t>(childRef(c0))), bitsf(static_cast<uint32_t>(childRef(c1))), 0.0f, 0.0f);
+        }
+        B.rootIsLeaf = ref[0].count > 0 ? 1 : 0;
+        B.rootFirst = ref[0].count > 0 ? ref[0].offset : 0;
+        B.rootCount = ref[0].count;
+        B.rootMin[0] = ref[0].bounds.lo.x;
+        B.rootMin[1] = ref[0].bounds.lo.y;
+        B.rootMin[2] = ref[0].bounds.lo.z;
+        B.rootMax[0] = ref[0].bounds.hi.x;
+        B.rootMax[1] = ref[0].bounds.hi.y;
+        B.rootMax[2] = ref[0].bounds.hi.z;
+    }
+
+    // lights and light sampler (LightSampler::build)
+    B.lights = s->lights;
+    const int nl = static_cast<int>(B.lights.size());
+    const int count = nl + (s->env.present ? 1 : 0);
+    B.lightCount = count;
+    B.topSlot.assign(static_cast<size_t>(count), -1);
+    B.trail.assign(static_cast<size_t>(count), 0ull);
+    B.trailDepth.assign(static_cast<size_t>(count), 0);
+    B.lightMode = count <= 1 ? 0 : 1;
+    if (count > kMaxExhaustive) {
+        std::vector<LItem> items;
+        for (int i = 0; i < nl; ++i) {
+            LBounds lb;
+            if (lightBounds(B.lights[static_cast<size_t>(i)], lb) && lb.phi > 0.0f) items.push_back({i, lb});
+            else B.infinite.push_back(i);
+        }
+        if (s->env.present) B.infinite.push_back(nl);
+        if (static_cast<int>(B.infinite.size()) + 1 > kMaxInfinite) {
+            B.infinite.clear();
+            B.lightMode = 0; // uniform (light_sampler.cpp:71-75)
+        } else {
+            for (size_t k = 0; k < B.infinite.size(); ++k) B.topSlot[static_cast<size_t>(B.infinite[k])] = static_cast<int16_t>(k);
+            if (!items.empty()) {
+                LightBvhBuilder lb;
+                lb.trail = &B.trail;
+                lb.depthOut = &B.trailDepth;
+                lb.nodes.reserve(2 * items.size());
+                lb.build(items, 0, static_cast<int>(items.size()), 0ull, 0);
+                B.lightNodes = lb.nodes;
+                for (size_t i = 0; i < lb.nodes.size(); ++i) {
+                    const LBounds& b = lb.nodeBounds[i];
+                    LightNodeGPU& n = B.lightNodes[i];
+                    n.bmin[0] = b.bounds.lo.x; n.bmin[1] = b.bounds.lo.y; n.bmin[2] = b.bounds.lo.z;
+                    n.bmax[0] = b.bounds.hi.x; n.bmax[1] = b.bounds.hi.y; n.bmax[2] = b.bounds.hi.z;
+                    n.w[0] = b.w.x; n.w[1] = b.w.y; n.w[2] = b.w.z;
+                    n.phi = b.phi;
+                    n.cosThetaO = b.cosThetaO;
+                    n.cosThetaE = b.cosThetaE;
+                    n.twoSided = b.twoSided ? 1 : 0;
+                }
+            }
+            B.lightMode = 2;
+        }
+    }
+    if (s->env.present) buildEnvironment(s->env);
+    s->built = true;
+    ++s->version;
+    return PE_OK;
+}
+
+const char* lastErrorCStr() { return tlsError.c_str(); }
+
+} // namespace pe
+
+using namespace pe;
+
+extern "C" {
+
+const char* pe_last_error(void) { return pe::lastErrorCStr(); }
+int32_t pe_abi_version(void) { return PE_ABI_VERSION; }
+
+// Reference defaults: DisneyMaterial members (disney.h:213-250), Dielectric members
+// (dielectric.h), specular 0.5.
+void pe_material_defaults(int32_t type, pe_material* m) {
+    if (!m) return;
+    std::memset(m, 0, sizeof(pe_material));
+    m->type = type;
+    for (int i = 0; i < 3; ++i) {
+        m->base_color[i] = 0.8f;
+        m->coat_tint[i] = 1.0f;
+        m->sheen_color[i] = 1.0f;
+        m->edge_tint[i] = 1.0f;
+        m->flake_color[i] = 0.9f;
+        m->absorb_color[i] = 1.0f;
+        m->scatter_color[i] = 1.0f;
+    }
+    m->subsurface_radius[0] = 1.0f;
+    m->subsurface_radius[1] = 0.2f;
+    m->subsurface_radius[2] = 0.1f;
+    m->metallic = 0.0f;
+    m->roughness = 0.5f;
+    m->specular = 0.5f;
+    m->clearcoat_roughness = 0.03f;
+    m->ior = 1.5f;
+    m->coat_ior = 1.5f;
+    m->sheen_roughness = 0.3f;
+    m->subsurface_scale = 0.05f;
+    m->thin_film_ior = 1.4f;
+    m->flake_size = 0.004f;
+    m->flake_roughness = 0.3f;
+    m->opacity = 1.0f;
+    m->absorb_distance = 1.0f;
+    if (type == PE_MAT_DIELECTRIC) {
+        for (int i = 0; i < 3; ++i) m->base_color[i] = 1.0f;
+    }
+}
+
+pe_scene* pe_scene_create(void) { return new (std::nothrow) pe_scene(); }
+void pe_scene_destroy(pe_scene* s) { delete s; }
+
+int32_t pe_scene_add_material(pe_scene* s, const pe_material* m) {
+    if (!s || !m) {
+        setError("pe_scene_add_material: null argument");
+        return -1;
+    }
+    if (m->type < PE_MAT_LAMBERT || m->type > PE_MAT_MIRROR) {
+        setError("pe_scene_add_material: unknown material type " + std::to_string(m->type));
+        return -1;
+    }
+    s->materialsIn.push_back(*m);
+    s->materials.push_back(resolveMaterial(*m));
+    s->built = false;
+    return static_cast<int32_t>(s->materials.size() - 1);
+}
+
+int32_t pe_scene_add_mesh(pe_scene* s, const float* positions, uint32_t nv, const float* normals, const float* uvs,
+                          const uint32_t* indices, uint32_t ntri, int32_t material) {
+    if (!s || (nv && !positions) || (ntri && !indices)) {
+        setError("pe_scene_add_mesh: null argument");
+        return PE_ERR_INVALID;
+    }
+    if (material < 0 || material >= static_cast<int32_t>(s->materials.size())) {
+        setError("pe_scene_add_mesh: material index out of range");
+        return PE_ERR_INVALID;
+    }
+    for (uint64_t i = 0; i < 3ull * ntri; ++i)
+        if (indices[i] >= nv) {
+            setError("pe_scene_add_mesh: vertex index out of range");
+            return PE_ERR_INVALID;
+        }
+    HostShape sh;
+    sh.material = material;
+    sh.pos.resize(nv);
+    for (uint32_t i = 0; i < nv; ++i) sh.pos[i] = mk(positions[3 * i], positions[3 * i + 1], positions[3 * i + 2]);
+    sh.idx.assign(indices, indices + 3ull * ntri);
+    if (normals) {
+        sh.nrm.resize(nv);
+        for (uint32_t i = 0; i < nv; ++i) sh.nrm[i] = mk(normals[3 * i], normals[3 * i + 1], normals[3 * i + 2]);
+    } else if (nv > 0 && ntri > 0) {
+        // TriangleMesh::calculateNormals (mesh.cpp:30-55)
+        sh.nrm.assign(nv, mk(0.0f));
+        for (size_t i = 0; i < sh.idx.size(); i += 3) {
+            const uint32_t a = sh.idx[i], b = sh.idx[i + 1], c = sh.idx[i + 2];
+            const V3 n = cross(sh.pos[b] - sh.pos[a], sh.pos[c] - sh.pos[a]);
+            sh.nrm[a] += n;
+            sh.nrm[b] += n;
+            sh.nrm[c] += n;
+        }
+        for (V3& n : sh.nrm)
+            if (len2(n) > 0.0f) n = normalize(n);
+    }
+    if (!sh.nrm.empty()) sh.flags |= SF_HAS_NORMALS;
+    if (uvs) {
+        sh.uv.resize(nv);
+        for (uint32_t i = 0; i < nv; ++i) sh.uv[i] = mk2(uvs[2 * i], uvs[2 * i + 1]);
+        sh.flags |= SF_HAS_UVS;
+    }
+    // Emissive mesh → one TriangleLight per triangle (scene.cpp:46-62).
+    const MatGPU& mg = s->materials[static_cast<size_t>(material)];
+    if (mg.flags & MF_EMISSIVE) {
+        sh.emitter = static_cast<int32_t>(s->lights.size());
+        for (uint32_t t = 0; t < ntri; ++t) {
+            const V3 p0 = sh.pos[sh.idx[3 * t]], p1 = sh.pos[sh.idx[3 * t + 1]], p2 = sh.pos[sh.idx[3 * t + 2]];
+            LightGPU l;
+            std::memset(&l, 0, sizeof(l));
+            l.type = LT_TRIANGLE;
+            const V3 n = cross(p1 - p0, p2 - p0);
+            const float len = length(n);
+            l.area = 0.5f * len;
+            const V3 nn = len > 0.0f ? n / len : mk(0.0f, 1.0f, 0.0f);
+            l.p0[0] = p0.x; l.p0[1] = p0.y; l.p0[2] = p0.z;
+            l.p1[0] = p1.x; l.p1[1] = p1.y; l.p1[2] = p1.z;
+            l.p2[0] = p2.x; l.p2[1] = p2.y; l.p2[2] = p2.z;
+            l.normal[0] = nn.x; l.normal[1] = nn.y; l.normal[2] = nn.z;
+            l.radiance_r = mg.emission[0];
+            l.radiance_g = mg.emission[1];
+            l.radiance_b = mg.emission[2];
+            s->lights.push_back(l);
+        }
+    }
+    s->shapes.push_back(std::move(sh));
+    s->built = false;
+    return PE_OK;
+}
+
+int32_t pe_scene_add_area_light(pe_scene* s, const float p[3], const float u[3], const float v[3], const float radiance[3],
+                                int32_t visible) {
+    if (!s || !p || !u || !v || !radiance) {
+        setError("pe_scene_add_area_light: null argument");
+        return PE_ERR_INVALID;
+    }
+    const int32_t index = static_cast<int32_t>(s->lights.size());
+    const V3 P = m3f(p), U = m3f(u), Vv = m3f(v);
+    LightGPU l;
+    std::memset(&l, 0, sizeof(l));
+    l.type = LT_AREA;
+    const V3 nrm = cross(U, Vv);
+    l.area = length(nrm);
+    const V3 N = normalize(nrm);
+    const float lu = length(U), lv = length(Vv);
+    l.rectangle = (lu > 0.0f && lv > 0.0f && std::fabs(dot(U, Vv)) <= 1e-4f * lu * lv) ? 1 : 0;
+    for (int i = 0; i < 3; ++i) {
+        l.p0[i] = p[i];
+        l.p1[i] = u[i];
+        l.p2[i] = v[i];
+    }
+    l.normal[0] = N.x; l.normal[1] = N.y; l.normal[2] = N.z;
+    l.radiance_r = radiance[0];
+    l.radiance_g = radiance[1];
+    l.radiance_b = radiance[2];
+    s->lights.push_back(l);
+    // Emissive black Lambertian quad in the BVH (scene.cpp:76-98).
+    pe_material em;
+    pe_material_defaults(PE_MAT_LAMBERT, &em);
+    em.base_color[0] = em.base_color[1] = em.base_color[2] = 0.0f;
+    em.emission[0] = radiance[0];
+    em.emission[1] = radiance[1];
+    em.emission[2] = radiance[2];
+    s->materialsIn.push_back(em);
+    s->materials.push_back(resolveMaterial(em));
+    const int32_t mat = static_cast<int32_t>(s->materials.size() - 1);
+    const V3 p0 = P, p1 = P + U, p2 = p1 + Vv, p3 = P + Vv;
+    const V2 uv0 = mk2(0, 0), uv1 = mk2(1, 0), uv2 = mk2(1, 1), uv3 = mk2(0, 1);
+    const V3 tris[2][3] = {{p0, p1, p2}, {p0, p2, p3}};
+    const V2 uvs[2][3] = {{uv0, uv1, uv2}, {uv0, uv2, uv3}};
+    for (int t = 0; t < 2; ++t) {
+        HostShape sh;
+        sh.material = mat;
+        sh.emitter = index;
+        sh.flags = SF_AREA_TRIANGLE | SF_HAS_NORMALS | SF_HAS_UVS;
+        for (int k = 0; k < 3; ++k) {
+            sh.pos.push_back(tris[t][k]);
+            sh.nrm.push_back(N);
+            sh.uv.push_back(uvs[t][k]);
+        }
+        sh.idx = {0, 1, 2};
+        if (!visible) {
+            sh.flags |= SF_CAMERA_INVISIBLE;
+            sh.mask = static_cast<uint8_t>(0x1F & ~1u);
+        }
+        s->shapes.push_back(std::move(sh));
+    }
+    s->built = false;
+    return PE_OK;
+}
+
+int32_t pe_scene_set_environment(pe_scene* s, const float* rgb, int32_t w, int32_t h, float rotation, float intensity) {
+    if (!s) {
+        setError("pe_scene_set_environment: null scene");
+        return PE_ERR_INVALID;
+    }
+    HostEnv& e = s->env;
+    const bool hadSun = e.hasSun;
+    const V3 sd = e.sunDirIn, sr = e.sunRadIn;
+    const float sc = e.sunCosIn;
+    e = HostEnv{};
+    e.present = true;
+    e.rotation = rotation;
+    e.intensity = intensity;
+    if (rgb && w > 0 && h > 0) {
+        e.hasImage = true;
+        e.width = w;
+        e.height = h;
+        e.image.assign(rgb, rgb + 3ull * static_cast<size_t>(w) * static_cast<size_t>(h));
+    }
+    e.hasSun = hadSun;
+    e.sunDirIn = sd;
+    e.sunRadIn = sr;
+    e.sunCosIn = sc;
+    s->built = false;
+    return PE_OK;
+}
+
+int32_t pe_scene_set_sun(pe_scene* s, const float direction[3], float cos_max, const float radiance[3]) {
+    if (!s || !direction || !radiance) {
+        setError("pe_scene_set_sun: null argument");
+        return PE_ERR_INVALID;
+    }
+    s->env.hasSun = true;
+    s->env.sunDirIn = m3f(direction);
+    s->env.sunCosIn = cos_max;
+    s->env.sunRadIn = m3f(radiance);
+    s->built = false;
+    return PE_OK;
+}
+
+int32_t pe_scene_set_background(pe_scene* s, int32_t mode, const float color[3]) {
+    if (!s || mode < PE_BG_ENVIRONMENT || mode > PE_BG_TRANSPARENT) {
+        setError("pe_scene_set_background: bad argument");
+        return PE_ERR_INVALID;
+    }
+    s->bgMode = mode;
+    if (color)
+        for (int i = 0; i < 3; ++i) s->bgColor[i] = color[i];
+    return PE_OK;
+}
+
+int32_t pe_scene_build(pe_scene* s) {
+    if (!s) {
+        setError("pe_scene_build: null scene");
+        return PE_ERR_INVALID;
+    }
+    try {
+        return pe::buildScene(s);
+    } catch (const std::bad_alloc&) {
+        setError("pe_scene_build: host out of memory");
+        return PE_ERR_OOM;
+    }
+}
+
+int32_t pe_scene_get_info(const pe_scene* s, pe_scene_info* out) {
+    if (!s || !out) {
+        setError("pe_scene_get_info: null argument");
+        return PE_ERR_INVALID;
+    }
+    std::memset(out, 0, sizeof(*out));
+    const HostBuild& B = s->build;
+    out->triangles = B.triVerts.size();
+    out->bvh_nodes = B.nodes.size() / 4;
+    out->bvh_leaves = B.leaves;
+    out->lights = B.lights.size();
+    out->light_bvh_nodes = B.lightNodes.size();
+    out->has_environment = s->env.present ? 1 : 0;
+    out->light_sampler_mode = B.lightMode;
+    out->device_bytes = B.nodes.size() * sizeof(float4) + B.tris.size() * sizeof(float4) +
+                        B.triVerts.size() * sizeof(int4) + B.pos.size() * sizeof(float4) * 2 + B.uv.size() * sizeof(float2);
+    return s->built ? PE_OK : PE_ERR_INVALID;
+}
+
+// PerspectiveCamera constructor + describeGpu (perspective_camera.cpp:12-57).
+void pe_camera_perspective(const float position[3], const float target[3], const float up[3], float vfov, float aspect,
+                           pe_camera* out) {
+    if (!out) return;
+    const V3 pos = m3f(position), tgt = m3f(target), upv = m3f(up);
+    const float theta = vfov * (kPi / 180.0f);
+    const float h = std::tan(theta * 0.5f);
+    const float vh = 2.0f * h;
+    const float vw = aspect * vh;
+    const V3 w = normalize(pos - tgt);
+    const V3 u = normalize(cross(upv, w));
+    const V3 v = cross(w, u);
+    const V3 horizontal = vw * u;
+    const V3 vertical = vh * v;
+    const V3 lowerLeft = pos - horizontal * 0.5f - vertical * 0.5f - w;
+    auto put = [](float* o, V3 a) { o[0] = a.x; o[1] = a.y; o[2] = a.z; };
+    put(out->position, pos);
+    put(out->lower_left, lowerLeft);
+    put(out->horizontal, horizontal);
+    put(out->vertical, vertical);
+    put(out->u, u);
+    put(out->v, v);
+    put(out->forward, -w);
+    out->lens_radius = 0.0f;
+    out->orthographic = 0;
+}
+
+} // extern "C"

@@ -1,0 +1,89 @@
+// pe_host.h — host-side scene representation and the flattened build the device uploads.
+#pragma once
+
+#include "photon_cuda.h"
+#include "pe_scene.h"
+
+#include <string>
+#include <vector>
+
+namespace pe {
+
+struct HostShape {
+    std::vector<V3> pos, nrm;
+    std::vector<V2> uv;
+    std::vector<uint32_t> idx;
+    int32_t material = -1;
+    uint32_t flags = 0;
+    int32_t emitter = -1;
+    uint8_t mask = 0x1F;
+};
+
+struct HostEnv {
+    bool present = false;
+    bool hasImage = false;
+    int width = 0, height = 0;
+    float rotation = 0.0f, intensity = 1.0f;
+    std::vector<float> image;                 // w*h*3
+    std::vector<float> fullFunc, misFunc;     // w*h
+    std::vector<float> fullMarg, misMarg;     // h+1
+    std::vector<float> fullCond, misCond;     // h*(w+1)
+    float fullInt = 0.0f, misInt = 0.0f;
+    bool fullValid = false, misValid = false;
+    float meanLuminance = 0.0f;
+    float sunPdfWeight = 0.0f;
+    V3 sunDir{0, 1, 0};
+    float sunCosMax = 1.0f;
+    V3 sunRadiance{0, 0, 0};
+    bool hasSun = false;
+    V3 sunDirIn{0, 1, 0};
+    float sunCosIn = 1.0f;
+    V3 sunRadIn{0, 0, 0};
+};
+
+// Everything the device uploads, as flat host arrays.
+struct HostBuild {
+    std::vector<float4> nodes;       // 4 per interior node
+    std::vector<float4> tris;        // 3 per leaf-ordered triangle
+    std::vector<int4> triVerts;      // per global triangle
+    std::vector<float4> pos, nrm;    // per vertex (global)
+    std::vector<float2> uv;
+    std::vector<ShapeInfo> shapes;
+    std::vector<MatGPU> materials;
+    std::vector<LightGPU> lights;
+    std::vector<LightNodeGPU> lightNodes;
+    std::vector<int16_t> topSlot;
+    std::vector<unsigned long long> trail;
+    std::vector<uint8_t> trailDepth;
+    std::vector<int32_t> infinite;
+    int32_t lightMode = 0;
+    int32_t lightCount = 0;
+    int32_t rootIsLeaf = 0, rootFirst = 0, rootCount = 0;
+    float rootMin[3] = {0, 0, 0}, rootMax[3] = {0, 0, 0};
+    uint64_t leaves = 0;
+    int maxDepth = 0;
+    bool hasShadowTransmitters = false;
+    bool hasVolumes = false;
+};
+
+} // namespace pe
+
+struct pe_scene {
+    std::vector<pe_material> materialsIn;
+    std::vector<pe::MatGPU> materials;
+    std::vector<pe::HostShape> shapes;
+    std::vector<pe::LightGPU> lights;
+    pe::HostEnv env;
+    int32_t bgMode = PE_BG_ENVIRONMENT;
+    float bgColor[3] = {0.18f, 0.18f, 0.18f};
+    bool built = false;
+    pe::HostBuild build;
+    uint64_t version = 0;
+};
+
+namespace pe {
+// Thread-local last error shared by the host and device halves of the ABI.
+void setError(const std::string& msg);
+const TablesGPU& staticTables();           // GGX / sheen / Sobol / spectral tables
+void fillFilterCdf(int type, float width, float* cdf); // 513 entries; cdf[0] = -1 for box
+}

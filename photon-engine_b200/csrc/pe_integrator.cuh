@@ -1,0 +1,444 @@
+// pe_integrator.cuh — the wavefront form of PathTracer::Li (src/integrators/path_tracer.cpp:321-890).
+//
+// One path slot per (pixel, sample) of a wave.  A slot's state lives in HBM as SoA float4
+// columns; each bounce runs three persistent kernels over compacted queues:
+//   closest-hit  (queue of live rays)            → hit records
+//   shade        (same queue) → next-ray queue + shadow queue (warp-aggregated appends)
+//   any-hit      (shadow queue)                  → adds visible NEE terms to the slot's L
+// The state machine below is Li's loop body split at its two scene queries.  Radiance terms are
+// added to L in the reference's order (emission of vertex k, NEE of vertex k, emission of
+// vertex k+1, ...), and each slot draws Sobol dimensions in the reference's order.
+#pragma once
+
+#include "pe_bsdf.h"
+#include "pe_light.h"
+#include "pe_trace.cuh"
+
+namespace pe {
+
+enum VisMask : uint32_t { VIS_CAMERA = 1u, VIS_DIFFUSE = 2u, VIS_GLOSSY = 4u, VIS_TRANSMISSION = 8u, VIS_SHADOW = 16u };
+
+// path flags (bits of state word)
+enum PathFlags : uint32_t {
+    PF_SPECULAR_BOUNCE = 1u << 0,
+    PF_CAMERA_RAY = 1u << 1,
+    PF_PICKER_VALID = 1u << 2,
+    PF_FIRST_SEGMENT = 1u << 3,
+};
+
+// Per-slot state columns (capacity P slots).
+struct Paths {
+    float4* rayO;    // origin xyz, visibility mask (bits)
+    float4* rayD;    // direction xyz, lastBsdfPdf
+    float4* thr;     // throughput xyz, wavelength
+    float4* L;       // radiance xyz, unused
+    float4* lastN;   // last shading normal xyz, flags (bits)
+    float4* lastP;   // last point xyz, Sobol dimension (bits)
+    float4* pickP;   // light-picker point xyz, pixel hash (bits)
+    float4* pickN;   // light-picker normal xyz, counters (bits: depth | diffuseBounces<<8 | passThroughs<<16 | skips<<24)
+    float4* hit;     // t, u, v, leaf prim (bits)
+    int32_t* queueA;
+    int32_t* queueB;
+    int32_t* shadowQ;
+    float4* shO;     // shadow origin xyz, tMax
+    float4* shD;     // shadow direction xyz, scalar (cos*w/(pdf*n))
+    float4* shC;     // f*Li xyz, flags (bit0: indirect)
+    float4* shT;     // throughput at NEE xyz
+    uint32_t* counters; // [0] queue A count, [1] queue B count, [2] shadow count, [3] error flags, [4..] stats
+};
+
+struct WaveArgs {
+    CamDev cam;
+    int width, height;
+    int pixelFirst, nPix;   // pixel range of this wave
+    int sampleFirst, nSamples;
+    uint64_t seed;
+    float filterWidth;
+    int maxDepth, rrDepth, shadowSamples;
+    float clampIndirect;
+};
+
+__device__ __forceinline__ uint32_t packCounters(int depth, int diffuse, int pass, int skips) {
+    return static_cast<uint32_t>(depth) | (static_cast<uint32_t>(diffuse) << 8) | (static_cast<uint32_t>(pass) << 16) |
+           (static_cast<uint32_t>(skips) << 24);
+}
+
+// Warp-aggregated queue append: one atomicAdd per warp (ballot + popc).
+__device__ __forceinline__ void queuePush(int32_t* queue, uint32_t* counter, bool want, int32_t value) {
+    const unsigned mask = __ballot_sync(__activemask(), want);
+    if (!want) return;
+    const int lane = threadIdx.x & 31;
+    const int leader = __ffs(mask) - 1;
+    const int rank = __popc(mask & ((1u << lane) - 1u));
+    uint32_t base = 0;
+    if (lane == leader) base = atomicAdd(counter, static_cast<uint32_t>(__popc(mask)));
+    base = __shfl_sync(mask, base, leader);
+    queue[base + rank] = value;
+}
+
+// ---- generate: camera rays for every slot of the wave ------------------------------------------
+__global__ void kGenerate(SceneGPU S, Paths P, WaveArgs A, int nSlots) {
+    const TablesGPU* T = S.tables;
+    for (int slot = blockIdx.x * blockDim.x + threadIdx.x; slot < nSlots; slot += gridDim.x * blockDim.x) {
+        const int sOff = slot / A.nPix;
+        const int pix = A.pixelFirst + (slot - sOff * A.nPix);
+        const int x = pix % A.width, y = pix / A.width;
+        Sobol sb;
+        sb.pixelHash = pixelHashOf(A.seed, x, y);
+        sb.revIndex = rev32(static_cast<uint32_t>(A.sampleFirst + sOff));
+        sb.dim = 0;
+        V3 o, d;
+        cameraRay(T, A.cam, A.filterWidth, x, y, A.width, A.height, sb, o, d);
+        P.rayO[slot] = make_float4(o.x, o.y, o.z, __uint_as_float(VIS_CAMERA));
+        P.rayD[slot] = make_float4(d.x, d.y, d.z, 0.0f);
+        P.thr[slot] = make_float4(1.0f, 1.0f, 1.0f, 0.0f);
+        P.L[slot] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        P.lastN[slot] = make_float4(0.0f, 1.0f, 0.0f, __uint_as_float(PF_SPECULAR_BOUNCE | PF_CAMERA_RAY | PF_FIRST_SEGMENT));
+        P.lastP[slot] = make_float4(o.x, o.y, o.z, __uint_as_float(sb.dim));
+        P.pickP[slot] = make_float4(0.0f, 0.0f, 0.0f, __uint_as_float(sb.pixelHash));
+        P.pickN[slot] = make_float4(0.0f, 0.0f, 0.0f, __uint_as_float(packCounters(0, 0, 0, 0)));
+        P.queueA[slot] = slot;
+    }
+}
+
+// ---- closest hit over a queue -----------------------------------------------------------------
+template <bool COUNT>
+__global__ void __launch_bounds__(128) kIntersect(SceneGPU S, Paths P, const int32_t* queue, const uint32_t* count,
+                                                  unsigned long long* stats) {
+    const int n = static_cast<int>(*count);
+    uint32_t nodes = 0, tris = 0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const int slot = queue[i];
+        const float4 ro = P.rayO[slot];
+        const float4 rd = P.rayD[slot];
+        const Hit h = traceClosest<COUNT>(S, mk(ro.x, ro.y, ro.z), mk(rd.x, rd.y, rd.z), __float_as_uint(ro.w), 0.0f,
+                                          1e30f, nodes, tris);
+        P.hit[slot] = make_float4(h.t, h.u, h.v, __int_as_float(h.prim));
+    }
+    if (COUNT) {
+        atomicAdd(&stats[0], static_cast<unsigned long long>(nodes));
+        atomicAdd(&stats[1], static_cast<unsigned long long>(tris));
+    }
+}
+
+// ---- any hit over the shadow queue ------------------------------------------------------------
+template <bool COUNT>
+__global__ void __launch_bounds__(128) kShadow(SceneGPU S, Paths P, const uint32_t* count, float clampIndirect,
+                                               unsigned long long* stats) {
+    const int n = static_cast<int>(*count);
+    uint32_t nodes = 0, tris = 0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const int slot = P.shadowQ[i];
+        const float4 so = P.shO[i];
+        const float4 sd = P.shD[i];
+        const bool occluded = traceAny<COUNT>(S, mk(so.x, so.y, so.z), mk(sd.x, sd.y, sd.z), VIS_SHADOW, 0.0f, so.w, nodes, tris);
+        if (occluded) continue;
+        const float4 sc = P.shC[i];
+        const float4 st = P.shT[i];
+        // neeLocal = f * Li * vis * (cos * w / (lightPdf * n)), vis = 1 on this path
+        const V3 neeLocal = (mk(sc.x, sc.y, sc.z) * mk(1.0f)) * sd.w;
+        V3 c = mk(st.x, st.y, st.z) * neeLocal;
+        if ((__float_as_uint(sc.w) & 1u) && clampIndirect > 0.0f) {
+            const float m = smax3(c.x, c.y, c.z);
+            if (m > clampIndirect) c = c * (clampIndirect / m);
+        }
+        if (!isFinite3(c)) continue;
+        float4 L = P.L[slot];
+        L.x += c.x;
+        L.y += c.y;
+        L.z += c.z;
+        P.L[slot] = L;
+    }
+    if (COUNT) {
+        atomicAdd(&stats[2], static_cast<unsigned long long>(nodes));
+        atomicAdd(&stats[3], static_cast<unsigned long long>(tris));
+    }
+}
+
+__device__ __forceinline__ void addL(float4& L, V3 c) {
+    if (!isFinite3(c)) return; // accumulate(): non-finite terms are skipped (path_tracer.cpp:355-359)
+    L.x += c.x;
+    L.y += c.y;
+    L.z += c.z;
+}
+
+// ---- shade: Li's loop body between two closest-hit queries ------------------------------------
+__global__ void __launch_bounds__(128) kShade(SceneGPU S, Paths P, WaveArgs A, const int32_t* queue, const uint32_t* count,
+                                              int32_t* nextQueue, uint32_t* nextCount) {
+    const TablesGPU* T = S.tables;
+    const int n = static_cast<int>(*count);
+    const int stride = gridDim.x * blockDim.x;
+    const int nIter = (n + stride - 1) / stride;
+    for (int it = 0; it < nIter; ++it) {
+        const int i = it * stride + blockIdx.x * blockDim.x + threadIdx.x;
+        bool cont = false;
+        int slot = -1;
+        if (i < n) {
+            slot = queue[i];
+            float4 ro = P.rayO[slot];
+            float4 rd = P.rayD[slot];
+            float4 th = P.thr[slot];
+            float4 L = P.L[slot];
+            float4 ln = P.lastN[slot];
+            float4 lp = P.lastP[slot];
+            float4 pp = P.pickP[slot];
+            float4 pn = P.pickN[slot];
+            const float4 hr = P.hit[slot];
+            uint32_t flags = __float_as_uint(ln.w);
+            uint32_t ctr = __float_as_uint(pn.w);
+            int depth = ctr & 0xFF, diffuseBounces = (ctr >> 8) & 0xFF, passThroughs = (ctr >> 16) & 0xFF,
+                skips = (ctr >> 24) & 0xFF;
+            Sobol sb;
+            sb.pixelHash = __float_as_uint(pp.w);
+            {
+                const int sOff = slot / A.nPix;
+                sb.revIndex = rev32(static_cast<uint32_t>(A.sampleFirst + sOff));
+            }
+            sb.dim = __float_as_uint(lp.w);
+            V3 thr = mk(th.x, th.y, th.z);
+            const V3 dir = mk(rd.x, rd.y, rd.z);
+            const V3 rayO = mk(ro.x, ro.y, ro.z);
+            const uint32_t rayMask = __float_as_uint(ro.w);
+            const float lastBsdfPdf = rd.w;
+            const bool specularBounce = flags & PF_SPECULAR_BOUNCE;
+            bool cameraRay = flags & PF_CAMERA_RAY;
+            const int shadowSamples = A.shadowSamples;
+            const int explicitLights = S.nLights;
+            const int prim = __float_as_int(hr.w);
+            const bool hit = prim >= 0;
+            Isect is;
+            bool done = false;
+            if (hit) {
+                Hit h;
+                h.t = hr.x;
+                h.u = hr.y;
+                h.v = hr.z;
+                h.prim = prim;
+                fillHit(S, h, dir, is);
+                // Camera-invisible light quads are passed through by camera rays; the vertex
+                // does not count (path_tracer.cpp:426-439).  Cutouts are not supported here.
+                if (cameraRay && (S.shapes[is.shape].flags & SF_CAMERA_INVISIBLE) && skips < 64) {
+                    const V3 no = offsetRayOrigin(is.point, is.pError, is.ng, dir);
+                    P.rayO[slot] = make_float4(no.x, no.y, no.z, ro.w);
+                    P.pickN[slot] = make_float4(pn.x, pn.y, pn.z, __uint_as_float(packCounters(depth, diffuseBounces, passThroughs, skips + 1)));
+                    cont = true;
+                    done = true;
+                }
+            }
+            if (!done) {
+                flags &= ~PF_FIRST_SEGMENT;
+                const V3 wo = -dir;
+                if (!hit) {
+                    // environment / background (path_tracer.cpp:482-514)
+                    if (depth == 0 && S.bgMode != PE_BG_ENVIRONMENT) {
+                        if (S.bgMode == PE_BG_COLOR) addL(L, thr * m3f(S.bgColor));
+                    } else if (S.env.present) {
+                        const V3 Le = envEval(S.env, dir);
+                        float weight = 1.0f;
+                        if (!specularBounce) {
+                            float pmf = 0.0f;
+                            if (flags & PF_PICKER_VALID) {
+                                LightCtx c;
+                                lightPrepare(S, mk(pp.x, pp.y, pp.z), mk(pn.x, pn.y, pn.z), c);
+                                pmf = lightCtxPmf(S, c, explicitLights);
+                            }
+                            const float lightPdf = pmf * envPdf(S.env, dir);
+                            weight = powerHeuristic(1, lastBsdfPdf, shadowSamples, lightPdf);
+                        }
+                        V3 c = thr * (Le * weight);
+                        if (diffuseBounces >= 2 && A.clampIndirect > 0.0f) {
+                            const float m = smax3(c.x, c.y, c.z);
+                            if (m > A.clampIndirect) c = c * (A.clampIndirect / m);
+                        }
+                        addL(L, c);
+                    }
+                    done = true;
+                } else {
+                    const MatGPU& mat = S.materials[is.material];
+                    // emission with MIS against the previous vertex's NEE (path_tracer.cpp:565-593)
+                    if (mat.flags & MF_EMISSIVE) {
+                        const ShapeInfo& sh = S.shapes[is.shape];
+                        int li = -1;
+                        if (sh.emitter >= 0)
+                            li = (sh.flags & SF_AREA_TRIANGLE) ? sh.emitter : sh.emitter + (is.tri - static_cast<int>(sh.firstTri));
+                        float weight = 1.0f;
+                        if (!specularBounce) {
+                            float lightPdf = 0.0f;
+                            if (li >= 0) {
+                                float pmf = 0.0f;
+                                if (flags & PF_PICKER_VALID) {
+                                    LightCtx c;
+                                    lightPrepare(S, mk(pp.x, pp.y, pp.z), mk(pn.x, pn.y, pn.z), c);
+                                    pmf = lightCtxPmf(S, c, li);
+                                }
+                                lightPdf = pmf * lightPdfHit(S.lights[li], mk(lp.x, lp.y, lp.z), is.point);
+                            }
+                            if (lightPdf > 0.0f && lastBsdfPdf > 0.0f)
+                                weight = powerHeuristic(1, lastBsdfPdf, shadowSamples, lightPdf);
+                        }
+                        V3 c = thr * (m3f(mat.emission) * weight);
+                        if (diffuseBounces >= 2 && A.clampIndirect > 0.0f) {
+                            const float m = smax3(c.x, c.y, c.z);
+                            if (m > A.clampIndirect) c = c * (A.clampIndirect / m);
+                        }
+                        addL(L, c);
+                    }
+                    if (depth >= A.maxDepth) done = true;
+                }
+                if (!done) {
+                    const MatGPU& mat = S.materials[is.material];
+                    ShadePoint sp;
+                    sp.p = is.point;
+                    sp.n = is.normal;
+                    sp.ng = is.ng;
+                    sp.tangent = is.tangent;
+                    sp.frontFace = is.frontFace;
+                    sp.wavelength = 0.0f;
+                    const bool isSpecular = (mat.flags & MF_DELTA) != 0;
+                    // next-event estimation (path_tracer.cpp:631-698)
+                    if (S.lightCount > 0 && !isSpecular) {
+                        LightCtx picker;
+                        lightPrepare(S, is.point, is.normal, picker);
+                        flags |= PF_PICKER_VALID;
+                        pp = make_float4(is.point.x, is.point.y, is.point.z, pp.w);
+                        pn.x = is.normal.x;
+                        pn.y = is.normal.y;
+                        pn.z = is.normal.z;
+                        for (int s = 0; s < shadowSamples; ++s) {
+                            float lightPmf = 0.0f;
+                            const int lightIndex = lightCtxSample(S, picker, get1D(sb), lightPmf);
+                            if (lightIndex < 0 || !(lightPmf > 0.0f)) {
+                                (void)get2D(T, sb);
+                                continue;
+                            }
+                            const bool fromEnv = lightIndex >= explicitLights;
+                            const V2 ul = get2D(T, sb);
+                            const LightSample ls = fromEnv ? envSample(S.env, ul) : sampleLight(S.lights[lightIndex], is.point, ul);
+                            if (!lsValid(ls)) continue;
+                            V3 so, sd;
+                            float stMax;
+                            if (!makeShadowRay(is, ls.wi, ls.distance, so, sd, stMax)) continue;
+                            float bsdfPdf = 0.0f;
+                            const V3 f = bsdfEvalPdf(T, mat, wo, ls.wi, sp, bsdfPdf, nullptr);
+                            const float cosTheta = fabsf(dot(ls.wi, is.normal));
+                            if (isBlack(f) || !(cosTheta > 0.0f)) continue;
+                            const float lightPdf = lightPmf * ls.pdf;
+                            const float weight = powerHeuristic(shadowSamples, lightPdf, 1, bsdfPdf);
+                            const float scalar = cosTheta * weight / (lightPdf * static_cast<float>(shadowSamples));
+                            const V3 fLi = f * ls.Li;
+                            uint32_t pos;
+                            {
+                                // shadow queue append (one record per sample)
+                                pos = atomicAdd(&P.counters[2], 1u);
+                            }
+                            P.shadowQ[pos] = slot;
+                            P.shO[pos] = make_float4(so.x, so.y, so.z, stMax);
+                            P.shD[pos] = make_float4(sd.x, sd.y, sd.z, scalar);
+                            P.shC[pos] = make_float4(fLi.x, fLi.y, fLi.z, __uint_as_float(diffuseBounces >= 1 ? 1u : 0u));
+                            P.shT[pos] = make_float4(thr.x, thr.y, thr.z, 0.0f);
+                        }
+                    }
+                    // BSDF sampling (path_tracer.cpp:700-743)
+                    const float uc = get1D(sb);
+                    const V2 u2 = get2D(T, sb);
+                    BsdfSample bs;
+                    const bool sampled = bsdfSample(T, mat, wo, sp, uc, u2, bs);
+                    if (!sampled || bs.subsurface || bs.pdf <= 0.0f || isBlack(bs.f)) {
+                        done = true;
+                    } else if (bs.passThrough) {
+                        thr *= bs.f * (fabsf(dot(bs.wi, is.normal)) / bs.pdf);
+                        if (!isFinite3(thr) || ++passThroughs > 64) {
+                            done = true;
+                        } else {
+                            const V3 no = spawnOrigin(is, bs.wi);
+                            ro = make_float4(no.x, no.y, no.z, ro.w);
+                            rd = make_float4(bs.wi.x, bs.wi.y, bs.wi.z, rd.w);
+                            skips = 0;
+                            cont = true;
+                        }
+                    } else {
+                        const V3 wi = bs.wi;
+                        const bool refracted = dot(wo, is.ng) * dot(wi, is.ng) < 0.0f;
+                        const float cosTheta = fabsf(dot(wi, is.normal));
+                        thr *= bs.f * (cosTheta / bs.pdf);
+                        if (!isFinite3(thr)) {
+                            done = true;
+                        } else {
+                            flags = bs.delta ? (flags | PF_SPECULAR_BOUNCE) : (flags & ~PF_SPECULAR_BOUNCE);
+                            if (!bs.delta) ++diffuseBounces;
+                            cameraRay = cameraRay && bs.delta && dot(wi, is.normal) < 0.0f;
+                            flags = cameraRay ? (flags | PF_CAMERA_RAY) : (flags & ~PF_CAMERA_RAY);
+                            const uint32_t nextMask = refracted ? VIS_TRANSMISSION : (bs.delta ? VIS_GLOSSY : VIS_DIFFUSE);
+                            ln = make_float4(is.normal.x, is.normal.y, is.normal.z, 0.0f);
+                            lp = make_float4(is.point.x, is.point.y, is.point.z, 0.0f);
+                            const V3 no = spawnOrigin(is, wi);
+                            ro = make_float4(no.x, no.y, no.z, __uint_as_float(nextMask));
+                            rd = make_float4(wi.x, wi.y, wi.z, bs.pdf);
+                            ++depth;
+                            skips = 0;
+                            cont = true;
+                            if (depth > A.rrDepth) {
+                                // russianRoulette (path_tracer.cpp:131-137)
+                                const float m = smax3(thr.x, thr.y, thr.z);
+                                if (!(m >= 1.0f)) {
+                                    if (!(m > 0.0f) || get1D(sb) >= m) {
+                                        cont = false;
+                                        done = true;
+                                    } else {
+                                        thr /= m;
+                                    }
+                                }
+                            }
+                        }
+                    }
+                }
+            }
+            // write back
+            P.L[slot] = L;
+            if (cont) {
+                P.rayO[slot] = ro;
+                P.rayD[slot] = rd;
+                P.thr[slot] = make_float4(thr.x, thr.y, thr.z, th.w);
+                P.lastN[slot] = make_float4(ln.x, ln.y, ln.z, __uint_as_float(flags));
+                P.lastP[slot] = make_float4(lp.x, lp.y, lp.z, __uint_as_float(sb.dim));
+                P.pickP[slot] = pp;
+                P.pickN[slot] = make_float4(pn.x, pn.y, pn.z, __uint_as_float(packCounters(depth, diffuseBounces, passThroughs, skips)));
+            }
+            (void)done;
+        }
+        queuePush(nextQueue, nextCount, cont, slot);
+    }
+}
+
+// ---- film: Film::addSample in sample order per pixel (src/core/image/film.cpp:56-69) ----------
+__global__ void kFilm(Paths P, WaveArgs A, float* sum, uint32_t* cnt, float* sumSq, unsigned long long* rejected) {
+    unsigned long long rej = 0;
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < A.nPix; p += gridDim.x * blockDim.x) {
+        const int pix = A.pixelFirst + p;
+        float sr = sum[3 * pix + 0], sg = sum[3 * pix + 1], sbb = sum[3 * pix + 2];
+        float sq = sumSq[pix];
+        uint32_t c = cnt[pix];
+        for (int s = 0; s < A.nSamples; ++s) {
+            const float4 L = P.L[s * A.nPix + p];
+            ++c;
+            const bool ok = finitef(L.x) && finitef(L.y) && finitef(L.z) && L.x >= 0.0f && L.y >= 0.0f && L.z >= 0.0f;
+            if (!ok) {
+                ++rej;
+                continue;
+            }
+            sr += L.x;
+            sg += L.y;
+            sbb += L.z;
+            const float lum = luminance(mk(L.x, L.y, L.z));
+            sq += lum * lum;
+        }
+        sum[3 * pix + 0] = sr;
+        sum[3 * pix + 1] = sg;
+        sum[3 * pix + 2] = sbb;
+        sumSq[pix] = sq;
+        cnt[pix] = c;
+    }
+    if (rej) atomicAdd(rejected, rej);
+}
+
+} // namespace pe

@@ -1,0 +1,187 @@
+// pe_scene.h — the flattened scene as the kernels read it from HBM.  Every array is a
+// separate allocation (SoA), 16-byte aligned, built once on the host (pe_host.cpp) and kept
+// resident until the next set_scene.
+//
+// Layout (per unit):
+//   BVH interior node   64 B  4 x float4: child boxes interleaved (c0.x, c1.x | c0.y, c1.y |
+//                             c0.z, c1.z) and child references; a leaf child is ~firstPrim with
+//                             its count beside it.  Same binary tree, same child order and the
+//                             same leaf triangle order as the reference's SAH BVH
+//                             (src/geometry/bvh.cpp:100-255), so traversal visits nodes and
+//                             tests triangles in the reference's order.
+//   leaf triangle       48 B  (v0, parallelEps) (e1, visibility mask) (e2, global triangle id),
+//                             the lean record of BVH::TriAccel (bvh.h:84-88) in leaf order
+//   triangle shading    16 B  vertex indices + shape id; vertices 16 B (pos), 16 B (normal), 8 B (uv)
+//   material           256 B  resolved parameters (pe_material plus derived constants)
+//   light               80 B  triangle light or rectangle (src/lights/area_light.h)
+#pragma once
+
+#include "pe_math.h"
+
+#if !defined(__CUDACC__)
+struct float4 { float x, y, z, w; };
+struct float2 { float x, y; };
+struct int4 { int x, y, z, w; };
+#endif
+
+namespace pe {
+
+constexpr int kTableN = 32;          // microfacet / sheen table resolution (microfacet.cpp:13)
+constexpr int kFilterBins = 512;     // pixel filter inverse CDF bins (pixel_filter.cpp:13)
+constexpr int kMaxExhaustive = 33;   // LightSampler::kMaxExhaustive (light_sampler.h:31)
+constexpr int kMaxInfinite = 16;     // LightSampler::kMaxInfinite
+constexpr int kMaxStack = 64;        // traversal stack entries; builder rejects deeper trees
+
+enum ShapeFlags : uint32_t {
+    SF_AREA_TRIANGLE = 1u,   // one of the two triangles of an AreaLight (a Triangle shape)
+    SF_CAMERA_INVISIBLE = 2u,
+    SF_HAS_NORMALS = 4u,
+    SF_HAS_UVS = 8u,
+};
+
+struct ShapeInfo {
+    int32_t material;
+    int32_t emitter;      // light index of triangle 0 (emissive mesh) or of the area light; -1 none
+    uint32_t flags;
+    uint32_t firstTri;    // global index of the shape's first triangle
+};
+
+// Resolved material (pe_material + constants derived on the host).
+struct MatGPU {
+    int32_t type;
+    int32_t flags;            // MF_*
+    float base[3];
+    float emission[3];
+    float metallic, roughness, specular, clearcoat, clearcoatRoughness;
+    float ior, specTrans, coatIor;
+    float coatTint[3];
+    float sheenColor[3];
+    int32_t hasSheenColor;
+    float anisotropy, sheen, sheenRoughness, diffuseRoughness, diffuseTransmission, subsurface;
+    float ssRadius[3];
+    float ssScale, ssAniso;
+    float edgeTint[3];
+    float thinFilmThickness, thinFilmIor;
+    float flakeDensity, flakeSize, flakeRoughness;
+    float flakeColor[3];
+    float opacity;
+    float glassRoughness;
+    float abbe;
+    float sigmaA[3], sigmaS[3];  // interior medium of a Dielectric (rebuildMedium)
+    float mediumG;
+    int32_t thinWalled;
+    float filmThickness;
+    float pad[8];
+};
+
+enum MatFlags : int32_t {
+    MF_EMISSIVE = 1,
+    MF_DELTA = 2,             // Material::isDelta
+    MF_VOLUME_BOUNDARY = 4,   // Material::isVolumeBoundary
+    MF_TRANSMITS_SHADOWS = 8,
+    MF_DISPERSIVE = 16,
+    MF_HAS_MEDIUM = 32,
+    MF_MEDIUM_SCATTERS = 64,
+};
+
+enum LightType : int32_t { LT_TRIANGLE = 0, LT_AREA = 1 };
+
+struct LightGPU {
+    int32_t type;
+    int32_t rectangle;  // AreaLight: u ⟂ v (spherical-rectangle sampling allowed)
+    float area;
+    float pad0;
+    float p0[3];        // triangle p0 | area position
+    float radiance_r;
+    float p1[3];        // triangle p1 | area u
+    float radiance_g;
+    float p2[3];        // triangle p2 | area v
+    float radiance_b;
+    float normal[3];
+    float pad1;
+};
+
+// Light BVH node (LightSampler::Node with LightBounds, light_sampler.h:57-61, light_bounds.h:16-26).
+struct LightNodeGPU {
+    float bmin[3], bmax[3];
+    float w[3];
+    float phi, cosThetaO, cosThetaE;
+    int32_t twoSided;
+    int32_t child1;
+    int32_t light;
+    int32_t pad;
+};
+
+struct TablesGPU {
+    float ggxE[kTableN * kTableN];
+    float ggxEa[kTableN * kTableN];
+    float ggxEb[kTableN * kTableN];
+    float avg0[kTableN], avg1[kTableN], avg2[kTableN];
+    float sheenE[kTableN * kTableN];
+    float filterCdf[kFilterBins + 1];
+    uint32_t sobolTab[4][256];
+    float spectralCdf[351];
+    float spectralPdf[350];
+    float spectralNorm[3];
+    float pad;
+};
+
+// Environment light (src/lights/environment_light.h:52-153).  The image distribution used for
+// light sampling and for pdfLi is the MIS-compensated one (m_mis).
+struct EnvGPU {
+    int32_t present;
+    int32_t width, height;
+    int32_t hasImage;
+    float rotation, intensity;
+    float meanLuminance;
+    float sunPdfWeight;
+    float sunDir[3];
+    float sunCosMax;
+    float sunRadiance[3];
+    float funcInt;      // m_mis.funcInt
+    int32_t valid;      // m_mis.valid()
+    int32_t pad[3];
+    const float* image; // w*h*3
+    const float* func;  // w*h
+    const float* marginalCdf; // h+1
+    const float* condCdf;     // h*(w+1)
+};
+
+struct SceneGPU {
+    // geometry
+    const float4* nodes;     // 4 float4 per interior node
+    const float4* tris;      // 3 float4 per leaf-ordered triangle
+    const int4* triVerts;    // per global triangle: i0, i1, i2, shape
+    const float4* pos;       // per vertex
+    const float4* nrm;       // per vertex
+    const float2* uv;        // per vertex
+    const ShapeInfo* shapes;
+    const MatGPU* materials;
+    int32_t rootIsLeaf;      // tiny scenes: the whole BVH is one leaf
+    int32_t rootFirst, rootCount;
+    int32_t nNodes;
+    float rootMin[3], rootMax[3];
+    uint32_t nTris;
+    int32_t nShapes;
+    // lights
+    const LightGPU* lights;
+    int32_t nLights;
+    int32_t lightMode;       // 0 uniform, 1 exhaustive, 2 light BVH
+    int32_t lightCount;      // candidates = nLights + env
+    int32_t nInfinite;
+    int32_t infinite[kMaxInfinite];
+    const LightNodeGPU* lightNodes;
+    int32_t nLightNodes;
+    int32_t pad0;
+    const int16_t* topSlot;          // per candidate
+    const unsigned long long* trail; // per candidate
+    const uint8_t* trailDepth;       // per candidate
+    EnvGPU env;
+    const TablesGPU* tables;
+    int32_t bgMode;
+    float bgColor[3];
+    int32_t hasShadowTransmitters;
+    int32_t hasVolumes;
+};
+
+} // namespace pe

@@ -1,0 +1,403 @@
+// pe_trace.cuh — ray/scene queries on the device: Owen-Sobol sampling, the camera ray of
+// Renderer::tracePixel, BVH traversal (closest hit and any hit), the hit record of
+// Triangle::fillHit and the robust ray-spawn rules of ray_spawn.h.
+//
+// Rounding: this file is compiled with -fmad=false and IEEE division / square root, and every
+// expression keeps the reference's operand order, so the slab test, Möller–Trumbore and the hit
+// record produce the reference CPU path's floats bit for bit.
+#pragma once
+
+#include "pe_math.h"
+#include "pe_scene.h"
+
+namespace pe {
+
+// ---- Owen-scrambled Sobol (src/samplers/sobol_sampler.cpp:111-146) --------------------------
+struct Sobol {
+    uint32_t pixelHash;
+    uint32_t revIndex;
+    uint32_t dim;
+};
+__device__ __forceinline__ uint32_t revSobol1(const TablesGPU* T, uint32_t index) {
+    return __ldg(&T->sobolTab[0][index & 0xFFu]) ^ __ldg(&T->sobolTab[1][(index >> 8) & 0xFFu]) ^
+           __ldg(&T->sobolTab[2][(index >> 16) & 0xFFu]) ^ __ldg(&T->sobolTab[3][index >> 24]);
+}
+__device__ __forceinline__ float get1D(Sobol& s) {
+    const uint32_t seed = hashMix(s.pixelHash, s.dim++);
+    const uint32_t index = rev32(lkPermute(s.revIndex, seed));
+    return unitFloat24(rev32(lkPermute(index, hashMix(seed, 0u))));
+}
+__device__ __forceinline__ V2 get2D(const TablesGPU* T, Sobol& s) {
+    const uint32_t seed = hashMix(s.pixelHash, s.dim++);
+    const uint32_t index = rev32(lkPermute(s.revIndex, seed));
+    const uint32_t x = rev32(lkPermute(index, hashMix(seed, 0u)));
+    const uint32_t y = rev32(lkPermute(revSobol1(T, index), hashMix(seed, 1u)));
+    return mk2(unitFloat24(x), unitFloat24(y));
+}
+
+// ---- camera ray (renderer.cpp:139-160, pixel_filter.cpp:84-91, perspective_camera.cpp:36-40) --
+struct CamDev {
+    V3 position, lowerLeft, horizontal, vertical;
+};
+__device__ __forceinline__ float filterSample1D(const TablesGPU* T, float filterWidth, float u) {
+    const float* cdf = T->filterCdf;
+    if (cdf[0] < 0.0f) return (u - 0.5f) * filterWidth;
+    // std::upper_bound over 513 entries
+    int lo = 0, count = kFilterBins + 1;
+    while (count > 0) {
+        const int step = count / 2;
+        const int it = lo + step;
+        if (!(u < cdf[it])) {
+            lo = it + 1;
+            count -= step + 1;
+        } else {
+            count = step;
+        }
+    }
+    const int i = iclamp(lo - 1, 0, kFilterBins - 1);
+    const float c0 = cdf[i], c1 = cdf[i + 1];
+    const float t = c1 > c0 ? (u - c0) / (c1 - c0) : 0.5f;
+    const float radius = 0.5f * filterWidth;
+    return -radius + (static_cast<float>(i) + sclamp(t, 0.0f, 1.0f)) * (filterWidth / kFilterBins);
+}
+// Primary ray of pixel (x, y): consumes Sobol dimensions 0 (filter) and 1 (lens).
+__device__ __forceinline__ void cameraRay(const TablesGPU* T, const CamDev& c, float filterWidth, int x, int y, int w,
+                                          int h, Sobol& s, V3& o, V3& d) {
+    const V2 u = get2D(T, s);
+    const float ox = filterSample1D(T, filterWidth, u.x);
+    const float oy = filterSample1D(T, filterWidth, u.y);
+    const float sx = (static_cast<float>(x) + 0.5f + ox) / static_cast<float>(w);
+    const float sy = 1.0f - (static_cast<float>(y) + 0.5f + oy) / static_cast<float>(h);
+    (void)get2D(T, s); // lens sample (consumed even by a pinhole camera)
+    const V3 target = c.lowerLeft + sx * c.horizontal + sy * c.vertical;
+    o = c.position;
+    d = normalize(target - c.position);
+}
+
+// ---- BVH traversal -------------------------------------------------------------------------
+// Slab test of BVH::hitBox (bvh.cpp:269-283), std::max/min argument order kept so NaNs resolve
+// exactly as there.
+__device__ __forceinline__ bool slab(float lox, float hix, float loy, float hiy, float loz, float hiz, V3 o, V3 inv,
+                                     float tMin, float tMax, float& tNear) {
+    float tx0 = (lox - o.x) * inv.x, tx1 = (hix - o.x) * inv.x;
+    if (tx0 > tx1) { const float t = tx0; tx0 = tx1; tx1 = t; }
+    float ty0 = (loy - o.y) * inv.y, ty1 = (hiy - o.y) * inv.y;
+    if (ty0 > ty1) { const float t = ty0; ty0 = ty1; ty1 = t; }
+    float tz0 = (loz - o.z) * inv.z, tz1 = (hiz - o.z) * inv.z;
+    if (tz0 > tz1) { const float t = tz0; tz0 = tz1; tz1 = t; }
+    const float t0 = smax(smax(tMin, tx0), smax(ty0, tz0));
+    const float t1 = smin(smin(tMax, tx1), smin(ty1, tz1)) * 1.0000004f;
+    tNear = t0;
+    return t0 <= t1;
+}
+
+// Lean Möller–Trumbore of BVH::hitTriangleLean (bvh.cpp:302-316).
+__device__ __forceinline__ bool triLean(const float4 a, const float4 b, const float4 c, V3 o, V3 d, float tMin,
+                                        float tMax, float& t, float& uu, float& vv) {
+    const V3 v0 = mk(a.x, a.y, a.z), e1 = mk(b.x, b.y, b.z), e2 = mk(c.x, c.y, c.z);
+    const V3 h = cross(d, e2);
+    const float A = dot(e1, h);
+    if (A * A <= a.w) return false;
+    const float f = 1.0f / A;
+    const V3 s = o - v0;
+    const float u = f * dot(s, h);
+    if (!(u >= 0.0f && u <= 1.0f)) return false;
+    const V3 q = cross(s, e1);
+    const float v = f * dot(d, q);
+    if (!(v >= 0.0f && u + v <= 1.0f)) return false;
+    t = f * dot(e2, q);
+    uu = u;
+    vv = v;
+    return t >= tMin && t <= tMax;
+}
+
+struct Hit {
+    float t, u, v;
+    int32_t prim; // leaf-order primitive index, -1 = miss
+};
+
+__device__ __forceinline__ void leafRange(int ref, int& first, int& count) {
+    const uint32_t v = ~static_cast<uint32_t>(ref);
+    first = static_cast<int>(v >> 8);
+    count = static_cast<int>(v & 0xFFu) + 1;
+}
+
+template <bool COUNT>
+__device__ __forceinline__ void testLeafClosest(const SceneGPU& S, int first, int count, V3 o, V3 d, uint32_t mask,
+                                                float tMin, float& tMax, Hit& best, uint32_t& triTests) {
+    for (int k = 0; k < count; ++k) {
+        const int pi = first + k;
+        const float4 a = __ldg(&S.tris[3 * pi + 0]);
+        const float4 b = __ldg(&S.tris[3 * pi + 1]);
+        if ((__float_as_uint(b.w) & mask) == 0u) continue;
+        const float4 c = __ldg(&S.tris[3 * pi + 2]);
+        if (COUNT) ++triTests;
+        float t, u, v;
+        if (triLean(a, b, c, o, d, tMin, tMax, t, u, v)) {
+            tMax = t;
+            best.t = t;
+            best.u = u;
+            best.v = v;
+            best.prim = pi;
+        }
+    }
+}
+
+// BVH::intersect (bvh.cpp:322-401): near child first, far child pushed with its entry
+// distance and skipped on pop when farther than the current hit.  The last triangle with
+// t <= tMax wins ties, as there.
+template <bool COUNT>
+__device__ Hit traceClosest(const SceneGPU& S, V3 o, V3 d, uint32_t mask, float tMin, float tMax, uint32_t& nodeVisits,
+                            uint32_t& triTests) {
+    Hit best;
+    best.prim = -1;
+    best.t = tMax;
+    best.u = best.v = 0.0f;
+    const V3 inv = mk(1.0f / d.x, 1.0f / d.y, 1.0f / d.z);
+    float tn;
+    if (S.nTris == 0) return best;
+    if (!slab(S.rootMin[0], S.rootMax[0], S.rootMin[1], S.rootMax[1], S.rootMin[2], S.rootMax[2], o, inv, tMin, tMax, tn))
+        return best;
+    if (S.rootIsLeaf) {
+        testLeafClosest<COUNT>(S, S.rootFirst, S.rootCount, o, d, mask, tMin, tMax, best, triTests);
+        return best;
+    }
+    int stackRef[kMaxStack];
+    float stackT[kMaxStack];
+    int sp = 0;
+    int cur = 0;
+    for (;;) {
+        if (cur < 0) {
+            int first, count;
+            leafRange(cur, first, count);
+            testLeafClosest<COUNT>(S, first, count, o, d, mask, tMin, tMax, best, triTests);
+        } else {
+            if (COUNT) ++nodeVisits;
+            const float4 n0 = __ldg(&S.nodes[4 * cur + 0]);
+            const float4 n1 = __ldg(&S.nodes[4 * cur + 1]);
+            const float4 n2 = __ldg(&S.nodes[4 * cur + 2]);
+            const float4 n3 = __ldg(&S.nodes[4 * cur + 3]);
+            float t0, t1;
+            const bool h0 = slab(n0.x, n0.y, n0.z, n0.w, n2.x, n2.y, o, inv, tMin, tMax, t0);
+            const bool h1 = slab(n1.x, n1.y, n1.z, n1.w, n2.z, n2.w, o, inv, tMin, tMax, t1);
+            const int c0 = __float_as_int(n3.x), c1 = __float_as_int(n3.y);
+            if (h0 && h1) {
+                if (t1 < t0) {
+                    stackRef[sp] = c0;
+                    stackT[sp] = t0;
+                    ++sp;
+                    cur = c1;
+                } else {
+                    stackRef[sp] = c1;
+                    stackT[sp] = t1;
+                    ++sp;
+                    cur = c0;
+                }
+                continue;
+            }
+            if (h0) {
+                cur = c0;
+                continue;
+            }
+            if (h1) {
+                cur = c1;
+                continue;
+            }
+        }
+        bool found = false;
+        while (sp > 0) {
+            --sp;
+            if (stackT[sp] <= tMax) {
+                cur = stackRef[sp];
+                found = true;
+                break;
+            }
+        }
+        if (!found) break;
+    }
+    return best;
+}
+
+// BVH::intersectAny (bvh.cpp:404-446): true when any triangle in [tMin, tMax] passes the
+// mask.  The answer does not depend on visiting order; near child first for early exit.
+template <bool COUNT>
+__device__ bool traceAny(const SceneGPU& S, V3 o, V3 d, uint32_t mask, float tMin, float tMax, uint32_t& nodeVisits,
+                         uint32_t& triTests) {
+    const V3 inv = mk(1.0f / d.x, 1.0f / d.y, 1.0f / d.z);
+    float tn;
+    if (S.nTris == 0) return false;
+    if (!slab(S.rootMin[0], S.rootMax[0], S.rootMin[1], S.rootMax[1], S.rootMin[2], S.rootMax[2], o, inv, tMin, tMax, tn))
+        return false;
+    int stackRef[kMaxStack];
+    int sp = 0;
+    int cur = S.rootIsLeaf ? static_cast<int>(~((static_cast<uint32_t>(S.rootFirst) << 8) | static_cast<uint32_t>(S.rootCount - 1))) : 0;
+    for (;;) {
+        if (cur < 0) {
+            int first, count;
+            leafRange(cur, first, count);
+            for (int k = 0; k < count; ++k) {
+                const int pi = first + k;
+                const float4 a = __ldg(&S.tris[3 * pi + 0]);
+                const float4 b = __ldg(&S.tris[3 * pi + 1]);
+                if ((__float_as_uint(b.w) & mask) == 0u) continue;
+                const float4 c = __ldg(&S.tris[3 * pi + 2]);
+                if (COUNT) ++triTests;
+                float t, u, v;
+                if (triLean(a, b, c, o, d, tMin, tMax, t, u, v)) return true;
+            }
+        } else {
+            if (COUNT) ++nodeVisits;
+            const float4 n0 = __ldg(&S.nodes[4 * cur + 0]);
+            const float4 n1 = __ldg(&S.nodes[4 * cur + 1]);
+            const float4 n2 = __ldg(&S.nodes[4 * cur + 2]);
+            const float4 n3 = __ldg(&S.nodes[4 * cur + 3]);
+            float t0, t1;
+            const bool h0 = slab(n0.x, n0.y, n0.z, n0.w, n2.x, n2.y, o, inv, tMin, tMax, t0);
+            const bool h1 = slab(n1.x, n1.y, n1.z, n1.w, n2.z, n2.w, o, inv, tMin, tMax, t1);
+            const int c0 = __float_as_int(n3.x), c1 = __float_as_int(n3.y);
+            if (h0 && h1) {
+                const bool farFirst = t1 < t0;
+                stackRef[sp++] = farFirst ? c0 : c1;
+                cur = farFirst ? c1 : c0;
+                continue;
+            }
+            if (h0) {
+                cur = c0;
+                continue;
+            }
+            if (h1) {
+                cur = c1;
+                continue;
+            }
+        }
+        if (sp == 0) break;
+        cur = stackRef[--sp];
+    }
+    return false;
+}
+
+// ---- hit record (src/geometry/triangle.cpp:54-133) -----------------------------------------
+struct Isect {
+    V3 point, normal, ng, tangent, pError, pSmooth;
+    float t;
+    bool frontFace, hasSmooth;
+    int32_t tri;    // global triangle index
+    int32_t shape;
+    int32_t material;
+};
+
+__device__ __forceinline__ V3 ld3(const float4* a, int i) {
+    const float4 v = __ldg(&a[i]);
+    return mk(v.x, v.y, v.z);
+}
+
+__device__ void fillHit(const SceneGPU& S, const Hit& h, V3 rayDir, Isect& is) {
+    const float4 e2w = __ldg(&S.tris[3 * h.prim + 2]);
+    const int g = static_cast<int>(__float_as_uint(e2w.w));
+    const int4 tv = __ldg(&S.triVerts[g]);
+    const V3 v0 = ld3(S.pos, tv.x), v1 = ld3(S.pos, tv.y), v2 = ld3(S.pos, tv.z);
+    const V3 n0 = ld3(S.nrm, tv.x), n1 = ld3(S.nrm, tv.y), n2 = ld3(S.nrm, tv.z);
+    const float2 uv0 = __ldg(&S.uv[tv.x]), uv1 = __ldg(&S.uv[tv.y]), uv2 = __ldg(&S.uv[tv.z]);
+    const float u = h.u, v = h.v;
+    const V3 edge1 = v1 - v0, edge2 = v2 - v0;
+    is.t = h.t;
+    const float w = 1.0f - u - v;
+    const V3 a0 = v0 * w, a1 = v1 * u, a2 = v2 * v;
+    is.point = a0 + a1 + a2;
+    const float iso = gammaN(32) * smax(smax(smax(maxComp(vabs(v0)), maxComp(vabs(v1))), maxComp(vabs(v2))), 1e-20f);
+    is.pError = (vabs(a0) + vabs(a1) + vabs(a2)) * gammaN(16) + mk(iso);
+    const V3 geomNormal = normalize(cross(edge1, edge2));
+    const bool hasN = len2(n0) > 0.0f && len2(n1) > 0.0f && len2(n2) > 0.0f;
+    const V3 shading = hasN ? normalize(n0 * w + n1 * u + n2 * v) : geomNormal;
+    is.ng = geomNormal;
+    is.frontFace = dot(rayDir, shading) < 0.0f;
+    is.normal = is.frontFace ? shading : -shading;
+    if (len2(is.ng) == 0.0f) is.ng = shading;
+    is.hasSmooth = false;
+    is.pSmooth = is.point;
+    if (hasN) {
+        const V3 p = is.point;
+        const V3 m0 = normalize(n0), m1 = normalize(n1), m2 = normalize(n2);
+        const V3 lift = m0 * (w * smax(0.0f, dot(v0 - p, m0))) + m1 * (u * smax(0.0f, dot(v1 - p, m1))) +
+                        m2 * (v * smax(0.0f, dot(v2 - p, m2)));
+        if (len2(lift) > 0.0f) {
+            is.pSmooth = p + lift;
+            is.hasSmooth = true;
+        }
+    }
+    const float d1x = uv1.x - uv0.x, d1y = uv1.y - uv0.y;
+    const float d2x = uv2.x - uv0.x, d2y = uv2.y - uv0.y;
+    const float r = d1x * d2y - d2x * d1y;
+    V3 tangent;
+    if (fabsf(r) < 1e-6f) {
+        const V3 n = is.normal;
+        const float sign = copysignf(1.0f, n.z);
+        const float ac = -1.0f / (sign + n.z);
+        const float bc = n.x * n.y * ac;
+        tangent = mk(1.0f + sign * n.x * n.x * ac, sign * bc, -sign * n.x);
+    } else {
+        const float invR = 1.0f / r;
+        tangent = (edge1 * d2y - edge2 * d1y) * invR;
+    }
+    is.tangent = normalize(tangent);
+    is.tri = g;
+    is.shape = tv.w;
+    is.material = S.shapes[tv.w].material;
+}
+
+// ---- robust spawning (src/geometry/ray_spawn.h) --------------------------------------------
+__device__ __forceinline__ V3 offsetRayOrigin(V3 p, V3 pError, V3 n, V3 w) {
+    const float d = dot(vabs(n), pError);
+    V3 off = n * d;
+    if (dot(w, n) < 0.0f) off = -off;
+    V3 po = p + off;
+    po.x = off.x > 0.0f ? nextUp(po.x) : (off.x < 0.0f ? nextDown(po.x) : po.x);
+    po.y = off.y > 0.0f ? nextUp(po.y) : (off.y < 0.0f ? nextDown(po.y) : po.y);
+    po.z = off.z > 0.0f ? nextUp(po.z) : (off.z < 0.0f ? nextDown(po.z) : po.z);
+    return po;
+}
+__device__ __forceinline__ V3 spawnNormal(const Isect& is) { return len2(is.ng) > 0.0f ? is.ng : is.normal; }
+__device__ __forceinline__ V3 spawnOrigin(const Isect& is, V3 dir) {
+    return offsetRayOrigin(is.point, is.pError, spawnNormal(is), dir);
+}
+__device__ __forceinline__ V3 shadowOrigin(const Isect& is, V3 toLight) {
+    const V3 n = spawnNormal(is);
+    V3 p = is.point;
+    if (is.hasSmooth) {
+        const V3 shadingOut = is.frontFace ? is.normal : -is.normal;
+        const V3 ngOut = dot(n, shadingOut) >= 0.0f ? n : -n;
+        const float NL = dot(shadingOut, toLight);
+        if (NL > 0.0f) {
+            const float kCutoff = 0.1f;
+            const float NgL = dot(ngOut, toLight);
+            const float amount = NL < kCutoff ? sclamp(2.0f - (NgL + NL) / kCutoff, 0.0f, 1.0f)
+                                              : sclamp(1.0f - NgL / kCutoff, 0.0f, 1.0f);
+            if (amount > 0.0f) p += (is.pSmooth - is.point) * amount;
+        }
+    }
+    return offsetRayOrigin(p, is.pError, n, toLight);
+}
+// makeShadowRay (path_tracer.cpp:144-157) with spawnRayTo (ray_spawn.h:75-85).
+__device__ __forceinline__ bool makeShadowRay(const Isect& is, V3 wi, float distance, V3& o, V3& d, float& tMax) {
+    if (!(distance < kFltMax) || distance >= 1e29f) {
+        o = shadowOrigin(is, wi);
+        d = wi;
+        tMax = 1e30f;
+        return true;
+    }
+    const V3 target = is.point + wi * distance;
+    const V3 toTarget = target - is.point;
+    const float len = length(toTarget);
+    if (!(len > 0.0f)) return false;
+    const V3 origin = shadowOrigin(is, toTarget / len);
+    const V3 dd = target - origin;
+    const float dist = length(dd);
+    const float slack = smax(dist * 1e-4f, 2e-6f * maxComp(vabs(target)));
+    if (!(dist > slack)) return false;
+    o = origin;
+    d = dd / dist;
+    tMax = dist - slack;
+    return true;
+}
+
+} // namespace pe

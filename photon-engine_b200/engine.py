@@ -1,0 +1,669 @@
+"""Host-side mirror of the reference engine's render API over the B200 C ABI.
+
+Names, argument meaning and error behaviour follow the reference's classes so code written
+against them reads the same here:
+
+=========================  ===============================================================
+reference                  here
+=========================  ===============================================================
+Lambertian, DisneyMaterial, Dielectric, Mirror (src/materials/*.h)    same names
+TriangleMesh (src/geometry/mesh.h:17-44)                               TriangleMesh
+AreaLight (src/lights/area_light.h:18-60)                              AreaLight
+EnvironmentLight (src/lights/environment_light.h:42-153)               EnvironmentLight
+Scene::addShape / addLight / setEnvironment / setBackground /
+  buildAccelerator (src/engine/scene.h:36-62)                          Scene
+PerspectiveCamera (src/camera/perspective_camera.h:14-35)              PerspectiveCamera
+RenderSettings (src/engine/render_settings.h:19-47)                    RenderSettings
+Film (src/core/image/film.h:23-76)                                     Film
+RenderDevice / DeviceInfo / DeviceFeatures /
+  RenderTargets (src/engine/render_device.h:37-86)                     CudaDevice etc.
+enumerateDevices / createDevice (render_device.cpp:80-157)             enumerate_devices / create_device
+RenderSession / SessionConfig (src/engine/render_session.h:34-98)      RenderSession / SessionConfig
+=========================  ===============================================================
+
+createDevice returns None and fills the error for an unusable id, as the reference does.
+There is no CPU fallback behind CudaDevice: every render goes through libphoton_cuda.so.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import dataclasses
+import enum
+import math
+import threading
+import time
+from typing import Optional
+
+import numpy as np
+
+from . import _capi as capi
+
+
+def _lib():
+    return capi.load()
+
+
+# ---------------------------------------------------------------------------------------------
+# materials
+class Material:
+    kind = -1
+
+    def __init__(self):
+        self._m = capi.pe_material()
+        _lib().pe_material_defaults(self.kind, C.byref(self._m))
+
+    @property
+    def struct(self) -> capi.pe_material:
+        return self._m
+
+    def emitted(self):
+        return tuple(self._m.emission)
+
+
+class Lambertian(Material):
+    kind = capi.PE_MAT_LAMBERT
+
+    def __init__(self, albedo, emission=(0.0, 0.0, 0.0)):
+        super().__init__()
+        self._m.base_color = capi.f3(albedo)
+        self._m.emission = capi.f3(emission)
+
+
+class DisneyMaterial(Material):
+    kind = capi.PE_MAT_DISNEY
+
+    def __init__(self, base_color, metallic: float, roughness: float, specular: float = 0.5):
+        super().__init__()
+        self._m.base_color = capi.f3(base_color)
+        self._m.metallic = metallic
+        self._m.roughness = roughness
+        self._m.specular = specular
+
+    def set_clear_coat(self, v): self._m.clearcoat = v
+    def set_clear_coat_roughness(self, v): self._m.clearcoat_roughness = v
+    def set_ior(self, v): self._m.ior = v
+    def set_specular_transmission(self, v): self._m.spec_transmission = v
+    def set_coat_ior(self, v): self._m.coat_ior = v
+    def set_coat_tint(self, c): self._m.coat_tint = capi.f3(c)
+
+    def set_sheen_color(self, c):
+        self._m.sheen_color = capi.f3(c)
+        self._m.has_sheen_color = 1
+
+    def set_anisotropy(self, v): self._m.anisotropy = v
+    def set_sheen(self, v): self._m.sheen = v
+    def set_sheen_roughness(self, v): self._m.sheen_roughness = v
+    def set_diffuse_roughness(self, v): self._m.diffuse_roughness = v
+    def set_diffuse_transmission(self, v): self._m.diffuse_transmission = v
+    def set_subsurface(self, v): self._m.subsurface = v
+    def set_subsurface_radius(self, c): self._m.subsurface_radius = capi.f3(c)
+    def set_subsurface_scale(self, v): self._m.subsurface_scale = v
+    def set_subsurface_anisotropy(self, v): self._m.subsurface_anisotropy = v
+    def set_edge_tint(self, c): self._m.edge_tint = capi.f3(c)
+
+    def set_thin_film(self, thickness_nm, ior):
+        self._m.thin_film_thickness = thickness_nm
+        self._m.thin_film_ior = ior
+
+    def set_flakes(self, density, size, roughness, color):
+        self._m.flake_density = density
+        self._m.flake_size = size
+        self._m.flake_roughness = roughness
+        self._m.flake_color = capi.f3(color)
+
+    def set_emission(self, c): self._m.emission = capi.f3(c)
+    def set_opacity(self, v): self._m.opacity = v
+
+
+class Dielectric(Material):
+    kind = capi.PE_MAT_DIELECTRIC
+
+    def __init__(self, ior: float, tint=(1.0, 1.0, 1.0), roughness: float = 0.0):
+        super().__init__()
+        self._m.ior = ior
+        self._m.base_color = capi.f3(tint)
+        self._m.glass_roughness = roughness
+
+    def set_abbe(self, v): self._m.abbe = v
+
+    def set_absorption(self, color, distance):
+        self._m.absorb_color = capi.f3(color)
+        self._m.absorb_distance = distance
+        self._m.has_absorption = 1
+
+    def set_scattering(self, density, color, anisotropy):
+        self._m.scatter_density = density
+        self._m.scatter_color = capi.f3(color)
+        self._m.scatter_anisotropy = anisotropy
+        self._m.has_scattering = 1
+
+    def set_thin_walled(self, v: bool): self._m.thin_walled = 1 if v else 0
+    def set_thin_film(self, thickness_nm): self._m.film_thickness = thickness_nm
+
+
+class Mirror(Material):
+    kind = capi.PE_MAT_MIRROR
+
+    def __init__(self, reflectance):
+        super().__init__()
+        self._m.base_color = capi.f3(reflectance)
+
+
+# ---------------------------------------------------------------------------------------------
+# shapes and lights
+class TriangleMesh:
+    def __init__(self, positions, normals=None, uvs=None, indices=None, material: Material | None = None):
+        self.positions = np.ascontiguousarray(positions, dtype=np.float32).reshape(-1, 3)
+        self.normals = None if normals is None or len(normals) == 0 else np.ascontiguousarray(normals, dtype=np.float32).reshape(-1, 3)
+        self.uvs = None if uvs is None or len(uvs) == 0 else np.ascontiguousarray(uvs, dtype=np.float32).reshape(-1, 2)
+        self.indices = np.ascontiguousarray(indices, dtype=np.uint32).reshape(-1, 3)
+        self.material = material
+
+    def num_triangles(self) -> int:
+        return int(self.indices.shape[0])
+
+
+class AreaLight:
+    def __init__(self, position, u, v, radiance):
+        self.position = tuple(map(float, position))
+        self.u = tuple(map(float, u))
+        self.v = tuple(map(float, v))
+        self.radiance = tuple(map(float, radiance))
+        self.visible_to_camera = True
+
+    def set_visible_to_camera(self, v: bool):
+        self.visible_to_camera = bool(v)
+
+
+class EnvironmentLight:
+    def __init__(self, image: Optional[np.ndarray], rotation: float = 0.0, intensity: float = 1.0):
+        self.image = None if image is None else np.ascontiguousarray(image, dtype=np.float32)
+        self.rotation = float(rotation)
+        self.intensity = float(intensity)
+        self.sun = None
+
+    def set_sun(self, direction, cos_max, radiance):
+        self.sun = (tuple(map(float, direction)), float(cos_max), tuple(map(float, radiance)))
+
+
+class BackgroundMode(enum.IntEnum):
+    Environment = capi.PE_BG_ENVIRONMENT
+    Color = capi.PE_BG_COLOR
+    Transparent = capi.PE_BG_TRANSPARENT
+
+
+@dataclasses.dataclass
+class Background:
+    mode: BackgroundMode = BackgroundMode.Environment
+    color: tuple = (0.18, 0.18, 0.18)
+
+
+class Scene:
+    """Immutable-after-build render scene.  ``ops`` records the add calls in order so the same
+    content can be replayed into another implementation (the parity tests do this)."""
+
+    def __init__(self):
+        self.ops: list = []
+        self.environment: Optional[EnvironmentLight] = None
+        self.background = Background()
+        self._handle = None
+        self._materials: list[Material] = []
+        self._mat_index: dict[int, int] = {}
+        self.info: Optional[capi.pe_scene_info] = None
+
+    def __del__(self):
+        try:
+            if self._handle:
+                _lib().pe_scene_destroy(self._handle)
+        except Exception:
+            pass
+
+    def add_shape(self, mesh: TriangleMesh):
+        if mesh.material is None:
+            raise ValueError("TriangleMesh needs a material")
+        self.ops.append(("mesh", mesh))
+
+    def add_light(self, light: AreaLight):
+        self.ops.append(("area", light))
+
+    def set_environment(self, env: Optional[EnvironmentLight]):
+        self.environment = env
+
+    def set_background(self, bg: Background):
+        self.background = bg
+
+    def materials(self) -> list[Material]:
+        out, seen = [], set()
+        for kind, obj in self.ops:
+            if kind == "mesh" and id(obj.material) not in seen:
+                seen.add(id(obj.material))
+                out.append(obj.material)
+        return out
+
+    def build_accelerator(self):
+        lib = _lib()
+        if self._handle:
+            lib.pe_scene_destroy(self._handle)
+        h = lib.pe_scene_create()
+        if not h:
+            raise MemoryError("pe_scene_create failed")
+        self._handle = h
+        mat_index = {}
+        for m in self.materials():
+            idx = lib.pe_scene_add_material(h, C.byref(m.struct))
+            if idx < 0:
+                capi.check(capi.PE_ERR_INVALID)
+            mat_index[id(m)] = idx
+        self._mat_index = mat_index
+        for kind, obj in self.ops:
+            if kind == "mesh":
+                capi.check(lib.pe_scene_add_mesh(h, capi.fptr(obj.positions), obj.positions.shape[0],
+                                                 capi.fptr(obj.normals), capi.fptr(obj.uvs), capi.uptr(obj.indices),
+                                                 obj.indices.shape[0], mat_index[id(obj.material)]))
+            else:
+                capi.check(lib.pe_scene_add_area_light(h, capi.f3(obj.position), capi.f3(obj.u), capi.f3(obj.v),
+                                                       capi.f3(obj.radiance), 1 if obj.visible_to_camera else 0))
+        env = self.environment
+        if env is not None:
+            img = env.image
+            if img is not None:
+                capi.check(lib.pe_scene_set_environment(h, capi.fptr(img), img.shape[1], img.shape[0], env.rotation,
+                                                        env.intensity))
+            else:
+                capi.check(lib.pe_scene_set_environment(h, None, 0, 0, env.rotation, env.intensity))
+            if env.sun is not None:
+                d, cm, r = env.sun
+                capi.check(lib.pe_scene_set_sun(h, capi.f3(d), cm, capi.f3(r)))
+        capi.check(lib.pe_scene_set_background(h, int(self.background.mode), capi.f3(self.background.color)))
+        capi.check(lib.pe_scene_build(h))
+        info = capi.pe_scene_info()
+        capi.check(lib.pe_scene_get_info(h, C.byref(info)))
+        self.info = info
+        return self
+
+    @property
+    def handle(self):
+        if not self._handle:
+            raise RuntimeError("Scene.build_accelerator() has not been called")
+        return self._handle
+
+
+# ---------------------------------------------------------------------------------------------
+class PerspectiveCamera:
+    def __init__(self, position, target, up, vfov_degrees: float, aspect: float):
+        self.position, self.target, self.up = position, target, up
+        self.vfov, self.aspect = float(vfov_degrees), float(aspect)
+        self._desc = capi.pe_camera()
+        _lib().pe_camera_perspective(capi.f3(position), capi.f3(target), capi.f3(up), self.vfov, self.aspect,
+                                     C.byref(self._desc))
+
+    def describe_gpu(self) -> capi.pe_camera:
+        return self._desc
+
+
+class PixelFilterType(enum.IntEnum):
+    Box = capi.PE_FILTER_BOX
+    Triangle = capi.PE_FILTER_TRIANGLE
+    Gaussian = capi.PE_FILTER_GAUSSIAN
+    BlackmanHarris = capi.PE_FILTER_BLACKMAN_HARRIS
+
+
+@dataclasses.dataclass
+class RenderSettings:
+    width: int = 512
+    height: int = 512
+    samples_per_pixel: int = 64
+    max_bounces: int = 8
+    tile_size: int = 32
+    num_threads: int = 0
+    adaptive_sampling: bool = False
+    clamp_indirect: float = 0.0
+    shadow_quality: int = 1
+    filter_type: PixelFilterType = PixelFilterType.BlackmanHarris
+    filter_width: float = 1.5
+    seed: int = 12345            # Renderer::renderSamples uses a fixed Sobol seed of 12345
+    rr_depth: int = 3            # PathTracer(maxBounces, 3, ...) in renderSamples
+    path_guiding: bool = False
+
+    def to_c(self) -> capi.pe_settings:
+        return capi.pe_settings(self.width, self.height, self.max_bounces, self.rr_depth, self.shadow_quality,
+                                int(self.filter_type), self.filter_width, self.clamp_indirect, self.seed)
+
+
+class Film:
+    """Per-pixel radiance sum, sample count and luminance² sum (src/core/image/film.h:23-76)."""
+
+    def __init__(self, width: int = 0, height: int = 0):
+        self.resize(width, height)
+
+    def resize(self, width: int, height: int):
+        self.width, self.height = max(0, width), max(0, height)
+        self.sum = np.zeros((self.height, self.width, 3), np.float32)
+        self.count = np.zeros((self.height, self.width), np.uint32)
+        self.sum_sq = np.zeros((self.height, self.width), np.float32)
+        self.rejected = 0
+
+    def clear(self):
+        self.resize(self.width, self.height)
+
+    def resolve(self) -> np.ndarray:
+        inv = np.zeros_like(self.sum_sq)
+        nz = self.count > 0
+        inv[nz] = 1.0 / self.count[nz].astype(np.float32)
+        return self.sum * inv[..., None]
+
+    def relative_error(self) -> np.ndarray:
+        n = self.count.astype(np.float32)
+        s = self.sum
+        mean = (0.212671 * s[..., 0] + 0.715160 * s[..., 1] + 0.072169 * s[..., 2]) / np.maximum(n, 1)
+        mean_sq = self.sum_sq / np.maximum(n, 1)
+        var = np.maximum(0.0, mean_sq - mean * mean) * n / np.maximum(n - 1, 1)
+        err = np.sqrt(var / np.maximum(n, 1)) / (np.maximum(mean, 0.0) + 0.01)
+        return np.where(n < 2, np.float32(1e30), err)
+
+    def merge(self, other: "Film"):
+        self.sum += other.sum
+        self.count += other.count
+        self.sum_sq += other.sum_sq
+        self.rejected += other.rejected
+
+
+@dataclasses.dataclass
+class RenderTargets:
+    beauty: Optional[Film] = None
+    aovs: object = None
+    passes: object = None
+
+
+@dataclasses.dataclass
+class SampleBatchResult:
+    completed: bool = True
+    samples_traced: int = 0
+
+
+@dataclasses.dataclass
+class DeviceFeatures:
+    aovs: bool = False
+    light_passes: bool = False
+    adaptive_sampling: bool = False
+
+
+class DeviceKind(enum.Enum):
+    Cpu = "cpu"
+    Cuda = "cuda"
+
+
+@dataclasses.dataclass
+class DeviceInfo:
+    id: str = ""
+    kind: DeviceKind = DeviceKind.Cuda
+    name: str = ""
+    threads: int = 0
+    memory_bytes: int = 0
+    compute_major: int = 0
+    compute_minor: int = 0
+    hardware_ray_tracing: bool = False
+    usable: bool = False
+    note: str = ""
+
+
+class SceneUpdateKind(enum.IntEnum):
+    Full = 0
+    Materials = 1
+    Lights = 2
+    Transforms = 3
+
+
+class CudaDevice:
+    """RenderDevice for one B200 (``cuda:N``).  Device handles are independent; one handle is
+    driven from one thread at a time (the reference's session contract)."""
+
+    def __init__(self, ordinal: int = 0):
+        lib = _lib()
+        err = C.create_string_buffer(512)
+        h = lib.pe_device_create(ordinal, err, len(err))
+        if not h:
+            raise capi.PhotonError(capi.PE_ERR_CUDA, err.value.decode())
+        self._h = h
+        self._scene: Optional[Scene] = None
+        di = capi.pe_device_info()
+        capi.check(lib.pe_device_info_get(h, C.byref(di)))
+        self._info = DeviceInfo(id=f"cuda:{ordinal}", kind=DeviceKind.Cuda, name=di.name.decode(),
+                                memory_bytes=di.memory_bytes, compute_major=di.compute_major,
+                                compute_minor=di.compute_minor, usable=True,
+                                note=f"sm_{di.compute_major}{di.compute_minor}, {di.sm_count} SMs, wavefront path tracer")
+        self._lock = threading.Lock()
+
+    def close(self):
+        if getattr(self, "_h", None):
+            _lib().pe_device_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def handle(self):
+        return self._h
+
+    def info(self) -> DeviceInfo:
+        return self._info
+
+    def features(self) -> DeviceFeatures:
+        return DeviceFeatures()
+
+    def set_scene(self, scene: Scene):
+        if scene.info is None:
+            scene.build_accelerator()
+        capi.check(_lib().pe_device_set_scene(self._h, scene.handle))
+        self._scene = scene
+
+    def update_scene(self, scene: Scene, kind: SceneUpdateKind = SceneUpdateKind.Full):
+        self.set_scene(scene)
+
+    def has_scene(self) -> bool:
+        return bool(_lib().pe_device_has_scene(self._h))
+
+    def render(self, camera: PerspectiveCamera, settings: RenderSettings, targets: RenderTargets, first_sample: int,
+               count: int, cancel=None) -> SampleBatchResult:
+        film = targets.beauty
+        if film is None:
+            raise ValueError("RenderTargets.beauty is required")
+        st = settings.to_c()
+        st.width, st.height = film.width, film.height
+        flag = None
+        if cancel is not None:
+            flag = cancel if isinstance(cancel, C.c_int32) else C.c_int32(1 if cancel else 0)
+        traced = C.c_uint64(0)
+        with self._lock:
+            rc = _lib().pe_device_render(self._h, C.byref(camera.describe_gpu()), C.byref(st), first_sample, count,
+                                         C.byref(flag) if flag is not None else None, capi.fptr(film.sum),
+                                         capi.uptr(film.count), capi.fptr(film.sum_sq), C.byref(traced))
+        if rc == capi.PE_ERR_CANCELLED:
+            return SampleBatchResult(False, traced.value)
+        capi.check(rc)
+        film.rejected += int(self.last_stats().rejected)
+        return SampleBatchResult(True, traced.value)
+
+    # resident-film path (no host film traffic per batch)
+    def render_resident(self, camera: PerspectiveCamera, settings: RenderSettings, first_sample: int, count: int):
+        st = settings.to_c()
+        capi.check(_lib().pe_device_render_resident(self._h, C.byref(camera.describe_gpu()), C.byref(st),
+                                                    first_sample, count, None))
+
+    def film_clear(self):
+        capi.check(_lib().pe_device_film_clear(self._h))
+
+    def film_read(self, width: int, height: int) -> Film:
+        f = Film(width, height)
+        capi.check(_lib().pe_device_film_read(self._h, capi.fptr(f.sum), capi.uptr(f.count), capi.fptr(f.sum_sq)))
+        return f
+
+    def synchronize(self):
+        capi.check(_lib().pe_device_synchronize(self._h))
+
+    def last_stats(self) -> capi.pe_render_stats:
+        s = capi.pe_render_stats()
+        capi.check(_lib().pe_device_last_stats(self._h, C.byref(s)))
+        return s
+
+    def set_counting(self, on: bool):
+        capi.check(_lib().pe_device_set_counting(self._h, 1 if on else 0))
+
+    # diagnostics
+    def trace_primary(self, camera: PerspectiveCamera, settings: RenderSettings, sample_index: int = 0):
+        n = settings.width * settings.height
+        shape = np.empty(n, np.int32)
+        prim = np.empty(n, np.int32)
+        t = np.empty(n, np.float32)
+        capi.check(_lib().pe_device_trace_primary(self._h, C.byref(camera.describe_gpu()), C.byref(settings.to_c()),
+                                                  sample_index, capi.iptr(shape), capi.iptr(prim), capi.fptr(t)))
+        return shape, prim, t
+
+    def sobol(self, seed: int, px, py, index, n_dims: int) -> np.ndarray:
+        px = np.ascontiguousarray(px, np.int32)
+        py = np.ascontiguousarray(py, np.int32)
+        index = np.ascontiguousarray(index, np.int32)
+        out = np.empty((len(px), n_dims, 2), np.float32)
+        capi.check(_lib().pe_device_sobol(self._h, seed, capi.iptr(px), capi.iptr(py), capi.iptr(index), len(px), n_dims,
+                                          capi.fptr(out)))
+        return out
+
+    def bsdf_probe(self, material_index: int, queries) -> list:
+        n = len(queries)
+        q = (capi.pe_bsdf_query * n)(*queries)
+        r = (capi.pe_bsdf_result * n)()
+        capi.check(_lib().pe_device_bsdf_probe(self._h, material_index, q, n, r))
+        return list(r)
+
+
+def enumerate_devices() -> list[DeviceInfo]:
+    out = [DeviceInfo(id="cpu", kind=DeviceKind.Cpu, name="host CPU", usable=False,
+                      note="the CPU path is the reference engine's own; this build provides cuda:N only")]
+    try:
+        n = _lib().pe_device_count()
+    except RuntimeError as e:
+        out.append(DeviceInfo(id="cuda:0", kind=DeviceKind.Cuda, usable=False, note=str(e)))
+        return out
+    for i in range(n):
+        out.append(DeviceInfo(id=f"cuda:{i}", kind=DeviceKind.Cuda, usable=True, note="B200 wavefront path tracer"))
+    return out
+
+
+def create_device(device_id: str = "auto", error: Optional[list] = None) -> Optional[CudaDevice]:
+    """createDevice: ``cuda:N`` or ``auto``; returns None and appends the reason to ``error``."""
+    try:
+        if device_id in ("auto", "cuda"):
+            ordinal = 0
+        elif device_id.startswith("cuda:"):
+            ordinal = int(device_id.split(":", 1)[1])
+        else:
+            raise ValueError(f"unknown device id '{device_id}' (this build serves cuda:N)")
+        return CudaDevice(ordinal)
+    except Exception as e:  # noqa: BLE001 — the reference reports, never throws
+        if error is not None:
+            error.append(str(e))
+        return None
+
+
+# ---------------------------------------------------------------------------------------------
+class RenderMode(enum.Enum):
+    Interactive = 0
+    Final = 1
+
+
+@dataclasses.dataclass
+class SessionConfig:
+    mode: RenderMode = RenderMode.Final
+    target_spp: int = 64
+    time_limit: float = 0.0
+    aovs: bool = False
+    passes: bool = False
+    batch_seconds: float = 0.5
+    max_batch: int = 64
+
+
+class RenderSession:
+    """Batch policy over a device (src/engine/render_session.cpp:17-101)."""
+
+    def __init__(self, device: CudaDevice):
+        self.device = device
+        self.camera = None
+        self.film = Film()
+        self.samples = 0
+        self.traced = 0
+        self.warnings: list[str] = []
+        self._sps = 0.0
+        self.last_batch_seconds = 0.0
+
+    def begin(self, camera, settings: RenderSettings, config: SessionConfig):
+        self.camera, self.settings, self.config = camera, dataclasses.replace(settings), dataclasses.replace(config)
+        self.warnings = []
+        f = self.device.features()
+        name = self.device.info().name
+        if self.config.aovs and not f.aovs:
+            self.config.aovs = False
+            self.warnings.append(f"{name}: AOVs are not supported; denoising uses colour only")
+        if self.config.passes and not f.light_passes:
+            self.config.passes = False
+            self.warnings.append(f"{name}: render passes are not supported; beauty only")
+        if self.settings.adaptive_sampling and not f.adaptive_sampling:
+            self.settings.adaptive_sampling = False
+            self.warnings.append(f"{name}: adaptive sampling is not supported; every pixel reaches the target")
+        self.film.resize(max(1, settings.width), max(1, settings.height))
+        self.samples = 0
+        self.traced = 0
+        self._sps = 0.0
+        self._start = time.perf_counter()
+
+    def seconds(self) -> float:
+        return time.perf_counter() - self._start
+
+    def finished(self) -> bool:
+        if self.config.target_spp > 0 and self.samples >= self.config.target_spp:
+            return True
+        return self.config.time_limit > 0.0 and self.samples > 0 and self.seconds() >= self.config.time_limit
+
+    def next_batch(self) -> int:
+        if self.config.mode == RenderMode.Interactive or self.samples == 0 or self._sps <= 0.0:
+            return 1
+        n = int(self.config.batch_seconds / self._sps)
+        n = min(max(n, 1), max(1, self.config.max_batch))
+        if self.config.target_spp > 0:
+            n = min(n, self.config.target_spp - self.samples)
+        if self.config.time_limit > 0.0:
+            left = self.config.time_limit - self.seconds()
+            n = min(n, max(1, int(left / self._sps)))
+        return max(1, n)
+
+    def advance(self, cancel=None) -> bool:
+        if self.camera is None or self.finished():
+            return False
+        count = self.next_batch()
+        t0 = time.perf_counter()
+        r = self.device.render(self.camera, self.settings, RenderTargets(beauty=self.film), self.samples, count, cancel)
+        self.last_batch_seconds = time.perf_counter() - t0
+        self.traced += r.samples_traced
+        if not r.completed:
+            return False
+        self.samples += count
+        per = self.last_batch_seconds / count
+        self._sps = 0.5 * (self._sps + per) if self._sps > 0.0 else per
+        return True
+
+    def average_samples(self) -> float:
+        px = float(self.film.width * self.film.height)
+        return self.traced / px if px > 0 else 0.0
+
+    def resolve(self) -> np.ndarray:
+        return self.film.resolve()
+
+
+def rel_mse(x: np.ndarray, ref: np.ndarray) -> float:
+    """relMSE = mean((x − ref)² / (ref² + 0.01)) over pixels and channels (scripts/compare_exr.py:30)."""
+    x = x.astype(np.float64)
+    ref = ref.astype(np.float64)
+    return float(np.mean((x - ref) ** 2 / (ref * ref + 0.01)))

@@ -1,0 +1,320 @@
+"""Throughput benchmark of the B200 path tracer on the product-scale torus-knot workload.
+
+Workload (one ``step``): one sample per pixel of a 1920×1080 frame of the ~1M-triangle torus
+knot with eight Disney materials, a 2048×1024 HDR sky (sun lobe 60 % of power) and a softbox,
+max depth 12 — i.e. 2,073,600 camera paths through the wavefront (generate, closest hit,
+shade, any hit, film) per step.  Metric: paths/s (W·H·spp / render seconds, the reference's
+msamplesPerSecond definition).
+
+``value``   device-resident: inputs in HBM, K steps into the resident film, CUDA events on the
+            library's stream, max over ranks.
+``e2e``     the same K steps through the public RenderDevice::render call with host films:
+            camera + settings in, the frame's film (sum, count, sum of squares) read back and
+            merged on the host every step.
+``roofline`` closest-hit traversal kernel: algorithmic bytes (BVH nodes visited × 64 B +
+            triangles tested × 48 B + ray record 32 B + hit record 16 B + queue index 4 B per
+            ray, counted on the device over one untimed step) ÷ its CUDA-event time, against
+            the measured HBM copy bandwidth.
+``cpu_baseline`` the reference engine's own CPU path (built with its shipping flags) on the same
+            scene and camera, all host threads, a bounded number of full-frame samples.
+
+``--impl reference`` times only that CPU implementation, one full-frame sample per step.
+``--gpus N`` (torchrun) runs N independent replicas, each rendering its own sample indices:
+the path does not shard further and needs no collective.
+"""
+from __future__ import annotations
+
+import argparse
+import datetime
+import json
+import os
+import pathlib
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = pathlib.Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+WIDTH, HEIGHT, DEPTH = 1920, 1080, 12
+NODE_BYTES, TRI_BYTES, RAY_BYTES, HIT_BYTES, QUEUE_BYTES = 64, 48, 32, 16, 4
+L2_NOTE = "inputs larger than L2: 140 MB resident scene + 300 MB path state per 2M-path wave (L2 126 MB)"
+
+
+def measured_peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+
+    FIELDS = "pci.bus_id,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active," \
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown," \
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap"
+
+    def __init__(self, pci_bus_id: str):
+        self.pci = pci_bus_id.lower()
+        self.proc = None
+        self.lines: list[str] = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                          "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        rows = []
+        for line in self.lines:
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            bus = f[0].lower()
+            if self.pci and not (bus.endswith(self.pci[-12:]) or self.pci.endswith(bus[-12:])):
+                continue
+            rows.append(f)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower().startswith("active")})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def build_workload(pe):
+    import importlib
+    sc = importlib.import_module("photon_engine_b200.scenes")
+    scene, cam, st = sc.torus_knot_scene(WIDTH, HEIGHT, 256, DEPTH)
+    scene.build_accelerator()
+    return scene, cam, st
+
+
+def cpu_reference(scene, cam, st, min_seconds: float, max_spp: int, first: int = 0):
+    """The reference's CPU path on all host threads: full-frame samples until min_seconds."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle
+    ref = oracle.RefScene(scene, fast=True)
+    threads = oracle.cpu_threads()
+    done, t0 = 0, time.perf_counter()
+    while done < max_spp:
+        ref.render(cam, st, first + done, 1, threads)
+        done += 1
+        if time.perf_counter() - t0 >= min_seconds:
+            break
+    dt = time.perf_counter() - t0
+    return WIDTH * HEIGHT * done / dt, threads, done, dt
+
+
+def run_reference(args):
+    world, rank, local = dist_setup()
+    if rank != 0:
+        return 0
+    pe = pe_load()
+    scene, cam, st = build_workload(pe)
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle
+    if not oracle.available(fast=True):
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libphoton_ref_fast.so was not built"}))
+        return 0
+    ref = oracle.RefScene(scene, fast=True)
+    threads = oracle.cpu_threads()
+    for w in range(args.warmup):
+        ref.render(cam, st, w, 1, threads)
+    t0 = time.perf_counter()
+    for k in range(args.steps):
+        ref.render(cam, st, args.warmup + k, 1, threads)
+    dt = time.perf_counter() - t0
+    value = WIDTH * HEIGHT * args.steps / dt
+    sample = f"{args.steps} full 1920x1080 frames at 1 spp (one per step)"
+    print(json.dumps({
+        "impl": "reference", "metric": "paths/s", "value": value, "unit": "paths/s", "n_gpus": 0,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * dt / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded procedural scene)",
+        "config": {"workload": "torus-knot 1M tris, 8 Disney materials, 2048x1024 HDR sky + softbox, 1920x1080, depth 12",
+                   "spp_per_step": 1, "threads": threads},
+        "cpu_baseline": {"value": value, "unit": "paths/s", "cores": threads, "kind": "reference", "sample": sample},
+        "e2e": {"value": value, "unit": "paths/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }))
+    return 0
+
+
+def pe_load():
+    import pe_pkg
+    return pe_pkg.load()
+
+
+def run_ours(args):
+    world, rank, local = dist_setup()
+    pg = None
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        pg = dist
+    pe = pe_load()
+    scene, cam, st = build_workload(pe)
+    dev = pe.CudaDevice(local)
+    dev.set_scene(scene)
+    base = rank * (args.warmup + args.steps + 8)  # disjoint sample indices per replica
+
+    # algorithmic bytes per closest-hit ray, counted on the device over one untimed step
+    dev.set_counting(True)
+    dev.render_resident(cam, st, base, 1)
+    cs = dev.last_stats()
+    dev.set_counting(False)
+    dev.film_clear()
+    for w in range(args.warmup):
+        dev.render_resident(cam, st, base + w, 1)
+    dev.synchronize()
+    if pg:
+        import torch
+        pg.barrier()
+    launches = 0
+    rays = 0
+    shadow_rays = 0
+    ms_isect = 0.0
+    n_isect = 0
+    with ClockSampler(dev.pci_bus_id) as clocks:
+        dev.timer_begin()
+        for k in range(args.steps):
+            dev.render_resident(cam, st, base + args.warmup + k, 1)
+            s = dev.last_stats()
+            launches += s.kernel_launches
+            rays += s.closest_rays
+            shadow_rays += s.shadow_rays
+            ms_isect += s.ms_intersect
+            n_isect += s.intersect_launches
+        ms = dev.timer_end()
+    if pg:
+        import torch
+        t = torch.tensor([ms], device=f"cuda:{local}")
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        ms = float(t.item())
+        pg.barrier()
+    total_paths = WIDTH * HEIGHT * args.steps * world
+    value = total_paths / (ms / 1000.0)
+
+    # end-to-end through RenderDevice::render with host films
+    film = pe.Film(WIDTH, HEIGHT)
+    for w in range(min(2, args.warmup)):
+        dev.render(cam, st, pe.RenderTargets(beauty=film), base + w, 1)
+    if pg:
+        pg.barrier()
+    t0 = time.perf_counter()
+    for k in range(args.steps):
+        dev.render(cam, st, pe.RenderTargets(beauty=film), base + args.warmup + k, 1)
+    e2e_s = time.perf_counter() - t0
+    if pg:
+        import torch
+        t = torch.tensor([e2e_s], device=f"cuda:{local}")
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e = total_paths / e2e_s
+
+    if rank != 0:
+        if pg:
+            pg.destroy_process_group()
+        dev.close()
+        return 0
+
+    # roofline of the closest-hit kernel: per-ray algorithmic bytes from the counting pass
+    bytes_per_ray = (cs.node_visits * NODE_BYTES + cs.tri_tests * TRI_BYTES) / max(1, cs.closest_rays) + \
+        RAY_BYTES + HIT_BYTES + QUEUE_BYTES
+    peak, peak_kind = measured_peaks()
+    achieved = (rays * bytes_per_ray) / (ms_isect / 1000.0) / 1e9 if ms_isect > 0 else None
+    traffic = None
+    tfile = ROOT / "profiles" / "closest_hit_dram_bytes_per_ray.txt"
+    if tfile.exists():
+        try:
+            per_ray = float(tfile.read_text().split()[0])
+            traffic = per_ray * rays / max(1, n_isect)
+        except (ValueError, IndexError):
+            traffic = None
+    roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+            "frac": (achieved / peak) if achieved else None, "traffic": traffic,
+            "kernel": "kIntersect (closest-hit BVH traversal)", "peak_kind": peak_kind,
+            "bytes_per_ray": bytes_per_ray, "avg_launch_ms": ms_isect / max(1, n_isect),
+            "rays_per_launch": rays / max(1, n_isect)}
+
+    cpu = None
+    if world == 1 and not args.no_cpu_baseline:
+        try:
+            v, threads, done, dt = cpu_reference(scene, cam, st, args.cpu_seconds, 64, first=100000)
+            cpu = {"value": v, "unit": "paths/s", "cores": threads, "kind": "reference",
+                   "sample": f"{done} full 1920x1080 frames at 1 spp ({dt:.1f} s), reference shipping build"}
+        except Exception as e:  # noqa: BLE001
+            cpu = {"value": None, "unit": "paths/s", "cores": 0, "kind": "reference", "sample": f"unavailable: {e}"}
+
+    out = {
+        "metric": "paths/s", "value": value, "unit": "paths/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded procedural scene)",
+        "config": {"workload": "torus-knot 1M tris, 8 Disney materials, 2048x1024 HDR sky + softbox, 1920x1080, depth 12",
+                   "spp_per_step": 1, "paths_per_step": WIDTH * HEIGHT, "triangles": int(scene.info.triangles),
+                   "l2": L2_NOTE, "parallelism": f"replicas x{world}"},
+        "rays_per_s": (rays + shadow_rays) * world / (ms / 1000.0),
+        "closest_rays_per_step": rays / args.steps, "shadow_rays_per_step": shadow_rays / args.steps,
+        "e2e": {"value": e2e, "unit": "paths/s", "h2d_bytes_per_step": 76 + 40,
+                "d2h_bytes_per_step": WIDTH * HEIGHT * (12 + 4 + 4)},
+        "gpu_launches": int(launches),
+        "roofline": roof,
+        "cpu_baseline": cpu,
+        "clocks": clocks.summary(),
+    }
+    print(json.dumps(out))
+    if pg:
+        pg.destroy_process_group()
+    dev.close()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=8)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=10.0)
+    args = ap.parse_args()
+    args.warmup = max(3, args.warmup)
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -180,6 +180,7 @@ typedef struct pe_device_info {
     int32_t sm_count;
     int32_t usable;
     int32_t feature_aovs, feature_light_passes, feature_adaptive;
+    char pci_bus_id[32];
 } pe_device_info;
 
 typedef struct pe_render_stats {
@@ -193,9 +194,12 @@ typedef struct pe_render_stats {
     float ms_shadow;           /* device time in any-hit traversal */
     float ms_shade;
     uint64_t intersect_launches;
-    uint64_t node_visits;      /* only when counting is enabled */
-    uint64_t tri_tests;
+    uint64_t node_visits;      /* closest-hit BVH node visits (counting enabled only) */
+    uint64_t tri_tests;        /* closest-hit triangle tests (counting enabled only) */
     uint32_t error_flags;      /* kernel error word (0 = none) */
+    uint64_t kernel_launches;  /* kernels this library launched in the last render call */
+    uint64_t shadow_node_visits; /* any-hit BVH node visits (counting enabled only) */
+    uint64_t shadow_tri_tests;   /* any-hit triangle tests (counting enabled only) */
 } pe_render_stats;
 
 const char* pe_last_error(void);
@@ -226,6 +230,10 @@ int32_t pe_device_synchronize(pe_device* d);
 int32_t pe_device_last_stats(pe_device* d, pe_render_stats* out);
 /* 1 = count BVH node visits and triangle tests in traversal kernels (slower). */
 int32_t pe_device_set_counting(pe_device* d, int32_t enabled);
+/* Device-stream timer: events recorded on the stream the kernels run on; end waits for the
+ * stop event and returns the elapsed device milliseconds. */
+int32_t pe_device_timer_begin(pe_device* d);
+int32_t pe_device_timer_end(pe_device* d, float* ms);
 
 /* ---- diagnostics used by parity tests --------------------------------------- */
 /* Camera ray of (x, y, sample_index) for every pixel, then closest hit:

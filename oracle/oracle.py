@@ -57,6 +57,8 @@ def _load(fast: bool = False):
         "ref_camera_perspective": (None, [FP, FP, FP, C.c_float, C.c_float, C.c_void_p]),
         "ref_render": (C.c_int32, [P, C.c_void_p, C.c_void_p, C.c_int32, C.c_int32, C.c_int32, FP, UP]),
         "ref_render_seeded": (C.c_int32, [P, C.c_void_p, C.c_void_p, C.c_int32, C.c_int32, C.c_int32, FP, UP]),
+"ref_render_rows": (C.c_int32, [P, C.c_void_p, C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.c_int32,
+                            C.c_int32, FP, UP]),
         "ref_trace_primary": (C.c_int32, [P, C.c_void_p, C.c_void_p, C.c_int32, IP, IP, FP]),
         "ref_sobol": (C.c_int32, [C.c_uint64, IP, IP, IP, C.c_size_t, C.c_int32, FP]),
         "ref_sobol_1d": (C.c_int32, [C.c_uint64, C.c_int32, C.c_int32, C.c_int32, C.c_int32, FP]),
@@ -137,6 +139,15 @@ class RefScene:
         fn = self.lib.ref_render_seeded if seeded else self.lib.ref_render
         fn(self.h, C.byref(camera.describe_gpu()), C.byref(settings.to_c()), first, count, threads, _f(mean),
            cnt.ctypes.data_as(UP))
+        return mean, cnt
+
+    def render_rows(self, camera, settings, first: int, count: int, y0: int, y1: int, threads: int = 0):
+        """tracePixel loop over rows [y0, y1) only (a bounded sample of the full-frame workload)."""
+        h, w = settings.height, settings.width
+        mean = np.zeros((h, w, 3), np.float32)
+        cnt = np.zeros((h, w), np.uint32)
+        self.lib.ref_render_rows(self.h, C.byref(camera.describe_gpu()), C.byref(settings.to_c()), first, count, threads,
+                                 y0, y1, _f(mean), cnt.ctypes.data_as(UP))
         return mean, cnt
 
     def trace_primary(self, camera, settings, sample_index: int = 0):

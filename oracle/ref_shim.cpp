@@ -288,11 +288,19 @@ int32_t ref_render(void* s, const pe_camera* cam, const pe_settings* st, int32_t
     return 0;
 }
 
-// tracePixel (renderer.cpp:139-160) with a caller-chosen Sobol seed; rows are split over
-// `threads` workers, each pixel accumulating its samples in index order (so the result equals
-// renderSamples' when seed == 12345 and the background mode is Environment).
+// tracePixel (renderer.cpp:139-160) with a caller-chosen Sobol seed over rows [y0, y1); rows
+// are split over `threads` workers, each pixel accumulating its samples in index order (so the
+// result equals renderSamples' when seed == 12345 and the background mode is Environment).
+int32_t ref_render_rows(void* s, const pe_camera* cam, const pe_settings* st, int32_t first, int32_t count,
+                        int32_t threads, int32_t y0, int32_t y1, float* mean_rgb, uint32_t* counts);
+
 int32_t ref_render_seeded(void* s, const pe_camera* cam, const pe_settings* st, int32_t first, int32_t count,
                           int32_t threads, float* mean_rgb, uint32_t* counts) {
+    return ref_render_rows(s, cam, st, first, count, threads, 0, st->height, mean_rgb, counts);
+}
+
+int32_t ref_render_rows(void* s, const pe_camera* cam, const pe_settings* st, int32_t first, int32_t count,
+                        int32_t threads, int32_t y0, int32_t y1, float* mean_rgb, uint32_t* counts) {
     auto* rs = static_cast<RefScene*>(s);
     DescCamera camera(*cam);
     const int w = st->width, h = st->height;
@@ -304,12 +312,13 @@ int32_t ref_render_seeded(void* s, const pe_camera* cam, const pe_settings* st, 
     pf.width = st->filter_width;
     const PixelFilterSampler filter(pf);
     const int nt = threads > 0 ? threads : hardwareThreads();
-    std::atomic<int> nextRow{0};
+    std::atomic<int> nextRow{y0 < 0 ? 0 : y0};
+    const int yEnd = y1 > h ? h : y1;
     auto work = [&]() {
         SobolSampler sampler(st->seed);
         for (;;) {
             const int y = nextRow.fetch_add(1);
-            if (y >= h) break;
+            if (y >= yEnd) break;
             for (int x = 0; x < w; ++x)
                 for (int si = first; si < first + count; ++si) {
                     sampler.startPixel(x, y);

@@ -62,7 +62,8 @@ class pe_scene_info(C.Structure):
 class pe_device_info(C.Structure):
     _fields_ = [("name", C.c_char * 128), ("memory_bytes", C.c_uint64), ("compute_major", C.c_int32),
                 ("compute_minor", C.c_int32), ("sm_count", C.c_int32), ("usable", C.c_int32),
-                ("feature_aovs", C.c_int32), ("feature_light_passes", C.c_int32), ("feature_adaptive", C.c_int32)]
+                ("feature_aovs", C.c_int32), ("feature_light_passes", C.c_int32), ("feature_adaptive", C.c_int32),
+                ("pci_bus_id", C.c_char * 32)]
 
 
 class pe_render_stats(C.Structure):
@@ -70,7 +71,8 @@ class pe_render_stats(C.Structure):
                 ("rejected", C.c_uint64), ("waves", C.c_uint64), ("ms_total", C.c_float),
                 ("ms_intersect", C.c_float), ("ms_shadow", C.c_float), ("ms_shade", C.c_float),
                 ("intersect_launches", C.c_uint64), ("node_visits", C.c_uint64), ("tri_tests", C.c_uint64),
-                ("error_flags", C.c_uint32)]
+                ("error_flags", C.c_uint32), ("kernel_launches", C.c_uint64),
+                ("shadow_node_visits", C.c_uint64), ("shadow_tri_tests", C.c_uint64)]
 
 
 class pe_bsdf_query(C.Structure):
@@ -117,6 +119,8 @@ SIGNATURES = {
     "pe_device_synchronize": (C.c_int32, [P]),
     "pe_device_last_stats": (C.c_int32, [P, C.POINTER(pe_render_stats)]),
     "pe_device_set_counting": (C.c_int32, [P, C.c_int32]),
+    "pe_device_timer_begin": (C.c_int32, [P]),
+    "pe_device_timer_end": (C.c_int32, [P, FP]),
     "pe_device_trace_primary": (C.c_int32, [P, C.POINTER(pe_camera), C.POINTER(pe_settings), C.c_int32, IP, IP, FP]),
     "pe_device_sobol": (C.c_int32, [P, C.c_uint64, IP, IP, IP, C.c_size_t, C.c_int32, FP]),
     "pe_device_bsdf_probe": (C.c_int32, [P, C.c_int32, C.POINTER(pe_bsdf_query), C.c_size_t, C.POINTER(pe_bsdf_result)]),

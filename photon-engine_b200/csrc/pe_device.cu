@@ -59,6 +59,7 @@ struct pe_device {
     float* fSq = nullptr;
     // timing
     cudaEvent_t evStart = nullptr, evStop = nullptr;
+    cudaEvent_t evT0 = nullptr, evT1 = nullptr;
     std::vector<cudaEvent_t> evPool;
     bool counting = false;
     pe_render_stats stats{};
@@ -229,6 +230,7 @@ int32_t renderWaves(pe_device* d, const pe_camera* cam, const pe_settings* st, i
             A.nSamples = ns;
             const int nSlots = A.nPix * ns;
             kGenerate<<<sm * 8, 256, 0, d->stream>>>(S, P, A, nSlots);
+            ++stats.kernel_launches;
             uint32_t live = static_cast<uint32_t>(nSlots);
             PE_CUDA(cudaMemcpyAsync(&P.counters[0], &live, sizeof(uint32_t), cudaMemcpyHostToDevice, d->stream));
             PE_CUDA(cudaMemsetAsync(&P.counters[1], 0, 2 * sizeof(uint32_t), d->stream));
@@ -254,6 +256,7 @@ int32_t renderWaves(pe_device* d, const pe_camera* cam, const pe_settings* st, i
                 else
                     kShadow<false><<<d->blocksShadow, 128, 0, d->stream>>>(S, P, &P.counters[2], A.clampIndirect, d->dStats);
                 PE_CUDA(cudaEventRecord(e3, d->stream));
+                stats.kernel_launches += 3;
                 isectEv.push_back({evUsed - 4, evUsed - 3});
                 shadeEv.push_back({evUsed - 3, evUsed - 2});
                 shadowEv.push_back({evUsed - 2, evUsed - 1});
@@ -272,6 +275,7 @@ int32_t renderWaves(pe_device* d, const pe_camera* cam, const pe_settings* st, i
                 std::swap(cIn, cOut);
             }
             kFilm<<<sm * 4, 256, 0, d->stream>>>(P, A, sum, cnt, sq, &d->dStats[4]);
+            ++stats.kernel_launches;
             PE_CUDA(cudaGetLastError());
         }
     }
@@ -299,8 +303,10 @@ int32_t renderWaves(pe_device* d, const pe_camera* cam, const pe_settings* st, i
         stats.ms_shadow += t;
     }
     stats.intersect_launches = isectEv.size();
-    stats.node_visits = hs[0] + hs[2];
-    stats.tri_tests = hs[1] + hs[3];
+    stats.node_visits = hs[0];
+    stats.tri_tests = hs[1];
+    stats.shadow_node_visits = hs[2];
+    stats.shadow_tri_tests = hs[3];
     stats.rejected = hs[4];
     stats.waves = isectEv.empty() ? 0 : 1;
     if (cancelled) {
@@ -430,6 +436,7 @@ pe_device* pe_device_create(int32_t ordinal, char* err, size_t errLen) {
     }
     if (cudaStreamCreateWithFlags(&d->stream, cudaStreamNonBlocking) != cudaSuccess ||
         cudaEventCreate(&d->evStart) != cudaSuccess || cudaEventCreate(&d->evStop) != cudaSuccess ||
+        cudaEventCreate(&d->evT0) != cudaSuccess || cudaEventCreate(&d->evT1) != cudaSuccess ||
         cudaMalloc(&d->dTables, sizeof(TablesGPU)) != cudaSuccess ||
         cudaMalloc(&d->dStats, 8 * sizeof(unsigned long long)) != cudaSuccess ||
         cudaMallocHost(&d->hCounters, 16 * sizeof(uint32_t)) != cudaSuccess) {
@@ -471,6 +478,8 @@ void pe_device_destroy(pe_device* d) {
     if (d->hCounters) cudaFreeHost(d->hCounters);
     for (cudaEvent_t e : d->evPool) cudaEventDestroy(e);
     if (d->evStart) cudaEventDestroy(d->evStart);
+    if (d->evT0) cudaEventDestroy(d->evT0);
+    if (d->evT1) cudaEventDestroy(d->evT1);
     if (d->evStop) cudaEventDestroy(d->evStop);
     if (d->stream) cudaStreamDestroy(d->stream);
     delete d;
@@ -488,6 +497,7 @@ int32_t pe_device_info_get(pe_device* d, pe_device_info* out) {
     out->compute_minor = d->prop.minor;
     out->sm_count = d->prop.multiProcessorCount;
     out->usable = 1;
+    cudaDeviceGetPCIBusId(out->pci_bus_id, sizeof(out->pci_bus_id), d->ordinal);
     return PE_OK;
 }
 
@@ -673,6 +683,20 @@ int32_t pe_device_last_stats(pe_device* d, pe_render_stats* out) {
 int32_t pe_device_set_counting(pe_device* d, int32_t enabled) {
     if (!d) return PE_ERR_INVALID;
     d->counting = enabled != 0;
+    return PE_OK;
+}
+
+int32_t pe_device_timer_begin(pe_device* d) {
+    if (!d) return PE_ERR_INVALID;
+    PE_CUDA(cudaEventRecord(d->evT0, d->stream));
+    return PE_OK;
+}
+
+int32_t pe_device_timer_end(pe_device* d, float* ms) {
+    if (!d || !ms) return PE_ERR_INVALID;
+    PE_CUDA(cudaEventRecord(d->evT1, d->stream));
+    PE_CUDA(cudaEventSynchronize(d->evT1));
+    PE_CUDA(cudaEventElapsedTime(ms, d->evT0, d->evT1));
     return PE_OK;
 }
 

@@ -432,6 +432,8 @@ class CudaDevice:
                                 memory_bytes=di.memory_bytes, compute_major=di.compute_major,
                                 compute_minor=di.compute_minor, usable=True,
                                 note=f"sm_{di.compute_major}{di.compute_minor}, {di.sm_count} SMs, wavefront path tracer")
+        self.pci_bus_id = di.pci_bus_id.decode()
+        self.sm_count = di.sm_count
         self._lock = threading.Lock()
 
     def close(self):
@@ -509,6 +511,14 @@ class CudaDevice:
         s = capi.pe_render_stats()
         capi.check(_lib().pe_device_last_stats(self._h, C.byref(s)))
         return s
+
+    def timer_begin(self):
+        capi.check(_lib().pe_device_timer_begin(self._h))
+
+    def timer_end(self) -> float:
+        ms = C.c_float(0.0)
+        capi.check(_lib().pe_device_timer_end(self._h, C.byref(ms)))
+        return float(ms.value)
 
     def set_counting(self, on: bool):
         capi.check(_lib().pe_device_set_counting(self._h, 1 if on else 0))

@@ -225,6 +225,28 @@ int32_t pe_device_render(pe_device* d, const pe_camera* cam, const pe_settings* 
 int32_t pe_device_render_resident(pe_device* d, const pe_camera* cam, const pe_settings* st, int32_t first_sample,
                                   int32_t count, const volatile int32_t* cancel);
 int32_t pe_device_film_clear(pe_device* d);
+
+/* Tile render that allocates no device memory.  No counterpart in the reference engine.
+ *
+ * For hosts that may not call cudaMalloc/cudaFree while they render: a viewport or plugin
+ * running inside another application that owns the GPU's memory budget and hands out device
+ * buffers from its own pool, or a render thread that must not hit the driver's allocator (which
+ * can block and fragment) in the middle of a frame.  The caller passes the inputs (camera,
+ * settings, the scene already set with pe_device_set_scene) and the outputs: sum_rgb
+ * (width*height*3 floats), sample_count and sum_lum_sq (width*height each), all DEVICE memory
+ * the caller owns, covering the whole film of st->width x st->height.  Samples
+ * [first_sample, first_sample+count) of the pixels in the rectangle (x0, y0, w, h) are added to
+ * them exactly as pe_device_render would add them; other pixels are not touched.
+ *
+ * The path state lives in one file-scope device array of 7.1 MB (room for 32768 paths), which
+ * every GPU that loads this library holds until the process exits; its address on a device is
+ * taken once, when the device is created.  A tile of more than 32768 pixels (w*h) is rejected
+ * with PE_ERR_LIMIT.  Every call uses the same array and finds the previous call's contents in
+ * it (the call clears what must start at zero), so calls that run on the GPU at the same time,
+ * from two threads or two device handles on one GPU, race and corrupt each other's results. */
+int32_t pe_device_render_tile_noalloc(pe_device* d, const pe_camera* cam, const pe_settings* st, int32_t x0, int32_t y0,
+                                      int32_t w, int32_t h, int32_t first_sample, int32_t count, float* sum_rgb,
+                                      uint32_t* sample_count, float* sum_lum_sq);
 int32_t pe_device_film_read(pe_device* d, float* sum_rgb, uint32_t* sample_count, float* sum_lum_sq);
 int32_t pe_device_synchronize(pe_device* d);
 int32_t pe_device_last_stats(pe_device* d, pe_render_stats* out);

@@ -115,6 +115,9 @@ SIGNATURES = {
                                      IP, FP, UP, FP, C.POINTER(C.c_uint64)]),
     "pe_device_render_resident": (C.c_int32, [P, C.POINTER(pe_camera), C.POINTER(pe_settings), C.c_int32, C.c_int32, IP]),
     "pe_device_film_clear": (C.c_int32, [P]),
+    "pe_device_render_tile_noalloc": (C.c_int32, [P, C.POINTER(pe_camera), C.POINTER(pe_settings), C.c_int32,
+                                                  C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_void_p,
+                                                  C.c_void_p, C.c_void_p]),
     "pe_device_film_read": (C.c_int32, [P, FP, UP, FP]),
     "pe_device_synchronize": (C.c_int32, [P]),
     "pe_device_last_stats": (C.c_int32, [P, C.POINTER(pe_render_stats)]),

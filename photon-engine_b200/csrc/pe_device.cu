@@ -64,6 +64,8 @@ struct pe_device {
     bool counting = false;
     pe_render_stats stats{};
     int blocksIntersect = 0, blocksShade = 0, blocksShadow = 0, blocksGen = 0;
+    unsigned char* noAllocBase = nullptr; // device address of g_noAllocScratch on this device
+    std::string noAllocError;
 };
 
 namespace {
@@ -187,19 +189,48 @@ WaveArgs makeWave(const pe_camera* cam, const pe_settings* st) {
 
 constexpr size_t kWaveSlots = size_t(1) << 21; // paths in flight per wave
 
-// The wavefront render of samples [first, first+count) into film (sum, cnt, sq) on the device.
+// Scratch of pe_device_render_tile_noalloc: path-state columns, queues, shadow records and
+// counters for kNoAllocSlots paths, carved out of one file-scope device array (7.1 MB).  Every
+// GPU that loads this library holds the array until the process exits.
+constexpr size_t kNoAllocSlots = size_t(1) << 15;
+constexpr size_t kNoAllocColumn = kNoAllocSlots * sizeof(float4);   // 512 KiB, 256-aligned
+constexpr size_t kNoAllocIndex = kNoAllocSlots * sizeof(int32_t);    // 128 KiB, 256-aligned
+constexpr size_t kNoAllocBytes = 13 * kNoAllocColumn + 3 * kNoAllocIndex + 256;
+static __device__ __align__(256) unsigned char g_noAllocScratch[kNoAllocBytes];
+
+// Path-state view of the scratch whose device address is `base`.
+Paths noAllocPaths(unsigned char* base) {
+    Paths P{};
+    size_t off = 0;
+    auto col = [&](float4*& c) { c = reinterpret_cast<float4*>(base + off); off += kNoAllocColumn; };
+    auto idx = [&](int32_t*& c) { c = reinterpret_cast<int32_t*>(base + off); off += kNoAllocIndex; };
+    col(P.rayO); col(P.rayD); col(P.thr); col(P.L); col(P.lastN); col(P.lastP); col(P.pickP); col(P.pickN); col(P.hit);
+    col(P.shO); col(P.shD); col(P.shC); col(P.shT);
+    idx(P.queueA); idx(P.queueB); idx(P.shadowQ);
+    P.counters = reinterpret_cast<uint32_t*>(base + off);
+    return P;
+}
+
+struct Tile {
+    int x0, y0, w, h;
+};
+
+// The wavefront render of samples [first, first+count) over `tile` into the film (sum, cnt, sq)
+// on the device, with path state in `P` (room for `capacity` slots).  With `timing` the
+// closest-hit / shade / any-hit launches are bracketed by events (stats.ms_*).
 int32_t renderWaves(pe_device* d, const pe_camera* cam, const pe_settings* st, int first, int count,
-                    const volatile int32_t* cancel, float* sum, uint32_t* cnt, float* sq) {
-    const size_t npix = static_cast<size_t>(st->width) * static_cast<size_t>(st->height);
-    const int pixChunk = static_cast<int>(std::min(npix, kWaveSlots));
-    const int samplesPerWave = static_cast<int>(std::max<size_t>(1, std::min<size_t>(static_cast<size_t>(count), kWaveSlots / pixChunk)));
-    int32_t rc = ensureCapacity(d, static_cast<size_t>(samplesPerWave) * static_cast<size_t>(pixChunk));
-    if (rc) return rc;
-    rc = ensureFilter(d, st->filter_type, st->filter_width);
+                    const volatile int32_t* cancel, float* sum, uint32_t* cnt, float* sq, Paths& P, size_t capacity,
+                    bool timing, Tile tile) {
+    const size_t npix = static_cast<size_t>(tile.w) * static_cast<size_t>(tile.h);
+    const int pixChunk = static_cast<int>(std::min(npix, capacity));
+    const int samplesPerWave = static_cast<int>(std::max<size_t>(1, std::min<size_t>(static_cast<size_t>(count), capacity / pixChunk)));
+    int32_t rc = ensureFilter(d, st->filter_type, st->filter_width);
     if (rc) return rc;
     WaveArgs A = makeWave(cam, st);
+    A.tileX = tile.x0;
+    A.tileY = tile.y0;
+    A.tileW = tile.w;
     const SceneGPU& S = d->scene;
-    Paths& P = d->paths;
     const int sm = d->prop.multiProcessorCount;
     pe_render_stats& stats = d->stats;
     std::memset(&stats, 0, sizeof(stats));
@@ -231,6 +262,7 @@ int32_t renderWaves(pe_device* d, const pe_camera* cam, const pe_settings* st, i
             const int nSlots = A.nPix * ns;
             kGenerate<<<sm * 8, 256, 0, d->stream>>>(S, P, A, nSlots);
             ++stats.kernel_launches;
+            ++stats.waves;
             uint32_t live = static_cast<uint32_t>(nSlots);
             PE_CUDA(cudaMemcpyAsync(&P.counters[0], &live, sizeof(uint32_t), cudaMemcpyHostToDevice, d->stream));
             PE_CUDA(cudaMemsetAsync(&P.counters[1], 0, 2 * sizeof(uint32_t), d->stream));
@@ -241,25 +273,30 @@ int32_t renderWaves(pe_device* d, const pe_camera* cam, const pe_settings* st, i
             stats.paths += static_cast<uint64_t>(nSlots);
             for (int iter = 0; live > 0; ++iter) {
                 stats.closest_rays += live;
-                cudaEvent_t e0, e1, e2, e3;
-                if ((rc = event(e0)) || (rc = event(e1)) || (rc = event(e2)) || (rc = event(e3))) return rc;
-                PE_CUDA(cudaEventRecord(e0, d->stream));
+                cudaEvent_t e0 = nullptr, e1 = nullptr, e2 = nullptr, e3 = nullptr;
+                if (timing) {
+                    if ((rc = event(e0)) || (rc = event(e1)) || (rc = event(e2)) || (rc = event(e3))) return rc;
+                    PE_CUDA(cudaEventRecord(e0, d->stream));
+                }
                 if (d->counting)
                     kIntersect<true><<<d->blocksIntersect, 128, 0, d->stream>>>(S, P, qIn, cIn, d->dStats);
                 else
                     kIntersect<false><<<d->blocksIntersect, 128, 0, d->stream>>>(S, P, qIn, cIn, d->dStats);
-                PE_CUDA(cudaEventRecord(e1, d->stream));
+                if (timing) PE_CUDA(cudaEventRecord(e1, d->stream));
                 kShade<<<d->blocksShade, 128, 0, d->stream>>>(S, P, A, qIn, cIn, qOut, cOut);
-                PE_CUDA(cudaEventRecord(e2, d->stream));
+                if (timing) PE_CUDA(cudaEventRecord(e2, d->stream));
                 if (d->counting)
                     kShadow<true><<<d->blocksShadow, 128, 0, d->stream>>>(S, P, &P.counters[2], A.clampIndirect, d->dStats);
                 else
                     kShadow<false><<<d->blocksShadow, 128, 0, d->stream>>>(S, P, &P.counters[2], A.clampIndirect, d->dStats);
-                PE_CUDA(cudaEventRecord(e3, d->stream));
                 stats.kernel_launches += 3;
-                isectEv.push_back({evUsed - 4, evUsed - 3});
-                shadeEv.push_back({evUsed - 3, evUsed - 2});
-                shadowEv.push_back({evUsed - 2, evUsed - 1});
+                ++stats.intersect_launches;
+                if (timing) {
+                    PE_CUDA(cudaEventRecord(e3, d->stream));
+                    isectEv.push_back({evUsed - 4, evUsed - 3});
+                    shadeEv.push_back({evUsed - 3, evUsed - 2});
+                    shadowEv.push_back({evUsed - 2, evUsed - 1});
+                }
                 PE_CUDA(cudaMemcpyAsync(d->hCounters, P.counters, 4 * sizeof(uint32_t), cudaMemcpyDeviceToHost, d->stream));
                 PE_CUDA(cudaStreamSynchronize(d->stream));
                 stats.shadow_rays += d->hCounters[2];
@@ -302,13 +339,11 @@ int32_t renderWaves(pe_device* d, const pe_camera* cam, const pe_settings* st, i
         cudaEventElapsedTime(&t, d->evPool[pr.first], d->evPool[pr.second]);
         stats.ms_shadow += t;
     }
-    stats.intersect_launches = isectEv.size();
     stats.node_visits = hs[0];
     stats.tri_tests = hs[1];
     stats.shadow_node_visits = hs[2];
     stats.shadow_tri_tests = hs[3];
     stats.rejected = hs[4];
-    stats.waves = isectEv.empty() ? 0 : 1;
     if (cancelled) {
         setError("render cancelled");
         return PE_ERR_CANCELLED;
@@ -461,6 +496,14 @@ pe_device* pe_device_create(int32_t ordinal, char* err, size_t errLen) {
         pe_device_destroy(d);
         return fail(std::string("kernel image not loadable on this device: ") + cudaMsg(le));
     }
+    // Device address of the no-allocation scratch on this device, taken once here with the
+    // device current (a host-side use of the array's name would not be a device address).
+    const cudaError_t se = cudaGetSymbolAddress(reinterpret_cast<void**>(&d->noAllocBase), g_noAllocScratch);
+    if (se != cudaSuccess) {
+        d->noAllocBase = nullptr;
+        d->noAllocError = std::string("cudaGetSymbolAddress(no-allocation scratch): ") + cudaMsg(se);
+        cudaGetLastError();
+    }
     return d;
 }
 
@@ -592,7 +635,9 @@ int32_t pe_device_render_resident(pe_device* d, const pe_camera* cam, const pe_s
     if (count <= 0) return PE_OK;
     PE_CUDA(cudaSetDevice(d->ordinal));
     if ((rc = ensureFilm(d, st->width, st->height))) return rc;
-    return renderWaves(d, cam, st, first, count, cancel, d->fSum, d->fCnt, d->fSq);
+    if ((rc = ensureCapacity(d, kWaveSlots))) return rc;
+    return renderWaves(d, cam, st, first, count, cancel, d->fSum, d->fCnt, d->fSq, d->paths, d->capacity, true,
+                       Tile{0, 0, st->width, st->height});
 }
 
 int32_t pe_device_film_clear(pe_device* d) {
@@ -644,7 +689,9 @@ int32_t pe_device_render(pe_device* d, const pe_camera* cam, const pe_settings* 
     PE_CUDA(cudaSetDevice(d->ordinal));
     if ((rc = ensureFilm(d, st->width, st->height))) return rc;
     if ((rc = pe_device_film_clear(d))) return rc;
-    const int32_t rr = renderWaves(d, cam, st, first, count, cancel, d->fSum, d->fCnt, d->fSq);
+    if ((rc = ensureCapacity(d, kWaveSlots))) return rc;
+    const int32_t rr = renderWaves(d, cam, st, first, count, cancel, d->fSum, d->fCnt, d->fSq, d->paths, d->capacity,
+                                   true, Tile{0, 0, st->width, st->height});
     if (rr != PE_OK && rr != PE_ERR_CANCELLED) return rr;
     const size_t n = static_cast<size_t>(st->width) * static_cast<size_t>(st->height);
     std::vector<float> s(n * 3), q(n);
@@ -663,6 +710,47 @@ int32_t pe_device_render(pe_device* d, const pe_camera* cam, const pe_settings* 
     }
     if (traced) *traced = tr;
     return rr;
+}
+
+// Tile render that allocates no device memory: path state lives in g_noAllocScratch, the film is
+// the caller's.  See include/photon_cuda.h for the contract.
+int32_t pe_device_render_tile_noalloc(pe_device* d, const pe_camera* cam, const pe_settings* st, int32_t x0, int32_t y0,
+                                      int32_t w, int32_t h, int32_t first, int32_t count, float* sumRgb,
+                                      uint32_t* sampleCount, float* sumLumSq) {
+    if (!d) {
+        setError("pe_device_render_tile_noalloc: null device");
+        return PE_ERR_INVALID;
+    }
+    if (!d->hasScene) {
+        setError("pe_device_render_tile_noalloc: render before set_scene");
+        return PE_ERR_NO_SCENE;
+    }
+    int32_t rc = checkSettings(cam, st);
+    if (rc) return rc;
+    if (!sumRgb || !sampleCount || !sumLumSq) {
+        setError("pe_device_render_tile_noalloc: film pointers must be device memory of width*height pixels");
+        return PE_ERR_INVALID;
+    }
+    if (x0 < 0 || y0 < 0 || w <= 0 || h <= 0 || x0 + w > st->width || y0 + h > st->height) {
+        setError("pe_device_render_tile_noalloc: tile outside the film");
+        return PE_ERR_INVALID;
+    }
+    if (static_cast<size_t>(w) * static_cast<size_t>(h) > kNoAllocSlots) {
+        setError("pe_device_render_tile_noalloc: tile of " + std::to_string(w) + "x" + std::to_string(h) +
+                 " pixels exceeds the maximum of " + std::to_string(kNoAllocSlots) + " pixels per call");
+        return PE_ERR_LIMIT;
+    }
+    if (!d->noAllocBase) {
+        setError("pe_device_render_tile_noalloc: scratch unavailable: " + d->noAllocError);
+        return PE_ERR_CUDA;
+    }
+    if (count <= 0) return PE_OK;
+    PE_CUDA(cudaSetDevice(d->ordinal));
+    Paths P = noAllocPaths(d->noAllocBase);
+    // The array keeps the previous call's contents; the queue and shadow counters must start at 0.
+    PE_CUDA(cudaMemsetAsync(P.counters, 0, 256, d->stream));
+    return renderWaves(d, cam, st, first, count, nullptr, sumRgb, sampleCount, sumLumSq, P, kNoAllocSlots, false,
+                       Tile{x0, y0, w, h});
 }
 
 int32_t pe_device_synchronize(pe_device* d) {

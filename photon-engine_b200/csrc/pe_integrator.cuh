@@ -50,7 +50,8 @@ struct Paths {
 struct WaveArgs {
     CamDev cam;
     int width, height;
-    int pixelFirst, nPix;   // pixel range of this wave
+    int tileX, tileY, tileW; // rendered rectangle of the film (whole frame: 0, 0, width)
+    int pixelFirst, nPix;   // range of tile-linear pixel indices of this wave
     int sampleFirst, nSamples;
     uint64_t seed;
     float filterWidth;
@@ -82,7 +83,7 @@ __global__ void kGenerate(SceneGPU S, Paths P, WaveArgs A, int nSlots) {
     for (int slot = blockIdx.x * blockDim.x + threadIdx.x; slot < nSlots; slot += gridDim.x * blockDim.x) {
         const int sOff = slot / A.nPix;
         const int pix = A.pixelFirst + (slot - sOff * A.nPix);
-        const int x = pix % A.width, y = pix / A.width;
+        const int x = A.tileX + pix % A.tileW, y = A.tileY + pix / A.tileW;
         Sobol sb;
         sb.pixelHash = pixelHashOf(A.seed, x, y);
         sb.revIndex = rev32(static_cast<uint32_t>(A.sampleFirst + sOff));
@@ -414,7 +415,8 @@ __global__ void __launch_bounds__(128) kShade(SceneGPU S, Paths P, WaveArgs A, c
 __global__ void kFilm(Paths P, WaveArgs A, float* sum, uint32_t* cnt, float* sumSq, unsigned long long* rejected) {
     unsigned long long rej = 0;
     for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < A.nPix; p += gridDim.x * blockDim.x) {
-        const int pix = A.pixelFirst + p;
+        const int tp = A.pixelFirst + p;
+        const int pix = (A.tileY + tp / A.tileW) * A.width + A.tileX + tp % A.tileW;
         float sr = sum[3 * pix + 0], sg = sum[3 * pix + 1], sbb = sum[3 * pix + 2];
         float sq = sumSq[pix];
         uint32_t c = cnt[pix];

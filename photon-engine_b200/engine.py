@@ -496,6 +496,14 @@ class CudaDevice:
         capi.check(_lib().pe_device_render_resident(self._h, C.byref(camera.describe_gpu()), C.byref(st),
                                                     first_sample, count, None))
 
+    def render_tile_noalloc(self, camera: PerspectiveCamera, settings: RenderSettings, x0: int, y0: int, w: int, h: int,
+                            first_sample: int, count: int, sum_ptr: int, count_ptr: int, sum_sq_ptr: int):
+        """Adds samples of one film rectangle into caller-owned device buffers without allocating
+        device memory (for hosts that cannot allocate while they render; see
+        pe_device_render_tile_noalloc in include/photon_cuda.h).  At most 32768 pixels per call."""
+        capi.check(_lib().pe_device_render_tile_noalloc(self._h, C.byref(camera.describe_gpu()), C.byref(settings.to_c()),
+                                                        x0, y0, w, h, first_sample, count, sum_ptr, count_ptr, sum_sq_ptr))
+
     def film_clear(self):
         capi.check(_lib().pe_device_film_clear(self._h))
 

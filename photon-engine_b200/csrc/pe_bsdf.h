@@ -186,7 +186,7 @@ PE_HD float thinFilmReflectance(float cos1, float n1, float n2, Cx n3, float thi
     const Cx rp = (cx(r12p, 0.0f) + r23p * e) / (cx(1.0f, 0.0f) + r12p * (r23p * e));
     return sclamp(0.5f * (cnorm(rs) + cnorm(rp)), 0.0f, 1.0f);
 }
-PE_HD V3 thinFilmRGB(float cos1, float filmIor, const Cx baseIor[3], float thicknessNm) {
+PE_HDN V3 thinFilmRGB(float cos1, float filmIor, const Cx baseIor[3], float thicknessNm) {
     const float lam[3][3] = {{610.0f, 640.0f, 670.0f}, {515.0f, 540.0f, 565.0f}, {440.0f, 465.0f, 490.0f}};
     V3 out;
     for (int c = 0; c < 3; ++c) {
@@ -496,7 +496,7 @@ PE_HD float pdfSpecTransmission(V3 woL, V3 wiL, const DisneyParams& p) {
 
 // Sum of all lobes f(wo, wi) (disney.cpp:223-311).  diffuseOut (may be null) receives the
 // diffuse share, used for the next-ray visibility class.
-PE_HD V3 disneyEval(const TablesGPU* T, V3 wo, V3 wi, const DisneyParams& p, V3* diffuseOut) {
+PE_HDN V3 disneyEval(const TablesGPU* T, V3 wo, V3 wi, const DisneyParams& p, V3* diffuseOut) {
     const Frame frame = shadingFrame(p.normal, p.tangent);
     const V3 woL = toLocal(frame, wo);
     const V3 wiL = toLocal(frame, wi);
@@ -592,7 +592,7 @@ PE_HD LobeWeights disneyLobeWeights(const DisneyParams& p) {
     return w;
 }
 
-PE_HD float disneyPdf(V3 wo, V3 wi, const DisneyParams& p) {
+PE_HDN float disneyPdf(V3 wo, V3 wi, const DisneyParams& p) {
     const Frame frame = shadingFrame(p.normal, p.tangent);
     const V3 woL = toLocal(frame, wo);
     const V3 wiL = toLocal(frame, wi);
@@ -649,7 +649,7 @@ PE_HD bool disneySampleSpecTransLobe(const DisneyParams& p, V3 woL, float u1, fl
 }
 
 // DisneyMaterial::sampleFull (disney.cpp:680-729).
-PE_HD bool disneySample(const TablesGPU* T, V3 wo, const DisneyParams& p, float uc, V2 u, BsdfSample& out) {
+PE_HDN bool disneySample(const TablesGPU* T, V3 wo, const DisneyParams& p, float uc, V2 u, BsdfSample& out) {
     out.delta = false;
     out.subsurface = false;
     out.passThrough = false;
@@ -846,7 +846,7 @@ PE_HD V3 glassShadowTransmittance(const MatGPU& m, V3 ng, V3 n, V3 dir) {
     const V3 nn = len2(ng) > 0.0f ? normalize(ng) : n;
     return (mk(1.0f) - thinWallReflectance(m, dot(dir, nn))) * m3(m.base);
 }
-PE_HD V3 glassEval(const MatGPU& m, V3 wo, V3 wi, const ShadePoint& sp, float& pdf) {
+PE_HDN V3 glassEval(const MatGPU& m, V3 wo, V3 wi, const ShadePoint& sp, float& pdf) {
     pdf = 0.0f;
     if (m.glassRoughness <= 1e-3f) return mk(0.0f);
     const GlassLocal g = glassFrame(wo, sp);
@@ -857,7 +857,7 @@ PE_HD V3 glassEval(const MatGPU& m, V3 wo, V3 wi, const ShadePoint& sp, float& p
     return glassEvalRough(g.wo, wiL, ior, alpha, m3(m.base));
 }
 // Dielectric::sampleFull / sampleWithLobe (dielectric.cpp:166-294).
-PE_HD bool glassSample(const MatGPU& m, V3 woW, const ShadePoint& sp, float uc, V2 u, BsdfSample& out) {
+PE_HDN bool glassSample(const MatGPU& m, V3 woW, const ShadePoint& sp, float uc, V2 u, BsdfSample& out) {
     out.subsurface = false;
     out.passThrough = false;
     out.weight = mk(0.0f);

@@ -110,13 +110,14 @@ int32_t ensureCapacity(pe_device* d, size_t slots) {
         if ((st = devAlloc(d->pathBufs, *c, slots))) return st;
     if ((st = devAlloc(d->pathBufs, P.queueA, slots))) return st;
     if ((st = devAlloc(d->pathBufs, P.queueB, slots))) return st;
-    // shadow records: one per slot and NEE sample (shadow quality <= 4)
-    const size_t sh = slots * 4;
-    if ((st = devAlloc(d->pathBufs, P.shadowQ, sh))) return st;
+    if ((st = devAlloc(d->pathBufs, P.sortQ, slots * kShadeKeys))) return st;
+    // shadow records: one per slot (shadow quality 1)
+    if ((st = devAlloc(d->pathBufs, P.shadowQ, slots))) return st;
     float4** scols[] = {&P.shO, &P.shD, &P.shC, &P.shT};
     for (float4** c : scols)
-        if ((st = devAlloc(d->pathBufs, *c, sh))) return st;
-    if ((st = devAlloc(d->pathBufs, P.counters, 16))) return st;
+        if ((st = devAlloc(d->pathBufs, *c, slots))) return st;
+    if ((st = devAlloc(d->pathBufs, P.counters, CNT_TOTAL))) return st;
+    P.capacity = static_cast<uint32_t>(slots);
     d->capacity = slots;
     return PE_OK;
 }
@@ -190,12 +191,12 @@ WaveArgs makeWave(const pe_camera* cam, const pe_settings* st) {
 constexpr size_t kWaveSlots = size_t(1) << 21; // paths in flight per wave
 
 // Scratch of pe_device_render_tile_noalloc: path-state columns, queues, shadow records and
-// counters for kNoAllocSlots paths, carved out of one file-scope device array (7.1 MB).  Every
+// counters for kNoAllocSlots paths, carved out of one file-scope device array (7.9 MB).  Every
 // GPU that loads this library holds the array until the process exits.
 constexpr size_t kNoAllocSlots = size_t(1) << 15;
 constexpr size_t kNoAllocColumn = kNoAllocSlots * sizeof(float4);   // 512 KiB, 256-aligned
 constexpr size_t kNoAllocIndex = kNoAllocSlots * sizeof(int32_t);    // 128 KiB, 256-aligned
-constexpr size_t kNoAllocBytes = 13 * kNoAllocColumn + 3 * kNoAllocIndex + 256;
+constexpr size_t kNoAllocBytes = 13 * kNoAllocColumn + (3 + kShadeKeys) * kNoAllocIndex + 256;
 static __device__ __align__(256) unsigned char g_noAllocScratch[kNoAllocBytes];
 
 // Path-state view of the scratch whose device address is `base`.
@@ -203,11 +204,12 @@ Paths noAllocPaths(unsigned char* base) {
     Paths P{};
     size_t off = 0;
     auto col = [&](float4*& c) { c = reinterpret_cast<float4*>(base + off); off += kNoAllocColumn; };
-    auto idx = [&](int32_t*& c) { c = reinterpret_cast<int32_t*>(base + off); off += kNoAllocIndex; };
+    auto idx = [&](int32_t*& c, size_t n) { c = reinterpret_cast<int32_t*>(base + off); off += n * kNoAllocIndex; };
     col(P.rayO); col(P.rayD); col(P.thr); col(P.L); col(P.lastN); col(P.lastP); col(P.pickP); col(P.pickN); col(P.hit);
     col(P.shO); col(P.shD); col(P.shC); col(P.shT);
-    idx(P.queueA); idx(P.queueB); idx(P.shadowQ);
+    idx(P.queueA, 1); idx(P.queueB, 1); idx(P.shadowQ, 1); idx(P.sortQ, kShadeKeys);
     P.counters = reinterpret_cast<uint32_t*>(base + off);
+    P.capacity = static_cast<uint32_t>(kNoAllocSlots);
     return P;
 }
 
@@ -264,8 +266,8 @@ int32_t renderWaves(pe_device* d, const pe_camera* cam, const pe_settings* st, i
             ++stats.kernel_launches;
             ++stats.waves;
             uint32_t live = static_cast<uint32_t>(nSlots);
+            PE_CUDA(cudaMemsetAsync(&P.counters[1], 0, (CNT_TOTAL - 1) * sizeof(uint32_t), d->stream));
             PE_CUDA(cudaMemcpyAsync(&P.counters[0], &live, sizeof(uint32_t), cudaMemcpyHostToDevice, d->stream));
-            PE_CUDA(cudaMemsetAsync(&P.counters[1], 0, 2 * sizeof(uint32_t), d->stream));
             int32_t* qIn = P.queueA;
             int32_t* qOut = P.queueB;
             uint32_t* cIn = &P.counters[0];
@@ -283,7 +285,7 @@ int32_t renderWaves(pe_device* d, const pe_camera* cam, const pe_settings* st, i
                 else
                     kIntersect<false><<<d->blocksIntersect, 128, 0, d->stream>>>(S, P, qIn, cIn, d->dStats);
                 if (timing) PE_CUDA(cudaEventRecord(e1, d->stream));
-                kShade<<<d->blocksShade, 128, 0, d->stream>>>(S, P, A, qIn, cIn, qOut, cOut);
+                kShade<<<d->blocksShade, 128, 0, d->stream>>>(S, P, A, qOut, cOut);
                 if (timing) PE_CUDA(cudaEventRecord(e2, d->stream));
                 if (d->counting)
                     kShadow<true><<<d->blocksShadow, 128, 0, d->stream>>>(S, P, &P.counters[2], A.clampIndirect, d->dStats);
@@ -305,9 +307,11 @@ int32_t renderWaves(pe_device* d, const pe_camera* cam, const pe_settings* st, i
                     setError("wavefront did not drain after 4096 iterations");
                     return PE_ERR_DEVICE;
                 }
-                // swap queues; reset the consumed counter and the shadow counter
+                // swap queues; reset the consumed queue's counter, the shadow counter, the work
+                // cursors and the shading-key bins
                 PE_CUDA(cudaMemsetAsync(cIn, 0, sizeof(uint32_t), d->stream));
-                PE_CUDA(cudaMemsetAsync(&P.counters[2], 0, sizeof(uint32_t), d->stream));
+                PE_CUDA(cudaMemsetAsync(&P.counters[CNT_SHADOW], 0, (CNT_KEYS + kShadeKeys - CNT_SHADOW) * sizeof(uint32_t),
+                                        d->stream));
                 std::swap(qIn, qOut);
                 std::swap(cIn, cOut);
             }

@@ -870,7 +870,10 @@ static int32_t buildScene(pe_scene* s) {
             const V3 e1 = p1 - p0, e2 = p2 - p0;
             const float eps = 1e-14f * len2(e1) * len2(e2);
             B.tris[3 * i + 0] = f4(p0.x, p0.y, p0.z, eps);
-            B.tris[3 * i + 1] = f4(e1.x, e1.y, e1.z, bitsf(triMask[g]));
+            // w: visibility mask (bits 0-7) and material type (bits 8-15; the shading key)
+            const uint32_t matType = static_cast<uint32_t>(s->materials[static_cast<size_t>(
+                s->shapes[static_cast<size_t>(tv.w)].material)].type);
+            B.tris[3 * i + 1] = f4(e1.x, e1.y, e1.z, bitsf(static_cast<uint32_t>(triMask[g]) | (matType << 8)));
             B.tris[3 * i + 2] = f4(e2.x, e2.y, e2.z, bitsf(g));
         }
         // interior nodes → 64-byte child-box nodes

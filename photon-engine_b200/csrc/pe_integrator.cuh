@@ -44,8 +44,24 @@ struct Paths {
     float4* shD;     // shadow direction xyz, scalar (cos*w/(pdf*n))
     float4* shC;     // f*Li xyz, flags (bit0: indirect)
     float4* shT;     // throughput at NEE xyz
-    uint32_t* counters; // [0] queue A count, [1] queue B count, [2] shadow count, [3] error flags, [4..] stats
+    int32_t* sortQ;  // kShadeKeys segments of `capacity` slots: rays binned by shading key
+    uint32_t capacity;
+    // [0] queue A count, [1] queue B count, [2] shadow count, [3] closest-hit work cursor,
+    // [4] any-hit work cursor, [5] shade work cursor, [6..10] rays per shading key, [11] errors
+    uint32_t* counters;
 };
+
+// Shading keys: 0 = miss, 1 + material type (Lambert, Disney, Dielectric, Mirror).
+constexpr int kShadeKeys = 5;
+enum CounterSlots { CNT_QA = 0, CNT_QB = 1, CNT_SHADOW = 2, CNT_WORK_ISECT = 3, CNT_WORK_SHADOW = 4,
+                    CNT_WORK_SHADE = 5, CNT_KEYS = 6, CNT_ERRORS = 11, CNT_TOTAL = 16 };
+
+// Persistent-warp work distribution: lane 0 claims the next 32 items for its warp.
+__device__ __forceinline__ int warpFetch(uint32_t* cursor) {
+    int base = 0;
+    if ((threadIdx.x & 31) == 0) base = static_cast<int>(atomicAdd(cursor, 32u));
+    return __shfl_sync(0xffffffffu, base, 0);
+}
 
 struct WaveArgs {
     CamDev cam;
@@ -103,18 +119,38 @@ __global__ void kGenerate(SceneGPU S, Paths P, WaveArgs A, int nSlots) {
 }
 
 // ---- closest hit over a queue -----------------------------------------------------------------
+// Closest hit for every queued ray; each ray is then binned by its shading key (miss or the
+// hit material's type) so the shading kernel runs warps of one material kind.
 template <bool COUNT>
 __global__ void __launch_bounds__(128) kIntersect(SceneGPU S, Paths P, const int32_t* queue, const uint32_t* count,
                                                   unsigned long long* stats) {
     const int n = static_cast<int>(*count);
     uint32_t nodes = 0, tris = 0;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const int slot = queue[i];
-        const float4 ro = P.rayO[slot];
-        const float4 rd = P.rayD[slot];
-        const Hit h = traceClosest<COUNT>(S, mk(ro.x, ro.y, ro.z), mk(rd.x, rd.y, rd.z), __float_as_uint(ro.w), 0.0f,
-                                          1e30f, nodes, tris);
-        P.hit[slot] = make_float4(h.t, h.u, h.v, __int_as_float(h.prim));
+    const int lane = threadIdx.x & 31;
+    for (;;) {
+        const int base = warpFetch(&P.counters[CNT_WORK_ISECT]);
+        if (base >= n) break;
+        const int i = base + lane;
+        int key = -1, slot = -1;
+        if (i < n) {
+            slot = queue[i];
+            const float4 ro = P.rayO[slot];
+            const float4 rd = P.rayD[slot];
+            const Hit h = traceClosest<COUNT>(S, mk(ro.x, ro.y, ro.z), mk(rd.x, rd.y, rd.z), __float_as_uint(ro.w), 0.0f,
+                                              1e30f, nodes, tris);
+            P.hit[slot] = make_float4(h.t, h.u, h.v, __int_as_float(h.prim));
+            key = h.prim < 0 ? 0 : 1 + static_cast<int>((h.meta >> 8) & 0xFFu);
+        }
+        // warp-aggregated append into the key's segment: one atomic per distinct key per warp
+        const unsigned peers = __match_any_sync(0xffffffffu, key);
+        if (key >= 0) {
+            const int leader = __ffs(peers) - 1;
+            const int rank = __popc(peers & ((1u << lane) - 1u));
+            uint32_t at = 0;
+            if (lane == leader) at = atomicAdd(&P.counters[CNT_KEYS + key], static_cast<uint32_t>(__popc(peers)));
+            at = __shfl_sync(peers, at, leader);
+            P.sortQ[static_cast<size_t>(key) * P.capacity + at + rank] = slot;
+        }
     }
     if (COUNT) {
         atomicAdd(&stats[0], static_cast<unsigned long long>(nodes));
@@ -128,7 +164,11 @@ __global__ void __launch_bounds__(128) kShadow(SceneGPU S, Paths P, const uint32
                                                unsigned long long* stats) {
     const int n = static_cast<int>(*count);
     uint32_t nodes = 0, tris = 0;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    for (;;) {
+        const int base = warpFetch(&P.counters[CNT_WORK_SHADOW]);
+        if (base >= n) break;
+        const int i = base + (threadIdx.x & 31);
+        if (i >= n) continue;
         const int slot = P.shadowQ[i];
         const float4 so = P.shO[i];
         const float4 sd = P.shD[i];
@@ -164,18 +204,31 @@ __device__ __forceinline__ void addL(float4& L, V3 c) {
 }
 
 // ---- shade: Li's loop body between two closest-hit queries ------------------------------------
-__global__ void __launch_bounds__(128) kShade(SceneGPU S, Paths P, WaveArgs A, const int32_t* queue, const uint32_t* count,
-                                              int32_t* nextQueue, uint32_t* nextCount) {
+// Consumes the rays binned by shading key (segment by segment, so a warp mostly shades one
+// material kind) and appends the continuing paths to nextQueue.
+__global__ void __launch_bounds__(128, 4) kShade(SceneGPU S, Paths P, WaveArgs A, int32_t* nextQueue, uint32_t* nextCount) {
     const TablesGPU* T = S.tables;
-    const int n = static_cast<int>(*count);
-    const int stride = gridDim.x * blockDim.x;
-    const int nIter = (n + stride - 1) / stride;
-    for (int it = 0; it < nIter; ++it) {
-        const int i = it * stride + blockIdx.x * blockDim.x + threadIdx.x;
+    uint32_t seg[kShadeKeys];
+    int n = 0;
+    for (int k = 0; k < kShadeKeys; ++k) {
+        seg[k] = P.counters[CNT_KEYS + k];
+        n += static_cast<int>(seg[k]);
+    }
+    const int lane = threadIdx.x & 31;
+    for (;;) {
+        const int base = warpFetch(&P.counters[CNT_WORK_SHADE]);
+        if (base >= n) break;
+        const int i = base + lane;
         bool cont = false;
         int slot = -1;
         if (i < n) {
-            slot = queue[i];
+            int k = 0;
+            uint32_t j = static_cast<uint32_t>(i);
+            while (k < kShadeKeys - 1 && j >= seg[k]) {
+                j -= seg[k];
+                ++k;
+            }
+            slot = P.sortQ[static_cast<size_t>(k) * P.capacity + j];
             float4 ro = P.rayO[slot];
             float4 rd = P.rayD[slot];
             float4 th = P.thr[slot];

@@ -93,7 +93,7 @@ PE_HD V3 sampleSphRect(const SphRect& r, V2 u) {
 constexpr float kMinSolidAngle = 1e-3f;
 
 // ---- explicit lights ------------------------------------------------------------------------
-PE_HD LightSample sampleLight(const LightGPU& l, V3 p, V2 u) {
+PE_HDN LightSample sampleLight(const LightGPU& l, V3 p, V2 u) {
     LightSample ls;
     ls.wi = mk(0.0f);
     ls.Li = mk(0.0f);
@@ -148,7 +148,7 @@ PE_HD LightSample sampleLight(const LightGPU& l, V3 p, V2 u) {
 }
 
 // Light::pdfLiHit for a BSDF ray from ref that hit the light's geometry at pHit.
-PE_HD float lightPdfHit(const LightGPU& l, V3 ref, V3 pHit) {
+PE_HDN float lightPdfHit(const LightGPU& l, V3 ref, V3 pHit) {
     const V3 nrm = m3f(l.normal);
     if (l.type == LT_TRIANGLE) {
         const V3 toL = pHit - ref;
@@ -235,7 +235,7 @@ PE_HD V3 envEvalSky(const EnvGPU& e, V3 dir) {
     const V2 uv = dirToEquirect(dir, e.rotation);
     return sampleEquirect(e, uv.x, uv.y) * e.intensity;
 }
-PE_HD V3 envEval(const EnvGPU& e, V3 dir) {
+PE_HDN V3 envEval(const EnvGPU& e, V3 dir) {
     V3 sun = mk(0.0f);
     if (e.sunPdfWeight > 0.0f && dot(normalize(dir), m3f(e.sunDir)) >= e.sunCosMax) sun = m3f(e.sunRadiance);
     return envEvalSky(e, dir) + sun;
@@ -253,7 +253,7 @@ PE_HD float envImagePdf(const EnvGPU& e, V3 wi) {
     const float f = e.func[static_cast<size_t>(y) * static_cast<size_t>(e.width) + static_cast<size_t>(x)];
     return (f / e.funcInt) * static_cast<float>(e.width * e.height) / (kTwoPi * kPi * sinTheta);
 }
-PE_HD float envPdf(const EnvGPU& e, V3 wi) {
+PE_HDN float envPdf(const EnvGPU& e, V3 wi) {
     if (e.sunPdfWeight <= 0.0f) return envImagePdf(e, wi);
     float pdf = 0.0f;
     if (dot(normalize(wi), m3f(e.sunDir)) >= e.sunCosMax) pdf += e.sunPdfWeight / (kTwoPi * (1.0f - e.sunCosMax));
@@ -307,7 +307,7 @@ PE_HD LightSample envSampleImage(const EnvGPU& e, V2 s) {
     ls.Li = envEval(e, ls.wi);
     return ls;
 }
-PE_HD LightSample envSample(const EnvGPU& e, V2 s) {
+PE_HDN LightSample envSample(const EnvGPU& e, V2 s) {
     LightSample ls;
     ls.wi = mk(0.0f);
     ls.Li = mk(0.0f);
@@ -395,7 +395,7 @@ PE_HD float candidateImportance(const SceneGPU& S, int idx, V3 p, V3 n) {
     return envImportance(S.env, n);
 }
 
-PE_HD void lightPrepare(const SceneGPU& S, V3 p, V3 n, LightCtx& c) {
+PE_HDN void lightPrepare(const SceneGPU& S, V3 p, V3 n, LightCtx& c) {
     c.p = p;
     c.n = n;
     c.owner = true;
@@ -432,7 +432,7 @@ PE_HD void lightPrepare(const SceneGPU& S, V3 p, V3 n, LightCtx& c) {
     c.uniform = false;
 }
 
-PE_HD int bvhLightSample(const SceneGPU& S, V3 p, V3 n, float u, float& pmf) {
+PE_HDN int bvhLightSample(const SceneGPU& S, V3 p, V3 n, float u, float& pmf) {
     pmf = 1.0f;
     int node = 0;
     for (int guard = 0; guard < 128; ++guard) {
@@ -459,7 +459,7 @@ PE_HD int bvhLightSample(const SceneGPU& S, V3 p, V3 n, float u, float& pmf) {
     pmf = 0.0f;
     return -1;
 }
-PE_HD float bvhLightPmf(const SceneGPU& S, V3 p, V3 n, int index) {
+PE_HDN float bvhLightPmf(const SceneGPU& S, V3 p, V3 n, int index) {
     if (index < 0 || index >= S.lightCount) return 0.0f;
     unsigned long long trail = S.trail[index];
     const int depth = S.trailDepth[index];
@@ -486,7 +486,7 @@ PE_HD float bvhLightPmf(const SceneGPU& S, V3 p, V3 n, int index) {
 }
 
 // Context::sample (light_sampler.cpp:195-228): candidate index (env = nLights) or -1.
-PE_HD int lightCtxSample(const SceneGPU& S, const LightCtx& c, float u, float& pmf) {
+PE_HDN int lightCtxSample(const SceneGPU& S, const LightCtx& c, float u, float& pmf) {
     pmf = 0.0f;
     if (!c.owner) return -1;
     const int n = S.lightCount;
@@ -521,7 +521,7 @@ PE_HD int lightCtxSample(const SceneGPU& S, const LightCtx& c, float u, float& p
 }
 
 // Context::pmf (light_sampler.cpp:230-241).
-PE_HD float lightCtxPmf(const SceneGPU& S, const LightCtx& c, int index) {
+PE_HDN float lightCtxPmf(const SceneGPU& S, const LightCtx& c, int index) {
     if (!c.owner) return 0.0f;
     if (index < 0 || index >= S.lightCount) return 0.0f;
     if (c.uniform) return 1.0f / static_cast<float>(S.lightCount);

@@ -11,8 +11,12 @@
 
 #if defined(__CUDACC__)
 #define PE_HD __host__ __device__ __forceinline__
+// Large BSDF / light routines stay out of line on the device: the shading kernel runs many
+// different ones in one warp and inlining them all overflows the instruction cache.
+#define PE_HDN __host__ __device__ __noinline__
 #else
 #define PE_HD inline
+#define PE_HDN inline
 #endif
 
 namespace pe {

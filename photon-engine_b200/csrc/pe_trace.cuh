@@ -114,6 +114,7 @@ __device__ __forceinline__ bool triLean(const float4 a, const float4 b, const fl
 struct Hit {
     float t, u, v;
     int32_t prim; // leaf-order primitive index, -1 = miss
+    uint32_t meta; // visibility mask | material type << 8 of the hit triangle
 };
 
 __device__ __forceinline__ void leafRange(int ref, int& first, int& count) {
@@ -139,6 +140,7 @@ __device__ __forceinline__ void testLeafClosest(const SceneGPU& S, int first, in
             best.u = u;
             best.v = v;
             best.prim = pi;
+            best.meta = __float_as_uint(b.w);
         }
     }
 }
@@ -151,6 +153,7 @@ __device__ Hit traceClosest(const SceneGPU& S, V3 o, V3 d, uint32_t mask, float 
                             uint32_t& triTests) {
     Hit best;
     best.prim = -1;
+    best.meta = 0;
     best.t = tMax;
     best.u = best.v = 0.0f;
     const V3 inv = mk(1.0f / d.x, 1.0f / d.y, 1.0f / d.z);
@@ -166,12 +169,11 @@ __device__ Hit traceClosest(const SceneGPU& S, V3 o, V3 d, uint32_t mask, float 
     float stackT[kMaxStack];
     int sp = 0;
     int cur = 0;
+    // while-while form: descend through interior nodes until a leaf (or nothing) is next, test the
+    // leaf, pop.  A ray's own sequence of node and triangle tests is the reference's; the loop
+    // shape only lets the lanes of a warp spend more of their steps in the same branch.
     for (;;) {
-        if (cur < 0) {
-            int first, count;
-            leafRange(cur, first, count);
-            testLeafClosest<COUNT>(S, first, count, o, d, mask, tMin, tMax, best, triTests);
-        } else {
+        while (cur >= 0) {
             if (COUNT) ++nodeVisits;
             const float4 n0 = __ldg(&S.nodes[4 * cur + 0]);
             const float4 n1 = __ldg(&S.nodes[4 * cur + 1]);
@@ -182,28 +184,32 @@ __device__ Hit traceClosest(const SceneGPU& S, V3 o, V3 d, uint32_t mask, float 
             const bool h1 = slab(n1.x, n1.y, n1.z, n1.w, n2.z, n2.w, o, inv, tMin, tMax, t1);
             const int c0 = __float_as_int(n3.x), c1 = __float_as_int(n3.y);
             if (h0 && h1) {
-                if (t1 < t0) {
-                    stackRef[sp] = c0;
-                    stackT[sp] = t0;
-                    ++sp;
-                    cur = c1;
-                } else {
-                    stackRef[sp] = c1;
-                    stackT[sp] = t1;
-                    ++sp;
-                    cur = c0;
-                }
-                continue;
-            }
-            if (h0) {
+                const bool farFirst = t1 < t0;
+                stackRef[sp] = farFirst ? c0 : c1;
+                stackT[sp] = farFirst ? t0 : t1;
+                ++sp;
+                cur = farFirst ? c1 : c0;
+            } else if (h0) {
                 cur = c0;
-                continue;
-            }
-            if (h1) {
+            } else if (h1) {
                 cur = c1;
-                continue;
+            } else {
+                // pop: entries farther than the current hit are skipped
+                bool found = false;
+                while (sp > 0) {
+                    --sp;
+                    if (stackT[sp] <= tMax) {
+                        cur = stackRef[sp];
+                        found = true;
+                        break;
+                    }
+                }
+                if (!found) return best;
             }
         }
+        int first, count;
+        leafRange(cur, first, count);
+        testLeafClosest<COUNT>(S, first, count, o, d, mask, tMin, tMax, best, triTests);
         bool found = false;
         while (sp > 0) {
             --sp;
@@ -213,9 +219,8 @@ __device__ Hit traceClosest(const SceneGPU& S, V3 o, V3 d, uint32_t mask, float 
                 break;
             }
         }
-        if (!found) break;
+        if (!found) return best;
     }
-    return best;
 }
 
 // BVH::intersectAny (bvh.cpp:404-446): true when any triangle in [tMin, tMax] passes the
@@ -232,20 +237,7 @@ __device__ bool traceAny(const SceneGPU& S, V3 o, V3 d, uint32_t mask, float tMi
     int sp = 0;
     int cur = S.rootIsLeaf ? static_cast<int>(~((static_cast<uint32_t>(S.rootFirst) << 8) | static_cast<uint32_t>(S.rootCount - 1))) : 0;
     for (;;) {
-        if (cur < 0) {
-            int first, count;
-            leafRange(cur, first, count);
-            for (int k = 0; k < count; ++k) {
-                const int pi = first + k;
-                const float4 a = __ldg(&S.tris[3 * pi + 0]);
-                const float4 b = __ldg(&S.tris[3 * pi + 1]);
-                if ((__float_as_uint(b.w) & mask) == 0u) continue;
-                const float4 c = __ldg(&S.tris[3 * pi + 2]);
-                if (COUNT) ++triTests;
-                float t, u, v;
-                if (triLean(a, b, c, o, d, tMin, tMax, t, u, v)) return true;
-            }
-        } else {
+        while (cur >= 0) {
             if (COUNT) ++nodeVisits;
             const float4 n0 = __ldg(&S.nodes[4 * cur + 0]);
             const float4 n1 = __ldg(&S.nodes[4 * cur + 1]);
@@ -259,21 +251,30 @@ __device__ bool traceAny(const SceneGPU& S, V3 o, V3 d, uint32_t mask, float tMi
                 const bool farFirst = t1 < t0;
                 stackRef[sp++] = farFirst ? c0 : c1;
                 cur = farFirst ? c1 : c0;
-                continue;
-            }
-            if (h0) {
+            } else if (h0) {
                 cur = c0;
-                continue;
-            }
-            if (h1) {
+            } else if (h1) {
                 cur = c1;
-                continue;
+            } else {
+                if (sp == 0) return false;
+                cur = stackRef[--sp];
             }
         }
-        if (sp == 0) break;
+        int first, count;
+        leafRange(cur, first, count);
+        for (int k = 0; k < count; ++k) {
+            const int pi = first + k;
+            const float4 a = __ldg(&S.tris[3 * pi + 0]);
+            const float4 b = __ldg(&S.tris[3 * pi + 1]);
+            if ((__float_as_uint(b.w) & mask) == 0u) continue;
+            const float4 c = __ldg(&S.tris[3 * pi + 2]);
+            if (COUNT) ++triTests;
+            float t, u, v;
+            if (triLean(a, b, c, o, d, tMin, tMax, t, u, v)) return true;
+        }
+        if (sp == 0) return false;
         cur = stackRef[--sp];
     }
-    return false;
 }
 
 // ---- hit record (src/geometry/triangle.cpp:54-133) -----------------------------------------
@@ -291,7 +292,7 @@ __device__ __forceinline__ V3 ld3(const float4* a, int i) {
     return mk(v.x, v.y, v.z);
 }
 
-__device__ void fillHit(const SceneGPU& S, const Hit& h, V3 rayDir, Isect& is) {
+__device__ __noinline__ void fillHit(const SceneGPU& S, const Hit& h, V3 rayDir, Isect& is) {
     const float4 e2w = __ldg(&S.tris[3 * h.prim + 2]);
     const int g = static_cast<int>(__float_as_uint(e2w.w));
     const int4 tv = __ldg(&S.triVerts[g]);

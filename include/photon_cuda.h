@@ -238,7 +238,7 @@ int32_t pe_device_film_clear(pe_device* d);
  * [first_sample, first_sample+count) of the pixels in the rectangle (x0, y0, w, h) are added to
  * them exactly as pe_device_render would add them; other pixels are not touched.
  *
- * The path state lives in one file-scope device array of 7.1 MB (room for 32768 paths), which
+ * The path state lives in one file-scope device array of 7.9 MB (room for 32768 paths), which
  * every GPU that loads this library holds until the process exits; its address on a device is
  * taken once, when the device is created.  A tile of more than 32768 pixels (w*h) is rejected
  * with PE_ERR_LIMIT.  Every call uses the same array and finds the previous call's contents in

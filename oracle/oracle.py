@@ -206,3 +206,98 @@ def sobol(seed: int, px, py, index, n_dims: int) -> np.ndarray:
 
 def cpu_threads() -> int:
     return len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else (os.cpu_count() or 1)
+
+
+# ---- the C restatement (pe_oracle.c): Lambert + emissive-triangle scenes --------------------
+class CamDesc(C.Structure):
+    _fields_ = [("position", C.c_float * 3), ("lower_left", C.c_float * 3), ("horizontal", C.c_float * 3),
+                ("vertical", C.c_float * 3)]
+
+
+def _load_restatement():
+    if "restatement" in _libs:
+        return _libs["restatement"]
+    if not RESTATEMENT_LIB.exists():
+        raise RuntimeError(f"{RESTATEMENT_LIB} missing: build it with `make -C oracle restatement`")
+    lib = C.CDLL(str(RESTATEMENT_LIB))
+    P = C.c_void_p
+    sig = {
+        "po_scene_create": (P, []),
+        "po_scene_destroy": (None, [P]),
+        "po_scene_add_mesh": (C.c_int32, [P, FP, C.c_uint32, UP, C.c_uint32, FP, FP]),
+        "po_sobol": (C.c_int32, [C.c_uint64, C.c_int32, C.c_int32, C.c_int32, C.c_int32, FP]),
+        "po_trace_primary": (C.c_int32, [P, C.POINTER(CamDesc), C.c_int32, C.c_int32, C.c_uint64, C.c_int32, IP, FP]),
+        "po_render": (C.c_int32, [P, C.POINTER(CamDesc), C.c_int32, C.c_int32, C.c_uint64, C.c_int32, C.c_int32,
+                                  C.c_int32, C.c_int32, C.c_int32, C.c_int32, FP]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _libs["restatement"] = lib
+    return lib
+
+
+def restatement_available() -> bool:
+    return RESTATEMENT_LIB.exists()
+
+
+def restated_sobol(seed: int, px: int, py: int, index: int, n_dims: int) -> np.ndarray:
+    out = np.empty((n_dims, 2), np.float32)
+    _load_restatement().po_sobol(seed, px, py, index, n_dims, _f(out))
+    return out
+
+
+class Restatement:
+    """The C restatement holding a product Scene made of Lambert meshes (emissive or not)."""
+
+    def __init__(self, scene):
+        self.lib = _load_restatement()
+        self.h = self.lib.po_scene_create()
+        self.first_tri = []
+        n = 0
+        for kind, obj in scene.ops:
+            if kind != "mesh" or obj.material.struct.type != 0:
+                raise ValueError("the restatement covers Lambert meshes only")
+            m = obj.material.struct
+            alb = np.array(m.base_color[:], np.float32)
+            emi = np.array(m.emission[:], np.float32)
+            self.lib.po_scene_add_mesh(self.h, _f(obj.positions), obj.positions.shape[0],
+                                       obj.indices.ctypes.data_as(UP), obj.indices.shape[0], _f(alb), _f(emi))
+            self.first_tri.append(n)
+            n += obj.indices.shape[0]
+        self.first_tri = np.array(self.first_tri + [n])
+
+    def __del__(self):
+        try:
+            self.lib.po_scene_destroy(self.h)
+        except Exception:
+            pass
+
+    @staticmethod
+    def _cam(camera):
+        g = camera.describe_gpu()
+        c = CamDesc()
+        c.position[:] = g.position[:]
+        c.lower_left[:] = g.lower_left[:]
+        c.horizontal[:] = g.horizontal[:]
+        c.vertical[:] = g.vertical[:]
+        return c
+
+    def trace_primary(self, camera, settings, sample_index: int = 0):
+        """(shape, prim, t) per pixel, shapes numbered in insertion order like the device's."""
+        n = settings.width * settings.height
+        tri = np.empty(n, np.int32)
+        t = np.empty(n, np.float32)
+        self.lib.po_trace_primary(self.h, C.byref(self._cam(camera)), settings.width, settings.height, settings.seed,
+                                  sample_index, tri.ctypes.data_as(IP), _f(t))
+        shape = np.where(tri >= 0, np.searchsorted(self.first_tri, tri, side="right") - 1, -1).astype(np.int32)
+        prim = np.where(tri >= 0, tri - self.first_tri[np.maximum(shape, 0)], -1).astype(np.int32)
+        return shape, prim, t
+
+    def render(self, camera, settings, first: int, count: int, y0: int = 0, y1: int | None = None):
+        h, w = settings.height, settings.width
+        mean = np.zeros((h, w, 3), np.float32)
+        self.lib.po_render(self.h, C.byref(self._cam(camera)), w, h, settings.seed, settings.max_bounces,
+                           settings.rr_depth, first, count, y0, h if y1 is None else y1, _f(mean))
+        return mean

@@ -10,6 +10,7 @@
 #include <algorithm>
 #include <cstring>
 #include <string>
+#include <thread>
 #include <vector>
 
 using namespace pe;
@@ -65,6 +66,8 @@ struct pe_device {
     pe_render_stats stats{};
     int blocksIntersect = 0, blocksShade = 0, blocksShadow = 0, blocksGen = 0;
     unsigned char* noAllocBase = nullptr; // device address of g_noAllocScratch on this device
+    void* stage = nullptr;                 // pinned staging of the batch film (host-film render)
+    size_t stageBytes = 0;
     std::string noAllocError;
 };
 
@@ -523,6 +526,7 @@ void pe_device_destroy(pe_device* d) {
     cudaFree(d->dTables);
     cudaFree(d->dStats);
     if (d->hCounters) cudaFreeHost(d->hCounters);
+    if (d->stage) cudaFreeHost(d->stage);
     for (cudaEvent_t e : d->evPool) cudaEventDestroy(e);
     if (d->evStart) cudaEventDestroy(d->evStart);
     if (d->evT0) cudaEventDestroy(d->evT0);
@@ -698,20 +702,41 @@ int32_t pe_device_render(pe_device* d, const pe_camera* cam, const pe_settings* 
                                    true, Tile{0, 0, st->width, st->height});
     if (rr != PE_OK && rr != PE_ERR_CANCELLED) return rr;
     const size_t n = static_cast<size_t>(st->width) * static_cast<size_t>(st->height);
-    std::vector<float> s(n * 3), q(n);
-    std::vector<uint32_t> c(n);
-    if ((rc = pe_device_film_read(d, s.data(), c.data(), q.data()))) return rc;
-    uint64_t tr = 0;
-    for (size_t i = 0; i < n; ++i) {
-        tr += c[i];
-        if (sampleCount) sampleCount[i] += c[i];
-        if (sumRgb) {
-            sumRgb[3 * i + 0] += s[3 * i + 0];
-            sumRgb[3 * i + 1] += s[3 * i + 1];
-            sumRgb[3 * i + 2] += s[3 * i + 2];
-        }
-        if (sumLumSq) sumLumSq[i] += q[i];
+    // batch film → pinned staging (one DMA per array), then merged into the caller's film on all
+    // host cores, as Film::addBatch does per pixel
+    const size_t bytes = n * 5 * sizeof(float);
+    if (d->stageBytes < bytes) {
+        if (d->stage) cudaFreeHost(d->stage);
+        d->stage = nullptr;
+        d->stageBytes = 0;
+        PE_CUDA(cudaMallocHost(&d->stage, bytes));
+        d->stageBytes = bytes;
     }
+    float* s = reinterpret_cast<float*>(d->stage);
+    uint32_t* c = reinterpret_cast<uint32_t*>(s + 3 * n);
+    float* q = s + 4 * n;
+    if ((rc = pe_device_film_read(d, s, c, q))) return rc;
+    const unsigned hw = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+    const size_t chunk = (n + hw - 1) / hw;
+    std::vector<uint64_t> partial(hw, 0);
+    auto merge = [&](unsigned t) {
+        const size_t b = t * chunk, e = std::min(n, b + chunk);
+        uint64_t tr = 0;
+        for (size_t i = b; i < e; ++i) tr += c[i];
+        if (sampleCount)
+            for (size_t i = b; i < e; ++i) sampleCount[i] += c[i];
+        if (sumRgb)
+            for (size_t i = 3 * b; i < 3 * e; ++i) sumRgb[i] += s[i];
+        if (sumLumSq)
+            for (size_t i = b; i < e; ++i) sumLumSq[i] += q[i];
+        partial[t] = tr;
+    };
+    std::vector<std::thread> pool;
+    for (unsigned t = 1; t < hw; ++t) pool.emplace_back(merge, t);
+    merge(0);
+    for (auto& th : pool) th.join();
+    uint64_t tr = 0;
+    for (uint64_t p : partial) tr += p;
     if (traced) *traced = tr;
     return rr;
 }

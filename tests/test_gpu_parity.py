@@ -100,3 +100,38 @@ def test_knot_image_matches_reference_at_equal_spp(pe, device, knot):
     mean_ref, _ = ref.render(cam, st, 0, 4)
     err = pe.rel_mse(film.resolve(), mean_ref)
     assert err < 1e-3, err
+
+
+GOLDEN = __import__("pathlib").Path(__file__).resolve().parent / "golden"
+
+
+def test_cornell_matches_golden_fixture(pe, device):
+    """Against fixtures made from the reference CPU path (tests/golden/make_golden.py); needs no
+    reference at run time."""
+    g = np.load(GOLDEN / "cornell_32.npz")
+    scene, cam, st = scenes().cornell_box(32, 32, 8, 8, seed=0)
+    scene.build_accelerator()
+    device.set_scene(scene)
+    shape, prim, t = device.trace_primary(cam, st, 0)
+    assert np.array_equal(shape, g["shape"]) and np.array_equal(prim, g["prim"])
+    assert np.array_equal(t.view(np.uint32), g["t"].view(np.uint32))
+    film = pe.Film(st.width, st.height)
+    device.render(cam, st, pe.RenderTargets(beauty=film), 0, 8)
+    assert np.array_equal(film.count, g["count"])
+    assert pe.rel_mse(film.resolve(), g["mean"]) < 1e-8
+
+
+def test_cornell_matches_c_restatement(pe, device):
+    import oracle
+    if not oracle.restatement_available():
+        pytest.skip("oracle/_ref/libpe_oracle.so not built")
+    scene, cam, st = scenes().cornell_box(64, 64, 4, 8, seed=0)
+    scene.build_accelerator()
+    device.set_scene(scene)
+    res = oracle.Restatement(scene)
+    a = device.trace_primary(cam, st, 2)
+    b = res.trace_primary(cam, st, 2)
+    assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1])
+    film = pe.Film(st.width, st.height)
+    device.render(cam, st, pe.RenderTargets(beauty=film), 0, 4)
+    assert pe.rel_mse(film.resolve(), res.render(cam, st, 0, 4)) < 1e-8

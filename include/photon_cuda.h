@@ -38,7 +38,7 @@
 extern "C" {
 #endif
 
-#define PE_ABI_VERSION 1
+#define PE_ABI_VERSION 2
 
 typedef enum pe_status {
     PE_OK = 0,
@@ -200,6 +200,9 @@ typedef struct pe_render_stats {
     uint64_t kernel_launches;  /* kernels this library launched in the last render call */
     uint64_t shadow_node_visits; /* any-hit BVH node visits (counting enabled only) */
     uint64_t shadow_tri_tests;   /* any-hit triangle tests (counting enabled only) */
+    uint64_t tail_paths;       /* paths finished by the per-thread tail kernel */
+    float ms_tail;             /* device time in the tail kernel (timed renders only) */
+    uint32_t pad0;
 } pe_render_stats;
 
 const char* pe_last_error(void);
@@ -238,7 +241,7 @@ int32_t pe_device_film_clear(pe_device* d);
  * [first_sample, first_sample+count) of the pixels in the rectangle (x0, y0, w, h) are added to
  * them exactly as pe_device_render would add them; other pixels are not touched.
  *
- * The path state lives in one file-scope device array of 7.9 MB (room for 32768 paths), which
+ * The path state lives in one file-scope device array of 8.5 MB (room for 32768 paths), which
  * every GPU that loads this library holds until the process exits; its address on a device is
  * taken once, when the device is created.  A tile of more than 32768 pixels (w*h) is rejected
  * with PE_ERR_LIMIT.  Every call uses the same array and finds the previous call's contents in
@@ -252,6 +255,12 @@ int32_t pe_device_synchronize(pe_device* d);
 int32_t pe_device_last_stats(pe_device* d, pe_render_stats* out);
 /* 1 = count BVH node visits and triangle tests in traversal kernels (slower). */
 int32_t pe_device_set_counting(pe_device* d, int32_t enabled);
+/* B200 tuning knob with no counterpart in the reference engine.  A wave's paths are traced
+ * bounce by bounce (one closest-hit, shade and any-hit launch per bounce) until at most `paths`
+ * remain live; those finish in one launch that runs each path to its end on one thread.  The
+ * film is the same either way.  -1 (default) = the paths one resident grid holds, 0 = never. */
+int32_t pe_device_set_tail_paths(pe_device* d, int64_t paths);
+int64_t pe_device_tail_paths(pe_device* d);
 /* Device-stream timer: events recorded on the stream the kernels run on; end waits for the
  * stop event and returns the elapsed device milliseconds. */
 int32_t pe_device_timer_begin(pe_device* d);

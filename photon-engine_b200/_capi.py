@@ -72,7 +72,8 @@ class pe_render_stats(C.Structure):
                 ("ms_intersect", C.c_float), ("ms_shadow", C.c_float), ("ms_shade", C.c_float),
                 ("intersect_launches", C.c_uint64), ("node_visits", C.c_uint64), ("tri_tests", C.c_uint64),
                 ("error_flags", C.c_uint32), ("kernel_launches", C.c_uint64),
-                ("shadow_node_visits", C.c_uint64), ("shadow_tri_tests", C.c_uint64)]
+                ("shadow_node_visits", C.c_uint64), ("shadow_tri_tests", C.c_uint64),
+                ("tail_paths", C.c_uint64), ("ms_tail", C.c_float), ("pad0", C.c_uint32)]
 
 
 class pe_bsdf_query(C.Structure):
@@ -122,6 +123,8 @@ SIGNATURES = {
     "pe_device_synchronize": (C.c_int32, [P]),
     "pe_device_last_stats": (C.c_int32, [P, C.POINTER(pe_render_stats)]),
     "pe_device_set_counting": (C.c_int32, [P, C.c_int32]),
+    "pe_device_set_tail_paths": (C.c_int32, [P, C.c_int64]),
+    "pe_device_tail_paths": (C.c_int64, [P]),
     "pe_device_timer_begin": (C.c_int32, [P]),
     "pe_device_timer_end": (C.c_int32, [P, FP]),
     "pe_device_trace_primary": (C.c_int32, [P, C.POINTER(pe_camera), C.POINTER(pe_settings), C.c_int32, IP, IP, FP]),

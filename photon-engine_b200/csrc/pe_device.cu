@@ -51,7 +51,9 @@ struct pe_device {
     size_t capacity = 0;
     std::vector<DevBuf> pathBufs;
     Paths paths{};
-    unsigned long long* dStats = nullptr; // [0] nodes, [1] tris (closest), [2] nodes, [3] tris (any), [4] rejected
+    // [0] nodes, [1] tris (closest), [2] nodes, [3] tris (any), [4] rejected, [5] closest rays,
+    // [6] shadow rays (both of the tail kernel), [7] paths ended at the per-path query bound
+    unsigned long long* dStats = nullptr;
     uint32_t* hCounters = nullptr;        // pinned
     // resident film
     int filmW = 0, filmH = 0;
@@ -64,7 +66,8 @@ struct pe_device {
     std::vector<cudaEvent_t> evPool;
     bool counting = false;
     pe_render_stats stats{};
-    int blocksIntersect = 0, blocksShade = 0, blocksShadow = 0, blocksGen = 0;
+    int blocksIntersect = 0, blocksShade = 0, blocksShadow = 0, blocksGen = 0, blocksTail = 0;
+    int64_t tailPaths = -1; // -1: one resident grid of the tail kernel; 0: no tail kernel
     unsigned char* noAllocBase = nullptr; // device address of g_noAllocScratch on this device
     void* stage = nullptr;                 // pinned staging of the batch film (host-film render)
     size_t stageBytes = 0;
@@ -108,7 +111,7 @@ int32_t ensureCapacity(pe_device* d, size_t slots) {
     d->capacity = 0;
     Paths& P = d->paths;
     int32_t st = 0;
-    float4** cols[] = {&P.rayO, &P.rayD, &P.thr, &P.L, &P.lastN, &P.lastP, &P.pickP, &P.pickN, &P.hit};
+    float4** cols[] = {&P.rayO, &P.rayD, &P.thr, &P.L, &P.lastN, &P.lastP, &P.pickP, &P.pickN, &P.hit, &P.med};
     for (float4** c : cols)
         if ((st = devAlloc(d->pathBufs, *c, slots))) return st;
     if ((st = devAlloc(d->pathBufs, P.queueA, slots))) return st;
@@ -163,6 +166,10 @@ int32_t checkSettings(const pe_camera* cam, const pe_settings* st) {
         setError("film size out of range (1..16384)");
         return PE_ERR_INVALID;
     }
+    if (st->max_bounces < 0 || st->max_bounces > 255) {
+        setError("max_bounces out of range (0..255)");
+        return PE_ERR_LIMIT;
+    }
     if (st->shadow_quality < 1 || st->shadow_quality > 1) {
         setError("shadow_quality other than 1 is not supported by this device");
         return PE_ERR_LIMIT;
@@ -192,14 +199,16 @@ WaveArgs makeWave(const pe_camera* cam, const pe_settings* st) {
 }
 
 constexpr size_t kWaveSlots = size_t(1) << 21; // paths in flight per wave
+// Bound on the bounce-by-bounce iterations of one wave (closest-hit queries of its longest path).
+constexpr int kMaxWavefrontIterations = kMaxPathQueries;
 
 // Scratch of pe_device_render_tile_noalloc: path-state columns, queues, shadow records and
-// counters for kNoAllocSlots paths, carved out of one file-scope device array (7.9 MB).  Every
+// counters for kNoAllocSlots paths, carved out of one file-scope device array (8.5 MB).  Every
 // GPU that loads this library holds the array until the process exits.
 constexpr size_t kNoAllocSlots = size_t(1) << 15;
 constexpr size_t kNoAllocColumn = kNoAllocSlots * sizeof(float4);   // 512 KiB, 256-aligned
 constexpr size_t kNoAllocIndex = kNoAllocSlots * sizeof(int32_t);    // 128 KiB, 256-aligned
-constexpr size_t kNoAllocBytes = 13 * kNoAllocColumn + (3 + kShadeKeys) * kNoAllocIndex + 256;
+constexpr size_t kNoAllocBytes = 14 * kNoAllocColumn + (3 + kShadeKeys) * kNoAllocIndex + 256;
 static __device__ __align__(256) unsigned char g_noAllocScratch[kNoAllocBytes];
 
 // Path-state view of the scratch whose device address is `base`.
@@ -209,6 +218,7 @@ Paths noAllocPaths(unsigned char* base) {
     auto col = [&](float4*& c) { c = reinterpret_cast<float4*>(base + off); off += kNoAllocColumn; };
     auto idx = [&](int32_t*& c, size_t n) { c = reinterpret_cast<int32_t*>(base + off); off += n * kNoAllocIndex; };
     col(P.rayO); col(P.rayD); col(P.thr); col(P.L); col(P.lastN); col(P.lastP); col(P.pickP); col(P.pickN); col(P.hit);
+    col(P.med);
     col(P.shO); col(P.shD); col(P.shC); col(P.shT);
     idx(P.queueA, 1); idx(P.queueB, 1); idx(P.shadowQ, 1); idx(P.sortQ, kShadeKeys);
     P.counters = reinterpret_cast<uint32_t*>(base + off);
@@ -251,7 +261,7 @@ int32_t renderWaves(pe_device* d, const pe_camera* cam, const pe_settings* st, i
         e = d->evPool[evUsed++];
         return PE_OK;
     };
-    std::vector<std::pair<size_t, size_t>> isectEv, shadowEv, shadeEv;
+    std::vector<std::pair<size_t, size_t>> isectEv, shadowEv, shadeEv, tailEv;
     bool cancelled = false;
     for (int s0 = first; s0 < first + count && !cancelled; s0 += samplesPerWave) {
         const int ns = std::min(samplesPerWave, first + count - s0);
@@ -276,7 +286,28 @@ int32_t renderWaves(pe_device* d, const pe_camera* cam, const pe_settings* st, i
             uint32_t* cIn = &P.counters[0];
             uint32_t* cOut = &P.counters[1];
             stats.paths += static_cast<uint64_t>(nSlots);
+            const int64_t tailPaths = d->tailPaths < 0 ? static_cast<int64_t>(d->blocksTail) * 128 : d->tailPaths;
             for (int iter = 0; live > 0; ++iter) {
+                if (static_cast<int64_t>(live) <= tailPaths) {
+                    // the rest of the wave: one thread per path until it ends
+                    const int grid = static_cast<int>(std::min<int64_t>(d->blocksTail, (static_cast<int64_t>(live) + 127) / 128));
+                    cudaEvent_t t0 = nullptr, t1 = nullptr;
+                    if (timing) {
+                        if ((rc = event(t0)) || (rc = event(t1))) return rc;
+                        PE_CUDA(cudaEventRecord(t0, d->stream));
+                    }
+                    if (d->counting)
+                        kTail<true><<<grid, 128, 0, d->stream>>>(S, P, A, qIn, cIn, d->dStats);
+                    else
+                        kTail<false><<<grid, 128, 0, d->stream>>>(S, P, A, qIn, cIn, d->dStats);
+                    if (timing) {
+                        PE_CUDA(cudaEventRecord(t1, d->stream));
+                        tailEv.push_back({evUsed - 2, evUsed - 1});
+                    }
+                    ++stats.kernel_launches;
+                    stats.tail_paths += live;
+                    break;
+                }
                 stats.closest_rays += live;
                 cudaEvent_t e0 = nullptr, e1 = nullptr, e2 = nullptr, e3 = nullptr;
                 if (timing) {
@@ -306,8 +337,8 @@ int32_t renderWaves(pe_device* d, const pe_camera* cam, const pe_settings* st, i
                 PE_CUDA(cudaStreamSynchronize(d->stream));
                 stats.shadow_rays += d->hCounters[2];
                 live = cOut == &P.counters[1] ? d->hCounters[1] : d->hCounters[0];
-                if (iter > 4096) {
-                    setError("wavefront did not drain after 4096 iterations");
+                if (iter > kMaxWavefrontIterations) {
+                    setError("wavefront did not drain after " + std::to_string(kMaxWavefrontIterations) + " iterations");
                     return PE_ERR_DEVICE;
                 }
                 // swap queues; reset the consumed queue's counter, the shadow counter, the work
@@ -346,11 +377,22 @@ int32_t renderWaves(pe_device* d, const pe_camera* cam, const pe_settings* st, i
         cudaEventElapsedTime(&t, d->evPool[pr.first], d->evPool[pr.second]);
         stats.ms_shadow += t;
     }
+    for (auto& pr : tailEv) {
+        float t = 0.0f;
+        cudaEventElapsedTime(&t, d->evPool[pr.first], d->evPool[pr.second]);
+        stats.ms_tail += t;
+    }
     stats.node_visits = hs[0];
     stats.tri_tests = hs[1];
     stats.shadow_node_visits = hs[2];
     stats.shadow_tri_tests = hs[3];
     stats.rejected = hs[4];
+    stats.closest_rays += hs[5];
+    stats.shadow_rays += hs[6];
+    if (hs[7] != 0) {
+        setError(std::to_string(hs[7]) + " paths exceeded the per-path query bound and were ended");
+        return PE_ERR_DEVICE;
+    }
     if (cancelled) {
         setError("render cancelled");
         return PE_ERR_CANCELLED;
@@ -498,6 +540,8 @@ pe_device* pe_device_create(int32_t ordinal, char* err, size_t errLen) {
     d->blocksShade = sm * std::max(1, b);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kShadow<false>, 128, 0);
     d->blocksShadow = sm * std::max(1, b);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kTail<true>, 128, 0);
+    d->blocksTail = sm * std::max(1, b);
     const cudaError_t le = cudaGetLastError();
     if (le != cudaSuccess) {
         pe_device_destroy(d);
@@ -620,6 +664,8 @@ int32_t pe_device_set_scene(pe_device* d, const pe_scene* s) {
     for (int i = 0; i < 3; ++i) G.bgColor[i] = s->bgColor[i];
     G.hasShadowTransmitters = B.hasShadowTransmitters ? 1 : 0;
     G.hasVolumes = B.hasVolumes ? 1 : 0;
+    G.hasSubsurface = B.hasSubsurface ? 1 : 0;
+    G.exitMaterial = B.exitMaterial;
     PE_CUDA(cudaStreamSynchronize(d->stream));
     d->scene = G;
     d->hasScene = true;
@@ -795,6 +841,24 @@ int32_t pe_device_last_stats(pe_device* d, pe_render_stats* out) {
     }
     *out = d->stats;
     return PE_OK;
+}
+
+int32_t pe_device_set_tail_paths(pe_device* d, int64_t paths) {
+    if (!d) {
+        setError("null device");
+        return PE_ERR_INVALID;
+    }
+    if (paths < -1) {
+        setError("tail paths must be -1 (automatic), 0 (off) or a path count");
+        return PE_ERR_INVALID;
+    }
+    d->tailPaths = paths;
+    return PE_OK;
+}
+
+int64_t pe_device_tail_paths(pe_device* d) {
+    if (!d) return -1;
+    return d->tailPaths < 0 ? static_cast<int64_t>(d->blocksTail) * 128 : d->tailPaths;
 }
 
 int32_t pe_device_set_counting(pe_device* d, int32_t enabled) {

@@ -15,6 +15,7 @@
 #include "pe_host.h"
 #include "pe_bsdf.h"
 #include "pe_light.h"
+#include "pe_medium.h"
 
 #include <algorithm>
 #include <cmath>
@@ -686,28 +687,14 @@ void buildGgxTables(TablesGPU& T) {
     }
 }
 
-// Wyman–Sloan–Shirley 2013 CIE fit → linear sRGB (spectral.cpp:15-31).
-float gpiece(float x, float mu, float s1, float s2) {
-    const float t = (x - mu) / (x < mu ? s1 : s2);
-    return std::exp(-0.5f * t * t);
-}
-V3 rawRGB(float l) {
-    const float X = 1.056f * gpiece(l, 599.8f, 37.9f, 31.0f) + 0.362f * gpiece(l, 442.0f, 16.0f, 26.7f) -
-                    0.065f * gpiece(l, 501.1f, 20.4f, 26.2f);
-    const float Y = 0.821f * gpiece(l, 568.8f, 46.9f, 40.5f) + 0.286f * gpiece(l, 530.9f, 16.3f, 31.1f);
-    const float Z = 1.217f * gpiece(l, 437.0f, 11.8f, 36.0f) + 0.681f * gpiece(l, 459.0f, 26.0f, 13.8f);
-    const float r = 3.2404542f * X - 1.5371385f * Y - 0.4985314f * Z;
-    const float gg = -0.9692660f * X + 1.8760108f * Y + 0.0415560f * Z;
-    const float b = 0.0556434f * X - 0.2040259f * Y + 1.0572252f * Z;
-    return mk(smax(0.0f, r), smax(0.0f, gg), smax(0.0f, b));
-}
+// Wavelength tables of sampleWavelength (spectral.cpp:33-62).
 void buildSpectral(TablesGPU& T) {
     const float lmin = 380.0f, lmax = 730.0f;
     constexpr int kBins = 350;
     V3 sum = mk(0.0f);
     constexpr int kSteps = 3500;
     const float dl = (lmax - lmin) / static_cast<float>(kSteps);
-    for (int i = 0; i < kSteps; ++i) sum += rawRGB(lmin + (static_cast<float>(i) + 0.5f) * dl);
+    for (int i = 0; i < kSteps; ++i) sum += spectralRaw(lmin + (static_cast<float>(i) + 0.5f) * dl);
     const V3 mean = sum / static_cast<float>(kSteps);
     const V3 norm = mk(1.0f / mean.x, 1.0f / mean.y, 1.0f / mean.z);
     const float bw = (lmax - lmin) / static_cast<float>(kBins);
@@ -715,7 +702,7 @@ void buildSpectral(TablesGPU& T) {
     T.spectralCdf[0] = 0.0f;
     float s[kBins];
     for (int i = 0; i < kBins; ++i) {
-        const V3 c = rawRGB(lmin + (static_cast<float>(i) + 0.5f) * bw) * norm;
+        const V3 c = spectralRaw(lmin + (static_cast<float>(i) + 0.5f) * bw) * norm;
         s[i] = c.x + c.y + c.z + 0.02f;
         acc += s[i];
         T.spectralCdf[i + 1] = acc;
@@ -785,6 +772,19 @@ static int32_t buildScene(pe_scene* s) {
     HostBuild& B = s->build;
     B = HostBuild{};
     B.materials = s->materials;
+    if (B.materials.size() >= 0xFFFFu) {
+        setError("scene has " + std::to_string(B.materials.size()) + " materials; at most 65534 are supported");
+        return PE_ERR_LIMIT;
+    }
+    // Exit vertex of a random-walk subsurface path: a white Lambert surface whose normal faces
+    // out of the object (path_tracer.cpp:56-59, 757-761); appended after the scene's materials.
+    {
+        pe_material wl;
+        pe_material_defaults(PE_MAT_LAMBERT, &wl);
+        wl.base_color[0] = wl.base_color[1] = wl.base_color[2] = 1.0f;
+        B.exitMaterial = static_cast<int32_t>(B.materials.size());
+        B.materials.push_back(resolveMaterial(wl));
+    }
     // shapes and global triangle / vertex numbering
     uint32_t nTris = 0, nVerts = 0;
     for (const HostShape& sh : s->shapes) {
@@ -841,8 +841,11 @@ static int32_t buildScene(pe_scene* s) {
     }
     for (const MatGPU& m : s->materials)
         if (m.flags & MF_TRANSMITS_SHADOWS) B.hasShadowTransmitters = true; // Scene::retainMaterial
-    for (const MatGPU& m : s->materials)
+    for (const MatGPU& m : s->materials) {
         if (m.flags & (MF_VOLUME_BOUNDARY)) B.hasVolumes = true;
+        if (m.type == PE_MAT_DISNEY && m.subsurface > 0.0f) B.hasSubsurface = true;
+        if (m.flags & MF_DISPERSIVE) B.hasDispersion = true;
+    }
 
     // SAH BVH
     if (nTris > 0) {

@@ -64,6 +64,9 @@ struct HostBuild {
     int maxDepth = 0;
     bool hasShadowTransmitters = false;
     bool hasVolumes = false;
+    bool hasSubsurface = false;
+    bool hasDispersion = false;
+    int32_t exitMaterial = -1;   // white Lambert of the subsurface exit vertex
 };
 
 } // namespace pe

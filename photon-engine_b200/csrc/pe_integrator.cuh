@@ -12,11 +12,22 @@
 
 #include "pe_bsdf.h"
 #include "pe_light.h"
+#include "pe_medium.h"
 #include "pe_trace.cuh"
 
 namespace pe {
 
-enum VisMask : uint32_t { VIS_CAMERA = 1u, VIS_DIFFUSE = 2u, VIS_GLOSSY = 4u, VIS_TRANSMISSION = 8u, VIS_SHADOW = 16u };
+enum VisMask : uint32_t { VIS_CAMERA = 1u, VIS_DIFFUSE = 2u, VIS_GLOSSY = 4u, VIS_TRANSMISSION = 8u, VIS_SHADOW = 16u,
+                          VIS_ALL = 0x1Fu };
+// Marks a random-walk ray in the ray's mask word.  Triangle masks never carry it, so it does
+// not change what the ray can hit; the closest-hit kernel bins such rays under their own key.
+constexpr uint32_t RAY_WALK = 1u << 31;
+constexpr int kMaxMediumEvents = 1024; // path_tracer.cpp:51
+constexpr int kMaxWalkSteps = 256;     // path_tracer.cpp:52
+// Closest-hit queries one path can make: at most 255 bounces, each preceded by up to 64 skipped
+// camera-invisible hits and 65 pass-throughs and followed by up to 256 walk steps, plus 1025
+// medium events, stays below this; a path that reaches it is counted as an error and ended.
+constexpr int kMaxPathQueries = 1 << 17;
 
 // path flags (bits of state word)
 enum PathFlags : uint32_t {
@@ -24,6 +35,7 @@ enum PathFlags : uint32_t {
     PF_CAMERA_RAY = 1u << 1,
     PF_PICKER_VALID = 1u << 2,
     PF_FIRST_SEGMENT = 1u << 3,
+    PF_WALK = 1u << 4,   // inside a random walk: lastP = σt, lastN = albedo, pickP.x = g
 };
 
 // Per-slot state columns (capacity P slots).
@@ -37,6 +49,7 @@ struct Paths {
     float4* pickP;   // light-picker point xyz, pixel hash (bits)
     float4* pickN;   // light-picker normal xyz, counters (bits: depth | diffuseBounces<<8 | passThroughs<<16 | skips<<24)
     float4* hit;     // t, u, v, leaf prim (bits)
+    float4* med;     // media stack slots 0,1 | slots 2,3 (bits), mediumEvents | walkStep<<16, stack depth
     int32_t* queueA;
     int32_t* queueB;
     int32_t* shadowQ;
@@ -47,14 +60,15 @@ struct Paths {
     int32_t* sortQ;  // kShadeKeys segments of `capacity` slots: rays binned by shading key
     uint32_t capacity;
     // [0] queue A count, [1] queue B count, [2] shadow count, [3] closest-hit work cursor,
-    // [4] any-hit work cursor, [5] shade work cursor, [6..10] rays per shading key, [11] errors
+    // [4] any-hit work cursor, [5] shade work cursor, [6..11] rays per shading key, [12] errors,
+    // [13] tail work cursor
     uint32_t* counters;
 };
 
-// Shading keys: 0 = miss, 1 + material type (Lambert, Disney, Dielectric, Mirror).
-constexpr int kShadeKeys = 5;
+// Shading keys: 0 = miss, 1 + material type (Lambert, Disney, Dielectric, Mirror), 5 = random-walk step.
+constexpr int kShadeKeys = 6;
 enum CounterSlots { CNT_QA = 0, CNT_QB = 1, CNT_SHADOW = 2, CNT_WORK_ISECT = 3, CNT_WORK_SHADOW = 4,
-                    CNT_WORK_SHADE = 5, CNT_KEYS = 6, CNT_ERRORS = 11, CNT_TOTAL = 16 };
+                    CNT_WORK_SHADE = 5, CNT_KEYS = 6, CNT_ERRORS = 12, CNT_WORK_TAIL = 13, CNT_TOTAL = 16 };
 
 // Persistent-warp work distribution: lane 0 claims the next 32 items for its warp.
 __device__ __forceinline__ int warpFetch(uint32_t* cursor) {
@@ -114,6 +128,7 @@ __global__ void kGenerate(SceneGPU S, Paths P, WaveArgs A, int nSlots) {
         P.lastP[slot] = make_float4(o.x, o.y, o.z, __uint_as_float(sb.dim));
         P.pickP[slot] = make_float4(0.0f, 0.0f, 0.0f, __uint_as_float(sb.pixelHash));
         P.pickN[slot] = make_float4(0.0f, 0.0f, 0.0f, __uint_as_float(packCounters(0, 0, 0, 0)));
+        if (S.hasVolumes | S.hasSubsurface) P.med[slot] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
         P.queueA[slot] = slot;
     }
 }
@@ -139,7 +154,8 @@ __global__ void __launch_bounds__(128) kIntersect(SceneGPU S, Paths P, const int
             const Hit h = traceClosest<COUNT>(S, mk(ro.x, ro.y, ro.z), mk(rd.x, rd.y, rd.z), __float_as_uint(ro.w), 0.0f,
                                               1e30f, nodes, tris);
             P.hit[slot] = make_float4(h.t, h.u, h.v, __int_as_float(h.prim));
-            key = h.prim < 0 ? 0 : 1 + static_cast<int>((h.meta >> 8) & 0xFFu);
+            key = (__float_as_uint(ro.w) & RAY_WALK) ? kShadeKeys - 1
+                  : (h.prim < 0 ? 0 : 1 + static_cast<int>((h.meta >> 8) & 0xFFu));
         }
         // warp-aggregated append into the key's segment: one atomic per distinct key per warp
         const unsigned peers = __match_any_sync(0xffffffffu, key);
@@ -156,6 +172,18 @@ __global__ void __launch_bounds__(128) kIntersect(SceneGPU S, Paths P, const int
         atomicAdd(&stats[0], static_cast<unsigned long long>(nodes));
         atomicAdd(&stats[1], static_cast<unsigned long long>(tris));
     }
+}
+
+// An unoccluded NEE sample's term: throughput × f·Li·vis·(cos·w / (lightPdf·n)) with vis = 1,
+// clamped when indirect (path_tracer.cpp:683-690).
+__device__ __forceinline__ V3 neeTerm(V3 fLi, float scalar, V3 thr, bool indirect, float clampIndirect) {
+    const V3 neeLocal = (fLi * mk(1.0f)) * scalar;
+    V3 c = thr * neeLocal;
+    if (indirect && clampIndirect > 0.0f) {
+        const float m = smax3(c.x, c.y, c.z);
+        if (m > clampIndirect) c = c * (clampIndirect / m);
+    }
+    return c;
 }
 
 // ---- any hit over the shadow queue ------------------------------------------------------------
@@ -176,13 +204,7 @@ __global__ void __launch_bounds__(128) kShadow(SceneGPU S, Paths P, const uint32
         if (occluded) continue;
         const float4 sc = P.shC[i];
         const float4 st = P.shT[i];
-        // neeLocal = f * Li * vis * (cos * w / (lightPdf * n)), vis = 1 on this path
-        const V3 neeLocal = (mk(sc.x, sc.y, sc.z) * mk(1.0f)) * sd.w;
-        V3 c = mk(st.x, st.y, st.z) * neeLocal;
-        if ((__float_as_uint(sc.w) & 1u) && clampIndirect > 0.0f) {
-            const float m = smax3(c.x, c.y, c.z);
-            if (m > clampIndirect) c = c * (clampIndirect / m);
-        }
+        const V3 c = neeTerm(mk(sc.x, sc.y, sc.z), sd.w, mk(st.x, st.y, st.z), (__float_as_uint(sc.w) & 1u) != 0, clampIndirect);
         if (!isFinite3(c)) continue;
         float4 L = P.L[slot];
         L.x += c.x;
@@ -203,11 +225,410 @@ __device__ __forceinline__ void addL(float4& L, V3 c) {
     L.z += c.z;
 }
 
+// russianRoulette (path_tracer.cpp:131-137): false ends the path.
+__device__ __forceinline__ bool russianRoulette(V3& thr, Sobol& sb) {
+    const float m = smax3(thr.x, thr.y, thr.z);
+    if (m >= 1.0f) return true;
+    if (!(m > 0.0f) || get1D(sb) >= m) return false;
+    thr /= m;
+    return true;
+}
+
+enum SegmentOutcome { SEG_SURFACE = 0, SEG_SCATTERED = 1, SEG_END = 2 };
+
+// Absorption and scattering over the segment a path just travelled inside the medium of the
+// innermost volume boundary it entered (path_tracer.cpp:456-479).  SEG_SCATTERED sets up the
+// next ray (origin newO, direction newD).
+__device__ __noinline__ int mediumSegment(const TablesGPU* T, const MatGPU& mm, V3 segStart, V3 dir, bool hit, V3 hitPoint,
+                                          Sobol& sb, V3& thr, uint32_t& volCtr, V3& newO, V3& newD) {
+    const float dirLen = length(dir);
+    const float segment = hit ? length(hitPoint - segStart) : kFltMax;
+    const V3 sA = m3f(mm.sigmaA), sS = m3f(mm.sigmaS);
+    if (mm.flags & MF_MEDIUM_SCATTERS) {
+        const float uc = get1D(sb);
+        const float u = get1D(sb);
+        float t = 0.0f;
+        if (sampleFreeFlight(sA + sS, sS, segment, hit, thr, uc, u, thr, t)) {
+            const uint32_t events = (volCtr & 0xFFFFu) + 1u;
+            volCtr = (volCtr & 0xFFFF0000u) | events;
+            if (events > static_cast<uint32_t>(kMaxMediumEvents) || !isFinite3(thr)) return SEG_END;
+            const V3 d = dir / dirLen;
+            newO = segStart + d * t;
+            newD = sampleHG(d, mm.mediumG, get2D(T, sb));
+            if (events > 8u && !russianRoulette(thr, sb)) return SEG_END;
+            return SEG_SCATTERED;
+        }
+    } else if (hit) {
+        thr *= expNeg(sA, segment);
+    } else if (!isBlack(sA)) {
+        return SEG_END; // open mesh: an infinitely long absorbing segment
+    }
+    if (isBlack(thr) || !isFinite3(thr)) return SEG_END;
+    return SEG_SURFACE;
+}
+
 // ---- shade: Li's loop body between two closest-hit queries ------------------------------------
+// One path's step: reads the slot's state and hit record, adds the radiance found to L and
+// writes back the state for its next closest-hit query.  A path is in one of three states at
+// each query: an ordinary ray (medium segment, then the surface or the sky), a step of a random
+// subsurface walk (PF_WALK), whose exit point is shaded at once as the walk's white-Lambert exit
+// vertex, or a ray scattered inside a medium (an ordinary ray with specularBounce set).  NEE
+// shadow rays go to the any-hit queue, or with INLINE_SHADOW are traced here and their terms
+// added to L at once, in the same order.  Returns whether the path goes on.
+template <bool INLINE_SHADOW, bool COUNT>
+__device__ __forceinline__ bool shadeSlot(const SceneGPU& S, const Paths& P, const WaveArgs& A, int slot,
+                                          uint32_t& shNodes, uint32_t& shTris, uint32_t& shRays) {
+    const TablesGPU* T = S.tables;
+    const bool volumetric = (S.hasVolumes | S.hasSubsurface) != 0;
+    bool cont = false;
+    float4 ro = P.rayO[slot];
+    float4 rd = P.rayD[slot];
+    float4 th = P.thr[slot];
+    float4 L = P.L[slot];
+    float4 ln = P.lastN[slot];
+    float4 lp = P.lastP[slot];
+    float4 pp = P.pickP[slot];
+    float4 pn = P.pickN[slot];
+    const float4 hr = P.hit[slot];
+    float4 md = volumetric ? P.med[slot] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    MediaStack media;
+    media.lo = __float_as_uint(md.x);
+    media.hi = __float_as_uint(md.y);
+    media.n = __float_as_int(md.w);
+    uint32_t volCtr = __float_as_uint(md.z);
+    float lambda = th.w; // 0 = RGB path; > 0 = single-wavelength path after a dispersive hit
+    uint32_t flags = __float_as_uint(ln.w);
+    uint32_t ctr = __float_as_uint(pn.w);
+    int depth = ctr & 0xFF, diffuseBounces = (ctr >> 8) & 0xFF, passThroughs = (ctr >> 16) & 0xFF,
+        skips = (ctr >> 24) & 0xFF;
+    Sobol sb;
+    sb.pixelHash = __float_as_uint(pp.w);
+    {
+        const int sOff = slot / A.nPix;
+        sb.revIndex = rev32(static_cast<uint32_t>(A.sampleFirst + sOff));
+    }
+    sb.dim = __float_as_uint(lp.w);
+    V3 thr = mk(th.x, th.y, th.z);
+    const V3 dir = mk(rd.x, rd.y, rd.z);
+    const V3 rayO = mk(ro.x, ro.y, ro.z);
+    const float lastBsdfPdf = rd.w;
+    const bool specularBounce = flags & PF_SPECULAR_BOUNCE;
+    bool cameraRay = flags & PF_CAMERA_RAY;
+    const int shadowSamples = A.shadowSamples;
+    const int explicitLights = S.nLights;
+    const int prim = __float_as_int(hr.w);
+    const bool hit = prim >= 0;
+    Isect is;
+    bool done = false;
+    bool vertex = false; // a surface vertex to shade (NEE + BSDF sampling) below
+    V3 wo = -dir;
+    if (flags & PF_WALK) {
+        // one step of the random walk (path_tracer.cpp:263-303)
+        const V3 sigT = mk(lp.x, lp.y, lp.z), alb = mk(ln.x, ln.y, ln.z);
+        const V3 sigS = alb * sigT;
+        uint32_t step = volCtr >> 16;
+        const float uc = get1D(sb);
+        const float uf = get1D(sb);
+        float t = 0.0f;
+        const bool scattered = sampleFreeFlight(sigT, sigS, hit ? hr.x : kFltMax, hit, thr * alb, uc, uf, thr, t);
+        if (!isFinite3(thr) || isBlack(thr)) {
+            done = true;
+        } else if (!scattered) {
+            if (!hit) {
+                done = true; // escaped through open geometry
+            } else {
+                Hit h;
+                h.t = hr.x;
+                h.u = hr.y;
+                h.v = hr.z;
+                h.prim = prim;
+                fillHit(S, h, dir, is);
+                // exit vertex: outward normal, white Lambert; the depth does not grow
+                is.normal = -is.normal;
+                is.material = S.exitMaterial;
+                flags &= ~PF_WALK;
+                wo = is.normal;
+                if (depth >= A.maxDepth) done = true;
+                else vertex = true;
+            }
+        } else {
+            const V3 no = rayO + dir * t;
+            const V3 nd = sampleHG(dir, pp.x, get2D(T, sb));
+            if ((step >= 8u && !russianRoulette(thr, sb)) || ++step >= static_cast<uint32_t>(kMaxWalkSteps)) {
+                done = true;
+            } else {
+                ro = make_float4(no.x, no.y, no.z, ro.w);
+                rd = make_float4(nd.x, nd.y, nd.z, rd.w);
+                volCtr = (volCtr & 0xFFFFu) | (step << 16);
+                cont = true;
+            }
+        }
+    } else {
+        if (hit) {
+            Hit h;
+            h.t = hr.x;
+            h.u = hr.y;
+            h.v = hr.z;
+            h.prim = prim;
+            fillHit(S, h, dir, is);
+            // Camera-invisible light quads are passed through by camera rays; the vertex
+            // does not count (path_tracer.cpp:426-439).  Cutouts are not supported here.
+            if (cameraRay && (S.shapes[is.shape].flags & SF_CAMERA_INVISIBLE) && skips < 64) {
+                const V3 no = offsetRayOrigin(is.point, is.pError, is.ng, dir);
+                ro = make_float4(no.x, no.y, no.z, ro.w);
+                ++skips;
+                cont = true;
+                done = true;
+            }
+        }
+        if (!done) {
+            flags &= ~PF_FIRST_SEGMENT;
+            // inside an object: absorption and, when the medium scatters, free flight
+            const int top = volumetric ? media.top() : -1;
+            if (top >= 0 && (S.materials[top].flags & MF_HAS_MEDIUM)) {
+                V3 no, nd;
+                const int r = mediumSegment(T, S.materials[top], rayO, dir, hit, is.point, sb, thr, volCtr, no, nd);
+                if (r == SEG_END) {
+                    done = true;
+                } else if (r == SEG_SCATTERED) {
+                    // the next query starts at the scattering point; no NEE inside, so
+                    // emission found next takes full weight
+                    ro = make_float4(no.x, no.y, no.z, __uint_as_float(VIS_DIFFUSE));
+                    rd = make_float4(nd.x, nd.y, nd.z, rd.w);
+                    flags = (flags | PF_SPECULAR_BOUNCE) & ~PF_CAMERA_RAY;
+                    cont = true;
+                    done = true;
+                }
+            }
+        }
+        if (!done) {
+            if (!hit) {
+                // environment / background (path_tracer.cpp:482-514)
+                if (depth == 0 && S.bgMode != PE_BG_ENVIRONMENT) {
+                    if (S.bgMode == PE_BG_COLOR) addL(L, thr * m3f(S.bgColor));
+                } else if (S.env.present) {
+                    const V3 Le = envEval(S.env, dir);
+                    float weight = 1.0f;
+                    if (!specularBounce) {
+                        float pmf = 0.0f;
+                        if (flags & PF_PICKER_VALID) {
+                            LightCtx c;
+                            lightPrepare(S, mk(pp.x, pp.y, pp.z), mk(pn.x, pn.y, pn.z), c);
+                            pmf = lightCtxPmf(S, c, explicitLights);
+                        }
+                        const float lightPdf = pmf * envPdf(S.env, dir);
+                        weight = powerHeuristic(1, lastBsdfPdf, shadowSamples, lightPdf);
+                    }
+                    V3 c = thr * (Le * weight);
+                    if (diffuseBounces >= 2 && A.clampIndirect > 0.0f) {
+                        const float m = smax3(c.x, c.y, c.z);
+                        if (m > A.clampIndirect) c = c * (A.clampIndirect / m);
+                    }
+                    addL(L, c);
+                }
+                done = true;
+            } else {
+                const MatGPU& mat = S.materials[is.material];
+                // emission with MIS against the previous vertex's NEE (path_tracer.cpp:565-593)
+                if (mat.flags & MF_EMISSIVE) {
+                    const ShapeInfo& sh = S.shapes[is.shape];
+                    int li = -1;
+                    if (sh.emitter >= 0)
+                        li = (sh.flags & SF_AREA_TRIANGLE) ? sh.emitter : sh.emitter + (is.tri - static_cast<int>(sh.firstTri));
+                    float weight = 1.0f;
+                    if (!specularBounce) {
+                        float lightPdf = 0.0f;
+                        if (li >= 0) {
+                            float pmf = 0.0f;
+                            if (flags & PF_PICKER_VALID) {
+                                LightCtx c;
+                                lightPrepare(S, mk(pp.x, pp.y, pp.z), mk(pn.x, pn.y, pn.z), c);
+                                pmf = lightCtxPmf(S, c, li);
+                            }
+                            lightPdf = pmf * lightPdfHit(S.lights[li], mk(lp.x, lp.y, lp.z), is.point);
+                        }
+                        if (lightPdf > 0.0f && lastBsdfPdf > 0.0f)
+                            weight = powerHeuristic(1, lastBsdfPdf, shadowSamples, lightPdf);
+                    }
+                    V3 c = thr * (m3f(mat.emission) * weight);
+                    if (diffuseBounces >= 2 && A.clampIndirect > 0.0f) {
+                        const float m = smax3(c.x, c.y, c.z);
+                        if (m > A.clampIndirect) c = c * (A.clampIndirect / m);
+                    }
+                    addL(L, c);
+                }
+                if (depth >= A.maxDepth) done = true;
+                else vertex = true;
+            }
+        }
+    }
+    if (vertex) {
+        const MatGPU& mat = S.materials[is.material];
+        // dispersion: the first wavelength-dependent surface fixes one λ for the path
+        if (lambda == 0.0f && (mat.flags & MF_DISPERSIVE)) {
+            V3 w;
+            lambda = sampleWavelength(T, get1D(sb), w);
+            thr *= w;
+        }
+        ShadePoint sp;
+        sp.p = is.point;
+        sp.n = is.normal;
+        sp.ng = is.ng;
+        sp.tangent = is.tangent;
+        sp.frontFace = is.frontFace;
+        sp.wavelength = lambda;
+        const bool isSpecular = (mat.flags & MF_DELTA) != 0;
+        // next-event estimation (path_tracer.cpp:631-698)
+        if (S.lightCount > 0 && !isSpecular) {
+            LightCtx picker;
+            lightPrepare(S, is.point, is.normal, picker);
+            flags |= PF_PICKER_VALID;
+            pp = make_float4(is.point.x, is.point.y, is.point.z, pp.w);
+            pn.x = is.normal.x;
+            pn.y = is.normal.y;
+            pn.z = is.normal.z;
+            for (int s = 0; s < shadowSamples; ++s) {
+                float lightPmf = 0.0f;
+                const int lightIndex = lightCtxSample(S, picker, get1D(sb), lightPmf);
+                if (lightIndex < 0 || !(lightPmf > 0.0f)) {
+                    (void)get2D(T, sb);
+                    continue;
+                }
+                const bool fromEnv = lightIndex >= explicitLights;
+                const V2 ul = get2D(T, sb);
+                const LightSample ls = fromEnv ? envSample(S.env, ul) : sampleLight(S.lights[lightIndex], is.point, ul);
+                if (!lsValid(ls)) continue;
+                V3 so, sd;
+                float stMax;
+                if (!makeShadowRay(is, ls.wi, ls.distance, so, sd, stMax)) continue;
+                float bsdfPdf = 0.0f;
+                const V3 f = bsdfEvalPdf(T, mat, wo, ls.wi, sp, bsdfPdf, nullptr);
+                const float cosTheta = fabsf(dot(ls.wi, is.normal));
+                if (isBlack(f) || !(cosTheta > 0.0f)) continue;
+                const float lightPdf = lightPmf * ls.pdf;
+                const float weight = powerHeuristic(shadowSamples, lightPdf, 1, bsdfPdf);
+                const float scalar = cosTheta * weight / (lightPdf * static_cast<float>(shadowSamples));
+                const V3 fLi = f * ls.Li;
+                if (INLINE_SHADOW) {
+                    // the any-hit query now; its term follows this vertex's emission in L
+                    ++shRays;
+                    if (!traceAny<COUNT>(S, so, sd, VIS_SHADOW, 0.0f, stMax, shNodes, shTris)) {
+                        const V3 c = neeTerm(fLi, scalar, thr, diffuseBounces >= 1, A.clampIndirect);
+                        if (isFinite3(c)) {
+                            L.x += c.x;
+                            L.y += c.y;
+                            L.z += c.z;
+                        }
+                    }
+                } else {
+                    // shadow queue append (one record per sample)
+                    const uint32_t pos = atomicAdd(&P.counters[CNT_SHADOW], 1u);
+                    P.shadowQ[pos] = slot;
+                    P.shO[pos] = make_float4(so.x, so.y, so.z, stMax);
+                    P.shD[pos] = make_float4(sd.x, sd.y, sd.z, scalar);
+                    P.shC[pos] = make_float4(fLi.x, fLi.y, fLi.z, __uint_as_float(diffuseBounces >= 1 ? 1u : 0u));
+                    P.shT[pos] = make_float4(thr.x, thr.y, thr.z, 0.0f);
+                }
+            }
+        }
+        // BSDF sampling (path_tracer.cpp:700-743)
+        const float uc = get1D(sb);
+        const V2 u2 = get2D(T, sb);
+        BsdfSample bs;
+        const bool sampled = bsdfSample(T, mat, wo, sp, uc, u2, bs);
+        if (!sampled) {
+            done = true;
+        } else if (bs.subsurface) {
+            // random-walk entry (path_tracer.cpp:745-761): the walk's coefficients ride
+            // in the columns it does not need (lastP, lastN, pickP.x)
+            V3 sigT, alb;
+            float g = 0.0f;
+            const DisneyParams dp = disneyResolve(mat, sp);
+            if (!disneySubsurfaceCoeffs(mat, dp, sigT, alb, g)) {
+                done = true;
+            } else {
+                thr *= bs.weight;
+                const V3 d = normalize(bs.wi);
+                const V3 no = spawnOrigin(is, d);
+                ro = make_float4(no.x, no.y, no.z, __uint_as_float(VIS_ALL | RAY_WALK));
+                rd = make_float4(d.x, d.y, d.z, rd.w);
+                lp = make_float4(sigT.x, sigT.y, sigT.z, 0.0f);
+                ln = make_float4(alb.x, alb.y, alb.z, 0.0f);
+                pp.x = g;
+                volCtr &= 0xFFFFu; // walk step 0
+                flags = (flags | PF_WALK) & ~PF_CAMERA_RAY;
+                cont = true;
+            }
+        } else if (bs.pdf <= 0.0f || isBlack(bs.f)) {
+            done = true;
+        } else if (bs.passThrough) {
+            thr *= bs.f * (fabsf(dot(bs.wi, is.normal)) / bs.pdf);
+            if (!isFinite3(thr) || ++passThroughs > 64) {
+                done = true;
+            } else {
+                const V3 no = spawnOrigin(is, bs.wi);
+                ro = make_float4(no.x, no.y, no.z, ro.w);
+                rd = make_float4(bs.wi.x, bs.wi.y, bs.wi.z, rd.w);
+                skips = 0;
+                cont = true;
+            }
+        } else {
+            const V3 wi = bs.wi;
+            const bool refracted = dot(wo, is.ng) * dot(wi, is.ng) < 0.0f;
+            const float cosTheta = fabsf(dot(wi, is.normal));
+            thr *= bs.f * (cosTheta / bs.pdf);
+            if (!isFinite3(thr)) {
+                done = true;
+            } else {
+                flags = bs.delta ? (flags | PF_SPECULAR_BOUNCE) : (flags & ~PF_SPECULAR_BOUNCE);
+                if (!bs.delta) ++diffuseBounces;
+                cameraRay = cameraRay && bs.delta && dot(wi, is.normal) < 0.0f;
+                flags = cameraRay ? (flags | PF_CAMERA_RAY) : (flags & ~PF_CAMERA_RAY);
+                // crossing a volume boundary: enter the object's medium from outside,
+                // leave it from inside
+                if (mat.flags & MF_VOLUME_BOUNDARY) {
+                    const float a = dot(wo, is.ng), b = dot(wi, is.ng);
+                    if (a * b < 0.0f) {
+                        if (a > 0.0f) media.enter(is.material);
+                        else media.leave(is.material);
+                    }
+                }
+                const uint32_t nextMask = refracted ? VIS_TRANSMISSION : (bs.delta ? VIS_GLOSSY : VIS_DIFFUSE);
+                ln = make_float4(is.normal.x, is.normal.y, is.normal.z, 0.0f);
+                lp = make_float4(is.point.x, is.point.y, is.point.z, 0.0f);
+                const V3 no = spawnOrigin(is, wi);
+                ro = make_float4(no.x, no.y, no.z, __uint_as_float(nextMask));
+                rd = make_float4(wi.x, wi.y, wi.z, bs.pdf);
+                ++depth;
+                skips = 0;
+                cont = true;
+                if (depth > A.rrDepth && !russianRoulette(thr, sb)) {
+                    cont = false;
+                    done = true;
+                }
+            }
+        }
+    }
+    // write back
+    P.L[slot] = L;
+    if (cont) {
+        P.rayO[slot] = ro;
+        P.rayD[slot] = rd;
+        P.thr[slot] = make_float4(thr.x, thr.y, thr.z, lambda);
+        P.lastN[slot] = make_float4(ln.x, ln.y, ln.z, __uint_as_float(flags));
+        P.lastP[slot] = make_float4(lp.x, lp.y, lp.z, __uint_as_float(sb.dim));
+        P.pickP[slot] = pp;
+        P.pickN[slot] = make_float4(pn.x, pn.y, pn.z, __uint_as_float(packCounters(depth, diffuseBounces, passThroughs, skips)));
+        if (volumetric)
+            P.med[slot] = make_float4(__uint_as_float(media.lo), __uint_as_float(media.hi), __uint_as_float(volCtr),
+                                      __int_as_float(media.n));
+    }
+    return cont;
+}
+
 // Consumes the rays binned by shading key (segment by segment, so a warp mostly shades one
 // material kind) and appends the continuing paths to nextQueue.
 __global__ void __launch_bounds__(128, 4) kShade(SceneGPU S, Paths P, WaveArgs A, int32_t* nextQueue, uint32_t* nextCount) {
-    const TablesGPU* T = S.tables;
     uint32_t seg[kShadeKeys];
     int n = 0;
     for (int k = 0; k < kShadeKeys; ++k) {
@@ -215,6 +636,7 @@ __global__ void __launch_bounds__(128, 4) kShade(SceneGPU S, Paths P, WaveArgs A
         n += static_cast<int>(seg[k]);
     }
     const int lane = threadIdx.x & 31;
+    uint32_t unused0 = 0, unused1 = 0, unused2 = 0;
     for (;;) {
         const int base = warpFetch(&P.counters[CNT_WORK_SHADE]);
         if (base >= n) break;
@@ -229,239 +651,48 @@ __global__ void __launch_bounds__(128, 4) kShade(SceneGPU S, Paths P, WaveArgs A
                 ++k;
             }
             slot = P.sortQ[static_cast<size_t>(k) * P.capacity + j];
-            float4 ro = P.rayO[slot];
-            float4 rd = P.rayD[slot];
-            float4 th = P.thr[slot];
-            float4 L = P.L[slot];
-            float4 ln = P.lastN[slot];
-            float4 lp = P.lastP[slot];
-            float4 pp = P.pickP[slot];
-            float4 pn = P.pickN[slot];
-            const float4 hr = P.hit[slot];
-            uint32_t flags = __float_as_uint(ln.w);
-            uint32_t ctr = __float_as_uint(pn.w);
-            int depth = ctr & 0xFF, diffuseBounces = (ctr >> 8) & 0xFF, passThroughs = (ctr >> 16) & 0xFF,
-                skips = (ctr >> 24) & 0xFF;
-            Sobol sb;
-            sb.pixelHash = __float_as_uint(pp.w);
-            {
-                const int sOff = slot / A.nPix;
-                sb.revIndex = rev32(static_cast<uint32_t>(A.sampleFirst + sOff));
-            }
-            sb.dim = __float_as_uint(lp.w);
-            V3 thr = mk(th.x, th.y, th.z);
-            const V3 dir = mk(rd.x, rd.y, rd.z);
-            const V3 rayO = mk(ro.x, ro.y, ro.z);
-            const uint32_t rayMask = __float_as_uint(ro.w);
-            const float lastBsdfPdf = rd.w;
-            const bool specularBounce = flags & PF_SPECULAR_BOUNCE;
-            bool cameraRay = flags & PF_CAMERA_RAY;
-            const int shadowSamples = A.shadowSamples;
-            const int explicitLights = S.nLights;
-            const int prim = __float_as_int(hr.w);
-            const bool hit = prim >= 0;
-            Isect is;
-            bool done = false;
-            if (hit) {
-                Hit h;
-                h.t = hr.x;
-                h.u = hr.y;
-                h.v = hr.z;
-                h.prim = prim;
-                fillHit(S, h, dir, is);
-                // Camera-invisible light quads are passed through by camera rays; the vertex
-                // does not count (path_tracer.cpp:426-439).  Cutouts are not supported here.
-                if (cameraRay && (S.shapes[is.shape].flags & SF_CAMERA_INVISIBLE) && skips < 64) {
-                    const V3 no = offsetRayOrigin(is.point, is.pError, is.ng, dir);
-                    P.rayO[slot] = make_float4(no.x, no.y, no.z, ro.w);
-                    P.pickN[slot] = make_float4(pn.x, pn.y, pn.z, __uint_as_float(packCounters(depth, diffuseBounces, passThroughs, skips + 1)));
-                    cont = true;
-                    done = true;
-                }
-            }
-            if (!done) {
-                flags &= ~PF_FIRST_SEGMENT;
-                const V3 wo = -dir;
-                if (!hit) {
-                    // environment / background (path_tracer.cpp:482-514)
-                    if (depth == 0 && S.bgMode != PE_BG_ENVIRONMENT) {
-                        if (S.bgMode == PE_BG_COLOR) addL(L, thr * m3f(S.bgColor));
-                    } else if (S.env.present) {
-                        const V3 Le = envEval(S.env, dir);
-                        float weight = 1.0f;
-                        if (!specularBounce) {
-                            float pmf = 0.0f;
-                            if (flags & PF_PICKER_VALID) {
-                                LightCtx c;
-                                lightPrepare(S, mk(pp.x, pp.y, pp.z), mk(pn.x, pn.y, pn.z), c);
-                                pmf = lightCtxPmf(S, c, explicitLights);
-                            }
-                            const float lightPdf = pmf * envPdf(S.env, dir);
-                            weight = powerHeuristic(1, lastBsdfPdf, shadowSamples, lightPdf);
-                        }
-                        V3 c = thr * (Le * weight);
-                        if (diffuseBounces >= 2 && A.clampIndirect > 0.0f) {
-                            const float m = smax3(c.x, c.y, c.z);
-                            if (m > A.clampIndirect) c = c * (A.clampIndirect / m);
-                        }
-                        addL(L, c);
-                    }
-                    done = true;
-                } else {
-                    const MatGPU& mat = S.materials[is.material];
-                    // emission with MIS against the previous vertex's NEE (path_tracer.cpp:565-593)
-                    if (mat.flags & MF_EMISSIVE) {
-                        const ShapeInfo& sh = S.shapes[is.shape];
-                        int li = -1;
-                        if (sh.emitter >= 0)
-                            li = (sh.flags & SF_AREA_TRIANGLE) ? sh.emitter : sh.emitter + (is.tri - static_cast<int>(sh.firstTri));
-                        float weight = 1.0f;
-                        if (!specularBounce) {
-                            float lightPdf = 0.0f;
-                            if (li >= 0) {
-                                float pmf = 0.0f;
-                                if (flags & PF_PICKER_VALID) {
-                                    LightCtx c;
-                                    lightPrepare(S, mk(pp.x, pp.y, pp.z), mk(pn.x, pn.y, pn.z), c);
-                                    pmf = lightCtxPmf(S, c, li);
-                                }
-                                lightPdf = pmf * lightPdfHit(S.lights[li], mk(lp.x, lp.y, lp.z), is.point);
-                            }
-                            if (lightPdf > 0.0f && lastBsdfPdf > 0.0f)
-                                weight = powerHeuristic(1, lastBsdfPdf, shadowSamples, lightPdf);
-                        }
-                        V3 c = thr * (m3f(mat.emission) * weight);
-                        if (diffuseBounces >= 2 && A.clampIndirect > 0.0f) {
-                            const float m = smax3(c.x, c.y, c.z);
-                            if (m > A.clampIndirect) c = c * (A.clampIndirect / m);
-                        }
-                        addL(L, c);
-                    }
-                    if (depth >= A.maxDepth) done = true;
-                }
-                if (!done) {
-                    const MatGPU& mat = S.materials[is.material];
-                    ShadePoint sp;
-                    sp.p = is.point;
-                    sp.n = is.normal;
-                    sp.ng = is.ng;
-                    sp.tangent = is.tangent;
-                    sp.frontFace = is.frontFace;
-                    sp.wavelength = 0.0f;
-                    const bool isSpecular = (mat.flags & MF_DELTA) != 0;
-                    // next-event estimation (path_tracer.cpp:631-698)
-                    if (S.lightCount > 0 && !isSpecular) {
-                        LightCtx picker;
-                        lightPrepare(S, is.point, is.normal, picker);
-                        flags |= PF_PICKER_VALID;
-                        pp = make_float4(is.point.x, is.point.y, is.point.z, pp.w);
-                        pn.x = is.normal.x;
-                        pn.y = is.normal.y;
-                        pn.z = is.normal.z;
-                        for (int s = 0; s < shadowSamples; ++s) {
-                            float lightPmf = 0.0f;
-                            const int lightIndex = lightCtxSample(S, picker, get1D(sb), lightPmf);
-                            if (lightIndex < 0 || !(lightPmf > 0.0f)) {
-                                (void)get2D(T, sb);
-                                continue;
-                            }
-                            const bool fromEnv = lightIndex >= explicitLights;
-                            const V2 ul = get2D(T, sb);
-                            const LightSample ls = fromEnv ? envSample(S.env, ul) : sampleLight(S.lights[lightIndex], is.point, ul);
-                            if (!lsValid(ls)) continue;
-                            V3 so, sd;
-                            float stMax;
-                            if (!makeShadowRay(is, ls.wi, ls.distance, so, sd, stMax)) continue;
-                            float bsdfPdf = 0.0f;
-                            const V3 f = bsdfEvalPdf(T, mat, wo, ls.wi, sp, bsdfPdf, nullptr);
-                            const float cosTheta = fabsf(dot(ls.wi, is.normal));
-                            if (isBlack(f) || !(cosTheta > 0.0f)) continue;
-                            const float lightPdf = lightPmf * ls.pdf;
-                            const float weight = powerHeuristic(shadowSamples, lightPdf, 1, bsdfPdf);
-                            const float scalar = cosTheta * weight / (lightPdf * static_cast<float>(shadowSamples));
-                            const V3 fLi = f * ls.Li;
-                            uint32_t pos;
-                            {
-                                // shadow queue append (one record per sample)
-                                pos = atomicAdd(&P.counters[2], 1u);
-                            }
-                            P.shadowQ[pos] = slot;
-                            P.shO[pos] = make_float4(so.x, so.y, so.z, stMax);
-                            P.shD[pos] = make_float4(sd.x, sd.y, sd.z, scalar);
-                            P.shC[pos] = make_float4(fLi.x, fLi.y, fLi.z, __uint_as_float(diffuseBounces >= 1 ? 1u : 0u));
-                            P.shT[pos] = make_float4(thr.x, thr.y, thr.z, 0.0f);
-                        }
-                    }
-                    // BSDF sampling (path_tracer.cpp:700-743)
-                    const float uc = get1D(sb);
-                    const V2 u2 = get2D(T, sb);
-                    BsdfSample bs;
-                    const bool sampled = bsdfSample(T, mat, wo, sp, uc, u2, bs);
-                    if (!sampled || bs.subsurface || bs.pdf <= 0.0f || isBlack(bs.f)) {
-                        done = true;
-                    } else if (bs.passThrough) {
-                        thr *= bs.f * (fabsf(dot(bs.wi, is.normal)) / bs.pdf);
-                        if (!isFinite3(thr) || ++passThroughs > 64) {
-                            done = true;
-                        } else {
-                            const V3 no = spawnOrigin(is, bs.wi);
-                            ro = make_float4(no.x, no.y, no.z, ro.w);
-                            rd = make_float4(bs.wi.x, bs.wi.y, bs.wi.z, rd.w);
-                            skips = 0;
-                            cont = true;
-                        }
-                    } else {
-                        const V3 wi = bs.wi;
-                        const bool refracted = dot(wo, is.ng) * dot(wi, is.ng) < 0.0f;
-                        const float cosTheta = fabsf(dot(wi, is.normal));
-                        thr *= bs.f * (cosTheta / bs.pdf);
-                        if (!isFinite3(thr)) {
-                            done = true;
-                        } else {
-                            flags = bs.delta ? (flags | PF_SPECULAR_BOUNCE) : (flags & ~PF_SPECULAR_BOUNCE);
-                            if (!bs.delta) ++diffuseBounces;
-                            cameraRay = cameraRay && bs.delta && dot(wi, is.normal) < 0.0f;
-                            flags = cameraRay ? (flags | PF_CAMERA_RAY) : (flags & ~PF_CAMERA_RAY);
-                            const uint32_t nextMask = refracted ? VIS_TRANSMISSION : (bs.delta ? VIS_GLOSSY : VIS_DIFFUSE);
-                            ln = make_float4(is.normal.x, is.normal.y, is.normal.z, 0.0f);
-                            lp = make_float4(is.point.x, is.point.y, is.point.z, 0.0f);
-                            const V3 no = spawnOrigin(is, wi);
-                            ro = make_float4(no.x, no.y, no.z, __uint_as_float(nextMask));
-                            rd = make_float4(wi.x, wi.y, wi.z, bs.pdf);
-                            ++depth;
-                            skips = 0;
-                            cont = true;
-                            if (depth > A.rrDepth) {
-                                // russianRoulette (path_tracer.cpp:131-137)
-                                const float m = smax3(thr.x, thr.y, thr.z);
-                                if (!(m >= 1.0f)) {
-                                    if (!(m > 0.0f) || get1D(sb) >= m) {
-                                        cont = false;
-                                        done = true;
-                                    } else {
-                                        thr /= m;
-                                    }
-                                }
-                            }
-                        }
-                    }
-                }
-            }
-            // write back
-            P.L[slot] = L;
-            if (cont) {
-                P.rayO[slot] = ro;
-                P.rayD[slot] = rd;
-                P.thr[slot] = make_float4(thr.x, thr.y, thr.z, th.w);
-                P.lastN[slot] = make_float4(ln.x, ln.y, ln.z, __uint_as_float(flags));
-                P.lastP[slot] = make_float4(lp.x, lp.y, lp.z, __uint_as_float(sb.dim));
-                P.pickP[slot] = pp;
-                P.pickN[slot] = make_float4(pn.x, pn.y, pn.z, __uint_as_float(packCounters(depth, diffuseBounces, passThroughs, skips)));
-            }
-            (void)done;
+            cont = shadeSlot<false, false>(S, P, A, slot, unused0, unused1, unused2);
         }
         queuePush(nextQueue, nextCount, cont, slot);
     }
+}
+
+// ---- tail: the last paths of a wave, each run to its end by one thread -------------------------
+// Once a wave's live queue fits in one resident grid, per-bounce launches cost more than they
+// save: each thread takes a path from the queue, alternates closest-hit queries with shadeSlot
+// (shadow rays inline) until the path ends, then takes the next.  The arithmetic and the order of
+// L's terms are the wavefront's, so the film is the same bit for bit.
+template <bool COUNT>
+__global__ void __launch_bounds__(128) kTail(SceneGPU S, Paths P, WaveArgs A, const int32_t* queue, const uint32_t* count,
+                                             unsigned long long* stats) {
+    const int n = static_cast<int>(*count);
+    uint32_t nodes = 0, tris = 0, shNodes = 0, shTris = 0, rays = 0, shRays = 0;
+    for (;;) {
+        const int i = static_cast<int>(atomicAdd(&P.counters[CNT_WORK_TAIL], 1u));
+        if (i >= n) break;
+        const int slot = queue[i];
+        for (int q = 0;; ++q) {
+            if (q >= kMaxPathQueries) {
+                atomicAdd(&stats[7], 1ull);
+                break;
+            }
+            const float4 ro = P.rayO[slot];
+            const float4 rd = P.rayD[slot];
+            const Hit h = traceClosest<COUNT>(S, mk(ro.x, ro.y, ro.z), mk(rd.x, rd.y, rd.z), __float_as_uint(ro.w), 0.0f,
+                                              1e30f, nodes, tris);
+            ++rays;
+            P.hit[slot] = make_float4(h.t, h.u, h.v, __int_as_float(h.prim));
+            if (!shadeSlot<true, COUNT>(S, P, A, slot, shNodes, shTris, shRays)) break;
+        }
+    }
+    if (COUNT) {
+        atomicAdd(&stats[0], static_cast<unsigned long long>(nodes));
+        atomicAdd(&stats[1], static_cast<unsigned long long>(tris));
+        atomicAdd(&stats[2], static_cast<unsigned long long>(shNodes));
+        atomicAdd(&stats[3], static_cast<unsigned long long>(shTris));
+    }
+    atomicAdd(&stats[5], static_cast<unsigned long long>(rays));
+    atomicAdd(&stats[6], static_cast<unsigned long long>(shRays));
 }
 
 // ---- film: Film::addSample in sample order per pixel (src/core/image/film.cpp:56-69) ----------

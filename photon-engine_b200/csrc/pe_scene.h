@@ -181,7 +181,9 @@ struct SceneGPU {
     int32_t bgMode;
     float bgColor[3];
     int32_t hasShadowTransmitters;
-    int32_t hasVolumes;
+    int32_t hasVolumes;      // some material is a volume boundary: paths carry a medium stack
+    int32_t hasSubsurface;   // some Disney material has a subsurface lobe (random walks)
+    int32_t exitMaterial;    // white Lambert of the subsurface exit vertex
 };
 
 } // namespace pe

@@ -531,6 +531,15 @@ class CudaDevice:
     def set_counting(self, on: bool):
         capi.check(_lib().pe_device_set_counting(self._h, 1 if on else 0))
 
+    def set_tail_paths(self, paths: int):
+        """Live paths at or below which a wave finishes in the per-thread tail kernel
+        (-1 = one resident grid, 0 = never); the film does not depend on it."""
+        capi.check(_lib().pe_device_set_tail_paths(self._h, int(paths)))
+
+    @property
+    def tail_paths(self) -> int:
+        return int(_lib().pe_device_tail_paths(self._h))
+
     # diagnostics
     def trace_primary(self, camera: PerspectiveCamera, settings: RenderSettings, sample_index: int = 0):
         n = settings.width * settings.height

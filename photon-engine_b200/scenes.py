@@ -10,6 +10,12 @@ scenes stand in for them with the stated sizes and value distributions.
                        clearcoat ~ U(0,1), base ~ U(0,1)³), a ground plane, a 2048×1024 float32
                        sky-gradient environment whose sun lobe holds 60 % of the power, and one
                        rectangular softbox; 1920×1080, 256 spp, depth 12 at product scale.
+* ``media_scene``      many lights and media, in millimetres: a seeded spiral LED strip of 1000
+                       quads (2000 emissive triangles, light-BVH NEE), a dispersive glass sphere
+                       (IOR 1.5, Abbe 35), an absorbing liquid cylinder (σa ~ U(0.1, 2)/mm per
+                       channel), a Henyey–Greenstein scattering sphere (g = 0.6) and a random-walk
+                       subsurface slab (mean free path 1–5 mm); ~200k triangles, 1280×720,
+                       512 spp, depth 24 at full size.
 """
 from __future__ import annotations
 
@@ -17,8 +23,8 @@ import math
 
 import numpy as np
 
-from .engine import (AreaLight, DisneyMaterial, EnvironmentLight, Lambertian, PerspectiveCamera, PixelFilterType,
-                     RenderSettings, Scene, TriangleMesh)
+from .engine import (AreaLight, Dielectric, DisneyMaterial, EnvironmentLight, Lambertian, PerspectiveCamera,
+                     PixelFilterType, RenderSettings, Scene, TriangleMesh)
 
 
 def _quad(p0, p1, p2, p3):
@@ -179,6 +185,174 @@ def torus_knot_scene(width: int = 1920, height: int = 1080, spp: int = 256, max_
     scene.add_light(softbox)
     scene.set_environment(EnvironmentLight(sky_environment(*env_size), 0.0, 1.0))
     camera = PerspectiveCamera((0.0, 4.5, -10.5), (0.0, 1.6, 0.0), (0.0, 1.0, 0.0), 40.0, width / height)
+    settings = RenderSettings(width=width, height=height, samples_per_pixel=spp, max_bounces=max_depth,
+                              filter_type=PixelFilterType.BlackmanHarris, filter_width=1.5)
+    return scene, camera, settings
+
+
+def uv_sphere(center, radius: float, nu: int, nv: int):
+    """Latitude-longitude sphere with smooth vertex normals, wound outward: nu·(nv−1)·2 triangles."""
+    cx, cy, cz = center
+    th = np.linspace(0.0, math.pi, nv + 1)
+    ph = np.linspace(0.0, 2.0 * math.pi, nu + 1)[:-1]
+    st, ct = np.sin(th)[:, None], np.cos(th)[:, None]
+    n = np.stack([st * np.cos(ph)[None, :], np.broadcast_to(ct, (nv + 1, nu)), st * np.sin(ph)[None, :]], -1)
+    n = n.reshape(-1, 3)
+    pos = (n * radius + np.array([cx, cy, cz])).astype(np.float32)
+    tris = []
+    for i in range(nv):
+        a = i * nu + np.arange(nu)
+        b = i * nu + (np.arange(nu) + 1) % nu
+        c = (i + 1) * nu + (np.arange(nu) + 1) % nu
+        d = (i + 1) * nu + np.arange(nu)
+        if i > 0:
+            tris.append(np.stack([a, b, c], -1))
+        if i < nv - 1:
+            tris.append(np.stack([a, c, d], -1))
+    return pos, n.astype(np.float32), np.concatenate(tris).astype(np.uint32)
+
+
+def cylinder(center, radius: float, height: float, nseg: int, nrings: int):
+    """Closed cylinder about +y (base at center.y): smooth side normals, flat caps, wound outward
+    (the geometric normal decides which side of a volume boundary a path is on)."""
+    cx, cy, cz = center
+    ph = np.linspace(0.0, 2.0 * math.pi, nseg + 1)[:-1]
+    ring = np.stack([np.cos(ph), np.zeros_like(ph), np.sin(ph)], -1)
+    ys = np.linspace(0.0, height, nrings + 1)
+    side = np.concatenate([ring * radius + np.array([cx, cy + y, cz]) for y in ys])
+    side_n = np.tile(ring, (nrings + 1, 1))
+    tris = []
+    for i in range(nrings):
+        a = i * nseg + np.arange(nseg)
+        b = i * nseg + (np.arange(nseg) + 1) % nseg
+        tris.append(np.stack([a, b + nseg, b], -1))
+        tris.append(np.stack([a, a + nseg, b + nseg], -1))
+    pos, nrm, idx = [side], [side_n], [np.concatenate(tris)]
+    base = side.shape[0]
+    for y, sgn in ((0.0, -1.0), (height, 1.0)):
+        rim = ring * radius + np.array([cx, cy + y, cz])
+        centre = np.array([[cx, cy + y, cz]])
+        pos.append(np.concatenate([centre, rim]))
+        nrm.append(np.tile([0.0, sgn, 0.0], (nseg + 1, 1)))
+        k = np.arange(nseg)
+        a, b = base + 1 + k, base + 1 + (k + 1) % nseg
+        c0 = np.full(nseg, base)
+        idx.append(np.stack([c0, b, a], -1) if sgn > 0 else np.stack([c0, a, b], -1))
+        base += nseg + 1
+    return (np.concatenate(pos).astype(np.float32), np.concatenate(nrm).astype(np.float32),
+            np.concatenate(idx).astype(np.uint32))
+
+
+def grid_box(center, size, n: int):
+    """Axis-aligned box whose faces are n×n quad grids (flat normals): 12·n² triangles."""
+    c = np.asarray(center, np.float64)
+    h = np.asarray(size, np.float64) * 0.5
+    t = np.linspace(-1.0, 1.0, n + 1)
+    pos, nrm, idx = [], [], []
+    base = 0
+    for axis in range(3):
+        for sgn in (-1.0, 1.0):
+            u_ax, v_ax = [a for a in range(3) if a != axis]
+            if sgn < 0:
+                u_ax, v_ax = v_ax, u_ax
+            uu, vv = np.meshgrid(t, t, indexing="ij")
+            p = np.zeros((n + 1, n + 1, 3))
+            p[..., axis] = sgn
+            p[..., u_ax] = uu
+            p[..., v_ax] = vv
+            p = p.reshape(-1, 3) * h + c
+            nn = np.zeros((p.shape[0], 3))
+            nn[:, axis] = sgn
+            i, j = np.meshgrid(np.arange(n), np.arange(n), indexing="ij")
+            a = (i * (n + 1) + j).ravel() + base
+            b = a + (n + 1)
+            tri = np.concatenate([np.stack([a, b, b + 1], -1), np.stack([a, b + 1, a + 1], -1)])
+            # outward winding: the geometric normal must agree with the face normal
+            e = np.cross(p[tri[:, 1] - base] - p[tri[:, 0] - base], p[tri[:, 2] - base] - p[tri[:, 0] - base])
+            if np.dot(e[0], nn[0]) < 0:
+                tri = tri[:, [0, 2, 1]]
+            pos.append(p)
+            nrm.append(nn)
+            idx.append(tri)
+            base += p.shape[0]
+    return (np.concatenate(pos).astype(np.float32), np.concatenate(nrm).astype(np.float32),
+            np.concatenate(idx).astype(np.uint32))
+
+
+def led_strip(n_quads: int, seed: int, height: float = 350.0, r0: float = 60.0, r1: float = 620.0,
+              turns: float = 3.2, size: float = 9.0):
+    """Spiral of downward-facing emissive quads (2 triangles each) above the floor."""
+    rng = np.random.default_rng(seed)
+    t = (np.arange(n_quads) + 0.5) / n_quads
+    a = 2.0 * math.pi * turns * t + rng.uniform(-0.01, 0.01, n_quads)
+    r = r0 + (r1 - r0) * t
+    cx, cz = r * np.cos(a), r * np.sin(a)
+    tx, tz = -np.sin(a), np.cos(a)          # along the strip
+    h = size * 0.5
+    rx, rz = np.cos(a), np.sin(a)           # across the strip (radial)
+    pos = np.zeros((n_quads, 4, 3))
+    for k, (su, sv) in enumerate(((-1, -1), (1, -1), (1, 1), (-1, 1))):
+        pos[:, k, 0] = cx + su * h * tx + sv * h * rx
+        pos[:, k, 2] = cz + su * h * tz + sv * h * rz
+        pos[:, k, 1] = height
+    # (0, 2, 1), (0, 3, 2): tangent × radial is +y, so this winding faces the floor
+    idx = np.arange(n_quads)[:, None] * 4 + np.array([[0, 2, 1], [0, 3, 2]]).reshape(1, 2, 3).transpose(1, 0, 2)
+    idx = np.concatenate([idx[0], idx[1]])
+    return pos.reshape(-1, 3).astype(np.float32), idx.astype(np.uint32)
+
+
+def media_scene(width: int = 1280, height: int = 720, spp: int = 512, max_depth: int = 24, seed: int = 11,
+                n_leds: int = 1000, sphere_res=(288, 144), cyl_res=(256, 48), slab_res: int = 24):
+    """Many-light and media workload (units: millimetres)."""
+    rng = np.random.default_rng(seed)
+    scene = Scene()
+    # room: floor and back wall
+    g = 1500.0
+    floor = Lambertian((0.7, 0.7, 0.7))
+    fp = np.array([(-g, 0.0, -g), (-g, 0.0, g), (g, 0.0, g), (g, 0.0, -g)], np.float32)
+    scene.add_shape(TriangleMesh(fp, None, None, np.array([[0, 1, 2], [0, 2, 3]], np.uint32), floor))
+    wall = Lambertian((0.55, 0.55, 0.6))
+    wp = np.array([(-g, 0.0, 800.0), (-g, 1200.0, 800.0), (g, 1200.0, 800.0), (g, 0.0, 800.0)], np.float32)
+    scene.add_shape(TriangleMesh(wp, None, None, np.array([[0, 1, 2], [0, 2, 3]], np.uint32), wall))
+    # LED strip: four seeded colours, each LED quad two triangle emitters
+    lpos, lidx = led_strip(n_leds, seed)
+    colours = [tuple(rng.uniform(2.0, 8.0) * np.array(c)) for c in ((1.0, 0.85, 0.6), (0.6, 0.8, 1.0), (1.0, 0.5, 0.4),
+                                                            (0.7, 1.0, 0.7))]
+    which = rng.integers(0, 4, n_leds)
+    for k, col in enumerate(colours):
+        q = np.nonzero(which == k)[0]
+        if q.size == 0:
+            continue
+        tri = lidx.reshape(2, n_leds, 3)[:, q].reshape(-1, 3)
+        used = np.unique(tri)
+        remap = np.full(lpos.shape[0], -1, np.int64)
+        remap[used] = np.arange(used.size)
+        scene.add_shape(TriangleMesh(lpos[used], None, None, remap[tri].astype(np.uint32),
+                                     Lambertian((0.0, 0.0, 0.0), emission=col)))
+    # dispersive glass sphere
+    glass = Dielectric(1.5)
+    glass.set_abbe(35.0)
+    p, n, i = uv_sphere((-250.0, 95.0, 60.0), 95.0, *sphere_res)
+    scene.add_shape(TriangleMesh(p, n, None, i, glass))
+    # Henyey–Greenstein scattering sphere (g = 0.6), mean free path ~ 25 mm
+    fog = Dielectric(1.33)
+    fog.set_scattering(0.04, (0.92, 0.9, 0.85), 0.6)
+    p, n, i = uv_sphere((250.0, 95.0, 60.0), 95.0, *sphere_res)
+    scene.add_shape(TriangleMesh(p, n, None, i, fog))
+    # Beer–Lambert liquid: σa per channel ~ U(0.1, 2) / mm, set as a colour over 1 mm
+    sigma_a = rng.uniform(0.1, 2.0, 3)
+    liquid = Dielectric(1.33)
+    liquid.set_absorption(tuple(np.exp(-sigma_a)), 1.0)
+    p, n, i = cylinder((0.0, 0.0, -170.0), 55.0, 110.0, *cyl_res)
+    scene.add_shape(TriangleMesh(p, n, None, i, liquid))
+    # random-walk subsurface slab, mean free path 1–5 mm per channel
+    skin = DisneyMaterial((0.9, 0.62, 0.5), 0.0, 0.45, 0.5)
+    skin.set_subsurface(1.0)
+    skin.set_subsurface_radius(tuple(rng.uniform(1.0, 5.0, 3)))
+    skin.set_subsurface_scale(1.0)
+    p, n, i = grid_box((0.0, 20.0, 230.0), (380.0, 40.0, 170.0), slab_res)
+    scene.add_shape(TriangleMesh(p, n, None, i, skin))
+    camera = PerspectiveCamera((0.0, 420.0, -950.0), (0.0, 70.0, 40.0), (0.0, 1.0, 0.0), 38.0, width / height)
     settings = RenderSettings(width=width, height=height, samples_per_pixel=spp, max_bounces=max_depth,
                               filter_type=PixelFilterType.BlackmanHarris, filter_width=1.5)
     return scene, camera, settings

@@ -29,7 +29,9 @@ def test_binding_covers_every_declared_symbol(pe):
 
 
 def test_abi_version(pe):
-    assert pe._capi.load().pe_abi_version() == 1
+    header = (ROOT / "include" / "photon_cuda.h").read_text()
+    want = int(re.search(r"#define PE_ABI_VERSION (\d+)", header).group(1))
+    assert pe._capi.load().pe_abi_version() == want
 
 
 def test_device_create_reports_error_without_crashing(pe):

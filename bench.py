@@ -204,9 +204,11 @@ def run_ours(args):
         pg.barrier()
     launches = 0
     rays = 0
+    rays_isect = 0
     shadow_rays = 0
     ms_isect = 0.0
     n_isect = 0
+    kernel_ms = {"closest_hit": 0.0, "shade": 0.0, "any_hit": 0.0, "tail": 0.0, "total": 0.0}
     with ClockSampler(dev.pci_bus_id) as clocks:
         dev.timer_begin()
         for k in range(args.steps):
@@ -214,9 +216,13 @@ def run_ours(args):
             s = dev.last_stats()
             launches += s.kernel_launches
             rays += s.closest_rays
+            rays_isect += s.closest_rays - s.tail_closest_rays
             shadow_rays += s.shadow_rays
             ms_isect += s.ms_intersect
             n_isect += s.intersect_launches
+            for key, v in (("closest_hit", s.ms_intersect), ("shade", s.ms_shade), ("any_hit", s.ms_shadow),
+                           ("tail", s.ms_tail), ("total", s.ms_total)):
+                kernel_ms[key] += v / args.steps
         ms = dev.timer_end()
     if pg:
         import torch
@@ -254,20 +260,21 @@ def run_ours(args):
     bytes_per_ray = (cs.node_visits * NODE_BYTES + cs.tri_tests * TRI_BYTES) / max(1, cs.closest_rays) + \
         RAY_BYTES + HIT_BYTES + QUEUE_BYTES
     peak, peak_kind = measured_peaks()
-    achieved = (rays * bytes_per_ray) / (ms_isect / 1000.0) / 1e9 if ms_isect > 0 else None
+    # only the rays the bounce-by-bounce closest-hit launches traced (the tail kernel's are its own)
+    achieved = (rays_isect * bytes_per_ray) / (ms_isect / 1000.0) / 1e9 if ms_isect > 0 else None
     traffic = None
     tfile = ROOT / "profiles" / "closest_hit_dram_bytes_per_ray.txt"
     if tfile.exists():
         try:
             per_ray = float(tfile.read_text().split()[0])
-            traffic = per_ray * rays / max(1, n_isect)
+            traffic = per_ray * rays_isect / max(1, n_isect)
         except (ValueError, IndexError):
             traffic = None
     roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
             "frac": (achieved / peak) if achieved else None, "traffic": traffic,
             "kernel": "kIntersect (closest-hit BVH traversal)", "peak_kind": peak_kind,
             "bytes_per_ray": bytes_per_ray, "avg_launch_ms": ms_isect / max(1, n_isect),
-            "rays_per_launch": rays / max(1, n_isect)}
+            "rays_per_launch": rays_isect / max(1, n_isect)}
 
     cpu = None
     if world == 1 and not args.no_cpu_baseline:
@@ -290,6 +297,7 @@ def run_ours(args):
         "e2e": {"value": e2e, "unit": "paths/s", "h2d_bytes_per_step": 76 + 40,
                 "d2h_bytes_per_step": WIDTH * HEIGHT * (12 + 4 + 4)},
         "gpu_launches": int(launches),
+        "kernel_ms_per_step": kernel_ms,
         "roofline": roof,
         "cpu_baseline": cpu,
         "clocks": clocks.summary(),
@@ -309,11 +317,37 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
+    ap.add_argument("--serve", action="store_true",
+                    help="served-mix benchmark (request server vs the plain per-request loop) instead")
+    ap.add_argument("--serve-requests", type=int, default=24)
+    ap.add_argument("--serve-quick", action="store_true", help="small scenes (a smoke run of the served mix)")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     if args.impl == "reference":
         return run_reference(args)
+    if args.serve:
+        return run_serve(args)
     return run_ours(args)
+
+
+def run_serve(args):
+    """The served mix on one GPU: request server vs the plain per-request loop (servebench.py)."""
+    pe = pe_load()
+    from photon_engine_b200 import servebench
+    dev = pe.CudaDevice(0)
+    with ClockSampler(dev.pci_bus_id) as clocks:
+        res = servebench.run(pe, dev, n_requests=args.serve_requests, quick=args.serve_quick)
+    s, p = res["served"], res["plain"]
+    out = {"metric": "served paths/s (Poisson mix over 4 resident scenes)", "value": s["paths_per_s"],
+           "unit": "paths/s", "n_gpus": 1, "higher_is_better": True, "dtype": "f32",
+           "data": "synthetic (seeded procedural scenes and request stream)",
+           "config": {"workload": "served mix: Cornell / 1M-tri knot / media / 5.2M-tri grid"
+                      + (" (reduced scenes)" if args.serve_quick else ""), **res["mix"]},
+           "served": s, "plain": p, "served_over_plain": res["speedup"],
+           "preview_p99_ms": s["preview_p99_ms"], "clocks": clocks.summary()}
+    print(json.dumps(out))
+    dev.close()
+    return 0
 
 
 if __name__ == "__main__":

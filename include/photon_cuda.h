@@ -38,7 +38,7 @@
 extern "C" {
 #endif
 
-#define PE_ABI_VERSION 2
+#define PE_ABI_VERSION 3
 
 typedef enum pe_status {
     PE_OK = 0,
@@ -203,6 +203,8 @@ typedef struct pe_render_stats {
     uint64_t tail_paths;       /* paths finished by the per-thread tail kernel */
     float ms_tail;             /* device time in the tail kernel (timed renders only) */
     uint32_t pad0;
+    uint64_t tail_closest_rays; /* closest-hit segments traced by the tail kernel (in closest_rays) */
+    uint64_t tail_shadow_rays;  /* any-hit segments traced by the tail kernel (in shadow_rays) */
 } pe_render_stats;
 
 const char* pe_last_error(void);
@@ -301,6 +303,63 @@ typedef struct pe_bsdf_result {
 } pe_bsdf_result;
 
 int32_t pe_device_bsdf_probe(pe_device* d, int32_t material, const pe_bsdf_query* q, size_t n, pe_bsdf_result* out);
+
+/* ---- Request server ---------------------------------------------------------------------------
+ * The served form of the render path; no class of the reference engine serves requests (its
+ * RenderSession drives one device for one view).  Scenes stay resident; each
+ * request (scene, camera, settings, spp) gets a device film when the HBM budget has room for
+ * it; a worker thread packs the pending sample ranges of the admitted requests of one scene into
+ * shared waves (continuous batching: a request submitted while waves run joins the next wave),
+ * highest priority first, then least remaining work.  A request's film equals, bit for bit, the
+ * film of pe_device_render over samples [0, spp) alone.  While a server runs it owns its device:
+ * render nothing else on that device until pe_server_destroy, after which the device has the
+ * scene it had before. */
+typedef struct pe_server pe_server;
+
+enum { PE_REQ_QUEUED = 0, PE_REQ_ACTIVE = 1, PE_REQ_DONE = 2, PE_REQ_FAILED = 3, PE_REQ_RELEASED = 4 };
+
+typedef struct pe_request_desc {
+    int32_t scene;          /* id from pe_server_add_scene */
+    pe_camera camera;
+    pe_settings settings;   /* film size, depth, filter, seed, ... */
+    int32_t spp;            /* samples [0, spp) per pixel */
+    int32_t priority;       /* larger first */
+} pe_request_desc;
+
+typedef struct pe_request_status {
+    int32_t state;          /* PE_REQ_* */
+    int32_t samples_done;   /* samples finished on every pixel */
+    double submit_ms;       /* server clock (ms since pe_server_create) */
+    double start_ms;        /* admitted: film allocated */
+    double done_ms;         /* last sample in the device film */
+    uint64_t paths;
+    int32_t error;          /* PE_* status of a failed request */
+    int32_t pad;
+} pe_request_status;
+
+typedef struct pe_server_stats {
+    uint64_t submitted, completed, failed;
+    uint64_t queued, active;
+    uint64_t waves, paths, segments;
+    double busy_ms;               /* device time of the waves */
+    uint64_t film_bytes, film_bytes_peak, budget_bytes, scene_bytes;
+} pe_server_stats;
+
+/* budget_bytes bounds the device memory of resident scenes plus admitted films. */
+pe_server* pe_server_create(pe_device* d, uint64_t budget_bytes, char* err, size_t err_len);
+void pe_server_destroy(pe_server* s);
+/* Uploads a built scene and keeps it resident; returns its id (>= 0) or a negative PE_* status. */
+int32_t pe_server_add_scene(pe_server* s, const pe_scene* scene);
+/* Queues a request; returns its id (>= 0) or a negative PE_* status (a film larger than the
+ * whole budget is PE_ERR_LIMIT). */
+int64_t pe_server_submit(pe_server* s, const pe_request_desc* r);
+int32_t pe_server_status(pe_server* s, int64_t id, pe_request_status* out);
+/* Waits until the request is done or failed, at most timeout_ms (< 0: no limit).  PE_OK when
+ * done, PE_ERR_CANCELLED on timeout, the request's error when it failed. */
+int32_t pe_server_wait(pe_server* s, int64_t id, int32_t timeout_ms);
+/* Copies a done request's film out (any pointer may be NULL) and releases its device memory. */
+int32_t pe_server_take(pe_server* s, int64_t id, float* sum_rgb, uint32_t* sample_count, float* sum_lum_sq);
+int32_t pe_server_get_stats(pe_server* s, pe_server_stats* out);
 
 #ifdef __cplusplus
 }

@@ -6,7 +6,8 @@ host-side mirror of the reference's RenderDevice / RenderSession / Scene API ove
 from . import _capi
 from .engine import (AreaLight, Background, BackgroundMode, CudaDevice, Dielectric, DeviceFeatures, DeviceInfo,
                      DisneyMaterial, EnvironmentLight, Film, Lambertian, Material, Mirror, PerspectiveCamera,
-                     PixelFilterType, RenderMode, RenderSession, RenderSettings, RenderTargets, SampleBatchResult,
+                     PixelFilterType, RenderMode, RenderServer, RenderSession, RenderSettings, RenderTargets, RequestStatus,
+                     SampleBatchResult,
                      Scene, SceneUpdateKind, SessionConfig, TriangleMesh, create_device, enumerate_devices, rel_mse)
 
 __all__ = [n for n in dir() if not n.startswith("_")] + ["_capi"]

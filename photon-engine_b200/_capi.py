@@ -73,7 +73,8 @@ class pe_render_stats(C.Structure):
                 ("intersect_launches", C.c_uint64), ("node_visits", C.c_uint64), ("tri_tests", C.c_uint64),
                 ("error_flags", C.c_uint32), ("kernel_launches", C.c_uint64),
                 ("shadow_node_visits", C.c_uint64), ("shadow_tri_tests", C.c_uint64),
-                ("tail_paths", C.c_uint64), ("ms_tail", C.c_float), ("pad0", C.c_uint32)]
+                ("tail_paths", C.c_uint64), ("ms_tail", C.c_float), ("pad0", C.c_uint32),
+                ("tail_closest_rays", C.c_uint64), ("tail_shadow_rays", C.c_uint64)]
 
 
 class pe_bsdf_query(C.Structure):
@@ -84,6 +85,27 @@ class pe_bsdf_query(C.Structure):
 class pe_bsdf_result(C.Structure):
     _fields_ = [("f", F3), ("pdf", C.c_float), ("sampled", C.c_int32), ("wi", F3), ("sf", F3), ("spdf", C.c_float),
                 ("delta", C.c_int32), ("pass_through", C.c_int32), ("subsurface", C.c_int32), ("weight", F3)]
+
+
+PE_REQ_QUEUED, PE_REQ_ACTIVE, PE_REQ_DONE, PE_REQ_FAILED, PE_REQ_RELEASED = 0, 1, 2, 3, 4
+
+
+class pe_request_desc(C.Structure):
+    _fields_ = [("scene", C.c_int32), ("camera", pe_camera), ("settings", pe_settings), ("spp", C.c_int32),
+                ("priority", C.c_int32)]
+
+
+class pe_request_status(C.Structure):
+    _fields_ = [("state", C.c_int32), ("samples_done", C.c_int32), ("submit_ms", C.c_double),
+                ("start_ms", C.c_double), ("done_ms", C.c_double), ("paths", C.c_uint64), ("error", C.c_int32),
+                ("pad", C.c_int32)]
+
+
+class pe_server_stats(C.Structure):
+    _fields_ = [("submitted", C.c_uint64), ("completed", C.c_uint64), ("failed", C.c_uint64),
+                ("queued", C.c_uint64), ("active", C.c_uint64), ("waves", C.c_uint64), ("paths", C.c_uint64),
+                ("segments", C.c_uint64), ("busy_ms", C.c_double), ("film_bytes", C.c_uint64),
+                ("film_bytes_peak", C.c_uint64), ("budget_bytes", C.c_uint64), ("scene_bytes", C.c_uint64)]
 
 
 # Every symbol include/photon_cuda.h declares, with its ctypes signature.
@@ -130,6 +152,14 @@ SIGNATURES = {
     "pe_device_trace_primary": (C.c_int32, [P, C.POINTER(pe_camera), C.POINTER(pe_settings), C.c_int32, IP, IP, FP]),
     "pe_device_sobol": (C.c_int32, [P, C.c_uint64, IP, IP, IP, C.c_size_t, C.c_int32, FP]),
     "pe_device_bsdf_probe": (C.c_int32, [P, C.c_int32, C.POINTER(pe_bsdf_query), C.c_size_t, C.POINTER(pe_bsdf_result)]),
+    "pe_server_create": (P, [P, C.c_uint64, C.c_char_p, C.c_size_t]),
+    "pe_server_destroy": (None, [P]),
+    "pe_server_add_scene": (C.c_int32, [P, P]),
+    "pe_server_submit": (C.c_int64, [P, C.POINTER(pe_request_desc)]),
+    "pe_server_status": (C.c_int32, [P, C.c_int64, C.POINTER(pe_request_status)]),
+    "pe_server_wait": (C.c_int32, [P, C.c_int64, C.c_int32]),
+    "pe_server_take": (C.c_int32, [P, C.c_int64, FP, UP, FP]),
+    "pe_server_get_stats": (C.c_int32, [P, C.POINTER(pe_server_stats)]),
 }
 
 _lib = None

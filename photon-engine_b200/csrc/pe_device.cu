@@ -1,8 +1,7 @@
 // pe_device.cu — the CUDA device behind the pe_device_* C ABI: resident scene upload, the
 // wavefront render loop (RenderDevice::render, src/engine/render_device.h:84-85) and the
 // diagnostics the parity tests call.  Built for sm_100a only.
-#include "photon_cuda.h"
-#include "pe_host.h"
+#include "pe_device_impl.h"
 #include "pe_integrator.cuh"
 
 #include <cuda_runtime.h>
@@ -14,96 +13,9 @@
 #include <vector>
 
 using namespace pe;
+using namespace pe_dev;
 
-namespace {
-
-const char* cudaMsg(cudaError_t e) { return cudaGetErrorString(e); }
-
-#define PE_CUDA(call)                                                                              \
-    do {                                                                                           \
-        const cudaError_t err__ = (call);                                                          \
-        if (err__ != cudaSuccess) {                                                                \
-            setError(std::string(#call) + ": " + cudaMsg(err__));                                  \
-            return err__ == cudaErrorMemoryAllocation ? PE_ERR_OOM : PE_ERR_CUDA;                  \
-        }                                                                                          \
-    } while (0)
-
-struct DevBuf {
-    void* p = nullptr;
-    size_t bytes = 0;
-};
-
-} // namespace
-
-struct pe_device {
-    int ordinal = 0;
-    cudaStream_t stream = nullptr;
-    cudaDeviceProp prop{};
-    // scene
-    std::vector<DevBuf> sceneBufs;
-    SceneGPU scene{};
-    bool hasScene = false;
-    TablesGPU* dTables = nullptr;
-    TablesGPU hTables{};
-    int filterType = -1;
-    float filterWidth = -1.0f;
-    // wavefront state
-    size_t capacity = 0;
-    std::vector<DevBuf> pathBufs;
-    Paths paths{};
-    // [0] nodes, [1] tris (closest), [2] nodes, [3] tris (any), [4] rejected, [5] closest rays,
-    // [6] shadow rays (both of the tail kernel), [7] paths ended at the per-path query bound
-    unsigned long long* dStats = nullptr;
-    uint32_t* hCounters = nullptr;        // pinned
-    // resident film
-    int filmW = 0, filmH = 0;
-    float* fSum = nullptr;
-    uint32_t* fCnt = nullptr;
-    float* fSq = nullptr;
-    // timing
-    cudaEvent_t evStart = nullptr, evStop = nullptr;
-    cudaEvent_t evT0 = nullptr, evT1 = nullptr;
-    std::vector<cudaEvent_t> evPool;
-    bool counting = false;
-    pe_render_stats stats{};
-    int blocksIntersect = 0, blocksShade = 0, blocksShadow = 0, blocksGen = 0, blocksTail = 0;
-    int64_t tailPaths = -1; // -1: one resident grid of the tail kernel; 0: no tail kernel
-    unsigned char* noAllocBase = nullptr; // device address of g_noAllocScratch on this device
-    void* stage = nullptr;                 // pinned staging of the batch film (host-film render)
-    size_t stageBytes = 0;
-    std::string noAllocError;
-};
-
-namespace {
-
-template <typename T>
-int32_t devAlloc(std::vector<DevBuf>& list, T*& out, size_t count) {
-    void* p = nullptr;
-    const size_t bytes = std::max<size_t>(count * sizeof(T), 16);
-    const cudaError_t e = cudaMalloc(&p, bytes);
-    if (e != cudaSuccess) {
-        setError(std::string("cudaMalloc(") + std::to_string(bytes) + "): " + cudaMsg(e));
-        return e == cudaErrorMemoryAllocation ? PE_ERR_OOM : PE_ERR_CUDA;
-    }
-    list.push_back({p, bytes});
-    out = static_cast<T*>(p);
-    return PE_OK;
-}
-
-template <typename T>
-int32_t upload(pe_device* d, std::vector<DevBuf>& list, const T*& dst, const std::vector<T>& src) {
-    T* p = nullptr;
-    const int32_t st = devAlloc(list, p, src.size());
-    if (st) return st;
-    if (!src.empty()) PE_CUDA(cudaMemcpyAsync(p, src.data(), src.size() * sizeof(T), cudaMemcpyHostToDevice, d->stream));
-    dst = p;
-    return PE_OK;
-}
-
-void freeList(std::vector<DevBuf>& list) {
-    for (DevBuf& b : list) cudaFree(b.p);
-    list.clear();
-}
+namespace pe_dev {
 
 int32_t ensureCapacity(pe_device* d, size_t slots) {
     if (slots <= d->capacity) return PE_OK;
@@ -128,13 +40,29 @@ int32_t ensureCapacity(pe_device* d, size_t slots) {
     return PE_OK;
 }
 
-int32_t ensureFilter(pe_device* d, int type, float width) {
-    if (type == d->filterType && width == d->filterWidth) return PE_OK;
-    fillFilterCdf(type, width, d->hTables.filterCdf);
-    PE_CUDA(cudaMemcpyAsync(d->dTables, &d->hTables, sizeof(TablesGPU), cudaMemcpyHostToDevice, d->stream));
-    d->filterType = type;
-    d->filterWidth = width;
-    return PE_OK;
+// Device inverse-CDF table of a pixel filter.  `wave` stamps the slot so that a wave under
+// construction never evicts a table one of its own segments uses.  Returns nullptr when every
+// slot is taken by the current wave.
+const float* filterTable(pe_device* d, int type, float width, uint64_t wave) {
+    int pick = -1;
+    for (int i = 0; i < kFilterSlots; ++i)
+        if (d->filterSlots[i].type == type && d->filterSlots[i].width == width) {
+            d->filterSlots[i].used = wave;
+            return d->dFilters + static_cast<size_t>(i) * (kFilterBins + 1);
+        }
+    for (int i = 0; i < kFilterSlots; ++i) {
+        if (d->filterSlots[i].used == wave) continue;
+        if (pick < 0 || d->filterSlots[i].used < d->filterSlots[pick].used) pick = i;
+    }
+    if (pick < 0) return nullptr;
+    float cdf[kFilterBins + 1];
+    fillFilterCdf(type, width, cdf);
+    // stream-ordered after every wave that read the slot's previous table
+    if (cudaMemcpyAsync(d->dFilters + static_cast<size_t>(pick) * (kFilterBins + 1), cdf, sizeof(cdf),
+                        cudaMemcpyHostToDevice, d->stream) != cudaSuccess)
+        return nullptr;
+    d->filterSlots[pick] = FilterSlot{type, width, wave};
+    return d->dFilters + static_cast<size_t>(pick) * (kFilterBins + 1);
 }
 
 int32_t ensureFilm(pe_device* d, int w, int h) {
@@ -181,8 +109,9 @@ int32_t checkSettings(const pe_camera* cam, const pe_settings* st) {
     return PE_OK;
 }
 
-WaveArgs makeWave(const pe_camera* cam, const pe_settings* st) {
-    WaveArgs A{};
+// A request's render settings as a wave segment (film, rectangle and ranges filled in later).
+WaveSeg makeSeg(const pe_camera* cam, const pe_settings* st) {
+    WaveSeg A{};
     A.cam.position = m3f(cam->position);
     A.cam.lowerLeft = m3f(cam->lower_left);
     A.cam.horizontal = m3f(cam->horizontal);
@@ -198,9 +127,6 @@ WaveArgs makeWave(const pe_camera* cam, const pe_settings* st) {
     return A;
 }
 
-constexpr size_t kWaveSlots = size_t(1) << 21; // paths in flight per wave
-// Bound on the bounce-by-bounce iterations of one wave (closest-hit queries of its longest path).
-constexpr int kMaxWavefrontIterations = kMaxPathQueries;
 
 // Scratch of pe_device_render_tile_noalloc: path-state columns, queues, shadow records and
 // counters for kNoAllocSlots paths, carved out of one file-scope device array (8.5 MB).  Every
@@ -226,134 +152,27 @@ Paths noAllocPaths(unsigned char* base) {
     return P;
 }
 
-struct Tile {
-    int x0, y0, w, h;
-};
+int32_t timerEvent(pe_device* d, RenderTimer& tm, cudaEvent_t& e) {
+    if (tm.evUsed >= d->evPool.size()) {
+        cudaEvent_t ne;
+        PE_CUDA(cudaEventCreate(&ne));
+        d->evPool.push_back(ne);
+    }
+    e = d->evPool[tm.evUsed++];
+    return PE_OK;
+}
 
-// The wavefront render of samples [first, first+count) over `tile` into the film (sum, cnt, sq)
-// on the device, with path state in `P` (room for `capacity` slots).  With `timing` the
-// closest-hit / shade / any-hit launches are bracketed by events (stats.ms_*).
-int32_t renderWaves(pe_device* d, const pe_camera* cam, const pe_settings* st, int first, int count,
-                    const volatile int32_t* cancel, float* sum, uint32_t* cnt, float* sq, Paths& P, size_t capacity,
-                    bool timing, Tile tile) {
-    const size_t npix = static_cast<size_t>(tile.w) * static_cast<size_t>(tile.h);
-    const int pixChunk = static_cast<int>(std::min(npix, capacity));
-    const int samplesPerWave = static_cast<int>(std::max<size_t>(1, std::min<size_t>(static_cast<size_t>(count), capacity / pixChunk)));
-    int32_t rc = ensureFilter(d, st->filter_type, st->filter_width);
-    if (rc) return rc;
-    WaveArgs A = makeWave(cam, st);
-    A.tileX = tile.x0;
-    A.tileY = tile.y0;
-    A.tileW = tile.w;
-    const SceneGPU& S = d->scene;
-    const int sm = d->prop.multiProcessorCount;
-    pe_render_stats& stats = d->stats;
-    std::memset(&stats, 0, sizeof(stats));
+// Starts a render call's statistics and its device clock.
+int32_t beginRender(pe_device* d) {
+    std::memset(&d->stats, 0, sizeof(d->stats));
     PE_CUDA(cudaMemsetAsync(d->dStats, 0, 8 * sizeof(unsigned long long), d->stream));
     PE_CUDA(cudaEventRecord(d->evStart, d->stream));
-    size_t evUsed = 0;
-    auto event = [&](cudaEvent_t& e) -> int32_t {
-        if (evUsed >= d->evPool.size()) {
-            cudaEvent_t ne;
-            PE_CUDA(cudaEventCreate(&ne));
-            d->evPool.push_back(ne);
-        }
-        e = d->evPool[evUsed++];
-        return PE_OK;
-    };
-    std::vector<std::pair<size_t, size_t>> isectEv, shadowEv, shadeEv, tailEv;
-    bool cancelled = false;
-    for (int s0 = first; s0 < first + count && !cancelled; s0 += samplesPerWave) {
-        const int ns = std::min(samplesPerWave, first + count - s0);
-        for (size_t p0 = 0; p0 < npix; p0 += static_cast<size_t>(pixChunk)) {
-            if (cancel && *cancel) {
-                cancelled = true;
-                break;
-            }
-            A.pixelFirst = static_cast<int>(p0);
-            A.nPix = static_cast<int>(std::min<size_t>(static_cast<size_t>(pixChunk), npix - p0));
-            A.sampleFirst = s0;
-            A.nSamples = ns;
-            const int nSlots = A.nPix * ns;
-            kGenerate<<<sm * 8, 256, 0, d->stream>>>(S, P, A, nSlots);
-            ++stats.kernel_launches;
-            ++stats.waves;
-            uint32_t live = static_cast<uint32_t>(nSlots);
-            PE_CUDA(cudaMemsetAsync(&P.counters[1], 0, (CNT_TOTAL - 1) * sizeof(uint32_t), d->stream));
-            PE_CUDA(cudaMemcpyAsync(&P.counters[0], &live, sizeof(uint32_t), cudaMemcpyHostToDevice, d->stream));
-            int32_t* qIn = P.queueA;
-            int32_t* qOut = P.queueB;
-            uint32_t* cIn = &P.counters[0];
-            uint32_t* cOut = &P.counters[1];
-            stats.paths += static_cast<uint64_t>(nSlots);
-            const int64_t tailPaths = d->tailPaths < 0 ? static_cast<int64_t>(d->blocksTail) * 128 : d->tailPaths;
-            for (int iter = 0; live > 0; ++iter) {
-                if (static_cast<int64_t>(live) <= tailPaths) {
-                    // the rest of the wave: one thread per path until it ends
-                    const int grid = static_cast<int>(std::min<int64_t>(d->blocksTail, (static_cast<int64_t>(live) + 127) / 128));
-                    cudaEvent_t t0 = nullptr, t1 = nullptr;
-                    if (timing) {
-                        if ((rc = event(t0)) || (rc = event(t1))) return rc;
-                        PE_CUDA(cudaEventRecord(t0, d->stream));
-                    }
-                    if (d->counting)
-                        kTail<true><<<grid, 128, 0, d->stream>>>(S, P, A, qIn, cIn, d->dStats);
-                    else
-                        kTail<false><<<grid, 128, 0, d->stream>>>(S, P, A, qIn, cIn, d->dStats);
-                    if (timing) {
-                        PE_CUDA(cudaEventRecord(t1, d->stream));
-                        tailEv.push_back({evUsed - 2, evUsed - 1});
-                    }
-                    ++stats.kernel_launches;
-                    stats.tail_paths += live;
-                    break;
-                }
-                stats.closest_rays += live;
-                cudaEvent_t e0 = nullptr, e1 = nullptr, e2 = nullptr, e3 = nullptr;
-                if (timing) {
-                    if ((rc = event(e0)) || (rc = event(e1)) || (rc = event(e2)) || (rc = event(e3))) return rc;
-                    PE_CUDA(cudaEventRecord(e0, d->stream));
-                }
-                if (d->counting)
-                    kIntersect<true><<<d->blocksIntersect, 128, 0, d->stream>>>(S, P, qIn, cIn, d->dStats);
-                else
-                    kIntersect<false><<<d->blocksIntersect, 128, 0, d->stream>>>(S, P, qIn, cIn, d->dStats);
-                if (timing) PE_CUDA(cudaEventRecord(e1, d->stream));
-                kShade<<<d->blocksShade, 128, 0, d->stream>>>(S, P, A, qOut, cOut);
-                if (timing) PE_CUDA(cudaEventRecord(e2, d->stream));
-                if (d->counting)
-                    kShadow<true><<<d->blocksShadow, 128, 0, d->stream>>>(S, P, &P.counters[2], A.clampIndirect, d->dStats);
-                else
-                    kShadow<false><<<d->blocksShadow, 128, 0, d->stream>>>(S, P, &P.counters[2], A.clampIndirect, d->dStats);
-                stats.kernel_launches += 3;
-                ++stats.intersect_launches;
-                if (timing) {
-                    PE_CUDA(cudaEventRecord(e3, d->stream));
-                    isectEv.push_back({evUsed - 4, evUsed - 3});
-                    shadeEv.push_back({evUsed - 3, evUsed - 2});
-                    shadowEv.push_back({evUsed - 2, evUsed - 1});
-                }
-                PE_CUDA(cudaMemcpyAsync(d->hCounters, P.counters, 4 * sizeof(uint32_t), cudaMemcpyDeviceToHost, d->stream));
-                PE_CUDA(cudaStreamSynchronize(d->stream));
-                stats.shadow_rays += d->hCounters[2];
-                live = cOut == &P.counters[1] ? d->hCounters[1] : d->hCounters[0];
-                if (iter > kMaxWavefrontIterations) {
-                    setError("wavefront did not drain after " + std::to_string(kMaxWavefrontIterations) + " iterations");
-                    return PE_ERR_DEVICE;
-                }
-                // swap queues; reset the consumed queue's counter, the shadow counter, the work
-                // cursors and the shading-key bins
-                PE_CUDA(cudaMemsetAsync(cIn, 0, sizeof(uint32_t), d->stream));
-                PE_CUDA(cudaMemsetAsync(&P.counters[CNT_SHADOW], 0, (CNT_KEYS + kShadeKeys - CNT_SHADOW) * sizeof(uint32_t),
-                                        d->stream));
-                std::swap(qIn, qOut);
-                std::swap(cIn, cOut);
-            }
-            kFilm<<<sm * 4, 256, 0, d->stream>>>(P, A, sum, cnt, sq, &d->dStats[4]);
-            ++stats.kernel_launches;
-            PE_CUDA(cudaGetLastError());
-        }
-    }
+    return PE_OK;
+}
+
+// Ends it: waits for the stream, then reads the device counters and per-kernel times.
+int32_t endRender(pe_device* d, const RenderTimer& tm) {
+    pe_render_stats& stats = d->stats;
     PE_CUDA(cudaEventRecord(d->evStop, d->stream));
     unsigned long long hs[8] = {};
     PE_CUDA(cudaMemcpyAsync(hs, d->dStats, sizeof(hs), cudaMemcpyDeviceToHost, d->stream));
@@ -362,26 +181,19 @@ int32_t renderWaves(pe_device* d, const pe_camera* cam, const pe_settings* st, i
     float ms = 0.0f;
     PE_CUDA(cudaEventElapsedTime(&ms, d->evStart, d->evStop));
     stats.ms_total = ms;
-    for (auto& pr : isectEv) {
-        float t = 0.0f;
-        cudaEventElapsedTime(&t, d->evPool[pr.first], d->evPool[pr.second]);
-        stats.ms_intersect += t;
-    }
-    for (auto& pr : shadeEv) {
-        float t = 0.0f;
-        cudaEventElapsedTime(&t, d->evPool[pr.first], d->evPool[pr.second]);
-        stats.ms_shade += t;
-    }
-    for (auto& pr : shadowEv) {
-        float t = 0.0f;
-        cudaEventElapsedTime(&t, d->evPool[pr.first], d->evPool[pr.second]);
-        stats.ms_shadow += t;
-    }
-    for (auto& pr : tailEv) {
-        float t = 0.0f;
-        cudaEventElapsedTime(&t, d->evPool[pr.first], d->evPool[pr.second]);
-        stats.ms_tail += t;
-    }
+    auto sum = [&](const std::vector<std::pair<size_t, size_t>>& v) {
+        float acc = 0.0f;
+        for (const auto& pr : v) {
+            float t = 0.0f;
+            cudaEventElapsedTime(&t, d->evPool[pr.first], d->evPool[pr.second]);
+            acc += t;
+        }
+        return acc;
+    };
+    stats.ms_intersect = sum(tm.isect);
+    stats.ms_shade = sum(tm.shade);
+    stats.ms_shadow = sum(tm.shadow);
+    stats.ms_tail = sum(tm.tail);
     stats.node_visits = hs[0];
     stats.tri_tests = hs[1];
     stats.shadow_node_visits = hs[2];
@@ -389,10 +201,166 @@ int32_t renderWaves(pe_device* d, const pe_camera* cam, const pe_settings* st, i
     stats.rejected = hs[4];
     stats.closest_rays += hs[5];
     stats.shadow_rays += hs[6];
+    stats.tail_closest_rays = hs[5];
+    stats.tail_shadow_rays = hs[6];
     if (hs[7] != 0) {
         setError(std::to_string(hs[7]) + " paths exceeded the per-path query bound and were ended");
         return PE_ERR_DEVICE;
     }
+    return PE_OK;
+}
+
+// The pinned segment table may be rewritten only once the previous wave's upload has run.
+int32_t segsWritable(pe_device* d) {
+    if (d->segsInFlight) {
+        PE_CUDA(cudaEventSynchronize(d->evSegs));
+        d->segsInFlight = false;
+    }
+    return PE_OK;
+}
+
+// One wave over the nSegs segments in d->hSegs (nSlots paths, nPix film pixels): uploads the
+// segment table, generates the camera rays, traces them bounce by bounce (closest hit → shade →
+// any hit) until the live paths fit the tail kernel, which finishes them, and adds every sample
+// to its segment's film in sample order.
+int32_t runWave(pe_device* d, Paths& P, int nSegs, int nSlots, int nPix, RenderTimer& tm) {
+    const SceneGPU& S = d->scene;
+    const int sm = d->prop.multiProcessorCount;
+    pe_render_stats& stats = d->stats;
+    int32_t rc = PE_OK;
+    PE_CUDA(cudaMemcpyAsync(d->dSegs, d->hSegs, static_cast<size_t>(nSegs) * sizeof(WaveSeg), cudaMemcpyHostToDevice,
+                            d->stream));
+    PE_CUDA(cudaEventRecord(d->evSegs, d->stream));
+    d->segsInFlight = true;
+    const Wave W{d->dSegs, nSegs, nSlots, nPix};
+    kGenerate<<<sm * 8, 256, 0, d->stream>>>(S, P, W);
+    ++stats.kernel_launches;
+    ++stats.waves;
+    uint32_t live = static_cast<uint32_t>(nSlots);
+    PE_CUDA(cudaMemsetAsync(&P.counters[1], 0, (CNT_TOTAL - 1) * sizeof(uint32_t), d->stream));
+    PE_CUDA(cudaMemcpyAsync(&P.counters[0], &live, sizeof(uint32_t), cudaMemcpyHostToDevice, d->stream));
+    int32_t* qIn = P.queueA;
+    int32_t* qOut = P.queueB;
+    uint32_t* cIn = &P.counters[0];
+    uint32_t* cOut = &P.counters[1];
+    stats.paths += static_cast<uint64_t>(nSlots);
+    const int64_t tailPaths = d->tailPaths < 0 ? static_cast<int64_t>(d->blocksTail) * 128 : d->tailPaths;
+    for (int iter = 0; live > 0; ++iter) {
+        if (static_cast<int64_t>(live) <= tailPaths) {
+            // the rest of the wave: one thread per path until it ends
+            const int grid = static_cast<int>(std::min<int64_t>(d->blocksTail, (static_cast<int64_t>(live) + 127) / 128));
+            cudaEvent_t t0 = nullptr, t1 = nullptr;
+            if (tm.timing) {
+                if ((rc = timerEvent(d, tm, t0)) || (rc = timerEvent(d, tm, t1))) return rc;
+                PE_CUDA(cudaEventRecord(t0, d->stream));
+            }
+            if (d->counting)
+                kTail<true><<<grid, 128, 0, d->stream>>>(S, P, W, qIn, cIn, d->dStats);
+            else
+                kTail<false><<<grid, 128, 0, d->stream>>>(S, P, W, qIn, cIn, d->dStats);
+            if (tm.timing) {
+                PE_CUDA(cudaEventRecord(t1, d->stream));
+                tm.tail.push_back({tm.evUsed - 2, tm.evUsed - 1});
+            }
+            ++stats.kernel_launches;
+            stats.tail_paths += live;
+            break;
+        }
+        stats.closest_rays += live;
+        cudaEvent_t e0 = nullptr, e1 = nullptr, e2 = nullptr, e3 = nullptr;
+        if (tm.timing) {
+            if ((rc = timerEvent(d, tm, e0)) || (rc = timerEvent(d, tm, e1)) || (rc = timerEvent(d, tm, e2)) ||
+                (rc = timerEvent(d, tm, e3)))
+                return rc;
+            PE_CUDA(cudaEventRecord(e0, d->stream));
+        }
+        if (d->counting)
+            kIntersect<true><<<d->blocksIntersect, 128, 0, d->stream>>>(S, P, qIn, cIn, d->dStats);
+        else
+            kIntersect<false><<<d->blocksIntersect, 128, 0, d->stream>>>(S, P, qIn, cIn, d->dStats);
+        if (tm.timing) PE_CUDA(cudaEventRecord(e1, d->stream));
+        kShade<<<d->blocksShade, 128, 0, d->stream>>>(S, P, W, qOut, cOut);
+        if (tm.timing) PE_CUDA(cudaEventRecord(e2, d->stream));
+        if (d->counting)
+            kShadow<true><<<d->blocksShadow, 128, 0, d->stream>>>(S, P, &P.counters[CNT_SHADOW], d->dStats);
+        else
+            kShadow<false><<<d->blocksShadow, 128, 0, d->stream>>>(S, P, &P.counters[CNT_SHADOW], d->dStats);
+        stats.kernel_launches += 3;
+        ++stats.intersect_launches;
+        if (tm.timing) {
+            PE_CUDA(cudaEventRecord(e3, d->stream));
+            tm.isect.push_back({tm.evUsed - 4, tm.evUsed - 3});
+            tm.shade.push_back({tm.evUsed - 3, tm.evUsed - 2});
+            tm.shadow.push_back({tm.evUsed - 2, tm.evUsed - 1});
+        }
+        PE_CUDA(cudaMemcpyAsync(d->hCounters, P.counters, 4 * sizeof(uint32_t), cudaMemcpyDeviceToHost, d->stream));
+        PE_CUDA(cudaStreamSynchronize(d->stream));
+        stats.shadow_rays += d->hCounters[CNT_SHADOW];
+        live = cOut == &P.counters[1] ? d->hCounters[1] : d->hCounters[0];
+        if (iter > kMaxWavefrontIterations) {
+            setError("wavefront did not drain after " + std::to_string(kMaxWavefrontIterations) + " iterations");
+            return PE_ERR_DEVICE;
+        }
+        // swap queues; reset the consumed queue's counter, the shadow counter, the work
+        // cursors and the shading-key bins
+        PE_CUDA(cudaMemsetAsync(cIn, 0, sizeof(uint32_t), d->stream));
+        PE_CUDA(cudaMemsetAsync(&P.counters[CNT_SHADOW], 0, (CNT_KEYS + kShadeKeys - CNT_SHADOW) * sizeof(uint32_t),
+                                d->stream));
+        std::swap(qIn, qOut);
+        std::swap(cIn, cOut);
+    }
+    kFilm<<<sm * 4, 256, 0, d->stream>>>(P, W, &d->dStats[4]);
+    ++stats.kernel_launches;
+    PE_CUDA(cudaGetLastError());
+    return PE_OK;
+}
+
+// The wavefront render of samples [first, first+count) over `tile` into the film (sum, cnt, sq)
+// on the device, with path state in `P` (room for `capacity` slots): waves of one segment each.
+// With `timing` the closest-hit / shade / any-hit / tail launches are bracketed by events.
+int32_t renderWaves(pe_device* d, const pe_camera* cam, const pe_settings* st, int first, int count,
+                    const volatile int32_t* cancel, float* sum, uint32_t* cnt, float* sq, Paths& P, size_t capacity,
+                    bool timing, Tile tile) {
+    const size_t npix = static_cast<size_t>(tile.w) * static_cast<size_t>(tile.h);
+    const int pixChunk = static_cast<int>(std::min(npix, capacity));
+    const int samplesPerWave = static_cast<int>(std::max<size_t>(1, std::min<size_t>(static_cast<size_t>(count), capacity / pixChunk)));
+    int32_t rc = beginRender(d);
+    if (rc) return rc;
+    WaveSeg base = makeSeg(cam, st);
+    base.filterCdf = filterTable(d, st->filter_type, st->filter_width, ++d->filterClock);
+    if (!base.filterCdf) {
+        setError("pixel filter table upload failed");
+        return PE_ERR_CUDA;
+    }
+    base.tileX = tile.x0;
+    base.tileY = tile.y0;
+    base.tileW = tile.w;
+    base.sum = sum;
+    base.cnt = cnt;
+    base.sq = sq;
+    RenderTimer tm;
+    tm.timing = timing;
+    bool cancelled = false;
+    for (int s0 = first; s0 < first + count && !cancelled; s0 += samplesPerWave) {
+        const int ns = std::min(samplesPerWave, first + count - s0);
+        for (size_t p0 = 0; p0 < npix; p0 += static_cast<size_t>(pixChunk)) {
+            if (cancel && *cancel) {
+                cancelled = true;
+                break;
+            }
+            if ((rc = segsWritable(d))) return rc;
+            WaveSeg& seg = d->hSegs[0];
+            seg = base;
+            seg.pixelFirst = static_cast<int>(p0);
+            seg.nPix = static_cast<int>(std::min<size_t>(static_cast<size_t>(pixChunk), npix - p0));
+            seg.sampleFirst = s0;
+            seg.nSamples = ns;
+            seg.slotFirst = 0;
+            seg.pixFirst = 0;
+            if ((rc = runWave(d, P, 1, seg.nPix * ns, seg.nPix, tm))) return rc;
+        }
+    }
+    if ((rc = endRender(d, tm))) return rc;
     if (cancelled) {
         setError("render cancelled");
         return PE_ERR_CANCELLED;
@@ -400,7 +368,7 @@ int32_t renderWaves(pe_device* d, const pe_camera* cam, const pe_settings* st, i
     return PE_OK;
 }
 
-__global__ void kTracePrimary(SceneGPU S, WaveArgs A, int nPix, int32_t* outShape, int32_t* outPrim, float* outT) {
+__global__ void kTracePrimary(SceneGPU S, WaveSeg A, int nPix, int32_t* outShape, int32_t* outPrim, float* outT) {
     for (int pix = blockIdx.x * blockDim.x + threadIdx.x; pix < nPix; pix += gridDim.x * blockDim.x) {
         const int x = pix % A.width, y = pix / A.width;
         Sobol sb;
@@ -408,7 +376,7 @@ __global__ void kTracePrimary(SceneGPU S, WaveArgs A, int nPix, int32_t* outShap
         sb.revIndex = rev32(static_cast<uint32_t>(A.sampleFirst));
         sb.dim = 0;
         V3 o, d;
-        cameraRay(S.tables, A.cam, A.filterWidth, x, y, A.width, A.height, sb, o, d);
+        cameraRay(S.tables, A.filterCdf, A.cam, A.filterWidth, x, y, A.width, A.height, sb, o, d);
         uint32_t a = 0, b = 0;
         const Hit h = traceClosest<false>(S, o, d, VIS_CAMERA, 0.0f, 1e30f, a, b);
         if (h.prim < 0) {
@@ -483,9 +451,77 @@ __global__ void kBsdfProbe(SceneGPU S, int material, const pe_bsdf_query* q, int
     }
 }
 
-} // namespace
+} // namespace pe_dev
+
+namespace pe_dev {
+
+int32_t uploadScene(pe_device* d, const pe_scene* s, SceneGPU& G, std::vector<DevBuf>& bufs) {
+    G = SceneGPU{};
+    const HostBuild& B = s->build;
+    int32_t rc = 0;
+    if ((rc = upload(d, bufs, G.nodes, B.nodes)) || (rc = upload(d, bufs, G.tris, B.tris)) ||
+        (rc = upload(d, bufs, G.triVerts, B.triVerts)) || (rc = upload(d, bufs, G.pos, B.pos)) ||
+        (rc = upload(d, bufs, G.nrm, B.nrm)) || (rc = upload(d, bufs, G.uv, B.uv)) ||
+        (rc = upload(d, bufs, G.shapes, B.shapes)) || (rc = upload(d, bufs, G.materials, B.materials)) ||
+        (rc = upload(d, bufs, G.lights, B.lights)) || (rc = upload(d, bufs, G.lightNodes, B.lightNodes)) ||
+        (rc = upload(d, bufs, G.topSlot, B.topSlot)) || (rc = upload(d, bufs, G.trail, B.trail)) ||
+        (rc = upload(d, bufs, G.trailDepth, B.trailDepth)))
+        return rc;
+    G.rootIsLeaf = B.rootIsLeaf;
+    G.rootFirst = B.rootFirst;
+    G.rootCount = B.rootCount;
+    G.nNodes = static_cast<int32_t>(B.nodes.size() / 4);
+    for (int i = 0; i < 3; ++i) {
+        G.rootMin[i] = B.rootMin[i];
+        G.rootMax[i] = B.rootMax[i];
+    }
+    G.nTris = static_cast<uint32_t>(B.triVerts.size());
+    G.nShapes = static_cast<int32_t>(B.shapes.size());
+    G.nLights = static_cast<int32_t>(B.lights.size());
+    G.lightMode = B.lightMode;
+    G.lightCount = B.lightCount;
+    G.nInfinite = static_cast<int32_t>(B.infinite.size());
+    for (size_t i = 0; i < B.infinite.size() && i < static_cast<size_t>(kMaxInfinite); ++i) G.infinite[i] = B.infinite[i];
+    G.nLightNodes = static_cast<int32_t>(B.lightNodes.size());
+    // environment (the MIS-compensated distribution drives sampling and pdfLi)
+    const HostEnv& e = s->env;
+    EnvGPU& E = G.env;
+    E.present = e.present ? 1 : 0;
+    E.width = e.width;
+    E.height = e.height;
+    E.hasImage = e.hasImage ? 1 : 0;
+    E.rotation = e.rotation;
+    E.intensity = e.intensity;
+    E.meanLuminance = e.meanLuminance;
+    E.sunPdfWeight = e.sunPdfWeight;
+    E.sunDir[0] = e.sunDir.x;
+    E.sunDir[1] = e.sunDir.y;
+    E.sunDir[2] = e.sunDir.z;
+    E.sunCosMax = e.sunCosMax;
+    E.sunRadiance[0] = e.sunRadiance.x;
+    E.sunRadiance[1] = e.sunRadiance.y;
+    E.sunRadiance[2] = e.sunRadiance.z;
+    E.funcInt = e.misInt;
+    E.valid = e.misValid ? 1 : 0;
+    if ((rc = upload(d, bufs, E.image, e.image)) || (rc = upload(d, bufs, E.func, e.misFunc)) ||
+        (rc = upload(d, bufs, E.marginalCdf, e.misMarg)) || (rc = upload(d, bufs, E.condCdf, e.misCond)))
+        return rc;
+    G.tables = d->dTables;
+    G.bgMode = s->bgMode;
+    for (int i = 0; i < 3; ++i) G.bgColor[i] = s->bgColor[i];
+    G.hasShadowTransmitters = B.hasShadowTransmitters ? 1 : 0;
+    G.hasVolumes = B.hasVolumes ? 1 : 0;
+    G.hasSubsurface = B.hasSubsurface ? 1 : 0;
+    G.exitMaterial = B.exitMaterial;
+    PE_CUDA(cudaStreamSynchronize(d->stream));
+    return PE_OK;
+}
+
+
+} // namespace pe_dev
 
 extern "C" {
+
 
 int32_t pe_device_count(void) {
     int n = 0;
@@ -515,22 +551,24 @@ pe_device* pe_device_create(int32_t ordinal, char* err, size_t errLen) {
     }
     cudaGetDeviceProperties(&d->prop, ordinal);
     if (d->prop.major < 10) {
+        const std::string msg = "device " + std::string(d->prop.name) + " is not sm_100 class; this build targets sm_100a only";
         delete d;
-        return fail("device " + std::string(d->prop.name) + " is not sm_100 class; this build targets sm_100a only");
+        return fail(msg);
     }
     if (cudaStreamCreateWithFlags(&d->stream, cudaStreamNonBlocking) != cudaSuccess ||
         cudaEventCreate(&d->evStart) != cudaSuccess || cudaEventCreate(&d->evStop) != cudaSuccess ||
         cudaEventCreate(&d->evT0) != cudaSuccess || cudaEventCreate(&d->evT1) != cudaSuccess ||
         cudaMalloc(&d->dTables, sizeof(TablesGPU)) != cudaSuccess ||
         cudaMalloc(&d->dStats, 8 * sizeof(unsigned long long)) != cudaSuccess ||
-        cudaMallocHost(&d->hCounters, 16 * sizeof(uint32_t)) != cudaSuccess) {
+        cudaMallocHost(&d->hCounters, 16 * sizeof(uint32_t)) != cudaSuccess ||
+        cudaMalloc(&d->dFilters, static_cast<size_t>(kFilterSlots) * (kFilterBins + 1) * sizeof(float)) != cudaSuccess ||
+        cudaMalloc(&d->dSegs, kMaxSegs * sizeof(WaveSeg)) != cudaSuccess ||
+        cudaMallocHost(&d->hSegs, kMaxSegs * sizeof(WaveSeg)) != cudaSuccess ||
+        cudaEventCreateWithFlags(&d->evSegs, cudaEventDisableTiming) != cudaSuccess) {
         pe_device_destroy(d);
         return fail("device initialisation failed");
     }
     d->hTables = staticTables();
-    fillFilterCdf(PE_FILTER_BOX, 1.0f, d->hTables.filterCdf);
-    d->filterType = PE_FILTER_BOX;
-    d->filterWidth = 1.0f;
     cudaMemcpy(d->dTables, &d->hTables, sizeof(TablesGPU), cudaMemcpyHostToDevice);
     int b = 0;
     const int sm = d->prop.multiProcessorCount;
@@ -569,6 +607,10 @@ void pe_device_destroy(pe_device* d) {
     cudaFree(d->fSq);
     cudaFree(d->dTables);
     cudaFree(d->dStats);
+    cudaFree(d->dFilters);
+    cudaFree(d->dSegs);
+    if (d->hSegs) cudaFreeHost(d->hSegs);
+    if (d->evSegs) cudaEventDestroy(d->evSegs);
     if (d->hCounters) cudaFreeHost(d->hCounters);
     if (d->stage) cudaFreeHost(d->stage);
     for (cudaEvent_t e : d->evPool) cudaEventDestroy(e);
@@ -609,64 +651,9 @@ int32_t pe_device_set_scene(pe_device* d, const pe_scene* s) {
     PE_CUDA(cudaStreamSynchronize(d->stream));
     freeList(d->sceneBufs);
     d->hasScene = false;
-    const HostBuild& B = s->build;
     SceneGPU G{};
-    int32_t rc = 0;
-    if ((rc = upload(d, d->sceneBufs, G.nodes, B.nodes)) || (rc = upload(d, d->sceneBufs, G.tris, B.tris)) ||
-        (rc = upload(d, d->sceneBufs, G.triVerts, B.triVerts)) || (rc = upload(d, d->sceneBufs, G.pos, B.pos)) ||
-        (rc = upload(d, d->sceneBufs, G.nrm, B.nrm)) || (rc = upload(d, d->sceneBufs, G.uv, B.uv)) ||
-        (rc = upload(d, d->sceneBufs, G.shapes, B.shapes)) || (rc = upload(d, d->sceneBufs, G.materials, B.materials)) ||
-        (rc = upload(d, d->sceneBufs, G.lights, B.lights)) || (rc = upload(d, d->sceneBufs, G.lightNodes, B.lightNodes)) ||
-        (rc = upload(d, d->sceneBufs, G.topSlot, B.topSlot)) || (rc = upload(d, d->sceneBufs, G.trail, B.trail)) ||
-        (rc = upload(d, d->sceneBufs, G.trailDepth, B.trailDepth)))
-        return rc;
-    G.rootIsLeaf = B.rootIsLeaf;
-    G.rootFirst = B.rootFirst;
-    G.rootCount = B.rootCount;
-    G.nNodes = static_cast<int32_t>(B.nodes.size() / 4);
-    for (int i = 0; i < 3; ++i) {
-        G.rootMin[i] = B.rootMin[i];
-        G.rootMax[i] = B.rootMax[i];
-    }
-    G.nTris = static_cast<uint32_t>(B.triVerts.size());
-    G.nShapes = static_cast<int32_t>(B.shapes.size());
-    G.nLights = static_cast<int32_t>(B.lights.size());
-    G.lightMode = B.lightMode;
-    G.lightCount = B.lightCount;
-    G.nInfinite = static_cast<int32_t>(B.infinite.size());
-    for (size_t i = 0; i < B.infinite.size() && i < static_cast<size_t>(kMaxInfinite); ++i) G.infinite[i] = B.infinite[i];
-    G.nLightNodes = static_cast<int32_t>(B.lightNodes.size());
-    // environment (the MIS-compensated distribution drives sampling and pdfLi)
-    const HostEnv& e = s->env;
-    EnvGPU& E = G.env;
-    E.present = e.present ? 1 : 0;
-    E.width = e.width;
-    E.height = e.height;
-    E.hasImage = e.hasImage ? 1 : 0;
-    E.rotation = e.rotation;
-    E.intensity = e.intensity;
-    E.meanLuminance = e.meanLuminance;
-    E.sunPdfWeight = e.sunPdfWeight;
-    E.sunDir[0] = e.sunDir.x;
-    E.sunDir[1] = e.sunDir.y;
-    E.sunDir[2] = e.sunDir.z;
-    E.sunCosMax = e.sunCosMax;
-    E.sunRadiance[0] = e.sunRadiance.x;
-    E.sunRadiance[1] = e.sunRadiance.y;
-    E.sunRadiance[2] = e.sunRadiance.z;
-    E.funcInt = e.misInt;
-    E.valid = e.misValid ? 1 : 0;
-    if ((rc = upload(d, d->sceneBufs, E.image, e.image)) || (rc = upload(d, d->sceneBufs, E.func, e.misFunc)) ||
-        (rc = upload(d, d->sceneBufs, E.marginalCdf, e.misMarg)) || (rc = upload(d, d->sceneBufs, E.condCdf, e.misCond)))
-        return rc;
-    G.tables = d->dTables;
-    G.bgMode = s->bgMode;
-    for (int i = 0; i < 3; ++i) G.bgColor[i] = s->bgColor[i];
-    G.hasShadowTransmitters = B.hasShadowTransmitters ? 1 : 0;
-    G.hasVolumes = B.hasVolumes ? 1 : 0;
-    G.hasSubsurface = B.hasSubsurface ? 1 : 0;
-    G.exitMaterial = B.exitMaterial;
-    PE_CUDA(cudaStreamSynchronize(d->stream));
+    const int32_t rc = uploadScene(d, s, G, d->sceneBufs);
+    if (rc) return rc;
     d->scene = G;
     d->hasScene = true;
     return PE_OK;
@@ -894,8 +881,12 @@ int32_t pe_device_trace_primary(pe_device* d, const pe_camera* cam, const pe_set
     int32_t rc = checkSettings(cam, st);
     if (rc) return rc;
     PE_CUDA(cudaSetDevice(d->ordinal));
-    if ((rc = ensureFilter(d, st->filter_type, st->filter_width))) return rc;
-    WaveArgs A = makeWave(cam, st);
+    WaveSeg A = makeSeg(cam, st);
+    A.filterCdf = filterTable(d, st->filter_type, st->filter_width, ++d->filterClock);
+    if (!A.filterCdf) {
+        setError("pixel filter table upload failed");
+        return PE_ERR_CUDA;
+    }
     A.sampleFirst = sampleIndex;
     const int n = st->width * st->height;
     std::vector<DevBuf> tmp;

@@ -1,0 +1,157 @@
+// pe_device_impl.h — the device object behind the pe_device_* C ABI and the wave machinery the
+// single-request render path and the request server share (definitions in pe_device.cu).
+#pragma once
+
+#include "photon_cuda.h"
+#include "pe_host.h"
+#include "pe_wave.h"
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <string>
+#include <utility>
+#include <vector>
+
+namespace pe_dev {
+
+using namespace pe;
+
+inline const char* cudaMsg(cudaError_t e) { return cudaGetErrorString(e); }
+
+#define PE_CUDA(call)                                                                              \
+    do {                                                                                           \
+        const cudaError_t err__ = (call);                                                          \
+        if (err__ != cudaSuccess) {                                                                \
+            ::pe::setError(std::string(#call) + ": " + ::pe_dev::cudaMsg(err__));                  \
+            return err__ == cudaErrorMemoryAllocation ? PE_ERR_OOM : PE_ERR_CUDA;                  \
+        }                                                                                          \
+    } while (0)
+
+struct DevBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+};
+
+constexpr int kFilterSlots = 16;
+constexpr int kMaxSegs = 64;                    // requests sharing one wave
+constexpr size_t kWaveSlots = size_t(1) << 21;  // paths in flight per wave
+// Bound on the bounce-by-bounce iterations of one wave (closest-hit queries of its longest path).
+constexpr int kMaxWavefrontIterations = kMaxPathQueries;
+
+struct FilterSlot {
+    int type = -1;
+    float width = -1.0f;
+    uint64_t used = 0;
+};
+
+struct Tile {
+    int x0, y0, w, h;
+};
+
+// Event bookkeeping of one render call: per-kernel device times when timing.
+struct RenderTimer {
+    bool timing = false;
+    size_t evUsed = 0;
+    std::vector<std::pair<size_t, size_t>> isect, shade, shadow, tail;
+};
+
+} // namespace pe_dev
+
+// One CUDA device: stream, resident scene, wave buffers, films and counters.
+struct pe_device {
+    using DevBuf = pe_dev::DevBuf;
+    using FilterSlot = pe_dev::FilterSlot;
+    using SceneGPU = pe::SceneGPU;
+    using TablesGPU = pe::TablesGPU;
+    using WaveSeg = pe::WaveSeg;
+    using Paths = pe::Paths;
+    int ordinal = 0;
+    cudaStream_t stream = nullptr;
+    cudaDeviceProp prop{};
+    // scene
+    std::vector<DevBuf> sceneBufs;
+    SceneGPU scene{};
+    bool hasScene = false;
+    TablesGPU* dTables = nullptr;
+    TablesGPU hTables{};
+    // pixel-filter inverse CDFs, one slot per (type, width) in use, least recently used replaced
+    float* dFilters = nullptr;
+    FilterSlot filterSlots[pe_dev::kFilterSlots];
+    uint64_t filterClock = 0;
+    // segment table of the wave being traced (pinned host copy, device copy)
+    WaveSeg* hSegs = nullptr;
+    WaveSeg* dSegs = nullptr;
+    cudaEvent_t evSegs = nullptr;
+    bool segsInFlight = false;
+    // wavefront state
+    size_t capacity = 0;
+    std::vector<DevBuf> pathBufs;
+    Paths paths{};
+    // [0] nodes, [1] tris (closest), [2] nodes, [3] tris (any), [4] rejected, [5] closest rays,
+    // [6] shadow rays (both of the tail kernel), [7] paths ended at the per-path query bound
+    unsigned long long* dStats = nullptr;
+    uint32_t* hCounters = nullptr;        // pinned
+    // resident film
+    int filmW = 0, filmH = 0;
+    float* fSum = nullptr;
+    uint32_t* fCnt = nullptr;
+    float* fSq = nullptr;
+    // timing
+    cudaEvent_t evStart = nullptr, evStop = nullptr;
+    cudaEvent_t evT0 = nullptr, evT1 = nullptr;
+    std::vector<cudaEvent_t> evPool;
+    bool counting = false;
+    pe_render_stats stats{};
+    int blocksIntersect = 0, blocksShade = 0, blocksShadow = 0, blocksGen = 0, blocksTail = 0;
+    int64_t tailPaths = -1; // -1: one resident grid of the tail kernel; 0: no tail kernel
+    unsigned char* noAllocBase = nullptr; // device address of g_noAllocScratch on this device
+    void* stage = nullptr;                 // pinned staging of the batch film (host-film render)
+    size_t stageBytes = 0;
+    std::string noAllocError;
+};
+
+
+namespace pe_dev {
+
+template <typename T>
+int32_t devAlloc(std::vector<DevBuf>& list, T*& out, size_t count) {
+    void* p = nullptr;
+    const size_t bytes = std::max<size_t>(count * sizeof(T), 16);
+    const cudaError_t e = cudaMalloc(&p, bytes);
+    if (e != cudaSuccess) {
+        setError(std::string("cudaMalloc(") + std::to_string(bytes) + "): " + cudaMsg(e));
+        return e == cudaErrorMemoryAllocation ? PE_ERR_OOM : PE_ERR_CUDA;
+    }
+    list.push_back({p, bytes});
+    out = static_cast<T*>(p);
+    return PE_OK;
+}
+
+template <typename T>
+int32_t upload(pe_device* d, std::vector<DevBuf>& list, const T*& dst, const std::vector<T>& src) {
+    T* p = nullptr;
+    const int32_t st = devAlloc(list, p, src.size());
+    if (st) return st;
+    if (!src.empty()) PE_CUDA(cudaMemcpyAsync(p, src.data(), src.size() * sizeof(T), cudaMemcpyHostToDevice, d->stream));
+    dst = p;
+    return PE_OK;
+}
+
+inline void freeList(std::vector<DevBuf>& list) {
+    for (DevBuf& b : list) cudaFree(b.p);
+    list.clear();
+}
+
+int32_t ensureCapacity(pe_device* d, size_t slots);
+int32_t checkSettings(const pe_camera* cam, const pe_settings* st);
+WaveSeg makeSeg(const pe_camera* cam, const pe_settings* st);
+const float* filterTable(pe_device* d, int type, float width, uint64_t wave);
+int32_t segsWritable(pe_device* d);
+int32_t beginRender(pe_device* d);
+int32_t endRender(pe_device* d, const RenderTimer& tm);
+int32_t runWave(pe_device* d, Paths& P, int nSegs, int nSlots, int nPix, RenderTimer& tm);
+// Uploads a built scene into device buffers owned by `bufs`; `out` gets their device view.
+int32_t uploadScene(pe_device* d, const pe_scene* s, SceneGPU& out, std::vector<DevBuf>& bufs);
+
+} // namespace pe_dev

@@ -14,61 +14,9 @@
 #include "pe_light.h"
 #include "pe_medium.h"
 #include "pe_trace.cuh"
+#include "pe_wave.h"
 
 namespace pe {
-
-enum VisMask : uint32_t { VIS_CAMERA = 1u, VIS_DIFFUSE = 2u, VIS_GLOSSY = 4u, VIS_TRANSMISSION = 8u, VIS_SHADOW = 16u,
-                          VIS_ALL = 0x1Fu };
-// Marks a random-walk ray in the ray's mask word.  Triangle masks never carry it, so it does
-// not change what the ray can hit; the closest-hit kernel bins such rays under their own key.
-constexpr uint32_t RAY_WALK = 1u << 31;
-constexpr int kMaxMediumEvents = 1024; // path_tracer.cpp:51
-constexpr int kMaxWalkSteps = 256;     // path_tracer.cpp:52
-// Closest-hit queries one path can make: at most 255 bounces, each preceded by up to 64 skipped
-// camera-invisible hits and 65 pass-throughs and followed by up to 256 walk steps, plus 1025
-// medium events, stays below this; a path that reaches it is counted as an error and ended.
-constexpr int kMaxPathQueries = 1 << 17;
-
-// path flags (bits of state word)
-enum PathFlags : uint32_t {
-    PF_SPECULAR_BOUNCE = 1u << 0,
-    PF_CAMERA_RAY = 1u << 1,
-    PF_PICKER_VALID = 1u << 2,
-    PF_FIRST_SEGMENT = 1u << 3,
-    PF_WALK = 1u << 4,   // inside a random walk: lastP = σt, lastN = albedo, pickP.x = g
-};
-
-// Per-slot state columns (capacity P slots).
-struct Paths {
-    float4* rayO;    // origin xyz, visibility mask (bits)
-    float4* rayD;    // direction xyz, lastBsdfPdf
-    float4* thr;     // throughput xyz, wavelength
-    float4* L;       // radiance xyz, unused
-    float4* lastN;   // last shading normal xyz, flags (bits)
-    float4* lastP;   // last point xyz, Sobol dimension (bits)
-    float4* pickP;   // light-picker point xyz, pixel hash (bits)
-    float4* pickN;   // light-picker normal xyz, counters (bits: depth | diffuseBounces<<8 | passThroughs<<16 | skips<<24)
-    float4* hit;     // t, u, v, leaf prim (bits)
-    float4* med;     // media stack slots 0,1 | slots 2,3 (bits), mediumEvents | walkStep<<16, stack depth
-    int32_t* queueA;
-    int32_t* queueB;
-    int32_t* shadowQ;
-    float4* shO;     // shadow origin xyz, tMax
-    float4* shD;     // shadow direction xyz, scalar (cos*w/(pdf*n))
-    float4* shC;     // f*Li xyz, flags (bit0: indirect)
-    float4* shT;     // throughput at NEE xyz
-    int32_t* sortQ;  // kShadeKeys segments of `capacity` slots: rays binned by shading key
-    uint32_t capacity;
-    // [0] queue A count, [1] queue B count, [2] shadow count, [3] closest-hit work cursor,
-    // [4] any-hit work cursor, [5] shade work cursor, [6..11] rays per shading key, [12] errors,
-    // [13] tail work cursor
-    uint32_t* counters;
-};
-
-// Shading keys: 0 = miss, 1 + material type (Lambert, Disney, Dielectric, Mirror), 5 = random-walk step.
-constexpr int kShadeKeys = 6;
-enum CounterSlots { CNT_QA = 0, CNT_QB = 1, CNT_SHADOW = 2, CNT_WORK_ISECT = 3, CNT_WORK_SHADOW = 4,
-                    CNT_WORK_SHADE = 5, CNT_KEYS = 6, CNT_ERRORS = 12, CNT_WORK_TAIL = 13, CNT_TOTAL = 16 };
 
 // Persistent-warp work distribution: lane 0 claims the next 32 items for its warp.
 __device__ __forceinline__ int warpFetch(uint32_t* cursor) {
@@ -77,17 +25,25 @@ __device__ __forceinline__ int warpFetch(uint32_t* cursor) {
     return __shfl_sync(0xffffffffu, base, 0);
 }
 
-struct WaveArgs {
-    CamDev cam;
-    int width, height;
-    int tileX, tileY, tileW; // rendered rectangle of the film (whole frame: 0, 0, width)
-    int pixelFirst, nPix;   // range of tile-linear pixel indices of this wave
-    int sampleFirst, nSamples;
-    uint64_t seed;
-    float filterWidth;
-    int maxDepth, rrDepth, shadowSamples;
-    float clampIndirect;
-};
+// Segment owning a wave slot / a wave pixel (binary search; one segment for a lone request).
+__device__ __forceinline__ int segOfSlot(const Wave& W, int slot) {
+    int lo = 0, hi = W.nSegs - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (W.segs[mid].slotFirst <= slot) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+__device__ __forceinline__ int segOfPixel(const Wave& W, int p) {
+    int lo = 0, hi = W.nSegs - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (W.segs[mid].pixFirst <= p) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
 
 __device__ __forceinline__ uint32_t packCounters(int depth, int diffuse, int pass, int skips) {
     return static_cast<uint32_t>(depth) | (static_cast<uint32_t>(diffuse) << 8) | (static_cast<uint32_t>(pass) << 16) |
@@ -108,18 +64,20 @@ __device__ __forceinline__ void queuePush(int32_t* queue, uint32_t* counter, boo
 }
 
 // ---- generate: camera rays for every slot of the wave ------------------------------------------
-__global__ void kGenerate(SceneGPU S, Paths P, WaveArgs A, int nSlots) {
+__global__ void kGenerate(SceneGPU S, Paths P, Wave W) {
     const TablesGPU* T = S.tables;
-    for (int slot = blockIdx.x * blockDim.x + threadIdx.x; slot < nSlots; slot += gridDim.x * blockDim.x) {
-        const int sOff = slot / A.nPix;
-        const int pix = A.pixelFirst + (slot - sOff * A.nPix);
+    for (int slot = blockIdx.x * blockDim.x + threadIdx.x; slot < W.nSlots; slot += gridDim.x * blockDim.x) {
+        const WaveSeg& A = W.segs[segOfSlot(W, slot)];
+        const int local = slot - A.slotFirst;
+        const int sOff = local / A.nPix;
+        const int pix = A.pixelFirst + (local - sOff * A.nPix);
         const int x = A.tileX + pix % A.tileW, y = A.tileY + pix / A.tileW;
         Sobol sb;
         sb.pixelHash = pixelHashOf(A.seed, x, y);
         sb.revIndex = rev32(static_cast<uint32_t>(A.sampleFirst + sOff));
         sb.dim = 0;
         V3 o, d;
-        cameraRay(T, A.cam, A.filterWidth, x, y, A.width, A.height, sb, o, d);
+        cameraRay(T, A.filterCdf, A.cam, A.filterWidth, x, y, A.width, A.height, sb, o, d);
         P.rayO[slot] = make_float4(o.x, o.y, o.z, __uint_as_float(VIS_CAMERA));
         P.rayD[slot] = make_float4(d.x, d.y, d.z, 0.0f);
         P.thr[slot] = make_float4(1.0f, 1.0f, 1.0f, 0.0f);
@@ -174,10 +132,57 @@ __global__ void __launch_bounds__(128) kIntersect(SceneGPU S, Paths P, const int
     }
 }
 
-// An unoccluded NEE sample's term: throughput × f·Li·vis·(cos·w / (lightPdf·n)) with vis = 1,
-// clamped when indirect (path_tracer.cpp:683-690).
-__device__ __forceinline__ V3 neeTerm(V3 fLi, float scalar, V3 thr, bool indirect, float clampIndirect) {
-    const V3 neeLocal = (fLi * mk(1.0f)) * scalar;
+// Surface coverage of a hit for a ray that may pass through cutouts (Material::opacity).
+__device__ __forceinline__ float surfaceOpacity(const MatGPU& m) {
+    return m.type == PE_MAT_DISNEY ? m.opacity : 1.0f;
+}
+
+// passesCutout (path_tracer.cpp:161-167): true = the ray goes on through this hit.
+__device__ __forceinline__ bool passesCutout(const MatGPU& m, Sobol& sb) {
+    const float alpha = surfaceOpacity(m);
+    if (alpha >= 1.0f) return false;
+    if (alpha <= 0.0f) return true;
+    return get1D(sb) >= alpha;
+}
+
+// Material::shadowTransmittance: thin-walled glass passes (1 − R_thin)·tint, a cutout Disney
+// surface 1 − opacity, every other surface nothing.
+__device__ __forceinline__ V3 surfaceShadowTransmittance(const MatGPU& m, const Isect& is, V3 dir) {
+    if (m.type == PE_MAT_DIELECTRIC) return glassShadowTransmittance(m, is.ng, is.normal, dir);
+    if (m.type == PE_MAT_DISNEY) return mk(1.0f - m.opacity);
+    return mk(0.0f);
+}
+
+// shadowTransmittance (path_tracer.cpp:172-202).  Without shadow-transmitting materials in the
+// scene it is the any-hit test; otherwise the shadow ray walks from surface to surface (at most
+// 64) through thin-walled glass and cutouts, multiplying their transmittance, and stops black at
+// any other surface.
+template <bool COUNT>
+__device__ V3 shadowVisibility(const SceneGPU& S, V3 o, V3 d, float tMax, uint32_t& nodes, uint32_t& tris) {
+    if (!S.hasShadowTransmitters) return traceAny<COUNT>(S, o, d, VIS_SHADOW, 0.0f, tMax, nodes, tris) ? mk(0.0f) : mk(1.0f);
+    V3 T = mk(1.0f);
+    V3 origin = o;
+    float remaining = tMax;
+    for (int i = 0; i < 64; ++i) {
+        const Hit h = traceClosest<COUNT>(S, origin, d, VIS_SHADOW, 0.0f, remaining, nodes, tris);
+        if (h.prim < 0) return T;
+        Isect is;
+        fillHit(S, h, d, is);
+        const MatGPU& m = S.materials[is.material];
+        if (!(m.flags & MF_TRANSMITS_SHADOWS)) return mk(0.0f);
+        T *= surfaceShadowTransmittance(m, is, d);
+        if (isBlack(T)) return T;
+        origin = offsetRayOrigin(is.point, is.pError, len2(is.ng) > 0.0f ? is.ng : is.normal, d);
+        remaining -= h.t;
+        if (remaining <= 0.0f) return T;
+    }
+    return mk(0.0f);
+}
+
+// A NEE sample's term: throughput × f·Li·vis·(cos·w / (lightPdf·n)), clamped when indirect
+// (path_tracer.cpp:683-690).
+__device__ __forceinline__ V3 neeTerm(V3 fLi, V3 vis, float scalar, V3 thr, bool indirect, float clampIndirect) {
+    const V3 neeLocal = (fLi * vis) * scalar;
     V3 c = thr * neeLocal;
     if (indirect && clampIndirect > 0.0f) {
         const float m = smax3(c.x, c.y, c.z);
@@ -188,8 +193,7 @@ __device__ __forceinline__ V3 neeTerm(V3 fLi, float scalar, V3 thr, bool indirec
 
 // ---- any hit over the shadow queue ------------------------------------------------------------
 template <bool COUNT>
-__global__ void __launch_bounds__(128) kShadow(SceneGPU S, Paths P, const uint32_t* count, float clampIndirect,
-                                               unsigned long long* stats) {
+__global__ void __launch_bounds__(128) kShadow(SceneGPU S, Paths P, const uint32_t* count, unsigned long long* stats) {
     const int n = static_cast<int>(*count);
     uint32_t nodes = 0, tris = 0;
     for (;;) {
@@ -200,11 +204,11 @@ __global__ void __launch_bounds__(128) kShadow(SceneGPU S, Paths P, const uint32
         const int slot = P.shadowQ[i];
         const float4 so = P.shO[i];
         const float4 sd = P.shD[i];
-        const bool occluded = traceAny<COUNT>(S, mk(so.x, so.y, so.z), mk(sd.x, sd.y, sd.z), VIS_SHADOW, 0.0f, so.w, nodes, tris);
-        if (occluded) continue;
+        const V3 vis = shadowVisibility<COUNT>(S, mk(so.x, so.y, so.z), mk(sd.x, sd.y, sd.z), so.w, nodes, tris);
+        if (isBlack(vis)) continue;
         const float4 sc = P.shC[i];
         const float4 st = P.shT[i];
-        const V3 c = neeTerm(mk(sc.x, sc.y, sc.z), sd.w, mk(st.x, st.y, st.z), (__float_as_uint(sc.w) & 1u) != 0, clampIndirect);
+        const V3 c = neeTerm(mk(sc.x, sc.y, sc.z), vis, sd.w, mk(st.x, st.y, st.z), (__float_as_uint(sc.w) & 1u) != 0, st.w);
         if (!isFinite3(c)) continue;
         float4 L = P.L[slot];
         L.x += c.x;
@@ -276,7 +280,7 @@ __device__ __noinline__ int mediumSegment(const TablesGPU* T, const MatGPU& mm, 
 // shadow rays go to the any-hit queue, or with INLINE_SHADOW are traced here and their terms
 // added to L at once, in the same order.  Returns whether the path goes on.
 template <bool INLINE_SHADOW, bool COUNT>
-__device__ __forceinline__ bool shadeSlot(const SceneGPU& S, const Paths& P, const WaveArgs& A, int slot,
+__device__ __forceinline__ bool shadeSlot(const SceneGPU& S, const Paths& P, const WaveSeg& A, int slot,
                                           uint32_t& shNodes, uint32_t& shTris, uint32_t& shRays) {
     const TablesGPU* T = S.tables;
     const bool volumetric = (S.hasVolumes | S.hasSubsurface) != 0;
@@ -304,7 +308,7 @@ __device__ __forceinline__ bool shadeSlot(const SceneGPU& S, const Paths& P, con
     Sobol sb;
     sb.pixelHash = __float_as_uint(pp.w);
     {
-        const int sOff = slot / A.nPix;
+        const int sOff = (slot - A.slotFirst) / A.nPix;
         sb.revIndex = rev32(static_cast<uint32_t>(A.sampleFirst + sOff));
     }
     sb.dim = __float_as_uint(lp.w);
@@ -371,9 +375,10 @@ __device__ __forceinline__ bool shadeSlot(const SceneGPU& S, const Paths& P, con
             h.v = hr.z;
             h.prim = prim;
             fillHit(S, h, dir, is);
-            // Camera-invisible light quads are passed through by camera rays; the vertex
-            // does not count (path_tracer.cpp:426-439).  Cutouts are not supported here.
-            if (cameraRay && (S.shapes[is.shape].flags & SF_CAMERA_INVISIBLE) && skips < 64) {
+            // Camera-invisible light quads (for camera rays) and cutouts are passed through;
+            // the vertex does not count (path_tracer.cpp:426-439).
+            if (skips < 64 && ((cameraRay && (S.shapes[is.shape].flags & SF_CAMERA_INVISIBLE)) ||
+                               passesCutout(S.materials[is.material], sb))) {
                 const V3 no = offsetRayOrigin(is.point, is.pError, is.ng, dir);
                 ro = make_float4(no.x, no.y, no.z, ro.w);
                 ++skips;
@@ -512,8 +517,9 @@ __device__ __forceinline__ bool shadeSlot(const SceneGPU& S, const Paths& P, con
                 if (INLINE_SHADOW) {
                     // the any-hit query now; its term follows this vertex's emission in L
                     ++shRays;
-                    if (!traceAny<COUNT>(S, so, sd, VIS_SHADOW, 0.0f, stMax, shNodes, shTris)) {
-                        const V3 c = neeTerm(fLi, scalar, thr, diffuseBounces >= 1, A.clampIndirect);
+                    const V3 vis = shadowVisibility<COUNT>(S, so, sd, stMax, shNodes, shTris);
+                    if (!isBlack(vis)) {
+                        const V3 c = neeTerm(fLi, vis, scalar, thr, diffuseBounces >= 1, A.clampIndirect);
                         if (isFinite3(c)) {
                             L.x += c.x;
                             L.y += c.y;
@@ -527,7 +533,7 @@ __device__ __forceinline__ bool shadeSlot(const SceneGPU& S, const Paths& P, con
                     P.shO[pos] = make_float4(so.x, so.y, so.z, stMax);
                     P.shD[pos] = make_float4(sd.x, sd.y, sd.z, scalar);
                     P.shC[pos] = make_float4(fLi.x, fLi.y, fLi.z, __uint_as_float(diffuseBounces >= 1 ? 1u : 0u));
-                    P.shT[pos] = make_float4(thr.x, thr.y, thr.z, 0.0f);
+                    P.shT[pos] = make_float4(thr.x, thr.y, thr.z, A.clampIndirect);
                 }
             }
         }
@@ -628,7 +634,7 @@ __device__ __forceinline__ bool shadeSlot(const SceneGPU& S, const Paths& P, con
 
 // Consumes the rays binned by shading key (segment by segment, so a warp mostly shades one
 // material kind) and appends the continuing paths to nextQueue.
-__global__ void __launch_bounds__(128, 4) kShade(SceneGPU S, Paths P, WaveArgs A, int32_t* nextQueue, uint32_t* nextCount) {
+__global__ void __launch_bounds__(128, 4) kShade(SceneGPU S, Paths P, Wave W, int32_t* nextQueue, uint32_t* nextCount) {
     uint32_t seg[kShadeKeys];
     int n = 0;
     for (int k = 0; k < kShadeKeys; ++k) {
@@ -651,7 +657,7 @@ __global__ void __launch_bounds__(128, 4) kShade(SceneGPU S, Paths P, WaveArgs A
                 ++k;
             }
             slot = P.sortQ[static_cast<size_t>(k) * P.capacity + j];
-            cont = shadeSlot<false, false>(S, P, A, slot, unused0, unused1, unused2);
+            cont = shadeSlot<false, false>(S, P, W.segs[segOfSlot(W, slot)], slot, unused0, unused1, unused2);
         }
         queuePush(nextQueue, nextCount, cont, slot);
     }
@@ -663,7 +669,7 @@ __global__ void __launch_bounds__(128, 4) kShade(SceneGPU S, Paths P, WaveArgs A
 // (shadow rays inline) until the path ends, then takes the next.  The arithmetic and the order of
 // L's terms are the wavefront's, so the film is the same bit for bit.
 template <bool COUNT>
-__global__ void __launch_bounds__(128) kTail(SceneGPU S, Paths P, WaveArgs A, const int32_t* queue, const uint32_t* count,
+__global__ void __launch_bounds__(128) kTail(SceneGPU S, Paths P, Wave W, const int32_t* queue, const uint32_t* count,
                                              unsigned long long* stats) {
     const int n = static_cast<int>(*count);
     uint32_t nodes = 0, tris = 0, shNodes = 0, shTris = 0, rays = 0, shRays = 0;
@@ -671,6 +677,7 @@ __global__ void __launch_bounds__(128) kTail(SceneGPU S, Paths P, WaveArgs A, co
         const int i = static_cast<int>(atomicAdd(&P.counters[CNT_WORK_TAIL], 1u));
         if (i >= n) break;
         const int slot = queue[i];
+        const WaveSeg& A = W.segs[segOfSlot(W, slot)];
         for (int q = 0;; ++q) {
             if (q >= kMaxPathQueries) {
                 atomicAdd(&stats[7], 1ull);
@@ -696,16 +703,19 @@ __global__ void __launch_bounds__(128) kTail(SceneGPU S, Paths P, WaveArgs A, co
 }
 
 // ---- film: Film::addSample in sample order per pixel (src/core/image/film.cpp:56-69) ----------
-__global__ void kFilm(Paths P, WaveArgs A, float* sum, uint32_t* cnt, float* sumSq, unsigned long long* rejected) {
+__global__ void kFilm(Paths P, Wave W, unsigned long long* rejected) {
     unsigned long long rej = 0;
-    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < A.nPix; p += gridDim.x * blockDim.x) {
+    for (int wp = blockIdx.x * blockDim.x + threadIdx.x; wp < W.nPix; wp += gridDim.x * blockDim.x) {
+        const WaveSeg& A = W.segs[segOfPixel(W, wp)];
+        const int p = wp - A.pixFirst;
         const int tp = A.pixelFirst + p;
         const int pix = (A.tileY + tp / A.tileW) * A.width + A.tileX + tp % A.tileW;
+        float* sum = A.sum;
         float sr = sum[3 * pix + 0], sg = sum[3 * pix + 1], sbb = sum[3 * pix + 2];
-        float sq = sumSq[pix];
-        uint32_t c = cnt[pix];
+        float sq = A.sq[pix];
+        uint32_t c = A.cnt[pix];
         for (int s = 0; s < A.nSamples; ++s) {
-            const float4 L = P.L[s * A.nPix + p];
+            const float4 L = P.L[A.slotFirst + s * A.nPix + p];
             ++c;
             const bool ok = finitef(L.x) && finitef(L.y) && finitef(L.z) && L.x >= 0.0f && L.y >= 0.0f && L.z >= 0.0f;
             if (!ok) {
@@ -721,8 +731,8 @@ __global__ void kFilm(Paths P, WaveArgs A, float* sum, uint32_t* cnt, float* sum
         sum[3 * pix + 0] = sr;
         sum[3 * pix + 1] = sg;
         sum[3 * pix + 2] = sbb;
-        sumSq[pix] = sq;
-        cnt[pix] = c;
+        A.sq[pix] = sq;
+        A.cnt[pix] = c;
     }
     if (rej) atomicAdd(rejected, rej);
 }

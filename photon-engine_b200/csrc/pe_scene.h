@@ -118,7 +118,6 @@ struct TablesGPU {
     float ggxEb[kTableN * kTableN];
     float avg0[kTableN], avg1[kTableN], avg2[kTableN];
     float sheenE[kTableN * kTableN];
-    float filterCdf[kFilterBins + 1];
     uint32_t sobolTab[4][256];
     float spectralCdf[351];
     float spectralPdf[350];

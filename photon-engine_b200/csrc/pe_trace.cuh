@@ -7,6 +7,8 @@
 // record produce the reference CPU path's floats bit for bit.
 #pragma once
 
+#include "pe_wave.h"
+
 #include "pe_math.h"
 #include "pe_scene.h"
 
@@ -36,11 +38,7 @@ __device__ __forceinline__ V2 get2D(const TablesGPU* T, Sobol& s) {
 }
 
 // ---- camera ray (renderer.cpp:139-160, pixel_filter.cpp:84-91, perspective_camera.cpp:36-40) --
-struct CamDev {
-    V3 position, lowerLeft, horizontal, vertical;
-};
-__device__ __forceinline__ float filterSample1D(const TablesGPU* T, float filterWidth, float u) {
-    const float* cdf = T->filterCdf;
+__device__ __forceinline__ float filterSample1D(const float* cdf, float filterWidth, float u) {
     if (cdf[0] < 0.0f) return (u - 0.5f) * filterWidth;
     // std::upper_bound over 513 entries
     int lo = 0, count = kFilterBins + 1;
@@ -61,11 +59,11 @@ __device__ __forceinline__ float filterSample1D(const TablesGPU* T, float filter
     return -radius + (static_cast<float>(i) + sclamp(t, 0.0f, 1.0f)) * (filterWidth / kFilterBins);
 }
 // Primary ray of pixel (x, y): consumes Sobol dimensions 0 (filter) and 1 (lens).
-__device__ __forceinline__ void cameraRay(const TablesGPU* T, const CamDev& c, float filterWidth, int x, int y, int w,
-                                          int h, Sobol& s, V3& o, V3& d) {
+__device__ __forceinline__ void cameraRay(const TablesGPU* T, const float* filterCdf, const CamDev& c, float filterWidth,
+                                          int x, int y, int w, int h, Sobol& s, V3& o, V3& d) {
     const V2 u = get2D(T, s);
-    const float ox = filterSample1D(T, filterWidth, u.x);
-    const float oy = filterSample1D(T, filterWidth, u.y);
+    const float ox = filterSample1D(filterCdf, filterWidth, u.x);
+    const float oy = filterSample1D(filterCdf, filterWidth, u.y);
     const float sx = (static_cast<float>(x) + 0.5f + ox) / static_cast<float>(w);
     const float sy = 1.0f - (static_cast<float>(y) + 0.5f + oy) / static_cast<float>(h);
     (void)get2D(T, s); // lens sample (consumed even by a pinhole camera)

@@ -1,0 +1,100 @@
+// pe_wave.h — the wavefront's data layout: per-path state columns in HBM, queue counters, and
+// the segment table that lets several render requests share one wave.  Plain structs, so the
+// host-side scheduler (compiled without device code) can build waves.
+#pragma once
+
+#include "pe_math.h"
+
+#include <cstdint>
+#include <vector_types.h>
+
+namespace pe {
+
+// Pinhole camera as PerspectiveCamera stores it (perspective_camera.cpp:36-40).
+struct CamDev {
+    V3 position, lowerLeft, horizontal, vertical;
+};
+
+enum VisMask : uint32_t { VIS_CAMERA = 1u, VIS_DIFFUSE = 2u, VIS_GLOSSY = 4u, VIS_TRANSMISSION = 8u, VIS_SHADOW = 16u,
+                          VIS_ALL = 0x1Fu };
+// Marks a random-walk ray in the ray's mask word.  Triangle masks never carry it, so it does
+// not change what the ray can hit; the closest-hit kernel bins such rays under their own key.
+constexpr uint32_t RAY_WALK = 1u << 31;
+constexpr int kMaxMediumEvents = 1024; // path_tracer.cpp:51
+constexpr int kMaxWalkSteps = 256;     // path_tracer.cpp:52
+// Closest-hit queries one path can make: at most 255 bounces, each preceded by up to 64 skipped
+// camera-invisible hits and 65 pass-throughs and followed by up to 256 walk steps, plus 1025
+// medium events, stays below this; a path that reaches it is counted as an error and ended.
+constexpr int kMaxPathQueries = 1 << 17;
+
+// path flags (bits of state word)
+enum PathFlags : uint32_t {
+    PF_SPECULAR_BOUNCE = 1u << 0,
+    PF_CAMERA_RAY = 1u << 1,
+    PF_PICKER_VALID = 1u << 2,
+    PF_FIRST_SEGMENT = 1u << 3,
+    PF_WALK = 1u << 4,   // inside a random walk: lastP = σt, lastN = albedo, pickP.x = g
+};
+
+// Per-slot state columns (capacity P slots).
+struct Paths {
+    float4* rayO;    // origin xyz, visibility mask (bits)
+    float4* rayD;    // direction xyz, lastBsdfPdf
+    float4* thr;     // throughput xyz, wavelength
+    float4* L;       // radiance xyz, unused
+    float4* lastN;   // last shading normal xyz, flags (bits)
+    float4* lastP;   // last point xyz, Sobol dimension (bits)
+    float4* pickP;   // light-picker point xyz, pixel hash (bits)
+    float4* pickN;   // light-picker normal xyz, counters (bits: depth | diffuseBounces<<8 | passThroughs<<16 | skips<<24)
+    float4* hit;     // t, u, v, leaf prim (bits)
+    float4* med;     // media stack slots 0,1 | slots 2,3 (bits), mediumEvents | walkStep<<16, stack depth
+    int32_t* queueA;
+    int32_t* queueB;
+    int32_t* shadowQ;
+    float4* shO;     // shadow origin xyz, tMax
+    float4* shD;     // shadow direction xyz, scalar (cos*w/(pdf*n))
+    float4* shC;     // f*Li xyz, flags (bit0: indirect)
+    float4* shT;     // throughput at NEE xyz
+    int32_t* sortQ;  // kShadeKeys segments of `capacity` slots: rays binned by shading key
+    uint32_t capacity;
+    // [0] queue A count, [1] queue B count, [2] shadow count, [3] closest-hit work cursor,
+    // [4] any-hit work cursor, [5] shade work cursor, [6..11] rays per shading key, [12] errors,
+    // [13] tail work cursor
+    uint32_t* counters;
+};
+
+// Shading keys: 0 = miss, 1 + material type (Lambert, Disney, Dielectric, Mirror), 5 = random-walk step.
+constexpr int kShadeKeys = 6;
+enum CounterSlots { CNT_QA = 0, CNT_QB = 1, CNT_SHADOW = 2, CNT_WORK_ISECT = 3, CNT_WORK_SHADOW = 4,
+                    CNT_WORK_SHADE = 5, CNT_KEYS = 6, CNT_ERRORS = 12, CNT_WORK_TAIL = 13, CNT_TOTAL = 16 };
+
+// One request's share of a wave: a rectangle of its film, a range of its sample indices and its
+// render settings.  Wave slots [slotFirst, slotFirst + nPix·nSamples) are its paths, sample-major
+// (slot = slotFirst + s·nPix + p), and its pixels are wave pixels [pixFirst, pixFirst + nPix).
+struct WaveSeg {
+    CamDev cam;
+    int width, height;      // film
+    int tileX, tileY, tileW; // rendered rectangle of the film (whole frame: 0, 0, width)
+    int pixelFirst, nPix;   // range of tile-linear pixel indices in this wave
+    int sampleFirst, nSamples;
+    uint64_t seed;
+    float filterWidth;
+    int maxDepth, rrDepth, shadowSamples;
+    float clampIndirect;
+    const float* filterCdf; // inverse-CDF table of the request's pixel filter
+    float* sum;             // the request's film on the device
+    uint32_t* cnt;
+    float* sq;
+    int slotFirst;
+    int pixFirst;
+};
+
+// The segments of one wave, ordered by slotFirst (and so by pixFirst).
+struct Wave {
+    const WaveSeg* segs;
+    int nSegs;
+    int nSlots;
+    int nPix;
+};
+
+} // namespace pe

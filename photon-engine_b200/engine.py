@@ -597,6 +597,91 @@ def create_device(device_id: str = "auto", error: Optional[list] = None) -> Opti
 
 
 # ---------------------------------------------------------------------------------------------
+@dataclasses.dataclass
+class RequestStatus:
+    state: int
+    samples_done: int
+    submit_ms: float
+    start_ms: float
+    done_ms: float
+    paths: int
+    error: int
+
+    @property
+    def done(self) -> bool:
+        return self.state in (capi.PE_REQ_DONE, capi.PE_REQ_RELEASED)
+
+    @property
+    def latency_ms(self) -> float:
+        return self.done_ms - self.submit_ms
+
+
+class RenderServer:
+    """Request server over one CudaDevice (pe_server_* in include/photon_cuda.h): resident scenes,
+    device films admitted against an HBM budget, and continuous batching of many requests into
+    shared waves.  A request's film equals a lone ``CudaDevice.render`` of samples [0, spp)."""
+
+    def __init__(self, device: CudaDevice, budget_bytes: int):
+        err = C.create_string_buffer(512)
+        h = _lib().pe_server_create(device.handle, int(budget_bytes), err, len(err))
+        if not h:
+            raise capi.PhotonError(capi.PE_ERR_INVALID, err.value.decode())
+        self._h = h
+        self.device = device
+        self._films = {}
+
+    def close(self):
+        if self._h:
+            _lib().pe_server_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def add_scene(self, scene: Scene) -> int:
+        if scene.info is None:
+            scene.build_accelerator()
+        sid = int(_lib().pe_server_add_scene(self._h, scene.handle))
+        if sid < 0:
+            capi.check(-sid)
+        return sid
+
+    def submit(self, scene_id: int, camera: PerspectiveCamera, settings: RenderSettings, spp: int,
+               priority: int = 0) -> int:
+        q = capi.pe_request_desc(scene_id, camera.describe_gpu(), settings.to_c(), int(spp), int(priority))
+        rid = int(_lib().pe_server_submit(self._h, C.byref(q)))
+        if rid < 0:
+            capi.check(-rid)
+        self._films[rid] = (settings.width, settings.height)
+        return rid
+
+    def status(self, rid: int) -> RequestStatus:
+        st = capi.pe_request_status()
+        capi.check(_lib().pe_server_status(self._h, rid, C.byref(st)))
+        return RequestStatus(st.state, st.samples_done, st.submit_ms, st.start_ms, st.done_ms, st.paths, st.error)
+
+    def wait(self, rid: int, timeout_ms: int = -1) -> bool:
+        rc = _lib().pe_server_wait(self._h, rid, int(timeout_ms))
+        if rc == capi.PE_ERR_CANCELLED:
+            return False
+        capi.check(rc)
+        return True
+
+    def take(self, rid: int) -> Film:
+        w, h = self._films.pop(rid)
+        f = Film(w, h)
+        capi.check(_lib().pe_server_take(self._h, rid, capi.fptr(f.sum), capi.uptr(f.count), capi.fptr(f.sum_sq)))
+        return f
+
+    def stats(self) -> capi.pe_server_stats:
+        s = capi.pe_server_stats()
+        capi.check(_lib().pe_server_get_stats(self._h, C.byref(s)))
+        return s
+
+
 class RenderMode(enum.Enum):
     Interactive = 0
     Final = 1

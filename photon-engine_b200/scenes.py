@@ -16,6 +16,9 @@ scenes stand in for them with the stated sizes and value distributions.
                        channel), a Henyey–Greenstein scattering sphere (g = 0.6) and a random-walk
                        subsurface slab (mean free path 1–5 mm); ~200k triangles, 1280×720,
                        512 spp, depth 24 at full size.
+* ``instanced_grid_scene`` a 5×4 grid of 20 seeded copies of a 262k-triangle torus knot
+                       (5.2M triangles, the copies flattened into one BVH: this engine has no
+                       instance level), eight Disney materials, the sky of the knot scene.
 """
 from __future__ import annotations
 
@@ -25,6 +28,20 @@ import numpy as np
 
 from .engine import (AreaLight, Dielectric, DisneyMaterial, EnvironmentLight, Lambertian, PerspectiveCamera,
                      PixelFilterType, RenderSettings, Scene, TriangleMesh)
+
+
+# Viewpoints of the workloads: (position, target, up, vertical fov in degrees).
+CAMERAS = {
+    "cornell": ((2.78, 2.73, -8.0), (2.78, 2.73, 0.0), (0.0, 1.0, 0.0), 39.3),
+    "knot": ((0.0, 4.5, -10.5), (0.0, 1.6, 0.0), (0.0, 1.0, 0.0), 40.0),
+    "media": ((0.0, 420.0, -950.0), (0.0, 70.0, 40.0), (0.0, 1.0, 0.0), 38.0),
+    "grid": ((0.0, 8.0, -13.0), (0.0, 1.0, 4.0), (0.0, 1.0, 0.0), 45.0),
+}
+
+
+def camera_for(name: str, width: int, height: int) -> PerspectiveCamera:
+    pos, target, up, fov = CAMERAS[name]
+    return PerspectiveCamera(pos, target, up, fov, width / height)
 
 
 def _quad(p0, p1, p2, p3):
@@ -80,7 +97,7 @@ def cornell_box(width: int = 256, height: int = 256, spp: int = 64, max_depth: i
                               ((3.68, 1.65, 3.51), (1.65, 3.3, 1.65), 15.0)):
         pos, idx = _box(center, size, ang)
         scene.add_shape(TriangleMesh(pos, None, None, idx, white))
-    camera = PerspectiveCamera((2.78, 2.73, -8.0), (2.78, 2.73, 0.0), (0.0, 1.0, 0.0), 39.3, width / height)
+    camera = camera_for("cornell", width, height)
     settings = RenderSettings(width=width, height=height, samples_per_pixel=spp, max_bounces=max_depth,
                               filter_type=PixelFilterType.Box, filter_width=1.0, seed=seed)
     return scene, camera, settings
@@ -184,7 +201,7 @@ def torus_knot_scene(width: int = 1920, height: int = 1080, spp: int = 256, max_
     softbox = AreaLight((-3.0, 6.5, -2.0), (3.0, 0.0, 0.0), (0.0, 0.0, 2.0), (12.0, 12.0, 12.0))
     scene.add_light(softbox)
     scene.set_environment(EnvironmentLight(sky_environment(*env_size), 0.0, 1.0))
-    camera = PerspectiveCamera((0.0, 4.5, -10.5), (0.0, 1.6, 0.0), (0.0, 1.0, 0.0), 40.0, width / height)
+    camera = camera_for("knot", width, height)
     settings = RenderSettings(width=width, height=height, samples_per_pixel=spp, max_bounces=max_depth,
                               filter_type=PixelFilterType.BlackmanHarris, filter_width=1.5)
     return scene, camera, settings
@@ -352,7 +369,39 @@ def media_scene(width: int = 1280, height: int = 720, spp: int = 512, max_depth:
     skin.set_subsurface_scale(1.0)
     p, n, i = grid_box((0.0, 20.0, 230.0), (380.0, 40.0, 170.0), slab_res)
     scene.add_shape(TriangleMesh(p, n, None, i, skin))
-    camera = PerspectiveCamera((0.0, 420.0, -950.0), (0.0, 70.0, 40.0), (0.0, 1.0, 0.0), 38.0, width / height)
+    camera = camera_for("media", width, height)
     settings = RenderSettings(width=width, height=height, samples_per_pixel=spp, max_bounces=max_depth,
                               filter_type=PixelFilterType.BlackmanHarris, filter_width=1.5)
     return scene, camera, settings
+
+
+def instanced_grid_scene(width: int = 1920, height: int = 1080, spp: int = 64, max_depth: int = 12, seed: int = 21,
+                         nx: int = 5, nz: int = 4, nu: int = 1024, nv: int = 128, env_size=(2048, 1024)):
+    """~5M triangles: nx·nz rotated, scaled copies of one knot mesh on a ground plane."""
+    rng = np.random.default_rng(seed)
+    mats = []
+    for _ in range(8):
+        m = DisneyMaterial(tuple(rng.uniform(0.0, 1.0, 3)), float(rng.choice([0.0, 1.0])),
+                           float(rng.uniform(0.05, 0.9)), 0.5)
+        m.set_clear_coat(float(rng.uniform(0.0, 1.0)))
+        mats.append(m)
+    pos, quads = torus_knot_mesh(nu, nv, seed=seed)
+    q = quads.reshape(-1, 4)
+    tri = np.concatenate([q[:, [0, 1, 2]], q[:, [0, 2, 3]]], axis=0).astype(np.uint32)
+    scene = Scene()
+    for i in range(nx):
+        for k in range(nz):
+            a = rng.uniform(0.0, 2.0 * math.pi)
+            sc = rng.uniform(0.6, 0.9)
+            c, s_ = math.cos(a), math.sin(a)
+            rot = np.array([[c, 0.0, s_], [0.0, 1.0, 0.0], [-s_, 0.0, c]])
+            offset = np.array([(i - (nx - 1) / 2) * 5.0, 0.0, (k - (nz - 1) / 2) * 5.0 + 4.0])
+            p = (pos @ rot.T) * sc + offset
+            scene.add_shape(TriangleMesh(p.astype(np.float32), None, None, tri, mats[int(rng.integers(0, 8))]))
+    g = 80.0
+    gp = np.array([(-g, 0.0, -g), (-g, 0.0, g), (g, 0.0, g), (g, 0.0, -g)], np.float32)
+    scene.add_shape(TriangleMesh(gp, None, None, np.array([[0, 1, 2], [0, 2, 3]], np.uint32), Lambertian((0.5, 0.5, 0.5))))
+    scene.set_environment(EnvironmentLight(sky_environment(*env_size), 0.0, 1.0))
+    settings = RenderSettings(width=width, height=height, samples_per_pixel=spp, max_bounces=max_depth,
+                              filter_type=PixelFilterType.BlackmanHarris, filter_width=1.5)
+    return scene, camera_for("grid", width, height), settings

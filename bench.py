@@ -1,9 +1,9 @@
 """Throughput benchmark of the B200 path tracer on the product-scale torus-knot workload.
 
-Workload (one ``step``): one sample per pixel of a 1920×1080 frame of the ~1M-triangle torus
+Workload (one ``step``): four samples per pixel of a 1920×1080 frame of the ~1M-triangle torus
 knot with eight Disney materials, a 2048×1024 HDR sky (sun lobe 60 % of power) and a softbox,
-max depth 12 — i.e. 2,073,600 camera paths through the wavefront (generate, closest hit,
-shade, any hit, film) per step.  Metric: paths/s (W·H·spp / render seconds, the reference's
+max depth 12 — i.e. 8,294,400 camera paths (four waves) through the wavefront (generate, closest
+hit, shade, any hit, tail, film) per step, a batch of the 256-spp frame.  Metric: paths/s (W·H·spp / render seconds, the reference's
 msamplesPerSecond definition).
 
 ``value``   device-resident: inputs in HBM, K steps into the resident film, CUDA events on the
@@ -39,6 +39,7 @@ ROOT = pathlib.Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
 WIDTH, HEIGHT, DEPTH = 1920, 1080, 12
+SPP_PER_STEP = 4  # one step = 4 samples per pixel of the 1080p frame (4 waves of ~2M paths)
 NODE_BYTES, TRI_BYTES, RAY_BYTES, HIT_BYTES, QUEUE_BYTES = 64, 48, 32, 16, 4
 L2_NOTE = "inputs larger than L2: 140 MB resident scene + 300 MB path state per 2M-path wave (L2 126 MB)"
 
@@ -188,16 +189,17 @@ def run_ours(args):
     scene, cam, st = build_workload(pe)
     dev = pe.CudaDevice(local)
     dev.set_scene(scene)
-    base = rank * (args.warmup + args.steps + 8)  # disjoint sample indices per replica
+    # disjoint sample indices per replica; step k renders samples base + SPP_PER_STEP·(1 + warmup + k) …
+    base = rank * (args.warmup + args.steps + 8) * SPP_PER_STEP
 
-    # algorithmic bytes per closest-hit ray, counted on the device over one untimed step
+    # algorithmic bytes per closest-hit ray, counted on the device over one untimed 1-spp pass
     dev.set_counting(True)
     dev.render_resident(cam, st, base, 1)
     cs = dev.last_stats()
     dev.set_counting(False)
     dev.film_clear()
     for w in range(args.warmup):
-        dev.render_resident(cam, st, base + w, 1)
+        dev.render_resident(cam, st, base + SPP_PER_STEP * (1 + w), SPP_PER_STEP)
     dev.synchronize()
     if pg:
         import torch
@@ -212,7 +214,7 @@ def run_ours(args):
     with ClockSampler(dev.pci_bus_id) as clocks:
         dev.timer_begin()
         for k in range(args.steps):
-            dev.render_resident(cam, st, base + args.warmup + k, 1)
+            dev.render_resident(cam, st, base + SPP_PER_STEP * (1 + args.warmup + k), SPP_PER_STEP)
             s = dev.last_stats()
             launches += s.kernel_launches
             rays += s.closest_rays
@@ -230,18 +232,18 @@ def run_ours(args):
         pg.all_reduce(t, op=pg.ReduceOp.MAX)
         ms = float(t.item())
         pg.barrier()
-    total_paths = WIDTH * HEIGHT * args.steps * world
+    total_paths = WIDTH * HEIGHT * SPP_PER_STEP * args.steps * world
     value = total_paths / (ms / 1000.0)
 
     # end-to-end through RenderDevice::render with host films
     film = pe.Film(WIDTH, HEIGHT)
     for w in range(min(2, args.warmup)):
-        dev.render(cam, st, pe.RenderTargets(beauty=film), base + w, 1)
+        dev.render(cam, st, pe.RenderTargets(beauty=film), base + SPP_PER_STEP * (1 + w), SPP_PER_STEP)
     if pg:
         pg.barrier()
     t0 = time.perf_counter()
     for k in range(args.steps):
-        dev.render(cam, st, pe.RenderTargets(beauty=film), base + args.warmup + k, 1)
+        dev.render(cam, st, pe.RenderTargets(beauty=film), base + SPP_PER_STEP * (1 + args.warmup + k), SPP_PER_STEP)
     e2e_s = time.perf_counter() - t0
     if pg:
         import torch
@@ -290,7 +292,8 @@ def run_ours(args):
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded procedural scene)",
         "config": {"workload": "torus-knot 1M tris, 8 Disney materials, 2048x1024 HDR sky + softbox, 1920x1080, depth 12",
-                   "spp_per_step": 1, "paths_per_step": WIDTH * HEIGHT, "triangles": int(scene.info.triangles),
+                   "spp_per_step": SPP_PER_STEP, "paths_per_step": WIDTH * HEIGHT * SPP_PER_STEP,
+                   "triangles": int(scene.info.triangles),
                    "l2": L2_NOTE, "parallelism": f"replicas x{world}"},
         "rays_per_s": (rays + shadow_rays) * world / (ms / 1000.0),
         "closest_rays_per_step": rays / args.steps, "shadow_rays_per_step": shadow_rays / args.steps,

@@ -341,7 +341,7 @@ typedef struct pe_server_stats {
     uint64_t submitted, completed, failed;
     uint64_t queued, active;
     uint64_t waves, paths, segments;
-    double busy_ms;               /* device time of the waves */
+    double busy_ms;               /* device time of the waves, each counted whole (two may overlap) */
     uint64_t film_bytes, film_bytes_peak, budget_bytes, scene_bytes;
 } pe_server_stats;
 

@@ -19,47 +19,52 @@ namespace pe_dev {
 
 int32_t ensureCapacity(pe_device* d, size_t slots) {
     if (slots <= d->capacity) return PE_OK;
-    freeList(d->pathBufs);
+    for (WaveLane& ln : d->lanes) freeList(ln.bufs);
     d->capacity = 0;
-    Paths& P = d->paths;
     int32_t st = 0;
-    float4** cols[] = {&P.rayO, &P.rayD, &P.thr, &P.L, &P.lastN, &P.lastP, &P.pickP, &P.pickN, &P.hit, &P.med};
-    for (float4** c : cols)
-        if ((st = devAlloc(d->pathBufs, *c, slots))) return st;
-    if ((st = devAlloc(d->pathBufs, P.queueA, slots))) return st;
-    if ((st = devAlloc(d->pathBufs, P.queueB, slots))) return st;
-    if ((st = devAlloc(d->pathBufs, P.sortQ, slots * kShadeKeys))) return st;
-    // shadow records: one per slot (shadow quality 1)
-    if ((st = devAlloc(d->pathBufs, P.shadowQ, slots))) return st;
-    float4** scols[] = {&P.shO, &P.shD, &P.shC, &P.shT};
-    for (float4** c : scols)
-        if ((st = devAlloc(d->pathBufs, *c, slots))) return st;
-    if ((st = devAlloc(d->pathBufs, P.counters, CNT_TOTAL))) return st;
-    P.capacity = static_cast<uint32_t>(slots);
+    for (WaveLane& ln : d->lanes) {
+        Paths& P = ln.paths;
+        float4** cols[] = {&P.rayO, &P.rayD, &P.thr, &P.L, &P.lastN, &P.lastP, &P.pickP, &P.pickN, &P.hit, &P.med};
+        for (float4** c : cols)
+            if ((st = devAlloc(ln.bufs, *c, slots))) return st;
+        if ((st = devAlloc(ln.bufs, P.queueA, slots))) return st;
+        if ((st = devAlloc(ln.bufs, P.queueB, slots))) return st;
+        if ((st = devAlloc(ln.bufs, P.sortQ, slots * kShadeKeys))) return st;
+        // shadow records: one per slot (shadow quality 1)
+        if ((st = devAlloc(ln.bufs, P.shadowQ, slots))) return st;
+        float4** scols[] = {&P.shO, &P.shD, &P.shC, &P.shT};
+        for (float4** c : scols)
+            if ((st = devAlloc(ln.bufs, *c, slots))) return st;
+        if ((st = devAlloc(ln.bufs, P.counters, CNT_TOTAL))) return st;
+        P.capacity = static_cast<uint32_t>(slots);
+    }
     d->capacity = slots;
     return PE_OK;
 }
 
 // Device inverse-CDF table of a pixel filter.  `wave` stamps the slot so that a wave under
-// construction never evicts a table one of its own segments uses.  Returns nullptr when every
-// slot is taken by the current wave.
-const float* filterTable(pe_device* d, int type, float width, uint64_t wave) {
+// construction never evicts a table that it or the previous wave (possibly still running on the
+// other lane) reads.  Returns nullptr when no slot is free of both.
+const float* filterTable(pe_device* d, int type, float width, uint64_t wave, cudaStream_t stream) {
     int pick = -1;
     for (int i = 0; i < kFilterSlots; ++i)
         if (d->filterSlots[i].type == type && d->filterSlots[i].width == width) {
             d->filterSlots[i].used = wave;
             return d->dFilters + static_cast<size_t>(i) * (kFilterBins + 1);
         }
-    for (int i = 0; i < kFilterSlots; ++i) {
-        if (d->filterSlots[i].used == wave) continue;
-        if (pick < 0 || d->filterSlots[i].used < d->filterSlots[pick].used) pick = i;
-    }
+    for (int i = 0; i < kFilterSlots && pick < 0; ++i)
+        if (d->filterSlots[i].type < 0) pick = i; // never filled
+    if (pick < 0)
+        for (int i = 0; i < kFilterSlots; ++i) {
+            if (d->filterSlots[i].used + 1 >= wave) continue; // this wave's or the wave still in flight
+            if (pick < 0 || d->filterSlots[i].used < d->filterSlots[pick].used) pick = i;
+        }
     if (pick < 0) return nullptr;
     float cdf[kFilterBins + 1];
     fillFilterCdf(type, width, cdf);
-    // stream-ordered after every wave that read the slot's previous table
+    // on the stream of the wave that reads it; no wave still in flight reads the evicted table
     if (cudaMemcpyAsync(d->dFilters + static_cast<size_t>(pick) * (kFilterBins + 1), cdf, sizeof(cdf),
-                        cudaMemcpyHostToDevice, d->stream) != cudaSuccess)
+                        cudaMemcpyHostToDevice, stream) != cudaSuccess)
         return nullptr;
     d->filterSlots[pick] = FilterSlot{type, width, wave};
     return d->dFilters + static_cast<size_t>(pick) * (kFilterBins + 1);
@@ -167,12 +172,20 @@ int32_t beginRender(pe_device* d) {
     std::memset(&d->stats, 0, sizeof(d->stats));
     PE_CUDA(cudaMemsetAsync(d->dStats, 0, 8 * sizeof(unsigned long long), d->stream));
     PE_CUDA(cudaEventRecord(d->evStart, d->stream));
+    PE_CUDA(cudaStreamWaitEvent(d->lanes[1].stream, d->evStart, 0));
+    d->filmLane = -1;
     return PE_OK;
 }
 
 // Ends it: waits for the stream, then reads the device counters and per-kernel times.
 int32_t endRender(pe_device* d, const RenderTimer& tm) {
     pe_render_stats& stats = d->stats;
+    // join the second lane into the device stream
+    if (d->lanes[1].pending) {
+        PE_CUDA(cudaStreamWaitEvent(d->stream, d->lanes[1].evDone, 0));
+        d->lanes[1].pending = false;
+    }
+    d->lanes[0].pending = false;
     PE_CUDA(cudaEventRecord(d->evStop, d->stream));
     unsigned long long hs[8] = {};
     PE_CUDA(cudaMemcpyAsync(hs, d->dStats, sizeof(hs), cudaMemcpyDeviceToHost, d->stream));
@@ -210,56 +223,62 @@ int32_t endRender(pe_device* d, const RenderTimer& tm) {
     return PE_OK;
 }
 
-// The pinned segment table may be rewritten only once the previous wave's upload has run.
-int32_t segsWritable(pe_device* d) {
-    if (d->segsInFlight) {
-        PE_CUDA(cudaEventSynchronize(d->evSegs));
-        d->segsInFlight = false;
+// A lane's pinned segment table may be rewritten only once its previous upload has run.
+int32_t segsWritable(pe_device* d, int lane) {
+    WaveLane& ln = d->lanes[lane];
+    if (ln.segsInFlight) {
+        PE_CUDA(cudaEventSynchronize(ln.evSegs));
+        ln.segsInFlight = false;
     }
     return PE_OK;
 }
 
-// One wave over the nSegs segments in d->hSegs (nSlots paths, nPix film pixels): uploads the
-// segment table, generates the camera rays, traces them bounce by bounce (closest hit → shade →
-// any hit) until the live paths fit the tail kernel, which finishes them, and adds every sample
-// to its segment's film in sample order.
-int32_t runWave(pe_device* d, Paths& P, int nSegs, int nSlots, int nPix, RenderTimer& tm) {
+// One wave on a lane over the nSegs segments in its segment table (nSlots paths, nPix film
+// pixels): uploads the table, generates the camera rays, traces them bounce by bounce (closest
+// hit → shade → any hit) until the live paths fit the tail kernel, which finishes them, and adds
+// every sample to its segment's film in sample order, after the previous wave's film kernel.
+// The host waits for each bounce's queue count, not for the tail or the film kernel.
+int32_t runWave(pe_device* d, int lane, Paths& P, int nSegs, int nSlots, int nPix, RenderTimer& tm) {
+    WaveLane& ln = d->lanes[lane];
+    const cudaStream_t cs = ln.stream;
+    (void)cudaGetLastError(); // launch errors below are this wave's, not an earlier call's
     const SceneGPU& S = d->scene;
     const int sm = d->prop.multiProcessorCount;
     pe_render_stats& stats = d->stats;
     int32_t rc = PE_OK;
-    PE_CUDA(cudaMemcpyAsync(d->dSegs, d->hSegs, static_cast<size_t>(nSegs) * sizeof(WaveSeg), cudaMemcpyHostToDevice,
-                            d->stream));
-    PE_CUDA(cudaEventRecord(d->evSegs, d->stream));
-    d->segsInFlight = true;
-    const Wave W{d->dSegs, nSegs, nSlots, nPix};
-    kGenerate<<<sm * 8, 256, 0, d->stream>>>(S, P, W);
+    PE_CUDA(cudaMemcpyAsync(ln.dSegs, ln.hSegs, static_cast<size_t>(nSegs) * sizeof(WaveSeg), cudaMemcpyHostToDevice,
+                            cs));
+    PE_CUDA(cudaEventRecord(ln.evSegs, cs));
+    ln.segsInFlight = true;
+    const Wave W{ln.dSegs, nSegs, nSlots, nPix};
+    kGenerate<<<sm * 8, 256, 0, cs>>>(S, P, W);
     ++stats.kernel_launches;
     ++stats.waves;
     uint32_t live = static_cast<uint32_t>(nSlots);
-    PE_CUDA(cudaMemsetAsync(&P.counters[1], 0, (CNT_TOTAL - 1) * sizeof(uint32_t), d->stream));
-    PE_CUDA(cudaMemcpyAsync(&P.counters[0], &live, sizeof(uint32_t), cudaMemcpyHostToDevice, d->stream));
+    PE_CUDA(cudaMemsetAsync(&P.counters[1], 0, (CNT_TOTAL - 1) * sizeof(uint32_t), cs));
+    PE_CUDA(cudaMemcpyAsync(&P.counters[0], &live, sizeof(uint32_t), cudaMemcpyHostToDevice, cs));
     int32_t* qIn = P.queueA;
     int32_t* qOut = P.queueB;
     uint32_t* cIn = &P.counters[0];
     uint32_t* cOut = &P.counters[1];
     stats.paths += static_cast<uint64_t>(nSlots);
-    const int64_t tailPaths = d->tailPaths < 0 ? static_cast<int64_t>(d->blocksTail) * 128 : d->tailPaths;
+    const int64_t tailPaths = d->tailPaths < 0 ? static_cast<int64_t>(d->blocksTail) * kTailBlock : d->tailPaths;
     for (int iter = 0; live > 0; ++iter) {
         if (static_cast<int64_t>(live) <= tailPaths) {
             // the rest of the wave: one thread per path until it ends
-            const int grid = static_cast<int>(std::min<int64_t>(d->blocksTail, (static_cast<int64_t>(live) + 127) / 128));
+            const int grid = static_cast<int>(
+                std::min<int64_t>(d->blocksTail, (static_cast<int64_t>(live) + kTailBlock - 1) / kTailBlock));
             cudaEvent_t t0 = nullptr, t1 = nullptr;
             if (tm.timing) {
                 if ((rc = timerEvent(d, tm, t0)) || (rc = timerEvent(d, tm, t1))) return rc;
-                PE_CUDA(cudaEventRecord(t0, d->stream));
+                PE_CUDA(cudaEventRecord(t0, cs));
             }
             if (d->counting)
-                kTail<true><<<grid, 128, 0, d->stream>>>(S, P, W, qIn, cIn, d->dStats);
+                kTail<true><<<grid, kTailBlock, 0, cs>>>(S, P, W, qIn, cIn, d->dStats);
             else
-                kTail<false><<<grid, 128, 0, d->stream>>>(S, P, W, qIn, cIn, d->dStats);
+                kTail<false><<<grid, kTailBlock, 0, cs>>>(S, P, W, qIn, cIn, d->dStats);
             if (tm.timing) {
-                PE_CUDA(cudaEventRecord(t1, d->stream));
+                PE_CUDA(cudaEventRecord(t1, cs));
                 tm.tail.push_back({tm.evUsed - 2, tm.evUsed - 1});
             }
             ++stats.kernel_launches;
@@ -272,44 +291,50 @@ int32_t runWave(pe_device* d, Paths& P, int nSegs, int nSlots, int nPix, RenderT
             if ((rc = timerEvent(d, tm, e0)) || (rc = timerEvent(d, tm, e1)) || (rc = timerEvent(d, tm, e2)) ||
                 (rc = timerEvent(d, tm, e3)))
                 return rc;
-            PE_CUDA(cudaEventRecord(e0, d->stream));
+            PE_CUDA(cudaEventRecord(e0, cs));
         }
         if (d->counting)
-            kIntersect<true><<<d->blocksIntersect, 128, 0, d->stream>>>(S, P, qIn, cIn, d->dStats);
+            kIntersect<true><<<d->blocksIntersect, 128, 0, cs>>>(S, P, qIn, cIn, d->dStats);
         else
-            kIntersect<false><<<d->blocksIntersect, 128, 0, d->stream>>>(S, P, qIn, cIn, d->dStats);
-        if (tm.timing) PE_CUDA(cudaEventRecord(e1, d->stream));
-        kShade<<<d->blocksShade, 128, 0, d->stream>>>(S, P, W, qOut, cOut);
-        if (tm.timing) PE_CUDA(cudaEventRecord(e2, d->stream));
+            kIntersect<false><<<d->blocksIntersect, 128, 0, cs>>>(S, P, qIn, cIn, d->dStats);
+        if (tm.timing) PE_CUDA(cudaEventRecord(e1, cs));
+        kShade<<<d->blocksShade, 128, 0, cs>>>(S, P, W, qOut, cOut);
+        if (tm.timing) PE_CUDA(cudaEventRecord(e2, cs));
         if (d->counting)
-            kShadow<true><<<d->blocksShadow, 128, 0, d->stream>>>(S, P, &P.counters[CNT_SHADOW], d->dStats);
+            kShadow<true><<<d->blocksShadow, 128, 0, cs>>>(S, P, &P.counters[CNT_SHADOW], d->dStats);
         else
-            kShadow<false><<<d->blocksShadow, 128, 0, d->stream>>>(S, P, &P.counters[CNT_SHADOW], d->dStats);
+            kShadow<false><<<d->blocksShadow, 128, 0, cs>>>(S, P, &P.counters[CNT_SHADOW], d->dStats);
         stats.kernel_launches += 3;
         ++stats.intersect_launches;
         if (tm.timing) {
-            PE_CUDA(cudaEventRecord(e3, d->stream));
+            PE_CUDA(cudaEventRecord(e3, cs));
             tm.isect.push_back({tm.evUsed - 4, tm.evUsed - 3});
             tm.shade.push_back({tm.evUsed - 3, tm.evUsed - 2});
             tm.shadow.push_back({tm.evUsed - 2, tm.evUsed - 1});
         }
-        PE_CUDA(cudaMemcpyAsync(d->hCounters, P.counters, 4 * sizeof(uint32_t), cudaMemcpyDeviceToHost, d->stream));
-        PE_CUDA(cudaStreamSynchronize(d->stream));
-        stats.shadow_rays += d->hCounters[CNT_SHADOW];
-        live = cOut == &P.counters[1] ? d->hCounters[1] : d->hCounters[0];
+        PE_CUDA(cudaMemcpyAsync(ln.hCounters, P.counters, 4 * sizeof(uint32_t), cudaMemcpyDeviceToHost, cs));
+        PE_CUDA(cudaStreamSynchronize(cs));
+        stats.shadow_rays += ln.hCounters[CNT_SHADOW];
+        live = cOut == &P.counters[1] ? ln.hCounters[1] : ln.hCounters[0];
         if (iter > kMaxWavefrontIterations) {
             setError("wavefront did not drain after " + std::to_string(kMaxWavefrontIterations) + " iterations");
             return PE_ERR_DEVICE;
         }
         // swap queues; reset the consumed queue's counter, the shadow counter, the work
         // cursors and the shading-key bins
-        PE_CUDA(cudaMemsetAsync(cIn, 0, sizeof(uint32_t), d->stream));
+        PE_CUDA(cudaMemsetAsync(cIn, 0, sizeof(uint32_t), cs));
         PE_CUDA(cudaMemsetAsync(&P.counters[CNT_SHADOW], 0, (CNT_KEYS + kShadeKeys - CNT_SHADOW) * sizeof(uint32_t),
-                                d->stream));
+                                cs));
         std::swap(qIn, qOut);
         std::swap(cIn, cOut);
     }
-    kFilm<<<sm * 4, 256, 0, d->stream>>>(P, W, &d->dStats[4]);
+    // films accumulate in wave order: after the other lane's last film kernel
+    if (d->filmLane >= 0 && d->filmLane != lane) PE_CUDA(cudaStreamWaitEvent(cs, d->evFilm, 0));
+    kFilm<<<sm * 4, 256, 0, cs>>>(P, W, &d->dStats[4]);
+    PE_CUDA(cudaEventRecord(d->evFilm, cs));
+    d->filmLane = lane;
+    PE_CUDA(cudaEventRecord(ln.evDone, cs));
+    ln.pending = true;
     ++stats.kernel_launches;
     PE_CUDA(cudaGetLastError());
     return PE_OK;
@@ -319,19 +344,20 @@ int32_t runWave(pe_device* d, Paths& P, int nSegs, int nSlots, int nPix, RenderT
 // on the device, with path state in `P` (room for `capacity` slots): waves of one segment each.
 // With `timing` the closest-hit / shade / any-hit / tail launches are bracketed by events.
 int32_t renderWaves(pe_device* d, const pe_camera* cam, const pe_settings* st, int first, int count,
-                    const volatile int32_t* cancel, float* sum, uint32_t* cnt, float* sq, Paths& P, size_t capacity,
+                    const volatile int32_t* cancel, float* sum, uint32_t* cnt, float* sq, Paths* scratch, size_t capacity,
                     bool timing, Tile tile) {
     const size_t npix = static_cast<size_t>(tile.w) * static_cast<size_t>(tile.h);
     const int pixChunk = static_cast<int>(std::min(npix, capacity));
     const int samplesPerWave = static_cast<int>(std::max<size_t>(1, std::min<size_t>(static_cast<size_t>(count), capacity / pixChunk)));
-    int32_t rc = beginRender(d);
-    if (rc) return rc;
     WaveSeg base = makeSeg(cam, st);
-    base.filterCdf = filterTable(d, st->filter_type, st->filter_width, ++d->filterClock);
+    // uploaded on the device stream before evStart, which the second lane waits for
+    base.filterCdf = filterTable(d, st->filter_type, st->filter_width, ++d->filterClock, d->stream);
     if (!base.filterCdf) {
         setError("pixel filter table upload failed");
         return PE_ERR_CUDA;
     }
+    int32_t rc = beginRender(d);
+    if (rc) return rc;
     base.tileX = tile.x0;
     base.tileY = tile.y0;
     base.tileW = tile.w;
@@ -348,8 +374,12 @@ int32_t renderWaves(pe_device* d, const pe_camera* cam, const pe_settings* st, i
                 cancelled = true;
                 break;
             }
-            if ((rc = segsWritable(d))) return rc;
-            WaveSeg& seg = d->hSegs[0];
+            // alternate lanes (the no-allocation scratch has one)
+            const int lane = scratch ? 0 : d->nextLane;
+            if (!scratch) d->nextLane ^= 1;
+            Paths& P = scratch ? *scratch : d->lanes[lane].paths;
+            if ((rc = segsWritable(d, lane))) return rc;
+            WaveSeg& seg = d->lanes[lane].hSegs[0];
             seg = base;
             seg.pixelFirst = static_cast<int>(p0);
             seg.nPix = static_cast<int>(std::min<size_t>(static_cast<size_t>(pixChunk), npix - p0));
@@ -357,7 +387,7 @@ int32_t renderWaves(pe_device* d, const pe_camera* cam, const pe_settings* st, i
             seg.nSamples = ns;
             seg.slotFirst = 0;
             seg.pixFirst = 0;
-            if ((rc = runWave(d, P, 1, seg.nPix * ns, seg.nPix, tm))) return rc;
+            if ((rc = runWave(d, lane, P, 1, seg.nPix * ns, seg.nPix, tm))) return rc;
         }
     }
     if ((rc = endRender(d, tm))) return rc;
@@ -560,13 +590,23 @@ pe_device* pe_device_create(int32_t ordinal, char* err, size_t errLen) {
         cudaEventCreate(&d->evT0) != cudaSuccess || cudaEventCreate(&d->evT1) != cudaSuccess ||
         cudaMalloc(&d->dTables, sizeof(TablesGPU)) != cudaSuccess ||
         cudaMalloc(&d->dStats, 8 * sizeof(unsigned long long)) != cudaSuccess ||
-        cudaMallocHost(&d->hCounters, 16 * sizeof(uint32_t)) != cudaSuccess ||
         cudaMalloc(&d->dFilters, static_cast<size_t>(kFilterSlots) * (kFilterBins + 1) * sizeof(float)) != cudaSuccess ||
-        cudaMalloc(&d->dSegs, kMaxSegs * sizeof(WaveSeg)) != cudaSuccess ||
-        cudaMallocHost(&d->hSegs, kMaxSegs * sizeof(WaveSeg)) != cudaSuccess ||
-        cudaEventCreateWithFlags(&d->evSegs, cudaEventDisableTiming) != cudaSuccess) {
+        cudaEventCreateWithFlags(&d->evFilm, cudaEventDisableTiming) != cudaSuccess) {
         pe_device_destroy(d);
         return fail("device initialisation failed");
+    }
+    for (int l = 0; l < 2; ++l) {
+        WaveLane& ln = d->lanes[l];
+        if ((l == 0 ? (ln.stream = d->stream, cudaSuccess) : cudaStreamCreateWithFlags(&ln.stream, cudaStreamNonBlocking)) !=
+                cudaSuccess ||
+            cudaMalloc(&ln.dSegs, kMaxSegs * sizeof(WaveSeg)) != cudaSuccess ||
+            cudaMallocHost(&ln.hSegs, kMaxSegs * sizeof(WaveSeg)) != cudaSuccess ||
+            cudaMallocHost(&ln.hCounters, 16 * sizeof(uint32_t)) != cudaSuccess ||
+            cudaEventCreateWithFlags(&ln.evSegs, cudaEventDisableTiming) != cudaSuccess ||
+            cudaEventCreate(&ln.evDone) != cudaSuccess) {
+            pe_device_destroy(d);
+            return fail("device initialisation failed");
+        }
     }
     d->hTables = staticTables();
     cudaMemcpy(d->dTables, &d->hTables, sizeof(TablesGPU), cudaMemcpyHostToDevice);
@@ -578,7 +618,7 @@ pe_device* pe_device_create(int32_t ordinal, char* err, size_t errLen) {
     d->blocksShade = sm * std::max(1, b);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kShadow<false>, 128, 0);
     d->blocksShadow = sm * std::max(1, b);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kTail<true>, 128, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kTail<true>, kTailBlock, 0);
     d->blocksTail = sm * std::max(1, b);
     const cudaError_t le = cudaGetLastError();
     if (le != cudaSuccess) {
@@ -600,18 +640,25 @@ void pe_device_destroy(pe_device* d) {
     if (!d) return;
     cudaSetDevice(d->ordinal);
     if (d->stream) cudaStreamSynchronize(d->stream);
+    if (d->lanes[1].stream) cudaStreamSynchronize(d->lanes[1].stream);
     freeList(d->sceneBufs);
-    freeList(d->pathBufs);
+    for (int l = 0; l < 2; ++l) {
+        WaveLane& ln = d->lanes[l];
+        freeList(ln.bufs);
+        cudaFree(ln.dSegs);
+        if (ln.hSegs) cudaFreeHost(ln.hSegs);
+        if (ln.hCounters) cudaFreeHost(ln.hCounters);
+        if (ln.evSegs) cudaEventDestroy(ln.evSegs);
+        if (ln.evDone) cudaEventDestroy(ln.evDone);
+        if (l == 1 && ln.stream) cudaStreamDestroy(ln.stream);
+    }
+    if (d->evFilm) cudaEventDestroy(d->evFilm);
     cudaFree(d->fSum);
     cudaFree(d->fCnt);
     cudaFree(d->fSq);
     cudaFree(d->dTables);
     cudaFree(d->dStats);
     cudaFree(d->dFilters);
-    cudaFree(d->dSegs);
-    if (d->hSegs) cudaFreeHost(d->hSegs);
-    if (d->evSegs) cudaEventDestroy(d->evSegs);
-    if (d->hCounters) cudaFreeHost(d->hCounters);
     if (d->stage) cudaFreeHost(d->stage);
     for (cudaEvent_t e : d->evPool) cudaEventDestroy(e);
     if (d->evStart) cudaEventDestroy(d->evStart);
@@ -677,7 +724,7 @@ int32_t pe_device_render_resident(pe_device* d, const pe_camera* cam, const pe_s
     PE_CUDA(cudaSetDevice(d->ordinal));
     if ((rc = ensureFilm(d, st->width, st->height))) return rc;
     if ((rc = ensureCapacity(d, kWaveSlots))) return rc;
-    return renderWaves(d, cam, st, first, count, cancel, d->fSum, d->fCnt, d->fSq, d->paths, d->capacity, true,
+    return renderWaves(d, cam, st, first, count, cancel, d->fSum, d->fCnt, d->fSq, nullptr, d->capacity, true,
                        Tile{0, 0, st->width, st->height});
 }
 
@@ -731,7 +778,7 @@ int32_t pe_device_render(pe_device* d, const pe_camera* cam, const pe_settings* 
     if ((rc = ensureFilm(d, st->width, st->height))) return rc;
     if ((rc = pe_device_film_clear(d))) return rc;
     if ((rc = ensureCapacity(d, kWaveSlots))) return rc;
-    const int32_t rr = renderWaves(d, cam, st, first, count, cancel, d->fSum, d->fCnt, d->fSq, d->paths, d->capacity,
+    const int32_t rr = renderWaves(d, cam, st, first, count, cancel, d->fSum, d->fCnt, d->fSq, nullptr, d->capacity,
                                    true, Tile{0, 0, st->width, st->height});
     if (rr != PE_OK && rr != PE_ERR_CANCELLED) return rr;
     const size_t n = static_cast<size_t>(st->width) * static_cast<size_t>(st->height);
@@ -811,7 +858,7 @@ int32_t pe_device_render_tile_noalloc(pe_device* d, const pe_camera* cam, const 
     Paths P = noAllocPaths(d->noAllocBase);
     // The array keeps the previous call's contents; the queue and shadow counters must start at 0.
     PE_CUDA(cudaMemsetAsync(P.counters, 0, 256, d->stream));
-    return renderWaves(d, cam, st, first, count, nullptr, sumRgb, sampleCount, sumLumSq, P, kNoAllocSlots, false,
+    return renderWaves(d, cam, st, first, count, nullptr, sumRgb, sampleCount, sumLumSq, &P, kNoAllocSlots, false,
                        Tile{x0, y0, w, h});
 }
 
@@ -845,7 +892,7 @@ int32_t pe_device_set_tail_paths(pe_device* d, int64_t paths) {
 
 int64_t pe_device_tail_paths(pe_device* d) {
     if (!d) return -1;
-    return d->tailPaths < 0 ? static_cast<int64_t>(d->blocksTail) * 128 : d->tailPaths;
+    return d->tailPaths < 0 ? static_cast<int64_t>(d->blocksTail) * kTailBlock : d->tailPaths;
 }
 
 int32_t pe_device_set_counting(pe_device* d, int32_t enabled) {
@@ -882,7 +929,7 @@ int32_t pe_device_trace_primary(pe_device* d, const pe_camera* cam, const pe_set
     if (rc) return rc;
     PE_CUDA(cudaSetDevice(d->ordinal));
     WaveSeg A = makeSeg(cam, st);
-    A.filterCdf = filterTable(d, st->filter_type, st->filter_width, ++d->filterClock);
+    A.filterCdf = filterTable(d, st->filter_type, st->filter_width, ++d->filterClock, d->stream);
     if (!A.filterCdf) {
         setError("pixel filter table upload failed");
         return PE_ERR_CUDA;

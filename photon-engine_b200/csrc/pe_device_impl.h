@@ -49,6 +49,22 @@ struct Tile {
     int x0, y0, w, h;
 };
 
+// One of a device's two wave pipelines: a stream, a path-state buffer, a segment table and a
+// counter readback.  Consecutive waves of a render alternate lanes, so one wave's tail runs
+// while the next wave traces its bounces; the film kernels stay in wave order.
+struct WaveLane {
+    cudaStream_t stream = nullptr;    // lane 0 runs on the device stream
+    std::vector<DevBuf> bufs;
+    Paths paths{};
+    WaveSeg* hSegs = nullptr;         // pinned
+    WaveSeg* dSegs = nullptr;
+    cudaEvent_t evSegs = nullptr;     // the segment upload of the lane's last wave
+    bool segsInFlight = false;
+    uint32_t* hCounters = nullptr;    // pinned
+    cudaEvent_t evDone = nullptr;     // after the lane's last film kernel (timed)
+    bool pending = false;             // evDone recorded since the render call began
+};
+
 // Event bookkeeping of one render call: per-kernel device times when timing.
 struct RenderTimer {
     bool timing = false;
@@ -79,19 +95,15 @@ struct pe_device {
     float* dFilters = nullptr;
     FilterSlot filterSlots[pe_dev::kFilterSlots];
     uint64_t filterClock = 0;
-    // segment table of the wave being traced (pinned host copy, device copy)
-    WaveSeg* hSegs = nullptr;
-    WaveSeg* dSegs = nullptr;
-    cudaEvent_t evSegs = nullptr;
-    bool segsInFlight = false;
-    // wavefront state
+    // wavefront state: two lanes of `capacity` path slots each
     size_t capacity = 0;
-    std::vector<DevBuf> pathBufs;
-    Paths paths{};
+    pe_dev::WaveLane lanes[2];
+    int nextLane = 0;
+    cudaEvent_t evFilm = nullptr;     // after the last film kernel of the render call
+    int filmLane = -1;                // lane that recorded evFilm (-1: none yet)
     // [0] nodes, [1] tris (closest), [2] nodes, [3] tris (any), [4] rejected, [5] closest rays,
     // [6] shadow rays (both of the tail kernel), [7] paths ended at the per-path query bound
     unsigned long long* dStats = nullptr;
-    uint32_t* hCounters = nullptr;        // pinned
     // resident film
     int filmW = 0, filmH = 0;
     float* fSum = nullptr;
@@ -146,11 +158,13 @@ inline void freeList(std::vector<DevBuf>& list) {
 int32_t ensureCapacity(pe_device* d, size_t slots);
 int32_t checkSettings(const pe_camera* cam, const pe_settings* st);
 WaveSeg makeSeg(const pe_camera* cam, const pe_settings* st);
-const float* filterTable(pe_device* d, int type, float width, uint64_t wave);
-int32_t segsWritable(pe_device* d);
+const float* filterTable(pe_device* d, int type, float width, uint64_t wave, cudaStream_t stream);
+int32_t segsWritable(pe_device* d, int lane);
 int32_t beginRender(pe_device* d);
 int32_t endRender(pe_device* d, const RenderTimer& tm);
-int32_t runWave(pe_device* d, Paths& P, int nSegs, int nSlots, int nPix, RenderTimer& tm);
+// One wave on `lane` over the nSegs segments in lanes[lane].hSegs, with path state `P` (the
+// lane's own buffer, or the no-allocation scratch).
+int32_t runWave(pe_device* d, int lane, Paths& P, int nSegs, int nSlots, int nPix, RenderTimer& tm);
 // Uploads a built scene into device buffers owned by `bufs`; `out` gets their device view.
 int32_t uploadScene(pe_device* d, const pe_scene* s, SceneGPU& out, std::vector<DevBuf>& bufs);
 

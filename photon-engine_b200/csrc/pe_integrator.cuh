@@ -668,8 +668,12 @@ __global__ void __launch_bounds__(128, 4) kShade(SceneGPU S, Paths P, Wave W, in
 // save: each thread takes a path from the queue, alternates closest-hit queries with shadeSlot
 // (shadow rays inline) until the path ends, then takes the next.  The arithmetic and the order of
 // L's terms are the wavefront's, so the film is the same bit for bit.
+// One warp per block: a block retires as soon as its own 32 paths end, handing its registers to
+// the next wave running on the other lane.
+constexpr int kTailBlock = 32;
+
 template <bool COUNT>
-__global__ void __launch_bounds__(128) kTail(SceneGPU S, Paths P, Wave W, const int32_t* queue, const uint32_t* count,
+__global__ void __launch_bounds__(kTailBlock) kTail(SceneGPU S, Paths P, Wave W, const int32_t* queue, const uint32_t* count,
                                              unsigned long long* stats) {
     const int n = static_cast<int>(*count);
     uint32_t nodes = 0, tris = 0, shNodes = 0, shTris = 0, rays = 0, shRays = 0;

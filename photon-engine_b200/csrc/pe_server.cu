@@ -2,6 +2,9 @@
 // admitted against an HBM budget, and a worker thread that packs the pending sample ranges of
 // many requests into shared waves (continuous batching).
 //
+// Waves alternate the device's two lanes: wave k+1 is planned and its bounces traced while wave
+// k's tail still runs; a request is done once the lane of its last wave has finished.
+//
 // Scheduling.  Admitted requests are ordered by (priority desc, remaining paths asc, id asc).
 // The first request picks the wave's scene; the wave is then filled, in that order, with one
 // chunk per admitted request of the same scene until its 2M path slots are used.  A chunk is
@@ -34,6 +37,7 @@ struct Request {
     int32_t priority = 0;
     int32_t state = PE_REQ_QUEUED;
     int32_t error = PE_OK;
+    std::string message; // of a failed request
     float* sum = nullptr;
     uint32_t* cnt = nullptr;
     float* sq = nullptr;
@@ -84,7 +88,17 @@ struct pe_server {
     SceneGPU savedScene{};
     bool savedHasScene = false;
     cudaStream_t copyStream = nullptr;
+    cudaEvent_t evAdmit = nullptr;   // after the film allocations of the last admission
     pe_server_stats stats{};
+    // the wave in flight on each lane, booked once the lane's done-event fires
+    struct InFlight {
+        bool valid = false;
+        std::vector<Chunk> chunks;
+        int32_t rc = PE_OK;
+        std::string message;
+        cudaEvent_t evStart = nullptr;
+    } inflight[2];
+    int lane = 0;
 
     double now() const { return std::chrono::duration<double, std::milli>(Clock::now() - t0).count(); }
 };
@@ -131,8 +145,8 @@ void admit(pe_server* S) {
     }
 }
 
-// Packs the next wave into d->hSegs; returns its segment count (0 = nothing to do).
-int planWave(pe_server* S, int& sceneOut, int& nSlots, int& nPix, std::vector<Chunk>& chunks) {
+// Packs the next wave into the lane's segment table; returns its segment count (0 = nothing to do).
+int planWave(pe_server* S, int lane, int& sceneOut, int& nSlots, int& nPix, std::vector<Chunk>& chunks) {
     pe_device* d = S->d;
     std::vector<int64_t> order = S->active;
     std::stable_sort(order.begin(), order.end(), [&](int64_t a, int64_t b) {
@@ -157,7 +171,7 @@ int planWave(pe_server* S, int& sceneOut, int& nSlots, int& nPix, std::vector<Ch
         const int64_t room = cap - nSlots;
         if (room <= 0 || nSegs >= kMaxSegs) break;
         if (nSegs > 0 && room < 4096) break; // not worth a segment
-        const float* filter = filterTable(d, r.st.filter_type, r.st.filter_width, clock);
+        const float* filter = filterTable(d, r.st.filter_type, r.st.filter_width, clock, d->lanes[lane].stream);
         if (!filter) break; // every filter slot is taken by this wave
         WaveSeg seg = makeSeg(&r.cam, &r.st);
         seg.filterCdf = filter;
@@ -192,7 +206,7 @@ int planWave(pe_server* S, int& sceneOut, int& nSlots, int& nPix, std::vector<Ch
                 c.closesRow = true;
             }
         }
-        d->hSegs[nSegs++] = seg;
+        d->lanes[lane].hSegs[nSegs++] = seg;
         nSlots += seg.nPix * seg.nSamples;
         nPix += seg.nPix;
         r.paths += static_cast<uint64_t>(seg.nPix) * static_cast<uint64_t>(seg.nSamples);
@@ -202,63 +216,111 @@ int planWave(pe_server* S, int& sceneOut, int& nSlots, int& nPix, std::vector<Ch
     return nSegs;
 }
 
+// Books a lane's finished wave (lock held): progress of its requests, completions, device time.
+// Returns false while the wave is still running.
+bool settleLane(pe_server* S, int l) {
+    auto& f = S->inflight[l];
+    if (!f.valid) return true;
+    WaveLane& ln = S->d->lanes[l];
+    if (f.rc == PE_OK) {
+        const cudaError_t e = cudaEventQuery(ln.evDone);
+        if (e == cudaErrorNotReady) return false;
+        if (e != cudaSuccess) {
+            f.rc = PE_ERR_CUDA;
+            f.message = std::string("wave: ") + cudaMsg(e);
+        } else {
+            float ms = 0.0f;
+            if (cudaEventElapsedTime(&ms, f.evStart, ln.evDone) == cudaSuccess) S->stats.busy_ms += ms;
+        }
+    }
+    const double t = S->now();
+    for (const Chunk& c : f.chunks) {
+        Request& r = S->requests[c.id];
+        if (f.rc != PE_OK) {
+            if (r.state == PE_REQ_ACTIVE) {
+                r.state = PE_REQ_FAILED;
+                r.error = f.rc;
+                r.message = f.message;
+                r.doneMs = t;
+                ++S->stats.failed;
+            }
+            continue;
+        }
+        r.samplesDone += c.samples + (c.closesRow ? 1 : 0);
+        if (r.samplesDone >= r.spp && r.state == PE_REQ_ACTIVE) {
+            r.state = PE_REQ_DONE;
+            r.doneMs = t;
+            ++S->stats.completed;
+        }
+    }
+    S->active.erase(std::remove_if(S->active.begin(), S->active.end(),
+                                   [&](int64_t id) { return S->requests[id].state != PE_REQ_ACTIVE; }),
+                    S->active.end());
+    f.valid = false;
+    S->cvDone.notify_all();
+    return true;
+}
+
+// The worker: alternates the device's two lanes, so the next wave's bounces run while the
+// previous wave finishes its tail.  The host waits on a lane only when it needs that lane again.
 void workerLoop(pe_server* S) {
     pe_device* d = S->d;
     cudaSetDevice(d->ordinal);
     std::vector<Chunk> chunks;
     for (;;) {
         std::unique_lock<std::mutex> lk(S->mu);
-        S->cvWork.wait(lk, [&] { return S->stop || !S->queued.empty() || !S->active.empty(); });
+        settleLane(S, 0);
+        settleLane(S, 1);
+        const bool inflight = S->inflight[0].valid || S->inflight[1].valid;
+        if (!inflight)
+            S->cvWork.wait(lk, [&] { return S->stop || !S->queued.empty() || !S->active.empty(); });
         if (S->stop) break;
         admit(S);
-        if (S->active.empty()) {
-            // everything queued waits for budget held by films not yet taken
-            S->cvWork.wait_for(lk, std::chrono::milliseconds(2));
+        cudaEventRecord(S->evAdmit, d->stream);
+        const int L = S->lane;
+        if (S->inflight[L].valid) {
+            // the lane is still busy with the wave before last: wait for it outside the lock
+            lk.unlock();
+            cudaEventSynchronize(d->lanes[L].evDone);
             continue;
         }
         int scene = -1, nSlots = 0, nPix = 0;
-        if (segsWritable(d) != PE_OK) break;
-        const int nSegs = planWave(S, scene, nSlots, nPix, chunks);
+        if (segsWritable(d, L) != PE_OK) break;
+        const int nSegs = planWave(S, L, scene, nSlots, nPix, chunks);
         if (nSegs == 0) {
-            S->cvWork.wait_for(lk, std::chrono::milliseconds(1));
+            if (inflight) {
+                // nothing new to trace: wait for the other lane's wave to finish
+                lk.unlock();
+                cudaEventSynchronize(d->lanes[L ^ 1].evDone);
+            } else {
+                // everything queued waits for budget held by films not yet taken
+                S->cvWork.wait_for(lk, std::chrono::milliseconds(2));
+            }
             continue;
         }
-        lk.unlock();
-        d->scene = S->scenes[static_cast<size_t>(scene)].gpu;
-        d->hasScene = true;
-        RenderTimer tm;
-        int32_t rc = beginRender(d);
-        if (rc == PE_OK) rc = runWave(d, d->paths, nSegs, nSlots, nPix, tm);
-        if (rc == PE_OK) rc = endRender(d, tm);
-        lk.lock();
-        const double t = S->now();
+        auto& f = S->inflight[L];
+        f.chunks = chunks;
+        f.valid = true;
         ++S->stats.waves;
         S->stats.segments += static_cast<uint64_t>(nSegs);
         S->stats.paths += static_cast<uint64_t>(nSlots);
-        S->stats.busy_ms += d->stats.ms_total;
-        for (const Chunk& c : chunks) {
-            Request& r = S->requests[c.id];
-            if (rc != PE_OK) {
-                if (r.state == PE_REQ_ACTIVE) {
-                    r.state = PE_REQ_FAILED;
-                    r.error = rc;
-                    r.doneMs = t;
-                    ++S->stats.failed;
-                }
-                continue;
-            }
-            r.samplesDone += c.samples + (c.closesRow ? 1 : 0);
-            if (r.samplesDone >= r.spp && r.state == PE_REQ_ACTIVE) {
-                r.state = PE_REQ_DONE;
-                r.doneMs = t;
-                ++S->stats.completed;
-            }
-        }
-        S->active.erase(std::remove_if(S->active.begin(), S->active.end(),
-                                       [&](int64_t id) { return S->requests[id].state != PE_REQ_ACTIVE; }),
-                        S->active.end());
-        S->cvDone.notify_all();
+        lk.unlock();
+        d->scene = S->scenes[static_cast<size_t>(scene)].gpu;
+        d->hasScene = true;
+        const cudaStream_t cs = d->lanes[L].stream;
+        RenderTimer tm;
+        int32_t rc = PE_OK;
+        if (cudaStreamWaitEvent(cs, S->evAdmit, 0) != cudaSuccess || cudaEventRecord(f.evStart, cs) != cudaSuccess)
+            rc = PE_ERR_CUDA;
+        if (rc == PE_OK) rc = runWave(d, L, d->lanes[L].paths, nSegs, nSlots, nPix, tm);
+        const std::string msg = rc == PE_OK ? std::string() : std::string(pe_last_error());
+        lk.lock();
+        f.rc = rc;
+        f.message = msg;
+        S->lane = L ^ 1;
     }
+    cudaStreamSynchronize(d->lanes[0].stream);
+    cudaStreamSynchronize(d->lanes[1].stream);
 }
 
 pe_server* failCreate(char* err, size_t n, const std::string& msg) {
@@ -286,10 +348,13 @@ pe_server* pe_server_create(pe_device* d, uint64_t budget, char* err, size_t err
     S->savedScene = d->scene;
     S->savedHasScene = d->hasScene;
     S->stats.budget_bytes = budget;
-    if (cudaStreamCreateWithFlags(&S->copyStream, cudaStreamNonBlocking) != cudaSuccess) {
+    if (cudaStreamCreateWithFlags(&S->copyStream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&S->evAdmit, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreate(&S->inflight[0].evStart) != cudaSuccess || cudaEventCreate(&S->inflight[1].evStart) != cudaSuccess) {
         delete S;
-        return failCreate(err, errLen, "pe_server_create: stream creation failed");
+        return failCreate(err, errLen, "pe_server_create: stream or event creation failed");
     }
+    d->filmLane = -1;
     S->worker = std::thread(workerLoop, S);
     return S;
 }
@@ -305,12 +370,16 @@ void pe_server_destroy(pe_server* S) {
     pe_device* d = S->d;
     cudaSetDevice(d->ordinal);
     cudaStreamSynchronize(d->stream);
+    cudaStreamSynchronize(d->lanes[1].stream);
     cudaStreamSynchronize(S->copyStream);
     for (auto& kv : S->requests)
         if (kv.second.sum) cudaFreeAsync(kv.second.sum, d->stream);
     cudaStreamSynchronize(d->stream);
     for (ResidentScene& rs : S->scenes) freeList(rs.bufs);
     cudaStreamDestroy(S->copyStream);
+    cudaEventDestroy(S->evAdmit);
+    cudaEventDestroy(S->inflight[0].evStart);
+    cudaEventDestroy(S->inflight[1].evStart);
     d->scene = S->savedScene;
     d->hasScene = S->savedHasScene;
     delete S;
@@ -427,7 +496,7 @@ int32_t pe_server_wait(pe_server* S, int64_t id, int32_t timeoutMs) {
     }
     const Request& r = S->requests[id];
     if (r.state == PE_REQ_FAILED) {
-        setError("pe_server_wait: request failed");
+        setError("pe_server_wait: request failed: " + r.message);
         return r.error;
     }
     return PE_OK;

@@ -304,6 +304,29 @@ typedef struct pe_bsdf_result {
 
 int32_t pe_device_bsdf_probe(pe_device* d, int32_t material, const pe_bsdf_query* q, size_t n, pe_bsdf_result* out);
 
+/* ---- Learned directional proposal ---------------------------------------------------------------
+ * A hash grid over the scene box (16 levels x 2 features) plus the shading normal and the view
+ * direction feed a 3x64 MLP (FP16 weights, FP32 accumulation) whose 40 outputs are an 8-lobe von
+ * Mises-Fisher mixture over incident directions: 5 per lobe (direction x, y, z before
+ * normalisation, log kappa clamped to [-6, 7], weight logit).  The learned counterpart of the
+ * reference's SD-tree guiding (src/integrators/path_guiding.cpp); no reference function computes
+ * it.  Parameter block layout (FP32): W1[64][48], b1[64], W2[64][64], b2, W3[64][64], b3,
+ * W4[64][64], b4[64] (15616 floats); grid 16 x 2^18 x 2 floats. */
+enum { PE_GUIDE_MLP_PARAMS = 15616, PE_GUIDE_GRID_PARAMS = 16 * 262144 * 2, PE_GUIDE_OUTPUTS = 40 };
+/* (Re)initialises the network from a seed over the box [box_min, box_max]. */
+int32_t pe_device_guide_reset(pe_device* d, uint64_t seed, const float box_min[3], const float box_max[3]);
+int32_t pe_device_guide_get(pe_device* d, float* mlp, float* grid);
+int32_t pe_device_guide_set(pe_device* d, const float* mlp, const float* grid);
+/* Network outputs for n queries (9 floats each: position, shading normal, direction to the
+ * viewer) → out (40 floats each).  tensor_cores = 1: the tcgen05 path the renderer uses; 0: the
+ * same network in FP32 on the SIMT cores. */
+int32_t pe_device_guide_eval(pe_device* d, const float* queries, int64_t n, int32_t tensor_cores, float* out);
+/* Gradient of sum_i c_i * (-log q(w_i | x_i)) over n samples (13 floats each: position, normal,
+ * view direction, sampled direction w, weight c) into mlp_grad / grid_grad (either may be NULL),
+ * and the loss; lr > 0 then takes one Adam step with the batch-mean gradient. */
+int32_t pe_device_guide_grad(pe_device* d, const float* samples, int64_t n, float lr, float* mlp_grad, float* grid_grad,
+                             float* loss);
+
 /* ---- Request server ---------------------------------------------------------------------------
  * The served form of the render path; no class of the reference engine serves requests (its
  * RenderSession drives one device for one view).  Scenes stay resident; each

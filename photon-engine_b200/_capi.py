@@ -88,6 +88,7 @@ class pe_bsdf_result(C.Structure):
 
 
 PE_REQ_QUEUED, PE_REQ_ACTIVE, PE_REQ_DONE, PE_REQ_FAILED, PE_REQ_RELEASED = 0, 1, 2, 3, 4
+PE_GUIDE_MLP_PARAMS, PE_GUIDE_GRID_PARAMS, PE_GUIDE_OUTPUTS = 15616, 16 * 262144 * 2, 40
 
 
 class pe_request_desc(C.Structure):
@@ -152,6 +153,11 @@ SIGNATURES = {
     "pe_device_trace_primary": (C.c_int32, [P, C.POINTER(pe_camera), C.POINTER(pe_settings), C.c_int32, IP, IP, FP]),
     "pe_device_sobol": (C.c_int32, [P, C.c_uint64, IP, IP, IP, C.c_size_t, C.c_int32, FP]),
     "pe_device_bsdf_probe": (C.c_int32, [P, C.c_int32, C.POINTER(pe_bsdf_query), C.c_size_t, C.POINTER(pe_bsdf_result)]),
+    "pe_device_guide_reset": (C.c_int32, [P, C.c_uint64, FP, FP]),
+    "pe_device_guide_get": (C.c_int32, [P, FP, FP]),
+    "pe_device_guide_set": (C.c_int32, [P, FP, FP]),
+    "pe_device_guide_eval": (C.c_int32, [P, FP, C.c_int64, C.c_int32, FP]),
+    "pe_device_guide_grad": (C.c_int32, [P, FP, C.c_int64, C.c_float, FP, FP, FP]),
     "pe_server_create": (P, [P, C.c_uint64, C.c_char_p, C.c_size_t]),
     "pe_server_destroy": (None, [P]),
     "pe_server_add_scene": (C.c_int32, [P, P]),

@@ -6,6 +6,7 @@
 #include "pe_host.h"
 #include "pe_wave.h"
 
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -72,6 +73,25 @@ struct RenderTimer {
     std::vector<std::pair<size_t, size_t>> isect, shade, shadow, tail;
 };
 
+// The learned directional proposal's parameters, optimiser state and control.
+struct GuideState {
+    std::vector<DevBuf> bufs;
+    float* mlp = nullptr;       // FP32 master weights
+    __half* mlp16 = nullptr;    // FP16 copy for the tensor cores
+    float* grid = nullptr;      // hash-grid features
+    float* gradMlp = nullptr;
+    float* gradGrid = nullptr;
+    float* mMlp = nullptr;
+    float* vMlp = nullptr;
+    float* mGrid = nullptr;
+    float* vGrid = nullptr;
+    float* loss = nullptr;
+    uint32_t* err = nullptr;    // tensor-core wait ran out
+    float boxMin[3] = {0, 0, 0}, boxMax[3] = {1, 1, 1};
+    int64_t step = 0;
+    int64_t samples = 0;
+};
+
 } // namespace pe_dev
 
 // One CUDA device: stream, resident scene, wave buffers, films and counters.
@@ -121,6 +141,7 @@ struct pe_device {
     void* stage = nullptr;                 // pinned staging of the batch film (host-film render)
     size_t stageBytes = 0;
     std::string noAllocError;
+    pe_dev::GuideState guide;
 };
 
 

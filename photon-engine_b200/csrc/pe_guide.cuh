@@ -24,7 +24,6 @@ constexpr int kGridFeatures = 2;
 constexpr int kGridLog2Table = 18;                 // 2^18 entries per level
 constexpr int kGridTable = 1 << kGridLog2Table;
 constexpr int kGridParams = kGridLevels * kGridTable * kGridFeatures;
-constexpr float kGridMinRes = 16.0f, kGridMaxRes = 2048.0f;
 constexpr int kNetIn = 48;                        // 32 grid + 3 normal + 3 view + 10 zero padding
 constexpr int kNetHidden = 64;
 constexpr int kNetOut = 64;                       // 40 used: 8 lobes × (direction 3, log κ, weight logit)
@@ -50,9 +49,11 @@ struct GuideNet {
 };
 
 // ---- hash-grid encoding (Müller et al. 2022) --------------------------------------------------
+// Level resolutions 16 · 2^(7l/15) rounded (16 … 2048): a fixed table, so that no rounding of a
+// transcendental function decides a grid cell.
 PE_HD float gridScale(int level) {
-    const float b = expf((logf(kGridMaxRes) - logf(kGridMinRes)) / static_cast<float>(kGridLevels - 1));
-    return floorf(kGridMinRes * powf(b, static_cast<float>(level)));
+    constexpr float kRes[kGridLevels] = {16, 22, 31, 42, 58, 81, 111, 154, 213, 294, 406, 562, 776, 1072, 1482, 2048};
+    return kRes[level];
 }
 
 PE_HD uint32_t gridIndex(int level, uint32_t x, uint32_t y, uint32_t z, uint32_t res) {

@@ -290,7 +290,7 @@ __device__ __forceinline__ V3 ld3(const float4* a, int i) {
     return mk(v.x, v.y, v.z);
 }
 
-__device__ __noinline__ void fillHit(const SceneGPU& S, const Hit& h, V3 rayDir, Isect& is) {
+static __device__ __noinline__ void fillHit(const SceneGPU& S, const Hit& h, V3 rayDir, Isect& is) {
     const float4 e2w = __ldg(&S.tris[3 * h.prim + 2]);
     const int g = static_cast<int>(__float_as_uint(e2w.w));
     const int4 tv = __ldg(&S.triVerts[g]);

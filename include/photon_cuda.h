@@ -326,6 +326,22 @@ int32_t pe_device_guide_eval(pe_device* d, const float* queries, int64_t n, int3
  * and the loss; lr > 0 then takes one Adam step with the batch-mean gradient. */
 int32_t pe_device_guide_grad(pe_device* d, const float* samples, int64_t n, float lr, float* mlp_grad, float* grid_grad,
                              float* loss);
+/* Rendering with the proposal: mode 1 trains the network after every wave on up to 64K of its
+ * paths (each one's first guidable vertex: the radiance that arrived along the sampled direction,
+ * over the sampling pdf) and, once warmup_steps Adam steps are done, draws every guidable vertex of the
+ * first bounces (not the tail kernel's) by one-sample MIS of proposal and BSDF, 50/50, as the
+ * reference's SD-tree guiding does.  The estimate stays unbiased; results depend on the
+ * training history, so batches no longer equal single passes bit for bit.  Guided renders use
+ * one wave lane.  mode 0 turns it off (the network is kept). */
+int32_t pe_device_set_guiding(pe_device* d, int32_t mode, int32_t warmup_steps, float lr);
+typedef struct pe_guide_info {
+    int32_t mode;
+    int32_t ready;       /* sampling with the proposal */
+    int64_t steps;       /* Adam steps taken */
+    float last_loss;     /* sum of c * (-log q) of the last batch */
+    float pad;
+} pe_guide_info;
+int32_t pe_device_guide_info(pe_device* d, pe_guide_info* out);
 
 /* ---- Request server ---------------------------------------------------------------------------
  * The served form of the render path; no class of the reference engine serves requests (its

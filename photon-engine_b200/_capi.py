@@ -91,6 +91,11 @@ PE_REQ_QUEUED, PE_REQ_ACTIVE, PE_REQ_DONE, PE_REQ_FAILED, PE_REQ_RELEASED = 0, 1
 PE_GUIDE_MLP_PARAMS, PE_GUIDE_GRID_PARAMS, PE_GUIDE_OUTPUTS = 15616, 16 * 262144 * 2, 40
 
 
+class pe_guide_info(C.Structure):
+    _fields_ = [("mode", C.c_int32), ("ready", C.c_int32), ("steps", C.c_int64), ("last_loss", C.c_float),
+                ("pad", C.c_float)]
+
+
 class pe_request_desc(C.Structure):
     _fields_ = [("scene", C.c_int32), ("camera", pe_camera), ("settings", pe_settings), ("spp", C.c_int32),
                 ("priority", C.c_int32)]
@@ -158,6 +163,8 @@ SIGNATURES = {
     "pe_device_guide_set": (C.c_int32, [P, FP, FP]),
     "pe_device_guide_eval": (C.c_int32, [P, FP, C.c_int64, C.c_int32, FP]),
     "pe_device_guide_grad": (C.c_int32, [P, FP, C.c_int64, C.c_float, FP, FP, FP]),
+    "pe_device_set_guiding": (C.c_int32, [P, C.c_int32, C.c_int32, C.c_float]),
+    "pe_device_guide_info": (C.c_int32, [P, C.POINTER(pe_guide_info)]),
     "pe_server_create": (P, [P, C.c_uint64, C.c_char_p, C.c_size_t]),
     "pe_server_destroy": (None, [P]),
     "pe_server_add_scene": (C.c_int32, [P, P]),

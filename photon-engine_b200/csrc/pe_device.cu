@@ -251,6 +251,11 @@ int32_t runWave(pe_device* d, int lane, Paths& P, int nSegs, int nSlots, int nPi
     PE_CUDA(cudaEventRecord(ln.evSegs, cs));
     ln.segsInFlight = true;
     const Wave W{ln.dSegs, nSegs, nSlots, nPix};
+    // learned proposal: record training samples; sample with it once warm
+    const GuideState& G = d->guide;
+    P.guiding = (G.mode && P.guideQ) ? (G.step >= G.warmup ? 2 : 1) : 0;
+    P.guideStride = 1;
+    while (nSlots / P.guideStride > kGuideTrainRows) P.guideStride *= 2;
     kGenerate<<<sm * 8, 256, 0, cs>>>(S, P, W);
     ++stats.kernel_launches;
     ++stats.waves;
@@ -262,7 +267,9 @@ int32_t runWave(pe_device* d, int lane, Paths& P, int nSegs, int nSlots, int nPi
     uint32_t* cIn = &P.counters[0];
     uint32_t* cOut = &P.counters[1];
     stats.paths += static_cast<uint64_t>(nSlots);
-    const int64_t tailPaths = d->tailPaths < 0 ? static_cast<int64_t>(d->blocksTail) * kTailBlock : d->tailPaths;
+    int64_t tailPaths = d->tailPaths < 0 ? static_cast<int64_t>(d->blocksTail) * kTailBlock : d->tailPaths;
+    // the tail kernel runs no inference: keep guided bounces in the wavefront until few paths remain
+    if (P.guiding == 2) tailPaths = std::min<int64_t>(tailPaths, kGuideTailPaths);
     for (int iter = 0; live > 0; ++iter) {
         if (static_cast<int64_t>(live) <= tailPaths) {
             // the rest of the wave: one thread per path until it ends
@@ -297,6 +304,7 @@ int32_t runWave(pe_device* d, int lane, Paths& P, int nSegs, int nSlots, int nPi
             kIntersect<true><<<d->blocksIntersect, 128, 0, cs>>>(S, P, qIn, cIn, d->dStats);
         else
             kIntersect<false><<<d->blocksIntersect, 128, 0, cs>>>(S, P, qIn, cIn, d->dStats);
+        if (P.guiding == 2 && (rc = guideQueries(d, cs, P, W, qIn, cIn))) return rc;
         if (tm.timing) PE_CUDA(cudaEventRecord(e1, cs));
         kShade<<<d->blocksShade, 128, 0, cs>>>(S, P, W, qOut, cOut);
         if (tm.timing) PE_CUDA(cudaEventRecord(e2, cs));
@@ -333,9 +341,10 @@ int32_t runWave(pe_device* d, int lane, Paths& P, int nSegs, int nSlots, int nPi
     kFilm<<<sm * 4, 256, 0, cs>>>(P, W, &d->dStats[4]);
     PE_CUDA(cudaEventRecord(d->evFilm, cs));
     d->filmLane = lane;
+    ++stats.kernel_launches;
+    if (P.guiding && (rc = guideLearn(d, cs, P, nSlots))) return rc;
     PE_CUDA(cudaEventRecord(ln.evDone, cs));
     ln.pending = true;
-    ++stats.kernel_launches;
     PE_CUDA(cudaGetLastError());
     return PE_OK;
 }
@@ -374,9 +383,11 @@ int32_t renderWaves(pe_device* d, const pe_camera* cam, const pe_settings* st, i
                 cancelled = true;
                 break;
             }
-            // alternate lanes (the no-allocation scratch has one)
-            const int lane = scratch ? 0 : d->nextLane;
-            if (!scratch) d->nextLane ^= 1;
+            // alternate lanes (the no-allocation scratch has one; guided renders keep to lane 0
+            // so that each wave's training step lands before the next wave's inference)
+            const bool oneLane = scratch || d->guide.mode;
+            const int lane = oneLane ? 0 : d->nextLane;
+            if (!oneLane) d->nextLane ^= 1;
             Paths& P = scratch ? *scratch : d->lanes[lane].paths;
             if ((rc = segsWritable(d, lane))) return rc;
             WaveSeg& seg = d->lanes[lane].hSegs[0];

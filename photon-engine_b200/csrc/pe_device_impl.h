@@ -37,6 +37,8 @@ struct DevBuf {
 constexpr int kFilterSlots = 16;
 constexpr int kMaxSegs = 64;                    // requests sharing one wave
 constexpr size_t kWaveSlots = size_t(1) << 21;  // paths in flight per wave
+// Live paths at or below which a guided wave hands its last paths to the tail kernel.
+constexpr int64_t kGuideTailPaths = 2048;
 // Bound on the bounce-by-bounce iterations of one wave (closest-hit queries of its longest path).
 constexpr int kMaxWavefrontIterations = kMaxPathQueries;
 
@@ -90,6 +92,12 @@ struct GuideState {
     float boxMin[3] = {0, 0, 0}, boxMax[3] = {1, 1, 1};
     int64_t step = 0;
     int64_t samples = 0;
+    // rendering with the proposal
+    int mode = 0;               // 0 off, 1 learned proposal (train every wave, sample once ready)
+    int warmup = 8;             // training steps before the renderer samples with the proposal
+    float lr = 5e-3f;
+    std::vector<DevBuf> laneBufs; // per-slot buffers of lane 0
+    size_t bufCapacity = 0;
 };
 
 } // namespace pe_dev
@@ -188,5 +196,9 @@ int32_t endRender(pe_device* d, const RenderTimer& tm);
 int32_t runWave(pe_device* d, int lane, Paths& P, int nSegs, int nSlots, int nPix, RenderTimer& tm);
 // Uploads a built scene into device buffers owned by `bufs`; `out` gets their device view.
 int32_t uploadScene(pe_device* d, const pe_scene* s, SceneGPU& out, std::vector<DevBuf>& bufs);
+// Learned proposal in the wave loop (pe_guide.cu): the bounce's queries and their tensor-core
+// inference, and after the film kernel the wave's training samples and one Adam step.
+int32_t guideQueries(pe_device* d, cudaStream_t s, Paths& P, const Wave& W, const int32_t* queue, const uint32_t* count);
+int32_t guideLearn(pe_device* d, cudaStream_t s, Paths& P, int nSlots);
 
 } // namespace pe_dev

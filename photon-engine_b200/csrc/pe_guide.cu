@@ -252,7 +252,8 @@ __global__ void __launch_bounds__(kTrainWarps * 32) kGuideTrain(GuideNet g, cons
 }
 
 __global__ void kGuideAdam(float* p, float* grad, float* m, float* v, int n, float lr, float scale, float c1, float c2) {
-    const float b1 = 0.9f, b2 = 0.99f, eps = 1e-8f;
+    // ε as small as instant-ngp's: hash-grid gradients are tiny and sparse
+    const float b1 = 0.9f, b2 = 0.99f, eps = 1e-15f;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const float gi = grad[i] * scale;
         grad[i] = 0.0f;
@@ -267,6 +268,75 @@ __global__ void kGuideAdam(float* p, float* grad, float* m, float* v, int n, flo
 
 __global__ void kGuideHalf(const float* p, __half* h, int n) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) h[i] = __float2half_rn(p[i]);
+}
+
+// ---- rendering: per-bounce queries and per-wave training samples -------------------------------
+// Query rows for the queued rays whose hit the next shading step may sample with the proposal:
+// surface hits (not random-walk steps) below the depth limit on guidable materials.
+__global__ void kGuideQuery(SceneGPU S, Paths P, Wave W, const int32_t* queue, const uint32_t* count) {
+    const int n = static_cast<int>(*count);
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const int slot = queue[i];
+        const float4 hr = P.hit[slot];
+        const int prim = __float_as_int(hr.w);
+        bool want = false;
+        V3 pnt, nrm, wo;
+        if (prim >= 0) {
+            const float4 ro = P.rayO[slot];
+            const int depth = static_cast<int>(__float_as_uint(P.pickN[slot].w) & 0xFFu);
+            const WaveSeg& A = W.segs[segOfSlot(W, slot)];
+            if (!(__float_as_uint(ro.w) & RAY_WALK) && depth < A.maxDepth) {
+                const float4 rd = P.rayD[slot];
+                Hit h;
+                h.t = hr.x;
+                h.u = hr.y;
+                h.v = hr.z;
+                h.prim = prim;
+                Isect is;
+                fillHit(S, h, mk(rd.x, rd.y, rd.z), is);
+                const MatGPU& m = S.materials[is.material];
+                want = (m.flags & (MF_DELTA | MF_VOLUME_BOUNDARY | MF_TRANSMITS_SHADOWS)) == 0;
+                pnt = is.point;
+                nrm = is.normal;
+                wo = mk(-rd.x, -rd.y, -rd.z);
+            }
+        }
+        if (want) {
+            const uint32_t r = atomicAdd(&P.counters[CNT_GUIDE_Q], 1u);
+            P.guideQ[3 * r + 0] = make_float4(pnt.x, pnt.y, pnt.z, 0.0f);
+            P.guideQ[3 * r + 1] = make_float4(nrm.x, nrm.y, nrm.z, 0.0f);
+            P.guideQ[3 * r + 2] = make_float4(wo.x, wo.y, wo.z, 0.0f);
+            P.guideSlot[r] = slot;
+        }
+    }
+}
+
+// Training samples of the wave's recorded paths.  A record holds the first guidable vertex
+// (point, normal, view direction, sampled direction ω, throughput before the bounce) and the
+// radiance the path had gathered before anything arrived along ω; what the path added since,
+// over that throughput, is f·cos·L(ω)/pdf for this one sample — the weight c of −c·log q(ω).
+__global__ void kGuideCollect(Paths P, int nSlots) {
+    for (int s = (blockIdx.x * blockDim.x + threadIdx.x) * P.guideStride; s < nSlots;
+         s += gridDim.x * blockDim.x * P.guideStride) {
+        float4* rec = P.guideRec + static_cast<size_t>(s) * 6;
+        const float4 r4 = rec[4];
+        if (r4.w == 0.0f) continue;
+        rec[4] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        const float4 L = P.L[s];
+        const V3 snap = r4.w == 2.0f ? mk(r4.x, r4.y, r4.z) : mk(L.x, L.y, L.z);
+        const float4 tb = rec[5];
+        const float tl = luminance(mk(tb.x, tb.y, tb.z));
+        const float gained = luminance(mk(L.x - snap.x, L.y - snap.y, L.z - snap.z));
+        if (!(tl > 0.0f) || !(gained > 0.0f)) continue;
+        const float c = fminf(gained / tl, 64.0f);
+        if (!pe::finitef(c)) continue;
+        const uint32_t r = atomicAdd(&P.counters[CNT_TRAIN], 1u);
+        const float4 wi = rec[3];
+        P.trainBuf[4 * r + 0] = rec[0];
+        P.trainBuf[4 * r + 1] = rec[1];
+        P.trainBuf[4 * r + 2] = rec[2];
+        P.trainBuf[4 * r + 3] = make_float4(wi.x, wi.y, wi.z, c);
+    }
 }
 
 } // namespace
@@ -382,9 +452,104 @@ int32_t guideTrain(pe_device* d, cudaStream_t s, const float4* samples, const ui
     return PE_OK;
 }
 
+int32_t guideQueries(pe_device* d, cudaStream_t s, Paths& P, const Wave& W, const int32_t* queue, const uint32_t* count) {
+    PE_CUDA(cudaMemsetAsync(&P.counters[CNT_GUIDE_Q], 0, sizeof(uint32_t), s));
+    kGuideQuery<<<d->blocksIntersect, 128, 0, s>>>(d->scene, P, W, queue, count);
+    PE_CUDA(cudaGetLastError());
+    return guideInfer(d, s, P.guideQ, P.guideSlot, &P.counters[CNT_GUIDE_Q], 0, static_cast<int>(P.capacity), P.guideOut,
+                      P.guideMark);
+}
+
+int32_t guideLearn(pe_device* d, cudaStream_t s, Paths& P, int nSlots) {
+    GuideState& G = d->guide;
+    const int maxRows = (nSlots + P.guideStride - 1) / P.guideStride;
+    kGuideCollect<<<std::max(1, (maxRows + 255) / 256), 256, 0, s>>>(P, nSlots);
+    PE_CUDA(cudaGetLastError());
+    const int32_t rc = guideTrain(d, s, P.trainBuf, &P.counters[CNT_TRAIN], 0, maxRows, G.lr);
+    if (rc) return rc;
+    PE_CUDA(cudaMemsetAsync(&P.counters[CNT_TRAIN], 0, sizeof(uint32_t), s));
+    return PE_OK;
+}
+
+// Per-slot proposal buffers of lane 0 (guided renders run on one lane, so that training between
+// waves never races an inference still reading the weights).
+int32_t guideBuffers(pe_device* d) {
+    GuideState& G = d->guide;
+    Paths& P = d->lanes[0].paths;
+    if (G.bufCapacity == d->capacity && P.guideQ) return PE_OK;
+    freeList(G.laneBufs);
+    const size_t cap = d->capacity;
+    int32_t rc = 0;
+    if ((rc = devAlloc(G.laneBufs, P.guideQ, cap * 3)) || (rc = devAlloc(G.laneBufs, P.guideSlot, cap)) ||
+        (rc = devAlloc(G.laneBufs, P.guideOut, cap * 10)) || (rc = devAlloc(G.laneBufs, P.guideMark, cap)) ||
+        (rc = devAlloc(G.laneBufs, P.guideRec, cap * 6)) ||
+        (rc = devAlloc(G.laneBufs, P.trainBuf, static_cast<size_t>(kGuideTrainRows + 1) * 4))) {
+        freeList(G.laneBufs);
+        P.guideQ = nullptr;
+        return rc;
+    }
+    PE_CUDA(cudaMemsetAsync(P.guideMark, 0, cap * sizeof(uint32_t), d->stream));
+    PE_CUDA(cudaMemsetAsync(P.guideRec, 0, cap * 6 * sizeof(float4), d->stream));
+    G.bufCapacity = cap;
+    return PE_OK;
+}
+
 } // namespace pe_dev
 
 extern "C" {
+
+int32_t pe_device_set_guiding(pe_device* d, int32_t mode, int32_t warmupSteps, float lr) {
+    if (!d || mode < 0 || mode > 1 || warmupSteps < 0 || !(lr >= 0.0f)) {
+        setError("pe_device_set_guiding: bad argument");
+        return PE_ERR_INVALID;
+    }
+    PE_CUDA(cudaSetDevice(d->ordinal));
+    GuideState& G = d->guide;
+    G.mode = mode;
+    G.warmup = warmupSteps;
+    G.lr = lr;
+    if (mode == 0) return PE_OK;
+    if (!d->hasScene) {
+        setError("pe_device_set_guiding: set a scene first (its box bounds the hash grid)");
+        return PE_ERR_NO_SCENE;
+    }
+    int32_t rc = PE_OK;
+    // a network is kept across calls while it was built over this scene's box
+    float lo[3], hi[3];
+    bool same = G.mlp != nullptr;
+    for (int i = 0; i < 3; ++i) {
+        const float pad = 1e-3f * (d->scene.rootMax[i] - d->scene.rootMin[i]) + 1e-6f;
+        lo[i] = d->scene.rootMin[i] - pad;
+        hi[i] = d->scene.rootMax[i] + pad;
+        same = same && lo[i] == G.boxMin[i] && hi[i] == G.boxMax[i];
+    }
+    if (!same) {
+        for (int i = 0; i < 3; ++i) {
+            G.boxMin[i] = lo[i];
+            G.boxMax[i] = hi[i];
+        }
+        if ((rc = guideReset(d, 0x9E3779B97F4A7C15ull))) return rc;
+    }
+    if ((rc = ensureCapacity(d, kWaveSlots))) return rc;
+    return guideBuffers(d);
+}
+
+int32_t pe_device_guide_info(pe_device* d, pe_guide_info* out) {
+    if (!d || !out) {
+        setError("pe_device_guide_info: null argument");
+        return PE_ERR_INVALID;
+    }
+    std::memset(out, 0, sizeof(*out));
+    const GuideState& G = d->guide;
+    out->mode = G.mode;
+    out->steps = G.step;
+    out->ready = G.mlp && G.step >= G.warmup ? 1 : 0;
+    if (G.mlp) {
+        PE_CUDA(cudaStreamSynchronize(d->stream));
+        PE_CUDA(cudaMemcpy(&out->last_loss, G.loss, sizeof(float), cudaMemcpyDeviceToHost));
+    }
+    return PE_OK;
+}
 
 int32_t pe_device_guide_reset(pe_device* d, uint64_t seed, const float boxMin[3], const float boxMax[3]) {
     if (!d || !boxMin || !boxMax) {

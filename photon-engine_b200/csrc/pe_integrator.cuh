@@ -11,6 +11,7 @@
 #pragma once
 
 #include "pe_bsdf.h"
+#include "pe_guide.cuh"
 #include "pe_light.h"
 #include "pe_medium.h"
 #include "pe_trace.cuh"
@@ -23,26 +24,6 @@ __device__ __forceinline__ int warpFetch(uint32_t* cursor) {
     int base = 0;
     if ((threadIdx.x & 31) == 0) base = static_cast<int>(atomicAdd(cursor, 32u));
     return __shfl_sync(0xffffffffu, base, 0);
-}
-
-// Segment owning a wave slot / a wave pixel (binary search; one segment for a lone request).
-__device__ __forceinline__ int segOfSlot(const Wave& W, int slot) {
-    int lo = 0, hi = W.nSegs - 1;
-    while (lo < hi) {
-        const int mid = (lo + hi + 1) >> 1;
-        if (W.segs[mid].slotFirst <= slot) lo = mid;
-        else hi = mid - 1;
-    }
-    return lo;
-}
-__device__ __forceinline__ int segOfPixel(const Wave& W, int p) {
-    int lo = 0, hi = W.nSegs - 1;
-    while (lo < hi) {
-        const int mid = (lo + hi + 1) >> 1;
-        if (W.segs[mid].pixFirst <= p) lo = mid;
-        else hi = mid - 1;
-    }
-    return lo;
 }
 
 __device__ __forceinline__ uint32_t packCounters(int depth, int diffuse, int pass, int skips) {
@@ -87,6 +68,10 @@ __global__ void kGenerate(SceneGPU S, Paths P, Wave W) {
         P.pickP[slot] = make_float4(0.0f, 0.0f, 0.0f, __uint_as_float(sb.pixelHash));
         P.pickN[slot] = make_float4(0.0f, 0.0f, 0.0f, __uint_as_float(packCounters(0, 0, 0, 0)));
         if (S.hasVolumes | S.hasSubsurface) P.med[slot] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        if (P.guiding) {
+            P.guideMark[slot] = 0u;
+            if (slot % P.guideStride == 0) P.guideRec[static_cast<size_t>(slot) * 6 + 4] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        }
         P.queueA[slot] = slot;
     }
 }
@@ -271,6 +256,79 @@ __device__ __noinline__ int mediumSegment(const TablesGPU* T, const MatGPU& mm, 
     return SEG_SURFACE;
 }
 
+// ---- learned proposal in the shading step ------------------------------------------------------
+// Vertices the proposal may serve: non-delta surfaces that are neither volume boundaries nor
+// shadow transmitters (the reference's useGuiding condition, path_tracer.cpp:623-626).
+__device__ __forceinline__ bool guidable(const MatGPU& m) {
+    return (m.flags & (MF_DELTA | MF_VOLUME_BOUNDARY | MF_TRANSMITS_SHADOWS)) == 0;
+}
+
+__device__ __noinline__ void slotLobes(const Paths& P, int slot, Lobes& L) {
+    float o[kNetUsedOut];
+    for (int j = 0; j < kNetUsedOut / 4; ++j) {
+        const float4 v = P.guideOut[static_cast<size_t>(slot) * 10 + j];
+        o[4 * j + 0] = v.x;
+        o[4 * j + 1] = v.y;
+        o[4 * j + 2] = v.z;
+        o[4 * j + 3] = v.w;
+    }
+    decodeLobes(o, L);
+}
+
+__device__ __noinline__ float guidePdf(const Paths& P, int slot, V3 w) {
+    Lobes L;
+    slotLobes(P, slot, L);
+    return lobesPdf(L, w);
+}
+
+// Training record of a path's first guidable vertex; its radiance along wi is what the path adds
+// from here on (kGuideCollect).  False when the path has one already.
+__device__ __noinline__ bool guideRecord(const Paths& P, int slot, V3 p, V3 n, V3 wo, V3 wi, V3 thrBefore) {
+    float4* rec = P.guideRec + static_cast<size_t>(slot) * 6;
+    if (rec[4].w != 0.0f) return false;
+    rec[0] = make_float4(p.x, p.y, p.z, 0.0f);
+    rec[1] = make_float4(n.x, n.y, n.z, 0.0f);
+    rec[2] = make_float4(wo.x, wo.y, wo.z, 0.0f);
+    rec[3] = make_float4(wi.x, wi.y, wi.z, 0.0f);
+    rec[4] = make_float4(0.0f, 0.0f, 0.0f, 1.0f);
+    rec[5] = make_float4(thrBefore.x, thrBefore.y, thrBefore.z, 0.0f);
+    return true;
+}
+
+// One-sample MIS of the proposal and the BSDF, 50/50 (path_tracer.cpp:703-735 with the
+// learned mixture in place of the SD-tree): the branch number picks the strategy, the
+// proposal draws a lobe from the rest of it and a direction from one get2D.
+__device__ __noinline__ bool guidedSample(const TablesGPU* T, const MatGPU& mat, V3 wo, const ShadePoint& sp, const Paths& P,
+                                          int slot, Sobol& sb, BsdfSample& bs) {
+    Lobes L;
+    slotLobes(P, slot, L);
+    const float uBranch = get1D(sb);
+    if (uBranch < 0.5f) {
+        const V3 gwi = lobesSample(L, uBranch * 2.0f, get2D(T, sb));
+        const float gPdf = lobesPdf(L, gwi);
+        if (!(gPdf > 0.0f)) return false;
+        float bPdf = 0.0f;
+        const V3 f = bsdfEvalPdf(T, mat, wo, gwi, sp, bPdf, nullptr);
+        const float mixPdf = 0.5f * gPdf + 0.5f * bPdf;
+        if (isBlack(f) || !(mixPdf > 0.0f)) return false;
+        bs.wi = gwi;
+        bs.f = f;
+        bs.pdf = mixPdf;
+        bs.delta = false;
+        bs.passThrough = false;
+        bs.subsurface = false;
+        bs.weight = mk(0.0f);
+        return true;
+    }
+    const float uc = get1D(sb);
+    const V2 u2 = get2D(T, sb);
+    if (!bsdfSample(T, mat, wo, sp, uc, u2, bs)) return false;
+    if (bs.subsurface) bs.weight = bs.weight * 2.0f;
+    else if (bs.delta || bs.passThrough) bs.pdf *= 0.5f;
+    else if (bs.pdf > 0.0f) bs.pdf = 0.5f * bs.pdf + 0.5f * lobesPdf(L, bs.wi);
+    return true;
+}
+
 // ---- shade: Li's loop body between two closest-hit queries ------------------------------------
 // One path's step: reads the slot's state and hit record, adds the radiance found to L and
 // writes back the state for its next closest-hit query.  A path is in one of three states at
@@ -302,6 +360,11 @@ __device__ __forceinline__ bool shadeSlot(const SceneGPU& S, const Paths& P, con
     uint32_t volCtr = __float_as_uint(md.z);
     float lambda = th.w; // 0 = RGB path; > 0 = single-wavelength path after a dispersive hit
     uint32_t flags = __float_as_uint(ln.w);
+    if (flags & PF_GUIDE_SNAP) {
+        // radiance so far, the previous vertex's NEE included: the training record's baseline
+        P.guideRec[static_cast<size_t>(slot) * 6 + 4] = make_float4(L.x, L.y, L.z, 2.0f);
+        flags &= ~PF_GUIDE_SNAP;
+    }
     uint32_t ctr = __float_as_uint(pn.w);
     int depth = ctr & 0xFF, diffuseBounces = (ctr >> 8) & 0xFF, passThroughs = (ctr >> 16) & 0xFF,
         skips = (ctr >> 24) & 0xFF;
@@ -483,6 +546,9 @@ __device__ __forceinline__ bool shadeSlot(const SceneGPU& S, const Paths& P, con
         sp.frontFace = is.frontFace;
         sp.wavelength = lambda;
         const bool isSpecular = (mat.flags & MF_DELTA) != 0;
+        // this bounce's proposal, when the inference kernel left one for the slot
+        const bool useGuide = P.guiding == 2 && guidable(mat) && P.guideMark[slot] != 0u;
+        if (useGuide) P.guideMark[slot] = 0u;
         // next-event estimation (path_tracer.cpp:631-698)
         if (S.lightCount > 0 && !isSpecular) {
             LightCtx picker;
@@ -511,7 +577,8 @@ __device__ __forceinline__ bool shadeSlot(const SceneGPU& S, const Paths& P, con
                 const float cosTheta = fabsf(dot(ls.wi, is.normal));
                 if (isBlack(f) || !(cosTheta > 0.0f)) continue;
                 const float lightPdf = lightPmf * ls.pdf;
-                const float weight = powerHeuristic(shadowSamples, lightPdf, 1, bsdfPdf);
+                const float contPdf = useGuide ? 0.5f * bsdfPdf + 0.5f * guidePdf(P, slot, ls.wi) : bsdfPdf;
+                const float weight = powerHeuristic(shadowSamples, lightPdf, 1, contPdf);
                 const float scalar = cosTheta * weight / (lightPdf * static_cast<float>(shadowSamples));
                 const V3 fLi = f * ls.Li;
                 if (INLINE_SHADOW) {
@@ -537,11 +604,16 @@ __device__ __forceinline__ bool shadeSlot(const SceneGPU& S, const Paths& P, con
                 }
             }
         }
-        // BSDF sampling (path_tracer.cpp:700-743)
-        const float uc = get1D(sb);
-        const V2 u2 = get2D(T, sb);
+        // BSDF (and proposal) sampling (path_tracer.cpp:700-743)
         BsdfSample bs;
-        const bool sampled = bsdfSample(T, mat, wo, sp, uc, u2, bs);
+        bool sampled;
+        if (useGuide) {
+            sampled = guidedSample(T, mat, wo, sp, P, slot, sb, bs);
+        } else {
+            const float uc = get1D(sb);
+            const V2 u2 = get2D(T, sb);
+            sampled = bsdfSample(T, mat, wo, sp, uc, u2, bs);
+        }
         if (!sampled) {
             done = true;
         } else if (bs.subsurface) {
@@ -582,7 +654,11 @@ __device__ __forceinline__ bool shadeSlot(const SceneGPU& S, const Paths& P, con
             const V3 wi = bs.wi;
             const bool refracted = dot(wo, is.ng) * dot(wi, is.ng) < 0.0f;
             const float cosTheta = fabsf(dot(wi, is.normal));
+            const V3 thrBefore = thr;
             thr *= bs.f * (cosTheta / bs.pdf);
+            if (P.guiding && !bs.delta && slot % P.guideStride == 0 && guidable(mat) && isFinite3(thr) &&
+                guideRecord(P, slot, is.point, is.normal, wo, wi, thrBefore))
+                flags |= PF_GUIDE_SNAP;
             if (!isFinite3(thr)) {
                 done = true;
             } else {

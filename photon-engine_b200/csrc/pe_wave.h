@@ -34,6 +34,7 @@ enum PathFlags : uint32_t {
     PF_PICKER_VALID = 1u << 2,
     PF_FIRST_SEGMENT = 1u << 3,
     PF_WALK = 1u << 4,   // inside a random walk: lastP = σt, lastN = albedo, pickP.x = g
+    PF_GUIDE_SNAP = 1u << 5, // the path's guide training record waits for its radiance snapshot
 };
 
 // Per-slot state columns (capacity P slots).
@@ -56,17 +57,29 @@ struct Paths {
     float4* shC;     // f*Li xyz, flags (bit0: indirect)
     float4* shT;     // throughput at NEE xyz
     int32_t* sortQ;  // kShadeKeys segments of `capacity` slots: rays binned by shading key
+    // learned proposal (null / 0 when off)
+    float4* guideQ;      // 3 per query row, compacted per bounce: hit point | shading normal | view direction
+    int32_t* guideSlot;  // slot of each query row
+    float4* guideOut;    // 10 per slot: the 40 network outputs of this bounce's proposal
+    uint32_t* guideMark; // 1 = guideOut holds this bounce's proposal for the slot
+    float4* guideRec;    // 6 per slot: training record of the first guidable vertex (see kGuideCollect)
+    float4* trainBuf;    // 4 per training sample, compacted per wave
+    int32_t guiding;     // 0 off, 1 record training samples, 2 record and sample with the proposal
+    int32_t guideStride; // one slot in guideStride records a training sample (about 64K per wave)
     uint32_t capacity;
     // [0] queue A count, [1] queue B count, [2] shadow count, [3] closest-hit work cursor,
     // [4] any-hit work cursor, [5] shade work cursor, [6..11] rays per shading key, [12] errors,
-    // [13] tail work cursor
+    // [13] tail work cursor, [14] guide query rows, [15] training samples
     uint32_t* counters;
 };
 
 // Shading keys: 0 = miss, 1 + material type (Lambert, Disney, Dielectric, Mirror), 5 = random-walk step.
 constexpr int kShadeKeys = 6;
 enum CounterSlots { CNT_QA = 0, CNT_QB = 1, CNT_SHADOW = 2, CNT_WORK_ISECT = 3, CNT_WORK_SHADOW = 4,
-                    CNT_WORK_SHADE = 5, CNT_KEYS = 6, CNT_ERRORS = 12, CNT_WORK_TAIL = 13, CNT_TOTAL = 16 };
+                    CNT_WORK_SHADE = 5, CNT_KEYS = 6, CNT_ERRORS = 12, CNT_WORK_TAIL = 13, CNT_GUIDE_Q = 14,
+                    CNT_TRAIN = 15, CNT_TOTAL = 16 };
+// Training samples of the learned proposal per wave (the record stride is chosen to give about this many).
+constexpr int kGuideTrainRows = 1 << 16;
 
 // One request's share of a wave: a rectangle of its film, a range of its sample indices and its
 // render settings.  Wave slots [slotFirst, slotFirst + nPix·nSamples) are its paths, sample-major
@@ -96,5 +109,28 @@ struct Wave {
     int nSlots;
     int nPix;
 };
+
+#ifdef __CUDACC__
+// Segment owning a wave slot / a wave pixel (binary search; one segment for a lone request).
+__device__ __forceinline__ int segOfSlot(const Wave& W, int slot) {
+    int lo = 0, hi = W.nSegs - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (W.segs[mid].slotFirst <= slot) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+__device__ __forceinline__ int segOfPixel(const Wave& W, int p) {
+    int lo = 0, hi = W.nSegs - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (W.segs[mid].pixFirst <= p) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+#endif
 
 } // namespace pe

@@ -16,6 +16,10 @@ scenes stand in for them with the stated sizes and value distributions.
                        channel), a Henyey–Greenstein scattering sphere (g = 0.6) and a random-walk
                        subsurface slab (mean free path 1–5 mm); ~200k triangles, 1280×720,
                        512 spp, depth 24 at full size.
+* ``room_scene``       indirect-lit interior: a closed 10×8×3 m room whose only opening is a
+                       1×1 m window in the sun-facing wall, lit by the knot scene's sky; three
+                       Disney torus knots, a sphere and tables on the floor (~0.5M triangles);
+                       1920×1080 at full size.  The learned proposal's workload.
 * ``instanced_grid_scene`` a 5×4 grid of 20 seeded copies of a 262k-triangle torus knot
                        (5.2M triangles, the copies flattened into one BVH: this engine has no
                        instance level), eight Disney materials, the sky of the knot scene.
@@ -36,6 +40,7 @@ CAMERAS = {
     "knot": ((0.0, 4.5, -10.5), (0.0, 1.6, 0.0), (0.0, 1.0, 0.0), 40.0),
     "media": ((0.0, 420.0, -950.0), (0.0, 70.0, 40.0), (0.0, 1.0, 0.0), 38.0),
     "grid": ((0.0, 8.0, -13.0), (0.0, 1.0, 4.0), (0.0, 1.0, 0.0), 45.0),
+    "room": ((4.2, 1.7, 3.4), (-1.5, 0.9, -2.5), (0.0, 1.0, 0.0), 62.0),
 }
 
 
@@ -405,3 +410,66 @@ def instanced_grid_scene(width: int = 1920, height: int = 1080, spp: int = 64, m
     settings = RenderSettings(width=width, height=height, samples_per_pixel=spp, max_bounces=max_depth,
                               filter_type=PixelFilterType.BlackmanHarris, filter_width=1.5)
     return scene, camera_for("grid", width, height), settings
+
+
+def _wall_grid(origin, u, v, nu, nv, hole=None):
+    """Quad grid origin + i/nu·u + j/nv·v, facing along u × v; cells whose centre lies in
+    hole = (u0, u1, v0, v1) (fractions of u and v) are left open."""
+    o, u, v = (np.asarray(a, np.float64) for a in (origin, u, v))
+    i, j = np.meshgrid(np.arange(nu + 1), np.arange(nv + 1), indexing="ij")
+    pos = o + (i / nu)[..., None] * u + (j / nv)[..., None] * v
+    pos = pos.reshape(-1, 3)
+    tris = []
+    for a in range(nu):
+        for b in range(nv):
+            if hole is not None:
+                cu, cv = (a + 0.5) / nu, (b + 0.5) / nv
+                if hole[0] <= cu <= hole[1] and hole[2] <= cv <= hole[3]:
+                    continue
+            p00 = a * (nv + 1) + b
+            p10 = (a + 1) * (nv + 1) + b
+            tris.append((p00, p10, p10 + 1))
+            tris.append((p00, p10 + 1, p00 + 1))
+    return pos.astype(np.float32), np.array(tris, np.uint32)
+
+
+def room_scene(width: int = 1920, height: int = 1080, spp: int = 64, max_depth: int = 12, seed: int = 5,
+               knot_res=(768, 96), env_size=(2048, 1024)):
+    """The indirect-lit interior (units: metres)."""
+    rng = np.random.default_rng(seed)
+    scene = Scene()
+    X, Y, Z = 5.0, 3.0, 4.0
+    wall = Lambertian((0.75, 0.72, 0.68))
+    floor = Lambertian((0.45, 0.33, 0.22))
+    ceil = Lambertian((0.85, 0.85, 0.85))
+    # inward-facing shell; the window is 1×1 m in the z = −4 wall, 1–2 m above the floor
+    for (o, u, v, nu, nv, hole, mat) in (
+            ((-X, 0.0, -Z), (2 * X, 0.0, 0.0), (0.0, Y, 0.0), 100, 30, (0.45, 0.55, 1 / 3, 2 / 3), wall),  # z = −4 (window)
+            ((X, 0.0, Z), (-2 * X, 0.0, 0.0), (0.0, Y, 0.0), 100, 30, None, wall),                         # z = +4
+            ((-X, 0.0, Z), (0.0, 0.0, -2 * Z), (0.0, Y, 0.0), 80, 30, None, wall),                          # x = −5
+            ((X, 0.0, -Z), (0.0, 0.0, 2 * Z), (0.0, Y, 0.0), 80, 30, None, wall),                           # x = +5
+            ((-X, 0.0, Z), (2 * X, 0.0, 0.0), (0.0, 0.0, -2 * Z), 100, 80, None, floor),                   # floor
+            ((-X, Y, -Z), (2 * X, 0.0, 0.0), (0.0, 0.0, 2 * Z), 100, 80, None, ceil)):                     # ceiling
+        pos, idx = _wall_grid(o, u, v, nu, nv, hole)
+        scene.add_shape(TriangleMesh(pos, None, None, idx, mat))
+    # furniture: three knots, a sphere, two tables
+    pos, quads = torus_knot_mesh(*knot_res, tube=0.38, seed=seed)
+    q = quads.reshape(-1, 4)
+    tri = np.concatenate([q[:, [0, 1, 2]], q[:, [0, 2, 3]]], axis=0).astype(np.uint32)
+    for k, (cx, cz, sc) in enumerate(((-2.5, -1.0, 0.45), (1.5, -2.0, 0.4), (0.0, 1.5, 0.5))):
+        m = DisneyMaterial(tuple(rng.uniform(0.2, 0.9, 3)), 0.0 if k != 1 else 1.0, float(rng.uniform(0.2, 0.6)), 0.5)
+        a = rng.uniform(0.0, 2.0 * math.pi)
+        c, s_ = math.cos(a), math.sin(a)
+        rot = np.array([[c, 0.0, s_], [0.0, 1.0, 0.0], [-s_, 0.0, c]])
+        p = (pos @ rot.T) * sc + np.array([cx, 1.0 * sc + 0.45, cz])
+        scene.add_shape(TriangleMesh(p.astype(np.float32), None, None, tri, m))
+    p, n, i = uv_sphere((3.0, 0.6, -1.0), 0.6, 256, 128)
+    scene.add_shape(TriangleMesh(p, n, None, i, DisneyMaterial((0.8, 0.8, 0.85), 0.0, 0.15, 0.5)))
+    table = Lambertian((0.5, 0.4, 0.3))
+    for (tx, tz) in ((-2.5, 2.5), (2.5, 2.0)):
+        pb, ib, = _box((tx, 0.4, tz), (1.6, 0.8, 1.0), 10.0)
+        scene.add_shape(TriangleMesh(pb, None, None, ib, table))
+    scene.set_environment(EnvironmentLight(sky_environment(*env_size), 0.0, 1.0))
+    settings = RenderSettings(width=width, height=height, samples_per_pixel=spp, max_bounces=max_depth,
+                              filter_type=PixelFilterType.BlackmanHarris, filter_width=1.5)
+    return scene, camera_for("room", width, height), settings

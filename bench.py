@@ -324,13 +324,46 @@ def main():
                     help="served-mix benchmark (request server vs the plain per-request loop) instead")
     ap.add_argument("--serve-requests", type=int, default=24)
     ap.add_argument("--serve-quick", action="store_true", help="small scenes (a smoke run of the served mix)")
+    ap.add_argument("--profile-case", action="store_true",
+                    help="a small case for kernel captures: 960x540 knot waves, then guided room waves")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     if args.impl == "reference":
         return run_reference(args)
     if args.serve:
         return run_serve(args)
+    if args.profile_case:
+        return run_profile_case()
     return run_ours(args)
+
+
+def run_profile_case():
+    """Small, fixed launches for ncu captures of single kernels (a few GB on the device): three
+    1-spp passes of the knot at 960×540 (≈518 k paths per wave), then four 2-spp passes of the
+    room at 320×180 with the learned proposal on (tensor-core inference and training kernels)."""
+    pe = pe_load()
+    from photon_engine_b200 import scenes
+    dev = pe.CudaDevice(0)
+    scene, cam, st = scenes.torus_knot_scene(960, 540, 1, 12)
+    scene.build_accelerator()
+    dev.set_scene(scene)
+    times = []
+    for k in range(3):
+        dev.render_resident(cam, st, k, 1)
+        times.append(dev.last_stats().ms_total)
+    room, rcam, rst = scenes.room_scene(320, 180, 2, 8, knot_res=(256, 32), env_size=(256, 128))
+    room.build_accelerator()
+    dev.set_scene(room)
+    lib = pe._capi.load()
+    pe._capi.check(lib.pe_device_set_guiding(dev.handle, 1, 1, 3e-3))
+    film = pe.Film(320, 180)
+    for k in range(4):
+        dev.render(rcam, rst, pe.RenderTargets(beauty=film), 2 * k, 2)
+        times.append(dev.last_stats().ms_total)
+    pe._capi.check(lib.pe_device_set_guiding(dev.handle, 0, 0, 0.0))
+    print(json.dumps({"profile_case_ms": times}))
+    dev.close()
+    return 0
 
 
 def run_serve(args):

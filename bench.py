@@ -189,6 +189,7 @@ def run_ours(args):
     scene, cam, st = build_workload(pe)
     dev = pe.CudaDevice(local)
     dev.set_scene(scene)
+    tail = dev.autotune(cam, st, SPP_PER_STEP)  # untimed set-up: picks the tail threshold
     # disjoint sample indices per replica; step k renders samples base + SPP_PER_STEP·(1 + warmup + k) …
     base = rank * (args.warmup + args.steps + 8) * SPP_PER_STEP
 
@@ -300,6 +301,7 @@ def run_ours(args):
         "e2e": {"value": e2e, "unit": "paths/s", "h2d_bytes_per_step": 76 + 40,
                 "d2h_bytes_per_step": WIDTH * HEIGHT * (12 + 4 + 4)},
         "gpu_launches": int(launches),
+        "autotuned_tail_paths": tail,
         "kernel_ms_per_step": kernel_ms,
         "roofline": roof,
         "cpu_baseline": cpu,

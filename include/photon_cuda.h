@@ -263,6 +263,10 @@ int32_t pe_device_set_counting(pe_device* d, int32_t enabled);
  * film is the same either way.  -1 (default) = the paths one resident grid holds, 0 = never. */
 int32_t pe_device_set_tail_paths(pe_device* d, int64_t paths);
 int64_t pe_device_tail_paths(pe_device* d);
+/* Autotuner (no reference counterpart): renders probe_spp samples of the view with each of a few
+ * tail thresholds (1/4, 1/2, 1 and 2 resident grids) into a scratch film, twice, and keeps the
+ * fastest of the second round; chosen (may be NULL) receives it.  The caller's films are untouched. */
+int32_t pe_device_autotune(pe_device* d, const pe_camera* cam, const pe_settings* st, int32_t probe_spp, int64_t* chosen);
 /* Device-stream timer: events recorded on the stream the kernels run on; end waits for the
  * stop event and returns the elapsed device milliseconds. */
 int32_t pe_device_timer_begin(pe_device* d);

@@ -153,6 +153,7 @@ SIGNATURES = {
     "pe_device_set_counting": (C.c_int32, [P, C.c_int32]),
     "pe_device_set_tail_paths": (C.c_int32, [P, C.c_int64]),
     "pe_device_tail_paths": (C.c_int64, [P]),
+    "pe_device_autotune": (C.c_int32, [P, C.POINTER(pe_camera), C.POINTER(pe_settings), C.c_int32, C.POINTER(C.c_int64)]),
     "pe_device_timer_begin": (C.c_int32, [P]),
     "pe_device_timer_end": (C.c_int32, [P, FP]),
     "pe_device_trace_primary": (C.c_int32, [P, C.POINTER(pe_camera), C.POINTER(pe_settings), C.c_int32, IP, IP, FP]),

@@ -888,6 +888,54 @@ int32_t pe_device_last_stats(pe_device* d, pe_render_stats* out) {
     return PE_OK;
 }
 
+// Times a few tail thresholds on probe renders of the caller's view into a scratch film and keeps
+// the fastest; the film never depends on the threshold, so tuning is free to pick any of them.
+int32_t pe_device_autotune(pe_device* d, const pe_camera* cam, const pe_settings* st, int32_t probeSpp,
+                           int64_t* chosen) {
+    if (!d) {
+        setError("pe_device_autotune: null device");
+        return PE_ERR_INVALID;
+    }
+    if (!d->hasScene) {
+        setError("pe_device_autotune: set a scene first");
+        return PE_ERR_NO_SCENE;
+    }
+    int32_t rc = checkSettings(cam, st);
+    if (rc) return rc;
+    PE_CUDA(cudaSetDevice(d->ordinal));
+    if ((rc = ensureCapacity(d, kWaveSlots))) return rc;
+    const size_t n = static_cast<size_t>(st->width) * static_cast<size_t>(st->height);
+    std::vector<DevBuf> tmp;
+    float* sum = nullptr;
+    uint32_t* cnt = nullptr;
+    float* sq = nullptr;
+    if ((rc = devAlloc(tmp, sum, n * 3)) || (rc = devAlloc(tmp, cnt, n)) || (rc = devAlloc(tmp, sq, n))) {
+        freeList(tmp);
+        return rc;
+    }
+    const int64_t grid = static_cast<int64_t>(d->blocksTail) * kTailBlock;
+    const int64_t candidates[] = {grid / 4, grid / 2, grid, 2 * grid};
+    const int spp = std::max(1, probeSpp);
+    const int64_t saved = d->tailPaths;
+    float best = 1e30f;
+    int64_t pick = -1;
+    for (int pass = 0; pass < 2 && rc == PE_OK; ++pass) // first pass warms caches and kernels
+        for (int64_t c : candidates) {
+            d->tailPaths = c;
+            rc = renderWaves(d, cam, st, 1 << 24, spp, nullptr, sum, cnt, sq, nullptr, d->capacity, false,
+                             Tile{0, 0, st->width, st->height});
+            if (rc) break;
+            if (pass == 1 && d->stats.ms_total < best) {
+                best = d->stats.ms_total;
+                pick = c;
+            }
+        }
+    freeList(tmp);
+    d->tailPaths = rc == PE_OK ? pick : saved;
+    if (chosen) *chosen = d->tailPaths;
+    return rc;
+}
+
 int32_t pe_device_set_tail_paths(pe_device* d, int64_t paths) {
     if (!d) {
         setError("null device");

@@ -540,6 +540,13 @@ class CudaDevice:
     def tail_paths(self) -> int:
         return int(_lib().pe_device_tail_paths(self._h))
 
+    def autotune(self, camera: PerspectiveCamera, settings: RenderSettings, probe_spp: int = 4) -> int:
+        """Picks the tail threshold that renders this view fastest (films are unaffected)."""
+        chosen = C.c_int64(0)
+        capi.check(_lib().pe_device_autotune(self._h, C.byref(camera.describe_gpu()), C.byref(settings.to_c()),
+                                             int(probe_spp), C.byref(chosen)))
+        return int(chosen.value)
+
     # diagnostics
     def trace_primary(self, camera: PerspectiveCamera, settings: RenderSettings, sample_index: int = 0):
         n = settings.width * settings.height

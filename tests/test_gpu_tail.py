@@ -67,3 +67,23 @@ def test_tail_paths_setting(device):
         assert device.tail_paths == 12345
     finally:
         device.set_tail_paths(-1)
+
+
+def test_autotune_picks_a_threshold_and_keeps_results(pe, device):
+    scene, cam, st = scenes().cornell_box(64, 64, 8, 8, seed=5)
+    scene.build_accelerator()
+    device.set_scene(scene)
+    try:
+        device.set_tail_paths(0)
+        a = pe.Film(st.width, st.height)
+        device.render(cam, st, pe.RenderTargets(beauty=a), 0, 8)
+        device.set_tail_paths(-1)
+        grid = device.tail_paths
+        chosen = device.autotune(cam, st, 2)
+        assert chosen in (grid // 4, grid // 2, grid, 2 * grid)
+        assert device.tail_paths == chosen
+        b = pe.Film(st.width, st.height)
+        device.render(cam, st, pe.RenderTargets(beauty=b), 0, 8)
+        assert np.array_equal(a.sum.view(np.uint32), b.sum.view(np.uint32))
+    finally:
+        device.set_tail_paths(-1)

@@ -113,6 +113,27 @@ def dist_setup():
     return world, rank, local
 
 
+def replica_sample_base(rank: int, warmup: int, steps: int) -> int:
+    """First sample index of a replica: the counting pass, warm-up and timed steps of each rank
+    use disjoint sample ranges [base, base + SPP_PER_STEP·(1 + warmup + steps))."""
+    return rank * (warmup + steps + 8) * SPP_PER_STEP
+
+
+def step_samples(base: int, warmup: int, k: int) -> int:
+    """First sample of timed step k after `warmup` warm-up steps (warm-up step w: step_samples(base, 0, w))."""
+    return base + SPP_PER_STEP * (1 + warmup + k)
+
+
+def max_over_ranks(value: float, pg, device: str) -> float:
+    """Whole-job time: the maximum over ranks (all ranks call this in the same order)."""
+    if pg is None:
+        return value
+    import torch
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
 def build_workload(pe):
     import importlib
     sc = importlib.import_module("photon_engine_b200.scenes")
@@ -191,7 +212,7 @@ def run_ours(args):
     dev.set_scene(scene)
     tail = dev.autotune(cam, st, SPP_PER_STEP)  # untimed set-up: picks the tail threshold
     # disjoint sample indices per replica; step k renders samples base + SPP_PER_STEP·(1 + warmup + k) …
-    base = rank * (args.warmup + args.steps + 8) * SPP_PER_STEP
+    base = replica_sample_base(rank, args.warmup, args.steps)
 
     # algorithmic bytes per closest-hit ray, counted on the device over one untimed 1-spp pass
     dev.set_counting(True)
@@ -200,7 +221,7 @@ def run_ours(args):
     dev.set_counting(False)
     dev.film_clear()
     for w in range(args.warmup):
-        dev.render_resident(cam, st, base + SPP_PER_STEP * (1 + w), SPP_PER_STEP)
+        dev.render_resident(cam, st, step_samples(base, 0, w), SPP_PER_STEP)
     dev.synchronize()
     if pg:
         import torch
@@ -215,7 +236,7 @@ def run_ours(args):
     with ClockSampler(dev.pci_bus_id) as clocks:
         dev.timer_begin()
         for k in range(args.steps):
-            dev.render_resident(cam, st, base + SPP_PER_STEP * (1 + args.warmup + k), SPP_PER_STEP)
+            dev.render_resident(cam, st, step_samples(base, args.warmup, k), SPP_PER_STEP)
             s = dev.last_stats()
             launches += s.kernel_launches
             rays += s.closest_rays
@@ -228,10 +249,7 @@ def run_ours(args):
                 kernel_ms[key] += v / args.steps
         ms = dev.timer_end()
     if pg:
-        import torch
-        t = torch.tensor([ms], device=f"cuda:{local}")
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        ms = float(t.item())
+        ms = max_over_ranks(ms, pg, f"cuda:{local}")
         pg.barrier()
     total_paths = WIDTH * HEIGHT * SPP_PER_STEP * args.steps * world
     value = total_paths / (ms / 1000.0)
@@ -239,18 +257,15 @@ def run_ours(args):
     # end-to-end through RenderDevice::render with host films
     film = pe.Film(WIDTH, HEIGHT)
     for w in range(min(2, args.warmup)):
-        dev.render(cam, st, pe.RenderTargets(beauty=film), base + SPP_PER_STEP * (1 + w), SPP_PER_STEP)
+        dev.render(cam, st, pe.RenderTargets(beauty=film), step_samples(base, 0, w), SPP_PER_STEP)
     if pg:
         pg.barrier()
     t0 = time.perf_counter()
     for k in range(args.steps):
-        dev.render(cam, st, pe.RenderTargets(beauty=film), base + SPP_PER_STEP * (1 + args.warmup + k), SPP_PER_STEP)
+        dev.render(cam, st, pe.RenderTargets(beauty=film), step_samples(base, args.warmup, k), SPP_PER_STEP)
     e2e_s = time.perf_counter() - t0
     if pg:
-        import torch
-        t = torch.tensor([e2e_s], device=f"cuda:{local}")
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        e2e_s = float(t.item())
+        e2e_s = max_over_ranks(e2e_s, pg, f"cuda:{local}")
     e2e = total_paths / e2e_s
 
     if rank != 0:

@@ -336,7 +336,12 @@ int32_t pe_device_guide_grad(pe_device* d, const float* samples, int64_t n, floa
  * first bounces (not the tail kernel's) by one-sample MIS of proposal and BSDF, 50/50, as the
  * reference's SD-tree guiding does.  The estimate stays unbiased; results depend on the
  * training history, so batches no longer equal single passes bit for bit.  Guided renders use
- * one wave lane.  mode 0 turns it off (the network is kept). */
+ * one wave lane.  mode 0 turns it off (the network is kept).
+ * mode 2 is the reference's SD-tree guiding (RenderSettings::pathGuiding, renderer.cpp:413-429):
+ * a render from sample 0, or the first one on a new scene, starts a new field over the scene's
+ * bounds; the first 32 samples run in chunks of 2, 2, 4, 8, 16, each recording its paths'
+ * vertices into the field and refining it after, and all later samples draw from the frozen field
+ * (path_tracer.cpp:625-735, 823-883).  warmup_steps and lr are ignored. */
 int32_t pe_device_set_guiding(pe_device* d, int32_t mode, int32_t warmup_steps, float lr);
 typedef struct pe_guide_info {
     int32_t mode;
@@ -346,6 +351,24 @@ typedef struct pe_guide_info {
     float pad;
 } pe_guide_info;
 int32_t pe_device_guide_info(pe_device* d, pe_guide_info* out);
+
+/* ---- SD-tree guiding (GuidingField / DirectionalTree, src/integrators/path_guiding.{h,cpp}) ---- */
+typedef struct pe_sdtree_info {
+    int32_t ready;           /* GuidingField::ready() */
+    int32_t refinements;     /* GuidingField::refine calls since the field was built */
+    int32_t samples;         /* samples per pixel the field was trained on (<= 32) */
+    int32_t spatial_leaves;  /* GuidingField::spatialLeafCount() */
+    int64_t quad_nodes;      /* nodes of all sampling quadtrees */
+    double energy;           /* sum of the sampling trees' totals */
+} pe_sdtree_info;
+int32_t pe_device_sdtree_info(pe_device* d, pe_sdtree_info* out);
+/* Host-only check of one directional quadtree (no device needed): splats n1 (direction,
+ * radiance) pairs, refines (DirectionalTree::buildFrom with split fraction 0.01, depth 10),
+ * splats n2 more into the refined topology, refines again, then evaluates pdf(qdirs[i]) → pdf_out[i]
+ * and sample(qu[i]) → sample_out[4i..4i+3] = (direction, pdf) for nq queries. */
+int32_t pe_sdtree_probe(const float* dirs1, const float* rad1, int32_t n1, const float* dirs2, const float* rad2,
+                        int32_t n2, const float* qdirs, const float* qu, int32_t nq, float* pdf_out,
+                        float* sample_out);
 
 /* ---- Request server ---------------------------------------------------------------------------
  * The served form of the render path; no class of the reference engine serves requests (its

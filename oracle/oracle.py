@@ -66,6 +66,8 @@ def _load(fast: bool = False):
         "ref_light_pick": (C.c_int32, [P, FP, FP, FP, C.c_size_t, IP, FP, FP]),
         "ref_light_sample": (C.c_int32, [P, C.c_int32, FP, FP, FP, C.c_size_t, FP, FP, FP, FP]),
         "ref_env_eval": (C.c_int32, [P, FP, C.c_size_t, FP, FP]),
+        "ref_render_guided": (C.c_int32, [P, C.c_void_p, C.c_void_p, C.c_int32, C.c_int32, C.c_int32, FP, UP]),
+        "ref_dtree_probe": (C.c_int32, [FP, FP, C.c_int32, FP, FP, C.c_int32, FP, FP, C.c_int32, FP, FP]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -139,6 +141,16 @@ class RefScene:
         fn = self.lib.ref_render_seeded if seeded else self.lib.ref_render
         fn(self.h, C.byref(camera.describe_gpu()), C.byref(settings.to_c()), first, count, threads, _f(mean),
            cnt.ctypes.data_as(UP))
+        return mean, cnt
+
+    def render_guided(self, camera, settings, first: int, count: int, threads: int = 0):
+        """Renderer::renderSamples with SD-tree path guiding on (a fresh field, trained over the
+        first 32 samples)."""
+        h, w = settings.height, settings.width
+        mean = np.zeros((h, w, 3), np.float32)
+        cnt = np.zeros((h, w), np.uint32)
+        self.lib.ref_render_guided(self.h, C.byref(camera.describe_gpu()), C.byref(settings.to_c()), first, count,
+                                   threads, _f(mean), cnt.ctypes.data_as(UP))
         return mean, cnt
 
     def render_rows(self, camera, settings, first: int, count: int, y0: int, y1: int, threads: int = 0):
@@ -301,3 +313,16 @@ class Restatement:
         self.lib.po_render(self.h, C.byref(self._cam(camera)), w, h, settings.seed, settings.max_bounces,
                            settings.rr_depth, first, count, y0, h if y1 is None else y1, _f(mean))
         return mean
+
+
+def dtree_probe(dirs1, rad1, dirs2, rad2, qdirs, qu, fast: bool = False):
+    """The reference's DirectionalTree after two training passes (splats, buildFrom, splats,
+    buildFrom): pdf of each query direction and (direction, pdf) of each query sample."""
+    lib = _load(fast)
+    a = [np.ascontiguousarray(x, np.float32) for x in (dirs1, rad1, dirs2, rad2, qdirs, qu)]
+    nq = len(a[4])
+    pdf = np.zeros(nq, np.float32)
+    smp = np.zeros((nq, 4), np.float32)
+    lib.ref_dtree_probe(_f(a[0]), _f(a[1]), len(a[1]), _f(a[2]), _f(a[3]), len(a[3]), _f(a[4]), _f(a[5]), nq,
+                        _f(pdf), _f(smp))
+    return pdf, smp

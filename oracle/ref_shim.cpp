@@ -12,6 +12,9 @@
 //   ref_sobol        SobolSampler (src/samplers/sobol_sampler.cpp:111-146)
 //   ref_bsdf_probe   Material::evalPdf / sampleFull (src/materials/*.cpp)
 //   ref_light_*      LightSampler::prepare/sample/pmf (src/lights/light_sampler.cpp:150-284)
+//   ref_render_guided  renderSamples with RenderSettings::pathGuiding (SD-tree guiding)
+//   ref_dtree_probe  DirectionalTree::addSplat / buildFrom / pdf / sample
+//                    (src/integrators/path_guiding.cpp:80-222)
 #include "photon_cuda.h"
 
 #include "camera/camera.h"
@@ -22,6 +25,7 @@
 #include "engine/renderer.h"
 #include "engine/scene.h"
 #include "geometry/mesh.h"
+#include "integrators/path_guiding.h"
 #include "integrators/path_tracer.h"
 #include "lights/area_light.h"
 #include "lights/environment_light.h"
@@ -285,6 +289,41 @@ int32_t ref_render(void* s, const pe_camera* cam, const pe_settings* st, int32_t
     Renderer renderer;
     renderer.renderSamples(rs->scene, camera, settings, film, first, count, nullptr);
     exportFilm(film, st->width, st->height, mean_rgb, counts);
+    return 0;
+}
+
+int32_t ref_render_guided(void* s, const pe_camera* cam, const pe_settings* st, int32_t first, int32_t count,
+                          int32_t threads, float* mean_rgb, uint32_t* counts) {
+    auto* rs = static_cast<RefScene*>(s);
+    DescCamera camera(*cam);
+    RenderSettings settings = toSettings(*st, threads > 0 ? threads : hardwareThreads());
+    settings.pathGuiding = true;
+    Film film(st->width, st->height);
+    Renderer renderer;
+    renderer.renderSamples(rs->scene, camera, settings, film, first, count, nullptr);
+    exportFilm(film, st->width, st->height, mean_rgb, counts);
+    return 0;
+}
+
+// Two training passes of one directional tree as a field leaf sees them (splats, buildFrom,
+// building = sampling, splats, buildFrom), then pdf and sample queries on the sampling tree.
+int32_t ref_dtree_probe(const float* dirs1, const float* rad1, int32_t n1, const float* dirs2, const float* rad2,
+                        int32_t n2, const float* qdirs, const float* qu, int32_t nq, float* pdf_out, float* sample_out) {
+    DirectionalTree building, sampling;
+    for (int32_t i = 0; i < n1; ++i) building.addSplat(guidingDirToCanonical(v3(dirs1 + 3 * i)), rad1[i]);
+    sampling.buildFrom(building, 0.01f, 10);
+    building = sampling;
+    for (int32_t i = 0; i < n2; ++i) building.addSplat(guidingDirToCanonical(v3(dirs2 + 3 * i)), rad2[i]);
+    sampling.buildFrom(building, 0.01f, 10);
+    for (int32_t i = 0; i < nq; ++i) {
+        pdf_out[i] = sampling.pdf(v3(qdirs + 3 * i));
+        float pdf = 0.0f;
+        const Vec3f w = sampling.sample(Vec2f(qu[2 * i], qu[2 * i + 1]), pdf);
+        sample_out[4 * i + 0] = w.x;
+        sample_out[4 * i + 1] = w.y;
+        sample_out[4 * i + 2] = w.z;
+        sample_out[4 * i + 3] = pdf;
+    }
     return 0;
 }
 

@@ -96,6 +96,11 @@ class pe_guide_info(C.Structure):
                 ("pad", C.c_float)]
 
 
+class pe_sdtree_info(C.Structure):
+    _fields_ = [("ready", C.c_int32), ("refinements", C.c_int32), ("samples", C.c_int32),
+                ("spatial_leaves", C.c_int32), ("quad_nodes", C.c_int64), ("energy", C.c_double)]
+
+
 class pe_request_desc(C.Structure):
     _fields_ = [("scene", C.c_int32), ("camera", pe_camera), ("settings", pe_settings), ("spp", C.c_int32),
                 ("priority", C.c_int32)]
@@ -166,6 +171,8 @@ SIGNATURES = {
     "pe_device_guide_grad": (C.c_int32, [P, FP, C.c_int64, C.c_float, FP, FP, FP]),
     "pe_device_set_guiding": (C.c_int32, [P, C.c_int32, C.c_int32, C.c_float]),
     "pe_device_guide_info": (C.c_int32, [P, C.POINTER(pe_guide_info)]),
+    "pe_device_sdtree_info": (C.c_int32, [P, C.POINTER(pe_sdtree_info)]),
+    "pe_sdtree_probe": (C.c_int32, [FP, FP, C.c_int32, FP, FP, C.c_int32, FP, FP, C.c_int32, FP, FP]),
     "pe_server_create": (P, [P, C.c_uint64, C.c_char_p, C.c_size_t]),
     "pe_server_destroy": (None, [P]),
     "pe_server_add_scene": (C.c_int32, [P, P]),

@@ -256,6 +256,9 @@ int32_t runWave(pe_device* d, int lane, Paths& P, int nSegs, int nSlots, int nPi
     P.guiding = (G.mode && P.guideQ) ? (G.step >= G.warmup ? 2 : 1) : 0;
     P.guideStride = 1;
     while (nSlots / P.guideStride > kGuideTrainRows) P.guideStride *= 2;
+    // SD-tree guiding: the field as it stands, recording and sampling as the schedule says
+    P.sdMode = (d->guideKind == 2 && P.sdRec) ? d->sd.waveMode : 0;
+    P.sd = d->sd.field;
     kGenerate<<<sm * 8, 256, 0, cs>>>(S, P, W);
     ++stats.kernel_launches;
     ++stats.waves;
@@ -343,6 +346,7 @@ int32_t runWave(pe_device* d, int lane, Paths& P, int nSegs, int nSlots, int nPi
     d->filmLane = lane;
     ++stats.kernel_launches;
     if (P.guiding && (rc = guideLearn(d, cs, P, nSlots))) return rc;
+    if ((P.sdMode & SD_RECORD) && (rc = sdRecord(d, cs, P, nSlots))) return rc;
     PE_CUDA(cudaEventRecord(ln.evDone, cs));
     ln.pending = true;
     PE_CUDA(cudaGetLastError());
@@ -376,30 +380,43 @@ int32_t renderWaves(pe_device* d, const pe_camera* cam, const pe_settings* st, i
     RenderTimer tm;
     tm.timing = timing;
     bool cancelled = false;
-    for (int s0 = first; s0 < first + count && !cancelled; s0 += samplesPerWave) {
-        const int ns = std::min(samplesPerWave, first + count - s0);
-        for (size_t p0 = 0; p0 < npix; p0 += static_cast<size_t>(pixChunk)) {
-            if (cancel && *cancel) {
-                cancelled = true;
-                break;
+    // SD-tree guiding trains over the first 32 samples in chunks of 2, 2, 4, 8, 16 with a
+    // refinement after each, then samples from the frozen field (renderer.cpp:476-526)
+    const bool sdGuided = d->guideKind == 2 && !scratch;
+    if (sdGuided && (rc = sdBeginRender(d, first))) return rc;
+    struct ModeReset {
+        pe_device* d;
+        ~ModeReset() { d->sd.waveMode = 0; }
+    } modeReset{d};
+    for (int cur = first; cur < first + count && !cancelled;) {
+        const int chunkEnd = sdGuided ? sdChunkEnd(d, cur, first + count) : first + count;
+        for (int s0 = cur; s0 < chunkEnd && !cancelled; s0 += samplesPerWave) {
+            const int ns = std::min(samplesPerWave, chunkEnd - s0);
+            for (size_t p0 = 0; p0 < npix; p0 += static_cast<size_t>(pixChunk)) {
+                if (cancel && *cancel) {
+                    cancelled = true;
+                    break;
+                }
+                // alternate lanes (the no-allocation scratch has one; guided renders keep to lane 0
+                // so that each wave's training step lands before the next wave's inference)
+                const bool oneLane = scratch || d->guide.mode || sdGuided;
+                const int lane = oneLane ? 0 : d->nextLane;
+                if (!oneLane) d->nextLane ^= 1;
+                Paths& P = scratch ? *scratch : d->lanes[lane].paths;
+                if ((rc = segsWritable(d, lane))) return rc;
+                WaveSeg& seg = d->lanes[lane].hSegs[0];
+                seg = base;
+                seg.pixelFirst = static_cast<int>(p0);
+                seg.nPix = static_cast<int>(std::min<size_t>(static_cast<size_t>(pixChunk), npix - p0));
+                seg.sampleFirst = s0;
+                seg.nSamples = ns;
+                seg.slotFirst = 0;
+                seg.pixFirst = 0;
+                if ((rc = runWave(d, lane, P, 1, seg.nPix * ns, seg.nPix, tm))) return rc;
             }
-            // alternate lanes (the no-allocation scratch has one; guided renders keep to lane 0
-            // so that each wave's training step lands before the next wave's inference)
-            const bool oneLane = scratch || d->guide.mode;
-            const int lane = oneLane ? 0 : d->nextLane;
-            if (!oneLane) d->nextLane ^= 1;
-            Paths& P = scratch ? *scratch : d->lanes[lane].paths;
-            if ((rc = segsWritable(d, lane))) return rc;
-            WaveSeg& seg = d->lanes[lane].hSegs[0];
-            seg = base;
-            seg.pixelFirst = static_cast<int>(p0);
-            seg.nPix = static_cast<int>(std::min<size_t>(static_cast<size_t>(pixChunk), npix - p0));
-            seg.sampleFirst = s0;
-            seg.nSamples = ns;
-            seg.slotFirst = 0;
-            seg.pixFirst = 0;
-            if ((rc = runWave(d, lane, P, 1, seg.nPix * ns, seg.nPix, tm))) return rc;
         }
+        if (sdGuided && !cancelled && (rc = sdEndChunk(d, chunkEnd - cur))) return rc;
+        cur = chunkEnd;
     }
     if ((rc = endRender(d, tm))) return rc;
     if (cancelled) {
@@ -714,6 +731,7 @@ int32_t pe_device_set_scene(pe_device* d, const pe_scene* s) {
     if (rc) return rc;
     d->scene = G;
     d->hasScene = true;
+    ++d->sceneSerial;
     return PE_OK;
 }
 
@@ -919,6 +937,10 @@ int32_t pe_device_autotune(pe_device* d, const pe_camera* cam, const pe_settings
     const int64_t saved = d->tailPaths;
     float best = 1e30f;
     int64_t pick = -1;
+    // probe renders neither train nor sample a guiding field
+    const int savedKind = d->guideKind, savedMode = d->guide.mode;
+    d->guideKind = 0;
+    d->guide.mode = 0;
     for (int pass = 0; pass < 2 && rc == PE_OK; ++pass) // first pass warms caches and kernels
         for (int64_t c : candidates) {
             d->tailPaths = c;
@@ -930,6 +952,8 @@ int32_t pe_device_autotune(pe_device* d, const pe_camera* cam, const pe_settings
                 pick = c;
             }
         }
+    d->guideKind = savedKind;
+    d->guide.mode = savedMode;
     freeList(tmp);
     d->tailPaths = rc == PE_OK ? pick : saved;
     if (chosen) *chosen = d->tailPaths;

@@ -100,6 +100,45 @@ struct GuideState {
     size_t bufCapacity = 0;
 };
 
+// SD-tree guiding field: host trees, their device copies, training schedule (pe_sdtree.cu).
+struct SdHost {
+    struct Node {
+        int axis = -1;
+        int child[2] = {-1, -1};
+        int leaf = -1;
+    };
+    struct Leaf {
+        std::vector<SdQuad> samp = std::vector<SdQuad>(1);
+        float sampSum = 0.0f;
+        std::vector<SdQuad> build = std::vector<SdQuad>(1);
+        int buildOffset = 0;
+    };
+    float boxMin[3] = {0, 0, 0}, boxMax[3] = {1, 1, 1};
+    std::vector<Node> nodes;
+    std::vector<Leaf> leaves;
+    bool ready = false;
+    int iteration = 0;
+    int samplesSeen = 0;      // samples traced since the last reset
+    int nextRefine = 2;       // refine at 2, 4, 8, 16, 32 samples, then frozen
+    size_t buildNodes = 0;
+    SdField field{};
+    std::vector<DevBuf> bufs;     // device copies of the trees
+    std::vector<DevBuf> laneBufs; // per-slot records of lane 0
+    size_t bufCapacity = 0;
+    uint64_t sceneSerial = 0;     // the scene the field was trained on
+    bool initialised = false;
+    int waveMode = 0;             // SdModeBits of the waves being launched
+
+    void reset(const float bmin[3], const float bmax[3]);
+    void split(int idx, int depth);
+    void refine(const std::vector<SdQuad>& buildSums, const std::vector<float>& buildSum,
+                const std::vector<uint32_t>& counts);
+    int32_t upload(cudaStream_t s);
+    int32_t refineOnDevice(cudaStream_t s);
+};
+
+std::vector<SdQuad> refineTopology(const std::vector<SdQuad>& samp, float sum, float frac, int maxDepth);
+
 } // namespace pe_dev
 
 // One CUDA device: stream, resident scene, wave buffers, films and counters.
@@ -150,6 +189,9 @@ struct pe_device {
     size_t stageBytes = 0;
     std::string noAllocError;
     pe_dev::GuideState guide;
+    int guideKind = 0;      // 0 none, 1 learned proposal, 2 SD-tree
+    pe_dev::SdHost sd;
+    uint64_t sceneSerial = 0; // counts pe_device_set_scene calls
 };
 
 
@@ -200,5 +242,14 @@ int32_t uploadScene(pe_device* d, const pe_scene* s, SceneGPU& out, std::vector<
 // inference, and after the film kernel the wave's training samples and one Adam step.
 int32_t guideQueries(pe_device* d, cudaStream_t s, Paths& P, const Wave& W, const int32_t* queue, const uint32_t* count);
 int32_t guideLearn(pe_device* d, cudaStream_t s, Paths& P, int nSlots);
+// SD-tree guiding (pe_sdtree.cu): splats of a wave's recorded vertices; per-slot record buffers.
+int32_t sdRecord(pe_device* d, cudaStream_t s, Paths& P, int nSlots);
+int32_t sdBuffers(pe_device* d);
+// The render's training schedule: a new field for a new scene or a render from sample 0; the end
+// of the chunk of samples [cur, end) that runs under one field (waveMode set for its waves); the
+// refinement once a chunk's samples bring the count to the next refinement point.
+int32_t sdBeginRender(pe_device* d, int first);
+int sdChunkEnd(pe_device* d, int cur, int end);
+int32_t sdEndChunk(pe_device* d, int samples);
 
 } // namespace pe_dev

@@ -499,16 +499,27 @@ int32_t guideBuffers(pe_device* d) {
 extern "C" {
 
 int32_t pe_device_set_guiding(pe_device* d, int32_t mode, int32_t warmupSteps, float lr) {
-    if (!d || mode < 0 || mode > 1 || warmupSteps < 0 || !(lr >= 0.0f)) {
+    if (!d || mode < 0 || mode > 2 || warmupSteps < 0 || !(lr >= 0.0f)) {
         setError("pe_device_set_guiding: bad argument");
         return PE_ERR_INVALID;
     }
     PE_CUDA(cudaSetDevice(d->ordinal));
     GuideState& G = d->guide;
-    G.mode = mode;
+    d->guideKind = mode;
+    if (mode != 2) d->sd.initialised = false; // the SD-tree field is dropped with its setting
+    G.mode = mode == 1 ? 1 : 0;
     G.warmup = warmupSteps;
     G.lr = lr;
     if (mode == 0) return PE_OK;
+    if (mode == 2) {
+        // SD-tree guiding: the field is built by the first render (RenderSettings::pathGuiding)
+        if (!d->hasScene) {
+            setError("pe_device_set_guiding: set a scene first (its bounds span the spatial tree)");
+            return PE_ERR_NO_SCENE;
+        }
+        int32_t rc = ensureCapacity(d, kWaveSlots);
+        return rc ? rc : sdBuffers(d);
+    }
     if (!d->hasScene) {
         setError("pe_device_set_guiding: set a scene first (its box bounds the hash grid)");
         return PE_ERR_NO_SCENE;
@@ -541,7 +552,7 @@ int32_t pe_device_guide_info(pe_device* d, pe_guide_info* out) {
     }
     std::memset(out, 0, sizeof(*out));
     const GuideState& G = d->guide;
-    out->mode = G.mode;
+    out->mode = d->guideKind;
     out->steps = G.step;
     out->ready = G.mlp && G.step >= G.warmup ? 1 : 0;
     if (G.mlp) {

@@ -329,6 +329,38 @@ __device__ __noinline__ bool guidedSample(const TablesGPU* T, const MatGPU& mat,
     return true;
 }
 
+// The same one-sample MIS with the SD-tree's sampling quadtree rooted at `root`
+// (path_tracer.cpp:703-735): a direction from one get2D on the guide branch, the BSDF's
+// get1D + get2D on the other.
+__device__ __noinline__ bool sdGuidedSample(const TablesGPU* T, const MatGPU& mat, V3 wo, const ShadePoint& sp,
+                                            const SdQuad* tree, int root, Sobol& sb, BsdfSample& bs) {
+    const float uBranch = get1D(sb);
+    if (uBranch < 0.5f) {
+        float gPdf = 0.0f;
+        const V3 gwi = sdTreeSample(tree, root, get2D(T, sb), gPdf);
+        if (!(gPdf > 0.0f)) return false;
+        float bPdf = 0.0f;
+        const V3 f = bsdfEvalPdf(T, mat, wo, gwi, sp, bPdf, nullptr);
+        const float mixPdf = 0.5f * gPdf + 0.5f * bPdf;
+        if (isBlack(f) || !(mixPdf > 0.0f)) return false;
+        bs.wi = gwi;
+        bs.f = f;
+        bs.pdf = mixPdf;
+        bs.delta = false;
+        bs.passThrough = false;
+        bs.subsurface = false;
+        bs.weight = mk(0.0f);
+        return true;
+    }
+    const float uc = get1D(sb);
+    const V2 u2 = get2D(T, sb);
+    if (!bsdfSample(T, mat, wo, sp, uc, u2, bs)) return false;
+    if (bs.subsurface) bs.weight = bs.weight * 2.0f;
+    else if (bs.delta || bs.passThrough) bs.pdf *= 0.5f;
+    else if (bs.pdf > 0.0f) bs.pdf = 0.5f * bs.pdf + 0.5f * sdTreePdf(tree, root, bs.wi);
+    return true;
+}
+
 // ---- shade: Li's loop body between two closest-hit queries ------------------------------------
 // One path's step: reads the slot's state and hit record, adds the radiance found to L and
 // writes back the state for its next closest-hit query.  A path is in one of three states at
@@ -362,7 +394,13 @@ __device__ __forceinline__ bool shadeSlot(const SceneGPU& S, const Paths& P, con
     uint32_t flags = __float_as_uint(ln.w);
     if (flags & PF_GUIDE_SNAP) {
         // radiance so far, the previous vertex's NEE included: the training record's baseline
-        P.guideRec[static_cast<size_t>(slot) * 6 + 4] = make_float4(L.x, L.y, L.z, 2.0f);
+        if (P.sdMode & SD_RECORD) {
+            const uint32_t n = P.sdCount[slot];
+            if (n > 0)
+                P.sdRec[(static_cast<size_t>(slot) * kSdRecords + n - 1) * 4 + 3] = make_float4(L.x, L.y, L.z, 2.0f);
+        } else {
+            P.guideRec[static_cast<size_t>(slot) * 6 + 4] = make_float4(L.x, L.y, L.z, 2.0f);
+        }
         flags &= ~PF_GUIDE_SNAP;
     }
     uint32_t ctr = __float_as_uint(pn.w);
@@ -549,6 +587,12 @@ __device__ __forceinline__ bool shadeSlot(const SceneGPU& S, const Paths& P, con
         // this bounce's proposal, when the inference kernel left one for the slot
         const bool useGuide = P.guiding == 2 && guidable(mat) && P.guideMark[slot] != 0u;
         if (useGuide) P.guideMark[slot] = 0u;
+        // or the SD-tree's sampling quadtree of the vertex's spatial leaf (path_tracer.cpp:627-629)
+        int sdRoot = -1;
+        if ((P.sdMode & SD_SAMPLE) && !useGuide && guidable(mat)) {
+            const int leaf = sdLeafWithData(P.sd, is.point);
+            if (leaf >= 0) sdRoot = P.sd.leaves[leaf].sampRoot;
+        }
         // next-event estimation (path_tracer.cpp:631-698)
         if (S.lightCount > 0 && !isSpecular) {
             LightCtx picker;
@@ -577,7 +621,9 @@ __device__ __forceinline__ bool shadeSlot(const SceneGPU& S, const Paths& P, con
                 const float cosTheta = fabsf(dot(ls.wi, is.normal));
                 if (isBlack(f) || !(cosTheta > 0.0f)) continue;
                 const float lightPdf = lightPmf * ls.pdf;
-                const float contPdf = useGuide ? 0.5f * bsdfPdf + 0.5f * guidePdf(P, slot, ls.wi) : bsdfPdf;
+                const float contPdf = useGuide     ? 0.5f * bsdfPdf + 0.5f * guidePdf(P, slot, ls.wi)
+                                      : sdRoot >= 0 ? 0.5f * bsdfPdf + 0.5f * sdTreePdf(P.sd.samp, sdRoot, ls.wi)
+                                                    : bsdfPdf;
                 const float weight = powerHeuristic(shadowSamples, lightPdf, 1, contPdf);
                 const float scalar = cosTheta * weight / (lightPdf * static_cast<float>(shadowSamples));
                 const V3 fLi = f * ls.Li;
@@ -609,6 +655,8 @@ __device__ __forceinline__ bool shadeSlot(const SceneGPU& S, const Paths& P, con
         bool sampled;
         if (useGuide) {
             sampled = guidedSample(T, mat, wo, sp, P, slot, sb, bs);
+        } else if (sdRoot >= 0) {
+            sampled = sdGuidedSample(T, mat, wo, sp, P.sd.samp, sdRoot, sb, bs);
         } else {
             const float uc = get1D(sb);
             const V2 u2 = get2D(T, sb);
@@ -687,6 +735,21 @@ __device__ __forceinline__ bool shadeSlot(const SceneGPU& S, const Paths& P, con
                 if (depth > A.rrDepth && !russianRoulette(thr, sb)) {
                     cont = false;
                     done = true;
+                }
+                // SD-tree training vertex (path_tracer.cpp:823-827, recordable ones only): its
+                // incident radiance is what L gains from here on over the throughput after the
+                // bounce and the roulette
+                if (cont && (P.sdMode & SD_RECORD) && !bs.delta && !(mat.flags & MF_VOLUME_BOUNDARY)) {
+                    const uint32_t n = P.sdCount[slot];
+                    if (n < static_cast<uint32_t>(kSdRecords)) {
+                        float4* rec = P.sdRec + (static_cast<size_t>(slot) * kSdRecords + n) * 4;
+                        rec[0] = make_float4(is.point.x, is.point.y, is.point.z, bs.pdf);
+                        rec[1] = make_float4(wi.x, wi.y, wi.z, 0.0f);
+                        rec[2] = make_float4(thr.x, thr.y, thr.z, 0.0f);
+                        rec[3] = make_float4(0.0f, 0.0f, 0.0f, 1.0f);
+                        P.sdCount[slot] = n + 1;
+                        flags |= PF_GUIDE_SNAP;
+                    }
                 }
             }
         }

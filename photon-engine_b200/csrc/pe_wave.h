@@ -4,6 +4,7 @@
 #pragma once
 
 #include "pe_math.h"
+#include "pe_sdtree.h"
 
 #include <cstdint>
 #include <vector_types.h>
@@ -66,6 +67,11 @@ struct Paths {
     float4* trainBuf;    // 4 per training sample, compacted per wave
     int32_t guiding;     // 0 off, 1 record training samples, 2 record and sample with the proposal
     int32_t guideStride; // one slot in guideStride records a training sample (about 64K per wave)
+    // SD-tree guiding (null / 0 when off)
+    SdField sd;          // sampling trees (read), building trees (splats)
+    int32_t sdMode;      // bit 0: record training vertices, bit 1: sample with the SD-tree
+    float4* sdRec;       // kSdRecords × 4 per slot: (point, pdf) | (ω, 0) | (throughput after, 0) | (radiance snapshot, state)
+    uint32_t* sdCount;   // recorded vertices per slot
     uint32_t capacity;
     // [0] queue A count, [1] queue B count, [2] shadow count, [3] closest-hit work cursor,
     // [4] any-hit work cursor, [5] shade work cursor, [6..11] rays per shading key, [12] errors,
@@ -78,6 +84,10 @@ constexpr int kShadeKeys = 6;
 enum CounterSlots { CNT_QA = 0, CNT_QB = 1, CNT_SHADOW = 2, CNT_WORK_ISECT = 3, CNT_WORK_SHADOW = 4,
                     CNT_WORK_SHADE = 5, CNT_KEYS = 6, CNT_ERRORS = 12, CNT_WORK_TAIL = 13, CNT_GUIDE_Q = 14,
                     CNT_TRAIN = 15, CNT_TOTAL = 16 };
+// Vertices an SD-tree training path records (the reference records up to 32; its paths in these
+// workloads rarely pass 8 guidable vertices).
+constexpr int kSdRecords = 8;
+enum SdModeBits { SD_RECORD = 1, SD_SAMPLE = 2 };
 // Training samples of the learned proposal per wave (the record stride is chosen to give about this many).
 constexpr int kGuideTrainRows = 1 << 16;
 

@@ -481,6 +481,7 @@ class CudaDevice:
             flag = cancel if isinstance(cancel, C.c_int32) else C.c_int32(1 if cancel else 0)
         traced = C.c_uint64(0)
         with self._lock:
+            self._sync_guiding(settings)
             rc = _lib().pe_device_render(self._h, C.byref(camera.describe_gpu()), C.byref(st), first_sample, count,
                                          C.byref(flag) if flag is not None else None, capi.fptr(film.sum),
                                          capi.uptr(film.count), capi.fptr(film.sum_sq), C.byref(traced))
@@ -490,8 +491,28 @@ class CudaDevice:
         film.rejected += int(self.last_stats().rejected)
         return SampleBatchResult(True, traced.value)
 
+    def _sync_guiding(self, settings: RenderSettings):
+        # RenderSettings::pathGuiding (renderer.cpp:413-429): SD-tree guiding on while it is set;
+        # turning it off drops the field
+        mode = getattr(self, "_guide_mode", 0)
+        if settings.path_guiding and mode != 2:
+            self.set_guiding(2)
+        elif not settings.path_guiding and mode == 2:
+            self.set_guiding(0)
+
+    def set_guiding(self, mode: int, warmup_steps: int = 0, lr: float = 0.0):
+        """0 off, 1 the learned directional proposal, 2 SD-tree guiding (pe_device_set_guiding)."""
+        capi.check(_lib().pe_device_set_guiding(self._h, int(mode), int(warmup_steps), float(lr)))
+        self._guide_mode = int(mode)
+
+    def sdtree_info(self) -> capi.pe_sdtree_info:
+        out = capi.pe_sdtree_info()
+        capi.check(_lib().pe_device_sdtree_info(self._h, C.byref(out)))
+        return out
+
     # resident-film path (no host film traffic per batch)
     def render_resident(self, camera: PerspectiveCamera, settings: RenderSettings, first_sample: int, count: int):
+        self._sync_guiding(settings)
         st = settings.to_c()
         capi.check(_lib().pe_device_render_resident(self._h, C.byref(camera.describe_gpu()), C.byref(st),
                                                     first_sample, count, None))

@@ -36,6 +36,10 @@ int32_t ensureCapacity(pe_device* d, size_t slots) {
         for (float4** c : scols)
             if ((st = devAlloc(ln.bufs, *c, slots))) return st;
         if ((st = devAlloc(ln.bufs, P.counters, CNT_TOTAL))) return st;
+        // path regeneration: slot → path, freed slots, radiance of kStreamFactor × slots paths
+        if ((st = devAlloc(ln.bufs, ln.pathOf, slots))) return st;
+        if ((st = devAlloc(ln.bufs, ln.freeQ, slots))) return st;
+        if ((st = devAlloc(ln.bufs, ln.Lout, slots * kStreamFactor))) return st;
         P.capacity = static_cast<uint32_t>(slots);
     }
     d->capacity = slots;
@@ -259,10 +263,22 @@ int32_t runWave(pe_device* d, int lane, Paths& P, int nSegs, int nSlots, int nPi
     // SD-tree guiding: the field as it stands, recording and sampling as the schedule says
     P.sdMode = (d->guideKind == 2 && P.sdRec) ? d->sd.waveMode : 0;
     P.sd = d->sd.field;
-    kGenerate<<<sm * 8, 256, 0, cs>>>(S, P, W);
+    // path regeneration: a wave of more paths than slots (unguided waves on a lane's own state)
+    const int64_t slotCap = static_cast<int64_t>(P.capacity);
+    const bool regen = &P == &ln.paths && ln.Lout && !P.guiding && !P.sdMode && nSlots > slotCap;
+    P.pathOf = regen ? ln.pathOf : nullptr;
+    P.freeQ = regen ? ln.freeQ : nullptr;
+    P.Lout = regen ? ln.Lout : nullptr;
+    if (nSlots > (regen ? slotCap * kStreamFactor : slotCap)) {
+        setError("wave of " + std::to_string(nSlots) + " paths exceeds its path state");
+        return PE_ERR_LIMIT;
+    }
+    const int firstPaths = static_cast<int>(std::min<int64_t>(nSlots, slotCap));
+    int nextPath = firstPaths;
+    kGenerate<<<sm * 8, 256, 0, cs>>>(S, P, W, firstPaths);
     ++stats.kernel_launches;
     ++stats.waves;
-    uint32_t live = static_cast<uint32_t>(nSlots);
+    uint32_t live = static_cast<uint32_t>(firstPaths);
     PE_CUDA(cudaMemsetAsync(&P.counters[1], 0, (CNT_TOTAL - 1) * sizeof(uint32_t), cs));
     PE_CUDA(cudaMemcpyAsync(&P.counters[0], &live, sizeof(uint32_t), cudaMemcpyHostToDevice, cs));
     int32_t* qIn = P.queueA;
@@ -274,7 +290,7 @@ int32_t runWave(pe_device* d, int lane, Paths& P, int nSegs, int nSlots, int nPi
     // the tail kernel runs no inference: keep guided bounces in the wavefront until few paths remain
     if (P.guiding == 2) tailPaths = std::min<int64_t>(tailPaths, kGuideTailPaths);
     for (int iter = 0; live > 0; ++iter) {
-        if (static_cast<int64_t>(live) <= tailPaths) {
+        if (static_cast<int64_t>(live) <= tailPaths && nextPath == nSlots) {
             // the rest of the wave: one thread per path until it ends
             const int grid = static_cast<int>(
                 std::min<int64_t>(d->blocksTail, (static_cast<int64_t>(live) + kTailBlock - 1) / kTailBlock));
@@ -293,6 +309,10 @@ int32_t runWave(pe_device* d, int lane, Paths& P, int nSegs, int nSlots, int nPi
             }
             ++stats.kernel_launches;
             stats.tail_paths += live;
+            if (regen) {
+                kFlush<<<sm * 4, 256, 0, cs>>>(P, qIn, cIn);
+                ++stats.kernel_launches;
+            }
             break;
         }
         stats.closest_rays += live;
@@ -323,11 +343,23 @@ int32_t runWave(pe_device* d, int lane, Paths& P, int nSegs, int nSlots, int nPi
             tm.shade.push_back({tm.evUsed - 3, tm.evUsed - 2});
             tm.shadow.push_back({tm.evUsed - 2, tm.evUsed - 1});
         }
-        PE_CUDA(cudaMemcpyAsync(ln.hCounters, P.counters, 4 * sizeof(uint32_t), cudaMemcpyDeviceToHost, cs));
+        PE_CUDA(cudaMemcpyAsync(ln.hCounters, P.counters, CNT_TOTAL * sizeof(uint32_t), cudaMemcpyDeviceToHost, cs));
         PE_CUDA(cudaStreamSynchronize(cs));
         stats.shadow_rays += ln.hCounters[CNT_SHADOW];
         live = cOut == &P.counters[1] ? ln.hCounters[1] : ln.hCounters[0];
-        if (iter > kMaxWavefrontIterations) {
+        if (regen) {
+            // ended paths hand over their radiance; their slots take the wave's next paths
+            const int freed = static_cast<int>(ln.hCounters[CNT_FREE]);
+            const int fresh = std::min(freed, nSlots - nextPath);
+            if (freed > 0) {
+                kRecycle<<<sm * 4, 256, 0, cs>>>(S, P, W, freed, fresh, nextPath, qOut, static_cast<int>(live), cOut);
+                ++stats.kernel_launches;
+                PE_CUDA(cudaMemsetAsync(&P.counters[CNT_FREE], 0, sizeof(uint32_t), cs));
+            }
+            nextPath += fresh;
+            live += static_cast<uint32_t>(fresh);
+        }
+        if (iter > kMaxWavefrontIterations * (regen ? kStreamFactor + 1 : 1)) {
             setError("wavefront did not drain after " + std::to_string(kMaxWavefrontIterations) + " iterations");
             return PE_ERR_DEVICE;
         }
@@ -360,8 +392,11 @@ int32_t renderWaves(pe_device* d, const pe_camera* cam, const pe_settings* st, i
                     const volatile int32_t* cancel, float* sum, uint32_t* cnt, float* sq, Paths* scratch, size_t capacity,
                     bool timing, Tile tile) {
     const size_t npix = static_cast<size_t>(tile.w) * static_cast<size_t>(tile.h);
-    const int pixChunk = static_cast<int>(std::min(npix, capacity));
-    const int samplesPerWave = static_cast<int>(std::max<size_t>(1, std::min<size_t>(static_cast<size_t>(count), capacity / pixChunk)));
+    // unguided waves on the lanes' own state regenerate paths: kStreamFactor × the slots per wave
+    const bool regenWaves = !scratch && !d->guide.mode && d->guideKind != 2;
+    const size_t pathCap = regenWaves ? capacity * kStreamFactor : capacity;
+    const int pixChunk = static_cast<int>(std::min(npix, pathCap));
+    const int samplesPerWave = static_cast<int>(std::max<size_t>(1, std::min<size_t>(static_cast<size_t>(count), pathCap / pixChunk)));
     WaveSeg base = makeSeg(cam, st);
     // uploaded on the device stream before evStart, which the second lane waits for
     base.filterCdf = filterTable(d, st->filter_type, st->filter_width, ++d->filterClock, d->stream);
@@ -629,7 +664,7 @@ pe_device* pe_device_create(int32_t ordinal, char* err, size_t errLen) {
                 cudaSuccess ||
             cudaMalloc(&ln.dSegs, kMaxSegs * sizeof(WaveSeg)) != cudaSuccess ||
             cudaMallocHost(&ln.hSegs, kMaxSegs * sizeof(WaveSeg)) != cudaSuccess ||
-            cudaMallocHost(&ln.hCounters, 16 * sizeof(uint32_t)) != cudaSuccess ||
+            cudaMallocHost(&ln.hCounters, 32 * sizeof(uint32_t)) != cudaSuccess ||
             cudaEventCreateWithFlags(&ln.evSegs, cudaEventDisableTiming) != cudaSuccess ||
             cudaEventCreate(&ln.evDone) != cudaSuccess) {
             pe_device_destroy(d);

@@ -64,6 +64,9 @@ struct WaveLane {
     cudaEvent_t evSegs = nullptr;     // the segment upload of the lane's last wave
     bool segsInFlight = false;
     uint32_t* hCounters = nullptr;    // pinned
+    int32_t* pathOf = nullptr;        // path regeneration buffers (in bufs)
+    int32_t* freeQ = nullptr;
+    float4* Lout = nullptr;
     cudaEvent_t evDone = nullptr;     // after the lane's last film kernel (timed)
     bool pending = false;             // evDone recorded since the render call began
 };

@@ -44,35 +44,67 @@ __device__ __forceinline__ void queuePush(int32_t* queue, uint32_t* counter, boo
     queue[base + rank] = value;
 }
 
-// ---- generate: camera rays for every slot of the wave ------------------------------------------
-__global__ void kGenerate(SceneGPU S, Paths P, Wave W) {
+// ---- generate: camera rays ------------------------------------------------------------------
+// Wave path `path` (its segment, sample and pixel) starts in `slot`.
+__device__ __forceinline__ void generatePath(const SceneGPU& S, const Paths& P, const Wave& W, int slot, int path) {
     const TablesGPU* T = S.tables;
-    for (int slot = blockIdx.x * blockDim.x + threadIdx.x; slot < W.nSlots; slot += gridDim.x * blockDim.x) {
-        const WaveSeg& A = W.segs[segOfSlot(W, slot)];
-        const int local = slot - A.slotFirst;
-        const int sOff = local / A.nPix;
-        const int pix = A.pixelFirst + (local - sOff * A.nPix);
-        const int x = A.tileX + pix % A.tileW, y = A.tileY + pix / A.tileW;
-        Sobol sb;
-        sb.pixelHash = pixelHashOf(A.seed, x, y);
-        sb.revIndex = rev32(static_cast<uint32_t>(A.sampleFirst + sOff));
-        sb.dim = 0;
-        V3 o, d;
-        cameraRay(T, A.filterCdf, A.cam, A.filterWidth, x, y, A.width, A.height, sb, o, d);
-        P.rayO[slot] = make_float4(o.x, o.y, o.z, __uint_as_float(VIS_CAMERA));
-        P.rayD[slot] = make_float4(d.x, d.y, d.z, 0.0f);
-        P.thr[slot] = make_float4(1.0f, 1.0f, 1.0f, 0.0f);
-        P.L[slot] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-        P.lastN[slot] = make_float4(0.0f, 1.0f, 0.0f, __uint_as_float(PF_SPECULAR_BOUNCE | PF_CAMERA_RAY | PF_FIRST_SEGMENT));
-        P.lastP[slot] = make_float4(o.x, o.y, o.z, __uint_as_float(sb.dim));
-        P.pickP[slot] = make_float4(0.0f, 0.0f, 0.0f, __uint_as_float(sb.pixelHash));
-        P.pickN[slot] = make_float4(0.0f, 0.0f, 0.0f, __uint_as_float(packCounters(0, 0, 0, 0)));
-        if (S.hasVolumes | S.hasSubsurface) P.med[slot] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-        if (P.guiding) {
-            P.guideMark[slot] = 0u;
-            if (slot % P.guideStride == 0) P.guideRec[static_cast<size_t>(slot) * 6 + 4] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-        }
+    const WaveSeg& A = W.segs[segOfSlot(W, path)];
+    const int local = path - A.slotFirst;
+    const int sOff = local / A.nPix;
+    const int pix = A.pixelFirst + (local - sOff * A.nPix);
+    const int x = A.tileX + pix % A.tileW, y = A.tileY + pix / A.tileW;
+    Sobol sb;
+    sb.pixelHash = pixelHashOf(A.seed, x, y);
+    sb.revIndex = rev32(static_cast<uint32_t>(A.sampleFirst + sOff));
+    sb.dim = 0;
+    V3 o, d;
+    cameraRay(T, A.filterCdf, A.cam, A.filterWidth, x, y, A.width, A.height, sb, o, d);
+    P.rayO[slot] = make_float4(o.x, o.y, o.z, __uint_as_float(VIS_CAMERA));
+    P.rayD[slot] = make_float4(d.x, d.y, d.z, 0.0f);
+    P.thr[slot] = make_float4(1.0f, 1.0f, 1.0f, 0.0f);
+    P.L[slot] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    P.lastN[slot] = make_float4(0.0f, 1.0f, 0.0f, __uint_as_float(PF_SPECULAR_BOUNCE | PF_CAMERA_RAY | PF_FIRST_SEGMENT));
+    P.lastP[slot] = make_float4(o.x, o.y, o.z, __uint_as_float(sb.dim));
+    P.pickP[slot] = make_float4(0.0f, 0.0f, 0.0f, __uint_as_float(sb.pixelHash));
+    P.pickN[slot] = make_float4(0.0f, 0.0f, 0.0f, __uint_as_float(packCounters(0, 0, 0, 0)));
+    if (S.hasVolumes | S.hasSubsurface) P.med[slot] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    if (P.guiding) {
+        P.guideMark[slot] = 0u;
+        if (slot % P.guideStride == 0) P.guideRec[static_cast<size_t>(slot) * 6 + 4] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    }
+    if (P.pathOf) P.pathOf[slot] = path;
+}
+
+// The wave's first `count` paths into slots [0, count), all queued.
+__global__ void kGenerate(SceneGPU S, Paths P, Wave W, int count) {
+    for (int slot = blockIdx.x * blockDim.x + threadIdx.x; slot < count; slot += gridDim.x * blockDim.x) {
+        generatePath(S, P, W, slot, slot);
         P.queueA[slot] = slot;
+    }
+}
+
+// After a bounce of a regenerating wave: every slot freed this bounce hands its path's radiance
+// to Lout (its NEE terms are in by now), and the first `fresh` of them take the wave's paths
+// [nextPath, nextPath + fresh), appended to the next closest-hit queue after its `queued` entries.
+__global__ void kRecycle(SceneGPU S, Paths P, Wave W, int freed, int fresh, int nextPath, int32_t* queue, int queued,
+                         uint32_t* queueCount) {
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < freed; k += gridDim.x * blockDim.x) {
+        const int slot = P.freeQ[k];
+        P.Lout[P.pathOf[slot]] = P.L[slot];
+        if (k < fresh) {
+            generatePath(S, P, W, slot, nextPath + k);
+            queue[queued + k] = slot;
+        }
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) *queueCount = static_cast<uint32_t>(queued + fresh);
+}
+
+// The radiance of the paths the tail kernel finished, to Lout.
+__global__ void kFlush(Paths P, const int32_t* queue, const uint32_t* count) {
+    const int n = static_cast<int>(*count);
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const int slot = queue[i];
+        P.Lout[P.pathOf[slot]] = P.L[slot];
     }
 }
 
@@ -370,7 +402,7 @@ __device__ __noinline__ bool sdGuidedSample(const TablesGPU* T, const MatGPU& ma
 // shadow rays go to the any-hit queue, or with INLINE_SHADOW are traced here and their terms
 // added to L at once, in the same order.  Returns whether the path goes on.
 template <bool INLINE_SHADOW, bool COUNT>
-__device__ __forceinline__ bool shadeSlot(const SceneGPU& S, const Paths& P, const WaveSeg& A, int slot,
+__device__ __forceinline__ bool shadeSlot(const SceneGPU& S, const Paths& P, const WaveSeg& A, int slot, int path,
                                           uint32_t& shNodes, uint32_t& shTris, uint32_t& shRays) {
     const TablesGPU* T = S.tables;
     const bool volumetric = (S.hasVolumes | S.hasSubsurface) != 0;
@@ -409,7 +441,7 @@ __device__ __forceinline__ bool shadeSlot(const SceneGPU& S, const Paths& P, con
     Sobol sb;
     sb.pixelHash = __float_as_uint(pp.w);
     {
-        const int sOff = (slot - A.slotFirst) / A.nPix;
+        const int sOff = (path - A.slotFirst) / A.nPix;
         sb.revIndex = rev32(static_cast<uint32_t>(A.sampleFirst + sOff));
     }
     sb.dim = __float_as_uint(lp.w);
@@ -796,9 +828,12 @@ __global__ void __launch_bounds__(128, 4) kShade(SceneGPU S, Paths P, Wave W, in
                 ++k;
             }
             slot = P.sortQ[static_cast<size_t>(k) * P.capacity + j];
-            cont = shadeSlot<false, false>(S, P, W.segs[segOfSlot(W, slot)], slot, unused0, unused1, unused2);
+            const int path = pathOfSlot(P, slot);
+            cont = shadeSlot<false, false>(S, P, W.segs[segOfSlot(W, path)], slot, path, unused0, unused1, unused2);
         }
         queuePush(nextQueue, nextCount, cont, slot);
+        // a regenerating wave refills the slots of ended paths
+        if (P.pathOf) queuePush(P.freeQ, &P.counters[CNT_FREE], !cont && slot >= 0, slot);
     }
 }
 
@@ -820,7 +855,8 @@ __global__ void __launch_bounds__(kTailBlock) kTail(SceneGPU S, Paths P, Wave W,
         const int i = static_cast<int>(atomicAdd(&P.counters[CNT_WORK_TAIL], 1u));
         if (i >= n) break;
         const int slot = queue[i];
-        const WaveSeg& A = W.segs[segOfSlot(W, slot)];
+        const int path = pathOfSlot(P, slot);
+        const WaveSeg& A = W.segs[segOfSlot(W, path)];
         for (int q = 0;; ++q) {
             if (q >= kMaxPathQueries) {
                 atomicAdd(&stats[7], 1ull);
@@ -832,7 +868,7 @@ __global__ void __launch_bounds__(kTailBlock) kTail(SceneGPU S, Paths P, Wave W,
                                               1e30f, nodes, tris);
             ++rays;
             P.hit[slot] = make_float4(h.t, h.u, h.v, __int_as_float(h.prim));
-            if (!shadeSlot<true, COUNT>(S, P, A, slot, shNodes, shTris, shRays)) break;
+            if (!shadeSlot<true, COUNT>(S, P, A, slot, path, shNodes, shTris, shRays)) break;
         }
     }
     if (COUNT) {
@@ -858,7 +894,8 @@ __global__ void kFilm(Paths P, Wave W, unsigned long long* rejected) {
         float sq = A.sq[pix];
         uint32_t c = A.cnt[pix];
         for (int s = 0; s < A.nSamples; ++s) {
-            const float4 L = P.L[A.slotFirst + s * A.nPix + p];
+            const int path = A.slotFirst + s * A.nPix + p;
+            const float4 L = P.Lout ? P.Lout[path] : P.L[path];
             ++c;
             const bool ok = finitef(L.x) && finitef(L.y) && finitef(L.z) && L.x >= 0.0f && L.y >= 0.0f && L.z >= 0.0f;
             if (!ok) {

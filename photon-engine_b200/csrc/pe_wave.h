@@ -72,6 +72,11 @@ struct Paths {
     int32_t sdMode;      // bit 0: record training vertices, bit 1: sample with the SD-tree
     float4* sdRec;       // kSdRecords × 4 per slot: (point, pdf) | (ω, 0) | (throughput after, 0) | (radiance snapshot, state)
     uint32_t* sdCount;   // recorded vertices per slot
+    // path regeneration (null in a wave whose paths are its slots): a wave of more paths than
+    // slots refills each slot freed by an ended path with the wave's next path
+    int32_t* pathOf;     // wave path index held by each slot
+    int32_t* freeQ;      // slots freed by the shading kernel this bounce
+    float4* Lout;        // radiance of each ended path, by wave path index (read by the film kernel)
     uint32_t capacity;
     // [0] queue A count, [1] queue B count, [2] shadow count, [3] closest-hit work cursor,
     // [4] any-hit work cursor, [5] shade work cursor, [6..11] rays per shading key, [12] errors,
@@ -83,7 +88,9 @@ struct Paths {
 constexpr int kShadeKeys = 6;
 enum CounterSlots { CNT_QA = 0, CNT_QB = 1, CNT_SHADOW = 2, CNT_WORK_ISECT = 3, CNT_WORK_SHADOW = 4,
                     CNT_WORK_SHADE = 5, CNT_KEYS = 6, CNT_ERRORS = 12, CNT_WORK_TAIL = 13, CNT_GUIDE_Q = 14,
-                    CNT_TRAIN = 15, CNT_TOTAL = 16 };
+                    CNT_TRAIN = 15, CNT_FREE = 16, CNT_TOTAL = 17 };
+// Paths per wave with regeneration, as a multiple of the slots.
+constexpr int kStreamFactor = 4;
 // Vertices an SD-tree training path records (the reference records up to 32; its paths in these
 // workloads rarely pass 8 guidable vertices).
 constexpr int kSdRecords = 8;
@@ -121,7 +128,9 @@ struct Wave {
 };
 
 #ifdef __CUDACC__
-// Segment owning a wave slot / a wave pixel (binary search; one segment for a lone request).
+// Wave path index held by a slot.
+__device__ __forceinline__ int pathOfSlot(const Paths& P, int slot) { return P.pathOf ? P.pathOf[slot] : slot; }
+// Segment owning a wave path / a wave pixel (binary search; one segment for a lone request).
 __device__ __forceinline__ int segOfSlot(const Wave& W, int slot) {
     int lo = 0, hi = W.nSegs - 1;
     while (lo < hi) {

@@ -17,30 +17,36 @@ using namespace pe_dev;
 
 namespace pe_dev {
 
+int32_t allocLane(WaveLane& ln, size_t slots) {
+    freeList(ln.bufs);
+    int32_t st = 0;
+    Paths& P = ln.paths;
+    float4** cols[] = {&P.rayO, &P.rayD, &P.thr, &P.L, &P.lastN, &P.lastP, &P.pickP, &P.pickN, &P.hit, &P.med};
+    for (float4** c : cols)
+        if ((st = devAlloc(ln.bufs, *c, slots))) return st;
+    if ((st = devAlloc(ln.bufs, P.queueA, slots))) return st;
+    if ((st = devAlloc(ln.bufs, P.queueB, slots))) return st;
+    if ((st = devAlloc(ln.bufs, P.sortQ, slots * kShadeKeys))) return st;
+    // shadow records: one per slot (shadow quality 1)
+    if ((st = devAlloc(ln.bufs, P.shadowQ, slots))) return st;
+    float4** scols[] = {&P.shO, &P.shD, &P.shC, &P.shT};
+    for (float4** c : scols)
+        if ((st = devAlloc(ln.bufs, *c, slots))) return st;
+    if ((st = devAlloc(ln.bufs, P.counters, CNT_TOTAL))) return st;
+    // path regeneration: slot → path, freed slots, radiance of kStreamFactor × slots paths
+    if ((st = devAlloc(ln.bufs, ln.pathOf, slots))) return st;
+    if ((st = devAlloc(ln.bufs, ln.freeQ, slots))) return st;
+    if ((st = devAlloc(ln.bufs, ln.Lout, slots * kStreamFactor))) return st;
+    P.capacity = static_cast<uint32_t>(slots);
+    return PE_OK;
+}
+
 int32_t ensureCapacity(pe_device* d, size_t slots) {
     if (slots <= d->capacity) return PE_OK;
-    for (WaveLane& ln : d->lanes) freeList(ln.bufs);
     d->capacity = 0;
-    int32_t st = 0;
     for (WaveLane& ln : d->lanes) {
-        Paths& P = ln.paths;
-        float4** cols[] = {&P.rayO, &P.rayD, &P.thr, &P.L, &P.lastN, &P.lastP, &P.pickP, &P.pickN, &P.hit, &P.med};
-        for (float4** c : cols)
-            if ((st = devAlloc(ln.bufs, *c, slots))) return st;
-        if ((st = devAlloc(ln.bufs, P.queueA, slots))) return st;
-        if ((st = devAlloc(ln.bufs, P.queueB, slots))) return st;
-        if ((st = devAlloc(ln.bufs, P.sortQ, slots * kShadeKeys))) return st;
-        // shadow records: one per slot (shadow quality 1)
-        if ((st = devAlloc(ln.bufs, P.shadowQ, slots))) return st;
-        float4** scols[] = {&P.shO, &P.shD, &P.shC, &P.shT};
-        for (float4** c : scols)
-            if ((st = devAlloc(ln.bufs, *c, slots))) return st;
-        if ((st = devAlloc(ln.bufs, P.counters, CNT_TOTAL))) return st;
-        // path regeneration: slot → path, freed slots, radiance of kStreamFactor × slots paths
-        if ((st = devAlloc(ln.bufs, ln.pathOf, slots))) return st;
-        if ((st = devAlloc(ln.bufs, ln.freeQ, slots))) return st;
-        if ((st = devAlloc(ln.bufs, ln.Lout, slots * kStreamFactor))) return st;
-        P.capacity = static_cast<uint32_t>(slots);
+        const int32_t st = allocLane(ln, slots);
+        if (st) return st;
     }
     d->capacity = slots;
     return PE_OK;
@@ -269,6 +275,10 @@ int32_t runWave(pe_device* d, int lane, Paths& P, int nSegs, int nSlots, int nPi
     P.pathOf = regen ? ln.pathOf : nullptr;
     P.freeQ = regen ? ln.freeQ : nullptr;
     P.Lout = regen ? ln.Lout : nullptr;
+    P.segLeft = nullptr;
+    P.born = nullptr;
+    P.sweepQ = nullptr;
+    P.sweepAge = 0;
     if (nSlots > (regen ? slotCap * kStreamFactor : slotCap)) {
         setError("wave of " + std::to_string(nSlots) + " paths exceeds its path state");
         return PE_ERR_LIMIT;
@@ -300,9 +310,9 @@ int32_t runWave(pe_device* d, int lane, Paths& P, int nSegs, int nSlots, int nPi
                 PE_CUDA(cudaEventRecord(t0, cs));
             }
             if (d->counting)
-                kTail<true><<<grid, kTailBlock, 0, cs>>>(S, P, W, qIn, cIn, d->dStats);
+                kTail<true><<<grid, kTailBlock, 0, cs>>>(S, P, W, qIn, cIn, &P.counters[CNT_WORK_TAIL], d->dStats);
             else
-                kTail<false><<<grid, kTailBlock, 0, cs>>>(S, P, W, qIn, cIn, d->dStats);
+                kTail<false><<<grid, kTailBlock, 0, cs>>>(S, P, W, qIn, cIn, &P.counters[CNT_WORK_TAIL], d->dStats);
             if (tm.timing) {
                 PE_CUDA(cudaEventRecord(t1, cs));
                 tm.tail.push_back({tm.evUsed - 2, tm.evUsed - 1});
@@ -310,7 +320,7 @@ int32_t runWave(pe_device* d, int lane, Paths& P, int nSegs, int nSlots, int nPi
             ++stats.kernel_launches;
             stats.tail_paths += live;
             if (regen) {
-                kFlush<<<sm * 4, 256, 0, cs>>>(P, qIn, cIn);
+                kFlush<<<sm * 4, 256, 0, cs>>>(P, W, qIn, cIn);
                 ++stats.kernel_launches;
             }
             break;
@@ -381,6 +391,157 @@ int32_t runWave(pe_device* d, int lane, Paths& P, int nSegs, int nSlots, int nPi
     if ((P.sdMode & SD_RECORD) && (rc = sdRecord(d, cs, P, nSlots))) return rc;
     PE_CUDA(cudaEventRecord(ln.evDone, cs));
     ln.pending = true;
+    PE_CUDA(cudaGetLastError());
+    return PE_OK;
+}
+
+// ---- continuous waves (the request server) ----------------------------------------------------
+// A lane whose wave never drains while work arrives: every bounce the slots of ended paths hand
+// their radiance to Lout and return to a free stack, from which new requests' paths are injected.
+
+int32_t loopBegin(pe_device* d, LaneLoop& L, uint32_t* segLeft) {
+    WaveLane& ln = *L.ln;
+    Paths& P = ln.paths;
+    const cudaStream_t cs = ln.stream;
+    (void)cudaGetLastError();
+    P.guiding = 0;
+    P.sdMode = 0;
+    P.pathOf = ln.pathOf;
+    P.freeQ = ln.freeQ;
+    P.Lout = ln.Lout;
+    P.segLeft = segLeft;
+    P.born = L.born;
+    P.sweepQ = nullptr;
+    P.sweepAge = 0;
+    P.iter = 0;
+    for (int b = 0; b < LaneLoop::kSweepBufs; ++b) L.sweepN[b] = 0;
+    L.sweeping = 0;
+    L.qIn = P.queueA;
+    L.qOut = P.queueB;
+    L.cIn = &P.counters[0];
+    L.cOut = &P.counters[1];
+    L.live = 0;
+    L.freeTop = static_cast<int>(P.capacity);
+    L.nextPath = 0;
+    L.pathCap = static_cast<int>(static_cast<int64_t>(P.capacity) * kStreamFactor);
+    L.iter = 0;
+    PE_CUDA(cudaMemsetAsync(P.counters, 0, CNT_TOTAL * sizeof(uint32_t), cs));
+    kInitFree<<<d->prop.multiProcessorCount * 4, 256, 0, cs>>>(P, static_cast<int>(P.capacity));
+    PE_CUDA(cudaGetLastError());
+    return PE_OK;
+}
+
+int32_t loopInject(pe_device* d, LaneLoop& L, const Wave& W, int fresh) {
+    if (fresh <= 0) return PE_OK;
+    WaveLane& ln = *L.ln;
+    Paths& P = ln.paths;
+    P.iter = L.iter;
+    kInject<<<d->prop.multiProcessorCount * 4, 256, 0, ln.stream>>>(L.scene, P, W, L.freeTop, fresh, L.nextPath, L.qIn,
+                                                                    static_cast<int>(L.live), L.cIn);
+    PE_CUDA(cudaGetLastError());
+    L.freeTop -= fresh;
+    L.nextPath += fresh;
+    L.live += static_cast<uint32_t>(fresh);
+    return PE_OK;
+}
+
+int32_t loopBounce(pe_device* d, LaneLoop& L, const Wave& W, uint32_t* hSegLeft, const uint32_t* dSegLeft, int segFirst,
+                   int segCount) {
+    WaveLane& ln = *L.ln;
+    Paths& P = ln.paths;
+    const cudaStream_t cs = ln.stream;
+    const SceneGPU& S = L.scene;
+    // a free sweep buffer takes this bounce's old paths (none free: no sweep this bounce)
+    int sweep = -1;
+    if (L.sweepAge > 0)
+        for (int b = 0; b < LaneLoop::kSweepBufs && sweep < 0; ++b)
+            if (L.sweepN[b] == 0) sweep = b;
+    P.sweepAge = sweep >= 0 ? L.sweepAge : 0;
+    P.sweepQ = sweep >= 0 ? L.sweepBuf[sweep] : nullptr;
+    P.iter = L.iter;
+    kIntersect<false><<<d->blocksIntersect, 128, 0, cs>>>(S, P, L.qIn, L.cIn, d->dStats);
+    kShade<<<d->blocksShade, 128, 0, cs>>>(S, P, W, L.qOut, L.cOut);
+    kShadow<false><<<d->blocksShadow, 128, 0, cs>>>(S, P, &P.counters[CNT_SHADOW], d->dStats);
+    PE_CUDA(cudaMemcpyAsync(ln.hCounters, P.counters, CNT_TOTAL * sizeof(uint32_t), cudaMemcpyDeviceToHost, cs));
+    // segment counts as of the previous bounce's flushes (one bounce behind)
+    if (segCount > 0)
+        PE_CUDA(cudaMemcpyAsync(hSegLeft + segFirst, dSegLeft + segFirst, static_cast<size_t>(segCount) * sizeof(uint32_t),
+                                cudaMemcpyDeviceToHost, cs));
+    PE_CUDA(cudaStreamSynchronize(cs));
+    L.live = L.cOut == &P.counters[1] ? ln.hCounters[1] : ln.hCounters[0];
+    const int top = static_cast<int>(ln.hCounters[CNT_FREE]);
+    const int freed = top - L.freeTop;
+    if (freed > 0) {
+        kFlushFreed<<<d->prop.multiProcessorCount * 4, 256, 0, cs>>>(P, W, L.freeTop, freed);
+    }
+    L.freeTop = top;
+    const int swept = static_cast<int>(ln.hCounters[CNT_SWEEP]);
+    if (sweep >= 0 && swept > 0) {
+        // the swept paths run to their end on the side stream, then hand over their radiance
+        PE_CUDA(cudaMemcpyAsync(&L.sweepCnt[sweep], &P.counters[CNT_SWEEP], sizeof(uint32_t), cudaMemcpyDeviceToDevice, cs));
+        PE_CUDA(cudaMemsetAsync(&P.counters[CNT_SWEEP], 0, sizeof(uint32_t), cs));
+        PE_CUDA(cudaEventRecord(L.evReady[sweep], cs));
+        PE_CUDA(cudaStreamWaitEvent(L.side, L.evReady[sweep], 0));
+        PE_CUDA(cudaMemsetAsync(&L.sweepCursor[sweep], 0, sizeof(uint32_t), L.side));
+        const int grid = static_cast<int>(std::min<int64_t>(d->blocksTail, (swept + kTailBlock - 1) / kTailBlock));
+        kTail<false><<<grid, kTailBlock, 0, L.side>>>(S, P, W, L.sweepBuf[sweep], &L.sweepCnt[sweep],
+                                                       &L.sweepCursor[sweep], d->dStats);
+        kFlush<<<d->prop.multiProcessorCount * 4, 256, 0, L.side>>>(P, W, L.sweepBuf[sweep], &L.sweepCnt[sweep]);
+        PE_CUDA(cudaEventRecord(L.evDone[sweep], L.side));
+        L.sweepN[sweep] = swept;
+        L.sweeping += swept;
+    }
+    PE_CUDA(cudaMemsetAsync(L.cIn, 0, sizeof(uint32_t), cs));
+    PE_CUDA(cudaMemsetAsync(&P.counters[CNT_SHADOW], 0, (CNT_KEYS + kShadeKeys - CNT_SHADOW) * sizeof(uint32_t), cs));
+    std::swap(L.qIn, L.qOut);
+    std::swap(L.cIn, L.cOut);
+    if (++L.iter > kMaxWavefrontIterations * 64) {
+        setError("continuous wave exceeded its bounce bound");
+        return PE_ERR_DEVICE;
+    }
+    PE_CUDA(cudaGetLastError());
+    return PE_OK;
+}
+
+int32_t loopTail(pe_device* d, LaneLoop& L, const Wave& W) {
+    if (L.live == 0) return PE_OK;
+    WaveLane& ln = *L.ln;
+    Paths& P = ln.paths;
+    const cudaStream_t cs = ln.stream;
+    const int grid = static_cast<int>(std::min<int64_t>(d->blocksTail, (static_cast<int64_t>(L.live) + kTailBlock - 1) / kTailBlock));
+    kTail<false><<<grid, kTailBlock, 0, cs>>>(L.scene, P, W, L.qIn, L.cIn, &P.counters[CNT_WORK_TAIL], d->dStats);
+    kFlush<<<d->prop.multiProcessorCount * 4, 256, 0, cs>>>(P, W, L.qIn, L.cIn);
+    L.live = 0;
+    PE_CUDA(cudaGetLastError());
+    return PE_OK;
+}
+
+int32_t loopReturn(pe_device* d, LaneLoop& L, bool wait) {
+    if (L.sweeping == 0) return PE_OK;
+    WaveLane& ln = *L.ln;
+    for (int b = 0; b < LaneLoop::kSweepBufs; ++b) {
+        if (L.sweepN[b] == 0) continue;
+        const cudaError_t e = wait ? cudaEventSynchronize(L.evDone[b]) : cudaEventQuery(L.evDone[b]);
+        if (e == cudaErrorNotReady) continue;
+        if (e != cudaSuccess) {
+            setError(std::string("sweep: ") + cudaMsg(e));
+            return PE_ERR_CUDA;
+        }
+        kReturnSlots<<<d->prop.multiProcessorCount * 2, 256, 0, ln.stream>>>(ln.paths, L.sweepBuf[b], L.sweepN[b],
+                                                                             L.freeTop);
+        PE_CUDA(cudaGetLastError());
+        L.freeTop += L.sweepN[b];
+        L.sweeping -= L.sweepN[b];
+        L.sweepN[b] = 0;
+    }
+    return PE_OK;
+}
+
+int32_t loopFilm(pe_device* d, LaneLoop& L, const WaveSeg* dSeg, int nPix) {
+    WaveLane& ln = *L.ln;
+    const Wave one{dSeg, 1, nPix, nPix};
+    kFilm<<<std::max(1, std::min(d->prop.multiProcessorCount * 4, (nPix + 255) / 256)), 256, 0, ln.stream>>>(
+        ln.paths, one, &d->dStats[4]);
     PE_CUDA(cudaGetLastError());
     return PE_OK;
 }

@@ -245,6 +245,45 @@ int32_t uploadScene(pe_device* d, const pe_scene* s, SceneGPU& out, std::vector<
 // inference, and after the film kernel the wave's training samples and one Adam step.
 int32_t guideQueries(pe_device* d, cudaStream_t s, Paths& P, const Wave& W, const int32_t* queue, const uint32_t* count);
 int32_t guideLearn(pe_device* d, cudaStream_t s, Paths& P, int nSlots);
+// A continuous wave on one lane (the request server): paths are injected into the slots that
+// ended paths free, bounce after bounce, until the server drains the lane with the tail kernel.
+struct LaneLoop {
+    WaveLane* ln = nullptr;  // the lane's path state, stream and readback buffers
+    SceneGPU scene{};   // the wave's scene (each lane may trace its own)
+    int32_t* qIn = nullptr;
+    int32_t* qOut = nullptr;
+    uint32_t* cIn = nullptr;
+    uint32_t* cOut = nullptr;
+    uint32_t live = 0;  // paths in the next closest-hit queue
+    int freeTop = 0;    // free slots on the stack
+    int nextPath = 0;   // wave path index of the next injected path
+    int pathCap = 0;    // paths the wave can hold (Lout)
+    int iter = 0;
+    // sweeps: paths alive for sweepAge bounces finish in tail-kernel launches on `side`
+    static constexpr int kSweepBufs = 8;
+    int sweepAge = 0;                    // 0: off
+    cudaStream_t side = nullptr;
+    int32_t* born = nullptr;             // device, one per slot
+    int32_t* sweepBuf[kSweepBufs] = {};  // device, one slot list per sweep in flight
+    uint32_t* sweepCnt = nullptr;        // device [kSweepBufs]
+    uint32_t* sweepCursor = nullptr;     // device [kSweepBufs]
+    cudaEvent_t evReady[kSweepBufs] = {}, evDone[kSweepBufs] = {};
+    int sweepN[kSweepBufs] = {};         // slots out in each sweep (0: buffer free)
+    int sweeping = 0;                    // slots out in all sweeps
+};
+// Path state of `slots` slots (with regeneration buffers) for one lane.
+int32_t allocLane(WaveLane& ln, size_t slots);
+int32_t loopBegin(pe_device* d, LaneLoop& L, uint32_t* segLeft);
+int32_t loopInject(pe_device* d, LaneLoop& L, const Wave& W, int fresh);
+// One bounce; syncs the lane, then reads back the live count, the freed slots and the remaining
+// path counts of segments [segFirst, segFirst + segCount).
+int32_t loopBounce(pe_device* d, LaneLoop& L, const Wave& W, uint32_t* hSegLeft, const uint32_t* dSegLeft, int segFirst,
+                   int segCount);
+int32_t loopTail(pe_device* d, LaneLoop& L, const Wave& W);
+// Returns the slots of finished sweeps to the free stack; with `wait`, waits for every sweep.
+int32_t loopReturn(pe_device* d, LaneLoop& L, bool wait);
+int32_t loopFilm(pe_device* d, LaneLoop& L, const WaveSeg* dSeg, int nPix);
+
 // SD-tree guiding (pe_sdtree.cu): splats of a wave's recorded vertices; per-slot record buffers.
 int32_t sdRecord(pe_device* d, cudaStream_t s, Paths& P, int nSlots);
 int32_t sdBuffers(pe_device* d);

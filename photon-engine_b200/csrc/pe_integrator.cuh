@@ -75,6 +75,16 @@ __device__ __forceinline__ void generatePath(const SceneGPU& S, const Paths& P, 
     if (P.pathOf) P.pathOf[slot] = path;
 }
 
+// Hands an ended path's radiance to Lout (and counts it off its segment when those are tracked).
+__device__ __forceinline__ void flushPath(const Paths& P, const Wave& W, int slot) {
+    const int path = P.pathOf[slot];
+    P.Lout[path] = P.L[slot];
+    if (P.segLeft) {
+        __threadfence(); // the radiance is visible before the segment's count says it is done
+        atomicSub(&P.segLeft[segOfSlot(W, path)], 1u);
+    }
+}
+
 // The wave's first `count` paths into slots [0, count), all queued.
 __global__ void kGenerate(SceneGPU S, Paths P, Wave W, int count) {
     for (int slot = blockIdx.x * blockDim.x + threadIdx.x; slot < count; slot += gridDim.x * blockDim.x) {
@@ -90,7 +100,7 @@ __global__ void kRecycle(SceneGPU S, Paths P, Wave W, int freed, int fresh, int 
                          uint32_t* queueCount) {
     for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < freed; k += gridDim.x * blockDim.x) {
         const int slot = P.freeQ[k];
-        P.Lout[P.pathOf[slot]] = P.L[slot];
+        flushPath(P, W, slot);
         if (k < fresh) {
             generatePath(S, P, W, slot, nextPath + k);
             queue[queued + k] = slot;
@@ -100,12 +110,44 @@ __global__ void kRecycle(SceneGPU S, Paths P, Wave W, int freed, int fresh, int 
 }
 
 // The radiance of the paths the tail kernel finished, to Lout.
-__global__ void kFlush(Paths P, const int32_t* queue, const uint32_t* count) {
+__global__ void kFlush(Paths P, Wave W, const int32_t* queue, const uint32_t* count) {
     const int n = static_cast<int>(*count);
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const int slot = queue[i];
-        P.Lout[P.pathOf[slot]] = P.L[slot];
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) flushPath(P, W, queue[i]);
+}
+
+// Continuous waves (the request server): freed slots form a stack (freeQ, its size in
+// counters[CNT_FREE]).  kFlushFreed hands over the radiance of the `freed` slots pushed this
+// bounce, above `base`; kInject then pops `fresh` slots for the wave's paths [nextPath, +fresh),
+// appended to the next closest-hit queue after its `queued` entries.
+__global__ void kFlushFreed(Paths P, Wave W, int base, int freed) {
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < freed; k += gridDim.x * blockDim.x)
+        flushPath(P, W, P.freeQ[base + k]);
+}
+
+__global__ void kInject(SceneGPU S, Paths P, Wave W, int top, int fresh, int nextPath, int32_t* queue, int queued,
+                        uint32_t* queueCount) {
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < fresh; k += gridDim.x * blockDim.x) {
+        const int slot = P.freeQ[top - fresh + k];
+        generatePath(S, P, W, slot, nextPath + k);
+        if (P.born) P.born[slot] = P.iter;
+        queue[queued + k] = slot;
     }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        *queueCount = static_cast<uint32_t>(queued + fresh);
+        P.counters[CNT_FREE] = static_cast<uint32_t>(top - fresh);
+    }
+}
+
+// Slots of a finished sweep back onto the free stack, above `top`.
+__global__ void kReturnSlots(Paths P, const int32_t* slots, int n, int top) {
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) P.freeQ[top + k] = slots[k];
+    if (blockIdx.x == 0 && threadIdx.x == 0) P.counters[CNT_FREE] = static_cast<uint32_t>(top + n);
+}
+
+// Every slot free: the stack holds slots [0, n).
+__global__ void kInitFree(Paths P, int n) {
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) P.freeQ[k] = k;
+    if (blockIdx.x == 0 && threadIdx.x == 0) P.counters[CNT_FREE] = static_cast<uint32_t>(n);
 }
 
 // ---- closest hit over a queue -----------------------------------------------------------------
@@ -818,7 +860,7 @@ __global__ void __launch_bounds__(128, 4) kShade(SceneGPU S, Paths P, Wave W, in
         const int base = warpFetch(&P.counters[CNT_WORK_SHADE]);
         if (base >= n) break;
         const int i = base + lane;
-        bool cont = false;
+        bool cont = false, sweepable = false;
         int slot = -1;
         if (i < n) {
             int k = 0;
@@ -829,9 +871,15 @@ __global__ void __launch_bounds__(128, 4) kShade(SceneGPU S, Paths P, Wave W, in
             }
             slot = P.sortQ[static_cast<size_t>(k) * P.capacity + j];
             const int path = pathOfSlot(P, slot);
-            cont = shadeSlot<false, false>(S, P, W.segs[segOfSlot(W, path)], slot, path, unused0, unused1, unused2);
+            const WaveSeg& A = W.segs[segOfSlot(W, path)];
+            cont = shadeSlot<false, false>(S, P, A, slot, path, unused0, unused1, unused2);
+            sweepable = (A.flags & SEG_SWEEP) != 0;
         }
-        queuePush(nextQueue, nextCount, cont, slot);
+        // a continuous wave sweeps its interactive paths that have lived sweepAge bounces into a
+        // tail launch, so that their requests do not wait on one bounce per wavefront step
+        const bool old = P.sweepAge > 0 && cont && sweepable && P.iter - P.born[slot] >= P.sweepAge;
+        queuePush(nextQueue, nextCount, cont && !old, slot);
+        if (P.sweepAge > 0) queuePush(P.sweepQ, &P.counters[CNT_SWEEP], old, slot);
         // a regenerating wave refills the slots of ended paths
         if (P.pathOf) queuePush(P.freeQ, &P.counters[CNT_FREE], !cont && slot >= 0, slot);
     }
@@ -848,11 +896,11 @@ constexpr int kTailBlock = 32;
 
 template <bool COUNT>
 __global__ void __launch_bounds__(kTailBlock) kTail(SceneGPU S, Paths P, Wave W, const int32_t* queue, const uint32_t* count,
-                                             unsigned long long* stats) {
+                                             uint32_t* cursor, unsigned long long* stats) {
     const int n = static_cast<int>(*count);
     uint32_t nodes = 0, tris = 0, shNodes = 0, shTris = 0, rays = 0, shRays = 0;
     for (;;) {
-        const int i = static_cast<int>(atomicAdd(&P.counters[CNT_WORK_TAIL], 1u));
+        const int i = static_cast<int>(atomicAdd(cursor, 1u));
         if (i >= n) break;
         const int slot = queue[i];
         const int path = pathOfSlot(P, slot);

@@ -1,19 +1,33 @@
 // pe_server.cu — the request server behind the pe_server_* C ABI: resident scenes, device films
-// admitted against an HBM budget, and a worker thread that packs the pending sample ranges of
-// many requests into shared waves (continuous batching).
+// admitted against an HBM budget, and continuous waves that take in new requests' paths as the
+// paths in flight end (continuous batching at path granularity).
 //
-// Waves alternate the device's two lanes: wave k+1 is planned and its bounces traced while wave
-// k's tail still runs; a request is done once the lane of its last wave has finished.
+// Four lanes, each driven by its own host thread and running one scene's continuous wave at a
+// time: the device's two lanes take the bulk requests, and two express lanes of their own path
+// state on high-priority streams take the interactive ones (at most 8M paths, or a priority above
+// 0; two, so that interactive requests of two scenes need not wait for each other); while an
+// express lane runs, the bulk lanes pause between bounces, so the GPU goes to the interactive
+// requests (stream priority alone does not preempt the bulk lanes' persistent kernels).  After every bounce the slots of ended paths hand their radiance to
+// the wave's per-path buffer and return to a free stack; the lane then injects the next paths of
+// the admitted requests of its scene, ordered by (priority desc, remaining paths asc, id asc).
+// A request's paths are planned as segments — whole-frame sample rows [s, s+k), or a pixel range
+// of one row — in increasing sample order, and each segment is added to the request's film once
+// all its paths have ended, in segment order, so every pixel adds its samples in the order a
+// lone render does and the film is bit-identical to pe_device_render's.
 //
-// Scheduling.  Admitted requests are ordered by (priority desc, remaining paths asc, id asc).
-// The first request picks the wave's scene; the wave is then filled, in that order, with one
-// chunk per admitted request of the same scene until its 2M path slots are used.  A chunk is
-// either whole-frame sample rows [s, s+k) or, when a frame does not fit, a pixel range of one
-// sample row.  A request's rows run in increasing sample order, so every pixel adds its samples
-// in the order a lone render does and the film is bit-identical to pe_device_render's.
+// A lane drains its wave (stops injecting, finishes the last paths with the tail kernel) when
+// its scene has no more work, when its path buffer is used up, or (bulk lanes) when a request of
+// a scene no lane is tracing outranks its own best pending request; the lane then starts a wave
+// of the best-ranked waiting scene.  A request is bound to one lane while it has segments in
+// flight.  Interactive paths that stay in a wave for 4 (express lanes) or 8 bounces finish in tail-kernel sweeps on a
+// side stream, so an interactive request does not wait one wavefront step per bounce of its
+// longest paths.
+
 #include "pe_device_impl.h"
 
 #include <chrono>
+#include <cstdio>
+#include <cstdlib>
 #include <condition_variable>
 #include <cstring>
 #include <deque>
@@ -46,7 +60,11 @@ struct Request {
     int32_t pixelCursor = 0;  // > 0 while a row is split over several waves
     int32_t samplesDone = 0;
     uint64_t paths = 0;
+    const float* filterCdf = nullptr; // the server's device table of its pixel filter
+    int32_t lane = -1;        // the lane holding its segments in flight (-1: none)
+    int32_t openSegs = 0;     // segments planned and not yet added to the film
     double submitMs = 0.0, startMs = 0.0, doneMs = 0.0;
+    double firstPathMs = -1.0, lastPathMs = -1.0, filmMs = -1.0; // trace: injections, last film kernel
 
     int64_t pixels() const { return static_cast<int64_t>(st.width) * st.height; }
     int64_t remaining() const { return (static_cast<int64_t>(spp) - sampleCursor) * pixels() - pixelCursor; }
@@ -58,12 +76,20 @@ struct ResidentScene {
     size_t bytes = 0;
 };
 
-// A wave's chunk of one request, kept for the progress update after the wave.
-struct Chunk {
-    int64_t id;
-    int32_t samples;    // whole rows handed out (0 for a partial row)
-    bool closesRow;     // a split row's last pixel range
+// One planned segment of a continuous wave.
+struct SegInfo {
+    int64_t id;         // request
+    int32_t samples;    // whole rows it completes (a split row's last pixel range completes 1)
+    int32_t nPix;
+    bool filmed;
 };
+
+constexpr int kServerSegs = 16384;      // segments per continuous wave
+constexpr int kMinChunk = 4096;         // smallest segment unless it finishes a request
+constexpr int kSweepAge = 8;            // bounces after which an interactive path leaves a bulk wave for a sweep
+constexpr int kExpressSweepAge = 4;     // the same on the express lanes
+constexpr size_t kExpressSlots = (size_t(1) << 22) + (size_t(1) << 20); // a 512² × 16-spp preview in one go
+constexpr int64_t kUrgentPaths = 8 << 20; // requests of at most this many paths are interactive (512² × 16 spp: 4.2M)
 
 size_t filmBytesOf(const pe_settings& st) {
     return static_cast<size_t>(st.width) * static_cast<size_t>(st.height) * (3 * sizeof(float) + sizeof(uint32_t) + sizeof(float));
@@ -88,26 +114,63 @@ struct pe_server {
     SceneGPU savedScene{};
     bool savedHasScene = false;
     cudaStream_t copyStream = nullptr;
+    cudaStream_t admitStream = nullptr; // film allocation and clearing
     cudaEvent_t evAdmit = nullptr;   // after the film allocations of the last admission
+    FILE* trace = nullptr;           // PE_SERVER_TRACE: one line per finished request and per wave
+    // pixel-filter tables, one per (type, width) in use; kept until the server is destroyed, as
+    // paths of a continuous wave may read them at any later bounce
+    std::map<std::pair<int, float>, float*> filters;
     pe_server_stats stats{};
-    // the wave in flight on each lane, booked once the lane's done-event fires
-    struct InFlight {
-        bool valid = false;
-        std::vector<Chunk> chunks;
-        int32_t rc = PE_OK;
-        std::string message;
-        cudaEvent_t evStart = nullptr;
-    } inflight[2];
-    int lane = 0;
+    // one continuous wave per lane, each driven by its own thread
+    struct LaneRun {
+        std::thread th;
+        WaveSeg* hSegs = nullptr;     // pinned segment table
+        WaveSeg* dSegs = nullptr;
+        uint32_t* hLeft = nullptr;    // pinned: paths left per segment (read back)
+        uint32_t* hInit = nullptr;    // pinned: initial counts (uploaded)
+        uint32_t* dLeft = nullptr;
+        std::vector<SegInfo> segs;
+        int scene = -1;
+        bool running = false;
+        bool draining = false;        // taking in no paths: the wave ends once its live paths fit the tail kernel
+        bool yielding = false;        // draining so that another scene gets this lane
+        int firstOpen = 0;            // first segment not yet filmed
+        int uploaded = 0;             // segments on the device
+        LaneLoop loop;
+        WaveLane own;                 // the express lane's own path state (bulk lanes use the device's)
+        cudaStream_t stream = nullptr;
+        std::vector<int64_t> doneAfterSync; // requests whose last film kernel is queued (no event free)
+        std::vector<std::pair<int64_t, cudaEvent_t>> doneEvents; // ... with an event after it
+        std::vector<cudaEvent_t> eventPool;
+        cudaEvent_t evStart = nullptr, evEnd = nullptr;
+    } lanes[4];
 
     double now() const { return std::chrono::duration<double, std::milli>(Clock::now() - t0).count(); }
 };
 
 namespace {
 
+// The server's table of a pixel filter, uploaded at its first use (lock held).
+const float* serverFilter(pe_server* S, int type, float width) {
+    const auto key = std::make_pair(type, width);
+    auto it = S->filters.find(key);
+    if (it != S->filters.end()) return it->second;
+    float cdf[kFilterBins + 1];
+    fillFilterCdf(type, width, cdf);
+    float* dev = nullptr;
+    if (cudaMalloc(&dev, sizeof(cdf)) != cudaSuccess) return nullptr;
+    if (cudaMemcpy(dev, cdf, sizeof(cdf), cudaMemcpyHostToDevice) != cudaSuccess) {
+        cudaFree(dev);
+        return nullptr;
+    }
+    S->filters[key] = dev;
+    return dev;
+}
+
 // Gives films to queued requests, in priority order, while the budget has room.  Called with
 // the lock held, on the worker thread.
-void admit(pe_server* S) {
+bool admit(pe_server* S) {
+    bool any = false;
     std::stable_sort(S->queued.begin(), S->queued.end(), [&](int64_t a, int64_t b) {
         const Request& ra = S->requests[a];
         const Request& rb = S->requests[b];
@@ -122,11 +185,23 @@ void admit(pe_server* S) {
         }
         const size_t n = static_cast<size_t>(r.pixels());
         void* p = nullptr;
-        cudaError_t e = cudaMallocAsync(&p, r.filmBytes, S->d->stream);
-        if (e == cudaSuccess) e = cudaMemsetAsync(p, 0, r.filmBytes, S->d->stream);
+        cudaError_t e = cudaMallocAsync(&p, r.filmBytes, S->admitStream);
+        if (e == cudaSuccess) e = cudaMemsetAsync(p, 0, r.filmBytes, S->admitStream);
         if (e != cudaSuccess) {
             r.state = PE_REQ_FAILED;
             r.error = e == cudaErrorMemoryAllocation ? PE_ERR_OOM : PE_ERR_CUDA;
+            r.doneMs = S->now();
+            ++S->stats.failed;
+            it = S->queued.erase(it);
+            S->cvDone.notify_all();
+            continue;
+        }
+        r.filterCdf = serverFilter(S, r.st.filter_type, r.st.filter_width);
+        if (!r.filterCdf) {
+            cudaFreeAsync(p, S->admitStream);
+            r.state = PE_REQ_FAILED;
+            r.error = PE_ERR_CUDA;
+            r.message = "pixel filter table upload failed";
             r.doneMs = S->now();
             ++S->stats.failed;
             it = S->queued.erase(it);
@@ -142,185 +217,429 @@ void admit(pe_server* S) {
         S->filmPeak = std::max(S->filmPeak, S->filmBytes);
         S->active.push_back(r.id);
         it = S->queued.erase(it);
+        any = true;
     }
+    return any;
 }
 
-// Packs the next wave into the lane's segment table; returns its segment count (0 = nothing to do).
-int planWave(pe_server* S, int lane, int& sceneOut, int& nSlots, int& nPix, std::vector<Chunk>& chunks) {
-    pe_device* d = S->d;
-    std::vector<int64_t> order = S->active;
-    std::stable_sort(order.begin(), order.end(), [&](int64_t a, int64_t b) {
-        const Request& ra = S->requests[a];
-        const Request& rb = S->requests[b];
-        if (ra.priority != rb.priority) return ra.priority > rb.priority;
-        if (ra.remaining() != rb.remaining()) return ra.remaining() < rb.remaining();
-        return a < b;
-    });
-    chunks.clear();
-    nSlots = 0;
-    nPix = 0;
-    int nSegs = 0;
-    int scene = -1;
-    const int64_t cap = static_cast<int64_t>(d->capacity);
-    const uint64_t clock = ++d->filterClock;
+bool ranksBefore(const Request& a, const Request& b) {
+    if (a.priority != b.priority) return a.priority > b.priority;
+    if (a.remaining() != b.remaining()) return a.remaining() < b.remaining();
+    return a.id < b.id;
+}
+
+bool hasWork(const Request& r) { return r.state == PE_REQ_ACTIVE && r.sampleCursor < r.spp; }
+
+bool urgent(const Request& r) { return r.priority > 0 || static_cast<int64_t>(r.spp) * r.pixels() <= kUrgentPaths; }
+
+constexpr int kLanes = 4;
+// lanes 0 and 1 trace bulk requests on the device's lanes, 2 and 3 are the express lanes
+bool express(int li) { return li >= 2; }
+
+// Whether an express lane is running (lock held): the bulk lanes then take in nothing.
+bool expressBusy(pe_server* S) {
+    for (int li = 2; li < kLanes; ++li)
+        if (S->lanes[li].running) return true;
+    return false;
+}
+
+// Whether lane `li` may take request `r` (lock held): the express lane takes the interactive
+// requests; a bulk lane takes the others, and an interactive one of its own scene while the
+// express lane is busy with another scene.
+bool eligible(pe_server* S, int li, const Request& r) {
+    if (r.lane >= 0 && r.lane != li) return false;
+    if (express(li)) return urgent(r);
+    if (!urgent(r)) return true;
+    // an interactive request of this bulk lane's scene while both express lanes trace others
+    for (int x = 2; x < kLanes; ++x)
+        if (!S->lanes[x].running || S->lanes[x].scene == r.scene) return false;
+    return S->lanes[li].running && S->lanes[li].scene == r.scene;
+}
+
+// The best-ranked admitted request with rows left that lane `li` may take (lock held).
+const Request* bestFor(pe_server* S, int li, int scene) {
+    const Request* best = nullptr;
+    for (int64_t id : S->active) {
+        const Request& r = S->requests[id];
+        if (!hasWork(r) || !eligible(S, li, r) || (scene >= 0 && r.scene != scene)) continue;
+        if (!best || ranksBefore(r, *best)) best = &r;
+    }
+    return best;
+}
+
+// Whether bulk lane `li` should stop taking paths so that a waiting scene gets a lane (lock
+// held): a bulk request of a scene that no running bulk lane traces outranks this lane's best
+// pending one, and the other bulk lane is not already making room.
+bool yieldLane(pe_server* S, int li) {
+    if (express(li)) return false;
+    const auto& me = S->lanes[li];
+    const auto& other = S->lanes[li ^ 1];
+    if (other.running && other.draining) return false;
+    if (!other.running) return false; // the idle bulk lane will take it
+    const Request* mine = bestFor(S, li, me.scene);
+    const Request* waiting = nullptr;
+    for (int64_t id : S->active) {
+        const Request& r = S->requests[id];
+        if (!hasWork(r) || r.lane >= 0 || urgent(r)) continue;
+        if (r.scene == me.scene || r.scene == other.scene) continue;
+        if (!waiting || ranksBefore(r, *waiting)) waiting = &r;
+    }
+    return waiting && (!mine || ranksBefore(*waiting, *mine));
+}
+
+// Plans up to `budget` paths of lane `li`'s scene as new segments (lock held); returns the paths.
+int planPaths(pe_server* S, int li, int budget) {
+    auto& R = S->lanes[li];
+    std::vector<int64_t> order;
+    for (int64_t id : S->active) {
+        const Request& r = S->requests[id];
+        if (hasWork(r) && r.scene == R.scene && eligible(S, li, r)) order.push_back(id);
+    }
+    std::sort(order.begin(), order.end(), [&](int64_t a, int64_t b) { return ranksBefore(S->requests[a], S->requests[b]); });
+    int planned = 0;
     for (int64_t id : order) {
         Request& r = S->requests[id];
-        if (r.sampleCursor >= r.spp) continue; // all rows handed out; waiting for its last wave
-        if (scene < 0) scene = r.scene;
-        if (r.scene != scene) continue;
-        const int64_t room = cap - nSlots;
-        if (room <= 0 || nSegs >= kMaxSegs) break;
-        if (nSegs > 0 && room < 4096) break; // not worth a segment
-        const float* filter = filterTable(d, r.st.filter_type, r.st.filter_width, clock, d->lanes[lane].stream);
-        if (!filter) break; // every filter slot is taken by this wave
-        WaveSeg seg = makeSeg(&r.cam, &r.st);
-        seg.filterCdf = filter;
-        seg.tileX = 0;
-        seg.tileY = 0;
-        seg.tileW = r.st.width;
-        seg.sum = r.sum;
-        seg.cnt = r.cnt;
-        seg.sq = r.sq;
-        seg.slotFirst = nSlots;
-        seg.pixFirst = nPix;
-        const int64_t npix = r.pixels();
-        Chunk c{id, 0, false};
-        if (r.pixelCursor == 0 && npix <= room) {
-            const int64_t rows = std::min<int64_t>(r.spp - r.sampleCursor, room / npix);
-            seg.pixelFirst = 0;
-            seg.nPix = static_cast<int>(npix);
-            seg.sampleFirst = r.sampleCursor;
-            seg.nSamples = static_cast<int>(rows);
-            r.sampleCursor += static_cast<int32_t>(rows);
-            c.samples = static_cast<int32_t>(rows);
-        } else {
-            const int64_t take = std::min<int64_t>(npix - r.pixelCursor, room);
-            seg.pixelFirst = r.pixelCursor;
-            seg.nPix = static_cast<int>(take);
-            seg.sampleFirst = r.sampleCursor;
-            seg.nSamples = 1;
-            r.pixelCursor += static_cast<int32_t>(take);
-            if (r.pixelCursor == npix) {
-                r.pixelCursor = 0;
-                r.sampleCursor += 1;
-                c.closesRow = true;
+        while (r.sampleCursor < r.spp) {
+            const int room = budget - planned;
+            const int64_t npix = r.pixels();
+            const int64_t left = r.remaining();
+            if (room < std::min<int64_t>(kMinChunk, left)) return planned;
+            if (static_cast<int>(R.segs.size()) >= kServerSegs) return planned;
+            WaveSeg seg = makeSeg(&r.cam, &r.st);
+            seg.filterCdf = r.filterCdf;
+            seg.tileX = 0;
+            seg.tileY = 0;
+            seg.tileW = r.st.width;
+            seg.sum = r.sum;
+            seg.cnt = r.cnt;
+            seg.sq = r.sq;
+            seg.slotFirst = R.loop.nextPath + planned;
+            seg.pixFirst = 0;
+            seg.flags = urgent(r) ? SEG_SWEEP : 0;
+            SegInfo info{id, 0, 0, false};
+            if (r.pixelCursor == 0 && npix <= room) {
+                const int64_t rows = std::min<int64_t>(r.spp - r.sampleCursor, room / npix);
+                seg.pixelFirst = 0;
+                seg.nPix = static_cast<int>(npix);
+                seg.sampleFirst = r.sampleCursor;
+                seg.nSamples = static_cast<int>(rows);
+                r.sampleCursor += static_cast<int32_t>(rows);
+                info.samples = static_cast<int32_t>(rows);
+            } else {
+                const int64_t take = std::min<int64_t>(npix - r.pixelCursor, room);
+                seg.pixelFirst = r.pixelCursor;
+                seg.nPix = static_cast<int>(take);
+                seg.sampleFirst = r.sampleCursor;
+                seg.nSamples = 1;
+                r.pixelCursor += static_cast<int32_t>(take);
+                if (r.pixelCursor == npix) {
+                    r.pixelCursor = 0;
+                    r.sampleCursor += 1;
+                    info.samples = 1;
+                }
             }
+            info.nPix = seg.nPix;
+            const int paths = seg.nPix * seg.nSamples;
+            const int k = static_cast<int>(R.segs.size());
+            R.hSegs[k] = seg;
+            R.hInit[k] = static_cast<uint32_t>(paths);
+            R.segs.push_back(info);
+            r.lane = li;
+            ++r.openSegs;
+            if (r.firstPathMs < 0.0) r.firstPathMs = S->now();
+            r.lastPathMs = S->now();
+            r.paths += static_cast<uint64_t>(paths);
+            planned += paths;
+            ++S->stats.segments;
         }
-        d->lanes[lane].hSegs[nSegs++] = seg;
-        nSlots += seg.nPix * seg.nSamples;
-        nPix += seg.nPix;
-        r.paths += static_cast<uint64_t>(seg.nPix) * static_cast<uint64_t>(seg.nSamples);
-        chunks.push_back(c);
     }
-    sceneOut = scene;
-    return nSegs;
+    return planned;
 }
 
-// Books a lane's finished wave (lock held): progress of its requests, completions, device time.
-// Returns false while the wave is still running.
-bool settleLane(pe_server* S, int l) {
-    auto& f = S->inflight[l];
-    if (!f.valid) return true;
-    WaveLane& ln = S->d->lanes[l];
-    if (f.rc == PE_OK) {
-        const cudaError_t e = cudaEventQuery(ln.evDone);
-        if (e == cudaErrorNotReady) return false;
-        if (e != cudaSuccess) {
-            f.rc = PE_ERR_CUDA;
-            f.message = std::string("wave: ") + cudaMsg(e);
-        } else {
-            float ms = 0.0f;
-            if (cudaEventElapsedTime(&ms, f.evStart, ln.evDone) == cudaSuccess) S->stats.busy_ms += ms;
-        }
-    }
-    const double t = S->now();
-    for (const Chunk& c : f.chunks) {
-        Request& r = S->requests[c.id];
-        if (f.rc != PE_OK) {
-            if (r.state == PE_REQ_ACTIVE) {
-                r.state = PE_REQ_FAILED;
-                r.error = f.rc;
-                r.message = f.message;
-                r.doneMs = t;
-                ++S->stats.failed;
-            }
+// Adds every completed segment to its request's film, in order (lock held, after a lane sync:
+// hLeft holds the counts read back).  `all`: the wave has ended, every segment is complete.
+int32_t filmSegments(pe_server* S, int li, bool all) {
+    auto& R = S->lanes[li];
+    const cudaStream_t cs = R.stream;
+    bool waited = false;
+    std::map<int64_t, bool> blocked; // a request with an earlier segment not yet complete
+    for (int k = R.firstOpen; k < static_cast<int>(R.segs.size()); ++k) {
+        SegInfo& g = R.segs[k];
+        if (g.filmed) continue;
+        if (blocked.count(g.id)) continue;
+        if (!all && R.hLeft[k] != 0u) {
+            blocked[g.id] = true;
             continue;
         }
-        r.samplesDone += c.samples + (c.closesRow ? 1 : 0);
-        if (r.samplesDone >= r.spp && r.state == PE_REQ_ACTIVE) {
-            r.state = PE_REQ_DONE;
-            r.doneMs = t;
-            ++S->stats.completed;
+        if (!waited) {
+            // films are allocated and cleared on the admission stream: film kernels come after
+            if (cudaStreamWaitEvent(cs, S->evAdmit, 0) != cudaSuccess) return PE_ERR_CUDA;
+            waited = true;
         }
+        int32_t rc = loopFilm(S->d, R.loop, R.dSegs + k, g.nPix);
+        if (rc) return rc;
+        g.filmed = true;
+        Request& r = S->requests[g.id];
+        r.samplesDone += g.samples;
+        --r.openSegs;
+        if (r.samplesDone >= r.spp) {
+            r.filmMs = S->now();
+            // done once the film kernel has run: an event after it, polled by the lane
+            if (!R.eventPool.empty() && cudaEventRecord(R.eventPool.back(), cs) == cudaSuccess) {
+                R.doneEvents.emplace_back(g.id, R.eventPool.back());
+                R.eventPool.pop_back();
+            } else {
+                R.doneAfterSync.push_back(g.id);
+            }
+        }
+    }
+    while (R.firstOpen < static_cast<int>(R.segs.size()) && R.segs[R.firstOpen].filmed) ++R.firstOpen;
+    return PE_OK;
+}
+
+// Requests whose film kernels have run (lock held, after a lane sync).
+void settleDone(pe_server* S, int li) {
+    auto& R = S->lanes[li];
+    const double t = S->now();
+    for (size_t k = 0; k < R.doneEvents.size();) {
+        if (cudaEventQuery(R.doneEvents[k].second) != cudaSuccess) {
+            ++k;
+            continue;
+        }
+        R.doneAfterSync.push_back(R.doneEvents[k].first);
+        R.eventPool.push_back(R.doneEvents[k].second);
+        R.doneEvents.erase(R.doneEvents.begin() + static_cast<long>(k));
+    }
+    for (int64_t id : R.doneAfterSync) {
+        Request& r = S->requests[id];
+        if (r.state != PE_REQ_ACTIVE) continue;
+        r.state = PE_REQ_DONE;
+        r.doneMs = t;
+        ++S->stats.completed;
+        if (S->trace)
+            std::fprintf(S->trace, "request %lld scene %d paths %llu lane %d submit %.2f admit %.2f first %.2f last %.2f film %.2f done %.2f\n",
+                         static_cast<long long>(r.id), r.scene, static_cast<unsigned long long>(r.paths), li, r.submitMs,
+                         r.startMs, r.firstPathMs, r.lastPathMs, r.filmMs, r.doneMs);
+        r.lane = -1;
+    }
+    if (!R.doneAfterSync.empty()) {
+        R.doneAfterSync.clear();
+        S->active.erase(std::remove_if(S->active.begin(), S->active.end(),
+                                       [&](int64_t id) { return S->requests[id].state != PE_REQ_ACTIVE; }),
+                        S->active.end());
+        S->cvDone.notify_all();
+        S->cvWork.notify_all();
+    }
+}
+
+// A lane's wave failed: its requests fail with it (lock held).
+void failLane(pe_server* S, int li, int32_t rc, const std::string& msg) {
+    auto& R = S->lanes[li];
+    const double t = S->now();
+    for (int64_t id : S->active) {
+        Request& r = S->requests[id];
+        if (r.lane != li || r.state != PE_REQ_ACTIVE) continue;
+        r.state = PE_REQ_FAILED;
+        r.error = rc;
+        r.message = msg;
+        r.doneMs = t;
+        ++S->stats.failed;
     }
     S->active.erase(std::remove_if(S->active.begin(), S->active.end(),
                                    [&](int64_t id) { return S->requests[id].state != PE_REQ_ACTIVE; }),
                     S->active.end());
-    f.valid = false;
+    R.running = false;
+    R.draining = false;
+    R.yielding = false;
+    R.segs.clear();
+    R.firstOpen = 0;
+    R.uploaded = 0;
+    R.doneAfterSync.clear();
     S->cvDone.notify_all();
-    return true;
+    S->cvWork.notify_all();
 }
 
-// The worker: alternates the device's two lanes, so the next wave's bounces run while the
-// previous wave finishes its tail.  The host waits on a lane only when it needs that lane again.
-void workerLoop(pe_server* S) {
+// Ends lane `li`'s wave (lock not held): the last live paths run to their end in the tail
+// kernel, every segment goes to its film, and the lane is free for another scene.
+int32_t endWave(pe_server* S, int li, const Wave& W) {
+    auto& R = S->lanes[li];
+    pe_device* d = S->d;
+    int32_t rc = loopReturn(d, R.loop, true);
+    if (rc == PE_OK) rc = loopTail(d, R.loop, W);
+    if (rc) return rc;
+    {
+        std::lock_guard<std::mutex> lk(S->mu);
+        rc = filmSegments(S, li, true);
+    }
+    if (rc) return rc;
+    const cudaStream_t cs = R.stream;
+    if (cudaEventRecord(R.evEnd, cs) != cudaSuccess || cudaStreamSynchronize(cs) != cudaSuccess) return PE_ERR_CUDA;
+    std::lock_guard<std::mutex> lk(S->mu);
+    float ms = 0.0f;
+    if (cudaEventElapsedTime(&ms, R.evStart, R.evEnd) == cudaSuccess) S->stats.busy_ms += ms;
+    if (S->trace)
+        std::fprintf(S->trace, "wave lane %d scene %d paths %d segments %zu bounces %d device_ms %.2f end %.2f yield %d\n", li,
+                     R.scene, R.loop.nextPath, R.segs.size(), R.loop.iter, ms, S->now(), R.yielding ? 1 : 0);
+    settleDone(S, li);
+    for (int64_t id : S->active) {
+        Request& r = S->requests[id];
+        if (r.lane == li && r.openSegs == 0) r.lane = -1; // free to continue on either lane
+    }
+    R.running = false;
+    R.draining = false;
+    R.yielding = false;
+    R.segs.clear();
+    R.firstOpen = 0;
+    R.uploaded = 0;
+    S->cvWork.notify_all();
+    return PE_OK;
+}
+
+void laneThread(pe_server* S, int li) {
     pe_device* d = S->d;
     cudaSetDevice(d->ordinal);
-    std::vector<Chunk> chunks;
+    auto& R = S->lanes[li];
+    const cudaStream_t cs = R.stream;
+    // the express lane hands its last paths to the tail kernel earlier: latency over efficiency
+    const int64_t tailPaths = pe_device_tail_paths(d) * (express(li) ? 4 : 1);
+    std::unique_lock<std::mutex> lk(S->mu);
     for (;;) {
-        std::unique_lock<std::mutex> lk(S->mu);
-        settleLane(S, 0);
-        settleLane(S, 1);
-        const bool inflight = S->inflight[0].valid || S->inflight[1].valid;
-        if (!inflight)
-            S->cvWork.wait(lk, [&] { return S->stop || !S->queued.empty() || !S->active.empty(); });
         if (S->stop) break;
-        admit(S);
-        cudaEventRecord(S->evAdmit, d->stream);
-        const int L = S->lane;
-        if (S->inflight[L].valid) {
-            // the lane is still busy with the wave before last: wait for it outside the lock
-            lk.unlock();
-            cudaEventSynchronize(d->lanes[L].evDone);
-            continue;
-        }
-        int scene = -1, nSlots = 0, nPix = 0;
-        if (segsWritable(d, L) != PE_OK) break;
-        const int nSegs = planWave(S, L, scene, nSlots, nPix, chunks);
-        if (nSegs == 0) {
-            if (inflight) {
-                // nothing new to trace: wait for the other lane's wave to finish
-                lk.unlock();
-                cudaEventSynchronize(d->lanes[L ^ 1].evDone);
-            } else {
-                // everything queued waits for budget held by films not yet taken
-                S->cvWork.wait_for(lk, std::chrono::milliseconds(2));
+        settleDone(S, li);
+        if (admit(S)) cudaEventRecord(S->evAdmit, S->admitStream);
+        if (!R.running) {
+            const Request* best = bestFor(S, li, -1);
+            if (!best) {
+                S->cvWork.wait_for(lk, std::chrono::milliseconds(5));
+                continue;
             }
+            R.scene = best->scene;
+            R.running = true;
+            R.draining = false;
+            R.yielding = false;
+            R.segs.clear();
+            R.firstOpen = 0;
+            R.uploaded = 0;
+            R.loop.scene = S->scenes[static_cast<size_t>(R.scene)].gpu;
+            ++S->stats.waves;
+            lk.unlock();
+            int32_t rc = loopBegin(d, R.loop, R.dLeft);
+            if (rc == PE_OK && cudaEventRecord(R.evStart, cs) != cudaSuccess) rc = PE_ERR_CUDA;
+            lk.lock();
+            if (rc) {
+                failLane(S, li, rc, pe_last_error());
+                continue;
+            }
+        }
+        LaneLoop& L = R.loop;
+        int fresh = 0;
+        if (!express(li) && expressBusy(S)) {
+            // an express lane runs: this bulk lane launches nothing, so that the interactive
+            // requests' kernels get every SM (running blocks are not preempted by priority);
+            // the express lanes notify when their waves end
+            S->cvWork.wait_for(lk, std::chrono::milliseconds(20), [&] { return S->stop || !expressBusy(S); });
             continue;
         }
-        auto& f = S->inflight[L];
-        f.chunks = chunks;
-        f.valid = true;
-        ++S->stats.waves;
-        S->stats.segments += static_cast<uint64_t>(nSegs);
-        S->stats.paths += static_cast<uint64_t>(nSlots);
+        {
+            // slots of finished sweeps are free again
+            const int32_t rr = loopReturn(d, L, false);
+            if (rr) {
+                failLane(S, li, rr, pe_last_error());
+                continue;
+            }
+        }
+        // making room for a waiting scene is final; running out of work is not (requests of
+        // this scene that arrive meanwhile are taken in while the wave has room)
+        if (!R.yielding && yieldLane(S, li)) R.yielding = true;
+        const bool room = L.pathCap - L.nextPath >= kMinChunk && static_cast<int>(R.segs.size()) < kServerSegs;
+        if (!R.yielding && room) {
+            fresh = planPaths(S, li, std::min(L.freeTop, L.pathCap - L.nextPath));
+            S->stats.paths += static_cast<uint64_t>(fresh);
+        }
+        R.draining = R.yielding || !room || !bestFor(S, li, R.scene);
+        const int nSegs = static_cast<int>(R.segs.size());
+        const int upFirst = R.uploaded;
+        R.uploaded = nSegs;
+        const bool draining = R.draining;
+        const int open = R.firstOpen;
         lk.unlock();
-        d->scene = S->scenes[static_cast<size_t>(scene)].gpu;
-        d->hasScene = true;
-        const cudaStream_t cs = d->lanes[L].stream;
-        RenderTimer tm;
         int32_t rc = PE_OK;
-        if (cudaStreamWaitEvent(cs, S->evAdmit, 0) != cudaSuccess || cudaEventRecord(f.evStart, cs) != cudaSuccess)
-            rc = PE_ERR_CUDA;
-        if (rc == PE_OK) rc = runWave(d, L, d->lanes[L].paths, nSegs, nSlots, nPix, tm);
+        const Wave W{R.dSegs, std::max(1, nSegs), L.nextPath + fresh, 0};
+        if (nSegs > upFirst) {
+            const size_t n = static_cast<size_t>(nSegs - upFirst);
+            if (cudaMemcpyAsync(R.dSegs + upFirst, R.hSegs + upFirst, n * sizeof(WaveSeg), cudaMemcpyHostToDevice, cs) !=
+                    cudaSuccess ||
+                cudaMemcpyAsync(R.dLeft + upFirst, R.hInit + upFirst, n * sizeof(uint32_t), cudaMemcpyHostToDevice, cs) !=
+                    cudaSuccess)
+                rc = PE_ERR_CUDA;
+        }
+        if (rc == PE_OK) rc = loopInject(d, L, W, fresh);
+        bool ended = false;
+        if (rc == PE_OK && (L.live == 0 || (draining && static_cast<int64_t>(L.live) <= tailPaths))) {
+            if (L.live == 0 && !draining) {
+                // nothing in flight and nothing to inject yet: wait for work
+                lk.lock();
+                S->cvWork.wait_for(lk, std::chrono::milliseconds(1));
+                continue;
+            }
+            rc = endWave(S, li, W);
+            ended = true;
+        } else if (rc == PE_OK) {
+            rc = loopBounce(d, L, W, R.hLeft, R.dLeft, open, nSegs - open);
+        }
         const std::string msg = rc == PE_OK ? std::string() : std::string(pe_last_error());
         lk.lock();
-        f.rc = rc;
-        f.message = msg;
-        S->lane = L ^ 1;
+        if (rc) {
+            failLane(S, li, rc, msg);
+            continue;
+        }
+        if (ended) continue;
+        settleDone(S, li);
+        rc = filmSegments(S, li, false);
+        if (rc) failLane(S, li, rc, "film kernel launch failed");
     }
-    cudaStreamSynchronize(d->lanes[0].stream);
-    cudaStreamSynchronize(d->lanes[1].stream);
+    lk.unlock();
+    cudaStreamSynchronize(cs);
+}
+
+// Frees the server's streams, events and segment tables, then the server.
+void releaseServer(pe_server* S) {
+    if (S->trace) std::fclose(S->trace);
+    if (S->copyStream) cudaStreamDestroy(S->copyStream);
+    if (S->admitStream) cudaStreamDestroy(S->admitStream);
+    if (S->evAdmit) cudaEventDestroy(S->evAdmit);
+    for (auto& kv : S->filters) cudaFree(kv.second);
+    for (auto& R : S->lanes) {
+        if (R.evStart) cudaEventDestroy(R.evStart);
+        if (R.evEnd) cudaEventDestroy(R.evEnd);
+        if (R.hSegs) cudaFreeHost(R.hSegs);
+        if (R.hLeft) cudaFreeHost(R.hLeft);
+        if (R.hInit) cudaFreeHost(R.hInit);
+        if (R.dSegs) cudaFree(R.dSegs);
+        if (R.dLeft) cudaFree(R.dLeft);
+        for (cudaEvent_t ev : R.eventPool) cudaEventDestroy(ev);
+        for (auto& pe : R.doneEvents) cudaEventDestroy(pe.second);
+        if (R.own.stream) {
+            cudaStreamSynchronize(R.own.stream);
+            freeList(R.own.bufs);
+            cudaStreamDestroy(R.own.stream);
+        }
+        if (R.own.hCounters) cudaFreeHost(R.own.hCounters);
+        LaneLoop& L = R.loop;
+        if (L.side) {
+            cudaStreamSynchronize(L.side);
+            cudaStreamDestroy(L.side);
+        }
+        if (L.born) cudaFree(L.born);
+        if (L.sweepCnt) cudaFree(L.sweepCnt);
+        if (L.sweepCursor) cudaFree(L.sweepCursor);
+        for (int b = 0; b < LaneLoop::kSweepBufs; ++b) {
+            if (L.sweepBuf[b]) cudaFree(L.sweepBuf[b]);
+            if (L.evReady[b]) cudaEventDestroy(L.evReady[b]);
+            if (L.evDone[b]) cudaEventDestroy(L.evDone[b]);
+        }
+    }
+    delete S;
 }
 
 pe_server* failCreate(char* err, size_t n, const std::string& msg) {
@@ -348,14 +667,53 @@ pe_server* pe_server_create(pe_device* d, uint64_t budget, char* err, size_t err
     S->savedScene = d->scene;
     S->savedHasScene = d->hasScene;
     S->stats.budget_bytes = budget;
-    if (cudaStreamCreateWithFlags(&S->copyStream, cudaStreamNonBlocking) != cudaSuccess ||
-        cudaEventCreateWithFlags(&S->evAdmit, cudaEventDisableTiming) != cudaSuccess ||
-        cudaEventCreate(&S->inflight[0].evStart) != cudaSuccess || cudaEventCreate(&S->inflight[1].evStart) != cudaSuccess) {
-        delete S;
-        return failCreate(err, errLen, "pe_server_create: stream or event creation failed");
+    bool ok = cudaStreamCreateWithFlags(&S->copyStream, cudaStreamNonBlocking) == cudaSuccess &&
+              cudaStreamCreateWithFlags(&S->admitStream, cudaStreamNonBlocking) == cudaSuccess &&
+              cudaEventCreateWithFlags(&S->evAdmit, cudaEventDisableTiming) == cudaSuccess;
+    int loPrio = 0, hiPrio = 0;
+    cudaDeviceGetStreamPriorityRange(&loPrio, &hiPrio);
+    for (int li = 0; li < kLanes && ok; ++li) {
+        auto& R = S->lanes[li];
+        if (express(li)) {
+            // the express lane: its own path state, on the highest-priority streams
+            ok = cudaStreamCreateWithPriority(&R.own.stream, cudaStreamNonBlocking, hiPrio) == cudaSuccess &&
+                 cudaMallocHost(&R.own.hCounters, 32 * sizeof(uint32_t)) == cudaSuccess &&
+                 allocLane(R.own, kExpressSlots) == PE_OK;
+            R.loop.ln = &R.own;
+        } else {
+            R.loop.ln = &d->lanes[li];
+        }
+        R.stream = R.loop.ln->stream;
+        for (int e = 0; e < 64 && ok; ++e) {
+            cudaEvent_t ev = nullptr;
+            ok = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) == cudaSuccess;
+            if (ok) R.eventPool.push_back(ev);
+        }
+        ok = ok && cudaEventCreate(&R.evStart) == cudaSuccess && cudaEventCreate(&R.evEnd) == cudaSuccess &&
+             cudaMallocHost(&R.hSegs, kServerSegs * sizeof(WaveSeg)) == cudaSuccess &&
+             cudaMallocHost(&R.hLeft, kServerSegs * sizeof(uint32_t)) == cudaSuccess &&
+             cudaMallocHost(&R.hInit, kServerSegs * sizeof(uint32_t)) == cudaSuccess &&
+             cudaMalloc(&R.dSegs, kServerSegs * sizeof(WaveSeg)) == cudaSuccess &&
+             cudaMalloc(&R.dLeft, kServerSegs * sizeof(uint32_t)) == cudaSuccess;
+        LaneLoop& L = R.loop;
+        const size_t cap = ok ? R.loop.ln->paths.capacity : 0;
+        L.sweepAge = express(li) ? kExpressSweepAge : kSweepAge;
+        ok = ok && cudaStreamCreateWithPriority(&L.side, cudaStreamNonBlocking, express(li) ? hiPrio : loPrio) == cudaSuccess &&
+             cudaMalloc(&L.born, cap * sizeof(int32_t)) == cudaSuccess &&
+             cudaMalloc(&L.sweepCnt, LaneLoop::kSweepBufs * sizeof(uint32_t)) == cudaSuccess &&
+             cudaMalloc(&L.sweepCursor, LaneLoop::kSweepBufs * sizeof(uint32_t)) == cudaSuccess;
+        for (int b = 0; b < LaneLoop::kSweepBufs; ++b)
+            ok = ok && cudaMalloc(&L.sweepBuf[b], cap * sizeof(int32_t)) == cudaSuccess &&
+                 cudaEventCreateWithFlags(&L.evReady[b], cudaEventDisableTiming) == cudaSuccess &&
+                 cudaEventCreateWithFlags(&L.evDone[b], cudaEventDisableTiming) == cudaSuccess;
+    }
+    if (!ok) {
+        releaseServer(S);
+        return failCreate(err, errLen, "pe_server_create: stream, event or segment table allocation failed");
     }
     d->filmLane = -1;
-    S->worker = std::thread(workerLoop, S);
+    if (const char* tp = std::getenv("PE_SERVER_TRACE")) S->trace = std::fopen(tp, "w");
+    for (int li = 0; li < kLanes; ++li) S->lanes[li].th = std::thread(laneThread, S, li);
     return S;
 }
 
@@ -366,23 +724,23 @@ void pe_server_destroy(pe_server* S) {
         S->stop = true;
     }
     S->cvWork.notify_all();
-    if (S->worker.joinable()) S->worker.join();
+    for (auto& R : S->lanes)
+        if (R.th.joinable()) R.th.join();
     pe_device* d = S->d;
     cudaSetDevice(d->ordinal);
     cudaStreamSynchronize(d->stream);
     cudaStreamSynchronize(d->lanes[1].stream);
+    for (int li = 2; li < kLanes; ++li)
+        if (S->lanes[li].stream) cudaStreamSynchronize(S->lanes[li].stream);
     cudaStreamSynchronize(S->copyStream);
+    cudaStreamSynchronize(S->admitStream);
     for (auto& kv : S->requests)
         if (kv.second.sum) cudaFreeAsync(kv.second.sum, d->stream);
     cudaStreamSynchronize(d->stream);
     for (ResidentScene& rs : S->scenes) freeList(rs.bufs);
-    cudaStreamDestroy(S->copyStream);
-    cudaEventDestroy(S->evAdmit);
-    cudaEventDestroy(S->inflight[0].evStart);
-    cudaEventDestroy(S->inflight[1].evStart);
     d->scene = S->savedScene;
     d->hasScene = S->savedHasScene;
-    delete S;
+    releaseServer(S);
 }
 
 int32_t pe_server_add_scene(pe_server* S, const pe_scene* scene) {

@@ -77,6 +77,13 @@ struct Paths {
     int32_t* pathOf;     // wave path index held by each slot
     int32_t* freeQ;      // slots freed by the shading kernel this bounce
     float4* Lout;        // radiance of each ended path, by wave path index (read by the film kernel)
+    uint32_t* segLeft;   // per segment: paths not yet ended (null unless the server tracks segments)
+    // sweeps (continuous waves): a path alive for sweepAge bounces leaves the wavefront for a
+    // tail-kernel launch on a side stream (sweepAge 0: off)
+    int32_t* born;       // bounce at which each slot's path was injected
+    int32_t* sweepQ;     // this bounce's swept slots (counted in counters[CNT_SWEEP])
+    int32_t sweepAge;
+    int32_t iter;        // current bounce of the continuous wave
     uint32_t capacity;
     // [0] queue A count, [1] queue B count, [2] shadow count, [3] closest-hit work cursor,
     // [4] any-hit work cursor, [5] shade work cursor, [6..11] rays per shading key, [12] errors,
@@ -88,9 +95,9 @@ struct Paths {
 constexpr int kShadeKeys = 6;
 enum CounterSlots { CNT_QA = 0, CNT_QB = 1, CNT_SHADOW = 2, CNT_WORK_ISECT = 3, CNT_WORK_SHADOW = 4,
                     CNT_WORK_SHADE = 5, CNT_KEYS = 6, CNT_ERRORS = 12, CNT_WORK_TAIL = 13, CNT_GUIDE_Q = 14,
-                    CNT_TRAIN = 15, CNT_FREE = 16, CNT_TOTAL = 17 };
+                    CNT_TRAIN = 15, CNT_FREE = 16, CNT_SWEEP = 17, CNT_TOTAL = 18 };
 // Paths per wave with regeneration, as a multiple of the slots.
-constexpr int kStreamFactor = 4;
+constexpr int kStreamFactor = 16;
 // Vertices an SD-tree training path records (the reference records up to 32; its paths in these
 // workloads rarely pass 8 guidable vertices).
 constexpr int kSdRecords = 8;
@@ -117,7 +124,10 @@ struct WaveSeg {
     float* sq;
     int slotFirst;
     int pixFirst;
+    int flags;              // SegFlags
+    int pad;
 };
+enum SegFlags { SEG_SWEEP = 1 }; // paths of the segment may leave a continuous wave for a sweep
 
 // The segments of one wave, ordered by slotFirst (and so by pixFirst).
 struct Wave {

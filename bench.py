@@ -2,8 +2,9 @@
 
 Workload (one ``step``): four samples per pixel of a 1920×1080 frame of the ~1M-triangle torus
 knot with eight Disney materials, a 2048×1024 HDR sky (sun lobe 60 % of power) and a softbox,
-max depth 12 — i.e. 8,294,400 camera paths (four waves) through the wavefront (generate, closest
-hit, shade, any hit, tail, film) per step, a batch of the 256-spp frame.  Metric: paths/s (W·H·spp / render seconds, the reference's
+max depth 12 — i.e. 8,294,400 camera paths per step, one wave through the 2M path slots (generate,
+then per bounce closest hit, shade, any hit and the refill of freed slots with the wave's next
+paths, then tail and film), a batch of the 256-spp frame.  Metric: paths/s (W·H·spp / render seconds, the reference's
 msamplesPerSecond definition).
 
 ``value``   device-resident: inputs in HBM, K steps into the resident film, CUDA events on the
@@ -39,7 +40,7 @@ ROOT = pathlib.Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
 WIDTH, HEIGHT, DEPTH = 1920, 1080, 12
-SPP_PER_STEP = 4  # one step = 4 samples per pixel of the 1080p frame (4 waves of ~2M paths)
+SPP_PER_STEP = 4  # one step = 4 samples per pixel of the 1080p frame (one wave of 8.3M paths)
 NODE_BYTES, TRI_BYTES, RAY_BYTES, HIT_BYTES, QUEUE_BYTES = 64, 48, 32, 16, 4
 L2_NOTE = "inputs larger than L2: 140 MB resident scene + 300 MB path state per 2M-path wave (L2 126 MB)"
 
@@ -341,6 +342,8 @@ def main():
                     help="served-mix benchmark (request server vs the plain per-request loop) instead")
     ap.add_argument("--serve-requests", type=int, default=24)
     ap.add_argument("--serve-quick", action="store_true", help="small scenes (a smoke run of the served mix)")
+    ap.add_argument("--guide", action="store_true",
+                    help="time to a relMSE target on the indirect-lit room: plain vs learned proposal vs SD-tree")
     ap.add_argument("--profile-case", action="store_true",
                     help="a small case for kernel captures: 960x540 knot waves, then guided room waves")
     args = ap.parse_args()
@@ -351,6 +354,8 @@ def main():
         return run_serve(args)
     if args.profile_case:
         return run_profile_case()
+    if args.guide:
+        return run_guide(args)
     return run_ours(args)
 
 
@@ -398,6 +403,21 @@ def run_serve(args):
                       + (" (reduced scenes)" if args.serve_quick else ""), **res["mix"]},
            "served": s, "plain": p, "served_over_plain": res["speedup"],
            "preview_p99_ms": s["preview_p99_ms"], "clocks": clocks.summary()}
+    print(json.dumps(out))
+    dev.close()
+    return 0
+
+
+def run_guide(args):
+    """Guided sampling's time to a relMSE target against plain sampling (guidebench.py)."""
+    pe = pe_load()
+    from photon_engine_b200 import guidebench
+    dev = pe.CudaDevice(0)
+    with ClockSampler(dev.pci_bus_id) as clocks:
+        res = guidebench.run(pe, dev)
+    out = {"metric": "time-to-relMSE speed-up of guided sampling (indirect-lit room)",
+           "value": res["time_to_relmse_speedup"], "unit": "x", "n_gpus": 1, "higher_is_better": True,
+           "dtype": "f32", "data": "synthetic (seeded procedural scene)", **res, "clocks": clocks.summary()}
     print(json.dumps(out))
     dev.close()
     return 0

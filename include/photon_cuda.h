@@ -317,7 +317,8 @@ int32_t pe_device_bsdf_probe(pe_device* d, int32_t material, const pe_bsdf_query
  * it.  Parameter block layout (FP32): W1[64][48], b1[64], W2[64][64], b2, W3[64][64], b3,
  * W4[64][64], b4[64] (15616 floats); grid 16 x 2^18 x 2 floats. */
 enum { PE_GUIDE_MLP_PARAMS = 15616, PE_GUIDE_GRID_PARAMS = 16 * 262144 * 2, PE_GUIDE_OUTPUTS = 40 };
-/* (Re)initialises the network from a seed over the box [box_min, box_max]. */
+/* (Re)initialises the network from a seed over the box [box_min, box_max]; with both NULL, over
+ * the current scene's box as pe_device_set_guiding chooses it (so a later set_guiding keeps it). */
 int32_t pe_device_guide_reset(pe_device* d, uint64_t seed, const float box_min[3], const float box_max[3]);
 int32_t pe_device_guide_get(pe_device* d, float* mlp, float* grid);
 int32_t pe_device_guide_set(pe_device* d, const float* mlp, const float* grid);

@@ -498,6 +498,15 @@ int32_t guideBuffers(pe_device* d) {
 
 extern "C" {
 
+// The hash grid's box: the scene's bounds, padded by 0.1 % of its extent.
+static void sceneGuideBox(const pe_device* d, float lo[3], float hi[3]) {
+    for (int i = 0; i < 3; ++i) {
+        const float pad = 1e-3f * (d->scene.rootMax[i] - d->scene.rootMin[i]) + 1e-6f;
+        lo[i] = d->scene.rootMin[i] - pad;
+        hi[i] = d->scene.rootMax[i] + pad;
+    }
+}
+
 int32_t pe_device_set_guiding(pe_device* d, int32_t mode, int32_t warmupSteps, float lr) {
     if (!d || mode < 0 || mode > 2 || warmupSteps < 0 || !(lr >= 0.0f)) {
         setError("pe_device_set_guiding: bad argument");
@@ -527,13 +536,9 @@ int32_t pe_device_set_guiding(pe_device* d, int32_t mode, int32_t warmupSteps, f
     int32_t rc = PE_OK;
     // a network is kept across calls while it was built over this scene's box
     float lo[3], hi[3];
+    sceneGuideBox(d, lo, hi);
     bool same = G.mlp != nullptr;
-    for (int i = 0; i < 3; ++i) {
-        const float pad = 1e-3f * (d->scene.rootMax[i] - d->scene.rootMin[i]) + 1e-6f;
-        lo[i] = d->scene.rootMin[i] - pad;
-        hi[i] = d->scene.rootMax[i] + pad;
-        same = same && lo[i] == G.boxMin[i] && hi[i] == G.boxMax[i];
-    }
+    for (int i = 0; i < 3; ++i) same = same && lo[i] == G.boxMin[i] && hi[i] == G.boxMax[i];
     if (!same) {
         for (int i = 0; i < 3; ++i) {
             G.boxMin[i] = lo[i];
@@ -563,14 +568,23 @@ int32_t pe_device_guide_info(pe_device* d, pe_guide_info* out) {
 }
 
 int32_t pe_device_guide_reset(pe_device* d, uint64_t seed, const float boxMin[3], const float boxMax[3]) {
-    if (!d || !boxMin || !boxMax) {
+    if (!d || (!boxMin) != (!boxMax)) {
         setError("pe_device_guide_reset: null argument");
         return PE_ERR_INVALID;
     }
     PE_CUDA(cudaSetDevice(d->ordinal));
-    for (int i = 0; i < 3; ++i) {
-        d->guide.boxMin[i] = boxMin[i];
-        d->guide.boxMax[i] = boxMax[i];
+    if (!boxMin) {
+        // the scene's box, padded as pe_device_set_guiding pads it
+        if (!d->hasScene) {
+            setError("pe_device_guide_reset: no box given and no scene set");
+            return PE_ERR_NO_SCENE;
+        }
+        sceneGuideBox(d, d->guide.boxMin, d->guide.boxMax);
+    } else {
+        for (int i = 0; i < 3; ++i) {
+            d->guide.boxMin[i] = boxMin[i];
+            d->guide.boxMax[i] = boxMax[i];
+        }
     }
     return guideReset(d, seed);
 }

@@ -38,7 +38,7 @@
 extern "C" {
 #endif
 
-#define PE_ABI_VERSION 3
+#define PE_ABI_VERSION 4
 
 typedef enum pe_status {
     PE_OK = 0,
@@ -95,6 +95,8 @@ typedef struct pe_material {
     float film_thickness;
     int32_t has_absorption; /* setAbsorption called (builds the interior medium) */
     int32_t has_scattering; /* setScattering called */
+    /* any type */
+    float round_edge_radius; /* Material::setRoundEdgeRadius (material.h:136); 0 = off */
 } pe_material;
 
 /* Camera as the reference's Camera::describeGpu() (src/camera/camera.h:17-29). */
@@ -123,6 +125,8 @@ typedef struct pe_settings {
     float filter_width;
     float clamp_indirect;   /* 0 = off */
     uint64_t seed;          /* Owen-Sobol seed (reference renderSamples: 12345) */
+    float ao_strength;      /* RenderSettings::aoStrength: contact AO at camera hits; 0 = off */
+    int32_t pad;
 } pe_settings;
 
 /* ---- scene builder --------------------------------------------------------- */
@@ -149,6 +153,11 @@ int32_t pe_scene_add_material(pe_scene* s, const pe_material* m);
  * An emissive material registers one triangle light per triangle. */
 int32_t pe_scene_add_mesh(pe_scene* s, const float* positions, uint32_t n_vertices, const float* normals,
                           const float* uvs, const uint32_t* indices, uint32_t n_triangles, int32_t material);
+/* Scene::setShadowCatcher (scene.h:90): the shape that camera rays see as the background darkened
+ * by the shadows falling on it (path_tracer.cpp:515-563); -1 = none.  Shapes count from 0 in the
+ * order they were added: one per pe_scene_add_mesh, two per pe_scene_add_area_light (its two
+ * triangles, as Scene::addLight adds them).  Call before pe_scene_build. */
+int32_t pe_scene_set_shadow_catcher(pe_scene* s, int32_t shape);
 /* Scene::addLight(AreaLight) — rectangle p + s*u + t*v, two-sided, plus its
  * two emissive triangles in the BVH (src/engine/scene.cpp:65-99). */
 int32_t pe_scene_add_area_light(pe_scene* s, const float p[3], const float u[3], const float v[3],

@@ -67,6 +67,7 @@ def _load(fast: bool = False):
         "ref_light_sample": (C.c_int32, [P, C.c_int32, FP, FP, FP, C.c_size_t, FP, FP, FP, FP]),
         "ref_env_eval": (C.c_int32, [P, FP, C.c_size_t, FP, FP]),
         "ref_render_guided": (C.c_int32, [P, C.c_void_p, C.c_void_p, C.c_int32, C.c_int32, C.c_int32, FP, UP]),
+        "ref_scene_set_shadow_catcher": (C.c_int32, [P, C.c_int32]),
         "ref_dtree_probe": (C.c_int32, [FP, FP, C.c_int32, FP, FP, C.c_int32, FP, FP, C.c_int32, FP, FP]),
     }
     for name, (res, args) in sig.items():
@@ -109,6 +110,8 @@ class RefScene:
                                                        _f3(obj.radiance), 1 if obj.visible_to_camera else 0)
             if rc != 0:
                 raise RuntimeError("reference rejected a shape")
+        if getattr(scene, "shadow_catcher", None) is not None:
+            self.lib.ref_scene_set_shadow_catcher(self.h, int(scene.shadow_catcher))
         env = scene.environment
         if env is not None:
             img = env.image

@@ -3,7 +3,7 @@
 // and bench.py's CPU-baseline leg load the library built from this file; the product never
 // does.  Each entry point drives the reference's public classes exactly as its own code does:
 //
-//   ref_scene_*      Scene::addShape / addLight / setEnvironment / buildAccelerator
+//   ref_scene_*      Scene::addShape / addLight / setEnvironment / setShadowCatcher / buildAccelerator
 //                    (src/engine/scene.cpp:18-185), own BVH forced (Scene::setPreferOwnBvh)
 //   ref_render       Renderer::renderSamples (src/engine/renderer.cpp:392-531); seed 12345
 //   ref_render_seeded  the same tile loop as renderSamples with a caller seed: tracePixel
@@ -90,8 +90,11 @@ struct RefScene {
 
 std::shared_ptr<Material> makeMaterial(const pe_material& m) {
     switch (m.type) {
-        case PE_MAT_LAMBERT:
-            return std::make_shared<Lambertian>(c3(m.base_color), c3(m.emission));
+        case PE_MAT_LAMBERT: {
+            auto l = std::make_shared<Lambertian>(c3(m.base_color), c3(m.emission));
+            l->setRoundEdgeRadius(m.round_edge_radius);
+            return l;
+        }
         case PE_MAT_DISNEY: {
             auto d = std::make_shared<DisneyMaterial>(c3(m.base_color), m.metallic, m.roughness, m.specular);
             d->setClearCoat(m.clearcoat);
@@ -115,6 +118,7 @@ std::shared_ptr<Material> makeMaterial(const pe_material& m) {
             if (m.flake_density > 0.0f) d->setFlakes(m.flake_density, m.flake_size, m.flake_roughness, c3(m.flake_color));
             d->setEmission(c3(m.emission));
             d->setOpacity(m.opacity);
+            d->setRoundEdgeRadius(m.round_edge_radius);
             return d;
         }
         case PE_MAT_DIELECTRIC: {
@@ -124,10 +128,14 @@ std::shared_ptr<Material> makeMaterial(const pe_material& m) {
             if (m.has_scattering) g->setScattering(m.scatter_density, c3(m.scatter_color), m.scatter_anisotropy);
             g->setThinWalled(m.thin_walled != 0);
             g->setThinFilm(m.film_thickness);
+            g->setRoundEdgeRadius(m.round_edge_radius);
             return g;
         }
-        case PE_MAT_MIRROR:
-            return std::make_shared<Mirror>(c3(m.base_color));
+        case PE_MAT_MIRROR: {
+            auto mi = std::make_shared<Mirror>(c3(m.base_color));
+            mi->setRoundEdgeRadius(m.round_edge_radius);
+            return mi;
+        }
         default:
             return nullptr;
     }
@@ -143,6 +151,7 @@ RenderSettings toSettings(const pe_settings& st, int threads) {
     s.filter.type = static_cast<PixelFilterType>(st.filter_type);
     s.filter.width = st.filter_width;
     s.clampIndirect = st.clamp_indirect;
+    s.aoStrength = st.ao_strength;
     s.numThreads = threads;
     return s;
 }
@@ -207,6 +216,18 @@ int32_t ref_scene_add_mesh(void* s, const float* pos, uint32_t nv, const float* 
     auto mesh = std::make_shared<TriangleMesh>(p, n, t, ind, rs->materials[static_cast<size_t>(material)].get());
     rs->scene.addShape(mesh);
     rs->indexNewShapes();
+    return 0;
+}
+
+// Scene::setShadowCatcher with the shape added `shape`-th (-1: none).
+int32_t ref_scene_set_shadow_catcher(void* s, int32_t shape) {
+    auto* rs = static_cast<RefScene*>(s);
+    const auto& shapes = rs->scene.shapes();
+    if (shape < 0 || shape >= static_cast<int32_t>(shapes.size())) {
+        rs->scene.setShadowCatcher(nullptr);
+        return shape < 0 ? 0 : -1;
+    }
+    rs->scene.setShadowCatcher(shapes[static_cast<size_t>(shape)].get());
     return 0;
 }
 
@@ -344,7 +365,7 @@ int32_t ref_render_rows(void* s, const pe_camera* cam, const pe_settings* st, in
     DescCamera camera(*cam);
     const int w = st->width, h = st->height;
     Film film(w, h);
-    PathTracer integrator(st->max_bounces, st->rr_depth, 0.0f, st->shadow_quality);
+    PathTracer integrator(st->max_bounces, st->rr_depth, st->ao_strength, st->shadow_quality);
     integrator.setClampIndirect(st->clamp_indirect);
     PixelFilter pf;
     pf.type = static_cast<PixelFilterType>(st->filter_type);
@@ -369,7 +390,14 @@ int32_t ref_render_rows(void* s, const pe_camera* cam, const pe_settings* st, in
                     Ray ray = camera.generateRay(sx, sy, lens);
                     ray.coneWidth = camera.pixelConeWidth(h);
                     ray.coneSpread = camera.pixelConeSpread(h);
-                    film.addSample(x, y, integrator.Li(ray, rs->scene, sampler));
+                    // as tracePixel: with a colour or transparent background the integrator gets
+                    // the primary-hit record, through which camera misses see that background
+                    if (rs->scene.background().mode == Background::Mode::Environment) {
+                        film.addSample(x, y, integrator.Li(ray, rs->scene, sampler));
+                    } else {
+                        PathTracer::PrimaryHit primary;
+                        film.addSample(x, y, integrator.Li(ray, rs->scene, sampler, &primary, nullptr));
+                    }
                 }
         }
     };

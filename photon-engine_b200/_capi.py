@@ -39,6 +39,7 @@ class pe_material(C.Structure):
         ("scatter_density", C.c_float), ("scatter_color", F3), ("scatter_anisotropy", C.c_float),
         ("thin_walled", C.c_int32), ("film_thickness", C.c_float),
         ("has_absorption", C.c_int32), ("has_scattering", C.c_int32),
+        ("round_edge_radius", C.c_float),
     ]
 
 
@@ -50,7 +51,8 @@ class pe_camera(C.Structure):
 class pe_settings(C.Structure):
     _fields_ = [("width", C.c_int32), ("height", C.c_int32), ("max_bounces", C.c_int32), ("rr_depth", C.c_int32),
                 ("shadow_quality", C.c_int32), ("filter_type", C.c_int32), ("filter_width", C.c_float),
-                ("clamp_indirect", C.c_float), ("seed", C.c_uint64)]
+                ("clamp_indirect", C.c_float), ("seed", C.c_uint64), ("ao_strength", C.c_float),
+                ("pad", C.c_int32)]
 
 
 class pe_scene_info(C.Structure):
@@ -127,6 +129,7 @@ UP = C.POINTER(C.c_uint32)
 SIGNATURES = {
     "pe_last_error": (C.c_char_p, []),
     "pe_abi_version": (C.c_int32, []),
+    "pe_scene_set_shadow_catcher": (C.c_int32, [P, C.c_int32]),
     "pe_material_defaults": (None, [C.c_int32, C.POINTER(pe_material)]),
     "pe_scene_create": (P, []),
     "pe_scene_destroy": (None, [P]),

@@ -121,6 +121,10 @@ int32_t checkSettings(const pe_camera* cam, const pe_settings* st) {
         setError("only the pinhole perspective camera is supported");
         return PE_ERR_LIMIT;
     }
+    if (!(st->ao_strength >= 0.0f) || !(st->ao_strength <= 1e30f)) {
+        setError("ao_strength must be finite and >= 0");
+        return PE_ERR_INVALID;
+    }
     return PE_OK;
 }
 
@@ -139,6 +143,7 @@ WaveSeg makeSeg(const pe_camera* cam, const pe_settings* st) {
     A.rrDepth = st->rr_depth;
     A.shadowSamples = st->shadow_quality < 1 ? 1 : st->shadow_quality;
     A.clampIndirect = st->clamp_indirect > 0.0f ? st->clamp_indirect : 0.0f;
+    A.aoStrength = st->ao_strength > 0.0f ? st->ao_strength : 0.0f;
     return A;
 }
 
@@ -760,6 +765,16 @@ int32_t uploadScene(pe_device* d, const pe_scene* s, SceneGPU& G, std::vector<De
     if ((rc = upload(d, bufs, E.image, e.image)) || (rc = upload(d, bufs, E.func, e.misFunc)) ||
         (rc = upload(d, bufs, E.marginalCdf, e.misMarg)) || (rc = upload(d, bufs, E.condCdf, e.misCond)))
         return rc;
+    // the shadow catcher samples the environment without MIS compensation (sampleLiFull)
+    G.envFull = E;
+    if (B.catcherShape >= 0) {
+        EnvGPU& F = G.envFull;
+        F.funcInt = e.fullInt;
+        F.valid = e.fullValid ? 1 : 0;
+        if ((rc = upload(d, bufs, F.func, e.fullFunc)) || (rc = upload(d, bufs, F.marginalCdf, e.fullMarg)) ||
+            (rc = upload(d, bufs, F.condCdf, e.fullCond)))
+            return rc;
+    }
     G.tables = d->dTables;
     G.bgMode = s->bgMode;
     for (int i = 0; i < 3; ++i) G.bgColor[i] = s->bgColor[i];
@@ -767,6 +782,7 @@ int32_t uploadScene(pe_device* d, const pe_scene* s, SceneGPU& G, std::vector<De
     G.hasVolumes = B.hasVolumes ? 1 : 0;
     G.hasSubsurface = B.hasSubsurface ? 1 : 0;
     G.exitMaterial = B.exitMaterial;
+    G.catcherShape = B.catcherShape;
     PE_CUDA(cudaStreamSynchronize(d->stream));
     return PE_OK;
 }

@@ -528,6 +528,7 @@ MatGPU resolveMaterial(const pe_material& m) {
     };
     c3(g.base, m.base_color);
     c3(g.emission, m.emission);
+    g.roundEdge = m.round_edge_radius > 0.0f ? m.round_edge_radius : 0.0f; // setRoundEdgeRadius
     if (m.type == PE_MAT_DISNEY) {
         g.metallic = m.metallic;
         g.roughness = smax(0.001f, m.roughness);
@@ -772,6 +773,7 @@ static int32_t buildScene(pe_scene* s) {
     HostBuild& B = s->build;
     B = HostBuild{};
     B.materials = s->materials;
+    B.catcherShape = s->catcherShape >= 0 && s->catcherShape < static_cast<int32_t>(s->shapes.size()) ? s->catcherShape : -1;
     if (B.materials.size() >= 0xFFFFu) {
         setError("scene has " + std::to_string(B.materials.size()) + " materials; at most 65534 are supported");
         return PE_ERR_LIMIT;
@@ -1099,6 +1101,16 @@ int32_t pe_scene_add_mesh(pe_scene* s, const float* positions, uint32_t nv, cons
         }
     }
     s->shapes.push_back(std::move(sh));
+    s->built = false;
+    return PE_OK;
+}
+
+int32_t pe_scene_set_shadow_catcher(pe_scene* s, int32_t shape) {
+    if (!s || shape < -1) {
+        setError("pe_scene_set_shadow_catcher: bad argument");
+        return PE_ERR_INVALID;
+    }
+    s->catcherShape = shape;
     s->built = false;
     return PE_OK;
 }

@@ -67,6 +67,7 @@ struct HostBuild {
     bool hasSubsurface = false;
     bool hasDispersion = false;
     int32_t exitMaterial = -1;   // white Lambert of the subsurface exit vertex
+    int32_t catcherShape = -1;   // shadow-catcher shape
 };
 
 } // namespace pe
@@ -80,6 +81,7 @@ struct pe_scene {
     int32_t bgMode = PE_BG_ENVIRONMENT;
     float bgColor[3] = {0.18f, 0.18f, 0.18f};
     bool built = false;
+    int32_t catcherShape = -1;   // Scene::setShadowCatcher
     pe::HostBuild build;
     uint64_t version = 0;
 };

@@ -435,6 +435,105 @@ __device__ __noinline__ bool sdGuidedSample(const TablesGPU* T, const MatGPU& ma
     return true;
 }
 
+// ---- surface effects of Li that cast rays of their own ------------------------------------------
+// Contact ambient occlusion (approxAo, path_tracer.cpp:27-45): `samples` cosine rays of at most
+// 0.35 over the shading normal; the path's throughput is scaled by lerp(1, visibility, strength).
+__device__ __noinline__ float approxAo(const SceneGPU& S, const Isect& is, Sobol& sb, float strength, int samples) {
+    if (strength <= 0.0f || samples <= 0) return 1.0f;
+    const TablesGPU* T = S.tables;
+    const Frame frame = frameFromNormal(is.normal);
+    float occ = 0.0f;
+    uint32_t n0 = 0, n1 = 0;
+    for (int i = 0; i < samples; ++i) {
+        const V3 local = sampleCosineHemisphere(get2D(T, sb));
+        const V3 dir = normalize(toWorld(frame, local));
+        if (traceAny<false>(S, spawnOrigin(is, dir), dir, VIS_SHADOW, 0.0f, 0.35f, n0, n1)) occ += 1.0f;
+    }
+    const float visibility = 1.0f - (occ / static_cast<float>(samples));
+    return lerpf(1.0f, visibility, strength);
+}
+
+// Rounded edges (roundedEdgeNormal, path_tracer.cpp:209-255): six points on a disk of `radius`
+// around the hit, each probed along one of the frame's axes (normal ½, tangents ¼ each) from both
+// sides with rays of 2·radius; the outward normals of hits on the same shape within 1.5·radius,
+// weighted by their projection on the probe axis, average with a quarter of the own normal.
+__device__ __noinline__ V3 roundedEdgeNormal(const SceneGPU& S, const Isect& is, float radius, Sobol& sb) {
+    const TablesGPU* T = S.tables;
+    const V3 N = is.normal;
+    const Frame f = frameFromNormal(N);
+    V3 sum = N * 0.25f;
+    uint32_t n0 = 0, n1 = 0;
+    for (int i = 0; i < 6; ++i) {
+        const float ua = get1D(sb);
+        const V2 dd = sampleDiskConcentric(get2D(T, sb));
+        const V2 d = mk2(dd.x * radius, dd.y * radius);
+        V3 axis, s, t;
+        if (ua < 0.5f) {
+            axis = f.n; s = f.s; t = f.t;
+        } else if (ua < 0.75f) {
+            axis = f.s; s = f.t; t = f.n;
+        } else {
+            axis = f.t; s = f.n; t = f.s;
+        }
+        for (int k = 0; k < 2; ++k) {
+            const float sign = k == 0 ? 1.0f : -1.0f;
+            const V3 origin = is.point + s * d.x + t * d.y + axis * (sign * radius);
+            const V3 rdir = axis * -sign;
+            const Hit h = traceClosest<false>(S, origin, rdir, VIS_ALL, 0.0f, 2.0f * radius, n0, n1);
+            if (h.prim < 0) continue;
+            Isect hit;
+            fillHit(S, h, rdir, hit);
+            if (hit.shape != is.shape) continue;
+            if (len2(hit.point - is.point) > 2.25f * radius * radius) continue;
+            const V3 outward = hit.frontFace ? hit.normal : -hit.normal;
+            sum += outward * fabsf(dot(outward, axis));
+        }
+    }
+    V3 n = normalize(sum);
+    const V3 outwardN = is.frontFace ? N : -N;
+    if (dot(n, outwardN) < 0.0f) n = -n;
+    return is.frontFace ? n : -n;
+}
+
+// Shadow catcher (path_tracer.cpp:515-563): a camera ray that hits the catcher sees the
+// background `bg` times the share `ratio` of the direct light, over 4 × shadowSamples NEE
+// samples, that reaches the hit point.
+__device__ __noinline__ V3 shadowCatcher(const SceneGPU& S, const Isect& is, V3 dir, int shadowSamples, Sobol& sb,
+                                         float& ratioOut) {
+    const TablesGPU* T = S.tables;
+    V3 bg = mk(0.0f);
+    if (S.bgMode == PE_BG_COLOR) bg = m3f(S.bgColor);
+    else if (S.bgMode == PE_BG_ENVIRONMENT && S.env.present) bg = envEval(S.env, dir);
+    float visible = 0.0f, total = 0.0f;
+    if (S.lightCount > 0) {
+        LightCtx picker;
+        lightPrepare(S, is.point, is.normal, picker);
+        const int n = 4 * shadowSamples;
+        uint32_t n0 = 0, n1 = 0;
+        for (int k = 0; k < n; ++k) {
+            float pmf = 0.0f;
+            const int li = lightCtxSample(S, picker, get1D(sb), pmf);
+            if (li < 0 || !(pmf > 0.0f)) {
+                (void)get2D(T, sb);
+                continue;
+            }
+            const V2 u = get2D(T, sb);
+            const LightSample ls = li < S.nLights ? sampleLight(S.lights[li], is.point, u) : envSampleFull(S.env, S.envFull, u);
+            const float cosT = dot(ls.wi, is.normal);
+            if (!lsValid(ls) || cosT <= 0.0f) continue;
+            const float c = luminance(ls.Li) * cosT / (pmf * ls.pdf);
+            if (!(c > 0.0f) || !pe::finitef(c)) continue;
+            total += c;
+            V3 so, sd;
+            float stMax;
+            if (makeShadowRay(is, ls.wi, ls.distance, so, sd, stMax))
+                visible += c * luminance(shadowVisibility<false>(S, so, sd, stMax, n0, n1));
+        }
+    }
+    ratioOut = total > 0.0f ? sclamp(visible / total, 0.0f, 1.0f) : 1.0f;
+    return bg;
+}
+
 // ---- shade: Li's loop body between two closest-hit queries ------------------------------------
 // One path's step: reads the slot's state and hit record, adds the radiance found to L and
 // writes back the state for its next closest-hit query.  A path is in one of three states at
@@ -500,6 +599,7 @@ __device__ __forceinline__ bool shadeSlot(const SceneGPU& S, const Paths& P, con
     Isect is;
     bool done = false;
     bool vertex = false; // a surface vertex to shade (NEE + BSDF sampling) below
+    bool exitVertex = false; // ... the exit vertex of a subsurface walk
     V3 wo = -dir;
     if (flags & PF_WALK) {
         // one step of the random walk (path_tracer.cpp:263-303)
@@ -527,6 +627,7 @@ __device__ __forceinline__ bool shadeSlot(const SceneGPU& S, const Paths& P, con
                 is.material = S.exitMaterial;
                 flags &= ~PF_WALK;
                 wo = is.normal;
+                exitVertex = true;
                 if (depth >= A.maxDepth) done = true;
                 else vertex = true;
             }
@@ -607,6 +708,12 @@ __device__ __forceinline__ bool shadeSlot(const SceneGPU& S, const Paths& P, con
                     addL(L, c);
                 }
                 done = true;
+            } else if (cameraRay && is.shape == S.catcherShape) {
+                // the shadow catcher ends the camera path with the shadowed background
+                float ratio = 1.0f;
+                const V3 bg = shadowCatcher(S, is, dir, shadowSamples, sb, ratio);
+                addL(L, thr * bg * ratio);
+                done = true;
             } else {
                 const MatGPU& mat = S.materials[is.material];
                 // emission with MIS against the previous vertex's NEE (path_tracer.cpp:565-593)
@@ -650,6 +757,13 @@ __device__ __forceinline__ bool shadeSlot(const SceneGPU& S, const Paths& P, con
             lambda = sampleWavelength(T, get1D(sb), w);
             thr *= w;
         }
+        // rounded edges on the first three vertices (not a walk's exit vertex), then contact AO at
+        // the camera hit (path_tracer.cpp:612-621)
+        if (depth <= 2 && mat.roundEdge > 0.0f && !exitVertex) {
+            const V3 n = roundedEdgeNormal(S, is, mat.roundEdge, sb);
+            if (dot(n, wo) > 0.02f) is.normal = n;
+        }
+        if (A.aoStrength > 0.0f && depth == 0) thr *= approxAo(S, is, sb, A.aoStrength, shadowSamples);
         ShadePoint sp;
         sp.p = is.point;
         sp.n = is.normal;

@@ -332,6 +332,28 @@ PE_HDN LightSample envSample(const EnvGPU& e, V2 s) {
     if (e.sunPdfWeight > 0.0f && img.pdf > 0.0f) img.pdf = envPdf(e, img.wi);
     return img;
 }
+
+// EnvironmentLight::sampleLiFull (environment_light.cpp:239-252): the sun cone as sampleLi, the
+// rest from the uncompensated image distribution (`full`: the same light with that
+// distribution's tables), its pdf then the full mixture's (pdfLiFull, :254-260).
+PE_HDN LightSample envSampleFull(const EnvGPU& e, const EnvGPU& full, V2 sample) {
+    if (e.sunPdfWeight > 0.0f && sample.x < e.sunPdfWeight) return envSample(e, sample);
+    V2 s = sample;
+    if (e.sunPdfWeight > 0.0f) {
+        if (e.sunPdfWeight >= 1.0f) {
+            LightSample none;
+            none.wi = mk(0.0f);
+            none.Li = mk(0.0f);
+            none.pdf = 0.0f;
+            none.distance = kFltMax;
+            return none;
+        }
+        s.x = smin((sample.x - e.sunPdfWeight) / (1.0f - e.sunPdfWeight), 0.99999994f);
+    }
+    LightSample ls = envSampleImage(full, s);
+    if (e.sunPdfWeight > 0.0f && ls.pdf > 0.0f) ls.pdf = envPdf(full, ls.wi);
+    return ls;
+}
 PE_HD float envImportance(const EnvGPU& e, V3 n) {
     float imp = kPi * e.meanLuminance;
     if (e.sunPdfWeight > 0.0f)

@@ -71,7 +71,8 @@ struct MatGPU {
     float mediumG;
     int32_t thinWalled;
     float filmThickness;
-    float pad[8];
+    float roundEdge;          // Material::roundEdgeRadius (0 = off)
+    float pad[7];
 };
 
 enum MatFlags : int32_t {
@@ -176,6 +177,7 @@ struct SceneGPU {
     const unsigned long long* trail; // per candidate
     const uint8_t* trailDepth;       // per candidate
     EnvGPU env;
+    EnvGPU envFull;          // the same light with its uncompensated distribution (shadow catcher)
     const TablesGPU* tables;
     int32_t bgMode;
     float bgColor[3];
@@ -183,6 +185,7 @@ struct SceneGPU {
     int32_t hasVolumes;      // some material is a volume boundary: paths carry a medium stack
     int32_t hasSubsurface;   // some Disney material has a subsurface lobe (random walks)
     int32_t exitMaterial;    // white Lambert of the subsurface exit vertex
+    int32_t catcherShape;    // Scene::setShadowCatcher's shape, -1 none
 };
 
 } // namespace pe

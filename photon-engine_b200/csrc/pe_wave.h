@@ -125,7 +125,7 @@ struct WaveSeg {
     int slotFirst;
     int pixFirst;
     int flags;              // SegFlags
-    int pad;
+    float aoStrength;       // RenderSettings::aoStrength (contact AO at camera hits)
 };
 enum SegFlags { SEG_SWEEP = 1 }; // paths of the segment may leave a continuous wave for a sweep
 

@@ -59,6 +59,11 @@ class Material:
     def emitted(self):
         return tuple(self._m.emission)
 
+    def set_round_edge_radius(self, r):
+        """Material::setRoundEdgeRadius: shading normals blend with the neighbouring faces within
+        this distance of an edge (first three vertices of a path)."""
+        self._m.round_edge_radius = max(0.0, float(r))
+
 
 class Lambertian(Material):
     kind = capi.PE_MAT_LAMBERT
@@ -210,6 +215,7 @@ class Scene:
         self._materials: list[Material] = []
         self._mat_index: dict[int, int] = {}
         self.info: Optional[capi.pe_scene_info] = None
+        self.shadow_catcher: Optional[int] = None
 
     def __del__(self):
         try:
@@ -228,6 +234,15 @@ class Scene:
 
     def set_environment(self, env: Optional[EnvironmentLight]):
         self.environment = env
+
+    def shape_count(self) -> int:
+        """Shapes added so far: one per mesh, two per area light (its two triangles)."""
+        return sum(1 if kind == "mesh" else 2 for kind, _ in self.ops)
+
+    def set_shadow_catcher(self, shape: Optional[int]):
+        """Scene::setShadowCatcher: camera rays see this shape (an index as counted by
+        shape_count at the time it was added) as the background darkened by its shadows."""
+        self.shadow_catcher = shape
 
     def set_background(self, bg: Background):
         self.background = bg
@@ -263,6 +278,8 @@ class Scene:
             else:
                 capi.check(lib.pe_scene_add_area_light(h, capi.f3(obj.position), capi.f3(obj.u), capi.f3(obj.v),
                                                        capi.f3(obj.radiance), 1 if obj.visible_to_camera else 0))
+        if self.shadow_catcher is not None:
+            capi.check(lib.pe_scene_set_shadow_catcher(h, int(self.shadow_catcher)))
         env = self.environment
         if env is not None:
             img = env.image
@@ -324,10 +341,12 @@ class RenderSettings:
     seed: int = 12345            # Renderer::renderSamples uses a fixed Sobol seed of 12345
     rr_depth: int = 3            # PathTracer(maxBounces, 3, ...) in renderSamples
     path_guiding: bool = False
+    ao_strength: float = 0.0     # RenderSettings::aoStrength: contact AO at camera hits
 
     def to_c(self) -> capi.pe_settings:
         return capi.pe_settings(self.width, self.height, self.max_bounces, self.rr_depth, self.shadow_quality,
-                                int(self.filter_type), self.filter_width, self.clamp_indirect, self.seed)
+                                int(self.filter_type), self.filter_width, self.clamp_indirect, self.seed,
+                                float(self.ao_strength), 0)
 
 
 class Film:

@@ -110,6 +110,8 @@ typedef struct pe_camera {
     float forward[3];
     float lens_radius;
     int32_t orthographic;
+    int32_t blades;         /* thin lens: aperture polygon sides (0 = round disk) */
+    float blade_rotation;   /* thin lens: polygon rotation, radians */
 } pe_camera;
 
 enum { PE_FILTER_BOX = 0, PE_FILTER_TRIANGLE = 1, PE_FILTER_GAUSSIAN = 2, PE_FILTER_BLACKMAN_HARRIS = 3 };
@@ -178,6 +180,16 @@ int32_t pe_scene_get_info(const pe_scene* s, pe_scene_info* out);
  * (src/camera/perspective_camera.cpp:12-32). */
 void pe_camera_perspective(const float position[3], const float target[3], const float up[3], float vfov_deg,
                            float aspect, pe_camera* out);
+/* ThinLensCamera (src/camera/thin_lens_camera.cpp:14-33, setApertureShape :31-34): depth of field
+ * with an aperture of `aperture_radius` focused at `focus_distance`; blades >= 3 makes the
+ * aperture a regular polygon rotated by rotation_deg. */
+void pe_camera_thin_lens(const float position[3], const float target[3], const float up[3], float vfov_deg,
+                         float aspect, float aperture_radius, float focus_distance, int32_t blades, float rotation_deg,
+                         pe_camera* out);
+/* OrthographicCamera (src/camera/orthographic_camera.cpp:11-41): parallel rays over a
+ * vertical_extent-high image plane through `position`. */
+void pe_camera_orthographic(const float position[3], const float target[3], const float up[3],
+                            float vertical_extent, float aspect, pe_camera* out);
 
 /* ---- device ---------------------------------------------------------------- */
 typedef struct pe_device pe_device;

@@ -68,6 +68,11 @@ def _load(fast: bool = False):
         "ref_env_eval": (C.c_int32, [P, FP, C.c_size_t, FP, FP]),
         "ref_render_guided": (C.c_int32, [P, C.c_void_p, C.c_void_p, C.c_int32, C.c_int32, C.c_int32, FP, UP]),
         "ref_scene_set_shadow_catcher": (C.c_int32, [P, C.c_int32]),
+        "ref_camera_create": (P, [C.c_int32, FP]),
+        "ref_camera_destroy": (None, [P]),
+        "ref_camera_describe": (None, [P, C.c_void_p]),
+        "ref_render_rows_camera": (C.c_int32, [P, P, C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.c_int32,
+                                               C.c_int32, FP, UP]),
         "ref_dtree_probe": (C.c_int32, [FP, FP, C.c_int32, FP, FP, C.c_int32, FP, FP, C.c_int32, FP, FP]),
     }
     for name, (res, args) in sig.items():
@@ -137,10 +142,20 @@ class RefScene:
 
     def render(self, camera, settings, first: int, count: int, threads: int = 0, seeded: bool = True):
         """Mean image (h, w, 3) and counts of samples [first, first+count).  ``seeded`` runs the
-        tracePixel loop with settings.seed; otherwise Renderer::renderSamples (seed 12345)."""
+        tracePixel loop with settings.seed; otherwise Renderer::renderSamples (seed 12345).  A
+        thin-lens or orthographic camera renders through the reference's own camera class."""
         h, w = settings.height, settings.width
         mean = np.zeros((h, w, 3), np.float32)
         cnt = np.zeros((h, w), np.uint32)
+        kind = camera.reference_params()[0] if hasattr(camera, "reference_params") else 0
+        if kind != 0 and seeded:
+            cam = reference_camera(camera, self.lib)
+            try:
+                self.lib.ref_render_rows_camera(self.h, cam, C.byref(settings.to_c()), first, count, threads, 0, h,
+                                                _f(mean), cnt.ctypes.data_as(UP))
+            finally:
+                self.lib.ref_camera_destroy(cam)
+            return mean, cnt
         fn = self.lib.ref_render_seeded if seeded else self.lib.ref_render
         fn(self.h, C.byref(camera.describe_gpu()), C.byref(settings.to_c()), first, count, threads, _f(mean),
            cnt.ctypes.data_as(UP))
@@ -329,3 +344,24 @@ def dtree_probe(dirs1, rad1, dirs2, rad2, qdirs, qu, fast: bool = False):
     lib.ref_dtree_probe(_f(a[0]), _f(a[1]), len(a[1]), _f(a[2]), _f(a[3]), len(a[3]), _f(a[4]), _f(a[5]), nq,
                         _f(pdf), _f(smp))
     return pdf, smp
+
+
+def reference_camera(camera, lib=None):
+    """The reference's own camera object equal to a product camera (caller destroys it)."""
+    lib = lib or _load()
+    kind, params = camera.reference_params()
+    p = np.asarray(params, np.float32)
+    return lib.ref_camera_create(int(kind), _f(p))
+
+
+def describe_reference_camera(camera):
+    """Camera::describeGpu of the reference's own camera class, as a pe_camera."""
+    lib = _load()
+    cam = reference_camera(camera, lib)
+    out = type(camera.describe_gpu())()
+    try:
+        lib.ref_camera_describe(cam, C.byref(out))
+    finally:
+        lib.ref_camera_destroy(cam)
+    return out
+

@@ -18,7 +18,9 @@
 #include "photon_cuda.h"
 
 #include "camera/camera.h"
+#include "camera/orthographic_camera.h"
 #include "camera/perspective_camera.h"
+#include "camera/thin_lens_camera.h"
 #include "core/image/film.h"
 #include "core/image/image.h"
 #include "core/image/pixel_filter.h"
@@ -359,10 +361,57 @@ int32_t ref_render_seeded(void* s, const pe_camera* cam, const pe_settings* st, 
     return ref_render_rows(s, cam, st, first, count, threads, 0, st->height, mean_rgb, counts);
 }
 
+static int32_t renderRowsWith(RefScene* rs, const Camera& camera, const pe_settings* st, int32_t first, int32_t count,
+                              int32_t threads, int32_t y0, int32_t y1, float* mean_rgb, uint32_t* counts);
+
 int32_t ref_render_rows(void* s, const pe_camera* cam, const pe_settings* st, int32_t first, int32_t count,
                         int32_t threads, int32_t y0, int32_t y1, float* mean_rgb, uint32_t* counts) {
-    auto* rs = static_cast<RefScene*>(s);
     DescCamera camera(*cam);
+    return renderRowsWith(static_cast<RefScene*>(s), camera, st, first, count, threads, y0, y1, mean_rgb, counts);
+}
+
+// The reference's own cameras: kind 0 PerspectiveCamera(position, target, up, vfov, aspect),
+// 1 ThinLensCamera(..., aperture, focus) + setApertureShape(blades, rotation degrees),
+// 2 OrthographicCamera(position, target, up, vertical extent, aspect).
+void* ref_camera_create(int32_t kind, const float* p) {
+    const Vec3f pos = v3(p), tgt = v3(p + 3), up = v3(p + 6);
+    if (kind == 0) return new PerspectiveCamera(pos, tgt, up, p[9], p[10]);
+    if (kind == 1) {
+        auto* c = new ThinLensCamera(pos, tgt, up, p[9], p[10], p[11], p[12]);
+        c->setApertureShape(static_cast<int>(p[13]), p[14]);
+        return c;
+    }
+    if (kind == 2) return new OrthographicCamera(pos, tgt, up, p[9], p[10]);
+    return nullptr;
+}
+
+void ref_camera_destroy(void* c) { delete static_cast<Camera*>(c); }
+
+void ref_camera_describe(void* c, pe_camera* out) {
+    const CameraGpuDesc d = static_cast<Camera*>(c)->describeGpu();
+    auto put = [](float* o, const Vec3f& a) { o[0] = a.x; o[1] = a.y; o[2] = a.z; };
+    put(out->position, d.position);
+    put(out->lower_left, d.lowerLeft);
+    put(out->horizontal, d.horizontal);
+    put(out->vertical, d.vertical);
+    put(out->u, d.u);
+    put(out->v, d.v);
+    put(out->forward, d.forward);
+    out->lens_radius = d.lensRadius;
+    out->orthographic = d.orthographic ? 1 : 0;
+    out->blades = d.blades;
+    out->blade_rotation = d.bladeRotation;
+}
+
+// ref_render_rows with one of the reference's own camera objects.
+int32_t ref_render_rows_camera(void* s, void* cam, const pe_settings* st, int32_t first, int32_t count, int32_t threads,
+                               int32_t y0, int32_t y1, float* mean_rgb, uint32_t* counts) {
+    return renderRowsWith(static_cast<RefScene*>(s), *static_cast<Camera*>(cam), st, first, count, threads, y0, y1,
+                          mean_rgb, counts);
+}
+
+static int32_t renderRowsWith(RefScene* rs, const Camera& camera, const pe_settings* st, int32_t first, int32_t count,
+                              int32_t threads, int32_t y0, int32_t y1, float* mean_rgb, uint32_t* counts) {
     const int w = st->width, h = st->height;
     Film film(w, h);
     PathTracer integrator(st->max_bounces, st->rr_depth, st->ao_strength, st->shadow_quality);

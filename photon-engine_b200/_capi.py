@@ -45,7 +45,7 @@ class pe_material(C.Structure):
 
 class pe_camera(C.Structure):
     _fields_ = [("position", F3), ("lower_left", F3), ("horizontal", F3), ("vertical", F3),
-                ("u", F3), ("v", F3), ("forward", F3), ("lens_radius", C.c_float), ("orthographic", C.c_int32)]
+                ("u", F3), ("v", F3), ("forward", F3), ("lens_radius", C.c_float), ("orthographic", C.c_int32), ("blades", C.c_int32), ("blade_rotation", C.c_float)]
 
 
 class pe_settings(C.Structure):
@@ -142,6 +142,9 @@ SIGNATURES = {
     "pe_scene_build": (C.c_int32, [P]),
     "pe_scene_get_info": (C.c_int32, [P, C.POINTER(pe_scene_info)]),
     "pe_camera_perspective": (None, [FP, FP, FP, C.c_float, C.c_float, C.POINTER(pe_camera)]),
+    "pe_camera_thin_lens": (None, [FP, FP, FP, C.c_float, C.c_float, C.c_float, C.c_float, C.c_int32, C.c_float,
+                                   C.POINTER(pe_camera)]),
+    "pe_camera_orthographic": (None, [FP, FP, FP, C.c_float, C.c_float, C.POINTER(pe_camera)]),
     "pe_device_count": (C.c_int32, []),
     "pe_device_create": (P, [C.c_int32, C.c_char_p, C.c_size_t]),
     "pe_device_destroy": (None, [P]),

@@ -117,9 +117,9 @@ int32_t checkSettings(const pe_camera* cam, const pe_settings* st) {
         setError("shadow_quality other than 1 is not supported by this device");
         return PE_ERR_LIMIT;
     }
-    if (cam->orthographic || cam->lens_radius > 0.0f) {
-        setError("only the pinhole perspective camera is supported");
-        return PE_ERR_LIMIT;
+    if (!(cam->lens_radius >= 0.0f) || cam->blades < 0 || cam->blades > 64) {
+        setError("camera lens radius must be >= 0 and blades in 0..64");
+        return PE_ERR_INVALID;
     }
     if (!(st->ao_strength >= 0.0f) || !(st->ao_strength <= 1e30f)) {
         setError("ao_strength must be finite and >= 0");
@@ -135,6 +135,13 @@ WaveSeg makeSeg(const pe_camera* cam, const pe_settings* st) {
     A.cam.lowerLeft = m3f(cam->lower_left);
     A.cam.horizontal = m3f(cam->horizontal);
     A.cam.vertical = m3f(cam->vertical);
+    A.cam.u = m3f(cam->u);
+    A.cam.v = m3f(cam->v);
+    A.cam.forward = m3f(cam->forward);
+    A.cam.lensRadius = cam->orthographic ? 0.0f : (cam->lens_radius > 0.0f ? cam->lens_radius : 0.0f);
+    A.cam.blades = cam->blades >= 3 ? cam->blades : 0;
+    A.cam.bladeRotation = cam->blade_rotation;
+    A.cam.orthographic = cam->orthographic ? 1 : 0;
     A.width = st->width;
     A.height = st->height;
     A.seed = st->seed;

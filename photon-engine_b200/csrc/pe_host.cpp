@@ -1284,6 +1284,63 @@ void pe_camera_perspective(const float position[3], const float target[3], const
     put(out->forward, -w);
     out->lens_radius = 0.0f;
     out->orthographic = 0;
+    out->blades = 0;
+    out->blade_rotation = 0.0f;
+}
+
+void pe_camera_thin_lens(const float position[3], const float target[3], const float up[3], float vfov, float aspect,
+                         float aperture, float focus, int32_t blades, float rotationDeg, pe_camera* out) {
+    if (!out) return;
+    const V3 pos = m3f(position), tgt = m3f(target), upv = m3f(up);
+    // the pinhole's frame with the image plane at the focus distance (thin_lens_camera.cpp:14-33)
+    const float theta = vfov * (kPi / 180.0f);
+    const float h = std::tan(theta * 0.5f);
+    const float vh = 2.0f * h * focus;
+    const float vw = aspect * vh;
+    const V3 w = normalize(pos - tgt);
+    const V3 u = normalize(cross(upv, w));
+    const V3 v = cross(w, u);
+    const V3 horizontal = vw * u;
+    const V3 vertical = vh * v;
+    const V3 lowerLeft = pos - horizontal * 0.5f - vertical * 0.5f - focus * w;
+    auto put = [](float* o, V3 a) { o[0] = a.x; o[1] = a.y; o[2] = a.z; };
+    put(out->position, pos);
+    put(out->lower_left, lowerLeft);
+    put(out->horizontal, horizontal);
+    put(out->vertical, vertical);
+    put(out->u, u);
+    put(out->v, v);
+    put(out->forward, -w);
+    out->lens_radius = aperture;
+    out->orthographic = 0;
+    out->blades = blades >= 3 ? blades : 0;
+    out->blade_rotation = rotationDeg * 0.017453292519943295f;
+}
+
+void pe_camera_orthographic(const float position[3], const float target[3], const float up[3], float extent,
+                            float aspect, pe_camera* out) {
+    if (!out) return;
+    const V3 pos = m3f(position), tgt = m3f(target), upv = m3f(up);
+    const V3 w = normalize(pos - tgt);
+    const V3 u = normalize(cross(upv, w));
+    const V3 v = cross(w, u);
+    const float height = extent > 1e-4f ? extent : 1.0f;
+    const float width = aspect * height;
+    const V3 horizontal = width * u;
+    const V3 vertical = height * v;
+    const V3 lowerLeft = pos - horizontal * 0.5f - vertical * 0.5f;
+    auto put = [](float* o, V3 a) { o[0] = a.x; o[1] = a.y; o[2] = a.z; };
+    put(out->position, lowerLeft + horizontal * 0.5f + vertical * 0.5f);
+    put(out->lower_left, lowerLeft);
+    put(out->horizontal, horizontal);
+    put(out->vertical, vertical);
+    put(out->u, len2(horizontal) > 0.0f ? normalize(horizontal) : mk(1.0f, 0.0f, 0.0f));
+    put(out->v, len2(vertical) > 0.0f ? normalize(vertical) : mk(0.0f, 1.0f, 0.0f));
+    put(out->forward, -w);
+    out->lens_radius = 0.0f;
+    out->orthographic = 1;
+    out->blades = 0;
+    out->blade_rotation = 0.0f;
 }
 
 } // extern "C"

@@ -66,10 +66,36 @@ __device__ __forceinline__ void cameraRay(const TablesGPU* T, const float* filte
     const float oy = filterSample1D(filterCdf, filterWidth, u.y);
     const float sx = (static_cast<float>(x) + 0.5f + ox) / static_cast<float>(w);
     const float sy = 1.0f - (static_cast<float>(y) + 0.5f + oy) / static_cast<float>(h);
-    (void)get2D(T, s); // lens sample (consumed even by a pinhole camera)
+    const V2 lens = get2D(T, s); // lens sample (consumed by every camera)
     const V3 target = c.lowerLeft + sx * c.horizontal + sy * c.vertical;
-    o = c.position;
-    d = normalize(target - c.position);
+    if (c.orthographic) {
+        // OrthographicCamera::generateRay (orthographic_camera.cpp:24-27)
+        o = target;
+        d = c.forward;
+    } else if (c.lensRadius > 0.0f) {
+        // ThinLensCamera::generateRay (thin_lens_camera.cpp:51-64): the focus-plane point seen
+        // from a point of the aperture (disk, or polygon of `blades` sides, :37-49)
+        V2 l;
+        if (c.blades >= 3) {
+            const float n = static_cast<float>(c.blades);
+            const float scaled = smin(lens.x * n, n - 1e-4f);
+            const float k = floorf(scaled);
+            const float ux = scaled - k;
+            const float a0 = c.bladeRotation + kTwoPi * k / n;
+            const float a1 = a0 + kTwoPi / n;
+            const float su0 = sqrtf(ux);
+            const float bx = 1.0f - su0, by = lens.y * su0; // uniformSampleTriangle
+            l = mk2(cosf(a0) * bx + cosf(a1) * by, sinf(a0) * bx + sinf(a1) * by);
+        } else {
+            l = sampleDiskConcentric(lens);
+        }
+        const V2 lp = mk2(l.x * c.lensRadius, l.y * c.lensRadius);
+        o = c.position + c.u * lp.x + c.v * lp.y;
+        d = normalize(target - o);
+    } else {
+        o = c.position;
+        d = normalize(target - c.position);
+    }
 }
 
 // ---- BVH traversal -------------------------------------------------------------------------

@@ -14,6 +14,11 @@ namespace pe {
 // Pinhole camera as PerspectiveCamera stores it (perspective_camera.cpp:36-40).
 struct CamDev {
     V3 position, lowerLeft, horizontal, vertical;
+    V3 u, v, forward;       // lens plane axes and view direction
+    float lensRadius;       // > 0: thin lens
+    int blades;             // thin lens: polygon aperture sides (0 = disk)
+    float bladeRotation;    // radians
+    int orthographic;
 };
 
 enum VisMask : uint32_t { VIS_CAMERA = 1u, VIS_DIFFUSE = 2u, VIS_GLOSSY = 4u, VIS_TRANSMISSION = 8u, VIS_SHADOW = 16u,

@@ -317,6 +317,43 @@ class PerspectiveCamera:
     def describe_gpu(self) -> capi.pe_camera:
         return self._desc
 
+    def reference_params(self):
+        """(kind, parameters) of the same camera in the reference's own classes (test oracle)."""
+        return 0, [*self.position, *self.target, *self.up, self.vfov, self.aspect]
+
+
+class ThinLensCamera(PerspectiveCamera):
+    """ThinLensCamera: depth of field (aperture radius, focus distance), optionally a polygonal
+    aperture of `blades` sides rotated by `rotation_degrees` (setApertureShape)."""
+
+    def __init__(self, position, target, up, vfov_degrees: float, aspect: float, aperture_radius: float,
+                 focus_distance: float, blades: int = 0, rotation_degrees: float = 0.0):
+        self.position, self.target, self.up = position, target, up
+        self.vfov, self.aspect = float(vfov_degrees), float(aspect)
+        self.aperture, self.focus = float(aperture_radius), float(focus_distance)
+        self.blades, self.rotation = int(blades), float(rotation_degrees)
+        self._desc = capi.pe_camera()
+        _lib().pe_camera_thin_lens(capi.f3(position), capi.f3(target), capi.f3(up), self.vfov, self.aspect,
+                                   self.aperture, self.focus, self.blades, self.rotation, C.byref(self._desc))
+
+    def reference_params(self):
+        return 1, [*self.position, *self.target, *self.up, self.vfov, self.aspect, self.aperture, self.focus,
+                   float(self.blades), self.rotation]
+
+
+class OrthographicCamera(PerspectiveCamera):
+    """OrthographicCamera: parallel rays over a `vertical_extent`-high image plane."""
+
+    def __init__(self, position, target, up, vertical_extent: float, aspect: float):
+        self.position, self.target, self.up = position, target, up
+        self.extent, self.aspect = float(vertical_extent), float(aspect)
+        self._desc = capi.pe_camera()
+        _lib().pe_camera_orthographic(capi.f3(position), capi.f3(target), capi.f3(up), self.extent, self.aspect,
+                                      C.byref(self._desc))
+
+    def reference_params(self):
+        return 2, [*self.position, *self.target, *self.up, self.extent, self.aspect]
+
 
 class PixelFilterType(enum.IntEnum):
     Box = capi.PE_FILTER_BOX

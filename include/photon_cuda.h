@@ -155,6 +155,16 @@ int32_t pe_scene_add_material(pe_scene* s, const pe_material* m);
  * An emissive material registers one triangle light per triangle. */
 int32_t pe_scene_add_mesh(pe_scene* s, const float* positions, uint32_t n_vertices, const float* normals,
                           const float* uvs, const uint32_t* indices, uint32_t n_triangles, int32_t material);
+/* Scene::tagShape (scene.h:108): the scene-node uid of a shape (counted as for
+ * pe_scene_set_shadow_catcher), which light links name. */
+int32_t pe_scene_tag_shape(pe_scene* s, int32_t shape, uint64_t node_uid);
+/* Light::setLightLink (light.h:23-32, 80-81) of explicit light `light` (the scene's lights in the
+ * order they were registered: one per area light, one per triangle of an emissive mesh): mode 0
+ * all receivers, 1 only those whose node uid is listed, 2 all but those; shadow_mode likewise for
+ * the blockers that shadow this light (others are passed through).  At most 63 distinct uids over
+ * all links (PE_ERR_LIMIT at pe_scene_build otherwise). */
+int32_t pe_scene_set_light_link(pe_scene* s, int32_t light, int32_t mode, const uint64_t* uids, int32_t n,
+                                int32_t shadow_mode, const uint64_t* shadow_uids, int32_t n_shadow);
 /* Scene::setShadowCatcher (scene.h:90): the shape that camera rays see as the background darkened
  * by the shadows falling on it (path_tracer.cpp:515-563); -1 = none.  Shapes count from 0 in the
  * order they were added: one per pe_scene_add_mesh, two per pe_scene_add_area_light (its two

@@ -68,6 +68,9 @@ def _load(fast: bool = False):
         "ref_env_eval": (C.c_int32, [P, FP, C.c_size_t, FP, FP]),
         "ref_render_guided": (C.c_int32, [P, C.c_void_p, C.c_void_p, C.c_int32, C.c_int32, C.c_int32, FP, UP]),
         "ref_scene_set_shadow_catcher": (C.c_int32, [P, C.c_int32]),
+        "ref_scene_tag_shape": (C.c_int32, [P, C.c_int32, C.c_uint64]),
+        "ref_scene_set_light_link": (C.c_int32, [P, C.c_int32, C.c_int32, C.POINTER(C.c_uint64), C.c_int32,
+                                                 C.c_int32, C.POINTER(C.c_uint64), C.c_int32]),
         "ref_camera_create": (P, [C.c_int32, FP]),
         "ref_camera_destroy": (None, [P]),
         "ref_camera_describe": (None, [P, C.c_void_p]),
@@ -117,6 +120,15 @@ class RefScene:
                 raise RuntimeError("reference rejected a shape")
         if getattr(scene, "shadow_catcher", None) is not None:
             self.lib.ref_scene_set_shadow_catcher(self.h, int(scene.shadow_catcher))
+        for shape, uid in getattr(scene, "shape_tags", {}).items():
+            if self.lib.ref_scene_tag_shape(self.h, int(shape), int(uid)) != 0:
+                raise RuntimeError("reference rejected a shape tag")
+        for light, (mode, uids, smode, suids) in getattr(scene, "light_links", {}).items():
+            a = (C.c_uint64 * max(1, len(uids)))(*uids)
+            b = (C.c_uint64 * max(1, len(suids)))(*suids)
+            if self.lib.ref_scene_set_light_link(self.h, int(light), int(mode), a, len(uids), int(smode), b,
+                                                 len(suids)) != 0:
+                raise RuntimeError("reference rejected a light link")
         env = scene.environment
         if env is not None:
             img = env.image

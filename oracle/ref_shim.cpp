@@ -3,7 +3,8 @@
 // and bench.py's CPU-baseline leg load the library built from this file; the product never
 // does.  Each entry point drives the reference's public classes exactly as its own code does:
 //
-//   ref_scene_*      Scene::addShape / addLight / setEnvironment / setShadowCatcher / buildAccelerator
+//   ref_scene_*      Scene::addShape / addLight / setEnvironment / setShadowCatcher / tagShape,
+//                    Light::setLightLink, Scene::buildAccelerator
 //                    (src/engine/scene.cpp:18-185), own BVH forced (Scene::setPreferOwnBvh)
 //   ref_render       Renderer::renderSamples (src/engine/renderer.cpp:392-531); seed 12345
 //   ref_render_seeded  the same tile loop as renderSamples with a caller seed: tracePixel
@@ -218,6 +219,31 @@ int32_t ref_scene_add_mesh(void* s, const float* pos, uint32_t nv, const float* 
     auto mesh = std::make_shared<TriangleMesh>(p, n, t, ind, rs->materials[static_cast<size_t>(material)].get());
     rs->scene.addShape(mesh);
     rs->indexNewShapes();
+    return 0;
+}
+
+// Scene::tagShape of the shape added `shape`-th.
+int32_t ref_scene_tag_shape(void* s, int32_t shape, uint64_t uid) {
+    auto* rs = static_cast<RefScene*>(s);
+    const auto& shapes = rs->scene.shapes();
+    if (shape < 0 || shape >= static_cast<int32_t>(shapes.size())) return -1;
+    rs->scene.tagShape(shapes[static_cast<size_t>(shape)].get(), uid);
+    return 0;
+}
+
+// Light::setLightLink of the scene's `light`-th light.
+int32_t ref_scene_set_light_link(void* s, int32_t light, int32_t mode, const uint64_t* uids, int32_t n,
+                                 int32_t shadowMode, const uint64_t* shadowUids, int32_t nShadow) {
+    auto* rs = static_cast<RefScene*>(s);
+    const auto& lights = rs->scene.lights();
+    if (light < 0 || light >= static_cast<int32_t>(lights.size())) return -1;
+    LightLinkSet l;
+    l.mode = static_cast<LightLinkSet::Mode>(mode);
+    l.nodeUids.assign(uids, uids + n);
+    l.shadowMode = static_cast<LightLinkSet::Mode>(shadowMode);
+    l.shadowNodeUids.assign(shadowUids, shadowUids + nShadow);
+    // the Scene owns non-const lights; it hands them out as const
+    const_cast<Light*>(lights[static_cast<size_t>(light)])->setLightLink(std::move(l));
     return 0;
 }
 

@@ -130,6 +130,9 @@ SIGNATURES = {
     "pe_last_error": (C.c_char_p, []),
     "pe_abi_version": (C.c_int32, []),
     "pe_scene_set_shadow_catcher": (C.c_int32, [P, C.c_int32]),
+    "pe_scene_tag_shape": (C.c_int32, [P, C.c_int32, C.c_uint64]),
+    "pe_scene_set_light_link": (C.c_int32, [P, C.c_int32, C.c_int32, C.POINTER(C.c_uint64), C.c_int32, C.c_int32,
+                                            C.POINTER(C.c_uint64), C.c_int32]),
     "pe_material_defaults": (None, [C.c_int32, C.POINTER(pe_material)]),
     "pe_scene_create": (P, []),
     "pe_scene_destroy": (None, [P]),

@@ -790,6 +790,9 @@ int32_t uploadScene(pe_device* d, const pe_scene* s, SceneGPU& G, std::vector<De
     G.hasSubsurface = B.hasSubsurface ? 1 : 0;
     G.exitMaterial = B.exitMaterial;
     G.catcherShape = B.catcherShape;
+    G.hasLightLinks = B.hasLightLinks;
+    G.hasShadowLinks = B.hasShadowLinks;
+    if (!B.links.empty() && (rc = upload(d, bufs, G.links, B.links))) return rc;
     PE_CUDA(cudaStreamSynchronize(d->stream));
     return PE_OK;
 }

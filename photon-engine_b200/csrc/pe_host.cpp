@@ -802,6 +802,42 @@ static int32_t buildScene(pe_scene* s) {
     B.nrm.resize(nVerts);
     B.uv.resize(nVerts);
     B.shapes.resize(s->shapes.size());
+    // light links: number the node uids that links name (Scene::buildAccelerator, scene.cpp:121-141)
+    std::vector<uint64_t> linkUids;
+    auto linkIndex = [&](uint64_t uid) -> int {
+        for (size_t k = 0; k < linkUids.size(); ++k)
+            if (linkUids[k] == uid) return static_cast<int>(k);
+        return -1;
+    };
+    B.links.clear();
+    if (!s->lightLinks.empty()) {
+        B.links.assign(s->lights.size(), LightLinkGPU{0ull, 0ull, 0, 0});
+        for (size_t li = 0; li < s->lightLinks.size() && li < s->lights.size(); ++li) {
+            const HostLightLink& hl = s->lightLinks[li];
+            LightLinkGPU& g = B.links[li];
+            g.mode = hl.mode;
+            g.shadowMode = hl.shadowMode;
+            auto addAll = [&](const std::vector<uint64_t>& uids, unsigned long long& mask) -> bool {
+                for (uint64_t u : uids) {
+                    int k = linkIndex(u);
+                    if (k < 0) {
+                        if (linkUids.size() >= static_cast<size_t>(kLinkNodeOther)) return false;
+                        k = static_cast<int>(linkUids.size());
+                        linkUids.push_back(u);
+                    }
+                    mask |= 1ull << k;
+                }
+                return true;
+            };
+            if ((hl.mode != 0 && !addAll(hl.uids, g.mask)) || (hl.shadowMode != 0 && !addAll(hl.shadowUids, g.shadowMask))) {
+                setError("light links name more than 63 distinct node uids");
+                return PE_ERR_LIMIT;
+            }
+            if (hl.mode != 0) B.hasLightLinks = 1;
+            if (hl.shadowMode != 0) B.hasShadowLinks = 1;
+        }
+        if (!B.hasLightLinks && !B.hasShadowLinks) B.links.clear();
+    }
     std::vector<Box> triBounds(nTris);
     std::vector<uint8_t> triMask(nTris);
     uint32_t t0 = 0, v0 = 0;
@@ -812,6 +848,11 @@ static int32_t buildScene(pe_scene* s) {
         info.emitter = sh.emitter;
         info.flags = sh.flags;
         info.firstTri = t0;
+        {
+            const uint64_t uid = si < s->shapeUid.size() ? s->shapeUid[si] : 0ull;
+            const int k = linkIndex(uid);
+            info.linkNode = k >= 0 ? k : kLinkNodeOther;
+        }
         for (size_t v = 0; v < sh.pos.size(); ++v) {
             B.pos[v0 + v] = f4(sh.pos[v].x, sh.pos[v].y, sh.pos[v].z, 0.0f);
             const V3 n = v < sh.nrm.size() ? sh.nrm[v] : mk(0.0f);
@@ -1101,6 +1142,34 @@ int32_t pe_scene_add_mesh(pe_scene* s, const float* positions, uint32_t nv, cons
         }
     }
     s->shapes.push_back(std::move(sh));
+    s->built = false;
+    return PE_OK;
+}
+
+int32_t pe_scene_tag_shape(pe_scene* s, int32_t shape, uint64_t nodeUid) {
+    if (!s || shape < 0) {
+        setError("pe_scene_tag_shape: bad argument");
+        return PE_ERR_INVALID;
+    }
+    if (s->shapeUid.size() <= static_cast<size_t>(shape)) s->shapeUid.resize(static_cast<size_t>(shape) + 1, 0ull);
+    s->shapeUid[static_cast<size_t>(shape)] = nodeUid;
+    s->built = false;
+    return PE_OK;
+}
+
+int32_t pe_scene_set_light_link(pe_scene* s, int32_t light, int32_t mode, const uint64_t* uids, int32_t n,
+                                int32_t shadowMode, const uint64_t* shadowUids, int32_t nShadow) {
+    if (!s || light < 0 || mode < 0 || mode > 2 || shadowMode < 0 || shadowMode > 2 || n < 0 || nShadow < 0 ||
+        (n > 0 && !uids) || (nShadow > 0 && !shadowUids)) {
+        setError("pe_scene_set_light_link: bad argument");
+        return PE_ERR_INVALID;
+    }
+    if (s->lightLinks.size() <= static_cast<size_t>(light)) s->lightLinks.resize(static_cast<size_t>(light) + 1);
+    HostLightLink& l = s->lightLinks[static_cast<size_t>(light)];
+    l.mode = mode;
+    l.shadowMode = shadowMode;
+    l.uids.assign(uids, uids + n);
+    l.shadowUids.assign(shadowUids, shadowUids + nShadow);
     s->built = false;
     return PE_OK;
 }

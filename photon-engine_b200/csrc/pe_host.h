@@ -68,6 +68,13 @@ struct HostBuild {
     bool hasDispersion = false;
     int32_t exitMaterial = -1;   // white Lambert of the subsurface exit vertex
     int32_t catcherShape = -1;   // shadow-catcher shape
+    std::vector<LightLinkGPU> links; // per explicit light, empty without links
+    int32_t hasLightLinks = 0, hasShadowLinks = 0;
+};
+
+struct HostLightLink {
+    int32_t mode = 0, shadowMode = 0;
+    std::vector<uint64_t> uids, shadowUids;
 };
 
 } // namespace pe
@@ -82,6 +89,8 @@ struct pe_scene {
     float bgColor[3] = {0.18f, 0.18f, 0.18f};
     bool built = false;
     int32_t catcherShape = -1;   // Scene::setShadowCatcher
+    std::vector<uint64_t> shapeUid;            // Scene::tagShape (0 = untagged)
+    std::vector<pe::HostLightLink> lightLinks; // Light::setLightLink, by explicit light index
     pe::HostBuild build;
     uint64_t version = 0;
 };

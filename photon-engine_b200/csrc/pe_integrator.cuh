@@ -212,13 +212,21 @@ __device__ __forceinline__ V3 surfaceShadowTransmittance(const MatGPU& m, const 
     return mk(0.0f);
 }
 
-// shadowTransmittance (path_tracer.cpp:172-202).  Without shadow-transmitting materials in the
-// scene it is the any-hit test; otherwise the shadow ray walks from surface to surface (at most
-// 64) through thin-walled glass and cutouts, multiplying their transmittance, and stops black at
-// any other surface.
+// Scene::hasShadowLinkFor: light `light` (explicit, else -1) lets some blockers through.
+__device__ __forceinline__ bool shadowLinkFor(const SceneGPU& S, int light) {
+    return S.hasShadowLinks && light >= 0 && S.links[light].shadowMode != 0;
+}
+
+// shadowTransmittance (path_tracer.cpp:172-202).  Without shadow-transmitting materials or a
+// shadow link for the light it is the any-hit test; otherwise the shadow ray walks from surface
+// to surface (at most 64), passing the blockers the light's shadow link leaves out and
+// multiplying the transmittance of thin-walled glass and cutouts, and stops black at any other
+// surface.
 template <bool COUNT>
-__device__ V3 shadowVisibility(const SceneGPU& S, V3 o, V3 d, float tMax, uint32_t& nodes, uint32_t& tris) {
-    if (!S.hasShadowTransmitters) return traceAny<COUNT>(S, o, d, VIS_SHADOW, 0.0f, tMax, nodes, tris) ? mk(0.0f) : mk(1.0f);
+__device__ V3 shadowVisibility(const SceneGPU& S, V3 o, V3 d, float tMax, int light, uint32_t& nodes, uint32_t& tris) {
+    const bool link = shadowLinkFor(S, light);
+    if (!S.hasShadowTransmitters && !link)
+        return traceAny<COUNT>(S, o, d, VIS_SHADOW, 0.0f, tMax, nodes, tris) ? mk(0.0f) : mk(1.0f);
     V3 T = mk(1.0f);
     V3 origin = o;
     float remaining = tMax;
@@ -227,6 +235,12 @@ __device__ V3 shadowVisibility(const SceneGPU& S, V3 o, V3 d, float tMax, uint32
         if (h.prim < 0) return T;
         Isect is;
         fillHit(S, h, d, is);
+        if (link && !linkAllows(S.links[light].shadowMode, S.links[light].shadowMask, S.shapes[is.shape].linkNode)) {
+            origin = offsetRayOrigin(is.point, is.pError, len2(is.ng) > 0.0f ? is.ng : is.normal, d);
+            remaining -= h.t;
+            if (remaining <= 0.0f) return T;
+            continue;
+        }
         const MatGPU& m = S.materials[is.material];
         if (!(m.flags & MF_TRANSMITS_SHADOWS)) return mk(0.0f);
         T *= surfaceShadowTransmittance(m, is, d);
@@ -263,7 +277,8 @@ __global__ void __launch_bounds__(128) kShadow(SceneGPU S, Paths P, const uint32
         const int slot = P.shadowQ[i];
         const float4 so = P.shO[i];
         const float4 sd = P.shD[i];
-        const V3 vis = shadowVisibility<COUNT>(S, mk(so.x, so.y, so.z), mk(sd.x, sd.y, sd.z), so.w, nodes, tris);
+        const int light = static_cast<int>(__float_as_uint(P.shC[i].w) >> 1) - 1;
+        const V3 vis = shadowVisibility<COUNT>(S, mk(so.x, so.y, so.z), mk(sd.x, sd.y, sd.z), so.w, light, nodes, tris);
         if (isBlack(vis)) continue;
         const float4 sc = P.shC[i];
         const float4 st = P.shT[i];
@@ -517,6 +532,11 @@ __device__ __noinline__ V3 shadowCatcher(const SceneGPU& S, const Isect& is, V3 
                 (void)get2D(T, sb);
                 continue;
             }
+            if (li < S.nLights && S.hasLightLinks &&
+                !linkAllows(S.links[li].mode, S.links[li].mask, S.shapes[is.shape].linkNode)) {
+                (void)get2D(T, sb);
+                continue;
+            }
             const V2 u = get2D(T, sb);
             const LightSample ls = li < S.nLights ? sampleLight(S.lights[li], is.point, u) : envSampleFull(S.env, S.envFull, u);
             const float cosT = dot(ls.wi, is.normal);
@@ -527,7 +547,7 @@ __device__ __noinline__ V3 shadowCatcher(const SceneGPU& S, const Isect& is, V3 
             V3 so, sd;
             float stMax;
             if (makeShadowRay(is, ls.wi, ls.distance, so, sd, stMax))
-                visible += c * luminance(shadowVisibility<false>(S, so, sd, stMax, n0, n1));
+                visible += c * luminance(shadowVisibility<false>(S, so, sd, stMax, li < S.nLights ? li : -1, n0, n1));
         }
     }
     ratioOut = total > 0.0f ? sclamp(visible / total, 0.0f, 1.0f) : 1.0f;
@@ -722,8 +742,13 @@ __device__ __forceinline__ bool shadeSlot(const SceneGPU& S, const Paths& P, con
                     int li = -1;
                     if (sh.emitter >= 0)
                         li = (sh.flags & SF_AREA_TRIANGLE) ? sh.emitter : sh.emitter + (is.tri - static_cast<int>(sh.firstTri));
+                    // Light linking: the previous receiver must be linked to this light
+                    // (path_tracer.cpp:571-572; camera rays always see it)
+                    const bool linked = depth == 0 || li < 0 || !S.hasLightLinks ||
+                                        linkAllows(S.links[li].mode, S.links[li].mask,
+                                                   static_cast<int>((flags >> kPrevNodeShift) & 0xFFu));
                     float weight = 1.0f;
-                    if (!specularBounce) {
+                    if (linked && !specularBounce) {
                         float lightPdf = 0.0f;
                         if (li >= 0) {
                             float pmf = 0.0f;
@@ -737,12 +762,14 @@ __device__ __forceinline__ bool shadeSlot(const SceneGPU& S, const Paths& P, con
                         if (lightPdf > 0.0f && lastBsdfPdf > 0.0f)
                             weight = powerHeuristic(1, lastBsdfPdf, shadowSamples, lightPdf);
                     }
-                    V3 c = thr * (m3f(mat.emission) * weight);
-                    if (diffuseBounces >= 2 && A.clampIndirect > 0.0f) {
-                        const float m = smax3(c.x, c.y, c.z);
-                        if (m > A.clampIndirect) c = c * (A.clampIndirect / m);
+                    if (linked) {
+                        V3 c = thr * (m3f(mat.emission) * weight);
+                        if (diffuseBounces >= 2 && A.clampIndirect > 0.0f) {
+                            const float m = smax3(c.x, c.y, c.z);
+                            if (m > A.clampIndirect) c = c * (A.clampIndirect / m);
+                        }
+                        addL(L, c);
                     }
-                    addL(L, c);
                 }
                 if (depth >= A.maxDepth) done = true;
                 else vertex = true;
@@ -798,6 +825,11 @@ __device__ __forceinline__ bool shadeSlot(const SceneGPU& S, const Paths& P, con
                     continue;
                 }
                 const bool fromEnv = lightIndex >= explicitLights;
+                if (!fromEnv && S.hasLightLinks &&
+                    !linkAllows(S.links[lightIndex].mode, S.links[lightIndex].mask, S.shapes[is.shape].linkNode)) {
+                    (void)get2D(T, sb);
+                    continue;
+                }
                 const V2 ul = get2D(T, sb);
                 const LightSample ls = fromEnv ? envSample(S.env, ul) : sampleLight(S.lights[lightIndex], is.point, ul);
                 if (!lsValid(ls)) continue;
@@ -818,7 +850,7 @@ __device__ __forceinline__ bool shadeSlot(const SceneGPU& S, const Paths& P, con
                 if (INLINE_SHADOW) {
                     // the any-hit query now; its term follows this vertex's emission in L
                     ++shRays;
-                    const V3 vis = shadowVisibility<COUNT>(S, so, sd, stMax, shNodes, shTris);
+                    const V3 vis = shadowVisibility<COUNT>(S, so, sd, stMax, fromEnv ? -1 : lightIndex, shNodes, shTris);
                     if (!isBlack(vis)) {
                         const V3 c = neeTerm(fLi, vis, scalar, thr, diffuseBounces >= 1, A.clampIndirect);
                         if (isFinite3(c)) {
@@ -833,7 +865,9 @@ __device__ __forceinline__ bool shadeSlot(const SceneGPU& S, const Paths& P, con
                     P.shadowQ[pos] = slot;
                     P.shO[pos] = make_float4(so.x, so.y, so.z, stMax);
                     P.shD[pos] = make_float4(sd.x, sd.y, sd.z, scalar);
-                    P.shC[pos] = make_float4(fLi.x, fLi.y, fLi.z, __uint_as_float(diffuseBounces >= 1 ? 1u : 0u));
+                    // flags: bit 0 indirect, bits 1.. the light index + 1 (0: the environment)
+                    const uint32_t lightBits = static_cast<uint32_t>(fromEnv ? 0 : lightIndex + 1) << 1;
+                    P.shC[pos] = make_float4(fLi.x, fLi.y, fLi.z, __uint_as_float((diffuseBounces >= 1 ? 1u : 0u) | lightBits));
                     P.shT[pos] = make_float4(thr.x, thr.y, thr.z, A.clampIndirect);
                 }
             }
@@ -899,6 +933,8 @@ __device__ __forceinline__ bool shadeSlot(const SceneGPU& S, const Paths& P, con
                 done = true;
             } else {
                 flags = bs.delta ? (flags | PF_SPECULAR_BOUNCE) : (flags & ~PF_SPECULAR_BOUNCE);
+                // this vertex is the next emission hit's receiver (path_tracer.cpp:832)
+                flags = (flags & ~kPrevNodeMask) | (static_cast<uint32_t>(S.shapes[is.shape].linkNode) << kPrevNodeShift);
                 if (!bs.delta) ++diffuseBounces;
                 cameraRay = cameraRay && bs.delta && dot(wi, is.normal) < 0.0f;
                 flags = cameraRay ? (flags | PF_CAMERA_RAY) : (flags & ~PF_CAMERA_RAY);

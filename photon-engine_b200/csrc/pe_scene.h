@@ -44,6 +44,16 @@ struct ShapeInfo {
     int32_t emitter;      // light index of triangle 0 (emissive mesh) or of the area light; -1 none
     uint32_t flags;
     uint32_t firstTri;    // global index of the shape's first triangle
+    int32_t linkNode;     // bit of its node uid in the light-link masks; kLinkNodeOther if no link names it
+};
+
+// Light linking (Light::setLightLink, Scene::isLightLinked / isShadowLinked, scene.cpp:121-141,
+// 242-256): the node uids that light links name are numbered 0..62; a link is a mode (0 all,
+// 1 include, 2 exclude) and a 64-bit mask over those numbers, for lit receivers and for blockers.
+constexpr int kLinkNodeOther = 63;
+struct LightLinkGPU {
+    unsigned long long mask, shadowMask;
+    int32_t mode, shadowMode;
 };
 
 // Resolved material (pe_material + constants derived on the host).
@@ -186,6 +196,15 @@ struct SceneGPU {
     int32_t hasSubsurface;   // some Disney material has a subsurface lobe (random walks)
     int32_t exitMaterial;    // white Lambert of the subsurface exit vertex
     int32_t catcherShape;    // Scene::setShadowCatcher's shape, -1 none
+    const LightLinkGPU* links; // per explicit light (null without light links)
+    int32_t hasLightLinks, hasShadowLinks;
 };
+
+// Scene::isLightLinked / isShadowLinked for light `li` (explicit) and a receiver or blocker node.
+PE_HD bool linkAllows(int mode, unsigned long long mask, int node) {
+    if (mode == 0) return true;
+    const bool found = node < kLinkNodeOther && ((mask >> node) & 1ull) != 0ull;
+    return mode == 1 ? found : !found;
+}
 
 } // namespace pe

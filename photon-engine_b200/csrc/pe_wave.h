@@ -42,6 +42,9 @@ enum PathFlags : uint32_t {
     PF_WALK = 1u << 4,   // inside a random walk: lastP = σt, lastN = albedo, pickP.x = g
     PF_GUIDE_SNAP = 1u << 5, // the path's guide training record waits for its radiance snapshot
 };
+// Bits 24..31 of the flags word: the light-link node of the path's last surface vertex.
+constexpr uint32_t kPrevNodeShift = 24;
+constexpr uint32_t kPrevNodeMask = 0xFFu << kPrevNodeShift;
 
 // Per-slot state columns (capacity P slots).
 struct Paths {

@@ -216,6 +216,8 @@ class Scene:
         self._mat_index: dict[int, int] = {}
         self.info: Optional[capi.pe_scene_info] = None
         self.shadow_catcher: Optional[int] = None
+        self.shape_tags: dict[int, int] = {}
+        self.light_links: dict[int, tuple] = {}
 
     def __del__(self):
         try:
@@ -238,6 +240,17 @@ class Scene:
     def shape_count(self) -> int:
         """Shapes added so far: one per mesh, two per area light (its two triangles)."""
         return sum(1 if kind == "mesh" else 2 for kind, _ in self.ops)
+
+    def tag_shape(self, shape: int, node_uid: int):
+        """Scene::tagShape: the scene-node uid that light links name this shape by."""
+        self.shape_tags[int(shape)] = int(node_uid)
+
+    def set_light_link(self, light: int, mode: int = 0, uids=(), shadow_mode: int = 0, shadow_uids=()):
+        """Light::setLightLink of explicit light `light` (one per area light, one per triangle of an
+        emissive mesh, in the order they were added): mode / shadow_mode 0 all, 1 include the
+        listed node uids, 2 exclude them."""
+        self.light_links[int(light)] = (int(mode), [int(u) for u in uids], int(shadow_mode),
+                                        [int(u) for u in shadow_uids])
 
     def set_shadow_catcher(self, shape: Optional[int]):
         """Scene::setShadowCatcher: camera rays see this shape (an index as counted by
@@ -280,6 +293,12 @@ class Scene:
                                                        capi.f3(obj.radiance), 1 if obj.visible_to_camera else 0))
         if self.shadow_catcher is not None:
             capi.check(lib.pe_scene_set_shadow_catcher(h, int(self.shadow_catcher)))
+        for shape, uid in self.shape_tags.items():
+            capi.check(lib.pe_scene_tag_shape(h, shape, uid))
+        for light, (mode, uids, smode, suids) in self.light_links.items():
+            a = (C.c_uint64 * max(1, len(uids)))(*uids)
+            b = (C.c_uint64 * max(1, len(suids)))(*suids)
+            capi.check(lib.pe_scene_set_light_link(h, light, mode, a, len(uids), smode, b, len(suids)))
         env = self.environment
         if env is not None:
             img = env.image

@@ -256,6 +256,25 @@ int32_t pe_device_render(pe_device* d, const pe_camera* cam, const pe_settings* 
                          int32_t count, const volatile int32_t* cancel, float* sum_rgb, uint32_t* sample_count,
                          float* sum_lum_sq, uint64_t* samples_traced);
 
+/* AOV films (AovFilms, src/engine/renderer.h:42-53): the first visible surface's albedo, its
+ * normal, and coverage — each a Film's arrays (sum of RGB, sample count, sum of squared
+ * luminance), merged like the beauty film; a NULL array is skipped. */
+typedef struct pe_aov_films {
+    float* albedo_sum;
+    uint32_t* albedo_count;
+    float* albedo_sum_sq;
+    float* normal_sum;   /* signed (Film::addSampleSigned); no squares are kept */
+    uint32_t* normal_count;
+    float* alpha_sum;    /* coverage in all three channels */
+    uint32_t* alpha_count;
+    float* alpha_sum_sq;
+} pe_aov_films;
+/* pe_device_render plus the AOV films of the same samples (RenderDevice::render with
+ * RenderTargets::aovs; tracePixel with wantAovs, renderer.cpp:139-204). */
+int32_t pe_device_render_aovs(pe_device* d, const pe_camera* cam, const pe_settings* st, int32_t first_sample,
+                              int32_t count, const volatile int32_t* cancel, float* sum_rgb, uint32_t* sample_count,
+                              float* sum_lum_sq, const pe_aov_films* aovs, uint64_t* traced);
+
 /* Same, accumulating into the device-resident film (kept across calls until
  * pe_device_film_clear; resized/cleared when width/height change). */
 int32_t pe_device_render_resident(pe_device* d, const pe_camera* cam, const pe_settings* st, int32_t first_sample,

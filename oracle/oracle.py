@@ -68,6 +68,8 @@ def _load(fast: bool = False):
         "ref_env_eval": (C.c_int32, [P, FP, C.c_size_t, FP, FP]),
         "ref_render_guided": (C.c_int32, [P, C.c_void_p, C.c_void_p, C.c_int32, C.c_int32, C.c_int32, FP, UP]),
         "ref_scene_set_shadow_catcher": (C.c_int32, [P, C.c_int32]),
+        "ref_render_aovs": (C.c_int32, [P, C.c_void_p, C.c_void_p, C.c_int32, C.c_int32, C.c_int32, FP, UP, FP, FP,
+                                        FP, UP]),
         "ref_scene_tag_shape": (C.c_int32, [P, C.c_int32, C.c_uint64]),
         "ref_scene_set_light_link": (C.c_int32, [P, C.c_int32, C.c_int32, C.POINTER(C.c_uint64), C.c_int32,
                                                  C.c_int32, C.POINTER(C.c_uint64), C.c_int32]),
@@ -172,6 +174,18 @@ class RefScene:
         fn(self.h, C.byref(camera.describe_gpu()), C.byref(settings.to_c()), first, count, threads, _f(mean),
            cnt.ctypes.data_as(UP))
         return mean, cnt
+
+    def render_aovs(self, camera, settings, first: int, count: int, threads: int = 0):
+        """Renderer::renderSamples with AovFilms (seed 12345): mean beauty, albedo, normal, alpha
+        and the counts."""
+        h, w = settings.height, settings.width
+        out = [np.zeros((h, w, 3), np.float32) for _ in range(4)]
+        cnt = np.zeros((h, w), np.uint32)
+        acnt = np.zeros((h, w), np.uint32)
+        self.lib.ref_render_aovs(self.h, C.byref(camera.describe_gpu()), C.byref(settings.to_c()), first, count,
+                                 threads, _f(out[0]), cnt.ctypes.data_as(UP), _f(out[1]), _f(out[2]), _f(out[3]),
+                                 acnt.ctypes.data_as(UP))
+        return out[0], out[1], out[2], out[3], cnt, acnt
 
     def render_guided(self, camera, settings, first: int, count: int, threads: int = 0):
         """Renderer::renderSamples with SD-tree path guiding on (a fresh field, trained over the

@@ -341,6 +341,26 @@ int32_t ref_render(void* s, const pe_camera* cam, const pe_settings* st, int32_t
     return 0;
 }
 
+// Renderer::renderSamples with AovFilms (seed 12345): the mean beauty, albedo, normal and alpha
+// images and their counts.
+int32_t ref_render_aovs(void* s, const pe_camera* cam, const pe_settings* st, int32_t first, int32_t count,
+                        int32_t threads, float* mean_rgb, uint32_t* counts, float* albedo, float* normal, float* alpha,
+                        uint32_t* aov_counts) {
+    auto* rs = static_cast<RefScene*>(s);
+    DescCamera camera(*cam);
+    RenderSettings settings = toSettings(*st, threads > 0 ? threads : hardwareThreads());
+    Film film(st->width, st->height);
+    AovFilms aovs;
+    aovs.resize(st->width, st->height);
+    Renderer renderer;
+    renderer.renderSamples(rs->scene, camera, settings, film, first, count, nullptr, &aovs);
+    exportFilm(film, st->width, st->height, mean_rgb, counts);
+    exportFilm(aovs.albedo, st->width, st->height, albedo, aov_counts);
+    exportFilm(aovs.normal, st->width, st->height, normal, nullptr);
+    exportFilm(aovs.alpha, st->width, st->height, alpha, nullptr);
+    return 0;
+}
+
 int32_t ref_render_guided(void* s, const pe_camera* cam, const pe_settings* st, int32_t first, int32_t count,
                           int32_t threads, float* mean_rgb, uint32_t* counts) {
     auto* rs = static_cast<RefScene*>(s);

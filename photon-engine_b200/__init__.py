@@ -4,7 +4,7 @@ The product is ``libphoton_cuda.so`` (C ABI in ``include/photon_cuda.h``); this 
 host-side mirror of the reference's RenderDevice / RenderSession / Scene API over it.
 """
 from . import _capi
-from .engine import (AreaLight, Background, BackgroundMode, CudaDevice, Dielectric, DeviceFeatures, DeviceInfo,
+from .engine import (AovFilms, AreaLight, Background, BackgroundMode, CudaDevice, Dielectric, DeviceFeatures, DeviceInfo,
                      DisneyMaterial, EnvironmentLight, Film, Lambertian, Material, Mirror, OrthographicCamera, PerspectiveCamera, ThinLensCamera,
                      PixelFilterType, RenderMode, RenderServer, RenderSession, RenderSettings, RenderTargets, RequestStatus,
                      SampleBatchResult,

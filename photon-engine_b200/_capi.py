@@ -103,6 +103,13 @@ class pe_sdtree_info(C.Structure):
                 ("spatial_leaves", C.c_int32), ("quad_nodes", C.c_int64), ("energy", C.c_double)]
 
 
+class pe_aov_films(C.Structure):
+    _fields_ = [("albedo_sum", C.POINTER(C.c_float)), ("albedo_count", C.POINTER(C.c_uint32)),
+                ("albedo_sum_sq", C.POINTER(C.c_float)), ("normal_sum", C.POINTER(C.c_float)),
+                ("normal_count", C.POINTER(C.c_uint32)), ("alpha_sum", C.POINTER(C.c_float)),
+                ("alpha_count", C.POINTER(C.c_uint32)), ("alpha_sum_sq", C.POINTER(C.c_float))]
+
+
 class pe_request_desc(C.Structure):
     _fields_ = [("scene", C.c_int32), ("camera", pe_camera), ("settings", pe_settings), ("spp", C.c_int32),
                 ("priority", C.c_int32)]
@@ -130,6 +137,9 @@ SIGNATURES = {
     "pe_last_error": (C.c_char_p, []),
     "pe_abi_version": (C.c_int32, []),
     "pe_scene_set_shadow_catcher": (C.c_int32, [P, C.c_int32]),
+    "pe_device_render_aovs": (C.c_int32, [P, C.POINTER(pe_camera), C.POINTER(pe_settings), C.c_int32, C.c_int32,
+                                          C.c_void_p, FP, C.POINTER(C.c_uint32), FP, C.POINTER(pe_aov_films),
+                                          C.POINTER(C.c_uint64)]),
     "pe_scene_tag_shape": (C.c_int32, [P, C.c_int32, C.c_uint64]),
     "pe_scene_set_light_link": (C.c_int32, [P, C.c_int32, C.c_int32, C.POINTER(C.c_uint64), C.c_int32, C.c_int32,
                                             C.POINTER(C.c_uint64), C.c_int32]),

@@ -283,11 +283,13 @@ int32_t runWave(pe_device* d, int lane, Paths& P, int nSegs, int nSlots, int nPi
     P.sd = d->sd.field;
     // path regeneration: a wave of more paths than slots (unguided waves on a lane's own state)
     const int64_t slotCap = static_cast<int64_t>(P.capacity);
-    const bool regen = &P == &ln.paths && ln.Lout && !P.guiding && !P.sdMode && nSlots > slotCap;
+    const bool regen = &P == &ln.paths && ln.Lout && !P.guiding && !P.sdMode && !d->aovTarget && nSlots > slotCap;
     P.pathOf = regen ? ln.pathOf : nullptr;
     P.freeQ = regen ? ln.freeQ : nullptr;
     P.Lout = regen ? ln.Lout : nullptr;
     P.segLeft = nullptr;
+    P.aovA = (d->aovTarget && &P == &ln.paths) ? ln.aovA : nullptr;
+    P.aovN = (d->aovTarget && &P == &ln.paths) ? ln.aovN : nullptr;
     P.born = nullptr;
     P.sweepQ = nullptr;
     P.sweepAge = 0;
@@ -422,6 +424,8 @@ int32_t loopBegin(pe_device* d, LaneLoop& L, uint32_t* segLeft) {
     P.freeQ = ln.freeQ;
     P.Lout = ln.Lout;
     P.segLeft = segLeft;
+    P.aovA = nullptr;
+    P.aovN = nullptr;
     P.born = L.born;
     P.sweepQ = nullptr;
     P.sweepAge = 0;
@@ -566,7 +570,7 @@ int32_t renderWaves(pe_device* d, const pe_camera* cam, const pe_settings* st, i
                     bool timing, Tile tile) {
     const size_t npix = static_cast<size_t>(tile.w) * static_cast<size_t>(tile.h);
     // unguided waves on the lanes' own state regenerate paths: kStreamFactor × the slots per wave
-    const bool regenWaves = !scratch && !d->guide.mode && d->guideKind != 2;
+    const bool regenWaves = !scratch && !d->guide.mode && d->guideKind != 2 && !d->aovTarget;
     const size_t pathCap = regenWaves ? capacity * kStreamFactor : capacity;
     const int pixChunk = static_cast<int>(std::min(npix, pathCap));
     const int samplesPerWave = static_cast<int>(std::max<size_t>(1, std::min<size_t>(static_cast<size_t>(count), pathCap / pixChunk)));
@@ -585,6 +589,7 @@ int32_t renderWaves(pe_device* d, const pe_camera* cam, const pe_settings* st, i
     base.sum = sum;
     base.cnt = cnt;
     base.sq = sq;
+    base.aov = scratch ? nullptr : d->aovTarget;
     RenderTimer tm;
     tm.timing = timing;
     bool cancelled = false;
@@ -895,6 +900,7 @@ void pe_device_destroy(pe_device* d) {
     for (int l = 0; l < 2; ++l) {
         WaveLane& ln = d->lanes[l];
         freeList(ln.bufs);
+        freeList(ln.aovBufs);
         cudaFree(ln.dSegs);
         if (ln.hSegs) cudaFreeHost(ln.hSegs);
         if (ln.hCounters) cudaFreeHost(ln.hCounters);
@@ -903,6 +909,7 @@ void pe_device_destroy(pe_device* d) {
         if (l == 1 && ln.stream) cudaStreamDestroy(ln.stream);
     }
     if (d->evFilm) cudaEventDestroy(d->evFilm);
+    cudaFree(d->aovFilm);
     cudaFree(d->fSum);
     cudaFree(d->fCnt);
     cudaFree(d->fSq);
@@ -1011,6 +1018,64 @@ int32_t pe_device_film_read(pe_device* d, float* sum, uint32_t* cnt, float* sq) 
 
 // RenderDevice::render with host films: the batch is rendered into a zeroed device film, read
 // back, and merged into the caller's arrays as Film::addBatch does (film.cpp:119-137).
+int32_t pe_device_render_aovs(pe_device* d, const pe_camera* cam, const pe_settings* st, int32_t first, int32_t count,
+                              const volatile int32_t* cancel, float* sumRgb, uint32_t* sampleCount, float* sumLumSq,
+                              const pe_aov_films* aovs, uint64_t* traced) {
+    if (!d || !aovs) {
+        setError("pe_device_render_aovs: null argument");
+        return PE_ERR_INVALID;
+    }
+    int32_t rc = checkSettings(cam, st);
+    if (rc) return rc;
+    if (count <= 0) return PE_OK;
+    PE_CUDA(cudaSetDevice(d->ordinal));
+    if ((rc = ensureCapacity(d, kWaveSlots))) return rc;
+    // per-slot AOVs of both lanes and the device AOV films
+    for (WaveLane& ln : d->lanes)
+        if (!ln.aovA) {
+            if ((rc = devAlloc(ln.aovBufs, ln.aovA, d->capacity)) || (rc = devAlloc(ln.aovBufs, ln.aovN, d->capacity))) {
+                freeList(ln.aovBufs);
+                ln.aovA = ln.aovN = nullptr;
+                return rc;
+            }
+        }
+    const size_t n = static_cast<size_t>(st->width) * static_cast<size_t>(st->height);
+    if (d->aovFilmPixels < n) {
+        cudaFree(d->aovFilm);
+        d->aovFilm = nullptr;
+        d->aovFilmPixels = 0;
+        PE_CUDA(cudaMalloc(&d->aovFilm, n * 15 * sizeof(float)));
+        d->aovFilmPixels = n;
+    }
+    PE_CUDA(cudaMemsetAsync(d->aovFilm, 0, n * 15 * sizeof(float), d->stream));
+    d->aovTarget = d->aovFilm;
+    struct Reset {
+        pe_device* d;
+        ~Reset() { d->aovTarget = nullptr; }
+    } reset{d};
+    rc = pe_device_render(d, cam, st, first, count, cancel, sumRgb, sampleCount, sumLumSq, traced);
+    if (rc != PE_OK && rc != PE_ERR_CANCELLED) return rc;
+    // the batch's AOV films, merged like the beauty film (Film::addBatch)
+    std::vector<float> h(n * 15);
+    PE_CUDA(cudaMemcpyAsync(h.data(), d->aovFilm, n * 15 * sizeof(float), cudaMemcpyDeviceToHost, d->stream));
+    PE_CUDA(cudaStreamSynchronize(d->stream));
+    float* sums[3] = {aovs->albedo_sum, aovs->normal_sum, aovs->alpha_sum};
+    uint32_t* cnts[3] = {aovs->albedo_count, aovs->normal_count, aovs->alpha_count};
+    float* sqs[3] = {aovs->albedo_sum_sq, nullptr, aovs->alpha_sum_sq};
+    for (int f = 0; f < 3; ++f) {
+        const float* fs = h.data() + static_cast<size_t>(f) * 5 * n;
+        const uint32_t* fc = reinterpret_cast<const uint32_t*>(fs + 3 * n);
+        const float* fq = fs + 4 * n;
+        if (sums[f])
+            for (size_t i = 0; i < 3 * n; ++i) sums[f][i] += fs[i];
+        if (cnts[f])
+            for (size_t i = 0; i < n; ++i) cnts[f][i] += fc[i];
+        if (sqs[f])
+            for (size_t i = 0; i < n; ++i) sqs[f][i] += fq[i];
+    }
+    return rc;
+}
+
 int32_t pe_device_render(pe_device* d, const pe_camera* cam, const pe_settings* st, int32_t first, int32_t count,
                          const volatile int32_t* cancel, float* sumRgb, uint32_t* sampleCount, float* sumLumSq,
                          uint64_t* traced) {

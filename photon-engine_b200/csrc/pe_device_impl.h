@@ -64,6 +64,9 @@ struct WaveLane {
     cudaEvent_t evSegs = nullptr;     // the segment upload of the lane's last wave
     bool segsInFlight = false;
     uint32_t* hCounters = nullptr;    // pinned
+    float4* aovA = nullptr;           // AOVs per slot (allocated on first use, in aovBufs)
+    float4* aovN = nullptr;
+    std::vector<DevBuf> aovBufs;
     int32_t* pathOf = nullptr;        // path regeneration buffers (in bufs)
     int32_t* freeQ = nullptr;
     float4* Lout = nullptr;
@@ -192,6 +195,9 @@ struct pe_device {
     size_t stageBytes = 0;
     std::string noAllocError;
     pe_dev::GuideState guide;
+    float* aovTarget = nullptr;     // AOV films of the render in progress (pe_device_render_aovs)
+    float* aovFilm = nullptr;       // device AOV films (15 floats per pixel)
+    size_t aovFilmPixels = 0;
     int guideKind = 0;      // 0 none, 1 learned proposal, 2 SD-tree
     pe_dev::SdHost sd;
     uint64_t sceneSerial = 0; // counts pe_device_set_scene calls

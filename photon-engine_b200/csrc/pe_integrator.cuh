@@ -683,6 +683,23 @@ __device__ __forceinline__ bool shadeSlot(const SceneGPU& S, const Paths& P, con
             }
         }
         if (!done) {
+            // AOVs of the camera path's first surface past the skipped ones (path_tracer.cpp:440-443;
+            // tracePixel, renderer.cpp:177-203): albedo, normal and coverage, or the background
+            if ((flags & PF_FIRST_SEGMENT) && P.aovA) {
+                const int path = pathOfSlot(P, slot);
+                if (hit) {
+                    const V3 a = clamp3(m3f(S.materials[is.material].base), 0.0f, 1.0f);
+                    P.aovA[path] = make_float4(a.x, a.y, a.z, 1.0f);
+                    P.aovN[path] = make_float4(is.normal.x, is.normal.y, is.normal.z, 0.0f);
+                } else {
+                    V3 a = mk(0.0f);
+                    if (S.bgMode == PE_BG_COLOR) a = m3f(S.bgColor);
+                    else if (S.env.present) a = envEval(S.env, dir);
+                    a = clamp3(a, 0.0f, 1.0f);
+                    P.aovA[path] = make_float4(a.x, a.y, a.z, 0.0f);
+                    P.aovN[path] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+                }
+            }
             flags &= ~PF_FIRST_SEGMENT;
             // inside an object: absorption and, when the medium scatters, free flight
             const int top = volumetric ? media.top() : -1;
@@ -706,7 +723,13 @@ __device__ __forceinline__ bool shadeSlot(const SceneGPU& S, const Paths& P, con
             if (!hit) {
                 // environment / background (path_tracer.cpp:482-514)
                 if (depth == 0 && S.bgMode != PE_BG_ENVIRONMENT) {
-                    if (S.bgMode == PE_BG_COLOR) addL(L, thr * m3f(S.bgColor));
+                    if (S.bgMode == PE_BG_COLOR) {
+                        addL(L, thr * m3f(S.bgColor));
+                    } else if (passThroughs > 0 && P.aovA) {
+                        // straight through thin glass to a transparent background: coverage is
+                        // what the glass held back
+                        P.aovA[pathOfSlot(P, slot)].w = smax(0.0f, 1.0f - luminance(thr));
+                    }
                 } else if (S.env.present) {
                     const V3 Le = envEval(S.env, dir);
                     float weight = 1.0f;
@@ -733,6 +756,12 @@ __device__ __forceinline__ bool shadeSlot(const SceneGPU& S, const Paths& P, con
                 float ratio = 1.0f;
                 const V3 bg = shadowCatcher(S, is, dir, shadowSamples, sb, ratio);
                 addL(L, thr * bg * ratio);
+                if (depth == 0 && P.aovA) {
+                    // the catcher's AOVs: the background it shows, its shadow as coverage
+                    const V3 a = clamp3(bg, 0.0f, 1.0f);
+                    P.aovA[pathOfSlot(P, slot)] =
+                        make_float4(a.x, a.y, a.z, S.bgMode == PE_BG_TRANSPARENT ? 1.0f - ratio : 1.0f);
+                }
                 done = true;
             } else {
                 const MatGPU& mat = S.materials[is.material];
@@ -1080,6 +1109,47 @@ __global__ void __launch_bounds__(kTailBlock) kTail(SceneGPU S, Paths P, Wave W,
 }
 
 // ---- film: Film::addSample in sample order per pixel (src/core/image/film.cpp:56-69) ----------
+// The AOV films of one pixel (addAovs, renderer.cpp:219-224): albedo and alpha by addSample,
+// the normal by addSampleSigned (film.cpp:73-85), in sample order.
+__device__ __noinline__ void filmAovs(const Paths& P, const WaveSeg& A, int p, int pix) {
+    const size_t n = static_cast<size_t>(A.width) * static_cast<size_t>(A.height);
+    for (int f = 0; f < 3; ++f) {
+        float* fsum = A.aov + static_cast<size_t>(f) * 5 * n;
+        uint32_t* fcnt = reinterpret_cast<uint32_t*>(fsum + 3 * n);
+        float* fsq = fsum + 4 * n;
+        float r = fsum[3 * pix + 0], g = fsum[3 * pix + 1], b = fsum[3 * pix + 2], q = fsq[pix];
+        uint32_t c = fcnt[pix];
+        for (int s = 0; s < A.nSamples; ++s) {
+            const int path = A.slotFirst + s * A.nPix + p;
+            V3 v;
+            if (f == 0) {
+                const float4 a = P.aovA[path];
+                v = mk(a.x, a.y, a.z);
+            } else if (f == 1) {
+                const float4 nn = P.aovN[path];
+                v = mk(nn.x, nn.y, nn.z);
+            } else {
+                v = mk(P.aovA[path].w);
+            }
+            ++c;
+            if (!(finitef(v.x) && finitef(v.y) && finitef(v.z))) continue;
+            if (f != 1 && !(v.x >= 0.0f && v.y >= 0.0f && v.z >= 0.0f)) continue;
+            r += v.x;
+            g += v.y;
+            b += v.z;
+            if (f != 1) {
+                const float lum = luminance(v);
+                q += lum * lum;
+            }
+        }
+        fsum[3 * pix + 0] = r;
+        fsum[3 * pix + 1] = g;
+        fsum[3 * pix + 2] = b;
+        fsq[pix] = q;
+        fcnt[pix] = c;
+    }
+}
+
 __global__ void kFilm(Paths P, Wave W, unsigned long long* rejected) {
     unsigned long long rej = 0;
     for (int wp = blockIdx.x * blockDim.x + threadIdx.x; wp < W.nPix; wp += gridDim.x * blockDim.x) {
@@ -1111,6 +1181,7 @@ __global__ void kFilm(Paths P, Wave W, unsigned long long* rejected) {
         sum[3 * pix + 2] = sbb;
         A.sq[pix] = sq;
         A.cnt[pix] = c;
+        if (A.aov && P.aovA) filmAovs(P, A, p, pix);
     }
     if (rej) atomicAdd(rejected, rej);
 }

@@ -86,6 +86,9 @@ struct Paths {
     int32_t* freeQ;      // slots freed by the shading kernel this bounce
     float4* Lout;        // radiance of each ended path, by wave path index (read by the film kernel)
     uint32_t* segLeft;   // per segment: paths not yet ended (null unless the server tracks segments)
+    // AOVs of each path (null unless requested): albedo + alpha, primary normal
+    float4* aovA;
+    float4* aovN;
     // sweeps (continuous waves): a path alive for sweepAge bounces leaves the wavefront for a
     // tail-kernel launch on a side stream (sweepAge 0: off)
     int32_t* born;       // bounce at which each slot's path was injected
@@ -130,6 +133,7 @@ struct WaveSeg {
     float* sum;             // the request's film on the device
     uint32_t* cnt;
     float* sq;
+    float* aov;             // AOV films (albedo, normal, alpha: each sum 3n, count n, sum of squares n), or null
     int slotFirst;
     int pixFirst;
     int flags;              // SegFlags

@@ -443,6 +443,19 @@ class Film:
         self.rejected += other.rejected
 
 
+class AovFilms:
+    """AovFilms (renderer.h:42-53): the first visible surface's albedo, its normal and coverage."""
+
+    def __init__(self, width: int = 0, height: int = 0):
+        self.albedo = Film(width, height)
+        self.normal = Film(width, height)
+        self.alpha = Film(width, height)
+
+    def resize(self, width: int, height: int):
+        for f in (self.albedo, self.normal, self.alpha):
+            f.resize(width, height)
+
+
 @dataclasses.dataclass
 class RenderTargets:
     beauty: Optional[Film] = None
@@ -458,7 +471,7 @@ class SampleBatchResult:
 
 @dataclasses.dataclass
 class DeviceFeatures:
-    aovs: bool = False
+    aovs: bool = True
     light_passes: bool = False
     adaptive_sampling: bool = False
 
@@ -555,11 +568,24 @@ class CudaDevice:
         if cancel is not None:
             flag = cancel if isinstance(cancel, C.c_int32) else C.c_int32(1 if cancel else 0)
         traced = C.c_uint64(0)
+        aovs = targets.aovs
         with self._lock:
             self._sync_guiding(settings)
-            rc = _lib().pe_device_render(self._h, C.byref(camera.describe_gpu()), C.byref(st), first_sample, count,
-                                         C.byref(flag) if flag is not None else None, capi.fptr(film.sum),
-                                         capi.uptr(film.count), capi.fptr(film.sum_sq), C.byref(traced))
+            if aovs is not None:
+                aovs.resize(film.width, film.height) if aovs.albedo.width != film.width or \
+                    aovs.albedo.height != film.height else None
+                out = capi.pe_aov_films(capi.fptr(aovs.albedo.sum), capi.uptr(aovs.albedo.count),
+                                        capi.fptr(aovs.albedo.sum_sq), capi.fptr(aovs.normal.sum),
+                                        capi.uptr(aovs.normal.count), capi.fptr(aovs.alpha.sum),
+                                        capi.uptr(aovs.alpha.count), capi.fptr(aovs.alpha.sum_sq))
+                rc = _lib().pe_device_render_aovs(self._h, C.byref(camera.describe_gpu()), C.byref(st), first_sample,
+                                                  count, C.byref(flag) if flag is not None else None,
+                                                  capi.fptr(film.sum), capi.uptr(film.count), capi.fptr(film.sum_sq),
+                                                  C.byref(out), C.byref(traced))
+            else:
+                rc = _lib().pe_device_render(self._h, C.byref(camera.describe_gpu()), C.byref(st), first_sample,
+                                             count, C.byref(flag) if flag is not None else None, capi.fptr(film.sum),
+                                             capi.uptr(film.count), capi.fptr(film.sum_sq), C.byref(traced))
         if rc == capi.PE_ERR_CANCELLED:
             return SampleBatchResult(False, traced.value)
         capi.check(rc)
@@ -808,6 +834,7 @@ class RenderSession:
         self.device = device
         self.camera = None
         self.film = Film()
+        self.aovs: Optional[AovFilms] = None
         self.samples = 0
         self.traced = 0
         self.warnings: list[str] = []
@@ -829,6 +856,7 @@ class RenderSession:
             self.settings.adaptive_sampling = False
             self.warnings.append(f"{name}: adaptive sampling is not supported; every pixel reaches the target")
         self.film.resize(max(1, settings.width), max(1, settings.height))
+        self.aovs = AovFilms(max(1, settings.width), max(1, settings.height)) if self.config.aovs else None
         self.samples = 0
         self.traced = 0
         self._sps = 0.0
@@ -859,7 +887,8 @@ class RenderSession:
             return False
         count = self.next_batch()
         t0 = time.perf_counter()
-        r = self.device.render(self.camera, self.settings, RenderTargets(beauty=self.film), self.samples, count, cancel)
+        r = self.device.render(self.camera, self.settings, RenderTargets(beauty=self.film, aovs=self.aovs), self.samples,
+                               count, cancel)
         self.last_batch_seconds = time.perf_counter() - t0
         self.traced += r.samples_traced
         if not r.completed:

@@ -38,7 +38,7 @@
 extern "C" {
 #endif
 
-#define PE_ABI_VERSION 4
+#define PE_ABI_VERSION 5
 
 typedef enum pe_status {
     PE_OK = 0,
@@ -170,6 +170,15 @@ int32_t pe_scene_set_light_link(pe_scene* s, int32_t light, int32_t mode, const 
  * order they were added: one per pe_scene_add_mesh, two per pe_scene_add_area_light (its two
  * triangles, as Scene::addLight adds them).  Call before pe_scene_build. */
 int32_t pe_scene_set_shadow_catcher(pe_scene* s, int32_t shape);
+/* Light::setLightGroup (src/lights/light.h:85) of light `light` (the numbering of
+ * pe_scene_set_light_link), or of the environment when light == -1; "" or NULL clears it.
+ * Scene::buildAccelerator forms the groups (src/engine/scene.cpp:144-174): none unless some
+ * light names one; then every light joins its group or "Default", the environment its group or
+ * "Env", at most PE_MAX_LIGHT_GROUPS groups. */
+int32_t pe_scene_set_light_group(pe_scene* s, int32_t light, const char* name);
+/* Scene::lightGroupNames after pe_scene_build: returns the number of groups and, when names is
+ * not NULL, writes them NUL-separated into names[0, capacity). */
+int32_t pe_scene_light_groups(const pe_scene* s, char* names, int32_t capacity);
 /* Scene::addLight(AreaLight) — rectangle p + s*u + t*v, two-sided, plus its
  * two emissive triangles in the BVH (src/engine/scene.cpp:65-99). */
 int32_t pe_scene_add_area_light(pe_scene* s, const float p[3], const float u[3], const float v[3],
@@ -274,6 +283,37 @@ typedef struct pe_aov_films {
 int32_t pe_device_render_aovs(pe_device* d, const pe_camera* cam, const pe_settings* st, int32_t first_sample,
                               int32_t count, const volatile int32_t* cancel, float* sum_rgb, uint32_t* sample_count,
                               float* sum_lum_sq, const pe_aov_films* aovs, uint64_t* traced);
+
+/* Render passes (RenderPassFilms, src/engine/renderer.h:59-98).  Each film is a Film's arrays
+ * (sum of RGB, sample count, sum of squared luminance; a NULL array is skipped), merged like
+ * the beauty film. */
+#define PE_MAX_LIGHT_GROUPS 16
+#define PE_LIGHT_PASSES 8
+typedef struct pe_film_arrays {
+    float* sum;
+    uint32_t* count;
+    float* sum_sq;
+} pe_film_arrays;
+typedef struct pe_pass_films {
+    /* LightPass order (src/integrators/path_tracer.h:21-24): diffuse direct, diffuse indirect,
+     * glossy direct, glossy indirect, transmission direct, transmission indirect, emission,
+     * background; their sum is the beauty film */
+    pe_film_arrays light[PE_LIGHT_PASSES];
+    pe_film_arrays depth;       /* distance from the camera ray's origin to the first hit */
+    pe_film_arrays position;    /* first hit point, signed (no squares are kept) */
+    pe_film_arrays object_id;   /* idColor of the hit shape's node uid (pe_scene_tag_shape) */
+    pe_film_arrays material_id; /* idColor of the hit material's index + 1 */
+    int32_t n_groups;           /* must equal pe_scene_light_groups of the device's scene */
+    int32_t pad;
+    pe_film_arrays groups[PE_MAX_LIGHT_GROUPS]; /* one per light group, in Scene::lightGroupNames order */
+} pe_pass_films;
+/* pe_device_render plus the render passes and, when aovs is not NULL, the AOV films of the same
+ * samples (RenderDevice::render with RenderTargets::passes; tracePixel with wantPasses,
+ * renderer.cpp:139-204, addPasses 206-217). */
+int32_t pe_device_render_passes(pe_device* d, const pe_camera* cam, const pe_settings* st, int32_t first_sample,
+                                int32_t count, const volatile int32_t* cancel, float* sum_rgb, uint32_t* sample_count,
+                                float* sum_lum_sq, const pe_aov_films* aovs, const pe_pass_films* passes,
+                                uint64_t* traced);
 
 /* Same, accumulating into the device-resident film (kept across calls until
  * pe_device_film_clear; resized/cleared when width/height change). */

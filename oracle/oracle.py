@@ -68,6 +68,9 @@ def _load(fast: bool = False):
         "ref_env_eval": (C.c_int32, [P, FP, C.c_size_t, FP, FP]),
         "ref_render_guided": (C.c_int32, [P, C.c_void_p, C.c_void_p, C.c_int32, C.c_int32, C.c_int32, FP, UP]),
         "ref_scene_set_shadow_catcher": (C.c_int32, [P, C.c_int32]),
+        "ref_scene_set_light_group": (C.c_int32, [P, C.c_int32, C.c_char_p]),
+        "ref_render_passes": (C.c_int32, [P, C.c_void_p, C.c_void_p, C.c_int32, C.c_int32, C.c_int32, FP, UP, FP, FP,
+                                          FP, C.c_int32]),
         "ref_render_aovs": (C.c_int32, [P, C.c_void_p, C.c_void_p, C.c_int32, C.c_int32, C.c_int32, FP, UP, FP, FP,
                                         FP, UP]),
         "ref_scene_tag_shape": (C.c_int32, [P, C.c_int32, C.c_uint64]),
@@ -131,7 +134,25 @@ class RefScene:
             if self.lib.ref_scene_set_light_link(self.h, int(light), int(mode), a, len(uids), int(smode), b,
                                                  len(suids)) != 0:
                 raise RuntimeError("reference rejected a light link")
+        # light groups: an area light's own, then Scene.set_light_group's (light numbering as in
+        # the product scene: one per area light, one per triangle of an emissive mesh)
+        groups, li = {}, 0
+        for kind, obj in scene.ops:
+            if kind == "mesh":
+                m = obj.material.struct
+                if m.type in (0, 1) and any(m.emission):
+                    li += obj.indices.shape[0]
+            else:
+                if getattr(obj, "light_group", ""):
+                    groups[li] = obj.light_group
+                li += 1
+        groups.update(getattr(scene, "light_groups", {}))
+        for light, name in groups.items():
+            if self.lib.ref_scene_set_light_group(self.h, int(light), name.encode()) != 0:
+                raise RuntimeError("reference rejected a light group")
         env = scene.environment
+        if env is not None and getattr(env, "light_group", ""):
+            self.lib.ref_scene_set_light_group(self.h, -1, env.light_group.encode())
         if env is not None:
             img = env.image
             sun = env.sun
@@ -174,6 +195,20 @@ class RefScene:
         fn(self.h, C.byref(camera.describe_gpu()), C.byref(settings.to_c()), first, count, threads, _f(mean),
            cnt.ctypes.data_as(UP))
         return mean, cnt
+
+    def render_passes(self, camera, settings, first: int, count: int, threads: int = 0):
+        """Renderer::renderSamples with RenderPassFilms (seed 12345): mean beauty, counts, the eight
+        light passes (8, h, w, 3), the data passes (depth, position, object id, material id) and
+        the light groups (G, h, w, 3)."""
+        h, w = settings.height, settings.width
+        mean = np.zeros((h, w, 3), np.float32)
+        cnt = np.zeros((h, w), np.uint32)
+        light = np.zeros((8, h, w, 3), np.float32)
+        data = np.zeros((4, h, w, 3), np.float32)
+        groups = np.zeros((16, h, w, 3), np.float32)
+        n = self.lib.ref_render_passes(self.h, C.byref(camera.describe_gpu()), C.byref(settings.to_c()), first, count,
+                                       threads, _f(mean), cnt.ctypes.data_as(UP), _f(light), _f(data), _f(groups), 16)
+        return mean, cnt, light, data, groups[:n]
 
     def render_aovs(self, camera, settings, first: int, count: int, threads: int = 0):
         """Renderer::renderSamples with AovFilms (seed 12345): mean beauty, albedo, normal, alpha

@@ -83,6 +83,7 @@ struct RefScene {
     std::vector<std::shared_ptr<Material>> materials;
     std::unordered_map<const void*, int> shapeIndex; // hitObject → insertion index
     int nextShape = 0;
+    std::string envGroup; // the environment's light group, applied at build
     void indexNewShapes() {
         const auto& shapes = scene.shapes();
         for (size_t i = static_cast<size_t>(nextShape); i < shapes.size(); ++i)
@@ -247,6 +248,20 @@ int32_t ref_scene_set_light_link(void* s, int32_t light, int32_t mode, const uin
     return 0;
 }
 
+// Light::setLightGroup of light `light` (scene.lights() order), or of the environment (-1; applied
+// when the scene is built).
+int32_t ref_scene_set_light_group(void* s, int32_t light, const char* name) {
+    auto* rs = static_cast<RefScene*>(s);
+    if (light < 0) {
+        rs->envGroup = name ? name : "";
+        return 0;
+    }
+    const auto& lights = rs->scene.lights();
+    if (light >= static_cast<int32_t>(lights.size())) return -1;
+    const_cast<Light*>(lights[static_cast<size_t>(light)])->setLightGroup(name ? name : "");
+    return 0;
+}
+
 // Scene::setShadowCatcher with the shape added `shape`-th (-1: none).
 int32_t ref_scene_set_shadow_catcher(void* s, int32_t shape) {
     auto* rs = static_cast<RefScene*>(s);
@@ -298,6 +313,8 @@ int32_t ref_scene_set_background(void* s, int32_t mode, const float* color) {
 
 int32_t ref_scene_build(void* s) {
     auto* rs = static_cast<RefScene*>(s);
+    if (!rs->envGroup.empty() && rs->scene.environment())
+        const_cast<EnvironmentLight*>(rs->scene.environment())->setLightGroup(rs->envGroup);
     rs->scene.buildAccelerator();
     return 0;
 }
@@ -359,6 +376,34 @@ int32_t ref_render_aovs(void* s, const pe_camera* cam, const pe_settings* st, in
     exportFilm(aovs.normal, st->width, st->height, normal, nullptr);
     exportFilm(aovs.alpha, st->width, st->height, alpha, nullptr);
     return 0;
+}
+
+// Renderer::renderSamples with RenderPassFilms (seed 12345): the mean beauty and counts, the
+// eight light passes (light: 8 images), the data passes (data: depth, position, object id,
+// material id) and the light groups (groups: up to max_groups images).  Returns the number of
+// light groups.
+int32_t ref_render_passes(void* s, const pe_camera* cam, const pe_settings* st, int32_t first, int32_t count,
+                          int32_t threads, float* mean_rgb, uint32_t* counts, float* light, float* data, float* groups,
+                          int32_t max_groups) {
+    auto* rs = static_cast<RefScene*>(s);
+    DescCamera camera(*cam);
+    RenderSettings settings = toSettings(*st, threads > 0 ? threads : hardwareThreads());
+    Film film(st->width, st->height);
+    RenderPassFilms passes;
+    passes.resize(st->width, st->height);
+    Renderer renderer;
+    renderer.renderSamples(rs->scene, camera, settings, film, first, count, nullptr, nullptr, &passes);
+    const size_t img = static_cast<size_t>(st->width) * static_cast<size_t>(st->height) * 3;
+    exportFilm(film, st->width, st->height, mean_rgb, counts);
+    for (int k = 0; k < static_cast<int>(LightPass::Count); ++k)
+        exportFilm(passes.light[k], st->width, st->height, light + static_cast<size_t>(k) * img, nullptr);
+    const Film* d[4] = {&passes.depth, &passes.position, &passes.objectId, &passes.materialId};
+    for (int k = 0; k < 4; ++k) exportFilm(*d[k], st->width, st->height, data + static_cast<size_t>(k) * img, nullptr);
+    const int n = static_cast<int>(passes.lightGroups.size());
+    for (int g = 0; g < n && g < max_groups; ++g)
+        exportFilm(passes.lightGroups[static_cast<size_t>(g)].second, st->width, st->height,
+                   groups + static_cast<size_t>(g) * img, nullptr);
+    return n;
 }
 
 int32_t ref_render_guided(void* s, const pe_camera* cam, const pe_settings* st, int32_t first, int32_t count,

@@ -5,8 +5,8 @@ host-side mirror of the reference's RenderDevice / RenderSession / Scene API ove
 """
 from . import _capi
 from .engine import (AovFilms, AreaLight, Background, BackgroundMode, CudaDevice, Dielectric, DeviceFeatures, DeviceInfo,
-                     DisneyMaterial, EnvironmentLight, Film, Lambertian, Material, Mirror, OrthographicCamera, PerspectiveCamera, ThinLensCamera,
-                     PixelFilterType, RenderMode, RenderServer, RenderSession, RenderSettings, RenderTargets, RequestStatus,
+                     DisneyMaterial, EnvironmentLight, Film, Lambertian, LightPass, Material, Mirror, OrthographicCamera, PerspectiveCamera, ThinLensCamera,
+                     PixelFilterType, RenderMode, RenderPassFilms, RenderServer, RenderSession, RenderSettings, RenderTargets, RequestStatus,
                      SampleBatchResult,
                      Scene, SceneUpdateKind, SessionConfig, TriangleMesh, create_device, enumerate_devices, rel_mse)
 

@@ -110,6 +110,20 @@ class pe_aov_films(C.Structure):
                 ("alpha_count", C.POINTER(C.c_uint32)), ("alpha_sum_sq", C.POINTER(C.c_float))]
 
 
+PE_MAX_LIGHT_GROUPS = 16
+PE_LIGHT_PASSES = 8
+
+
+class pe_film_arrays(C.Structure):
+    _fields_ = [("sum", C.POINTER(C.c_float)), ("count", C.POINTER(C.c_uint32)), ("sum_sq", C.POINTER(C.c_float))]
+
+
+class pe_pass_films(C.Structure):
+    _fields_ = [("light", pe_film_arrays * PE_LIGHT_PASSES), ("depth", pe_film_arrays), ("position", pe_film_arrays),
+                ("object_id", pe_film_arrays), ("material_id", pe_film_arrays), ("n_groups", C.c_int32),
+                ("pad", C.c_int32), ("groups", pe_film_arrays * PE_MAX_LIGHT_GROUPS)]
+
+
 class pe_request_desc(C.Structure):
     _fields_ = [("scene", C.c_int32), ("camera", pe_camera), ("settings", pe_settings), ("spp", C.c_int32),
                 ("priority", C.c_int32)]
@@ -137,6 +151,12 @@ SIGNATURES = {
     "pe_last_error": (C.c_char_p, []),
     "pe_abi_version": (C.c_int32, []),
     "pe_scene_set_shadow_catcher": (C.c_int32, [P, C.c_int32]),
+    "pe_scene_set_light_group": (C.c_int32, [P, C.c_int32, C.c_char_p]),
+    "pe_scene_light_groups": (C.c_int32, [P, C.c_char_p, C.c_int32]),
+    "pe_device_render_passes": (C.c_int32, [P, C.POINTER(pe_camera), C.POINTER(pe_settings), C.c_int32, C.c_int32,
+                                            C.POINTER(C.c_int32), C.POINTER(C.c_float), C.POINTER(C.c_uint32),
+                                            C.POINTER(C.c_float), C.POINTER(pe_aov_films), C.POINTER(pe_pass_films),
+                                            C.POINTER(C.c_uint64)]),
     "pe_device_render_aovs": (C.c_int32, [P, C.POINTER(pe_camera), C.POINTER(pe_settings), C.c_int32, C.c_int32,
                                           C.c_void_p, FP, C.POINTER(C.c_uint32), FP, C.POINTER(pe_aov_films),
                                           C.POINTER(C.c_uint64)]),

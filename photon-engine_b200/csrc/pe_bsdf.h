@@ -494,13 +494,18 @@ PE_HD float pdfSpecTransmission(V3 woL, V3 wiL, const DisneyParams& p) {
     return visible * fabsf(wiDotH) / (s * s);
 }
 
-// Sum of all lobes f(wo, wi) (disney.cpp:223-311).  diffuseOut (may be null) receives the
-// diffuse share, used for the next-ray visibility class.
-PE_HDN V3 disneyEval(const TablesGPU* T, V3 wo, V3 wi, const DisneyParams& p, V3* diffuseOut) {
+// f(wo, wi) in the lobe groups of the render passes (LobeSplit, material.h:53-57).
+struct LobeSplit3 {
+    V3 diffuse, glossy, transmission;
+};
+
+// Sum of all lobes f(wo, wi) (disney.cpp:223-311).  split (may be null) receives the sum in
+// lobe groups as DisneyMaterial::evalSplit forms it (disney.cpp:654-658).
+PE_HDN V3 disneyEval(const TablesGPU* T, V3 wo, V3 wi, const DisneyParams& p, LobeSplit3* split) {
     const Frame frame = shadingFrame(p.normal, p.tangent);
     const V3 woL = toLocal(frame, wo);
     const V3 wiL = toLocal(frame, wi);
-    if (diffuseOut) *diffuseOut = mk(0.0f);
+    if (split) split->diffuse = split->glossy = split->transmission = mk(0.0f);
     if (woL.z <= 0.0f) return mk(0.0f);
     const float cosThetaO = woL.z;
     const float coatO = coatTransmit(T, p, cosThetaO);
@@ -518,6 +523,7 @@ PE_HDN V3 disneyEval(const TablesGPU* T, V3 wo, V3 wi, const DisneyParams& p, V3
             ft += p.base * (trans * kInvPi * coatO * layerFactor(T, dl, cosThetaO, muI) * sh) * cTint;
         }
         if (stW > 0.0f) ft += evalSpecTransmission(woL, wiL, p) * coatO * cTint;
+        if (split) split->transmission = ft;
         return ft;
     }
     const V3 hL = normalize(woL + wiL);
@@ -552,7 +558,10 @@ PE_HDN V3 disneyEval(const TablesGPU* T, V3 wo, V3 wi, const DisneyParams& p, V3
         }
     }
     if (p.clearCoat <= 0.0f) {
-        if (diffuseOut) *diffuseOut = baseDiffuse;
+        if (split) {
+            split->diffuse = baseDiffuse;
+            split->glossy = base - baseDiffuse;
+        }
         return base;
     }
     const float alphaC = p.clearCoatRoughness * p.clearCoatRoughness;
@@ -563,7 +572,10 @@ PE_HDN V3 disneyEval(const TablesGPU* T, V3 wo, V3 wi, const DisneyParams& p, V3
     const float msC = 1.0f + f0c * (1.0f / ggxDirectionalAlbedo(T, cosThetaO, alphaC) - 1.0f);
     const V3 fCoat = mk(p.clearCoat * Fc * Dc * Gc / (4.0f * cosThetaO * cosThetaI) * msC);
     const V3 coatAtt = cTint * (coatO * coatTransmit(T, p, cosThetaI));
-    if (diffuseOut) *diffuseOut = baseDiffuse * coatAtt;
+    if (split) {
+        split->diffuse = baseDiffuse * coatAtt;
+        split->glossy = (base - baseDiffuse) * coatAtt + fCoat;
+    }
     return base * coatAtt + fCoat;
 }
 
@@ -933,29 +945,33 @@ PE_HDN bool glassSample(const MatGPU& m, V3 woW, const ShadePoint& sp, float uc,
 // ---------------------------------------------------------------------------------------------
 // Dispatch (Material::evalPdf / sampleFull)
 PE_HD V3 bsdfEvalPdf(const TablesGPU* T, const MatGPU& m, V3 wo, V3 wi, const ShadePoint& sp, float& pdf,
-                     V3* diffuseOut) {
-    if (diffuseOut) *diffuseOut = mk(0.0f);
+                     LobeSplit3* split) {
+    if (split) split->diffuse = split->glossy = split->transmission = mk(0.0f);
+    V3 f;
     switch (m.type) {
-        case 0: {
-            const V3 f = lambertEval(m, wo, wi, sp.n, pdf);
-            if (diffuseOut) {
-                // Material::evalSplit default: same geometric side → diffuse (material.h:139-145)
-                const V3 nn = len2(sp.ng) > 0.0f ? sp.ng : sp.n;
-                *diffuseOut = dot(wo, nn) * dot(wi, nn) >= 0.0f ? f : mk(0.0f);
-            }
-            return f;
-        }
+        case 0:
+            f = lambertEval(m, wo, wi, sp.n, pdf);
+            break;
         case 1: {
             const DisneyParams p = disneyResolve(m, sp);
             pdf = disneyPdf(wo, wi, p);
-            return disneyEval(T, wo, wi, p, diffuseOut);
+            return disneyEval(T, wo, wi, p, split);
         }
         case 2:
-            return glassEval(m, wo, wi, sp, pdf);
+            f = glassEval(m, wo, wi, sp, pdf);
+            break;
         default:
             pdf = 0.0f;
             return mk(0.0f);
     }
+    if (split) {
+        // Material::evalSplit (material.h:154-160) and Dielectric::evalSplit (dielectric.cpp:279-286):
+        // same side of the geometric surface → diffuse (glass: glossy), else transmission
+        const V3 nn = len2(sp.ng) > 0.0f ? sp.ng : sp.n;
+        if (dot(wo, nn) * dot(wi, nn) >= 0.0f) (m.type == 2 ? split->glossy : split->diffuse) = f;
+        else split->transmission = f;
+    }
+    return f;
 }
 
 PE_HD bool bsdfSample(const TablesGPU* T, const MatGPU& m, V3 wo, const ShadePoint& sp, float uc, V2 u,

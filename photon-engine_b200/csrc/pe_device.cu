@@ -283,13 +283,18 @@ int32_t runWave(pe_device* d, int lane, Paths& P, int nSegs, int nSlots, int nPi
     P.sd = d->sd.field;
     // path regeneration: a wave of more paths than slots (unguided waves on a lane's own state)
     const int64_t slotCap = static_cast<int64_t>(P.capacity);
-    const bool regen = &P == &ln.paths && ln.Lout && !P.guiding && !P.sdMode && !d->aovTarget && nSlots > slotCap;
+    const bool regen = &P == &ln.paths && ln.Lout && !P.guiding && !P.sdMode && !d->aovTarget && !d->passTarget &&
+                       nSlots > slotCap;
     P.pathOf = regen ? ln.pathOf : nullptr;
     P.freeQ = regen ? ln.freeQ : nullptr;
     P.Lout = regen ? ln.Lout : nullptr;
     P.segLeft = nullptr;
     P.aovA = (d->aovTarget && &P == &ln.paths) ? ln.aovA : nullptr;
     P.aovN = (d->aovTarget && &P == &ln.paths) ? ln.aovN : nullptr;
+    const bool passes = d->passTarget && &P == &ln.paths;
+    P.pass = passes ? ln.pass : nullptr;
+    P.shPass = passes ? ln.shPass : nullptr;
+    P.passStride = passes ? d->passStride : 0;
     P.born = nullptr;
     P.sweepQ = nullptr;
     P.sweepAge = 0;
@@ -426,6 +431,9 @@ int32_t loopBegin(pe_device* d, LaneLoop& L, uint32_t* segLeft) {
     P.segLeft = segLeft;
     P.aovA = nullptr;
     P.aovN = nullptr;
+    P.pass = nullptr;
+    P.shPass = nullptr;
+    P.passStride = 0;
     P.born = L.born;
     P.sweepQ = nullptr;
     P.sweepAge = 0;
@@ -570,7 +578,7 @@ int32_t renderWaves(pe_device* d, const pe_camera* cam, const pe_settings* st, i
                     bool timing, Tile tile) {
     const size_t npix = static_cast<size_t>(tile.w) * static_cast<size_t>(tile.h);
     // unguided waves on the lanes' own state regenerate paths: kStreamFactor × the slots per wave
-    const bool regenWaves = !scratch && !d->guide.mode && d->guideKind != 2 && !d->aovTarget;
+    const bool regenWaves = !scratch && !d->guide.mode && d->guideKind != 2 && !d->aovTarget && !d->passTarget;
     const size_t pathCap = regenWaves ? capacity * kStreamFactor : capacity;
     const int pixChunk = static_cast<int>(std::min(npix, pathCap));
     const int samplesPerWave = static_cast<int>(std::max<size_t>(1, std::min<size_t>(static_cast<size_t>(count), pathCap / pixChunk)));
@@ -590,6 +598,7 @@ int32_t renderWaves(pe_device* d, const pe_camera* cam, const pe_settings* st, i
     base.cnt = cnt;
     base.sq = sq;
     base.aov = scratch ? nullptr : d->aovTarget;
+    base.pass = scratch ? nullptr : d->passTarget;
     RenderTimer tm;
     tm.timing = timing;
     bool cancelled = false;
@@ -798,6 +807,11 @@ int32_t uploadScene(pe_device* d, const pe_scene* s, SceneGPU& G, std::vector<De
     G.hasLightLinks = B.hasLightLinks;
     G.hasShadowLinks = B.hasShadowLinks;
     if (!B.links.empty() && (rc = upload(d, bufs, G.links, B.links))) return rc;
+    G.nLightGroups = static_cast<int32_t>(B.groupNames.size());
+    G.envGroup = B.envGroup;
+    if (!B.lightGroup.empty() && (rc = upload(d, bufs, G.lightGroup, B.lightGroup))) return rc;
+    if ((rc = upload(d, bufs, G.idColor, B.idColor))) return rc;
+    d->lightGroups = G.nLightGroups;
     PE_CUDA(cudaStreamSynchronize(d->stream));
     return PE_OK;
 }
@@ -901,6 +915,7 @@ void pe_device_destroy(pe_device* d) {
         WaveLane& ln = d->lanes[l];
         freeList(ln.bufs);
         freeList(ln.aovBufs);
+        freeList(ln.passBufs);
         cudaFree(ln.dSegs);
         if (ln.hSegs) cudaFreeHost(ln.hSegs);
         if (ln.hCounters) cudaFreeHost(ln.hCounters);
@@ -910,6 +925,7 @@ void pe_device_destroy(pe_device* d) {
     }
     if (d->evFilm) cudaEventDestroy(d->evFilm);
     cudaFree(d->aovFilm);
+    cudaFree(d->passFilm);
     cudaFree(d->fSum);
     cudaFree(d->fCnt);
     cudaFree(d->fSq);
@@ -1016,8 +1032,121 @@ int32_t pe_device_film_read(pe_device* d, float* sum, uint32_t* cnt, float* sq) 
     return PE_OK;
 }
 
-// RenderDevice::render with host films: the batch is rendered into a zeroed device film, read
-// back, and merged into the caller's arrays as Film::addBatch does (film.cpp:119-137).
+// Adds a device film block (5 floats per pixel: sum 3n, count n, sum of squares n) to a Film's
+// host arrays as Film::addBatch does (film.cpp:119-137); a null array is skipped.
+static void mergeFilm(const float* fs, size_t n, float* sum, uint32_t* cnt, float* sq) {
+    const uint32_t* fc = reinterpret_cast<const uint32_t*>(fs + 3 * n);
+    const float* fq = fs + 4 * n;
+    if (sum)
+        for (size_t i = 0; i < 3 * n; ++i) sum[i] += fs[i];
+    if (cnt)
+        for (size_t i = 0; i < n; ++i) cnt[i] += fc[i];
+    if (sq)
+        for (size_t i = 0; i < n; ++i) sq[i] += fq[i];
+}
+
+// RenderDevice::render with AOV and / or pass targets: per-slot outputs on both lanes, zeroed
+// device films, the beauty render, then every film read back and merged into the caller's.
+static int32_t renderTargets(pe_device* d, const pe_camera* cam, const pe_settings* st, int32_t first, int32_t count,
+                             const volatile int32_t* cancel, float* sumRgb, uint32_t* sampleCount, float* sumLumSq,
+                             const pe_aov_films* aovs, const pe_pass_films* passes, uint64_t* traced) {
+    int32_t rc = checkSettings(cam, st);
+    if (rc) return rc;
+    if (count <= 0) return PE_OK;
+    if (!d->hasScene) {
+        setError("render before set_scene");
+        return PE_ERR_NO_SCENE;
+    }
+    if (passes && passes->n_groups != d->lightGroups) {
+        setError("pe_device_render_passes: " + std::to_string(passes->n_groups) + " light-group films for a scene with " +
+                 std::to_string(d->lightGroups) + " light groups");
+        return PE_ERR_INVALID;
+    }
+    PE_CUDA(cudaSetDevice(d->ordinal));
+    if ((rc = ensureCapacity(d, kWaveSlots))) return rc;
+    const size_t n = static_cast<size_t>(st->width) * static_cast<size_t>(st->height);
+    if (aovs) {
+        for (WaveLane& ln : d->lanes)
+            if (!ln.aovA) {
+                if ((rc = devAlloc(ln.aovBufs, ln.aovA, d->capacity)) || (rc = devAlloc(ln.aovBufs, ln.aovN, d->capacity))) {
+                    freeList(ln.aovBufs);
+                    ln.aovA = ln.aovN = nullptr;
+                    return rc;
+                }
+            }
+        if (d->aovFilmPixels < n) {
+            cudaFree(d->aovFilm);
+            d->aovFilm = nullptr;
+            d->aovFilmPixels = 0;
+            PE_CUDA(cudaMalloc(&d->aovFilm, n * 15 * sizeof(float)));
+            d->aovFilmPixels = n;
+        }
+        PE_CUDA(cudaMemsetAsync(d->aovFilm, 0, n * 15 * sizeof(float), d->stream));
+    }
+    const int32_t stride = PASS_GROUPS + d->lightGroups;
+    const size_t passFloats = static_cast<size_t>(PFILM_GROUPS + d->lightGroups) * 5 * n;
+    if (passes) {
+        for (WaveLane& ln : d->lanes)
+            if (!ln.pass || ln.passStride != stride) {
+                freeList(ln.passBufs);
+                ln.pass = ln.shPass = nullptr;
+                ln.passStride = 0;
+                if ((rc = devAlloc(ln.passBufs, ln.pass, d->capacity * static_cast<size_t>(stride))) ||
+                    (rc = devAlloc(ln.passBufs, ln.shPass, d->capacity * 3))) {
+                    freeList(ln.passBufs);
+                    ln.pass = ln.shPass = nullptr;
+                    return rc;
+                }
+                ln.passStride = stride;
+            }
+        if (d->passFilmFloats < passFloats) {
+            cudaFree(d->passFilm);
+            d->passFilm = nullptr;
+            d->passFilmFloats = 0;
+            PE_CUDA(cudaMalloc(&d->passFilm, passFloats * sizeof(float)));
+            d->passFilmFloats = passFloats;
+        }
+        PE_CUDA(cudaMemsetAsync(d->passFilm, 0, passFloats * sizeof(float), d->stream));
+    }
+    d->aovTarget = aovs ? d->aovFilm : nullptr;
+    d->passTarget = passes ? d->passFilm : nullptr;
+    d->passStride = passes ? stride : 0;
+    struct Reset {
+        pe_device* d;
+        ~Reset() {
+            d->aovTarget = nullptr;
+            d->passTarget = nullptr;
+            d->passStride = 0;
+        }
+    } reset{d};
+    rc = pe_device_render(d, cam, st, first, count, cancel, sumRgb, sampleCount, sumLumSq, traced);
+    if (rc != PE_OK && rc != PE_ERR_CANCELLED) return rc;
+    if (aovs) {
+        std::vector<float> h(n * 15);
+        PE_CUDA(cudaMemcpyAsync(h.data(), d->aovFilm, n * 15 * sizeof(float), cudaMemcpyDeviceToHost, d->stream));
+        PE_CUDA(cudaStreamSynchronize(d->stream));
+        mergeFilm(h.data(), n, aovs->albedo_sum, aovs->albedo_count, aovs->albedo_sum_sq);
+        mergeFilm(h.data() + 5 * n, n, aovs->normal_sum, aovs->normal_count, nullptr);
+        mergeFilm(h.data() + 10 * n, n, aovs->alpha_sum, aovs->alpha_count, aovs->alpha_sum_sq);
+    }
+    if (passes) {
+        std::vector<float> h(passFloats);
+        PE_CUDA(cudaMemcpyAsync(h.data(), d->passFilm, passFloats * sizeof(float), cudaMemcpyDeviceToHost, d->stream));
+        PE_CUDA(cudaStreamSynchronize(d->stream));
+        const pe_film_arrays* films[PFILM_GROUPS + PE_MAX_LIGHT_GROUPS];
+        for (int k = 0; k < PE_LIGHT_PASSES; ++k) films[k] = &passes->light[k];
+        films[PFILM_DEPTH] = &passes->depth;
+        films[PFILM_POSITION] = &passes->position;
+        films[PFILM_OBJECT] = &passes->object_id;
+        films[PFILM_MATERIAL] = &passes->material_id;
+        for (int g = 0; g < d->lightGroups; ++g) films[PFILM_GROUPS + g] = &passes->groups[g];
+        for (int f = 0; f < PFILM_GROUPS + d->lightGroups; ++f)
+            mergeFilm(h.data() + static_cast<size_t>(f) * 5 * n, n, films[f]->sum, films[f]->count,
+                      f == PFILM_POSITION ? nullptr : films[f]->sum_sq);
+    }
+    return rc;
+}
+
 int32_t pe_device_render_aovs(pe_device* d, const pe_camera* cam, const pe_settings* st, int32_t first, int32_t count,
                               const volatile int32_t* cancel, float* sumRgb, uint32_t* sampleCount, float* sumLumSq,
                               const pe_aov_films* aovs, uint64_t* traced) {
@@ -1025,55 +1154,18 @@ int32_t pe_device_render_aovs(pe_device* d, const pe_camera* cam, const pe_setti
         setError("pe_device_render_aovs: null argument");
         return PE_ERR_INVALID;
     }
-    int32_t rc = checkSettings(cam, st);
-    if (rc) return rc;
-    if (count <= 0) return PE_OK;
-    PE_CUDA(cudaSetDevice(d->ordinal));
-    if ((rc = ensureCapacity(d, kWaveSlots))) return rc;
-    // per-slot AOVs of both lanes and the device AOV films
-    for (WaveLane& ln : d->lanes)
-        if (!ln.aovA) {
-            if ((rc = devAlloc(ln.aovBufs, ln.aovA, d->capacity)) || (rc = devAlloc(ln.aovBufs, ln.aovN, d->capacity))) {
-                freeList(ln.aovBufs);
-                ln.aovA = ln.aovN = nullptr;
-                return rc;
-            }
-        }
-    const size_t n = static_cast<size_t>(st->width) * static_cast<size_t>(st->height);
-    if (d->aovFilmPixels < n) {
-        cudaFree(d->aovFilm);
-        d->aovFilm = nullptr;
-        d->aovFilmPixels = 0;
-        PE_CUDA(cudaMalloc(&d->aovFilm, n * 15 * sizeof(float)));
-        d->aovFilmPixels = n;
+    return renderTargets(d, cam, st, first, count, cancel, sumRgb, sampleCount, sumLumSq, aovs, nullptr, traced);
+}
+
+int32_t pe_device_render_passes(pe_device* d, const pe_camera* cam, const pe_settings* st, int32_t first,
+                                int32_t count, const volatile int32_t* cancel, float* sumRgb, uint32_t* sampleCount,
+                                float* sumLumSq, const pe_aov_films* aovs, const pe_pass_films* passes,
+                                uint64_t* traced) {
+    if (!d || !passes) {
+        setError("pe_device_render_passes: null argument");
+        return PE_ERR_INVALID;
     }
-    PE_CUDA(cudaMemsetAsync(d->aovFilm, 0, n * 15 * sizeof(float), d->stream));
-    d->aovTarget = d->aovFilm;
-    struct Reset {
-        pe_device* d;
-        ~Reset() { d->aovTarget = nullptr; }
-    } reset{d};
-    rc = pe_device_render(d, cam, st, first, count, cancel, sumRgb, sampleCount, sumLumSq, traced);
-    if (rc != PE_OK && rc != PE_ERR_CANCELLED) return rc;
-    // the batch's AOV films, merged like the beauty film (Film::addBatch)
-    std::vector<float> h(n * 15);
-    PE_CUDA(cudaMemcpyAsync(h.data(), d->aovFilm, n * 15 * sizeof(float), cudaMemcpyDeviceToHost, d->stream));
-    PE_CUDA(cudaStreamSynchronize(d->stream));
-    float* sums[3] = {aovs->albedo_sum, aovs->normal_sum, aovs->alpha_sum};
-    uint32_t* cnts[3] = {aovs->albedo_count, aovs->normal_count, aovs->alpha_count};
-    float* sqs[3] = {aovs->albedo_sum_sq, nullptr, aovs->alpha_sum_sq};
-    for (int f = 0; f < 3; ++f) {
-        const float* fs = h.data() + static_cast<size_t>(f) * 5 * n;
-        const uint32_t* fc = reinterpret_cast<const uint32_t*>(fs + 3 * n);
-        const float* fq = fs + 4 * n;
-        if (sums[f])
-            for (size_t i = 0; i < 3 * n; ++i) sums[f][i] += fs[i];
-        if (cnts[f])
-            for (size_t i = 0; i < n; ++i) cnts[f][i] += fc[i];
-        if (sqs[f])
-            for (size_t i = 0; i < n; ++i) sqs[f][i] += fq[i];
-    }
-    return rc;
+    return renderTargets(d, cam, st, first, count, cancel, sumRgb, sampleCount, sumLumSq, aovs, passes, traced);
 }
 
 int32_t pe_device_render(pe_device* d, const pe_camera* cam, const pe_settings* st, int32_t first, int32_t count,

@@ -67,6 +67,10 @@ struct WaveLane {
     float4* aovA = nullptr;           // AOVs per slot (allocated on first use, in aovBufs)
     float4* aovN = nullptr;
     std::vector<DevBuf> aovBufs;
+    float4* pass = nullptr;           // render passes per slot and per shadow record (passBufs)
+    float4* shPass = nullptr;
+    int32_t passStride = 0;
+    std::vector<DevBuf> passBufs;
     int32_t* pathOf = nullptr;        // path regeneration buffers (in bufs)
     int32_t* freeQ = nullptr;
     float4* Lout = nullptr;
@@ -162,6 +166,7 @@ struct pe_device {
     std::vector<DevBuf> sceneBufs;
     SceneGPU scene{};
     bool hasScene = false;
+    int32_t lightGroups = 0;        // light groups of the scene set (its pass films need one each)
     TablesGPU* dTables = nullptr;
     TablesGPU hTables{};
     // pixel-filter inverse CDFs, one slot per (type, width) in use, least recently used replaced
@@ -198,6 +203,10 @@ struct pe_device {
     float* aovTarget = nullptr;     // AOV films of the render in progress (pe_device_render_aovs)
     float* aovFilm = nullptr;       // device AOV films (15 floats per pixel)
     size_t aovFilmPixels = 0;
+    float* passTarget = nullptr;    // render-pass films of the render in progress (pe_device_render_passes)
+    int32_t passStride = 0;         // its per-path block (PASS_GROUPS + light groups)
+    float* passFilm = nullptr;      // device pass films (5 floats per pixel per film)
+    size_t passFilmFloats = 0;
     int guideKind = 0;      // 0 none, 1 learned proposal, 2 SD-tree
     pe_dev::SdHost sd;
     uint64_t sceneSerial = 0; // counts pe_device_set_scene calls

@@ -715,6 +715,30 @@ void buildSpectral(TablesGPU& T) {
     T.spectralNorm[2] = norm.z;
 }
 
+// The data passes' colour of an id (idColor, renderer.cpp:252-271): 0 is black; otherwise the
+// splitmix64 finaliser of id + 0x9e3779b97f4a7c15 gives a hue, stepped by the golden-ratio
+// conjugate, shown at saturation 0.75 and value 1.
+V3 idColorOf(uint64_t id) {
+    if (id == 0) return mk(0.0f);
+    uint64_t z = id + 0x9e3779b97f4a7c15ull;
+    z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
+    z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
+    z ^= z >> 31;
+    const float hue = std::fmod(static_cast<float>(z >> 40) * 0x1p-24f + 0.618034f, 1.0f) * 6.0f;
+    const float frac = hue - std::floor(hue);
+    const float lo = 1.0f * (1.0f - 0.75f);
+    const float falling = 1.0f * (1.0f - 0.75f * frac);
+    const float rising = 1.0f * (1.0f - 0.75f * (1.0f - frac));
+    switch (static_cast<int>(hue) % 6) {
+        case 0: return mk(1.0f, rising, lo);
+        case 1: return mk(falling, 1.0f, lo);
+        case 2: return mk(lo, 1.0f, rising);
+        case 3: return mk(lo, falling, 1.0f);
+        case 4: return mk(rising, lo, 1.0f);
+        default: return mk(1.0f, lo, falling);
+    }
+}
+
 } // namespace
 
 const TablesGPU& staticTables() {
@@ -1006,6 +1030,40 @@ static int32_t buildScene(pe_scene* s) {
         }
     }
     if (s->env.present) buildEnvironment(s->env);
+    // light groups (scene.cpp:144-174): only when some light or the environment names one; then
+    // every light joins its group or "Default", the environment its group or "Env", at most 16
+    // groups (later names fall into group 0)
+    B.groupNames.clear();
+    B.lightGroup.clear();
+    B.envGroup = -1;
+    bool anyGroup = s->env.present && !s->envLightGroup.empty();
+    for (size_t i = 0; i < s->lights.size() && i < s->lightGroups.size(); ++i)
+        if (!s->lightGroups[i].empty()) anyGroup = true;
+    if (anyGroup) {
+        auto groupOf = [&](const std::string& name) -> int32_t {
+            for (size_t g = 0; g < B.groupNames.size(); ++g)
+                if (B.groupNames[g] == name) return static_cast<int32_t>(g);
+            if (B.groupNames.size() >= static_cast<size_t>(PE_MAX_LIGHT_GROUPS)) return 0;
+            B.groupNames.push_back(name);
+            return static_cast<int32_t>(B.groupNames.size() - 1);
+        };
+        B.lightGroup.resize(s->lights.size());
+        for (size_t i = 0; i < s->lights.size(); ++i) {
+            const std::string& g = i < s->lightGroups.size() ? s->lightGroups[i] : std::string();
+            B.lightGroup[i] = groupOf(g.empty() ? std::string("Default") : g);
+        }
+        if (s->env.present) B.envGroup = groupOf(s->envLightGroup.empty() ? std::string("Env") : s->envLightGroup);
+    }
+    // data-pass colours: shapes by their node uid, materials by their index + 1
+    B.idColor.resize(B.shapes.size() + B.materials.size());
+    for (size_t i = 0; i < B.shapes.size(); ++i) {
+        const V3 c = idColorOf(i < s->shapeUid.size() ? s->shapeUid[i] : 0ull);
+        B.idColor[i] = f4(c.x, c.y, c.z, 0.0f);
+    }
+    for (size_t m = 0; m < B.materials.size(); ++m) {
+        const V3 c = idColorOf(static_cast<uint64_t>(m) + 1ull);
+        B.idColor[B.shapes.size() + m] = f4(c.x, c.y, c.z, 0.0f);
+    }
     s->built = true;
     ++s->version;
     return PE_OK;
@@ -1172,6 +1230,45 @@ int32_t pe_scene_set_light_link(pe_scene* s, int32_t light, int32_t mode, const 
     l.shadowUids.assign(shadowUids, shadowUids + nShadow);
     s->built = false;
     return PE_OK;
+}
+
+int32_t pe_scene_set_light_group(pe_scene* s, int32_t light, const char* name) {
+    if (!s || light < -1) {
+        setError("pe_scene_set_light_group: bad argument");
+        return PE_ERR_INVALID;
+    }
+    const std::string g = name ? std::string(name) : std::string();
+    if (light < 0) {
+        s->envLightGroup = g;
+    } else {
+        if (s->lightGroups.size() <= static_cast<size_t>(light)) s->lightGroups.resize(static_cast<size_t>(light) + 1);
+        s->lightGroups[static_cast<size_t>(light)] = g;
+    }
+    s->built = false;
+    return PE_OK;
+}
+
+int32_t pe_scene_light_groups(const pe_scene* s, char* names, int32_t capacity) {
+    if (!s || capacity < 0 || (capacity > 0 && !names)) {
+        setError("pe_scene_light_groups: bad argument");
+        return PE_ERR_INVALID;
+    }
+    if (!s->built) {
+        setError("pe_scene_light_groups: scene not built");
+        return PE_ERR_NO_SCENE;
+    }
+    const std::vector<std::string>& g = s->build.groupNames;
+    if (names) {
+        std::string all;
+        for (const std::string& n : g) {
+            all += n;
+            all.push_back('\0');
+        }
+        const size_t k = std::min(all.size(), static_cast<size_t>(capacity));
+        std::memcpy(names, all.data(), k);
+        if (k < all.size() && capacity > 0) names[capacity - 1] = '\0';
+    }
+    return static_cast<int32_t>(g.size());
 }
 
 int32_t pe_scene_set_shadow_catcher(pe_scene* s, int32_t shape) {

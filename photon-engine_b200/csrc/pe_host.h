@@ -70,6 +70,13 @@ struct HostBuild {
     int32_t catcherShape = -1;   // shadow-catcher shape
     std::vector<LightLinkGPU> links; // per explicit light, empty without links
     int32_t hasLightLinks = 0, hasShadowLinks = 0;
+    // light groups (Scene::buildAccelerator, scene.cpp:144-174): names, group of each light, of
+    // the environment; empty when no light names a group
+    std::vector<std::string> groupNames;
+    std::vector<int32_t> lightGroup;
+    int32_t envGroup = -1;
+    // data-pass colours: object id of each shape, then material id of each material
+    std::vector<float4> idColor;
 };
 
 struct HostLightLink {
@@ -91,6 +98,8 @@ struct pe_scene {
     int32_t catcherShape = -1;   // Scene::setShadowCatcher
     std::vector<uint64_t> shapeUid;            // Scene::tagShape (0 = untagged)
     std::vector<pe::HostLightLink> lightLinks; // Light::setLightLink, by explicit light index
+    std::vector<std::string> lightGroups;      // Light::setLightGroup, by light index ("" = none)
+    std::string envLightGroup;                 // the environment's Light::setLightGroup
     pe::HostBuild build;
     uint64_t version = 0;
 };

@@ -46,6 +46,60 @@ __device__ __forceinline__ void queuePush(int32_t* queue, uint32_t* counter, boo
 
 // ---- generate: camera rays ------------------------------------------------------------------
 // Wave path `path` (its segment, sample and pixel) starts in `slot`.
+// ---- render passes (path_tracer.cpp:373-395) ---------------------------------------------------
+__device__ __forceinline__ float4* passBlock(const Paths& P, int path) {
+    return P.pass + static_cast<size_t>(path) * static_cast<size_t>(P.passStride);
+}
+__device__ __forceinline__ void passAdd(float4* q, V3 c) {
+    float4 v = *q;
+    v.x += c.x;
+    v.y += c.y;
+    v.z += c.z;
+    *q = v;
+}
+// Shares of f's diffuse, glossy and transmission groups, per channel; 1, 0, 0 where the groups
+// sum to zero (path_tracer.cpp:683-690, 803-811).
+__device__ __forceinline__ void lobeShares(const LobeSplit3& sp, V3 out[3]) {
+    const V3 sum = sp.diffuse + sp.glossy + sp.transmission;
+    const V3* parts[3] = {&sp.diffuse, &sp.glossy, &sp.transmission};
+    for (int k = 0; k < 3; ++k) {
+        out[k].x = sum.x > 0.0f ? parts[k]->x / sum.x : (k == 0 ? 1.0f : 0.0f);
+        out[k].y = sum.y > 0.0f ? parts[k]->y / sum.y : (k == 0 ? 1.0f : 0.0f);
+        out[k].z = sum.z > 0.0f ? parts[k]->z / sum.z : (k == 0 ? 1.0f : 0.0f);
+    }
+}
+// creditGroup: a term of light group `group` (ids outside the groups count for group 0).
+__device__ __noinline__ void creditGroup(const SceneGPU& S, const Paths& P, int path, int group, V3 added) {
+    if (S.nLightGroups <= 0 || isBlack(added)) return;
+    const int g = (group >= 0 && group < S.nLightGroups) ? group : 0;
+    if (g < PE_MAX_LIGHT_GROUPS) passAdd(passBlock(P, path) + PASS_GROUPS + g, added);
+}
+// creditPath: light reaching the path past its first surface, split by that surface's lobe
+// shares into the direct (found by the first bounce) or indirect passes.
+__device__ __noinline__ void creditPath(const Paths& P, int path, V3 added, bool direct) {
+    float4* b = passBlock(P, path);
+    for (int k = 0; k < 3; ++k) {
+        const float4 share = b[PASS_LOBES + k];
+        passAdd(b + 2 * k + (direct ? 0 : 1), added * mk(share.x, share.y, share.z));
+    }
+}
+__device__ __forceinline__ int lightGroupOf(const SceneGPU& S, int light) {
+    return light < 0 ? S.envGroup : (S.lightGroup ? S.lightGroup[light] : -1);
+}
+// A NEE term's passes: its light's group, and the direct passes by the vertex's own lobe shares
+// at the first surface (shares non-null), else the first surface's shares as indirect light.
+__device__ __noinline__ void creditNee(const SceneGPU& S, const Paths& P, int path, int light, V3 added,
+                                       const float4* shares) {
+    if (isBlack(added)) return;
+    creditGroup(S, P, path, lightGroupOf(S, light), added);
+    if (shares) {
+        float4* b = passBlock(P, path);
+        for (int k = 0; k < 3; ++k) passAdd(b + 2 * k, added * mk(shares[k].x, shares[k].y, shares[k].z));
+    } else {
+        creditPath(P, path, added, false);
+    }
+}
+
 __device__ __forceinline__ void generatePath(const SceneGPU& S, const Paths& P, const Wave& W, int slot, int path) {
     const TablesGPU* T = S.tables;
     const WaveSeg& A = W.segs[segOfSlot(W, path)];
@@ -71,6 +125,12 @@ __device__ __forceinline__ void generatePath(const SceneGPU& S, const Paths& P, 
     if (P.guiding) {
         P.guideMark[slot] = 0u;
         if (slot % P.guideStride == 0) P.guideRec[static_cast<size_t>(slot) * 6 + 4] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    }
+    if (P.pass) {
+        float4* b = passBlock(P, path);
+        for (int k = 0; k < P.passStride; ++k) b[k] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        b[PASS_LOBES] = make_float4(1.0f, 1.0f, 1.0f, 0.0f);
+        b[PASS_HIT] = make_float4(o.x, o.y, o.z, 0.0f);
     }
     if (P.pathOf) P.pathOf[slot] = path;
 }
@@ -289,6 +349,10 @@ __global__ void __launch_bounds__(128) kShadow(SceneGPU S, Paths P, const uint32
         L.y += c.y;
         L.z += c.z;
         P.L[slot] = L;
+        if (P.pass) {
+            const float4* shares = P.shPass + 3 * static_cast<size_t>(i);
+            creditNee(S, P, pathOfSlot(P, slot), light, c, shares[0].w != 0.0f ? shares : nullptr);
+        }
     }
     if (COUNT) {
         atomicAdd(&stats[2], static_cast<unsigned long long>(nodes));
@@ -296,11 +360,14 @@ __global__ void __launch_bounds__(128) kShadow(SceneGPU S, Paths P, const uint32
     }
 }
 
-__device__ __forceinline__ void addL(float4& L, V3 c) {
-    if (!isFinite3(c)) return; // accumulate(): non-finite terms are skipped (path_tracer.cpp:355-359)
+// accumulate(): adds a finite term and returns it; a non-finite one is skipped and counts as
+// black (path_tracer.cpp:355-359).
+__device__ __forceinline__ V3 addL(float4& L, V3 c) {
+    if (!isFinite3(c)) return mk(0.0f);
     L.x += c.x;
     L.y += c.y;
     L.z += c.z;
+    return c;
 }
 
 // russianRoulette (path_tracer.cpp:131-137): false ends the path.
@@ -685,6 +752,15 @@ __device__ __forceinline__ bool shadeSlot(const SceneGPU& S, const Paths& P, con
         if (!done) {
             // AOVs of the camera path's first surface past the skipped ones (path_tracer.cpp:440-443;
             // tracePixel, renderer.cpp:177-203): albedo, normal and coverage, or the background
+            // data passes of the first hit (tracePixel, renderer.cpp:162-176)
+            if ((flags & PF_FIRST_SEGMENT) && P.pass && hit) {
+                float4* b = passBlock(P, path);
+                const float4 o = b[PASS_HIT];
+                b[PASS_HIT] = make_float4(is.point.x, is.point.y, is.point.z, length(is.point - mk(o.x, o.y, o.z)));
+                const float4 oc = S.idColor[is.shape];
+                b[PASS_OBJECT] = make_float4(oc.x, oc.y, oc.z, 1.0f);
+                b[PASS_MATERIAL] = S.idColor[S.nShapes + is.material];
+            }
             if ((flags & PF_FIRST_SEGMENT) && P.aovA) {
                 const int path = pathOfSlot(P, slot);
                 if (hit) {
@@ -724,7 +800,11 @@ __device__ __forceinline__ bool shadeSlot(const SceneGPU& S, const Paths& P, con
                 // environment / background (path_tracer.cpp:482-514)
                 if (depth == 0 && S.bgMode != PE_BG_ENVIRONMENT) {
                     if (S.bgMode == PE_BG_COLOR) {
-                        addL(L, thr * m3f(S.bgColor));
+                        const V3 added = addL(L, thr * m3f(S.bgColor));
+                        if (P.pass) {
+                            passAdd(passBlock(P, path) + PASS_BACKGROUND, added);
+                            creditGroup(S, P, path, S.envGroup, added);
+                        }
                     } else if (passThroughs > 0 && P.aovA) {
                         // straight through thin glass to a transparent background: coverage is
                         // what the glass held back
@@ -748,14 +828,23 @@ __device__ __forceinline__ bool shadeSlot(const SceneGPU& S, const Paths& P, con
                         const float m = smax3(c.x, c.y, c.z);
                         if (m > A.clampIndirect) c = c * (A.clampIndirect / m);
                     }
-                    addL(L, c);
+                    const V3 added = addL(L, c);
+                    if (P.pass) {
+                        if (depth == 0) passAdd(passBlock(P, path) + PASS_BACKGROUND, added);
+                        else creditPath(P, path, added, depth == 1);
+                        creditGroup(S, P, path, S.envGroup, added);
+                    }
                 }
                 done = true;
             } else if (cameraRay && is.shape == S.catcherShape) {
                 // the shadow catcher ends the camera path with the shadowed background
                 float ratio = 1.0f;
                 const V3 bg = shadowCatcher(S, is, dir, shadowSamples, sb, ratio);
-                addL(L, thr * bg * ratio);
+                const V3 added = addL(L, thr * bg * ratio);
+                if (P.pass) {
+                    passAdd(passBlock(P, path) + PASS_BACKGROUND, added);
+                    creditGroup(S, P, path, S.envGroup, added);
+                }
                 if (depth == 0 && P.aovA) {
                     // the catcher's AOVs: the background it shows, its shadow as coverage
                     const V3 a = clamp3(bg, 0.0f, 1.0f);
@@ -797,7 +886,12 @@ __device__ __forceinline__ bool shadeSlot(const SceneGPU& S, const Paths& P, con
                             const float m = smax3(c.x, c.y, c.z);
                             if (m > A.clampIndirect) c = c * (A.clampIndirect / m);
                         }
-                        addL(L, c);
+                        const V3 added = addL(L, c);
+                        if (P.pass) {
+                            if (depth == 0) passAdd(passBlock(P, path) + PASS_EMISSION, added);
+                            else creditPath(P, path, added, depth == 1);
+                            creditGroup(S, P, path, li >= 0 ? lightGroupOf(S, li) : 0, added);
+                        }
                     }
                 }
                 if (depth >= A.maxDepth) done = true;
@@ -866,7 +960,9 @@ __device__ __forceinline__ bool shadeSlot(const SceneGPU& S, const Paths& P, con
                 float stMax;
                 if (!makeShadowRay(is, ls.wi, ls.distance, so, sd, stMax)) continue;
                 float bsdfPdf = 0.0f;
-                const V3 f = bsdfEvalPdf(T, mat, wo, ls.wi, sp, bsdfPdf, nullptr);
+                LobeSplit3 split;
+                const bool firstShares = P.pass && depth == 0;
+                const V3 f = bsdfEvalPdf(T, mat, wo, ls.wi, sp, bsdfPdf, firstShares ? &split : nullptr);
                 const float cosTheta = fabsf(dot(ls.wi, is.normal));
                 if (isBlack(f) || !(cosTheta > 0.0f)) continue;
                 const float lightPdf = lightPmf * ls.pdf;
@@ -886,6 +982,15 @@ __device__ __forceinline__ bool shadeSlot(const SceneGPU& S, const Paths& P, con
                             L.x += c.x;
                             L.y += c.y;
                             L.z += c.z;
+                            if (P.pass) {
+                                float4 shares[3];
+                                if (firstShares) {
+                                    V3 sh[3];
+                                    lobeShares(split, sh);
+                                    for (int k = 0; k < 3; ++k) shares[k] = make_float4(sh[k].x, sh[k].y, sh[k].z, 1.0f);
+                                }
+                                creditNee(S, P, path, fromEnv ? -1 : lightIndex, c, firstShares ? shares : nullptr);
+                            }
                         }
                     }
                 } else {
@@ -898,6 +1003,16 @@ __device__ __forceinline__ bool shadeSlot(const SceneGPU& S, const Paths& P, con
                     const uint32_t lightBits = static_cast<uint32_t>(fromEnv ? 0 : lightIndex + 1) << 1;
                     P.shC[pos] = make_float4(fLi.x, fLi.y, fLi.z, __uint_as_float((diffuseBounces >= 1 ? 1u : 0u) | lightBits));
                     P.shT[pos] = make_float4(thr.x, thr.y, thr.z, A.clampIndirect);
+                    if (P.pass) {
+                        float4* q = P.shPass + 3 * static_cast<size_t>(pos);
+                        if (firstShares) {
+                            V3 sh[3];
+                            lobeShares(split, sh);
+                            for (int k = 0; k < 3; ++k) q[k] = make_float4(sh[k].x, sh[k].y, sh[k].z, 1.0f);
+                        } else {
+                            q[0] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+                        }
+                    }
                 }
             }
         }
@@ -952,6 +1067,22 @@ __device__ __forceinline__ bool shadeSlot(const SceneGPU& S, const Paths& P, con
         } else {
             const V3 wi = bs.wi;
             const bool refracted = dot(wo, is.ng) * dot(wi, is.ng) < 0.0f;
+            if (P.pass && depth == 0) {
+                // the first surface's lobe shares: all later light splits by them (path_tracer.cpp:797-812)
+                V3 sh[3];
+                if (bs.delta) {
+                    sh[0] = mk(0.0f);
+                    sh[1] = mk(refracted ? 0.0f : 1.0f);
+                    sh[2] = mk(refracted ? 1.0f : 0.0f);
+                } else {
+                    LobeSplit3 split;
+                    float unusedPdf = 0.0f;
+                    (void)bsdfEvalPdf(T, mat, wo, wi, sp, unusedPdf, &split);
+                    lobeShares(split, sh);
+                }
+                float4* b = passBlock(P, path);
+                for (int k = 0; k < 3; ++k) b[PASS_LOBES + k] = make_float4(sh[k].x, sh[k].y, sh[k].z, 0.0f);
+            }
             const float cosTheta = fabsf(dot(wi, is.normal));
             const V3 thrBefore = thr;
             thr *= bs.f * (cosTheta / bs.pdf);
@@ -1150,6 +1281,50 @@ __device__ __noinline__ void filmAovs(const Paths& P, const WaveSeg& A, int p, i
     }
 }
 
+// The render-pass films of one pixel (addPasses, renderer.cpp:206-217), in sample order: light
+// passes, depth, ids and light groups by addSample, the position by addSampleSigned.
+__device__ __noinline__ void filmPasses(const Paths& P, const WaveSeg& A, int p, int pix) {
+    const size_t n = static_cast<size_t>(A.width) * static_cast<size_t>(A.height);
+    const int nFilms = PFILM_GROUPS + (P.passStride - PASS_GROUPS);
+    for (int f = 0; f < nFilms; ++f) {
+        float* fsum = A.pass + static_cast<size_t>(f) * 5 * n;
+        uint32_t* fcnt = reinterpret_cast<uint32_t*>(fsum + 3 * n);
+        float* fsq = fsum + 4 * n;
+        const int slotOf = f < PFILM_DEPTH ? f
+                         : f == PFILM_DEPTH || f == PFILM_POSITION ? PASS_HIT
+                         : f == PFILM_OBJECT ? PASS_OBJECT
+                         : f == PFILM_MATERIAL ? PASS_MATERIAL
+                                               : PASS_GROUPS + (f - PFILM_GROUPS);
+        const bool isSigned = f == PFILM_POSITION;
+        float r = fsum[3 * pix + 0], g = fsum[3 * pix + 1], b = fsum[3 * pix + 2], q = fsq[pix];
+        uint32_t c = fcnt[pix];
+        for (int s = 0; s < A.nSamples; ++s) {
+            const float4* blk = passBlock(P, A.slotFirst + s * A.nPix + p);
+            const float4 v4 = blk[slotOf];
+            V3 v = mk(v4.x, v4.y, v4.z);
+            if (f == PFILM_DEPTH || f == PFILM_POSITION) {
+                const bool hit = blk[PASS_OBJECT].w != 0.0f;
+                v = !hit ? mk(0.0f) : f == PFILM_DEPTH ? mk(v4.w) : v;
+            }
+            ++c;
+            if (!(finitef(v.x) && finitef(v.y) && finitef(v.z))) continue;
+            if (!isSigned && !(v.x >= 0.0f && v.y >= 0.0f && v.z >= 0.0f)) continue;
+            r += v.x;
+            g += v.y;
+            b += v.z;
+            if (!isSigned) {
+                const float lum = luminance(v);
+                q += lum * lum;
+            }
+        }
+        fsum[3 * pix + 0] = r;
+        fsum[3 * pix + 1] = g;
+        fsum[3 * pix + 2] = b;
+        fsq[pix] = q;
+        fcnt[pix] = c;
+    }
+}
+
 __global__ void kFilm(Paths P, Wave W, unsigned long long* rejected) {
     unsigned long long rej = 0;
     for (int wp = blockIdx.x * blockDim.x + threadIdx.x; wp < W.nPix; wp += gridDim.x * blockDim.x) {
@@ -1182,6 +1357,7 @@ __global__ void kFilm(Paths P, Wave W, unsigned long long* rejected) {
         A.sq[pix] = sq;
         A.cnt[pix] = c;
         if (A.aov && P.aovA) filmAovs(P, A, p, pix);
+        if (A.pass && P.pass) filmPasses(P, A, p, pix);
     }
     if (rej) atomicAdd(rejected, rej);
 }

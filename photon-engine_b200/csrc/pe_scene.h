@@ -198,6 +198,11 @@ struct SceneGPU {
     int32_t catcherShape;    // Scene::setShadowCatcher's shape, -1 none
     const LightLinkGPU* links; // per explicit light (null without light links)
     int32_t hasLightLinks, hasShadowLinks;
+    // render passes: light group of each light (null without groups), their number, the
+    // environment's group; data-pass colours (shapes, then materials)
+    const int32_t* lightGroup;
+    int32_t nLightGroups, envGroup;
+    const float4* idColor;
 };
 
 // Scene::isLightLinked / isShadowLinked for light `li` (explicit) and a receiver or blocker node.

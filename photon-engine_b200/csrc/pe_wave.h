@@ -89,6 +89,11 @@ struct Paths {
     // AOVs of each path (null unless requested): albedo + alpha, primary normal
     float4* aovA;
     float4* aovN;
+    // render passes of each path (null unless requested): passStride float4 per path, laid out
+    // as PassSlots says; shPass: 3 per shadow record, the lobe shares of a first-vertex NEE term
+    float4* pass;
+    float4* shPass;
+    int32_t passStride;
     // sweeps (continuous waves): a path alive for sweepAge bounces leaves the wavefront for a
     // tail-kernel launch on a side stream (sweepAge 0: off)
     int32_t* born;       // bounce at which each slot's path was injected
@@ -101,6 +106,15 @@ struct Paths {
     // [13] tail work cursor, [14] guide query rows, [15] training samples
     uint32_t* counters;
 };
+
+// A path's render-pass block (float4 slots): the eight light passes (LightPass order), the
+// lobe shares of the first bounce (firstLobe, path_tracer.cpp:375), the camera ray's origin and
+// then the first hit (xyz, w = distance), the object and material id colours (w of the object
+// slot: 1 on a hit), then one slot per light group.
+enum PassSlots { PASS_DIFFUSE_DIRECT = 0, PASS_EMISSION = 6, PASS_BACKGROUND = 7, PASS_LOBES = 8, PASS_HIT = 11,
+                 PASS_OBJECT = 12, PASS_MATERIAL = 13, PASS_GROUPS = 14 };
+// Films of the pass target, 5 floats per pixel each (sum 3n, count n, sum of squares n).
+enum PassFilms { PFILM_DEPTH = 8, PFILM_POSITION = 9, PFILM_OBJECT = 10, PFILM_MATERIAL = 11, PFILM_GROUPS = 12 };
 
 // Shading keys: 0 = miss, 1 + material type (Lambert, Disney, Dielectric, Mirror), 5 = random-walk step.
 constexpr int kShadeKeys = 6;
@@ -134,6 +148,7 @@ struct WaveSeg {
     uint32_t* cnt;
     float* sq;
     float* aov;             // AOV films (albedo, normal, alpha: each sum 3n, count n, sum of squares n), or null
+    float* pass;            // render-pass films (PassFilms order, 5n floats each), or null
     int slotFirst;
     int pixFirst;
     int flags;              // SegFlags

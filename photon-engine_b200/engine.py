@@ -175,9 +175,14 @@ class AreaLight:
         self.v = tuple(map(float, v))
         self.radiance = tuple(map(float, radiance))
         self.visible_to_camera = True
+        self.light_group = ""
 
     def set_visible_to_camera(self, v: bool):
         self.visible_to_camera = bool(v)
+
+    def set_light_group(self, name: str):
+        """Light::setLightGroup (light.h:85): the render pass (LG_<name>) this light's light goes to."""
+        self.light_group = str(name)
 
 
 class EnvironmentLight:
@@ -186,6 +191,11 @@ class EnvironmentLight:
         self.rotation = float(rotation)
         self.intensity = float(intensity)
         self.sun = None
+        self.light_group = ""
+
+    def set_light_group(self, name: str):
+        """Light::setLightGroup of the environment (its pass is LG_<name>; "Env" by default)."""
+        self.light_group = str(name)
 
     def set_sun(self, direction, cos_max, radiance):
         self.sun = (tuple(map(float, direction)), float(cos_max), tuple(map(float, radiance)))
@@ -218,6 +228,7 @@ class Scene:
         self.shadow_catcher: Optional[int] = None
         self.shape_tags: dict[int, int] = {}
         self.light_links: dict[int, tuple] = {}
+        self.light_groups: dict[int, str] = {}
 
     def __del__(self):
         try:
@@ -251,6 +262,21 @@ class Scene:
         listed node uids, 2 exclude them."""
         self.light_links[int(light)] = (int(mode), [int(u) for u in uids], int(shadow_mode),
                                         [int(u) for u in shadow_uids])
+
+    def set_light_group(self, light: int, name: str):
+        """Light::setLightGroup of light `light` (numbered as set_light_link numbers them); an
+        AreaLight's own set_light_group does the same for it."""
+        self.light_groups[int(light)] = str(name)
+
+    def light_group_names(self) -> list[str]:
+        """Scene::lightGroupNames of the built scene (scene.cpp:144-174)."""
+        lib = _lib()
+        n = lib.pe_scene_light_groups(self.handle, None, 0)
+        if n < 0:
+            capi.check(n)
+        buf = C.create_string_buffer(16 * 256)
+        lib.pe_scene_light_groups(self.handle, buf, len(buf))
+        return [x.decode() for x in buf.raw.split(b"\0")[:n]]
 
     def set_shadow_catcher(self, shape: Optional[int]):
         """Scene::setShadowCatcher: camera rays see this shape (an index as counted by
@@ -295,6 +321,19 @@ class Scene:
             capi.check(lib.pe_scene_set_shadow_catcher(h, int(self.shadow_catcher)))
         for shape, uid in self.shape_tags.items():
             capi.check(lib.pe_scene_tag_shape(h, shape, uid))
+        groups, li = {}, 0
+        for kind, obj in self.ops:
+            if kind == "mesh":
+                m = obj.material.struct
+                if m.type in (capi.PE_MAT_LAMBERT, capi.PE_MAT_DISNEY) and any(m.emission):
+                    li += obj.indices.shape[0]
+            else:
+                if obj.light_group:
+                    groups[li] = obj.light_group
+                li += 1
+        groups.update(self.light_groups)
+        for light, name in groups.items():
+            capi.check(lib.pe_scene_set_light_group(h, light, name.encode()))
         for light, (mode, uids, smode, suids) in self.light_links.items():
             a = (C.c_uint64 * max(1, len(uids)))(*uids)
             b = (C.c_uint64 * max(1, len(suids)))(*suids)
@@ -310,6 +349,8 @@ class Scene:
             if env.sun is not None:
                 d, cm, r = env.sun
                 capi.check(lib.pe_scene_set_sun(h, capi.f3(d), cm, capi.f3(r)))
+            if env.light_group:
+                capi.check(lib.pe_scene_set_light_group(h, -1, env.light_group.encode()))
         capi.check(lib.pe_scene_set_background(h, int(self.background.mode), capi.f3(self.background.color)))
         capi.check(lib.pe_scene_build(h))
         info = capi.pe_scene_info()
@@ -456,6 +497,54 @@ class AovFilms:
             f.resize(width, height)
 
 
+class LightPass(enum.IntEnum):
+    """LightPass (path_tracer.h:21-24); the films' channel names are lightPassName's."""
+    DiffuseDirect = 0
+    DiffuseIndirect = 1
+    GlossyDirect = 2
+    GlossyIndirect = 3
+    TransmissionDirect = 4
+    TransmissionIndirect = 5
+    Emission = 6
+    Background = 7
+
+
+class RenderPassFilms:
+    """RenderPassFilms (renderer.h:59-98): the eight light passes (their sum is the beauty film),
+    the data passes of the first hit (depth, position, object and material id colours) and one
+    film per light group, as (name, Film) pairs in Scene::lightGroupNames order."""
+
+    def __init__(self, width: int = 0, height: int = 0):
+        self.light = [Film(width, height) for _ in range(len(LightPass))]
+        self.depth = Film(width, height)
+        self.position = Film(width, height)
+        self.object_id = Film(width, height)
+        self.material_id = Film(width, height)
+        self.light_groups: list[tuple[str, Film]] = []
+
+    def init_light_groups(self, width: int, height: int, names):
+        self.light_groups = [(n, Film(width, height)) for n in names]
+
+    def resize(self, width: int, height: int):
+        for f in (*self.light, self.depth, self.position, self.object_id, self.material_id):
+            f.resize(width, height)
+        for _, f in self.light_groups:
+            f.resize(width, height)
+
+    def to_c(self) -> capi.pe_pass_films:
+        def arr(f: Film):
+            return capi.pe_film_arrays(capi.fptr(f.sum), capi.uptr(f.count), capi.fptr(f.sum_sq))
+        out = capi.pe_pass_films()
+        for k, f in enumerate(self.light):
+            out.light[k] = arr(f)
+        out.depth, out.position = arr(self.depth), arr(self.position)
+        out.object_id, out.material_id = arr(self.object_id), arr(self.material_id)
+        out.n_groups = len(self.light_groups)
+        for g, (_, f) in enumerate(self.light_groups[:capi.PE_MAX_LIGHT_GROUPS]):
+            out.groups[g] = arr(f)
+        return out
+
+
 @dataclasses.dataclass
 class RenderTargets:
     beauty: Optional[Film] = None
@@ -472,7 +561,7 @@ class SampleBatchResult:
 @dataclasses.dataclass
 class DeviceFeatures:
     aovs: bool = True
-    light_passes: bool = False
+    light_passes: bool = True
     adaptive_sampling: bool = False
 
 
@@ -569,11 +658,33 @@ class CudaDevice:
             flag = cancel if isinstance(cancel, C.c_int32) else C.c_int32(1 if cancel else 0)
         traced = C.c_uint64(0)
         aovs = targets.aovs
+        passes = targets.passes
         with self._lock:
             self._sync_guiding(settings)
-            if aovs is not None:
-                aovs.resize(film.width, film.height) if aovs.albedo.width != film.width or \
-                    aovs.albedo.height != film.height else None
+            if aovs is not None and (aovs.albedo.width != film.width or aovs.albedo.height != film.height):
+                aovs.resize(film.width, film.height)
+            if passes is not None:
+                # renderSamples sizes the passes from the film and re-forms the light groups when
+                # they do not match the scene's (renderer.cpp:401-406)
+                if passes.depth.width != film.width or passes.depth.height != film.height:
+                    passes.resize(film.width, film.height)
+                names = self._scene.light_group_names() if self._scene is not None else []
+                if [n for n, _ in passes.light_groups] != names or any(
+                        f.width != film.width or f.height != film.height for _, f in passes.light_groups):
+                    passes.init_light_groups(film.width, film.height, names)
+                pout = passes.to_c()
+                aout = None
+                if aovs is not None:
+                    aout = capi.pe_aov_films(capi.fptr(aovs.albedo.sum), capi.uptr(aovs.albedo.count),
+                                             capi.fptr(aovs.albedo.sum_sq), capi.fptr(aovs.normal.sum),
+                                             capi.uptr(aovs.normal.count), capi.fptr(aovs.alpha.sum),
+                                             capi.uptr(aovs.alpha.count), capi.fptr(aovs.alpha.sum_sq))
+                rc = _lib().pe_device_render_passes(self._h, C.byref(camera.describe_gpu()), C.byref(st), first_sample,
+                                                    count, C.byref(flag) if flag is not None else None,
+                                                    capi.fptr(film.sum), capi.uptr(film.count), capi.fptr(film.sum_sq),
+                                                    C.byref(aout) if aout is not None else None, C.byref(pout),
+                                                    C.byref(traced))
+            elif aovs is not None:
                 out = capi.pe_aov_films(capi.fptr(aovs.albedo.sum), capi.uptr(aovs.albedo.count),
                                         capi.fptr(aovs.albedo.sum_sq), capi.fptr(aovs.normal.sum),
                                         capi.uptr(aovs.normal.count), capi.fptr(aovs.alpha.sum),
@@ -835,6 +946,7 @@ class RenderSession:
         self.camera = None
         self.film = Film()
         self.aovs: Optional[AovFilms] = None
+        self.passes: Optional[RenderPassFilms] = None
         self.samples = 0
         self.traced = 0
         self.warnings: list[str] = []
@@ -857,6 +969,7 @@ class RenderSession:
             self.warnings.append(f"{name}: adaptive sampling is not supported; every pixel reaches the target")
         self.film.resize(max(1, settings.width), max(1, settings.height))
         self.aovs = AovFilms(max(1, settings.width), max(1, settings.height)) if self.config.aovs else None
+        self.passes = RenderPassFilms(max(1, settings.width), max(1, settings.height)) if self.config.passes else None
         self.samples = 0
         self.traced = 0
         self._sps = 0.0
@@ -887,7 +1000,7 @@ class RenderSession:
             return False
         count = self.next_batch()
         t0 = time.perf_counter()
-        r = self.device.render(self.camera, self.settings, RenderTargets(beauty=self.film, aovs=self.aovs), self.samples,
+        r = self.device.render(self.camera, self.settings, RenderTargets(beauty=self.film, aovs=self.aovs, passes=self.passes), self.samples,
                                count, cancel)
         self.last_batch_seconds = time.perf_counter() - t0
         self.traced += r.samples_traced

@@ -38,7 +38,7 @@
 extern "C" {
 #endif
 
-#define PE_ABI_VERSION 5
+#define PE_ABI_VERSION 6
 
 typedef enum pe_status {
     PE_OK = 0,
@@ -128,7 +128,9 @@ typedef struct pe_settings {
     float clamp_indirect;   /* 0 = off */
     uint64_t seed;          /* Owen-Sobol seed (reference renderSamples: 12345) */
     float ao_strength;      /* RenderSettings::aoStrength: contact AO at camera hits; 0 = off */
-    int32_t pad;
+    int32_t adaptive_sampling;    /* RenderSettings::adaptiveSampling: clean pixels stop early */
+    float noise_threshold;        /* relative standard error target (reference default 0.02; >= 1e-4 used) */
+    int32_t min_adaptive_samples; /* samples before any decision (reference default 16; >= 2 used) */
 } pe_settings;
 
 /* ---- scene builder --------------------------------------------------------- */

@@ -69,6 +69,10 @@ def _load(fast: bool = False):
         "ref_render_guided": (C.c_int32, [P, C.c_void_p, C.c_void_p, C.c_int32, C.c_int32, C.c_int32, FP, UP]),
         "ref_scene_set_shadow_catcher": (C.c_int32, [P, C.c_int32]),
         "ref_scene_set_light_group": (C.c_int32, [P, C.c_int32, C.c_char_p]),
+        "ref_film_create": (P, [C.c_int32, C.c_int32]),
+        "ref_film_destroy": (None, [P]),
+        "ref_film_export": (C.c_int32, [P, C.c_int32, C.c_int32, FP, UP]),
+        "ref_render_film": (C.c_int64, [P, C.c_void_p, C.c_void_p, C.c_int32, C.c_int32, C.c_int32, P]),
         "ref_render_passes": (C.c_int32, [P, C.c_void_p, C.c_void_p, C.c_int32, C.c_int32, C.c_int32, FP, UP, FP, FP,
                                           FP, C.c_int32]),
         "ref_render_aovs": (C.c_int32, [P, C.c_void_p, C.c_void_p, C.c_int32, C.c_int32, C.c_int32, FP, UP, FP, FP,
@@ -97,6 +101,27 @@ def _f(a):
 
 def _f3(v):
     return (C.c_float * 3)(*[float(x) for x in v])
+
+
+class RefFilm:
+    """A reference Film kept across render calls."""
+
+    def __init__(self, width: int, height: int, fast: bool = False):
+        self.lib = _load(fast)
+        self.width, self.height = width, height
+        self.h = self.lib.ref_film_create(width, height)
+
+    def __del__(self):
+        try:
+            self.lib.ref_film_destroy(self.h)
+        except Exception:
+            pass
+
+    def mean_and_counts(self):
+        mean = np.zeros((self.height, self.width, 3), np.float32)
+        cnt = np.zeros((self.height, self.width), np.uint32)
+        self.lib.ref_film_export(self.h, self.width, self.height, _f(mean), cnt.ctypes.data_as(UP))
+        return mean, cnt
 
 
 class RefScene:
@@ -195,6 +220,12 @@ class RefScene:
         fn(self.h, C.byref(camera.describe_gpu()), C.byref(settings.to_c()), first, count, threads, _f(mean),
            cnt.ctypes.data_as(UP))
         return mean, cnt
+
+    def render_into(self, film: "RefFilm", camera, settings, first: int, count: int, threads: int = 0) -> int:
+        """Renderer::renderSamples (seed 12345) adding samples [first, first+count) to a kept film
+        (adaptive sampling reads it); returns the samples traced."""
+        return int(self.lib.ref_render_film(self.h, C.byref(camera.describe_gpu()), C.byref(settings.to_c()), first,
+                                            count, threads, film.h))
 
     def render_passes(self, camera, settings, first: int, count: int, threads: int = 0):
         """Renderer::renderSamples with RenderPassFilms (seed 12345): mean beauty, counts, the eight

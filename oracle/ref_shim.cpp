@@ -156,6 +156,9 @@ RenderSettings toSettings(const pe_settings& st, int threads) {
     s.filter.width = st.filter_width;
     s.clampIndirect = st.clamp_indirect;
     s.aoStrength = st.ao_strength;
+    s.adaptiveSampling = st.adaptive_sampling != 0;
+    s.noiseThreshold = st.noise_threshold;
+    s.minAdaptiveSamples = st.min_adaptive_samples;
     s.numThreads = threads;
     return s;
 }
@@ -356,6 +359,27 @@ int32_t ref_render(void* s, const pe_camera* cam, const pe_settings* st, int32_t
     renderer.renderSamples(rs->scene, camera, settings, film, first, count, nullptr);
     exportFilm(film, st->width, st->height, mean_rgb, counts);
     return 0;
+}
+
+// A Film kept across calls (adaptive sampling reads the accumulated film).
+void* ref_film_create(int32_t w, int32_t h) { return new Film(w, h); }
+void ref_film_destroy(void* f) { delete static_cast<Film*>(f); }
+int32_t ref_film_export(void* f, int32_t w, int32_t h, float* mean_rgb, uint32_t* counts) {
+    exportFilm(*static_cast<Film*>(f), w, h, mean_rgb, counts);
+    return 0;
+}
+
+// Renderer::renderSamples (seed 12345) adding samples [first, first+count) to a kept film;
+// returns SampleBatchResult::samplesTraced.
+int64_t ref_render_film(void* s, const pe_camera* cam, const pe_settings* st, int32_t first, int32_t count,
+                        int32_t threads, void* film) {
+    auto* rs = static_cast<RefScene*>(s);
+    DescCamera camera(*cam);
+    RenderSettings settings = toSettings(*st, threads > 0 ? threads : hardwareThreads());
+    Renderer renderer;
+    const SampleBatchResult r =
+        renderer.renderSamples(rs->scene, camera, settings, *static_cast<Film*>(film), first, count, nullptr);
+    return static_cast<int64_t>(r.samplesTraced);
 }
 
 // Renderer::renderSamples with AovFilms (seed 12345): the mean beauty, albedo, normal and alpha

@@ -52,7 +52,7 @@ class pe_settings(C.Structure):
     _fields_ = [("width", C.c_int32), ("height", C.c_int32), ("max_bounces", C.c_int32), ("rr_depth", C.c_int32),
                 ("shadow_quality", C.c_int32), ("filter_type", C.c_int32), ("filter_width", C.c_float),
                 ("clamp_indirect", C.c_float), ("seed", C.c_uint64), ("ao_strength", C.c_float),
-                ("pad", C.c_int32)]
+                ("adaptive_sampling", C.c_int32), ("noise_threshold", C.c_float), ("min_adaptive_samples", C.c_int32)]
 
 
 class pe_scene_info(C.Structure):

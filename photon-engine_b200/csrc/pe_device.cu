@@ -573,10 +573,12 @@ int32_t loopFilm(pe_device* d, LaneLoop& L, const WaveSeg* dSeg, int nPix) {
 // The wavefront render of samples [first, first+count) over `tile` into the film (sum, cnt, sq)
 // on the device, with path state in `P` (room for `capacity` slots): waves of one segment each.
 // With `timing` the closest-hit / shade / any-hit / tail launches are bracketed by events.
+// With `pixList` the pixels rendered are the nList film pixels it names (tile: the whole frame).
 int32_t renderWaves(pe_device* d, const pe_camera* cam, const pe_settings* st, int first, int count,
                     const volatile int32_t* cancel, float* sum, uint32_t* cnt, float* sq, Paths* scratch, size_t capacity,
-                    bool timing, Tile tile) {
-    const size_t npix = static_cast<size_t>(tile.w) * static_cast<size_t>(tile.h);
+                    bool timing, Tile tile, const int32_t* pixList = nullptr, size_t nList = 0) {
+    const size_t npix = pixList ? nList : static_cast<size_t>(tile.w) * static_cast<size_t>(tile.h);
+    if (npix == 0) return PE_OK;
     // unguided waves on the lanes' own state regenerate paths: kStreamFactor × the slots per wave
     const bool regenWaves = !scratch && !d->guide.mode && d->guideKind != 2 && !d->aovTarget && !d->passTarget;
     const size_t pathCap = regenWaves ? capacity * kStreamFactor : capacity;
@@ -599,6 +601,7 @@ int32_t renderWaves(pe_device* d, const pe_camera* cam, const pe_settings* st, i
     base.sq = sq;
     base.aov = scratch ? nullptr : d->aovTarget;
     base.pass = scratch ? nullptr : d->passTarget;
+    base.pixList = pixList;
     RenderTimer tm;
     tm.timing = timing;
     bool cancelled = false;
@@ -645,6 +648,151 @@ int32_t renderWaves(pe_device* d, const pe_camera* cam, const pe_settings* st, i
         setError("render cancelled");
         return PE_ERR_CANCELLED;
     }
+    return PE_OK;
+}
+
+// ---- adaptive sampling (renderer.cpp:442-467, 498-500) ------------------------------------------
+// Film::relativeError (film.cpp:100-109): the relative standard error of the pixel's mean
+// luminance; 1e30 below two samples.
+__device__ __forceinline__ float pixelRelError(const float* sum, const uint32_t* cnt, const float* sq, int i) {
+    const uint32_t n = cnt[i];
+    if (n < 2) return 1e30f;
+    const float nf = static_cast<float>(n);
+    const float mean = (0.212671f * sum[3 * i + 0] + 0.715160f * sum[3 * i + 1] + 0.072169f * sum[3 * i + 2]) / nf;
+    const float meanSq = sq[i] / nf;
+    const float var = fmaxf(0.0f, meanSq - mean * mean) * nf / static_cast<float>(n - 1);
+    return sqrtf(var / nf) / (fmaxf(mean, 0.0f) + 0.01f);
+}
+
+// Warp-aggregated append of the lanes whose `keep` is set (all 32 lanes of the warp call it).
+__device__ __forceinline__ void appendPixel(int32_t* list, uint32_t* count, bool keep, int32_t pixel) {
+    const unsigned mask = __ballot_sync(0xFFFFFFFFu, keep);
+    if (!mask) return;
+    const int lane = threadIdx.x & 31;
+    const int leader = __ffs(mask) - 1;
+    uint32_t base = 0;
+    if (lane == leader) base = atomicAdd(count, static_cast<uint32_t>(__popc(mask)));
+    base = __shfl_sync(0xFFFFFFFFu, base, leader);
+    if (keep) list[base + __popc(mask & ((1u << lane) - 1u))] = pixel;
+}
+
+// Pixels whose accumulated error is below the threshold.
+__global__ void kAdaptiveClean(const float* sum, const uint32_t* cnt, const float* sq, int n, float threshold,
+                               uint8_t* clean) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        clean[i] = pixelRelError(sum, cnt, sq, i) < threshold ? 1 : 0;
+}
+
+// The batch's pixels: all of them, or (with `clean`) those that are not clean together with all
+// eight neighbours (edges clamped).  Blocks step over whole blocks of pixels, so every warp runs
+// each iteration with all its lanes.
+__global__ void kAdaptiveList(const uint8_t* clean, int w, int h, int32_t* list, uint32_t* count) {
+    const int n = w * h;
+    const int stride = gridDim.x * blockDim.x;
+    for (int base = blockIdx.x * blockDim.x; base < n; base += stride) {
+        const int i = base + static_cast<int>(threadIdx.x);
+        bool keep = i < n;
+        if (keep && clean) {
+            const int x = i % w, y = i / w;
+            bool all = true;
+            for (int dy = -1; dy <= 1 && all; ++dy)
+                for (int dx = -1; dx <= 1 && all; ++dx) {
+                    const int nx = min(max(x + dx, 0), w - 1), ny = min(max(y + dy, 0), h - 1);
+                    all = clean[ny * w + nx] != 0;
+                }
+            keep = !all;
+        }
+        appendPixel(list, count, keep, i);
+    }
+}
+
+// The listed pixels that go on after a check: those whose error is not yet below the threshold.
+__global__ void kAdaptiveStop(const float* sum, const uint32_t* cnt, const float* sq, const int32_t* in, int nIn,
+                              float threshold, int32_t* out, uint32_t* count) {
+    const int stride = gridDim.x * blockDim.x;
+    for (int base = blockIdx.x * blockDim.x; base < nIn; base += stride) {
+        const int j = base + static_cast<int>(threadIdx.x);
+        const int px = j < nIn ? in[j] : -1;
+        appendPixel(out, count, px >= 0 && !(pixelRelError(sum, cnt, sq, px) < threshold), px);
+    }
+}
+
+// Adaptive render of samples [first, first+count) into the device film, which holds the pixels'
+// accumulated samples: pixels that are clean together with their neighbours skip the batch (once
+// the film holds minAdaptiveSamples), and after every sample index that is a multiple of 8 (at
+// least minAdaptiveSamples, before the batch's end) the pixels whose error fell below the
+// threshold stop.  Renderer::renderSamples decides the same per pixel (renderer.cpp:442-467,
+// 498-500), so every pixel takes the same samples and the film the same sums.
+int32_t renderAdaptive(pe_device* d, const pe_camera* cam, const pe_settings* st, int first, int count,
+                       const volatile int32_t* cancel, uint64_t* traced) {
+    if (d->guideKind == 2) {
+        setError("adaptive sampling together with SD-tree guiding is not supported by this device");
+        return PE_ERR_INVALID;
+    }
+    const int w = st->width, h = st->height;
+    const size_t n = static_cast<size_t>(w) * static_cast<size_t>(h);
+    if (d->adaptPixels < n) {
+        cudaFree(d->adaptList[0]);
+        cudaFree(d->adaptList[1]);
+        cudaFree(d->adaptClean);
+        d->adaptList[0] = d->adaptList[1] = nullptr;
+        d->adaptClean = nullptr;
+        d->adaptPixels = 0;
+        PE_CUDA(cudaMalloc(&d->adaptList[0], n * sizeof(int32_t)));
+        PE_CUDA(cudaMalloc(&d->adaptList[1], n * sizeof(int32_t)));
+        PE_CUDA(cudaMalloc(&d->adaptClean, n));
+        d->adaptPixels = n;
+    }
+    if (!d->adaptCount) PE_CUDA(cudaMalloc(&d->adaptCount, 2 * sizeof(uint32_t)));
+    const float threshold = std::max(1e-4f, st->noise_threshold);
+    const int minSpp = std::max(2, st->min_adaptive_samples);
+    const int threads = 256;
+    auto gridFor = [&](size_t items) {
+        return static_cast<int>(std::max<size_t>(1, std::min<size_t>((items + threads - 1) / threads, 148 * 16)));
+    };
+    cudaStream_t cs = d->stream;
+    PE_CUDA(cudaMemsetAsync(d->adaptCount, 0, 2 * sizeof(uint32_t), cs));
+    const bool skip = first >= minSpp;
+    if (skip)
+        kAdaptiveClean<<<gridFor(n), threads, 0, cs>>>(d->fSum, d->fCnt, d->fSq, static_cast<int>(n), threshold,
+                                                       d->adaptClean);
+    kAdaptiveList<<<gridFor(n), threads, 0, cs>>>(skip ? d->adaptClean : nullptr, w, h, d->adaptList[0], d->adaptCount);
+    PE_CUDA(cudaGetLastError());
+    uint32_t active = 0;
+    PE_CUDA(cudaMemcpyAsync(&active, d->adaptCount, sizeof(uint32_t), cudaMemcpyDeviceToHost, cs));
+    PE_CUDA(cudaStreamSynchronize(cs));
+    int cur = first, which = 0;
+    const int end = first + count;
+    uint64_t done = 0;
+    while (cur < end && active > 0) {
+        // the next check: the first multiple of 8 after cur that is at least minSpp, before the end
+        int e = end;
+        for (int k = (cur / 8 + 1) * 8; k < end; k += 8)
+            if (k >= minSpp) {
+                e = k;
+                break;
+            }
+        const int32_t rc = renderWaves(d, cam, st, cur, e - cur, cancel, d->fSum, d->fCnt, d->fSq, nullptr, d->capacity,
+                                       true, Tile{0, 0, w, h}, d->adaptList[which], active);
+        if (rc != PE_OK) {
+            if (traced) *traced = done;
+            return rc;
+        }
+        done += static_cast<uint64_t>(active) * static_cast<uint64_t>(e - cur);
+        cur = e;
+        if (cur < end) {
+            uint32_t* outCount = d->adaptCount + 1 - which;
+            PE_CUDA(cudaMemsetAsync(outCount, 0, sizeof(uint32_t), cs));
+            kAdaptiveStop<<<gridFor(active), threads, 0, cs>>>(d->fSum, d->fCnt, d->fSq, d->adaptList[which],
+                                                               static_cast<int>(active), threshold,
+                                                               d->adaptList[1 - which], outCount);
+            PE_CUDA(cudaGetLastError());
+            PE_CUDA(cudaMemcpyAsync(&active, outCount, sizeof(uint32_t), cudaMemcpyDeviceToHost, cs));
+            PE_CUDA(cudaStreamSynchronize(cs));
+            which = 1 - which;
+        }
+    }
+    if (traced) *traced = done;
     return PE_OK;
 }
 
@@ -926,6 +1074,10 @@ void pe_device_destroy(pe_device* d) {
     if (d->evFilm) cudaEventDestroy(d->evFilm);
     cudaFree(d->aovFilm);
     cudaFree(d->passFilm);
+    cudaFree(d->adaptList[0]);
+    cudaFree(d->adaptList[1]);
+    cudaFree(d->adaptClean);
+    cudaFree(d->adaptCount);
     cudaFree(d->fSum);
     cudaFree(d->fCnt);
     cudaFree(d->fSq);
@@ -998,6 +1150,7 @@ int32_t pe_device_render_resident(pe_device* d, const pe_camera* cam, const pe_s
     PE_CUDA(cudaSetDevice(d->ordinal));
     if ((rc = ensureFilm(d, st->width, st->height))) return rc;
     if ((rc = ensureCapacity(d, kWaveSlots))) return rc;
+    if (st->adaptive_sampling) return renderAdaptive(d, cam, st, first, count, cancel, nullptr);
     return renderWaves(d, cam, st, first, count, cancel, d->fSum, d->fCnt, d->fSq, nullptr, d->capacity, true,
                        Tile{0, 0, st->width, st->height});
 }
@@ -1184,6 +1337,23 @@ int32_t pe_device_render(pe_device* d, const pe_camera* cam, const pe_settings* 
     if (count <= 0) return PE_OK;
     PE_CUDA(cudaSetDevice(d->ordinal));
     if ((rc = ensureFilm(d, st->width, st->height))) return rc;
+    if (st->adaptive_sampling) {
+        // the decisions read the accumulated film: the caller's film goes to the device, takes
+        // the batch's samples there in sample order, and comes back whole
+        if (!sumRgb || !sampleCount || !sumLumSq) {
+            setError("adaptive sampling needs the film's sums, counts and squared-luminance sums");
+            return PE_ERR_INVALID;
+        }
+        const size_t n = static_cast<size_t>(st->width) * static_cast<size_t>(st->height);
+        if ((rc = ensureCapacity(d, kWaveSlots))) return rc;
+        PE_CUDA(cudaMemcpyAsync(d->fSum, sumRgb, n * 3 * sizeof(float), cudaMemcpyHostToDevice, d->stream));
+        PE_CUDA(cudaMemcpyAsync(d->fCnt, sampleCount, n * sizeof(uint32_t), cudaMemcpyHostToDevice, d->stream));
+        PE_CUDA(cudaMemcpyAsync(d->fSq, sumLumSq, n * sizeof(float), cudaMemcpyHostToDevice, d->stream));
+        const int32_t ar = renderAdaptive(d, cam, st, first, count, cancel, traced);
+        if (ar != PE_OK && ar != PE_ERR_CANCELLED) return ar;
+        if ((rc = pe_device_film_read(d, sumRgb, sampleCount, sumLumSq))) return rc;
+        return ar;
+    }
     if ((rc = pe_device_film_clear(d))) return rc;
     if ((rc = ensureCapacity(d, kWaveSlots))) return rc;
     const int32_t rr = renderWaves(d, cam, st, first, count, cancel, d->fSum, d->fCnt, d->fSq, nullptr, d->capacity,
@@ -1260,6 +1430,10 @@ int32_t pe_device_render_tile_noalloc(pe_device* d, const pe_camera* cam, const 
     if (!d->noAllocBase) {
         setError("pe_device_render_tile_noalloc: scratch unavailable: " + d->noAllocError);
         return PE_ERR_CUDA;
+    }
+    if (st->adaptive_sampling) {
+        setError("pe_device_render_tile_noalloc: adaptive sampling needs the device's own film (pe_device_render)");
+        return PE_ERR_INVALID;
     }
     if (count <= 0) return PE_OK;
     PE_CUDA(cudaSetDevice(d->ordinal));

@@ -166,6 +166,11 @@ struct pe_device {
     std::vector<DevBuf> sceneBufs;
     SceneGPU scene{};
     bool hasScene = false;
+    // adaptive sampling: the pixels still sampled (two lists), the clean-pixel mask, list sizes
+    int32_t* adaptList[2] = {nullptr, nullptr};
+    uint8_t* adaptClean = nullptr;
+    uint32_t* adaptCount = nullptr;
+    size_t adaptPixels = 0;
     int32_t lightGroups = 0;        // light groups of the scene set (its pass films need one each)
     TablesGPU* dTables = nullptr;
     TablesGPU hTables{};

@@ -106,7 +106,9 @@ __device__ __forceinline__ void generatePath(const SceneGPU& S, const Paths& P, 
     const int local = path - A.slotFirst;
     const int sOff = local / A.nPix;
     const int pix = A.pixelFirst + (local - sOff * A.nPix);
-    const int x = A.tileX + pix % A.tileW, y = A.tileY + pix / A.tileW;
+    const int fp = A.pixList ? A.pixList[pix] : -1;
+    const int x = fp >= 0 ? fp % A.width : A.tileX + pix % A.tileW;
+    const int y = fp >= 0 ? fp / A.width : A.tileY + pix / A.tileW;
     Sobol sb;
     sb.pixelHash = pixelHashOf(A.seed, x, y);
     sb.revIndex = rev32(static_cast<uint32_t>(A.sampleFirst + sOff));
@@ -1157,7 +1159,7 @@ __device__ __forceinline__ bool shadeSlot(const SceneGPU& S, const Paths& P, con
 
 // Consumes the rays binned by shading key (segment by segment, so a warp mostly shades one
 // material kind) and appends the continuing paths to nextQueue.
-__global__ void __launch_bounds__(128, 4) kShade(SceneGPU S, Paths P, Wave W, int32_t* nextQueue, uint32_t* nextCount) {
+__global__ void __launch_bounds__(128, 6) kShade(SceneGPU S, Paths P, Wave W, int32_t* nextQueue, uint32_t* nextCount) {
     uint32_t seg[kShadeKeys];
     int n = 0;
     for (int k = 0; k < kShadeKeys; ++k) {
@@ -1331,7 +1333,7 @@ __global__ void kFilm(Paths P, Wave W, unsigned long long* rejected) {
         const WaveSeg& A = W.segs[segOfPixel(W, wp)];
         const int p = wp - A.pixFirst;
         const int tp = A.pixelFirst + p;
-        const int pix = (A.tileY + tp / A.tileW) * A.width + A.tileX + tp % A.tileW;
+        const int pix = A.pixList ? A.pixList[tp] : (A.tileY + tp / A.tileW) * A.width + A.tileX + tp % A.tileW;
         float* sum = A.sum;
         float sr = sum[3 * pix + 0], sg = sum[3 * pix + 1], sbb = sum[3 * pix + 2];
         float sq = A.sq[pix];

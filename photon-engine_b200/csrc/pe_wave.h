@@ -137,6 +137,7 @@ struct WaveSeg {
     CamDev cam;
     int width, height;      // film
     int tileX, tileY, tileW; // rendered rectangle of the film (whole frame: 0, 0, width)
+    const int32_t* pixList;  // film pixel (y·width + x) of each tile-linear pixel, or null: the rectangle
     int pixelFirst, nPix;   // range of tile-linear pixel indices in this wave
     int sampleFirst, nSamples;
     uint64_t seed;

@@ -439,11 +439,14 @@ class RenderSettings:
     rr_depth: int = 3            # PathTracer(maxBounces, 3, ...) in renderSamples
     path_guiding: bool = False
     ao_strength: float = 0.0     # RenderSettings::aoStrength: contact AO at camera hits
+    noise_threshold: float = 0.02    # adaptive: relative standard error target (render_settings.h:31)
+    min_adaptive_samples: int = 16   # adaptive: samples before any decision (render_settings.h:32)
 
     def to_c(self) -> capi.pe_settings:
         return capi.pe_settings(self.width, self.height, self.max_bounces, self.rr_depth, self.shadow_quality,
                                 int(self.filter_type), self.filter_width, self.clamp_indirect, self.seed,
-                                float(self.ao_strength), 0)
+                                float(self.ao_strength), 1 if self.adaptive_sampling else 0,
+                                float(self.noise_threshold), int(self.min_adaptive_samples))
 
 
 class Film:
@@ -562,7 +565,7 @@ class SampleBatchResult:
 class DeviceFeatures:
     aovs: bool = True
     light_passes: bool = True
-    adaptive_sampling: bool = False
+    adaptive_sampling: bool = True
 
 
 class DeviceKind(enum.Enum):
@@ -949,6 +952,7 @@ class RenderSession:
         self.passes: Optional[RenderPassFilms] = None
         self.samples = 0
         self.traced = 0
+        self._converged = False
         self.warnings: list[str] = []
         self._sps = 0.0
         self.last_batch_seconds = 0.0
@@ -972,6 +976,7 @@ class RenderSession:
         self.passes = RenderPassFilms(max(1, settings.width), max(1, settings.height)) if self.config.passes else None
         self.samples = 0
         self.traced = 0
+        self._converged = False
         self._sps = 0.0
         self._start = time.perf_counter()
 
@@ -979,6 +984,8 @@ class RenderSession:
         return time.perf_counter() - self._start
 
     def finished(self) -> bool:
+        if self._converged:
+            return True
         if self.config.target_spp > 0 and self.samples >= self.config.target_spp:
             return True
         return self.config.time_limit > 0.0 and self.samples > 0 and self.seconds() >= self.config.time_limit
@@ -1009,7 +1016,15 @@ class RenderSession:
         self.samples += count
         per = self.last_batch_seconds / count
         self._sps = 0.5 * (self._sps + per) if self._sps > 0.0 else per
+        # adaptive sampling: a batch that traced nothing means every pixel is clean
+        # (render_session.cpp:99)
+        if self.settings.adaptive_sampling and r.samples_traced == 0:
+            self._converged = True
         return True
+
+    def converged(self) -> bool:
+        """RenderSession::converged: adaptive sampling left no pixel to sample."""
+        return self._converged
 
     def average_samples(self) -> float:
         px = float(self.film.width * self.film.height)

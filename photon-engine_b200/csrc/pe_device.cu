@@ -328,10 +328,15 @@ int32_t runWave(pe_device* d, int lane, Paths& P, int nSegs, int nSlots, int nPi
                 if ((rc = timerEvent(d, tm, t0)) || (rc = timerEvent(d, tm, t1))) return rc;
                 PE_CUDA(cudaEventRecord(t0, cs));
             }
-            if (d->counting)
-                kTail<true><<<grid, kTailBlock, 0, cs>>>(S, P, W, qIn, cIn, &P.counters[CNT_WORK_TAIL], d->dStats);
+            const bool out = P.aovA || P.pass;
+            if (d->counting && out)
+                kTail<true, true><<<grid, kTailBlock, 0, cs>>>(S, P, W, qIn, cIn, &P.counters[CNT_WORK_TAIL], d->dStats);
+            else if (d->counting)
+                kTail<true, false><<<grid, kTailBlock, 0, cs>>>(S, P, W, qIn, cIn, &P.counters[CNT_WORK_TAIL], d->dStats);
+            else if (out)
+                kTail<false, true><<<grid, kTailBlock, 0, cs>>>(S, P, W, qIn, cIn, &P.counters[CNT_WORK_TAIL], d->dStats);
             else
-                kTail<false><<<grid, kTailBlock, 0, cs>>>(S, P, W, qIn, cIn, &P.counters[CNT_WORK_TAIL], d->dStats);
+                kTail<false, false><<<grid, kTailBlock, 0, cs>>>(S, P, W, qIn, cIn, &P.counters[CNT_WORK_TAIL], d->dStats);
             if (tm.timing) {
                 PE_CUDA(cudaEventRecord(t1, cs));
                 tm.tail.push_back({tm.evUsed - 2, tm.evUsed - 1});
@@ -358,7 +363,10 @@ int32_t runWave(pe_device* d, int lane, Paths& P, int nSegs, int nSlots, int nPi
             kIntersect<false><<<d->blocksIntersect, 128, 0, cs>>>(S, P, qIn, cIn, d->dStats);
         if (P.guiding == 2 && (rc = guideQueries(d, cs, P, W, qIn, cIn))) return rc;
         if (tm.timing) PE_CUDA(cudaEventRecord(e1, cs));
-        kShade<<<d->blocksShade, 128, 0, cs>>>(S, P, W, qOut, cOut);
+        if (P.aovA || P.pass)
+            kShade<true><<<d->blocksShade, 128, 0, cs>>>(S, P, W, qOut, cOut);
+        else
+            kShade<false><<<d->blocksShade, 128, 0, cs>>>(S, P, W, qOut, cOut);
         if (tm.timing) PE_CUDA(cudaEventRecord(e2, cs));
         if (d->counting)
             kShadow<true><<<d->blocksShadow, 128, 0, cs>>>(S, P, &P.counters[CNT_SHADOW], d->dStats);
@@ -484,7 +492,7 @@ int32_t loopBounce(pe_device* d, LaneLoop& L, const Wave& W, uint32_t* hSegLeft,
     P.sweepQ = sweep >= 0 ? L.sweepBuf[sweep] : nullptr;
     P.iter = L.iter;
     kIntersect<false><<<d->blocksIntersect, 128, 0, cs>>>(S, P, L.qIn, L.cIn, d->dStats);
-    kShade<<<d->blocksShade, 128, 0, cs>>>(S, P, W, L.qOut, L.cOut);
+    kShade<false><<<d->blocksShade, 128, 0, cs>>>(S, P, W, L.qOut, L.cOut);
     kShadow<false><<<d->blocksShadow, 128, 0, cs>>>(S, P, &P.counters[CNT_SHADOW], d->dStats);
     PE_CUDA(cudaMemcpyAsync(ln.hCounters, P.counters, CNT_TOTAL * sizeof(uint32_t), cudaMemcpyDeviceToHost, cs));
     // segment counts as of the previous bounce's flushes (one bounce behind)
@@ -508,7 +516,7 @@ int32_t loopBounce(pe_device* d, LaneLoop& L, const Wave& W, uint32_t* hSegLeft,
         PE_CUDA(cudaStreamWaitEvent(L.side, L.evReady[sweep], 0));
         PE_CUDA(cudaMemsetAsync(&L.sweepCursor[sweep], 0, sizeof(uint32_t), L.side));
         const int grid = static_cast<int>(std::min<int64_t>(d->blocksTail, (swept + kTailBlock - 1) / kTailBlock));
-        kTail<false><<<grid, kTailBlock, 0, L.side>>>(S, P, W, L.sweepBuf[sweep], &L.sweepCnt[sweep],
+        kTail<false, false><<<grid, kTailBlock, 0, L.side>>>(S, P, W, L.sweepBuf[sweep], &L.sweepCnt[sweep],
                                                        &L.sweepCursor[sweep], d->dStats);
         kFlush<<<d->prop.multiProcessorCount * 4, 256, 0, L.side>>>(P, W, L.sweepBuf[sweep], &L.sweepCnt[sweep]);
         PE_CUDA(cudaEventRecord(L.evDone[sweep], L.side));
@@ -533,7 +541,7 @@ int32_t loopTail(pe_device* d, LaneLoop& L, const Wave& W) {
     Paths& P = ln.paths;
     const cudaStream_t cs = ln.stream;
     const int grid = static_cast<int>(std::min<int64_t>(d->blocksTail, (static_cast<int64_t>(L.live) + kTailBlock - 1) / kTailBlock));
-    kTail<false><<<grid, kTailBlock, 0, cs>>>(L.scene, P, W, L.qIn, L.cIn, &P.counters[CNT_WORK_TAIL], d->dStats);
+    kTail<false, false><<<grid, kTailBlock, 0, cs>>>(L.scene, P, W, L.qIn, L.cIn, &P.counters[CNT_WORK_TAIL], d->dStats);
     kFlush<<<d->prop.multiProcessorCount * 4, 256, 0, cs>>>(P, W, L.qIn, L.cIn);
     L.live = 0;
     PE_CUDA(cudaGetLastError());
@@ -1031,11 +1039,11 @@ pe_device* pe_device_create(int32_t ordinal, char* err, size_t errLen) {
     const int sm = d->prop.multiProcessorCount;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kIntersect<false>, 128, 0);
     d->blocksIntersect = sm * std::max(1, b);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kShade, 128, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kShade<false>, 128, 0);
     d->blocksShade = sm * std::max(1, b);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kShadow<false>, 128, 0);
     d->blocksShadow = sm * std::max(1, b);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kTail<true>, kTailBlock, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kTail<true, false>, kTailBlock, 0);
     d->blocksTail = sm * std::max(1, b);
     const cudaError_t le = cudaGetLastError();
     if (le != cudaSuccess) {

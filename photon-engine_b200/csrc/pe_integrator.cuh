@@ -631,7 +631,7 @@ __device__ __noinline__ V3 shadowCatcher(const SceneGPU& S, const Isect& is, V3 
 // vertex, or a ray scattered inside a medium (an ordinary ray with specularBounce set).  NEE
 // shadow rays go to the any-hit queue, or with INLINE_SHADOW are traced here and their terms
 // added to L at once, in the same order.  Returns whether the path goes on.
-template <bool INLINE_SHADOW, bool COUNT>
+template <bool INLINE_SHADOW, bool COUNT, bool OUT>
 __device__ __forceinline__ bool shadeSlot(const SceneGPU& S, const Paths& P, const WaveSeg& A, int slot, int path,
                                           uint32_t& shNodes, uint32_t& shTris, uint32_t& shRays) {
     const TablesGPU* T = S.tables;
@@ -755,7 +755,7 @@ __device__ __forceinline__ bool shadeSlot(const SceneGPU& S, const Paths& P, con
             // AOVs of the camera path's first surface past the skipped ones (path_tracer.cpp:440-443;
             // tracePixel, renderer.cpp:177-203): albedo, normal and coverage, or the background
             // data passes of the first hit (tracePixel, renderer.cpp:162-176)
-            if ((flags & PF_FIRST_SEGMENT) && P.pass && hit) {
+            if ((flags & PF_FIRST_SEGMENT) && (OUT && P.pass) && hit) {
                 float4* b = passBlock(P, path);
                 const float4 o = b[PASS_HIT];
                 b[PASS_HIT] = make_float4(is.point.x, is.point.y, is.point.z, length(is.point - mk(o.x, o.y, o.z)));
@@ -763,7 +763,7 @@ __device__ __forceinline__ bool shadeSlot(const SceneGPU& S, const Paths& P, con
                 b[PASS_OBJECT] = make_float4(oc.x, oc.y, oc.z, 1.0f);
                 b[PASS_MATERIAL] = S.idColor[S.nShapes + is.material];
             }
-            if ((flags & PF_FIRST_SEGMENT) && P.aovA) {
+            if ((flags & PF_FIRST_SEGMENT) && OUT && P.aovA) {
                 const int path = pathOfSlot(P, slot);
                 if (hit) {
                     const V3 a = clamp3(m3f(S.materials[is.material].base), 0.0f, 1.0f);
@@ -803,11 +803,11 @@ __device__ __forceinline__ bool shadeSlot(const SceneGPU& S, const Paths& P, con
                 if (depth == 0 && S.bgMode != PE_BG_ENVIRONMENT) {
                     if (S.bgMode == PE_BG_COLOR) {
                         const V3 added = addL(L, thr * m3f(S.bgColor));
-                        if (P.pass) {
+                        if ((OUT && P.pass)) {
                             passAdd(passBlock(P, path) + PASS_BACKGROUND, added);
                             creditGroup(S, P, path, S.envGroup, added);
                         }
-                    } else if (passThroughs > 0 && P.aovA) {
+                    } else if (passThroughs > 0 && OUT && P.aovA) {
                         // straight through thin glass to a transparent background: coverage is
                         // what the glass held back
                         P.aovA[pathOfSlot(P, slot)].w = smax(0.0f, 1.0f - luminance(thr));
@@ -831,7 +831,7 @@ __device__ __forceinline__ bool shadeSlot(const SceneGPU& S, const Paths& P, con
                         if (m > A.clampIndirect) c = c * (A.clampIndirect / m);
                     }
                     const V3 added = addL(L, c);
-                    if (P.pass) {
+                    if ((OUT && P.pass)) {
                         if (depth == 0) passAdd(passBlock(P, path) + PASS_BACKGROUND, added);
                         else creditPath(P, path, added, depth == 1);
                         creditGroup(S, P, path, S.envGroup, added);
@@ -843,11 +843,11 @@ __device__ __forceinline__ bool shadeSlot(const SceneGPU& S, const Paths& P, con
                 float ratio = 1.0f;
                 const V3 bg = shadowCatcher(S, is, dir, shadowSamples, sb, ratio);
                 const V3 added = addL(L, thr * bg * ratio);
-                if (P.pass) {
+                if ((OUT && P.pass)) {
                     passAdd(passBlock(P, path) + PASS_BACKGROUND, added);
                     creditGroup(S, P, path, S.envGroup, added);
                 }
-                if (depth == 0 && P.aovA) {
+                if (depth == 0 && OUT && P.aovA) {
                     // the catcher's AOVs: the background it shows, its shadow as coverage
                     const V3 a = clamp3(bg, 0.0f, 1.0f);
                     P.aovA[pathOfSlot(P, slot)] =
@@ -889,7 +889,7 @@ __device__ __forceinline__ bool shadeSlot(const SceneGPU& S, const Paths& P, con
                             if (m > A.clampIndirect) c = c * (A.clampIndirect / m);
                         }
                         const V3 added = addL(L, c);
-                        if (P.pass) {
+                        if ((OUT && P.pass)) {
                             if (depth == 0) passAdd(passBlock(P, path) + PASS_EMISSION, added);
                             else creditPath(P, path, added, depth == 1);
                             creditGroup(S, P, path, li >= 0 ? lightGroupOf(S, li) : 0, added);
@@ -963,7 +963,7 @@ __device__ __forceinline__ bool shadeSlot(const SceneGPU& S, const Paths& P, con
                 if (!makeShadowRay(is, ls.wi, ls.distance, so, sd, stMax)) continue;
                 float bsdfPdf = 0.0f;
                 LobeSplit3 split;
-                const bool firstShares = P.pass && depth == 0;
+                const bool firstShares = (OUT && P.pass) && depth == 0;
                 const V3 f = bsdfEvalPdf(T, mat, wo, ls.wi, sp, bsdfPdf, firstShares ? &split : nullptr);
                 const float cosTheta = fabsf(dot(ls.wi, is.normal));
                 if (isBlack(f) || !(cosTheta > 0.0f)) continue;
@@ -984,7 +984,7 @@ __device__ __forceinline__ bool shadeSlot(const SceneGPU& S, const Paths& P, con
                             L.x += c.x;
                             L.y += c.y;
                             L.z += c.z;
-                            if (P.pass) {
+                            if ((OUT && P.pass)) {
                                 float4 shares[3];
                                 if (firstShares) {
                                     V3 sh[3];
@@ -1005,7 +1005,7 @@ __device__ __forceinline__ bool shadeSlot(const SceneGPU& S, const Paths& P, con
                     const uint32_t lightBits = static_cast<uint32_t>(fromEnv ? 0 : lightIndex + 1) << 1;
                     P.shC[pos] = make_float4(fLi.x, fLi.y, fLi.z, __uint_as_float((diffuseBounces >= 1 ? 1u : 0u) | lightBits));
                     P.shT[pos] = make_float4(thr.x, thr.y, thr.z, A.clampIndirect);
-                    if (P.pass) {
+                    if ((OUT && P.pass)) {
                         float4* q = P.shPass + 3 * static_cast<size_t>(pos);
                         if (firstShares) {
                             V3 sh[3];
@@ -1069,7 +1069,7 @@ __device__ __forceinline__ bool shadeSlot(const SceneGPU& S, const Paths& P, con
         } else {
             const V3 wi = bs.wi;
             const bool refracted = dot(wo, is.ng) * dot(wi, is.ng) < 0.0f;
-            if (P.pass && depth == 0) {
+            if ((OUT && P.pass) && depth == 0) {
                 // the first surface's lobe shares: all later light splits by them (path_tracer.cpp:797-812)
                 V3 sh[3];
                 if (bs.delta) {
@@ -1159,6 +1159,8 @@ __device__ __forceinline__ bool shadeSlot(const SceneGPU& S, const Paths& P, con
 
 // Consumes the rays binned by shading key (segment by segment, so a warp mostly shades one
 // material kind) and appends the continuing paths to nextQueue.
+// OUT: the wave records AOVs or render passes (their code is compiled out of the plain kernel).
+template <bool OUT>
 __global__ void __launch_bounds__(128, 6) kShade(SceneGPU S, Paths P, Wave W, int32_t* nextQueue, uint32_t* nextCount) {
     uint32_t seg[kShadeKeys];
     int n = 0;
@@ -1184,7 +1186,7 @@ __global__ void __launch_bounds__(128, 6) kShade(SceneGPU S, Paths P, Wave W, in
             slot = P.sortQ[static_cast<size_t>(k) * P.capacity + j];
             const int path = pathOfSlot(P, slot);
             const WaveSeg& A = W.segs[segOfSlot(W, path)];
-            cont = shadeSlot<false, false>(S, P, A, slot, path, unused0, unused1, unused2);
+            cont = shadeSlot<false, false, OUT>(S, P, A, slot, path, unused0, unused1, unused2);
             sweepable = (A.flags & SEG_SWEEP) != 0;
         }
         // a continuous wave sweeps its interactive paths that have lived sweepAge bounces into a
@@ -1206,7 +1208,7 @@ __global__ void __launch_bounds__(128, 6) kShade(SceneGPU S, Paths P, Wave W, in
 // the next wave running on the other lane.
 constexpr int kTailBlock = 32;
 
-template <bool COUNT>
+template <bool COUNT, bool OUT>
 __global__ void __launch_bounds__(kTailBlock) kTail(SceneGPU S, Paths P, Wave W, const int32_t* queue, const uint32_t* count,
                                              uint32_t* cursor, unsigned long long* stats) {
     const int n = static_cast<int>(*count);
@@ -1228,7 +1230,7 @@ __global__ void __launch_bounds__(kTailBlock) kTail(SceneGPU S, Paths P, Wave W,
                                               1e30f, nodes, tris);
             ++rays;
             P.hit[slot] = make_float4(h.t, h.u, h.v, __int_as_float(h.prim));
-            if (!shadeSlot<true, COUNT>(S, P, A, slot, path, shNodes, shTris, shRays)) break;
+            if (!shadeSlot<true, COUNT, OUT>(S, P, A, slot, path, shNodes, shTris, shRays)) break;
         }
     }
     if (COUNT) {

@@ -38,7 +38,7 @@
 extern "C" {
 #endif
 
-#define PE_ABI_VERSION 6
+#define PE_ABI_VERSION 7
 
 typedef enum pe_status {
     PE_OK = 0,
@@ -97,6 +97,11 @@ typedef struct pe_material {
     int32_t has_scattering; /* setScattering called */
     /* any type */
     float round_edge_radius; /* Material::setRoundEdgeRadius (material.h:136); 0 = off */
+    /* Disney image maps (DisneyMaterial::set{Albedo,Roughness,Metalness,Normal}Image, disney.h:142-145):
+     * indices from pe_scene_add_texture, -1 none; roughness reads green, metalness blue */
+    int32_t albedo_texture, roughness_texture, metalness_texture, normal_texture;
+    int32_t texture_mapping;  /* 0 UV, 1 box projection (DisneyMaterial::TextureMapping) */
+    float texture_scale;      /* DisneyMaterial::setTextureScale (≥ 1e-4) */
 } pe_material;
 
 /* Camera as the reference's Camera::describeGpu() (src/camera/camera.h:17-29). */
@@ -172,6 +177,10 @@ int32_t pe_scene_set_light_link(pe_scene* s, int32_t light, int32_t mode, const 
  * order they were added: one per pe_scene_add_mesh, two per pe_scene_add_area_light (its two
  * triangles, as Scene::addLight adds them).  Call before pe_scene_build. */
 int32_t pe_scene_set_shadow_catcher(pe_scene* s, int32_t shape);
+/* An RGB float image (w*h*3, row 0 first) for the Disney image maps; returns its index (>= 0)
+ * or a negative status.  Lookups are Image::sampleBilinear's (src/core/image/image.cpp:98-225):
+ * bilinear, wrapping, without mipmaps. */
+int32_t pe_scene_add_texture(pe_scene* s, const float* rgb, int32_t width, int32_t height);
 /* Light::setLightGroup (src/lights/light.h:85) of light `light` (the numbering of
  * pe_scene_set_light_link), or of the environment when light == -1; "" or NULL clears it.
  * Scene::buildAccelerator forms the groups (src/engine/scene.cpp:144-174): none unless some

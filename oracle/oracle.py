@@ -69,6 +69,7 @@ def _load(fast: bool = False):
         "ref_render_guided": (C.c_int32, [P, C.c_void_p, C.c_void_p, C.c_int32, C.c_int32, C.c_int32, FP, UP]),
         "ref_scene_set_shadow_catcher": (C.c_int32, [P, C.c_int32]),
         "ref_scene_set_light_group": (C.c_int32, [P, C.c_int32, C.c_char_p]),
+        "ref_scene_add_texture": (C.c_int32, [P, FP, C.c_int32, C.c_int32]),
         "ref_film_create": (P, [C.c_int32, C.c_int32]),
         "ref_film_destroy": (None, [P]),
         "ref_film_export": (C.c_int32, [P, C.c_int32, C.c_int32, FP, UP]),
@@ -130,10 +131,15 @@ class RefScene:
     def __init__(self, scene, fast: bool = False):
         self.lib = _load(fast)
         self.h = self.lib.ref_scene_create()
+        tex_index = {}
+        for img in (scene.textures() if hasattr(scene, "textures") else []):
+            tex_index[id(img)] = self.lib.ref_scene_add_texture(self.h, _f(img), img.shape[1], img.shape[0])
         mat_index = {}
         for kind, obj in scene.ops:
             if kind == "mesh" and id(obj.material) not in mat_index:
-                idx = self.lib.ref_scene_add_material(self.h, C.byref(obj.material.struct))
+                struct = obj.material.struct_with(tex_index) if hasattr(obj.material, "struct_with") \
+                    else obj.material.struct
+                idx = self.lib.ref_scene_add_material(self.h, C.byref(struct))
                 if idx < 0:
                     raise RuntimeError("reference rejected a material")
                 mat_index[id(obj.material)] = idx

@@ -84,6 +84,7 @@ struct RefScene {
     std::unordered_map<const void*, int> shapeIndex; // hitObject → insertion index
     int nextShape = 0;
     std::string envGroup; // the environment's light group, applied at build
+    std::vector<std::shared_ptr<Image>> textures; // ref_scene_add_texture
     void indexNewShapes() {
         const auto& shapes = scene.shapes();
         for (size_t i = static_cast<size_t>(nextShape); i < shapes.size(); ++i)
@@ -195,10 +196,37 @@ void* ref_scene_create() {
 
 void ref_scene_destroy(void* s) { delete static_cast<RefScene*>(s); }
 
+// An RGB float image (row 0 first) for the Disney image maps; returns its index.
+int32_t ref_scene_add_texture(void* s, const float* rgb, int32_t w, int32_t h) {
+    auto* rs = static_cast<RefScene*>(s);
+    auto img = std::make_shared<Image>(w, h);
+    for (int y = 0; y < h; ++y)
+        for (int x = 0; x < w; ++x) {
+            const float* px = rgb + 3 * (static_cast<size_t>(y) * static_cast<size_t>(w) + static_cast<size_t>(x));
+            img->setPixel(x, y, Color3f(px[0], px[1], px[2]));
+        }
+    rs->textures.push_back(img);
+    return static_cast<int32_t>(rs->textures.size() - 1);
+}
+
 int32_t ref_scene_add_material(void* s, const pe_material* m) {
     auto* rs = static_cast<RefScene*>(s);
     auto mat = makeMaterial(*m);
     if (!mat) return -1;
+    if (m->type == PE_MAT_DISNEY) {
+        // image maps, mapping and scale (DisneyMaterial::set*Image / setTextureMapping / setTextureScale)
+        auto* d = static_cast<DisneyMaterial*>(mat.get());
+        auto tex = [&](int32_t i) -> std::shared_ptr<Image> {
+            return i >= 0 && i < static_cast<int32_t>(rs->textures.size()) ? rs->textures[static_cast<size_t>(i)] : nullptr;
+        };
+        if (auto t = tex(m->albedo_texture)) d->setAlbedoImage(t);
+        if (auto t = tex(m->roughness_texture)) d->setRoughnessImage(t);
+        if (auto t = tex(m->metalness_texture)) d->setMetalnessImage(t);
+        if (auto t = tex(m->normal_texture)) d->setNormalImage(t);
+        d->setTextureMapping(m->texture_mapping == 1 ? DisneyMaterial::TextureMapping::Box
+                                                     : DisneyMaterial::TextureMapping::UV);
+        d->setTextureScale(m->texture_scale);
+    }
     rs->materials.push_back(mat);
     rs->scene.retainMaterial(mat);
     return static_cast<int32_t>(rs->materials.size() - 1);

@@ -40,6 +40,8 @@ class pe_material(C.Structure):
         ("thin_walled", C.c_int32), ("film_thickness", C.c_float),
         ("has_absorption", C.c_int32), ("has_scattering", C.c_int32),
         ("round_edge_radius", C.c_float),
+        ("albedo_texture", C.c_int32), ("roughness_texture", C.c_int32), ("metalness_texture", C.c_int32),
+        ("normal_texture", C.c_int32), ("texture_mapping", C.c_int32), ("texture_scale", C.c_float),
     ]
 
 
@@ -167,6 +169,7 @@ SIGNATURES = {
     "pe_scene_create": (P, []),
     "pe_scene_destroy": (None, [P]),
     "pe_scene_add_material": (C.c_int32, [P, C.POINTER(pe_material)]),
+    "pe_scene_add_texture": (C.c_int32, [P, C.POINTER(C.c_float), C.c_int32, C.c_int32]),
     "pe_scene_add_mesh": (C.c_int32, [P, FP, C.c_uint32, FP, FP, UP, C.c_uint32, C.c_int32]),
     "pe_scene_add_area_light": (C.c_int32, [P, FP, FP, FP, FP, C.c_int32]),
     "pe_scene_set_environment": (C.c_int32, [P, FP, C.c_int32, C.c_int32, C.c_float, C.c_float]),

@@ -231,6 +231,8 @@ PE_HD V3 eonEval(V3 rho, float r, V3 wi, V3 wo) {
 // ---------------------------------------------------------------------------------------------
 // Shading point as seen by a material (the SurfaceInteraction fields materials read).
 struct ShadePoint {
+    V2 uv;                  // surface uv (texture lookups)
+    const TexGPU* textures; // the scene's image textures (may be null)
     V3 p;        // point
     V3 n;        // shading normal, facing the incoming ray
     V3 ng;       // outward geometric normal
@@ -302,6 +304,75 @@ PE_HD void resolveFlake(V3 point, float size, float density, float rough, Disney
     p.flakeNormal = normalize(toWorld(f, mk(sinT * cosf(phi), sinT * sinf(phi), cosT)));
 }
 
+// Image::sampleLevel(0, u, v) (image.cpp:168-225): bilinear with wrap, texel centres at +0.5.
+PE_HD V3 texBilinear(const TexGPU& t, float u, float v) {
+    const int w = t.width, h = t.height;
+    if (w <= 0 || h <= 0) return mk(0.0f);
+    u = u - floorf(u);
+    v = v - floorf(v);
+    const float x = u * static_cast<float>(w) - 0.5f;
+    const float y = v * static_cast<float>(h) - 0.5f;
+    const int x0 = static_cast<int>(floorf(x));
+    const int y0 = static_cast<int>(floorf(y));
+    const float fx = x - static_cast<float>(x0);
+    const float fy = y - static_cast<float>(y0);
+    auto wrap = [](int i, int n) {
+        i %= n;
+        return i < 0 ? i + n : i;
+    };
+    const int xa = wrap(x0, w), xb = wrap(x0 + 1, w), ya = wrap(y0, h), yb = wrap(y0 + 1, h);
+    auto at = [&](int px, int py) {
+        const float* c = t.texels + (static_cast<size_t>(py) * static_cast<size_t>(w) + static_cast<size_t>(px)) * 3;
+        return mk(c[0], c[1], c[2]);
+    };
+    const V3 c0 = at(xa, ya) * (1.0f - fx) + at(xb, ya) * fx;
+    const V3 c1 = at(xa, yb) * (1.0f - fx) + at(xb, yb) * fx;
+    return c0 * (1.0f - fy) + c1 * fy;
+}
+
+// DisneyMaterial::textureCoord (disney.cpp:517-526): the uv scaled, or a box projection of the
+// point onto the plane across the geometric normal's largest axis.
+PE_HD V2 textureCoord(const MatGPU& m, const ShadePoint& sp) {
+    V2 uv;
+    if (m.texMapping == 0) {
+        uv = sp.uv;
+    } else {
+        const V3 n = len2(sp.ng) > 0.0f ? sp.ng : sp.n;
+        const float ax = fabsf(n.x), ay = fabsf(n.y), az = fabsf(n.z);
+        const V3 p = sp.p;
+        uv = (ax >= ay && ax >= az) ? mk2(p.z, p.y) : (ay >= az ? mk2(p.x, p.z) : mk2(p.x, p.y));
+    }
+    return mk2(uv.x * m.texScale, uv.y * m.texScale);
+}
+
+// The image maps of DisneyMaterial::resolve (disney.cpp:565-596): base colour, roughness (green),
+// metalness (blue) and a tangent-space normal map.
+PE_HDN void applyTextures(const MatGPU& m, const ShadePoint& sp, V3& base, float& roughness, float& metallic,
+                          V3& normal) {
+    const V2 uv = textureCoord(m, sp);
+    if (m.texAlbedo >= 0) base = texBilinear(sp.textures[m.texAlbedo], uv.x, uv.y);
+    if (m.texRoughness >= 0) roughness = smax(0.001f, texBilinear(sp.textures[m.texRoughness], uv.x, uv.y).y);
+    if (m.texMetalness >= 0) metallic = sclamp(texBilinear(sp.textures[m.texMetalness], uv.x, uv.y).z, 0.0f, 1.0f);
+    if (m.texNormal >= 0) {
+        const V3 c = texBilinear(sp.textures[m.texNormal], uv.x, uv.y);
+        const V3 nTs = mk(c.x * 2.0f - 1.0f, c.y * 2.0f - 1.0f, c.z * 2.0f - 1.0f);
+        const V3 N = sp.n;
+        V3 T = sp.tangent;
+        if (len2(T) < 1e-8f) T = frameFromNormal(N).s;
+        V3 B = cross(N, T);
+        if (len2(B) < 1e-8f) {
+            const Frame f = frameFromNormal(N);
+            B = f.t;
+            T = f.s;
+        } else {
+            B = normalize(B);
+            T = normalize(cross(B, N));
+        }
+        normal = normalize(T * nTs.x + B * nTs.y + N * nTs.z);
+        if (dot(normal, N) < 0.0f) normal = -normal;
+    }
+}
+
 PE_HD DisneyParams disneyResolve(const MatGPU& m, const ShadePoint& sp) {
     DisneyParams p;
     p.base = m3(m.base);
@@ -325,6 +396,8 @@ PE_HD DisneyParams disneyResolve(const MatGPU& m, const ShadePoint& sp) {
     p.normal = sp.n;
     p.tangent = sp.tangent;
     p.frontFace = sp.frontFace;
+    if (sp.textures && (m.texAlbedo >= 0 || m.texRoughness >= 0 || m.texMetalness >= 0 || m.texNormal >= 0))
+        applyTextures(m, sp, p.base, p.roughness, p.metallic, p.normal);
     p.edgeTint = m3(m.edgeTint);
     p.thinFilmThickness = m.thinFilmThickness;
     p.thinFilmIor = m.thinFilmIor;

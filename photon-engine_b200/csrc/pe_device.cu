@@ -849,6 +849,8 @@ __global__ void kBsdfProbe(SceneGPU S, int material, const pe_bsdf_query* q, int
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const MatGPU& m = S.materials[material];
         ShadePoint sp;
+        sp.uv = mk2(0.0f, 0.0f);
+        sp.textures = nullptr;
         sp.p = m3f(q[i].point);
         sp.n = m3f(q[i].normal);
         sp.ng = m3f(q[i].ng);
@@ -963,6 +965,20 @@ int32_t uploadScene(pe_device* d, const pe_scene* s, SceneGPU& G, std::vector<De
     G.hasLightLinks = B.hasLightLinks;
     G.hasShadowLinks = B.hasShadowLinks;
     if (!B.links.empty() && (rc = upload(d, bufs, G.links, B.links))) return rc;
+    // image textures: the texels of each, then the table of them
+    G.textures = nullptr;
+    if (!s->textures.empty()) {
+        std::vector<TexGPU> tex(s->textures.size());
+        for (size_t i = 0; i < s->textures.size(); ++i) {
+            const float* texels = nullptr;
+            if ((rc = upload(d, bufs, texels, s->textures[i].texels))) return rc;
+            tex[i].texels = texels;
+            tex[i].width = s->textures[i].width;
+            tex[i].height = s->textures[i].height;
+        }
+        if ((rc = upload(d, bufs, G.textures, tex))) return rc;
+    }
+    G.nTextures = static_cast<int32_t>(s->textures.size());
     G.nLightGroups = static_cast<int32_t>(B.groupNames.size());
     G.envGroup = B.envGroup;
     if (!B.lightGroup.empty() && (rc = upload(d, bufs, G.lightGroup, B.lightGroup))) return rc;

@@ -529,6 +529,14 @@ MatGPU resolveMaterial(const pe_material& m) {
     c3(g.base, m.base_color);
     c3(g.emission, m.emission);
     g.roundEdge = m.round_edge_radius > 0.0f ? m.round_edge_radius : 0.0f; // setRoundEdgeRadius
+    // image maps: Disney only (the other materials have none)
+    const bool disney = m.type == PE_MAT_DISNEY;
+    g.texAlbedo = disney ? m.albedo_texture : -1;
+    g.texRoughness = disney ? m.roughness_texture : -1;
+    g.texMetalness = disney ? m.metalness_texture : -1;
+    g.texNormal = disney ? m.normal_texture : -1;
+    g.texMapping = m.texture_mapping == 1 ? 1 : 0;
+    g.texScale = m.texture_scale > 1e-4f ? m.texture_scale : 1e-4f; // setTextureScale
     if (m.type == PE_MAT_DISNEY) {
         g.metallic = m.metallic;
         g.roughness = smax(0.001f, m.roughness);
@@ -1086,6 +1094,8 @@ void pe_material_defaults(int32_t type, pe_material* m) {
     if (!m) return;
     std::memset(m, 0, sizeof(pe_material));
     m->type = type;
+    m->albedo_texture = m->roughness_texture = m->metalness_texture = m->normal_texture = -1;
+    m->texture_scale = 1.0f;
     for (int i = 0; i < 3; ++i) {
         m->base_color[i] = 0.8f;
         m->coat_tint[i] = 1.0f;
@@ -1128,6 +1138,11 @@ int32_t pe_scene_add_material(pe_scene* s, const pe_material* m) {
         setError("pe_scene_add_material: unknown material type " + std::to_string(m->type));
         return -1;
     }
+    for (int32_t t : {m->albedo_texture, m->roughness_texture, m->metalness_texture, m->normal_texture})
+        if (t < -1 || t >= static_cast<int32_t>(s->textures.size())) {
+            setError("pe_scene_add_material: texture index " + std::to_string(t) + " not added with pe_scene_add_texture");
+            return -1;
+        }
     s->materialsIn.push_back(*m);
     s->materials.push_back(resolveMaterial(*m));
     s->built = false;
@@ -1269,6 +1284,20 @@ int32_t pe_scene_light_groups(const pe_scene* s, char* names, int32_t capacity) 
         if (k < all.size() && capacity > 0) names[capacity - 1] = '\0';
     }
     return static_cast<int32_t>(g.size());
+}
+
+int32_t pe_scene_add_texture(pe_scene* s, const float* rgb, int32_t width, int32_t height) {
+    if (!s || !rgb || width <= 0 || height <= 0) {
+        setError("pe_scene_add_texture: bad argument");
+        return PE_ERR_INVALID;
+    }
+    pe_scene::Texture t;
+    t.width = width;
+    t.height = height;
+    t.texels.assign(rgb, rgb + static_cast<size_t>(width) * static_cast<size_t>(height) * 3);
+    s->textures.push_back(std::move(t));
+    s->built = false;
+    return static_cast<int32_t>(s->textures.size() - 1);
 }
 
 int32_t pe_scene_set_shadow_catcher(pe_scene* s, int32_t shape) {

@@ -87,6 +87,11 @@ struct HostLightLink {
 } // namespace pe
 
 struct pe_scene {
+    struct Texture {
+        std::vector<float> texels; // width·height·3
+        int32_t width = 0, height = 0;
+    };
+    std::vector<Texture> textures;             // pe_scene_add_texture
     std::vector<pe_material> materialsIn;
     std::vector<pe::MatGPU> materials;
     std::vector<pe::HostShape> shapes;

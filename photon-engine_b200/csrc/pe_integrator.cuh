@@ -917,6 +917,8 @@ __device__ __forceinline__ bool shadeSlot(const SceneGPU& S, const Paths& P, con
         }
         if (A.aoStrength > 0.0f && depth == 0) thr *= approxAo(S, is, sb, A.aoStrength, shadowSamples);
         ShadePoint sp;
+        sp.uv = is.uv;
+        sp.textures = S.textures;
         sp.p = is.point;
         sp.n = is.normal;
         sp.ng = is.ng;

@@ -82,7 +82,18 @@ struct MatGPU {
     int32_t thinWalled;
     float filmThickness;
     float roundEdge;          // Material::roundEdgeRadius (0 = off)
-    float pad[7];
+    // DisneyMaterial image textures (disney.h:133-145): texture indices (-1 none), mapping
+    // (0 UV, 1 box), scale
+    int32_t texAlbedo, texRoughness, texMetalness, texNormal;
+    int32_t texMapping;
+    float texScale;
+    float pad;
+};
+
+// An RGB float image (Image, Float32 storage) read by bilinear lookups with wrap.
+struct TexGPU {
+    const float* texels; // width·height·3
+    int32_t width, height;
 };
 
 enum MatFlags : int32_t {
@@ -203,6 +214,8 @@ struct SceneGPU {
     const int32_t* lightGroup;
     int32_t nLightGroups, envGroup;
     const float4* idColor;
+    const TexGPU* textures;  // image textures (null without any)
+    int32_t nTextures;
 };
 
 // Scene::isLightLinked / isShadowLinked for light `li` (explicit) and a receiver or blocker node.

@@ -309,6 +309,7 @@ struct Isect {
     int32_t tri;    // global triangle index
     int32_t shape;
     int32_t material;
+    V2 uv;          // interpolated vertex uv (0 without uvs)
 };
 
 __device__ __forceinline__ V3 ld3(const float4* a, int i) {
@@ -350,6 +351,8 @@ static __device__ __noinline__ void fillHit(const SceneGPU& S, const Hit& h, V3 
             is.hasSmooth = true;
         }
     }
+    is.uv.x = (uv0.x * w + uv1.x * u) + uv2.x * v;
+    is.uv.y = (uv0.y * w + uv1.y * u) + uv2.y * v;
     const float d1x = uv1.x - uv0.x, d1y = uv1.y - uv0.y;
     const float d2x = uv2.x - uv0.x, d2y = uv2.y - uv0.y;
     const float r = d1x * d2y - d2x * d1y;

@@ -47,14 +47,25 @@ def _lib():
 # materials
 class Material:
     kind = -1
+    _maps = ("albedo", "roughness", "metalness", "normal")
 
     def __init__(self):
         self._m = capi.pe_material()
         _lib().pe_material_defaults(self.kind, C.byref(self._m))
+        self.images: dict[str, np.ndarray] = {}
 
     @property
     def struct(self) -> capi.pe_material:
         return self._m
+
+    def struct_with(self, texture_index) -> capi.pe_material:
+        """The material's C description with its image maps numbered by `texture_index`
+        (id of the image array → index of pe_scene_add_texture)."""
+        m = capi.pe_material()
+        C.memmove(C.byref(m), C.byref(self._m), C.sizeof(m))
+        for k, img in self.images.items():
+            setattr(m, k + "_texture", texture_index[id(img)])
+        return m
 
     def emitted(self):
         return tuple(self._m.emission)
@@ -76,6 +87,36 @@ class Lambertian(Material):
 
 class DisneyMaterial(Material):
     kind = capi.PE_MAT_DISNEY
+
+    def _set_image(self, key, image):
+        img = np.ascontiguousarray(image, dtype=np.float32)
+        if img.ndim != 3 or img.shape[2] != 3:
+            raise ValueError("image maps are (height, width, 3) float arrays")
+        self.images[key] = img
+
+    def set_albedo_image(self, image):
+        """DisneyMaterial::setAlbedoImage: the base colour from an RGB image."""
+        self._set_image("albedo", image)
+
+    def set_roughness_image(self, image):
+        """DisneyMaterial::setRoughnessImage: roughness from the image's green channel."""
+        self._set_image("roughness", image)
+
+    def set_metalness_image(self, image):
+        """DisneyMaterial::setMetalnessImage: metalness from the image's blue channel."""
+        self._set_image("metalness", image)
+
+    def set_normal_image(self, image):
+        """DisneyMaterial::setNormalImage: a tangent-space normal map."""
+        self._set_image("normal", image)
+
+    def set_texture_mapping(self, box: bool):
+        """DisneyMaterial::setTextureMapping: UV (False) or box projection (True)."""
+        self._m.texture_mapping = 1 if box else 0
+
+    def set_texture_scale(self, s: float):
+        """DisneyMaterial::setTextureScale (at least 1e-4)."""
+        self._m.texture_scale = max(1e-4, float(s))
 
     def __init__(self, base_color, metallic: float, roughness: float, specular: float = 0.5):
         super().__init__()
@@ -294,6 +335,17 @@ class Scene:
                 out.append(obj.material)
         return out
 
+    def textures(self) -> list:
+        """The image maps of the scene's materials, each once, in material order."""
+        out, seen = [], set()
+        for m in self.materials():
+            for k in Material._maps:
+                img = getattr(m, "images", {}).get(k)
+                if img is not None and id(img) not in seen:
+                    seen.add(id(img))
+                    out.append(img)
+        return out
+
     def build_accelerator(self):
         lib = _lib()
         if self._handle:
@@ -302,9 +354,15 @@ class Scene:
         if not h:
             raise MemoryError("pe_scene_create failed")
         self._handle = h
+        tex_index = {}
+        for img in self.textures():
+            t = lib.pe_scene_add_texture(h, capi.fptr(img), img.shape[1], img.shape[0])
+            if t < 0:
+                capi.check(t)
+            tex_index[id(img)] = t
         mat_index = {}
         for m in self.materials():
-            idx = lib.pe_scene_add_material(h, C.byref(m.struct))
+            idx = lib.pe_scene_add_material(h, C.byref(m.struct_with(tex_index)))
             if idx < 0:
                 capi.check(capi.PE_ERR_INVALID)
             mat_index[id(m)] = idx

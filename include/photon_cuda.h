@@ -181,6 +181,9 @@ int32_t pe_scene_set_shadow_catcher(pe_scene* s, int32_t shape);
  * or a negative status.  Lookups are Image::sampleBilinear's (src/core/image/image.cpp:98-225):
  * bilinear, wrapping, without mipmaps. */
 int32_t pe_scene_add_texture(pe_scene* s, const float* rgb, int32_t width, int32_t height);
+/* Image::buildMipmaps (src/core/image/image.cpp:102-155) of texture `texture`: lookups then
+ * select a level from the ray cone's footprint (sampleTex, src/materials/disney.cpp:530-539). */
+int32_t pe_scene_build_texture_mipmaps(pe_scene* s, int32_t texture);
 /* Light::setLightGroup (src/lights/light.h:85) of light `light` (the numbering of
  * pe_scene_set_light_link), or of the environment when light == -1; "" or NULL clears it.
  * Scene::buildAccelerator forms the groups (src/engine/scene.cpp:144-174): none unless some

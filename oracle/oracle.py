@@ -70,6 +70,7 @@ def _load(fast: bool = False):
         "ref_scene_set_shadow_catcher": (C.c_int32, [P, C.c_int32]),
         "ref_scene_set_light_group": (C.c_int32, [P, C.c_int32, C.c_char_p]),
         "ref_scene_add_texture": (C.c_int32, [P, FP, C.c_int32, C.c_int32]),
+        "ref_scene_build_texture_mipmaps": (C.c_int32, [P, C.c_int32]),
         "ref_film_create": (P, [C.c_int32, C.c_int32]),
         "ref_film_destroy": (None, [P]),
         "ref_film_export": (C.c_int32, [P, C.c_int32, C.c_int32, FP, UP]),
@@ -134,6 +135,8 @@ class RefScene:
         tex_index = {}
         for img in (scene.textures() if hasattr(scene, "textures") else []):
             tex_index[id(img)] = self.lib.ref_scene_add_texture(self.h, _f(img), img.shape[1], img.shape[0])
+            if scene.texture_has_mipmaps(img):
+                self.lib.ref_scene_build_texture_mipmaps(self.h, tex_index[id(img)])
         mat_index = {}
         for kind, obj in scene.ops:
             if kind == "mesh" and id(obj.material) not in mat_index:

@@ -209,6 +209,14 @@ int32_t ref_scene_add_texture(void* s, const float* rgb, int32_t w, int32_t h) {
     return static_cast<int32_t>(rs->textures.size() - 1);
 }
 
+// Image::buildMipmaps of texture `i`.
+int32_t ref_scene_build_texture_mipmaps(void* s, int32_t i) {
+    auto* rs = static_cast<RefScene*>(s);
+    if (i < 0 || i >= static_cast<int32_t>(rs->textures.size())) return -1;
+    rs->textures[static_cast<size_t>(i)]->buildMipmaps();
+    return 0;
+}
+
 int32_t ref_scene_add_material(void* s, const pe_material* m) {
     auto* rs = static_cast<RefScene*>(s);
     auto mat = makeMaterial(*m);

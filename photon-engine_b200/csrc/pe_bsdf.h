@@ -233,6 +233,8 @@ PE_HD V3 eonEval(V3 rho, float r, V3 wi, V3 wo) {
 struct ShadePoint {
     V2 uv;                  // surface uv (texture lookups)
     const TexGPU* textures; // the scene's image textures (may be null)
+    float footprint;        // ray-cone footprint at the hit (0: none; mip LOD)
+    float uvDensity;
     V3 p;        // point
     V3 n;        // shading normal, facing the incoming ray
     V3 ng;       // outward geometric normal
@@ -304,10 +306,13 @@ PE_HD void resolveFlake(V3 point, float size, float density, float rough, Disney
     p.flakeNormal = normalize(toWorld(f, mk(sinT * cosf(phi), sinT * sinf(phi), cosT)));
 }
 
-// Image::sampleLevel(0, u, v) (image.cpp:168-225): bilinear with wrap, texel centres at +0.5.
-PE_HD V3 texBilinear(const TexGPU& t, float u, float v) {
-    const int w = t.width, h = t.height;
-    if (w <= 0 || h <= 0) return mk(0.0f);
+// Image::sampleLevel (image.cpp:168-225): bilinear with wrap, texel centres at +0.5, on mip
+// level `level` (clamped to the last; 0 without mipmaps).
+PE_HD V3 texBilinear(const TexGPU& t, float u, float v, int level = 0) {
+    if (t.width <= 0 || t.height <= 0) return mk(0.0f);
+    const int l = t.levels > 1 && level > 0 ? (level < t.levels ? level : t.levels - 1) : 0;
+    const int w = t.levelW[l], h = t.levelH[l];
+    const float* texels = t.texels + t.levelOffset[l];
     u = u - floorf(u);
     v = v - floorf(v);
     const float x = u * static_cast<float>(w) - 0.5f;
@@ -322,12 +327,37 @@ PE_HD V3 texBilinear(const TexGPU& t, float u, float v) {
     };
     const int xa = wrap(x0, w), xb = wrap(x0 + 1, w), ya = wrap(y0, h), yb = wrap(y0 + 1, h);
     auto at = [&](int px, int py) {
-        const float* c = t.texels + (static_cast<size_t>(py) * static_cast<size_t>(w) + static_cast<size_t>(px)) * 3;
+        const float* c = texels + (static_cast<size_t>(py) * static_cast<size_t>(w) + static_cast<size_t>(px)) * 3;
         return mk(c[0], c[1], c[2]);
     };
     const V3 c0 = at(xa, ya) * (1.0f - fx) + at(xb, ya) * fx;
     const V3 c1 = at(xa, yb) * (1.0f - fx) + at(xb, yb) * fx;
     return c0 * (1.0f - fy) + c1 * fy;
+}
+
+// Image::sampleMip (image.cpp:227-239): trilinear between the two levels around `lod`.
+PE_HD V3 texMip(const TexGPU& t, float u, float v, float lod) {
+    if (t.levels <= 1 || lod <= 0.0f) return texBilinear(t, u, v, 0);
+    const int maxLvl = t.levels - 1;
+    const float clamped = sclamp(lod, 0.0f, static_cast<float>(maxLvl));
+    const int l0 = static_cast<int>(floorf(clamped));
+    const int l1 = l0 + 1 < maxLvl ? l0 + 1 : maxLvl;
+    const float frac = clamped - static_cast<float>(l0);
+    if (l0 == l1 || frac <= 1e-5f) return texBilinear(t, u, v, l0);
+    return texBilinear(t, u, v, l0) * (1.0f - frac) + texBilinear(t, u, v, l1) * frac;
+}
+
+// sampleTex (disney.cpp:530-539): with a ray footprint and mipmaps, the level whose texels match
+// the footprint; else level 0.
+PE_HD V3 texLookup(const TexGPU& t, V2 uv, const ShadePoint& sp, float texScale) {
+    if (sp.footprint > 0.0f && t.levels > 1) {
+        const float density = sp.uvDensity > 0.0f ? sp.uvDensity : 1.0f;
+        const float texelExtent = sqrtf(static_cast<float>(t.width) * static_cast<float>(t.height));
+        const float footprintTexels = sp.footprint * density * texScale * texelExtent;
+        const float lod = footprintTexels > 1.0f ? log2f(footprintTexels) : 0.0f;
+        return texMip(t, uv.x, uv.y, lod);
+    }
+    return texBilinear(t, uv.x, uv.y, 0);
 }
 
 // DisneyMaterial::textureCoord (disney.cpp:517-526): the uv scaled, or a box projection of the
@@ -350,11 +380,12 @@ PE_HD V2 textureCoord(const MatGPU& m, const ShadePoint& sp) {
 PE_HDN void applyTextures(const MatGPU& m, const ShadePoint& sp, V3& base, float& roughness, float& metallic,
                           V3& normal) {
     const V2 uv = textureCoord(m, sp);
-    if (m.texAlbedo >= 0) base = texBilinear(sp.textures[m.texAlbedo], uv.x, uv.y);
-    if (m.texRoughness >= 0) roughness = smax(0.001f, texBilinear(sp.textures[m.texRoughness], uv.x, uv.y).y);
-    if (m.texMetalness >= 0) metallic = sclamp(texBilinear(sp.textures[m.texMetalness], uv.x, uv.y).z, 0.0f, 1.0f);
+    if (m.texAlbedo >= 0) base = texLookup(sp.textures[m.texAlbedo], uv, sp, m.texScale);
+    if (m.texRoughness >= 0) roughness = smax(0.001f, texLookup(sp.textures[m.texRoughness], uv, sp, m.texScale).y);
+    if (m.texMetalness >= 0)
+        metallic = sclamp(texLookup(sp.textures[m.texMetalness], uv, sp, m.texScale).z, 0.0f, 1.0f);
     if (m.texNormal >= 0) {
-        const V3 c = texBilinear(sp.textures[m.texNormal], uv.x, uv.y);
+        const V3 c = texLookup(sp.textures[m.texNormal], uv, sp, m.texScale);
         const V3 nTs = mk(c.x * 2.0f - 1.0f, c.y * 2.0f - 1.0f, c.z * 2.0f - 1.0f);
         const V3 N = sp.n;
         V3 T = sp.tangent;

@@ -33,6 +33,7 @@ int32_t allocLane(WaveLane& ln, size_t slots) {
     for (float4** c : scols)
         if ((st = devAlloc(ln.bufs, *c, slots))) return st;
     if ((st = devAlloc(ln.bufs, P.counters, CNT_TOTAL))) return st;
+    if ((st = devAlloc(ln.bufs, P.cone, slots))) return st;
     // path regeneration: slot → path, freed slots, radiance of kStreamFactor × slots paths
     if ((st = devAlloc(ln.bufs, ln.pathOf, slots))) return st;
     if ((st = devAlloc(ln.bufs, ln.freeQ, slots))) return st;
@@ -151,6 +152,18 @@ WaveSeg makeSeg(const pe_camera* cam, const pe_settings* st) {
     A.shadowSamples = st->shadow_quality < 1 ? 1 : st->shadow_quality;
     A.clampIndirect = st->clamp_indirect > 0.0f ? st->clamp_indirect : 0.0f;
     A.aoStrength = st->ao_strength > 0.0f ? st->ao_strength : 0.0f;
+    // Camera::pixelConeWidth / pixelConeSpread (camera.h:94-109): a pixel's width for the
+    // orthographic camera, the angle a pixel subtends at the image plane's centre otherwise
+    if (st->height > 0) {
+        const float h = static_cast<float>(st->height);
+        if (A.cam.orthographic) {
+            A.coneWidth = length(A.cam.vertical) / h;
+        } else {
+            const V3 center = A.cam.lowerLeft + A.cam.horizontal * 0.5f + A.cam.vertical * 0.5f;
+            const float dist = smax(1e-4f, length(center - A.cam.position));
+            A.coneSpread = std::atan(length(A.cam.vertical) / (dist * h));
+        }
+    }
     return A;
 }
 
@@ -967,14 +980,31 @@ int32_t uploadScene(pe_device* d, const pe_scene* s, SceneGPU& G, std::vector<De
     if (!B.links.empty() && (rc = upload(d, bufs, G.links, B.links))) return rc;
     // image textures: the texels of each, then the table of them
     G.textures = nullptr;
+    G.hasMips = 0;
     if (!s->textures.empty()) {
         std::vector<TexGPU> tex(s->textures.size());
+        G.hasMips = 0;
         for (size_t i = 0; i < s->textures.size(); ++i) {
+            const pe_scene::Texture& src = s->textures[i];
+            std::vector<float> all = src.texels;
+            std::memset(&tex[i], 0, sizeof(TexGPU));
+            tex[i].width = src.width;
+            tex[i].height = src.height;
+            tex[i].levels = 1;
+            tex[i].levelW[0] = src.width;
+            tex[i].levelH[0] = src.height;
+            for (size_t l = 0; l < src.mips.size() && l + 1 < static_cast<size_t>(kMaxMipLevels); ++l) {
+                const int k = static_cast<int>(l) + 1;
+                tex[i].levelOffset[k] = static_cast<int32_t>(all.size());
+                tex[i].levelW[k] = src.mipW[l];
+                tex[i].levelH[k] = src.mipH[l];
+                all.insert(all.end(), src.mips[l].begin(), src.mips[l].end());
+                tex[i].levels = k + 1;
+            }
+            if (tex[i].levels > 1) G.hasMips = 1;
             const float* texels = nullptr;
-            if ((rc = upload(d, bufs, texels, s->textures[i].texels))) return rc;
+            if ((rc = upload(d, bufs, texels, all))) return rc;
             tex[i].texels = texels;
-            tex[i].width = s->textures[i].width;
-            tex[i].height = s->textures[i].height;
         }
         if ((rc = upload(d, bufs, G.textures, tex))) return rc;
     }

@@ -1300,6 +1300,47 @@ int32_t pe_scene_add_texture(pe_scene* s, const float* rgb, int32_t width, int32
     return static_cast<int32_t>(s->textures.size() - 1);
 }
 
+// Image::buildMipmaps (image.cpp:102-155), Float32 storage: each level the 2×2 box mean of the
+// one before (the last row / column repeated on odd sizes), down to 1×1.
+int32_t pe_scene_build_texture_mipmaps(pe_scene* s, int32_t texture) {
+    if (!s || texture < 0 || texture >= static_cast<int32_t>(s->textures.size())) {
+        setError("pe_scene_build_texture_mipmaps: bad texture index");
+        return PE_ERR_INVALID;
+    }
+    pe_scene::Texture& t = s->textures[static_cast<size_t>(texture)];
+    t.mips.clear();
+    t.mipW.clear();
+    t.mipH.clear();
+    int pw = t.width, ph = t.height;
+    const std::vector<float>* prev = &t.texels;
+    while ((pw > 1 || ph > 1) && t.mips.size() + 1 < static_cast<size_t>(kMaxMipLevels)) {
+        const int nw = std::max(1, pw / 2), nh = std::max(1, ph / 2);
+        std::vector<float> next(static_cast<size_t>(nw) * static_cast<size_t>(nh) * 3, 0.0f);
+        for (int y = 0; y < nh; ++y) {
+            const int ya = std::min(2 * y, ph - 1), yb = std::min(2 * y + 1, ph - 1);
+            for (int x = 0; x < nw; ++x) {
+                const int xa = std::min(2 * x, pw - 1), xb = std::min(2 * x + 1, pw - 1);
+                auto at = [&](int px, int py) {
+                    return (static_cast<size_t>(py) * static_cast<size_t>(pw) + static_cast<size_t>(px)) * 3;
+                };
+                const size_t o = (static_cast<size_t>(y) * static_cast<size_t>(nw) + static_cast<size_t>(x)) * 3;
+                for (int c = 0; c < 3; ++c)
+                    next[o + static_cast<size_t>(c)] =
+                        0.25f * ((*prev)[at(xa, ya) + c] + (*prev)[at(xb, ya) + c] + (*prev)[at(xa, yb) + c] +
+                                 (*prev)[at(xb, yb) + c]);
+            }
+        }
+        t.mips.push_back(std::move(next));
+        t.mipW.push_back(nw);
+        t.mipH.push_back(nh);
+        prev = &t.mips.back();
+        pw = nw;
+        ph = nh;
+    }
+    s->built = false;
+    return PE_OK;
+}
+
 int32_t pe_scene_set_shadow_catcher(pe_scene* s, int32_t shape) {
     if (!s || shape < -1) {
         setError("pe_scene_set_shadow_catcher: bad argument");

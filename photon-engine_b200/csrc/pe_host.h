@@ -90,6 +90,8 @@ struct pe_scene {
     struct Texture {
         std::vector<float> texels; // width·height·3
         int32_t width = 0, height = 0;
+        std::vector<std::vector<float>> mips; // levels 1.. (pe_scene_build_texture_mipmaps)
+        std::vector<int32_t> mipW, mipH;
     };
     std::vector<Texture> textures;             // pe_scene_add_texture
     std::vector<pe_material> materialsIn;

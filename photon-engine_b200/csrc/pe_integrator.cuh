@@ -128,6 +128,7 @@ __device__ __forceinline__ void generatePath(const SceneGPU& S, const Paths& P, 
         P.guideMark[slot] = 0u;
         if (slot % P.guideStride == 0) P.guideRec[static_cast<size_t>(slot) * 6 + 4] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     }
+    if (S.hasMips && P.cone) P.cone[slot] = make_float2(A.coneWidth, A.coneSpread);
     if (P.pass) {
         float4* b = passBlock(P, path);
         for (int k = 0; k < P.passStride; ++k) b[k] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
@@ -685,6 +686,9 @@ __device__ __forceinline__ bool shadeSlot(const SceneGPU& S, const Paths& P, con
     const int explicitLights = S.nLights;
     const int prim = __float_as_int(hr.w);
     const bool hit = prim >= 0;
+    // ray cone (path_tracer.cpp:428-454, 777-783, 853-857): only scenes with mipmapped textures
+    const bool cones = S.hasMips && P.cone;
+    float2 cone = cones ? P.cone[slot] : make_float2(0.0f, 0.0f);
     Isect is;
     bool done = false;
     bool vertex = false; // a surface vertex to shade (NEE + BSDF sampling) below
@@ -746,6 +750,7 @@ __device__ __forceinline__ bool shadeSlot(const SceneGPU& S, const Paths& P, con
                                passesCutout(S.materials[is.material], sb))) {
                 const V3 no = offsetRayOrigin(is.point, is.pError, is.ng, dir);
                 ro = make_float4(no.x, no.y, no.z, ro.w);
+                if (cones) cone.x = cone.x + cone.y * smax(0.0f, is.t);
                 ++skips;
                 cont = true;
                 done = true;
@@ -792,6 +797,7 @@ __device__ __forceinline__ bool shadeSlot(const SceneGPU& S, const Paths& P, con
                     ro = make_float4(no.x, no.y, no.z, __uint_as_float(VIS_DIFFUSE));
                     rd = make_float4(nd.x, nd.y, nd.z, rd.w);
                     flags = (flags | PF_SPECULAR_BOUNCE) & ~PF_CAMERA_RAY;
+                    if (cones) cone = make_float2(0.0f, 0.0f); // a new ray without a cone (path_tracer.cpp:465)
                     cont = true;
                     done = true;
                 }
@@ -919,6 +925,13 @@ __device__ __forceinline__ bool shadeSlot(const SceneGPU& S, const Paths& P, con
         ShadePoint sp;
         sp.uv = is.uv;
         sp.textures = S.textures;
+        sp.uvDensity = is.uvDensity;
+        sp.footprint = 0.0f;
+        if (cones && !exitVertex && (cone.x > 0.0f || cone.y > 0.0f)) {
+            const V3 nGeom = len2(is.ng) > 0.0f ? is.ng : is.normal;
+            const float cosInc = smax(0.15f, fabsf(dot(-dir, nGeom)));
+            sp.footprint = (cone.x + cone.y * smax(0.0f, is.t)) / cosInc;
+        }
         sp.p = is.point;
         sp.n = is.normal;
         sp.ng = is.ng;
@@ -1065,6 +1078,7 @@ __device__ __forceinline__ bool shadeSlot(const SceneGPU& S, const Paths& P, con
                 const V3 no = spawnOrigin(is, bs.wi);
                 ro = make_float4(no.x, no.y, no.z, ro.w);
                 rd = make_float4(bs.wi.x, bs.wi.y, bs.wi.z, rd.w);
+                if (cones) cone.x = cone.x + cone.y * smax(0.0f, is.t);
                 skips = 0;
                 cont = true;
             }
@@ -1112,6 +1126,10 @@ __device__ __forceinline__ bool shadeSlot(const SceneGPU& S, const Paths& P, con
                     }
                 }
                 const uint32_t nextMask = refracted ? VIS_TRANSMISSION : (bs.delta ? VIS_GLOSSY : VIS_DIFFUSE);
+                if (cones) {
+                    cone.x = cone.x + cone.y * smax(0.0f, is.t);
+                    cone.y = cone.y + (bs.delta ? 0.0f : 0.12f);
+                }
                 ln = make_float4(is.normal.x, is.normal.y, is.normal.z, 0.0f);
                 lp = make_float4(is.point.x, is.point.y, is.point.z, 0.0f);
                 const V3 no = spawnOrigin(is, wi);
@@ -1145,6 +1163,7 @@ __device__ __forceinline__ bool shadeSlot(const SceneGPU& S, const Paths& P, con
     // write back
     P.L[slot] = L;
     if (cont) {
+        if (cones) P.cone[slot] = cone;
         P.rayO[slot] = ro;
         P.rayD[slot] = rd;
         P.thr[slot] = make_float4(thr.x, thr.y, thr.z, lambda);

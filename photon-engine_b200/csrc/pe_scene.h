@@ -90,10 +90,15 @@ struct MatGPU {
     float pad;
 };
 
-// An RGB float image (Image, Float32 storage) read by bilinear lookups with wrap.
+// An RGB float image (Image, Float32 storage) read by bilinear lookups with wrap; with mipmaps
+// (Image::buildMipmaps) its levels follow level 0 in `texels`.
+constexpr int kMaxMipLevels = 16;
 struct TexGPU {
-    const float* texels; // width·height·3
+    const float* texels; // level 0 then levels 1.. (each width·height·3)
     int32_t width, height;
+    int32_t levels;      // 1 without mipmaps
+    int32_t levelW[kMaxMipLevels], levelH[kMaxMipLevels];
+    int32_t levelOffset[kMaxMipLevels]; // in floats
 };
 
 enum MatFlags : int32_t {
@@ -216,6 +221,7 @@ struct SceneGPU {
     const float4* idColor;
     const TexGPU* textures;  // image textures (null without any)
     int32_t nTextures;
+    int32_t hasMips;         // some texture has mipmaps: paths carry ray cones for its LOD
 };
 
 // Scene::isLightLinked / isShadowLinked for light `li` (explicit) and a receiver or blocker node.

@@ -310,6 +310,7 @@ struct Isect {
     int32_t shape;
     int32_t material;
     V2 uv;          // interpolated vertex uv (0 without uvs)
+    float uvDensity; // sqrt(|uv area| / world area) (scenes with mipmapped textures only)
 };
 
 __device__ __forceinline__ V3 ld3(const float4* a, int i) {
@@ -356,6 +357,12 @@ static __device__ __noinline__ void fillHit(const SceneGPU& S, const Hit& h, V3 
     const float d1x = uv1.x - uv0.x, d1y = uv1.y - uv0.y;
     const float d2x = uv2.x - uv0.x, d2y = uv2.y - uv0.y;
     const float r = d1x * d2y - d2x * d1y;
+    is.uvDensity = 1.0f;
+    if (S.hasMips) {
+        // Triangle::fillHit's texel-density term (triangle.cpp:114-118)
+        const float worldArea2 = length(cross(edge1, edge2));
+        is.uvDensity = (worldArea2 > 1e-12f && fabsf(r) > 1e-12f) ? sqrtf(fabsf(r) / worldArea2) : 0.0f;
+    }
     V3 tangent;
     if (fabsf(r) < 1e-6f) {
         const V3 n = is.normal;

@@ -94,6 +94,9 @@ struct Paths {
     float4* pass;
     float4* shPass;
     int32_t passStride;
+    // ray cone of each slot's current ray: width, spread (null without; read only in scenes
+    // with mipmapped textures)
+    float2* cone;
     // sweeps (continuous waves): a path alive for sweepAge bounces leaves the wavefront for a
     // tail-kernel launch on a side stream (sweepAge 0: off)
     int32_t* born;       // bounce at which each slot's path was injected
@@ -154,6 +157,7 @@ struct WaveSeg {
     int pixFirst;
     int flags;              // SegFlags
     float aoStrength;       // RenderSettings::aoStrength (contact AO at camera hits)
+    float coneWidth, coneSpread; // camera rays' cone (Camera::pixelConeWidth / pixelConeSpread)
 };
 enum SegFlags { SEG_SWEEP = 1 }; // paths of the segment may leave a continuous wave for a sweep
 

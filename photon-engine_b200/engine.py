@@ -53,6 +53,7 @@ class Material:
         self._m = capi.pe_material()
         _lib().pe_material_defaults(self.kind, C.byref(self._m))
         self.images: dict[str, np.ndarray] = {}
+        self.mipmapped: set[int] = set()  # ids of images given with mipmaps
 
     @property
     def struct(self) -> capi.pe_material:
@@ -88,27 +89,30 @@ class Lambertian(Material):
 class DisneyMaterial(Material):
     kind = capi.PE_MAT_DISNEY
 
-    def _set_image(self, key, image):
+    def _set_image(self, key, image, mipmaps):
         img = np.ascontiguousarray(image, dtype=np.float32)
         if img.ndim != 3 or img.shape[2] != 3:
             raise ValueError("image maps are (height, width, 3) float arrays")
         self.images[key] = img
+        if mipmaps:
+            self.mipmapped.add(id(img))
 
-    def set_albedo_image(self, image):
+    # `mipmaps`: Image::buildMipmaps on the image, so that lookups pick a level from the ray cone
+    def set_albedo_image(self, image, mipmaps: bool = False):
         """DisneyMaterial::setAlbedoImage: the base colour from an RGB image."""
-        self._set_image("albedo", image)
+        self._set_image("albedo", image, mipmaps)
 
-    def set_roughness_image(self, image):
+    def set_roughness_image(self, image, mipmaps: bool = False):
         """DisneyMaterial::setRoughnessImage: roughness from the image's green channel."""
-        self._set_image("roughness", image)
+        self._set_image("roughness", image, mipmaps)
 
-    def set_metalness_image(self, image):
+    def set_metalness_image(self, image, mipmaps: bool = False):
         """DisneyMaterial::setMetalnessImage: metalness from the image's blue channel."""
-        self._set_image("metalness", image)
+        self._set_image("metalness", image, mipmaps)
 
-    def set_normal_image(self, image):
+    def set_normal_image(self, image, mipmaps: bool = False):
         """DisneyMaterial::setNormalImage: a tangent-space normal map."""
-        self._set_image("normal", image)
+        self._set_image("normal", image, mipmaps)
 
     def set_texture_mapping(self, box: bool):
         """DisneyMaterial::setTextureMapping: UV (False) or box projection (True)."""
@@ -346,6 +350,9 @@ class Scene:
                     out.append(img)
         return out
 
+    def texture_has_mipmaps(self, img) -> bool:
+        return any(id(img) in getattr(m, "mipmapped", ()) for m in self.materials())
+
     def build_accelerator(self):
         lib = _lib()
         if self._handle:
@@ -359,6 +366,8 @@ class Scene:
             t = lib.pe_scene_add_texture(h, capi.fptr(img), img.shape[1], img.shape[0])
             if t < 0:
                 capi.check(t)
+            if self.texture_has_mipmaps(img):
+                capi.check(lib.pe_scene_build_texture_mipmaps(h, t))
             tex_index[id(img)] = t
         mat_index = {}
         for m in self.materials():

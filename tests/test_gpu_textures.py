@@ -110,3 +110,43 @@ def test_texture_index_is_checked(pe):
         assert lib.pe_scene_add_material(s, m) >= 0
     finally:
         lib.pe_scene_destroy(s)
+
+
+def test_mipmapped_maps_match_reference(pe, device, oracle):
+    """Mipmapped images (Image::buildMipmaps) looked up at the level of the ray cone's footprint
+    (sampleTex, disney.cpp:530-539; cones path_tracer.cpp:428-454, 853-857): a receding floor
+    whose far texels shrink below a pixel, seen directly and in a mirror."""
+    S = scenes()
+    scene = pe.Scene()
+    rng = np.random.default_rng(5)
+    checker = np.kron(rng.uniform(0.05, 0.95, (16, 16, 3)).astype(np.float32), np.ones((4, 4, 1), np.float32))
+    floor = pe.DisneyMaterial((0.5, 0.5, 0.5), 0.0, 0.6, 0.5)
+    floor.set_albedo_image(checker, mipmaps=True)
+    floor.set_texture_scale(6.0)
+    pos, uv, idx = _grid_quad((-20.0, 0.0, -2.0), (40.0, 0.0, 0.0), (0.0, 0.0, 60.0), 8)
+    scene.add_shape(pe.TriangleMesh(pos, None, uv, idx, floor))
+    p, n, i = S.uv_sphere((1.5, 1.0, 4.0), 1.0, 48, 24)
+    scene.add_shape(pe.TriangleMesh(p, n, None, i, pe.Mirror((0.9, 0.9, 0.9))))
+    scene.add_light(pe.AreaLight((-2.0, 6.0, 2.0), (4.0, 0.0, 0.0), (0.0, 0.0, 4.0), (12.0, 12.0, 12.0)))
+    sky = np.ones((16, 32, 3), np.float32) * 0.5
+    scene.set_environment(pe.EnvironmentLight(sky, 0.0, 1.0))
+    cam = pe.PerspectiveCamera((0.0, 1.5, -1.5), (0.0, 0.5, 10.0), (0.0, 1.0, 0.0), 50.0, 1.0)
+    st = pe.RenderSettings(width=64, height=64, max_bounces=4, seed=7)
+    scene.build_accelerator()
+    device.set_scene(scene)
+    spp = 8
+    film = pe.Film(st.width, st.height)
+    device.render(cam, st, pe.RenderTargets(beauty=film), 0, spp)
+    mean_ref, cnt_ref = oracle.RefScene(scene).render(cam, st, 0, spp)
+    img = film.resolve()
+    err = pe.rel_mse(img, mean_ref)
+    same = float(np.mean(np.all(np.abs(img - mean_ref) <= 1e-4 * np.maximum(1.0, np.abs(mean_ref)), axis=-1)))
+    bias = float(img.mean() / max(1e-12, mean_ref.mean()) - 1.0)
+    assert err < 1e-4 and same > 0.99 and abs(bias) < 1e-3, (err, same, bias)
+    # the mip levels matter: without them the far floor aliases to other colours
+    floor.mipmapped.clear()
+    scene.build_accelerator()
+    device.set_scene(scene)
+    plain = pe.Film(st.width, st.height)
+    device.render(cam, st, pe.RenderTargets(beauty=plain), 0, spp)
+    assert pe.rel_mse(plain.resolve(), img) > 1e-4

@@ -38,7 +38,7 @@
 extern "C" {
 #endif
 
-#define PE_ABI_VERSION 7
+#define PE_ABI_VERSION 8
 
 typedef enum pe_status {
     PE_OK = 0,
@@ -102,6 +102,7 @@ typedef struct pe_material {
     int32_t albedo_texture, roughness_texture, metalness_texture, normal_texture;
     int32_t texture_mapping;  /* 0 UV, 1 box projection (DisneyMaterial::TextureMapping) */
     float texture_scale;      /* DisneyMaterial::setTextureScale (≥ 1e-4) */
+    int32_t opacity_texture;  /* DisneyMaterial::setOpacityImage: opacity × the red channel, -1 none */
 } pe_material;
 
 /* Camera as the reference's Camera::describeGpu() (src/camera/camera.h:17-29). */

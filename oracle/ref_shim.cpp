@@ -231,6 +231,7 @@ int32_t ref_scene_add_material(void* s, const pe_material* m) {
         if (auto t = tex(m->roughness_texture)) d->setRoughnessImage(t);
         if (auto t = tex(m->metalness_texture)) d->setMetalnessImage(t);
         if (auto t = tex(m->normal_texture)) d->setNormalImage(t);
+        if (auto t = tex(m->opacity_texture)) d->setOpacityImage(t);
         d->setTextureMapping(m->texture_mapping == 1 ? DisneyMaterial::TextureMapping::Box
                                                      : DisneyMaterial::TextureMapping::UV);
         d->setTextureScale(m->texture_scale);

@@ -42,6 +42,7 @@ class pe_material(C.Structure):
         ("round_edge_radius", C.c_float),
         ("albedo_texture", C.c_int32), ("roughness_texture", C.c_int32), ("metalness_texture", C.c_int32),
         ("normal_texture", C.c_int32), ("texture_mapping", C.c_int32), ("texture_scale", C.c_float),
+        ("opacity_texture", C.c_int32),
     ]
 
 

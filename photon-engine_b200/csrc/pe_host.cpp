@@ -535,6 +535,7 @@ MatGPU resolveMaterial(const pe_material& m) {
     g.texRoughness = disney ? m.roughness_texture : -1;
     g.texMetalness = disney ? m.metalness_texture : -1;
     g.texNormal = disney ? m.normal_texture : -1;
+    g.texOpacity = disney ? m.opacity_texture : -1;
     g.texMapping = m.texture_mapping == 1 ? 1 : 0;
     g.texScale = m.texture_scale > 1e-4f ? m.texture_scale : 1e-4f; // setTextureScale
     if (m.type == PE_MAT_DISNEY) {
@@ -578,7 +579,7 @@ MatGPU resolveMaterial(const pe_material& m) {
         }
         g.opacity = sclamp(m.opacity, 0.0f, 1.0f);
         if (g.specTrans > 0.0f) g.flags |= MF_VOLUME_BOUNDARY;
-        if (g.opacity < 1.0f) g.flags |= MF_TRANSMITS_SHADOWS;
+        if (g.opacity < 1.0f || m.opacity_texture >= 0) g.flags |= MF_TRANSMITS_SHADOWS; // disney.h:158
     } else if (m.type == PE_MAT_DIELECTRIC) {
         g.ior = m.ior;
         g.glassRoughness = m.glass_roughness;
@@ -1095,6 +1096,7 @@ void pe_material_defaults(int32_t type, pe_material* m) {
     std::memset(m, 0, sizeof(pe_material));
     m->type = type;
     m->albedo_texture = m->roughness_texture = m->metalness_texture = m->normal_texture = -1;
+    m->opacity_texture = -1;
     m->texture_scale = 1.0f;
     for (int i = 0; i < 3; ++i) {
         m->base_color[i] = 0.8f;
@@ -1138,7 +1140,8 @@ int32_t pe_scene_add_material(pe_scene* s, const pe_material* m) {
         setError("pe_scene_add_material: unknown material type " + std::to_string(m->type));
         return -1;
     }
-    for (int32_t t : {m->albedo_texture, m->roughness_texture, m->metalness_texture, m->normal_texture})
+    for (int32_t t : {m->albedo_texture, m->roughness_texture, m->metalness_texture, m->normal_texture,
+                      m->opacity_texture})
         if (t < -1 || t >= static_cast<int32_t>(s->textures.size())) {
             setError("pe_scene_add_material: texture index " + std::to_string(t) + " not added with pe_scene_add_texture");
             return -1;

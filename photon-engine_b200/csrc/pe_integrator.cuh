@@ -254,14 +254,25 @@ __global__ void __launch_bounds__(128) kIntersect(SceneGPU S, Paths P, const int
     }
 }
 
-// Surface coverage of a hit for a ray that may pass through cutouts (Material::opacity).
-__device__ __forceinline__ float surfaceOpacity(const MatGPU& m) {
-    return m.type == PE_MAT_DISNEY ? m.opacity : 1.0f;
+// Surface coverage of a hit for a ray that may pass through cutouts (DisneyMaterial::opacity,
+// disney.cpp:505-509: the opacity times the opacity map's red channel, a level-0 lookup).
+__device__ __noinline__ float mappedOpacity(const SceneGPU& S, const MatGPU& m, const Isect& is) {
+    ShadePoint sp;
+    sp.uv = is.uv;
+    sp.p = is.point;
+    sp.n = is.normal;
+    sp.ng = is.ng;
+    const V2 uv = textureCoord(m, sp);
+    return m.opacity * sclamp(texBilinear(S.textures[m.texOpacity], uv.x, uv.y, 0).x, 0.0f, 1.0f);
+}
+__device__ __forceinline__ float surfaceOpacity(const SceneGPU& S, const MatGPU& m, const Isect& is) {
+    if (m.type != PE_MAT_DISNEY) return 1.0f;
+    return m.texOpacity >= 0 ? mappedOpacity(S, m, is) : m.opacity;
 }
 
 // passesCutout (path_tracer.cpp:161-167): true = the ray goes on through this hit.
-__device__ __forceinline__ bool passesCutout(const MatGPU& m, Sobol& sb) {
-    const float alpha = surfaceOpacity(m);
+__device__ __forceinline__ bool passesCutout(const SceneGPU& S, const MatGPU& m, const Isect& is, Sobol& sb) {
+    const float alpha = surfaceOpacity(S, m, is);
     if (alpha >= 1.0f) return false;
     if (alpha <= 0.0f) return true;
     return get1D(sb) >= alpha;
@@ -269,9 +280,9 @@ __device__ __forceinline__ bool passesCutout(const MatGPU& m, Sobol& sb) {
 
 // Material::shadowTransmittance: thin-walled glass passes (1 − R_thin)·tint, a cutout Disney
 // surface 1 − opacity, every other surface nothing.
-__device__ __forceinline__ V3 surfaceShadowTransmittance(const MatGPU& m, const Isect& is, V3 dir) {
+__device__ __forceinline__ V3 surfaceShadowTransmittance(const SceneGPU& S, const MatGPU& m, const Isect& is, V3 dir) {
     if (m.type == PE_MAT_DIELECTRIC) return glassShadowTransmittance(m, is.ng, is.normal, dir);
-    if (m.type == PE_MAT_DISNEY) return mk(1.0f - m.opacity);
+    if (m.type == PE_MAT_DISNEY) return mk(1.0f - surfaceOpacity(S, m, is));
     return mk(0.0f);
 }
 
@@ -306,7 +317,7 @@ __device__ V3 shadowVisibility(const SceneGPU& S, V3 o, V3 d, float tMax, int li
         }
         const MatGPU& m = S.materials[is.material];
         if (!(m.flags & MF_TRANSMITS_SHADOWS)) return mk(0.0f);
-        T *= surfaceShadowTransmittance(m, is, d);
+        T *= surfaceShadowTransmittance(S, m, is, d);
         if (isBlack(T)) return T;
         origin = offsetRayOrigin(is.point, is.pError, len2(is.ng) > 0.0f ? is.ng : is.normal, d);
         remaining -= h.t;
@@ -747,7 +758,7 @@ __device__ __forceinline__ bool shadeSlot(const SceneGPU& S, const Paths& P, con
             // Camera-invisible light quads (for camera rays) and cutouts are passed through;
             // the vertex does not count (path_tracer.cpp:426-439).
             if (skips < 64 && ((cameraRay && (S.shapes[is.shape].flags & SF_CAMERA_INVISIBLE)) ||
-                               passesCutout(S.materials[is.material], sb))) {
+                               passesCutout(S, S.materials[is.material], is, sb))) {
                 const V3 no = offsetRayOrigin(is.point, is.pError, is.ng, dir);
                 ro = make_float4(no.x, no.y, no.z, ro.w);
                 if (cones) cone.x = cone.x + cone.y * smax(0.0f, is.t);

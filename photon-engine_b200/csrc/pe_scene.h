@@ -87,7 +87,7 @@ struct MatGPU {
     int32_t texAlbedo, texRoughness, texMetalness, texNormal;
     int32_t texMapping;
     float texScale;
-    float pad;
+    int32_t texOpacity;       // opacity map (DisneyMaterial::setOpacityImage), red channel
 };
 
 // An RGB float image (Image, Float32 storage) read by bilinear lookups with wrap; with mipmaps

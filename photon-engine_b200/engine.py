@@ -47,7 +47,7 @@ def _lib():
 # materials
 class Material:
     kind = -1
-    _maps = ("albedo", "roughness", "metalness", "normal")
+    _maps = ("albedo", "roughness", "metalness", "normal", "opacity")
 
     def __init__(self):
         self._m = capi.pe_material()
@@ -113,6 +113,11 @@ class DisneyMaterial(Material):
     def set_normal_image(self, image, mipmaps: bool = False):
         """DisneyMaterial::setNormalImage: a tangent-space normal map."""
         self._set_image("normal", image, mipmaps)
+
+    def set_opacity_image(self, image):
+        """DisneyMaterial::setOpacityImage: coverage = opacity × the image's red channel
+        (cutouts for camera, bounce and shadow rays)."""
+        self._set_image("opacity", image, False)
 
     def set_texture_mapping(self, box: bool):
         """DisneyMaterial::setTextureMapping: UV (False) or box projection (True)."""

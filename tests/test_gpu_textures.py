@@ -150,3 +150,37 @@ def test_mipmapped_maps_match_reference(pe, device, oracle):
     plain = pe.Film(st.width, st.height)
     device.render(cam, st, pe.RenderTargets(beauty=plain), 0, spp)
     assert pe.rel_mse(plain.resolve(), img) > 1e-4
+
+
+def test_opacity_map_matches_reference(pe, device, oracle):
+    """DisneyMaterial::setOpacityImage: coverage = opacity × the map's red channel for camera
+    and bounce rays (passesCutout, path_tracer.cpp:161-167) and for shadow rays
+    (shadowTransmittance, disney.cpp:511-513)."""
+    S = scenes()
+    scene, cam, st = S.cornell_box(64, 64, 8, 6, seed=0)
+    st.seed = 7
+    y, x = np.mgrid[0:32, 0:32].astype(np.float32) / 32.0
+    stripes = np.zeros((32, 32, 3), np.float32)
+    stripes[..., 0] = np.where(np.sin(2 * np.pi * 5 * (x + 0.3 * y)) > 0.0, 1.0, 0.15)
+    leaf = pe.DisneyMaterial((0.2, 0.6, 0.2), 0.0, 0.5, 0.5)
+    leaf.set_opacity_image(stripes)
+    pos, uv, idx = _grid_quad((0.8, 0.4, 1.2), (3.6, 0.0, 0.4), (0.0, 3.8, 0.0), 2)
+    scene.add_shape(pe.TriangleMesh(pos, None, uv, idx, leaf))
+    scene.build_accelerator()
+    device.set_scene(scene)
+    spp = 8
+    film = pe.Film(st.width, st.height)
+    device.render(cam, st, pe.RenderTargets(beauty=film), 0, spp)
+    mean_ref, cnt_ref = oracle.RefScene(scene).render(cam, st, 0, spp)
+    img = film.resolve()
+    err = pe.rel_mse(img, mean_ref)
+    same = float(np.mean(np.all(np.abs(img - mean_ref) <= 1e-4 * np.maximum(1.0, np.abs(mean_ref)), axis=-1)))
+    bias = float(img.mean() / max(1e-12, mean_ref.mean()) - 1.0)
+    assert err < 1e-4 and same > 0.99 and abs(bias) < 1e-3, (err, same, bias)
+    # the map shows: an opaque pane renders differently
+    leaf.images.clear()
+    scene.build_accelerator()
+    device.set_scene(scene)
+    opaque = pe.Film(st.width, st.height)
+    device.render(cam, st, pe.RenderTargets(beauty=opaque), 0, spp)
+    assert pe.rel_mse(opaque.resolve(), img) > 1e-3

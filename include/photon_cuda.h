@@ -178,6 +178,10 @@ int32_t pe_scene_set_light_link(pe_scene* s, int32_t light, int32_t mode, const 
  * order they were added: one per pe_scene_add_mesh, two per pe_scene_add_area_light (its two
  * triangles, as Scene::addLight adds them).  Call before pe_scene_build. */
 int32_t pe_scene_set_shadow_catcher(pe_scene* s, int32_t shape);
+/* Replaces material `index` of a scene (built or not) for an incremental update: its type,
+ * emission and the media, shadow-transmission and subsurface switches must stay as they were,
+ * else PE_ERR_LIMIT (rebuild the scene).  Then pe_device_update_materials sends it to a device. */
+int32_t pe_scene_set_material(pe_scene* s, int32_t index, const pe_material* m);
 /* An RGB float image (w*h*3, row 0 first) for the Disney image maps; returns its index (>= 0)
  * or a negative status.  Lookups are Image::sampleBilinear's (src/core/image/image.cpp:98-225):
  * bilinear, wrapping, without mipmaps. */
@@ -270,6 +274,10 @@ void pe_device_destroy(pe_device* d);
 int32_t pe_device_info_get(pe_device* d, pe_device_info* out);
 int32_t pe_device_set_scene(pe_device* d, const pe_scene* s);
 int32_t pe_device_has_scene(pe_device* d);
+/* RenderDevice::updateScene with SceneUpdateKind::Materials (src/engine/render_device.h:77-79):
+ * copies the material table of the scene last set (same build) to the device again, leaving its
+ * geometry, BVH, lights and textures in place. */
+int32_t pe_device_update_materials(pe_device* d, const pe_scene* s);
 
 /* RenderDevice::render: adds samples [first_sample, first_sample+count) to every
  * pixel and accumulates into the caller's host arrays exactly as

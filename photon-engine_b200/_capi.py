@@ -172,6 +172,8 @@ SIGNATURES = {
     "pe_scene_add_material": (C.c_int32, [P, C.POINTER(pe_material)]),
     "pe_scene_add_texture": (C.c_int32, [P, C.POINTER(C.c_float), C.c_int32, C.c_int32]),
     "pe_scene_build_texture_mipmaps": (C.c_int32, [P, C.c_int32]),
+    "pe_scene_set_material": (C.c_int32, [P, C.c_int32, C.POINTER(pe_material)]),
+    "pe_device_update_materials": (C.c_int32, [P, P]),
     "pe_scene_add_mesh": (C.c_int32, [P, FP, C.c_uint32, FP, FP, UP, C.c_uint32, C.c_int32]),
     "pe_scene_add_area_light": (C.c_int32, [P, FP, FP, FP, FP, C.c_int32]),
     "pe_scene_set_environment": (C.c_int32, [P, FP, C.c_int32, C.c_int32, C.c_float, C.c_float]),

@@ -1182,6 +1182,32 @@ int32_t pe_device_set_scene(pe_device* d, const pe_scene* s) {
     if (rc) return rc;
     d->scene = G;
     d->hasScene = true;
+    d->sceneSrc = s;
+    d->sceneVersion = s->version;
+    d->sceneMaterials = s->build.materials.size();
+    ++d->sceneSerial;
+    return PE_OK;
+}
+
+// RenderDevice::updateScene(scene, SceneUpdateKind::Materials) (render_device.h:77-79): the
+// material table of the scene already set is copied again; its geometry, BVH, lights and
+// textures stay on the device.
+int32_t pe_device_update_materials(pe_device* d, const pe_scene* s) {
+    if (!d || !s) {
+        setError("pe_device_update_materials: null argument");
+        return PE_ERR_INVALID;
+    }
+    if (!d->hasScene || d->sceneSrc != s || d->sceneVersion != s->version || !s->built ||
+        s->build.materials.size() != d->sceneMaterials) {
+        setError("pe_device_update_materials: the device holds another build of the scene (call pe_device_set_scene)");
+        return PE_ERR_INVALID;
+    }
+    PE_CUDA(cudaSetDevice(d->ordinal));
+    PE_CUDA(cudaStreamSynchronize(d->stream));
+    PE_CUDA(cudaStreamSynchronize(d->lanes[1].stream));
+    PE_CUDA(cudaMemcpyAsync(const_cast<MatGPU*>(d->scene.materials), s->build.materials.data(),
+                            s->build.materials.size() * sizeof(MatGPU), cudaMemcpyHostToDevice, d->stream));
+    PE_CUDA(cudaStreamSynchronize(d->stream));
     ++d->sceneSerial;
     return PE_OK;
 }

@@ -171,7 +171,10 @@ struct pe_device {
     uint8_t* adaptClean = nullptr;
     uint32_t* adaptCount = nullptr;
     size_t adaptPixels = 0;
-    int32_t lightGroups = 0;        // light groups of the scene set (its pass films need one each)
+    int32_t lightGroups = 0;
+    const pe_scene* sceneSrc = nullptr; // the scene last set, and its build version
+    uint64_t sceneVersion = 0;
+    size_t sceneMaterials = 0;        // light groups of the scene set (its pass films need one each)
     TablesGPU* dTables = nullptr;
     TablesGPU hTables{};
     // pixel-filter inverse CDFs, one slot per (type, width) in use, least recently used replaced

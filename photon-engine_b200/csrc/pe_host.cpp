@@ -1152,6 +1152,40 @@ int32_t pe_scene_add_material(pe_scene* s, const pe_material* m) {
     return static_cast<int32_t>(s->materials.size() - 1);
 }
 
+int32_t pe_scene_set_material(pe_scene* s, int32_t index, const pe_material* m) {
+    if (!s || !m || index < 0 || index >= static_cast<int32_t>(s->materialsIn.size())) {
+        setError("pe_scene_set_material: bad argument");
+        return PE_ERR_INVALID;
+    }
+    for (int32_t t : {m->albedo_texture, m->roughness_texture, m->metalness_texture, m->normal_texture,
+                      m->opacity_texture})
+        if (t < -1 || t >= static_cast<int32_t>(s->textures.size())) {
+            setError("pe_scene_set_material: texture index " + std::to_string(t) + " not added");
+            return PE_ERR_INVALID;
+        }
+    const MatGPU g = resolveMaterial(*m);
+    const MatGPU& old = s->materials[static_cast<size_t>(index)];
+    // what the built scene derived from the material (its lights, the triangles' shading keys,
+    // the media, shadow and walk switches) must stay as it is
+    const int32_t structural = MF_EMISSIVE | MF_DELTA | MF_VOLUME_BOUNDARY | MF_TRANSMITS_SHADOWS | MF_DISPERSIVE |
+                               MF_HAS_MEDIUM | MF_MEDIUM_SCATTERS;
+    const bool walks = g.type == PE_MAT_DISNEY && g.subsurface > 0.0f;
+    const bool walked = old.type == PE_MAT_DISNEY && old.subsurface > 0.0f;
+    const bool emissionMoved = g.emission[0] != old.emission[0] || g.emission[1] != old.emission[1] ||
+                               g.emission[2] != old.emission[2];
+    if (g.type != old.type || (g.flags & structural) != (old.flags & structural) || walks != walked ||
+        emissionMoved) {
+        setError("pe_scene_set_material: the change needs a full rebuild (type, emission, media, shadow or walk "
+                 "properties differ)");
+        return PE_ERR_LIMIT;
+    }
+    s->materialsIn[static_cast<size_t>(index)] = *m;
+    s->materials[static_cast<size_t>(index)] = g;
+    if (s->built && static_cast<size_t>(index) < s->build.materials.size()) s->build.materials[static_cast<size_t>(index)] = g;
+    ++s->materialVersion;
+    return PE_OK;
+}
+
 int32_t pe_scene_add_mesh(pe_scene* s, const float* positions, uint32_t nv, const float* normals, const float* uvs,
                           const uint32_t* indices, uint32_t ntri, int32_t material) {
     if (!s || (nv && !positions) || (ntri && !indices)) {

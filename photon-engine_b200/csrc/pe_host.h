@@ -109,6 +109,7 @@ struct pe_scene {
     std::string envLightGroup;                 // the environment's Light::setLightGroup
     pe::HostBuild build;
     uint64_t version = 0;
+    uint64_t materialVersion = 0; // pe_scene_set_material edits since the build
 };
 
 namespace pe {

@@ -279,6 +279,7 @@ class Scene:
         self.shape_tags: dict[int, int] = {}
         self.light_links: dict[int, tuple] = {}
         self.light_groups: dict[int, str] = {}
+        self._tex_index: dict = {}
 
     def __del__(self):
         try:
@@ -355,6 +356,21 @@ class Scene:
                     out.append(img)
         return out
 
+    def sync_materials(self) -> bool:
+        """Sends every material's current parameters to the built scene without rebuilding it
+        (pe_scene_set_material); False when some change needs a rebuild (type, emission, media,
+        shadow or walk switches, a new image)."""
+        if not self._handle:
+            return False
+        lib = _lib()
+        for m in self.materials():
+            idx = self._mat_index.get(id(m))
+            if idx is None or any(id(img) not in self._tex_index for img in getattr(m, "images", {}).values()):
+                return False
+            if lib.pe_scene_set_material(self._handle, idx, C.byref(m.struct_with(self._tex_index))) != capi.PE_OK:
+                return False
+        return True
+
     def texture_has_mipmaps(self, img) -> bool:
         return any(id(img) in getattr(m, "mipmapped", ()) for m in self.materials())
 
@@ -374,6 +390,7 @@ class Scene:
             if self.texture_has_mipmaps(img):
                 capi.check(lib.pe_scene_build_texture_mipmaps(h, t))
             tex_index[id(img)] = t
+        self._tex_index = tex_index
         mat_index = {}
         for m in self.materials():
             idx = lib.pe_scene_add_material(h, C.byref(m.struct_with(tex_index)))
@@ -715,8 +732,16 @@ class CudaDevice:
         capi.check(_lib().pe_device_set_scene(self._h, scene.handle))
         self._scene = scene
 
-    def update_scene(self, scene: Scene, kind: SceneUpdateKind = SceneUpdateKind.Full):
+    def update_scene(self, scene: Scene, kind: SceneUpdateKind = SceneUpdateKind.Full) -> bool:
+        """RenderDevice::updateScene.  Materials: the edited parameters go to the device without a
+        rebuild when the change allows it (returns True); otherwise, and for the other kinds, the
+        scene is rebuilt and set again (returns False)."""
+        if kind == SceneUpdateKind.Materials and self._scene is scene and scene.sync_materials():
+            if _lib().pe_device_update_materials(self._h, scene.handle) == capi.PE_OK:
+                return True
+        scene.build_accelerator()
         self.set_scene(scene)
+        return False
 
     def has_scene(self) -> bool:
         return bool(_lib().pe_device_has_scene(self._h))

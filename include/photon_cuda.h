@@ -38,7 +38,7 @@
 extern "C" {
 #endif
 
-#define PE_ABI_VERSION 8
+#define PE_ABI_VERSION 9
 
 typedef enum pe_status {
     PE_OK = 0,
@@ -178,6 +178,10 @@ int32_t pe_scene_set_light_link(pe_scene* s, int32_t light, int32_t mode, const 
  * order they were added: one per pe_scene_add_mesh, two per pe_scene_add_area_light (its two
  * triangles, as Scene::addLight adds them).  Call before pe_scene_build. */
 int32_t pe_scene_set_shadow_catcher(pe_scene* s, int32_t shape);
+/* Scene::setShapeName / setMaterialName: the names the Cryptomatte ids hash (unnamed shapes are
+ * "object_<node uid>" or "shape_<n>", unnamed materials "material_<n>", renderer.cpp:75-118). */
+int32_t pe_scene_set_shape_name(pe_scene* s, int32_t shape, const char* name);
+int32_t pe_scene_set_material_name(pe_scene* s, int32_t material, const char* name);
 /* Replaces material `index` of a scene (built or not) for an incremental update: its type,
  * emission and the media, shadow-transmission and subsurface switches must stay as they were,
  * else PE_ERR_LIMIT (rebuild the scene).  Then pe_device_update_materials sends it to a device. */
@@ -329,6 +333,11 @@ typedef struct pe_pass_films {
     int32_t n_groups;           /* must equal pe_scene_light_groups of the device's scene */
     int32_t pad;
     pe_film_arrays groups[PE_MAX_LIGHT_GROUPS]; /* one per light group, in Scene::lightGroupNames order */
+    /* Cryptomatte (CryptoFilm, src/core/image/cryptomatte.h): when not NULL, count·w·h floats
+     * each, the object and material id of every sample (index (sample − first)·w·h + y·w + x;
+     * 0 on a miss), for the caller's CryptoFilm::addSample */
+    float* crypto_object;
+    float* crypto_material;
 } pe_pass_films;
 /* pe_device_render plus the render passes and, when aovs is not NULL, the AOV films of the same
  * samples (RenderDevice::render with RenderTargets::passes; tracePixel with wantPasses,

@@ -70,6 +70,9 @@ def _load(fast: bool = False):
         "ref_scene_set_shadow_catcher": (C.c_int32, [P, C.c_int32]),
         "ref_scene_set_light_group": (C.c_int32, [P, C.c_int32, C.c_char_p]),
         "ref_scene_add_texture": (C.c_int32, [P, FP, C.c_int32, C.c_int32]),
+        "ref_render_crypto": (C.c_int32, [P, C.c_void_p, C.c_void_p, C.c_int32, C.c_int32, C.c_int32, FP, C.c_int32]),
+        "ref_scene_set_shape_name": (C.c_int32, [P, C.c_int32, C.c_char_p]),
+        "ref_scene_set_material_name": (C.c_int32, [P, C.c_int32, C.c_char_p]),
         "ref_scene_build_texture_mipmaps": (C.c_int32, [P, C.c_int32]),
         "ref_film_create": (P, [C.c_int32, C.c_int32]),
         "ref_film_destroy": (None, [P]),
@@ -162,6 +165,11 @@ class RefScene:
         for shape, uid in getattr(scene, "shape_tags", {}).items():
             if self.lib.ref_scene_tag_shape(self.h, int(shape), int(uid)) != 0:
                 raise RuntimeError("reference rejected a shape tag")
+        for shape, name in getattr(scene, "shape_names", {}).items():
+            self.lib.ref_scene_set_shape_name(self.h, int(shape), name.encode())
+        for mat, name in getattr(scene, "material_names", {}).values():
+            if id(mat) in mat_index:
+                self.lib.ref_scene_set_material_name(self.h, mat_index[id(mat)], name.encode())
         for light, (mode, uids, smode, suids) in getattr(scene, "light_links", {}).items():
             a = (C.c_uint64 * max(1, len(uids)))(*uids)
             b = (C.c_uint64 * max(1, len(suids)))(*suids)
@@ -235,6 +243,14 @@ class RefScene:
         (adaptive sampling reads it); returns the samples traced."""
         return int(self.lib.ref_render_film(self.h, C.byref(camera.describe_gpu()), C.byref(settings.to_c()), first,
                                             count, threads, film.h))
+
+    def render_crypto(self, camera, settings, first: int, count: int, k: int = 8, threads: int = 0):
+        """CryptoFilm::pixelRanks of the object and material films after renderSamples with passes
+        (seed 12345): (2, h, w, k, 2) of (id, coverage), unused entries 0."""
+        out = np.zeros((2, settings.height, settings.width, k, 2), np.float32)
+        self.lib.ref_render_crypto(self.h, C.byref(camera.describe_gpu()), C.byref(settings.to_c()), first, count,
+                                   threads, _f(out), k)
+        return out
 
     def render_passes(self, camera, settings, first: int, count: int, threads: int = 0):
         """Renderer::renderSamples with RenderPassFilms (seed 12345): mean beauty, counts, the eight

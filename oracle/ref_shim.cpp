@@ -467,6 +467,48 @@ int32_t ref_render_passes(void* s, const pe_camera* cam, const pe_settings* st, 
     return n;
 }
 
+// Renderer::renderSamples with RenderPassFilms and both CryptoFilms on (seed 12345): per pixel
+// the first `k` entries of CryptoFilm::pixelRanks (id, coverage) of the object film, then of the
+// material film, into out[2][h][w][k][2] (unused entries 0).
+int32_t ref_render_crypto(void* s, const pe_camera* cam, const pe_settings* st, int32_t first, int32_t count,
+                          int32_t threads, float* out, int32_t k) {
+    auto* rs = static_cast<RefScene*>(s);
+    DescCamera camera(*cam);
+    RenderSettings settings = toSettings(*st, threads > 0 ? threads : hardwareThreads());
+    Film film(st->width, st->height);
+    RenderPassFilms passes;
+    passes.resize(st->width, st->height);
+    Renderer renderer;
+    renderer.renderSamples(rs->scene, camera, settings, film, first, count, nullptr, nullptr, &passes);
+    const CryptoFilm* films[2] = {&passes.cryptoObject, &passes.cryptoMaterial};
+    for (int f = 0; f < 2; ++f)
+        for (int y = 0; y < st->height; ++y)
+            for (int x = 0; x < st->width; ++x) {
+                const auto ranks = films[f]->pixelRanks(x, y);
+                float* o = out + ((static_cast<size_t>(f) * st->height + y) * st->width + x) * static_cast<size_t>(k) * 2;
+                for (int j = 0; j < k && j < static_cast<int>(ranks.size()); ++j) {
+                    o[2 * j] = ranks[static_cast<size_t>(j)].first;
+                    o[2 * j + 1] = ranks[static_cast<size_t>(j)].second;
+                }
+            }
+    return 0;
+}
+
+// Scene::setShapeName / setMaterialName of the `i`-th shape / material added.
+int32_t ref_scene_set_shape_name(void* s, int32_t shape, const char* name) {
+    auto* rs = static_cast<RefScene*>(s);
+    const auto& shapes = rs->scene.shapes();
+    if (shape < 0 || shape >= static_cast<int32_t>(shapes.size())) return -1;
+    rs->scene.setShapeName(shapes[static_cast<size_t>(shape)].get(), name ? name : "");
+    return 0;
+}
+int32_t ref_scene_set_material_name(void* s, int32_t material, const char* name) {
+    auto* rs = static_cast<RefScene*>(s);
+    if (material < 0 || material >= static_cast<int32_t>(rs->materials.size())) return -1;
+    rs->scene.setMaterialName(rs->materials[static_cast<size_t>(material)].get(), name ? name : "");
+    return 0;
+}
+
 int32_t ref_render_guided(void* s, const pe_camera* cam, const pe_settings* st, int32_t first, int32_t count,
                           int32_t threads, float* mean_rgb, uint32_t* counts) {
     auto* rs = static_cast<RefScene*>(s);

@@ -124,7 +124,8 @@ class pe_film_arrays(C.Structure):
 class pe_pass_films(C.Structure):
     _fields_ = [("light", pe_film_arrays * PE_LIGHT_PASSES), ("depth", pe_film_arrays), ("position", pe_film_arrays),
                 ("object_id", pe_film_arrays), ("material_id", pe_film_arrays), ("n_groups", C.c_int32),
-                ("pad", C.c_int32), ("groups", pe_film_arrays * PE_MAX_LIGHT_GROUPS)]
+                ("pad", C.c_int32), ("groups", pe_film_arrays * PE_MAX_LIGHT_GROUPS),
+                ("crypto_object", C.POINTER(C.c_float)), ("crypto_material", C.POINTER(C.c_float))]
 
 
 class pe_request_desc(C.Structure):
@@ -173,6 +174,8 @@ SIGNATURES = {
     "pe_scene_add_texture": (C.c_int32, [P, C.POINTER(C.c_float), C.c_int32, C.c_int32]),
     "pe_scene_build_texture_mipmaps": (C.c_int32, [P, C.c_int32]),
     "pe_scene_set_material": (C.c_int32, [P, C.c_int32, C.POINTER(pe_material)]),
+    "pe_scene_set_shape_name": (C.c_int32, [P, C.c_int32, C.c_char_p]),
+    "pe_scene_set_material_name": (C.c_int32, [P, C.c_int32, C.c_char_p]),
     "pe_device_update_materials": (C.c_int32, [P, P]),
     "pe_scene_add_mesh": (C.c_int32, [P, FP, C.c_uint32, FP, FP, UP, C.c_uint32, C.c_int32]),
     "pe_scene_add_area_light": (C.c_int32, [P, FP, FP, FP, FP, C.c_int32]),

@@ -623,6 +623,9 @@ int32_t renderWaves(pe_device* d, const pe_camera* cam, const pe_settings* st, i
     base.aov = scratch ? nullptr : d->aovTarget;
     base.pass = scratch ? nullptr : d->passTarget;
     base.pixList = pixList;
+    base.cryptoObj = scratch ? nullptr : d->cryptoObj;
+    base.cryptoMat = scratch ? nullptr : d->cryptoMat;
+    base.cryptoFirst = d->cryptoFirst;
     RenderTimer tm;
     tm.timing = timing;
     bool cancelled = false;
@@ -1341,17 +1344,30 @@ static int32_t renderTargets(pe_device* d, const pe_camera* cam, const pe_settin
         }
         PE_CUDA(cudaMemsetAsync(d->passFilm, 0, passFloats * sizeof(float), d->stream));
     }
+    // per-sample Cryptomatte ids: a device buffer for the call, freed on return
+    const size_t cryptoFloats = static_cast<size_t>(count) * n;
+    float* cryptoBuf = nullptr;
+    if (passes && passes->crypto_object && passes->crypto_material) {
+        PE_CUDA(cudaMalloc(&cryptoBuf, 2 * cryptoFloats * sizeof(float)));
+        PE_CUDA(cudaMemsetAsync(cryptoBuf, 0, 2 * cryptoFloats * sizeof(float), d->stream));
+    }
     d->aovTarget = aovs ? d->aovFilm : nullptr;
     d->passTarget = passes ? d->passFilm : nullptr;
     d->passStride = passes ? stride : 0;
+    d->cryptoObj = cryptoBuf;
+    d->cryptoMat = cryptoBuf ? cryptoBuf + cryptoFloats : nullptr;
+    d->cryptoFirst = first;
     struct Reset {
         pe_device* d;
+        float* buf;
         ~Reset() {
             d->aovTarget = nullptr;
             d->passTarget = nullptr;
             d->passStride = 0;
+            d->cryptoObj = d->cryptoMat = nullptr;
+            if (buf) cudaFree(buf);
         }
-    } reset{d};
+    } reset{d, cryptoBuf};
     rc = pe_device_render(d, cam, st, first, count, cancel, sumRgb, sampleCount, sumLumSq, traced);
     if (rc != PE_OK && rc != PE_ERR_CANCELLED) return rc;
     if (aovs) {
@@ -1376,6 +1392,13 @@ static int32_t renderTargets(pe_device* d, const pe_camera* cam, const pe_settin
         for (int f = 0; f < PFILM_GROUPS + d->lightGroups; ++f)
             mergeFilm(h.data() + static_cast<size_t>(f) * 5 * n, n, films[f]->sum, films[f]->count,
                       f == PFILM_POSITION ? nullptr : films[f]->sum_sq);
+        if (cryptoBuf) {
+            PE_CUDA(cudaMemcpyAsync(passes->crypto_object, cryptoBuf, cryptoFloats * sizeof(float),
+                                    cudaMemcpyDeviceToHost, d->stream));
+            PE_CUDA(cudaMemcpyAsync(passes->crypto_material, cryptoBuf + cryptoFloats, cryptoFloats * sizeof(float),
+                                    cudaMemcpyDeviceToHost, d->stream));
+            PE_CUDA(cudaStreamSynchronize(d->stream));
+        }
     }
     return rc;
 }

@@ -212,6 +212,9 @@ struct pe_device {
     float* aovFilm = nullptr;       // device AOV films (15 floats per pixel)
     size_t aovFilmPixels = 0;
     float* passTarget = nullptr;    // render-pass films of the render in progress (pe_device_render_passes)
+    float* cryptoObj = nullptr;     // per-sample Cryptomatte ids of that render (or null)
+    float* cryptoMat = nullptr;
+    int32_t cryptoFirst = 0;
     int32_t passStride = 0;         // its per-path block (PASS_GROUPS + light groups)
     float* passFilm = nullptr;      // device pass films (5 floats per pixel per film)
     size_t passFilmFloats = 0;

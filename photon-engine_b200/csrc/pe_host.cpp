@@ -748,6 +748,45 @@ V3 idColorOf(uint64_t id) {
     }
 }
 
+// MurmurHash3_x86_32 (Austin Appleby's public-domain hash, seed 0): the Cryptomatte 1.2 name
+// hash (cryptomatte.cpp:36-78).
+uint32_t murmur3(const std::string& key) {
+    auto rotl = [](uint32_t x, int r) { return (x << r) | (x >> (32 - r)); };
+    const size_t len = key.size();
+    const auto* bytes = reinterpret_cast<const uint8_t*>(key.data());
+    uint32_t h = 0u;
+    const uint32_t c1 = 0xcc9e2d51u, c2 = 0x1b873593u;
+    size_t i = 0;
+    for (; i + 4 <= len; i += 4) {
+        uint32_t k = static_cast<uint32_t>(bytes[i]) | (static_cast<uint32_t>(bytes[i + 1]) << 8) |
+                     (static_cast<uint32_t>(bytes[i + 2]) << 16) | (static_cast<uint32_t>(bytes[i + 3]) << 24);
+        k = rotl(k * c1, 15) * c2;
+        h = rotl(h ^ k, 13) * 5u + 0xe6546b64u;
+    }
+    uint32_t k = 0u;
+    for (size_t j = len - i; j > 0; --j) k = (k << 8) | bytes[i + j - 1];
+    if (len - i > 0) h ^= rotl(k * c1, 15) * c2;
+    h ^= static_cast<uint32_t>(len);
+    h ^= h >> 16;
+    h *= 0x85ebca6bu;
+    h ^= h >> 13;
+    h *= 0xc2b2ae35u;
+    h ^= h >> 16;
+    return h;
+}
+
+// The hash as a float id (cryptoHashToFloat, cryptomatte.cpp:82-92): exponents 0 and 255 have
+// their lowest bit flipped, so the id is a finite, normal float.
+float cryptoId(const std::string& name) {
+    if (name.empty()) return 0.0f;
+    uint32_t h = murmur3(name);
+    const uint32_t e = (h >> 23) & 0xFFu;
+    if (e == 0u || e == 0xFFu) h = (h & 0x807FFFFFu) | ((e ^ 1u) << 23);
+    float f;
+    std::memcpy(&f, &h, sizeof(f));
+    return f;
+}
+
 } // namespace
 
 const TablesGPU& staticTables() {
@@ -1073,6 +1112,29 @@ static int32_t buildScene(pe_scene* s) {
         const V3 c = idColorOf(static_cast<uint64_t>(m) + 1ull);
         B.idColor[B.shapes.size() + m] = f4(c.x, c.y, c.z, 0.0f);
     }
+    // Cryptomatte ids in w (buildCryptoLookup, renderer.cpp:75-118): a shape by its name, else
+    // "object_<node uid>", else "shape_<n>" counting the unnamed untagged shapes; a material by
+    // its name, else "material_<n>" counting unnamed materials as the shapes first use them
+    {
+        size_t anonShape = 0, anonMat = 0;
+        std::vector<int> matSeen(s->materials.size(), 0);
+        for (size_t i = 0; i < B.shapes.size(); ++i) {
+            const std::string& nm = i < s->shapeNames.size() ? s->shapeNames[i] : std::string();
+            const uint64_t uid = i < s->shapeUid.size() ? s->shapeUid[i] : 0ull;
+            const std::string name = !nm.empty() ? nm
+                                   : uid != 0 ? "object_" + std::to_string(uid)
+                                              : "shape_" + std::to_string(anonShape++);
+            B.idColor[i].w = cryptoId(name);
+            const int mi = B.shapes[i].material;
+            if (mi >= 0 && static_cast<size_t>(mi) < s->materials.size() && !matSeen[static_cast<size_t>(mi)]) {
+                matSeen[static_cast<size_t>(mi)] = 1;
+                const std::string& mn = static_cast<size_t>(mi) < s->materialNames.size() ? s->materialNames[static_cast<size_t>(mi)]
+                                                                                         : std::string();
+                B.idColor[B.shapes.size() + static_cast<size_t>(mi)].w =
+                    cryptoId(!mn.empty() ? mn : "material_" + std::to_string(anonMat++));
+            }
+        }
+    }
     s->built = true;
     ++s->version;
     return PE_OK;
@@ -1374,6 +1436,29 @@ int32_t pe_scene_build_texture_mipmaps(pe_scene* s, int32_t texture) {
         pw = nw;
         ph = nh;
     }
+    s->built = false;
+    return PE_OK;
+}
+
+int32_t pe_scene_set_shape_name(pe_scene* s, int32_t shape, const char* name) {
+    if (!s || shape < 0) {
+        setError("pe_scene_set_shape_name: bad argument");
+        return PE_ERR_INVALID;
+    }
+    if (s->shapeNames.size() <= static_cast<size_t>(shape)) s->shapeNames.resize(static_cast<size_t>(shape) + 1);
+    s->shapeNames[static_cast<size_t>(shape)] = name ? name : "";
+    s->built = false;
+    return PE_OK;
+}
+
+int32_t pe_scene_set_material_name(pe_scene* s, int32_t material, const char* name) {
+    if (!s || material < 0) {
+        setError("pe_scene_set_material_name: bad argument");
+        return PE_ERR_INVALID;
+    }
+    if (s->materialNames.size() <= static_cast<size_t>(material))
+        s->materialNames.resize(static_cast<size_t>(material) + 1);
+    s->materialNames[static_cast<size_t>(material)] = name ? name : "";
     s->built = false;
     return PE_OK;
 }

@@ -107,6 +107,8 @@ struct pe_scene {
     std::vector<pe::HostLightLink> lightLinks; // Light::setLightLink, by explicit light index
     std::vector<std::string> lightGroups;      // Light::setLightGroup, by light index ("" = none)
     std::string envLightGroup;                 // the environment's Light::setLightGroup
+    std::vector<std::string> shapeNames;       // Scene::setShapeName ("" = unnamed)
+    std::vector<std::string> materialNames;    // Scene::setMaterialName
     pe::HostBuild build;
     uint64_t version = 0;
     uint64_t materialVersion = 0; // pe_scene_set_material edits since the build

@@ -778,6 +778,8 @@ __device__ __forceinline__ bool shadeSlot(const SceneGPU& S, const Paths& P, con
                 const float4 oc = S.idColor[is.shape];
                 b[PASS_OBJECT] = make_float4(oc.x, oc.y, oc.z, 1.0f);
                 b[PASS_MATERIAL] = S.idColor[S.nShapes + is.material];
+                // Cryptomatte ids ride in the w of the id colours (renderer.cpp:170-175)
+                b[PASS_CRYPTO] = make_float4(oc.w, b[PASS_MATERIAL].w, 0.0f, 0.0f);
             }
             if ((flags & PF_FIRST_SEGMENT) && OUT && P.aovA) {
                 const int path = pathOfSlot(P, slot);
@@ -1358,6 +1360,15 @@ __device__ __noinline__ void filmPasses(const Paths& P, const WaveSeg& A, int p,
         fsum[3 * pix + 2] = b;
         fsq[pix] = q;
         fcnt[pix] = c;
+    }
+    if (A.cryptoObj) {
+        // each sample's Cryptomatte ids; the host adds them to its CryptoFilms
+        for (int s = 0; s < A.nSamples; ++s) {
+            const float4 id = passBlock(P, A.slotFirst + s * A.nPix + p)[PASS_CRYPTO];
+            const size_t o = static_cast<size_t>(A.sampleFirst + s - A.cryptoFirst) * n + static_cast<size_t>(pix);
+            A.cryptoObj[o] = id.x;
+            A.cryptoMat[o] = id.y;
+        }
     }
 }
 

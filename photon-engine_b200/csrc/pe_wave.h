@@ -113,9 +113,10 @@ struct Paths {
 // A path's render-pass block (float4 slots): the eight light passes (LightPass order), the
 // lobe shares of the first bounce (firstLobe, path_tracer.cpp:375), the camera ray's origin and
 // then the first hit (xyz, w = distance), the object and material id colours (w of the object
-// slot: 1 on a hit), then one slot per light group.
+// slot: 1 on a hit), the Cryptomatte object and material ids of the hit, then one slot per
+// light group.
 enum PassSlots { PASS_DIFFUSE_DIRECT = 0, PASS_EMISSION = 6, PASS_BACKGROUND = 7, PASS_LOBES = 8, PASS_HIT = 11,
-                 PASS_OBJECT = 12, PASS_MATERIAL = 13, PASS_GROUPS = 14 };
+                 PASS_OBJECT = 12, PASS_MATERIAL = 13, PASS_CRYPTO = 14, PASS_GROUPS = 15 };
 // Films of the pass target, 5 floats per pixel each (sum 3n, count n, sum of squares n).
 enum PassFilms { PFILM_DEPTH = 8, PFILM_POSITION = 9, PFILM_OBJECT = 10, PFILM_MATERIAL = 11, PFILM_GROUPS = 12 };
 
@@ -153,6 +154,9 @@ struct WaveSeg {
     float* sq;
     float* aov;             // AOV films (albedo, normal, alpha: each sum 3n, count n, sum of squares n), or null
     float* pass;            // render-pass films (PassFilms order, 5n floats each), or null
+    float* cryptoObj;       // Cryptomatte ids per (sample − cryptoFirst, film pixel), or null
+    float* cryptoMat;
+    int cryptoFirst;
     int slotFirst;
     int pixFirst;
     int flags;              // SegFlags

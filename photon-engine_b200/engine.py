@@ -280,6 +280,8 @@ class Scene:
         self.light_links: dict[int, tuple] = {}
         self.light_groups: dict[int, str] = {}
         self._tex_index: dict = {}
+        self.shape_names: dict[int, str] = {}
+        self.material_names: dict[int, tuple] = {}
 
     def __del__(self):
         try:
@@ -313,6 +315,14 @@ class Scene:
         listed node uids, 2 exclude them."""
         self.light_links[int(light)] = (int(mode), [int(u) for u in uids], int(shadow_mode),
                                         [int(u) for u in shadow_uids])
+
+    def set_shape_name(self, shape: int, name: str):
+        """Scene::setShapeName: the name the shape's Cryptomatte id hashes."""
+        self.shape_names[int(shape)] = str(name)
+
+    def set_material_name(self, material, name: str):
+        """Scene::setMaterialName: the name the material's Cryptomatte id hashes."""
+        self.material_names[id(material)] = (material, str(name))
 
     def set_light_group(self, light: int, name: str):
         """Light::setLightGroup of light `light` (numbered as set_light_link numbers them); an
@@ -410,6 +420,11 @@ class Scene:
             capi.check(lib.pe_scene_set_shadow_catcher(h, int(self.shadow_catcher)))
         for shape, uid in self.shape_tags.items():
             capi.check(lib.pe_scene_tag_shape(h, shape, uid))
+        for shape, name in self.shape_names.items():
+            capi.check(lib.pe_scene_set_shape_name(h, shape, name.encode()))
+        for mat, name in self.material_names.values():
+            if id(mat) in mat_index:
+                capi.check(lib.pe_scene_set_material_name(h, mat_index[id(mat)], name.encode()))
         groups, li = {}, 0
         for kind, obj in self.ops:
             if kind == "mesh":
@@ -601,6 +616,36 @@ class LightPass(enum.IntEnum):
     Background = 7
 
 
+class CryptoFilm:
+    """CryptoFilm (cryptomatte.h): per pixel the samples taken and the count of each Cryptomatte
+    id (a float hash of an object or material name) among them."""
+
+    def __init__(self, width: int, height: int):
+        self.width, self.height = width, height
+        self.total = np.zeros((height, width), np.uint32)
+        self.counts: dict = {}   # (y, x) → {id: count}
+
+    def add_samples(self, ids: np.ndarray, taken: np.ndarray):
+        """CryptoFilm::addSample for each sample: ids (n, h, w), taken (n, h, w) bool."""
+        self.total += taken.sum(axis=0).astype(np.uint32)
+        n, h, w = ids.shape
+        flat = ids.reshape(n, -1)
+        hit = (flat != 0.0) & taken.reshape(n, -1)
+        for p in np.nonzero(hit.any(axis=0))[0]:
+            vals, cnt = np.unique(flat[hit[:, p], p], return_counts=True)
+            d = self.counts.setdefault((int(p) // w, int(p) % w), {})
+            for v, c in zip(vals.tolist(), cnt.tolist()):
+                d[v] = d.get(v, 0) + int(c)
+
+    def pixel_ranks(self, x: int, y: int):
+        """CryptoFilm::pixelRanks: (id, coverage) by falling coverage."""
+        d = self.counts.get((y, x), {})
+        t = int(self.total[y, x])
+        if t == 0:
+            return []
+        return sorted(((i, c / t) for i, c in d.items()), key=lambda e: -e[1])
+
+
 class RenderPassFilms:
     """RenderPassFilms (renderer.h:59-98): the eight light passes (their sum is the beauty film),
     the data passes of the first hit (depth, position, object and material id colours) and one
@@ -613,6 +658,13 @@ class RenderPassFilms:
         self.object_id = Film(width, height)
         self.material_id = Film(width, height)
         self.light_groups: list[tuple[str, Film]] = []
+        self.crypto_object: Optional[CryptoFilm] = None    # enable_cryptomatte
+        self.crypto_material: Optional[CryptoFilm] = None
+
+    def enable_cryptomatte(self):
+        """CryptoObject and CryptoMaterial films (the reference fills them when they are sized)."""
+        w, h = self.depth.width, self.depth.height
+        self.crypto_object, self.crypto_material = CryptoFilm(w, h), CryptoFilm(w, h)
 
     def init_light_groups(self, width: int, height: int, names):
         self.light_groups = [(n, Film(width, height)) for n in names]
@@ -773,6 +825,12 @@ class CudaDevice:
                         f.width != film.width or f.height != film.height for _, f in passes.light_groups):
                     passes.init_light_groups(film.width, film.height, names)
                 pout = passes.to_c()
+                crypto = None
+                if passes.crypto_object is not None:
+                    crypto = (np.zeros((count, film.height, film.width), np.float32),
+                              np.zeros((count, film.height, film.width), np.float32))
+                    pout.crypto_object, pout.crypto_material = capi.fptr(crypto[0]), capi.fptr(crypto[1])
+                    counts_before = film.count.copy()
                 aout = None
                 if aovs is not None:
                     aout = capi.pe_aov_films(capi.fptr(aovs.albedo.sum), capi.uptr(aovs.albedo.count),
@@ -784,6 +842,11 @@ class CudaDevice:
                                                     capi.fptr(film.sum), capi.uptr(film.count), capi.fptr(film.sum_sq),
                                                     C.byref(aout) if aout is not None else None, C.byref(pout),
                                                     C.byref(traced))
+                if crypto is not None and rc == capi.PE_OK:
+                    # every pixel took every sample unless adaptive sampling stopped it
+                    taken = np.arange(count)[:, None, None] < (film.count - counts_before)[None]
+                    passes.crypto_object.add_samples(crypto[0], taken)
+                    passes.crypto_material.add_samples(crypto[1], taken)
             elif aovs is not None:
                 out = capi.pe_aov_films(capi.fptr(aovs.albedo.sum), capi.uptr(aovs.albedo.count),
                                         capi.fptr(aovs.albedo.sum_sq), capi.fptr(aovs.normal.sum),

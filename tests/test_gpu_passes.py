@@ -152,3 +152,34 @@ def test_passes_with_aovs_and_across_batches(pe, device):
         pass
     assert sess.passes is not None and not sess.warnings
     assert int(sess.passes.light[0].count.min()) == 4
+
+
+def test_cryptomatte_matches_reference(pe, device, oracle):
+    """CryptoObject / CryptoMaterial (CryptoFilm, cryptomatte.cpp; ids of the first hit,
+    renderer.cpp:170-175, named as buildCryptoLookup names them, renderer.cpp:75-118): per pixel
+    the same ids with the same coverage as the reference's pixelRanks."""
+    scene, cam, st = _pass_scene(pe)
+    scene.set_shape_name(0, "Floor")
+    metal = scene.ops[1][1].material
+    scene.set_material_name(metal, "BrushedGold")
+    scene.build_accelerator()
+    device.set_scene(scene)
+    spp = 8
+    passes = pe.RenderPassFilms(st.width, st.height)
+    passes.enable_cryptomatte()
+    device.render(cam, st, pe.RenderTargets(beauty=pe.Film(st.width, st.height), passes=passes), 0, spp)
+    ref = oracle.RefScene(scene).render_crypto(cam, st, 0, spp)
+    worst = 0.0
+    ids = set()
+    for f, film in enumerate((passes.crypto_object, passes.crypto_material)):
+        for y in range(st.height):
+            for x in range(st.width):
+                mine = dict(film.pixel_ranks(x, y))
+                theirs = {float(i): float(c) for i, c in ref[f, y, x] if c > 0.0}
+                assert set(mine) == set(theirs), (f, x, y, mine, theirs)
+                for i, c in theirs.items():
+                    worst = max(worst, abs(mine[i] - c))
+                ids.update(mine)
+    assert worst < 1e-6, worst
+    # floor, metal, glass, emitter and the sky-free pixels give several distinct ids
+    assert len(ids) >= 6, ids

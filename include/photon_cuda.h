@@ -193,6 +193,10 @@ int32_t pe_scene_add_texture(pe_scene* s, const float* rgb, int32_t width, int32
 /* Image::buildMipmaps (src/core/image/image.cpp:102-155) of texture `texture`: lookups then
  * select a level from the ray cone's footprint (sampleTex, src/materials/disney.cpp:530-539). */
 int32_t pe_scene_build_texture_mipmaps(pe_scene* s, int32_t texture);
+/* An 8-bit RGB image (Image::createCompact8, src/core/image/image.cpp:49-60): sRGB-encoded when
+ * srgb != 0, else linear; looked up as the reference decodes it (a 256-entry table; mip levels
+ * quantised to 8 bits).  The device holds the decoded values as floats. */
+int32_t pe_scene_add_texture_u8(pe_scene* s, const uint8_t* rgb, int32_t width, int32_t height, int32_t srgb);
 /* Light::setLightGroup (src/lights/light.h:85) of light `light` (the numbering of
  * pe_scene_set_light_link), or of the environment when light == -1; "" or NULL clears it.
  * Scene::buildAccelerator forms the groups (src/engine/scene.cpp:144-174): none unless some

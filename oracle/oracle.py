@@ -74,6 +74,7 @@ def _load(fast: bool = False):
         "ref_scene_set_shape_name": (C.c_int32, [P, C.c_int32, C.c_char_p]),
         "ref_scene_set_material_name": (C.c_int32, [P, C.c_int32, C.c_char_p]),
         "ref_scene_build_texture_mipmaps": (C.c_int32, [P, C.c_int32]),
+        "ref_scene_add_texture_u8": (C.c_int32, [P, C.c_void_p, C.c_int32, C.c_int32, C.c_int32]),
         "ref_film_create": (P, [C.c_int32, C.c_int32]),
         "ref_film_destroy": (None, [P]),
         "ref_film_export": (C.c_int32, [P, C.c_int32, C.c_int32, FP, UP]),
@@ -137,7 +138,12 @@ class RefScene:
         self.h = self.lib.ref_scene_create()
         tex_index = {}
         for img in (scene.textures() if hasattr(scene, "textures") else []):
-            tex_index[id(img)] = self.lib.ref_scene_add_texture(self.h, _f(img), img.shape[1], img.shape[0])
+            if img.dtype == np.uint8:
+                srgb = not any(id(img) in getattr(m, "linear_u8", ()) for m in scene.materials())
+                tex_index[id(img)] = self.lib.ref_scene_add_texture_u8(self.h, img.ctypes.data, img.shape[1],
+                                                                       img.shape[0], 1 if srgb else 0)
+            else:
+                tex_index[id(img)] = self.lib.ref_scene_add_texture(self.h, _f(img), img.shape[1], img.shape[0])
             if scene.texture_has_mipmaps(img):
                 self.lib.ref_scene_build_texture_mipmaps(self.h, tex_index[id(img)])
         mat_index = {}

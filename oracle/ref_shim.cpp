@@ -209,6 +209,15 @@ int32_t ref_scene_add_texture(void* s, const float* rgb, int32_t w, int32_t h) {
     return static_cast<int32_t>(rs->textures.size() - 1);
 }
 
+// Image::createCompact8 (8-bit, sRGB-encoded when srgb != 0) for the Disney image maps.
+int32_t ref_scene_add_texture_u8(void* s, const uint8_t* rgb, int32_t w, int32_t h, int32_t srgb) {
+    auto* rs = static_cast<RefScene*>(s);
+    auto img = std::make_shared<Image>(Image::createCompact8(
+        w, h, rgb, srgb ? Image::StorageFormat::U8Srgb : Image::StorageFormat::U8Linear));
+    rs->textures.push_back(img);
+    return static_cast<int32_t>(rs->textures.size() - 1);
+}
+
 // Image::buildMipmaps of texture `i`.
 int32_t ref_scene_build_texture_mipmaps(void* s, int32_t i) {
     auto* rs = static_cast<RefScene*>(s);

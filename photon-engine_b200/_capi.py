@@ -173,6 +173,7 @@ SIGNATURES = {
     "pe_scene_add_material": (C.c_int32, [P, C.POINTER(pe_material)]),
     "pe_scene_add_texture": (C.c_int32, [P, C.POINTER(C.c_float), C.c_int32, C.c_int32]),
     "pe_scene_build_texture_mipmaps": (C.c_int32, [P, C.c_int32]),
+    "pe_scene_add_texture_u8": (C.c_int32, [P, C.POINTER(C.c_uint8), C.c_int32, C.c_int32, C.c_int32]),
     "pe_scene_set_material": (C.c_int32, [P, C.c_int32, C.POINTER(pe_material)]),
     "pe_scene_set_shape_name": (C.c_int32, [P, C.c_int32, C.c_char_p]),
     "pe_scene_set_material_name": (C.c_int32, [P, C.c_int32, C.c_char_p]),

@@ -1401,6 +1401,49 @@ int32_t pe_scene_add_texture(pe_scene* s, const float* rgb, int32_t width, int32
 
 // Image::buildMipmaps (image.cpp:102-155), Float32 storage: each level the 2×2 box mean of the
 // one before (the last row / column repeated on odd sizes), down to 1×1.
+// 8-bit storage (Image::StorageFormat U8Srgb / U8Linear, image.cpp:14-36): the sRGB transfer
+// of IEC 61966-2-1, decoded through a 256-entry table, encoded with round-to-nearest.
+static float srgbToLinear(float e) { return e <= 0.04045f ? e / 12.92f : std::pow((e + 0.055f) / 1.055f, 2.4f); }
+static float linearToSrgb(float l) {
+    l = std::min(std::max(l, 0.0f), 1.0f);
+    return l <= 0.0031308f ? 12.92f * l : 1.055f * std::pow(l, 1.0f / 2.4f) - 0.055f;
+}
+static const float* decodeTable(int32_t format) {
+    static float srgb[256], lin[256];
+    static bool ready = false;
+    if (!ready) {
+        for (int i = 0; i < 256; ++i) {
+            srgb[i] = srgbToLinear(static_cast<float>(i) / 255.0f);
+            lin[i] = static_cast<float>(i) / 255.0f;
+        }
+        ready = true;
+    }
+    return format == 1 ? srgb : lin;
+}
+static uint8_t encode8(float v, int32_t format) {
+    const float c = std::min(std::max(v, 0.0f), 1.0f);
+    const float e = format == 1 ? linearToSrgb(c) : c;
+    return static_cast<uint8_t>(std::lround(e * 255.0f));
+}
+
+int32_t pe_scene_add_texture_u8(pe_scene* s, const uint8_t* rgb, int32_t width, int32_t height, int32_t srgb) {
+    if (!s || !rgb || width <= 0 || height <= 0) {
+        setError("pe_scene_add_texture_u8: bad argument");
+        return PE_ERR_INVALID;
+    }
+    pe_scene::Texture t;
+    t.width = width;
+    t.height = height;
+    t.format = srgb ? 1 : 2;
+    const float* lut = decodeTable(t.format);
+    const size_t n = static_cast<size_t>(width) * static_cast<size_t>(height) * 3;
+    t.texels.resize(n);
+    for (size_t i = 0; i < n; ++i) t.texels[i] = lut[rgb[i]];
+    s->textures.push_back(std::move(t));
+    s->built = false;
+    return static_cast<int32_t>(s->textures.size() - 1);
+}
+
 int32_t pe_scene_build_texture_mipmaps(pe_scene* s, int32_t texture) {
     if (!s || texture < 0 || texture >= static_cast<int32_t>(s->textures.size())) {
         setError("pe_scene_build_texture_mipmaps: bad texture index");
@@ -1435,6 +1478,12 @@ int32_t pe_scene_build_texture_mipmaps(pe_scene* s, int32_t texture) {
         prev = &t.mips.back();
         pw = nw;
         ph = nh;
+    }
+    if (t.format != 0) {
+        // 8-bit images keep each level quantised (the chain itself runs in float)
+        const float* lut = decodeTable(t.format);
+        for (std::vector<float>& level : t.mips)
+            for (float& v : level) v = lut[encode8(v, t.format)];
     }
     s->built = false;
     return PE_OK;

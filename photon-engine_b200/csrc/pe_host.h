@@ -92,6 +92,7 @@ struct pe_scene {
         int32_t width = 0, height = 0;
         std::vector<std::vector<float>> mips; // levels 1.. (pe_scene_build_texture_mipmaps)
         std::vector<int32_t> mipW, mipH;
+        int32_t format = 0; // 0 float, 1 8-bit sRGB, 2 8-bit linear (texels hold the decoded values)
     };
     std::vector<Texture> textures;             // pe_scene_add_texture
     std::vector<pe_material> materialsIn;

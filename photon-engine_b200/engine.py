@@ -54,6 +54,7 @@ class Material:
         _lib().pe_material_defaults(self.kind, C.byref(self._m))
         self.images: dict[str, np.ndarray] = {}
         self.mipmapped: set[int] = set()  # ids of images given with mipmaps
+        self.linear_u8: set[int] = set()  # ids of 8-bit images stored linear (not sRGB)
 
     @property
     def struct(self) -> capi.pe_material:
@@ -89,30 +90,36 @@ class Lambertian(Material):
 class DisneyMaterial(Material):
     kind = capi.PE_MAT_DISNEY
 
-    def _set_image(self, key, image, mipmaps):
-        img = np.ascontiguousarray(image, dtype=np.float32)
+    def _set_image(self, key, image, mipmaps, srgb=True):
+        # float images are linear; uint8 images are sRGB-encoded unless srgb=False
+        # (Image::createCompact8 with U8Srgb / U8Linear)
+        src = np.asarray(image)
+        img = np.ascontiguousarray(src, dtype=np.uint8 if src.dtype == np.uint8 else np.float32)
         if img.ndim != 3 or img.shape[2] != 3:
-            raise ValueError("image maps are (height, width, 3) float arrays")
+            raise ValueError("image maps are (height, width, 3) arrays")
         self.images[key] = img
+        if img.dtype == np.uint8 and not srgb:
+            self.linear_u8.add(id(img))
         if mipmaps:
             self.mipmapped.add(id(img))
 
     # `mipmaps`: Image::buildMipmaps on the image, so that lookups pick a level from the ray cone
-    def set_albedo_image(self, image, mipmaps: bool = False):
-        """DisneyMaterial::setAlbedoImage: the base colour from an RGB image."""
-        self._set_image("albedo", image, mipmaps)
+    def set_albedo_image(self, image, mipmaps: bool = False, srgb: bool = True):
+        """DisneyMaterial::setAlbedoImage: the base colour from an RGB image (float, or uint8
+        sRGB-encoded unless srgb=False)."""
+        self._set_image("albedo", image, mipmaps, srgb)
 
-    def set_roughness_image(self, image, mipmaps: bool = False):
+    def set_roughness_image(self, image, mipmaps: bool = False, srgb: bool = False):
         """DisneyMaterial::setRoughnessImage: roughness from the image's green channel."""
-        self._set_image("roughness", image, mipmaps)
+        self._set_image("roughness", image, mipmaps, srgb)
 
-    def set_metalness_image(self, image, mipmaps: bool = False):
+    def set_metalness_image(self, image, mipmaps: bool = False, srgb: bool = False):
         """DisneyMaterial::setMetalnessImage: metalness from the image's blue channel."""
-        self._set_image("metalness", image, mipmaps)
+        self._set_image("metalness", image, mipmaps, srgb)
 
-    def set_normal_image(self, image, mipmaps: bool = False):
+    def set_normal_image(self, image, mipmaps: bool = False, srgb: bool = False):
         """DisneyMaterial::setNormalImage: a tangent-space normal map."""
-        self._set_image("normal", image, mipmaps)
+        self._set_image("normal", image, mipmaps, srgb)
 
     def set_opacity_image(self, image):
         """DisneyMaterial::setOpacityImage: coverage = opacity × the image's red channel
@@ -394,7 +401,12 @@ class Scene:
         self._handle = h
         tex_index = {}
         for img in self.textures():
-            t = lib.pe_scene_add_texture(h, capi.fptr(img), img.shape[1], img.shape[0])
+            if img.dtype == np.uint8:
+                srgb = not any(id(img) in getattr(m, "linear_u8", ()) for m in self.materials())
+                t = lib.pe_scene_add_texture_u8(h, img.ctypes.data_as(C.POINTER(C.c_uint8)), img.shape[1], img.shape[0],
+                                                1 if srgb else 0)
+            else:
+                t = lib.pe_scene_add_texture(h, capi.fptr(img), img.shape[1], img.shape[0])
             if t < 0:
                 capi.check(t)
             if self.texture_has_mipmaps(img):

@@ -184,3 +184,33 @@ def test_opacity_map_matches_reference(pe, device, oracle):
     opaque = pe.Film(st.width, st.height)
     device.render(cam, st, pe.RenderTargets(beauty=opaque), 0, spp)
     assert pe.rel_mse(opaque.resolve(), img) > 1e-3
+
+
+def test_8bit_images_match_reference(pe, device, oracle):
+    """8-bit images (Image::createCompact8): an sRGB-encoded base colour with mipmaps (levels
+    quantised to 8 bits, image.cpp:102-155) and a linear 8-bit roughness map, against the
+    reference's lookups of the same bytes."""
+    S = scenes()
+    scene, cam, st = S.cornell_box(64, 64, 8, 6, seed=0)
+    st.seed = 7
+    rng = np.random.default_rng(9)
+    albedo = np.kron(rng.integers(0, 256, (8, 8, 3)), np.ones((4, 4, 1), np.int64)).astype(np.uint8)
+    rough = np.zeros((16, 16, 3), np.uint8)
+    rough[..., 1] = rng.integers(20, 230, (16, 16))
+    m = pe.DisneyMaterial((0.5, 0.5, 0.5), 0.0, 0.5, 0.5)
+    m.set_albedo_image(albedo, mipmaps=True)
+    m.set_roughness_image(rough)
+    m.set_texture_scale(3.0)
+    pos, uv, idx = _grid_quad((0.3, 0.01, 0.3), (4.9, 0.0, 0.0), (0.0, 0.0, 4.9), 4)
+    scene.add_shape(pe.TriangleMesh(pos, None, uv, idx, m))
+    scene.build_accelerator()
+    device.set_scene(scene)
+    spp = 8
+    film = pe.Film(st.width, st.height)
+    device.render(cam, st, pe.RenderTargets(beauty=film), 0, spp)
+    mean_ref, _ = oracle.RefScene(scene).render(cam, st, 0, spp)
+    img = film.resolve()
+    err = pe.rel_mse(img, mean_ref)
+    same = float(np.mean(np.all(np.abs(img - mean_ref) <= 1e-4 * np.maximum(1.0, np.abs(mean_ref)), axis=-1)))
+    bias = float(img.mean() / max(1e-12, mean_ref.mean()) - 1.0)
+    assert err < 1e-4 and same > 0.99 and abs(bias) < 1e-3, (err, same, bias)

@@ -186,6 +186,8 @@ int32_t pe_scene_set_material_name(pe_scene* s, int32_t material, const char* na
  * emission and the media, shadow-transmission and subsurface switches must stay as they were,
  * else PE_ERR_LIMIT (rebuild the scene).  Then pe_device_update_materials sends it to a device. */
 int32_t pe_scene_set_material(pe_scene* s, int32_t index, const pe_material* m);
+/* AreaLight radiance of light `light` (a built scene's light sampler is rebuilt on the host). */
+int32_t pe_scene_set_area_light_radiance(pe_scene* s, int32_t light, const float radiance[3]);
 /* An RGB float image (w*h*3, row 0 first) for the Disney image maps; returns its index (>= 0)
  * or a negative status.  Lookups are Image::sampleBilinear's (src/core/image/image.cpp:98-225):
  * bilinear, wrapping, without mipmaps. */
@@ -286,6 +288,10 @@ int32_t pe_device_has_scene(pe_device* d);
  * copies the material table of the scene last set (same build) to the device again, leaving its
  * geometry, BVH, lights and textures in place. */
 int32_t pe_device_update_materials(pe_device* d, const pe_scene* s);
+/* SceneUpdateKind::Lights: after pe_scene_set_area_light_radiance edits, the lights, their quads'
+ * materials and the light sampler go to the device again (PE_ERR_LIMIT when the sampler's tree
+ * changed shape: set the scene again). */
+int32_t pe_device_update_lights(pe_device* d, const pe_scene* s);
 
 /* RenderDevice::render: adds samples [first_sample, first_sample+count) to every
  * pixel and accumulates into the caller's host arrays exactly as

@@ -1188,6 +1188,46 @@ int32_t pe_device_set_scene(pe_device* d, const pe_scene* s) {
     d->sceneSrc = s;
     d->sceneVersion = s->version;
     d->sceneMaterials = s->build.materials.size();
+    d->sceneLightNodes = s->build.lightNodes.size();
+    ++d->sceneSerial;
+    return PE_OK;
+}
+
+// RenderDevice::updateScene(scene, SceneUpdateKind::Lights): the lights, their emissive quads'
+// materials and the light sampler of the scene already set are copied again, when the sampler
+// keeps its shape (same node count and mode); else PE_ERR_LIMIT and the caller sets the scene.
+int32_t pe_device_update_lights(pe_device* d, const pe_scene* s) {
+    if (!d || !s) {
+        setError("pe_device_update_lights: null argument");
+        return PE_ERR_INVALID;
+    }
+    const HostBuild& B = s->build;
+    if (!d->hasScene || d->sceneSrc != s || d->sceneVersion != s->version || !s->built ||
+        B.materials.size() != d->sceneMaterials || B.lights.size() != static_cast<size_t>(d->scene.nLights)) {
+        setError("pe_device_update_lights: the device holds another build of the scene (call pe_device_set_scene)");
+        return PE_ERR_INVALID;
+    }
+    if (B.lightNodes.size() != d->sceneLightNodes || B.lightMode != d->scene.lightMode ||
+        B.infinite.size() > static_cast<size_t>(kMaxInfinite)) {
+        setError("pe_device_update_lights: the light sampler changed shape (call pe_device_set_scene)");
+        return PE_ERR_LIMIT;
+    }
+    PE_CUDA(cudaSetDevice(d->ordinal));
+    PE_CUDA(cudaStreamSynchronize(d->stream));
+    PE_CUDA(cudaStreamSynchronize(d->lanes[1].stream));
+    SceneGPU& G = d->scene;
+    auto put = [&](const void* dst, const void* src, size_t bytes) -> cudaError_t {
+        return bytes ? cudaMemcpyAsync(const_cast<void*>(dst), src, bytes, cudaMemcpyHostToDevice, d->stream) : cudaSuccess;
+    };
+    PE_CUDA(put(G.lights, B.lights.data(), B.lights.size() * sizeof(LightGPU)));
+    PE_CUDA(put(G.materials, B.materials.data(), B.materials.size() * sizeof(MatGPU)));
+    if (G.lightNodes) PE_CUDA(put(G.lightNodes, B.lightNodes.data(), B.lightNodes.size() * sizeof(LightNodeGPU)));
+    if (G.topSlot) PE_CUDA(put(G.topSlot, B.topSlot.data(), B.topSlot.size() * sizeof(int16_t)));
+    if (G.trail) PE_CUDA(put(G.trail, B.trail.data(), B.trail.size() * sizeof(unsigned long long)));
+    if (G.trailDepth) PE_CUDA(put(G.trailDepth, B.trailDepth.data(), B.trailDepth.size() * sizeof(uint8_t)));
+    G.nInfinite = static_cast<int32_t>(B.infinite.size());
+    for (size_t i = 0; i < B.infinite.size(); ++i) G.infinite[i] = B.infinite[i];
+    PE_CUDA(cudaStreamSynchronize(d->stream));
     ++d->sceneSerial;
     return PE_OK;
 }

@@ -174,7 +174,8 @@ struct pe_device {
     int32_t lightGroups = 0;
     const pe_scene* sceneSrc = nullptr; // the scene last set, and its build version
     uint64_t sceneVersion = 0;
-    size_t sceneMaterials = 0;        // light groups of the scene set (its pass films need one each)
+    size_t sceneMaterials = 0;
+    size_t sceneLightNodes = 0;        // light groups of the scene set (its pass films need one each)
     TablesGPU* dTables = nullptr;
     TablesGPU hTables{};
     // pixel-filter inverse CDFs, one slot per (type, width) in use, least recently used replaced

@@ -841,6 +841,56 @@ void fillFilterCdf(int type, float width, float* cdf) {
 }
 
 // ---------------------------------------------------------------------------------------------
+// The lights and the light sampler of a scene (LightSampler::build, light_sampler.cpp:42-115):
+// exhaustive up to kMaxExhaustive candidates, else infinite lights on top of a light BVH.
+static void buildLightSampler(const pe_scene* s, HostBuild& B) {
+    B.infinite.clear();
+    B.lightNodes.clear();
+    B.lights = s->lights;
+    const int nl = static_cast<int>(B.lights.size());
+    const int count = nl + (s->env.present ? 1 : 0);
+    B.lightCount = count;
+    B.topSlot.assign(static_cast<size_t>(count), -1);
+    B.trail.assign(static_cast<size_t>(count), 0ull);
+    B.trailDepth.assign(static_cast<size_t>(count), 0);
+    B.lightMode = count <= 1 ? 0 : 1;
+    if (count > kMaxExhaustive) {
+        std::vector<LItem> items;
+        for (int i = 0; i < nl; ++i) {
+            LBounds lb;
+            if (lightBounds(B.lights[static_cast<size_t>(i)], lb) && lb.phi > 0.0f) items.push_back({i, lb});
+            else B.infinite.push_back(i);
+        }
+        if (s->env.present) B.infinite.push_back(nl);
+        if (static_cast<int>(B.infinite.size()) + 1 > kMaxInfinite) {
+            B.infinite.clear();
+            B.lightMode = 0; // uniform (light_sampler.cpp:71-75)
+        } else {
+            for (size_t k = 0; k < B.infinite.size(); ++k) B.topSlot[static_cast<size_t>(B.infinite[k])] = static_cast<int16_t>(k);
+            if (!items.empty()) {
+                LightBvhBuilder lb;
+                lb.trail = &B.trail;
+                lb.depthOut = &B.trailDepth;
+                lb.nodes.reserve(2 * items.size());
+                lb.build(items, 0, static_cast<int>(items.size()), 0ull, 0);
+                B.lightNodes = lb.nodes;
+                for (size_t i = 0; i < lb.nodes.size(); ++i) {
+                    const LBounds& b = lb.nodeBounds[i];
+                    LightNodeGPU& n = B.lightNodes[i];
+                    n.bmin[0] = b.bounds.lo.x; n.bmin[1] = b.bounds.lo.y; n.bmin[2] = b.bounds.lo.z;
+                    n.bmax[0] = b.bounds.hi.x; n.bmax[1] = b.bounds.hi.y; n.bmax[2] = b.bounds.hi.z;
+                    n.w[0] = b.w.x; n.w[1] = b.w.y; n.w[2] = b.w.z;
+                    n.phi = b.phi;
+                    n.cosThetaO = b.cosThetaO;
+                    n.cosThetaE = b.cosThetaE;
+                    n.twoSided = b.twoSided ? 1 : 0;
+                }
+            }
+            B.lightMode = 2;
+        }
+    }
+}
+
 static int32_t buildScene(pe_scene* s) {
     HostBuild& B = s->build;
     B = HostBuild{};
@@ -1033,50 +1083,7 @@ static int32_t buildScene(pe_scene* s) {
         B.rootMax[2] = ref[0].bounds.hi.z;
     }
 
-    // lights and light sampler (LightSampler::build)
-    B.lights = s->lights;
-    const int nl = static_cast<int>(B.lights.size());
-    const int count = nl + (s->env.present ? 1 : 0);
-    B.lightCount = count;
-    B.topSlot.assign(static_cast<size_t>(count), -1);
-    B.trail.assign(static_cast<size_t>(count), 0ull);
-    B.trailDepth.assign(static_cast<size_t>(count), 0);
-    B.lightMode = count <= 1 ? 0 : 1;
-    if (count > kMaxExhaustive) {
-        std::vector<LItem> items;
-        for (int i = 0; i < nl; ++i) {
-            LBounds lb;
-            if (lightBounds(B.lights[static_cast<size_t>(i)], lb) && lb.phi > 0.0f) items.push_back({i, lb});
-            else B.infinite.push_back(i);
-        }
-        if (s->env.present) B.infinite.push_back(nl);
-        if (static_cast<int>(B.infinite.size()) + 1 > kMaxInfinite) {
-            B.infinite.clear();
-            B.lightMode = 0; // uniform (light_sampler.cpp:71-75)
-        } else {
-            for (size_t k = 0; k < B.infinite.size(); ++k) B.topSlot[static_cast<size_t>(B.infinite[k])] = static_cast<int16_t>(k);
-            if (!items.empty()) {
-                LightBvhBuilder lb;
-                lb.trail = &B.trail;
-                lb.depthOut = &B.trailDepth;
-                lb.nodes.reserve(2 * items.size());
-                lb.build(items, 0, static_cast<int>(items.size()), 0ull, 0);
-                B.lightNodes = lb.nodes;
-                for (size_t i = 0; i < lb.nodes.size(); ++i) {
-                    const LBounds& b = lb.nodeBounds[i];
-                    LightNodeGPU& n = B.lightNodes[i];
-                    n.bmin[0] = b.bounds.lo.x; n.bmin[1] = b.bounds.lo.y; n.bmin[2] = b.bounds.lo.z;
-                    n.bmax[0] = b.bounds.hi.x; n.bmax[1] = b.bounds.hi.y; n.bmax[2] = b.bounds.hi.z;
-                    n.w[0] = b.w.x; n.w[1] = b.w.y; n.w[2] = b.w.z;
-                    n.phi = b.phi;
-                    n.cosThetaO = b.cosThetaO;
-                    n.cosThetaE = b.cosThetaE;
-                    n.twoSided = b.twoSided ? 1 : 0;
-                }
-            }
-            B.lightMode = 2;
-        }
-    }
+    buildLightSampler(s, B);
     if (s->env.present) buildEnvironment(s->env);
     // light groups (scene.cpp:144-174): only when some light or the environment names one; then
     // every light joins its group or "Default", the environment its group or "Env", at most 16
@@ -1244,6 +1251,35 @@ int32_t pe_scene_set_material(pe_scene* s, int32_t index, const pe_material* m) 
     s->materialsIn[static_cast<size_t>(index)] = *m;
     s->materials[static_cast<size_t>(index)] = g;
     if (s->built && static_cast<size_t>(index) < s->build.materials.size()) s->build.materials[static_cast<size_t>(index)] = g;
+    ++s->materialVersion;
+    return PE_OK;
+}
+
+int32_t pe_scene_set_area_light_radiance(pe_scene* s, int32_t light, const float radiance[3]) {
+    if (!s || !radiance || light < 0 || light >= static_cast<int32_t>(s->lights.size()) ||
+        s->lights[static_cast<size_t>(light)].type != LT_AREA) {
+        setError("pe_scene_set_area_light_radiance: not an area light");
+        return PE_ERR_INVALID;
+    }
+    if (!(radiance[0] > 0.0f || radiance[1] > 0.0f || radiance[2] > 0.0f)) {
+        setError("pe_scene_set_area_light_radiance: a dark light changes the scene's emitters (rebuild)");
+        return PE_ERR_LIMIT;
+    }
+    LightGPU& l = s->lights[static_cast<size_t>(light)];
+    l.radiance_r = radiance[0];
+    l.radiance_g = radiance[1];
+    l.radiance_b = radiance[2];
+    // the quad's own emissive material (its two triangles in the BVH)
+    for (const HostShape& sh : s->shapes)
+        if ((sh.flags & SF_AREA_TRIANGLE) && sh.emitter == light) {
+            pe_material& m = s->materialsIn[static_cast<size_t>(sh.material)];
+            for (int i = 0; i < 3; ++i) m.emission[i] = radiance[i];
+            s->materials[static_cast<size_t>(sh.material)] = resolveMaterial(m);
+            if (s->built) s->build.materials[static_cast<size_t>(sh.material)] = s->materials[static_cast<size_t>(sh.material)];
+            break;
+        }
+    // the light sampler weighs lights by their power
+    if (s->built) buildLightSampler(s, s->build);
     ++s->materialVersion;
     return PE_OK;
 }

@@ -388,6 +388,23 @@ class Scene:
                 return False
         return True
 
+    def sync_lights(self) -> bool:
+        """Sends every AreaLight's current radiance to the built scene without rebuilding its BVH
+        (pe_scene_set_area_light_radiance); False when that is not possible."""
+        if not self._handle:
+            return False
+        lib, li = _lib(), 0
+        for kind, obj in self.ops:
+            if kind == "mesh":
+                m = obj.material.struct
+                if m.type in (capi.PE_MAT_LAMBERT, capi.PE_MAT_DISNEY) and any(m.emission):
+                    li += obj.indices.shape[0]
+            else:
+                if lib.pe_scene_set_area_light_radiance(self._handle, li, capi.f3(obj.radiance)) != capi.PE_OK:
+                    return False
+                li += 1
+        return True
+
     def texture_has_mipmaps(self, img) -> bool:
         return any(id(img) in getattr(m, "mipmapped", ()) for m in self.materials())
 
@@ -802,6 +819,9 @@ class CudaDevice:
         scene is rebuilt and set again (returns False)."""
         if kind == SceneUpdateKind.Materials and self._scene is scene and scene.sync_materials():
             if _lib().pe_device_update_materials(self._h, scene.handle) == capi.PE_OK:
+                return True
+        if kind == SceneUpdateKind.Lights and self._scene is scene and scene.sync_lights():
+            if _lib().pe_device_update_lights(self._h, scene.handle) == capi.PE_OK:
                 return True
         scene.build_accelerator()
         self.set_scene(scene)

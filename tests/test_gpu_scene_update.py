@@ -37,3 +37,26 @@ def test_material_update_equals_rebuild(pe, device):
     # a change of type falls back to a rebuild
     scene.ops[-1][1].material = pe.Lambertian((0.5, 0.5, 0.5))
     assert device.update_scene(scene, pe.SceneUpdateKind.Materials) is False
+
+
+def test_light_update_equals_rebuild(pe, device):
+    """SceneUpdateKind::Lights: a new AreaLight radiance reaches the device (lights, the quad's
+    emission, the light sampler) without a rebuild; the frame equals a rebuilt scene's."""
+    S = importlib.import_module("photon_engine_b200.scenes")
+    scene, cam, st = S.cornell_box(48, 48, 8, 6, seed=0)
+    key = pe.AreaLight((1.0, 4.5, 1.0), (1.0, 0.0, 0.0), (0.0, 0.0, 1.0), (6.0, 6.0, 6.0))
+    scene.add_light(key)
+    scene.build_accelerator()
+    device.set_scene(scene)
+    before = pe.Film(st.width, st.height)
+    device.render(cam, st, pe.RenderTargets(beauty=before), 0, 4)
+    key.radiance = (20.0, 9.0, 3.0)
+    assert device.update_scene(scene, pe.SceneUpdateKind.Lights) is True
+    updated = pe.Film(st.width, st.height)
+    device.render(cam, st, pe.RenderTargets(beauty=updated), 0, 4)
+    assert pe.rel_mse(updated.resolve(), before.resolve()) > 1e-4
+    scene.build_accelerator()
+    device.set_scene(scene)
+    rebuilt = pe.Film(st.width, st.height)
+    device.render(cam, st, pe.RenderTargets(beauty=rebuilt), 0, 4)
+    assert np.array_equal(updated.sum, rebuilt.sum) and np.array_equal(updated.count, rebuilt.count)

@@ -19,7 +19,8 @@ msamplesPerSecond definition).
 ``cpu_baseline`` the reference engine's own CPU path (built with its shipping flags) on the same
             scene and camera, all host threads, a bounded number of full-frame samples.
 
-``--impl reference`` times only that CPU implementation, one full-frame sample per step.
+``--impl reference`` times only that CPU implementation (Renderer::renderSamples) on the same
+            workload and step, four full-frame samples per step, with no product library loaded.
 ``--gpus N`` (torchrun) runs N independent replicas, each rendering its own sample indices:
 the path does not shard further and needs no collective.
 """
@@ -135,62 +136,105 @@ def max_over_ranks(value: float, pg, device: str) -> float:
     return float(t.item())
 
 
+def _scenegen():
+    """The workload generator (plain numpy), loaded by file path so that the reference arm
+    imports no product module and loads no product library."""
+    import importlib.util
+    name = "_photon_scenegen"
+    if name not in sys.modules:
+        spec = importlib.util.spec_from_file_location(name, ROOT / "photon-engine_b200" / "scenegen.py")
+        mod = importlib.util.module_from_spec(spec)
+        sys.modules[name] = mod
+        spec.loader.exec_module(mod)
+    return sys.modules[name]
+
+
+def workload_description(width=WIDTH, height=HEIGHT, nu=4096, nv=128, env_size=(2048, 1024)):
+    return _scenegen().torus_knot(width, height, 256, DEPTH, nu, nv, env_size)
+
+
+def workload_config(desc) -> dict:
+    """The config both arms report (one workload, one step definition)."""
+    st = desc["settings"]
+    return {"workload": "torus-knot 1M tris, 8 Disney materials, 2048x1024 HDR sky + softbox, 1920x1080, depth 12",
+            "spp_per_step": SPP_PER_STEP, "paths_per_step": st["width"] * st["height"] * SPP_PER_STEP,
+            "triangles": _scenegen().triangle_count(desc), "l2": L2_NOTE, "parallelism": "replicas x1"}
+
+
 def build_workload(pe):
     import importlib
     sc = importlib.import_module("photon_engine_b200.scenes")
-    scene, cam, st = sc.torus_knot_scene(WIDTH, HEIGHT, 256, DEPTH)
+    desc = workload_description()
+    scene, cam, st = sc.from_description(desc)
     scene.build_accelerator()
-    return scene, cam, st
+    return scene, cam, st, desc
 
 
-def cpu_reference(scene, cam, st, min_seconds: float, max_spp: int, first: int = 0):
-    """The reference's CPU path on all host threads: full-frame samples until min_seconds."""
+def cpu_reference(desc, min_seconds: float, max_spp: int, first: int = 0):
+    """The reference's stock CPU path (Renderer::renderSamples, shipping build) on all host
+    threads: full-frame samples until min_seconds."""
     sys.path.insert(0, str(ROOT / "oracle"))
     import oracle
-    ref = oracle.RefScene(scene, fast=True)
+    ref = oracle.ref_scene_from_description(desc, fast=True)
+    cam = oracle.DescCamera(desc["camera"], fast=True)
+    st = oracle.DescSettings(desc["settings"])
     threads = oracle.cpu_threads()
     done, t0 = 0, time.perf_counter()
     while done < max_spp:
-        ref.render(cam, st, first + done, 1, threads)
+        oracle.render_stock(ref, cam, st, first + done, 1, threads)
         done += 1
         if time.perf_counter() - t0 >= min_seconds:
             break
     dt = time.perf_counter() - t0
-    return WIDTH * HEIGHT * done / dt, threads, done, dt
+    return st.width * st.height * done / dt, threads, done, dt
 
 
 def run_reference(args):
+    """The reference's own CPU implementation of the path (Renderer::renderSamples of the
+    reference sources, built with its shipping flags) on the same workload and step: no product
+    module or library is loaded in this process."""
     world, rank, local = dist_setup()
     if rank != 0:
         return 0
-    pe = pe_load()
-    scene, cam, st = build_workload(pe)
     sys.path.insert(0, str(ROOT / "oracle"))
     import oracle
     if not oracle.available(fast=True):
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libphoton_ref_fast.so was not built"}))
         return 0
-    ref = oracle.RefScene(scene, fast=True)
+    desc = workload_description()
+    ref = oracle.ref_scene_from_description(desc, fast=True)
+    cam = oracle.DescCamera(desc["camera"], fast=True)
+    st = oracle.DescSettings(desc["settings"])
     threads = oracle.cpu_threads()
     for w in range(args.warmup):
-        ref.render(cam, st, w, 1, threads)
+        oracle.render_stock(ref, cam, st, step_samples(0, 0, w), SPP_PER_STEP, threads)
     t0 = time.perf_counter()
     for k in range(args.steps):
-        ref.render(cam, st, args.warmup + k, 1, threads)
+        oracle.render_stock(ref, cam, st, step_samples(0, args.warmup, k), SPP_PER_STEP, threads)
     dt = time.perf_counter() - t0
-    value = WIDTH * HEIGHT * args.steps / dt
-    sample = f"{args.steps} full 1920x1080 frames at 1 spp (one per step)"
+    value = st.width * st.height * SPP_PER_STEP * args.steps / dt
+    sample = f"{args.steps} steps of {SPP_PER_STEP} spp over the full 1920x1080 frame (Renderer::renderSamples)"
     print(json.dumps({
         "impl": "reference", "metric": "paths/s", "value": value, "unit": "paths/s", "n_gpus": 0,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * dt / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-        "data": "synthetic (seeded procedural scene)",
-        "config": {"workload": "torus-knot 1M tris, 8 Disney materials, 2048x1024 HDR sky + softbox, 1920x1080, depth 12",
-                   "spp_per_step": 1, "threads": threads},
+        "data": "synthetic (seeded procedural scene)", "config": workload_config(desc),
         "cpu_baseline": {"value": value, "unit": "paths/s", "cores": threads, "kind": "reference", "sample": sample},
         "e2e": {"value": value, "unit": "paths/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "loaded_libraries": loaded_libraries(),
     }))
     return 0
+
+
+def loaded_libraries() -> list:
+    """Shared objects of this repository mapped into the process."""
+    try:
+        maps = pathlib.Path("/proc/self/maps").read_text().splitlines()
+    except OSError:
+        return []
+    root = str(ROOT)
+    return sorted({line.split()[-1][len(root) + 1:] for line in maps
+                   if line.split()[-1].startswith(root) and line.split()[-1].endswith(".so")})
 
 
 def pe_load():
@@ -208,7 +252,7 @@ def run_ours(args):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
         pg = dist
     pe = pe_load()
-    scene, cam, st = build_workload(pe)
+    scene, cam, st, desc = build_workload(pe)
     dev = pe.CudaDevice(local)
     dev.set_scene(scene)
     tail = dev.autotune(cam, st, SPP_PER_STEP)  # untimed set-up: picks the tail threshold
@@ -298,7 +342,7 @@ def run_ours(args):
     cpu = None
     if world == 1 and not args.no_cpu_baseline:
         try:
-            v, threads, done, dt = cpu_reference(scene, cam, st, args.cpu_seconds, 64, first=100000)
+            v, threads, done, dt = cpu_reference(desc, args.cpu_seconds, 64, first=100000)
             cpu = {"value": v, "unit": "paths/s", "cores": threads, "kind": "reference",
                    "sample": f"{done} full 1920x1080 frames at 1 spp ({dt:.1f} s), reference shipping build"}
         except Exception as e:  # noqa: BLE001
@@ -308,10 +352,7 @@ def run_ours(args):
         "metric": "paths/s", "value": value, "unit": "paths/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded procedural scene)",
-        "config": {"workload": "torus-knot 1M tris, 8 Disney materials, 2048x1024 HDR sky + softbox, 1920x1080, depth 12",
-                   "spp_per_step": SPP_PER_STEP, "paths_per_step": WIDTH * HEIGHT * SPP_PER_STEP,
-                   "triangles": int(scene.info.triangles),
-                   "l2": L2_NOTE, "parallelism": f"replicas x{world}"},
+        "config": {**workload_config(desc), "parallelism": f"replicas x{world}"},
         "rays_per_s": (rays + shadow_rays) * world / (ms / 1000.0),
         "closest_rays_per_step": rays / args.steps, "shadow_rays_per_step": shadow_rays / args.steps,
         "e2e": {"value": e2e, "unit": "paths/s", "h2d_bytes_per_step": 76 + 40,

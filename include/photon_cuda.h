@@ -373,7 +373,15 @@ int32_t pe_device_film_clear(pe_device* d);
  * (width*height*3 floats), sample_count and sum_lum_sq (width*height each), all DEVICE memory
  * the caller owns, covering the whole film of st->width x st->height.  Samples
  * [first_sample, first_sample+count) of the pixels in the rectangle (x0, y0, w, h) are added to
- * them exactly as pe_device_render would add them; other pixels are not touched.
+ * them exactly as pe_device_render would add them; other pixels are not touched.  Each film
+ * pointer is checked to be memory of this device that holds the whole film (PE_ERR_INVALID
+ * otherwise).  The call runs on the library's own non-blocking stream and does not wait for the
+ * caller's streams: finish writing the film buffers before calling, and synchronize the device
+ * (pe_device_synchronize) before reading them.
+ *
+ * It renders plain paths only: a device with guided sampling on (pe_device_set_guiding) and a
+ * scene with mipmapped image maps (whose level of detail needs a per-path ray cone) are rejected
+ * with PE_ERR_INVALID, as is adaptive sampling; render those with pe_device_render.
  *
  * The path state lives in one file-scope device array of 8.5 MB (room for 32768 paths), which
  * every GPU that loads this library holds until the process exits; its address on a device is

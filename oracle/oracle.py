@@ -92,6 +92,8 @@ def _load(fast: bool = False):
         "ref_render_rows_camera": (C.c_int32, [P, P, C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.c_int32,
                                                C.c_int32, FP, UP]),
         "ref_dtree_probe": (C.c_int32, [FP, FP, C.c_int32, FP, FP, C.c_int32, FP, FP, C.c_int32, FP, FP]),
+        "ref_render_camera": (C.c_int32, [P, P, C.c_void_p, C.c_int32, C.c_int32, C.c_int32, FP, UP]),
+        "ref_material_defaults": (None, [C.c_int32, C.c_void_p]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -355,6 +357,114 @@ def sobol(seed: int, px, py, index, n_dims: int) -> np.ndarray:
     _load().ref_sobol(seed, px.ctypes.data_as(IP), py.ctypes.data_as(IP), index.ctypes.data_as(IP), len(px), n_dims,
                       _f(out))
     return out
+
+
+def _abi():
+    """The C ABI's structure layouts (include/photon_cuda.h), from the package's ctypes binding
+    loaded by file path: that module declares structures only and loads no library."""
+    import importlib.util
+    import sys
+    name = "_photon_abi_structs"
+    if name not in sys.modules:
+        spec = importlib.util.spec_from_file_location(name, HERE.parent / "photon-engine_b200" / "_capi.py")
+        mod = importlib.util.module_from_spec(spec)
+        sys.modules[name] = mod
+        spec.loader.exec_module(mod)
+    return sys.modules[name]
+
+
+class DescSettings:
+    """RenderSettings of a scene description (the fields the reference's renderer reads)."""
+
+    def __init__(self, d: dict):
+        self.width, self.height = int(d["width"]), int(d["height"])
+        self.max_bounces = int(d.get("max_bounces", 8))
+        self.rr_depth = int(d.get("rr_depth", 3))
+        self.shadow_quality = int(d.get("shadow_quality", 1))
+        self.filter_type = int(d.get("filter_type", 3))
+        self.filter_width = float(d.get("filter_width", 1.5))
+        self.seed = int(d.get("seed", 12345))
+
+    def to_c(self):
+        return _abi().pe_settings(self.width, self.height, self.max_bounces, self.rr_depth, self.shadow_quality,
+                                  self.filter_type, self.filter_width, 0.0, self.seed, 0.0, 0, 0.02, 16)
+
+
+class DescCamera:
+    """The reference's own PerspectiveCamera of a scene description."""
+
+    def __init__(self, d: dict, fast: bool = False):
+        self.lib = _load(fast)
+        p = np.array([*d["position"], *d["target"], *d["up"], d["vfov"], d["aspect"]], np.float32)
+        self.h = self.lib.ref_camera_create(0, _f(p))
+
+    def __del__(self):
+        try:
+            self.lib.ref_camera_destroy(self.h)
+        except Exception:
+            pass
+
+
+def ref_scene_from_description(desc: dict, fast: bool = False) -> "RefScene":
+    """The reference's Scene built from a plain scene description (photon-engine_b200/scenegen.py)
+    through the reference's own Scene API, with no product code or library involved: materials
+    in first-use order, then shapes and area lights in op order, then the environment."""
+    lib = _load(fast)
+    abi = _abi()
+    rs = RefScene.__new__(RefScene)
+    rs.lib = lib
+    rs.h = lib.ref_scene_create()
+    order = []
+    for kind, o in desc["ops"]:
+        if kind == "mesh" and o["material"] not in order:
+            order.append(o["material"])
+    index = {}
+    for k in order:
+        d = desc["materials"][k]
+        m = abi.pe_material()
+        lib.ref_material_defaults(int(d["type"]), C.byref(m))
+        for key, value in d.items():
+            if key != "type":
+                setattr(m, key, _f3(value) if isinstance(value, (tuple, list, np.ndarray)) else value)
+        index[k] = lib.ref_scene_add_material(rs.h, C.byref(m))
+        if index[k] < 0:
+            raise RuntimeError("reference rejected a material")
+    rs.mat_index = index
+    for kind, o in desc["ops"]:
+        if kind == "mesh":
+            pos = np.ascontiguousarray(o["positions"], np.float32)
+            idx = np.ascontiguousarray(o["indices"], np.uint32)
+            nrm = o.get("normals")
+            uv = o.get("uvs")
+            nrm = None if nrm is None else np.ascontiguousarray(nrm, np.float32)
+            uv = None if uv is None else np.ascontiguousarray(uv, np.float32)
+            rc = lib.ref_scene_add_mesh(rs.h, _f(pos), pos.shape[0], _f(nrm), _f(uv), idx.ctypes.data_as(UP),
+                                        idx.shape[0], index[o["material"]])
+        else:
+            rc = lib.ref_scene_add_area_light(rs.h, _f3(o["position"]), _f3(o["u"]), _f3(o["v"]), _f3(o["radiance"]),
+                                              1)
+        if rc != 0:
+            raise RuntimeError("reference rejected a shape")
+    env = desc.get("environment")
+    if env is not None:
+        img = np.ascontiguousarray(env["image"], np.float32)
+        lib.ref_scene_set_environment(rs.h, _f(img), img.shape[1], img.shape[0], float(env["rotation"]),
+                                      float(env["intensity"]), None, 1.0, None)
+    lib.ref_scene_set_background(rs.h, 0, _f3((0.18, 0.18, 0.18)))
+    lib.ref_scene_build(rs.h)
+    return rs
+
+
+def render_stock(ref: "RefScene", camera: DescCamera, settings: DescSettings, first: int, count: int,
+                 threads: int = 0):
+    """Renderer::renderSamples (the stock CPU path, Sobol seed 12345) of samples
+    [first, first+count): mean image (h, w, 3) and counts."""
+    h, w = settings.height, settings.width
+    mean = np.zeros((h, w, 3), np.float32)
+    cnt = np.zeros((h, w), np.uint32)
+    ref.lib.ref_render_camera(ref.h, camera.h, C.byref(settings.to_c()), first, count, threads, _f(mean),
+                              cnt.ctypes.data_as(UP))
+    return mean, cnt
 
 
 def cpu_threads() -> int:

@@ -407,6 +407,49 @@ int32_t ref_render(void* s, const pe_camera* cam, const pe_settings* st, int32_t
     return 0;
 }
 
+// Renderer::renderSamples through one of the reference's own camera objects (ref_camera_create):
+// the stock CPU path end to end, as CpuDevice::render runs it.
+int32_t ref_render_camera(void* s, void* cam, const pe_settings* st, int32_t first, int32_t count, int32_t threads,
+                          float* mean_rgb, uint32_t* counts) {
+    auto* rs = static_cast<RefScene*>(s);
+    RenderSettings settings = toSettings(*st, threads > 0 ? threads : hardwareThreads());
+    Film film(st->width, st->height);
+    Renderer renderer;
+    renderer.renderSamples(rs->scene, *static_cast<const Camera*>(cam), settings, film, first, count, nullptr);
+    exportFilm(film, st->width, st->height, mean_rgb, counts);
+    return 0;
+}
+
+// The documented starting values of a pe_material description (include/photon_cuda.h), so that a
+// description can be filled without the product library: zeros, no image maps, texture scale 1,
+// base 0.8 (1 for glass tints), white tints, subsurface radius (1, 0.2, 0.1), roughness and
+// specular 0.5, coat roughness 0.03, IORs 1.5, sheen roughness 0.3, subsurface scale 0.05,
+// thin-film IOR 1.4, flakes 0.004 / 0.3 / 0.9, opacity 1, absorption distance 1.
+void ref_material_defaults(int32_t type, pe_material* m) {
+    std::memset(m, 0, sizeof(pe_material));
+    m->type = type;
+    m->albedo_texture = m->roughness_texture = m->metalness_texture = m->normal_texture = m->opacity_texture = -1;
+    m->texture_scale = 1.0f;
+    const float sr[3] = {1.0f, 0.2f, 0.1f};
+    for (int i = 0; i < 3; ++i) {
+        m->base_color[i] = type == PE_MAT_DIELECTRIC ? 1.0f : 0.8f;
+        m->coat_tint[i] = m->sheen_color[i] = m->edge_tint[i] = 1.0f;
+        m->absorb_color[i] = m->scatter_color[i] = 1.0f;
+        m->flake_color[i] = 0.9f;
+        m->subsurface_radius[i] = sr[i];
+    }
+    m->roughness = m->specular = 0.5f;
+    m->clearcoat_roughness = 0.03f;
+    m->ior = m->coat_ior = 1.5f;
+    m->sheen_roughness = 0.3f;
+    m->subsurface_scale = 0.05f;
+    m->thin_film_ior = 1.4f;
+    m->flake_size = 0.004f;
+    m->flake_roughness = 0.3f;
+    m->opacity = 1.0f;
+    m->absorb_distance = 1.0f;
+}
+
 // A Film kept across calls (adaptive sampling reads the accumulated film).
 void* ref_film_create(int32_t w, int32_t h) { return new Film(w, h); }
 void ref_film_destroy(void* f) { delete static_cast<Film*>(f); }

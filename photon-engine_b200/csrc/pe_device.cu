@@ -1542,6 +1542,48 @@ int32_t pe_device_render(pe_device* d, const pe_camera* cam, const pe_settings* 
     return rr;
 }
 
+// A caller's film buffer must be memory of this device that holds `bytes` from `p` on: a host
+// pointer, another device's memory or a short buffer would make the film kernel write outside it.
+// The allocation's extent comes from the driver's cuMemGetAddressRange, reached through the
+// runtime's entry-point query (no link against the driver library).
+static int32_t checkFilmPointer(pe_device* d, const char* name, const void* p, size_t bytes) {
+    cudaPointerAttributes a{};
+    const cudaError_t e = cudaPointerGetAttributes(&a, p);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        setError(std::string("pe_device_render_tile_noalloc: ") + name + " is not CUDA memory: " + cudaMsg(e));
+        return PE_ERR_INVALID;
+    }
+    if ((a.type != cudaMemoryTypeDevice && a.type != cudaMemoryTypeManaged) || a.device != d->ordinal) {
+        setError(std::string("pe_device_render_tile_noalloc: ") + name + " must be device (or managed) memory of device " +
+                 std::to_string(d->ordinal));
+        return PE_ERR_INVALID;
+    }
+    using GetRange = int (*)(unsigned long long*, size_t*, unsigned long long);
+    static GetRange getRange = [] {
+        void* fn = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        if (cudaGetDriverEntryPoint("cuMemGetAddressRange", &fn, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess) {
+            cudaGetLastError();
+            fn = nullptr;
+        }
+        return reinterpret_cast<GetRange>(fn);
+    }();
+    if (getRange) {
+        unsigned long long base = 0;
+        size_t size = 0;
+        const unsigned long long addr = reinterpret_cast<unsigned long long>(p);
+        if (getRange(&base, &size, addr) == 0 && addr + bytes > base + size) {
+            setError(std::string("pe_device_render_tile_noalloc: ") + name + " holds " +
+                     std::to_string(base + size - addr) + " bytes from the given address; the film needs " +
+                     std::to_string(bytes));
+            return PE_ERR_INVALID;
+        }
+    }
+    return PE_OK;
+}
+
 // Tile render that allocates no device memory: path state lives in g_noAllocScratch, the film is
 // the caller's.  See include/photon_cuda.h for the contract.
 int32_t pe_device_render_tile_noalloc(pe_device* d, const pe_camera* cam, const pe_settings* st, int32_t x0, int32_t y0,
@@ -1578,8 +1620,24 @@ int32_t pe_device_render_tile_noalloc(pe_device* d, const pe_camera* cam, const 
         setError("pe_device_render_tile_noalloc: adaptive sampling needs the device's own film (pe_device_render)");
         return PE_ERR_INVALID;
     }
-    if (count <= 0) return PE_OK;
+    // The scratch holds plain path state only: no guiding records, no ray-cone column.
+    if (d->guideKind != 0) {
+        setError("pe_device_render_tile_noalloc: guided sampling (pe_device_set_guiding) is on; the tile entry "
+                 "renders unguided paths only");
+        return PE_ERR_INVALID;
+    }
+    if (d->scene.hasMips) {
+        setError("pe_device_render_tile_noalloc: the scene has mipmapped image maps, whose level of detail needs a "
+                 "per-path ray cone the tile entry does not keep");
+        return PE_ERR_INVALID;
+    }
     PE_CUDA(cudaSetDevice(d->ordinal));
+    const size_t px = static_cast<size_t>(st->width) * static_cast<size_t>(st->height);
+    rc = checkFilmPointer(d, "sum_rgb", sumRgb, px * 3 * sizeof(float));
+    if (!rc) rc = checkFilmPointer(d, "sample_count", sampleCount, px * sizeof(uint32_t));
+    if (!rc) rc = checkFilmPointer(d, "sum_lum_sq", sumLumSq, px * sizeof(float));
+    if (rc) return rc;
+    if (count <= 0) return PE_OK;
     Paths P = noAllocPaths(d->noAllocBase);
     // The array keeps the previous call's contents; the queue and shadow counters must start at 0.
     PE_CUDA(cudaMemsetAsync(P.counters, 0, 256, d->stream));

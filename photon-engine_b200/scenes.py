@@ -30,18 +30,13 @@ import math
 
 import numpy as np
 
-from .engine import (AreaLight, Dielectric, DisneyMaterial, EnvironmentLight, Lambertian, PerspectiveCamera,
-                     PixelFilterType, RenderSettings, Scene, TriangleMesh)
+from . import _capi as capi
+from . import scenegen
+from .engine import (AreaLight, Dielectric, DisneyMaterial, EnvironmentLight, Lambertian, Material, Mirror,
+                     PerspectiveCamera, PixelFilterType, RenderSettings, Scene, TriangleMesh)
 
 
-# Viewpoints of the workloads: (position, target, up, vertical fov in degrees).
-CAMERAS = {
-    "cornell": ((2.78, 2.73, -8.0), (2.78, 2.73, 0.0), (0.0, 1.0, 0.0), 39.3),
-    "knot": ((0.0, 4.5, -10.5), (0.0, 1.6, 0.0), (0.0, 1.0, 0.0), 40.0),
-    "media": ((0.0, 420.0, -950.0), (0.0, 70.0, 40.0), (0.0, 1.0, 0.0), 38.0),
-    "grid": ((0.0, 8.0, -13.0), (0.0, 1.0, 4.0), (0.0, 1.0, 0.0), 45.0),
-    "room": ((4.2, 1.7, 3.4), (-1.5, 0.9, -2.5), (0.0, 1.0, 0.0), 62.0),
-}
+CAMERAS = scenegen.CAMERAS
 
 
 def camera_for(name: str, width: int, height: int) -> PerspectiveCamera:
@@ -108,108 +103,51 @@ def cornell_box(width: int = 256, height: int = 256, spp: int = 64, max_depth: i
     return scene, camera, settings
 
 
-def _knot_curve(t, p=2, q=3):
-    r = np.cos(q * t) + 2.0
-    return np.stack([r * np.cos(p * t), -np.sin(q * t), r * np.sin(p * t)], axis=-1)
+torus_knot_mesh = scenegen.knot_mesh
+sky_environment = scenegen.sky_image
+
+_MATERIAL_CLASSES = {scenegen.MAT_LAMBERT: Lambertian, scenegen.MAT_DISNEY: DisneyMaterial,
+                     scenegen.MAT_DIELECTRIC: Dielectric, scenegen.MAT_MIRROR: Mirror}
 
 
-def torus_knot_mesh(nu: int = 4096, nv: int = 128, tube: float = 0.38, seed: int = 1):
-    """(2,3) torus knot tube with nu × nv quads (2·nu·nv triangles), seeded radial jitter."""
-    rng = np.random.default_rng(seed)
-    t = np.linspace(0.0, 2.0 * np.pi, nu, endpoint=False)
-    c = _knot_curve(t)
-    dt = 1e-3
-    tangent = _knot_curve(t + dt) - _knot_curve(t - dt)
-    tangent /= np.linalg.norm(tangent, axis=1, keepdims=True)
-    # rotation-minimising frame by parallel transport
-    nrm = np.empty_like(tangent)
-    ref = np.array([0.0, 1.0, 0.0])
-    n0 = np.cross(tangent[0], ref)
-    nrm[0] = n0 / np.linalg.norm(n0)
-    for i in range(1, nu):
-        n = nrm[i - 1] - tangent[i] * np.dot(nrm[i - 1], tangent[i])
-        nrm[i] = n / np.linalg.norm(n)
-    binrm = np.cross(tangent, nrm)
-    ang = np.linspace(0.0, 2.0 * np.pi, nv, endpoint=False)
-    radius = tube * (1.0 + 0.02 * rng.standard_normal((nu, nv)))
-    pos = (c[:, None, :] + radius[..., None] * (np.cos(ang)[None, :, None] * nrm[:, None, :] +
-                                                np.sin(ang)[None, :, None] * binrm[:, None, :]))
-    pos = (pos + np.array([0.0, 1.9, 0.0])).astype(np.float32).reshape(-1, 3)
-    i = np.arange(nu)[:, None]
-    j = np.arange(nv)[None, :]
-    a = i * nv + j
-    b = ((i + 1) % nu) * nv + j
-    cc = ((i + 1) % nu) * nv + (j + 1) % nv
-    d = i * nv + (j + 1) % nv
-    quads = np.stack([a, b, cc, d], axis=-1).reshape(nu, nv, 4)
-    return pos, quads
+def material_from_description(d: dict) -> Material:
+    """A product material from a description dict: pe_material_defaults of its type, then each
+    named pe_material field."""
+    cls = _MATERIAL_CLASSES[int(d["type"])]
+    m = cls.__new__(cls)
+    Material.__init__(m)
+    for key, value in d.items():
+        if key == "type":
+            continue
+        setattr(m.struct, key, capi.f3(value) if isinstance(value, (tuple, list, np.ndarray)) else value)
+    return m
 
 
-def sky_environment(width: int = 2048, height: int = 1024, sun_dir=(0.45, 0.62, -0.64), sun_share: float = 0.6,
-                    sun_sigma_deg: float = 1.5, seed: int = 2) -> np.ndarray:
-    """Sky gradient plus one Gaussian sun lobe holding ``sun_share`` of the (solid-angle weighted)
-    luminance, in the reference's equirect convention (v = θ/π, y up, φ = atan2(−z, x) + π)."""
-    rng = np.random.default_rng(seed)
-    v = (np.arange(height) + 0.5) / height
-    u = (np.arange(width) + 0.5) / width
-    theta = v * np.pi
-    a = u * 2.0 * np.pi - np.pi
-    st = np.sin(theta)[:, None]
-    d = np.stack([st * np.cos(a)[None, :], np.cos(theta)[:, None] * np.ones((1, width)), -st * np.sin(a)[None, :]], -1)
-    up = d[..., 1]
-    zenith = np.array([0.25, 0.45, 1.0])
-    horizon = np.array([1.0, 0.95, 0.9])
-    ground = np.array([0.18, 0.16, 0.14])
-    tsky = np.clip(up, 0.0, 1.0)[..., None]
-    sky = np.where(up[..., None] >= 0.0, horizon * (1 - tsky) + zenith * tsky, ground)
-    sky = sky * (1.0 + 0.02 * rng.standard_normal((height, width, 1)))
-    sdir = np.asarray(sun_dir, np.float64)
-    sdir /= np.linalg.norm(sdir)
-    cosang = np.clip((d * sdir).sum(-1), -1.0, 1.0)
-    ang = np.arccos(cosang)
-    lobe = np.exp(-0.5 * (ang / np.radians(sun_sigma_deg)) ** 2)
-    w = np.sin(theta)[:, None]
-    lum = lambda img: (0.212671 * img[..., 0] + 0.715160 * img[..., 1] + 0.072169 * img[..., 2])
-    sky_power = float((lum(sky) * w).sum())
-    lobe_power = float((lobe * w).sum())
-    k = sun_share / (1.0 - sun_share) * sky_power / lobe_power
-    sun_color = np.array([1.0, 0.93, 0.8])
-    img = sky + k * lobe[..., None] * sun_color / lum(sun_color[None, None, :])[..., None]
-    return img.astype(np.float32)
+def from_description(desc: dict):
+    """(Scene, PerspectiveCamera, RenderSettings) of a scenegen description."""
+    mats = [material_from_description(m) for m in desc["materials"]]
+    scene = Scene()
+    for kind, o in desc["ops"]:
+        if kind == "mesh":
+            scene.add_shape(TriangleMesh(o["positions"], o.get("normals"), o.get("uvs"), o["indices"],
+                                         mats[o["material"]]))
+        else:
+            scene.add_light(AreaLight(o["position"], o["u"], o["v"], o["radiance"]))
+    env = desc.get("environment")
+    if env is not None:
+        scene.set_environment(EnvironmentLight(env["image"], env["rotation"], env["intensity"]))
+    c = desc["camera"]
+    camera = PerspectiveCamera(c["position"], c["target"], c["up"], c["vfov"], c["aspect"])
+    st = dict(desc["settings"])
+    st["filter_type"] = PixelFilterType(st["filter_type"])
+    return scene, camera, RenderSettings(**st)
 
 
 def torus_knot_scene(width: int = 1920, height: int = 1080, spp: int = 256, max_depth: int = 12, nu: int = 4096,
                      nv: int = 128, env_size=(2048, 1024), seed: int = 7, clusters: int = 64):
-    """Product-scale workload: ~1M-triangle torus knot, eight Disney materials, HDR sky, softbox."""
-    rng = np.random.default_rng(seed)
-    mats = []
-    for _ in range(8):
-        m = DisneyMaterial(tuple(rng.uniform(0.0, 1.0, 3)), float(rng.choice([0.0, 1.0])),
-                           float(rng.uniform(0.05, 0.9)), 0.5)
-        m.set_clear_coat(float(rng.uniform(0.0, 1.0)))
-        mats.append(m)
-    scene = Scene()
-    pos, quads = torus_knot_mesh(nu, nv, seed=seed)
-    # random face clusters: contiguous runs of rings along the knot, each with one material
-    cuts = np.sort(rng.choice(np.arange(1, nu), clusters - 1, replace=False))
-    bounds = np.concatenate([[0], cuts, [nu]])
-    for k in range(clusters):
-        q = quads[bounds[k]:bounds[k + 1]].reshape(-1, 4)
-        tri = np.concatenate([q[:, [0, 1, 2]], q[:, [0, 2, 3]]], axis=0)
-        used = np.unique(tri)
-        remap = np.full(pos.shape[0], -1, np.int64)
-        remap[used] = np.arange(used.size)
-        scene.add_shape(TriangleMesh(pos[used], None, None, remap[tri].astype(np.uint32), mats[int(rng.integers(0, 8))]))
-    g = 40.0
-    gp = np.array([(-g, 0.0, -g), (-g, 0.0, g), (g, 0.0, g), (g, 0.0, -g)], np.float32)
-    scene.add_shape(TriangleMesh(gp, None, None, np.array([[0, 1, 2], [0, 2, 3]], np.uint32), Lambertian((0.5, 0.5, 0.5))))
-    softbox = AreaLight((-3.0, 6.5, -2.0), (3.0, 0.0, 0.0), (0.0, 0.0, 2.0), (12.0, 12.0, 12.0))
-    scene.add_light(softbox)
-    scene.set_environment(EnvironmentLight(sky_environment(*env_size), 0.0, 1.0))
-    camera = camera_for("knot", width, height)
-    settings = RenderSettings(width=width, height=height, samples_per_pixel=spp, max_bounces=max_depth,
-                              filter_type=PixelFilterType.BlackmanHarris, filter_width=1.5)
-    return scene, camera, settings
+    """Product-scale workload: ~1M-triangle torus knot, eight Disney materials, HDR sky, softbox
+    (``scenegen.torus_knot``)."""
+    return from_description(scenegen.torus_knot(width, height, spp, max_depth, nu, nv, env_size, seed, clusters))
 
 
 def uv_sphere(center, radius: float, nu: int, nv: int):

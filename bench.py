@@ -12,7 +12,7 @@ msamplesPerSecond definition).
 ``e2e``     the same K steps through the public RenderDevice::render call with host films:
             camera + settings in, the frame's film (sum, count, sum of squares) read back and
             merged on the host every step.
-``roofline`` closest-hit traversal kernel: algorithmic bytes (BVH nodes visited × 64 B +
+``roofline`` closest-hit traversal kernel: algorithmic bytes (4-wide BVH nodes visited × 128 B +
             triangles tested × 48 B + ray record 32 B + hit record 16 B + queue index 4 B per
             ray, counted on the device over one untimed step) ÷ its CUDA-event time, against
             the measured HBM copy bandwidth.
@@ -42,7 +42,7 @@ sys.path.insert(0, str(ROOT))
 
 WIDTH, HEIGHT, DEPTH = 1920, 1080, 12
 SPP_PER_STEP = 4  # one step = 4 samples per pixel of the 1080p frame (one wave of 8.3M paths)
-NODE_BYTES, TRI_BYTES, RAY_BYTES, HIT_BYTES, QUEUE_BYTES = 64, 48, 32, 16, 4
+NODE_BYTES, TRI_BYTES, RAY_BYTES, HIT_BYTES, QUEUE_BYTES = 128, 48, 32, 16, 4  # 4-wide BVH node: 128 B
 L2_NOTE = "inputs larger than L2: 140 MB resident scene + 300 MB path state per 2M-path wave (L2 126 MB)"
 
 

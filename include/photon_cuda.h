@@ -357,6 +357,17 @@ int32_t pe_device_render_passes(pe_device* d, const pe_camera* cam, const pe_set
                                 float* sum_lum_sq, const pe_aov_films* aovs, const pe_pass_films* passes,
                                 uint64_t* traced);
 
+/* A render region: pe_device_render restricted to the pixels of the rectangle (x0, y0, w, h) of
+ * the st->width x st->height frame.  No counterpart in the reference's RenderDevice; it serves
+ * crop renders (a viewport's border region, fixed crop windows of a convergence check) without
+ * tracing the rest of the frame.  The host films cover the whole frame as for pe_device_render;
+ * only the region's pixels change, each exactly as a whole-frame render would change it (same
+ * paths, same per-pixel sample order).  Adaptive sampling is rejected (PE_ERR_INVALID). */
+int32_t pe_device_render_region(pe_device* d, const pe_camera* cam, const pe_settings* st, int32_t x0, int32_t y0,
+                                int32_t w, int32_t h, int32_t first_sample, int32_t count,
+                                const volatile int32_t* cancel, float* sum_rgb, uint32_t* sample_count,
+                                float* sum_lum_sq, uint64_t* samples_traced);
+
 /* Same, accumulating into the device-resident film (kept across calls until
  * pe_device_film_clear; resized/cleared when width/height change). */
 int32_t pe_device_render_resident(pe_device* d, const pe_camera* cam, const pe_settings* st, int32_t first_sample,
@@ -416,9 +427,15 @@ int32_t pe_device_timer_end(pe_device* d, float* ms);
 /* Camera ray of (x, y, sample_index) for every pixel, then closest hit:
  * shape index (mesh/area-light triangle order of insertion; -1 = miss),
  * triangle index within the shape, t.  Follows Renderer tracePixel +
- * BVH::intersect (src/engine/renderer.cpp:139-160, src/geometry/bvh.cpp:322-401). */
+ * BVH::intersect (src/engine/renderer.cpp:139-160, src/geometry/bvh.cpp:322-401),
+ * through the 4-wide tree the render kernels traverse: t equals the reference's bit
+ * for bit; where two triangles give the identical t the other of them may be reported. */
 int32_t pe_device_trace_primary(pe_device* d, const pe_camera* cam, const pe_settings* st, int32_t sample_index,
                                 int32_t* out_shape, int32_t* out_prim, float* out_t);
+/* The same through the binary tree in the reference's own visiting order (near child first,
+ * last tested triangle wins a tie), so ids are the reference's bit for bit, ties included. */
+int32_t pe_device_trace_primary_ordered(pe_device* d, const pe_camera* cam, const pe_settings* st,
+                                        int32_t sample_index, int32_t* out_shape, int32_t* out_prim, float* out_t);
 
 /* Owen-scrambled Sobol values: for each i, (px[i], py[i], index[i]) and
  * n_dims consecutive 2-D dimensions → out[i*n_dims*2 + 2*k + {0,1}]. */

@@ -22,6 +22,7 @@ REF_DIR = HERE / "_ref"
 PARITY_LIB = REF_DIR / "libphoton_ref.so"
 FAST_LIB = REF_DIR / "libphoton_ref_fast.so"
 RESTATEMENT_LIB = REF_DIR / "libpe_oracle.so"
+ADAPTER_LIB = REF_DIR / "libpe_adapter.so"  # the reference engine + the drop-in adapter over libphoton_cuda.so
 
 FP = C.POINTER(C.c_float)
 IP = C.POINTER(C.c_int32)
@@ -34,11 +35,17 @@ def available(fast: bool = False) -> bool:
     return (FAST_LIB if fast else PARITY_LIB).exists()
 
 
-def _load(fast: bool = False):
-    key = "fast" if fast else "parity"
+def adapter_available() -> bool:
+    return ADAPTER_LIB.exists()
+
+
+def _load(fast=False):
+    """fast: False the parity build, True the shipping build, "adapter" the parity build linked
+    with the drop-in RenderDevice adapter."""
+    key = "adapter" if fast == "adapter" else ("fast" if fast else "parity")
     if key in _libs:
         return _libs[key]
-    path = FAST_LIB if fast else PARITY_LIB
+    path = ADAPTER_LIB if key == "adapter" else (FAST_LIB if fast else PARITY_LIB)
     if not path.exists():
         raise RuntimeError(f"{path} missing: build it with `make -C oracle` where the reference sources exist")
     lib = C.CDLL(str(path))
@@ -94,7 +101,13 @@ def _load(fast: bool = False):
         "ref_dtree_probe": (C.c_int32, [FP, FP, C.c_int32, FP, FP, C.c_int32, FP, FP, C.c_int32, FP, FP]),
         "ref_render_camera": (C.c_int32, [P, P, C.c_void_p, C.c_int32, C.c_int32, C.c_int32, FP, UP]),
         "ref_material_defaults": (None, [C.c_int32, C.c_void_p]),
+        "ref_render_rect": (C.c_int32, [P, P, C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32,
+                                        C.c_int32, C.c_int32, FP, UP]),
     }
+    if key == "adapter":
+        sig["ref_session_cuda"] = (C.c_int32, [P, P, C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.c_int32, FP, UP, FP,
+                                               IP, C.c_char_p, C.c_size_t])
+        sig["ref_session_cuda_update"] = (C.c_int32, [P, C.c_int32, C.c_int32, FP])
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
         fn.restype = res
@@ -245,6 +258,52 @@ class RefScene:
         fn(self.h, C.byref(camera.describe_gpu()), C.byref(settings.to_c()), first, count, threads, _f(mean),
            cnt.ctypes.data_as(UP))
         return mean, cnt
+
+    def render_rect(self, camera, settings, rect, first: int, count: int, threads: int = 0):
+        """Mean (h, w, 3) and counts of samples [first, first+count) of the pixels of
+        rect = (x0, y0, w, h) of the frame: the seeded tracePixel loop through the reference's own
+        camera class."""
+        x0, y0, w, h = (int(v) for v in rect)
+        mean = np.zeros((h, w, 3), np.float32)
+        cnt = np.zeros((h, w), np.uint32)
+        cam = reference_camera(camera, self.lib)
+        try:
+            rc = self.lib.ref_render_rect(self.h, cam, C.byref(settings.to_c()), first, count, threads, x0, y0, w, h,
+                                          _f(mean), cnt.ctypes.data_as(UP))
+        finally:
+            self.lib.ref_camera_destroy(cam)
+        if rc != 0:
+            raise ValueError(f"rectangle {rect} outside the {settings.width}x{settings.height} frame")
+        return mean, cnt
+
+    def session_cuda(self, camera, settings, spp: int, batch: int = 8, aovs: bool = False, adaptive: bool = False):
+        """RenderSession (begin, advance until finished) on the B200 device through the drop-in
+        RenderDevice adapter (RefScene built with fast="adapter").  Returns (mean, counts,
+        albedo mean or None, samples per pixel done, features bits: 1 aovs, 2 lightPasses, 4
+        adaptiveSampling)."""
+        h, w = settings.height, settings.width
+        mean = np.zeros((h, w, 3), np.float32)
+        cnt = np.zeros((h, w), np.uint32)
+        alb = np.zeros((h, w, 3), np.float32) if aovs else None
+        feats = C.c_int32(0)
+        err = C.create_string_buffer(512)
+        cam = reference_camera(camera, self.lib)
+        try:
+            done = self.lib.ref_session_cuda(self.h, cam, C.byref(settings.to_c()), spp, batch, 1 if aovs else 0,
+                                             1 if adaptive else 0, _f(mean), cnt.ctypes.data_as(UP), _f(alb),
+                                             C.byref(feats), err, len(err))
+        finally:
+            self.lib.ref_camera_destroy(cam)
+        if done < 0:
+            raise RuntimeError(f"adapter session failed ({done}): {err.value.decode()}")
+        return mean, cnt, alb, int(done), int(feats.value)
+
+    def session_cuda_update(self, kind: int, index: int, rgb):
+        """Edits the reference scene (kind 1: material `index`'s Disney base colour; kind 2:
+        AreaLight `index`'s radiance) and calls the adapter's RenderDevice::updateScene."""
+        rc = self.lib.ref_session_cuda_update(self.h, int(kind), int(index), _f3(rgb))
+        if rc != 0:
+            raise RuntimeError(f"adapter update failed ({rc})")
 
     def render_into(self, film: "RefFilm", camera, settings, first: int, count: int, threads: int = 0) -> int:
         """Renderer::renderSamples (seed 12345) adding samples [first, first+count) to a kept film

@@ -37,6 +37,11 @@
 #include "materials/lambertian.h"
 #include "materials/mirror.h"
 #include "samplers/sobol_sampler.h"
+#ifdef PE_WITH_ADAPTER
+#include "engine/render_session.h"
+#include "adapter/cuda_render_device.h"
+#include <cstdio>
+#endif
 
 #include <atomic>
 #include <cstring>
@@ -703,6 +708,63 @@ static int32_t renderRowsWith(RefScene* rs, const Camera& camera, const pe_setti
     return 0;
 }
 
+// The seeded tracePixel loop of ref_render_rows over one rectangle of the frame (x0, y0, cw, ch),
+// through the reference's own camera object: mean (ch, cw, 3) and counts (ch, cw) of the crop.
+int32_t ref_render_rect(void* s, void* cam, const pe_settings* st, int32_t first, int32_t count, int32_t threads,
+                        int32_t x0, int32_t y0, int32_t cw, int32_t ch, float* mean_rgb, uint32_t* counts) {
+    auto* rs = static_cast<RefScene*>(s);
+    const Camera& camera = *static_cast<const Camera*>(cam);
+    const int w = st->width, h = st->height;
+    if (x0 < 0 || y0 < 0 || cw <= 0 || ch <= 0 || x0 + cw > w || y0 + ch > h) return -1;
+    Film film(w, h);
+    PathTracer integrator(st->max_bounces, st->rr_depth, st->ao_strength, st->shadow_quality);
+    integrator.setClampIndirect(st->clamp_indirect);
+    PixelFilter pf;
+    pf.type = static_cast<PixelFilterType>(st->filter_type);
+    pf.width = st->filter_width;
+    const PixelFilterSampler filter(pf);
+    const int nt = threads > 0 ? threads : hardwareThreads();
+    std::atomic<int> next{0};
+    auto work = [&]() {
+        SobolSampler sampler(st->seed);
+        for (;;) {
+            const int k = next.fetch_add(1);
+            if (k >= cw * ch) break;
+            const int x = x0 + k % cw, y = y0 + k / cw;
+            for (int si = first; si < first + count; ++si) {
+                sampler.startPixel(x, y);
+                sampler.startSample(si);
+                const Vec2f offset = filter.sample(sampler.get2D());
+                const float sx = (static_cast<float>(x) + 0.5f + offset.x) / static_cast<float>(w);
+                const float sy = 1.0f - (static_cast<float>(y) + 0.5f + offset.y) / static_cast<float>(h);
+                const Vec2f lens = sampler.get2D();
+                Ray ray = camera.generateRay(sx, sy, lens);
+                ray.coneWidth = camera.pixelConeWidth(h);
+                ray.coneSpread = camera.pixelConeSpread(h);
+                if (rs->scene.background().mode == Background::Mode::Environment) {
+                    film.addSample(x, y, integrator.Li(ray, rs->scene, sampler));
+                } else {
+                    PathTracer::PrimaryHit primary;
+                    film.addSample(x, y, integrator.Li(ray, rs->scene, sampler, &primary, nullptr));
+                }
+            }
+        }
+    };
+    std::vector<std::thread> pool;
+    for (int i = 0; i < nt; ++i) pool.emplace_back(work);
+    for (auto& t : pool) t.join();
+    std::vector<float> mean(static_cast<size_t>(w) * h * 3);
+    std::vector<uint32_t> cnt(static_cast<size_t>(w) * h);
+    exportFilm(film, w, h, mean.data(), cnt.data());
+    for (int y = 0; y < ch; ++y)
+        for (int x = 0; x < cw; ++x) {
+            const size_t src = static_cast<size_t>(y0 + y) * w + x0 + x, dst = static_cast<size_t>(y) * cw + x;
+            for (int c = 0; c < 3; ++c) mean_rgb[3 * dst + c] = mean[3 * src + c];
+            counts[dst] = cnt[src];
+        }
+    return 0;
+}
+
 // Primary hit per pixel for one sample index: tracePixel's camera ray, then the first
 // Scene::intersect of PathTracer::Li with the camera visibility mask (path_tracer.cpp:326,420).
 int32_t ref_trace_primary(void* s, const pe_camera* cam, const pe_settings* st, int32_t sample_index,
@@ -872,5 +934,89 @@ int32_t ref_env_eval(void* s, const float* dirs, size_t n, float* out_rgb, float
     }
     return 0;
 }
+
+#ifdef PE_WITH_ADAPTER
+// The B200 device through the drop-in adapter (photon-engine_b200/adapter), driven by the
+// reference's own RenderSession (src/engine/render_session.cpp:17-101) on a reference Scene: the
+// parity check of the adapter itself.  One device per process, created on first use.
+static std::unique_ptr<RenderDevice>& cudaAdapterDevice(std::string* err) {
+    static std::unique_ptr<RenderDevice> dev;
+    if (!dev) dev = createCudaRenderDevice(0, err);
+    return dev;
+}
+
+// Full RenderSession on the adapter: begin(camera, settings with `spp` samples, Final mode, maxBatch
+// `batch`), advance() until finished.  Beauty mean and counts (h, w) come back; with aovs, the
+// albedo film's mean too.  features = the device's (aovs, lightPasses, adaptive) as bits 0-2.
+int32_t ref_session_cuda(void* s, void* cam, const pe_settings* st, int32_t spp, int32_t batch, int32_t aovs,
+                         int32_t adaptive, float* mean_rgb, uint32_t* counts, float* albedo_mean, int32_t* features,
+                         char* err, size_t errLen) {
+    auto* rs = static_cast<RefScene*>(s);
+    std::string e;
+    auto& dev = cudaAdapterDevice(&e);
+    if (!dev) {
+        std::snprintf(err, errLen, "%s", e.c_str());
+        return -1;
+    }
+    const DeviceFeatures f = dev->features();
+    *features = (f.aovs ? 1 : 0) | (f.lightPasses ? 2 : 0) | (f.adaptiveSampling ? 4 : 0);
+    dev->setScene(std::shared_ptr<const Scene>(std::shared_ptr<const Scene>{}, &rs->scene));
+    if (!dev->hasScene()) {
+        std::snprintf(err, errLen, "the adapter did not take the scene");
+        return -2;
+    }
+    RenderSettings settings = toSettings(*st, hardwareThreads());
+    settings.samplesPerPixel = spp;
+    settings.adaptiveSampling = adaptive != 0;
+    settings.noiseThreshold = st->noise_threshold;
+    settings.minAdaptiveSamples = st->min_adaptive_samples;
+    SessionConfig config;
+    config.mode = RenderMode::Final;
+    config.targetSpp = spp;
+    config.aovs = aovs != 0;
+    config.maxBatch = batch;
+    RenderSession session(*dev);
+    session.begin(std::shared_ptr<const Camera>(std::shared_ptr<const Camera>{}, static_cast<const Camera*>(cam)),
+                  settings, config);
+    int guard = 0;
+    while (!session.finished() && guard++ < 100000)
+        if (!session.advance(nullptr)) break;
+    exportFilm(session.film(), st->width, st->height, mean_rgb, counts);
+    if (aovs && albedo_mean && session.aovs()) {
+        std::vector<uint32_t> c(static_cast<size_t>(st->width) * static_cast<size_t>(st->height));
+        exportFilm(session.aovs()->albedo, st->width, st->height, albedo_mean, c.data());
+    }
+    return session.samples();
+}
+
+// SceneUpdateKind edits through the adapter: kind 1 sets material `index`'s base colour (a Disney
+// material) or albedo-free Lambert is left alone; kind 2 sets AreaLight `index`'s radiance; then
+// RenderDevice::updateScene(scene, kind).
+int32_t ref_session_cuda_update(void* s, int32_t kind, int32_t index, const float* rgb) {
+    auto* rs = static_cast<RefScene*>(s);
+    std::string e;
+    auto& dev = cudaAdapterDevice(&e);
+    if (!dev) return -1;
+    if (kind == 1) {
+        if (index < 0 || index >= static_cast<int32_t>(rs->materials.size())) return -2;
+        auto* d = dynamic_cast<DisneyMaterial*>(rs->materials[static_cast<size_t>(index)].get());
+        if (!d) return -3;
+        d->setBaseColor(c3(rgb));
+        dev->updateScene(std::shared_ptr<const Scene>(std::shared_ptr<const Scene>{}, &rs->scene),
+                         SceneUpdateKind::Materials);
+    } else if (kind == 2) {
+        int k = 0;
+        for (const Light* l : rs->scene.lights())
+            if (auto* a = dynamic_cast<const AreaLight*>(l)) {
+                if (k++ == index) const_cast<AreaLight*>(a)->setRadiance(c3(rgb));
+            }
+        dev->updateScene(std::shared_ptr<const Scene>(std::shared_ptr<const Scene>{}, &rs->scene),
+                         SceneUpdateKind::Lights);
+    } else {
+        return -4;
+    }
+    return dev->hasScene() ? 0 : -5;
+}
+#endif
 
 } // extern "C"

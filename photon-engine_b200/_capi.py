@@ -200,6 +200,9 @@ SIGNATURES = {
     "pe_device_render": (C.c_int32, [P, C.POINTER(pe_camera), C.POINTER(pe_settings), C.c_int32, C.c_int32,
                                      IP, FP, UP, FP, C.POINTER(C.c_uint64)]),
     "pe_device_render_resident": (C.c_int32, [P, C.POINTER(pe_camera), C.POINTER(pe_settings), C.c_int32, C.c_int32, IP]),
+    "pe_device_render_region": (C.c_int32, [P, C.POINTER(pe_camera), C.POINTER(pe_settings), C.c_int32, C.c_int32,
+                                            C.c_int32, C.c_int32, C.c_int32, C.c_int32, IP, FP, UP, FP,
+                                            C.POINTER(C.c_uint64)]),
     "pe_device_film_clear": (C.c_int32, [P]),
     "pe_device_render_tile_noalloc": (C.c_int32, [P, C.POINTER(pe_camera), C.POINTER(pe_settings), C.c_int32,
                                                   C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_void_p,
@@ -214,6 +217,8 @@ SIGNATURES = {
     "pe_device_timer_begin": (C.c_int32, [P]),
     "pe_device_timer_end": (C.c_int32, [P, FP]),
     "pe_device_trace_primary": (C.c_int32, [P, C.POINTER(pe_camera), C.POINTER(pe_settings), C.c_int32, IP, IP, FP]),
+    "pe_device_trace_primary_ordered": (C.c_int32, [P, C.POINTER(pe_camera), C.POINTER(pe_settings), C.c_int32, IP, IP,
+                                                    FP]),
     "pe_device_sobol": (C.c_int32, [P, C.c_uint64, IP, IP, IP, C.c_size_t, C.c_int32, FP]),
     "pe_device_bsdf_probe": (C.c_int32, [P, C.c_int32, C.POINTER(pe_bsdf_query), C.c_size_t, C.POINTER(pe_bsdf_result)]),
     "pe_device_guide_reset": (C.c_int32, [P, C.c_uint64, FP, FP]),

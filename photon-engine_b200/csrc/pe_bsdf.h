@@ -1047,12 +1047,15 @@ PE_HDN bool glassSample(const MatGPU& m, V3 woW, const ShadePoint& sp, float uc,
 }
 
 // ---------------------------------------------------------------------------------------------
-// Dispatch (Material::evalPdf / sampleFull)
-PE_HD V3 bsdfEvalPdf(const TablesGPU* T, const MatGPU& m, V3 wo, V3 wi, const ShadePoint& sp, float& pdf,
-                     LobeSplit3* split) {
+// Dispatch (Material::evalPdf / sampleFull).  MT >= 0 fixes the material type at compile time
+// (a kernel that shades one material kind carries only that kind's code); MT < 0 reads m.type.
+template <int MT>
+PE_HD V3 bsdfEvalPdfT(const TablesGPU* T, const MatGPU& m, V3 wo, V3 wi, const ShadePoint& sp, float& pdf,
+                      LobeSplit3* split) {
+    const int type = MT >= 0 ? MT : m.type;
     if (split) split->diffuse = split->glossy = split->transmission = mk(0.0f);
     V3 f;
-    switch (m.type) {
+    switch (type) {
         case 0:
             f = lambertEval(m, wo, wi, sp.n, pdf);
             break;
@@ -1072,15 +1075,21 @@ PE_HD V3 bsdfEvalPdf(const TablesGPU* T, const MatGPU& m, V3 wo, V3 wi, const Sh
         // Material::evalSplit (material.h:154-160) and Dielectric::evalSplit (dielectric.cpp:279-286):
         // same side of the geometric surface → diffuse (glass: glossy), else transmission
         const V3 nn = len2(sp.ng) > 0.0f ? sp.ng : sp.n;
-        if (dot(wo, nn) * dot(wi, nn) >= 0.0f) (m.type == 2 ? split->glossy : split->diffuse) = f;
+        if (dot(wo, nn) * dot(wi, nn) >= 0.0f) (type == 2 ? split->glossy : split->diffuse) = f;
         else split->transmission = f;
     }
     return f;
 }
 
-PE_HD bool bsdfSample(const TablesGPU* T, const MatGPU& m, V3 wo, const ShadePoint& sp, float uc, V2 u,
-                      BsdfSample& out) {
-    switch (m.type) {
+PE_HD V3 bsdfEvalPdf(const TablesGPU* T, const MatGPU& m, V3 wo, V3 wi, const ShadePoint& sp, float& pdf,
+                     LobeSplit3* split) {
+    return bsdfEvalPdfT<-1>(T, m, wo, wi, sp, pdf, split);
+}
+
+template <int MT>
+PE_HD bool bsdfSampleT(const TablesGPU* T, const MatGPU& m, V3 wo, const ShadePoint& sp, float uc, V2 u,
+                       BsdfSample& out) {
+    switch (MT >= 0 ? MT : m.type) {
         case 0:
             return lambertSample(m, wo, sp.n, u, out);
         case 1:
@@ -1092,6 +1101,11 @@ PE_HD bool bsdfSample(const TablesGPU* T, const MatGPU& m, V3 wo, const ShadePoi
         default:
             return false;
     }
+}
+
+PE_HD bool bsdfSample(const TablesGPU* T, const MatGPU& m, V3 wo, const ShadePoint& sp, float uc, V2 u,
+                      BsdfSample& out) {
+    return bsdfSampleT<-1>(T, m, wo, sp, uc, u, out);
 }
 
 } // namespace pe

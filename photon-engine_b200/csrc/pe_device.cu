@@ -168,6 +168,18 @@ WaveSeg makeSeg(const pe_camera* cam, const pe_settings* st) {
 }
 
 
+// SceneGPU::leanShading of a scene: true when none of its materials and scene settings use a
+// shading feature that the lean shading kernels compile out.
+int32_t leanShadingOf(const SceneGPU& G, const std::vector<MatGPU>& mats) {
+    if (G.hasVolumes || G.hasSubsurface || G.hasMips || G.hasLightLinks || G.hasShadowLinks || G.catcherShape >= 0)
+        return 0;
+    for (const MatGPU& m : mats) {
+        if (m.roundEdge > 0.0f || (m.flags & (MF_DISPERSIVE | MF_VOLUME_BOUNDARY | MF_HAS_MEDIUM))) return 0;
+        if (m.type == PE_MAT_DISNEY && (m.opacity < 1.0f || m.texOpacity >= 0)) return 0;
+    }
+    return 1;
+}
+
 // Scratch of pe_device_render_tile_noalloc: path-state columns, queues, shadow records and
 // counters for kNoAllocSlots paths, carved out of one file-scope device array (8.5 MB).  Every
 // GPU that loads this library holds the array until the process exits.
@@ -190,6 +202,32 @@ Paths noAllocPaths(unsigned char* base) {
     P.counters = reinterpret_cast<uint32_t*>(base + off);
     P.capacity = static_cast<uint32_t>(kNoAllocSlots);
     return P;
+}
+
+// The lean shading kernels of one bounce, one per shading key whose material type the scene
+// uses (the miss key always); returns the number of launches.
+int launchLeanShade(pe_device* d, const SceneGPU& S, const Paths& P, const Wave& W, int32_t* qOut, uint32_t* cOut,
+                    cudaStream_t cs, bool out) {
+    int n = 0;
+    auto one = [&](auto kernel, int key) {
+        if (key > 0 && !(S.materialTypes & (1 << (key - 1)))) return;
+        kernel<<<d->blocksShadeKey[key], 128, 0, cs>>>(S, P, W, qOut, cOut);
+        ++n;
+    };
+    if (out) {
+        one(kShadeKey<true, 0>, 0);
+        one(kShadeKey<true, 1>, 1);
+        one(kShadeKey<true, 2>, 2);
+        one(kShadeKey<true, 3>, 3);
+        one(kShadeKey<true, 4>, 4);
+    } else {
+        one(kShadeKey<false, 0>, 0);
+        one(kShadeKey<false, 1>, 1);
+        one(kShadeKey<false, 2>, 2);
+        one(kShadeKey<false, 3>, 3);
+        one(kShadeKey<false, 4>, 4);
+    }
+    return n;
 }
 
 int32_t timerEvent(pe_device* d, RenderTimer& tm, cudaEvent_t& e) {
@@ -328,6 +366,12 @@ int32_t runWave(pe_device* d, int lane, Paths& P, int nSegs, int nSlots, int nPi
     uint32_t* cIn = &P.counters[0];
     uint32_t* cOut = &P.counters[1];
     stats.paths += static_cast<uint64_t>(nSlots);
+    // lean shading (one specialised kernel per shading key) for plain surface scenes that
+    // neither guide nor record; shadows without transmitters or shadow links are plain any-hits
+    bool noAo = true;
+    for (int k = 0; k < nSegs; ++k) noAo = noAo && !(ln.hSegs[k].aoStrength > 0.0f);
+    const bool lean = S.leanShading && !P.guiding && !P.sdMode && noAo && !d->counting;
+    const bool anyHitShadows = !S.hasShadowTransmitters && !S.hasShadowLinks;
     int64_t tailPaths = d->tailPaths < 0 ? static_cast<int64_t>(d->blocksTail) * kTailBlock : d->tailPaths;
     // the tail kernel runs no inference: keep guided bounces in the wavefront until few paths remain
     if (P.guiding == 2) tailPaths = std::min<int64_t>(tailPaths, kGuideTailPaths);
@@ -342,7 +386,10 @@ int32_t runWave(pe_device* d, int lane, Paths& P, int nSegs, int nSlots, int nPi
                 PE_CUDA(cudaEventRecord(t0, cs));
             }
             const bool out = P.aovA || P.pass;
-            if (d->counting && out)
+            if (lean && !d->counting && !out)
+                kTail<false, false, true><<<std::min(grid, d->blocksTailLean), kTailBlock, 0, cs>>>(
+                    S, P, W, qIn, cIn, &P.counters[CNT_WORK_TAIL], d->dStats);
+            else if (d->counting && out)
                 kTail<true, true><<<grid, kTailBlock, 0, cs>>>(S, P, W, qIn, cIn, &P.counters[CNT_WORK_TAIL], d->dStats);
             else if (d->counting)
                 kTail<true, false><<<grid, kTailBlock, 0, cs>>>(S, P, W, qIn, cIn, &P.counters[CNT_WORK_TAIL], d->dStats);
@@ -376,16 +423,20 @@ int32_t runWave(pe_device* d, int lane, Paths& P, int nSegs, int nSlots, int nPi
             kIntersect<false><<<d->blocksIntersect, 128, 0, cs>>>(S, P, qIn, cIn, d->dStats);
         if (P.guiding == 2 && (rc = guideQueries(d, cs, P, W, qIn, cIn))) return rc;
         if (tm.timing) PE_CUDA(cudaEventRecord(e1, cs));
-        if (P.aovA || P.pass)
+        if (lean)
+            stats.kernel_launches += launchLeanShade(d, S, P, W, qOut, cOut, cs, P.aovA || P.pass);
+        else if (P.aovA || P.pass)
             kShade<true><<<d->blocksShade, 128, 0, cs>>>(S, P, W, qOut, cOut);
         else
             kShade<false><<<d->blocksShade, 128, 0, cs>>>(S, P, W, qOut, cOut);
         if (tm.timing) PE_CUDA(cudaEventRecord(e2, cs));
         if (d->counting)
             kShadow<true><<<d->blocksShadow, 128, 0, cs>>>(S, P, &P.counters[CNT_SHADOW], d->dStats);
+        else if (anyHitShadows)
+            kShadow<false, true><<<d->blocksShadowAny, 128, 0, cs>>>(S, P, &P.counters[CNT_SHADOW], d->dStats);
         else
             kShadow<false><<<d->blocksShadow, 128, 0, cs>>>(S, P, &P.counters[CNT_SHADOW], d->dStats);
-        stats.kernel_launches += 3;
+        stats.kernel_launches += lean ? 2 : 3;
         ++stats.intersect_launches;
         if (tm.timing) {
             PE_CUDA(cudaEventRecord(e3, cs));
@@ -418,6 +469,7 @@ int32_t runWave(pe_device* d, int lane, Paths& P, int nSegs, int nSlots, int nPi
         PE_CUDA(cudaMemsetAsync(cIn, 0, sizeof(uint32_t), cs));
         PE_CUDA(cudaMemsetAsync(&P.counters[CNT_SHADOW], 0, (CNT_KEYS + kShadeKeys - CNT_SHADOW) * sizeof(uint32_t),
                                 cs));
+        if (lean) PE_CUDA(cudaMemsetAsync(&P.counters[CNT_WORK_KEYS], 0, kShadeKeys * sizeof(uint32_t), cs));
         std::swap(qIn, qOut);
         std::swap(cIn, cOut);
     }
@@ -820,6 +872,9 @@ int32_t renderAdaptive(pe_device* d, const pe_camera* cam, const pe_settings* st
     return PE_OK;
 }
 
+// WIDE: the traversal the render kernels use (4-wide tree); else the binary tree in the
+// reference's visiting order.
+template <bool WIDE>
 __global__ void kTracePrimary(SceneGPU S, WaveSeg A, int nPix, int32_t* outShape, int32_t* outPrim, float* outT) {
     for (int pix = blockIdx.x * blockDim.x + threadIdx.x; pix < nPix; pix += gridDim.x * blockDim.x) {
         const int x = pix % A.width, y = pix / A.width;
@@ -830,7 +885,8 @@ __global__ void kTracePrimary(SceneGPU S, WaveSeg A, int nPix, int32_t* outShape
         V3 o, d;
         cameraRay(S.tables, A.filterCdf, A.cam, A.filterWidth, x, y, A.width, A.height, sb, o, d);
         uint32_t a = 0, b = 0;
-        const Hit h = traceClosest<false>(S, o, d, VIS_CAMERA, 0.0f, 1e30f, a, b);
+        const Hit h = WIDE ? traceClosestWide<false>(S, o, d, VIS_CAMERA, 0.0f, 1e30f, a, b)
+                           : traceClosest<false>(S, o, d, VIS_CAMERA, 0.0f, 1e30f, a, b);
         if (h.prim < 0) {
             outShape[pix] = -1;
             outPrim[pix] = -1;
@@ -913,7 +969,8 @@ int32_t uploadScene(pe_device* d, const pe_scene* s, SceneGPU& G, std::vector<De
     G = SceneGPU{};
     const HostBuild& B = s->build;
     int32_t rc = 0;
-    if ((rc = upload(d, bufs, G.nodes, B.nodes)) || (rc = upload(d, bufs, G.tris, B.tris)) ||
+    if ((rc = upload(d, bufs, G.nodes, B.nodes)) || (rc = upload(d, bufs, G.wide, B.wide)) ||
+        (rc = upload(d, bufs, G.tris, B.tris)) ||
         (rc = upload(d, bufs, G.triVerts, B.triVerts)) || (rc = upload(d, bufs, G.pos, B.pos)) ||
         (rc = upload(d, bufs, G.nrm, B.nrm)) || (rc = upload(d, bufs, G.uv, B.uv)) ||
         (rc = upload(d, bufs, G.shapes, B.shapes)) || (rc = upload(d, bufs, G.materials, B.materials)) ||
@@ -1012,6 +1069,9 @@ int32_t uploadScene(pe_device* d, const pe_scene* s, SceneGPU& G, std::vector<De
         if ((rc = upload(d, bufs, G.textures, tex))) return rc;
     }
     G.nTextures = static_cast<int32_t>(s->textures.size());
+    G.leanShading = leanShadingOf(G, B.materials);
+    G.materialTypes = 0;
+    for (const MatGPU& m : B.materials) G.materialTypes |= 1 << m.type;
     G.nLightGroups = static_cast<int32_t>(B.groupNames.size());
     G.envGroup = B.envGroup;
     if (!B.lightGroup.empty() && (rc = upload(d, bufs, G.lightGroup, B.lightGroup))) return rc;
@@ -1094,6 +1154,20 @@ pe_device* pe_device_create(int32_t ordinal, char* err, size_t errLen) {
     d->blocksShadow = sm * std::max(1, b);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kTail<true, false>, kTailBlock, 0);
     d->blocksTail = sm * std::max(1, b);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kTail<false, false, true>, kTailBlock, 0);
+    d->blocksTailLean = sm * std::max(1, b);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kShadow<false, true>, 128, 0);
+    d->blocksShadowAny = sm * std::max(1, b);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kShadeKey<false, 0>, 128, 0);
+    d->blocksShadeKey[0] = sm * std::max(1, b);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kShadeKey<false, 1>, 128, 0);
+    d->blocksShadeKey[1] = sm * std::max(1, b);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kShadeKey<false, 2>, 128, 0);
+    d->blocksShadeKey[2] = sm * std::max(1, b);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kShadeKey<false, 3>, 128, 0);
+    d->blocksShadeKey[3] = sm * std::max(1, b);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kShadeKey<false, 4>, 128, 0);
+    d->blocksShadeKey[4] = sm * std::max(1, b);
     const cudaError_t le = cudaGetLastError();
     if (le != cudaSuccess) {
         pe_device_destroy(d);
@@ -1251,6 +1325,7 @@ int32_t pe_device_update_materials(pe_device* d, const pe_scene* s) {
     PE_CUDA(cudaMemcpyAsync(const_cast<MatGPU*>(d->scene.materials), s->build.materials.data(),
                             s->build.materials.size() * sizeof(MatGPU), cudaMemcpyHostToDevice, d->stream));
     PE_CUDA(cudaStreamSynchronize(d->stream));
+    d->scene.leanShading = leanShadingOf(d->scene, s->build.materials);
     ++d->sceneSerial;
     return PE_OK;
 }
@@ -1464,6 +1539,59 @@ int32_t pe_device_render_passes(pe_device* d, const pe_camera* cam, const pe_set
     return renderTargets(d, cam, st, first, count, cancel, sumRgb, sampleCount, sumLumSq, aovs, passes, traced);
 }
 
+// One batch into the device film (cleared first), read back through pinned staging and added to
+// the caller's host film over the tile's pixels on all host cores, as Film::addBatch does per pixel.
+static int32_t renderHostFilm(pe_device* d, const pe_camera* cam, const pe_settings* st, int32_t first, int32_t count,
+                              const volatile int32_t* cancel, float* sumRgb, uint32_t* sampleCount, float* sumLumSq,
+                              uint64_t* traced, Tile tile) {
+    int32_t rc;
+    if ((rc = pe_device_film_clear(d))) return rc;
+    if ((rc = ensureCapacity(d, kWaveSlots))) return rc;
+    const int32_t rr = renderWaves(d, cam, st, first, count, cancel, d->fSum, d->fCnt, d->fSq, nullptr, d->capacity,
+                                   true, tile);
+    if (rr != PE_OK && rr != PE_ERR_CANCELLED) return rr;
+    const size_t n = static_cast<size_t>(st->width) * static_cast<size_t>(st->height);
+    const size_t bytes = n * 5 * sizeof(float);
+    if (d->stageBytes < bytes) {
+        if (d->stage) cudaFreeHost(d->stage);
+        d->stage = nullptr;
+        d->stageBytes = 0;
+        PE_CUDA(cudaMallocHost(&d->stage, bytes));
+        d->stageBytes = bytes;
+    }
+    float* s = reinterpret_cast<float*>(d->stage);
+    uint32_t* c = reinterpret_cast<uint32_t*>(s + 3 * n);
+    float* q = s + 4 * n;
+    if ((rc = pe_device_film_read(d, s, c, q))) return rc;
+    const unsigned hw = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+    const size_t rows = static_cast<size_t>(tile.h), W = static_cast<size_t>(st->width);
+    const size_t chunk = (rows + hw - 1) / hw;
+    std::vector<uint64_t> partial(hw, 0);
+    auto merge = [&](unsigned t) {
+        uint64_t tr = 0;
+        for (size_t r = t * chunk; r < std::min(rows, (t + 1) * chunk); ++r) {
+            const size_t b = (static_cast<size_t>(tile.y0) + r) * W + static_cast<size_t>(tile.x0);
+            const size_t e = b + static_cast<size_t>(tile.w);
+            for (size_t i = b; i < e; ++i) tr += c[i];
+            if (sampleCount)
+                for (size_t i = b; i < e; ++i) sampleCount[i] += c[i];
+            if (sumRgb)
+                for (size_t i = 3 * b; i < 3 * e; ++i) sumRgb[i] += s[i];
+            if (sumLumSq)
+                for (size_t i = b; i < e; ++i) sumLumSq[i] += q[i];
+        }
+        partial[t] = tr;
+    };
+    std::vector<std::thread> pool;
+    for (unsigned t = 1; t < hw; ++t) pool.emplace_back(merge, t);
+    merge(0);
+    for (auto& th : pool) th.join();
+    uint64_t tr = 0;
+    for (uint64_t p : partial) tr += p;
+    if (traced) *traced = tr;
+    return rr;
+}
+
 int32_t pe_device_render(pe_device* d, const pe_camera* cam, const pe_settings* st, int32_t first, int32_t count,
                          const volatile int32_t* cancel, float* sumRgb, uint32_t* sampleCount, float* sumLumSq,
                          uint64_t* traced) {
@@ -1497,49 +1625,35 @@ int32_t pe_device_render(pe_device* d, const pe_camera* cam, const pe_settings* 
         if ((rc = pe_device_film_read(d, sumRgb, sampleCount, sumLumSq))) return rc;
         return ar;
     }
-    if ((rc = pe_device_film_clear(d))) return rc;
-    if ((rc = ensureCapacity(d, kWaveSlots))) return rc;
-    const int32_t rr = renderWaves(d, cam, st, first, count, cancel, d->fSum, d->fCnt, d->fSq, nullptr, d->capacity,
-                                   true, Tile{0, 0, st->width, st->height});
-    if (rr != PE_OK && rr != PE_ERR_CANCELLED) return rr;
-    const size_t n = static_cast<size_t>(st->width) * static_cast<size_t>(st->height);
-    // batch film → pinned staging (one DMA per array), then merged into the caller's film on all
-    // host cores, as Film::addBatch does per pixel
-    const size_t bytes = n * 5 * sizeof(float);
-    if (d->stageBytes < bytes) {
-        if (d->stage) cudaFreeHost(d->stage);
-        d->stage = nullptr;
-        d->stageBytes = 0;
-        PE_CUDA(cudaMallocHost(&d->stage, bytes));
-        d->stageBytes = bytes;
+    return renderHostFilm(d, cam, st, first, count, cancel, sumRgb, sampleCount, sumLumSq, traced,
+                          Tile{0, 0, st->width, st->height});
+}
+
+int32_t pe_device_render_region(pe_device* d, const pe_camera* cam, const pe_settings* st, int32_t x0, int32_t y0,
+                                int32_t w, int32_t h, int32_t first, int32_t count, const volatile int32_t* cancel,
+                                float* sumRgb, uint32_t* sampleCount, float* sumLumSq, uint64_t* traced) {
+    if (!d) {
+        setError("null device");
+        return PE_ERR_INVALID;
     }
-    float* s = reinterpret_cast<float*>(d->stage);
-    uint32_t* c = reinterpret_cast<uint32_t*>(s + 3 * n);
-    float* q = s + 4 * n;
-    if ((rc = pe_device_film_read(d, s, c, q))) return rc;
-    const unsigned hw = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
-    const size_t chunk = (n + hw - 1) / hw;
-    std::vector<uint64_t> partial(hw, 0);
-    auto merge = [&](unsigned t) {
-        const size_t b = t * chunk, e = std::min(n, b + chunk);
-        uint64_t tr = 0;
-        for (size_t i = b; i < e; ++i) tr += c[i];
-        if (sampleCount)
-            for (size_t i = b; i < e; ++i) sampleCount[i] += c[i];
-        if (sumRgb)
-            for (size_t i = 3 * b; i < 3 * e; ++i) sumRgb[i] += s[i];
-        if (sumLumSq)
-            for (size_t i = b; i < e; ++i) sumLumSq[i] += q[i];
-        partial[t] = tr;
-    };
-    std::vector<std::thread> pool;
-    for (unsigned t = 1; t < hw; ++t) pool.emplace_back(merge, t);
-    merge(0);
-    for (auto& th : pool) th.join();
-    uint64_t tr = 0;
-    for (uint64_t p : partial) tr += p;
-    if (traced) *traced = tr;
-    return rr;
+    if (!d->hasScene) {
+        setError("render before set_scene");
+        return PE_ERR_NO_SCENE;
+    }
+    int32_t rc = checkSettings(cam, st);
+    if (rc) return rc;
+    if (x0 < 0 || y0 < 0 || w <= 0 || h <= 0 || x0 + w > st->width || y0 + h > st->height) {
+        setError("pe_device_render_region: region outside the film");
+        return PE_ERR_INVALID;
+    }
+    if (st->adaptive_sampling) {
+        setError("pe_device_render_region: adaptive sampling renders whole films (pe_device_render)");
+        return PE_ERR_INVALID;
+    }
+    if (count <= 0) return PE_OK;
+    PE_CUDA(cudaSetDevice(d->ordinal));
+    if ((rc = ensureFilm(d, st->width, st->height))) return rc;
+    return renderHostFilm(d, cam, st, first, count, cancel, sumRgb, sampleCount, sumLumSq, traced, Tile{x0, y0, w, h});
 }
 
 // A caller's film buffer must be memory of this device that holds `bytes` from `p` on: a host
@@ -1752,8 +1866,21 @@ int32_t pe_device_timer_end(pe_device* d, float* ms) {
     return PE_OK;
 }
 
+static int32_t tracePrimary(pe_device* d, const pe_camera* cam, const pe_settings* st, int32_t sampleIndex,
+                            int32_t* outShape, int32_t* outPrim, float* outT, bool wide);
+
 int32_t pe_device_trace_primary(pe_device* d, const pe_camera* cam, const pe_settings* st, int32_t sampleIndex,
                                 int32_t* outShape, int32_t* outPrim, float* outT) {
+    return tracePrimary(d, cam, st, sampleIndex, outShape, outPrim, outT, true);
+}
+
+int32_t pe_device_trace_primary_ordered(pe_device* d, const pe_camera* cam, const pe_settings* st, int32_t sampleIndex,
+                                        int32_t* outShape, int32_t* outPrim, float* outT) {
+    return tracePrimary(d, cam, st, sampleIndex, outShape, outPrim, outT, false);
+}
+
+static int32_t tracePrimary(pe_device* d, const pe_camera* cam, const pe_settings* st, int32_t sampleIndex,
+                            int32_t* outShape, int32_t* outPrim, float* outT, bool wide) {
     if (!d || !outShape || !outPrim || !outT) {
         setError("null argument");
         return PE_ERR_INVALID;
@@ -1781,7 +1908,10 @@ int32_t pe_device_trace_primary(pe_device* d, const pe_camera* cam, const pe_set
         freeList(tmp);
         return rc;
     }
-    kTracePrimary<<<d->prop.multiProcessorCount * 8, 128, 0, d->stream>>>(d->scene, A, n, dS, dP, dT);
+    if (wide)
+        kTracePrimary<true><<<d->prop.multiProcessorCount * 8, 128, 0, d->stream>>>(d->scene, A, n, dS, dP, dT);
+    else
+        kTracePrimary<false><<<d->prop.multiProcessorCount * 8, 128, 0, d->stream>>>(d->scene, A, n, dS, dP, dT);
     cudaMemcpyAsync(outShape, dS, n * sizeof(int32_t), cudaMemcpyDeviceToHost, d->stream);
     cudaMemcpyAsync(outPrim, dP, n * sizeof(int32_t), cudaMemcpyDeviceToHost, d->stream);
     cudaMemcpyAsync(outT, dT, n * sizeof(float), cudaMemcpyDeviceToHost, d->stream);

@@ -203,6 +203,8 @@ struct pe_device {
     bool counting = false;
     pe_render_stats stats{};
     int blocksIntersect = 0, blocksShade = 0, blocksShadow = 0, blocksGen = 0, blocksTail = 0;
+    int blocksShadeKey[5] = {0, 0, 0, 0, 0}; // lean shading kernel of each key (miss, 4 material types)
+    int blocksShadowAny = 0, blocksTailLean = 0;
     int64_t tailPaths = -1; // -1: one resident grid of the tail kernel; 0: no tail kernel
     unsigned char* noAllocBase = nullptr; // device address of g_noAllocScratch on this device
     void* stage = nullptr;                 // pinned staging of the batch film (host-film render)

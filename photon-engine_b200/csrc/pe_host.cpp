@@ -228,6 +228,66 @@ inline float4 f4(float x, float y, float z, float w) {
     return r;
 }
 
+// 4-wide collapse of the flattened binary BVH for the traversal kernels.  A wide node holds the
+// children left after repeatedly replacing its largest-area interior child by that child's two
+// children (at most four; leaves are never opened), in the binary tree's left-to-right order, so
+// every box and leaf is one of the binary tree's.  Layout per node, 8 float4 (128 bytes, one L2
+// line): lo.x, hi.x, lo.y, hi.y, lo.z, hi.z of the four children (SoA, one child per lane),
+// then the child references (interior: wide node index; leaf: ~(first << 8 | count-1)), then
+// the child count.  Nodes are written depth-first, a node before its children.
+static int collapseWide(const std::vector<RefNode>& ref, std::vector<float4>& out, int& maxDepth, int node = 0,
+                        int depth = 1) {
+    maxDepth = std::max(maxDepth, depth);
+    int kids[4] = {node + 1, ref[static_cast<size_t>(node)].offset, -1, -1};
+    int n = 2;
+    while (n < 4) {
+        int best = -1;
+        float bestArea = -1.0f;
+        for (int k = 0; k < n; ++k) {
+            const RefNode& c = ref[static_cast<size_t>(kids[k])];
+            if (c.count == 0 && c.bounds.surfaceArea() > bestArea) {
+                best = k;
+                bestArea = c.bounds.surfaceArea();
+            }
+        }
+        if (best < 0) break;
+        const int c = kids[best];
+        for (int k = n; k > best + 1; --k) kids[k] = kids[k - 1];
+        kids[best] = c + 1;
+        kids[best + 1] = ref[static_cast<size_t>(c)].offset;
+        ++n;
+    }
+    const size_t me = out.size() / 8;
+    out.resize(out.size() + 8, float4{0.0f, 0.0f, 0.0f, 0.0f});
+    float lo[3][4], hi[3][4];
+    int32_t child[4] = {0, 0, 0, 0};
+    for (int k = 0; k < 4; ++k) {
+        for (int a = 0; a < 3; ++a) {
+            lo[a][k] = 0.0f;
+            hi[a][k] = 0.0f;
+        }
+    }
+    for (int k = 0; k < n; ++k) {
+        const RefNode& c = ref[static_cast<size_t>(kids[k])];
+        lo[0][k] = c.bounds.lo.x;
+        lo[1][k] = c.bounds.lo.y;
+        lo[2][k] = c.bounds.lo.z;
+        hi[0][k] = c.bounds.hi.x;
+        hi[1][k] = c.bounds.hi.y;
+        hi[2][k] = c.bounds.hi.z;
+        child[k] = c.count > 0 ? ~((c.offset << 8) | (c.count - 1)) : collapseWide(ref, out, maxDepth, kids[k], depth + 1);
+    }
+    float4* w = out.data() + me * 8;
+    for (int a = 0; a < 3; ++a) {
+        w[2 * a] = f4(lo[a][0], lo[a][1], lo[a][2], lo[a][3]);
+        w[2 * a + 1] = f4(hi[a][0], hi[a][1], hi[a][2], hi[a][3]);
+    }
+    w[6] = f4(bitsf(static_cast<uint32_t>(child[0])), bitsf(static_cast<uint32_t>(child[1])),
+              bitsf(static_cast<uint32_t>(child[2])), bitsf(static_cast<uint32_t>(child[3])));
+    w[7] = f4(bitsf(static_cast<uint32_t>(n)), 0.0f, 0.0f, 0.0f);
+    return static_cast<int>(me);
+}
+
 // ---------------------------------------------------------------------------------------------
 // light BVH (light_sampler.cpp:24-148, light_bounds.cpp:73-109)
 struct LBounds {
@@ -1072,6 +1132,17 @@ static int32_t buildScene(pe_scene* s) {
             B.nodes[k + 2] = f4(b0.lo.z, b0.hi.z, b1.lo.z, b1.hi.z);
             B.nodes[k + 3] = f4(bitsf(static_cast<uint32_t>(childRef(c0))), bitsf(static_cast<uint32_t>(childRef(c1))), 0.0f, 0.0f);
         }
+        // 4-wide nodes for the traversal kernels (the same leaves, boxes and leaf order)
+        if (ref[0].count == 0) {
+            int depth4 = 0;
+            collapseWide(ref, B.wide, depth4);
+            B.wideDepth = depth4;
+            if (3 * depth4 + 1 > kWideStack) {
+                setError("4-wide BVH depth " + std::to_string(depth4) + " exceeds the traversal stack of " +
+                         std::to_string(kWideStack));
+                return PE_ERR_LIMIT;
+            }
+        }
         B.rootIsLeaf = ref[0].count > 0 ? 1 : 0;
         B.rootFirst = ref[0].count > 0 ? ref[0].offset : 0;
         B.rootCount = ref[0].count;
@@ -1146,6 +1217,8 @@ static int32_t buildScene(pe_scene* s) {
     ++s->version;
     return PE_OK;
 }
+
+
 
 const char* lastErrorCStr() { return tlsError.c_str(); }
 

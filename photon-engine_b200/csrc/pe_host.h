@@ -44,6 +44,8 @@ struct HostEnv {
 // Everything the device uploads, as flat host arrays.
 struct HostBuild {
     std::vector<float4> nodes;       // 4 per interior node
+    std::vector<float4> wide;        // 8 per 4-wide node (traversal kernels)
+    int wideDepth = 0;
     std::vector<float4> tris;        // 3 per leaf-ordered triangle
     std::vector<int4> triVerts;      // per global triangle
     std::vector<float4> pos, nrm;    // per vertex (global)

@@ -231,7 +231,7 @@ __global__ void __launch_bounds__(128) kIntersect(SceneGPU S, Paths P, const int
             slot = queue[i];
             const float4 ro = P.rayO[slot];
             const float4 rd = P.rayD[slot];
-            const Hit h = traceClosest<COUNT>(S, mk(ro.x, ro.y, ro.z), mk(rd.x, rd.y, rd.z), __float_as_uint(ro.w), 0.0f,
+            const Hit h = traceClosestWide<COUNT>(S, mk(ro.x, ro.y, ro.z), mk(rd.x, rd.y, rd.z), __float_as_uint(ro.w), 0.0f,
                                               1e30f, nodes, tris);
             P.hit[slot] = make_float4(h.t, h.u, h.v, __int_as_float(h.prim));
             key = (__float_as_uint(ro.w) & RAY_WALK) ? kShadeKeys - 1
@@ -300,12 +300,12 @@ template <bool COUNT>
 __device__ V3 shadowVisibility(const SceneGPU& S, V3 o, V3 d, float tMax, int light, uint32_t& nodes, uint32_t& tris) {
     const bool link = shadowLinkFor(S, light);
     if (!S.hasShadowTransmitters && !link)
-        return traceAny<COUNT>(S, o, d, VIS_SHADOW, 0.0f, tMax, nodes, tris) ? mk(0.0f) : mk(1.0f);
+        return traceAnyWide<COUNT>(S, o, d, VIS_SHADOW, 0.0f, tMax, nodes, tris) ? mk(0.0f) : mk(1.0f);
     V3 T = mk(1.0f);
     V3 origin = o;
     float remaining = tMax;
     for (int i = 0; i < 64; ++i) {
-        const Hit h = traceClosest<COUNT>(S, origin, d, VIS_SHADOW, 0.0f, remaining, nodes, tris);
+        const Hit h = traceClosestWide<COUNT>(S, origin, d, VIS_SHADOW, 0.0f, remaining, nodes, tris);
         if (h.prim < 0) return T;
         Isect is;
         fillHit(S, h, d, is);
@@ -339,7 +339,9 @@ __device__ __forceinline__ V3 neeTerm(V3 fLi, V3 vis, float scalar, V3 thr, bool
 }
 
 // ---- any hit over the shadow queue ------------------------------------------------------------
-template <bool COUNT>
+// ANY: the scene has neither shadow-transmitting surfaces nor shadow links, so visibility is
+// the plain any-hit query (and the transmittance walk is compiled out).
+template <bool COUNT, bool ANY = false>
 __global__ void __launch_bounds__(128) kShadow(SceneGPU S, Paths P, const uint32_t* count, unsigned long long* stats) {
     const int n = static_cast<int>(*count);
     uint32_t nodes = 0, tris = 0;
@@ -352,7 +354,9 @@ __global__ void __launch_bounds__(128) kShadow(SceneGPU S, Paths P, const uint32
         const float4 so = P.shO[i];
         const float4 sd = P.shD[i];
         const int light = static_cast<int>(__float_as_uint(P.shC[i].w) >> 1) - 1;
-        const V3 vis = shadowVisibility<COUNT>(S, mk(so.x, so.y, so.z), mk(sd.x, sd.y, sd.z), so.w, light, nodes, tris);
+        const V3 vis = ANY ? (traceAnyWide<COUNT>(S, mk(so.x, so.y, so.z), mk(sd.x, sd.y, sd.z), VIS_SHADOW, 0.0f, so.w, nodes,
+                                              tris) ? mk(0.0f) : mk(1.0f))
+                           : shadowVisibility<COUNT>(S, mk(so.x, so.y, so.z), mk(sd.x, sd.y, sd.z), so.w, light, nodes, tris);
         if (isBlack(vis)) continue;
         const float4 sc = P.shC[i];
         const float4 st = P.shT[i];
@@ -543,7 +547,7 @@ __device__ __noinline__ float approxAo(const SceneGPU& S, const Isect& is, Sobol
     for (int i = 0; i < samples; ++i) {
         const V3 local = sampleCosineHemisphere(get2D(T, sb));
         const V3 dir = normalize(toWorld(frame, local));
-        if (traceAny<false>(S, spawnOrigin(is, dir), dir, VIS_SHADOW, 0.0f, 0.35f, n0, n1)) occ += 1.0f;
+        if (traceAnyWide<false>(S, spawnOrigin(is, dir), dir, VIS_SHADOW, 0.0f, 0.35f, n0, n1)) occ += 1.0f;
     }
     const float visibility = 1.0f - (occ / static_cast<float>(samples));
     return lerpf(1.0f, visibility, strength);
@@ -575,7 +579,7 @@ __device__ __noinline__ V3 roundedEdgeNormal(const SceneGPU& S, const Isect& is,
             const float sign = k == 0 ? 1.0f : -1.0f;
             const V3 origin = is.point + s * d.x + t * d.y + axis * (sign * radius);
             const V3 rdir = axis * -sign;
-            const Hit h = traceClosest<false>(S, origin, rdir, VIS_ALL, 0.0f, 2.0f * radius, n0, n1);
+            const Hit h = traceClosestWide<false>(S, origin, rdir, VIS_ALL, 0.0f, 2.0f * radius, n0, n1);
             if (h.prim < 0) continue;
             Isect hit;
             fillHit(S, h, rdir, hit);
@@ -643,11 +647,18 @@ __device__ __noinline__ V3 shadowCatcher(const SceneGPU& S, const Isect& is, V3 
 // vertex, or a ray scattered inside a medium (an ordinary ray with specularBounce set).  NEE
 // shadow rays go to the any-hit queue, or with INLINE_SHADOW are traced here and their terms
 // added to L at once, in the same order.  Returns whether the path goes on.
-template <bool INLINE_SHADOW, bool COUNT, bool OUT>
+//
+// KEY selects a specialised instantiation: -1 the full shader; otherwise a lean one for waves
+// whose scene has SceneGPU::leanShading and that neither guide nor record, with every feature
+// those waves cannot reach compiled out (so the code fits in registers); KEY >= 0 also fixes the
+// shading key (0 a miss, 1 + material type a surface hit), -2 leaves it to the hit.
+template <bool INLINE_SHADOW, bool COUNT, bool OUT, int KEY = -1>
 __device__ __forceinline__ bool shadeSlot(const SceneGPU& S, const Paths& P, const WaveSeg& A, int slot, int path,
                                           uint32_t& shNodes, uint32_t& shTris, uint32_t& shRays) {
+    constexpr bool LEAN = KEY != -1;
+    constexpr int MT = KEY >= 1 ? KEY - 1 : -1; // the material type a surface key fixes
     const TablesGPU* T = S.tables;
-    const bool volumetric = (S.hasVolumes | S.hasSubsurface) != 0;
+    const bool volumetric = !LEAN && (S.hasVolumes | S.hasSubsurface) != 0;
     bool cont = false;
     float4 ro = P.rayO[slot];
     float4 rd = P.rayD[slot];
@@ -666,7 +677,7 @@ __device__ __forceinline__ bool shadeSlot(const SceneGPU& S, const Paths& P, con
     uint32_t volCtr = __float_as_uint(md.z);
     float lambda = th.w; // 0 = RGB path; > 0 = single-wavelength path after a dispersive hit
     uint32_t flags = __float_as_uint(ln.w);
-    if (flags & PF_GUIDE_SNAP) {
+    if (!LEAN && (flags & PF_GUIDE_SNAP)) {
         // radiance so far, the previous vertex's NEE included: the training record's baseline
         if (P.sdMode & SD_RECORD) {
             const uint32_t n = P.sdCount[slot];
@@ -696,16 +707,16 @@ __device__ __forceinline__ bool shadeSlot(const SceneGPU& S, const Paths& P, con
     const int shadowSamples = A.shadowSamples;
     const int explicitLights = S.nLights;
     const int prim = __float_as_int(hr.w);
-    const bool hit = prim >= 0;
+    const bool hit = KEY == 0 ? false : (KEY > 0 ? true : prim >= 0);
     // ray cone (path_tracer.cpp:428-454, 777-783, 853-857): only scenes with mipmapped textures
-    const bool cones = S.hasMips && P.cone;
+    const bool cones = !LEAN && S.hasMips && P.cone;
     float2 cone = cones ? P.cone[slot] : make_float2(0.0f, 0.0f);
     Isect is;
     bool done = false;
     bool vertex = false; // a surface vertex to shade (NEE + BSDF sampling) below
     bool exitVertex = false; // ... the exit vertex of a subsurface walk
     V3 wo = -dir;
-    if (flags & PF_WALK) {
+    if (!LEAN && (flags & PF_WALK)) {
         // one step of the random walk (path_tracer.cpp:263-303)
         const V3 sigT = mk(lp.x, lp.y, lp.z), alb = mk(ln.x, ln.y, ln.z);
         const V3 sigS = alb * sigT;
@@ -758,7 +769,7 @@ __device__ __forceinline__ bool shadeSlot(const SceneGPU& S, const Paths& P, con
             // Camera-invisible light quads (for camera rays) and cutouts are passed through;
             // the vertex does not count (path_tracer.cpp:426-439).
             if (skips < 64 && ((cameraRay && (S.shapes[is.shape].flags & SF_CAMERA_INVISIBLE)) ||
-                               passesCutout(S, S.materials[is.material], is, sb))) {
+                               (!LEAN && passesCutout(S, S.materials[is.material], is, sb)))) {
                 const V3 no = offsetRayOrigin(is.point, is.pError, is.ng, dir);
                 ro = make_float4(no.x, no.y, no.z, ro.w);
                 if (cones) cone.x = cone.x + cone.y * smax(0.0f, is.t);
@@ -857,7 +868,7 @@ __device__ __forceinline__ bool shadeSlot(const SceneGPU& S, const Paths& P, con
                     }
                 }
                 done = true;
-            } else if (cameraRay && is.shape == S.catcherShape) {
+            } else if (!LEAN && cameraRay && is.shape == S.catcherShape) {
                 // the shadow catcher ends the camera path with the shadowed background
                 float ratio = 1.0f;
                 const V3 bg = shadowCatcher(S, is, dir, shadowSamples, sb, ratio);
@@ -883,7 +894,7 @@ __device__ __forceinline__ bool shadeSlot(const SceneGPU& S, const Paths& P, con
                         li = (sh.flags & SF_AREA_TRIANGLE) ? sh.emitter : sh.emitter + (is.tri - static_cast<int>(sh.firstTri));
                     // Light linking: the previous receiver must be linked to this light
                     // (path_tracer.cpp:571-572; camera rays always see it)
-                    const bool linked = depth == 0 || li < 0 || !S.hasLightLinks ||
+                    const bool linked = depth == 0 || li < 0 || LEAN || !S.hasLightLinks ||
                                         linkAllows(S.links[li].mode, S.links[li].mask,
                                                    static_cast<int>((flags >> kPrevNodeShift) & 0xFFu));
                     float weight = 1.0f;
@@ -923,18 +934,18 @@ __device__ __forceinline__ bool shadeSlot(const SceneGPU& S, const Paths& P, con
     if (vertex) {
         const MatGPU& mat = S.materials[is.material];
         // dispersion: the first wavelength-dependent surface fixes one λ for the path
-        if (lambda == 0.0f && (mat.flags & MF_DISPERSIVE)) {
+        if (!LEAN && lambda == 0.0f && (mat.flags & MF_DISPERSIVE)) {
             V3 w;
             lambda = sampleWavelength(T, get1D(sb), w);
             thr *= w;
         }
         // rounded edges on the first three vertices (not a walk's exit vertex), then contact AO at
         // the camera hit (path_tracer.cpp:612-621)
-        if (depth <= 2 && mat.roundEdge > 0.0f && !exitVertex) {
+        if (!LEAN && depth <= 2 && mat.roundEdge > 0.0f && !exitVertex) {
             const V3 n = roundedEdgeNormal(S, is, mat.roundEdge, sb);
             if (dot(n, wo) > 0.02f) is.normal = n;
         }
-        if (A.aoStrength > 0.0f && depth == 0) thr *= approxAo(S, is, sb, A.aoStrength, shadowSamples);
+        if (!LEAN && A.aoStrength > 0.0f && depth == 0) thr *= approxAo(S, is, sb, A.aoStrength, shadowSamples);
         ShadePoint sp;
         sp.uv = is.uv;
         sp.textures = S.textures;
@@ -953,11 +964,11 @@ __device__ __forceinline__ bool shadeSlot(const SceneGPU& S, const Paths& P, con
         sp.wavelength = lambda;
         const bool isSpecular = (mat.flags & MF_DELTA) != 0;
         // this bounce's proposal, when the inference kernel left one for the slot
-        const bool useGuide = P.guiding == 2 && guidable(mat) && P.guideMark[slot] != 0u;
+        const bool useGuide = !LEAN && P.guiding == 2 && guidable(mat) && P.guideMark[slot] != 0u;
         if (useGuide) P.guideMark[slot] = 0u;
         // or the SD-tree's sampling quadtree of the vertex's spatial leaf (path_tracer.cpp:627-629)
         int sdRoot = -1;
-        if ((P.sdMode & SD_SAMPLE) && !useGuide && guidable(mat)) {
+        if (!LEAN && (P.sdMode & SD_SAMPLE) && !useGuide && guidable(mat)) {
             const int leaf = sdLeafWithData(P.sd, is.point);
             if (leaf >= 0) sdRoot = P.sd.leaves[leaf].sampRoot;
         }
@@ -978,7 +989,7 @@ __device__ __forceinline__ bool shadeSlot(const SceneGPU& S, const Paths& P, con
                     continue;
                 }
                 const bool fromEnv = lightIndex >= explicitLights;
-                if (!fromEnv && S.hasLightLinks &&
+                if (!LEAN && !fromEnv && S.hasLightLinks &&
                     !linkAllows(S.links[lightIndex].mode, S.links[lightIndex].mask, S.shapes[is.shape].linkNode)) {
                     (void)get2D(T, sb);
                     continue;
@@ -992,7 +1003,7 @@ __device__ __forceinline__ bool shadeSlot(const SceneGPU& S, const Paths& P, con
                 float bsdfPdf = 0.0f;
                 LobeSplit3 split;
                 const bool firstShares = (OUT && P.pass) && depth == 0;
-                const V3 f = bsdfEvalPdf(T, mat, wo, ls.wi, sp, bsdfPdf, firstShares ? &split : nullptr);
+                const V3 f = bsdfEvalPdfT<MT>(T, mat, wo, ls.wi, sp, bsdfPdf, firstShares ? &split : nullptr);
                 const float cosTheta = fabsf(dot(ls.wi, is.normal));
                 if (isBlack(f) || !(cosTheta > 0.0f)) continue;
                 const float lightPdf = lightPmf * ls.pdf;
@@ -1056,11 +1067,11 @@ __device__ __forceinline__ bool shadeSlot(const SceneGPU& S, const Paths& P, con
         } else {
             const float uc = get1D(sb);
             const V2 u2 = get2D(T, sb);
-            sampled = bsdfSample(T, mat, wo, sp, uc, u2, bs);
+            sampled = bsdfSampleT<MT>(T, mat, wo, sp, uc, u2, bs);
         }
         if (!sampled) {
             done = true;
-        } else if (bs.subsurface) {
+        } else if (!LEAN && bs.subsurface) {
             // random-walk entry (path_tracer.cpp:745-761): the walk's coefficients ride
             // in the columns it does not need (lastP, lastN, pickP.x)
             V3 sigT, alb;
@@ -1108,7 +1119,7 @@ __device__ __forceinline__ bool shadeSlot(const SceneGPU& S, const Paths& P, con
                 } else {
                     LobeSplit3 split;
                     float unusedPdf = 0.0f;
-                    (void)bsdfEvalPdf(T, mat, wo, wi, sp, unusedPdf, &split);
+                    (void)bsdfEvalPdfT<MT>(T, mat, wo, wi, sp, unusedPdf, &split);
                     lobeShares(split, sh);
                 }
                 float4* b = passBlock(P, path);
@@ -1117,7 +1128,7 @@ __device__ __forceinline__ bool shadeSlot(const SceneGPU& S, const Paths& P, con
             const float cosTheta = fabsf(dot(wi, is.normal));
             const V3 thrBefore = thr;
             thr *= bs.f * (cosTheta / bs.pdf);
-            if (P.guiding && !bs.delta && slot % P.guideStride == 0 && guidable(mat) && isFinite3(thr) &&
+            if (!LEAN && P.guiding && !bs.delta && slot % P.guideStride == 0 && guidable(mat) && isFinite3(thr) &&
                 guideRecord(P, slot, is.point, is.normal, wo, wi, thrBefore))
                 flags |= PF_GUIDE_SNAP;
             if (!isFinite3(thr)) {
@@ -1131,7 +1142,7 @@ __device__ __forceinline__ bool shadeSlot(const SceneGPU& S, const Paths& P, con
                 flags = cameraRay ? (flags | PF_CAMERA_RAY) : (flags & ~PF_CAMERA_RAY);
                 // crossing a volume boundary: enter the object's medium from outside,
                 // leave it from inside
-                if (mat.flags & MF_VOLUME_BOUNDARY) {
+                if (!LEAN && (mat.flags & MF_VOLUME_BOUNDARY)) {
                     const float a = dot(wo, is.ng), b = dot(wi, is.ng);
                     if (a * b < 0.0f) {
                         if (a > 0.0f) media.enter(is.material);
@@ -1158,7 +1169,7 @@ __device__ __forceinline__ bool shadeSlot(const SceneGPU& S, const Paths& P, con
                 // SD-tree training vertex (path_tracer.cpp:823-827, recordable ones only): its
                 // incident radiance is what L gains from here on over the throughput after the
                 // bounce and the roulette
-                if (cont && (P.sdMode & SD_RECORD) && !bs.delta && !(mat.flags & MF_VOLUME_BOUNDARY)) {
+                if (!LEAN && cont && (P.sdMode & SD_RECORD) && !bs.delta && !(mat.flags & MF_VOLUME_BOUNDARY)) {
                     const uint32_t n = P.sdCount[slot];
                     if (n < static_cast<uint32_t>(kSdRecords)) {
                         float4* rec = P.sdRec + (static_cast<size_t>(slot) * kSdRecords + n) * 4;
@@ -1233,6 +1244,32 @@ __global__ void __launch_bounds__(128, 6) kShade(SceneGPU S, Paths P, Wave W, in
     }
 }
 
+// The lean shading kernel of one shading key: the rays of that key's bin only, shaded by the
+// shadeSlot instantiation that carries the code of that key alone (waves of lean-shading scenes
+// without guiding; one launch per key, each with the registers its key needs).
+template <bool OUT, int KEY>
+__global__ void __launch_bounds__(128) kShadeKey(SceneGPU S, Paths P, Wave W, int32_t* nextQueue, uint32_t* nextCount) {
+    const int n = static_cast<int>(P.counters[CNT_KEYS + KEY]);
+    const int32_t* bin = P.sortQ + static_cast<size_t>(KEY) * P.capacity;
+    const int lane = threadIdx.x & 31;
+    uint32_t unused0 = 0, unused1 = 0, unused2 = 0;
+    for (;;) {
+        const int base = warpFetch(&P.counters[CNT_WORK_KEYS + KEY]);
+        if (base >= n) break;
+        const int i = base + lane;
+        bool cont = false;
+        int slot = -1;
+        if (i < n) {
+            slot = bin[i];
+            const int path = pathOfSlot(P, slot);
+            const WaveSeg& A = W.segs[segOfSlot(W, path)];
+            cont = shadeSlot<false, false, OUT, KEY>(S, P, A, slot, path, unused0, unused1, unused2);
+        }
+        queuePush(nextQueue, nextCount, cont, slot);
+        if (P.pathOf) queuePush(P.freeQ, &P.counters[CNT_FREE], !cont && slot >= 0, slot);
+    }
+}
+
 // ---- tail: the last paths of a wave, each run to its end by one thread -------------------------
 // Once a wave's live queue fits in one resident grid, per-bounce launches cost more than they
 // save: each thread takes a path from the queue, alternates closest-hit queries with shadeSlot
@@ -1242,7 +1279,7 @@ __global__ void __launch_bounds__(128, 6) kShade(SceneGPU S, Paths P, Wave W, in
 // the next wave running on the other lane.
 constexpr int kTailBlock = 32;
 
-template <bool COUNT, bool OUT>
+template <bool COUNT, bool OUT, bool LEAN = false>
 __global__ void __launch_bounds__(kTailBlock) kTail(SceneGPU S, Paths P, Wave W, const int32_t* queue, const uint32_t* count,
                                              uint32_t* cursor, unsigned long long* stats) {
     const int n = static_cast<int>(*count);
@@ -1260,11 +1297,11 @@ __global__ void __launch_bounds__(kTailBlock) kTail(SceneGPU S, Paths P, Wave W,
             }
             const float4 ro = P.rayO[slot];
             const float4 rd = P.rayD[slot];
-            const Hit h = traceClosest<COUNT>(S, mk(ro.x, ro.y, ro.z), mk(rd.x, rd.y, rd.z), __float_as_uint(ro.w), 0.0f,
+            const Hit h = traceClosestWide<COUNT>(S, mk(ro.x, ro.y, ro.z), mk(rd.x, rd.y, rd.z), __float_as_uint(ro.w), 0.0f,
                                               1e30f, nodes, tris);
             ++rays;
             P.hit[slot] = make_float4(h.t, h.u, h.v, __int_as_float(h.prim));
-            if (!shadeSlot<true, COUNT, OUT>(S, P, A, slot, path, shNodes, shTris, shRays)) break;
+            if (!shadeSlot<true, COUNT, OUT, LEAN ? -2 : -1>(S, P, A, slot, path, shNodes, shTris, shRays)) break;
         }
     }
     if (COUNT) {

@@ -31,6 +31,7 @@ constexpr int kFilterBins = 512;     // pixel filter inverse CDF bins (pixel_fil
 constexpr int kMaxExhaustive = 33;   // LightSampler::kMaxExhaustive (light_sampler.h:31)
 constexpr int kMaxInfinite = 16;     // LightSampler::kMaxInfinite
 constexpr int kMaxStack = 64;        // traversal stack entries; builder rejects deeper trees
+constexpr int kWideStack = 96;       // 4-wide traversal stack entries (at most 3 per level + 1)
 
 enum ShapeFlags : uint32_t {
     SF_AREA_TRIANGLE = 1u,   // one of the two triangles of an AreaLight (a Triangle shape)
@@ -176,6 +177,7 @@ struct EnvGPU {
 struct SceneGPU {
     // geometry
     const float4* nodes;     // 4 float4 per interior node
+    const float4* wide;      // 8 float4 per 4-wide node (null when the root is a leaf)
     const float4* tris;      // 3 float4 per leaf-ordered triangle
     const int4* triVerts;    // per global triangle: i0, i1, i2, shape
     const float4* pos;       // per vertex
@@ -222,6 +224,11 @@ struct SceneGPU {
     const TexGPU* textures;  // image textures (null without any)
     int32_t nTextures;
     int32_t hasMips;         // some texture has mipmaps: paths carry ray cones for its LOD
+    // 1 when no material or scene setting needs the shading features a plain surface scene
+    // leaves unused (volumes, subsurface walks, dispersion, cutouts, rounded edges, ray cones,
+    // light or shadow links, a shadow catcher): its waves may shade with the lean kernels
+    int32_t leanShading;
+    int32_t materialTypes;   // bit t: some material has type t
 };
 
 // Scene::isLightLinked / isShadowLinked for light `li` (explicit) and a receiver or blocker node.

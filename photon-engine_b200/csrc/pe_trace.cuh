@@ -7,6 +7,8 @@
 // record produce the reference CPU path's floats bit for bit.
 #pragma once
 
+#include <limits>
+
 #include "pe_wave.h"
 
 #include "pe_math.h"
@@ -282,6 +284,171 @@ __device__ bool traceAny(const SceneGPU& S, V3 o, V3 d, uint32_t mask, float tMi
             } else {
                 if (sp == 0) return false;
                 cur = stackRef[--sp];
+            }
+        }
+        int first, count;
+        leafRange(cur, first, count);
+        for (int k = 0; k < count; ++k) {
+            const int pi = first + k;
+            const float4 a = __ldg(&S.tris[3 * pi + 0]);
+            const float4 b = __ldg(&S.tris[3 * pi + 1]);
+            if ((__float_as_uint(b.w) & mask) == 0u) continue;
+            const float4 c = __ldg(&S.tris[3 * pi + 2]);
+            if (COUNT) ++triTests;
+            float t, u, v;
+            if (triLean(a, b, c, o, d, tMin, tMax, t, u, v)) return true;
+        }
+        if (sp == 0) return false;
+        cur = stackRef[--sp];
+    }
+}
+
+// ---- 4-wide traversal ----------------------------------------------------------------------
+// The kernels traverse the 4-wide collapse of the binary tree (pe_host.cpp collapseWide): one
+// 128-byte node per step tests four child boxes with the same slab arithmetic, so a ray makes
+// about half the dependent node fetches of the binary walk.  Closest hit: children hit are
+// visited nearest entry first (ties by child order), the others pushed with their entry
+// distance and skipped on pop when farther than the current hit, as in the binary walk.  Every
+// triangle that can hold the closest hit is tested with the same arithmetic, so the hit
+// distance is the binary walk's; only when two triangles give the bit-identical distance (a ray
+// through a shared edge or vertex) may the other of them win, because the last one tested wins.
+constexpr float kInf = std::numeric_limits<float>::infinity();
+
+struct WideNode {
+    float4 lx, hx, ly, hy, lz, hz;
+    int4 child;
+    int count;
+};
+__device__ __forceinline__ WideNode loadWide(const float4* w, int i) {
+    WideNode n;
+    const float4* p = w + 8 * static_cast<size_t>(i);
+    n.lx = __ldg(p + 0);
+    n.hx = __ldg(p + 1);
+    n.ly = __ldg(p + 2);
+    n.hy = __ldg(p + 3);
+    n.lz = __ldg(p + 4);
+    n.hz = __ldg(p + 5);
+    const float4 c = __ldg(p + 6);
+    n.child = make_int4(__float_as_int(c.x), __float_as_int(c.y), __float_as_int(c.z), __float_as_int(c.w));
+    n.count = __float_as_int(__ldg(reinterpret_cast<const float*>(p + 7)));
+    return n;
+}
+// Entry distances of the four children (+inf where a child is absent or missed).
+__device__ __forceinline__ void wideSlabs(const WideNode& n, V3 o, V3 inv, float tMin, float tMax, float t[4]) {
+    float tn;
+    t[0] = slab(n.lx.x, n.hx.x, n.ly.x, n.hy.x, n.lz.x, n.hz.x, o, inv, tMin, tMax, tn) ? tn : kInf;
+    t[1] = slab(n.lx.y, n.hx.y, n.ly.y, n.hy.y, n.lz.y, n.hz.y, o, inv, tMin, tMax, tn) ? tn : kInf;
+    t[2] = n.count > 2 && slab(n.lx.z, n.hx.z, n.ly.z, n.hy.z, n.lz.z, n.hz.z, o, inv, tMin, tMax, tn) ? tn : kInf;
+    t[3] = n.count > 3 && slab(n.lx.w, n.hx.w, n.ly.w, n.hy.w, n.lz.w, n.hz.w, o, inv, tMin, tMax, tn) ? tn : kInf;
+}
+// Compare-exchange on (distance, child order): a total order, so equal distances keep child order.
+__device__ __forceinline__ void cmpx(float& ta, int& ra, int& ka, float& tb, int& rb, int& kb) {
+    if (ta > tb || (ta == tb && ka > kb)) {
+        const float t = ta; ta = tb; tb = t;
+        const int r = ra; ra = rb; rb = r;
+        const int k = ka; ka = kb; kb = k;
+    }
+}
+
+template <bool COUNT>
+__device__ Hit traceClosestWide(const SceneGPU& S, V3 o, V3 d, uint32_t mask, float tMin, float tMax,
+                                uint32_t& nodeVisits, uint32_t& triTests) {
+    Hit best;
+    best.prim = -1;
+    best.meta = 0;
+    best.t = tMax;
+    best.u = best.v = 0.0f;
+    const V3 inv = mk(1.0f / d.x, 1.0f / d.y, 1.0f / d.z);
+    float tn;
+    if (S.nTris == 0) return best;
+    if (!slab(S.rootMin[0], S.rootMax[0], S.rootMin[1], S.rootMax[1], S.rootMin[2], S.rootMax[2], o, inv, tMin, tMax, tn))
+        return best;
+    if (S.rootIsLeaf) {
+        testLeafClosest<COUNT>(S, S.rootFirst, S.rootCount, o, d, mask, tMin, tMax, best, triTests);
+        return best;
+    }
+    int stackRef[kWideStack];
+    float stackT[kWideStack];
+    int sp = 0;
+    int cur = 0;
+    for (;;) {
+        while (cur >= 0) {
+            if (COUNT) ++nodeVisits;
+            const WideNode n = loadWide(S.wide, cur);
+            float t[4];
+            wideSlabs(n, o, inv, tMin, tMax, t);
+            float t0 = t[0], t1 = t[1], t2 = t[2], t3 = t[3];
+            int r0 = n.child.x, r1 = n.child.y, r2 = n.child.z, r3 = n.child.w;
+            int k0 = 0, k1 = 1, k2 = 2, k3 = 3;
+            cmpx(t0, r0, k0, t1, r1, k1);
+            cmpx(t2, r2, k2, t3, r3, k3);
+            cmpx(t0, r0, k0, t2, r2, k2);
+            cmpx(t1, r1, k1, t3, r3, k3);
+            cmpx(t1, r1, k1, t2, r2, k2);
+            if (t0 == kInf) {
+                bool found = false;
+                while (sp > 0) {
+                    --sp;
+                    if (stackT[sp] <= tMax) {
+                        cur = stackRef[sp];
+                        found = true;
+                        break;
+                    }
+                }
+                if (!found) return best;
+                continue;
+            }
+            // farther children first onto the stack, so they pop nearest first
+            if (t3 != kInf) { stackRef[sp] = r3; stackT[sp] = t3; ++sp; }
+            if (t2 != kInf) { stackRef[sp] = r2; stackT[sp] = t2; ++sp; }
+            if (t1 != kInf) { stackRef[sp] = r1; stackT[sp] = t1; ++sp; }
+            cur = r0;
+        }
+        int first, count;
+        leafRange(cur, first, count);
+        testLeafClosest<COUNT>(S, first, count, o, d, mask, tMin, tMax, best, triTests);
+        bool found = false;
+        while (sp > 0) {
+            --sp;
+            if (stackT[sp] <= tMax) {
+                cur = stackRef[sp];
+                found = true;
+                break;
+            }
+        }
+        if (!found) return best;
+    }
+}
+
+// Any hit over the 4-wide tree: the answer does not depend on the visiting order.
+template <bool COUNT>
+__device__ bool traceAnyWide(const SceneGPU& S, V3 o, V3 d, uint32_t mask, float tMin, float tMax, uint32_t& nodeVisits,
+                             uint32_t& triTests) {
+    const V3 inv = mk(1.0f / d.x, 1.0f / d.y, 1.0f / d.z);
+    float tn;
+    if (S.nTris == 0) return false;
+    if (!slab(S.rootMin[0], S.rootMax[0], S.rootMin[1], S.rootMax[1], S.rootMin[2], S.rootMax[2], o, inv, tMin, tMax, tn))
+        return false;
+    int stackRef[kWideStack];
+    int sp = 0;
+    int cur = S.rootIsLeaf ? static_cast<int>(~((static_cast<uint32_t>(S.rootFirst) << 8) | static_cast<uint32_t>(S.rootCount - 1))) : 0;
+    for (;;) {
+        while (cur >= 0) {
+            if (COUNT) ++nodeVisits;
+            const WideNode n = loadWide(S.wide, cur);
+            float t[4];
+            wideSlabs(n, o, inv, tMin, tMax, t);
+            // the first child hit is next, the other hits wait on the stack
+            int next = -1;
+            if (t[0] != kInf) next = n.child.x;
+            if (t[1] != kInf) { if (next == -1) next = n.child.y; else stackRef[sp++] = n.child.y; }
+            if (t[2] != kInf) { if (next == -1) next = n.child.z; else stackRef[sp++] = n.child.z; }
+            if (t[3] != kInf) { if (next == -1) next = n.child.w; else stackRef[sp++] = n.child.w; }
+            if (next == -1) {
+                if (sp == 0) return false;
+                cur = stackRef[--sp];
+            } else {
+                cur = next;
             }
         }
         int first, count;

@@ -124,7 +124,8 @@ enum PassFilms { PFILM_DEPTH = 8, PFILM_POSITION = 9, PFILM_OBJECT = 10, PFILM_M
 constexpr int kShadeKeys = 6;
 enum CounterSlots { CNT_QA = 0, CNT_QB = 1, CNT_SHADOW = 2, CNT_WORK_ISECT = 3, CNT_WORK_SHADOW = 4,
                     CNT_WORK_SHADE = 5, CNT_KEYS = 6, CNT_ERRORS = 12, CNT_WORK_TAIL = 13, CNT_GUIDE_Q = 14,
-                    CNT_TRAIN = 15, CNT_FREE = 16, CNT_SWEEP = 17, CNT_TOTAL = 18 };
+                    CNT_TRAIN = 15, CNT_FREE = 16, CNT_SWEEP = 17, CNT_WORK_KEYS = 18,
+                    CNT_TOTAL = CNT_WORK_KEYS + kShadeKeys };
 // Paths per wave with regeneration, as a multiple of the slots.
 constexpr int kStreamFactor = 16;
 // Vertices an SD-tree training path records (the reference records up to 32; its paths in these

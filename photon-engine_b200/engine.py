@@ -898,6 +898,21 @@ class CudaDevice:
         film.rejected += int(self.last_stats().rejected)
         return SampleBatchResult(True, traced.value)
 
+    def render_region(self, camera: PerspectiveCamera, settings: RenderSettings, film: Film, region, first_sample: int,
+                      count: int) -> SampleBatchResult:
+        """Adds samples [first_sample, first_sample+count) to the pixels of region = (x0, y0, w, h)
+        of a whole-frame film, each exactly as render() would (pe_device_render_region)."""
+        self._sync_guiding(settings)
+        if film.width != settings.width or film.height != settings.height:
+            film.resize(settings.width, settings.height)
+        x0, y0, w, h = (int(v) for v in region)
+        traced = C.c_uint64(0)
+        capi.check(_lib().pe_device_render_region(self._h, C.byref(camera.describe_gpu()), C.byref(settings.to_c()),
+                                                  x0, y0, w, h, first_sample, count, None, capi.fptr(film.sum),
+                                                  capi.uptr(film.count), capi.fptr(film.sum_sq), C.byref(traced)))
+        film.rejected += int(self.last_stats().rejected)
+        return SampleBatchResult(True, traced.value)
+
     def _sync_guiding(self, settings: RenderSettings):
         # RenderSettings::pathGuiding (renderer.cpp:413-429): SD-tree guiding on while it is set;
         # turning it off drops the field
@@ -976,13 +991,17 @@ class CudaDevice:
         return int(chosen.value)
 
     # diagnostics
-    def trace_primary(self, camera: PerspectiveCamera, settings: RenderSettings, sample_index: int = 0):
+    def trace_primary(self, camera: PerspectiveCamera, settings: RenderSettings, sample_index: int = 0,
+                      ordered: bool = False):
+        """Primary hit (shape, triangle within the shape, t) per pixel: through the 4-wide tree the
+        render kernels use, or (ordered=True) the binary tree in the reference's visiting order."""
         n = settings.width * settings.height
         shape = np.empty(n, np.int32)
         prim = np.empty(n, np.int32)
         t = np.empty(n, np.float32)
-        capi.check(_lib().pe_device_trace_primary(self._h, C.byref(camera.describe_gpu()), C.byref(settings.to_c()),
-                                                  sample_index, capi.iptr(shape), capi.iptr(prim), capi.fptr(t)))
+        fn = _lib().pe_device_trace_primary_ordered if ordered else _lib().pe_device_trace_primary
+        capi.check(fn(self._h, C.byref(camera.describe_gpu()), C.byref(settings.to_c()), sample_index,
+                      capi.iptr(shape), capi.iptr(prim), capi.fptr(t)))
         return shape, prim, t
 
     def sobol(self, seed: int, px, py, index, n_dims: int) -> np.ndarray:

@@ -40,14 +40,27 @@ def cornell(pe, device, oracle):
     return scene, cam, st, oracle.RefScene(scene)
 
 
+def wide_hits_match(mine, ref):
+    """The 4-wide traversal's primary hits against the reference's: every distance bit-identical,
+    ids equal except at ties (two triangles at the identical distance); returns the tie count."""
+    ms, mp, mt = mine
+    rs, rp, rt = ref
+    assert np.array_equal(mt.view(np.uint32), rt.view(np.uint32))
+    same = (ms == rs) & (mp == rp)
+    ties = ~same & (mp >= 0) & (rp >= 0)
+    assert np.array_equal(~same, ties), np.count_nonzero(~same & ~ties)
+    return int(np.count_nonzero(ties))
+
+
 def test_cornell_primary_hits_bit_exact(device, cornell):
     scene, cam, st, ref = cornell
     for s in (0, 1, 7):
-        ms, mp, mt = device.trace_primary(cam, st, s)
+        ms, mp, mt = device.trace_primary(cam, st, s, ordered=True)
         rs, rp, rt = ref.trace_primary(cam, st, s)
         assert np.array_equal(ms, rs)
         assert np.array_equal(mp, rp)
         assert np.array_equal(mt.view(np.uint32), rt.view(np.uint32))
+        assert wide_hits_match(device.trace_primary(cam, st, s), (rs, rp, rt)) <= 2
 
 
 def test_cornell_image_matches_reference_at_equal_spp(pe, device, cornell):
@@ -85,12 +98,14 @@ def knot(pe, device, oracle):
 
 def test_knot_primary_hits(device, knot):
     scene, cam, st, ref = knot
-    ms, mp, mt = device.trace_primary(cam, st, 3)
+    ms, mp, mt = device.trace_primary(cam, st, 3, ordered=True)
     rs, rp, rt = ref.trace_primary(cam, st, 3)
     same = (ms == rs) & (mp == rp)
-    # ties (equal t on a shared edge) resolve by traversal order, which is the reference's
+    # the binary tree in the reference's order resolves ties (equal t on a shared edge) as it does
     assert same.mean() == 1.0, np.count_nonzero(~same)
-    assert np.array_equal(mt.view(np.uint32)[same], rt.view(np.uint32)[same])
+    assert np.array_equal(mt.view(np.uint32), rt.view(np.uint32))
+    # the 4-wide tree of the render kernels: same distances, ties counted
+    assert wide_hits_match(device.trace_primary(cam, st, 3), (rs, rp, rt)) <= 1e-4 * ms.size
 
 
 def test_knot_image_matches_reference_at_equal_spp(pe, device, knot):
@@ -112,9 +127,10 @@ def test_cornell_matches_golden_fixture(pe, device):
     scene, cam, st = scenes().cornell_box(32, 32, 8, 8, seed=0)
     scene.build_accelerator()
     device.set_scene(scene)
-    shape, prim, t = device.trace_primary(cam, st, 0)
+    shape, prim, t = device.trace_primary(cam, st, 0, ordered=True)
     assert np.array_equal(shape, g["shape"]) and np.array_equal(prim, g["prim"])
     assert np.array_equal(t.view(np.uint32), g["t"].view(np.uint32))
+    assert wide_hits_match(device.trace_primary(cam, st, 0), (g["shape"], g["prim"], g["t"])) <= 2
     film = pe.Film(st.width, st.height)
     device.render(cam, st, pe.RenderTargets(beauty=film), 0, 8)
     assert np.array_equal(film.count, g["count"])
@@ -129,7 +145,7 @@ def test_cornell_matches_c_restatement(pe, device):
     scene.build_accelerator()
     device.set_scene(scene)
     res = oracle.Restatement(scene)
-    a = device.trace_primary(cam, st, 2)
+    a = device.trace_primary(cam, st, 2, ordered=True)
     b = res.trace_primary(cam, st, 2)
     assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1])
     film = pe.Film(st.width, st.height)

@@ -163,6 +163,10 @@ int32_t pe_scene_add_material(pe_scene* s, const pe_material* m);
  * An emissive material registers one triangle light per triangle. */
 int32_t pe_scene_add_mesh(pe_scene* s, const float* positions, uint32_t n_vertices, const float* normals,
                           const float* uvs, const uint32_t* indices, uint32_t n_triangles, int32_t material);
+/* Sphere (src/geometry/sphere.h): an analytic sphere of the given centre and radius (> 0), one
+ * shape and one BVH primitive, hit by Sphere::intersect's quadratic (sphere.cpp:12-90).  Like the
+ * reference it is never a light, even with an emissive material. */
+int32_t pe_scene_add_sphere(pe_scene* s, const float center[3], float radius, int32_t material);
 /* Scene::tagShape (scene.h:108): the scene-node uid of a shape (counted as for
  * pe_scene_set_shadow_catcher), which light links name. */
 int32_t pe_scene_tag_shape(pe_scene* s, int32_t shape, uint64_t node_uid);

@@ -100,6 +100,7 @@ def _load(fast=False):
                                                C.c_int32, FP, UP]),
         "ref_dtree_probe": (C.c_int32, [FP, FP, C.c_int32, FP, FP, C.c_int32, FP, FP, C.c_int32, FP, FP]),
         "ref_render_camera": (C.c_int32, [P, P, C.c_void_p, C.c_int32, C.c_int32, C.c_int32, FP, UP]),
+        "ref_scene_add_sphere": (C.c_int32, [P, FP, C.c_float, C.c_int32]),
         "ref_material_defaults": (None, [C.c_int32, C.c_void_p]),
         "ref_render_rect": (C.c_int32, [P, P, C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32,
                                         C.c_int32, C.c_int32, FP, UP]),
@@ -163,7 +164,7 @@ class RefScene:
                 self.lib.ref_scene_build_texture_mipmaps(self.h, tex_index[id(img)])
         mat_index = {}
         for kind, obj in scene.ops:
-            if kind == "mesh" and id(obj.material) not in mat_index:
+            if kind in ("mesh", "sphere") and id(obj.material) not in mat_index:
                 struct = obj.material.struct_with(tex_index) if hasattr(obj.material, "struct_with") \
                     else obj.material.struct
                 idx = self.lib.ref_scene_add_material(self.h, C.byref(struct))
@@ -172,7 +173,9 @@ class RefScene:
                 mat_index[id(obj.material)] = idx
         self.mat_index = mat_index
         for kind, obj in scene.ops:
-            if kind == "mesh":
+            if kind == "sphere":
+                rc = self.lib.ref_scene_add_sphere(self.h, _f3(obj.center), obj.radius, mat_index[id(obj.material)])
+            elif kind == "mesh":
                 rc = self.lib.ref_scene_add_mesh(self.h, _f(obj.positions), obj.positions.shape[0], _f(obj.normals),
                                                  _f(obj.uvs), obj.indices.ctypes.data_as(UP), obj.indices.shape[0],
                                                  mat_index[id(obj.material)])
@@ -201,6 +204,8 @@ class RefScene:
         # the product scene: one per area light, one per triangle of an emissive mesh)
         groups, li = {}, 0
         for kind, obj in scene.ops:
+            if kind == "sphere":
+                continue
             if kind == "mesh":
                 m = obj.material.struct
                 if m.type in (0, 1) and any(m.emission):

@@ -28,6 +28,7 @@
 #include "engine/renderer.h"
 #include "engine/scene.h"
 #include "geometry/mesh.h"
+#include "geometry/sphere.h"
 #include "integrators/path_guiding.h"
 #include "integrators/path_tracer.h"
 #include "lights/area_light.h"
@@ -278,6 +279,15 @@ int32_t ref_scene_add_mesh(void* s, const float* pos, uint32_t nv, const float* 
 }
 
 // Scene::tagShape of the shape added `shape`-th.
+// Scene::addShape of a Sphere (src/geometry/sphere.h).
+int32_t ref_scene_add_sphere(void* s, const float* center, float radius, int32_t material) {
+    auto* rs = static_cast<RefScene*>(s);
+    if (material < 0 || material >= static_cast<int32_t>(rs->materials.size())) return -1;
+    rs->scene.addShape(std::make_shared<Sphere>(v3(center), radius, rs->materials[static_cast<size_t>(material)].get()));
+    rs->indexNewShapes();
+    return 0;
+}
+
 int32_t ref_scene_tag_shape(void* s, int32_t shape, uint64_t uid) {
     auto* rs = static_cast<RefScene*>(s);
     const auto& shapes = rs->scene.shapes();

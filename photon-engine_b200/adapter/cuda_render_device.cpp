@@ -21,6 +21,7 @@
 #include "core/image/image.h"
 #include "engine/scene.h"
 #include "geometry/mesh.h"
+#include "geometry/sphere.h"
 #include "geometry/surface_interaction.h"
 #include "geometry/triangle.h"
 #include "lights/area_light.h"
@@ -203,6 +204,15 @@ struct PeScene {
                     error = pe_last_error();
                     return false;
                 }
+            } else if (auto* sp = dynamic_cast<const Sphere*>(shape)) {
+                const int32_t mat = material(sp->material());
+                if (mat < 0) return false;
+                float c[3];
+                put3(c, sp->center());
+                if (pe_scene_add_sphere(s, c, sp->radius(), mat) != PE_OK) {
+                    error = pe_last_error();
+                    return false;
+                }
             } else if (dynamic_cast<const Triangle*>(shape) && (secondHalf || nextArea < areas.size())) {
                 if (!secondHalf) {
                     const AreaLight* a = areas[nextArea++];
@@ -219,7 +229,7 @@ struct PeScene {
                 secondHalf = !secondHalf;
             } else {
                 error = "shape " + std::to_string(i) + " is of a kind the CUDA device does not trace "
-                        "(spheres, mesh instances and stand-alone triangles)";
+                        "(mesh instances and stand-alone triangles)";
                 return false;
             }
             if (shape == scene.shadowCatcherShape()) pe_scene_set_shadow_catcher(s, index);

@@ -972,7 +972,7 @@ static int32_t buildScene(pe_scene* s) {
     // shapes and global triangle / vertex numbering
     uint32_t nTris = 0, nVerts = 0;
     for (const HostShape& sh : s->shapes) {
-        nTris += static_cast<uint32_t>(sh.idx.size() / 3);
+        nTris += sh.sphere ? 1u : static_cast<uint32_t>(sh.idx.size() / 3);
         nVerts += static_cast<uint32_t>(sh.pos.size());
     }
     if (nTris >= (1u << 23)) {
@@ -1044,6 +1044,19 @@ static int32_t buildScene(pe_scene* s) {
             uv.y = v < sh.uv.size() ? sh.uv[v].y : 0.0f;
             B.uv[v0 + v] = uv;
         }
+        if (sh.sphere) {
+            // one primitive, no vertices: its triVerts entry carries only the shape
+            B.triVerts[t0] = int4{-1, -1, -1, static_cast<int>(si)};
+            Box b;
+            b.lo = sh.center - mk(sh.radius);
+            b.hi = sh.center + mk(sh.radius);
+            triBounds[t0] = b;
+            triMask[t0] = sh.mask;
+            t0 += 1;
+            const MatGPU& ms = s->materials[static_cast<size_t>(sh.material)];
+            if (ms.flags & MF_TRANSMITS_SHADOWS) B.hasShadowTransmitters = true;
+            continue;
+        }
         const size_t nt = sh.idx.size() / 3;
         for (size_t t = 0; t < nt; ++t) {
             int4 tv;
@@ -1092,6 +1105,16 @@ static int32_t buildScene(pe_scene* s) {
         for (size_t i = 0; i < sb.ordered.size(); ++i) {
             const uint32_t g = static_cast<uint32_t>(sb.ordered[i]);
             const int4 tv = B.triVerts[g];
+            if (tv.x < 0) {
+                // analytic sphere: (centre, radius), meta with the sphere bit, global id
+                const HostShape& sh = s->shapes[static_cast<size_t>(tv.w)];
+                const uint32_t matType = static_cast<uint32_t>(s->materials[static_cast<size_t>(sh.material)].type);
+                B.tris[3 * i + 0] = f4(sh.center.x, sh.center.y, sh.center.z, sh.radius);
+                B.tris[3 * i + 1] = f4(0.0f, 0.0f, 0.0f,
+                                       bitsf(static_cast<uint32_t>(triMask[g]) | (matType << 8) | PRIM_SPHERE));
+                B.tris[3 * i + 2] = f4(0.0f, 0.0f, 0.0f, bitsf(g));
+                continue;
+            }
             const V3 p0 = mk(B.pos[tv.x].x, B.pos[tv.x].y, B.pos[tv.x].z);
             const V3 p1 = mk(B.pos[tv.y].x, B.pos[tv.y].y, B.pos[tv.y].z);
             const V3 p2 = mk(B.pos[tv.z].x, B.pos[tv.z].y, B.pos[tv.z].z);
@@ -1422,6 +1445,30 @@ int32_t pe_scene_add_mesh(pe_scene* s, const float* positions, uint32_t nv, cons
             s->lights.push_back(l);
         }
     }
+    s->shapes.push_back(std::move(sh));
+    s->built = false;
+    return PE_OK;
+}
+
+int32_t pe_scene_add_sphere(pe_scene* s, const float center[3], float radius, int32_t material) {
+    if (!s || !center) {
+        setError("pe_scene_add_sphere: null argument");
+        return PE_ERR_INVALID;
+    }
+    if (material < 0 || material >= static_cast<int32_t>(s->materials.size())) {
+        setError("pe_scene_add_sphere: material index out of range");
+        return PE_ERR_INVALID;
+    }
+    if (!(radius > 0.0f) || !std::isfinite(radius)) {
+        setError("pe_scene_add_sphere: the radius must be positive and finite");
+        return PE_ERR_INVALID;
+    }
+    HostShape sh;
+    sh.sphere = true;
+    sh.center = mk(center[0], center[1], center[2]);
+    sh.radius = radius;
+    sh.material = material;
+    sh.flags = SF_SPHERE;
     s->shapes.push_back(std::move(sh));
     s->built = false;
     return PE_OK;

@@ -17,6 +17,9 @@ struct HostShape {
     uint32_t flags = 0;
     int32_t emitter = -1;
     uint8_t mask = 0x1F;
+    bool sphere = false;        // an analytic sphere (Sphere, src/geometry/sphere.h): one primitive
+    V3 center{0.0f, 0.0f, 0.0f};
+    float radius = 0.0f;
 };
 
 struct HostEnv {

@@ -308,7 +308,7 @@ __device__ V3 shadowVisibility(const SceneGPU& S, V3 o, V3 d, float tMax, int li
         const Hit h = traceClosestWide<COUNT>(S, origin, d, VIS_SHADOW, 0.0f, remaining, nodes, tris);
         if (h.prim < 0) return T;
         Isect is;
-        fillHit(S, h, d, is);
+        fillHit(S, h, origin, d, is);
         if (link && !linkAllows(S.links[light].shadowMode, S.links[light].shadowMask, S.shapes[is.shape].linkNode)) {
             origin = offsetRayOrigin(is.point, is.pError, len2(is.ng) > 0.0f ? is.ng : is.normal, d);
             remaining -= h.t;
@@ -582,7 +582,7 @@ __device__ __noinline__ V3 roundedEdgeNormal(const SceneGPU& S, const Isect& is,
             const Hit h = traceClosestWide<false>(S, origin, rdir, VIS_ALL, 0.0f, 2.0f * radius, n0, n1);
             if (h.prim < 0) continue;
             Isect hit;
-            fillHit(S, h, rdir, hit);
+            fillHit(S, h, origin, rdir, hit);
             if (hit.shape != is.shape) continue;
             if (len2(hit.point - is.point) > 2.25f * radius * radius) continue;
             const V3 outward = hit.frontFace ? hit.normal : -hit.normal;
@@ -736,7 +736,7 @@ __device__ __forceinline__ bool shadeSlot(const SceneGPU& S, const Paths& P, con
                 h.u = hr.y;
                 h.v = hr.z;
                 h.prim = prim;
-                fillHit(S, h, dir, is);
+                fillHit(S, h, rayO, dir, is);
                 // exit vertex: outward normal, white Lambert; the depth does not grow
                 is.normal = -is.normal;
                 is.material = S.exitMaterial;
@@ -765,7 +765,7 @@ __device__ __forceinline__ bool shadeSlot(const SceneGPU& S, const Paths& P, con
             h.u = hr.y;
             h.v = hr.z;
             h.prim = prim;
-            fillHit(S, h, dir, is);
+            fillHit(S, h, rayO, dir, is);
             // Camera-invisible light quads (for camera rays) and cutouts are passed through;
             // the vertex does not count (path_tracer.cpp:426-439).
             if (skips < 64 && ((cameraRay && (S.shapes[is.shape].flags & SF_CAMERA_INVISIBLE)) ||

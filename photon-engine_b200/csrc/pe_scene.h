@@ -38,7 +38,12 @@ enum ShapeFlags : uint32_t {
     SF_CAMERA_INVISIBLE = 2u,
     SF_HAS_NORMALS = 4u,
     SF_HAS_UVS = 8u,
+    SF_SPHERE = 16u,         // an analytic sphere
 };
+
+// A leaf record whose b.w meta has this bit is an analytic sphere (Sphere, src/geometry/sphere.h):
+// a = (centre, radius); the other words hold the meta and the global primitive id as for a triangle.
+constexpr uint32_t PRIM_SPHERE = 1u << 16;
 
 struct ShapeInfo {
     int32_t material;

@@ -137,6 +137,39 @@ __device__ __forceinline__ bool triLean(const float4 a, const float4 b, const fl
     return t >= tMin && t <= tMax;
 }
 
+// Sphere::intersect's root choice (src/geometry/sphere.cpp:12-40) with solveQuadratic
+// (src/core/math/utils.h:64-88): the nearer root inside [tMin, tMax], else the farther one.
+__device__ __forceinline__ bool sphereLean(const float4 a, V3 o, V3 d, float tMin, float tMax, float& t) {
+    const V3 oc = o - mk(a.x, a.y, a.z);
+    const float qa = dot(d, d);
+    const float qb = 2.0f * dot(oc, d);
+    const float qc = dot(oc, oc) - a.w * a.w;
+    float t0, t1;
+    if (fabsf(qa) < 1e-6f) {
+        if (fabsf(qb) < 1e-6f) return false;
+        t0 = t1 = -qc / qb;
+    } else {
+        const float disc = qb * qb - 4.0f * qa * qc;
+        if (disc < 0.0f) return false;
+        const float sq = sqrtf(disc);
+        const float q = -0.5f * (qb + (qb < 0.0f ? -sq : sq));
+        t0 = q / qa;
+        t1 = qc / q;
+        if (t0 > t1) {
+            const float x = t0;
+            t0 = t1;
+            t1 = x;
+        }
+    }
+    float th = t0;
+    if (th < tMin || th > tMax) {
+        th = t1;
+        if (th < tMin || th > tMax) return false;
+    }
+    t = th;
+    return true;
+}
+
 struct Hit {
     float t, u, v;
     int32_t prim; // leaf-order primitive index, -1 = miss
@@ -157,10 +190,14 @@ __device__ __forceinline__ void testLeafClosest(const SceneGPU& S, int first, in
         const float4 a = __ldg(&S.tris[3 * pi + 0]);
         const float4 b = __ldg(&S.tris[3 * pi + 1]);
         if ((__float_as_uint(b.w) & mask) == 0u) continue;
-        const float4 c = __ldg(&S.tris[3 * pi + 2]);
         if (COUNT) ++triTests;
-        float t, u, v;
-        if (triLean(a, b, c, o, d, tMin, tMax, t, u, v)) {
+        float t, u = 0.0f, v = 0.0f;
+        if (__float_as_uint(b.w) & PRIM_SPHERE) {
+            if (!sphereLean(a, o, d, tMin, tMax, t)) continue;
+        } else if (!triLean(a, b, __ldg(&S.tris[3 * pi + 2]), o, d, tMin, tMax, t, u, v)) {
+            continue;
+        }
+        {
             tMax = t;
             best.t = t;
             best.u = u;
@@ -293,10 +330,13 @@ __device__ bool traceAny(const SceneGPU& S, V3 o, V3 d, uint32_t mask, float tMi
             const float4 a = __ldg(&S.tris[3 * pi + 0]);
             const float4 b = __ldg(&S.tris[3 * pi + 1]);
             if ((__float_as_uint(b.w) & mask) == 0u) continue;
-            const float4 c = __ldg(&S.tris[3 * pi + 2]);
             if (COUNT) ++triTests;
             float t, u, v;
-            if (triLean(a, b, c, o, d, tMin, tMax, t, u, v)) return true;
+            if (__float_as_uint(b.w) & PRIM_SPHERE) {
+                if (sphereLean(a, o, d, tMin, tMax, t)) return true;
+            } else if (triLean(a, b, __ldg(&S.tris[3 * pi + 2]), o, d, tMin, tMax, t, u, v)) {
+                return true;
+            }
         }
         if (sp == 0) return false;
         cur = stackRef[--sp];
@@ -458,10 +498,13 @@ __device__ bool traceAnyWide(const SceneGPU& S, V3 o, V3 d, uint32_t mask, float
             const float4 a = __ldg(&S.tris[3 * pi + 0]);
             const float4 b = __ldg(&S.tris[3 * pi + 1]);
             if ((__float_as_uint(b.w) & mask) == 0u) continue;
-            const float4 c = __ldg(&S.tris[3 * pi + 2]);
             if (COUNT) ++triTests;
             float t, u, v;
-            if (triLean(a, b, c, o, d, tMin, tMax, t, u, v)) return true;
+            if (__float_as_uint(b.w) & PRIM_SPHERE) {
+                if (sphereLean(a, o, d, tMin, tMax, t)) return true;
+            } else if (triLean(a, b, __ldg(&S.tris[3 * pi + 2]), o, d, tMin, tMax, t, u, v)) {
+                return true;
+            }
         }
         if (sp == 0) return false;
         cur = stackRef[--sp];
@@ -485,10 +528,54 @@ __device__ __forceinline__ V3 ld3(const float4* a, int i) {
     return mk(v.x, v.y, v.z);
 }
 
-static __device__ __noinline__ void fillHit(const SceneGPU& S, const Hit& h, V3 rayDir, Isect& is) {
+// Sphere::intersect's record (src/geometry/sphere.cpp:40-90): the point projected back onto the
+// sphere, its error bound, the outward normal faced to the ray, spherical uv and the ∂P/∂φ tangent.
+static __device__ __noinline__ void fillSphereHit(const SceneGPU& S, const Hit& h, V3 rayO, V3 rayDir, int g, int shape,
+                                                  Isect& is) {
+    const float4 a = __ldg(&S.tris[3 * h.prim + 0]);
+    const V3 c = mk(a.x, a.y, a.z);
+    const float r = a.w;
+    is.t = h.t;
+    V3 local = (rayO + rayDir * h.t) - c;
+    const float len = length(local);
+    if (len > 0.0f) local = local * (r / len);
+    is.point = c + local;
+    const float iso = gammaN(32) * smax(r + maxComp(vabs(c)), 1e-20f);
+    is.pError = (vabs(local) + vabs(c)) * gammaN(16) + mk(iso);
+    is.hasSmooth = false;
+    is.pSmooth = is.point;
+    const V3 outward = local / r;
+    is.ng = outward;
+    is.frontFace = dot(rayDir, outward) < 0.0f;
+    is.normal = is.frontFace ? outward : -outward;
+    if (len2(is.ng) == 0.0f) is.ng = outward;
+    const float theta = acosf(sclamp(outward.y, -1.0f, 1.0f));
+    float phi = atan2f(-outward.z, outward.x) + kPi;
+    if (phi < 0.0f) phi += kTwoPi;
+    is.uv.x = phi / kTwoPi;
+    is.uv.y = theta / kPi;
+    is.uvDensity = 1.0f;
+    V3 tangent = mk(outward.z, 0.0f, -outward.x);
+    if (len2(tangent) == 0.0f) {
+        const float sign = copysignf(1.0f, outward.z);
+        const float ac = -1.0f / (sign + outward.z);
+        const float bc = outward.x * outward.y * ac;
+        tangent = mk(1.0f + sign * outward.x * outward.x * ac, sign * bc, -sign * outward.x);
+    }
+    is.tangent = normalize(tangent);
+    is.tri = g;
+    is.shape = shape;
+    is.material = S.shapes[shape].material;
+}
+
+static __device__ __noinline__ void fillHit(const SceneGPU& S, const Hit& h, V3 rayO, V3 rayDir, Isect& is) {
     const float4 e2w = __ldg(&S.tris[3 * h.prim + 2]);
     const int g = static_cast<int>(__float_as_uint(e2w.w));
     const int4 tv = __ldg(&S.triVerts[g]);
+    if (__float_as_uint(__ldg(&S.tris[3 * h.prim + 1]).w) & PRIM_SPHERE) {
+        fillSphereHit(S, h, rayO, rayDir, g, tv.w, is);
+        return;
+    }
     const V3 v0 = ld3(S.pos, tv.x), v1 = ld3(S.pos, tv.y), v2 = ld3(S.pos, tv.z);
     const V3 n0 = ld3(S.nrm, tv.x), n1 = ld3(S.nrm, tv.y), n2 = ld3(S.nrm, tv.z);
     const float2 uv0 = __ldg(&S.uv[tv.x]), uv1 = __ldg(&S.uv[tv.y]), uv2 = __ldg(&S.uv[tv.z]);

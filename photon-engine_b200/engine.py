@@ -225,6 +225,18 @@ class TriangleMesh:
         return int(self.indices.shape[0])
 
 
+class Sphere:
+    """Sphere (src/geometry/sphere.h): an analytic sphere with one material."""
+
+    def __init__(self, center, radius: float, material: Material | None = None):
+        self.center = tuple(map(float, center))
+        self.radius = float(radius)
+        self.material = material
+
+    def num_triangles(self) -> int:
+        return 0
+
+
 class AreaLight:
     def __init__(self, position, u, v, radiance):
         self.position = tuple(map(float, position))
@@ -297,10 +309,11 @@ class Scene:
         except Exception:
             pass
 
-    def add_shape(self, mesh: TriangleMesh):
-        if mesh.material is None:
-            raise ValueError("TriangleMesh needs a material")
-        self.ops.append(("mesh", mesh))
+    def add_shape(self, shape):
+        """Scene::addShape of a TriangleMesh or a Sphere."""
+        if shape.material is None:
+            raise ValueError(f"{type(shape).__name__} needs a material")
+        self.ops.append(("sphere" if isinstance(shape, Sphere) else "mesh", shape))
 
     def add_light(self, light: AreaLight):
         self.ops.append(("area", light))
@@ -310,7 +323,7 @@ class Scene:
 
     def shape_count(self) -> int:
         """Shapes added so far: one per mesh, two per area light (its two triangles)."""
-        return sum(1 if kind == "mesh" else 2 for kind, _ in self.ops)
+        return sum(2 if kind == "area" else 1 for kind, _ in self.ops)
 
     def tag_shape(self, shape: int, node_uid: int):
         """Scene::tagShape: the scene-node uid that light links name this shape by."""
@@ -357,7 +370,7 @@ class Scene:
     def materials(self) -> list[Material]:
         out, seen = [], set()
         for kind, obj in self.ops:
-            if kind == "mesh" and id(obj.material) not in seen:
+            if kind in ("mesh", "sphere") and id(obj.material) not in seen:
                 seen.add(id(obj.material))
                 out.append(obj.material)
         return out
@@ -395,6 +408,8 @@ class Scene:
             return False
         lib, li = _lib(), 0
         for kind, obj in self.ops:
+            if kind == "sphere":
+                continue
             if kind == "mesh":
                 m = obj.material.struct
                 if m.type in (capi.PE_MAT_LAMBERT, capi.PE_MAT_DISNEY) and any(m.emission):
@@ -442,6 +457,8 @@ class Scene:
                 capi.check(lib.pe_scene_add_mesh(h, capi.fptr(obj.positions), obj.positions.shape[0],
                                                  capi.fptr(obj.normals), capi.fptr(obj.uvs), capi.uptr(obj.indices),
                                                  obj.indices.shape[0], mat_index[id(obj.material)]))
+            elif kind == "sphere":
+                capi.check(lib.pe_scene_add_sphere(h, capi.f3(obj.center), obj.radius, mat_index[id(obj.material)]))
             else:
                 capi.check(lib.pe_scene_add_area_light(h, capi.f3(obj.position), capi.f3(obj.u), capi.f3(obj.v),
                                                        capi.f3(obj.radiance), 1 if obj.visible_to_camera else 0))
@@ -456,6 +473,8 @@ class Scene:
                 capi.check(lib.pe_scene_set_material_name(h, mat_index[id(mat)], name.encode()))
         groups, li = {}, 0
         for kind, obj in self.ops:
+            if kind == "sphere":
+                continue
             if kind == "mesh":
                 m = obj.material.struct
                 if m.type in (capi.PE_MAT_LAMBERT, capi.PE_MAT_DISNEY) and any(m.emission):

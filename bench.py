@@ -255,7 +255,9 @@ def run_ours(args):
     scene, cam, st, desc = build_workload(pe)
     dev = pe.CudaDevice(local)
     dev.set_scene(scene)
-    tail = dev.autotune(cam, st, SPP_PER_STEP)  # untimed set-up: picks the tail threshold
+    tail = dev.autotune(cam, st, SPP_PER_STEP)  # untimed set-up: picks traversal, register budget, tail
+    tuning = dev.tuning()
+    tune_log = dev.autotune_log()
     # disjoint sample indices per replica; step k renders samples base + SPP_PER_STEP·(1 + warmup + k) …
     base = replica_sample_base(rank, args.warmup, args.steps)
 
@@ -320,7 +322,8 @@ def run_ours(args):
         return 0
 
     # roofline of the closest-hit kernel: per-ray algorithmic bytes from the counting pass
-    bytes_per_ray = (cs.node_visits * NODE_BYTES + cs.tri_tests * TRI_BYTES) / max(1, cs.closest_rays) + \
+    node_bytes = 64 if tuning["closest_traversal"] == 0 else NODE_BYTES  # binary node 64 B, 4-wide 128 B
+    bytes_per_ray = (cs.node_visits * node_bytes + cs.tri_tests * TRI_BYTES) / max(1, cs.closest_rays) + \
         RAY_BYTES + HIT_BYTES + QUEUE_BYTES
     peak, peak_kind = measured_peaks()
     # only the rays the bounce-by-bounce closest-hit launches traced (the tail kernel's are its own)
@@ -338,6 +341,18 @@ def run_ours(args):
             "kernel": "kIntersect (closest-hit BVH traversal)", "peak_kind": peak_kind,
             "bytes_per_ray": bytes_per_ray, "avg_launch_ms": ms_isect / max(1, n_isect),
             "rays_per_launch": rays_isect / max(1, n_isect)}
+
+    # the shading kernels (one lean kernel per shading key): algorithmic bytes per shaded path —
+    # nine 16-byte state columns and the binned slot index in; eight columns out; the hit record's
+    # triangle (16 B vertex ids, 3 × 40 B vertex position / normal / uv); one 64-byte shadow record
+    # and its 4-byte queue entry per NEE sample; a 4-byte next-queue entry
+    shade_bytes = 9 * 16 + 4 + 8 * 16 + 16 + 3 * 40 + 68 * shadow_rays / max(1, rays_isect) + 4
+    shade_ms = kernel_ms["shade"] * args.steps
+    shade_achieved = (rays_isect * shade_bytes) / (shade_ms / 1000.0) / 1e9 if shade_ms > 0 else None
+    roof_shade = {"bound": "hbm", "achieved": shade_achieved, "peak": peak, "unit": "GB/s",
+                  "frac": (shade_achieved / peak) if shade_achieved else None, "kernel": "kShadeKey (lean shading)",
+                  "peak_kind": peak_kind, "bytes_per_path": shade_bytes,
+                  "paths_per_step": rays_isect / args.steps}
 
     cpu = None
     if world == 1 and not args.no_cpu_baseline:
@@ -359,8 +374,11 @@ def run_ours(args):
                 "d2h_bytes_per_step": WIDTH * HEIGHT * (12 + 4 + 4)},
         "gpu_launches": int(launches),
         "autotuned_tail_paths": tail,
+        "tuning": tuning,
+        "autotune_log": tune_log.strip().splitlines(),
         "kernel_ms_per_step": kernel_ms,
         "roofline": roof,
+        "roofline_shade": roof_shade,
         "cpu_baseline": cpu,
         "clocks": clocks.summary(),
     }

@@ -422,6 +422,23 @@ int64_t pe_device_tail_paths(pe_device* d);
  * tail thresholds (1/4, 1/2, 1 and 2 resident grids) into a scratch film, twice, and keeps the
  * fastest of the second round; chosen (may be NULL) receives it.  The caller's films are untouched. */
 int32_t pe_device_autotune(pe_device* d, const pe_camera* cam, const pe_settings* st, int32_t probe_spp, int64_t* chosen);
+
+/* B200 tuning knobs with no counterpart in the reference engine; none changes a film.  The
+ * autotuner above sets all three by coordinate descent on probe renders of the caller's frame
+ * (closest-hit traversal, then the shading register budget, then the tail threshold). */
+typedef struct pe_tuning {
+    int64_t tail_paths;        /* as pe_device_set_tail_paths */
+    int32_t closest_traversal; /* bounce-by-bounce closest hits: 0 the binary tree, 1 the 4-wide tree,
+                                  2 / 3 the 4-wide tree with the first 8 / 16 stack entries of each
+                                  thread in shared memory (the rest in local memory) */
+    int32_t shade_budget;      /* lean shading kernels: 0 the compiler's register count, 1 at most 128
+                                  registers a thread (four 128-thread blocks per SM) */
+} pe_tuning;
+int32_t pe_device_get_tuning(pe_device* d, pe_tuning* out);
+int32_t pe_device_set_tuning(pe_device* d, const pe_tuning* t);
+/* The last pe_device_autotune's probe times, one "knob=value time ms" line each, into buf
+ * (NUL-terminated, truncated to len); returns the full length. */
+int32_t pe_device_autotune_log(pe_device* d, char* buf, size_t len);
 /* Device-stream timer: events recorded on the stream the kernels run on; end waits for the
  * stop event and returns the elapsed device milliseconds. */
 int32_t pe_device_timer_begin(pe_device* d);

@@ -64,6 +64,10 @@ class pe_scene_info(C.Structure):
                 ("has_environment", C.c_int32), ("light_sampler_mode", C.c_int32)]
 
 
+class pe_tuning(C.Structure):
+    _fields_ = [("tail_paths", C.c_int64), ("closest_traversal", C.c_int32), ("shade_budget", C.c_int32)]
+
+
 class pe_device_info(C.Structure):
     _fields_ = [("name", C.c_char * 128), ("memory_bytes", C.c_uint64), ("compute_major", C.c_int32),
                 ("compute_minor", C.c_int32), ("sm_count", C.c_int32), ("usable", C.c_int32),
@@ -214,6 +218,9 @@ SIGNATURES = {
     "pe_device_set_counting": (C.c_int32, [P, C.c_int32]),
     "pe_device_set_tail_paths": (C.c_int32, [P, C.c_int64]),
     "pe_device_tail_paths": (C.c_int64, [P]),
+    "pe_device_get_tuning": (C.c_int32, [P, C.POINTER(pe_tuning)]),
+    "pe_device_set_tuning": (C.c_int32, [P, C.POINTER(pe_tuning)]),
+    "pe_device_autotune_log": (C.c_int32, [P, C.c_char_p, C.c_size_t]),
     "pe_device_autotune": (C.c_int32, [P, C.POINTER(pe_camera), C.POINTER(pe_settings), C.c_int32, C.POINTER(C.c_int64)]),
     "pe_device_timer_begin": (C.c_int32, [P]),
     "pe_device_timer_end": (C.c_int32, [P, FP]),

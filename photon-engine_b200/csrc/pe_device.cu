@@ -209,12 +209,19 @@ Paths noAllocPaths(unsigned char* base) {
 int launchLeanShade(pe_device* d, const SceneGPU& S, const Paths& P, const Wave& W, int32_t* qOut, uint32_t* cOut,
                     cudaStream_t cs, bool out) {
     int n = 0;
+    const int budget = d->shadeBudget;
     auto one = [&](auto kernel, int key) {
         if (key > 0 && !(S.materialTypes & (1 << (key - 1)))) return;
-        kernel<<<d->blocksShadeKey[key], 128, 0, cs>>>(S, P, W, qOut, cOut);
+        kernel<<<d->blocksShadeKey[budget][key], 128, 0, cs>>>(S, P, W, qOut, cOut);
         ++n;
     };
-    if (out) {
+    if (!out && budget == 1) {
+        one(kShadeKey<false, 0, 4>, 0);
+        one(kShadeKey<false, 1, 4>, 1);
+        one(kShadeKey<false, 2, 4>, 2);
+        one(kShadeKey<false, 3, 4>, 3);
+        one(kShadeKey<false, 4, 4>, 4);
+    } else if (out) {
         one(kShadeKey<true, 0>, 0);
         one(kShadeKey<true, 1>, 1);
         one(kShadeKey<true, 2>, 2);
@@ -417,8 +424,16 @@ int32_t runWave(pe_device* d, int lane, Paths& P, int nSegs, int nSlots, int nPi
                 return rc;
             PE_CUDA(cudaEventRecord(e0, cs));
         }
-        if (d->counting)
+        if (d->counting && d->closestMode == TRACE_BINARY)
+            kIntersect<true, TRACE_BINARY><<<d->blocksIntersectMode[0], 128, 0, cs>>>(S, P, qIn, cIn, d->dStats);
+        else if (d->counting)
             kIntersect<true><<<d->blocksIntersect, 128, 0, cs>>>(S, P, qIn, cIn, d->dStats);
+        else if (d->closestMode == TRACE_BINARY)
+            kIntersect<false, TRACE_BINARY><<<d->blocksIntersectMode[0], 128, 0, cs>>>(S, P, qIn, cIn, d->dStats);
+        else if (d->closestMode == TRACE_WIDE_SMEM8)
+            kIntersect<false, TRACE_WIDE_SMEM8><<<d->blocksIntersectMode[2], 128, 0, cs>>>(S, P, qIn, cIn, d->dStats);
+        else if (d->closestMode == TRACE_WIDE_SMEM16)
+            kIntersect<false, TRACE_WIDE_SMEM16><<<d->blocksIntersectMode[3], 128, 0, cs>>>(S, P, qIn, cIn, d->dStats);
         else
             kIntersect<false><<<d->blocksIntersect, 128, 0, cs>>>(S, P, qIn, cIn, d->dStats);
         if (P.guiding == 2 && (rc = guideQueries(d, cs, P, W, qIn, cIn))) return rc;
@@ -1158,16 +1173,25 @@ pe_device* pe_device_create(int32_t ordinal, char* err, size_t errLen) {
     d->blocksTailLean = sm * std::max(1, b);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kShadow<false, true>, 128, 0);
     d->blocksShadowAny = sm * std::max(1, b);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kShadeKey<false, 0>, 128, 0);
-    d->blocksShadeKey[0] = sm * std::max(1, b);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kShadeKey<false, 1>, 128, 0);
-    d->blocksShadeKey[1] = sm * std::max(1, b);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kShadeKey<false, 2>, 128, 0);
-    d->blocksShadeKey[2] = sm * std::max(1, b);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kShadeKey<false, 3>, 128, 0);
-    d->blocksShadeKey[3] = sm * std::max(1, b);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kShadeKey<false, 4>, 128, 0);
-    d->blocksShadeKey[4] = sm * std::max(1, b);
+    auto occ = [&](auto kernel, int threads) {
+        int nb = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kernel, threads, 0);
+        return sm * std::max(1, nb);
+    };
+    d->blocksShadeKey[0][0] = occ(kShadeKey<false, 0>, 128);
+    d->blocksShadeKey[0][1] = occ(kShadeKey<false, 1>, 128);
+    d->blocksShadeKey[0][2] = occ(kShadeKey<false, 2>, 128);
+    d->blocksShadeKey[0][3] = occ(kShadeKey<false, 3>, 128);
+    d->blocksShadeKey[0][4] = occ(kShadeKey<false, 4>, 128);
+    d->blocksShadeKey[1][0] = occ(kShadeKey<false, 0, 4>, 128);
+    d->blocksShadeKey[1][1] = occ(kShadeKey<false, 1, 4>, 128);
+    d->blocksShadeKey[1][2] = occ(kShadeKey<false, 2, 4>, 128);
+    d->blocksShadeKey[1][3] = occ(kShadeKey<false, 3, 4>, 128);
+    d->blocksShadeKey[1][4] = occ(kShadeKey<false, 4, 4>, 128);
+    d->blocksIntersectMode[TRACE_BINARY] = occ(kIntersect<false, TRACE_BINARY>, 128);
+    d->blocksIntersectMode[TRACE_WIDE] = occ(kIntersect<false, TRACE_WIDE>, 128);
+    d->blocksIntersectMode[TRACE_WIDE_SMEM8] = occ(kIntersect<false, TRACE_WIDE_SMEM8>, 128);
+    d->blocksIntersectMode[TRACE_WIDE_SMEM16] = occ(kIntersect<false, TRACE_WIDE_SMEM16>, 128);
     const cudaError_t le = cudaGetLastError();
     if (le != cudaSuccess) {
         pe_device_destroy(d);
@@ -1776,6 +1800,10 @@ int32_t pe_device_last_stats(pe_device* d, pe_render_stats* out) {
 
 // Times a few tail thresholds on probe renders of the caller's view into a scratch film and keeps
 // the fastest; the film never depends on the threshold, so tuning is free to pick any of them.
+// Coordinate descent over the tuning knobs on probe renders of the caller's frame (samples from
+// 2^24 on, into a scratch film): the closest-hit traversal variant, then the shading kernels'
+// register budget, then the tail threshold; each candidate is timed twice and its faster render
+// counts, after one warm-up render.  The films are the same for every choice.
 int32_t pe_device_autotune(pe_device* d, const pe_camera* cam, const pe_settings* st, int32_t probeSpp,
                            int64_t* chosen) {
     if (!d) {
@@ -1799,33 +1827,99 @@ int32_t pe_device_autotune(pe_device* d, const pe_camera* cam, const pe_settings
         freeList(tmp);
         return rc;
     }
-    const int64_t grid = static_cast<int64_t>(d->blocksTail) * kTailBlock;
-    const int64_t candidates[] = {grid / 4, grid / 2, grid, 2 * grid};
     const int spp = std::max(1, probeSpp);
-    const int64_t saved = d->tailPaths;
-    float best = 1e30f;
-    int64_t pick = -1;
     // probe renders neither train nor sample a guiding field
     const int savedKind = d->guideKind, savedMode = d->guide.mode;
     d->guideKind = 0;
     d->guide.mode = 0;
-    for (int pass = 0; pass < 2 && rc == PE_OK; ++pass) // first pass warms caches and kernels
-        for (int64_t c : candidates) {
-            d->tailPaths = c;
-            rc = renderWaves(d, cam, st, 1 << 24, spp, nullptr, sum, cnt, sq, nullptr, d->capacity, false,
-                             Tile{0, 0, st->width, st->height});
-            if (rc) break;
-            if (pass == 1 && d->stats.ms_total < best) {
-                best = d->stats.ms_total;
-                pick = c;
+    const int64_t savedTail = d->tailPaths;
+    const int savedClosest = d->closestMode, savedBudget = d->shadeBudget;
+    std::string log;
+    auto probe = [&](float& ms) -> int32_t {
+        ms = 1e30f;
+        for (int k = 0; k < 2; ++k) {
+            const int32_t r = renderWaves(d, cam, st, 1 << 24, spp, nullptr, sum, cnt, sq, nullptr, d->capacity, false,
+                                          Tile{0, 0, st->width, st->height});
+            if (r) return r;
+            ms = std::min(ms, d->stats.ms_total);
+        }
+        return PE_OK;
+    };
+    float warm = 0.0f;
+    rc = probe(warm);
+    // one knob at a time, the others at their best so far
+    auto tune = [&](const char* name, auto set, const std::vector<int64_t>& values) {
+        float best = 1e30f;
+        int64_t pick = values.front();
+        for (int64_t v : values) {
+            if (rc) return;
+            set(v);
+            float ms = 0.0f;
+            rc = probe(ms);
+            log += std::string(name) + "=" + std::to_string(v) + " " + std::to_string(ms) + " ms\n";
+            if (!rc && ms < best) {
+                best = ms;
+                pick = v;
             }
         }
+        set(pick);
+    };
+    tune("closest_traversal", [&](int64_t v) { d->closestMode = static_cast<int>(v); },
+         {TRACE_WIDE, TRACE_BINARY, TRACE_WIDE_SMEM8, TRACE_WIDE_SMEM16});
+    tune("shade_budget", [&](int64_t v) { d->shadeBudget = static_cast<int>(v); }, {0, 1});
+    const int64_t grid = static_cast<int64_t>(d->blocksTail) * kTailBlock;
+    tune("tail_paths", [&](int64_t v) { d->tailPaths = v; }, {grid / 4, grid / 2, grid, 2 * grid});
     d->guideKind = savedKind;
     d->guide.mode = savedMode;
     freeList(tmp);
-    d->tailPaths = rc == PE_OK ? pick : saved;
+    if (rc) {
+        d->tailPaths = savedTail;
+        d->closestMode = savedClosest;
+        d->shadeBudget = savedBudget;
+    }
+    d->tuneLog = log;
     if (chosen) *chosen = d->tailPaths;
     return rc;
+}
+
+int32_t pe_device_get_tuning(pe_device* d, pe_tuning* out) {
+    if (!d || !out) {
+        setError("pe_device_get_tuning: null argument");
+        return PE_ERR_INVALID;
+    }
+    out->tail_paths = d->tailPaths;
+    out->closest_traversal = d->closestMode;
+    out->shade_budget = d->shadeBudget;
+    return PE_OK;
+}
+
+int32_t pe_device_set_tuning(pe_device* d, const pe_tuning* t) {
+    if (!d || !t) {
+        setError("pe_device_set_tuning: null argument");
+        return PE_ERR_INVALID;
+    }
+    if (t->tail_paths < -1 || t->closest_traversal < 0 || t->closest_traversal > 3 || t->shade_budget < 0 ||
+        t->shade_budget > 1) {
+        setError("pe_device_set_tuning: value out of range");
+        return PE_ERR_INVALID;
+    }
+    d->tailPaths = t->tail_paths;
+    d->closestMode = t->closest_traversal;
+    d->shadeBudget = t->shade_budget;
+    return PE_OK;
+}
+
+int32_t pe_device_autotune_log(pe_device* d, char* buf, size_t len) {
+    if (!d) {
+        setError("null device");
+        return PE_ERR_INVALID;
+    }
+    if (buf && len > 0) {
+        const size_t k = std::min(len - 1, d->tuneLog.size());
+        std::memcpy(buf, d->tuneLog.data(), k);
+        buf[k] = 0;
+    }
+    return static_cast<int32_t>(d->tuneLog.size());
 }
 
 int32_t pe_device_set_tail_paths(pe_device* d, int64_t paths) {

@@ -203,8 +203,13 @@ struct pe_device {
     bool counting = false;
     pe_render_stats stats{};
     int blocksIntersect = 0, blocksShade = 0, blocksShadow = 0, blocksGen = 0, blocksTail = 0;
-    int blocksShadeKey[5] = {0, 0, 0, 0, 0}; // lean shading kernel of each key (miss, 4 material types)
+    int blocksShadeKey[2][5] = {{0, 0, 0, 0, 0}, {0, 0, 0, 0, 0}}; // lean shading kernels: [budget][key]
     int blocksShadowAny = 0, blocksTailLean = 0;
+    int blocksIntersectMode[4] = {0, 0, 0, 0};
+    // tuning (pe_tuning): closest-hit traversal variant, register budget of the lean shading kernels
+    int closestMode = 1;  // TraceMode
+    int shadeBudget = 0;  // 0 the compiler's register count, 1 at most 128 registers (4 blocks per SM)
+    std::string tuneLog;  // the last autotune's probe times
     int64_t tailPaths = -1; // -1: one resident grid of the tail kernel; 0: no tail kernel
     unsigned char* noAllocBase = nullptr; // device address of g_noAllocScratch on this device
     void* stage = nullptr;                 // pinned staging of the batch film (host-film render)

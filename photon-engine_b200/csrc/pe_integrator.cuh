@@ -216,9 +216,15 @@ __global__ void kInitFree(Paths P, int n) {
 // ---- closest hit over a queue -----------------------------------------------------------------
 // Closest hit for every queued ray; each ray is then binned by its shading key (miss or the
 // hit material's type) so the shading kernel runs warps of one material kind.
-template <bool COUNT>
+// Closest-hit traversal variants the tuner chooses among (pe_tuning::closest_traversal).
+enum TraceMode { TRACE_BINARY = 0, TRACE_WIDE = 1, TRACE_WIDE_SMEM8 = 2, TRACE_WIDE_SMEM16 = 3 };
+constexpr int traceStackShared(int mode) { return mode == TRACE_WIDE_SMEM8 ? 8 : (mode == TRACE_WIDE_SMEM16 ? 16 : 0); }
+
+template <bool COUNT, int MODE = TRACE_WIDE>
 __global__ void __launch_bounds__(128) kIntersect(SceneGPU S, Paths P, const int32_t* queue, const uint32_t* count,
                                                   unsigned long long* stats) {
+    constexpr int SD = traceStackShared(MODE);
+    __shared__ uint2 sstack[SD > 0 ? SD * 128 : 1];
     const int n = static_cast<int>(*count);
     uint32_t nodes = 0, tris = 0;
     const int lane = threadIdx.x & 31;
@@ -231,8 +237,11 @@ __global__ void __launch_bounds__(128) kIntersect(SceneGPU S, Paths P, const int
             slot = queue[i];
             const float4 ro = P.rayO[slot];
             const float4 rd = P.rayD[slot];
-            const Hit h = traceClosestWide<COUNT>(S, mk(ro.x, ro.y, ro.z), mk(rd.x, rd.y, rd.z), __float_as_uint(ro.w), 0.0f,
-                                              1e30f, nodes, tris);
+            const V3 o = mk(ro.x, ro.y, ro.z), d = mk(rd.x, rd.y, rd.z);
+            const uint32_t vmask = __float_as_uint(ro.w);
+            const Hit h = MODE == TRACE_BINARY ? traceClosest<COUNT>(S, o, d, vmask, 0.0f, 1e30f, nodes, tris)
+                                               : traceClosestWide<COUNT, SD>(S, o, d, vmask, 0.0f, 1e30f, nodes, tris,
+                                                                             sstack + threadIdx.x);
             P.hit[slot] = make_float4(h.t, h.u, h.v, __int_as_float(h.prim));
             key = (__float_as_uint(ro.w) & RAY_WALK) ? kShadeKeys - 1
                   : (h.prim < 0 ? 0 : 1 + static_cast<int>((h.meta >> 8) & 0xFFu));
@@ -1247,8 +1256,10 @@ __global__ void __launch_bounds__(128, 6) kShade(SceneGPU S, Paths P, Wave W, in
 // The lean shading kernel of one shading key: the rays of that key's bin only, shaded by the
 // shadeSlot instantiation that carries the code of that key alone (waves of lean-shading scenes
 // without guiding; one launch per key, each with the registers its key needs).
-template <bool OUT, int KEY>
-__global__ void __launch_bounds__(128) kShadeKey(SceneGPU S, Paths P, Wave W, int32_t* nextQueue, uint32_t* nextCount) {
+// MINB: at least this many 128-thread blocks per SM (__launch_bounds__), i.e. a register budget
+// of 65536 / (128·MINB) per thread; 1 leaves the count to the compiler (pe_tuning::shade_budget).
+template <bool OUT, int KEY, int MINB = 1>
+__global__ void __launch_bounds__(128, MINB) kShadeKey(SceneGPU S, Paths P, Wave W, int32_t* nextQueue, uint32_t* nextCount) {
     const int n = static_cast<int>(P.counters[CNT_KEYS + KEY]);
     const int32_t* bin = P.sortQ + static_cast<size_t>(KEY) * P.capacity;
     const int lane = threadIdx.x & 31;

@@ -390,9 +390,24 @@ __device__ __forceinline__ void cmpx(float& ta, int& ra, int& ka, float& tb, int
     }
 }
 
-template <bool COUNT>
+// The traversal stack of one thread: its first SD entries in shared memory (`shared` points at
+// the thread's column of a [SD][128] block array, stride 128), the rest in local memory.
+template <int SD>
+struct TraceStack {
+    uint2* shared;
+    uint2 local[kWideStack - SD];
+    __device__ __forceinline__ void put(int i, int ref, float t) {
+        const uint2 e = make_uint2(static_cast<uint32_t>(ref), __float_as_uint(t));
+        if (SD > 0 && i < SD) shared[i * 128] = e;
+        else local[i - SD] = e;
+    }
+    __device__ __forceinline__ uint2 get(int i) const { return (SD > 0 && i < SD) ? shared[i * 128] : local[i - SD]; }
+};
+
+// SD: stack entries kept in shared memory (`sstack`: this thread's column); 0 keeps all in local.
+template <bool COUNT, int SD = 0>
 __device__ Hit traceClosestWide(const SceneGPU& S, V3 o, V3 d, uint32_t mask, float tMin, float tMax,
-                                uint32_t& nodeVisits, uint32_t& triTests) {
+                                uint32_t& nodeVisits, uint32_t& triTests, uint2* sstack = nullptr) {
     Hit best;
     best.prim = -1;
     best.meta = 0;
@@ -407,8 +422,8 @@ __device__ Hit traceClosestWide(const SceneGPU& S, V3 o, V3 d, uint32_t mask, fl
         testLeafClosest<COUNT>(S, S.rootFirst, S.rootCount, o, d, mask, tMin, tMax, best, triTests);
         return best;
     }
-    int stackRef[kWideStack];
-    float stackT[kWideStack];
+    TraceStack<SD> stack;
+    stack.shared = sstack;
     int sp = 0;
     int cur = 0;
     for (;;) {
@@ -428,9 +443,9 @@ __device__ Hit traceClosestWide(const SceneGPU& S, V3 o, V3 d, uint32_t mask, fl
             if (t0 == kInf) {
                 bool found = false;
                 while (sp > 0) {
-                    --sp;
-                    if (stackT[sp] <= tMax) {
-                        cur = stackRef[sp];
+                    const uint2 e = stack.get(--sp);
+                    if (__uint_as_float(e.y) <= tMax) {
+                        cur = static_cast<int>(e.x);
                         found = true;
                         break;
                     }
@@ -439,9 +454,9 @@ __device__ Hit traceClosestWide(const SceneGPU& S, V3 o, V3 d, uint32_t mask, fl
                 continue;
             }
             // farther children first onto the stack, so they pop nearest first
-            if (t3 != kInf) { stackRef[sp] = r3; stackT[sp] = t3; ++sp; }
-            if (t2 != kInf) { stackRef[sp] = r2; stackT[sp] = t2; ++sp; }
-            if (t1 != kInf) { stackRef[sp] = r1; stackT[sp] = t1; ++sp; }
+            if (t3 != kInf) stack.put(sp++, r3, t3);
+            if (t2 != kInf) stack.put(sp++, r2, t2);
+            if (t1 != kInf) stack.put(sp++, r1, t1);
             cur = r0;
         }
         int first, count;
@@ -449,9 +464,9 @@ __device__ Hit traceClosestWide(const SceneGPU& S, V3 o, V3 d, uint32_t mask, fl
         testLeafClosest<COUNT>(S, first, count, o, d, mask, tMin, tMax, best, triTests);
         bool found = false;
         while (sp > 0) {
-            --sp;
-            if (stackT[sp] <= tMax) {
-                cur = stackRef[sp];
+            const uint2 e = stack.get(--sp);
+            if (__uint_as_float(e.y) <= tMax) {
+                cur = static_cast<int>(e.x);
                 found = true;
                 break;
             }

@@ -1009,6 +1009,24 @@ class CudaDevice:
                                              int(probe_spp), C.byref(chosen)))
         return int(chosen.value)
 
+    def tuning(self) -> dict:
+        """The device's tuning knobs (pe_tuning): tail_paths, closest_traversal, shade_budget."""
+        t = capi.pe_tuning()
+        capi.check(_lib().pe_device_get_tuning(self._h, C.byref(t)))
+        return {"tail_paths": int(t.tail_paths), "closest_traversal": int(t.closest_traversal),
+                "shade_budget": int(t.shade_budget)}
+
+    def set_tuning(self, tail_paths: int = -1, closest_traversal: int = 1, shade_budget: int = 0):
+        capi.check(_lib().pe_device_set_tuning(self._h, C.byref(capi.pe_tuning(tail_paths, closest_traversal,
+                                                                                shade_budget))))
+
+    def autotune_log(self) -> str:
+        """The last autotune's probe times ("knob=value time ms" per line)."""
+        n = _lib().pe_device_autotune_log(self._h, None, 0)
+        buf = C.create_string_buffer(max(1, n + 1))
+        _lib().pe_device_autotune_log(self._h, buf, len(buf))
+        return buf.value.decode()
+
     # diagnostics
     def trace_primary(self, camera: PerspectiveCamera, settings: RenderSettings, sample_index: int = 0,
                       ordered: bool = False):

@@ -100,9 +100,15 @@ def test_tile_rejects_films_it_cannot_write(pe, device):
     host = np.zeros((64, 64, 3), np.float32)
     with pytest.raises(pe._capi.PhotonError, match="device"):
         device.render_tile_noalloc(cam, st, 0, 0, 32, 32, 0, 1, host.ctypes.data, c.data_ptr(), q.data_ptr())
-    short = torch.zeros(100, dtype=torch.float32, device="cuda")
-    with pytest.raises(pe._capi.PhotonError, match="the film needs"):
-        device.render_tile_noalloc(cam, st, 0, 0, 32, 32, 0, 1, s.data_ptr(), c.data_ptr(), short.data_ptr())
+    # a buffer of its own (torch's caching allocator would hand out a slice of a larger block)
+    from cuda.bindings import runtime as rt
+    err, short = rt.cudaMalloc(400)
+    assert err == rt.cudaError_t.cudaSuccess
+    try:
+        with pytest.raises(pe._capi.PhotonError, match="the film needs"):
+            device.render_tile_noalloc(cam, st, 0, 0, 32, 32, 0, 1, s.data_ptr(), c.data_ptr(), int(short))
+    finally:
+        rt.cudaFree(short)
     # the device still renders afterwards
     device.render_tile_noalloc(cam, st, 0, 0, 32, 32, 0, 1, s.data_ptr(), c.data_ptr(), q.data_ptr())
     device.synchronize()

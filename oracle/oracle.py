@@ -101,6 +101,8 @@ def _load(fast=False):
         "ref_dtree_probe": (C.c_int32, [FP, FP, C.c_int32, FP, FP, C.c_int32, FP, FP, C.c_int32, FP, FP]),
         "ref_render_camera": (C.c_int32, [P, P, C.c_void_p, C.c_int32, C.c_int32, C.c_int32, FP, UP]),
         "ref_scene_add_sphere": (C.c_int32, [P, FP, C.c_float, C.c_int32]),
+        "ref_load_project": (P, [C.c_char_p, C.c_float, IP, FP, IP, IP, FP, C.c_char_p, C.c_size_t]),
+        "ref_scene_shapes": (C.c_int32, [P, IP, IP, FP, C.c_int32]),
         "ref_material_defaults": (None, [C.c_int32, C.c_void_p]),
         "ref_render_rect": (C.c_int32, [P, P, C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32,
                                         C.c_int32, C.c_int32, FP, UP]),
@@ -519,6 +521,51 @@ def ref_scene_from_description(desc: dict, fast: bool = False) -> "RefScene":
     return rs
 
 
+class ProjectCamera:
+    """The reference's camera of a loaded project (ref_camera_create parameters)."""
+
+    def __init__(self, kind: int, params):
+        self.kind = int(kind)
+        self.params = [float(x) for x in params]
+
+    def reference_params(self):
+        n = {0: 11, 1: 15, 2: 11}[self.kind]
+        return self.kind, self.params[:n]
+
+    def describe_gpu(self):
+        return describe_reference_camera(self)
+
+
+def load_project(path, width: int, height: int):
+    """The reference's loadProject + buildRenderScene of a .photon file: (RefScene, camera,
+    max bounces, filter type, filter width)."""
+    lib = _load()
+    kind = C.c_int32(0)
+    cam = (C.c_float * 16)()
+    mb, ft = C.c_int32(0), C.c_int32(0)
+    fw = C.c_float(0.0)
+    err = C.create_string_buffer(1024)
+    h = lib.ref_load_project(str(path).encode(), float(width) / float(height), C.byref(kind), cam, C.byref(mb),
+                             C.byref(ft), C.byref(fw), err, len(err))
+    if not h:
+        raise RuntimeError(f"reference loadProject failed: {err.value.decode(errors='replace')}")
+    rs = RefScene.__new__(RefScene)
+    rs.lib = lib
+    rs.h = h
+    return rs, ProjectCamera(kind.value, list(cam)), mb.value, ft.value, fw.value
+
+
+def scene_shapes(ref: "RefScene"):
+    """(kind, triangles, bounds (n, 6)) of each shape of a reference scene (kind 0 mesh, 1 sphere,
+    2 area-light triangle, 3 other)."""
+    n = ref.lib.ref_scene_shapes(ref.h, None, None, None, 0)
+    kind = np.zeros(n, np.int32)
+    tris = np.zeros(n, np.int32)
+    b = np.zeros((n, 6), np.float32)
+    ref.lib.ref_scene_shapes(ref.h, kind.ctypes.data_as(IP), tris.ctypes.data_as(IP), _f(b), n)
+    return kind, tris, b
+
+
 def render_stock(ref: "RefScene", camera: DescCamera, settings: DescSettings, first: int, count: int,
                  threads: int = 0):
     """Renderer::renderSamples (the stock CPU path, Sobol seed 12345) of samples
@@ -655,7 +702,7 @@ def describe_reference_camera(camera):
     """Camera::describeGpu of the reference's own camera class, as a pe_camera."""
     lib = _load()
     cam = reference_camera(camera, lib)
-    out = type(camera.describe_gpu())()
+    out = _abi().pe_camera()
     try:
         lib.ref_camera_describe(cam, C.byref(out))
     finally:

@@ -29,6 +29,8 @@
 #include "engine/scene.h"
 #include "geometry/mesh.h"
 #include "geometry/sphere.h"
+#include "geometry/mesh_instance.h"
+#include "geometry/triangle.h"
 #include "integrators/path_guiding.h"
 #include "integrators/path_tracer.h"
 #include "lights/area_light.h"
@@ -38,6 +40,10 @@
 #include "materials/lambertian.h"
 #include "materials/mirror.h"
 #include "samplers/sobol_sampler.h"
+#include "scene/document.h"
+#include "scene/project_io.h"
+#include "scene/scene_graph.h"
+#include <nlohmann/json.hpp>
 #ifdef PE_WITH_ADAPTER
 #include "engine/render_session.h"
 #include "adapter/cuda_render_device.h"
@@ -85,7 +91,10 @@ private:
 };
 
 struct RefScene {
-    Scene scene;
+    std::shared_ptr<Scene> holder;
+    Scene& scene;
+    RefScene() : holder(std::make_shared<Scene>()), scene(*holder) {}
+    explicit RefScene(std::shared_ptr<Scene> s) : holder(std::move(s)), scene(*holder) {}
     std::vector<std::shared_ptr<Material>> materials;
     std::unordered_map<const void*, int> shapeIndex; // hitObject → insertion index
     int nextShape = 0;
@@ -279,6 +288,84 @@ int32_t ref_scene_add_mesh(void* s, const float* pos, uint32_t nv, const float* 
 }
 
 // Scene::tagShape of the shape added `shape`-th.
+// loadProject + buildRenderScene, the CLI's path for a .photon file (main.cpp:197-206, 214-260):
+// the project's render scene; its orbit camera (cameraFromJson, main.cpp:88-110) as
+// ref_camera_create parameters; the render block's max bounces and pixel filter.
+void* ref_load_project(const char* path, float aspect, int32_t* camKind, float* cam, int32_t* maxBounces,
+                       int32_t* filterType, float* filterWidth, char* err, size_t errLen) {
+    SceneGraph graph;
+    ProjectData data;
+    std::string e;
+    if (!loadProject(path, graph, data, &e)) {
+        std::snprintf(err, errLen, "%s", e.c_str());
+        return nullptr;
+    }
+    EnvironmentCache cache;
+    auto scene = buildRenderScene(graph, data.lights, data.environment, cache, false);
+    auto* rs = new RefScene(scene);
+    rs->indexNewShapes();
+    const nlohmann::json& c = data.camera;
+    Vec3f target(0, 0.5f, 0);
+    if (auto t = c.find("target"); t != c.end() && t->is_array() && t->size() == 3)
+        target = Vec3f((*t)[0].get<float>(), (*t)[1].get<float>(), (*t)[2].get<float>());
+    const float r = c.value("radius", 5.0f), th = c.value("theta", 1.15f), ph = c.value("phi", 0.45f);
+    const float fov = c.value("fov", 35.0f);
+    const Vec3f eye = target + Vec3f(std::sin(th) * std::cos(ph), std::cos(th), std::sin(th) * std::sin(ph)) * r;
+    const float head[9] = {eye.x, eye.y, eye.z, target.x, target.y, target.z, 0.0f, 1.0f, 0.0f};
+    for (int i = 0; i < 9; ++i) cam[i] = head[i];
+    cam[10] = aspect;
+    if (c.value("orthographic", false)) {
+        *camKind = 2;
+        cam[9] = 2.0f * std::tan(fov * DEG_TO_RAD * 0.5f) * r;
+    } else if (c.value("aperture", 0.0f) > 0.0f) {
+        *camKind = 1;
+        cam[9] = fov;
+        cam[11] = c.value("aperture", 0.0f);
+        cam[12] = c.value("focusExplicit", false) ? c.value("focusDistance", r) : r;
+        cam[13] = static_cast<float>(c.value("apertureBlades", 0));
+        cam[14] = c.value("bladeRotation", 0.0f);
+    } else {
+        *camKind = 0;
+        cam[9] = fov;
+    }
+    *maxBounces = data.render.value("maxBounces", 8);
+    PixelFilterType ft = PixelFilterType::Box;
+    parsePixelFilter(data.render.value("pixelFilter", std::string("box")).c_str(), ft);
+    *filterType = static_cast<int32_t>(ft);
+    *filterWidth = data.render.value("filterWidth", ft == PixelFilterType::Box ? 1.0f : 1.5f);
+    return rs;
+}
+
+// The shapes of a scene in order: kind (0 mesh instance or mesh, 1 sphere, 2 area-light triangle,
+// 3 other) and, per shape, its triangle count, world bounds (6 floats) and sphere radius.
+int32_t ref_scene_shapes(void* s, int32_t* kind, int32_t* tris, float* bounds, int32_t cap) {
+    auto* rs = static_cast<RefScene*>(s);
+    const auto& shapes = rs->scene.shapes();
+    const int32_t n = static_cast<int32_t>(shapes.size());
+    for (int32_t i = 0; i < n && i < cap; ++i) {
+        const Shape* sh = shapes[static_cast<size_t>(i)].get();
+        int32_t k = 3, t = 0;
+        if (auto* mi = dynamic_cast<const MeshInstance*>(sh)) {
+            k = 0;
+            t = mi->mesh() ? static_cast<int32_t>(mi->mesh()->numTriangles()) : 0;
+        } else if (auto* m = dynamic_cast<const TriangleMesh*>(sh)) {
+            k = 0;
+            t = static_cast<int32_t>(m->numTriangles());
+        } else if (dynamic_cast<const Sphere*>(sh)) {
+            k = 1;
+        } else if (dynamic_cast<const Triangle*>(sh)) {
+            k = 2;
+            t = 1;
+        }
+        kind[i] = k;
+        tris[i] = t;
+        const AABB b = sh->bounds();
+        const float v[6] = {b.pMin.x, b.pMin.y, b.pMin.z, b.pMax.x, b.pMax.y, b.pMax.z};
+        for (int j = 0; j < 6; ++j) bounds[6 * i + j] = v[j];
+    }
+    return n;
+}
+
 // Scene::addShape of a Sphere (src/geometry/sphere.h).
 int32_t ref_scene_add_sphere(void* s, const float* center, float radius, int32_t material) {
     auto* rs = static_cast<RefScene*>(s);

@@ -167,6 +167,28 @@ int32_t pe_scene_add_mesh(pe_scene* s, const float* positions, uint32_t n_vertic
  * shape and one BVH primitive, hit by Sphere::intersect's quadratic (sphere.cpp:12-90).  Like the
  * reference it is never a light, even with an emissive material. */
 int32_t pe_scene_add_sphere(pe_scene* s, const float center[3], float radius, int32_t material);
+
+/* Mesh instancing (MeshInstance, src/geometry/mesh_instance.h; Scene::addShape, scene.cpp:23-41).
+ * pe_scene_add_blas keeps a triangle mesh for instancing and returns its id (or -PE_*): it gets
+ * its own BVH (a BLAS, built once, at most 2,097,151 triangles; a mesh of at most 16 triangles is
+ * one leaf tested in index order) and is not a shape by itself.  pe_scene_add_instance places it
+ * by a row-major local-to-world matrix (column vectors, translation in the last column) with the
+ * inverse the caller composed (NULL: Mat4f::inverse's cofactor expansion) and a material; the
+ * instance is one shape and one top-level primitive, rays are carried into its space and its
+ * BLAS walked (mesh_instance.cpp:104-133).  At most 1023 instances a scene.  An emissive
+ * instance gives one light per triangle, placed by the transform. */
+int32_t pe_scene_add_blas(pe_scene* s, const float* positions, uint32_t nv, const float* normals, const float* uvs,
+                          const uint32_t* indices, uint32_t ntri);
+int32_t pe_scene_add_instance(pe_scene* s, int32_t blas, const float local_to_world[16], const float world_to_local[16],
+                              int32_t material);
+/* SceneUpdateKind::Transforms: new matrices for instance shape `shape` of a built scene; then
+ * pe_device_update_transforms refits the top-level tree on the device without rebuilding any
+ * BLAS.  An emissive instance (its lights move) returns PE_ERR_LIMIT: rebuild the scene. */
+int32_t pe_scene_set_instance_transform(pe_scene* s, int32_t shape, const float local_to_world[16],
+                                        const float world_to_local[16]);
+/* Refits a built scene's top-level tree to its instances' current matrices: boxes recomputed
+ * bottom up, the tree's shape and leaf order kept (pe_device_update_transforms calls it). */
+int32_t pe_scene_refit(pe_scene* s);
 /* Scene::tagShape (scene.h:108): the scene-node uid of a shape (counted as for
  * pe_scene_set_shadow_catcher), which light links name. */
 int32_t pe_scene_tag_shape(pe_scene* s, int32_t shape, uint64_t node_uid);
@@ -296,6 +318,11 @@ int32_t pe_device_update_materials(pe_device* d, const pe_scene* s);
  * materials and the light sampler go to the device again (PE_ERR_LIMIT when the sampler's tree
  * changed shape: set the scene again). */
 int32_t pe_device_update_lights(pe_device* d, const pe_scene* s);
+/* SceneUpdateKind::Transforms: after pe_scene_set_instance_transform edits, refits the scene's
+ * top-level tree and sends only it, the instance table and the root box; no BLAS is rebuilt or
+ * sent.  The film is the one a rebuilt scene gives, except where two triangles give the
+ * identical hit distance (the refitted tree may visit them in another order). */
+int32_t pe_device_update_transforms(pe_device* d, pe_scene* s);
 
 /* RenderDevice::render: adds samples [first_sample, first_sample+count) to every
  * pixel and accumulates into the caller's host arrays exactly as

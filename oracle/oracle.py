@@ -101,6 +101,9 @@ def _load(fast=False):
         "ref_dtree_probe": (C.c_int32, [FP, FP, C.c_int32, FP, FP, C.c_int32, FP, FP, C.c_int32, FP, FP]),
         "ref_render_camera": (C.c_int32, [P, P, C.c_void_p, C.c_int32, C.c_int32, C.c_int32, FP, UP]),
         "ref_scene_add_sphere": (C.c_int32, [P, FP, C.c_float, C.c_int32]),
+        "ref_scene_add_blas": (C.c_int32, [P, FP, C.c_uint32, FP, FP, UP, C.c_uint32]),
+        "ref_scene_add_instance": (C.c_int32, [P, C.c_int32, FP, FP, C.c_int32]),
+        "ref_scene_move_instance": (C.c_int32, [P, C.c_int32, FP, FP]),
         "ref_load_project": (P, [C.c_char_p, C.c_float, IP, FP, IP, IP, FP, C.c_char_p, C.c_size_t]),
         "ref_scene_shapes": (C.c_int32, [P, IP, IP, FP, C.c_int32]),
         "ref_material_defaults": (None, [C.c_int32, C.c_void_p]),
@@ -166,7 +169,7 @@ class RefScene:
                 self.lib.ref_scene_build_texture_mipmaps(self.h, tex_index[id(img)])
         mat_index = {}
         for kind, obj in scene.ops:
-            if kind in ("mesh", "sphere") and id(obj.material) not in mat_index:
+            if kind in ("mesh", "sphere", "instance") and id(obj.material) not in mat_index:
                 struct = obj.material.struct_with(tex_index) if hasattr(obj.material, "struct_with") \
                     else obj.material.struct
                 idx = self.lib.ref_scene_add_material(self.h, C.byref(struct))
@@ -174,9 +177,18 @@ class RefScene:
                     raise RuntimeError("reference rejected a material")
                 mat_index[id(obj.material)] = idx
         self.mat_index = mat_index
+        blas_index = {}
         for kind, obj in scene.ops:
             if kind == "sphere":
                 rc = self.lib.ref_scene_add_sphere(self.h, _f3(obj.center), obj.radius, mat_index[id(obj.material)])
+            elif kind == "instance":
+                mesh = obj.mesh
+                if id(mesh) not in blas_index:
+                    blas_index[id(mesh)] = self.lib.ref_scene_add_blas(
+                        self.h, _f(mesh.positions), mesh.positions.shape[0], _f(mesh.normals), _f(mesh.uvs),
+                        mesh.indices.ctypes.data_as(UP), mesh.indices.shape[0])
+                rc = self.lib.ref_scene_add_instance(self.h, blas_index[id(mesh)], _f(obj.local_to_world),
+                                                     _f(obj.world_to_local), mat_index[id(obj.material)])
             elif kind == "mesh":
                 rc = self.lib.ref_scene_add_mesh(self.h, _f(obj.positions), obj.positions.shape[0], _f(obj.normals),
                                                  _f(obj.uvs), obj.indices.ctypes.data_as(UP), obj.indices.shape[0],
@@ -208,10 +220,10 @@ class RefScene:
         for kind, obj in scene.ops:
             if kind == "sphere":
                 continue
-            if kind == "mesh":
+            if kind in ("mesh", "instance"):
                 m = obj.material.struct
                 if m.type in (0, 1) and any(m.emission):
-                    li += obj.indices.shape[0]
+                    li += (obj.mesh if kind == "instance" else obj).indices.shape[0]
             else:
                 if getattr(obj, "light_group", ""):
                     groups[li] = obj.light_group
@@ -305,9 +317,18 @@ class RefScene:
             raise RuntimeError(f"adapter session failed ({done}): {err.value.decode()}")
         return mean, cnt, alb, int(done), int(feats.value)
 
-    def session_cuda_update(self, kind: int, index: int, rgb):
+    def move_instance(self, shape: int, local_to_world, world_to_local=None):
+        """Places MeshInstance `shape` anew with another matrix (same mesh and material) and
+        rebuilds the reference scene's accelerator."""
+        m = np.ascontiguousarray(local_to_world, np.float32).reshape(16)
+        mi = None if world_to_local is None else np.ascontiguousarray(world_to_local, np.float32).reshape(16)
+        if self.lib.ref_scene_move_instance(self.h, int(shape), _f(m), None if mi is None else _f(mi)) != 0:
+            raise ValueError(f"shape {shape} is not a mesh instance")
+
+    def session_cuda_update(self, kind: int, index: int = 0, rgb=(0.0, 0.0, 0.0)):
         """Edits the reference scene (kind 1: material `index`'s Disney base colour; kind 2:
-        AreaLight `index`'s radiance) and calls the adapter's RenderDevice::updateScene."""
+        AreaLight `index`'s radiance; kind 3: nothing, the instances were moved by move_instance)
+        and calls the adapter's RenderDevice::updateScene with that SceneUpdateKind."""
         rc = self.lib.ref_session_cuda_update(self.h, int(kind), int(index), _f3(rgb))
         if rc != 0:
             raise RuntimeError(f"adapter update failed ({rc})")

@@ -90,6 +90,11 @@ private:
     CameraGpuDesc m_d;
 };
 
+struct RefScene;
+struct RefBlas {
+    std::shared_ptr<TriangleMesh> mesh;
+};
+
 struct RefScene {
     std::shared_ptr<Scene> holder;
     Scene& scene;
@@ -100,6 +105,9 @@ struct RefScene {
     int nextShape = 0;
     std::string envGroup; // the environment's light group, applied at build
     std::vector<std::shared_ptr<Image>> textures; // ref_scene_add_texture
+    std::vector<std::shared_ptr<TriangleMesh>> blases; // ref_scene_add_blas
+    uint64_t id = ++counter;                            // unique over the process's RefScenes
+    static inline uint64_t counter = 0;
     void indexNewShapes() {
         const auto& shapes = scene.shapes();
         for (size_t i = static_cast<size_t>(nextShape); i < shapes.size(); ++i)
@@ -364,6 +372,70 @@ int32_t ref_scene_shapes(void* s, int32_t* kind, int32_t* tris, float* bounds, i
         for (int j = 0; j < 6; ++j) bounds[6 * i + j] = v[j];
     }
     return n;
+}
+
+// A TriangleMesh kept for instancing (its material is the instance's).
+int32_t ref_scene_add_blas(void* s, const float* pos, uint32_t nv, const float* nrm, const float* uv, const uint32_t* idx,
+                           uint32_t ntri) {
+    auto* rs = static_cast<RefScene*>(s);
+    std::vector<Vec3f> p(nv), n;
+    std::vector<Vec2f> t;
+    for (uint32_t i = 0; i < nv; ++i) p[i] = v3(pos + 3 * i);
+    if (nrm) {
+        n.resize(nv);
+        for (uint32_t i = 0; i < nv; ++i) n[i] = v3(nrm + 3 * i);
+    }
+    if (uv) {
+        t.resize(nv);
+        for (uint32_t i = 0; i < nv; ++i) t[i] = Vec2f(uv[2 * i], uv[2 * i + 1]);
+    }
+    std::vector<uint32_t> ix(idx, idx + 3ull * ntri);
+    rs->blases.push_back(std::make_shared<TriangleMesh>(p, n, t, ix, nullptr));
+    return static_cast<int32_t>(rs->blases.size() - 1);
+}
+
+// Scene::addShape of a MeshInstance of BLAS `blas` with Transform(l2w, w2l) and a material.
+int32_t ref_scene_add_instance(void* s, int32_t blas, const float* l2w, const float* w2l, int32_t material) {
+    auto* rs = static_cast<RefScene*>(s);
+    if (blas < 0 || blas >= static_cast<int32_t>(rs->blases.size()) || material < 0 ||
+        material >= static_cast<int32_t>(rs->materials.size()))
+        return -1;
+    Mat4f m, mi;
+    for (int r = 0; r < 4; ++r)
+        for (int c = 0; c < 4; ++c) {
+            m(r, c) = l2w[4 * r + c];
+            if (w2l) mi(r, c) = w2l[4 * r + c];
+        }
+    const Transform xf = w2l ? Transform(m, mi) : Transform(m);
+    rs->scene.addShape(std::make_shared<MeshInstance>(rs->blases[static_cast<size_t>(blas)], xf,
+                                                      rs->materials[static_cast<size_t>(material)].get()));
+    rs->indexNewShapes();
+    return 0;
+}
+
+// Moves MeshInstance `shape`: a MeshInstance's matrix is fixed at construction, so an application
+// that animates one places a new MeshInstance of the same mesh and material in its scene (the
+// document rebuild of buildRenderScene).  The shape slot is replaced in place and the scene's
+// accelerator rebuilt; 0, or -1 when `shape` is not a MeshInstance.
+int32_t ref_scene_move_instance(void* s, int32_t shape, const float* l2w, const float* w2l) {
+    auto* rs = static_cast<RefScene*>(s);
+    auto& shapes = const_cast<std::vector<std::shared_ptr<Shape>>&>(rs->scene.shapes());
+    if (shape < 0 || shape >= static_cast<int32_t>(shapes.size())) return -1;
+    auto* old = dynamic_cast<MeshInstance*>(shapes[static_cast<size_t>(shape)].get());
+    if (!old) return -1;
+    Mat4f m, mi;
+    for (int r = 0; r < 4; ++r)
+        for (int c = 0; c < 4; ++c) {
+            m(r, c) = l2w[4 * r + c];
+            if (w2l) mi(r, c) = w2l[4 * r + c];
+        }
+    const Transform xf = w2l ? Transform(m, mi) : Transform(m);
+    auto moved = std::make_shared<MeshInstance>(old->mesh(), xf, old->material());
+    rs->shapeIndex.erase(old);
+    rs->shapeIndex[moved.get()] = shape;
+    shapes[static_cast<size_t>(shape)] = std::move(moved);
+    rs->scene.buildAccelerator();
+    return 0;
 }
 
 // Scene::addShape of a Sphere (src/geometry/sphere.h).
@@ -1036,6 +1108,8 @@ int32_t ref_env_eval(void* s, const float* dirs, size_t n, float* out_rgb, float
 // The B200 device through the drop-in adapter (photon-engine_b200/adapter), driven by the
 // reference's own RenderSession (src/engine/render_session.cpp:17-101) on a reference Scene: the
 // parity check of the adapter itself.  One device per process, created on first use.
+static uint64_t g_adapterScene = 0; // RefScene::id of the scene the adapter device holds
+
 static std::unique_ptr<RenderDevice>& cudaAdapterDevice(std::string* err) {
     static std::unique_ptr<RenderDevice> dev;
     if (!dev) dev = createCudaRenderDevice(0, err);
@@ -1057,7 +1131,11 @@ int32_t ref_session_cuda(void* s, void* cam, const pe_settings* st, int32_t spp,
     }
     const DeviceFeatures f = dev->features();
     *features = (f.aovs ? 1 : 0) | (f.lightPasses ? 2 : 0) | (f.adaptiveSampling ? 4 : 0);
-    dev->setScene(std::shared_ptr<const Scene>(std::shared_ptr<const Scene>{}, &rs->scene));
+    // a session on the scene the adapter already holds keeps it (its updateScene edits included)
+    if (g_adapterScene != rs->id || !dev->hasScene()) {
+        dev->setScene(std::shared_ptr<const Scene>(std::shared_ptr<const Scene>{}, &rs->scene));
+        g_adapterScene = rs->id;
+    }
     if (!dev->hasScene()) {
         std::snprintf(err, errLen, "the adapter did not take the scene");
         return -2;
@@ -1109,6 +1187,10 @@ int32_t ref_session_cuda_update(void* s, int32_t kind, int32_t index, const floa
             }
         dev->updateScene(std::shared_ptr<const Scene>(std::shared_ptr<const Scene>{}, &rs->scene),
                          SceneUpdateKind::Lights);
+    } else if (kind == 3) {
+        // the scene's MeshInstances were moved (ref_scene_move_instance)
+        dev->updateScene(std::shared_ptr<const Scene>(std::shared_ptr<const Scene>{}, &rs->scene),
+                         SceneUpdateKind::Transforms);
     } else {
         return -4;
     }

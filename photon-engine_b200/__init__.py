@@ -5,9 +5,9 @@ host-side mirror of the reference's RenderDevice / RenderSession / Scene API ove
 """
 from . import _capi
 from .engine import (AovFilms, AreaLight, Background, BackgroundMode, CudaDevice, Dielectric, DeviceFeatures, DeviceInfo,
-                     DisneyMaterial, EnvironmentLight, Film, Lambertian, LightPass, Material, Mirror, OrthographicCamera, PerspectiveCamera, ThinLensCamera,
+                     DisneyMaterial, EnvironmentLight, Film, Lambertian, LightPass, Material, MeshInstance, Mirror, OrthographicCamera, PerspectiveCamera, ThinLensCamera,
                      PixelFilterType, RenderMode, RenderPassFilms, RenderServer, RenderSession, RenderSettings, RenderTargets, RequestStatus,
                      SampleBatchResult,
-                     Scene, SceneUpdateKind, SessionConfig, TriangleMesh, create_device, enumerate_devices, rel_mse)
+                     Scene, SceneUpdateKind, SessionConfig, Sphere, TriangleMesh, create_device, enumerate_devices, rel_mse)
 
 __all__ = [n for n in dir() if not n.startswith("_")] + ["_capi"]

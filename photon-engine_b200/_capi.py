@@ -184,6 +184,11 @@ SIGNATURES = {
     "pe_device_update_materials": (C.c_int32, [P, P]),
     "pe_device_update_lights": (C.c_int32, [P, P]),
     "pe_scene_set_area_light_radiance": (C.c_int32, [P, C.c_int32, C.POINTER(C.c_float)]),
+    "pe_scene_add_blas": (C.c_int32, [P, FP, C.c_uint32, FP, FP, UP, C.c_uint32]),
+    "pe_scene_add_instance": (C.c_int32, [P, C.c_int32, FP, FP, C.c_int32]),
+    "pe_scene_set_instance_transform": (C.c_int32, [P, C.c_int32, FP, FP]),
+    "pe_scene_refit": (C.c_int32, [P]),
+    "pe_device_update_transforms": (C.c_int32, [P, P]),
     "pe_scene_add_sphere": (C.c_int32, [P, C.POINTER(C.c_float), C.c_float, C.c_int32]),
     "pe_scene_add_mesh": (C.c_int32, [P, FP, C.c_uint32, FP, FP, UP, C.c_uint32, C.c_int32]),
     "pe_scene_add_area_light": (C.c_int32, [P, FP, FP, FP, FP, C.c_int32]),

@@ -4,8 +4,9 @@
 //            is one shape, an AreaLight's quad two, as scene.cpp:65-99 adds them), so shape, light
 //            and material numbering — and with it tags, names, light groups and links, the shadow
 //            catcher — are the reference's; then pe_scene_build and pe_device_set_scene.
-// updateScene Materials / Lights edit the kept pe_scene and re-send only that (SceneUpdateKind,
-//            render_device.h:34); anything else rebuilds.
+// updateScene Materials / Lights / Transforms edit the kept pe_scene and re-send only that
+//            (SceneUpdateKind, render_device.h:34; Transforms refits the top-level tree over the
+//            instances' BLASes); anything else rebuilds.
 // render     [firstSample, firstSample+count) in one device call into fresh batch arrays, added to
 //            the caller's films with Film::addBatch (film.cpp:119-137) as a GPU readback is; AOVs
 //            and render passes likewise; Cryptomatte ids per sample through CryptoFilm::addSample.
@@ -21,6 +22,7 @@
 #include "core/image/image.h"
 #include "engine/scene.h"
 #include "geometry/mesh.h"
+#include "geometry/mesh_instance.h"
 #include "geometry/sphere.h"
 #include "geometry/surface_interaction.h"
 #include "geometry/triangle.h"
@@ -62,6 +64,15 @@ struct PeScene {
     std::unordered_map<const Image*, int32_t> textures;
     std::unordered_map<const Material*, int32_t> materials;
     std::vector<std::pair<int32_t, const AreaLight*>> areaLights; // light index of each AreaLight
+    std::unordered_map<const TriangleMesh*, int32_t> blases;      // meshes of MeshInstances
+    // every shape as built: its pointer and, for a MeshInstance, its mesh and material (kept by
+    // value so a Transforms update can compare a scene whose old shapes are gone)
+    struct Placed {
+        const Shape* shape;
+        const TriangleMesh* mesh;
+        const Material* material;
+    };
+    std::vector<Placed> placed;
     std::string error;
 
     ~PeScene() { pe_scene_destroy(s); }
@@ -80,6 +91,34 @@ struct PeScene {
         if (t >= 0 && img->hasMipmaps() && pe_scene_build_texture_mipmaps(s, t) != PE_OK) t = -1;
         textures[img.get()] = t;
         return t;
+    }
+
+    // SceneUpdateKind::Transforms: `scene` holds the shapes as built except MeshInstances placed
+    // anew (same mesh and material, another matrix; a MeshInstance's matrix is fixed at
+    // construction, so a moved instance is a new object).  Sends their matrices; false when
+    // anything else changed, an instance moves with motion blur or emits light.
+    bool moveInstances(const Scene& scene) {
+        const auto& shapes = scene.shapes();
+        if (shapes.size() != placed.size()) return false;
+        for (size_t i = 0; i < shapes.size(); ++i) {
+            const Shape* now = shapes[i].get();
+            const auto* mi = dynamic_cast<const MeshInstance*>(now);
+            if (now == placed[i].shape && !mi) continue;
+            if (!mi || !placed[i].mesh || mi->mesh().get() != placed[i].mesh || mi->material() != placed[i].material ||
+                mi->hasMotion())
+                return false;
+            float l2w[16], w2l[16];
+            const Transform& xf = mi->transform0();
+            for (int r = 0; r < 4; ++r)
+                for (int c = 0; c < 4; ++c) {
+                    l2w[4 * r + c] = xf.matrix()(r, c);
+                    w2l[4 * r + c] = xf.inverseMatrix()(r, c);
+                }
+            if (pe_scene_set_instance_transform(s, static_cast<int32_t>(i), l2w, w2l) != PE_OK) return false;
+            placed[i].shape = now;
+        }
+        source = &scene;
+        return true;
     }
 
     // Material::* parameters as pe_material (the device clamps them as the setters do).
@@ -192,6 +231,8 @@ struct PeScene {
         for (size_t i = 0; i < shapes.size(); ++i) {
             const Shape* shape = shapes[i].get();
             const int32_t index = static_cast<int32_t>(i);
+            const auto* inst = dynamic_cast<const MeshInstance*>(shape);
+            placed.push_back({shape, inst ? inst->mesh().get() : nullptr, inst ? inst->material() : nullptr});
             if (auto* m = dynamic_cast<const TriangleMesh*>(shape)) {
                 const int32_t mat = material(m->material());
                 if (mat < 0) return false;
@@ -201,6 +242,44 @@ struct PeScene {
                 if (pe_scene_add_mesh(s, P.empty() ? nullptr : &P[0].x, static_cast<uint32_t>(P.size()),
                                       N.empty() ? nullptr : &N[0].x, UV.empty() ? nullptr : &UV[0].x,
                                       m->indices().data(), static_cast<uint32_t>(m->numTriangles()), mat) != PE_OK) {
+                    error = pe_last_error();
+                    return false;
+                }
+            } else if (auto* mi = dynamic_cast<const MeshInstance*>(shape)) {
+                // a MeshInstance: its mesh once as a BLAS, then the instance with both matrices
+                if (!mi->mesh()) {
+                    error = "a mesh instance without a mesh";
+                    return false;
+                }
+                const TriangleMesh* m = mi->mesh().get();
+                auto it = blases.find(m);
+                if (it == blases.end()) {
+                    const auto& P = m->positions();
+                    const auto& N = m->normals();
+                    const auto& UV = m->uvs();
+                    const int32_t b = pe_scene_add_blas(s, &P[0].x, static_cast<uint32_t>(P.size()),
+                                                        N.empty() ? nullptr : &N[0].x, UV.empty() ? nullptr : &UV[0].x,
+                                                        m->indices().data(), static_cast<uint32_t>(m->numTriangles()));
+                    if (b < 0) {
+                        error = pe_last_error();
+                        return false;
+                    }
+                    it = blases.emplace(m, b).first;
+                }
+                if (mi->hasMotion()) {
+                    error = "moving mesh instances (motion blur) are not carried";
+                    return false;
+                }
+                const int32_t mat = material(mi->material());
+                if (mat < 0) return false;
+                float l2w[16], w2l[16];
+                const Transform& xf = mi->transform0();
+                for (int r = 0; r < 4; ++r)
+                    for (int c = 0; c < 4; ++c) {
+                        l2w[4 * r + c] = xf.matrix()(r, c);
+                        w2l[4 * r + c] = xf.inverseMatrix()(r, c);
+                    }
+                if (pe_scene_add_instance(s, it->second, l2w, w2l, mat) != PE_OK) {
                     error = pe_last_error();
                     return false;
                 }
@@ -229,7 +308,7 @@ struct PeScene {
                 secondHalf = !secondHalf;
             } else {
                 error = "shape " + std::to_string(i) + " is of a kind the CUDA device does not trace "
-                        "(mesh instances and stand-alone triangles)";
+                        "(stand-alone triangles)";
                 return false;
             }
             if (shape == scene.shadowCatcherShape()) pe_scene_set_shadow_catcher(s, index);
@@ -343,7 +422,16 @@ public:
     }
 
     void updateScene(std::shared_ptr<const Scene> scene, SceneUpdateKind kind) override {
-        if (!m_scene || scene.get() != m_scene->source) return setScene(std::move(scene));
+        if (!scene || !m_scene) return setScene(std::move(scene));
+        if (kind == SceneUpdateKind::Transforms) {
+            // new instance matrices: the device refits its top-level tree, no BLAS is rebuilt
+            if (m_scene->moveInstances(*scene) && pe_device_update_transforms(m_dev, m_scene->s) == PE_OK) {
+                m_sceneRef = std::move(scene);
+                return;
+            }
+            return setScene(std::move(scene));
+        }
+        if (scene.get() != m_scene->source) return setScene(std::move(scene));
         bool ok = false;
         if (kind == SceneUpdateKind::Materials) {
             ok = true;
@@ -367,7 +455,7 @@ public:
             }
             ok = ok && pe_device_update_lights(m_dev, m_scene->s) == PE_OK;
         }
-        if (!ok) setScene(std::move(scene)); // the change needs a rebuild (or is a transform)
+        if (!ok) setScene(std::move(scene)); // the change needs a rebuild
     }
 
     SampleBatchResult render(const Camera& camera, const RenderSettings& settings, RenderTargets& targets,

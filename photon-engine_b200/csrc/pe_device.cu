@@ -907,9 +907,15 @@ __global__ void kTracePrimary(SceneGPU S, WaveSeg A, int nPix, int32_t* outShape
             outPrim[pix] = -1;
             outT[pix] = 0.0f;
         } else {
-            const float4 e2w = __ldg(&S.tris[3 * h.prim + 2]);
+            int rec = h.prim, shape;
+            if (isInstanceHit(h.prim)) {
+                const InstGPU& I = S.instances[instanceOfHit(h.prim)];
+                rec = I.recBase + localOfHit(h.prim);
+                shape = I.shape;
+            }
+            const float4 e2w = __ldg(&S.tris[3 * rec + 2]);
             const int g = static_cast<int>(__float_as_uint(e2w.w));
-            const int shape = __ldg(&S.triVerts[g]).w;
+            if (!isInstanceHit(h.prim)) shape = __ldg(&S.triVerts[g]).w;
             outShape[pix] = shape;
             outPrim[pix] = g - static_cast<int>(S.shapes[shape].firstTri);
             outT[pix] = h.t;
@@ -985,6 +991,7 @@ int32_t uploadScene(pe_device* d, const pe_scene* s, SceneGPU& G, std::vector<De
     const HostBuild& B = s->build;
     int32_t rc = 0;
     if ((rc = upload(d, bufs, G.nodes, B.nodes)) || (rc = upload(d, bufs, G.wide, B.wide)) ||
+        (rc = upload(d, bufs, G.instances, B.instances)) ||
         (rc = upload(d, bufs, G.tris, B.tris)) ||
         (rc = upload(d, bufs, G.triVerts, B.triVerts)) || (rc = upload(d, bufs, G.pos, B.pos)) ||
         (rc = upload(d, bufs, G.nrm, B.nrm)) || (rc = upload(d, bufs, G.uv, B.uv)) ||
@@ -1084,6 +1091,7 @@ int32_t uploadScene(pe_device* d, const pe_scene* s, SceneGPU& G, std::vector<De
         if ((rc = upload(d, bufs, G.textures, tex))) return rc;
     }
     G.nTextures = static_cast<int32_t>(s->textures.size());
+    G.nInstances = static_cast<int32_t>(B.instances.size());
     G.leanShading = leanShadingOf(G, B.materials);
     G.materialTypes = 0;
     for (const MatGPU& m : B.materials) G.materialTypes |= 1 << m.type;
@@ -1350,6 +1358,41 @@ int32_t pe_device_update_materials(pe_device* d, const pe_scene* s) {
                             s->build.materials.size() * sizeof(MatGPU), cudaMemcpyHostToDevice, d->stream));
     PE_CUDA(cudaStreamSynchronize(d->stream));
     d->scene.leanShading = leanShadingOf(d->scene, s->build.materials);
+    ++d->sceneSerial;
+    return PE_OK;
+}
+
+// SceneUpdateKind::Transforms: the top-level tree refitted on the host (pe_scene_refit) and only
+// its nodes, the instance table and the root box sent; BLASes stay as they are on the device.
+int32_t pe_device_update_transforms(pe_device* d, pe_scene* s) {
+    if (!d || !s) {
+        setError("pe_device_update_transforms: null argument");
+        return PE_ERR_INVALID;
+    }
+    if (!d->hasScene || d->sceneSrc != s || d->sceneVersion != s->version || !s->built) {
+        setError("pe_device_update_transforms: the device holds another build of the scene (call pe_device_set_scene)");
+        return PE_ERR_INVALID;
+    }
+    int32_t rc = pe_scene_refit(s);
+    if (rc) return rc;
+    const HostBuild& B = s->build;
+    PE_CUDA(cudaSetDevice(d->ordinal));
+    PE_CUDA(cudaStreamSynchronize(d->stream));
+    PE_CUDA(cudaStreamSynchronize(d->lanes[1].stream));
+    if (B.tlasInterior > 0)
+        PE_CUDA(cudaMemcpyAsync(const_cast<float4*>(d->scene.nodes), B.nodes.data(),
+                                static_cast<size_t>(B.tlasInterior) * 4 * sizeof(float4), cudaMemcpyHostToDevice, d->stream));
+    if (!B.tlasWideKids.empty())
+        PE_CUDA(cudaMemcpyAsync(const_cast<float4*>(d->scene.wide), B.wide.data(),
+                                B.tlasWideKids.size() * 8 * sizeof(float4), cudaMemcpyHostToDevice, d->stream));
+    if (!B.instances.empty())
+        PE_CUDA(cudaMemcpyAsync(const_cast<InstGPU*>(d->scene.instances), B.instances.data(),
+                                B.instances.size() * sizeof(InstGPU), cudaMemcpyHostToDevice, d->stream));
+    PE_CUDA(cudaStreamSynchronize(d->stream));
+    for (int k = 0; k < 3; ++k) {
+        d->scene.rootMin[k] = B.rootMin[k];
+        d->scene.rootMax[k] = B.rootMax[k];
+    }
     ++d->sceneSerial;
     return PE_OK;
 }

@@ -95,6 +95,90 @@ struct RefNode { // BVHNode (bvh.h:27-36): 32-byte depth-first node
     int count;   // leaf prim count, 0 for interior
 };
 
+// ---- transforms (src/core/math/mat.h, transform.cpp), row-major 4×4 ------------------------------
+constexpr uint32_t VIS_ALL_MASK = 0x1Fu; // a BLAS is traversed with every visibility bit (mesh_instance.cpp:110)
+constexpr int32_t kNoRoot = static_cast<int32_t>(0x80000000u);
+
+// Mat4f::inverse (mat.h:130-175): cofactors from the 2×2 minors of the top and bottom row pairs,
+// identity for a singular matrix.
+void mat4Inverse(const float* m, float* o) {
+    auto d = [&](int r, int c) { return m[4 * r + c]; };
+    const float s0 = d(0, 0) * d(1, 1) - d(1, 0) * d(0, 1);
+    const float s1 = d(0, 0) * d(1, 2) - d(1, 0) * d(0, 2);
+    const float s2 = d(0, 0) * d(1, 3) - d(1, 0) * d(0, 3);
+    const float s3 = d(0, 1) * d(1, 2) - d(1, 1) * d(0, 2);
+    const float s4 = d(0, 1) * d(1, 3) - d(1, 1) * d(0, 3);
+    const float s5 = d(0, 2) * d(1, 3) - d(1, 2) * d(0, 3);
+    const float c5 = d(2, 2) * d(3, 3) - d(3, 2) * d(2, 3);
+    const float c4 = d(2, 1) * d(3, 3) - d(3, 1) * d(2, 3);
+    const float c3 = d(2, 1) * d(3, 2) - d(3, 1) * d(2, 2);
+    const float c2 = d(2, 0) * d(3, 3) - d(3, 0) * d(2, 3);
+    const float c1 = d(2, 0) * d(3, 2) - d(3, 0) * d(2, 2);
+    const float c0 = d(2, 0) * d(3, 1) - d(3, 0) * d(2, 1);
+    const float det = s0 * c5 - s1 * c4 + s2 * c3 + s3 * c2 - s4 * c1 + s5 * c0;
+    if (det == 0.0f) {
+        for (int k = 0; k < 16; ++k) o[k] = (k % 5 == 0) ? 1.0f : 0.0f;
+        return;
+    }
+    const float id = 1.0f / det;
+    o[0] = (d(1, 1) * c5 - d(1, 2) * c4 + d(1, 3) * c3) * id;
+    o[1] = (-d(0, 1) * c5 + d(0, 2) * c4 - d(0, 3) * c3) * id;
+    o[2] = (d(3, 1) * s5 - d(3, 2) * s4 + d(3, 3) * s3) * id;
+    o[3] = (-d(2, 1) * s5 + d(2, 2) * s4 - d(2, 3) * s3) * id;
+    o[4] = (-d(1, 0) * c5 + d(1, 2) * c2 - d(1, 3) * c1) * id;
+    o[5] = (d(0, 0) * c5 - d(0, 2) * c2 + d(0, 3) * c1) * id;
+    o[6] = (-d(3, 0) * s5 + d(3, 2) * s2 - d(3, 3) * s1) * id;
+    o[7] = (d(2, 0) * s5 - d(2, 2) * s2 + d(2, 3) * s1) * id;
+    o[8] = (d(1, 0) * c4 - d(1, 1) * c2 + d(1, 3) * c0) * id;
+    o[9] = (-d(0, 0) * c4 + d(0, 1) * c2 - d(0, 3) * c0) * id;
+    o[10] = (d(3, 0) * s4 - d(3, 1) * s2 + d(3, 3) * s0) * id;
+    o[11] = (-d(2, 0) * s4 + d(2, 1) * s2 - d(2, 3) * s0) * id;
+    o[12] = (-d(1, 0) * c3 + d(1, 1) * c1 - d(1, 2) * c0) * id;
+    o[13] = (d(0, 0) * c3 - d(0, 1) * c1 + d(0, 2) * c0) * id;
+    o[14] = (-d(3, 0) * s3 + d(3, 1) * s1 - d(3, 2) * s0) * id;
+    o[15] = (d(2, 0) * s3 - d(2, 1) * s1 + d(2, 2) * s0) * id;
+}
+
+// Transform::transformPoint (transform.cpp:15-26).
+V3 xfPoint(const float* m, V3 p) {
+    const float x = m[0] * p.x + m[1] * p.y + m[2] * p.z + m[3];
+    const float y = m[4] * p.x + m[5] * p.y + m[6] * p.z + m[7];
+    const float z = m[8] * p.x + m[9] * p.y + m[10] * p.z + m[11];
+    const float w = m[12] * p.x + m[13] * p.y + m[14] * p.z + m[15];
+    if (w != 1.0f && w != 0.0f) {
+        const float iw = 1.0f / w;
+        return mk(x * iw, y * iw, z * iw);
+    }
+    return mk(x, y, z);
+}
+
+// Transform::transformAABB (transform.cpp:83-110): Arvo's bound of the transformed box.
+Box xfAABB(const float* m, const Box& b) {
+    float lo[3] = {m[3], m[7], m[11]}, hi[3] = {m[3], m[7], m[11]};
+    const float bl[3] = {b.lo.x, b.lo.y, b.lo.z}, bh[3] = {b.hi.x, b.hi.y, b.hi.z};
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) {
+            const float a = m[4 * i + j] * bl[j], c = m[4 * i + j] * bh[j];
+            if (a < c) {
+                lo[i] += a;
+                hi[i] += c;
+            } else {
+                lo[i] += c;
+                hi[i] += a;
+            }
+        }
+    Box r;
+    r.lo = mk(lo[0], lo[1], lo[2]);
+    r.hi = mk(hi[0], hi[1], hi[2]);
+    return r;
+}
+
+// det3x3 of mesh_instance.cpp:11-15.
+float det3x3(const float* m) {
+    return m[0] * (m[5] * m[10] - m[6] * m[9]) - m[1] * (m[4] * m[10] - m[6] * m[8]) +
+           m[2] * (m[4] * m[9] - m[5] * m[8]);
+}
+
 class SahBuilder {
 public:
     std::vector<BuildPrim> prims;
@@ -236,7 +320,7 @@ inline float4 f4(float x, float y, float z, float w) {
 // then the child references (interior: wide node index; leaf: ~(first << 8 | count-1)), then
 // the child count.  Nodes are written depth-first, a node before its children.
 static int collapseWide(const std::vector<RefNode>& ref, std::vector<float4>& out, int& maxDepth, int node = 0,
-                        int depth = 1) {
+                        int depth = 1, int recBase = 0, std::vector<int4>* kidsOut = nullptr) {
     maxDepth = std::max(maxDepth, depth);
     int kids[4] = {node + 1, ref[static_cast<size_t>(node)].offset, -1, -1};
     int n = 2;
@@ -259,6 +343,11 @@ static int collapseWide(const std::vector<RefNode>& ref, std::vector<float4>& ou
     }
     const size_t me = out.size() / 8;
     out.resize(out.size() + 8, float4{0.0f, 0.0f, 0.0f, 0.0f});
+    if (kidsOut) {
+        // the binary nodes a wide node's children are (for refitting its boxes in place)
+        if (kidsOut->size() <= me) kidsOut->resize(me + 1, int4{-1, -1, -1, -1});
+        (*kidsOut)[me] = int4{kids[0], kids[1], kids[2], kids[3]};
+    }
     float lo[3][4], hi[3][4];
     int32_t child[4] = {0, 0, 0, 0};
     for (int k = 0; k < 4; ++k) {
@@ -275,7 +364,8 @@ static int collapseWide(const std::vector<RefNode>& ref, std::vector<float4>& ou
         hi[0][k] = c.bounds.hi.x;
         hi[1][k] = c.bounds.hi.y;
         hi[2][k] = c.bounds.hi.z;
-        child[k] = c.count > 0 ? ~((c.offset << 8) | (c.count - 1)) : collapseWide(ref, out, maxDepth, kids[k], depth + 1);
+        child[k] = c.count > 0 ? ~(((c.offset + recBase) << 8) | (c.count - 1))
+                               : collapseWide(ref, out, maxDepth, kids[k], depth + 1, recBase, kidsOut);
     }
     float4* w = out.data() + me * 8;
     for (int a = 0; a < 3; ++a) {
@@ -286,6 +376,40 @@ static int collapseWide(const std::vector<RefNode>& ref, std::vector<float4>& ou
               bitsf(static_cast<uint32_t>(child[2])), bitsf(static_cast<uint32_t>(child[3])));
     w[7] = f4(bitsf(static_cast<uint32_t>(n)), 0.0f, 0.0f, 0.0f);
     return static_cast<int>(me);
+}
+
+// The binary tree's interior nodes as 64-byte child-box nodes appended to B.nodes (leaf
+// references offset by recBase); returns the root's reference (kNoRoot for a leaf too large).
+static int32_t emitBinaryNodes(const std::vector<RefNode>& ref, int recBase, HostBuild& B) {
+    const int base = static_cast<int>(B.nodes.size() / 4);
+    std::vector<int> gpuIndex(ref.size(), -1);
+    int nInterior = 0;
+    for (size_t i = 0; i < ref.size(); ++i) {
+        if (ref[i].count == 0) gpuIndex[i] = base + nInterior++;
+        else ++B.leaves;
+        if (ref[i].count > 256) {
+            setError("BVH leaf with more than 256 triangles");
+            return kNoRoot;
+        }
+    }
+    auto childRef = [&](int c) -> int {
+        const RefNode& n = ref[static_cast<size_t>(c)];
+        if (n.count > 0) return ~(((n.offset + recBase) << 8) | (n.count - 1));
+        return gpuIndex[static_cast<size_t>(c)];
+    };
+    B.nodes.resize(static_cast<size_t>(base + nInterior) * 4);
+    for (size_t i = 0; i < ref.size(); ++i) {
+        if (ref[i].count != 0) continue;
+        const int c0 = static_cast<int>(i) + 1, c1 = ref[i].offset;
+        const Box& b0 = ref[static_cast<size_t>(c0)].bounds;
+        const Box& b1 = ref[static_cast<size_t>(c1)].bounds;
+        const size_t k = static_cast<size_t>(gpuIndex[i]) * 4;
+        B.nodes[k + 0] = f4(b0.lo.x, b0.hi.x, b0.lo.y, b0.hi.y);
+        B.nodes[k + 1] = f4(b1.lo.x, b1.hi.x, b1.lo.y, b1.hi.y);
+        B.nodes[k + 2] = f4(b0.lo.z, b0.hi.z, b1.lo.z, b1.hi.z);
+        B.nodes[k + 3] = f4(bitsf(static_cast<uint32_t>(childRef(c0))), bitsf(static_cast<uint32_t>(childRef(c1))), 0.0f, 0.0f);
+    }
+    return ref[0].count > 0 ? childRef(0) : gpuIndex[0];
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -972,8 +1096,17 @@ static int32_t buildScene(pe_scene* s) {
     // shapes and global triangle / vertex numbering
     uint32_t nTris = 0, nVerts = 0;
     for (const HostShape& sh : s->shapes) {
-        nTris += sh.sphere ? 1u : static_cast<uint32_t>(sh.idx.size() / 3);
+        nTris += (sh.sphere || sh.blas >= 0) ? 1u : static_cast<uint32_t>(sh.idx.size() / 3);
         nVerts += static_cast<uint32_t>(sh.pos.size());
+    }
+    const uint32_t nTlas = nTris;
+    // BLAS triangles and vertices follow the top level's
+    std::vector<uint32_t> blasFirstTri(s->blases.size()), blasFirstVert(s->blases.size());
+    for (size_t b = 0; b < s->blases.size(); ++b) {
+        blasFirstTri[b] = nTris;
+        blasFirstVert[b] = nVerts;
+        nTris += static_cast<uint32_t>(s->blases[b].idx.size() / 3);
+        nVerts += static_cast<uint32_t>(s->blases[b].pos.size());
     }
     if (nTris >= (1u << 23)) {
         setError("scene has " + std::to_string(nTris) + " triangles; the flattened BVH encodes at most 8388607");
@@ -1044,6 +1177,21 @@ static int32_t buildScene(pe_scene* s) {
             uv.y = v < sh.uv.size() ? sh.uv[v].y : 0.0f;
             B.uv[v0 + v] = uv;
         }
+        if (sh.blas >= 0) {
+            // one top-level primitive; its bounds are the BLAS's box under the transform
+            // (Transform::transformAABB, Arvo's method, transform.cpp:83-110)
+            B.triVerts[t0] = int4{-2, sh.blas, 0, static_cast<int>(si)};
+            const HostBlas& hb = s->blases[static_cast<size_t>(sh.blas)];
+            Box lb;
+            for (const V3& p : hb.pos) lb = lb.merged(Box{p, p});
+            triBounds[t0] = xfAABB(sh.l2w, lb);
+            triMask[t0] = sh.mask;
+            info.firstTri = blasFirstTri[static_cast<size_t>(sh.blas)];
+            t0 += 1;
+            const MatGPU& mi = s->materials[static_cast<size_t>(sh.material)];
+            if (mi.flags & MF_TRANSMITS_SHADOWS) B.hasShadowTransmitters = true;
+            continue;
+        }
         if (sh.sphere) {
             // one primitive, no vertices: its triVerts entry carries only the shape
             B.triVerts[t0] = int4{-1, -1, -1, static_cast<int>(si)};
@@ -1077,6 +1225,22 @@ static int32_t buildScene(pe_scene* s) {
         const MatGPU& mg = s->materials[static_cast<size_t>(sh.material)];
         if (mg.flags & MF_TRANSMITS_SHADOWS) B.hasShadowTransmitters = true;
     }
+    for (size_t b = 0; b < s->blases.size(); ++b) {
+        const HostBlas& hb = s->blases[b];
+        const uint32_t vb = blasFirstVert[b], tb = blasFirstTri[b];
+        for (size_t v = 0; v < hb.pos.size(); ++v) {
+            B.pos[vb + v] = f4(hb.pos[v].x, hb.pos[v].y, hb.pos[v].z, 0.0f);
+            const V3 n = v < hb.nrm.size() ? hb.nrm[v] : mk(0.0f);
+            B.nrm[vb + v] = f4(n.x, n.y, n.z, 0.0f);
+            float2 uv;
+            uv.x = v < hb.uv.size() ? hb.uv[v].x : 0.0f;
+            uv.y = v < hb.uv.size() ? hb.uv[v].y : 0.0f;
+            B.uv[vb + v] = uv;
+        }
+        for (size_t t = 0; t < hb.idx.size() / 3; ++t)
+            B.triVerts[tb + t] = int4{static_cast<int>(vb + hb.idx[3 * t]), static_cast<int>(vb + hb.idx[3 * t + 1]),
+                                      static_cast<int>(vb + hb.idx[3 * t + 2]), -1};
+    }
     for (const MatGPU& m : s->materials)
         if (m.flags & MF_TRANSMITS_SHADOWS) B.hasShadowTransmitters = true; // Scene::retainMaterial
     for (const MatGPU& m : s->materials) {
@@ -1086,12 +1250,36 @@ static int32_t buildScene(pe_scene* s) {
     }
 
     // SAH BVH
-    if (nTris > 0) {
+    B.tlasPrims = nTlas;
+    B.instances.clear();
+    std::vector<int> instOfShape(s->shapes.size(), -1);
+    for (size_t si = 0; si < s->shapes.size(); ++si)
+        if (s->shapes[si].blas >= 0) {
+            if (static_cast<int32_t>(B.instances.size()) >= kMaxInstances) {
+                setError("scene has more than " + std::to_string(kMaxInstances) + " mesh instances");
+                return PE_ERR_LIMIT;
+            }
+            instOfShape[si] = static_cast<int>(B.instances.size());
+            B.instances.emplace_back();
+        }
+    // the BVH leaf record of a triangle (lean Möller–Trumbore data), in local or world space
+    auto triRecord = [&](size_t i, uint32_t g, uint32_t meta) {
+        const int4 tv = B.triVerts[g];
+        const V3 p0 = mk(B.pos[tv.x].x, B.pos[tv.x].y, B.pos[tv.x].z);
+        const V3 p1 = mk(B.pos[tv.y].x, B.pos[tv.y].y, B.pos[tv.y].z);
+        const V3 p2 = mk(B.pos[tv.z].x, B.pos[tv.z].y, B.pos[tv.z].z);
+        const V3 e1 = p1 - p0, e2 = p2 - p0;
+        const float eps = 1e-14f * len2(e1) * len2(e2);
+        B.tris[3 * i + 0] = f4(p0.x, p0.y, p0.z, eps);
+        B.tris[3 * i + 1] = f4(e1.x, e1.y, e1.z, bitsf(meta));
+        B.tris[3 * i + 2] = f4(e2.x, e2.y, e2.z, bitsf(g));
+    };
+    if (nTlas > 0) {
         SahBuilder sb;
-        sb.prims.reserve(nTris);
-        for (uint32_t i = 0; i < nTris; ++i) sb.prims.emplace_back(i, triBounds[i]);
-        sb.ordered.reserve(nTris);
-        BuildNode* root = sb.build(0, static_cast<int>(nTris));
+        sb.prims.reserve(nTlas);
+        for (uint32_t i = 0; i < nTlas; ++i) sb.prims.emplace_back(i, triBounds[i]);
+        sb.ordered.reserve(nTlas);
+        BuildNode* root = sb.build(0, static_cast<int>(nTlas));
         std::vector<RefNode> ref(static_cast<size_t>(sb.total));
         int offset = 0;
         sb.flatten(root, ref, &offset, 0, B.maxDepth);
@@ -1105,6 +1293,16 @@ static int32_t buildScene(pe_scene* s) {
         for (size_t i = 0; i < sb.ordered.size(); ++i) {
             const uint32_t g = static_cast<uint32_t>(sb.ordered[i]);
             const int4 tv = B.triVerts[g];
+            if (tv.x == -2) {
+                // mesh instance: its index; the instance's visibility mask and material type
+                const HostShape& sh = s->shapes[static_cast<size_t>(tv.w)];
+                const uint32_t matType = static_cast<uint32_t>(s->materials[static_cast<size_t>(sh.material)].type);
+                B.tris[3 * i + 0] = f4(bitsf(static_cast<uint32_t>(instOfShape[static_cast<size_t>(tv.w)])), 0.0f, 0.0f, 0.0f);
+                B.tris[3 * i + 1] = f4(0.0f, 0.0f, 0.0f,
+                                       bitsf(static_cast<uint32_t>(triMask[g]) | (matType << 8) | PRIM_INSTANCE));
+                B.tris[3 * i + 2] = f4(0.0f, 0.0f, 0.0f, bitsf(g));
+                continue;
+            }
             if (tv.x < 0) {
                 // analytic sphere: (centre, radius), meta with the sphere bit, global id
                 const HostShape& sh = s->shapes[static_cast<size_t>(tv.w)];
@@ -1115,50 +1313,31 @@ static int32_t buildScene(pe_scene* s) {
                 B.tris[3 * i + 2] = f4(0.0f, 0.0f, 0.0f, bitsf(g));
                 continue;
             }
-            const V3 p0 = mk(B.pos[tv.x].x, B.pos[tv.x].y, B.pos[tv.x].z);
-            const V3 p1 = mk(B.pos[tv.y].x, B.pos[tv.y].y, B.pos[tv.y].z);
-            const V3 p2 = mk(B.pos[tv.z].x, B.pos[tv.z].y, B.pos[tv.z].z);
-            const V3 e1 = p1 - p0, e2 = p2 - p0;
-            const float eps = 1e-14f * len2(e1) * len2(e2);
-            B.tris[3 * i + 0] = f4(p0.x, p0.y, p0.z, eps);
             // w: visibility mask (bits 0-7) and material type (bits 8-15; the shading key)
             const uint32_t matType = static_cast<uint32_t>(s->materials[static_cast<size_t>(
                 s->shapes[static_cast<size_t>(tv.w)].material)].type);
-            B.tris[3 * i + 1] = f4(e1.x, e1.y, e1.z, bitsf(static_cast<uint32_t>(triMask[g]) | (matType << 8)));
-            B.tris[3 * i + 2] = f4(e2.x, e2.y, e2.z, bitsf(g));
+            triRecord(i, g, static_cast<uint32_t>(triMask[g]) | (matType << 8));
         }
         // interior nodes → 64-byte child-box nodes
-        std::vector<int> gpuIndex(ref.size(), -1);
-        int nInterior = 0;
-        for (size_t i = 0; i < ref.size(); ++i) {
-            if (ref[i].count == 0) gpuIndex[i] = nInterior++;
-            else ++B.leaves;
-            if (ref[i].count > 256) {
-                setError("BVH leaf with more than 256 triangles");
-                return PE_ERR_LIMIT;
-            }
-        }
-        auto childRef = [&](int c) -> int {
-            const RefNode& n = ref[static_cast<size_t>(c)];
-            if (n.count > 0) return ~((n.offset << 8) | (n.count - 1));
-            return gpuIndex[static_cast<size_t>(c)];
-        };
-        B.nodes.resize(static_cast<size_t>(nInterior) * 4);
-        for (size_t i = 0; i < ref.size(); ++i) {
-            if (ref[i].count != 0) continue;
-            const int c0 = static_cast<int>(i) + 1, c1 = ref[i].offset;
-            const Box& b0 = ref[static_cast<size_t>(c0)].bounds;
-            const Box& b1 = ref[static_cast<size_t>(c1)].bounds;
-            const size_t k = static_cast<size_t>(gpuIndex[i]) * 4;
-            B.nodes[k + 0] = f4(b0.lo.x, b0.hi.x, b0.lo.y, b0.hi.y);
-            B.nodes[k + 1] = f4(b1.lo.x, b1.hi.x, b1.lo.y, b1.hi.y);
-            B.nodes[k + 2] = f4(b0.lo.z, b0.hi.z, b1.lo.z, b1.hi.z);
-            B.nodes[k + 3] = f4(bitsf(static_cast<uint32_t>(childRef(c0))), bitsf(static_cast<uint32_t>(childRef(c1))), 0.0f, 0.0f);
-        }
+        if (emitBinaryNodes(ref, 0, B) == kNoRoot) return PE_ERR_LIMIT;
         // 4-wide nodes for the traversal kernels (the same leaves, boxes and leaf order)
+        B.tlasRef.resize(ref.size());
+        for (size_t i = 0; i < ref.size(); ++i) {
+            const Box& b = ref[i].bounds;
+            B.tlasRef[i] = HostBuild::TreeNode{{b.lo.x, b.lo.y, b.lo.z}, {b.hi.x, b.hi.y, b.hi.z}, ref[i].offset, ref[i].count};
+        }
+        B.tlasOrdered.assign(sb.ordered.begin(), sb.ordered.end());
+        B.tlasPrimBounds.resize(6 * static_cast<size_t>(nTlas));
+        for (uint32_t i = 0; i < nTlas; ++i) {
+            const Box& b = triBounds[i];
+            const float v[6] = {b.lo.x, b.lo.y, b.lo.z, b.hi.x, b.hi.y, b.hi.z};
+            std::copy(v, v + 6, &B.tlasPrimBounds[6 * i]);
+        }
+        B.tlasInterior = static_cast<int32_t>(B.nodes.size() / 4);
+        B.tlasWideKids.clear();
         if (ref[0].count == 0) {
             int depth4 = 0;
-            collapseWide(ref, B.wide, depth4);
+            collapseWide(ref, B.wide, depth4, 0, 1, 0, &B.tlasWideKids);
             B.wideDepth = depth4;
             if (3 * depth4 + 1 > kWideStack) {
                 setError("4-wide BVH depth " + std::to_string(depth4) + " exceeds the traversal stack of " +
@@ -1175,6 +1354,77 @@ static int32_t buildScene(pe_scene* s) {
         B.rootMax[0] = ref[0].bounds.hi.x;
         B.rootMax[1] = ref[0].bounds.hi.y;
         B.rootMax[2] = ref[0].bounds.hi.z;
+    }
+    // BLASes: each mesh kept for instancing gets its own tree over its triangles in local space
+    // (BVH::buildMesh, bvh.cpp:58-90), or — at most 16 triangles — one leaf in index order, the
+    // order TriangleMesh::intersectAccelerated tests small meshes in (mesh.cpp:151-155).  Their
+    // leaf records follow the top level's; their nodes follow the top level's nodes.
+    std::vector<int32_t> blasRootB(s->blases.size()), blasRootW(s->blases.size()), blasRec(s->blases.size());
+    uint32_t rec = nTlas;
+    if (!s->blases.empty()) B.tris.resize(static_cast<size_t>(nTris) * 3);
+    for (size_t b = 0; b < s->blases.size(); ++b) {
+        const HostBlas& hb = s->blases[b];
+        const uint32_t n = static_cast<uint32_t>(hb.idx.size() / 3), tb = blasFirstTri[b];
+        blasRec[b] = static_cast<int32_t>(rec);
+        if (n <= 16) {
+            for (uint32_t k = 0; k < n; ++k) triRecord(rec + k, tb + k, VIS_ALL_MASK);
+            blasRootB[b] = blasRootW[b] = static_cast<int32_t>(~((rec << 8) | (n - 1)));
+        } else {
+            SahBuilder bb;
+            bb.prims.reserve(n);
+            for (uint32_t k = 0; k < n; ++k) {
+                const V3 p0 = hb.pos[hb.idx[3 * k]], p1 = hb.pos[hb.idx[3 * k + 1]], p2 = hb.pos[hb.idx[3 * k + 2]];
+                Box bx;
+                bx.lo = vmin(vmin(p0, p1), p2);
+                bx.hi = vmax(vmax(p0, p1), p2);
+                bb.prims.emplace_back(k, bx);
+            }
+            bb.ordered.reserve(n);
+            BuildNode* root = bb.build(0, static_cast<int>(n));
+            std::vector<RefNode> bref(static_cast<size_t>(bb.total));
+            int offset = 0, depth = 0;
+            bb.flatten(root, bref, &offset, 0, depth);
+            if (depth + 2 > kMaxStack) {
+                setError("BLAS depth " + std::to_string(depth) + " exceeds the traversal stack of " + std::to_string(kMaxStack));
+                return PE_ERR_LIMIT;
+            }
+            for (size_t i = 0; i < bb.ordered.size(); ++i)
+                triRecord(rec + i, tb + static_cast<uint32_t>(bb.ordered[i]), VIS_ALL_MASK);
+            const int32_t rb = emitBinaryNodes(bref, static_cast<int>(rec), B);
+            if (rb == kNoRoot) return PE_ERR_LIMIT;
+            blasRootB[b] = rb;
+            if (bref[0].count == 0) {
+                int depth4 = 0;
+                blasRootW[b] = collapseWide(bref, B.wide, depth4, 0, 1, static_cast<int>(rec));
+                if (3 * depth4 + 1 > kWideStack) {
+                    setError("4-wide BLAS depth " + std::to_string(depth4) + " exceeds the traversal stack of " +
+                             std::to_string(kWideStack));
+                    return PE_ERR_LIMIT;
+                }
+            } else {
+                blasRootW[b] = rb;
+            }
+        }
+        rec += n;
+    }
+    for (size_t si = 0; si < s->shapes.size(); ++si) {
+        const int ii = instOfShape[si];
+        if (ii < 0) continue;
+        const HostShape& sh = s->shapes[si];
+        InstGPU& g = B.instances[static_cast<size_t>(ii)];
+        std::memset(&g, 0, sizeof(g));
+        for (int r = 0; r < 4; ++r) {
+            g.w2l[r] = f4(sh.w2l[4 * r], sh.w2l[4 * r + 1], sh.w2l[4 * r + 2], sh.w2l[4 * r + 3]);
+            g.l2w[r] = f4(sh.l2w[4 * r], sh.l2w[4 * r + 1], sh.l2w[4 * r + 2], sh.l2w[4 * r + 3]);
+        }
+        const size_t bl = static_cast<size_t>(sh.blas);
+        g.rootBinary = blasRootB[bl];
+        g.rootWide = blasRootW[bl];
+        g.recBase = blasRec[bl];
+        g.firstTri = static_cast<int32_t>(blasFirstTri[bl]);
+        g.shape = static_cast<int32_t>(si);
+        g.material = sh.material;
+        g.uvScale = std::cbrt(std::max(std::fabs(det3x3(sh.l2w)), 1e-12f));
     }
 
     buildLightSampler(s, B);
@@ -1447,6 +1697,210 @@ int32_t pe_scene_add_mesh(pe_scene* s, const float* positions, uint32_t nv, cons
     }
     s->shapes.push_back(std::move(sh));
     s->built = false;
+    return PE_OK;
+}
+
+int32_t pe_scene_add_blas(pe_scene* s, const float* positions, uint32_t nv, const float* normals, const float* uvs,
+                          const uint32_t* indices, uint32_t ntri) {
+    if (!s || !positions || !indices || nv == 0 || ntri == 0) {
+        setError("pe_scene_add_blas: a mesh for instancing needs vertices and triangles");
+        return -PE_ERR_INVALID;
+    }
+    if (ntri > static_cast<uint32_t>(kMaxBlasRecords)) {
+        setError("pe_scene_add_blas: at most " + std::to_string(kMaxBlasRecords) + " triangles a mesh for instancing");
+        return -PE_ERR_LIMIT;
+    }
+    for (uint64_t i = 0; i < 3ull * ntri; ++i)
+        if (indices[i] >= nv) {
+            setError("pe_scene_add_blas: vertex index out of range");
+            return -PE_ERR_INVALID;
+        }
+    HostBlas hb;
+    hb.pos.resize(nv);
+    for (uint32_t i = 0; i < nv; ++i) hb.pos[i] = mk(positions[3 * i], positions[3 * i + 1], positions[3 * i + 2]);
+    hb.idx.assign(indices, indices + 3ull * ntri);
+    if (normals) {
+        hb.nrm.resize(nv);
+        for (uint32_t i = 0; i < nv; ++i) hb.nrm[i] = mk(normals[3 * i], normals[3 * i + 1], normals[3 * i + 2]);
+    } else {
+        // TriangleMesh::calculateNormals (mesh.cpp:30-55)
+        hb.nrm.assign(nv, mk(0.0f));
+        for (size_t i = 0; i < hb.idx.size(); i += 3) {
+            const uint32_t a = hb.idx[i], b = hb.idx[i + 1], c = hb.idx[i + 2];
+            const V3 n = cross(hb.pos[b] - hb.pos[a], hb.pos[c] - hb.pos[a]);
+            hb.nrm[a] += n;
+            hb.nrm[b] += n;
+            hb.nrm[c] += n;
+        }
+        for (V3& n : hb.nrm)
+            if (len2(n) > 0.0f) n = normalize(n);
+    }
+    hb.flags = SF_HAS_NORMALS;
+    if (uvs) {
+        hb.uv.resize(nv);
+        for (uint32_t i = 0; i < nv; ++i) hb.uv[i] = mk2(uvs[2 * i], uvs[2 * i + 1]);
+        hb.flags |= SF_HAS_UVS;
+    }
+    s->blases.push_back(std::move(hb));
+    s->built = false;
+    return static_cast<int32_t>(s->blases.size() - 1);
+}
+
+int32_t pe_scene_add_instance(pe_scene* s, int32_t blas, const float localToWorld[16], const float worldToLocal[16],
+                              int32_t material) {
+    if (!s || !localToWorld) {
+        setError("pe_scene_add_instance: null argument");
+        return PE_ERR_INVALID;
+    }
+    if (blas < 0 || blas >= static_cast<int32_t>(s->blases.size())) {
+        setError("pe_scene_add_instance: no such mesh for instancing");
+        return PE_ERR_INVALID;
+    }
+    if (material < 0 || material >= static_cast<int32_t>(s->materials.size())) {
+        setError("pe_scene_add_instance: material index out of range");
+        return PE_ERR_INVALID;
+    }
+    HostShape sh;
+    sh.blas = blas;
+    sh.material = material;
+    std::memcpy(sh.l2w, localToWorld, sizeof(sh.l2w));
+    if (worldToLocal) std::memcpy(sh.w2l, worldToLocal, sizeof(sh.w2l));
+    else mat4Inverse(sh.l2w, sh.w2l);
+    const HostBlas& hb = s->blases[static_cast<size_t>(blas)];
+    sh.flags = SF_INSTANCE | hb.flags;
+    // An emissive instance: one TriangleLight per triangle of its mesh, placed by the transform
+    // (Scene::addShape, scene.cpp:23-41).
+    const MatGPU& mg = s->materials[static_cast<size_t>(material)];
+    if (mg.flags & MF_EMISSIVE) {
+        sh.emitter = static_cast<int32_t>(s->lights.size());
+        for (size_t t = 0; t < hb.idx.size() / 3; ++t) {
+            const V3 p0 = xfPoint(sh.l2w, hb.pos[hb.idx[3 * t]]), p1 = xfPoint(sh.l2w, hb.pos[hb.idx[3 * t + 1]]),
+                     p2 = xfPoint(sh.l2w, hb.pos[hb.idx[3 * t + 2]]);
+            LightGPU l;
+            std::memset(&l, 0, sizeof(l));
+            l.type = LT_TRIANGLE;
+            const V3 n = cross(p1 - p0, p2 - p0);
+            const float len = length(n);
+            l.area = 0.5f * len;
+            const V3 nn = len > 0.0f ? n / len : mk(0.0f, 1.0f, 0.0f);
+            l.p0[0] = p0.x; l.p0[1] = p0.y; l.p0[2] = p0.z;
+            l.p1[0] = p1.x; l.p1[1] = p1.y; l.p1[2] = p1.z;
+            l.p2[0] = p2.x; l.p2[1] = p2.y; l.p2[2] = p2.z;
+            l.normal[0] = nn.x; l.normal[1] = nn.y; l.normal[2] = nn.z;
+            l.radiance_r = mg.emission[0];
+            l.radiance_g = mg.emission[1];
+            l.radiance_b = mg.emission[2];
+            s->lights.push_back(l);
+        }
+    }
+    s->shapes.push_back(std::move(sh));
+    s->built = false;
+    return PE_OK;
+}
+
+int32_t pe_scene_set_instance_transform(pe_scene* s, int32_t shape, const float localToWorld[16],
+                                        const float worldToLocal[16]) {
+    if (!s || !localToWorld || shape < 0 || shape >= static_cast<int32_t>(s->shapes.size()) ||
+        s->shapes[static_cast<size_t>(shape)].blas < 0) {
+        setError("pe_scene_set_instance_transform: not a mesh instance");
+        return PE_ERR_INVALID;
+    }
+    HostShape& sh = s->shapes[static_cast<size_t>(shape)];
+    if (sh.emitter >= 0) {
+        setError("pe_scene_set_instance_transform: an emissive instance moves its lights; rebuild the scene");
+        return PE_ERR_LIMIT;
+    }
+    std::memcpy(sh.l2w, localToWorld, sizeof(sh.l2w));
+    if (worldToLocal) std::memcpy(sh.w2l, worldToLocal, sizeof(sh.w2l));
+    else mat4Inverse(sh.l2w, sh.w2l);
+    ++s->transformVersion;
+    return PE_OK;
+}
+
+// Refits the built scene's top-level tree after pe_scene_set_instance_transform: each moved
+// instance's box again (transformAABB of its BLAS box), leaf and interior boxes recomputed bottom
+// up with the tree's shape and leaf order kept, the binary and 4-wide top-level nodes and the
+// instance table rewritten in place.  No BLAS is touched.
+int32_t pe_scene_refit(pe_scene* s) {
+    if (!s || !s->built) {
+        setError("pe_scene_refit: the scene is not built");
+        return PE_ERR_INVALID;
+    }
+    HostBuild& B = s->build;
+    if (B.tlasRef.empty()) return PE_OK;
+    // primitive boxes: moved instances from their new matrices
+    int ii = 0;
+    std::vector<int> instShape; // instance shapes in shape order, as the instance table holds them
+    for (size_t si = 0; si < s->shapes.size(); ++si)
+        if (s->shapes[si].blas >= 0) instShape.push_back(static_cast<int>(si));
+    for (uint32_t p = 0; p < B.tlasPrims; ++p) {
+        const int4 tv = B.triVerts[p];
+        if (tv.x != -2) continue;
+        const HostShape& sh = s->shapes[static_cast<size_t>(tv.w)];
+        const HostBlas& hb = s->blases[static_cast<size_t>(sh.blas)];
+        Box lb;
+        for (const V3& q : hb.pos) lb = lb.merged(Box{q, q});
+        const Box wb = xfAABB(sh.l2w, lb);
+        const float v[6] = {wb.lo.x, wb.lo.y, wb.lo.z, wb.hi.x, wb.hi.y, wb.hi.z};
+        std::copy(v, v + 6, &B.tlasPrimBounds[6 * p]);
+    }
+    // bottom up: a node's children follow it in depth-first order
+    std::vector<Box> nb(B.tlasRef.size());
+    for (size_t k = B.tlasRef.size(); k-- > 0;) {
+        const HostBuild::TreeNode& n = B.tlasRef[k];
+        Box b;
+        if (n.count > 0) {
+            for (int j = 0; j < n.count; ++j) {
+                const float* v = &B.tlasPrimBounds[6 * B.tlasOrdered[static_cast<size_t>(n.offset + j)]];
+                b = b.merged(Box{mk(v[0], v[1], v[2]), mk(v[3], v[4], v[5])});
+            }
+        } else {
+            b = nb[k + 1].merged(nb[static_cast<size_t>(n.offset)]);
+        }
+        nb[k] = b;
+        HostBuild::TreeNode& w = B.tlasRef[k];
+        w.lo[0] = b.lo.x; w.lo[1] = b.lo.y; w.lo[2] = b.lo.z;
+        w.hi[0] = b.hi.x; w.hi[1] = b.hi.y; w.hi[2] = b.hi.z;
+    }
+    // binary interior nodes, in the order they were emitted
+    int gi = 0;
+    for (size_t k = 0; k < B.tlasRef.size(); ++k) {
+        if (B.tlasRef[k].count != 0) continue;
+        const Box& b0 = nb[k + 1];
+        const Box& b1 = nb[static_cast<size_t>(B.tlasRef[k].offset)];
+        float4* q = &B.nodes[static_cast<size_t>(gi++) * 4];
+        q[0] = f4(b0.lo.x, b0.hi.x, b0.lo.y, b0.hi.y);
+        q[1] = f4(b1.lo.x, b1.hi.x, b1.lo.y, b1.hi.y);
+        q[2] = f4(b0.lo.z, b0.hi.z, b1.lo.z, b1.hi.z);
+    }
+    // 4-wide nodes of the top level
+    for (size_t w = 0; w < B.tlasWideKids.size(); ++w) {
+        const int kids[4] = {B.tlasWideKids[w].x, B.tlasWideKids[w].y, B.tlasWideKids[w].z, B.tlasWideKids[w].w};
+        float lo[3][4] = {}, hi[3][4] = {};
+        for (int c = 0; c < 4; ++c) {
+            if (kids[c] < 0) continue;
+            const Box& b = nb[static_cast<size_t>(kids[c])];
+            lo[0][c] = b.lo.x; lo[1][c] = b.lo.y; lo[2][c] = b.lo.z;
+            hi[0][c] = b.hi.x; hi[1][c] = b.hi.y; hi[2][c] = b.hi.z;
+        }
+        float4* q = &B.wide[w * 8];
+        for (int a = 0; a < 3; ++a) {
+            q[2 * a] = f4(lo[a][0], lo[a][1], lo[a][2], lo[a][3]);
+            q[2 * a + 1] = f4(hi[a][0], hi[a][1], hi[a][2], hi[a][3]);
+        }
+    }
+    B.rootMin[0] = nb[0].lo.x; B.rootMin[1] = nb[0].lo.y; B.rootMin[2] = nb[0].lo.z;
+    B.rootMax[0] = nb[0].hi.x; B.rootMax[1] = nb[0].hi.y; B.rootMax[2] = nb[0].hi.z;
+    for (int si : instShape) {
+        const HostShape& sh = s->shapes[static_cast<size_t>(si)];
+        InstGPU& g = B.instances[static_cast<size_t>(ii++)];
+        for (int r = 0; r < 4; ++r) {
+            g.w2l[r] = f4(sh.w2l[4 * r], sh.w2l[4 * r + 1], sh.w2l[4 * r + 2], sh.w2l[4 * r + 3]);
+            g.l2w[r] = f4(sh.l2w[4 * r], sh.l2w[4 * r + 1], sh.l2w[4 * r + 2], sh.l2w[4 * r + 3]);
+        }
+        g.uvScale = std::cbrt(std::max(std::fabs(det3x3(sh.l2w)), 1e-12f));
+    }
+    ++s->refitVersion;
     return PE_OK;
 }
 
@@ -1810,7 +2264,10 @@ int32_t pe_scene_get_info(const pe_scene* s, pe_scene_info* out) {
     }
     std::memset(out, 0, sizeof(*out));
     const HostBuild& B = s->build;
-    out->triangles = B.triVerts.size();
+    // triangles stored once: scene meshes and each instanced mesh's BLAS (sphere and instance
+    // primitives are not triangles)
+    out->triangles = static_cast<uint64_t>(
+        std::count_if(B.triVerts.begin(), B.triVerts.end(), [](const int4& v) { return v.x >= 0; }));
     out->bvh_nodes = B.nodes.size() / 4;
     out->bvh_leaves = B.leaves;
     out->lights = B.lights.size();
@@ -1818,7 +2275,8 @@ int32_t pe_scene_get_info(const pe_scene* s, pe_scene_info* out) {
     out->has_environment = s->env.present ? 1 : 0;
     out->light_sampler_mode = B.lightMode;
     out->device_bytes = B.nodes.size() * sizeof(float4) + B.tris.size() * sizeof(float4) +
-                        B.triVerts.size() * sizeof(int4) + B.pos.size() * sizeof(float4) * 2 + B.uv.size() * sizeof(float2);
+                        B.triVerts.size() * sizeof(int4) + B.pos.size() * sizeof(float4) * 2 + B.uv.size() * sizeof(float2) +
+                        B.wide.size() * sizeof(float4) + B.instances.size() * sizeof(InstGPU);
     return s->built ? PE_OK : PE_ERR_INVALID;
 }
 

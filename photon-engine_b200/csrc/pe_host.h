@@ -20,6 +20,16 @@ struct HostShape {
     bool sphere = false;        // an analytic sphere (Sphere, src/geometry/sphere.h): one primitive
     V3 center{0.0f, 0.0f, 0.0f};
     float radius = 0.0f;
+    int32_t blas = -1;          // a MeshInstance of this BLAS (src/geometry/mesh_instance.h): one primitive
+    float l2w[16] = {}, w2l[16] = {}; // its local-to-world matrix and inverse, row-major
+};
+
+// A mesh kept for instancing: its own BVH (BLAS), shared by its instances.
+struct HostBlas {
+    std::vector<V3> pos, nrm;
+    std::vector<V2> uv;
+    std::vector<uint32_t> idx;
+    uint32_t flags = 0;         // SF_HAS_NORMALS / SF_HAS_UVS
 };
 
 struct HostEnv {
@@ -49,6 +59,18 @@ struct HostBuild {
     std::vector<float4> nodes;       // 4 per interior node
     std::vector<float4> wide;        // 8 per 4-wide node (traversal kernels)
     int wideDepth = 0;
+    std::vector<InstGPU> instances;  // per MeshInstance shape (in shape order)
+    uint32_t tlasPrims = 0;          // leaf records of the top-level tree; BLAS records follow
+    // the top-level tree as built, for refitting its boxes after instance transforms change
+    struct TreeNode {
+        float lo[3], hi[3];
+        int32_t offset, count;   // leaf: first leaf-order primitive and count; interior: second child, 0
+    };
+    std::vector<TreeNode> tlasRef;
+    std::vector<size_t> tlasOrdered;
+    std::vector<float> tlasPrimBounds; // 6 per primitive: lo, hi
+    std::vector<int4> tlasWideKids;  // per top-level wide node, its children's binary node indices
+    int32_t tlasInterior = 0;        // binary interior nodes of the top level (the first in `nodes`)
     std::vector<float4> tris;        // 3 per leaf-ordered triangle
     std::vector<int4> triVerts;      // per global triangle
     std::vector<float4> pos, nrm;    // per vertex (global)
@@ -103,6 +125,7 @@ struct pe_scene {
     std::vector<pe_material> materialsIn;
     std::vector<pe::MatGPU> materials;
     std::vector<pe::HostShape> shapes;
+    std::vector<pe::HostBlas> blases;          // pe_scene_add_blas
     std::vector<pe::LightGPU> lights;
     pe::HostEnv env;
     int32_t bgMode = PE_BG_ENVIRONMENT;
@@ -118,6 +141,8 @@ struct pe_scene {
     pe::HostBuild build;
     uint64_t version = 0;
     uint64_t materialVersion = 0; // pe_scene_set_material edits since the build
+    uint64_t transformVersion = 0; // pe_scene_set_instance_transform edits since the build
+    uint64_t refitVersion = 0;     // pe_scene_refit calls since the build
 };
 
 namespace pe {

@@ -39,11 +39,31 @@ enum ShapeFlags : uint32_t {
     SF_HAS_NORMALS = 4u,
     SF_HAS_UVS = 8u,
     SF_SPHERE = 16u,         // an analytic sphere
+    SF_INSTANCE = 32u,       // a MeshInstance
 };
 
 // A leaf record whose b.w meta has this bit is an analytic sphere (Sphere, src/geometry/sphere.h):
 // a = (centre, radius); the other words hold the meta and the global primitive id as for a triangle.
 constexpr uint32_t PRIM_SPHERE = 1u << 16;
+// ... or a MeshInstance: a.x holds the instance index; its BLAS's leaf records follow the top
+// level's in the same array, its nodes the top level's nodes.
+constexpr uint32_t PRIM_INSTANCE = 1u << 17;
+// A closest hit inside an instance is reported as kInstanceHit | instance << 21 | BLAS-local
+// record (negative, never -1): at most kMaxInstances instances, kMaxBlasRecords records a BLAS.
+constexpr int32_t kMaxInstances = 1023;
+constexpr int32_t kMaxBlasRecords = (1 << 21) - 1;
+
+// A MeshInstance (mesh_instance.cpp): world-to-local and local-to-world (row-major rows 0-3), its
+// BLAS's root in the binary and in the 4-wide tree (a node index or a leaf reference) and first
+// leaf record, the global id of the BLAS's first triangle, the shape and the material.
+struct InstGPU {
+    float4 w2l[4];
+    float4 l2w[4];
+    int32_t rootBinary, rootWide, recBase, firstTri;
+    int32_t shape, material;
+    float uvScale;   // 1 / cbrt(|det|) of the 3×3 part (uvDensity, mesh_instance.cpp:95-98)
+    int32_t pad;
+};
 
 struct ShapeInfo {
     int32_t material;
@@ -234,6 +254,8 @@ struct SceneGPU {
     // light or shadow links, a shadow catcher): its waves may shade with the lean kernels
     int32_t leanShading;
     int32_t materialTypes;   // bit t: some material has type t
+    const InstGPU* instances; // MeshInstances (null without)
+    int32_t nInstances;
 };
 
 // Scene::isLightLinked / isShadowLinked for light `li` (explicit) and a receiver or blocker node.

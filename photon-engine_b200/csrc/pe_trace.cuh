@@ -182,56 +182,153 @@ __device__ __forceinline__ void leafRange(int ref, int& first, int& count) {
     count = static_cast<int>(v & 0xFFu) + 1;
 }
 
-template <bool COUNT>
+// Transform::transformPoint / transformVector (transform.cpp:15-40) with a row-major 4×4.
+__device__ __forceinline__ V3 xfPointD(const float4* m, V3 p) {
+    const float4 r0 = __ldg(&m[0]), r1 = __ldg(&m[1]), r2 = __ldg(&m[2]), r3 = __ldg(&m[3]);
+    const float x = r0.x * p.x + r0.y * p.y + r0.z * p.z + r0.w;
+    const float y = r1.x * p.x + r1.y * p.y + r1.z * p.z + r1.w;
+    const float z = r2.x * p.x + r2.y * p.y + r2.z * p.z + r2.w;
+    const float w = r3.x * p.x + r3.y * p.y + r3.z * p.z + r3.w;
+    if (w != 1.0f && w != 0.0f) {
+        const float iw = 1.0f / w;
+        return mk(x * iw, y * iw, z * iw);
+    }
+    return mk(x, y, z);
+}
+__device__ __forceinline__ V3 xfVectorD(const float4* m, V3 v) {
+    const float4 r0 = __ldg(&m[0]), r1 = __ldg(&m[1]), r2 = __ldg(&m[2]);
+    return mk(r0.x * v.x + r0.y * v.y + r0.z * v.z, r1.x * v.x + r1.y * v.y + r1.z * v.z,
+              r2.x * v.x + r2.y * v.y + r2.z * v.z);
+}
+// A closest hit inside mesh instance `inst` at its BLAS-local record `local` (negative, never -1).
+__device__ __forceinline__ int32_t instanceHitCode(int inst, int local) {
+    return static_cast<int32_t>(0x80000000u | (static_cast<uint32_t>(inst) << 21) | static_cast<uint32_t>(local));
+}
+__device__ __forceinline__ bool isInstanceHit(int32_t prim) { return prim < -1; }
+__device__ __forceinline__ int instanceOfHit(int32_t prim) { return static_cast<int>((static_cast<uint32_t>(prim) >> 21) & 0x3FFu); }
+__device__ __forceinline__ int localOfHit(int32_t prim) { return static_cast<int>(static_cast<uint32_t>(prim) & 0x1FFFFFu); }
+
+template <bool COUNT, int LEVEL>
+__device__ void walkClosest(const SceneGPU& S, int cur, V3 o, V3 d, V3 inv, uint32_t mask, float tMin, float& tMax,
+                            Hit& best, uint32_t& nodeVisits, uint32_t& triTests);
+template <bool COUNT, int SD, int LEVEL>
+__device__ void walkClosestWide(const SceneGPU& S, int cur, V3 o, V3 d, V3 inv, uint32_t mask, float tMin, float& tMax,
+                                Hit& best, uint32_t& nodeVisits, uint32_t& triTests, uint2* sstack);
+template <bool COUNT, int LEVEL>
+__device__ bool walkAny(const SceneGPU& S, int cur, V3 o, V3 d, V3 inv, uint32_t mask, float tMin, float tMax,
+                        uint32_t& nodeVisits, uint32_t& triTests);
+template <bool COUNT, int LEVEL>
+__device__ bool walkAnyWide(const SceneGPU& S, int cur, V3 o, V3 d, V3 inv, uint32_t mask, float tMin, float tMax,
+                            uint32_t& nodeVisits, uint32_t& triTests);
+
+// MeshInstance::intersect (mesh_instance.cpp:104-115): the ray carried into the instance's space
+// by its world-to-local matrix (direction not renormalised, so t is shared), its BLAS walked
+// with every visibility bit; a hit shortens the world ray as it shortens the local one.
+template <bool COUNT, bool WIDE>
+__device__ __noinline__ void instanceClosest(const SceneGPU& S, int inst, uint32_t meta, V3 o, V3 d, float tMin,
+                                             float& tMax, Hit& best, uint32_t& nodeVisits, uint32_t& triTests) {
+    const InstGPU& I = S.instances[inst];
+    const V3 lo = xfPointD(I.w2l, o), ld = xfVectorD(I.w2l, d);
+    const V3 linv = mk(1.0f / ld.x, 1.0f / ld.y, 1.0f / ld.z);
+    Hit h;
+    h.prim = -1;
+    h.meta = 0;
+    h.t = tMax;
+    h.u = h.v = 0.0f;
+    float tm = tMax;
+    if (WIDE)
+        walkClosestWide<COUNT, 0, 1>(S, I.rootWide, lo, ld, linv, 0x1Fu, tMin, tm, h, nodeVisits, triTests, nullptr);
+    else
+        walkClosest<COUNT, 1>(S, I.rootBinary, lo, ld, linv, 0x1Fu, tMin, tm, h, nodeVisits, triTests);
+    if (h.prim < 0) return;
+    tMax = tm;
+    best.t = h.t;
+    best.u = h.u;
+    best.v = h.v;
+    best.prim = instanceHitCode(inst, h.prim - I.recBase);
+    best.meta = meta;
+}
+
+template <bool COUNT, bool WIDE>
+__device__ __noinline__ bool instanceAny(const SceneGPU& S, int inst, V3 o, V3 d, float tMin, float tMax,
+                                         uint32_t& nodeVisits, uint32_t& triTests) {
+    const InstGPU& I = S.instances[inst];
+    const V3 lo = xfPointD(I.w2l, o), ld = xfVectorD(I.w2l, d);
+    const V3 linv = mk(1.0f / ld.x, 1.0f / ld.y, 1.0f / ld.z);
+    return WIDE ? walkAnyWide<COUNT, 1>(S, I.rootWide, lo, ld, linv, 0x1Fu, tMin, tMax, nodeVisits, triTests)
+                : walkAny<COUNT, 1>(S, I.rootBinary, lo, ld, linv, 0x1Fu, tMin, tMax, nodeVisits, triTests);
+}
+
+// The primitives of one leaf, in order: triangles (lean Möller–Trumbore), spheres and, at the top
+// level, mesh instances; the last one with t <= tMax wins a tie, as in BVH::intersect.
+template <bool COUNT, int LEVEL, bool WIDE>
 __device__ __forceinline__ void testLeafClosest(const SceneGPU& S, int first, int count, V3 o, V3 d, uint32_t mask,
-                                                float tMin, float& tMax, Hit& best, uint32_t& triTests) {
+                                                float tMin, float& tMax, Hit& best, uint32_t& nodeVisits,
+                                                uint32_t& triTests) {
     for (int k = 0; k < count; ++k) {
         const int pi = first + k;
         const float4 a = __ldg(&S.tris[3 * pi + 0]);
         const float4 b = __ldg(&S.tris[3 * pi + 1]);
-        if ((__float_as_uint(b.w) & mask) == 0u) continue;
+        const uint32_t meta = __float_as_uint(b.w);
+        if ((meta & mask) == 0u) continue;
+        if (LEVEL == 0 && (meta & PRIM_INSTANCE)) {
+            instanceClosest<COUNT, WIDE>(S, __float_as_int(a.x), meta, o, d, tMin, tMax, best, nodeVisits, triTests);
+            continue;
+        }
         if (COUNT) ++triTests;
         float t, u = 0.0f, v = 0.0f;
-        if (__float_as_uint(b.w) & PRIM_SPHERE) {
+        if (meta & PRIM_SPHERE) {
             if (!sphereLean(a, o, d, tMin, tMax, t)) continue;
         } else if (!triLean(a, b, __ldg(&S.tris[3 * pi + 2]), o, d, tMin, tMax, t, u, v)) {
             continue;
         }
-        {
-            tMax = t;
-            best.t = t;
-            best.u = u;
-            best.v = v;
-            best.prim = pi;
-            best.meta = __float_as_uint(b.w);
-        }
+        tMax = t;
+        best.t = t;
+        best.u = u;
+        best.v = v;
+        best.prim = pi;
+        best.meta = meta;
     }
 }
 
-// BVH::intersect (bvh.cpp:322-401): near child first, far child pushed with its entry
-// distance and skipped on pop when farther than the current hit.  The last triangle with
-// t <= tMax wins ties, as there.
-template <bool COUNT>
-__device__ Hit traceClosest(const SceneGPU& S, V3 o, V3 d, uint32_t mask, float tMin, float tMax, uint32_t& nodeVisits,
-                            uint32_t& triTests) {
-    Hit best;
-    best.prim = -1;
-    best.meta = 0;
-    best.t = tMax;
-    best.u = best.v = 0.0f;
-    const V3 inv = mk(1.0f / d.x, 1.0f / d.y, 1.0f / d.z);
-    float tn;
-    if (S.nTris == 0) return best;
-    if (!slab(S.rootMin[0], S.rootMax[0], S.rootMin[1], S.rootMax[1], S.rootMin[2], S.rootMax[2], o, inv, tMin, tMax, tn))
-        return best;
-    if (S.rootIsLeaf) {
-        testLeafClosest<COUNT>(S, S.rootFirst, S.rootCount, o, d, mask, tMin, tMax, best, triTests);
-        return best;
+template <bool COUNT, int LEVEL, bool WIDE>
+__device__ __forceinline__ bool testLeafAny(const SceneGPU& S, int first, int count, V3 o, V3 d, uint32_t mask,
+                                            float tMin, float tMax, uint32_t& nodeVisits, uint32_t& triTests) {
+    for (int k = 0; k < count; ++k) {
+        const int pi = first + k;
+        const float4 a = __ldg(&S.tris[3 * pi + 0]);
+        const float4 b = __ldg(&S.tris[3 * pi + 1]);
+        const uint32_t meta = __float_as_uint(b.w);
+        if ((meta & mask) == 0u) continue;
+        if (LEVEL == 0 && (meta & PRIM_INSTANCE)) {
+            if (instanceAny<COUNT, WIDE>(S, __float_as_int(a.x), o, d, tMin, tMax, nodeVisits, triTests)) return true;
+            continue;
+        }
+        if (COUNT) ++triTests;
+        float t, u, v;
+        if (meta & PRIM_SPHERE) {
+            if (sphereLean(a, o, d, tMin, tMax, t)) return true;
+        } else if (triLean(a, b, __ldg(&S.tris[3 * pi + 2]), o, d, tMin, tMax, t, u, v)) {
+            return true;
+        }
     }
+    return false;
+}
+
+// The root of the top-level tree as a walk's first reference: node 0, or the leaf it is.
+__device__ __forceinline__ int rootRef(const SceneGPU& S) {
+    return S.rootIsLeaf ? static_cast<int>(~((static_cast<uint32_t>(S.rootFirst) << 8) | static_cast<uint32_t>(S.rootCount - 1)))
+                        : 0;
+}
+
+// BVH::intersect (bvh.cpp:322-401) from reference `cur`: near child first, far child pushed with
+// its entry distance and skipped on pop when farther than the current hit.
+template <bool COUNT, int LEVEL>
+__device__ void walkClosest(const SceneGPU& S, int cur, V3 o, V3 d, V3 inv, uint32_t mask, float tMin, float& tMax,
+                            Hit& best, uint32_t& nodeVisits, uint32_t& triTests) {
     int stackRef[kMaxStack];
     float stackT[kMaxStack];
     int sp = 0;
-    int cur = 0;
     // while-while form: descend through interior nodes until a leaf (or nothing) is next, test the
     // leaf, pop.  A ray's own sequence of node and triangle tests is the reference's; the loop
     // shape only lets the lanes of a warp spend more of their steps in the same branch.
@@ -267,12 +364,12 @@ __device__ Hit traceClosest(const SceneGPU& S, V3 o, V3 d, uint32_t mask, float 
                         break;
                     }
                 }
-                if (!found) return best;
+                if (!found) return;
             }
         }
         int first, count;
         leafRange(cur, first, count);
-        testLeafClosest<COUNT>(S, first, count, o, d, mask, tMin, tMax, best, triTests);
+        testLeafClosest<COUNT, LEVEL, false>(S, first, count, o, d, mask, tMin, tMax, best, nodeVisits, triTests);
         bool found = false;
         while (sp > 0) {
             --sp;
@@ -282,23 +379,35 @@ __device__ Hit traceClosest(const SceneGPU& S, V3 o, V3 d, uint32_t mask, float 
                 break;
             }
         }
-        if (!found) return best;
+        if (!found) return;
     }
 }
 
-// BVH::intersectAny (bvh.cpp:404-446): true when any triangle in [tMin, tMax] passes the
-// mask.  The answer does not depend on visiting order; near child first for early exit.
+// Closest hit over the binary tree in the reference's visiting order; the last triangle with
+// t <= tMax wins ties, as in BVH::intersect.
 template <bool COUNT>
-__device__ bool traceAny(const SceneGPU& S, V3 o, V3 d, uint32_t mask, float tMin, float tMax, uint32_t& nodeVisits,
-                         uint32_t& triTests) {
+__device__ Hit traceClosest(const SceneGPU& S, V3 o, V3 d, uint32_t mask, float tMin, float tMax, uint32_t& nodeVisits,
+                            uint32_t& triTests) {
+    Hit best;
+    best.prim = -1;
+    best.meta = 0;
+    best.t = tMax;
+    best.u = best.v = 0.0f;
     const V3 inv = mk(1.0f / d.x, 1.0f / d.y, 1.0f / d.z);
     float tn;
-    if (S.nTris == 0) return false;
+    if (S.nTris == 0) return best;
     if (!slab(S.rootMin[0], S.rootMax[0], S.rootMin[1], S.rootMax[1], S.rootMin[2], S.rootMax[2], o, inv, tMin, tMax, tn))
-        return false;
+        return best;
+    walkClosest<COUNT, 0>(S, rootRef(S), o, d, inv, mask, tMin, tMax, best, nodeVisits, triTests);
+    return best;
+}
+
+// BVH::intersectAny (bvh.cpp:404-446) from reference `cur`.
+template <bool COUNT, int LEVEL>
+__device__ bool walkAny(const SceneGPU& S, int cur, V3 o, V3 d, V3 inv, uint32_t mask, float tMin, float tMax,
+                        uint32_t& nodeVisits, uint32_t& triTests) {
     int stackRef[kMaxStack];
     int sp = 0;
-    int cur = S.rootIsLeaf ? static_cast<int>(~((static_cast<uint32_t>(S.rootFirst) << 8) | static_cast<uint32_t>(S.rootCount - 1))) : 0;
     for (;;) {
         while (cur >= 0) {
             if (COUNT) ++nodeVisits;
@@ -325,22 +434,23 @@ __device__ bool traceAny(const SceneGPU& S, V3 o, V3 d, uint32_t mask, float tMi
         }
         int first, count;
         leafRange(cur, first, count);
-        for (int k = 0; k < count; ++k) {
-            const int pi = first + k;
-            const float4 a = __ldg(&S.tris[3 * pi + 0]);
-            const float4 b = __ldg(&S.tris[3 * pi + 1]);
-            if ((__float_as_uint(b.w) & mask) == 0u) continue;
-            if (COUNT) ++triTests;
-            float t, u, v;
-            if (__float_as_uint(b.w) & PRIM_SPHERE) {
-                if (sphereLean(a, o, d, tMin, tMax, t)) return true;
-            } else if (triLean(a, b, __ldg(&S.tris[3 * pi + 2]), o, d, tMin, tMax, t, u, v)) {
-                return true;
-            }
-        }
+        if (testLeafAny<COUNT, LEVEL, false>(S, first, count, o, d, mask, tMin, tMax, nodeVisits, triTests)) return true;
         if (sp == 0) return false;
         cur = stackRef[--sp];
     }
+}
+
+// BVH::intersectAny (bvh.cpp:404-446): true when any primitive in [tMin, tMax] passes the mask.
+// The answer does not depend on visiting order; near child first for early exit.
+template <bool COUNT>
+__device__ bool traceAny(const SceneGPU& S, V3 o, V3 d, uint32_t mask, float tMin, float tMax, uint32_t& nodeVisits,
+                         uint32_t& triTests) {
+    const V3 inv = mk(1.0f / d.x, 1.0f / d.y, 1.0f / d.z);
+    float tn;
+    if (S.nTris == 0) return false;
+    if (!slab(S.rootMin[0], S.rootMax[0], S.rootMin[1], S.rootMax[1], S.rootMin[2], S.rootMax[2], o, inv, tMin, tMax, tn))
+        return false;
+    return walkAny<COUNT, 0>(S, rootRef(S), o, d, inv, mask, tMin, tMax, nodeVisits, triTests);
 }
 
 // ---- 4-wide traversal ----------------------------------------------------------------------
@@ -404,28 +514,14 @@ struct TraceStack {
     __device__ __forceinline__ uint2 get(int i) const { return (SD > 0 && i < SD) ? shared[i * 128] : local[i - SD]; }
 };
 
-// SD: stack entries kept in shared memory (`sstack`: this thread's column); 0 keeps all in local.
-template <bool COUNT, int SD = 0>
-__device__ Hit traceClosestWide(const SceneGPU& S, V3 o, V3 d, uint32_t mask, float tMin, float tMax,
-                                uint32_t& nodeVisits, uint32_t& triTests, uint2* sstack = nullptr) {
-    Hit best;
-    best.prim = -1;
-    best.meta = 0;
-    best.t = tMax;
-    best.u = best.v = 0.0f;
-    const V3 inv = mk(1.0f / d.x, 1.0f / d.y, 1.0f / d.z);
-    float tn;
-    if (S.nTris == 0) return best;
-    if (!slab(S.rootMin[0], S.rootMax[0], S.rootMin[1], S.rootMax[1], S.rootMin[2], S.rootMax[2], o, inv, tMin, tMax, tn))
-        return best;
-    if (S.rootIsLeaf) {
-        testLeafClosest<COUNT>(S, S.rootFirst, S.rootCount, o, d, mask, tMin, tMax, best, triTests);
-        return best;
-    }
+// The 4-wide walk from reference `cur`.  SD: stack entries kept in shared memory (`sstack`:
+// this thread's column); 0 keeps all in local memory.
+template <bool COUNT, int SD, int LEVEL>
+__device__ void walkClosestWide(const SceneGPU& S, int cur, V3 o, V3 d, V3 inv, uint32_t mask, float tMin, float& tMax,
+                                Hit& best, uint32_t& nodeVisits, uint32_t& triTests, uint2* sstack) {
     TraceStack<SD> stack;
     stack.shared = sstack;
     int sp = 0;
-    int cur = 0;
     for (;;) {
         while (cur >= 0) {
             if (COUNT) ++nodeVisits;
@@ -450,7 +546,7 @@ __device__ Hit traceClosestWide(const SceneGPU& S, V3 o, V3 d, uint32_t mask, fl
                         break;
                     }
                 }
-                if (!found) return best;
+                if (!found) return;
                 continue;
             }
             // farther children first onto the stack, so they pop nearest first
@@ -461,7 +557,7 @@ __device__ Hit traceClosestWide(const SceneGPU& S, V3 o, V3 d, uint32_t mask, fl
         }
         int first, count;
         leafRange(cur, first, count);
-        testLeafClosest<COUNT>(S, first, count, o, d, mask, tMin, tMax, best, triTests);
+        testLeafClosest<COUNT, LEVEL, true>(S, first, count, o, d, mask, tMin, tMax, best, nodeVisits, triTests);
         bool found = false;
         while (sp > 0) {
             const uint2 e = stack.get(--sp);
@@ -471,22 +567,33 @@ __device__ Hit traceClosestWide(const SceneGPU& S, V3 o, V3 d, uint32_t mask, fl
                 break;
             }
         }
-        if (!found) return best;
+        if (!found) return;
     }
 }
 
-// Any hit over the 4-wide tree: the answer does not depend on the visiting order.
-template <bool COUNT>
-__device__ bool traceAnyWide(const SceneGPU& S, V3 o, V3 d, uint32_t mask, float tMin, float tMax, uint32_t& nodeVisits,
-                             uint32_t& triTests) {
+template <bool COUNT, int SD = 0>
+__device__ Hit traceClosestWide(const SceneGPU& S, V3 o, V3 d, uint32_t mask, float tMin, float tMax,
+                                uint32_t& nodeVisits, uint32_t& triTests, uint2* sstack = nullptr) {
+    Hit best;
+    best.prim = -1;
+    best.meta = 0;
+    best.t = tMax;
+    best.u = best.v = 0.0f;
     const V3 inv = mk(1.0f / d.x, 1.0f / d.y, 1.0f / d.z);
     float tn;
-    if (S.nTris == 0) return false;
+    if (S.nTris == 0) return best;
     if (!slab(S.rootMin[0], S.rootMax[0], S.rootMin[1], S.rootMax[1], S.rootMin[2], S.rootMax[2], o, inv, tMin, tMax, tn))
-        return false;
+        return best;
+    walkClosestWide<COUNT, SD, 0>(S, rootRef(S), o, d, inv, mask, tMin, tMax, best, nodeVisits, triTests, sstack);
+    return best;
+}
+
+// Any hit over the 4-wide tree from reference `cur`: the answer does not depend on the order.
+template <bool COUNT, int LEVEL>
+__device__ bool walkAnyWide(const SceneGPU& S, int cur, V3 o, V3 d, V3 inv, uint32_t mask, float tMin, float tMax,
+                            uint32_t& nodeVisits, uint32_t& triTests) {
     int stackRef[kWideStack];
     int sp = 0;
-    int cur = S.rootIsLeaf ? static_cast<int>(~((static_cast<uint32_t>(S.rootFirst) << 8) | static_cast<uint32_t>(S.rootCount - 1))) : 0;
     for (;;) {
         while (cur >= 0) {
             if (COUNT) ++nodeVisits;
@@ -508,22 +615,21 @@ __device__ bool traceAnyWide(const SceneGPU& S, V3 o, V3 d, uint32_t mask, float
         }
         int first, count;
         leafRange(cur, first, count);
-        for (int k = 0; k < count; ++k) {
-            const int pi = first + k;
-            const float4 a = __ldg(&S.tris[3 * pi + 0]);
-            const float4 b = __ldg(&S.tris[3 * pi + 1]);
-            if ((__float_as_uint(b.w) & mask) == 0u) continue;
-            if (COUNT) ++triTests;
-            float t, u, v;
-            if (__float_as_uint(b.w) & PRIM_SPHERE) {
-                if (sphereLean(a, o, d, tMin, tMax, t)) return true;
-            } else if (triLean(a, b, __ldg(&S.tris[3 * pi + 2]), o, d, tMin, tMax, t, u, v)) {
-                return true;
-            }
-        }
+        if (testLeafAny<COUNT, LEVEL, true>(S, first, count, o, d, mask, tMin, tMax, nodeVisits, triTests)) return true;
         if (sp == 0) return false;
         cur = stackRef[--sp];
     }
+}
+
+template <bool COUNT>
+__device__ bool traceAnyWide(const SceneGPU& S, V3 o, V3 d, uint32_t mask, float tMin, float tMax, uint32_t& nodeVisits,
+                             uint32_t& triTests) {
+    const V3 inv = mk(1.0f / d.x, 1.0f / d.y, 1.0f / d.z);
+    float tn;
+    if (S.nTris == 0) return false;
+    if (!slab(S.rootMin[0], S.rootMax[0], S.rootMin[1], S.rootMax[1], S.rootMin[2], S.rootMax[2], o, inv, tMin, tMax, tn))
+        return false;
+    return walkAnyWide<COUNT, 0>(S, rootRef(S), o, d, inv, mask, tMin, tMax, nodeVisits, triTests);
 }
 
 // ---- hit record (src/geometry/triangle.cpp:54-133) -----------------------------------------
@@ -583,14 +689,80 @@ static __device__ __noinline__ void fillSphereHit(const SceneGPU& S, const Hit& 
     is.material = S.shapes[shape].material;
 }
 
+// Triangle::fillHit's record of leaf record h.prim, in the space its vertices are in; returns the
+// triangle's vertex indices and (w) shape, which a mesh instance's triangle does not have.
+static __device__ __forceinline__ int4 fillTriangleHit(const SceneGPU& S, const Hit& h, V3 rayDir, Isect& is);
+
+// transformHitToWorld (mesh_instance.cpp:57-100): point and smooth point by the local-to-world
+// matrix, both normals by its inverse transpose and renormalised (the shading normal faced to
+// the world ray), the tangent carried and made orthogonal again, a world error bound from the
+// matrix's absolute rows plus a relative and an absolute slack, the texel density rescaled.
+static __device__ __noinline__ void instanceToWorld(const InstGPU& I, V3 rayDir, Isect& is) {
+    const V3 localOutNg = is.ng;
+    const V3 localOutNs = is.frontFace ? is.normal : -is.normal;
+    is.point = xfPointD(I.l2w, is.point);
+    is.pSmooth = is.hasSmooth ? xfPointD(I.l2w, is.pSmooth) : is.point;
+    const float4 i0 = __ldg(&I.w2l[0]), i1 = __ldg(&I.w2l[1]), i2 = __ldg(&I.w2l[2]);
+    auto xfNormal = [&](V3 n) {
+        return mk(i0.x * n.x + i1.x * n.y + i2.x * n.z, i0.y * n.x + i1.y * n.y + i2.y * n.z,
+                  i0.z * n.x + i1.z * n.y + i2.z * n.z);
+    };
+    V3 ngW = xfNormal(localOutNg);
+    if (len2(ngW) > 0.0f) ngW = normalize(ngW);
+    V3 nsW = xfNormal(localOutNs);
+    if (len2(nsW) > 0.0f) nsW = normalize(nsW);
+    else nsW = ngW;
+    is.ng = ngW;
+    is.frontFace = dot(rayDir, nsW) < 0.0f;
+    is.normal = is.frontFace ? nsW : -nsW;
+    if (len2(is.ng) == 0.0f) is.ng = nsW;
+    V3 tW = xfVectorD(I.l2w, is.tangent);
+    tW = tW - is.normal * dot(is.normal, tW);
+    if (len2(tW) > 1e-12f) {
+        is.tangent = normalize(tW);
+    } else {
+        const V3 n = is.normal;
+        const float sign = copysignf(1.0f, n.z);
+        const float a = -1.0f / (sign + n.z);
+        const float b = n.x * n.y * a;
+        is.tangent = normalize(mk(1.0f + sign * n.x * n.x * a, sign * b, -sign * n.x));
+    }
+    const float4 m0 = __ldg(&I.l2w[0]), m1 = __ldg(&I.l2w[1]), m2 = __ldg(&I.l2w[2]);
+    const V3 r0 = mk(fabsf(m0.x), fabsf(m0.y), fabsf(m0.z)), r1 = mk(fabsf(m1.x), fabsf(m1.y), fabsf(m1.z)),
+             r2 = mk(fabsf(m2.x), fabsf(m2.y), fabsf(m2.z));
+    const V3 pAbs = vabs(is.point);
+    is.pError = mk(dot(r0, is.pError), dot(r1, is.pError), dot(r2, is.pError)) + pAbs * 1e-5f + mk(1e-6f);
+    if (is.uvDensity > 0.0f) is.uvDensity = is.uvDensity / I.uvScale;
+}
+
 static __device__ __noinline__ void fillHit(const SceneGPU& S, const Hit& h, V3 rayO, V3 rayDir, Isect& is) {
+    if (isInstanceHit(h.prim)) {
+        // MeshInstance::shadeInstanceHit (mesh_instance.cpp:125-133): the triangle's record in the
+        // instance's space, carried to world space
+        const InstGPU& I = S.instances[instanceOfHit(h.prim)];
+        Hit hl = h;
+        hl.prim = I.recBase + localOfHit(h.prim);
+        fillTriangleHit(S, hl, xfVectorD(I.w2l, rayDir), is);
+        instanceToWorld(I, rayDir, is);
+        is.shape = I.shape;
+        is.material = I.material;
+        return;
+    }
+    const float4 e2w = __ldg(&S.tris[3 * h.prim + 2]);
+    const int g = static_cast<int>(__float_as_uint(e2w.w));
+    if (__float_as_uint(__ldg(&S.tris[3 * h.prim + 1]).w) & PRIM_SPHERE) {
+        fillSphereHit(S, h, rayO, rayDir, g, __ldg(&S.triVerts[g]).w, is);
+        return;
+    }
+    const int4 tv = fillTriangleHit(S, h, rayDir, is);
+    is.shape = tv.w;
+    is.material = S.shapes[tv.w].material;
+}
+
+static __device__ __forceinline__ int4 fillTriangleHit(const SceneGPU& S, const Hit& h, V3 rayDir, Isect& is) {
     const float4 e2w = __ldg(&S.tris[3 * h.prim + 2]);
     const int g = static_cast<int>(__float_as_uint(e2w.w));
     const int4 tv = __ldg(&S.triVerts[g]);
-    if (__float_as_uint(__ldg(&S.tris[3 * h.prim + 1]).w) & PRIM_SPHERE) {
-        fillSphereHit(S, h, rayO, rayDir, g, tv.w, is);
-        return;
-    }
     const V3 v0 = ld3(S.pos, tv.x), v1 = ld3(S.pos, tv.y), v2 = ld3(S.pos, tv.z);
     const V3 n0 = ld3(S.nrm, tv.x), n1 = ld3(S.nrm, tv.y), n2 = ld3(S.nrm, tv.z);
     const float2 uv0 = __ldg(&S.uv[tv.x]), uv1 = __ldg(&S.uv[tv.y]), uv2 = __ldg(&S.uv[tv.z]);
@@ -645,8 +817,7 @@ static __device__ __noinline__ void fillHit(const SceneGPU& S, const Hit& h, V3 
     }
     is.tangent = normalize(tangent);
     is.tri = g;
-    is.shape = tv.w;
-    is.material = S.shapes[tv.w].material;
+    return tv;
 }
 
 // ---- robust spawning (src/geometry/ray_spawn.h) --------------------------------------------

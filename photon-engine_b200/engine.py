@@ -237,6 +237,25 @@ class Sphere:
         return 0
 
 
+class MeshInstance:
+    """MeshInstance (src/geometry/mesh_instance.h): a TriangleMesh placed by a local-to-world 4×4
+    matrix (row-major, column vectors; translation in the last column), with the instance's own
+    material (else the mesh's).  Instances of one mesh share its BVH (a BLAS) on the device; the
+    top-level tree holds one primitive per instance.  `world_to_local` is the matrix's inverse as
+    the caller composed it (Transform keeps both); omitted, it is computed by Mat4f::inverse's
+    cofactor expansion."""
+
+    def __init__(self, mesh: TriangleMesh, local_to_world, material: Material | None = None, world_to_local=None):
+        self.mesh = mesh
+        self.local_to_world = np.ascontiguousarray(local_to_world, dtype=np.float32).reshape(4, 4)
+        self.world_to_local = None if world_to_local is None else \
+            np.ascontiguousarray(world_to_local, dtype=np.float32).reshape(4, 4)
+        self.material = material if material is not None else mesh.material
+
+    def num_triangles(self) -> int:
+        return 0
+
+
 class AreaLight:
     def __init__(self, position, u, v, radiance):
         self.position = tuple(map(float, position))
@@ -313,7 +332,8 @@ class Scene:
         """Scene::addShape of a TriangleMesh or a Sphere."""
         if shape.material is None:
             raise ValueError(f"{type(shape).__name__} needs a material")
-        self.ops.append(("sphere" if isinstance(shape, Sphere) else "mesh", shape))
+        kind = "sphere" if isinstance(shape, Sphere) else ("instance" if isinstance(shape, MeshInstance) else "mesh")
+        self.ops.append((kind, shape))
 
     def add_light(self, light: AreaLight):
         self.ops.append(("area", light))
@@ -370,7 +390,7 @@ class Scene:
     def materials(self) -> list[Material]:
         out, seen = [], set()
         for kind, obj in self.ops:
-            if kind in ("mesh", "sphere") and id(obj.material) not in seen:
+            if kind in ("mesh", "sphere", "instance") and id(obj.material) not in seen:
                 seen.add(id(obj.material))
                 out.append(obj.material)
         return out
@@ -410,14 +430,29 @@ class Scene:
         for kind, obj in self.ops:
             if kind == "sphere":
                 continue
-            if kind == "mesh":
+            if kind in ("mesh", "instance"):
                 m = obj.material.struct
                 if m.type in (capi.PE_MAT_LAMBERT, capi.PE_MAT_DISNEY) and any(m.emission):
-                    li += obj.indices.shape[0]
+                    li += (obj.mesh if kind == "instance" else obj).indices.shape[0]
             else:
                 if lib.pe_scene_set_area_light_radiance(self._handle, li, capi.f3(obj.radiance)) != capi.PE_OK:
                     return False
                 li += 1
+        return True
+
+    def sync_transforms(self) -> bool:
+        """Sends every MeshInstance's current matrices to the built scene
+        (pe_scene_set_instance_transform); False when that is not possible (an emissive instance)."""
+        if not self._handle:
+            return False
+        lib = _lib()
+        shape = 0
+        for kind, obj in self.ops:
+            if kind == "instance":
+                if lib.pe_scene_set_instance_transform(self._handle, shape, capi.fptr(obj.local_to_world),
+                                                       capi.fptr(obj.world_to_local)) != capi.PE_OK:
+                    return False
+            shape += 2 if kind == "area" else 1
         return True
 
     def texture_has_mipmaps(self, img) -> bool:
@@ -446,6 +481,7 @@ class Scene:
             tex_index[id(img)] = t
         self._tex_index = tex_index
         mat_index = {}
+        blas_index = {}
         for m in self.materials():
             idx = lib.pe_scene_add_material(h, C.byref(m.struct_with(tex_index)))
             if idx < 0:
@@ -459,6 +495,18 @@ class Scene:
                                                  obj.indices.shape[0], mat_index[id(obj.material)]))
             elif kind == "sphere":
                 capi.check(lib.pe_scene_add_sphere(h, capi.f3(obj.center), obj.radius, mat_index[id(obj.material)]))
+            elif kind == "instance":
+                mesh = obj.mesh
+                b = blas_index.get(id(mesh))
+                if b is None:
+                    b = lib.pe_scene_add_blas(h, capi.fptr(mesh.positions), mesh.positions.shape[0],
+                                              capi.fptr(mesh.normals), capi.fptr(mesh.uvs), capi.uptr(mesh.indices),
+                                              mesh.indices.shape[0])
+                    if b < 0:
+                        capi.check(-b)
+                    blas_index[id(mesh)] = b
+                capi.check(lib.pe_scene_add_instance(h, b, capi.fptr(obj.local_to_world), capi.fptr(obj.world_to_local),
+                                                     mat_index[id(obj.material)]))
             else:
                 capi.check(lib.pe_scene_add_area_light(h, capi.f3(obj.position), capi.f3(obj.u), capi.f3(obj.v),
                                                        capi.f3(obj.radiance), 1 if obj.visible_to_camera else 0))
@@ -475,10 +523,10 @@ class Scene:
         for kind, obj in self.ops:
             if kind == "sphere":
                 continue
-            if kind == "mesh":
+            if kind in ("mesh", "instance"):
                 m = obj.material.struct
                 if m.type in (capi.PE_MAT_LAMBERT, capi.PE_MAT_DISNEY) and any(m.emission):
-                    li += obj.indices.shape[0]
+                    li += (obj.mesh if kind == "instance" else obj).indices.shape[0]
             else:
                 if obj.light_group:
                     groups[li] = obj.light_group
@@ -833,14 +881,18 @@ class CudaDevice:
         self._scene = scene
 
     def update_scene(self, scene: Scene, kind: SceneUpdateKind = SceneUpdateKind.Full) -> bool:
-        """RenderDevice::updateScene.  Materials: the edited parameters go to the device without a
-        rebuild when the change allows it (returns True); otherwise, and for the other kinds, the
-        scene is rebuilt and set again (returns False)."""
+        """RenderDevice::updateScene.  Materials, Lights and Transforms (MeshInstance matrices: the
+        top-level tree is refitted, no BLAS rebuilt) go to the device without a rebuild when the
+        change allows it (returns True); otherwise, and for Full, the scene is rebuilt and set
+        again (returns False)."""
         if kind == SceneUpdateKind.Materials and self._scene is scene and scene.sync_materials():
             if _lib().pe_device_update_materials(self._h, scene.handle) == capi.PE_OK:
                 return True
         if kind == SceneUpdateKind.Lights and self._scene is scene and scene.sync_lights():
             if _lib().pe_device_update_lights(self._h, scene.handle) == capi.PE_OK:
+                return True
+        if kind == SceneUpdateKind.Transforms and self._scene is scene and scene.sync_transforms():
+            if _lib().pe_device_update_transforms(self._h, scene.handle) == capi.PE_OK:
                 return True
         scene.build_accelerator()
         self.set_scene(scene)

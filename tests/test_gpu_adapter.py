@@ -76,3 +76,29 @@ def test_adapter_adaptive_session_converges(pe, device, adapter_oracle):
     assert np.isfinite(mean).all() and mean.mean() > 0.0
     assert cnt.min() >= 8 and cnt.max() <= 64
     assert cnt.mean() < 64, "no pixel stopped early"
+
+
+def test_adapter_carries_instances_and_their_transforms(pe, device, adapter_oracle):
+    """MeshInstances through the adapter (one BLAS per mesh), then SceneUpdateKind::Transforms with
+    the instances placed anew in the reference scene: the adapter refits, the mirror refits."""
+    H = importlib.import_module("test_instances")
+    scene, cam, st = H.instanced_cornell(pe, 48, 48, 8, 6)
+    film, _ = _mirror(pe, device, scene, cam, st, 8)
+    ref = adapter_oracle.RefScene(scene, fast="adapter")
+    mean, cnt, _, done, _ = ref.session_cuda(cam, st, 8, batch=3)
+    assert done == 8 and np.array_equal(cnt, film.count)
+    assert pe.rel_mse(mean, film.resolve()) <= 1e-10
+    n = scene.shape_count()
+    moved = [H.rot_y(1.1, (2.2, 0.8, 2.0), 1.0), H.rot_y(0.2, (3.2, 2.0, 3.0), 0.7)]
+    for k, m in enumerate(moved):
+        ref.move_instance(n - 2 + k, m)
+    ref.session_cuda_update(3)
+    mean, cnt, _, _, _ = ref.session_cuda(cam, st, 8, batch=8)
+    inst = [o for kind, o in scene.ops if kind == "instance"]
+    for o, m in zip(inst, moved):
+        o.local_to_world, o.world_to_local = m, None
+    assert device.update_scene(scene, pe.SceneUpdateKind.Transforms)
+    film2 = pe.Film(st.width, st.height)
+    device.render(cam, st, pe.RenderTargets(beauty=film2), 0, 8)
+    assert np.array_equal(cnt, film2.count)
+    assert pe.rel_mse(mean, film2.resolve()) <= 1e-10

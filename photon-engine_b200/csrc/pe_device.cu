@@ -902,7 +902,7 @@ __global__ void kTracePrimary(SceneGPU S, WaveSeg A, int nPix, int32_t* outShape
         uint32_t a = 0, b = 0;
         const Hit h = WIDE ? traceClosestWide<false>(S, o, d, VIS_CAMERA, 0.0f, 1e30f, a, b)
                            : traceClosest<false>(S, o, d, VIS_CAMERA, 0.0f, 1e30f, a, b);
-        if (h.prim < 0) {
+        if (isMiss(h.prim)) {
             outShape[pix] = -1;
             outPrim[pix] = -1;
             outT[pix] = 0.0f;

@@ -281,7 +281,7 @@ __global__ void kGuideQuery(SceneGPU S, Paths P, Wave W, const int32_t* queue, c
         const int prim = __float_as_int(hr.w);
         bool want = false;
         V3 pnt, nrm, wo;
-        if (prim >= 0) {
+        if (!isMiss(prim)) {
             const float4 ro = P.rayO[slot];
             const int depth = static_cast<int>(__float_as_uint(P.pickN[slot].w) & 0xFFu);
             const WaveSeg& A = W.segs[segOfSlot(W, slot)];

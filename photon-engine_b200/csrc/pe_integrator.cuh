@@ -244,7 +244,7 @@ __global__ void __launch_bounds__(128) kIntersect(SceneGPU S, Paths P, const int
                                                                              sstack + threadIdx.x);
             P.hit[slot] = make_float4(h.t, h.u, h.v, __int_as_float(h.prim));
             key = (__float_as_uint(ro.w) & RAY_WALK) ? kShadeKeys - 1
-                  : (h.prim < 0 ? 0 : 1 + static_cast<int>((h.meta >> 8) & 0xFFu));
+                  : (isMiss(h.prim) ? 0 : 1 + static_cast<int>((h.meta >> 8) & 0xFFu));
         }
         // warp-aggregated append into the key's segment: one atomic per distinct key per warp
         const unsigned peers = __match_any_sync(0xffffffffu, key);
@@ -315,7 +315,7 @@ __device__ V3 shadowVisibility(const SceneGPU& S, V3 o, V3 d, float tMax, int li
     float remaining = tMax;
     for (int i = 0; i < 64; ++i) {
         const Hit h = traceClosestWide<COUNT>(S, origin, d, VIS_SHADOW, 0.0f, remaining, nodes, tris);
-        if (h.prim < 0) return T;
+        if (isMiss(h.prim)) return T;
         Isect is;
         fillHit(S, h, origin, d, is);
         if (link && !linkAllows(S.links[light].shadowMode, S.links[light].shadowMask, S.shapes[is.shape].linkNode)) {
@@ -589,7 +589,7 @@ __device__ __noinline__ V3 roundedEdgeNormal(const SceneGPU& S, const Isect& is,
             const V3 origin = is.point + s * d.x + t * d.y + axis * (sign * radius);
             const V3 rdir = axis * -sign;
             const Hit h = traceClosestWide<false>(S, origin, rdir, VIS_ALL, 0.0f, 2.0f * radius, n0, n1);
-            if (h.prim < 0) continue;
+            if (isMiss(h.prim)) continue;
             Isect hit;
             fillHit(S, h, origin, rdir, hit);
             if (hit.shape != is.shape) continue;
@@ -716,7 +716,7 @@ __device__ __forceinline__ bool shadeSlot(const SceneGPU& S, const Paths& P, con
     const int shadowSamples = A.shadowSamples;
     const int explicitLights = S.nLights;
     const int prim = __float_as_int(hr.w);
-    const bool hit = KEY == 0 ? false : (KEY > 0 ? true : prim >= 0);
+    const bool hit = KEY == 0 ? false : (KEY > 0 ? true : !isMiss(prim));
     // ray cone (path_tracer.cpp:428-454, 777-783, 853-857): only scenes with mipmapped textures
     const bool cones = !LEAN && S.hasMips && P.cone;
     float2 cone = cones ? P.cone[slot] : make_float2(0.0f, 0.0f);

@@ -205,6 +205,8 @@ __device__ __forceinline__ int32_t instanceHitCode(int inst, int local) {
     return static_cast<int32_t>(0x80000000u | (static_cast<uint32_t>(inst) << 21) | static_cast<uint32_t>(local));
 }
 __device__ __forceinline__ bool isInstanceHit(int32_t prim) { return prim < -1; }
+// A miss: -1 only (instance hits are negative too).
+__device__ __forceinline__ bool isMiss(int32_t prim) { return prim == -1; }
 __device__ __forceinline__ int instanceOfHit(int32_t prim) { return static_cast<int>((static_cast<uint32_t>(prim) >> 21) & 0x3FFu); }
 __device__ __forceinline__ int localOfHit(int32_t prim) { return static_cast<int>(static_cast<uint32_t>(prim) & 0x1FFFFFu); }
 

@@ -118,6 +118,18 @@ typedef struct pe_camera {
     int32_t orthographic;
     int32_t blades;         /* thin lens: aperture polygon sides (0 = round disk) */
     float blade_rotation;   /* thin lens: polygon rotation, radians */
+    /* Camera::setShutterEnd (camera.h:48-55): the pose at shutter close (t = 1) when has_shutter_end
+     * is non-zero.  With motion blur a ray at time t > 0 mixes the two descriptions linearly, its
+     * lens a round disk (Camera::generateRay(u, v, lens, time), camera.h:58-90). */
+    int32_t has_shutter_end;
+    float end_position[3];
+    float end_lower_left[3];
+    float end_horizontal[3];
+    float end_vertical[3];
+    float end_u[3];
+    float end_v[3];
+    float end_forward[3];
+    float end_lens_radius;
 } pe_camera;
 
 enum { PE_FILTER_BOX = 0, PE_FILTER_TRIANGLE = 1, PE_FILTER_GAUSSIAN = 2, PE_FILTER_BLACKMAN_HARRIS = 3 };
@@ -137,6 +149,9 @@ typedef struct pe_settings {
     int32_t adaptive_sampling;    /* RenderSettings::adaptiveSampling: clean pixels stop early */
     float noise_threshold;        /* relative standard error target (reference default 0.02; >= 1e-4 used) */
     int32_t min_adaptive_samples; /* samples before any decision (reference default 16; >= 2 used) */
+    int32_t motion_blur;    /* RenderSettings::motionBlur: each camera sample draws a shutter time
+                               (one more Sobol dimension, renderer.cpp:152-153) that moves the
+                               camera and mesh instances with a motion transform */
 } pe_settings;
 
 /* ---- scene builder --------------------------------------------------------- */
@@ -181,6 +196,20 @@ int32_t pe_scene_add_blas(pe_scene* s, const float* positions, uint32_t nv, cons
                           const uint32_t* indices, uint32_t ntri);
 int32_t pe_scene_add_instance(pe_scene* s, int32_t blas, const float local_to_world[16], const float world_to_local[16],
                               int32_t material);
+/* MeshInstance::setMotionTransform (mesh_instance.h:20-21): instance shape `shape`'s local-to-world
+ * matrix at shutter close (t = 1; world_to_local its inverse, NULL = Mat4f::inverse).  A ray at
+ * time t meets the instance under interpolateTransform(t0, t1, t) (quat.cpp: translation and scale
+ * linear, rotation by SLERP); its top-level box merges five poses over the shutter.  Lights of an
+ * emissive instance stay at t0, as Scene::addShape places them.  Call before pe_scene_build. */
+int32_t pe_scene_set_instance_motion(pe_scene* s, int32_t shape, const float local_to_world_end[16],
+                                     const float world_to_local_end[16]);
+/* Shape::bounds of shape `shape` (world box: lo xyz, hi xyz): a mesh's vertices, a sphere's cube,
+ * a mesh instance's BLAS box under its transform (Arvo), over the shutter for a moving instance. */
+int32_t pe_scene_shape_bounds(const pe_scene* s, int32_t shape, float out[6]);
+/* Transform(m)'s inverse as the reference computes it (Mat4f::inverse, mat.h:130-175: cofactors
+ * of 2×2 minors, identity for a singular matrix), row-major; what pe_scene_add_instance uses when
+ * world_to_local is NULL.  For composing Transform products (A·B)⁻¹ = B⁻¹·A⁻¹ on the host. */
+void pe_mat4_inverse(const float m[16], float out[16]);
 /* SceneUpdateKind::Transforms: new matrices for instance shape `shape` of a built scene; then
  * pe_device_update_transforms refits the top-level tree on the device without rebuilding any
  * BLAS.  An emissive instance (its lights move) returns PE_ERR_LIMIT: rebuild the scene. */
@@ -208,6 +237,10 @@ int32_t pe_scene_set_shadow_catcher(pe_scene* s, int32_t shape);
  * "object_<node uid>" or "shape_<n>", unnamed materials "material_<n>", renderer.cpp:75-118). */
 int32_t pe_scene_set_shape_name(pe_scene* s, int32_t shape, const char* name);
 int32_t pe_scene_set_material_name(pe_scene* s, int32_t material, const char* name);
+/* Shape::setVisibilityMask (shape.h:27-29; VisibilityMask, ray.h:18-25): the ray classes that see
+ * shape `shape`, bits camera 1, diffuse 2, glossy 4, transmission 8, shadow 16 (default 31).  A
+ * mesh instance's mask is tested at the top level only.  Call before pe_scene_build. */
+int32_t pe_scene_set_shape_visibility(pe_scene* s, int32_t shape, uint32_t mask);
 /* Replaces material `index` of a scene (built or not) for an incremental update: its type,
  * emission and the media, shadow-transmission and subsurface switches must stay as they were,
  * else PE_ERR_LIMIT (rebuild the scene).  Then pe_device_update_materials sends it to a device. */

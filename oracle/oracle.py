@@ -79,6 +79,7 @@ def _load(fast=False):
         "ref_scene_add_texture": (C.c_int32, [P, FP, C.c_int32, C.c_int32]),
         "ref_render_crypto": (C.c_int32, [P, C.c_void_p, C.c_void_p, C.c_int32, C.c_int32, C.c_int32, FP, C.c_int32]),
         "ref_scene_set_shape_name": (C.c_int32, [P, C.c_int32, C.c_char_p]),
+        "ref_scene_set_shape_visibility": (C.c_int32, [P, C.c_int32, C.c_uint32]),
         "ref_scene_set_material_name": (C.c_int32, [P, C.c_int32, C.c_char_p]),
         "ref_scene_build_texture_mipmaps": (C.c_int32, [P, C.c_int32]),
         "ref_scene_add_texture_u8": (C.c_int32, [P, C.c_void_p, C.c_int32, C.c_int32, C.c_int32]),
@@ -104,6 +105,9 @@ def _load(fast=False):
         "ref_scene_add_blas": (C.c_int32, [P, FP, C.c_uint32, FP, FP, UP, C.c_uint32]),
         "ref_scene_add_instance": (C.c_int32, [P, C.c_int32, FP, FP, C.c_int32]),
         "ref_scene_move_instance": (C.c_int32, [P, C.c_int32, FP, FP]),
+        "ref_scene_set_instance_motion": (C.c_int32, [P, C.c_int32, FP, FP]),
+        "ref_scene_shape_count": (C.c_int32, [P]),
+        "ref_camera_set_shutter_end": (None, [P, P]),
         "ref_load_project": (P, [C.c_char_p, C.c_float, IP, FP, IP, IP, FP, C.c_char_p, C.c_size_t]),
         "ref_scene_shapes": (C.c_int32, [P, IP, IP, FP, C.c_int32]),
         "ref_material_defaults": (None, [C.c_int32, C.c_void_p]),
@@ -189,6 +193,9 @@ class RefScene:
                         mesh.indices.ctypes.data_as(UP), mesh.indices.shape[0])
                 rc = self.lib.ref_scene_add_instance(self.h, blas_index[id(mesh)], _f(obj.local_to_world),
                                                      _f(obj.world_to_local), mat_index[id(obj.material)])
+                if rc == 0 and getattr(obj, "local_to_world_end", None) is not None:
+                    rc = self.lib.ref_scene_set_instance_motion(self.h, self.lib.ref_scene_shape_count(self.h) - 1,
+                                                                _f(obj.local_to_world_end), _f(obj.world_to_local_end))
             elif kind == "mesh":
                 rc = self.lib.ref_scene_add_mesh(self.h, _f(obj.positions), obj.positions.shape[0], _f(obj.normals),
                                                  _f(obj.uvs), obj.indices.ctypes.data_as(UP), obj.indices.shape[0],
@@ -205,6 +212,11 @@ class RefScene:
                 raise RuntimeError("reference rejected a shape tag")
         for shape, name in getattr(scene, "shape_names", {}).items():
             self.lib.ref_scene_set_shape_name(self.h, int(shape), name.encode())
+        shape = 0
+        for kind, obj in scene.ops:
+            if kind != "area" and getattr(obj, "visibility_mask", 0x1F) != 0x1F:
+                self.lib.ref_scene_set_shape_visibility(self.h, shape, int(obj.visibility_mask))
+            shape += 2 if kind == "area" else 1
         for mat, name in getattr(scene, "material_names", {}).values():
             if id(mat) in mat_index:
                 self.lib.ref_scene_set_material_name(self.h, mat_index[id(mat)], name.encode())
@@ -716,7 +728,13 @@ def reference_camera(camera, lib=None):
     lib = lib or _load()
     kind, params = camera.reference_params()
     p = np.asarray(params, np.float32)
-    return lib.ref_camera_create(int(kind), _f(p))
+    cam = lib.ref_camera_create(int(kind), _f(p))
+    end = getattr(camera, "shutter_end", None)
+    if end is not None:  # Camera::setShutterEnd from the end camera's own description
+        e = reference_camera(end, lib)
+        lib.ref_camera_set_shutter_end(cam, e)
+        lib.ref_camera_destroy(e)
+    return cam
 
 
 def describe_reference_camera(camera):

@@ -78,6 +78,21 @@ public:
         m_d.forward = v3(c.forward);
         m_d.lensRadius = 0.0f;
         m_d.orthographic = false;
+        if (c.has_shutter_end) setShutterEnd(endDesc(c));
+    }
+    // Camera::setShutterEnd's description from the pe_camera's end fields.
+    static CameraGpuDesc endDesc(const pe_camera& c) {
+        CameraGpuDesc e;
+        e.position = v3(c.end_position);
+        e.lowerLeft = v3(c.end_lower_left);
+        e.horizontal = v3(c.end_horizontal);
+        e.vertical = v3(c.end_vertical);
+        e.u = v3(c.end_u);
+        e.v = v3(c.end_v);
+        e.forward = v3(c.end_forward);
+        e.lensRadius = c.end_lens_radius;
+        e.orthographic = c.orthographic != 0;
+        return e;
     }
     Ray generateRay(float u, float v, const Vec2f&) const override {
         Vec3f targetPoint = m_d.lowerLeft + u * m_d.horizontal + v * m_d.vertical;
@@ -183,6 +198,7 @@ RenderSettings toSettings(const pe_settings& st, int threads) {
     s.adaptiveSampling = st.adaptive_sampling != 0;
     s.noiseThreshold = st.noise_threshold;
     s.minAdaptiveSamples = st.min_adaptive_samples;
+    s.motionBlur = st.motion_blur != 0;
     s.numThreads = threads;
     return s;
 }
@@ -411,6 +427,32 @@ int32_t ref_scene_add_instance(void* s, int32_t blas, const float* l2w, const fl
                                                       rs->materials[static_cast<size_t>(material)].get()));
     rs->indexNewShapes();
     return 0;
+}
+
+int32_t ref_scene_shape_count(void* s) {
+    return static_cast<int32_t>(static_cast<RefScene*>(s)->scene.shapes().size());
+}
+
+// MeshInstance::setMotionTransform of instance shape `shape` (before ref_scene_build).
+int32_t ref_scene_set_instance_motion(void* s, int32_t shape, const float* l2w, const float* w2l) {
+    auto* rs = static_cast<RefScene*>(s);
+    const auto& shapes = rs->scene.shapes();
+    if (shape < 0 || shape >= static_cast<int32_t>(shapes.size())) return -1;
+    auto* mi = dynamic_cast<MeshInstance*>(shapes[static_cast<size_t>(shape)].get());
+    if (!mi) return -1;
+    Mat4f m, inv;
+    for (int r = 0; r < 4; ++r)
+        for (int c = 0; c < 4; ++c) {
+            m(r, c) = l2w[4 * r + c];
+            if (w2l) inv(r, c) = w2l[4 * r + c];
+        }
+    mi->setMotionTransform(w2l ? Transform(m, inv) : Transform(m));
+    return 0;
+}
+
+// Camera::setShutterEnd of one of the reference's own cameras (ref_camera_create) to another's pose.
+void ref_camera_set_shutter_end(void* cam, void* end) {
+    static_cast<Camera*>(cam)->setShutterEnd(*static_cast<const Camera*>(end));
 }
 
 // Moves MeshInstance `shape`: a MeshInstance's matrix is fixed at construction, so an application
@@ -728,6 +770,14 @@ int32_t ref_scene_set_shape_name(void* s, int32_t shape, const char* name) {
     rs->scene.setShapeName(shapes[static_cast<size_t>(shape)].get(), name ? name : "");
     return 0;
 }
+// Shape::setVisibilityMask (shape.h:27-29) of shape `shape`.
+int32_t ref_scene_set_shape_visibility(void* s, int32_t shape, uint32_t mask) {
+    auto* rs = static_cast<RefScene*>(s);
+    const auto& shapes = rs->scene.shapes();
+    if (shape < 0 || shape >= static_cast<int32_t>(shapes.size())) return -1;
+    shapes[static_cast<size_t>(shape)]->setVisibilityMask(static_cast<uint8_t>(mask & VisAll));
+    return 0;
+}
 int32_t ref_scene_set_material_name(void* s, int32_t material, const char* name) {
     auto* rs = static_cast<RefScene*>(s);
     if (material < 0 || material >= static_cast<int32_t>(rs->materials.size())) return -1;
@@ -856,7 +906,8 @@ static int32_t renderRowsWith(RefScene* rs, const Camera& camera, const pe_setti
                     const float sx = (static_cast<float>(x) + 0.5f + offset.x) / static_cast<float>(w);
                     const float sy = 1.0f - (static_cast<float>(y) + 0.5f + offset.y) / static_cast<float>(h);
                     const Vec2f lens = sampler.get2D();
-                    Ray ray = camera.generateRay(sx, sy, lens);
+                    Ray ray = st->motion_blur ? camera.generateRay(sx, sy, lens, sampler.get1D())
+                                              : camera.generateRay(sx, sy, lens);
                     ray.coneWidth = camera.pixelConeWidth(h);
                     ray.coneSpread = camera.pixelConeSpread(h);
                     // as tracePixel: with a colour or transparent background the integrator gets
@@ -907,7 +958,8 @@ int32_t ref_render_rect(void* s, void* cam, const pe_settings* st, int32_t first
                 const float sx = (static_cast<float>(x) + 0.5f + offset.x) / static_cast<float>(w);
                 const float sy = 1.0f - (static_cast<float>(y) + 0.5f + offset.y) / static_cast<float>(h);
                 const Vec2f lens = sampler.get2D();
-                Ray ray = camera.generateRay(sx, sy, lens);
+                Ray ray = st->motion_blur ? camera.generateRay(sx, sy, lens, sampler.get1D())
+                                          : camera.generateRay(sx, sy, lens);
                 ray.coneWidth = camera.pixelConeWidth(h);
                 ray.coneSpread = camera.pixelConeSpread(h);
                 if (rs->scene.background().mode == Background::Mode::Environment) {

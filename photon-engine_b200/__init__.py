@@ -4,7 +4,7 @@ The product is ``libphoton_cuda.so`` (C ABI in ``include/photon_cuda.h``); this 
 host-side mirror of the reference's RenderDevice / RenderSession / Scene API over it.
 """
 from . import _capi
-from .engine import (AovFilms, AreaLight, Background, BackgroundMode, CudaDevice, Dielectric, DeviceFeatures, DeviceInfo,
+from .engine import (VIS_ALL, VIS_CAMERA, VIS_DIFFUSE, VIS_GLOSSY, VIS_SHADOW, VIS_TRANSMISSION, AovFilms, AreaLight, Background, BackgroundMode, CudaDevice, Dielectric, DeviceFeatures, DeviceInfo,
                      DisneyMaterial, EnvironmentLight, Film, Lambertian, LightPass, Material, MeshInstance, Mirror, OrthographicCamera, PerspectiveCamera, ThinLensCamera,
                      PixelFilterType, RenderMode, RenderPassFilms, RenderServer, RenderSession, RenderSettings, RenderTargets, RequestStatus,
                      SampleBatchResult,

@@ -48,14 +48,17 @@ class pe_material(C.Structure):
 
 class pe_camera(C.Structure):
     _fields_ = [("position", F3), ("lower_left", F3), ("horizontal", F3), ("vertical", F3),
-                ("u", F3), ("v", F3), ("forward", F3), ("lens_radius", C.c_float), ("orthographic", C.c_int32), ("blades", C.c_int32), ("blade_rotation", C.c_float)]
+                ("u", F3), ("v", F3), ("forward", F3), ("lens_radius", C.c_float), ("orthographic", C.c_int32), ("blades", C.c_int32), ("blade_rotation", C.c_float),
+                ("has_shutter_end", C.c_int32), ("end_position", F3), ("end_lower_left", F3), ("end_horizontal", F3),
+                ("end_vertical", F3), ("end_u", F3), ("end_v", F3), ("end_forward", F3), ("end_lens_radius", C.c_float)]
 
 
 class pe_settings(C.Structure):
     _fields_ = [("width", C.c_int32), ("height", C.c_int32), ("max_bounces", C.c_int32), ("rr_depth", C.c_int32),
                 ("shadow_quality", C.c_int32), ("filter_type", C.c_int32), ("filter_width", C.c_float),
                 ("clamp_indirect", C.c_float), ("seed", C.c_uint64), ("ao_strength", C.c_float),
-                ("adaptive_sampling", C.c_int32), ("noise_threshold", C.c_float), ("min_adaptive_samples", C.c_int32)]
+                ("adaptive_sampling", C.c_int32), ("noise_threshold", C.c_float), ("min_adaptive_samples", C.c_int32),
+                ("motion_blur", C.c_int32)]
 
 
 class pe_scene_info(C.Structure):
@@ -180,6 +183,7 @@ SIGNATURES = {
     "pe_scene_add_texture_u8": (C.c_int32, [P, C.POINTER(C.c_uint8), C.c_int32, C.c_int32, C.c_int32]),
     "pe_scene_set_material": (C.c_int32, [P, C.c_int32, C.POINTER(pe_material)]),
     "pe_scene_set_shape_name": (C.c_int32, [P, C.c_int32, C.c_char_p]),
+    "pe_scene_set_shape_visibility": (C.c_int32, [P, C.c_int32, C.c_uint32]),
     "pe_scene_set_material_name": (C.c_int32, [P, C.c_int32, C.c_char_p]),
     "pe_device_update_materials": (C.c_int32, [P, P]),
     "pe_device_update_lights": (C.c_int32, [P, P]),
@@ -188,6 +192,9 @@ SIGNATURES = {
     "pe_scene_add_instance": (C.c_int32, [P, C.c_int32, FP, FP, C.c_int32]),
     "pe_scene_set_instance_transform": (C.c_int32, [P, C.c_int32, FP, FP]),
     "pe_scene_refit": (C.c_int32, [P]),
+    "pe_scene_set_instance_motion": (C.c_int32, [P, C.c_int32, FP, FP]),
+    "pe_mat4_inverse": (None, [FP, FP]),
+    "pe_scene_shape_bounds": (C.c_int32, [P, C.c_int32, FP]),
     "pe_device_update_transforms": (C.c_int32, [P, P]),
     "pe_scene_add_sphere": (C.c_int32, [P, C.POINTER(C.c_float), C.c_float, C.c_int32]),
     "pe_scene_add_mesh": (C.c_int32, [P, FP, C.c_uint32, FP, FP, UP, C.c_uint32, C.c_int32]),

@@ -58,6 +58,15 @@ void put3(float* o, const Vec3f& v) {
 
 // The scene content as the C ABI's flat description, built once per setScene and kept for
 // incremental updates.
+// A Transform's matrix and inverse as the row-major arrays of the C ABI.
+void putTransform(const Transform& xf, float* m, float* inv) {
+    for (int r = 0; r < 4; ++r)
+        for (int c = 0; c < 4; ++c) {
+            m[4 * r + c] = xf.matrix()(r, c);
+            inv[4 * r + c] = xf.inverseMatrix()(r, c);
+        }
+}
+
 struct PeScene {
     pe_scene* s = nullptr;
     const Scene* source = nullptr;
@@ -108,12 +117,7 @@ struct PeScene {
                 mi->hasMotion())
                 return false;
             float l2w[16], w2l[16];
-            const Transform& xf = mi->transform0();
-            for (int r = 0; r < 4; ++r)
-                for (int c = 0; c < 4; ++c) {
-                    l2w[4 * r + c] = xf.matrix()(r, c);
-                    w2l[4 * r + c] = xf.inverseMatrix()(r, c);
-                }
+            putTransform(mi->transform0(), l2w, w2l);
             if (pe_scene_set_instance_transform(s, static_cast<int32_t>(i), l2w, w2l) != PE_OK) return false;
             placed[i].shape = now;
         }
@@ -266,22 +270,20 @@ struct PeScene {
                     }
                     it = blases.emplace(m, b).first;
                 }
-                if (mi->hasMotion()) {
-                    error = "moving mesh instances (motion blur) are not carried";
-                    return false;
-                }
                 const int32_t mat = material(mi->material());
                 if (mat < 0) return false;
                 float l2w[16], w2l[16];
-                const Transform& xf = mi->transform0();
-                for (int r = 0; r < 4; ++r)
-                    for (int c = 0; c < 4; ++c) {
-                        l2w[4 * r + c] = xf.matrix()(r, c);
-                        w2l[4 * r + c] = xf.inverseMatrix()(r, c);
-                    }
+                putTransform(mi->transform0(), l2w, w2l);
                 if (pe_scene_add_instance(s, it->second, l2w, w2l, mat) != PE_OK) {
                     error = pe_last_error();
                     return false;
+                }
+                if (mi->hasMotion()) { // setMotionTransform: the pose at shutter close
+                    putTransform(mi->transform1(), l2w, w2l);
+                    if (pe_scene_set_instance_motion(s, index, l2w, w2l) != PE_OK) {
+                        error = pe_last_error();
+                        return false;
+                    }
                 }
             } else if (auto* sp = dynamic_cast<const Sphere*>(shape)) {
                 const int32_t mat = material(sp->material());
@@ -316,6 +318,9 @@ struct PeScene {
                 pe_scene_tag_shape(s, index, it->second);
             if (auto it = names.find(shape); it != names.end() && !it->second.empty())
                 pe_scene_set_shape_name(s, index, it->second.c_str());
+            // an AreaLight's triangles carry their own camera visibility (pe_scene_add_area_light)
+            if (!dynamic_cast<const Triangle*>(shape) && shape->visibilityMask() != VisAll)
+                pe_scene_set_shape_visibility(s, index, shape->visibilityMask());
         }
         for (const auto& [m, name] : scene.materialNames())
             if (auto it = materials.find(m); it != materials.end() && !name.empty())
@@ -479,11 +484,23 @@ public:
         pc.orthographic = c.orthographic ? 1 : 0;
         pc.blades = c.blades;
         pc.blade_rotation = c.bladeRotation;
+        if (camera.hasShutterEnd()) { // Camera::setShutterEnd
+            const CameraGpuDesc e = camera.describeGpuEnd();
+            pc.has_shutter_end = 1;
+            put3(pc.end_position, e.position);
+            put3(pc.end_lower_left, e.lowerLeft);
+            put3(pc.end_horizontal, e.horizontal);
+            put3(pc.end_vertical, e.vertical);
+            put3(pc.end_u, e.u);
+            put3(pc.end_v, e.v);
+            put3(pc.end_forward, e.forward);
+            pc.end_lens_radius = e.lensRadius;
+        }
         // Renderer::renderSamples: Sobol seed 12345, roulette after depth 3 (renderer.cpp:431-432)
         pe_settings ps{w, h, settings.maxBounces, 3, settings.shadowQuality,
                        static_cast<int32_t>(settings.filter.type), settings.filter.width, settings.clampIndirect,
                        12345u, settings.aoStrength, settings.adaptiveSampling ? 1 : 0, settings.noiseThreshold,
-                       settings.minAdaptiveSamples};
+                       settings.minAdaptiveSamples, settings.motionBlur ? 1 : 0};
         // RenderSettings::pathGuiding: the SD-tree on the device (trained over samples 0-31)
         if (settings.pathGuiding != m_guiding) {
             if (pe_device_set_guiding(m_dev, settings.pathGuiding ? 2 : 0, 0, 0.0f) != PE_OK) return r;

@@ -34,6 +34,7 @@ int32_t allocLane(WaveLane& ln, size_t slots) {
         if ((st = devAlloc(ln.bufs, *c, slots))) return st;
     if ((st = devAlloc(ln.bufs, P.counters, CNT_TOTAL))) return st;
     if ((st = devAlloc(ln.bufs, P.cone, slots))) return st;
+    if ((st = devAlloc(ln.bufs, P.time, slots))) return st;
     // path regeneration: slot → path, freed slots, radiance of kStreamFactor × slots paths
     if ((st = devAlloc(ln.bufs, ln.pathOf, slots))) return st;
     if ((st = devAlloc(ln.bufs, ln.freeQ, slots))) return st;
@@ -143,6 +144,18 @@ WaveSeg makeSeg(const pe_camera* cam, const pe_settings* st) {
     A.cam.blades = cam->blades >= 3 ? cam->blades : 0;
     A.cam.bladeRotation = cam->blade_rotation;
     A.cam.orthographic = cam->orthographic ? 1 : 0;
+    A.cam.hasEnd = cam->has_shutter_end ? 1 : 0;
+    if (A.cam.hasEnd) {
+        A.cam.position1 = m3f(cam->end_position);
+        A.cam.lowerLeft1 = m3f(cam->end_lower_left);
+        A.cam.horizontal1 = m3f(cam->end_horizontal);
+        A.cam.vertical1 = m3f(cam->end_vertical);
+        A.cam.u1 = m3f(cam->end_u);
+        A.cam.v1 = m3f(cam->end_v);
+        A.cam.forward1 = m3f(cam->end_forward);
+        A.cam.lensRadius1 = cam->end_lens_radius;
+    }
+    A.flags = st->motion_blur ? SEG_MOTION : 0;
     A.width = st->width;
     A.height = st->height;
     A.seed = st->seed;
@@ -1092,6 +1105,8 @@ int32_t uploadScene(pe_device* d, const pe_scene* s, SceneGPU& G, std::vector<De
     }
     G.nTextures = static_cast<int32_t>(s->textures.size());
     G.nInstances = static_cast<int32_t>(B.instances.size());
+    // moving instances: null without, which also keeps the kernels from reading path times
+    if (!B.motions.empty() && (rc = upload(d, bufs, G.motions, B.motions))) return rc;
     G.leanShading = leanShadingOf(G, B.materials);
     G.materialTypes = 0;
     for (const MatGPU& m : B.materials) G.materialTypes |= 1 << m.type;
@@ -1805,6 +1820,11 @@ int32_t pe_device_render_tile_noalloc(pe_device* d, const pe_camera* cam, const 
     if (d->guideKind != 0) {
         setError("pe_device_render_tile_noalloc: guided sampling (pe_device_set_guiding) is on; the tile entry "
                  "renders unguided paths only");
+        return PE_ERR_INVALID;
+    }
+    if (d->scene.motions && st->motion_blur) {
+        setError("pe_device_render_tile_noalloc: motion blur over moving instances needs a shutter time per path, "
+                 "which the fixed scratch does not hold; use pe_device_render");
         return PE_ERR_INVALID;
     }
     if (d->scene.hasMips) {

@@ -293,7 +293,7 @@ __global__ void kGuideQuery(SceneGPU S, Paths P, Wave W, const int32_t* queue, c
                 h.v = hr.z;
                 h.prim = prim;
                 Isect is;
-                fillHit(S, h, mk(ro.x, ro.y, ro.z), mk(rd.x, rd.y, rd.z), is);
+                fillHit(S, h, mk(ro.x, ro.y, ro.z), mk(rd.x, rd.y, rd.z), is, pathTime(S, P, slot));
                 const MatGPU& m = S.materials[is.material];
                 want = (m.flags & (MF_DELTA | MF_VOLUME_BOUNDARY | MF_TRANSMITS_SHADOWS)) == 0;
                 pnt = is.point;

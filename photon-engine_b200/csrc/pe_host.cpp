@@ -16,6 +16,7 @@
 #include "pe_bsdf.h"
 #include "pe_light.h"
 #include "pe_medium.h"
+#include "pe_xform.h"
 
 #include <algorithm>
 #include <cmath>
@@ -99,45 +100,6 @@ struct RefNode { // BVHNode (bvh.h:27-36): 32-byte depth-first node
 constexpr uint32_t VIS_ALL_MASK = 0x1Fu; // a BLAS is traversed with every visibility bit (mesh_instance.cpp:110)
 constexpr int32_t kNoRoot = static_cast<int32_t>(0x80000000u);
 
-// Mat4f::inverse (mat.h:130-175): cofactors from the 2×2 minors of the top and bottom row pairs,
-// identity for a singular matrix.
-void mat4Inverse(const float* m, float* o) {
-    auto d = [&](int r, int c) { return m[4 * r + c]; };
-    const float s0 = d(0, 0) * d(1, 1) - d(1, 0) * d(0, 1);
-    const float s1 = d(0, 0) * d(1, 2) - d(1, 0) * d(0, 2);
-    const float s2 = d(0, 0) * d(1, 3) - d(1, 0) * d(0, 3);
-    const float s3 = d(0, 1) * d(1, 2) - d(1, 1) * d(0, 2);
-    const float s4 = d(0, 1) * d(1, 3) - d(1, 1) * d(0, 3);
-    const float s5 = d(0, 2) * d(1, 3) - d(1, 2) * d(0, 3);
-    const float c5 = d(2, 2) * d(3, 3) - d(3, 2) * d(2, 3);
-    const float c4 = d(2, 1) * d(3, 3) - d(3, 1) * d(2, 3);
-    const float c3 = d(2, 1) * d(3, 2) - d(3, 1) * d(2, 2);
-    const float c2 = d(2, 0) * d(3, 3) - d(3, 0) * d(2, 3);
-    const float c1 = d(2, 0) * d(3, 2) - d(3, 0) * d(2, 2);
-    const float c0 = d(2, 0) * d(3, 1) - d(3, 0) * d(2, 1);
-    const float det = s0 * c5 - s1 * c4 + s2 * c3 + s3 * c2 - s4 * c1 + s5 * c0;
-    if (det == 0.0f) {
-        for (int k = 0; k < 16; ++k) o[k] = (k % 5 == 0) ? 1.0f : 0.0f;
-        return;
-    }
-    const float id = 1.0f / det;
-    o[0] = (d(1, 1) * c5 - d(1, 2) * c4 + d(1, 3) * c3) * id;
-    o[1] = (-d(0, 1) * c5 + d(0, 2) * c4 - d(0, 3) * c3) * id;
-    o[2] = (d(3, 1) * s5 - d(3, 2) * s4 + d(3, 3) * s3) * id;
-    o[3] = (-d(2, 1) * s5 + d(2, 2) * s4 - d(2, 3) * s3) * id;
-    o[4] = (-d(1, 0) * c5 + d(1, 2) * c2 - d(1, 3) * c1) * id;
-    o[5] = (d(0, 0) * c5 - d(0, 2) * c2 + d(0, 3) * c1) * id;
-    o[6] = (-d(3, 0) * s5 + d(3, 2) * s2 - d(3, 3) * s1) * id;
-    o[7] = (d(2, 0) * s5 - d(2, 2) * s2 + d(2, 3) * s1) * id;
-    o[8] = (d(1, 0) * c4 - d(1, 1) * c2 + d(1, 3) * c0) * id;
-    o[9] = (-d(0, 0) * c4 + d(0, 1) * c2 - d(0, 3) * c0) * id;
-    o[10] = (d(3, 0) * s4 - d(3, 1) * s2 + d(3, 3) * s0) * id;
-    o[11] = (-d(2, 0) * s4 + d(2, 1) * s2 - d(2, 3) * s0) * id;
-    o[12] = (-d(1, 0) * c3 + d(1, 1) * c1 - d(1, 2) * c0) * id;
-    o[13] = (d(0, 0) * c3 - d(0, 1) * c1 + d(0, 2) * c0) * id;
-    o[14] = (-d(3, 0) * s3 + d(3, 1) * s1 - d(3, 2) * s0) * id;
-    o[15] = (d(2, 0) * s3 - d(2, 1) * s1 + d(2, 2) * s0) * id;
-}
 
 // Transform::transformPoint (transform.cpp:15-26).
 V3 xfPoint(const float* m, V3 p) {
@@ -173,10 +135,102 @@ Box xfAABB(const float* m, const Box& b) {
     return r;
 }
 
-// det3x3 of mesh_instance.cpp:11-15.
-float det3x3(const float* m) {
-    return m[0] * (m[5] * m[10] - m[6] * m[9]) - m[1] * (m[4] * m[10] - m[6] * m[8]) +
-           m[2] * (m[4] * m[9] - m[5] * m[8]);
+
+// decomposeTRS (quat.cpp): translation, unit rotation (Quatf::fromMat3 of the orthonormalised
+// columns) and signed scale of an affine matrix.
+void decomposeTRS(const float* m, float* pos, float* rot, float* scale) {
+    pos[0] = m[3];
+    pos[1] = m[7];
+    pos[2] = m[11];
+    const V3 c0 = mk(m[0], m[4], m[8]), c1 = mk(m[1], m[5], m[9]), c2 = mk(m[2], m[6], m[10]);
+    const float sx = length(c0), sy = length(c1);
+    float sz = length(c2);
+    const float det = dot(c0, cross(c1, c2));
+    if (det < 0.0f) sz = -sz;
+    scale[0] = sx;
+    scale[1] = sy;
+    scale[2] = sz;
+    const V3 x = sx > 1e-8f ? c0 / sx : mk(1.0f, 0.0f, 0.0f);
+    V3 y = sy > 1e-8f ? c1 / sy : mk(0.0f, 1.0f, 0.0f);
+    y = y - x * dot(x, y);
+    if (len2(y) > 1e-12f) y = normalize(y);
+    else y = std::fabs(x.y) < 0.9f ? normalize(cross(x, mk(0.0f, 1.0f, 0.0f))) : normalize(cross(x, mk(1.0f, 0.0f, 0.0f)));
+    const V3 z = normalize(cross(x, y));
+    // Quatf::fromMat3 of r = [x y z] (columns)
+    const float r00 = x.x, r10 = x.y, r20 = x.z, r01 = y.x, r11 = y.y, r21 = y.z, r02 = z.x, r12 = z.y, r22 = z.z;
+    const float trace = r00 + r11 + r22;
+    float q[4];
+    if (trace > 0.0f) {
+        const float s = std::sqrt(trace + 1.0f) * 2.0f;
+        q[3] = 0.25f * s;
+        q[0] = (r21 - r12) / s;
+        q[1] = (r02 - r20) / s;
+        q[2] = (r10 - r01) / s;
+    } else if (r00 > r11 && r00 > r22) {
+        const float s = std::sqrt(std::max(1e-12f, 1.0f + r00 - r11 - r22)) * 2.0f;
+        q[3] = (r21 - r12) / s;
+        q[0] = 0.25f * s;
+        q[1] = (r01 + r10) / s;
+        q[2] = (r02 + r20) / s;
+    } else if (r11 > r22) {
+        const float s = std::sqrt(std::max(1e-12f, 1.0f + r11 - r00 - r22)) * 2.0f;
+        q[3] = (r02 - r20) / s;
+        q[0] = (r01 + r10) / s;
+        q[1] = 0.25f * s;
+        q[2] = (r12 + r21) / s;
+    } else {
+        const float s = std::sqrt(std::max(1e-12f, 1.0f + r22 - r00 - r11)) * 2.0f;
+        q[3] = (r10 - r01) / s;
+        q[0] = (r02 + r20) / s;
+        q[1] = (r12 + r21) / s;
+        q[2] = 0.25f * s;
+    }
+    quatNormalized(q, rot);
+}
+
+// The time-independent half of interpolateTransform(t0, t1, ·) (quat.cpp): both poses decomposed,
+// the rotations normalised (Quatf::slerp), the second flipped onto the short arc, the arc's angle
+// and sine by the C library.
+MotionTRS motionTRS(const float* m0, const float* m1) {
+    MotionTRS M;
+    std::memset(&M, 0, sizeof(M));
+    float r0[4], r1[4], a[4], b[4];
+    decomposeTRS(m0, M.p0, r0, M.s0);
+    decomposeTRS(m1, M.p1, r1, M.s1);
+    quatNormalized(r0, a);
+    quatNormalized(r1, b);
+    for (int k = 0; k < 4; ++k) {
+        M.qa[k] = static_cast<double>(a[k]);
+        M.qb[k] = static_cast<double>(b[k]);
+    }
+    double d = M.qa[0] * M.qb[0] + M.qa[1] * M.qb[1] + M.qa[2] * M.qb[2] + M.qa[3] * M.qb[3];
+    if (d < 0.0) {
+        d = -d;
+        for (int k = 0; k < 4; ++k) M.qb[k] = -M.qb[k];
+    }
+    M.linear = d > 0.9995 ? 1 : 0;
+    M.theta = std::acos(d < -1.0 ? -1.0 : (d > 1.0 ? 1.0 : d));
+    M.sinT = std::sin(M.theta);
+    return M;
+}
+
+// MeshInstance::recomputeBounds (mesh_instance.cpp:36-53): the local box under the transform, or
+// for a moving instance the union over five poses a = 0, 1/4, .., 1 of the shutter.
+Box instanceBox(const HostShape& sh, const Box& local) {
+    if (!sh.motion) return xfAABB(sh.l2w, local);
+    const MotionTRS M = motionTRS(sh.l2w, sh.l2w1);
+    Box merged;
+    for (int i = 0; i <= 4; ++i) {
+        const float a = static_cast<float>(i) / 4.0f;
+        float m[16], inv[16];
+        const float* use = m;
+        if (a <= 0.0f) use = sh.l2w;
+        else if (a >= 1.0f) use = sh.l2w1;
+        else motionPoseAt(M, a, m, inv);
+        const Box b = xfAABB(use, local);
+        merged = merged.merged(b);
+    }
+    return merged;
 }
 
 class SahBuilder {
@@ -1184,7 +1238,7 @@ static int32_t buildScene(pe_scene* s) {
             const HostBlas& hb = s->blases[static_cast<size_t>(sh.blas)];
             Box lb;
             for (const V3& p : hb.pos) lb = lb.merged(Box{p, p});
-            triBounds[t0] = xfAABB(sh.l2w, lb);
+            triBounds[t0] = instanceBox(sh, lb);
             triMask[t0] = sh.mask;
             info.firstTri = blasFirstTri[static_cast<size_t>(sh.blas)];
             t0 += 1;
@@ -1252,6 +1306,7 @@ static int32_t buildScene(pe_scene* s) {
     // SAH BVH
     B.tlasPrims = nTlas;
     B.instances.clear();
+    B.motions.clear();
     std::vector<int> instOfShape(s->shapes.size(), -1);
     for (size_t si = 0; si < s->shapes.size(); ++si)
         if (s->shapes[si].blas >= 0) {
@@ -1424,7 +1479,20 @@ static int32_t buildScene(pe_scene* s) {
         g.firstTri = static_cast<int32_t>(blasFirstTri[bl]);
         g.shape = static_cast<int32_t>(si);
         g.material = sh.material;
-        g.uvScale = std::cbrt(std::max(std::fabs(det3x3(sh.l2w)), 1e-12f));
+        g.uvScale = uvScaleOf(sh.l2w);
+        g.motion = -1;
+        if (sh.motion) {
+            g.motion = static_cast<int32_t>(B.motions.size());
+            InstMotionGPU mg;
+            std::memset(&mg, 0, sizeof(mg));
+            for (int r = 0; r < 4; ++r) {
+                mg.l2w1[r] = f4(sh.l2w1[4 * r], sh.l2w1[4 * r + 1], sh.l2w1[4 * r + 2], sh.l2w1[4 * r + 3]);
+                mg.w2l1[r] = f4(sh.w2l1[4 * r], sh.w2l1[4 * r + 1], sh.w2l1[4 * r + 2], sh.w2l1[4 * r + 3]);
+            }
+            mg.trs = motionTRS(sh.l2w, sh.l2w1);
+            mg.uvScale1 = uvScaleOf(sh.l2w1);
+            B.motions.push_back(mg);
+        }
     }
 
     buildLightSampler(s, B);
@@ -1810,6 +1878,10 @@ int32_t pe_scene_set_instance_transform(pe_scene* s, int32_t shape, const float 
         setError("pe_scene_set_instance_transform: an emissive instance moves its lights; rebuild the scene");
         return PE_ERR_LIMIT;
     }
+    if (sh.motion) {
+        setError("pe_scene_set_instance_transform: a moving instance; rebuild the scene");
+        return PE_ERR_LIMIT;
+    }
     std::memcpy(sh.l2w, localToWorld, sizeof(sh.l2w));
     if (worldToLocal) std::memcpy(sh.w2l, worldToLocal, sizeof(sh.w2l));
     else mat4Inverse(sh.l2w, sh.w2l);
@@ -1840,7 +1912,7 @@ int32_t pe_scene_refit(pe_scene* s) {
         const HostBlas& hb = s->blases[static_cast<size_t>(sh.blas)];
         Box lb;
         for (const V3& q : hb.pos) lb = lb.merged(Box{q, q});
-        const Box wb = xfAABB(sh.l2w, lb);
+        const Box wb = instanceBox(sh, lb);
         const float v[6] = {wb.lo.x, wb.lo.y, wb.lo.z, wb.hi.x, wb.hi.y, wb.hi.z};
         std::copy(v, v + 6, &B.tlasPrimBounds[6 * p]);
     }
@@ -1898,7 +1970,7 @@ int32_t pe_scene_refit(pe_scene* s) {
             g.w2l[r] = f4(sh.w2l[4 * r], sh.w2l[4 * r + 1], sh.w2l[4 * r + 2], sh.w2l[4 * r + 3]);
             g.l2w[r] = f4(sh.l2w[4 * r], sh.l2w[4 * r + 1], sh.l2w[4 * r + 2], sh.l2w[4 * r + 3]);
         }
-        g.uvScale = std::cbrt(std::max(std::fabs(det3x3(sh.l2w)), 1e-12f));
+        g.uvScale = uvScaleOf(sh.l2w);
     }
     ++s->refitVersion;
     return PE_OK;
@@ -2110,6 +2182,60 @@ int32_t pe_scene_set_shape_name(pe_scene* s, int32_t shape, const char* name) {
     return PE_OK;
 }
 
+int32_t pe_scene_set_instance_motion(pe_scene* s, int32_t shape, const float localToWorldEnd[16],
+                                     const float worldToLocalEnd[16]) {
+    if (!s || !localToWorldEnd || shape < 0 || shape >= static_cast<int32_t>(s->shapes.size()) ||
+        s->shapes[static_cast<size_t>(shape)].blas < 0) {
+        setError("pe_scene_set_instance_motion: not a mesh instance");
+        return PE_ERR_INVALID;
+    }
+    HostShape& sh = s->shapes[static_cast<size_t>(shape)];
+    sh.motion = true;
+    std::memcpy(sh.l2w1, localToWorldEnd, sizeof(sh.l2w1));
+    if (worldToLocalEnd) std::memcpy(sh.w2l1, worldToLocalEnd, sizeof(sh.w2l1));
+    else mat4Inverse(sh.l2w1, sh.w2l1);
+    s->built = false;
+    return PE_OK;
+}
+
+int32_t pe_scene_shape_bounds(const pe_scene* s, int32_t shape, float out[6]) {
+    if (!s || !out || shape < 0 || shape >= static_cast<int32_t>(s->shapes.size())) {
+        setError("pe_scene_shape_bounds: no such shape");
+        return PE_ERR_INVALID;
+    }
+    const HostShape& sh = s->shapes[static_cast<size_t>(shape)];
+    Box b;
+    if (sh.blas >= 0) {
+        Box local;
+        for (const V3& p : s->blases[static_cast<size_t>(sh.blas)].pos) local = local.merged(Box{p, p});
+        b = instanceBox(sh, local);
+    } else if (sh.sphere) {
+        b = Box{sh.center - mk(sh.radius), sh.center + mk(sh.radius)};
+    } else {
+        for (const V3& p : sh.pos) b = b.merged(Box{p, p});
+    }
+    const float v[6] = {b.lo.x, b.lo.y, b.lo.z, b.hi.x, b.hi.y, b.hi.z};
+    std::copy(v, v + 6, out);
+    return PE_OK;
+}
+
+void pe_mat4_inverse(const float m[16], float out[16]) {
+    if (m && out) mat4Inverse(m, out);
+}
+
+// Shape::setVisibilityMask (shape.h:27-29): the ray classes (camera, diffuse, glossy,
+// transmission, shadow) that see shape `shape`; a mesh instance's mask is tested at the top level
+// only (mesh_instance.cpp:106).
+int32_t pe_scene_set_shape_visibility(pe_scene* s, int32_t shape, uint32_t mask) {
+    if (!s || shape < 0 || shape >= static_cast<int32_t>(s->shapes.size())) {
+        setError("pe_scene_set_shape_visibility: no such shape");
+        return PE_ERR_INVALID;
+    }
+    s->shapes[static_cast<size_t>(shape)].mask = static_cast<uint8_t>(mask & 0x1Fu);
+    s->built = false;
+    return PE_OK;
+}
+
 int32_t pe_scene_set_material_name(pe_scene* s, int32_t material, const char* name) {
     if (!s || material < 0) {
         setError("pe_scene_set_material_name: bad argument");
@@ -2276,7 +2402,8 @@ int32_t pe_scene_get_info(const pe_scene* s, pe_scene_info* out) {
     out->light_sampler_mode = B.lightMode;
     out->device_bytes = B.nodes.size() * sizeof(float4) + B.tris.size() * sizeof(float4) +
                         B.triVerts.size() * sizeof(int4) + B.pos.size() * sizeof(float4) * 2 + B.uv.size() * sizeof(float2) +
-                        B.wide.size() * sizeof(float4) + B.instances.size() * sizeof(InstGPU);
+                        B.wide.size() * sizeof(float4) + B.instances.size() * sizeof(InstGPU) +
+                        B.motions.size() * sizeof(InstMotionGPU);
     return s->built ? PE_OK : PE_ERR_INVALID;
 }
 

@@ -22,6 +22,8 @@ struct HostShape {
     float radius = 0.0f;
     int32_t blas = -1;          // a MeshInstance of this BLAS (src/geometry/mesh_instance.h): one primitive
     float l2w[16] = {}, w2l[16] = {}; // its local-to-world matrix and inverse, row-major
+    bool motion = false;        // MeshInstance::setMotionTransform: the pose at shutter close
+    float l2w1[16] = {}, w2l1[16] = {};
 };
 
 // A mesh kept for instancing: its own BVH (BLAS), shared by its instances.
@@ -60,6 +62,7 @@ struct HostBuild {
     std::vector<float4> wide;        // 8 per 4-wide node (traversal kernels)
     int wideDepth = 0;
     std::vector<InstGPU> instances;  // per MeshInstance shape (in shape order)
+    std::vector<InstMotionGPU> motions; // per moving instance
     uint32_t tlasPrims = 0;          // leaf records of the top-level tree; BLAS records follow
     // the top-level tree as built, for refitting its boxes after instance transforms change
     struct TreeNode {

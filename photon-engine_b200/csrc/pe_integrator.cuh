@@ -114,7 +114,9 @@ __device__ __forceinline__ void generatePath(const SceneGPU& S, const Paths& P, 
     sb.revIndex = rev32(static_cast<uint32_t>(A.sampleFirst + sOff));
     sb.dim = 0;
     V3 o, d;
-    cameraRay(T, A.filterCdf, A.cam, A.filterWidth, x, y, A.width, A.height, sb, o, d);
+    float time;
+    cameraRay(T, A.filterCdf, A.cam, A.filterWidth, x, y, A.width, A.height, sb, o, d, (A.flags & SEG_MOTION) != 0, &time);
+    if (S.motions && P.time) P.time[slot] = time;
     P.rayO[slot] = make_float4(o.x, o.y, o.z, __uint_as_float(VIS_CAMERA));
     P.rayD[slot] = make_float4(d.x, d.y, d.z, 0.0f);
     P.thr[slot] = make_float4(1.0f, 1.0f, 1.0f, 0.0f);
@@ -239,9 +241,10 @@ __global__ void __launch_bounds__(128) kIntersect(SceneGPU S, Paths P, const int
             const float4 rd = P.rayD[slot];
             const V3 o = mk(ro.x, ro.y, ro.z), d = mk(rd.x, rd.y, rd.z);
             const uint32_t vmask = __float_as_uint(ro.w);
-            const Hit h = MODE == TRACE_BINARY ? traceClosest<COUNT>(S, o, d, vmask, 0.0f, 1e30f, nodes, tris)
+            const float time = pathTime(S, P, slot);
+            const Hit h = MODE == TRACE_BINARY ? traceClosest<COUNT>(S, o, d, vmask, 0.0f, 1e30f, nodes, tris, time)
                                                : traceClosestWide<COUNT, SD>(S, o, d, vmask, 0.0f, 1e30f, nodes, tris,
-                                                                             sstack + threadIdx.x);
+                                                                             sstack + threadIdx.x, time);
             P.hit[slot] = make_float4(h.t, h.u, h.v, __int_as_float(h.prim));
             key = (__float_as_uint(ro.w) & RAY_WALK) ? kShadeKeys - 1
                   : (isMiss(h.prim) ? 0 : 1 + static_cast<int>((h.meta >> 8) & 0xFFu));
@@ -306,18 +309,19 @@ __device__ __forceinline__ bool shadowLinkFor(const SceneGPU& S, int light) {
 // multiplying the transmittance of thin-walled glass and cutouts, and stops black at any other
 // surface.
 template <bool COUNT>
-__device__ V3 shadowVisibility(const SceneGPU& S, V3 o, V3 d, float tMax, int light, uint32_t& nodes, uint32_t& tris) {
+__device__ V3 shadowVisibility(const SceneGPU& S, V3 o, V3 d, float tMax, int light, uint32_t& nodes, uint32_t& tris,
+                              float time) {
     const bool link = shadowLinkFor(S, light);
     if (!S.hasShadowTransmitters && !link)
-        return traceAnyWide<COUNT>(S, o, d, VIS_SHADOW, 0.0f, tMax, nodes, tris) ? mk(0.0f) : mk(1.0f);
+        return traceAnyWide<COUNT>(S, o, d, VIS_SHADOW, 0.0f, tMax, nodes, tris, time) ? mk(0.0f) : mk(1.0f);
     V3 T = mk(1.0f);
     V3 origin = o;
     float remaining = tMax;
     for (int i = 0; i < 64; ++i) {
-        const Hit h = traceClosestWide<COUNT>(S, origin, d, VIS_SHADOW, 0.0f, remaining, nodes, tris);
+        const Hit h = traceClosestWide<COUNT>(S, origin, d, VIS_SHADOW, 0.0f, remaining, nodes, tris, nullptr, time);
         if (isMiss(h.prim)) return T;
         Isect is;
-        fillHit(S, h, origin, d, is);
+        fillHit(S, h, origin, d, is, time);
         if (link && !linkAllows(S.links[light].shadowMode, S.links[light].shadowMask, S.shapes[is.shape].linkNode)) {
             origin = offsetRayOrigin(is.point, is.pError, len2(is.ng) > 0.0f ? is.ng : is.normal, d);
             remaining -= h.t;
@@ -363,9 +367,11 @@ __global__ void __launch_bounds__(128) kShadow(SceneGPU S, Paths P, const uint32
         const float4 so = P.shO[i];
         const float4 sd = P.shD[i];
         const int light = static_cast<int>(__float_as_uint(P.shC[i].w) >> 1) - 1;
+        const float time = pathTime(S, P, slot);
         const V3 vis = ANY ? (traceAnyWide<COUNT>(S, mk(so.x, so.y, so.z), mk(sd.x, sd.y, sd.z), VIS_SHADOW, 0.0f, so.w, nodes,
-                                              tris) ? mk(0.0f) : mk(1.0f))
-                           : shadowVisibility<COUNT>(S, mk(so.x, so.y, so.z), mk(sd.x, sd.y, sd.z), so.w, light, nodes, tris);
+                                              tris, time) ? mk(0.0f) : mk(1.0f))
+                           : shadowVisibility<COUNT>(S, mk(so.x, so.y, so.z), mk(sd.x, sd.y, sd.z), so.w, light, nodes, tris,
+                                                     time);
         if (isBlack(vis)) continue;
         const float4 sc = P.shC[i];
         const float4 st = P.shT[i];
@@ -547,7 +553,8 @@ __device__ __noinline__ bool sdGuidedSample(const TablesGPU* T, const MatGPU& ma
 // ---- surface effects of Li that cast rays of their own ------------------------------------------
 // Contact ambient occlusion (approxAo, path_tracer.cpp:27-45): `samples` cosine rays of at most
 // 0.35 over the shading normal; the path's throughput is scaled by lerp(1, visibility, strength).
-__device__ __noinline__ float approxAo(const SceneGPU& S, const Isect& is, Sobol& sb, float strength, int samples) {
+__device__ __noinline__ float approxAo(const SceneGPU& S, const Isect& is, Sobol& sb, float strength, int samples,
+                                       float time) {
     if (strength <= 0.0f || samples <= 0) return 1.0f;
     const TablesGPU* T = S.tables;
     const Frame frame = frameFromNormal(is.normal);
@@ -556,7 +563,7 @@ __device__ __noinline__ float approxAo(const SceneGPU& S, const Isect& is, Sobol
     for (int i = 0; i < samples; ++i) {
         const V3 local = sampleCosineHemisphere(get2D(T, sb));
         const V3 dir = normalize(toWorld(frame, local));
-        if (traceAnyWide<false>(S, spawnOrigin(is, dir), dir, VIS_SHADOW, 0.0f, 0.35f, n0, n1)) occ += 1.0f;
+        if (traceAnyWide<false>(S, spawnOrigin(is, dir), dir, VIS_SHADOW, 0.0f, 0.35f, n0, n1, time)) occ += 1.0f;
     }
     const float visibility = 1.0f - (occ / static_cast<float>(samples));
     return lerpf(1.0f, visibility, strength);
@@ -566,7 +573,7 @@ __device__ __noinline__ float approxAo(const SceneGPU& S, const Isect& is, Sobol
 // around the hit, each probed along one of the frame's axes (normal ½, tangents ¼ each) from both
 // sides with rays of 2·radius; the outward normals of hits on the same shape within 1.5·radius,
 // weighted by their projection on the probe axis, average with a quarter of the own normal.
-__device__ __noinline__ V3 roundedEdgeNormal(const SceneGPU& S, const Isect& is, float radius, Sobol& sb) {
+__device__ __noinline__ V3 roundedEdgeNormal(const SceneGPU& S, const Isect& is, float radius, Sobol& sb, float time) {
     const TablesGPU* T = S.tables;
     const V3 N = is.normal;
     const Frame f = frameFromNormal(N);
@@ -588,10 +595,10 @@ __device__ __noinline__ V3 roundedEdgeNormal(const SceneGPU& S, const Isect& is,
             const float sign = k == 0 ? 1.0f : -1.0f;
             const V3 origin = is.point + s * d.x + t * d.y + axis * (sign * radius);
             const V3 rdir = axis * -sign;
-            const Hit h = traceClosestWide<false>(S, origin, rdir, VIS_ALL, 0.0f, 2.0f * radius, n0, n1);
+            const Hit h = traceClosestWide<false>(S, origin, rdir, VIS_ALL, 0.0f, 2.0f * radius, n0, n1, nullptr, time);
             if (isMiss(h.prim)) continue;
             Isect hit;
-            fillHit(S, h, origin, rdir, hit);
+            fillHit(S, h, origin, rdir, hit, time);
             if (hit.shape != is.shape) continue;
             if (len2(hit.point - is.point) > 2.25f * radius * radius) continue;
             const V3 outward = hit.frontFace ? hit.normal : -hit.normal;
@@ -608,7 +615,7 @@ __device__ __noinline__ V3 roundedEdgeNormal(const SceneGPU& S, const Isect& is,
 // background `bg` times the share `ratio` of the direct light, over 4 × shadowSamples NEE
 // samples, that reaches the hit point.
 __device__ __noinline__ V3 shadowCatcher(const SceneGPU& S, const Isect& is, V3 dir, int shadowSamples, Sobol& sb,
-                                         float& ratioOut) {
+                                         float& ratioOut, float time) {
     const TablesGPU* T = S.tables;
     V3 bg = mk(0.0f);
     if (S.bgMode == PE_BG_COLOR) bg = m3f(S.bgColor);
@@ -641,7 +648,7 @@ __device__ __noinline__ V3 shadowCatcher(const SceneGPU& S, const Isect& is, V3 
             V3 so, sd;
             float stMax;
             if (makeShadowRay(is, ls.wi, ls.distance, so, sd, stMax))
-                visible += c * luminance(shadowVisibility<false>(S, so, sd, stMax, li < S.nLights ? li : -1, n0, n1));
+                visible += c * luminance(shadowVisibility<false>(S, so, sd, stMax, li < S.nLights ? li : -1, n0, n1, time));
         }
     }
     ratioOut = total > 0.0f ? sclamp(visible / total, 0.0f, 1.0f) : 1.0f;
@@ -717,6 +724,7 @@ __device__ __forceinline__ bool shadeSlot(const SceneGPU& S, const Paths& P, con
     const int explicitLights = S.nLights;
     const int prim = __float_as_int(hr.w);
     const bool hit = KEY == 0 ? false : (KEY > 0 ? true : !isMiss(prim));
+    const float time = pathTime(S, P, slot);
     // ray cone (path_tracer.cpp:428-454, 777-783, 853-857): only scenes with mipmapped textures
     const bool cones = !LEAN && S.hasMips && P.cone;
     float2 cone = cones ? P.cone[slot] : make_float2(0.0f, 0.0f);
@@ -745,7 +753,7 @@ __device__ __forceinline__ bool shadeSlot(const SceneGPU& S, const Paths& P, con
                 h.u = hr.y;
                 h.v = hr.z;
                 h.prim = prim;
-                fillHit(S, h, rayO, dir, is);
+                fillHit(S, h, rayO, dir, is, time);
                 // exit vertex: outward normal, white Lambert; the depth does not grow
                 is.normal = -is.normal;
                 is.material = S.exitMaterial;
@@ -774,7 +782,7 @@ __device__ __forceinline__ bool shadeSlot(const SceneGPU& S, const Paths& P, con
             h.u = hr.y;
             h.v = hr.z;
             h.prim = prim;
-            fillHit(S, h, rayO, dir, is);
+            fillHit(S, h, rayO, dir, is, time);
             // Camera-invisible light quads (for camera rays) and cutouts are passed through;
             // the vertex does not count (path_tracer.cpp:426-439).
             if (skips < 64 && ((cameraRay && (S.shapes[is.shape].flags & SF_CAMERA_INVISIBLE)) ||
@@ -880,7 +888,7 @@ __device__ __forceinline__ bool shadeSlot(const SceneGPU& S, const Paths& P, con
             } else if (!LEAN && cameraRay && is.shape == S.catcherShape) {
                 // the shadow catcher ends the camera path with the shadowed background
                 float ratio = 1.0f;
-                const V3 bg = shadowCatcher(S, is, dir, shadowSamples, sb, ratio);
+                const V3 bg = shadowCatcher(S, is, dir, shadowSamples, sb, ratio, time);
                 const V3 added = addL(L, thr * bg * ratio);
                 if ((OUT && P.pass)) {
                     passAdd(passBlock(P, path) + PASS_BACKGROUND, added);
@@ -951,10 +959,10 @@ __device__ __forceinline__ bool shadeSlot(const SceneGPU& S, const Paths& P, con
         // rounded edges on the first three vertices (not a walk's exit vertex), then contact AO at
         // the camera hit (path_tracer.cpp:612-621)
         if (!LEAN && depth <= 2 && mat.roundEdge > 0.0f && !exitVertex) {
-            const V3 n = roundedEdgeNormal(S, is, mat.roundEdge, sb);
+            const V3 n = roundedEdgeNormal(S, is, mat.roundEdge, sb, time);
             if (dot(n, wo) > 0.02f) is.normal = n;
         }
-        if (!LEAN && A.aoStrength > 0.0f && depth == 0) thr *= approxAo(S, is, sb, A.aoStrength, shadowSamples);
+        if (!LEAN && A.aoStrength > 0.0f && depth == 0) thr *= approxAo(S, is, sb, A.aoStrength, shadowSamples, time);
         ShadePoint sp;
         sp.uv = is.uv;
         sp.textures = S.textures;
@@ -1025,7 +1033,7 @@ __device__ __forceinline__ bool shadeSlot(const SceneGPU& S, const Paths& P, con
                 if (INLINE_SHADOW) {
                     // the any-hit query now; its term follows this vertex's emission in L
                     ++shRays;
-                    const V3 vis = shadowVisibility<COUNT>(S, so, sd, stMax, fromEnv ? -1 : lightIndex, shNodes, shTris);
+                    const V3 vis = shadowVisibility<COUNT>(S, so, sd, stMax, fromEnv ? -1 : lightIndex, shNodes, shTris, time);
                     if (!isBlack(vis)) {
                         const V3 c = neeTerm(fLi, vis, scalar, thr, diffuseBounces >= 1, A.clampIndirect);
                         if (isFinite3(c)) {
@@ -1309,7 +1317,7 @@ __global__ void __launch_bounds__(kTailBlock) kTail(SceneGPU S, Paths P, Wave W,
             const float4 ro = P.rayO[slot];
             const float4 rd = P.rayD[slot];
             const Hit h = traceClosestWide<COUNT>(S, mk(ro.x, ro.y, ro.z), mk(rd.x, rd.y, rd.z), __float_as_uint(ro.w), 0.0f,
-                                              1e30f, nodes, tris);
+                                              1e30f, nodes, tris, nullptr, pathTime(S, P, slot));
             ++rays;
             P.hit[slot] = make_float4(h.t, h.u, h.v, __int_as_float(h.prim));
             if (!shadeSlot<true, COUNT, OUT, LEAN ? -2 : -1>(S, P, A, slot, path, shNodes, shTris, shRays)) break;

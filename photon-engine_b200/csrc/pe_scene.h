@@ -17,6 +17,7 @@
 #pragma once
 
 #include "pe_math.h"
+#include "pe_xform.h"
 
 #if !defined(__CUDACC__)
 struct float4 { float x, y, z, w; };
@@ -62,7 +63,16 @@ struct InstGPU {
     int32_t rootBinary, rootWide, recBase, firstTri;
     int32_t shape, material;
     float uvScale;   // 1 / cbrt(|det|) of the 3×3 part (uvDensity, mesh_instance.cpp:95-98)
-    int32_t pad;
+    int32_t motion;  // index into SceneGPU::motions of a moving instance, -1 none
+};
+
+// A moving MeshInstance (MeshInstance::setMotionTransform): the pose at shutter close as given and
+// the time-independent half of interpolateTransform for the poses between.
+struct InstMotionGPU {
+    float4 l2w1[4], w2l1[4];
+    MotionTRS trs;
+    float uvScale1;
+    int32_t pad[3];
 };
 
 struct ShapeInfo {
@@ -256,6 +266,7 @@ struct SceneGPU {
     int32_t materialTypes;   // bit t: some material has type t
     const InstGPU* instances; // MeshInstances (null without)
     int32_t nInstances;
+    const InstMotionGPU* motions; // moving instances (null without)
 };
 
 // Scene::isLightLinked / isShadowLinked for light `li` (explicit) and a receiver or blocker node.

@@ -315,7 +315,7 @@ int planPaths(pe_server* S, int li, int budget) {
             seg.sq = r.sq;
             seg.slotFirst = R.loop.nextPath + planned;
             seg.pixFirst = 0;
-            seg.flags = urgent(r) ? SEG_SWEEP : 0;
+            seg.flags = (seg.flags & SEG_MOTION) | (urgent(r) ? SEG_SWEEP : 0);
             SegInfo info{id, 0, 0, false};
             if (r.pixelCursor == 0 && npix <= room) {
                 const int64_t rows = std::min<int64_t>(r.spp - r.sampleCursor, room / npix);

@@ -60,15 +60,52 @@ __device__ __forceinline__ float filterSample1D(const float* cdf, float filterWi
     const float radius = 0.5f * filterWidth;
     return -radius + (static_cast<float>(i) + sclamp(t, 0.0f, 1.0f)) * (filterWidth / kFilterBins);
 }
-// Primary ray of pixel (x, y): consumes Sobol dimensions 0 (filter) and 1 (lens).
+// Camera::generateRay(u, v, lens, time) with a shutter-close pose and 0 < time (camera.h:58-90):
+// the two descriptions mixed linearly, a round lens of the mixed radius.
+static __device__ __noinline__ void cameraRayMoving(const CamDev& c, float sx, float sy, V2 lens, float t, V3& o, V3& d) {
+    const float b = 1.0f - t;
+    auto mix3 = [&](V3 p, V3 q) { return p * b + q * t; };
+    const V3 ll = mix3(c.lowerLeft, c.lowerLeft1), horiz = mix3(c.horizontal, c.horizontal1),
+             vert = mix3(c.vertical, c.vertical1);
+    if (c.orthographic) {
+        o = ll + horiz * sx + vert * sy;
+        d = normalize(mix3(c.forward, c.forward1));
+        return;
+    }
+    const V3 pos = mix3(c.position, c.position1);
+    const float radius = c.lensRadius * b + c.lensRadius1 * t;
+    o = pos;
+    if (radius > 0.0f) {
+        const V3 cu = normalize(mix3(c.u, c.u1)), cv = normalize(mix3(c.v, c.v1));
+        const V2 l = sampleDiskConcentric(lens);
+        const V2 lp = mk2(l.x * radius, l.y * radius);
+        o = pos + cu * lp.x + cv * lp.y;
+    }
+    const V3 target = ll + horiz * sx + vert * sy;
+    d = normalize(target - o);
+}
+
+// Primary ray of pixel (x, y): consumes Sobol dimensions 0 (filter) and 1 (lens), and with motion
+// blur 2 (the shutter time, renderer.cpp:152-153), returned in `time` (0 without).
 __device__ __forceinline__ void cameraRay(const TablesGPU* T, const float* filterCdf, const CamDev& c, float filterWidth,
-                                          int x, int y, int w, int h, Sobol& s, V3& o, V3& d) {
+                                          int x, int y, int w, int h, Sobol& s, V3& o, V3& d, bool motion = false,
+                                          float* time = nullptr) {
     const V2 u = get2D(T, s);
     const float ox = filterSample1D(filterCdf, filterWidth, u.x);
     const float oy = filterSample1D(filterCdf, filterWidth, u.y);
     const float sx = (static_cast<float>(x) + 0.5f + ox) / static_cast<float>(w);
     const float sy = 1.0f - (static_cast<float>(y) + 0.5f + oy) / static_cast<float>(h);
     const V2 lens = get2D(T, s); // lens sample (consumed by every camera)
+    if (motion) {
+        const float t = sclamp(get1D(s), 0.0f, 1.0f);
+        if (time) *time = t;
+        if (c.hasEnd && t > 0.0f) {
+            cameraRayMoving(c, sx, sy, lens, t, o, d);
+            return;
+        }
+    } else if (time) {
+        *time = 0.0f;
+    }
     const V3 target = c.lowerLeft + sx * c.horizontal + sy * c.vertical;
     if (c.orthographic) {
         // OrthographicCamera::generateRay (orthographic_camera.cpp:24-27)
@@ -182,9 +219,10 @@ __device__ __forceinline__ void leafRange(int ref, int& first, int& count) {
     count = static_cast<int>(v & 0xFFu) + 1;
 }
 
-// Transform::transformPoint / transformVector (transform.cpp:15-40) with a row-major 4×4.
+// Transform::transformPoint / transformVector (transform.cpp:15-40) with a row-major 4×4, in
+// global memory (an instance's own pose) or a thread's local array (a pose between).
 __device__ __forceinline__ V3 xfPointD(const float4* m, V3 p) {
-    const float4 r0 = __ldg(&m[0]), r1 = __ldg(&m[1]), r2 = __ldg(&m[2]), r3 = __ldg(&m[3]);
+    const float4 r0 = m[0], r1 = m[1], r2 = m[2], r3 = m[3];
     const float x = r0.x * p.x + r0.y * p.y + r0.z * p.z + r0.w;
     const float y = r1.x * p.x + r1.y * p.y + r1.z * p.z + r1.w;
     const float z = r2.x * p.x + r2.y * p.y + r2.z * p.z + r2.w;
@@ -196,7 +234,7 @@ __device__ __forceinline__ V3 xfPointD(const float4* m, V3 p) {
     return mk(x, y, z);
 }
 __device__ __forceinline__ V3 xfVectorD(const float4* m, V3 v) {
-    const float4 r0 = __ldg(&m[0]), r1 = __ldg(&m[1]), r2 = __ldg(&m[2]);
+    const float4 r0 = m[0], r1 = m[1], r2 = m[2];
     return mk(r0.x * v.x + r0.y * v.y + r0.z * v.z, r1.x * v.x + r1.y * v.y + r1.z * v.z,
               r2.x * v.x + r2.y * v.y + r2.z * v.z);
 }
@@ -212,25 +250,62 @@ __device__ __forceinline__ int localOfHit(int32_t prim) { return static_cast<int
 
 template <bool COUNT, int LEVEL>
 __device__ void walkClosest(const SceneGPU& S, int cur, V3 o, V3 d, V3 inv, uint32_t mask, float tMin, float& tMax,
-                            Hit& best, uint32_t& nodeVisits, uint32_t& triTests);
+                            Hit& best, uint32_t& nodeVisits, uint32_t& triTests, float time);
 template <bool COUNT, int SD, int LEVEL>
 __device__ void walkClosestWide(const SceneGPU& S, int cur, V3 o, V3 d, V3 inv, uint32_t mask, float tMin, float& tMax,
-                                Hit& best, uint32_t& nodeVisits, uint32_t& triTests, uint2* sstack);
+                                Hit& best, uint32_t& nodeVisits, uint32_t& triTests, uint2* sstack, float time);
 template <bool COUNT, int LEVEL>
 __device__ bool walkAny(const SceneGPU& S, int cur, V3 o, V3 d, V3 inv, uint32_t mask, float tMin, float tMax,
-                        uint32_t& nodeVisits, uint32_t& triTests);
+                        uint32_t& nodeVisits, uint32_t& triTests, float time);
 template <bool COUNT, int LEVEL>
 __device__ bool walkAnyWide(const SceneGPU& S, int cur, V3 o, V3 d, V3 inv, uint32_t mask, float tMin, float tMax,
-                            uint32_t& nodeVisits, uint32_t& triTests);
+                            uint32_t& nodeVisits, uint32_t& triTests, float time);
+
+// MeshInstance::transformAt (mesh_instance.cpp:31-34): the instance's matrices at shutter time
+// `time` — its own (no motion, or time ≤ 0), the shutter-close pose (time ≥ 1), or
+// interpolateTransform's pose between, written to `buf` (local-to-world rows, then the inverse).
+static __device__ __noinline__ void instancePoseBetween(const MotionTRS& M, float a, float4* buf, float& uvScale) {
+    float m[16], inv[16];
+    motionPoseAt(M, a, m, inv);
+    for (int r = 0; r < 4; ++r) {
+        buf[r] = make_float4(m[4 * r], m[4 * r + 1], m[4 * r + 2], m[4 * r + 3]);
+        buf[4 + r] = make_float4(inv[4 * r], inv[4 * r + 1], inv[4 * r + 2], inv[4 * r + 3]);
+    }
+    uvScale = uvScaleOf(m);
+}
+__device__ __forceinline__ void instancePose(const SceneGPU& S, const InstGPU& I, float time, float4* buf,
+                                             const float4*& l2w, const float4*& w2l, float& uvScale) {
+    l2w = I.l2w;
+    w2l = I.w2l;
+    uvScale = I.uvScale;
+    if (I.motion < 0) return;
+    const float a = sclamp(time, 0.0f, 1.0f);
+    if (a <= 0.0f) return;
+    const InstMotionGPU& M = S.motions[I.motion];
+    if (a >= 1.0f) {
+        l2w = M.l2w1;
+        w2l = M.w2l1;
+        uvScale = M.uvScale1;
+        return;
+    }
+    instancePoseBetween(M.trs, a, buf, uvScale);
+    l2w = buf;
+    w2l = buf + 4;
+}
 
 // MeshInstance::intersect (mesh_instance.cpp:104-115): the ray carried into the instance's space
-// by its world-to-local matrix (direction not renormalised, so t is shared), its BLAS walked
-// with every visibility bit; a hit shortens the world ray as it shortens the local one.
+// by its world-to-local matrix at the ray's time (direction not renormalised, so t is shared), its
+// BLAS walked with every visibility bit; a hit shortens the world ray as it shortens the local one.
 template <bool COUNT, bool WIDE>
 __device__ __noinline__ void instanceClosest(const SceneGPU& S, int inst, uint32_t meta, V3 o, V3 d, float tMin,
-                                             float& tMax, Hit& best, uint32_t& nodeVisits, uint32_t& triTests) {
+                                             float& tMax, Hit& best, uint32_t& nodeVisits, uint32_t& triTests,
+                                             float time) {
     const InstGPU& I = S.instances[inst];
-    const V3 lo = xfPointD(I.w2l, o), ld = xfVectorD(I.w2l, d);
+    float4 buf[8];
+    const float4 *l2w, *w2l;
+    float uvScale;
+    instancePose(S, I, time, buf, l2w, w2l, uvScale);
+    const V3 lo = xfPointD(w2l, o), ld = xfVectorD(w2l, d);
     const V3 linv = mk(1.0f / ld.x, 1.0f / ld.y, 1.0f / ld.z);
     Hit h;
     h.prim = -1;
@@ -239,9 +314,9 @@ __device__ __noinline__ void instanceClosest(const SceneGPU& S, int inst, uint32
     h.u = h.v = 0.0f;
     float tm = tMax;
     if (WIDE)
-        walkClosestWide<COUNT, 0, 1>(S, I.rootWide, lo, ld, linv, 0x1Fu, tMin, tm, h, nodeVisits, triTests, nullptr);
+        walkClosestWide<COUNT, 0, 1>(S, I.rootWide, lo, ld, linv, 0x1Fu, tMin, tm, h, nodeVisits, triTests, nullptr, 0.0f);
     else
-        walkClosest<COUNT, 1>(S, I.rootBinary, lo, ld, linv, 0x1Fu, tMin, tm, h, nodeVisits, triTests);
+        walkClosest<COUNT, 1>(S, I.rootBinary, lo, ld, linv, 0x1Fu, tMin, tm, h, nodeVisits, triTests, 0.0f);
     if (h.prim < 0) return;
     tMax = tm;
     best.t = h.t;
@@ -253,12 +328,16 @@ __device__ __noinline__ void instanceClosest(const SceneGPU& S, int inst, uint32
 
 template <bool COUNT, bool WIDE>
 __device__ __noinline__ bool instanceAny(const SceneGPU& S, int inst, V3 o, V3 d, float tMin, float tMax,
-                                         uint32_t& nodeVisits, uint32_t& triTests) {
+                                         uint32_t& nodeVisits, uint32_t& triTests, float time) {
     const InstGPU& I = S.instances[inst];
-    const V3 lo = xfPointD(I.w2l, o), ld = xfVectorD(I.w2l, d);
+    float4 buf[8];
+    const float4 *l2w, *w2l;
+    float uvScale;
+    instancePose(S, I, time, buf, l2w, w2l, uvScale);
+    const V3 lo = xfPointD(w2l, o), ld = xfVectorD(w2l, d);
     const V3 linv = mk(1.0f / ld.x, 1.0f / ld.y, 1.0f / ld.z);
-    return WIDE ? walkAnyWide<COUNT, 1>(S, I.rootWide, lo, ld, linv, 0x1Fu, tMin, tMax, nodeVisits, triTests)
-                : walkAny<COUNT, 1>(S, I.rootBinary, lo, ld, linv, 0x1Fu, tMin, tMax, nodeVisits, triTests);
+    return WIDE ? walkAnyWide<COUNT, 1>(S, I.rootWide, lo, ld, linv, 0x1Fu, tMin, tMax, nodeVisits, triTests, 0.0f)
+                : walkAny<COUNT, 1>(S, I.rootBinary, lo, ld, linv, 0x1Fu, tMin, tMax, nodeVisits, triTests, 0.0f);
 }
 
 // The primitives of one leaf, in order: triangles (lean Möller–Trumbore), spheres and, at the top
@@ -266,7 +345,7 @@ __device__ __noinline__ bool instanceAny(const SceneGPU& S, int inst, V3 o, V3 d
 template <bool COUNT, int LEVEL, bool WIDE>
 __device__ __forceinline__ void testLeafClosest(const SceneGPU& S, int first, int count, V3 o, V3 d, uint32_t mask,
                                                 float tMin, float& tMax, Hit& best, uint32_t& nodeVisits,
-                                                uint32_t& triTests) {
+                                                uint32_t& triTests, float time) {
     for (int k = 0; k < count; ++k) {
         const int pi = first + k;
         const float4 a = __ldg(&S.tris[3 * pi + 0]);
@@ -274,7 +353,7 @@ __device__ __forceinline__ void testLeafClosest(const SceneGPU& S, int first, in
         const uint32_t meta = __float_as_uint(b.w);
         if ((meta & mask) == 0u) continue;
         if (LEVEL == 0 && (meta & PRIM_INSTANCE)) {
-            instanceClosest<COUNT, WIDE>(S, __float_as_int(a.x), meta, o, d, tMin, tMax, best, nodeVisits, triTests);
+            instanceClosest<COUNT, WIDE>(S, __float_as_int(a.x), meta, o, d, tMin, tMax, best, nodeVisits, triTests, time);
             continue;
         }
         if (COUNT) ++triTests;
@@ -295,7 +374,8 @@ __device__ __forceinline__ void testLeafClosest(const SceneGPU& S, int first, in
 
 template <bool COUNT, int LEVEL, bool WIDE>
 __device__ __forceinline__ bool testLeafAny(const SceneGPU& S, int first, int count, V3 o, V3 d, uint32_t mask,
-                                            float tMin, float tMax, uint32_t& nodeVisits, uint32_t& triTests) {
+                                            float tMin, float tMax, uint32_t& nodeVisits, uint32_t& triTests,
+                                            float time) {
     for (int k = 0; k < count; ++k) {
         const int pi = first + k;
         const float4 a = __ldg(&S.tris[3 * pi + 0]);
@@ -303,7 +383,7 @@ __device__ __forceinline__ bool testLeafAny(const SceneGPU& S, int first, int co
         const uint32_t meta = __float_as_uint(b.w);
         if ((meta & mask) == 0u) continue;
         if (LEVEL == 0 && (meta & PRIM_INSTANCE)) {
-            if (instanceAny<COUNT, WIDE>(S, __float_as_int(a.x), o, d, tMin, tMax, nodeVisits, triTests)) return true;
+            if (instanceAny<COUNT, WIDE>(S, __float_as_int(a.x), o, d, tMin, tMax, nodeVisits, triTests, time)) return true;
             continue;
         }
         if (COUNT) ++triTests;
@@ -327,7 +407,7 @@ __device__ __forceinline__ int rootRef(const SceneGPU& S) {
 // its entry distance and skipped on pop when farther than the current hit.
 template <bool COUNT, int LEVEL>
 __device__ void walkClosest(const SceneGPU& S, int cur, V3 o, V3 d, V3 inv, uint32_t mask, float tMin, float& tMax,
-                            Hit& best, uint32_t& nodeVisits, uint32_t& triTests) {
+                            Hit& best, uint32_t& nodeVisits, uint32_t& triTests, float time) {
     int stackRef[kMaxStack];
     float stackT[kMaxStack];
     int sp = 0;
@@ -371,7 +451,7 @@ __device__ void walkClosest(const SceneGPU& S, int cur, V3 o, V3 d, V3 inv, uint
         }
         int first, count;
         leafRange(cur, first, count);
-        testLeafClosest<COUNT, LEVEL, false>(S, first, count, o, d, mask, tMin, tMax, best, nodeVisits, triTests);
+        testLeafClosest<COUNT, LEVEL, false>(S, first, count, o, d, mask, tMin, tMax, best, nodeVisits, triTests, time);
         bool found = false;
         while (sp > 0) {
             --sp;
@@ -389,7 +469,7 @@ __device__ void walkClosest(const SceneGPU& S, int cur, V3 o, V3 d, V3 inv, uint
 // t <= tMax wins ties, as in BVH::intersect.
 template <bool COUNT>
 __device__ Hit traceClosest(const SceneGPU& S, V3 o, V3 d, uint32_t mask, float tMin, float tMax, uint32_t& nodeVisits,
-                            uint32_t& triTests) {
+                            uint32_t& triTests, float time = 0.0f) {
     Hit best;
     best.prim = -1;
     best.meta = 0;
@@ -400,14 +480,14 @@ __device__ Hit traceClosest(const SceneGPU& S, V3 o, V3 d, uint32_t mask, float 
     if (S.nTris == 0) return best;
     if (!slab(S.rootMin[0], S.rootMax[0], S.rootMin[1], S.rootMax[1], S.rootMin[2], S.rootMax[2], o, inv, tMin, tMax, tn))
         return best;
-    walkClosest<COUNT, 0>(S, rootRef(S), o, d, inv, mask, tMin, tMax, best, nodeVisits, triTests);
+    walkClosest<COUNT, 0>(S, rootRef(S), o, d, inv, mask, tMin, tMax, best, nodeVisits, triTests, time);
     return best;
 }
 
 // BVH::intersectAny (bvh.cpp:404-446) from reference `cur`.
 template <bool COUNT, int LEVEL>
 __device__ bool walkAny(const SceneGPU& S, int cur, V3 o, V3 d, V3 inv, uint32_t mask, float tMin, float tMax,
-                        uint32_t& nodeVisits, uint32_t& triTests) {
+                        uint32_t& nodeVisits, uint32_t& triTests, float time) {
     int stackRef[kMaxStack];
     int sp = 0;
     for (;;) {
@@ -436,7 +516,7 @@ __device__ bool walkAny(const SceneGPU& S, int cur, V3 o, V3 d, V3 inv, uint32_t
         }
         int first, count;
         leafRange(cur, first, count);
-        if (testLeafAny<COUNT, LEVEL, false>(S, first, count, o, d, mask, tMin, tMax, nodeVisits, triTests)) return true;
+        if (testLeafAny<COUNT, LEVEL, false>(S, first, count, o, d, mask, tMin, tMax, nodeVisits, triTests, time)) return true;
         if (sp == 0) return false;
         cur = stackRef[--sp];
     }
@@ -446,13 +526,13 @@ __device__ bool walkAny(const SceneGPU& S, int cur, V3 o, V3 d, V3 inv, uint32_t
 // The answer does not depend on visiting order; near child first for early exit.
 template <bool COUNT>
 __device__ bool traceAny(const SceneGPU& S, V3 o, V3 d, uint32_t mask, float tMin, float tMax, uint32_t& nodeVisits,
-                         uint32_t& triTests) {
+                         uint32_t& triTests, float time = 0.0f) {
     const V3 inv = mk(1.0f / d.x, 1.0f / d.y, 1.0f / d.z);
     float tn;
     if (S.nTris == 0) return false;
     if (!slab(S.rootMin[0], S.rootMax[0], S.rootMin[1], S.rootMax[1], S.rootMin[2], S.rootMax[2], o, inv, tMin, tMax, tn))
         return false;
-    return walkAny<COUNT, 0>(S, rootRef(S), o, d, inv, mask, tMin, tMax, nodeVisits, triTests);
+    return walkAny<COUNT, 0>(S, rootRef(S), o, d, inv, mask, tMin, tMax, nodeVisits, triTests, time);
 }
 
 // ---- 4-wide traversal ----------------------------------------------------------------------
@@ -520,7 +600,7 @@ struct TraceStack {
 // this thread's column); 0 keeps all in local memory.
 template <bool COUNT, int SD, int LEVEL>
 __device__ void walkClosestWide(const SceneGPU& S, int cur, V3 o, V3 d, V3 inv, uint32_t mask, float tMin, float& tMax,
-                                Hit& best, uint32_t& nodeVisits, uint32_t& triTests, uint2* sstack) {
+                                Hit& best, uint32_t& nodeVisits, uint32_t& triTests, uint2* sstack, float time) {
     TraceStack<SD> stack;
     stack.shared = sstack;
     int sp = 0;
@@ -559,7 +639,7 @@ __device__ void walkClosestWide(const SceneGPU& S, int cur, V3 o, V3 d, V3 inv, 
         }
         int first, count;
         leafRange(cur, first, count);
-        testLeafClosest<COUNT, LEVEL, true>(S, first, count, o, d, mask, tMin, tMax, best, nodeVisits, triTests);
+        testLeafClosest<COUNT, LEVEL, true>(S, first, count, o, d, mask, tMin, tMax, best, nodeVisits, triTests, time);
         bool found = false;
         while (sp > 0) {
             const uint2 e = stack.get(--sp);
@@ -575,7 +655,7 @@ __device__ void walkClosestWide(const SceneGPU& S, int cur, V3 o, V3 d, V3 inv, 
 
 template <bool COUNT, int SD = 0>
 __device__ Hit traceClosestWide(const SceneGPU& S, V3 o, V3 d, uint32_t mask, float tMin, float tMax,
-                                uint32_t& nodeVisits, uint32_t& triTests, uint2* sstack = nullptr) {
+                                uint32_t& nodeVisits, uint32_t& triTests, uint2* sstack = nullptr, float time = 0.0f) {
     Hit best;
     best.prim = -1;
     best.meta = 0;
@@ -586,14 +666,14 @@ __device__ Hit traceClosestWide(const SceneGPU& S, V3 o, V3 d, uint32_t mask, fl
     if (S.nTris == 0) return best;
     if (!slab(S.rootMin[0], S.rootMax[0], S.rootMin[1], S.rootMax[1], S.rootMin[2], S.rootMax[2], o, inv, tMin, tMax, tn))
         return best;
-    walkClosestWide<COUNT, SD, 0>(S, rootRef(S), o, d, inv, mask, tMin, tMax, best, nodeVisits, triTests, sstack);
+    walkClosestWide<COUNT, SD, 0>(S, rootRef(S), o, d, inv, mask, tMin, tMax, best, nodeVisits, triTests, sstack, time);
     return best;
 }
 
 // Any hit over the 4-wide tree from reference `cur`: the answer does not depend on the order.
 template <bool COUNT, int LEVEL>
 __device__ bool walkAnyWide(const SceneGPU& S, int cur, V3 o, V3 d, V3 inv, uint32_t mask, float tMin, float tMax,
-                            uint32_t& nodeVisits, uint32_t& triTests) {
+                            uint32_t& nodeVisits, uint32_t& triTests, float time) {
     int stackRef[kWideStack];
     int sp = 0;
     for (;;) {
@@ -617,7 +697,7 @@ __device__ bool walkAnyWide(const SceneGPU& S, int cur, V3 o, V3 d, V3 inv, uint
         }
         int first, count;
         leafRange(cur, first, count);
-        if (testLeafAny<COUNT, LEVEL, true>(S, first, count, o, d, mask, tMin, tMax, nodeVisits, triTests)) return true;
+        if (testLeafAny<COUNT, LEVEL, true>(S, first, count, o, d, mask, tMin, tMax, nodeVisits, triTests, time)) return true;
         if (sp == 0) return false;
         cur = stackRef[--sp];
     }
@@ -625,13 +705,18 @@ __device__ bool walkAnyWide(const SceneGPU& S, int cur, V3 o, V3 d, V3 inv, uint
 
 template <bool COUNT>
 __device__ bool traceAnyWide(const SceneGPU& S, V3 o, V3 d, uint32_t mask, float tMin, float tMax, uint32_t& nodeVisits,
-                             uint32_t& triTests) {
+                             uint32_t& triTests, float time = 0.0f) {
     const V3 inv = mk(1.0f / d.x, 1.0f / d.y, 1.0f / d.z);
     float tn;
     if (S.nTris == 0) return false;
     if (!slab(S.rootMin[0], S.rootMax[0], S.rootMin[1], S.rootMax[1], S.rootMin[2], S.rootMax[2], o, inv, tMin, tMax, tn))
         return false;
-    return walkAnyWide<COUNT, 0>(S, rootRef(S), o, d, inv, mask, tMin, tMax, nodeVisits, triTests);
+    return walkAnyWide<COUNT, 0>(S, rootRef(S), o, d, inv, mask, tMin, tMax, nodeVisits, triTests, time);
+}
+
+// Shutter time of the path in `slot` (Ray::time): read only where the scene has moving instances.
+__device__ __forceinline__ float pathTime(const SceneGPU& S, const Paths& P, int slot) {
+    return (S.motions && P.time) ? P.time[slot] : 0.0f;
 }
 
 // ---- hit record (src/geometry/triangle.cpp:54-133) -----------------------------------------
@@ -699,12 +784,13 @@ static __device__ __forceinline__ int4 fillTriangleHit(const SceneGPU& S, const 
 // matrix, both normals by its inverse transpose and renormalised (the shading normal faced to
 // the world ray), the tangent carried and made orthogonal again, a world error bound from the
 // matrix's absolute rows plus a relative and an absolute slack, the texel density rescaled.
-static __device__ __noinline__ void instanceToWorld(const InstGPU& I, V3 rayDir, Isect& is) {
+static __device__ __noinline__ void instanceToWorld(const float4* l2w, const float4* w2l, float uvScale, V3 rayDir,
+                                                    Isect& is) {
     const V3 localOutNg = is.ng;
     const V3 localOutNs = is.frontFace ? is.normal : -is.normal;
-    is.point = xfPointD(I.l2w, is.point);
-    is.pSmooth = is.hasSmooth ? xfPointD(I.l2w, is.pSmooth) : is.point;
-    const float4 i0 = __ldg(&I.w2l[0]), i1 = __ldg(&I.w2l[1]), i2 = __ldg(&I.w2l[2]);
+    is.point = xfPointD(l2w, is.point);
+    is.pSmooth = is.hasSmooth ? xfPointD(l2w, is.pSmooth) : is.point;
+    const float4 i0 = w2l[0], i1 = w2l[1], i2 = w2l[2];
     auto xfNormal = [&](V3 n) {
         return mk(i0.x * n.x + i1.x * n.y + i2.x * n.z, i0.y * n.x + i1.y * n.y + i2.y * n.z,
                   i0.z * n.x + i1.z * n.y + i2.z * n.z);
@@ -718,7 +804,7 @@ static __device__ __noinline__ void instanceToWorld(const InstGPU& I, V3 rayDir,
     is.frontFace = dot(rayDir, nsW) < 0.0f;
     is.normal = is.frontFace ? nsW : -nsW;
     if (len2(is.ng) == 0.0f) is.ng = nsW;
-    V3 tW = xfVectorD(I.l2w, is.tangent);
+    V3 tW = xfVectorD(l2w, is.tangent);
     tW = tW - is.normal * dot(is.normal, tW);
     if (len2(tW) > 1e-12f) {
         is.tangent = normalize(tW);
@@ -729,23 +815,28 @@ static __device__ __noinline__ void instanceToWorld(const InstGPU& I, V3 rayDir,
         const float b = n.x * n.y * a;
         is.tangent = normalize(mk(1.0f + sign * n.x * n.x * a, sign * b, -sign * n.x));
     }
-    const float4 m0 = __ldg(&I.l2w[0]), m1 = __ldg(&I.l2w[1]), m2 = __ldg(&I.l2w[2]);
+    const float4 m0 = l2w[0], m1 = l2w[1], m2 = l2w[2];
     const V3 r0 = mk(fabsf(m0.x), fabsf(m0.y), fabsf(m0.z)), r1 = mk(fabsf(m1.x), fabsf(m1.y), fabsf(m1.z)),
              r2 = mk(fabsf(m2.x), fabsf(m2.y), fabsf(m2.z));
     const V3 pAbs = vabs(is.point);
     is.pError = mk(dot(r0, is.pError), dot(r1, is.pError), dot(r2, is.pError)) + pAbs * 1e-5f + mk(1e-6f);
-    if (is.uvDensity > 0.0f) is.uvDensity = is.uvDensity / I.uvScale;
+    if (is.uvDensity > 0.0f) is.uvDensity = is.uvDensity / uvScale;
 }
 
-static __device__ __noinline__ void fillHit(const SceneGPU& S, const Hit& h, V3 rayO, V3 rayDir, Isect& is) {
+static __device__ __noinline__ void fillHit(const SceneGPU& S, const Hit& h, V3 rayO, V3 rayDir, Isect& is,
+                                            float time = 0.0f) {
     if (isInstanceHit(h.prim)) {
         // MeshInstance::shadeInstanceHit (mesh_instance.cpp:125-133): the triangle's record in the
-        // instance's space, carried to world space
+        // instance's space at the ray's time, carried to world space
         const InstGPU& I = S.instances[instanceOfHit(h.prim)];
+        float4 buf[8];
+        const float4 *l2w, *w2l;
+        float uvScale;
+        instancePose(S, I, time, buf, l2w, w2l, uvScale);
         Hit hl = h;
         hl.prim = I.recBase + localOfHit(h.prim);
-        fillTriangleHit(S, hl, xfVectorD(I.w2l, rayDir), is);
-        instanceToWorld(I, rayDir, is);
+        fillTriangleHit(S, hl, xfVectorD(w2l, rayDir), is);
+        instanceToWorld(l2w, w2l, uvScale, rayDir, is);
         is.shape = I.shape;
         is.material = I.material;
         return;

@@ -19,6 +19,10 @@ struct CamDev {
     int blades;             // thin lens: polygon aperture sides (0 = disk)
     float bladeRotation;    // radians
     int orthographic;
+    // Camera::setShutterEnd: the description at shutter close (hasEnd = 0: none)
+    int hasEnd;
+    V3 position1, lowerLeft1, horizontal1, vertical1, u1, v1, forward1;
+    float lensRadius1;
 };
 
 enum VisMask : uint32_t { VIS_CAMERA = 1u, VIS_DIFFUSE = 2u, VIS_GLOSSY = 4u, VIS_TRANSMISSION = 8u, VIS_SHADOW = 16u,
@@ -57,6 +61,7 @@ struct Paths {
     float4* pickP;   // light-picker point xyz, pixel hash (bits)
     float4* pickN;   // light-picker normal xyz, counters (bits: depth | diffuseBounces<<8 | passThroughs<<16 | skips<<24)
     float4* hit;     // t, u, v, leaf prim (bits)
+    float* time;     // shutter time of the path's rays (read where the scene has moving instances)
     float4* med;     // media stack slots 0,1 | slots 2,3 (bits), mediumEvents | walkStep<<16, stack depth
     int32_t* queueA;
     int32_t* queueB;
@@ -164,7 +169,9 @@ struct WaveSeg {
     float aoStrength;       // RenderSettings::aoStrength (contact AO at camera hits)
     float coneWidth, coneSpread; // camera rays' cone (Camera::pixelConeWidth / pixelConeSpread)
 };
-enum SegFlags { SEG_SWEEP = 1 }; // paths of the segment may leave a continuous wave for a sweep
+// SEG_SWEEP: paths of the segment may leave a continuous wave for a sweep; SEG_MOTION:
+// RenderSettings::motionBlur (each camera sample draws a shutter time)
+enum SegFlags { SEG_SWEEP = 1, SEG_MOTION = 2 };
 
 // The segments of one wave, ordered by slotFirst (and so by pixFirst).
 struct Wave {

@@ -213,6 +213,11 @@ class Mirror(Material):
 
 # ---------------------------------------------------------------------------------------------
 # shapes and lights
+# VisibilityMask (src/core/math/ray.h:18-25): the ray classes a shape is seen by
+VIS_CAMERA, VIS_DIFFUSE, VIS_GLOSSY, VIS_TRANSMISSION, VIS_SHADOW = 1, 2, 4, 8, 16
+VIS_ALL = 0x1F
+
+
 class TriangleMesh:
     def __init__(self, positions, normals=None, uvs=None, indices=None, material: Material | None = None):
         self.positions = np.ascontiguousarray(positions, dtype=np.float32).reshape(-1, 3)
@@ -220,6 +225,11 @@ class TriangleMesh:
         self.uvs = None if uvs is None or len(uvs) == 0 else np.ascontiguousarray(uvs, dtype=np.float32).reshape(-1, 2)
         self.indices = np.ascontiguousarray(indices, dtype=np.uint32).reshape(-1, 3)
         self.material = material
+        self.visibility_mask = VIS_ALL
+
+    def set_visibility_mask(self, mask: int):
+        """Shape::setVisibilityMask: VIS_CAMERA | VIS_DIFFUSE | VIS_GLOSSY | VIS_TRANSMISSION | VIS_SHADOW."""
+        self.visibility_mask = int(mask) & VIS_ALL
 
     def num_triangles(self) -> int:
         return int(self.indices.shape[0])
@@ -232,6 +242,9 @@ class Sphere:
         self.center = tuple(map(float, center))
         self.radius = float(radius)
         self.material = material
+        self.visibility_mask = VIS_ALL
+
+    set_visibility_mask = TriangleMesh.set_visibility_mask
 
     def num_triangles(self) -> int:
         return 0
@@ -251,6 +264,21 @@ class MeshInstance:
         self.world_to_local = None if world_to_local is None else \
             np.ascontiguousarray(world_to_local, dtype=np.float32).reshape(4, 4)
         self.material = material if material is not None else mesh.material
+        self.visibility_mask = VIS_ALL
+        self.local_to_world_end = None
+        self.world_to_local_end = None
+
+    def set_motion_transform(self, local_to_world_end, world_to_local_end=None):
+        """MeshInstance::setMotionTransform: the pose at shutter close (t = 1).  Rays at time t meet
+        the instance under interpolateTransform (translation and scale linear, rotation SLERP)."""
+        self.local_to_world_end = np.ascontiguousarray(local_to_world_end, dtype=np.float32).reshape(4, 4)
+        self.world_to_local_end = None if world_to_local_end is None else \
+            np.ascontiguousarray(world_to_local_end, dtype=np.float32).reshape(4, 4)
+
+    def has_motion(self) -> bool:
+        return self.local_to_world_end is not None
+
+    set_visibility_mask = TriangleMesh.set_visibility_mask
 
     def num_triangles(self) -> int:
         return 0
@@ -488,6 +516,7 @@ class Scene:
                 capi.check(capi.PE_ERR_INVALID)
             mat_index[id(m)] = idx
         self._mat_index = mat_index
+        shape_count = 0
         for kind, obj in self.ops:
             if kind == "mesh":
                 capi.check(lib.pe_scene_add_mesh(h, capi.fptr(obj.positions), obj.positions.shape[0],
@@ -507,15 +536,24 @@ class Scene:
                     blas_index[id(mesh)] = b
                 capi.check(lib.pe_scene_add_instance(h, b, capi.fptr(obj.local_to_world), capi.fptr(obj.world_to_local),
                                                      mat_index[id(obj.material)]))
+                if obj.has_motion():
+                    capi.check(lib.pe_scene_set_instance_motion(h, shape_count, capi.fptr(obj.local_to_world_end),
+                                                                capi.fptr(obj.world_to_local_end)))
             else:
                 capi.check(lib.pe_scene_add_area_light(h, capi.f3(obj.position), capi.f3(obj.u), capi.f3(obj.v),
                                                        capi.f3(obj.radiance), 1 if obj.visible_to_camera else 0))
+            shape_count += 2 if kind == "area" else 1
         if self.shadow_catcher is not None:
             capi.check(lib.pe_scene_set_shadow_catcher(h, int(self.shadow_catcher)))
         for shape, uid in self.shape_tags.items():
             capi.check(lib.pe_scene_tag_shape(h, shape, uid))
         for shape, name in self.shape_names.items():
             capi.check(lib.pe_scene_set_shape_name(h, shape, name.encode()))
+        shape = 0
+        for kind, obj in self.ops:
+            if kind != "area" and obj.visibility_mask != VIS_ALL:
+                capi.check(lib.pe_scene_set_shape_visibility(h, shape, obj.visibility_mask))
+            shape += 2 if kind == "area" else 1
         for mat, name in self.material_names.values():
             if id(mat) in mat_index:
                 capi.check(lib.pe_scene_set_material_name(h, mat_index[id(mat)], name.encode()))
@@ -576,6 +614,20 @@ class PerspectiveCamera:
 
     def describe_gpu(self) -> capi.pe_camera:
         return self._desc
+
+    def set_shutter_end(self, end: "PerspectiveCamera"):
+        """Camera::setShutterEnd: `end`'s pose at shutter close (t = 1).  With motion blur a ray at
+        time t > 0 mixes the two descriptions linearly (a round lens of the mixed radius)."""
+        e = end.describe_gpu()
+        d = self._desc
+        d.has_shutter_end = 1
+        for f in ("position", "lower_left", "horizontal", "vertical", "u", "v", "forward"):
+            setattr(d, "end_" + f, capi.f3(tuple(getattr(e, f))))
+        d.end_lens_radius = e.lens_radius
+        self.shutter_end = end
+
+    def has_shutter_end(self) -> bool:
+        return bool(self._desc.has_shutter_end)
 
     def reference_params(self):
         """(kind, parameters) of the same camera in the reference's own classes (test oracle)."""
@@ -641,12 +693,14 @@ class RenderSettings:
     ao_strength: float = 0.0     # RenderSettings::aoStrength: contact AO at camera hits
     noise_threshold: float = 0.02    # adaptive: relative standard error target (render_settings.h:31)
     min_adaptive_samples: int = 16   # adaptive: samples before any decision (render_settings.h:32)
+    motion_blur: bool = False        # RenderSettings::motionBlur: a shutter time per camera sample
 
     def to_c(self) -> capi.pe_settings:
         return capi.pe_settings(self.width, self.height, self.max_bounces, self.rr_depth, self.shadow_quality,
                                 int(self.filter_type), self.filter_width, self.clamp_indirect, self.seed,
                                 float(self.ao_strength), 1 if self.adaptive_sampling else 0,
-                                float(self.noise_threshold), int(self.min_adaptive_samples))
+                                float(self.noise_threshold), int(self.min_adaptive_samples),
+                                1 if self.motion_blur else 0)
 
 
 class Film:

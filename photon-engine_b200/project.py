@@ -13,9 +13,10 @@ and builds the render scene, camera and settings the reference builds from it, f
   subsurface, edge tint, thin film, flakes; for glass thin walls, absorption, scattering, Abbe);
 * nodes (project_io.cpp:268-412, scene_graph.cpp:166-225): groups, "mesh" nodes with inline
   geometry (p, n, uv, i), "sphere" nodes; row-major 4×4 "xf" transforms composed parent × local;
-  invisible nodes and their subtrees skipped; meshes carried to world space here (the reference
-  keeps them as MeshInstance BLAS + transform — same surfaces, the last bits of positions and
-  error bounds differ), spheres as Sphere(world centre, radius × largest axis scale);
+  invisible nodes and their subtrees skipped; each mesh node a MeshInstance of its local mesh
+  under the composed Transform (matrix parent·local, inverse local⁻¹·parent⁻¹, each node's inverse
+  Mat4f::inverse of its "xf"), spheres as Sphere(world centre, radius × largest axis scale); the
+  node's "visibility" ray mask on both;
 * the automatic ground quad under the scene (scene_graph.cpp:151-165, document.cpp:327-343);
 * area lights (document.cpp:67-117), temperature-free colour × intensity;
 * the environment (project_io.cpp:543-583, document.cpp:118-140, 216-231): a Radiance .hdr
@@ -71,11 +72,16 @@ def _mat_mul(a, b):
     return out
 
 
-def _xf(j):
+def _transform(j):
+    """readTransform (project_io.cpp:94-101): Transform(m) of the node's "xf" (its inverse by
+    Mat4f::inverse), or the identity Transform without one."""
     x = j.get("xf")
     if not isinstance(x, list) or len(x) != 16:
-        return np.eye(4, dtype=F)
-    return np.array(x, F).reshape(4, 4)
+        return np.eye(4, dtype=F), np.eye(4, dtype=F)
+    m = np.array(x, F).reshape(4, 4)
+    inv = np.empty((4, 4), F)
+    E._lib().pe_mat4_inverse(E.capi.fptr(np.ascontiguousarray(m)), E.capi.fptr(inv))
+    return m, inv
 
 
 def _points(m, p):
@@ -279,14 +285,17 @@ class _Graph:
         self.lo = np.minimum(self.lo, p.min(0)).astype(F)
         self.hi = np.maximum(self.hi, p.max(0)).astype(F)
 
-    def compile(self, scene, j, parent, inherited=None):
+    def compile(self, scene, j, parent, parent_inv):
         if j.get("source") is not None:
             raise ProjectError("imported model sources (\"source\" nodes) are not read")
         if "transformKeys" in j:
             raise ProjectError("animated node transforms are not carried")
         if not j.get("visible", True):
             return
-        world = _mat_mul(parent, _xf(j))
+        local, local_inv = _transform(j)
+        world = _mat_mul(parent, local)              # Transform::operator* (transform.cpp:117-122)
+        world_inv = _mat_mul(local_inv, parent_inv)
+        vis = int(j.get("visibility", E.VIS_ALL)) & E.VIS_ALL
         mi = j.get("material", -1)
         mat = self.materials[mi] if isinstance(mi, int) and 0 <= mi < len(self.materials) else None
         kind = j.get("type", "group")
@@ -301,17 +310,13 @@ class _Graph:
             idx = np.array(g.get("i", []), np.int64)
             if p.size == 0 or idx.size % 3 != 0 or (idx.size and idx.max() >= p.shape[0]):
                 return  # meshFromJson rejects the node
-            pw = _points(world, p)
-            self._merge(pw)
+            self._merge(_points(world, p))
             if mat is not None:
-                nw = None
-                if n.shape[0] == p.shape[0]:
-                    inv_t = np.linalg.inv(world.astype(np.float64))[:3, :3].T
-                    nw = (n.astype(np.float64) @ inv_t.T)
-                    ln = np.linalg.norm(nw, axis=1, keepdims=True)
-                    nw = np.where(ln > 0, nw / np.where(ln > 0, ln, 1.0), 0.0).astype(F)
-                scene.add_shape(E.TriangleMesh(pw, nw, uv if uv.shape[0] == p.shape[0] else None,
-                                               idx.astype(np.uint32).reshape(-1, 3), mat))
+                mesh = E.TriangleMesh(p, n if n.shape[0] == p.shape[0] else None,
+                                      uv if uv.shape[0] == p.shape[0] else None, idx.astype(np.uint32).reshape(-1, 3), mat)
+                inst = E.MeshInstance(mesh, world, mat, world_inv)
+                inst.set_visibility_mask(vis)
+                scene.add_shape(inst)
                 self._name(scene, name, mat)
         elif kind == "sphere":
             r = float(j.get("radius", 1.0))
@@ -321,10 +326,12 @@ class _Graph:
             if mat is not None and r > 0:
                 axes = _vectors(world, np.eye(3, dtype=F))
                 s = max(float(np.sqrt(np.float32(np.dot(a, a)))) for a in axes)
-                scene.add_shape(E.Sphere(tuple(float(x) for x in c), float(F(r) * F(s)), mat))
+                sphere = E.Sphere(tuple(float(x) for x in c), float(F(r) * F(s)), mat)
+                sphere.set_visibility_mask(vis)
+                scene.add_shape(sphere)
                 self._name(scene, name, mat)
         for child in j.get("children", []):
-            self.compile(scene, child, world)
+            self.compile(scene, child, world, world_inv)
 
     def _name(self, scene, name, mat):
         shape = scene.shape_count() - 1
@@ -345,7 +352,7 @@ def load_project(path, width: int = 512, height: int = 512, spp: int = 64):
     scene = E.Scene()
     graph = _Graph(root.get("nodes", []), materials)
     for n in graph.nodes:
-        graph.compile(scene, n, np.eye(4, dtype=F))
+        graph.compile(scene, n, np.eye(4, dtype=F), np.eye(4, dtype=F))
     env = root.get("environment", {})
     if env.get("kind", "image") == "sky":
         raise ProjectError("the physical sky environment is not carried")

@@ -20,9 +20,9 @@ scenes stand in for them with the stated sizes and value distributions.
                        1×1 m window in the sun-facing wall, lit by the knot scene's sky; three
                        Disney torus knots, a sphere and tables on the floor (~0.5M triangles);
                        1920×1080 at full size.  The learned proposal's workload.
-* ``instanced_grid_scene`` a 5×4 grid of 20 seeded copies of a 262k-triangle torus knot
-                       (5.2M triangles, the copies flattened into one BVH: this engine has no
-                       instance level), eight Disney materials, the sky of the knot scene.
+* ``instanced_grid_scene`` a 5×4 grid of 20 seeded MeshInstances of one 262k-triangle torus
+                       knot (5.2M triangles seen, one BLAS of 262k stored), eight Disney
+                       materials, the sky of the knot scene.
 """
 from __future__ import annotations
 
@@ -32,7 +32,7 @@ import numpy as np
 
 from . import _capi as capi
 from . import scenegen
-from .engine import (AreaLight, Dielectric, DisneyMaterial, EnvironmentLight, Lambertian, Material, Mirror,
+from .engine import (AreaLight, Dielectric, DisneyMaterial, EnvironmentLight, Lambertian, Material, MeshInstance, Mirror,
                      PerspectiveCamera, PixelFilterType, RenderSettings, Scene, TriangleMesh)
 
 
@@ -320,7 +320,8 @@ def media_scene(width: int = 1280, height: int = 720, spp: int = 512, max_depth:
 
 def instanced_grid_scene(width: int = 1920, height: int = 1080, spp: int = 64, max_depth: int = 12, seed: int = 21,
                          nx: int = 5, nz: int = 4, nu: int = 1024, nv: int = 128, env_size=(2048, 1024)):
-    """~5M triangles: nx·nz rotated, scaled copies of one knot mesh on a ground plane."""
+    """~5M triangles seen: nx·nz rotated, scaled MeshInstances of one knot mesh (one BLAS on the
+    device) on a ground plane, each with its own material."""
     rng = np.random.default_rng(seed)
     mats = []
     for _ in range(8):
@@ -332,15 +333,16 @@ def instanced_grid_scene(width: int = 1920, height: int = 1080, spp: int = 64, m
     q = quads.reshape(-1, 4)
     tri = np.concatenate([q[:, [0, 1, 2]], q[:, [0, 2, 3]]], axis=0).astype(np.uint32)
     scene = Scene()
+    knot = TriangleMesh(pos.astype(np.float32), None, None, tri, mats[0])
     for i in range(nx):
         for k in range(nz):
             a = rng.uniform(0.0, 2.0 * math.pi)
             sc = rng.uniform(0.6, 0.9)
             c, s_ = math.cos(a), math.sin(a)
-            rot = np.array([[c, 0.0, s_], [0.0, 1.0, 0.0], [-s_, 0.0, c]])
-            offset = np.array([(i - (nx - 1) / 2) * 5.0, 0.0, (k - (nz - 1) / 2) * 5.0 + 4.0])
-            p = (pos @ rot.T) * sc + offset
-            scene.add_shape(TriangleMesh(p.astype(np.float32), None, None, tri, mats[int(rng.integers(0, 8))]))
+            m = np.eye(4)
+            m[:3, :3] = np.array([[c, 0.0, s_], [0.0, 1.0, 0.0], [-s_, 0.0, c]]) * sc
+            m[:3, 3] = ((i - (nx - 1) / 2) * 5.0, 0.0, (k - (nz - 1) / 2) * 5.0 + 4.0)
+            scene.add_shape(MeshInstance(knot, m.astype(np.float32), mats[int(rng.integers(0, 8))]))
     g = 80.0
     gp = np.array([(-g, 0.0, -g), (-g, 0.0, g), (g, 0.0, g), (g, 0.0, -g)], np.float32)
     scene.add_shape(TriangleMesh(gp, None, None, np.array([[0, 1, 2], [0, 2, 3]], np.uint32), Lambertian((0.5, 0.5, 0.5))))

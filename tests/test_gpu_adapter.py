@@ -83,6 +83,7 @@ def test_adapter_carries_instances_and_their_transforms(pe, device, adapter_orac
     the instances placed anew in the reference scene: the adapter refits, the mirror refits."""
     H = importlib.import_module("test_instances")
     scene, cam, st = H.instanced_cornell(pe, 48, 48, 8, 6)
+    st.seed = 12345  # Renderer::renderSamples' Sobol seed, which the session uses
     film, _ = _mirror(pe, device, scene, cam, st, 8)
     ref = adapter_oracle.RefScene(scene, fast="adapter")
     mean, cnt, _, done, _ = ref.session_cuda(cam, st, 8, batch=3)

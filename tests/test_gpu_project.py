@@ -5,8 +5,9 @@ sky, a Gaussian pixel filter) loaded by photon-engine_b200/project.py.
 
 * against the reference's CPU path on the same loaded scene and samples: relMSE ≤ 1e-4 with
   ≥ 99 % of pixels equal to 1e-4 relative, as the other equal-spp parity renders;
-* end to end against the reference's own loadProject + buildRenderScene of the same file at
-  256 spp: relMSE ≤ 1e-3 (the reference keeps meshes as instances; see tests/test_project.py).
+* end to end against the reference's own loadProject + buildRenderScene of the same file (the
+  loader builds the reference's scene bit for bit: mesh nodes as MeshInstances, tests/test_project.py),
+  the same bar at 16 spp.
 """
 import importlib
 import pathlib
@@ -36,12 +37,15 @@ def test_project_renders_as_the_reference(pe, device, oracle):
 
 def test_project_end_to_end_against_the_reference_loader(pe, device, oracle):
     proj = importlib.import_module("photon_engine_b200.project")
-    scene, cam, st = proj.load_project(PROJECT, 48, 36, 256)
+    scene, cam, st = proj.load_project(PROJECT, 96, 72, 16)
     scene.build_accelerator()
     device.set_scene(scene)
     film = pe.Film(st.width, st.height)
-    device.render(cam, st, pe.RenderTargets(beauty=film), 0, 256)
-    ref, rcam, *_ = oracle.load_project(PROJECT, 48, 36)
-    mean_ref, cnt = oracle.RefScene.render(ref, rcam, st, 0, 256)
+    device.render(cam, st, pe.RenderTargets(beauty=film), 0, 16)
+    ref, rcam, *_ = oracle.load_project(PROJECT, 96, 72)
+    mean_ref, cnt = oracle.RefScene.render(ref, rcam, st, 0, 16)
     assert np.array_equal(film.count, cnt)
-    assert pe.rel_mse(film.resolve(), mean_ref) <= 1e-3
+    img = film.resolve()
+    err = pe.rel_mse(img, mean_ref)
+    same = float(np.mean(np.all(np.abs(img - mean_ref) <= 1e-4 * np.maximum(1.0, np.abs(mean_ref)), axis=-1)))
+    assert err <= 1e-4 and same >= 0.99, (err, same)

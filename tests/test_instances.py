@@ -125,3 +125,42 @@ def test_reference_moved_instance_traces_as_a_scene_built_moved(pe, oracle):
         assert np.array_equal(x, y)
     with pytest.raises(ValueError):
         ref.move_instance(0, moved)
+
+
+def moving_cornell(pe, w=48, h=48, spp=4, depth=6, seed=12345):
+    """The instanced Cornell box with its red cube moving (translation, a half turn and a scale
+    change over the shutter) and the mirror cube static."""
+    scene, cam, st = instanced_cornell(pe, w, h, spp, depth)
+    st.seed = seed
+    inst = [o for k, o in scene.ops if k == "instance"]
+    inst[0].set_motion_transform(rot_y(2.0, (2.2, 1.3, 2.0), 0.8))
+    return scene, cam, st
+
+
+def test_moving_instance_bounds_match_reference(pe, oracle):
+    """MeshInstance::recomputeBounds over the shutter: the union of five interpolated poses
+    (interpolateTransform: decomposeTRS, SLERP in double, composeTRS) bit for bit."""
+    scene, cam, st = moving_cornell(pe)
+    scene.build_accelerator()
+    lib = pe._capi.load()
+    ref = oracle.RefScene(scene)
+    kind, tris, bounds = oracle.scene_shapes(ref)
+    out = np.empty(6, np.float32)
+    for i in range(scene.shape_count()):
+        assert lib.pe_scene_shape_bounds(scene.handle, i, pe._capi.fptr(out)) == pe._capi.PE_OK
+        assert np.array_equal(out, bounds[i]), (i, out, bounds[i])
+    n = scene.shape_count()
+    static = rot_y(0.5, (1.5, 0.6, 1.6), 1.2)
+    lo = bounds[n - 2][:3]
+    assert (lo < static[:3, 3] - 0.5).any(), "the moving cube's box spans the shutter"
+
+
+def test_moving_instance_refuses_a_refit(pe):
+    scene, cam, st = moving_cornell(pe)
+    scene.build_accelerator()
+    lib = pe._capi.load()
+    eye = np.eye(4, dtype=np.float32)
+    n = scene.shape_count()
+    f = pe._capi.fptr
+    assert lib.pe_scene_set_instance_transform(scene.handle, n - 2, f(eye), f(eye)) == pe._capi.PE_ERR_LIMIT
+    assert lib.pe_scene_set_instance_motion(scene.handle, 0, f(eye), None) == pe._capi.PE_ERR_INVALID

@@ -208,7 +208,7 @@ struct pe_device {
     int blocksIntersectMode[4] = {0, 0, 0, 0};
     // tuning (pe_tuning): closest-hit traversal variant, register budget of the lean shading kernels
     int closestMode = 1;  // TraceMode
-    int shadeBudget = 0;  // 0 the compiler's register count, 1 at most 128 registers (4 blocks per SM)
+    int shadeBudget = 1;  // 0 the compiler's register count, 1 (default) at most 128 registers (4 blocks per SM)
     std::string tuneLog;  // the last autotune's probe times
     int64_t tailPaths = -1; // -1: one resident grid of the tail kernel; 0: no tail kernel
     unsigned char* noAllocBase = nullptr; // device address of g_noAllocScratch on this device

@@ -115,8 +115,8 @@ int32_t checkSettings(const pe_camera* cam, const pe_settings* st) {
         setError("max_bounces out of range (0..255)");
         return PE_ERR_LIMIT;
     }
-    if (st->shadow_quality < 1 || st->shadow_quality > 1) {
-        setError("shadow_quality other than 1 is not supported by this device");
+    if (st->shadow_quality < 1 || st->shadow_quality > 64) {
+        setError("shadow_quality out of range (1..64)");
         return PE_ERR_LIMIT;
     }
     if (!(cam->lens_radius >= 0.0f) || cam->blades < 0 || cam->blades > 64) {
@@ -388,9 +388,12 @@ int32_t runWave(pe_device* d, int lane, Paths& P, int nSegs, int nSlots, int nPi
     stats.paths += static_cast<uint64_t>(nSlots);
     // lean shading (one specialised kernel per shading key) for plain surface scenes that
     // neither guide nor record; shadows without transmitters or shadow links are plain any-hits
-    bool noAo = true;
-    for (int k = 0; k < nSegs; ++k) noAo = noAo && !(ln.hSegs[k].aoStrength > 0.0f);
-    const bool lean = S.leanShading && !P.guiding && !P.sdMode && noAo && !d->counting;
+    bool noAo = true, inlineShadows = false;
+    for (int k = 0; k < nSegs; ++k) {
+        noAo = noAo && !(ln.hSegs[k].aoStrength > 0.0f);
+        inlineShadows = inlineShadows || ln.hSegs[k].shadowSamples > 1;
+    }
+    const bool lean = S.leanShading && !P.guiding && !P.sdMode && noAo && !d->counting && !inlineShadows;
     const bool anyHitShadows = !S.hasShadowTransmitters && !S.hasShadowLinks;
     int64_t tailPaths = d->tailPaths < 0 ? static_cast<int64_t>(d->blocksTail) * kTailBlock : d->tailPaths;
     // the tail kernel runs no inference: keep guided bounces in the wavefront until few paths remain
@@ -453,6 +456,10 @@ int32_t runWave(pe_device* d, int lane, Paths& P, int nSegs, int nSlots, int nPi
         if (tm.timing) PE_CUDA(cudaEventRecord(e1, cs));
         if (lean)
             stats.kernel_launches += launchLeanShade(d, S, P, W, qOut, cOut, cs, P.aovA || P.pass);
+        else if (inlineShadows && (P.aovA || P.pass))
+            kShade<true, true><<<d->blocksShade, 128, 0, cs>>>(S, P, W, qOut, cOut);
+        else if (inlineShadows)
+            kShade<false, true><<<d->blocksShade, 128, 0, cs>>>(S, P, W, qOut, cOut);
         else if (P.aovA || P.pass)
             kShade<true><<<d->blocksShade, 128, 0, cs>>>(S, P, W, qOut, cOut);
         else

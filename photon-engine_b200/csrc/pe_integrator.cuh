@@ -1222,7 +1222,9 @@ __device__ __forceinline__ bool shadeSlot(const SceneGPU& S, const Paths& P, con
 // Consumes the rays binned by shading key (segment by segment, so a warp mostly shades one
 // material kind) and appends the continuing paths to nextQueue.
 // OUT: the wave records AOVs or render passes (their code is compiled out of the plain kernel).
-template <bool OUT>
+// INLINE: NEE shadow rays are traced here, each sample's term added in the sample loop's order
+// (waves with shadowQuality > 1, whose several records per vertex the shadow queue does not hold).
+template <bool OUT, bool INLINE = false>
 __global__ void __launch_bounds__(128, 6) kShade(SceneGPU S, Paths P, Wave W, int32_t* nextQueue, uint32_t* nextCount) {
     uint32_t seg[kShadeKeys];
     int n = 0;
@@ -1248,7 +1250,7 @@ __global__ void __launch_bounds__(128, 6) kShade(SceneGPU S, Paths P, Wave W, in
             slot = P.sortQ[static_cast<size_t>(k) * P.capacity + j];
             const int path = pathOfSlot(P, slot);
             const WaveSeg& A = W.segs[segOfSlot(W, path)];
-            cont = shadeSlot<false, false, OUT>(S, P, A, slot, path, unused0, unused1, unused2);
+            cont = shadeSlot<INLINE, false, OUT>(S, P, A, slot, path, unused0, unused1, unused2);
             sweepable = (A.flags & SEG_SWEEP) != 0;
         }
         // a continuous wave sweeps its interactive paths that have lived sweepAge bounces into a

@@ -20,10 +20,14 @@
 #include "pe_xform.h"
 
 #if !defined(__CUDACC__)
-struct float4 { float x, y, z, w; };
-struct float2 { float x, y; };
-struct int4 { int x, y, z, w; };
+// The host compiler's stand-ins for CUDA's vector types, with CUDA's alignment, so that every
+// struct below has one layout in both compilers.
+struct alignas(16) float4 { float x, y, z, w; };
+struct alignas(8) float2 { float x, y; };
+struct alignas(16) int4 { int x, y, z, w; };
 #endif
+static_assert(alignof(float4) == 16 && alignof(int4) == 16 && alignof(float2) == 8,
+              "host and device must lay out the scene structs alike");
 
 namespace pe {
 

@@ -777,7 +777,12 @@ int64_t pe_server_submit(pe_server* S, const pe_request_desc* q) {
         setError("pe_server_submit: null argument");
         return -PE_ERR_INVALID;
     }
-    const int32_t rc = checkSettings(&q->camera, &q->settings);
+    int32_t rc = checkSettings(&q->camera, &q->settings);
+    if (rc == PE_OK && q->settings.shadow_quality > 1) {
+        setError("pe_server_submit: shadow_quality > 1 (several shadow rays a vertex): render the request with "
+                 "pe_device_render");
+        rc = PE_ERR_LIMIT;
+    }
     if (rc) return -rc;
     if (q->spp <= 0) {
         setError("pe_server_submit: spp must be positive");

@@ -515,6 +515,14 @@ int32_t pe_device_trace_primary(pe_device* d, const pe_camera* cam, const pe_set
                                 int32_t* out_shape, int32_t* out_prim, float* out_t);
 /* The same through the binary tree in the reference's own visiting order (near child first,
  * last tested triangle wins a tie), so ids are the reference's bit for bit, ties included. */
+/* Ray queries against the device's scene (Scene::intersect / intersectAny, bvh.cpp:322-446;
+ * a test probe): n rays (origins, directions xyz; t in [0, t_max[i]]) with visibility mask `mask`
+ * at shutter time `time`.  mode 0: closest hit on the binary tree in the reference's visiting
+ * order, 1: closest hit on the 4-wide tree — shape, triangle within the shape and t (shape -1 on
+ * a miss); 2: any hit on the 4-wide tree — out_shape 1 when occluded, else 0. */
+int32_t pe_device_trace_rays(pe_device* d, const float* origins, const float* directions, const float* t_max,
+                             int32_t n, int32_t mode, uint32_t mask, float time, int32_t* out_shape,
+                             int32_t* out_prim, float* out_t);
 int32_t pe_device_trace_primary_ordered(pe_device* d, const pe_camera* cam, const pe_settings* st,
                                         int32_t sample_index, int32_t* out_shape, int32_t* out_prim, float* out_t);
 

@@ -107,6 +107,7 @@ def _load(fast=False):
         "ref_scene_move_instance": (C.c_int32, [P, C.c_int32, FP, FP]),
         "ref_scene_set_instance_motion": (C.c_int32, [P, C.c_int32, FP, FP]),
         "ref_scene_shape_count": (C.c_int32, [P]),
+        "ref_trace_rays": (C.c_int32, [P, FP, FP, FP, C.c_int32, C.c_int32, C.c_uint32, C.c_float, IP, IP, FP]),
         "ref_camera_set_shutter_end": (None, [P, P]),
         "ref_load_project": (P, [C.c_char_p, C.c_float, IP, FP, IP, IP, FP, C.c_char_p, C.c_size_t]),
         "ref_scene_shapes": (C.c_int32, [P, IP, IP, FP, C.c_int32]),
@@ -403,6 +404,19 @@ class RefScene:
         self.lib.ref_render_rows(self.h, C.byref(camera.describe_gpu()), C.byref(settings.to_c()), first, count, threads,
                                  y0, y1, _f(mean), cnt.ctypes.data_as(UP))
         return mean, cnt
+
+    def trace_rays(self, origins, directions, t_max, mode: int = 0, mask: int = 0x1F, time: float = 0.0):
+        """Scene::intersect (mode 0) / intersectAny (mode 2) of rays: (shape, prim, t) arrays."""
+        o = np.ascontiguousarray(origins, np.float32).reshape(-1, 3)
+        d = np.ascontiguousarray(directions, np.float32).reshape(-1, 3)
+        tm = np.ascontiguousarray(t_max, np.float32).reshape(-1)
+        n = o.shape[0]
+        shape = np.empty(n, np.int32)
+        prim = np.empty(n, np.int32)
+        t = np.empty(n, np.float32)
+        self.lib.ref_trace_rays(self.h, _f(o), _f(d), _f(tm), n, int(mode), int(mask), float(time),
+                                shape.ctypes.data_as(IP), prim.ctypes.data_as(IP), _f(t))
+        return shape, prim, t
 
     def trace_primary(self, camera, settings, sample_index: int = 0):
         n = settings.width * settings.height

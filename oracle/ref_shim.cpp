@@ -1034,6 +1034,39 @@ int32_t ref_trace_primary(void* s, const pe_camera* cam, const pe_settings* st, 
     return 0;
 }
 
+// Scene::intersect / intersectAny of n rays (t in [0, t_max[i]], the visibility mask, the shutter
+// time): mode 0 closest hit (shape, triangle within it, t; shape -1 on a miss), 2 any hit
+// (out_shape 1 when occluded).
+int32_t ref_trace_rays(void* s, const float* o, const float* d, const float* tmax, int32_t n, int32_t mode,
+                       uint32_t mask, float time, int32_t* out_shape, int32_t* out_prim, float* out_t) {
+    auto* rs = static_cast<RefScene*>(s);
+    for (int32_t i = 0; i < n; ++i) {
+        Ray ray(v3(o + 3 * i), v3(d + 3 * i));
+        ray.tMin = 0.0f;
+        ray.tMax = tmax[i];
+        ray.visibilityMask = static_cast<uint8_t>(mask);
+        ray.time = time;
+        if (mode == 2) {
+            out_shape[i] = rs->scene.intersectAny(ray) ? 1 : 0;
+            out_prim[i] = -1;
+            out_t[i] = 0.0f;
+            continue;
+        }
+        SurfaceInteraction isect;
+        if (rs->scene.intersect(ray, isect)) {
+            auto it = rs->shapeIndex.find(isect.hitObject);
+            out_shape[i] = it == rs->shapeIndex.end() ? -2 : it->second;
+            out_prim[i] = isect.primIndex < 0 ? 0 : isect.primIndex;
+            out_t[i] = isect.t;
+        } else {
+            out_shape[i] = -1;
+            out_prim[i] = -1;
+            out_t[i] = 0.0f;
+        }
+    }
+    return 0;
+}
+
 int32_t ref_sobol(uint64_t seed, const int32_t* px, const int32_t* py, const int32_t* index, size_t n, int32_t ndims,
                   float* out) {
     SobolSampler s(seed);

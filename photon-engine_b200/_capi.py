@@ -194,6 +194,7 @@ SIGNATURES = {
     "pe_scene_refit": (C.c_int32, [P]),
     "pe_scene_set_instance_motion": (C.c_int32, [P, C.c_int32, FP, FP]),
     "pe_mat4_inverse": (None, [FP, FP]),
+    "pe_device_trace_rays": (C.c_int32, [P, FP, FP, FP, C.c_int32, C.c_int32, C.c_uint32, C.c_float, IP, IP, FP]),
     "pe_scene_shape_bounds": (C.c_int32, [P, C.c_int32, FP]),
     "pe_device_update_transforms": (C.c_int32, [P, P]),
     "pe_scene_add_sphere": (C.c_int32, [P, C.POINTER(C.c_float), C.c_float, C.c_int32]),

@@ -943,6 +943,42 @@ __global__ void kTracePrimary(SceneGPU S, WaveSeg A, int nPix, int32_t* outShape
     }
 }
 
+// Ray queries of pe_device_trace_rays: closest hit (binary tree in the reference's visiting
+// order, or the 4-wide tree) or any hit (4-wide), at a shutter time.
+template <int MODE>
+__global__ void kTraceRays(SceneGPU S, const float* o, const float* dir, const float* tMax, int n, uint32_t mask,
+                           float time, int32_t* outShape, int32_t* outPrim, float* outT) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const V3 ro = mk(o[3 * i], o[3 * i + 1], o[3 * i + 2]), rd = mk(dir[3 * i], dir[3 * i + 1], dir[3 * i + 2]);
+        uint32_t a = 0, b = 0;
+        if (MODE == 2) {
+            outShape[i] = traceAnyWide<false>(S, ro, rd, mask, 0.0f, tMax[i], a, b, time) ? 1 : 0;
+            outPrim[i] = -1;
+            outT[i] = 0.0f;
+            continue;
+        }
+        const Hit h = MODE == 1 ? traceClosestWide<false>(S, ro, rd, mask, 0.0f, tMax[i], a, b, nullptr, time)
+                                : traceClosest<false>(S, ro, rd, mask, 0.0f, tMax[i], a, b, time);
+        if (isMiss(h.prim)) {
+            outShape[i] = -1;
+            outPrim[i] = -1;
+            outT[i] = 0.0f;
+            continue;
+        }
+        int rec = h.prim, shape = -1;
+        if (isInstanceHit(h.prim)) {
+            const InstGPU& I = S.instances[instanceOfHit(h.prim)];
+            rec = I.recBase + localOfHit(h.prim);
+            shape = I.shape;
+        }
+        const int g = static_cast<int>(__float_as_uint(__ldg(&S.tris[3 * rec + 2]).w));
+        if (!isInstanceHit(h.prim)) shape = __ldg(&S.triVerts[g]).w;
+        outShape[i] = shape;
+        outPrim[i] = g - static_cast<int>(S.shapes[shape].firstTri);
+        outT[i] = h.t;
+    }
+}
+
 __global__ void kSobol(const TablesGPU* T, uint64_t seed, const int32_t* px, const int32_t* py, const int32_t* idx, int n,
                        int nd, float* out) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
@@ -2083,6 +2119,48 @@ static int32_t tracePrimary(pe_device* d, const pe_camera* cam, const pe_setting
     freeList(tmp);
     if (e != cudaSuccess) {
         setError(std::string("trace_primary: ") + cudaMsg(e));
+        return PE_ERR_CUDA;
+    }
+    return PE_OK;
+}
+
+int32_t pe_device_trace_rays(pe_device* d, const float* origins, const float* directions, const float* t_max, int32_t n,
+                             int32_t mode, uint32_t mask, float time, int32_t* out_shape, int32_t* out_prim, float* out_t) {
+    if (!d || !origins || !directions || !t_max || n < 0 || mode < 0 || mode > 2 || !out_shape || !out_prim || !out_t) {
+        setError("pe_device_trace_rays: bad argument");
+        return PE_ERR_INVALID;
+    }
+    if (!d->hasScene) {
+        setError("pe_device_trace_rays: no scene");
+        return PE_ERR_NO_SCENE;
+    }
+    if (n == 0) return PE_OK;
+    PE_CUDA(cudaSetDevice(d->ordinal));
+    std::vector<DevBuf> tmp;
+    float *dO = nullptr, *dD = nullptr, *dM = nullptr, *dT = nullptr;
+    int32_t *dS = nullptr, *dP = nullptr;
+    const size_t m = static_cast<size_t>(n);
+    int32_t rc;
+    if ((rc = devAlloc(tmp, dO, 3 * m)) || (rc = devAlloc(tmp, dD, 3 * m)) || (rc = devAlloc(tmp, dM, m)) ||
+        (rc = devAlloc(tmp, dT, m)) || (rc = devAlloc(tmp, dS, m)) || (rc = devAlloc(tmp, dP, m))) {
+        freeList(tmp);
+        return rc;
+    }
+    cudaMemcpyAsync(dO, origins, 3 * m * sizeof(float), cudaMemcpyHostToDevice, d->stream);
+    cudaMemcpyAsync(dD, directions, 3 * m * sizeof(float), cudaMemcpyHostToDevice, d->stream);
+    cudaMemcpyAsync(dM, t_max, m * sizeof(float), cudaMemcpyHostToDevice, d->stream);
+    const int grid = d->prop.multiProcessorCount * 8;
+    const SceneGPU& S = d->scene;
+    if (mode == 0) kTraceRays<0><<<grid, 128, 0, d->stream>>>(S, dO, dD, dM, n, mask, time, dS, dP, dT);
+    else if (mode == 1) kTraceRays<1><<<grid, 128, 0, d->stream>>>(S, dO, dD, dM, n, mask, time, dS, dP, dT);
+    else kTraceRays<2><<<grid, 128, 0, d->stream>>>(S, dO, dD, dM, n, mask, time, dS, dP, dT);
+    cudaMemcpyAsync(out_shape, dS, m * sizeof(int32_t), cudaMemcpyDeviceToHost, d->stream);
+    cudaMemcpyAsync(out_prim, dP, m * sizeof(int32_t), cudaMemcpyDeviceToHost, d->stream);
+    cudaMemcpyAsync(out_t, dT, m * sizeof(float), cudaMemcpyDeviceToHost, d->stream);
+    const cudaError_t e = cudaStreamSynchronize(d->stream);
+    freeList(tmp);
+    if (e != cudaSuccess) {
+        setError(std::string("trace_rays: ") + cudaMsg(e));
         return PE_ERR_CUDA;
     }
     return PE_OK;

@@ -682,13 +682,15 @@ __device__ bool walkAnyWide(const SceneGPU& S, int cur, V3 o, V3 d, V3 inv, uint
             const WideNode n = loadWide(S.wide, cur);
             float t[4];
             wideSlabs(n, o, inv, tMin, tMax, t);
-            // the first child hit is next, the other hits wait on the stack
-            int next = -1;
-            if (t[0] != kInf) next = n.child.x;
-            if (t[1] != kInf) { if (next == -1) next = n.child.y; else stackRef[sp++] = n.child.y; }
-            if (t[2] != kInf) { if (next == -1) next = n.child.z; else stackRef[sp++] = n.child.z; }
-            if (t[3] != kInf) { if (next == -1) next = n.child.w; else stackRef[sp++] = n.child.w; }
-            if (next == -1) {
+            // the first child hit is next, the other hits wait on the stack (a flag, not a
+            // sentinel reference: the leaf of primitive 0 alone is encoded as ~0 = -1)
+            int next = 0;
+            bool have = false;
+            if (t[0] != kInf) { next = n.child.x; have = true; }
+            if (t[1] != kInf) { if (!have) { next = n.child.y; have = true; } else stackRef[sp++] = n.child.y; }
+            if (t[2] != kInf) { if (!have) { next = n.child.z; have = true; } else stackRef[sp++] = n.child.z; }
+            if (t[3] != kInf) { if (!have) { next = n.child.w; have = true; } else stackRef[sp++] = n.child.w; }
+            if (!have) {
                 if (sp == 0) return false;
                 cur = stackRef[--sp];
             } else {

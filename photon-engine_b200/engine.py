@@ -1147,6 +1147,21 @@ class CudaDevice:
                       capi.iptr(shape), capi.iptr(prim), capi.fptr(t)))
         return shape, prim, t
 
+    def trace_rays(self, origins, directions, t_max, mode: int = 1, mask: int = VIS_ALL, time: float = 0.0):
+        """Ray queries against the scene (a test probe): mode 0 closest hit on the binary tree in
+        the reference's order, 1 closest hit on the 4-wide tree — (shape, prim, t), shape -1 on a
+        miss — or 2 any hit — (occluded 0/1, -1, 0)."""
+        o = np.ascontiguousarray(origins, np.float32).reshape(-1, 3)
+        d = np.ascontiguousarray(directions, np.float32).reshape(-1, 3)
+        tm = np.ascontiguousarray(t_max, np.float32).reshape(-1)
+        n = o.shape[0]
+        shape = np.empty(n, np.int32)
+        prim = np.empty(n, np.int32)
+        t = np.empty(n, np.float32)
+        capi.check(_lib().pe_device_trace_rays(self._h, capi.fptr(o), capi.fptr(d), capi.fptr(tm), n, int(mode), int(mask),
+                                               float(time), capi.iptr(shape), capi.iptr(prim), capi.fptr(t)))
+        return shape, prim, t
+
     def sobol(self, seed: int, px, py, index, n_dims: int) -> np.ndarray:
         px = np.ascontiguousarray(px, np.int32)
         py = np.ascontiguousarray(py, np.int32)

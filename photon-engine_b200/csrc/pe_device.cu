@@ -834,12 +834,11 @@ __global__ void kAdaptiveStop(const float* sum, const uint32_t* cnt, const float
 // least minAdaptiveSamples, before the batch's end) the pixels whose error fell below the
 // threshold stop.  Renderer::renderSamples decides the same per pixel (renderer.cpp:442-467,
 // 498-500), so every pixel takes the same samples and the film the same sums.
+// With SD-tree guiding (renderer.cpp:413-526 runs both in one renderSamples) each check interval
+// is further split at the field's refinements by renderWaves: a pixel's stops depend on its own
+// samples only, and each refinement sees the samples of every pixel still rendering, as there.
 int32_t renderAdaptive(pe_device* d, const pe_camera* cam, const pe_settings* st, int first, int count,
                        const volatile int32_t* cancel, uint64_t* traced) {
-    if (d->guideKind == 2) {
-        setError("adaptive sampling together with SD-tree guiding is not supported by this device");
-        return PE_ERR_INVALID;
-    }
     const int w = st->width, h = st->height;
     const size_t n = static_cast<size_t>(w) * static_cast<size_t>(h);
     if (d->adaptPixels < n) {

@@ -5,7 +5,9 @@ moving, at several shutter times) and the visibility masks.
 
 Tolerance: closest hits on the binary tree (the reference's visiting order): shape, triangle and
 distance bit-exact; on the 4-wide tree: distances bit-exact (a bit-identical tie may name the
-other triangle); any-hit answers identical.
+other triangle); any-hit answers identical.  A sphere hit's triangle number is not compared: the
+reference's Sphere::intersect leaves SurfaceInteraction::primIndex as an earlier candidate of the
+same traversal set it (an instance's triangle), which nothing downstream reads for spheres.
 """
 import importlib
 import pathlib
@@ -43,11 +45,21 @@ def shadow_rays(light_pos, light_u, light_v, lo, hi, n, seed):
     return p.astype(np.float32), (d / dist[:, None]).astype(np.float32), (dist * 0.999).astype(np.float32)
 
 
-def check_queries(device, ref, o, d, tm, mask=0x1F, time=0.0):
+def sphere_shapes(scene):
+    out, shape = [], 0
+    for kind, _ in scene.ops:
+        if kind == "sphere":
+            out.append(shape)
+        shape += 2 if kind == "area" else 1
+    return np.array(out, np.int32)
+
+
+def check_queries(device, ref, o, d, tm, mask=0x1F, time=0.0, spheres=()):
     rs, rp, rt = ref.trace_rays(o, d, tm, 0, mask, time)
     ms, mp, mt = device.trace_rays(o, d, tm, 0, mask, time)
     assert np.array_equal(ms, rs), (int((ms != rs).sum()), np.nonzero(ms != rs)[0][:8])
-    assert np.array_equal(mp, rp)
+    tri = ~np.isin(rs, np.asarray(spheres, np.int32))
+    assert np.array_equal(mp[tri], rp[tri]), (int((mp[tri] != rp[tri]).sum()))
     assert np.array_equal(mt.view(np.uint32), rt.view(np.uint32))
     ws, _, wt = device.trace_rays(o, d, tm, 1, mask, time)
     assert np.array_equal(wt.view(np.uint32), rt.view(np.uint32))
@@ -78,11 +90,12 @@ def test_project_rays_match_reference(pe, device, oracle):
     ref = oracle.RefScene(scene)
     lo, hi = scene_box(scene)
     o, d, tm = rays_through(lo, hi, 20000, 1)
-    hit = check_queries(device, ref, o, d, tm)
+    sph = sphere_shapes(scene)
+    hit = check_queries(device, ref, o, d, tm, spheres=sph)
     assert (hit >= 0).mean() > 0.3
     area = next(obj for kind, obj in scene.ops if kind == "area")
     o, d, tm = shadow_rays(area.position, area.u, area.v, lo, hi, 20000, 2)
-    check_queries(device, ref, o, d, tm, mask=16)
+    check_queries(device, ref, o, d, tm, mask=16, spheres=sph)
 
 
 def test_instanced_cornell_rays_match_reference(pe, device, oracle):

@@ -142,3 +142,42 @@ def test_guided_cornell_agrees_with_reference(pe, device, oracle):
     assert abs(float(mine.mean() / ref.mean()) - 1.0) < 0.02
     assert abs(float(theirs.mean() / ref.mean()) - 1.0) < 0.02
     assert e_mine < 2.0 * e_theirs, (e_mine, e_theirs)
+
+
+def test_adaptive_and_guided_together(pe, device, oracle):
+    """Adaptive sampling with the SD-tree on in one render (Renderer::renderSamples runs both,
+    renderer.cpp:413-526): the field trains on the pixels still rendering, pixels stop at the
+    8-sample checks; the reference's own adaptive guided render of the same view is the
+    comparison.  Both are unbiased against a converged plain render, take a similar number of
+    samples, and reach a similar error."""
+    scene, cam, st = scenes().cornell_box(48, 48, 64, 8, seed=0)
+    scene.build_accelerator()
+    device.set_scene(scene)
+    try:
+        ref = _render(pe, device, cam, st, 1 << 20, 8192, batch=1024)
+        st.path_guiding = True
+        st.adaptive_sampling = True
+        st.noise_threshold = 0.05
+        st.min_adaptive_samples = 8
+        film = pe.Film(st.width, st.height)
+        device.render(cam, st, pe.RenderTargets(beauty=film), 0, 64)
+        info = device.sdtree_info()
+        mine, cnt = film.resolve(), film.count
+    finally:
+        st.path_guiding = False
+        st.adaptive_sampling = False
+        device.set_guiding(0)
+    assert info.refinements == 5 and info.ready
+    assert cnt.min() >= 8 and cnt.max() <= 64 and cnt.mean() < 64, "some pixels stop early"
+    st.path_guiding = True
+    st.adaptive_sampling = True
+    theirs, tcnt = oracle.RefScene(scene).render_guided(cam, st, 0, 64)
+    st.path_guiding = False
+    st.adaptive_sampling = False
+    assert tcnt.min() >= 8 and tcnt.mean() < 64
+    assert abs(cnt.mean() / tcnt.mean() - 1.0) < 0.15, (cnt.mean(), tcnt.mean())
+    k = 0.18 / float(ref.mean())
+    e_mine = pe.rel_mse(mine * k, ref * k)
+    e_theirs = pe.rel_mse(theirs * k, ref * k)
+    assert abs(float(mine.mean() / ref.mean()) - 1.0) < 0.03
+    assert e_mine < 1.5 * e_theirs, (e_mine, e_theirs)

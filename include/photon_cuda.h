@@ -484,15 +484,18 @@ int64_t pe_device_tail_paths(pe_device* d);
 int32_t pe_device_autotune(pe_device* d, const pe_camera* cam, const pe_settings* st, int32_t probe_spp, int64_t* chosen);
 
 /* B200 tuning knobs with no counterpart in the reference engine; none changes a film.  The
- * autotuner above sets all three by coordinate descent on probe renders of the caller's frame
- * (closest-hit traversal, then the shading register budget, then the tail threshold). */
+ * autotuner above sets all four by coordinate descent on probe renders of the caller's frame
+ * (closest-hit traversal, any-hit traversal, the shading register budget, the tail threshold). */
 typedef struct pe_tuning {
     int64_t tail_paths;        /* as pe_device_set_tail_paths */
     int32_t closest_traversal; /* bounce-by-bounce closest hits: 0 the binary tree, 1 the 4-wide tree,
                                   2 / 3 the 4-wide tree with the first 8 / 16 stack entries of each
-                                  thread in shared memory (the rest in local memory) */
+                                  thread in shared memory (the rest in local memory), 4 / 5 with the
+                                  top 4 / 8 stack entries in registers */
     int32_t shade_budget;      /* lean shading kernels: 0 the compiler's register count, 1 (default) at
                                   most 128 registers a thread (four 128-thread blocks per SM) */
+    int32_t any_traversal;     /* plain any-hit shadows: 0 the stack in local memory, 1 its top 4
+                                  entries in registers */
 } pe_tuning;
 int32_t pe_device_get_tuning(pe_device* d, pe_tuning* out);
 int32_t pe_device_set_tuning(pe_device* d, const pe_tuning* t);

@@ -68,7 +68,8 @@ class pe_scene_info(C.Structure):
 
 
 class pe_tuning(C.Structure):
-    _fields_ = [("tail_paths", C.c_int64), ("closest_traversal", C.c_int32), ("shade_budget", C.c_int32)]
+    _fields_ = [("tail_paths", C.c_int64), ("closest_traversal", C.c_int32), ("shade_budget", C.c_int32),
+                ("any_traversal", C.c_int32)]
 
 
 class pe_device_info(C.Structure):

@@ -450,6 +450,10 @@ int32_t runWave(pe_device* d, int lane, Paths& P, int nSegs, int nSlots, int nPi
             kIntersect<false, TRACE_WIDE_SMEM8><<<d->blocksIntersectMode[2], 128, 0, cs>>>(S, P, qIn, cIn, d->dStats);
         else if (d->closestMode == TRACE_WIDE_SMEM16)
             kIntersect<false, TRACE_WIDE_SMEM16><<<d->blocksIntersectMode[3], 128, 0, cs>>>(S, P, qIn, cIn, d->dStats);
+        else if (d->closestMode == TRACE_WIDE_REG4)
+            kIntersect<false, TRACE_WIDE_REG4><<<d->blocksIntersectMode[4], 128, 0, cs>>>(S, P, qIn, cIn, d->dStats);
+        else if (d->closestMode == TRACE_WIDE_REG8)
+            kIntersect<false, TRACE_WIDE_REG8><<<d->blocksIntersectMode[5], 128, 0, cs>>>(S, P, qIn, cIn, d->dStats);
         else
             kIntersect<false><<<d->blocksIntersect, 128, 0, cs>>>(S, P, qIn, cIn, d->dStats);
         if (P.guiding == 2 && (rc = guideQueries(d, cs, P, W, qIn, cIn))) return rc;
@@ -467,6 +471,8 @@ int32_t runWave(pe_device* d, int lane, Paths& P, int nSegs, int nSlots, int nPi
         if (tm.timing) PE_CUDA(cudaEventRecord(e2, cs));
         if (d->counting)
             kShadow<true><<<d->blocksShadow, 128, 0, cs>>>(S, P, &P.counters[CNT_SHADOW], d->dStats);
+        else if (anyHitShadows && d->anyMode == 1)
+            kShadow<false, true, 4><<<d->blocksShadowAnyWindow, 128, 0, cs>>>(S, P, &P.counters[CNT_SHADOW], d->dStats);
         else if (anyHitShadows)
             kShadow<false, true><<<d->blocksShadowAny, 128, 0, cs>>>(S, P, &P.counters[CNT_SHADOW], d->dStats);
         else
@@ -1257,6 +1263,9 @@ pe_device* pe_device_create(int32_t ordinal, char* err, size_t errLen) {
     d->blocksIntersectMode[TRACE_WIDE] = occ(kIntersect<false, TRACE_WIDE>, 128);
     d->blocksIntersectMode[TRACE_WIDE_SMEM8] = occ(kIntersect<false, TRACE_WIDE_SMEM8>, 128);
     d->blocksIntersectMode[TRACE_WIDE_SMEM16] = occ(kIntersect<false, TRACE_WIDE_SMEM16>, 128);
+    d->blocksIntersectMode[TRACE_WIDE_REG4] = occ(kIntersect<false, TRACE_WIDE_REG4>, 128);
+    d->blocksIntersectMode[TRACE_WIDE_REG8] = occ(kIntersect<false, TRACE_WIDE_REG8>, 128);
+    d->blocksShadowAnyWindow = occ(kShadow<false, true, 4>, 128);
     const cudaError_t le = cudaGetLastError();
     if (le != cudaSuccess) {
         pe_device_destroy(d);
@@ -1938,7 +1947,7 @@ int32_t pe_device_autotune(pe_device* d, const pe_camera* cam, const pe_settings
     d->guideKind = 0;
     d->guide.mode = 0;
     const int64_t savedTail = d->tailPaths;
-    const int savedClosest = d->closestMode, savedBudget = d->shadeBudget;
+    const int savedClosest = d->closestMode, savedBudget = d->shadeBudget, savedAny = d->anyMode;
     std::string log;
     auto probe = [&](float& ms) -> int32_t {
         ms = 1e30f;
@@ -1970,7 +1979,8 @@ int32_t pe_device_autotune(pe_device* d, const pe_camera* cam, const pe_settings
         set(pick);
     };
     tune("closest_traversal", [&](int64_t v) { d->closestMode = static_cast<int>(v); },
-         {TRACE_WIDE, TRACE_BINARY, TRACE_WIDE_SMEM8, TRACE_WIDE_SMEM16});
+         {TRACE_WIDE, TRACE_BINARY, TRACE_WIDE_SMEM8, TRACE_WIDE_SMEM16, TRACE_WIDE_REG4, TRACE_WIDE_REG8});
+    tune("any_traversal", [&](int64_t v) { d->anyMode = static_cast<int>(v); }, {0, 1});
     tune("shade_budget", [&](int64_t v) { d->shadeBudget = static_cast<int>(v); }, {0, 1});
     const int64_t grid = static_cast<int64_t>(d->blocksTail) * kTailBlock;
     tune("tail_paths", [&](int64_t v) { d->tailPaths = v; }, {grid / 4, grid / 2, grid, 2 * grid});
@@ -1981,6 +1991,7 @@ int32_t pe_device_autotune(pe_device* d, const pe_camera* cam, const pe_settings
         d->tailPaths = savedTail;
         d->closestMode = savedClosest;
         d->shadeBudget = savedBudget;
+        d->anyMode = savedAny;
     }
     d->tuneLog = log;
     if (chosen) *chosen = d->tailPaths;
@@ -1995,6 +2006,7 @@ int32_t pe_device_get_tuning(pe_device* d, pe_tuning* out) {
     out->tail_paths = d->tailPaths;
     out->closest_traversal = d->closestMode;
     out->shade_budget = d->shadeBudget;
+    out->any_traversal = d->anyMode;
     return PE_OK;
 }
 
@@ -2003,14 +2015,15 @@ int32_t pe_device_set_tuning(pe_device* d, const pe_tuning* t) {
         setError("pe_device_set_tuning: null argument");
         return PE_ERR_INVALID;
     }
-    if (t->tail_paths < -1 || t->closest_traversal < 0 || t->closest_traversal > 3 || t->shade_budget < 0 ||
-        t->shade_budget > 1) {
+    if (t->tail_paths < -1 || t->closest_traversal < 0 || t->closest_traversal >= TRACE_MODES || t->shade_budget < 0 ||
+        t->shade_budget > 1 || t->any_traversal < 0 || t->any_traversal > 1) {
         setError("pe_device_set_tuning: value out of range");
         return PE_ERR_INVALID;
     }
     d->tailPaths = t->tail_paths;
     d->closestMode = t->closest_traversal;
     d->shadeBudget = t->shade_budget;
+    d->anyMode = t->any_traversal;
     return PE_OK;
 }
 

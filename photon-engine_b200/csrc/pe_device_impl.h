@@ -205,7 +205,9 @@ struct pe_device {
     int blocksIntersect = 0, blocksShade = 0, blocksShadow = 0, blocksGen = 0, blocksTail = 0;
     int blocksShadeKey[2][5] = {{0, 0, 0, 0, 0}, {0, 0, 0, 0, 0}}; // lean shading kernels: [budget][key]
     int blocksShadowAny = 0, blocksTailLean = 0;
-    int blocksIntersectMode[4] = {0, 0, 0, 0};
+    int blocksIntersectMode[6] = {0, 0, 0, 0, 0, 0};
+    int blocksShadowAnyWindow = 0; // kShadow with the any-hit stack's top entries in registers
+    int anyMode = 0;               // pe_tuning::any_traversal
     // tuning (pe_tuning): closest-hit traversal variant, register budget of the lean shading kernels
     int closestMode = 1;  // TraceMode
     int shadeBudget = 1;  // 0 the compiler's register count, 1 (default) at most 128 registers (4 blocks per SM)

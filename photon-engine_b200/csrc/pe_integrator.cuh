@@ -219,8 +219,16 @@ __global__ void kInitFree(Paths P, int n) {
 // Closest hit for every queued ray; each ray is then binned by its shading key (miss or the
 // hit material's type) so the shading kernel runs warps of one material kind.
 // Closest-hit traversal variants the tuner chooses among (pe_tuning::closest_traversal).
-enum TraceMode { TRACE_BINARY = 0, TRACE_WIDE = 1, TRACE_WIDE_SMEM8 = 2, TRACE_WIDE_SMEM16 = 3 };
-constexpr int traceStackShared(int mode) { return mode == TRACE_WIDE_SMEM8 ? 8 : (mode == TRACE_WIDE_SMEM16 ? 16 : 0); }
+// Closest-hit traversals: the binary tree in the reference's order; the 4-wide tree with its stack
+// in local memory, its first 8 / 16 entries in shared memory, or its top 4 / 8 entries in registers.
+enum TraceMode { TRACE_BINARY = 0, TRACE_WIDE = 1, TRACE_WIDE_SMEM8 = 2, TRACE_WIDE_SMEM16 = 3, TRACE_WIDE_REG4 = 4,
+                 TRACE_WIDE_REG8 = 5, TRACE_MODES = 6 };
+constexpr int traceStackShared(int mode) {
+    return mode == TRACE_WIDE_SMEM8 ? 8
+         : mode == TRACE_WIDE_SMEM16 ? 16
+         : mode == TRACE_WIDE_REG4 ? -4
+         : mode == TRACE_WIDE_REG8 ? -8 : 0;
+}
 
 template <bool COUNT, int MODE = TRACE_WIDE>
 __global__ void __launch_bounds__(128) kIntersect(SceneGPU S, Paths P, const int32_t* queue, const uint32_t* count,
@@ -354,7 +362,8 @@ __device__ __forceinline__ V3 neeTerm(V3 fLi, V3 vis, float scalar, V3 thr, bool
 // ---- any hit over the shadow queue ------------------------------------------------------------
 // ANY: the scene has neither shadow-transmitting surfaces nor shadow links, so visibility is
 // the plain any-hit query (and the transmittance walk is compiled out).
-template <bool COUNT, bool ANY = false>
+// AW: the any-hit walk's top AW stack entries in registers (0: all in local memory).
+template <bool COUNT, bool ANY = false, int AW = 0>
 __global__ void __launch_bounds__(128) kShadow(SceneGPU S, Paths P, const uint32_t* count, unsigned long long* stats) {
     const int n = static_cast<int>(*count);
     uint32_t nodes = 0, tris = 0;
@@ -368,8 +377,8 @@ __global__ void __launch_bounds__(128) kShadow(SceneGPU S, Paths P, const uint32
         const float4 sd = P.shD[i];
         const int light = static_cast<int>(__float_as_uint(P.shC[i].w) >> 1) - 1;
         const float time = pathTime(S, P, slot);
-        const V3 vis = ANY ? (traceAnyWide<COUNT>(S, mk(so.x, so.y, so.z), mk(sd.x, sd.y, sd.z), VIS_SHADOW, 0.0f, so.w, nodes,
-                                              tris, time) ? mk(0.0f) : mk(1.0f))
+        const V3 vis = ANY ? (traceAnyWide<COUNT, AW>(S, mk(so.x, so.y, so.z), mk(sd.x, sd.y, sd.z), VIS_SHADOW, 0.0f, so.w,
+                                                  nodes, tris, time) ? mk(0.0f) : mk(1.0f))
                            : shadowVisibility<COUNT>(S, mk(so.x, so.y, so.z), mk(sd.x, sd.y, sd.z), so.w, light, nodes, tris,
                                                      time);
         if (isBlack(vis)) continue;

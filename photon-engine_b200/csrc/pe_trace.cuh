@@ -257,7 +257,7 @@ __device__ void walkClosestWide(const SceneGPU& S, int cur, V3 o, V3 d, V3 inv, 
 template <bool COUNT, int LEVEL>
 __device__ bool walkAny(const SceneGPU& S, int cur, V3 o, V3 d, V3 inv, uint32_t mask, float tMin, float tMax,
                         uint32_t& nodeVisits, uint32_t& triTests, float time);
-template <bool COUNT, int LEVEL>
+template <bool COUNT, int LEVEL, int AW = 0>
 __device__ bool walkAnyWide(const SceneGPU& S, int cur, V3 o, V3 d, V3 inv, uint32_t mask, float tMin, float tMax,
                             uint32_t& nodeVisits, uint32_t& triTests, float time);
 
@@ -582,18 +582,56 @@ __device__ __forceinline__ void cmpx(float& ta, int& ra, int& ka, float& tb, int
     }
 }
 
-// The traversal stack of one thread: its first SD entries in shared memory (`shared` points at
-// the thread's column of a [SD][128] block array, stride 128), the rest in local memory.
+// A traversal stack whose top K entries live in registers (shifted on every push and pop, so
+// every index is static) and the rest in the thread's local memory: a walk pushes and pops mostly
+// within a few entries of the top, so most of its stack traffic never reaches memory.
+template <typename T, int K, int N>
+struct WindowStack {
+    T top[K];
+    T rest[N - K];
+    int n = 0;
+    __device__ __forceinline__ void push(T e) {
+        if (n >= K) rest[n - K] = top[K - 1];
+#pragma unroll
+        for (int i = K - 1; i > 0; --i) top[i] = top[i - 1];
+        top[0] = e;
+        ++n;
+    }
+    __device__ __forceinline__ T pop() {
+        const T e = top[0];
+#pragma unroll
+        for (int i = 0; i < K - 1; ++i) top[i] = top[i + 1];
+        --n;
+        if (n >= K) top[K - 1] = rest[n - K];
+        return e;
+    }
+    __device__ __forceinline__ bool empty() const { return n == 0; }
+};
+
+// The closest-hit walk's stack of (reference, entry distance) pairs.  SD > 0: its first SD entries
+// in shared memory (`shared` points at the thread's column of a [SD][128] block array, stride 128),
+// the rest in local memory; SD == 0: all in local memory; SD < 0: the top −SD entries in registers.
+template <int SD, bool WINDOW = (SD < 0)>
+struct TraceStack;
 template <int SD>
-struct TraceStack {
+struct TraceStack<SD, false> {
     uint2* shared;
     uint2 local[kWideStack - SD];
-    __device__ __forceinline__ void put(int i, int ref, float t) {
-        const uint2 e = make_uint2(static_cast<uint32_t>(ref), __float_as_uint(t));
-        if (SD > 0 && i < SD) shared[i * 128] = e;
-        else local[i - SD] = e;
+    int sp = 0;
+    __device__ __forceinline__ void push(uint2 e) {
+        if (SD > 0 && sp < SD) shared[sp * 128] = e;
+        else local[sp - SD] = e;
+        ++sp;
     }
-    __device__ __forceinline__ uint2 get(int i) const { return (SD > 0 && i < SD) ? shared[i * 128] : local[i - SD]; }
+    __device__ __forceinline__ uint2 pop() {
+        --sp;
+        return (SD > 0 && sp < SD) ? shared[sp * 128] : local[sp - SD];
+    }
+    __device__ __forceinline__ bool empty() const { return sp == 0; }
+};
+template <int SD>
+struct TraceStack<SD, true> : WindowStack<uint2, -SD, kWideStack> {
+    uint2* shared;
 };
 
 // The 4-wide walk from reference `cur`.  SD: stack entries kept in shared memory (`sstack`:
@@ -603,7 +641,6 @@ __device__ void walkClosestWide(const SceneGPU& S, int cur, V3 o, V3 d, V3 inv, 
                                 Hit& best, uint32_t& nodeVisits, uint32_t& triTests, uint2* sstack, float time) {
     TraceStack<SD> stack;
     stack.shared = sstack;
-    int sp = 0;
     for (;;) {
         while (cur >= 0) {
             if (COUNT) ++nodeVisits;
@@ -620,8 +657,8 @@ __device__ void walkClosestWide(const SceneGPU& S, int cur, V3 o, V3 d, V3 inv, 
             cmpx(t1, r1, k1, t2, r2, k2);
             if (t0 == kInf) {
                 bool found = false;
-                while (sp > 0) {
-                    const uint2 e = stack.get(--sp);
+                while (!stack.empty()) {
+                    const uint2 e = stack.pop();
                     if (__uint_as_float(e.y) <= tMax) {
                         cur = static_cast<int>(e.x);
                         found = true;
@@ -632,17 +669,17 @@ __device__ void walkClosestWide(const SceneGPU& S, int cur, V3 o, V3 d, V3 inv, 
                 continue;
             }
             // farther children first onto the stack, so they pop nearest first
-            if (t3 != kInf) stack.put(sp++, r3, t3);
-            if (t2 != kInf) stack.put(sp++, r2, t2);
-            if (t1 != kInf) stack.put(sp++, r1, t1);
+            if (t3 != kInf) stack.push(make_uint2(static_cast<uint32_t>(r3), __float_as_uint(t3)));
+            if (t2 != kInf) stack.push(make_uint2(static_cast<uint32_t>(r2), __float_as_uint(t2)));
+            if (t1 != kInf) stack.push(make_uint2(static_cast<uint32_t>(r1), __float_as_uint(t1)));
             cur = r0;
         }
         int first, count;
         leafRange(cur, first, count);
         testLeafClosest<COUNT, LEVEL, true>(S, first, count, o, d, mask, tMin, tMax, best, nodeVisits, triTests, time);
         bool found = false;
-        while (sp > 0) {
-            const uint2 e = stack.get(--sp);
+        while (!stack.empty()) {
+            const uint2 e = stack.pop();
             if (__uint_as_float(e.y) <= tMax) {
                 cur = static_cast<int>(e.x);
                 found = true;
@@ -671,9 +708,39 @@ __device__ Hit traceClosestWide(const SceneGPU& S, V3 o, V3 d, uint32_t mask, fl
 }
 
 // Any hit over the 4-wide tree from reference `cur`: the answer does not depend on the order.
-template <bool COUNT, int LEVEL>
+// AW > 0: the top AW stack entries in registers (WindowStack), else all in local memory.
+template <bool COUNT, int LEVEL, int AW>
 __device__ bool walkAnyWide(const SceneGPU& S, int cur, V3 o, V3 d, V3 inv, uint32_t mask, float tMin, float tMax,
                             uint32_t& nodeVisits, uint32_t& triTests, float time) {
+    if constexpr (AW > 0) {
+        WindowStack<int, AW, kWideStack> stack;
+        for (;;) {
+            while (cur >= 0) {
+                if (COUNT) ++nodeVisits;
+                const WideNode n = loadWide(S.wide, cur);
+                float t[4];
+                wideSlabs(n, o, inv, tMin, tMax, t);
+                int next = 0;
+                bool have = false;
+                if (t[0] != kInf) { next = n.child.x; have = true; }
+                if (t[1] != kInf) { if (!have) { next = n.child.y; have = true; } else stack.push(n.child.y); }
+                if (t[2] != kInf) { if (!have) { next = n.child.z; have = true; } else stack.push(n.child.z); }
+                if (t[3] != kInf) { if (!have) { next = n.child.w; have = true; } else stack.push(n.child.w); }
+                if (!have) {
+                    if (stack.empty()) return false;
+                    cur = stack.pop();
+                } else {
+                    cur = next;
+                }
+            }
+            int first, count;
+            leafRange(cur, first, count);
+            if (testLeafAny<COUNT, LEVEL, true>(S, first, count, o, d, mask, tMin, tMax, nodeVisits, triTests, time))
+                return true;
+            if (stack.empty()) return false;
+            cur = stack.pop();
+        }
+    }
     int stackRef[kWideStack];
     int sp = 0;
     for (;;) {
@@ -705,7 +772,7 @@ __device__ bool walkAnyWide(const SceneGPU& S, int cur, V3 o, V3 d, V3 inv, uint
     }
 }
 
-template <bool COUNT>
+template <bool COUNT, int AW = 0>
 __device__ bool traceAnyWide(const SceneGPU& S, V3 o, V3 d, uint32_t mask, float tMin, float tMax, uint32_t& nodeVisits,
                              uint32_t& triTests, float time = 0.0f) {
     const V3 inv = mk(1.0f / d.x, 1.0f / d.y, 1.0f / d.z);
@@ -713,7 +780,7 @@ __device__ bool traceAnyWide(const SceneGPU& S, V3 o, V3 d, uint32_t mask, float
     if (S.nTris == 0) return false;
     if (!slab(S.rootMin[0], S.rootMax[0], S.rootMin[1], S.rootMax[1], S.rootMin[2], S.rootMax[2], o, inv, tMin, tMax, tn))
         return false;
-    return walkAnyWide<COUNT, 0>(S, rootRef(S), o, d, inv, mask, tMin, tMax, nodeVisits, triTests, time);
+    return walkAnyWide<COUNT, 0, AW>(S, rootRef(S), o, d, inv, mask, tMin, tMax, nodeVisits, triTests, time);
 }
 
 // Shutter time of the path in `slot` (Ray::time): read only where the scene has moving instances.

@@ -1116,15 +1116,15 @@ class CudaDevice:
         return int(chosen.value)
 
     def tuning(self) -> dict:
-        """The device's tuning knobs (pe_tuning): tail_paths, closest_traversal, shade_budget."""
+        """The device's tuning knobs (pe_tuning): tail_paths, closest_traversal, shade_budget, any_traversal."""
         t = capi.pe_tuning()
         capi.check(_lib().pe_device_get_tuning(self._h, C.byref(t)))
         return {"tail_paths": int(t.tail_paths), "closest_traversal": int(t.closest_traversal),
-                "shade_budget": int(t.shade_budget)}
+                "shade_budget": int(t.shade_budget), "any_traversal": int(t.any_traversal)}
 
-    def set_tuning(self, tail_paths: int = -1, closest_traversal: int = 1, shade_budget: int = 0):
+    def set_tuning(self, tail_paths: int = -1, closest_traversal: int = 1, shade_budget: int = 1, any_traversal: int = 0):
         capi.check(_lib().pe_device_set_tuning(self._h, C.byref(capi.pe_tuning(tail_paths, closest_traversal,
-                                                                                shade_budget))))
+                                                                                shade_budget, any_traversal))))
 
     def autotune_log(self) -> str:
         """The last autotune's probe times ("knob=value time ms" per line)."""

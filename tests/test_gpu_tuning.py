@@ -1,0 +1,41 @@
+"""The device's tuning knobs (pe_tuning) change how fast a film is made, never the film: every
+4-wide closest-hit traversal variant (stack in local memory, first 8 / 16 entries in shared
+memory, top 4 / 8 entries in registers) visits the same nodes in the same order, the any-hit
+variants answer the same, the shading register budgets and tail thresholds run the same code, so
+their films are bit-identical; the binary tree may resolve a bit-identical distance tie to the
+other triangle of a shared edge, so its film is compared at the equal-spp bar.
+"""
+import importlib
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def test_tuning_knobs_leave_the_film_unchanged(pe, device):
+    S = importlib.import_module("photon_engine_b200.scenes")
+    scene, cam, st = S.torus_knot_scene(160, 90, 4, 8, nu=256, nv=16, env_size=(128, 64))
+    scene.build_accelerator()
+    device.set_scene(scene)
+
+    def film(**kw):
+        device.set_tuning(**kw)
+        f = pe.Film(st.width, st.height)
+        device.render(cam, st, pe.RenderTargets(beauty=f), 0, 4)
+        return f
+
+    try:
+        base = film(closest_traversal=1, shade_budget=1, any_traversal=0)
+        for mode in (2, 3, 4, 5):
+            f = film(closest_traversal=mode, shade_budget=1, any_traversal=0)
+            assert np.array_equal(f.sum, base.sum) and np.array_equal(f.count, base.count), mode
+        for kw in ({"any_traversal": 1}, {"shade_budget": 0}, {"tail_paths": 1024}, {"tail_paths": 0}):
+            args = {"closest_traversal": 1, "shade_budget": 1, "any_traversal": 0, **kw}
+            f = film(**args)
+            assert np.array_equal(f.sum, base.sum), kw
+        binary = film(closest_traversal=0, shade_budget=1, any_traversal=0)
+        assert np.array_equal(binary.count, base.count)
+        assert pe.rel_mse(binary.resolve(), base.resolve()) <= 1e-4
+    finally:
+        device.set_tuning()

@@ -598,8 +598,13 @@ int32_t loopBounce(pe_device* d, LaneLoop& L, const Wave& W, uint32_t* hSegLeft,
     P.sweepQ = sweep >= 0 ? L.sweepBuf[sweep] : nullptr;
     P.iter = L.iter;
     kIntersect<false><<<d->blocksIntersect, 128, 0, cs>>>(S, P, L.qIn, L.cIn, d->dStats);
-    kShade<false><<<d->blocksShade, 128, 0, cs>>>(S, P, W, L.qOut, L.cOut);
-    kShadow<false><<<d->blocksShadow, 128, 0, cs>>>(S, P, &P.counters[CNT_SHADOW], d->dStats);
+    // lean-shading scenes shade with the per-key kernels, as a lone render does
+    if (L.lean) launchLeanShade(d, S, P, W, L.qOut, L.cOut, cs, false);
+    else kShade<false><<<d->blocksShade, 128, 0, cs>>>(S, P, W, L.qOut, L.cOut);
+    if (!S.hasShadowTransmitters && !S.hasShadowLinks)
+        kShadow<false, true><<<d->blocksShadowAny, 128, 0, cs>>>(S, P, &P.counters[CNT_SHADOW], d->dStats);
+    else
+        kShadow<false><<<d->blocksShadow, 128, 0, cs>>>(S, P, &P.counters[CNT_SHADOW], d->dStats);
     PE_CUDA(cudaMemcpyAsync(ln.hCounters, P.counters, CNT_TOTAL * sizeof(uint32_t), cudaMemcpyDeviceToHost, cs));
     // segment counts as of the previous bounce's flushes (one bounce behind)
     if (segCount > 0)
@@ -621,9 +626,14 @@ int32_t loopBounce(pe_device* d, LaneLoop& L, const Wave& W, uint32_t* hSegLeft,
         PE_CUDA(cudaEventRecord(L.evReady[sweep], cs));
         PE_CUDA(cudaStreamWaitEvent(L.side, L.evReady[sweep], 0));
         PE_CUDA(cudaMemsetAsync(&L.sweepCursor[sweep], 0, sizeof(uint32_t), L.side));
-        const int grid = static_cast<int>(std::min<int64_t>(d->blocksTail, (swept + kTailBlock - 1) / kTailBlock));
-        kTail<false, false><<<grid, kTailBlock, 0, L.side>>>(S, P, W, L.sweepBuf[sweep], &L.sweepCnt[sweep],
-                                                       &L.sweepCursor[sweep], d->dStats);
+        const int grid = static_cast<int>(std::min<int64_t>(L.lean ? d->blocksTailLean : d->blocksTail,
+                                                            (swept + kTailBlock - 1) / kTailBlock));
+        if (L.lean)
+            kTail<false, false, true><<<grid, kTailBlock, 0, L.side>>>(S, P, W, L.sweepBuf[sweep], &L.sweepCnt[sweep],
+                                                                     &L.sweepCursor[sweep], d->dStats);
+        else
+            kTail<false, false><<<grid, kTailBlock, 0, L.side>>>(S, P, W, L.sweepBuf[sweep], &L.sweepCnt[sweep],
+                                                           &L.sweepCursor[sweep], d->dStats);
         kFlush<<<d->prop.multiProcessorCount * 4, 256, 0, L.side>>>(P, W, L.sweepBuf[sweep], &L.sweepCnt[sweep]);
         PE_CUDA(cudaEventRecord(L.evDone[sweep], L.side));
         L.sweepN[sweep] = swept;
@@ -631,6 +641,7 @@ int32_t loopBounce(pe_device* d, LaneLoop& L, const Wave& W, uint32_t* hSegLeft,
     }
     PE_CUDA(cudaMemsetAsync(L.cIn, 0, sizeof(uint32_t), cs));
     PE_CUDA(cudaMemsetAsync(&P.counters[CNT_SHADOW], 0, (CNT_KEYS + kShadeKeys - CNT_SHADOW) * sizeof(uint32_t), cs));
+    if (L.lean) PE_CUDA(cudaMemsetAsync(&P.counters[CNT_WORK_KEYS], 0, kShadeKeys * sizeof(uint32_t), cs));
     std::swap(L.qIn, L.qOut);
     std::swap(L.cIn, L.cOut);
     if (++L.iter > kMaxWavefrontIterations * 64) {
@@ -646,8 +657,13 @@ int32_t loopTail(pe_device* d, LaneLoop& L, const Wave& W) {
     WaveLane& ln = *L.ln;
     Paths& P = ln.paths;
     const cudaStream_t cs = ln.stream;
-    const int grid = static_cast<int>(std::min<int64_t>(d->blocksTail, (static_cast<int64_t>(L.live) + kTailBlock - 1) / kTailBlock));
-    kTail<false, false><<<grid, kTailBlock, 0, cs>>>(L.scene, P, W, L.qIn, L.cIn, &P.counters[CNT_WORK_TAIL], d->dStats);
+    const int grid = static_cast<int>(std::min<int64_t>(L.lean ? d->blocksTailLean : d->blocksTail,
+                                                        (static_cast<int64_t>(L.live) + kTailBlock - 1) / kTailBlock));
+    if (L.lean)
+        kTail<false, false, true><<<grid, kTailBlock, 0, cs>>>(L.scene, P, W, L.qIn, L.cIn, &P.counters[CNT_WORK_TAIL],
+                                                              d->dStats);
+    else
+        kTail<false, false><<<grid, kTailBlock, 0, cs>>>(L.scene, P, W, L.qIn, L.cIn, &P.counters[CNT_WORK_TAIL], d->dStats);
     kFlush<<<d->prop.multiProcessorCount * 4, 256, 0, cs>>>(P, W, L.qIn, L.cIn);
     L.live = 0;
     PE_CUDA(cudaGetLastError());

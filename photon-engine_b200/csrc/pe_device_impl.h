@@ -291,6 +291,7 @@ struct LaneLoop {
     uint32_t* cIn = nullptr;
     uint32_t* cOut = nullptr;
     uint32_t live = 0;  // paths in the next closest-hit queue
+    bool lean = false;  // the lean per-key shading kernels (a lean-shading scene, no segment with AO)
     int freeTop = 0;    // free slots on the stack
     int nextPath = 0;   // wave path index of the next injected path
     int pathCap = 0;    // paths the wave can hold (Lout)

@@ -1287,15 +1287,19 @@ __global__ void __launch_bounds__(128, MINB) kShadeKey(SceneGPU S, Paths P, Wave
         const int base = warpFetch(&P.counters[CNT_WORK_KEYS + KEY]);
         if (base >= n) break;
         const int i = base + lane;
-        bool cont = false;
+        bool cont = false, sweepable = false;
         int slot = -1;
         if (i < n) {
             slot = bin[i];
             const int path = pathOfSlot(P, slot);
             const WaveSeg& A = W.segs[segOfSlot(W, path)];
             cont = shadeSlot<false, false, OUT, KEY>(S, P, A, slot, path, unused0, unused1, unused2);
+            sweepable = (A.flags & SEG_SWEEP) != 0;
         }
-        queuePush(nextQueue, nextCount, cont, slot);
+        // continuous waves sweep interactive paths that have lived sweepAge bounces, as kShade does
+        const bool old = P.sweepAge > 0 && cont && sweepable && P.iter - P.born[slot] >= P.sweepAge;
+        queuePush(nextQueue, nextCount, cont && !old, slot);
+        if (P.sweepAge > 0) queuePush(P.sweepQ, &P.counters[CNT_SWEEP], old, slot);
         if (P.pathOf) queuePush(P.freeQ, &P.counters[CNT_FREE], !cont && slot >= 0, slot);
     }
 }

@@ -135,6 +135,8 @@ struct pe_server {
         bool draining = false;        // taking in no paths: the wave ends once its live paths fit the tail kernel
         bool yielding = false;        // draining so that another scene gets this lane
         int firstOpen = 0;            // first segment not yet filmed
+        int aoChecked = 0;            // segments looked at for contact AO
+        bool anyAo = false;           // some segment of the wave has contact AO (full shading kernel)
         int uploaded = 0;             // segments on the device
         LaneLoop loop;
         WaveLane own;                 // the express lane's own path state (bulk lanes use the device's)
@@ -519,6 +521,8 @@ void laneThread(pe_server* S, int li) {
             R.yielding = false;
             R.segs.clear();
             R.firstOpen = 0;
+            R.aoChecked = 0;
+            R.anyAo = false;
             R.uploaded = 0;
             R.loop.scene = S->scenes[static_cast<size_t>(R.scene)].gpu;
             ++S->stats.waves;
@@ -558,6 +562,9 @@ void laneThread(pe_server* S, int li) {
         }
         R.draining = R.yielding || !room || !bestFor(S, li, R.scene);
         const int nSegs = static_cast<int>(R.segs.size());
+        for (; R.aoChecked < nSegs; ++R.aoChecked)
+            if (R.hSegs[R.aoChecked].aoStrength > 0.0f) R.anyAo = true;
+        L.lean = L.scene.leanShading && !R.anyAo;
         const int upFirst = R.uploaded;
         R.uploaded = nSegs;
         const bool draining = R.draining;

@@ -591,7 +591,7 @@ int32_t loopBounce(pe_device* d, LaneLoop& L, const Wave& W, uint32_t* hSegLeft,
     const SceneGPU& S = L.scene;
     // a free sweep buffer takes this bounce's old paths (none free: no sweep this bounce)
     int sweep = -1;
-    if (L.sweepAge > 0)
+    if (L.sweepAge > 0 && (L.sweepLive <= 0 || static_cast<int64_t>(L.live) <= L.sweepLive))
         for (int b = 0; b < LaneLoop::kSweepBufs && sweep < 0; ++b)
             if (L.sweepN[b] == 0) sweep = b;
     P.sweepAge = sweep >= 0 ? L.sweepAge : 0;

@@ -299,6 +299,7 @@ struct LaneLoop {
     // sweeps: paths alive for sweepAge bounces finish in tail-kernel launches on `side`
     static constexpr int kSweepBufs = 8;
     int sweepAge = 0;                    // 0: off
+    int64_t sweepLive = 0;               // sweep only when the wave holds at most this many live paths (0: always)
     cudaStream_t side = nullptr;
     int32_t* born = nullptr;             // device, one per slot
     int32_t* sweepBuf[kSweepBufs] = {};  // device, one slot list per sweep in flight

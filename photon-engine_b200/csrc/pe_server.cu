@@ -110,6 +110,7 @@ struct pe_server {
     std::condition_variable cvWork, cvDone;
     std::thread worker;
     bool stop = false;
+    std::thread watcher;             // marks requests done as soon as their film kernels have run
     Clock::time_point t0;
     SceneGPU savedScene{};
     bool savedHasScene = false;
@@ -609,6 +610,21 @@ void laneThread(pe_server* S, int li) {
     cudaStreamSynchronize(cs);
 }
 
+// Polls the lanes' completion events every 0.2 ms, so that a request is done (and its waiters
+// wake) when its last film kernel has run, not when its lane next returns from a bounce.
+void watchThread(pe_server* S) {
+    cudaSetDevice(S->d->ordinal);
+    for (;;) {
+        {
+            std::lock_guard<std::mutex> lk(S->mu);
+            if (S->stop) return;
+            for (int li = 0; li < kLanes; ++li)
+                if (!S->lanes[li].doneEvents.empty()) settleDone(S, li);
+        }
+        std::this_thread::sleep_for(std::chrono::microseconds(200));
+    }
+}
+
 // Frees the server's streams, events and segment tables, then the server.
 void releaseServer(pe_server* S) {
     if (S->trace) std::fclose(S->trace);
@@ -705,6 +721,10 @@ pe_server* pe_server_create(pe_device* d, uint64_t budget, char* err, size_t err
         LaneLoop& L = R.loop;
         const size_t cap = ok ? R.loop.ln->paths.capacity : 0;
         L.sweepAge = express(li) ? kExpressSweepAge : kSweepAge;
+        // an express wave holds only interactive paths: sweeping millions of them into the tail
+        // kernel (one thread per path) would be slower than their wavefront bounces, so it sweeps
+        // only the stragglers of a wave that has shrunk to a few tail grids
+        L.sweepLive = express(li) ? 4 * pe_device_tail_paths(d) : 0;
         ok = ok && cudaStreamCreateWithPriority(&L.side, cudaStreamNonBlocking, express(li) ? hiPrio : loPrio) == cudaSuccess &&
              cudaMalloc(&L.born, cap * sizeof(int32_t)) == cudaSuccess &&
              cudaMalloc(&L.sweepCnt, LaneLoop::kSweepBufs * sizeof(uint32_t)) == cudaSuccess &&
@@ -721,6 +741,7 @@ pe_server* pe_server_create(pe_device* d, uint64_t budget, char* err, size_t err
     d->filmLane = -1;
     if (const char* tp = std::getenv("PE_SERVER_TRACE")) S->trace = std::fopen(tp, "w");
     for (int li = 0; li < kLanes; ++li) S->lanes[li].th = std::thread(laneThread, S, li);
+    S->watcher = std::thread(watchThread, S);
     return S;
 }
 
@@ -733,6 +754,7 @@ void pe_server_destroy(pe_server* S) {
     S->cvWork.notify_all();
     for (auto& R : S->lanes)
         if (R.th.joinable()) R.th.join();
+    if (S->watcher.joinable()) S->watcher.join();
     pe_device* d = S->d;
     cudaSetDevice(d->ordinal);
     cudaStreamSynchronize(d->stream);

@@ -491,11 +491,12 @@ typedef struct pe_tuning {
     int32_t closest_traversal; /* bounce-by-bounce closest hits: 0 the binary tree, 1 the 4-wide tree,
                                   2 / 3 the 4-wide tree with the first 8 / 16 stack entries of each
                                   thread in shared memory (the rest in local memory), 4 / 5 with the
-                                  top 4 / 8 stack entries in registers */
+                                  top 4 / 8 stack entries in registers, 6 (default) the 4-wide tree
+                                  capped at 64 registers (eight 128-thread blocks per SM) */
     int32_t shade_budget;      /* lean shading kernels: 0 the compiler's register count, 1 (default) at
                                   most 128 registers a thread (four 128-thread blocks per SM) */
     int32_t any_traversal;     /* plain any-hit shadows: 0 the stack in local memory, 1 its top 4
-                                  entries in registers */
+                                  entries in registers, 2 (default) capped at 64 registers */
 } pe_tuning;
 int32_t pe_device_get_tuning(pe_device* d, pe_tuning* out);
 int32_t pe_device_set_tuning(pe_device* d, const pe_tuning* t);

@@ -454,6 +454,8 @@ int32_t runWave(pe_device* d, int lane, Paths& P, int nSegs, int nSlots, int nPi
             kIntersect<false, TRACE_WIDE_REG4><<<d->blocksIntersectMode[4], 128, 0, cs>>>(S, P, qIn, cIn, d->dStats);
         else if (d->closestMode == TRACE_WIDE_REG8)
             kIntersect<false, TRACE_WIDE_REG8><<<d->blocksIntersectMode[5], 128, 0, cs>>>(S, P, qIn, cIn, d->dStats);
+        else if (d->closestMode == TRACE_WIDE_OCC8)
+            kIntersect<false, TRACE_WIDE_OCC8><<<d->blocksIntersectMode[6], 128, 0, cs>>>(S, P, qIn, cIn, d->dStats);
         else
             kIntersect<false><<<d->blocksIntersect, 128, 0, cs>>>(S, P, qIn, cIn, d->dStats);
         if (P.guiding == 2 && (rc = guideQueries(d, cs, P, W, qIn, cIn))) return rc;
@@ -473,6 +475,8 @@ int32_t runWave(pe_device* d, int lane, Paths& P, int nSegs, int nSlots, int nPi
             kShadow<true><<<d->blocksShadow, 128, 0, cs>>>(S, P, &P.counters[CNT_SHADOW], d->dStats);
         else if (anyHitShadows && d->anyMode == 1)
             kShadow<false, true, 4><<<d->blocksShadowAnyWindow, 128, 0, cs>>>(S, P, &P.counters[CNT_SHADOW], d->dStats);
+        else if (anyHitShadows && d->anyMode == 2)
+            kShadow<false, true, 0, 8><<<d->blocksShadowAnyOcc8, 128, 0, cs>>>(S, P, &P.counters[CNT_SHADOW], d->dStats);
         else if (anyHitShadows)
             kShadow<false, true><<<d->blocksShadowAny, 128, 0, cs>>>(S, P, &P.counters[CNT_SHADOW], d->dStats);
         else
@@ -1282,6 +1286,8 @@ pe_device* pe_device_create(int32_t ordinal, char* err, size_t errLen) {
     d->blocksIntersectMode[TRACE_WIDE_REG4] = occ(kIntersect<false, TRACE_WIDE_REG4>, 128);
     d->blocksIntersectMode[TRACE_WIDE_REG8] = occ(kIntersect<false, TRACE_WIDE_REG8>, 128);
     d->blocksShadowAnyWindow = occ(kShadow<false, true, 4>, 128);
+    d->blocksIntersectMode[TRACE_WIDE_OCC8] = occ(kIntersect<false, TRACE_WIDE_OCC8>, 128);
+    d->blocksShadowAnyOcc8 = occ(kShadow<false, true, 0, 8>, 128);
     const cudaError_t le = cudaGetLastError();
     if (le != cudaSuccess) {
         pe_device_destroy(d);
@@ -1995,8 +2001,9 @@ int32_t pe_device_autotune(pe_device* d, const pe_camera* cam, const pe_settings
         set(pick);
     };
     tune("closest_traversal", [&](int64_t v) { d->closestMode = static_cast<int>(v); },
-         {TRACE_WIDE, TRACE_BINARY, TRACE_WIDE_SMEM8, TRACE_WIDE_SMEM16, TRACE_WIDE_REG4, TRACE_WIDE_REG8});
-    tune("any_traversal", [&](int64_t v) { d->anyMode = static_cast<int>(v); }, {0, 1});
+         {TRACE_WIDE, TRACE_BINARY, TRACE_WIDE_SMEM8, TRACE_WIDE_SMEM16, TRACE_WIDE_REG4, TRACE_WIDE_REG8,
+          TRACE_WIDE_OCC8});
+    tune("any_traversal", [&](int64_t v) { d->anyMode = static_cast<int>(v); }, {0, 1, 2});
     tune("shade_budget", [&](int64_t v) { d->shadeBudget = static_cast<int>(v); }, {0, 1});
     const int64_t grid = static_cast<int64_t>(d->blocksTail) * kTailBlock;
     tune("tail_paths", [&](int64_t v) { d->tailPaths = v; }, {grid / 4, grid / 2, grid, 2 * grid});
@@ -2032,7 +2039,7 @@ int32_t pe_device_set_tuning(pe_device* d, const pe_tuning* t) {
         return PE_ERR_INVALID;
     }
     if (t->tail_paths < -1 || t->closest_traversal < 0 || t->closest_traversal >= TRACE_MODES || t->shade_budget < 0 ||
-        t->shade_budget > 1 || t->any_traversal < 0 || t->any_traversal > 1) {
+        t->shade_budget > 1 || t->any_traversal < 0 || t->any_traversal > 2) {
         setError("pe_device_set_tuning: value out of range");
         return PE_ERR_INVALID;
     }

@@ -205,11 +205,12 @@ struct pe_device {
     int blocksIntersect = 0, blocksShade = 0, blocksShadow = 0, blocksGen = 0, blocksTail = 0;
     int blocksShadeKey[2][5] = {{0, 0, 0, 0, 0}, {0, 0, 0, 0, 0}}; // lean shading kernels: [budget][key]
     int blocksShadowAny = 0, blocksTailLean = 0;
-    int blocksIntersectMode[6] = {0, 0, 0, 0, 0, 0};
+    int blocksIntersectMode[7] = {0, 0, 0, 0, 0, 0, 0};
+    int blocksShadowAnyOcc8 = 0;   // kShadow capped at 64 registers
     int blocksShadowAnyWindow = 0; // kShadow with the any-hit stack's top entries in registers
-    int anyMode = 0;               // pe_tuning::any_traversal
+    int anyMode = 2;               // pe_tuning::any_traversal (default: the 64-register cap)
     // tuning (pe_tuning): closest-hit traversal variant, register budget of the lean shading kernels
-    int closestMode = 1;  // TraceMode
+    int closestMode = 6;  // TraceMode (default: TRACE_WIDE_OCC8, the autotuner's pick on the knot frame)
     int shadeBudget = 1;  // 0 the compiler's register count, 1 (default) at most 128 registers (4 blocks per SM)
     std::string tuneLog;  // the last autotune's probe times
     int64_t tailPaths = -1; // -1: one resident grid of the tail kernel; 0: no tail kernel

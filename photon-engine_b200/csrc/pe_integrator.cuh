@@ -221,8 +221,10 @@ __global__ void kInitFree(Paths P, int n) {
 // Closest-hit traversal variants the tuner chooses among (pe_tuning::closest_traversal).
 // Closest-hit traversals: the binary tree in the reference's order; the 4-wide tree with its stack
 // in local memory, its first 8 / 16 entries in shared memory, or its top 4 / 8 entries in registers.
+// TRACE_WIDE_OCC8: the 4-wide walk capped at 64 registers, eight 128-thread blocks per SM.
 enum TraceMode { TRACE_BINARY = 0, TRACE_WIDE = 1, TRACE_WIDE_SMEM8 = 2, TRACE_WIDE_SMEM16 = 3, TRACE_WIDE_REG4 = 4,
-                 TRACE_WIDE_REG8 = 5, TRACE_MODES = 6 };
+                 TRACE_WIDE_REG8 = 5, TRACE_WIDE_OCC8 = 6, TRACE_MODES = 7 };
+constexpr int traceMinBlocks(int mode) { return mode == TRACE_WIDE_OCC8 ? 8 : 1; }
 constexpr int traceStackShared(int mode) {
     return mode == TRACE_WIDE_SMEM8 ? 8
          : mode == TRACE_WIDE_SMEM16 ? 16
@@ -231,8 +233,8 @@ constexpr int traceStackShared(int mode) {
 }
 
 template <bool COUNT, int MODE = TRACE_WIDE>
-__global__ void __launch_bounds__(128) kIntersect(SceneGPU S, Paths P, const int32_t* queue, const uint32_t* count,
-                                                  unsigned long long* stats) {
+__global__ void __launch_bounds__(128, traceMinBlocks(MODE)) kIntersect(SceneGPU S, Paths P, const int32_t* queue,
+                                                                        const uint32_t* count, unsigned long long* stats) {
     constexpr int SD = traceStackShared(MODE);
     __shared__ uint2 sstack[SD > 0 ? SD * 128 : 1];
     const int n = static_cast<int>(*count);
@@ -363,8 +365,10 @@ __device__ __forceinline__ V3 neeTerm(V3 fLi, V3 vis, float scalar, V3 thr, bool
 // ANY: the scene has neither shadow-transmitting surfaces nor shadow links, so visibility is
 // the plain any-hit query (and the transmittance walk is compiled out).
 // AW: the any-hit walk's top AW stack entries in registers (0: all in local memory).
-template <bool COUNT, bool ANY = false, int AW = 0>
-__global__ void __launch_bounds__(128) kShadow(SceneGPU S, Paths P, const uint32_t* count, unsigned long long* stats) {
+// MINB: at least this many 128-thread blocks per SM (8: a 64-register cap).
+template <bool COUNT, bool ANY = false, int AW = 0, int MINB = 1>
+__global__ void __launch_bounds__(128, MINB) kShadow(SceneGPU S, Paths P, const uint32_t* count,
+                                                    unsigned long long* stats) {
     const int n = static_cast<int>(*count);
     uint32_t nodes = 0, tris = 0;
     for (;;) {

@@ -1122,7 +1122,7 @@ class CudaDevice:
         return {"tail_paths": int(t.tail_paths), "closest_traversal": int(t.closest_traversal),
                 "shade_budget": int(t.shade_budget), "any_traversal": int(t.any_traversal)}
 
-    def set_tuning(self, tail_paths: int = -1, closest_traversal: int = 1, shade_budget: int = 1, any_traversal: int = 0):
+    def set_tuning(self, tail_paths: int = -1, closest_traversal: int = 6, shade_budget: int = 1, any_traversal: int = 2):
         capi.check(_lib().pe_device_set_tuning(self._h, C.byref(capi.pe_tuning(tail_paths, closest_traversal,
                                                                                 shade_budget, any_traversal))))
 

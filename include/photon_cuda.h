@@ -494,7 +494,8 @@ typedef struct pe_tuning {
                                   top 4 / 8 stack entries in registers, 6 (default) the 4-wide tree
                                   capped at 64 registers (eight 128-thread blocks per SM) */
     int32_t shade_budget;      /* lean shading kernels: 0 the compiler's register count, 1 (default) at
-                                  most 128 registers a thread (four 128-thread blocks per SM) */
+                                  most 128 registers a thread (four 128-thread blocks per SM), 2 at
+                                  most 96 (five blocks) */
     int32_t any_traversal;     /* plain any-hit shadows: 0 the stack in local memory, 1 its top 4
                                   entries in registers, 2 (default) capped at 64 registers */
 } pe_tuning;

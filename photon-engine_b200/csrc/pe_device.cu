@@ -228,7 +228,13 @@ int launchLeanShade(pe_device* d, const SceneGPU& S, const Paths& P, const Wave&
         kernel<<<d->blocksShadeKey[budget][key], 128, 0, cs>>>(S, P, W, qOut, cOut);
         ++n;
     };
-    if (!out && budget == 1) {
+    if (!out && budget == 2) {
+        one(kShadeKey<false, 0, 5>, 0);
+        one(kShadeKey<false, 1, 5>, 1);
+        one(kShadeKey<false, 2, 5>, 2);
+        one(kShadeKey<false, 3, 5>, 3);
+        one(kShadeKey<false, 4, 5>, 4);
+    } else if (!out && budget == 1) {
         one(kShadeKey<false, 0, 4>, 0);
         one(kShadeKey<false, 1, 4>, 1);
         one(kShadeKey<false, 2, 4>, 2);
@@ -1279,6 +1285,11 @@ pe_device* pe_device_create(int32_t ordinal, char* err, size_t errLen) {
     d->blocksShadeKey[1][2] = occ(kShadeKey<false, 2, 4>, 128);
     d->blocksShadeKey[1][3] = occ(kShadeKey<false, 3, 4>, 128);
     d->blocksShadeKey[1][4] = occ(kShadeKey<false, 4, 4>, 128);
+    d->blocksShadeKey[2][0] = occ(kShadeKey<false, 0, 5>, 128);
+    d->blocksShadeKey[2][1] = occ(kShadeKey<false, 1, 5>, 128);
+    d->blocksShadeKey[2][2] = occ(kShadeKey<false, 2, 5>, 128);
+    d->blocksShadeKey[2][3] = occ(kShadeKey<false, 3, 5>, 128);
+    d->blocksShadeKey[2][4] = occ(kShadeKey<false, 4, 5>, 128);
     d->blocksIntersectMode[TRACE_BINARY] = occ(kIntersect<false, TRACE_BINARY>, 128);
     d->blocksIntersectMode[TRACE_WIDE] = occ(kIntersect<false, TRACE_WIDE>, 128);
     d->blocksIntersectMode[TRACE_WIDE_SMEM8] = occ(kIntersect<false, TRACE_WIDE_SMEM8>, 128);
@@ -2004,7 +2015,7 @@ int32_t pe_device_autotune(pe_device* d, const pe_camera* cam, const pe_settings
          {TRACE_WIDE, TRACE_BINARY, TRACE_WIDE_SMEM8, TRACE_WIDE_SMEM16, TRACE_WIDE_REG4, TRACE_WIDE_REG8,
           TRACE_WIDE_OCC8});
     tune("any_traversal", [&](int64_t v) { d->anyMode = static_cast<int>(v); }, {0, 1, 2});
-    tune("shade_budget", [&](int64_t v) { d->shadeBudget = static_cast<int>(v); }, {0, 1});
+    tune("shade_budget", [&](int64_t v) { d->shadeBudget = static_cast<int>(v); }, {0, 1, 2});
     const int64_t grid = static_cast<int64_t>(d->blocksTail) * kTailBlock;
     tune("tail_paths", [&](int64_t v) { d->tailPaths = v; }, {grid / 4, grid / 2, grid, 2 * grid});
     d->guideKind = savedKind;
@@ -2039,7 +2050,7 @@ int32_t pe_device_set_tuning(pe_device* d, const pe_tuning* t) {
         return PE_ERR_INVALID;
     }
     if (t->tail_paths < -1 || t->closest_traversal < 0 || t->closest_traversal >= TRACE_MODES || t->shade_budget < 0 ||
-        t->shade_budget > 1 || t->any_traversal < 0 || t->any_traversal > 2) {
+        t->shade_budget > 2 || t->any_traversal < 0 || t->any_traversal > 2) {
         setError("pe_device_set_tuning: value out of range");
         return PE_ERR_INVALID;
     }

@@ -203,7 +203,7 @@ struct pe_device {
     bool counting = false;
     pe_render_stats stats{};
     int blocksIntersect = 0, blocksShade = 0, blocksShadow = 0, blocksGen = 0, blocksTail = 0;
-    int blocksShadeKey[2][5] = {{0, 0, 0, 0, 0}, {0, 0, 0, 0, 0}}; // lean shading kernels: [budget][key]
+    int blocksShadeKey[3][5] = {}; // lean shading kernels: [budget][key]
     int blocksShadowAny = 0, blocksTailLean = 0;
     int blocksIntersectMode[7] = {0, 0, 0, 0, 0, 0, 0};
     int blocksShadowAnyOcc8 = 0;   // kShadow capped at 64 registers

@@ -30,7 +30,7 @@ def test_tuning_knobs_leave_the_film_unchanged(pe, device):
         for mode in (2, 3, 4, 5, 6):
             f = film(closest_traversal=mode, shade_budget=1, any_traversal=0)
             assert np.array_equal(f.sum, base.sum) and np.array_equal(f.count, base.count), mode
-        for kw in ({"any_traversal": 1}, {"any_traversal": 2}, {"shade_budget": 0}, {"tail_paths": 1024}, {"tail_paths": 0}):
+        for kw in ({"any_traversal": 1}, {"any_traversal": 2}, {"shade_budget": 0}, {"shade_budget": 2}, {"tail_paths": 1024}, {"tail_paths": 0}):
             args = {"closest_traversal": 1, "shade_budget": 1, "any_traversal": 0, **kw}
             f = film(**args)
             assert np.array_equal(f.sum, base.sum), kw

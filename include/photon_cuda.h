@@ -492,7 +492,8 @@ typedef struct pe_tuning {
                                   2 / 3 the 4-wide tree with the first 8 / 16 stack entries of each
                                   thread in shared memory (the rest in local memory), 4 / 5 with the
                                   top 4 / 8 stack entries in registers, 6 (default) the 4-wide tree
-                                  capped at 64 registers (eight 128-thread blocks per SM) */
+                                  capped at 64 registers (eight 128-thread blocks per SM), 7 / 8 that
+                                  with the first 8 / 16 stack entries in shared memory */
     int32_t shade_budget;      /* lean shading kernels: 0 the compiler's register count, 1 (default) at
                                   most 128 registers a thread (four 128-thread blocks per SM), 2 at
                                   most 96 (five blocks) */

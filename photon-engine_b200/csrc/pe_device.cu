@@ -462,6 +462,10 @@ int32_t runWave(pe_device* d, int lane, Paths& P, int nSegs, int nSlots, int nPi
             kIntersect<false, TRACE_WIDE_REG8><<<d->blocksIntersectMode[5], 128, 0, cs>>>(S, P, qIn, cIn, d->dStats);
         else if (d->closestMode == TRACE_WIDE_OCC8)
             kIntersect<false, TRACE_WIDE_OCC8><<<d->blocksIntersectMode[6], 128, 0, cs>>>(S, P, qIn, cIn, d->dStats);
+        else if (d->closestMode == TRACE_WIDE_SMEM8_OCC8)
+            kIntersect<false, TRACE_WIDE_SMEM8_OCC8><<<d->blocksIntersectMode[7], 128, 0, cs>>>(S, P, qIn, cIn, d->dStats);
+        else if (d->closestMode == TRACE_WIDE_SMEM16_OCC8)
+            kIntersect<false, TRACE_WIDE_SMEM16_OCC8><<<d->blocksIntersectMode[8], 128, 0, cs>>>(S, P, qIn, cIn, d->dStats);
         else
             kIntersect<false><<<d->blocksIntersect, 128, 0, cs>>>(S, P, qIn, cIn, d->dStats);
         if (P.guiding == 2 && (rc = guideQueries(d, cs, P, W, qIn, cIn))) return rc;
@@ -1298,6 +1302,8 @@ pe_device* pe_device_create(int32_t ordinal, char* err, size_t errLen) {
     d->blocksIntersectMode[TRACE_WIDE_REG8] = occ(kIntersect<false, TRACE_WIDE_REG8>, 128);
     d->blocksShadowAnyWindow = occ(kShadow<false, true, 4>, 128);
     d->blocksIntersectMode[TRACE_WIDE_OCC8] = occ(kIntersect<false, TRACE_WIDE_OCC8>, 128);
+    d->blocksIntersectMode[TRACE_WIDE_SMEM8_OCC8] = occ(kIntersect<false, TRACE_WIDE_SMEM8_OCC8>, 128);
+    d->blocksIntersectMode[TRACE_WIDE_SMEM16_OCC8] = occ(kIntersect<false, TRACE_WIDE_SMEM16_OCC8>, 128);
     d->blocksShadowAnyOcc8 = occ(kShadow<false, true, 0, 8>, 128);
     const cudaError_t le = cudaGetLastError();
     if (le != cudaSuccess) {
@@ -2013,7 +2019,7 @@ int32_t pe_device_autotune(pe_device* d, const pe_camera* cam, const pe_settings
     };
     tune("closest_traversal", [&](int64_t v) { d->closestMode = static_cast<int>(v); },
          {TRACE_WIDE, TRACE_BINARY, TRACE_WIDE_SMEM8, TRACE_WIDE_SMEM16, TRACE_WIDE_REG4, TRACE_WIDE_REG8,
-          TRACE_WIDE_OCC8});
+          TRACE_WIDE_OCC8, TRACE_WIDE_SMEM8_OCC8, TRACE_WIDE_SMEM16_OCC8});
     tune("any_traversal", [&](int64_t v) { d->anyMode = static_cast<int>(v); }, {0, 1, 2});
     tune("shade_budget", [&](int64_t v) { d->shadeBudget = static_cast<int>(v); }, {0, 1, 2});
     const int64_t grid = static_cast<int64_t>(d->blocksTail) * kTailBlock;

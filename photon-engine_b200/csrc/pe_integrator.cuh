@@ -221,13 +221,15 @@ __global__ void kInitFree(Paths P, int n) {
 // Closest-hit traversal variants the tuner chooses among (pe_tuning::closest_traversal).
 // Closest-hit traversals: the binary tree in the reference's order; the 4-wide tree with its stack
 // in local memory, its first 8 / 16 entries in shared memory, or its top 4 / 8 entries in registers.
-// TRACE_WIDE_OCC8: the 4-wide walk capped at 64 registers, eight 128-thread blocks per SM.
+// TRACE_WIDE_OCC8: the 4-wide walk capped at 64 registers, eight 128-thread blocks per SM; with
+// the first 8 / 16 stack entries in shared memory as well (TRACE_WIDE_SMEM8_OCC8 / _SMEM16_OCC8).
 enum TraceMode { TRACE_BINARY = 0, TRACE_WIDE = 1, TRACE_WIDE_SMEM8 = 2, TRACE_WIDE_SMEM16 = 3, TRACE_WIDE_REG4 = 4,
-                 TRACE_WIDE_REG8 = 5, TRACE_WIDE_OCC8 = 6, TRACE_MODES = 7 };
-constexpr int traceMinBlocks(int mode) { return mode == TRACE_WIDE_OCC8 ? 8 : 1; }
+                 TRACE_WIDE_REG8 = 5, TRACE_WIDE_OCC8 = 6, TRACE_WIDE_SMEM8_OCC8 = 7, TRACE_WIDE_SMEM16_OCC8 = 8,
+                 TRACE_MODES = 9 };
+constexpr int traceMinBlocks(int mode) { return mode >= TRACE_WIDE_OCC8 ? 8 : 1; }
 constexpr int traceStackShared(int mode) {
-    return mode == TRACE_WIDE_SMEM8 ? 8
-         : mode == TRACE_WIDE_SMEM16 ? 16
+    return (mode == TRACE_WIDE_SMEM8 || mode == TRACE_WIDE_SMEM8_OCC8) ? 8
+         : (mode == TRACE_WIDE_SMEM16 || mode == TRACE_WIDE_SMEM16_OCC8) ? 16
          : mode == TRACE_WIDE_REG4 ? -4
          : mode == TRACE_WIDE_REG8 ? -8 : 0;
 }

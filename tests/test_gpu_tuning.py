@@ -27,7 +27,7 @@ def test_tuning_knobs_leave_the_film_unchanged(pe, device):
 
     try:
         base = film(closest_traversal=1, shade_budget=1, any_traversal=0)
-        for mode in (2, 3, 4, 5, 6):
+        for mode in (2, 3, 4, 5, 6, 7, 8):
             f = film(closest_traversal=mode, shade_budget=1, any_traversal=0)
             assert np.array_equal(f.sum, base.sum) and np.array_equal(f.count, base.count), mode
         for kw in ({"any_traversal": 1}, {"any_traversal": 2}, {"shade_budget": 0}, {"shade_budget": 2}, {"tail_paths": 1024}, {"tail_paths": 0}):

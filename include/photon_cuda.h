@@ -493,7 +493,12 @@ typedef struct pe_tuning {
                                   thread in shared memory (the rest in local memory), 4 / 5 with the
                                   top 4 / 8 stack entries in registers, 6 (default) the 4-wide tree
                                   capped at 64 registers (eight 128-thread blocks per SM), 7 / 8 that
-                                  with the first 8 / 16 stack entries in shared memory */
+                                  with the first 8 / 16 stack entries in shared memory, 9 that with
+                                  leaf tests postponed until the warp holds a leaf in every lane.
+                                  Mode 9 only on request (the autotuner leaves it out): which of two
+                                  triangles at a bit-identical distance wins then depends on the
+                                  rays that share the warp, so films are no longer bit-identical
+                                  across batchings and switch points where such ties occur */
     int32_t shade_budget;      /* lean shading kernels: 0 the compiler's register count, 1 (default) at
                                   most 128 registers a thread (four 128-thread blocks per SM), 2 at
                                   most 96 (five blocks) */

@@ -466,6 +466,8 @@ int32_t runWave(pe_device* d, int lane, Paths& P, int nSegs, int nSlots, int nPi
             kIntersect<false, TRACE_WIDE_SMEM8_OCC8><<<d->blocksIntersectMode[7], 128, 0, cs>>>(S, P, qIn, cIn, d->dStats);
         else if (d->closestMode == TRACE_WIDE_SMEM16_OCC8)
             kIntersect<false, TRACE_WIDE_SMEM16_OCC8><<<d->blocksIntersectMode[8], 128, 0, cs>>>(S, P, qIn, cIn, d->dStats);
+        else if (d->closestMode == TRACE_WIDE_SPEC_OCC8)
+            kIntersect<false, TRACE_WIDE_SPEC_OCC8><<<d->blocksIntersectMode[9], 128, 0, cs>>>(S, P, qIn, cIn, d->dStats);
         else
             kIntersect<false><<<d->blocksIntersect, 128, 0, cs>>>(S, P, qIn, cIn, d->dStats);
         if (P.guiding == 2 && (rc = guideQueries(d, cs, P, W, qIn, cIn))) return rc;
@@ -1304,6 +1306,7 @@ pe_device* pe_device_create(int32_t ordinal, char* err, size_t errLen) {
     d->blocksIntersectMode[TRACE_WIDE_OCC8] = occ(kIntersect<false, TRACE_WIDE_OCC8>, 128);
     d->blocksIntersectMode[TRACE_WIDE_SMEM8_OCC8] = occ(kIntersect<false, TRACE_WIDE_SMEM8_OCC8>, 128);
     d->blocksIntersectMode[TRACE_WIDE_SMEM16_OCC8] = occ(kIntersect<false, TRACE_WIDE_SMEM16_OCC8>, 128);
+    d->blocksIntersectMode[TRACE_WIDE_SPEC_OCC8] = occ(kIntersect<false, TRACE_WIDE_SPEC_OCC8>, 128);
     d->blocksShadowAnyOcc8 = occ(kShadow<false, true, 0, 8>, 128);
     const cudaError_t le = cudaGetLastError();
     if (le != cudaSuccess) {

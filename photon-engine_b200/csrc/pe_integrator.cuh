@@ -225,7 +225,9 @@ __global__ void kInitFree(Paths P, int n) {
 // the first 8 / 16 stack entries in shared memory as well (TRACE_WIDE_SMEM8_OCC8 / _SMEM16_OCC8).
 enum TraceMode { TRACE_BINARY = 0, TRACE_WIDE = 1, TRACE_WIDE_SMEM8 = 2, TRACE_WIDE_SMEM16 = 3, TRACE_WIDE_REG4 = 4,
                  TRACE_WIDE_REG8 = 5, TRACE_WIDE_OCC8 = 6, TRACE_WIDE_SMEM8_OCC8 = 7, TRACE_WIDE_SMEM16_OCC8 = 8,
-                 TRACE_MODES = 9 };
+                 TRACE_WIDE_SPEC_OCC8 = 9, TRACE_MODES = 10 };
+// TRACE_WIDE_SPEC_OCC8: the 64-register walk with postponed leaves (walkClosestWideSpec).
+constexpr bool traceSpeculative(int mode) { return mode == TRACE_WIDE_SPEC_OCC8; }
 constexpr int traceMinBlocks(int mode) { return mode >= TRACE_WIDE_OCC8 ? 8 : 1; }
 constexpr int traceStackShared(int mode) {
     return (mode == TRACE_WIDE_SMEM8 || mode == TRACE_WIDE_SMEM8_OCC8) ? 8
@@ -255,7 +257,8 @@ __global__ void __launch_bounds__(128, traceMinBlocks(MODE)) kIntersect(SceneGPU
             const uint32_t vmask = __float_as_uint(ro.w);
             const float time = pathTime(S, P, slot);
             const Hit h = MODE == TRACE_BINARY ? traceClosest<COUNT>(S, o, d, vmask, 0.0f, 1e30f, nodes, tris, time)
-                                               : traceClosestWide<COUNT, SD>(S, o, d, vmask, 0.0f, 1e30f, nodes, tris,
+                                               : traceClosestWide<COUNT, SD, traceSpeculative(MODE)>(
+                                                     S, o, d, vmask, 0.0f, 1e30f, nodes, tris,
                                                                              sstack + threadIdx.x, time);
             P.hit[slot] = make_float4(h.t, h.u, h.v, __int_as_float(h.prim));
             key = (__float_as_uint(ro.w) & RAY_WALK) ? kShadeKeys - 1

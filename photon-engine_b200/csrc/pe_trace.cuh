@@ -690,7 +690,75 @@ __device__ void walkClosestWide(const SceneGPU& S, int cur, V3 o, V3 d, V3 inv, 
     }
 }
 
-template <bool COUNT, int SD = 0>
+// The 4-wide walk with postponed leaves (speculative traversal after Aila and Laine, "Understanding
+// the Efficiency of Ray Traversal on GPUs", 2009): a lane that reaches a leaf keeps it aside and
+// goes on descending until every active lane of its warp holds one, then the warp tests its
+// leaves together, so leaf tests and node steps stop interleaving across the lanes.  Leaves are
+// tested in another order than the depth-first walk's and tMax shrinks later, so a few more nodes
+// are visited; every leaf that can hold a closer hit is still tested, so the distance is the same.
+template <bool COUNT, int SD, int LEVEL>
+__device__ void walkClosestWideSpec(const SceneGPU& S, int cur, V3 o, V3 d, V3 inv, uint32_t mask, float tMin,
+                                    float& tMax, Hit& best, uint32_t& nodeVisits, uint32_t& triTests, uint2* sstack,
+                                    float time) {
+    TraceStack<SD> stack;
+    stack.shared = sstack;
+    auto popNext = [&]() {
+        while (!stack.empty()) {
+            const uint2 e = stack.pop();
+            if (__uint_as_float(e.y) <= tMax) {
+                cur = static_cast<int>(e.x);
+                return true;
+            }
+        }
+        return false;
+    };
+    bool alive = true;       // `cur` holds a reference still to visit
+    bool hasLeaf = false;    // a leaf is kept aside for the next test
+    int leafRef = 0;
+    while (alive || hasLeaf) {
+        while (alive && (cur >= 0 || !hasLeaf)) {
+            if (cur < 0) {
+                // a leaf and none kept aside: keep it, take the next reference
+                leafRef = cur;
+                hasLeaf = true;
+                alive = popNext();
+            } else {
+                if (COUNT) ++nodeVisits;
+                const WideNode n = loadWide(S.wide, cur);
+                float t[4];
+                wideSlabs(n, o, inv, tMin, tMax, t);
+                float t0 = t[0], t1 = t[1], t2 = t[2], t3 = t[3];
+                int r0 = n.child.x, r1 = n.child.y, r2 = n.child.z, r3 = n.child.w;
+                int k0 = 0, k1 = 1, k2 = 2, k3 = 3;
+                cmpx(t0, r0, k0, t1, r1, k1);
+                cmpx(t2, r2, k2, t3, r3, k3);
+                cmpx(t0, r0, k0, t2, r2, k2);
+                cmpx(t1, r1, k1, t3, r3, k3);
+                cmpx(t1, r1, k1, t2, r2, k2);
+                if (t0 == kInf) {
+                    alive = popNext();
+                } else {
+                    if (t3 != kInf) stack.push(make_uint2(static_cast<uint32_t>(r3), __float_as_uint(t3)));
+                    if (t2 != kInf) stack.push(make_uint2(static_cast<uint32_t>(r2), __float_as_uint(t2)));
+                    if (t1 != kInf) stack.push(make_uint2(static_cast<uint32_t>(r1), __float_as_uint(t1)));
+                    cur = r0;
+                }
+            }
+            // every lane still walking holds a leaf: test them together
+            if (!__any_sync(__activemask(), !hasLeaf)) break;
+        }
+        if (hasLeaf) {
+            int first, count;
+            leafRange(leafRef, first, count);
+            testLeafClosest<COUNT, LEVEL, true>(S, first, count, o, d, mask, tMin, tMax, best, nodeVisits, triTests, time);
+            hasLeaf = false;
+            // the reference in hand may have become too far while the leaf was aside; it is an
+            // interior node or a leaf, tested against tMax when it is visited or kept
+        }
+    }
+}
+
+template <bool COUNT, int SD = 0, bool SPEC = false>
 __device__ Hit traceClosestWide(const SceneGPU& S, V3 o, V3 d, uint32_t mask, float tMin, float tMax,
                                 uint32_t& nodeVisits, uint32_t& triTests, uint2* sstack = nullptr, float time = 0.0f) {
     Hit best;
@@ -703,7 +771,11 @@ __device__ Hit traceClosestWide(const SceneGPU& S, V3 o, V3 d, uint32_t mask, fl
     if (S.nTris == 0) return best;
     if (!slab(S.rootMin[0], S.rootMax[0], S.rootMin[1], S.rootMax[1], S.rootMin[2], S.rootMax[2], o, inv, tMin, tMax, tn))
         return best;
-    walkClosestWide<COUNT, SD, 0>(S, rootRef(S), o, d, inv, mask, tMin, tMax, best, nodeVisits, triTests, sstack, time);
+    if (SPEC)
+        walkClosestWideSpec<COUNT, SD, 0>(S, rootRef(S), o, d, inv, mask, tMin, tMax, best, nodeVisits, triTests, sstack,
+                                          time);
+    else
+        walkClosestWide<COUNT, SD, 0>(S, rootRef(S), o, d, inv, mask, tMin, tMax, best, nodeVisits, triTests, sstack, time);
     return best;
 }
 

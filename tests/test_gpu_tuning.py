@@ -1,9 +1,10 @@
 """The device's tuning knobs (pe_tuning) change how fast a film is made, never the film: every
 4-wide closest-hit traversal variant (stack in local memory, first 8 / 16 entries in shared
-memory, top 4 / 8 entries in registers) visits the same nodes in the same order, the any-hit
-variants answer the same, the shading register budgets and tail thresholds run the same code, so
-their films are bit-identical; the binary tree may resolve a bit-identical distance tie to the
-other triangle of a shared edge, so its film is compared at the equal-spp bar.
+memory, top 4 / 8 entries in registers, a 64-register cap) visits the same nodes in the same
+order, the any-hit variants answer the same, the shading register budgets and tail thresholds
+run the same code, so their films are bit-identical; the binary tree may resolve a
+bit-identical distance tie to the other triangle of a shared edge, and so may the walk with
+postponed leaf tests, so their films are compared at the equal-spp bar.
 """
 import importlib
 
@@ -34,6 +35,10 @@ def test_tuning_knobs_leave_the_film_unchanged(pe, device):
             args = {"closest_traversal": 1, "shade_budget": 1, "any_traversal": 0, **kw}
             f = film(**args)
             assert np.array_equal(f.sum, base.sum), kw
+        # postponed leaf tests (mode 9) visit leaves in another order: ties may go the other way
+        spec = film(closest_traversal=9, shade_budget=1, any_traversal=0)
+        assert np.array_equal(spec.count, base.count)
+        assert pe.rel_mse(spec.resolve(), base.resolve()) <= 1e-4
         binary = film(closest_traversal=0, shade_budget=1, any_traversal=0)
         assert np.array_equal(binary.count, base.count)
         assert pe.rel_mse(binary.resolve(), base.resolve()) <= 1e-4

@@ -255,9 +255,16 @@ def run_ours(args):
     scene, cam, st, desc = build_workload(pe)
     dev = pe.CudaDevice(local)
     dev.set_scene(scene)
-    tail = dev.autotune(cam, st, SPP_PER_STEP)  # untimed set-up: picks traversal, register budget, tail
+    if args.tuning:
+        # fixed knobs instead of the autotuner (for profiler runs, whose timings the tuner cannot trust)
+        closest, anyhit, budget, tail = (int(v) for v in args.tuning.split(","))
+        dev.set_tuning(tail_paths=tail, closest_traversal=closest, shade_budget=budget, any_traversal=anyhit)
+        tune_log = "fixed by --tuning"
+    else:
+        dev.autotune(cam, st, SPP_PER_STEP)  # untimed set-up: picks traversal, register budget, tail
+        tune_log = dev.autotune_log()
     tuning = dev.tuning()
-    tune_log = dev.autotune_log()
+    tail = tuning["tail_paths"]
     # disjoint sample indices per replica; step k renders samples base + SPP_PER_STEP·(1 + warmup + k) …
     base = replica_sample_base(rank, args.warmup, args.steps)
 
@@ -396,6 +403,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--tuning", default="",
+                    help="closest,any,budget,tail: fixed device tuning instead of the autotuner (profiler runs)")
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--serve", action="store_true",
                     help="served-mix benchmark (request server vs the plain per-request loop) instead")

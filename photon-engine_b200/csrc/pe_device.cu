@@ -332,6 +332,43 @@ int32_t segsWritable(pe_device* d, int lane) {
     return PE_OK;
 }
 
+static_assert(sizeof(pe_device::blocksIntersectMode) / sizeof(int) == TRACE_MODES, "a grid size per traversal mode");
+
+// The closest-hit kernel of the tuned traversal (pe_tuning::closest_traversal) over a queue.
+void launchClosest(pe_device* d, const SceneGPU& S, const Paths& P, const int32_t* q, const uint32_t* c, cudaStream_t cs) {
+    const int* g = d->blocksIntersectMode;
+    unsigned long long* st = d->dStats;
+    switch (d->closestMode) {
+    case TRACE_BINARY: kIntersect<false, TRACE_BINARY><<<g[TRACE_BINARY], 128, 0, cs>>>(S, P, q, c, st); break;
+    case TRACE_WIDE_SMEM8: kIntersect<false, TRACE_WIDE_SMEM8><<<g[TRACE_WIDE_SMEM8], 128, 0, cs>>>(S, P, q, c, st); break;
+    case TRACE_WIDE_SMEM16: kIntersect<false, TRACE_WIDE_SMEM16><<<g[TRACE_WIDE_SMEM16], 128, 0, cs>>>(S, P, q, c, st); break;
+    case TRACE_WIDE_REG4: kIntersect<false, TRACE_WIDE_REG4><<<g[TRACE_WIDE_REG4], 128, 0, cs>>>(S, P, q, c, st); break;
+    case TRACE_WIDE_REG8: kIntersect<false, TRACE_WIDE_REG8><<<g[TRACE_WIDE_REG8], 128, 0, cs>>>(S, P, q, c, st); break;
+    case TRACE_WIDE_OCC8: kIntersect<false, TRACE_WIDE_OCC8><<<g[TRACE_WIDE_OCC8], 128, 0, cs>>>(S, P, q, c, st); break;
+    case TRACE_WIDE_SMEM8_OCC8:
+        kIntersect<false, TRACE_WIDE_SMEM8_OCC8><<<g[TRACE_WIDE_SMEM8_OCC8], 128, 0, cs>>>(S, P, q, c, st);
+        break;
+    case TRACE_WIDE_SMEM16_OCC8:
+        kIntersect<false, TRACE_WIDE_SMEM16_OCC8><<<g[TRACE_WIDE_SMEM16_OCC8], 128, 0, cs>>>(S, P, q, c, st);
+        break;
+    case TRACE_WIDE_SPEC_OCC8:
+        kIntersect<false, TRACE_WIDE_SPEC_OCC8><<<g[TRACE_WIDE_SPEC_OCC8], 128, 0, cs>>>(S, P, q, c, st);
+        break;
+    default: kIntersect<false><<<d->blocksIntersect, 128, 0, cs>>>(S, P, q, c, st); break;
+    }
+}
+
+// The plain any-hit shadow kernel of the tuned variant (pe_tuning::any_traversal).
+void launchShadowAny(pe_device* d, const SceneGPU& S, const Paths& P, cudaStream_t cs) {
+    uint32_t* n = &P.counters[CNT_SHADOW];
+    unsigned long long* st = d->dStats;
+    switch (d->anyMode) {
+    case 1: kShadow<false, true, 4><<<d->blocksShadowAnyWindow, 128, 0, cs>>>(S, P, n, st); break;
+    case 2: kShadow<false, true, 0, 8><<<d->blocksShadowAnyOcc8, 128, 0, cs>>>(S, P, n, st); break;
+    default: kShadow<false, true><<<d->blocksShadowAny, 128, 0, cs>>>(S, P, n, st); break;
+    }
+}
+
 // One wave on a lane over the nSegs segments in its segment table (nSlots paths, nPix film
 // pixels): uploads the table, generates the camera rays, traces them bounce by bounce (closest
 // hit → shade → any hit) until the live paths fit the tail kernel, which finishes them, and adds
@@ -416,8 +453,10 @@ int32_t runWave(pe_device* d, int lane, Paths& P, int nSegs, int nSlots, int nPi
             }
             const bool out = P.aovA || P.pass;
             if (lean && !d->counting && !out)
-                kTail<false, false, true><<<std::min(grid, d->blocksTailLean), kTailBlock, 0, cs>>>(
-                    S, P, W, qIn, cIn, &P.counters[CNT_WORK_TAIL], d->dStats);
+                kTailLockstep<<<static_cast<int>(std::min<int64_t>(d->blocksTailLockstep,
+                                                                   (static_cast<int64_t>(live) + kTailLockstepBlock - 1) /
+                                                                       kTailLockstepBlock)),
+                                kTailLockstepBlock, 0, cs>>>(S, P, W, qIn, cIn, &P.counters[CNT_WORK_TAIL], d->dStats);
             else if (d->counting && out)
                 kTail<true, true><<<grid, kTailBlock, 0, cs>>>(S, P, W, qIn, cIn, &P.counters[CNT_WORK_TAIL], d->dStats);
             else if (d->counting)
@@ -450,26 +489,8 @@ int32_t runWave(pe_device* d, int lane, Paths& P, int nSegs, int nSlots, int nPi
             kIntersect<true, TRACE_BINARY><<<d->blocksIntersectMode[0], 128, 0, cs>>>(S, P, qIn, cIn, d->dStats);
         else if (d->counting)
             kIntersect<true><<<d->blocksIntersect, 128, 0, cs>>>(S, P, qIn, cIn, d->dStats);
-        else if (d->closestMode == TRACE_BINARY)
-            kIntersect<false, TRACE_BINARY><<<d->blocksIntersectMode[0], 128, 0, cs>>>(S, P, qIn, cIn, d->dStats);
-        else if (d->closestMode == TRACE_WIDE_SMEM8)
-            kIntersect<false, TRACE_WIDE_SMEM8><<<d->blocksIntersectMode[2], 128, 0, cs>>>(S, P, qIn, cIn, d->dStats);
-        else if (d->closestMode == TRACE_WIDE_SMEM16)
-            kIntersect<false, TRACE_WIDE_SMEM16><<<d->blocksIntersectMode[3], 128, 0, cs>>>(S, P, qIn, cIn, d->dStats);
-        else if (d->closestMode == TRACE_WIDE_REG4)
-            kIntersect<false, TRACE_WIDE_REG4><<<d->blocksIntersectMode[4], 128, 0, cs>>>(S, P, qIn, cIn, d->dStats);
-        else if (d->closestMode == TRACE_WIDE_REG8)
-            kIntersect<false, TRACE_WIDE_REG8><<<d->blocksIntersectMode[5], 128, 0, cs>>>(S, P, qIn, cIn, d->dStats);
-        else if (d->closestMode == TRACE_WIDE_OCC8)
-            kIntersect<false, TRACE_WIDE_OCC8><<<d->blocksIntersectMode[6], 128, 0, cs>>>(S, P, qIn, cIn, d->dStats);
-        else if (d->closestMode == TRACE_WIDE_SMEM8_OCC8)
-            kIntersect<false, TRACE_WIDE_SMEM8_OCC8><<<d->blocksIntersectMode[7], 128, 0, cs>>>(S, P, qIn, cIn, d->dStats);
-        else if (d->closestMode == TRACE_WIDE_SMEM16_OCC8)
-            kIntersect<false, TRACE_WIDE_SMEM16_OCC8><<<d->blocksIntersectMode[8], 128, 0, cs>>>(S, P, qIn, cIn, d->dStats);
-        else if (d->closestMode == TRACE_WIDE_SPEC_OCC8)
-            kIntersect<false, TRACE_WIDE_SPEC_OCC8><<<d->blocksIntersectMode[9], 128, 0, cs>>>(S, P, qIn, cIn, d->dStats);
         else
-            kIntersect<false><<<d->blocksIntersect, 128, 0, cs>>>(S, P, qIn, cIn, d->dStats);
+            launchClosest(d, S, P, qIn, cIn, cs);
         if (P.guiding == 2 && (rc = guideQueries(d, cs, P, W, qIn, cIn))) return rc;
         if (tm.timing) PE_CUDA(cudaEventRecord(e1, cs));
         if (lean)
@@ -485,12 +506,8 @@ int32_t runWave(pe_device* d, int lane, Paths& P, int nSegs, int nSlots, int nPi
         if (tm.timing) PE_CUDA(cudaEventRecord(e2, cs));
         if (d->counting)
             kShadow<true><<<d->blocksShadow, 128, 0, cs>>>(S, P, &P.counters[CNT_SHADOW], d->dStats);
-        else if (anyHitShadows && d->anyMode == 1)
-            kShadow<false, true, 4><<<d->blocksShadowAnyWindow, 128, 0, cs>>>(S, P, &P.counters[CNT_SHADOW], d->dStats);
-        else if (anyHitShadows && d->anyMode == 2)
-            kShadow<false, true, 0, 8><<<d->blocksShadowAnyOcc8, 128, 0, cs>>>(S, P, &P.counters[CNT_SHADOW], d->dStats);
         else if (anyHitShadows)
-            kShadow<false, true><<<d->blocksShadowAny, 128, 0, cs>>>(S, P, &P.counters[CNT_SHADOW], d->dStats);
+            launchShadowAny(d, S, P, cs);
         else
             kShadow<false><<<d->blocksShadow, 128, 0, cs>>>(S, P, &P.counters[CNT_SHADOW], d->dStats);
         stats.kernel_launches += lean ? 2 : 3;
@@ -613,12 +630,13 @@ int32_t loopBounce(pe_device* d, LaneLoop& L, const Wave& W, uint32_t* hSegLeft,
     P.sweepAge = sweep >= 0 ? L.sweepAge : 0;
     P.sweepQ = sweep >= 0 ? L.sweepBuf[sweep] : nullptr;
     P.iter = L.iter;
-    kIntersect<false><<<d->blocksIntersect, 128, 0, cs>>>(S, P, L.qIn, L.cIn, d->dStats);
+    // the tuned closest-hit and any-hit kernels, as a lone render uses
+    launchClosest(d, S, P, L.qIn, L.cIn, cs);
     // lean-shading scenes shade with the per-key kernels, as a lone render does
     if (L.lean) launchLeanShade(d, S, P, W, L.qOut, L.cOut, cs, false);
     else kShade<false><<<d->blocksShade, 128, 0, cs>>>(S, P, W, L.qOut, L.cOut);
     if (!S.hasShadowTransmitters && !S.hasShadowLinks)
-        kShadow<false, true><<<d->blocksShadowAny, 128, 0, cs>>>(S, P, &P.counters[CNT_SHADOW], d->dStats);
+        launchShadowAny(d, S, P, cs);
     else
         kShadow<false><<<d->blocksShadow, 128, 0, cs>>>(S, P, &P.counters[CNT_SHADOW], d->dStats);
     PE_CUDA(cudaMemcpyAsync(ln.hCounters, P.counters, CNT_TOTAL * sizeof(uint32_t), cudaMemcpyDeviceToHost, cs));
@@ -1274,6 +1292,8 @@ pe_device* pe_device_create(int32_t ordinal, char* err, size_t errLen) {
     d->blocksTail = sm * std::max(1, b);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kTail<false, false, true>, kTailBlock, 0);
     d->blocksTailLean = sm * std::max(1, b);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kTailLockstep, kTailLockstepBlock, 0);
+    d->blocksTailLockstep = sm * std::max(1, b);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kShadow<false, true>, 128, 0);
     d->blocksShadowAny = sm * std::max(1, b);
     auto occ = [&](auto kernel, int threads) {

@@ -205,7 +205,8 @@ struct pe_device {
     int blocksIntersect = 0, blocksShade = 0, blocksShadow = 0, blocksGen = 0, blocksTail = 0;
     int blocksShadeKey[3][5] = {}; // lean shading kernels: [budget][key]
     int blocksShadowAny = 0, blocksTailLean = 0;
-    int blocksIntersectMode[10] = {};
+    int blocksTailLockstep = 0; // kTailLockstep: the lean tail of lone renders, 128-thread blocks
+    int blocksIntersectMode[10] = {}; // per TraceMode
     int blocksShadowAnyOcc8 = 0;   // kShadow capped at 64 registers
     int blocksShadowAnyWindow = 0; // kShadow with the any-hit stack's top entries in registers
     int anyMode = 2;               // pe_tuning::any_traversal (default: the 64-register cap)

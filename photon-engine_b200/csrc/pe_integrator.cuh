@@ -1357,6 +1357,59 @@ __global__ void __launch_bounds__(kTailBlock) kTail(SceneGPU S, Paths P, Wave W,
     atomicAdd(&stats[6], static_cast<unsigned long long>(shRays));
 }
 
+// The lean tail of a lone render in lockstep: the same per-path work as kTail<…, LEAN>, but the
+// four warps of a 128-thread block meet at a barrier between each bounce's closest-hit query and
+// its shading, so the warps sharing an SM run the same phase's code at once.  The loop body
+// (traversal, every lean material's shading, the inline shadow ray) is far larger than an SM
+// sub-partition's instruction cache; warps of 32-thread blocks, each at its own point of the
+// loop, spend most of their stalls fetching instructions.  Threads whose paths have ended take
+// the queue's next path at the top of the loop; the block leaves when none of its threads holds
+// one.  Each path's queries and terms are kTail's, so the film is the same bit for bit.
+constexpr int kTailLockstepBlock = 128;
+__global__ void __launch_bounds__(kTailLockstepBlock) kTailLockstep(SceneGPU S, Paths P, Wave W, const int32_t* queue,
+                                                                  const uint32_t* count, uint32_t* cursor,
+                                                                  unsigned long long* stats) {
+    const int n = static_cast<int>(*count);
+    uint32_t nodes = 0, tris = 0, shNodes = 0, shTris = 0, rays = 0, shRays = 0;
+    int slot = -1, path = 0, q = 0;
+    const WaveSeg* A = nullptr;
+    bool exhausted = false; // this thread found the queue taken
+    for (;;) {
+        if (slot < 0 && !exhausted) {
+            const int i = static_cast<int>(atomicAdd(cursor, 1u));
+            if (i < n) {
+                slot = queue[i];
+                path = pathOfSlot(P, slot);
+                A = &W.segs[segOfSlot(W, path)];
+                q = 0;
+            } else {
+                exhausted = true;
+            }
+        }
+        if (!__syncthreads_or(slot >= 0)) break;
+        if (slot >= 0) {
+            const float4 ro = P.rayO[slot];
+            const float4 rd = P.rayD[slot];
+            const Hit h = traceClosestWide<false>(S, mk(ro.x, ro.y, ro.z), mk(rd.x, rd.y, rd.z), __float_as_uint(ro.w), 0.0f,
+                                              1e30f, nodes, tris, nullptr, pathTime(S, P, slot));
+            ++rays;
+            P.hit[slot] = make_float4(h.t, h.u, h.v, __int_as_float(h.prim));
+        }
+        __syncthreads();
+        if (slot >= 0) {
+            if (!shadeSlot<true, false, false, -2>(S, P, *A, slot, path, shNodes, shTris, shRays)) {
+                slot = -1;
+            } else if (++q >= kMaxPathQueries) {
+                // as kTail: a path past the per-path query bound is ended and reported
+                atomicAdd(&stats[7], 1ull);
+                slot = -1;
+            }
+        }
+    }
+    atomicAdd(&stats[5], static_cast<unsigned long long>(rays));
+    atomicAdd(&stats[6], static_cast<unsigned long long>(shRays));
+}
+
 // ---- film: Film::addSample in sample order per pixel (src/core/image/film.cpp:56-69) ----------
 // The AOV films of one pixel (addAovs, renderer.cpp:219-224): albedo and alpha by addSample,
 // the normal by addSampleSigned (film.cpp:73-85), in sample order.

@@ -43,7 +43,8 @@ sys.path.insert(0, str(ROOT))
 WIDTH, HEIGHT, DEPTH = 1920, 1080, 12
 SPP_PER_STEP = 4  # one step = 4 samples per pixel of the 1080p frame (one wave of 8.3M paths)
 NODE_BYTES, TRI_BYTES, RAY_BYTES, HIT_BYTES, QUEUE_BYTES = 128, 48, 32, 16, 4  # 4-wide BVH node: 128 B
-L2_NOTE = "inputs larger than L2: 140 MB resident scene + 300 MB path state per 2M-path wave (L2 126 MB)"
+L2_NOTE = ("inputs larger than L2: 140 MB resident scene + 0.6-1.2 GB of path state for the 4-8M paths in flight "
+           "(L2 126 MB)")
 
 
 def measured_peaks():
@@ -257,8 +258,11 @@ def run_ours(args):
     dev.set_scene(scene)
     if args.tuning:
         # fixed knobs instead of the autotuner (for profiler runs, whose timings the tuner cannot trust)
-        closest, anyhit, budget, tail = (int(v) for v in args.tuning.split(","))
-        dev.set_tuning(tail_paths=tail, closest_traversal=closest, shade_budget=budget, any_traversal=anyhit)
+        knobs = [int(v) for v in args.tuning.split(",")]
+        closest, anyhit, budget, tail = knobs[:4]
+        slots = knobs[4] if len(knobs) > 4 else 1 << 22
+        dev.set_tuning(tail_paths=tail, closest_traversal=closest, shade_budget=budget, any_traversal=anyhit,
+                       wave_slots=slots)
         tune_log = "fixed by --tuning"
     else:
         dev.autotune(cam, st, SPP_PER_STEP)  # untimed set-up: picks traversal, register budget, tail
@@ -404,7 +408,8 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--tuning", default="",
-                    help="closest,any,budget,tail: fixed device tuning instead of the autotuner (profiler runs)")
+                    help="closest,any,budget,tail[,wave_slots]: fixed device tuning instead of the autotuner "
+                         "(profiler runs)")
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--serve", action="store_true",
                     help="served-mix benchmark (request server vs the plain per-request loop) instead")

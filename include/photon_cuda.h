@@ -38,7 +38,7 @@
 extern "C" {
 #endif
 
-#define PE_ABI_VERSION 9
+#define PE_ABI_VERSION 10
 
 typedef enum pe_status {
     PE_OK = 0,
@@ -484,8 +484,9 @@ int64_t pe_device_tail_paths(pe_device* d);
 int32_t pe_device_autotune(pe_device* d, const pe_camera* cam, const pe_settings* st, int32_t probe_spp, int64_t* chosen);
 
 /* B200 tuning knobs with no counterpart in the reference engine; none changes a film.  The
- * autotuner above sets all four by coordinate descent on probe renders of the caller's frame
- * (closest-hit traversal, any-hit traversal, the shading register budget, the tail threshold). */
+ * autotuner above sets all five by coordinate descent on probe renders of the caller's frame
+ * (paths in flight per wave, closest-hit traversal, any-hit traversal, the shading register
+ * budget, the tail threshold). */
 typedef struct pe_tuning {
     int64_t tail_paths;        /* as pe_device_set_tail_paths */
     int32_t closest_traversal; /* bounce-by-bounce closest hits: 0 the binary tree, 1 the 4-wide tree,
@@ -504,6 +505,12 @@ typedef struct pe_tuning {
                                   most 96 (five blocks) */
     int32_t any_traversal;     /* plain any-hit shadows: 0 the stack in local memory, 1 its top 4
                                   entries in registers, 2 (default) capped at 64 registers */
+    int64_t wave_slots;        /* paths in flight in a regenerating wave (unguided renders without
+                                  AOV or pass targets): 2^20 … 2^23, default 2^22; 0 on input keeps
+                                  the current value.  Each of the device's two lanes holds path
+                                  state for that many paths (about 1.3 KB a slot with the radiance
+                                  of the paths the slots cycle through), allocated at the next
+                                  render and never shrunk */
 } pe_tuning;
 int32_t pe_device_get_tuning(pe_device* d, pe_tuning* out);
 int32_t pe_device_set_tuning(pe_device* d, const pe_tuning* t);

@@ -69,7 +69,7 @@ class pe_scene_info(C.Structure):
 
 class pe_tuning(C.Structure):
     _fields_ = [("tail_paths", C.c_int64), ("closest_traversal", C.c_int32), ("shade_budget", C.c_int32),
-                ("any_traversal", C.c_int32)]
+                ("any_traversal", C.c_int32), ("wave_slots", C.c_int64)]
 
 
 class pe_device_info(C.Structure):

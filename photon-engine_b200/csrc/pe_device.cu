@@ -43,14 +43,21 @@ int32_t allocLane(WaveLane& ln, size_t slots) {
     return PE_OK;
 }
 
+// Per-slot buffers of `slots` paths (d->capacity: guided, AOV and pass waves size their own
+// buffers by it); each lane's path state holds max(slots, d->waveSlots) slots, the regenerating
+// waves' paths in flight.  Grows only.
 int32_t ensureCapacity(pe_device* d, size_t slots) {
-    if (slots <= d->capacity) return PE_OK;
+    const size_t cap = std::max(slots, d->capacity);
+    const size_t lane = std::max(cap, d->waveSlots);
+    if (cap == d->capacity && lane <= d->laneSlots) return PE_OK;
     d->capacity = 0;
+    d->laneSlots = 0;
     for (WaveLane& ln : d->lanes) {
-        const int32_t st = allocLane(ln, slots);
+        const int32_t st = allocLane(ln, lane);
         if (st) return st;
     }
-    d->capacity = slots;
+    d->capacity = cap;
+    d->laneSlots = lane;
     return PE_OK;
 }
 
@@ -395,10 +402,14 @@ int32_t runWave(pe_device* d, int lane, Paths& P, int nSegs, int nSlots, int nPi
     // SD-tree guiding: the field as it stands, recording and sampling as the schedule says
     P.sdMode = (d->guideKind == 2 && P.sdRec) ? d->sd.waveMode : 0;
     P.sd = d->sd.field;
-    // path regeneration: a wave of more paths than slots (unguided waves on a lane's own state)
-    const int64_t slotCap = static_cast<int64_t>(P.capacity);
-    const bool regen = &P == &ln.paths && ln.Lout && !P.guiding && !P.sdMode && !d->aovTarget && !d->passTarget &&
-                       nSlots > slotCap;
+    // path regeneration: a wave of more paths than slots (unguided waves on a lane's own state,
+    // wave_slots of them in flight); other waves on a lane's state use d->capacity slots, which
+    // the guide, AOV and pass buffers are sized by
+    const bool lanePaths = &P == &ln.paths;
+    const bool regenOk = lanePaths && ln.Lout && !P.guiding && !P.sdMode && !d->aovTarget && !d->passTarget;
+    const int64_t slotCap = static_cast<int64_t>(
+        std::min<size_t>(P.capacity, regenOk ? d->waveSlots : (lanePaths ? d->capacity : P.capacity)));
+    const bool regen = regenOk && nSlots > slotCap;
     P.pathOf = regen ? ln.pathOf : nullptr;
     P.freeQ = regen ? ln.freeQ : nullptr;
     P.Lout = regen ? ln.Lout : nullptr;
@@ -745,7 +756,9 @@ int32_t renderWaves(pe_device* d, const pe_camera* cam, const pe_settings* st, i
     if (npix == 0) return PE_OK;
     // unguided waves on the lanes' own state regenerate paths: kStreamFactor × the slots per wave
     const bool regenWaves = !scratch && !d->guide.mode && d->guideKind != 2 && !d->aovTarget && !d->passTarget;
-    const size_t pathCap = regenWaves ? capacity * kStreamFactor : capacity;
+    // regenerating waves keep pe_tuning::wave_slots paths in flight (the lanes hold that many)
+    const size_t waveCap = regenWaves ? std::min(d->waveSlots, d->laneSlots) : capacity;
+    const size_t pathCap = regenWaves ? waveCap * kStreamFactor : waveCap;
     const int pixChunk = static_cast<int>(std::min(npix, pathCap));
     const int samplesPerWave = static_cast<int>(std::max<size_t>(1, std::min<size_t>(static_cast<size_t>(count), pathCap / pixChunk)));
     WaveSeg base = makeSeg(cam, st);
@@ -2010,6 +2023,7 @@ int32_t pe_device_autotune(pe_device* d, const pe_camera* cam, const pe_settings
     d->guide.mode = 0;
     const int64_t savedTail = d->tailPaths;
     const int savedClosest = d->closestMode, savedBudget = d->shadeBudget, savedAny = d->anyMode;
+    const size_t savedWave = d->waveSlots;
     std::string log;
     auto probe = [&](float& ms) -> int32_t {
         ms = 1e30f;
@@ -2040,6 +2054,13 @@ int32_t pe_device_autotune(pe_device* d, const pe_camera* cam, const pe_settings
         }
         set(pick);
     };
+    // paths in flight first: every later probe runs at the chosen wave size (lanes grow as needed)
+    tune("wave_slots",
+         [&](int64_t v) {
+             d->waveSlots = static_cast<size_t>(v);
+             if (!rc) rc = ensureCapacity(d, kWaveSlots);
+         },
+         {static_cast<int64_t>(kWaveSlots), static_cast<int64_t>(kDefaultWaveSlots), static_cast<int64_t>(kMaxWaveSlots)});
     tune("closest_traversal", [&](int64_t v) { d->closestMode = static_cast<int>(v); },
          {TRACE_WIDE, TRACE_BINARY, TRACE_WIDE_SMEM8, TRACE_WIDE_SMEM16, TRACE_WIDE_REG4, TRACE_WIDE_REG8,
           TRACE_WIDE_OCC8, TRACE_WIDE_SMEM8_OCC8, TRACE_WIDE_SMEM16_OCC8});
@@ -2055,6 +2076,7 @@ int32_t pe_device_autotune(pe_device* d, const pe_camera* cam, const pe_settings
         d->closestMode = savedClosest;
         d->shadeBudget = savedBudget;
         d->anyMode = savedAny;
+        d->waveSlots = savedWave;
     }
     d->tuneLog = log;
     if (chosen) *chosen = d->tailPaths;
@@ -2070,6 +2092,7 @@ int32_t pe_device_get_tuning(pe_device* d, pe_tuning* out) {
     out->closest_traversal = d->closestMode;
     out->shade_budget = d->shadeBudget;
     out->any_traversal = d->anyMode;
+    out->wave_slots = static_cast<int64_t>(d->waveSlots);
     return PE_OK;
 }
 
@@ -2079,7 +2102,9 @@ int32_t pe_device_set_tuning(pe_device* d, const pe_tuning* t) {
         return PE_ERR_INVALID;
     }
     if (t->tail_paths < -1 || t->closest_traversal < 0 || t->closest_traversal >= TRACE_MODES || t->shade_budget < 0 ||
-        t->shade_budget > 2 || t->any_traversal < 0 || t->any_traversal > 2) {
+        t->shade_budget > 2 || t->any_traversal < 0 || t->any_traversal > 2 ||
+        (t->wave_slots != 0 && (t->wave_slots < static_cast<int64_t>(kMinWaveSlots) ||
+                                t->wave_slots > static_cast<int64_t>(kMaxWaveSlots)))) {
         setError("pe_device_set_tuning: value out of range");
         return PE_ERR_INVALID;
     }
@@ -2087,6 +2112,7 @@ int32_t pe_device_set_tuning(pe_device* d, const pe_tuning* t) {
     d->closestMode = t->closest_traversal;
     d->shadeBudget = t->shade_budget;
     d->anyMode = t->any_traversal;
+    if (t->wave_slots != 0) d->waveSlots = static_cast<size_t>(t->wave_slots);
     return PE_OK;
 }
 

@@ -36,7 +36,11 @@ struct DevBuf {
 
 constexpr int kFilterSlots = 16;
 constexpr int kMaxSegs = 64;                    // requests sharing one wave
-constexpr size_t kWaveSlots = size_t(1) << 21;  // paths in flight per wave
+constexpr size_t kWaveSlots = size_t(1) << 21;  // paths in flight per wave (guided, AOV and pass waves; servers)
+// Paths in flight per regenerating wave (pe_tuning::wave_slots): the default, and the range
+constexpr size_t kDefaultWaveSlots = size_t(1) << 22;
+constexpr size_t kMinWaveSlots = size_t(1) << 20;
+constexpr size_t kMaxWaveSlots = size_t(1) << 23;
 // Live paths at or below which a guided wave hands its last paths to the tail kernel.
 constexpr int64_t kGuideTailPaths = 2048;
 // Bound on the bounce-by-bounce iterations of one wave (closest-hit queries of its longest path).
@@ -207,6 +211,8 @@ struct pe_device {
     int blocksShadowAny = 0, blocksTailLean = 0;
     int blocksTailLockstep = 0; // kTailLockstep: the lean tail of lone renders, 128-thread blocks
     int blocksIntersectMode[10] = {}; // per TraceMode
+    size_t waveSlots = pe_dev::kDefaultWaveSlots; // pe_tuning::wave_slots: paths in flight per regenerating wave
+    size_t laneSlots = 0;                 // slots of path state allocated per lane (>= capacity, waveSlots)
     int blocksShadowAnyOcc8 = 0;   // kShadow capped at 64 registers
     int blocksShadowAnyWindow = 0; // kShadow with the any-hit stack's top entries in registers
     int anyMode = 2;               // pe_tuning::any_traversal (default: the 64-register cap)

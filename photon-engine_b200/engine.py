@@ -1116,15 +1116,19 @@ class CudaDevice:
         return int(chosen.value)
 
     def tuning(self) -> dict:
-        """The device's tuning knobs (pe_tuning): tail_paths, closest_traversal, shade_budget, any_traversal."""
+        """The device's tuning knobs (pe_tuning): tail_paths, closest_traversal, shade_budget, any_traversal,
+        wave_slots."""
         t = capi.pe_tuning()
         capi.check(_lib().pe_device_get_tuning(self._h, C.byref(t)))
         return {"tail_paths": int(t.tail_paths), "closest_traversal": int(t.closest_traversal),
-                "shade_budget": int(t.shade_budget), "any_traversal": int(t.any_traversal)}
+                "shade_budget": int(t.shade_budget), "any_traversal": int(t.any_traversal),
+                "wave_slots": int(t.wave_slots)}
 
-    def set_tuning(self, tail_paths: int = -1, closest_traversal: int = 6, shade_budget: int = 1, any_traversal: int = 2):
+    def set_tuning(self, tail_paths: int = -1, closest_traversal: int = 6, shade_budget: int = 1, any_traversal: int = 2,
+                   wave_slots: int = 1 << 22):
         capi.check(_lib().pe_device_set_tuning(self._h, C.byref(capi.pe_tuning(tail_paths, closest_traversal,
-                                                                                shade_budget, any_traversal))))
+                                                                                shade_budget, any_traversal,
+                                                                                wave_slots))))
 
     def autotune_log(self) -> str:
         """The last autotune's probe times ("knob=value time ms" per line)."""

@@ -44,3 +44,28 @@ def test_tuning_knobs_leave_the_film_unchanged(pe, device):
         assert pe.rel_mse(binary.resolve(), base.resolve()) <= 1e-4
     finally:
         device.set_tuning()
+
+
+def test_wave_slots_leave_the_film_unchanged(pe, device):
+    """Paths in flight per wave (pe_tuning::wave_slots): 3.7M paths through 1M slots regenerate
+    paths in freed slots, through 4M slots they all start at once; the film is the same."""
+    S = importlib.import_module("photon_engine_b200.scenes")
+    scene, cam, st = S.torus_knot_scene(640, 360, 16, 8, nu=256, nv=16, env_size=(128, 64))
+    scene.build_accelerator()
+    device.set_scene(scene)
+
+    def film(slots):
+        device.set_tuning(wave_slots=slots)
+        assert device.tuning()["wave_slots"] == slots
+        f = pe.Film(st.width, st.height)
+        device.render(cam, st, pe.RenderTargets(beauty=f), 0, 16)
+        return f
+
+    try:
+        small, large = film(1 << 20), film(1 << 22)
+        assert np.array_equal(small.count, large.count)
+        assert np.array_equal(small.sum, large.sum) and np.array_equal(small.sum_sq, large.sum_sq)
+        with pytest.raises(Exception):
+            device.set_tuning(wave_slots=1 << 24)
+    finally:
+        device.set_tuning()

@@ -1770,13 +1770,39 @@ static int32_t renderHostFilm(pe_device* d, const pe_camera* cam, const pe_setti
     float* s = reinterpret_cast<float*>(d->stage);
     uint32_t* c = reinterpret_cast<uint32_t*>(s + 3 * n);
     float* q = s + 4 * n;
-    if ((rc = pe_device_film_read(d, s, c, q))) return rc;
     const unsigned hw = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
     const size_t rows = static_cast<size_t>(tile.h), W = static_cast<size_t>(st->width);
     const size_t chunk = (rows + hw - 1) / hw;
+    // the tile's rows come back in hw pieces, one copy each on the device stream; each piece is
+    // merged by its own thread as soon as its copy has landed, while the later pieces copy
+    std::vector<cudaEvent_t> landed(hw, nullptr);
+    struct EventsGuard {
+        std::vector<cudaEvent_t>& ev;
+        ~EventsGuard() {
+            for (cudaEvent_t e : ev)
+                if (e) cudaEventDestroy(e);
+        }
+    } eventsGuard{landed};
+    for (unsigned t = 0; t < hw; ++t) {
+        const size_t r0 = std::min(rows, t * chunk), r1 = std::min(rows, (t + 1) * chunk);
+        const size_t b = (static_cast<size_t>(tile.y0) + r0) * W, e = (static_cast<size_t>(tile.y0) + r1) * W;
+        if (e > b) {
+            PE_CUDA(cudaMemcpyAsync(s + 3 * b, d->fSum + 3 * b, 3 * (e - b) * sizeof(float), cudaMemcpyDeviceToHost,
+                                    d->stream));
+            PE_CUDA(cudaMemcpyAsync(c + b, d->fCnt + b, (e - b) * sizeof(uint32_t), cudaMemcpyDeviceToHost, d->stream));
+            PE_CUDA(cudaMemcpyAsync(q + b, d->fSq + b, (e - b) * sizeof(float), cudaMemcpyDeviceToHost, d->stream));
+        }
+        PE_CUDA(cudaEventCreateWithFlags(&landed[t], cudaEventDisableTiming));
+        PE_CUDA(cudaEventRecord(landed[t], d->stream));
+    }
     std::vector<uint64_t> partial(hw, 0);
+    std::vector<int> copyFailed(hw, 0);
     auto merge = [&](unsigned t) {
         uint64_t tr = 0;
+        if (cudaEventSynchronize(landed[t]) != cudaSuccess) {
+            copyFailed[t] = 1;
+            return;
+        }
         for (size_t r = t * chunk; r < std::min(rows, (t + 1) * chunk); ++r) {
             const size_t b = (static_cast<size_t>(tile.y0) + r) * W + static_cast<size_t>(tile.x0);
             const size_t e = b + static_cast<size_t>(tile.w);
@@ -1794,6 +1820,11 @@ static int32_t renderHostFilm(pe_device* d, const pe_camera* cam, const pe_setti
     for (unsigned t = 1; t < hw; ++t) pool.emplace_back(merge, t);
     merge(0);
     for (auto& th : pool) th.join();
+    for (int f : copyFailed)
+        if (f) {
+            setError(std::string("film read-back failed: ") + cudaMsg(cudaGetLastError()));
+            return PE_ERR_CUDA;
+        }
     uint64_t tr = 0;
     for (uint64_t p : partial) tr += p;
     if (traced) *traced = tr;

@@ -341,6 +341,15 @@ int32_t segsWritable(pe_device* d, int lane) {
 
 static_assert(sizeof(pe_device::blocksIntersectMode) / sizeof(int) == TRACE_MODES, "a grid size per traversal mode");
 
+// The tail in lockstep over `n` queued paths (count and cursor on the device).
+void launchTailLockstep(pe_device* d, bool lean, const SceneGPU& S, const Paths& P, const Wave& W, const int32_t* queue,
+                        const uint32_t* count, uint32_t* cursor, int64_t n, cudaStream_t cs) {
+    const int grid = static_cast<int>(std::max<int64_t>(
+        1, std::min<int64_t>(d->blocksTailLockstep[lean ? 1 : 0], (n + kTailLockstepBlock - 1) / kTailLockstepBlock)));
+    if (lean) kTailLockstep<true><<<grid, kTailLockstepBlock, 0, cs>>>(S, P, W, queue, count, cursor, d->dStats);
+    else kTailLockstep<false><<<grid, kTailLockstepBlock, 0, cs>>>(S, P, W, queue, count, cursor, d->dStats);
+}
+
 // The closest-hit kernel of the tuned traversal (pe_tuning::closest_traversal) over a queue.
 void launchClosest(pe_device* d, const SceneGPU& S, const Paths& P, const int32_t* q, const uint32_t* c, cudaStream_t cs) {
     const int* g = d->blocksIntersectMode;
@@ -464,10 +473,7 @@ int32_t runWave(pe_device* d, int lane, Paths& P, int nSegs, int nSlots, int nPi
             }
             const bool out = P.aovA || P.pass;
             if (lean && !d->counting && !out)
-                kTailLockstep<<<static_cast<int>(std::min<int64_t>(d->blocksTailLockstep,
-                                                                   (static_cast<int64_t>(live) + kTailLockstepBlock - 1) /
-                                                                       kTailLockstepBlock)),
-                                kTailLockstepBlock, 0, cs>>>(S, P, W, qIn, cIn, &P.counters[CNT_WORK_TAIL], d->dStats);
+                launchTailLockstep(d, true, S, P, W, qIn, cIn, &P.counters[CNT_WORK_TAIL], live, cs);
             else if (d->counting && out)
                 kTail<true, true><<<grid, kTailBlock, 0, cs>>>(S, P, W, qIn, cIn, &P.counters[CNT_WORK_TAIL], d->dStats);
             else if (d->counting)
@@ -475,7 +481,7 @@ int32_t runWave(pe_device* d, int lane, Paths& P, int nSegs, int nSlots, int nPi
             else if (out)
                 kTail<false, true><<<grid, kTailBlock, 0, cs>>>(S, P, W, qIn, cIn, &P.counters[CNT_WORK_TAIL], d->dStats);
             else
-                kTail<false, false><<<grid, kTailBlock, 0, cs>>>(S, P, W, qIn, cIn, &P.counters[CNT_WORK_TAIL], d->dStats);
+                launchTailLockstep(d, false, S, P, W, qIn, cIn, &P.counters[CNT_WORK_TAIL], live, cs);
             if (tm.timing) {
                 PE_CUDA(cudaEventRecord(t1, cs));
                 tm.tail.push_back({tm.evUsed - 2, tm.evUsed - 1});
@@ -671,14 +677,8 @@ int32_t loopBounce(pe_device* d, LaneLoop& L, const Wave& W, uint32_t* hSegLeft,
         PE_CUDA(cudaEventRecord(L.evReady[sweep], cs));
         PE_CUDA(cudaStreamWaitEvent(L.side, L.evReady[sweep], 0));
         PE_CUDA(cudaMemsetAsync(&L.sweepCursor[sweep], 0, sizeof(uint32_t), L.side));
-        const int grid = static_cast<int>(std::min<int64_t>(L.lean ? d->blocksTailLean : d->blocksTail,
-                                                            (swept + kTailBlock - 1) / kTailBlock));
-        if (L.lean)
-            kTail<false, false, true><<<grid, kTailBlock, 0, L.side>>>(S, P, W, L.sweepBuf[sweep], &L.sweepCnt[sweep],
-                                                                     &L.sweepCursor[sweep], d->dStats);
-        else
-            kTail<false, false><<<grid, kTailBlock, 0, L.side>>>(S, P, W, L.sweepBuf[sweep], &L.sweepCnt[sweep],
-                                                           &L.sweepCursor[sweep], d->dStats);
+        launchTailLockstep(d, L.lean, S, P, W, L.sweepBuf[sweep], &L.sweepCnt[sweep], &L.sweepCursor[sweep],
+                           static_cast<int64_t>(swept), L.side);
         kFlush<<<d->prop.multiProcessorCount * 4, 256, 0, L.side>>>(P, W, L.sweepBuf[sweep], &L.sweepCnt[sweep]);
         PE_CUDA(cudaEventRecord(L.evDone[sweep], L.side));
         L.sweepN[sweep] = swept;
@@ -702,13 +702,7 @@ int32_t loopTail(pe_device* d, LaneLoop& L, const Wave& W) {
     WaveLane& ln = *L.ln;
     Paths& P = ln.paths;
     const cudaStream_t cs = ln.stream;
-    const int grid = static_cast<int>(std::min<int64_t>(L.lean ? d->blocksTailLean : d->blocksTail,
-                                                        (static_cast<int64_t>(L.live) + kTailBlock - 1) / kTailBlock));
-    if (L.lean)
-        kTail<false, false, true><<<grid, kTailBlock, 0, cs>>>(L.scene, P, W, L.qIn, L.cIn, &P.counters[CNT_WORK_TAIL],
-                                                              d->dStats);
-    else
-        kTail<false, false><<<grid, kTailBlock, 0, cs>>>(L.scene, P, W, L.qIn, L.cIn, &P.counters[CNT_WORK_TAIL], d->dStats);
+    launchTailLockstep(d, L.lean, L.scene, P, W, L.qIn, L.cIn, &P.counters[CNT_WORK_TAIL], static_cast<int64_t>(L.live), cs);
     kFlush<<<d->prop.multiProcessorCount * 4, 256, 0, cs>>>(P, W, L.qIn, L.cIn);
     L.live = 0;
     PE_CUDA(cudaGetLastError());
@@ -1303,10 +1297,10 @@ pe_device* pe_device_create(int32_t ordinal, char* err, size_t errLen) {
     d->blocksShadow = sm * std::max(1, b);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kTail<true, false>, kTailBlock, 0);
     d->blocksTail = sm * std::max(1, b);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kTail<false, false, true>, kTailBlock, 0);
-    d->blocksTailLean = sm * std::max(1, b);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kTailLockstep, kTailLockstepBlock, 0);
-    d->blocksTailLockstep = sm * std::max(1, b);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kTailLockstep<false>, kTailLockstepBlock, 0);
+    d->blocksTailLockstep[0] = sm * std::max(1, b);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kTailLockstep<true>, kTailLockstepBlock, 0);
+    d->blocksTailLockstep[1] = sm * std::max(1, b);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kShadow<false, true>, 128, 0);
     d->blocksShadowAny = sm * std::max(1, b);
     auto occ = [&](auto kernel, int threads) {

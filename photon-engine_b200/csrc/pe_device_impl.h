@@ -208,8 +208,8 @@ struct pe_device {
     pe_render_stats stats{};
     int blocksIntersect = 0, blocksShade = 0, blocksShadow = 0, blocksGen = 0, blocksTail = 0;
     int blocksShadeKey[3][5] = {}; // lean shading kernels: [budget][key]
-    int blocksShadowAny = 0, blocksTailLean = 0;
-    int blocksTailLockstep = 0; // kTailLockstep: the lean tail of lone renders, 128-thread blocks
+    int blocksShadowAny = 0;
+    int blocksTailLockstep[2] = {}; // kTailLockstep<LEAN>: [0] full, [1] lean shading; 128-thread blocks
     int blocksIntersectMode[10] = {}; // per TraceMode
     size_t waveSlots = pe_dev::kDefaultWaveSlots; // pe_tuning::wave_slots: paths in flight per regenerating wave
     size_t laneSlots = 0;                 // slots of path state allocated per lane (>= capacity, waveSlots)

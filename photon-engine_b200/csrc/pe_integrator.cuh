@@ -1317,12 +1317,12 @@ __global__ void __launch_bounds__(128, MINB) kShadeKey(SceneGPU S, Paths P, Wave
 // Once a wave's live queue fits in one resident grid, per-bounce launches cost more than they
 // save: each thread takes a path from the queue, alternates closest-hit queries with shadeSlot
 // (shadow rays inline) until the path ends, then takes the next.  The arithmetic and the order of
-// L's terms are the wavefront's, so the film is the same bit for bit.
-// One warp per block: a block retires as soon as its own 32 paths end, handing its registers to
-// the next wave running on the other lane.
+// L's terms are the wavefront's, so the film is the same bit for bit.  This one-warp-per-block
+// form serves the counting pass and waves with AOV or pass outputs; plain waves and the request
+// server's sweeps and drains use kTailLockstep below.
 constexpr int kTailBlock = 32;
 
-template <bool COUNT, bool OUT, bool LEAN = false>
+template <bool COUNT, bool OUT>
 __global__ void __launch_bounds__(kTailBlock) kTail(SceneGPU S, Paths P, Wave W, const int32_t* queue, const uint32_t* count,
                                              uint32_t* cursor, unsigned long long* stats) {
     const int n = static_cast<int>(*count);
@@ -1344,7 +1344,7 @@ __global__ void __launch_bounds__(kTailBlock) kTail(SceneGPU S, Paths P, Wave W,
                                               1e30f, nodes, tris, nullptr, pathTime(S, P, slot));
             ++rays;
             P.hit[slot] = make_float4(h.t, h.u, h.v, __int_as_float(h.prim));
-            if (!shadeSlot<true, COUNT, OUT, LEAN ? -2 : -1>(S, P, A, slot, path, shNodes, shTris, shRays)) break;
+            if (!shadeSlot<true, COUNT, OUT>(S, P, A, slot, path, shNodes, shTris, shRays)) break;
         }
     }
     if (COUNT) {
@@ -1357,7 +1357,7 @@ __global__ void __launch_bounds__(kTailBlock) kTail(SceneGPU S, Paths P, Wave W,
     atomicAdd(&stats[6], static_cast<unsigned long long>(shRays));
 }
 
-// The lean tail of a lone render in lockstep: the same per-path work as kTail<…, LEAN>, but the
+// The tail in lockstep: the same per-path work as kTail<false, false, LEAN>, but the
 // four warps of a 128-thread block meet at a barrier between each bounce's closest-hit query and
 // its shading, so the warps sharing an SM run the same phase's code at once.  The loop body
 // (traversal, every lean material's shading, the inline shadow ray) is far larger than an SM
@@ -1366,6 +1366,7 @@ __global__ void __launch_bounds__(kTailBlock) kTail(SceneGPU S, Paths P, Wave W,
 // the queue's next path at the top of the loop; the block leaves when none of its threads holds
 // one.  Each path's queries and terms are kTail's, so the film is the same bit for bit.
 constexpr int kTailLockstepBlock = 128;
+template <bool LEAN>
 __global__ void __launch_bounds__(kTailLockstepBlock) kTailLockstep(SceneGPU S, Paths P, Wave W, const int32_t* queue,
                                                                   const uint32_t* count, uint32_t* cursor,
                                                                   unsigned long long* stats) {
@@ -1397,7 +1398,7 @@ __global__ void __launch_bounds__(kTailLockstepBlock) kTailLockstep(SceneGPU S, 
         }
         __syncthreads();
         if (slot >= 0) {
-            if (!shadeSlot<true, false, false, -2>(S, P, *A, slot, path, shNodes, shTris, shRays)) {
+            if (!shadeSlot<true, false, false, LEAN ? -2 : -1>(S, P, *A, slot, path, shNodes, shTris, shRays)) {
                 slot = -1;
             } else if (++q >= kMaxPathQueries) {
                 // as kTail: a path past the per-path query bound is ended and reported

@@ -260,7 +260,7 @@ def run_ours(args):
         # fixed knobs instead of the autotuner (for profiler runs, whose timings the tuner cannot trust)
         knobs = [int(v) for v in args.tuning.split(",")]
         closest, anyhit, budget, tail = knobs[:4]
-        slots = knobs[4] if len(knobs) > 4 else 1 << 22
+        slots = knobs[4] if len(knobs) > 4 else 1 << 23
         dev.set_tuning(tail_paths=tail, closest_traversal=closest, shade_budget=budget, any_traversal=anyhit,
                        wave_slots=slots)
         tune_log = "fixed by --tuning"

@@ -506,11 +506,11 @@ typedef struct pe_tuning {
     int32_t any_traversal;     /* plain any-hit shadows: 0 the stack in local memory, 1 its top 4
                                   entries in registers, 2 (default) capped at 64 registers */
     int64_t wave_slots;        /* paths in flight in a regenerating wave (unguided renders without
-                                  AOV or pass targets): 2^20 … 2^23, default 2^22; 0 on input keeps
+                                  AOV or pass targets): 2^20 … 2^23, default 2^23; 0 on input keeps
                                   the current value.  Each of the device's two lanes holds path
                                   state for that many paths (536 B a slot, 256 B of it the radiance
-                                  of the paths the slots cycle through: 4.5 GB for both lanes at
-                                  2^22), allocated at the next render and never shrunk */
+                                  of the paths the slots cycle through: 9 GB for both lanes at
+                                  2^23), allocated at the next render and never shrunk */
 } pe_tuning;
 int32_t pe_device_get_tuning(pe_device* d, pe_tuning* out);
 int32_t pe_device_set_tuning(pe_device* d, const pe_tuning* t);

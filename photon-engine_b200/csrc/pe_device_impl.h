@@ -38,7 +38,7 @@ constexpr int kFilterSlots = 16;
 constexpr int kMaxSegs = 64;                    // requests sharing one wave
 constexpr size_t kWaveSlots = size_t(1) << 21;  // paths in flight per wave (guided, AOV and pass waves; servers)
 // Paths in flight per regenerating wave (pe_tuning::wave_slots): the default, and the range
-constexpr size_t kDefaultWaveSlots = size_t(1) << 22;
+constexpr size_t kDefaultWaveSlots = size_t(1) << 23;
 constexpr size_t kMinWaveSlots = size_t(1) << 20;
 constexpr size_t kMaxWaveSlots = size_t(1) << 23;
 // Live paths at or below which a guided wave hands its last paths to the tail kernel.

@@ -1125,7 +1125,7 @@ class CudaDevice:
                 "wave_slots": int(t.wave_slots)}
 
     def set_tuning(self, tail_paths: int = -1, closest_traversal: int = 6, shade_budget: int = 1, any_traversal: int = 2,
-                   wave_slots: int = 1 << 22):
+                   wave_slots: int = 1 << 23):
         capi.check(_lib().pe_device_set_tuning(self._h, C.byref(capi.pe_tuning(tail_paths, closest_traversal,
                                                                                 shade_budget, any_traversal,
                                                                                 wave_slots))))
